@@ -1,0 +1,108 @@
+"""ctypes binding of libaeolus_b200.so (the C-ABI of include/aeolus_b200.h).
+
+The library is built in-tree (aeolus_b200/lib/libaeolus_b200.so, see
+`aeolus_b200.build`).  There is no fallback: if the library is missing or
+a symbol is absent, loading raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libaeolus_b200.so")
+
+# every entry point include/aeolus_b200.h declares
+SYMBOLS = (
+    "aeo_create", "aeo_destroy", "aeo_set_field", "aeo_get_field", "aeo_step_rk3", "aeo_step_euler",
+    "aeo_pressure_solve", "aeo_project", "aeo_kinetic_energy", "aeo_max_divergence", "aeo_step_rk3_async",
+    "aeo_synchronize", "aeo_profile_step", "aeo_launches_per_step", "aeo_stream", "aeo_fill_uniform", "aeo_last_error",
+    "aeo_version",
+)
+
+
+class AeoConfig(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("hx", C.c_int32), ("hy", C.c_int32), ("hz", C.c_int32),
+        ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double),
+        ("x0", C.c_double), ("y0", C.c_double), ("z0", C.c_double),
+        ("bc_x", C.c_int32), ("bc_y", C.c_int32), ("bc_z", C.c_int32),
+        ("stretched", C.c_int32), ("core", C.c_int32), ("advection", C.c_int32),
+        ("solver", C.c_int32), ("precision", C.c_int32),
+        ("nu", C.c_double), ("theta0", C.c_double), ("g", C.c_double), ("f_coriolis", C.c_double),
+        ("c_s", C.c_double), ("pr_t", C.c_double), ("flux_bot", C.c_double), ("flux_top", C.c_double),
+        ("sponge_alpha", C.c_double), ("sponge_zstart", C.c_double),
+        ("device", C.c_int32),
+    ]
+
+
+_lib = None
+
+KERNEL_CLASSES = ("sgs", "sweep", "div_fftx", "ffty", "zsolve", "ifftx", "correct", "halo")
+
+STATUS = {0: "ok", 1: "argument", 2: "cuda", 3: "numerical", 4: "state"}
+
+
+class AeolusError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"aeolus_b200 [{STATUS.get(status, status)}]: {msg}")
+        self.status = status
+
+
+class NumericalFailure(AeolusError):
+    """Non-finite state or failed solve (the reference's NumericalFailure,
+    src/TimeIntegration.jl:610)."""
+
+
+def load():
+    """Load the shared library (raises when it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libaeolus_b200.so not built: {LIB_PATH} is missing (run aeolus_b200.build())")
+    lib = C.CDLL(LIB_PATH)
+    for s in SYMBOLS:
+        if not hasattr(lib, s):
+            raise ImportError(f"libaeolus_b200.so lacks the symbol {s}")
+    P = C.c_void_p
+    D = C.POINTER(C.c_double)
+    lib.aeo_create.argtypes = [C.POINTER(AeoConfig), D, D, D, D, C.POINTER(P)]
+    lib.aeo_destroy.argtypes = [P]
+    lib.aeo_set_field.argtypes = [P, C.c_int32, D]
+    lib.aeo_get_field.argtypes = [P, C.c_int32, D]
+    lib.aeo_step_rk3.argtypes = [P, C.c_double, C.c_int32]
+    lib.aeo_step_rk3_async.argtypes = [P, C.c_double, C.c_int32]
+    lib.aeo_step_euler.argtypes = [P, C.c_double, C.c_int32]
+    lib.aeo_synchronize.argtypes = [P]
+    lib.aeo_pressure_solve.argtypes = [P, D, D]
+    lib.aeo_project.argtypes = [P]
+    lib.aeo_kinetic_energy.argtypes = [P, D]
+    lib.aeo_max_divergence.argtypes = [P, D]
+    lib.aeo_profile_step.argtypes = [P, C.c_double, D, C.c_int32]
+    lib.aeo_launches_per_step.argtypes = [P, C.POINTER(C.c_int32)]
+    lib.aeo_stream.argtypes = [P]
+    lib.aeo_stream.restype = C.c_void_p
+    lib.aeo_fill_uniform.argtypes = [P, C.c_int32, C.c_uint64, C.c_uint32, C.c_double, C.c_int32]
+    lib.aeo_last_error.argtypes = [P]
+    lib.aeo_last_error.restype = C.c_char_p
+    lib.aeo_version.restype = C.c_char_p
+    for s in SYMBOLS:
+        f = getattr(lib, s)
+        if s not in ("aeo_stream", "aeo_last_error", "aeo_version"):
+            f.restype = C.c_int32
+    _lib = lib
+    return lib
+
+
+def check(status: int, handle=None):
+    if status == 0:
+        return
+    lib = load()
+    msg = lib.aeo_last_error(handle).decode(errors="replace")
+    if status == 3:
+        raise NumericalFailure(status, msg)
+    if status == 1:
+        raise ValueError(f"aeolus_b200: {msg}")
+    raise AeolusError(status, msg)

@@ -1,0 +1,110 @@
+"""Seeded synthetic inputs of the benchmark cases.
+
+All noise comes from the counter-based Philox4x32-10 generator the reference
+uses for reproducible streams (`philox4x32`, `counter_rng`,
+src/Backends.jl:1607-1739): key = (seed >> 32, seed), counter =
+(block 0, stream, id lo, id hi) with id the interior linear cell index
+(x fastest) and stream a field number, and the first 64-bit draw
+x1 << 32 | x0 mapped to [0, 1) by its top 53 bits.  The same numbers come
+from `aeo_fill_uniform` on the device.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .grids import Grid
+
+_M0 = np.uint64(0xD2511F53)
+_M1 = np.uint64(0xCD9E8D57)
+_W0 = np.uint32(0x9E3779B9)
+_W1 = np.uint32(0xBB67AE85)
+_MASK = np.uint64(0xFFFFFFFF)
+
+STREAM_U, STREAM_V, STREAM_W, STREAM_THETA = 0, 1, 2, 3
+
+
+def philox4x32(ctr, key):
+    """Philox4x32-10 block function on arrays (src/Backends.jl:1621-1636).
+    ctr: 4 uint32 arrays (or scalars), key: 2 uint32 values."""
+    c0, c1, c2, c3 = (np.asarray(c, dtype=np.uint32) for c in ctr)
+    k0 = np.uint32(key[0])
+    k1 = np.uint32(key[1])
+    with np.errstate(over="ignore"):
+        for r in range(10):
+            p0 = _M0 * c0.astype(np.uint64)
+            p1 = _M1 * c2.astype(np.uint64)
+            hi0 = (p0 >> np.uint64(32)).astype(np.uint32)
+            lo0 = (p0 & _MASK).astype(np.uint32)
+            hi1 = (p1 >> np.uint64(32)).astype(np.uint32)
+            lo1 = (p1 & _MASK).astype(np.uint32)
+            c0, c1, c2, c3 = hi1 ^ c1 ^ k0, lo1, hi0 ^ c3 ^ k1, lo0
+            if r < 9:
+                k0 = np.uint32((int(k0) + int(_W0)) & 0xFFFFFFFF)
+                k1 = np.uint32((int(k1) + int(_W1)) & 0xFFFFFFFF)
+    return c0, c1, c2, c3
+
+
+def philox_uniform(seed: int, stream: int, n: int) -> np.ndarray:
+    """U[0, 1) draws of the streams (seed, stream, id) for id in 0..n-1."""
+    seed &= (1 << 64) - 1
+    ids = np.arange(n, dtype=np.uint64)
+    ctr = (np.zeros(n, np.uint32), np.full(n, stream, np.uint32), (ids & _MASK).astype(np.uint32),
+           (ids >> np.uint64(32)).astype(np.uint32))
+    x0, x1, _, _ = philox4x32(ctr, (seed >> 32, seed & 0xFFFFFFFF))
+    x = (x1.astype(np.uint64) << np.uint64(32)) | x0.astype(np.uint64)
+    return (x >> np.uint64(11)).astype(np.float64) * (2.0 ** -53)
+
+
+def uniform_noise(grid: Grid, seed: int, stream: int, amp: float) -> np.ndarray:
+    """amp*(2U-1) on the interior, shape (Nz, Ny, Nx)."""
+    u = philox_uniform(seed, stream, grid.ncells)
+    return (amp * (2.0 * u - 1.0)).reshape(grid.nz, grid.ny, grid.nx)
+
+
+def embed(grid: Grid, interior: np.ndarray) -> np.ndarray:
+    """A storage array (zero halos) holding `interior` (Nz, Ny, Nx)."""
+    a = grid.zeros()
+    a[grid.interior] = interior
+    return a
+
+
+def taylor_green(grid: Grid, seed: int = 1, amp: float = 1e-3):
+    """Taylor-Green vortex u = sin x cos y cos z, v = -cos x sin y cos z, w = 0,
+    each at its face position, plus seeded uniform noise of amplitude `amp`
+    on u, v, w; theta passive with zero mean (uniform noise, mean removed).
+    Returns storage arrays (u, v, w, theta)."""
+    xc, yc, zc = grid.xnodes("c"), grid.ynodes("c"), grid.znodes("c")
+    xf, yf = grid.xnodes("fx"), grid.ynodes("fy")
+    Z, Y, X = np.meshgrid(zc, yc, xf, indexing="ij")
+    u = np.sin(X) * np.cos(Y) * np.cos(Z)
+    Z, Y, X = np.meshgrid(zc, yf, xc, indexing="ij")
+    v = -np.cos(X) * np.sin(Y) * np.cos(Z)
+    w = np.zeros((grid.nz, grid.ny, grid.nx))
+    if amp != 0:
+        u = u + uniform_noise(grid, seed, STREAM_U, amp)
+        v = v + uniform_noise(grid, seed, STREAM_V, amp)
+        w = w + uniform_noise(grid, seed, STREAM_W, amp)
+    th = uniform_noise(grid, seed, STREAM_THETA, 1.0)
+    th = th - th.mean()
+    return embed(grid, u), embed(grid, v), embed(grid, w), embed(grid, th)
+
+
+def cbl_theta_profile(z: np.ndarray, theta_ml: float = 300.0, z_inv: float = 1000.0, jump: float = 3.0,
+                      lapse: float = 3e-3) -> np.ndarray:
+    """Dry convective boundary layer: theta_ml up to z_inv, then a jump and a
+    constant lapse rate above."""
+    z = np.asarray(z, dtype=np.float64)
+    return np.where(z < z_inv, theta_ml, theta_ml + jump + lapse * (z - z_inv))
+
+
+def cbl_initial(grid: Grid, seed: int = 1, noise: float = 0.1, noise_levels: int = 10):
+    """Rest state with the CBL theta profile and seeded uniform +-noise in the
+    lowest `noise_levels` levels.  Returns (u, v, w, theta) storage arrays and
+    the interior theta profile."""
+    prof = cbl_theta_profile(grid.znodes("c"))
+    th = np.broadcast_to(prof[:, None, None], (grid.nz, grid.ny, grid.nx)).copy()
+    nz_noise = min(noise_levels, grid.nz)
+    pert = uniform_noise(grid, seed, STREAM_THETA, noise)
+    th[:nz_noise] += pert[:nz_noise]
+    z = np.zeros((grid.nz, grid.ny, grid.nx))
+    return embed(grid, z), embed(grid, z), embed(grid, z), embed(grid, th), prof

@@ -1,0 +1,213 @@
+"""The host-side mirror of the reference's step-core interface.
+
+`Simulation` holds one domain on a B200 through the C-ABI.  Its methods are
+the reference's operations on a `BoussinesqSimulation`
+(src/Simulations.jl:168-246) or a sound-proof simulation
+(src/Anelastic.jl:1559): `step_rk3` (`step_rk3!`, src/Simulations.jl:843),
+`step` (`step!`, :481), `kinetic_energy` (:992), `max_divergence` (:1045)
+and the pressure-solver seam `pressure_solve` (`solve!`,
+src/PressureSolvers.jl:41-80).  Fields move as the reference's `Field.data`
+storage arrays (numpy shape (Nz+2Hz, Ny+2Hy, Nx+2Hx), Float64).
+
+Errors follow the reference: a bad argument raises ValueError (ArgumentError),
+a non-finite state after a step raises NumericalFailure.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from .grids import PERIODIC, WALL, Grid
+from .reference_state import anelastic_profiles
+from .spec import ADVECTION, CORES, FIELDS, PRECISIONS, SOLVERS, CoreSpec
+
+_D = C.POINTER(C.c_double)
+
+
+def _ptr(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    return a.ctypes.data_as(_D)
+
+
+class Simulation:
+    def __init__(self, spec: CoreSpec, device: int = 0):
+        self.spec = spec
+        self.grid = spec.grid
+        lib = _lib.load()
+        g = spec.grid
+        cfg = _lib.AeoConfig()
+        cfg.nx, cfg.ny, cfg.nz = g.size
+        cfg.hx, cfg.hy, cfg.hz = g.halo
+        cfg.lx, cfg.ly, cfg.lz = g.extent
+        cfg.x0, cfg.y0, cfg.z0 = g.origin
+        cfg.bc_x = cfg.bc_y = 0
+        cfg.bc_z = 0 if g.bc_z == PERIODIC else 1
+        cfg.stretched = 1 if g.stretched else 0
+        cfg.core = CORES[spec.core]
+        cfg.advection = ADVECTION[spec.advection]
+        cfg.solver = SOLVERS[spec.solver]
+        cfg.precision = PRECISIONS[spec.precision]
+        cfg.nu, cfg.theta0, cfg.g, cfg.f_coriolis = spec.nu, spec.theta0, spec.g, spec.f_coriolis
+        cfg.c_s, cfg.pr_t = spec.c_s, spec.pr_t
+        cfg.flux_bot, cfg.flux_top = spec.flux_bot, spec.flux_top
+        cfg.sponge_alpha, cfg.sponge_zstart = spec.sponge_alpha, spec.sponge_zstart
+        cfg.device = device
+        self._keep = [spec.grid.zf, spec.wc, spec.wf, spec.thf]
+        h = C.c_void_p()
+        st = lib.aeo_create(C.byref(cfg), _ptr(g.zf), _ptr(spec.wc), _ptr(spec.wf), _ptr(spec.thf), C.byref(h))
+        _lib.check(st, None)
+        self._h = h
+        self._lib = lib
+
+    # ---- lifecycle ------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.aeo_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---- fields ---------------------------------------------------------------
+    def set_field(self, name: str, data: np.ndarray):
+        a = np.ascontiguousarray(data, dtype=np.float64)
+        if a.shape != self.grid.storage_shape:
+            raise ValueError(f"{name}: expected storage shape {self.grid.storage_shape}, got {a.shape}")
+        _lib.check(self._lib.aeo_set_field(self._h, FIELDS[name], _ptr(a)), self._h)
+
+    def get_field(self, name: str, out: Optional[np.ndarray] = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.grid.storage_shape)
+        _lib.check(self._lib.aeo_get_field(self._h, FIELDS[name], _ptr(out)), self._h)
+        return out
+
+    def set_state(self, u, v, w, theta):
+        self.set_field("u", u)
+        self.set_field("v", v)
+        self.set_field("w", w)
+        self.set_field("theta", theta)
+
+    def get_state(self):
+        return tuple(self.get_field(n) for n in ("u", "v", "w", "theta"))
+
+    def fill_uniform(self, name: str, seed: int, stream: int, amp: float, add: bool = False):
+        _lib.check(self._lib.aeo_fill_uniform(self._h, FIELDS[name], seed, stream, amp, 1 if add else 0), self._h)
+
+    # ---- stepping ---------------------------------------------------------------
+    def step_rk3(self, dt: float, nsteps: int = 1):
+        _lib.check(self._lib.aeo_step_rk3(self._h, float(dt), int(nsteps)), self._h)
+
+    def step_rk3_async(self, dt: float, nsteps: int = 1):
+        _lib.check(self._lib.aeo_step_rk3_async(self._h, float(dt), int(nsteps)), self._h)
+
+    def synchronize(self):
+        _lib.check(self._lib.aeo_synchronize(self._h), self._h)
+
+    def step(self, dt: float, nsteps: int = 1):
+        _lib.check(self._lib.aeo_step_euler(self._h, float(dt), int(nsteps)), self._h)
+
+    def project(self):
+        """One Chorin projection of the current velocity (dt = 1)."""
+        _lib.check(self._lib.aeo_project(self._h), self._h)
+
+    # ---- solver seam and diagnostics ------------------------------------------
+    def pressure_solve(self, src: np.ndarray) -> np.ndarray:
+        g = self.grid
+        s = np.ascontiguousarray(src, dtype=np.float64)
+        if s.shape != (g.nz, g.ny, g.nx):
+            raise ValueError(f"source must have the interior shape {(g.nz, g.ny, g.nx)}")
+        out = np.empty_like(s)
+        _lib.check(self._lib.aeo_pressure_solve(self._h, _ptr(s), _ptr(out)), self._h)
+        return out
+
+    def kinetic_energy(self) -> float:
+        v = C.c_double()
+        _lib.check(self._lib.aeo_kinetic_energy(self._h, C.byref(v)), self._h)
+        return v.value
+
+    def max_divergence(self) -> float:
+        v = C.c_double()
+        _lib.check(self._lib.aeo_max_divergence(self._h, C.byref(v)), self._h)
+        return v.value
+
+    def profile_step(self, dt: float) -> dict:
+        """One RK3 step launch by launch with CUDA events between kernel
+        groups: device milliseconds per kernel class (advances the state)."""
+        n = len(_lib.KERNEL_CLASSES)
+        buf = (C.c_double * n)()
+        _lib.check(self._lib.aeo_profile_step(self._h, float(dt), buf, n), self._h)
+        return {k: buf[i] for i, k in enumerate(_lib.KERNEL_CLASSES)}
+
+    def launches_per_step(self) -> int:
+        v = C.c_int32()
+        _lib.check(self._lib.aeo_launches_per_step(self._h, C.byref(v)), self._h)
+        return v.value
+
+    @property
+    def stream(self) -> int:
+        return self._lib.aeo_stream(self._h)
+
+
+def boussinesq_simulation(grid: Grid, *, nu=0.0, theta0=0.0, g=9.81, f_coriolis=0.0, c_s=0.0, pr_t=1 / 3,
+                          flux_bot=0.0, flux_top=0.0, sponge_alpha=0.0, sponge_zstart=None,
+                          advection="centred", precision="fp64", solver=None, device=0) -> Simulation:
+    """`BoussinesqSimulation(mesh; ν, θ₀, g_accel, f_coriolis, C_s, Pr_t,
+    θ_flux_bottom, θ_flux_top, sponge_α_max, sponge_z_start)`
+    (src/Simulations.jl:232-246) on the B200."""
+    spec = CoreSpec(grid=grid, core="boussinesq", advection=advection, solver=solver, precision=precision,
+                    nu=nu, theta0=theta0, g=g, f_coriolis=f_coriolis, c_s=c_s, pr_t=pr_t, flux_bot=flux_bot,
+                    flux_top=flux_top, sponge_alpha=sponge_alpha, sponge_zstart=sponge_zstart)
+    return Simulation(spec, device)
+
+
+def anelastic_spec(grid: Grid, rho_c, theta_c, **kw) -> CoreSpec:
+    prof = anelastic_profiles(grid, rho_c, theta_c)
+    return CoreSpec(grid=grid, core="anelastic", wc=prof["wc"], wf=prof["wf"], thf=prof["thf"], **kw)
+
+
+def anelastic_simulation(grid: Grid, rho_c, theta_c, *, nu=0.0, g=9.81, f_coriolis=0.0, c_s=0.0, pr_t=1 / 3,
+                         flux_bot=0.0, flux_top=0.0, sponge_alpha=0.0, sponge_zstart=None, precision="fp64",
+                         device=0) -> Simulation:
+    """The anelastic (W = rho_bar) sound-proof core (src/Anelastic.jl:1559,
+    :1791-1948) with the direct FFT-tridiagonal weighted solver
+    (DirectWeightedPoissonSolver, src/Anelastic.jl:987-1021)."""
+    spec = anelastic_spec(grid, rho_c, theta_c, nu=nu, g=g, f_coriolis=f_coriolis, c_s=c_s, pr_t=pr_t,
+                          flux_bot=flux_bot, flux_top=flux_top, sponge_alpha=sponge_alpha,
+                          sponge_zstart=sponge_zstart, precision=precision)
+    return Simulation(spec, device)
+
+
+# reference-named free functions
+def step_rk3(sim: Simulation, dt: float, nsteps: int = 1):
+    sim.step_rk3(dt, nsteps)
+    return sim
+
+
+def step(sim: Simulation, dt: float, nsteps: int = 1):
+    sim.step(dt, nsteps)
+    return sim
+
+
+def kinetic_energy(sim: Simulation) -> float:
+    return sim.kinetic_energy()
+
+
+def max_divergence(sim: Simulation) -> float:
+    return sim.max_divergence()

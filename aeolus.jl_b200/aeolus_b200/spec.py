@@ -1,0 +1,80 @@
+"""The description of one domain's dynamical core: grid + physics + solver.
+
+`CoreSpec` carries what the reference spreads over the constructor keywords
+of `BoussinesqSimulation` (src/Simulations.jl:232-246), the sound-proof
+simulation (src/Anelastic.jl:1559) and the TOML `[core]` / `[advection]` /
+`[sgs]` / pressure-solver sections (src/config/simulation_driver.jl:416-495).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from .grids import PERIODIC, WALL, Grid
+
+CORES = {"boussinesq": 0, "anelastic": 1}
+ADVECTION = {"centred": 0, "weno_js5": 1, "weno_z5": 2}
+SOLVERS = {"fft": 0, "column": 1}
+PRECISIONS = {"fp64": 0, "fp32_mixed": 1}
+FIELDS = {"u": 0, "v": 1, "w": 2, "theta": 3, "p": 4, "nut": 5}
+
+
+@dataclass
+class CoreSpec:
+    grid: Grid
+    core: str = "boussinesq"
+    advection: str = "centred"
+    solver: Optional[str] = None        # default: fft when z is periodic, else column
+    precision: str = "fp64"
+    nu: float = 0.0
+    theta0: float = 0.0
+    g: float = 9.81
+    f_coriolis: float = 0.0
+    c_s: float = 0.0
+    pr_t: float = 1.0 / 3.0
+    flux_bot: float = 0.0
+    flux_top: float = 0.0
+    sponge_alpha: float = 0.0
+    sponge_zstart: Optional[float] = None
+    wc: Optional[np.ndarray] = field(default=None, repr=False)
+    wf: Optional[np.ndarray] = field(default=None, repr=False)
+    thf: Optional[np.ndarray] = field(default=None, repr=False)
+
+    def __post_init__(self):
+        if self.core not in CORES:
+            raise ValueError(f"core must be one of {list(CORES)}, got {self.core!r}")
+        if self.advection not in ADVECTION:
+            raise ValueError(f"advection must be one of {list(ADVECTION)}, got {self.advection!r}")
+        if self.precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {list(PRECISIONS)}, got {self.precision!r}")
+        if self.solver is None:
+            # _default_solver, src/Simulations.jl:1137-1144
+            self.solver = "fft" if self.grid.bc_z == PERIODIC else "column"
+        if self.solver not in SOLVERS:
+            raise ValueError(f"solver must be one of {list(SOLVERS)}, got {self.solver!r}")
+        if self.sponge_zstart is None:
+            self.sponge_zstart = self.grid.origin[2] + self.grid.extent[2]
+        if self.core == "anelastic":
+            if self.wc is None or self.wf is None:
+                raise ValueError("the anelastic core needs the padded weights wc and wf")
+            if self.grid.bc_z != WALL:
+                raise ValueError("the anelastic core needs walls in z")
+            nzs = self.grid.nz + 2 * self.grid.halo[2]
+            self.wc = np.ascontiguousarray(self.wc, dtype=np.float64)
+            self.wf = np.ascontiguousarray(self.wf, dtype=np.float64)
+            if self.wc.shape != (nzs,) or self.wf.shape != (nzs + 1,):
+                raise ValueError(f"wc needs {nzs} and wf {nzs + 1} storage levels")
+            if self.thf is not None:
+                self.thf = np.ascontiguousarray(self.thf, dtype=np.float64)
+                if self.thf.shape != (nzs + 1,):
+                    raise ValueError(f"thf needs {nzs + 1} storage levels")
+        if self.advection != "centred":
+            if self.grid.stretched or self.core != "boussinesq":
+                raise ValueError("WENO advection is defined on a uniform Boussinesq grid "
+                                 "(momentum_advect_weno_z!, src/AdvectionSchemes.jl:1195)")
+            if min(self.grid.halo) < 3:
+                raise ValueError("WENO-5 needs halo >= 3 in every direction")
+        if self.c_s != 0 and not self.pr_t > 0:
+            raise ValueError("pr_t must be positive")

@@ -1,0 +1,130 @@
+// aeo_common.cuh -- layouts, metrics and small helpers shared by the kernels.
+//
+// Device layout.  The stencil inputs (the stage states u, v, w, theta and the
+// eddy viscosity) live in PADDED arrays: interior (nx, ny, nz) plus a halo of
+// AEO_H = 3 cells in y and z and an x offset of AEO_HX = 8 cells, so that
+// each interior row starts on a 32-byte sector for fp32 and fp64.  Index
+//   q(i, j, k) = (i + AEO_HX) + px * ((j + AEO_H) + py * (k + AEO_H)),
+//   px = nx + 2*AEO_HX, py = ny + 2*AEO_H,
+// with (i, j, k) interior coordinates that may step into the halo.  Halos hold
+// the values the reference's fill_halos! puts there
+// (src/boundary_conditions/halo_kernels.jl:100-140, x then y then z).
+// Everything else (predictor velocities, the potential, pressure, the
+// Poisson source) is interior-only, q = i + nx*(j + ny*k); kernels that read
+// its neighbours apply the boundary maps themselves.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define AEO_HX 8
+#define AEO_H 3
+#define AEO_LH 4   // offset of level k in the per-level metric vectors
+
+enum { LOC_C = 0, LOC_FX = 1, LOC_FY = 2, LOC_FZ = 3 };
+
+template <typename R>
+struct cplx {
+    R x, y;
+};
+
+template <typename R>
+__device__ __forceinline__ cplx<R> cmk(R a, R b) {
+    cplx<R> c;
+    c.x = a;
+    c.y = b;
+    return c;
+}
+template <typename R>
+__device__ __forceinline__ cplx<R> cadd(cplx<R> a, cplx<R> b) { return cmk<R>(a.x + b.x, a.y + b.y); }
+template <typename R>
+__device__ __forceinline__ cplx<R> csub(cplx<R> a, cplx<R> b) { return cmk<R>(a.x - b.x, a.y - b.y); }
+template <typename R>
+__device__ __forceinline__ cplx<R> cmul(cplx<R> a, cplx<R> b) {
+    return cmk<R>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename R>
+__device__ __forceinline__ cplx<R> cconj(cplx<R> a) { return cmk<R>(a.x, -a.y); }
+
+// Geometry of one domain, passed by value to every kernel.
+struct Geo {
+    int nx, ny, nz;
+    int px, py;            // padded row / plane extents
+    long long sy, sz;      // padded strides of j and k
+    long long nin;         // nx*ny*nz
+    int bc_z;              // 0 periodic, 1 wall
+    int uniform;           // 1: uniform z metrics
+    double dx, dy, dz;
+    double idx, idy, idx2, idy2, idz, idz2, delta_u;
+    // per-level vectors, entry (k + AEO_LH) for level k (interior 0-based)
+    const double* idzc;
+    const double* idzf;
+    const double* idz_off;
+    const double* wlo;
+    const double* whi;
+    const double* alo;
+    const double* ahi;
+    const double* delta;
+    const double* zc;
+    const double* zf;
+    // sound-proof weights (NULL for the Boussinesq core), same indexing
+    const double* wc;
+    const double* wf;
+    const double* thf;
+};
+
+__device__ __forceinline__ long long pidx(const Geo& g, int i, int j, int k) {
+    return (long long)(i + AEO_HX) + (long long)(j + AEO_H) * g.sy + (long long)(k + AEO_H) * g.sz;
+}
+__device__ __forceinline__ long long iidx(const Geo& g, int i, int j, int k) {
+    return (long long)i + (long long)g.nx * ((long long)j + (long long)g.ny * (long long)k);
+}
+__device__ __forceinline__ double lvl(const double* a, int k) { return __ldg(a + k + AEO_LH); }
+
+__device__ __forceinline__ int wrapi(int i, int n) {
+    i %= n;
+    return i < 0 ? i + n : i;
+}
+
+// The composite boundary map of the reference's halo fill for a point that
+// may lie outside the interior: periodic wrap in x and y; in z periodic wrap,
+// or for an ImpermeableWall the mirror (cell-centred and horizontal-face
+// fields) or the odd extension about the zero wall faces (w).  Returns the
+// multiplier: 1, -1 or 0 (the wall face itself).
+__device__ __forceinline__ int zmap(const Geo& g, int k, int loc, int* kk) {
+    if (g.bc_z == 0) {
+        *kk = wrapi(k, g.nz);
+        return 1;
+    }
+    if (loc != LOC_FZ) {
+        if (k < 0) k = -k - 1;
+        else if (k >= g.nz) k = 2 * g.nz - 1 - k;
+        *kk = k;
+        return 1;
+    }
+    if (k == 0 || k == g.nz) {
+        *kk = 0;
+        return 0;
+    }
+    if (k < 0) {
+        *kk = -k;
+        return -1;
+    }
+    if (k > g.nz) {
+        *kk = 2 * g.nz - k;
+        return -1;
+    }
+    *kk = k;
+    return 1;
+}
+
+template <typename R>
+__device__ __forceinline__ R ld_mapped_interior(const Geo& g, const R* __restrict__ a, int i, int j, int k, int loc) {
+    int kk;
+    int s = zmap(g, k, loc, &kk);
+    if (s == 0) return R(0);
+    R v = __ldg(a + iidx(g, wrapi(i, g.nx), wrapi(j, g.ny), kk));
+    return s > 0 ? v : -v;
+}
+
+#define AEO_CHECK_LAUNCH() ((void)0)

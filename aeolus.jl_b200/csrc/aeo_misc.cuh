@@ -1,0 +1,255 @@
+// aeo_misc.cuh -- halo fills, the projection's correction, host-layout
+// packing, reductions and the Philox input generator.
+#pragma once
+
+#include "aeo_common.cuh"
+
+// ---- halo fill of padded arrays (gather form) ------------------------------------
+// Every point of the AEO_H-wide shell around the interior takes the value of
+// the composite boundary map (zmap / wrap), which is what the reference's
+// axis-ordered fill (x, then y, then z) leaves there
+// (src/boundary_conditions/halo_kernels.jl:100-140, src/BoundaryConditions.jl:228-258).
+template <typename R>
+struct HaloSet {
+    R* f[5];
+    int loc[5];
+    int nf;
+};
+
+__device__ __forceinline__ void shell_point(const Geo& g, long long t, int* i, int* j, int* k) {
+    const int H = AEO_H;
+    const long long bx = g.nx + 2 * H, by = g.ny + 2 * H;
+    const long long nzs = 2LL * H * bx * by;          // the two z slabs
+    if (t < nzs) {
+        long long s = t;
+        *i = (int)(s % bx) - H; s /= bx;
+        *j = (int)(s % by) - H; s /= by;
+        int kz = (int)s;
+        *k = kz < H ? kz - H : g.nz + (kz - H);
+        return;
+    }
+    t -= nzs;
+    const long long nys = 2LL * H * bx * g.nz;        // the two y slabs (interior k)
+    if (t < nys) {
+        long long s = t;
+        *i = (int)(s % bx) - H; s /= bx;
+        int jy = (int)(s % (2 * H)); s /= (2 * H);
+        *j = jy < H ? jy - H : g.ny + (jy - H);
+        *k = (int)s;
+        return;
+    }
+    t -= nys;                                          // the two x slabs (interior j, k)
+    long long s = t;
+    int ix = (int)(s % (2 * H)); s /= (2 * H);
+    *i = ix < H ? ix - H : g.nx + (ix - H);
+    *j = (int)(s % g.ny); s /= g.ny;
+    *k = (int)s;
+}
+
+__host__ __device__ __forceinline__ long long shell_count(const Geo& g) {
+    const long long H = AEO_H, bx = g.nx + 2 * H, by = g.ny + 2 * H;
+    return 2 * H * bx * by + 2 * H * bx * g.nz + 2 * H * (long long)g.ny * g.nz;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) halo_fill_kernel(Geo g, HaloSet<R> hs) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= shell_count(g)) return;
+    int i, j, k;
+    shell_point(g, t, &i, &j, &k);
+    int ii = wrapi(i, g.nx), jj = wrapi(j, g.ny);
+    for (int f = 0; f < hs.nf; ++f) {
+        int kk;
+        int s = zmap(g, k, hs.loc[f], &kk);
+        R v = s == 0 ? R(0) : hs.f[f][pidx(g, ii, jj, kk)];
+        hs.f[f][pidx(g, i, j, k)] = s < 0 ? -v : v;
+    }
+}
+
+// The wall face of w (interior k = 0) is zero after every fill.
+template <typename R>
+__global__ void wall_face_zero_kernel(Geo g, R* w) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (i < g.nx) w[pidx(g, i, j, 0)] = R(0);
+}
+
+// ---- the projection's correction (src/FiniteVolume.jl:1823-1849) ---------------
+// u = c(u* - d(phi)/dx, u0) (likewise v, w), p = phi/dt; c(x, s) = ca*s + cb*x
+// in RK3 stages 2 and 3 (_Lin2r, src/Simulations.jl:1194-1198).
+template <typename R, bool UNI>
+__global__ void __launch_bounds__(256) correct_kernel(Geo g, const R* __restrict__ us, const R* __restrict__ vs,
+                                                      const R* __restrict__ ws, const R* __restrict__ phi,
+                                                      const R* u0, const R* v0,
+                                                      const R* w0, R* uo, R* vo,
+                                                      R* wo, R* __restrict__ p, R inv_dt, R ca, R cb,
+                                                      int stage) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+    const long long qi = iidx(g, i, j, k), qp = pidx(g, i, j, k);
+    R pc = __ldg(phi + qi);
+    R pw = ld_mapped_interior(g, phi, i - 1, j, k, LOC_C);
+    R ps = ld_mapped_interior(g, phi, i, j - 1, k, LOC_C);
+    R pb = ld_mapped_interior(g, phi, i, j, k - 1, LOC_C);
+    R idzf = UNI ? R(g.idz) : R(lvl(g.idzf, k));
+    R un = __ldg(us + qi) - (pc - pw) * R(g.idx);
+    R vn = __ldg(vs + qi) - (pc - ps) * R(g.idy);
+    R wn = __ldg(ws + qi) - (pc - pb) * idzf;
+    if (stage) {
+        un = ca * u0[qp] + cb * un;
+        vn = ca * v0[qp] + cb * vn;
+        wn = ca * w0[qp] + cb * wn;
+    }
+    uo[qp] = un;
+    vo[qp] = vn;
+    wo[qp] = wn;
+    p[qi] = pc * inv_dt;
+}
+
+// ---- host-layout packing ----------------------------------------------------------
+// Host storage (reference layout, halos hh) <-> device padded interior.
+template <typename R>
+__global__ void unpack_host_kernel(Geo g, const double* __restrict__ hsrc, int hx, int hy, int hz,
+                                   R* __restrict__ dst, int padded) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y, k = blockIdx.z;
+    if (i >= g.nx) return;
+    long long HX = g.nx + 2LL * hx, HY = g.ny + 2LL * hy;
+    double v = hsrc[(i + hx) + HX * ((j + hy) + HY * (long long)(k + hz))];
+    if (padded) dst[pidx(g, i, j, k)] = R(v);
+    else dst[iidx(g, i, j, k)] = R(v);
+}
+
+// Fill the whole host storage array from the device interior through the
+// composite boundary map (loc < 0: halos zero).
+template <typename R>
+__global__ void pack_host_kernel(Geo g, double* __restrict__ hdst, int hx, int hy, int hz,
+                                 const R* __restrict__ src, int padded, int loc) {
+    long long HX = g.nx + 2LL * hx, HY = g.ny + 2LL * hy, HZ = g.nz + 2LL * hz;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= HX * HY * HZ) return;
+    int i = (int)(t % HX) - hx;
+    int j = (int)((t / HX) % HY) - hy;
+    int k = (int)(t / (HX * HY)) - hz;
+    bool inside = i >= 0 && i < g.nx && j >= 0 && j < g.ny && k >= 0 && k < g.nz;
+    double v = 0.0;
+    if (inside || loc >= 0) {
+        int kk;
+        int s = inside ? 1 : zmap(g, k, loc, &kk);
+        if (inside) kk = k;
+        if (s != 0) {
+            int ii = inside ? i : wrapi(i, g.nx), jj = inside ? j : wrapi(j, g.ny);
+            R r = padded ? src[pidx(g, ii, jj, kk)] : src[iidx(g, ii, jj, kk)];
+            v = s > 0 ? (double)r : -(double)r;
+        }
+    }
+    hdst[t] = v;
+}
+
+// interior-sized double <-> interior R
+template <typename R>
+__global__ void convert_kernel(long long n, const double* __restrict__ a, R* __restrict__ b) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) b[t] = R(a[t]);
+}
+template <typename R>
+__global__ void convert_back_kernel(long long n, const R* __restrict__ a, double* __restrict__ b) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) b[t] = double(a[t]);
+}
+
+// ---- deterministic FP64 reductions --------------------------------------------------
+// Per-level partial sums, each level summed by one CTA in a fixed order,
+// then the levels in ascending k (the canonical plane sums of
+// src/Backends.jl:1349-1357; src/Simulations.jl:992-1014).
+template <typename R, bool UNI>
+__global__ void __launch_bounds__(256) ke_levels_kernel(Geo g, const R* __restrict__ u, const R* __restrict__ v,
+                                                        const R* __restrict__ w, double* __restrict__ part) {
+    __shared__ double red[256];
+    int k = blockIdx.x;
+    double acc = 0.0;
+    double dzc = UNI ? 1.0 : 1.0 / lvl(g.idzc, k), dzf = UNI ? 1.0 : 1.0 / lvl(g.idzf, k);
+    for (int e = threadIdx.x; e < g.nx * g.ny; e += blockDim.x) {
+        int i = e % g.nx, j = e / g.nx;
+        long long q = pidx(g, i, j, k);
+        double uu = u[q], vv = v[q], ww = w[q];
+        if (UNI) acc += uu * uu + vv * vv + ww * ww;
+        else acc += (uu * uu + vv * vv) * dzc + ww * ww * dzf;
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[k] = red[0];
+}
+
+template <typename R, bool ANEL, bool UNI>
+__global__ void __launch_bounds__(256) maxdiv_levels_kernel(Geo g, const R* __restrict__ u, const R* __restrict__ v,
+                                                            const R* __restrict__ w, double* __restrict__ part) {
+    __shared__ double red[256];
+    int k = blockIdx.x;
+    double acc = 0.0;
+    double idz = UNI ? g.idz : lvl(g.idzc, k);
+    for (int e = threadIdx.x; e < g.nx * g.ny; e += blockDim.x) {
+        int i = e % g.nx, j = e / g.nx;
+        long long q = pidx(g, i, j, k);
+        double du = ((double)u[q + 1] - (double)u[q]) * g.idx;
+        double dv = ((double)v[q + g.sy] - (double)v[q]) * g.idy;
+        double d;
+        if (ANEL) {
+            double wc = lvl(g.wc, k), wfb = lvl(g.wf, k), wft = lvl(g.wf, k + 1);
+            d = (wc * (du + dv) + (wft * (double)w[q + g.sz] - wfb * (double)w[q]) * idz) / wc;
+        } else {
+            d = du + dv + ((double)w[q + g.sz] - (double)w[q]) * idz;
+        }
+        acc = fmax(acc, fabs(d));
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[k] = red[0];
+}
+
+// non-finite check of the state (status word for the host)
+template <typename R>
+__global__ void finite_check_kernel(Geo g, const R* __restrict__ a, int* __restrict__ flag) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= g.nx) return;
+    R v = a[pidx(g, i, j, k)];
+    if (!isfinite((double)v)) atomicOr(flag, 1);
+}
+
+// ---- Philox4x32-10 (src/Backends.jl:1607-1640) ------------------------------------
+__device__ __forceinline__ void philox4x32(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 1; r <= 10; ++r) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c[0]), lo0 = 0xD2511F53u * c[0];
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]), lo1 = 0xCD9E8D57u * c[2];
+        uint32_t n0 = hi1 ^ c[1] ^ k0, n1 = lo1, n2 = hi0 ^ c[3] ^ k1, n3 = lo0;
+        c[0] = n0; c[1] = n1; c[2] = n2; c[3] = n3;
+        if (r < 10) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+    }
+}
+
+// out(interior id) = amp*(2U-1), U from the first 64-bit draw of stream
+// (seed, stream, id): its top 53 bits over 2^53.
+template <typename R>
+__global__ void philox_fill_kernel(Geo g, R* __restrict__ dst, int padded, uint64_t seed, uint32_t stream, double amp,
+                                   int add) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.nin) return;
+    uint32_t c[4] = {0u, stream, (uint32_t)t, (uint32_t)((unsigned long long)t >> 32)};
+    philox4x32(c, (uint32_t)(seed >> 32), (uint32_t)seed);
+    uint64_t x = ((uint64_t)c[1] << 32) | (uint64_t)c[0];
+    double u01 = (double)(x >> 11) * 0x1.0p-53;
+    double val = amp * (2.0 * u01 - 1.0);
+    int i = (int)(t % g.nx), j = (int)((t / g.nx) % g.ny), k = (int)(t / ((long long)g.nx * g.ny));
+    long long q = padded ? pidx(g, i, j, k) : t;
+    dst[q] = add ? R((double)dst[q] + val) : R(val);
+}

@@ -1,0 +1,423 @@
+// aeo_sweep.cuh -- the fused tendency + predictor sweep of one RK3 substage.
+//
+// One launch computes, per interior cell, the tendencies of u, v, w and theta
+// (advection, molecular diffusion, Smagorinsky SGS, buoyancy, Coriolis, wall
+// fluxes, sponge) and writes the predictor u* = u + dt*t (interior-only
+// arrays) and the updated, stage-combined theta (padded array).  It restates
+// the reference's substage passes, src/Simulations.jl:548-620 (Boussinesq)
+// and src/Anelastic.jl:1809-1849 (sound-proof), whose point bodies are
+//   centred momentum   src/FiniteVolume.jl:730-797 (_mom_u/v/w_at)
+//   centred scalar     src/FiniteVolume.jl:1682-1693 (_adv_centered_at)
+//   W-weighted forms   src/Anelastic.jl:1193-1306 (_wmom_u/v/w, _wscal)
+//   WENO-JS5 / WENO-Z5 src/AdvectionSchemes.jl:240-255, :319-333, :623-699,
+//                      :1203-1256 (_b_recon!, _b_mrecon_u/v/w!)
+//   Laplacian          src/FiniteVolume.jl:271-280 (_lap_at)
+//   Smagorinsky        src/FiniteVolume.jl:936-944, src/Operators.jl:451-496
+//   eddy viscosity     src/FiniteVolume.jl:969-1042, :1280-1300, :1473-1492
+//   buoyancy           src/FiniteVolume.jl:838-858, src/Anelastic.jl:1343-1350
+//   wall fluxes        src/FiniteVolume.jl:417-440
+//   sponge             src/FiniteVolume.jl:578-702
+//   predictor / stage  src/Simulations.jl:690-694, :1182-1198
+#pragma once
+
+#include "aeo_common.cuh"
+
+template <typename R>
+struct SweepArgs {
+    Geo g;
+    const R* u;
+    const R* v;
+    const R* w;
+    const R* th;
+    const R* nut;   // padded eddy viscosity (SGS only)
+    const R* th0;   // padded step-start theta (stages 2, 3)
+    R* us;          // interior predictor velocities
+    R* vs;
+    R* ws;
+    R* th_out;      // padded
+    R dt, ca, cb;
+    int stage;
+    R nu, gacc, theta0, fcor, inv_prt, pr_t, flux_bot, flux_top, sp_alpha, sp_zstart, sp_inv;
+};
+
+// ---- metric accessors (src/FiniteVolume.jl:146-186) -----------------------
+template <typename R, bool UNI>
+struct Met {
+    const Geo& g;
+    __device__ Met(const Geo& gg) : g(gg) {}
+    __device__ __forceinline__ R idz(int k) const { return UNI ? R(g.idz) : R(lvl(g.idzc, k)); }
+    __device__ __forceinline__ R idzf(int k) const { return UNI ? R(g.idz) : R(lvl(g.idzf, k)); }
+    __device__ __forceinline__ R idz_off(int k) const { return UNI ? R(g.idz) : R(lvl(g.idz_off, k)); }
+    __device__ __forceinline__ R zface(int k, R lo, R hi) const {
+        return UNI ? R(0.5) * (lo + hi) : R(lvl(g.wlo, k)) * lo + R(lvl(g.whi, k)) * hi;
+    }
+    __device__ __forceinline__ R zflux(int k, R lo, R hi) const {
+        return UNI ? R(0.5) * (lo + hi) : R(lvl(g.alo, k)) * lo + R(lvl(g.ahi, k)) * hi;
+    }
+    __device__ __forceinline__ R lapz(int loc, int k, R fm, R c, R fp) const {
+        if (UNI) return (fp - R(2) * c + fm) * R(g.idz2);
+        if (loc == LOC_FZ) return ((fp - c) * R(lvl(g.idzc, k)) - (c - fm) * R(lvl(g.idzc, k - 1))) * R(lvl(g.idzf, k));
+        return ((fp - c) * R(lvl(g.idzf, k + 1)) - (c - fm) * R(lvl(g.idzf, k))) * R(lvl(g.idzc, k));
+    }
+    __device__ __forceinline__ R filter(int k) const { return UNI ? R(g.delta_u) : R(lvl(g.delta, k)); }
+};
+
+// padded-array accessor around the thread's point
+template <typename R>
+struct Nb {
+    const R* __restrict__ p;
+    long long sy, sz;
+    __device__ __forceinline__ R operator()(int di, int dj, int dk) const {
+        return __ldg(p + di + (long long)dj * sy + (long long)dk * sz);
+    }
+};
+
+// ---- WENO reconstructions (src/AdvectionSchemes.jl:105-120, :240-255, :319-333)
+template <typename R>
+__device__ __forceinline__ R beta3(R a1, R a2) { return a1 * a1 + R(13.0 / 3.0) * (a2 * a2); }
+
+template <typename R, int ADV>
+__device__ __forceinline__ R weno5_left(R v1, R v2, R v3, R v4, R v5) {
+    R q0 = (R(2) * v1 - R(7) * v2 + R(11) * v3) / R(6);
+    R q1 = (-v2 + R(5) * v3 + R(2) * v4) / R(6);
+    R q2 = (R(2) * v3 + R(5) * v4 - v5) / R(6);
+    R d2a = (v1 - R(2) * v2 + v3) / R(2);
+    R d2b = (v2 - R(2) * v3 + v4) / R(2);
+    R d2c = (v3 - R(2) * v4 + v5) / R(2);
+    R b0 = beta3<R>((v1 - R(4) * v2 + R(3) * v3) / R(2), d2a);
+    R b1 = beta3<R>((v4 - v2) / R(2), d2b);
+    R b2 = beta3<R>((R(-3) * v3 + R(4) * v4 - v5) / R(2), d2c);
+    R a0, a1, a2;
+    if (ADV == 2) {  // WENO-Z5, p = 2, eps = eps(T)^2
+        const R eps = sizeof(R) == 8 ? R(4.930380657631324e-32) : R(1.4210854715202004e-14);
+        R tau = fabs(b0 - b2);
+        R t0 = tau / (b0 + eps), t1 = tau / (b1 + eps), t2 = tau / (b2 + eps);
+        a0 = R(0.1) * (R(1) + t0 * t0);
+        a1 = R(0.6) * (R(1) + t1 * t1);
+        a2 = R(0.3) * (R(1) + t2 * t2);
+    } else {         // WENO-JS5, eps = 1e-6
+        const R e = R(1e-6);
+        a0 = R(0.1) / ((b0 + e) * (b0 + e));
+        a1 = R(0.6) / ((b1 + e) * (b1 + e));
+        a2 = R(0.3) / ((b2 + e) * (b2 + e));
+    }
+    return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
+}
+
+// Upwinded face value between cells c and c+1 along the axis of stride st
+// (src/AdvectionSchemes.jl:623-666); `at` points at cell c.
+template <typename R, int ADV>
+__device__ __forceinline__ R face_val(const R* __restrict__ at, long long st, R vel) {
+    if (vel >= R(0))
+        return weno5_left<R, ADV>(__ldg(at - 2 * st), __ldg(at - st), __ldg(at), __ldg(at + st), __ldg(at + 2 * st));
+    return weno5_left<R, ADV>(__ldg(at + 3 * st), __ldg(at + 2 * st), __ldg(at + st), __ldg(at), __ldg(at - st));
+}
+
+// ---- the sweep --------------------------------------------------------------
+template <typename R, int ADV, bool SGS, bool ANEL, bool UNI>
+__global__ void __launch_bounds__(256) sweep_kernel(SweepArgs<R> a) {
+    const Geo& g = a.g;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+    Met<R, UNI> m(g);
+    const long long q = pidx(g, i, j, k);
+    const long long sy = g.sy, sz = g.sz;
+    Nb<R> U{a.u + q, sy, sz}, V{a.v + q, sy, sz}, W{a.w + q, sy, sz}, T{a.th + q, sy, sz};
+    const R idx = R(g.idx), idy = R(g.idy), idx2 = R(g.idx2), idy2 = R(g.idy2);
+    const R h = R(0.5);
+    R tu, tv, tw, tt;
+
+    if (ANEL) {
+        // W-weighted centred forms (src/Anelastic.jl:1193-1306)
+        R iwc = R(1) / R(lvl(g.wc, k)), wfb = R(lvl(g.wf, k)), wft = R(lvl(g.wf, k + 1));
+        {
+            R uce = h * (U(0, 0, 0) + U(1, 0, 0)), ucw = h * (U(-1, 0, 0) + U(0, 0, 0));
+            R d_uu_dx = (uce * uce - ucw * ucw) * idx;
+            R vun = h * (V(-1, 1, 0) + V(0, 1, 0)), uvn = h * (U(0, 0, 0) + U(0, 1, 0));
+            R vus = h * (V(-1, 0, 0) + V(0, 0, 0)), uvs = h * (U(0, -1, 0) + U(0, 0, 0));
+            R d_vu_dy = (vun * uvn - vus * uvs) * idy;
+            R wut = h * (W(-1, 0, 1) + W(0, 0, 1)), uwt = h * (U(0, 0, 0) + U(0, 0, 1));
+            R wub = h * (W(-1, 0, 0) + W(0, 0, 0)), uwb = h * (U(0, 0, -1) + U(0, 0, 0));
+            R d_wu_dz = (wft * wut * uwt - wfb * wub * uwb) * m.idz(k) * iwc;
+            tu = R(0) - (d_uu_dx + d_vu_dy + d_wu_dz);
+        }
+        {
+            R uve = h * (U(1, -1, 0) + U(1, 0, 0)), vue = h * (V(0, 0, 0) + V(1, 0, 0));
+            R uvw = h * (U(0, -1, 0) + U(0, 0, 0)), vuw = h * (V(-1, 0, 0) + V(0, 0, 0));
+            R d_uv_dx = (uve * vue - uvw * vuw) * idx;
+            R vcn = h * (V(0, 0, 0) + V(0, 1, 0)), vcs = h * (V(0, -1, 0) + V(0, 0, 0));
+            R d_vv_dy = (vcn * vcn - vcs * vcs) * idy;
+            R wvt = h * (W(0, -1, 1) + W(0, 0, 1)), vwt = h * (V(0, 0, 0) + V(0, 0, 1));
+            R wvb = h * (W(0, -1, 0) + W(0, 0, 0)), vwb = h * (V(0, 0, -1) + V(0, 0, 0));
+            R d_wv_dz = (wft * wvt * vwt - wfb * wvb * vwb) * m.idz(k) * iwc;
+            tv = R(0) - (d_uv_dx + d_vv_dy + d_wv_dz);
+        }
+        {
+            R iwf = R(1) / R(lvl(g.wf, k)), wcb = R(lvl(g.wc, k - 1)), wct = R(lvl(g.wc, k));
+            R uwe = m.zflux(k, U(1, 0, -1), U(1, 0, 0)), wue = h * (W(0, 0, 0) + W(1, 0, 0));
+            R uww = m.zflux(k, U(0, 0, -1), U(0, 0, 0)), wuw = h * (W(-1, 0, 0) + W(0, 0, 0));
+            R d_uw_dx = (uwe * wue - uww * wuw) * idx;
+            R vwn = m.zflux(k, V(0, 1, -1), V(0, 1, 0)), wvn = h * (W(0, 0, 0) + W(0, 1, 0));
+            R vws = m.zflux(k, V(0, 0, -1), V(0, 0, 0)), wvs = h * (W(0, -1, 0) + W(0, 0, 0));
+            R d_vw_dy = (vwn * wvn - vws * wvs) * idy;
+            R wtop = h * (W(0, 0, 0) + W(0, 0, 1)), wbot = h * (W(0, 0, -1) + W(0, 0, 0));
+            R d_ww_dz = (wct * wtop * wtop - wcb * wbot * wbot) * m.idzf(k) * iwf;
+            tw = R(0) - (d_uw_dx + d_vw_dy + d_ww_dz);
+        }
+        {
+            R ue = U(1, 0, 0) * h * (T(0, 0, 0) + T(1, 0, 0)), uw = U(0, 0, 0) * h * (T(-1, 0, 0) + T(0, 0, 0));
+            R vn = V(0, 1, 0) * h * (T(0, 0, 0) + T(0, 1, 0)), vs = V(0, 0, 0) * h * (T(0, -1, 0) + T(0, 0, 0));
+            R wt = wft * W(0, 0, 1) * h * (T(0, 0, 0) + T(0, 0, 1)), wb = wfb * W(0, 0, 0) * h * (T(0, 0, -1) + T(0, 0, 0));
+            tt = R(0) - ((ue - uw) * idx + (vn - vs) * idy + (wt - wb) * m.idz(k) * iwc);
+        }
+    } else if (ADV == 0) {
+        // centred flux form (src/FiniteVolume.jl:730-797, :1682-1693)
+        {
+            R uce = h * (U(0, 0, 0) + U(1, 0, 0)), ucw = h * (U(-1, 0, 0) + U(0, 0, 0));
+            R d_uu_dx = (uce * uce - ucw * ucw) * idx;
+            R vun = h * (V(-1, 1, 0) + V(0, 1, 0)), uvn = h * (U(0, 0, 0) + U(0, 1, 0));
+            R vus = h * (V(-1, 0, 0) + V(0, 0, 0)), uvs = h * (U(0, -1, 0) + U(0, 0, 0));
+            R d_vu_dy = (vun * uvn - vus * uvs) * idy;
+            R wut = h * (W(-1, 0, 1) + W(0, 0, 1)), uwt = h * (U(0, 0, 0) + U(0, 0, 1));
+            R wub = h * (W(-1, 0, 0) + W(0, 0, 0)), uwb = h * (U(0, 0, -1) + U(0, 0, 0));
+            R d_wu_dz = (wut * uwt - wub * uwb) * m.idz(k);
+            tu = R(0) - (d_uu_dx + d_vu_dy + d_wu_dz);
+        }
+        {
+            R uve = h * (U(1, -1, 0) + U(1, 0, 0)), vue = h * (V(0, 0, 0) + V(1, 0, 0));
+            R uvw = h * (U(0, -1, 0) + U(0, 0, 0)), vuw = h * (V(-1, 0, 0) + V(0, 0, 0));
+            R d_uv_dx = (uve * vue - uvw * vuw) * idx;
+            R vcn = h * (V(0, 0, 0) + V(0, 1, 0)), vcs = h * (V(0, -1, 0) + V(0, 0, 0));
+            R d_vv_dy = (vcn * vcn - vcs * vcs) * idy;
+            R wvt = h * (W(0, -1, 1) + W(0, 0, 1)), vwt = h * (V(0, 0, 0) + V(0, 0, 1));
+            R wvb = h * (W(0, -1, 0) + W(0, 0, 0)), vwb = h * (V(0, 0, -1) + V(0, 0, 0));
+            R d_wv_dz = (wvt * vwt - wvb * vwb) * m.idz(k);
+            tv = R(0) - (d_uv_dx + d_vv_dy + d_wv_dz);
+        }
+        {
+            R uwe = m.zflux(k, U(1, 0, -1), U(1, 0, 0)), wue = h * (W(0, 0, 0) + W(1, 0, 0));
+            R uww = m.zflux(k, U(0, 0, -1), U(0, 0, 0)), wuw = h * (W(-1, 0, 0) + W(0, 0, 0));
+            R d_uw_dx = (uwe * wue - uww * wuw) * idx;
+            R vwn = m.zflux(k, V(0, 1, -1), V(0, 1, 0)), wvn = h * (W(0, 0, 0) + W(0, 1, 0));
+            R vws = m.zflux(k, V(0, 0, -1), V(0, 0, 0)), wvs = h * (W(0, -1, 0) + W(0, 0, 0));
+            R d_vw_dy = (vwn * wvn - vws * wvs) * idy;
+            R wct = h * (W(0, 0, 0) + W(0, 0, 1)), wcb = h * (W(0, 0, -1) + W(0, 0, 0));
+            R d_ww_dz = (wct * wct - wcb * wcb) * m.idzf(k);
+            tw = R(0) - (d_uw_dx + d_vw_dy + d_ww_dz);
+        }
+        {
+            R ue = U(1, 0, 0) * h * (T(0, 0, 0) + T(1, 0, 0)), uw = U(0, 0, 0) * h * (T(-1, 0, 0) + T(0, 0, 0));
+            R vn = V(0, 1, 0) * h * (T(0, 0, 0) + T(0, 1, 0)), vs = V(0, 0, 0) * h * (T(0, -1, 0) + T(0, 0, 0));
+            R wt = W(0, 0, 1) * h * (T(0, 0, 0) + T(0, 0, 1)), wb = W(0, 0, 0) * h * (T(0, 0, -1) + T(0, 0, 0));
+            tt = R(0) - ((ue - uw) * idx + (vn - vs) * idy + (wt - wb) * m.idz(k));
+        }
+    } else {
+        // WENO flux forms on a uniform grid (src/AdvectionSchemes.jl:685-699, :1203-1256)
+        const R idz = R(g.idz);
+        const R* up = a.u + q;
+        const R* vp = a.v + q;
+        const R* wp = a.w + q;
+        const R* tp = a.th + q;
+        {
+            R Ue = (U(0, 0, 0) + U(1, 0, 0)) / R(2), Uw = (U(-1, 0, 0) + U(0, 0, 0)) / R(2);
+            R dx = (Ue * face_val<R, ADV>(up, 1, Ue) - Uw * face_val<R, ADV>(up - 1, 1, Uw)) * idx;
+            R Vn = (V(-1, 1, 0) + V(0, 1, 0)) / R(2), Vs = (V(-1, 0, 0) + V(0, 0, 0)) / R(2);
+            R dy = (Vn * face_val<R, ADV>(up, sy, Vn) - Vs * face_val<R, ADV>(up - sy, sy, Vs)) * idy;
+            R Wt = (W(-1, 0, 1) + W(0, 0, 1)) / R(2), Wb = (W(-1, 0, 0) + W(0, 0, 0)) / R(2);
+            R dz = (Wt * face_val<R, ADV>(up, sz, Wt) - Wb * face_val<R, ADV>(up - sz, sz, Wb)) * idz;
+            tu = R(0) - (dx + dy + dz);
+        }
+        {
+            R Ue = (U(1, -1, 0) + U(1, 0, 0)) / R(2), Uw = (U(0, -1, 0) + U(0, 0, 0)) / R(2);
+            R dx = (Ue * face_val<R, ADV>(vp, 1, Ue) - Uw * face_val<R, ADV>(vp - 1, 1, Uw)) * idx;
+            R Vn = (V(0, 0, 0) + V(0, 1, 0)) / R(2), Vs = (V(0, -1, 0) + V(0, 0, 0)) / R(2);
+            R dy = (Vn * face_val<R, ADV>(vp, sy, Vn) - Vs * face_val<R, ADV>(vp - sy, sy, Vs)) * idy;
+            R Wt = (W(0, -1, 1) + W(0, 0, 1)) / R(2), Wb = (W(0, -1, 0) + W(0, 0, 0)) / R(2);
+            R dz = (Wt * face_val<R, ADV>(vp, sz, Wt) - Wb * face_val<R, ADV>(vp - sz, sz, Wb)) * idz;
+            tv = R(0) - (dx + dy + dz);
+        }
+        {
+            R Ue = (U(1, 0, -1) + U(1, 0, 0)) / R(2), Uw = (U(0, 0, -1) + U(0, 0, 0)) / R(2);
+            R dx = (Ue * face_val<R, ADV>(wp, 1, Ue) - Uw * face_val<R, ADV>(wp - 1, 1, Uw)) * idx;
+            R Vn = (V(0, 1, -1) + V(0, 1, 0)) / R(2), Vs = (V(0, 0, -1) + V(0, 0, 0)) / R(2);
+            R dy = (Vn * face_val<R, ADV>(wp, sy, Vn) - Vs * face_val<R, ADV>(wp - sy, sy, Vs)) * idy;
+            R Wt = (W(0, 0, 0) + W(0, 0, 1)) / R(2), Wb = (W(0, 0, -1) + W(0, 0, 0)) / R(2);
+            R dz = (Wt * face_val<R, ADV>(wp, sz, Wt) - Wb * face_val<R, ADV>(wp - sz, sz, Wb)) * idz;
+            tw = R(0) - (dx + dy + dz);
+        }
+        {
+            R uw = U(0, 0, 0), ue = U(1, 0, 0);
+            R Fx = (ue * face_val<R, ADV>(tp, 1, ue) - uw * face_val<R, ADV>(tp - 1, 1, uw)) * idx;
+            R vs = V(0, 0, 0), vn = V(0, 1, 0);
+            R Fy = (vn * face_val<R, ADV>(tp, sy, vn) - vs * face_val<R, ADV>(tp - sy, sy, vs)) * idy;
+            R wb = W(0, 0, 0), wt = W(0, 0, 1);
+            R Fz = (wt * face_val<R, ADV>(tp, sz, wt) - wb * face_val<R, ADV>(tp - sz, sz, wb)) * idz;
+            tt = R(0) - (Fx + Fy + Fz);
+        }
+    }
+
+    // molecular viscosity / diffusion
+    if (a.nu != R(0)) {
+        R c;
+        c = U(0, 0, 0);
+        tu = tu + a.nu * ((U(1, 0, 0) - R(2) * c + U(-1, 0, 0)) * idx2 + (U(0, 1, 0) - R(2) * c + U(0, -1, 0)) * idy2 +
+                          m.lapz(LOC_FX, k, U(0, 0, -1), c, U(0, 0, 1)));
+        c = V(0, 0, 0);
+        tv = tv + a.nu * ((V(1, 0, 0) - R(2) * c + V(-1, 0, 0)) * idx2 + (V(0, 1, 0) - R(2) * c + V(0, -1, 0)) * idy2 +
+                          m.lapz(LOC_FY, k, V(0, 0, -1), c, V(0, 0, 1)));
+        c = W(0, 0, 0);
+        tw = tw + a.nu * ((W(1, 0, 0) - R(2) * c + W(-1, 0, 0)) * idx2 + (W(0, 1, 0) - R(2) * c + W(0, -1, 0)) * idy2 +
+                          m.lapz(LOC_FZ, k, W(0, 0, -1), c, W(0, 0, 1)));
+        c = T(0, 0, 0);
+        tt = tt + a.nu * ((T(1, 0, 0) - R(2) * c + T(-1, 0, 0)) * idx2 + (T(0, 1, 0) - R(2) * c + T(0, -1, 0)) * idy2 +
+                          m.lapz(LOC_C, k, T(0, 0, -1), c, T(0, 0, 1)));
+    }
+
+    // Smagorinsky SGS fluxes (eddy viscosity from the nut array, halos filled)
+    if (SGS) {
+        Nb<R> N{a.nut + q, sy, sz};
+        const R q4 = R(0.25);
+        {
+            R fxE = N(0, 0, 0) * (U(1, 0, 0) - U(0, 0, 0)) * idx;
+            R fxW = N(-1, 0, 0) * (U(0, 0, 0) - U(-1, 0, 0)) * idx;
+            R eN = q4 * (N(-1, 0, 0) + N(0, 0, 0) + N(-1, 1, 0) + N(0, 1, 0));
+            R eS = q4 * (N(-1, -1, 0) + N(0, -1, 0) + N(-1, 0, 0) + N(0, 0, 0));
+            R fyN = eN * (U(0, 1, 0) - U(0, 0, 0)) * idy;
+            R fyS = eS * (U(0, 0, 0) - U(0, -1, 0)) * idy;
+            R eT = q4 * (N(-1, 0, 0) + N(0, 0, 0) + N(-1, 0, 1) + N(0, 0, 1));
+            R eB = q4 * (N(-1, 0, -1) + N(0, 0, -1) + N(-1, 0, 0) + N(0, 0, 0));
+            R fzT = eT * (U(0, 0, 1) - U(0, 0, 0)) * m.idzf(k + 1);
+            R fzB = eB * (U(0, 0, 0) - U(0, 0, -1)) * m.idzf(k);
+            R vert = ANEL ? (R(lvl(g.wf, k + 1)) * fzT - R(lvl(g.wf, k)) * fzB) * m.idz(k) / R(lvl(g.wc, k))
+                          : (fzT - fzB) * m.idz(k);
+            tu += (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
+        }
+        {
+            R fyN = N(0, 0, 0) * (V(0, 1, 0) - V(0, 0, 0)) * idy;
+            R fyS = N(0, -1, 0) * (V(0, 0, 0) - V(0, -1, 0)) * idy;
+            R eE = q4 * (N(0, -1, 0) + N(1, -1, 0) + N(0, 0, 0) + N(1, 0, 0));
+            R eW = q4 * (N(-1, -1, 0) + N(0, -1, 0) + N(-1, 0, 0) + N(0, 0, 0));
+            R fxE = eE * (V(1, 0, 0) - V(0, 0, 0)) * idx;
+            R fxW = eW * (V(0, 0, 0) - V(-1, 0, 0)) * idx;
+            R eT = q4 * (N(0, -1, 0) + N(0, 0, 0) + N(0, -1, 1) + N(0, 0, 1));
+            R eB = q4 * (N(0, -1, -1) + N(0, 0, -1) + N(0, -1, 0) + N(0, 0, 0));
+            R fzT = eT * (V(0, 0, 1) - V(0, 0, 0)) * m.idzf(k + 1);
+            R fzB = eB * (V(0, 0, 0) - V(0, 0, -1)) * m.idzf(k);
+            R vert = ANEL ? (R(lvl(g.wf, k + 1)) * fzT - R(lvl(g.wf, k)) * fzB) * m.idz(k) / R(lvl(g.wc, k))
+                          : (fzT - fzB) * m.idz(k);
+            tv += (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
+        }
+        {
+            R fzT = N(0, 0, 0) * (W(0, 0, 1) - W(0, 0, 0)) * m.idz(k);
+            R fzB = N(0, 0, -1) * (W(0, 0, 0) - W(0, 0, -1)) * m.idz(k - 1);
+            R eE = q4 * (N(0, 0, -1) + N(1, 0, -1) + N(0, 0, 0) + N(1, 0, 0));
+            R eW = q4 * (N(-1, 0, -1) + N(0, 0, -1) + N(-1, 0, 0) + N(0, 0, 0));
+            R fxE = eE * (W(1, 0, 0) - W(0, 0, 0)) * idx;
+            R fxW = eW * (W(0, 0, 0) - W(-1, 0, 0)) * idx;
+            R eN = q4 * (N(0, 0, -1) + N(0, 1, -1) + N(0, 0, 0) + N(0, 1, 0));
+            R eS = q4 * (N(0, -1, -1) + N(0, 0, -1) + N(0, -1, 0) + N(0, 0, 0));
+            R fyN = eN * (W(0, 1, 0) - W(0, 0, 0)) * idy;
+            R fyS = eS * (W(0, 0, 0) - W(0, -1, 0)) * idy;
+            R vert = ANEL ? (R(lvl(g.wc, k)) * fzT - R(lvl(g.wc, k - 1)) * fzB) * m.idzf(k) / R(lvl(g.wf, k))
+                          : (fzT - fzB) * m.idzf(k);
+            tw += (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
+        }
+        if (!ANEL) {
+            R nE = h * (N(0, 0, 0) + N(1, 0, 0)), nW = h * (N(-1, 0, 0) + N(0, 0, 0));
+            R nN = h * (N(0, 0, 0) + N(0, 1, 0)), nS = h * (N(0, -1, 0) + N(0, 0, 0));
+            R nT = h * (N(0, 0, 0) + N(0, 0, 1)), nB = h * (N(0, 0, -1) + N(0, 0, 0));
+            R fxE = nE * (T(1, 0, 0) - T(0, 0, 0)) * idx, fxW = nW * (T(0, 0, 0) - T(-1, 0, 0)) * idx;
+            R fyN = nN * (T(0, 1, 0) - T(0, 0, 0)) * idy, fyS = nS * (T(0, 0, 0) - T(0, -1, 0)) * idy;
+            R fzT = nT * (T(0, 0, 1) - T(0, 0, 0)) * m.idzf(k + 1), fzB = nB * (T(0, 0, 0) - T(0, 0, -1)) * m.idzf(k);
+            tt += a.inv_prt * ((fxE - fxW) * idx + (fyN - fyS) * idy + (fzT - fzB) * m.idz(k));
+        } else {
+            // kappa = nut / Pr_t, the W-weighted form
+            R pr = a.pr_t;
+            R K0 = N(0, 0, 0) / pr;
+            R fxE = h * (K0 + N(1, 0, 0) / pr) * (T(1, 0, 0) - T(0, 0, 0)) * idx;
+            R fxW = h * (N(-1, 0, 0) / pr + K0) * (T(0, 0, 0) - T(-1, 0, 0)) * idx;
+            R fyN = h * (K0 + N(0, 1, 0) / pr) * (T(0, 1, 0) - T(0, 0, 0)) * idy;
+            R fyS = h * (N(0, -1, 0) / pr + K0) * (T(0, 0, 0) - T(0, -1, 0)) * idy;
+            R fzT = h * (K0 + N(0, 0, 1) / pr) * (T(0, 0, 1) - T(0, 0, 0)) * m.idzf(k + 1);
+            R fzB = h * (N(0, 0, -1) / pr + K0) * (T(0, 0, 0) - T(0, 0, -1)) * m.idzf(k);
+            R vert = (R(lvl(g.wf, k + 1)) * fzT - R(lvl(g.wf, k)) * fzB) * m.idz(k) / R(lvl(g.wc, k));
+            tt += (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
+        }
+    }
+
+    // buoyancy on the z faces
+    if (ANEL) {
+        if (a.gacc != R(0)) {
+            R tb = R(lvl(g.thf, k));
+            R coef = a.gacc / tb;
+            tw += coef * (m.zface(k, T(0, 0, -1), T(0, 0, 0)) - tb);
+        }
+    } else if (a.theta0 != R(0)) {
+        tw += (a.gacc / a.theta0) * (m.zface(k, T(0, 0, -1), T(0, 0, 0)) - a.theta0);
+    }
+    // Coriolis
+    if (a.fcor != R(0)) {
+        R v_at_u = R(0.25) * (V(-1, 0, 0) + V(0, 0, 0) + V(-1, 1, 0) + V(0, 1, 0));
+        tu += a.fcor * v_at_u;
+        R u_at_v = R(0.25) * (U(0, -1, 0) + U(1, -1, 0) + U(0, 0, 0) + U(1, 0, 0));
+        tv -= a.fcor * u_at_v;
+    }
+    // prescribed wall fluxes of theta
+    if (k == 0) tt += a.flux_bot * m.idz(0);
+    if (k == g.nz - 1) tt -= a.flux_top * m.idz(g.nz - 1);
+    // Rayleigh sponge toward rest
+    if (a.sp_alpha != R(0)) {
+        double zc = lvl(g.zc, k), zf = lvl(g.zf, k);
+        if (zc >= (double)a.sp_zstart) {
+            R s = sin(R(0.5 * 3.14159265358979323846) * (R(zc) - a.sp_zstart) * a.sp_inv);
+            R r = a.sp_alpha * s * s;
+            tu -= r * U(0, 0, 0);
+            tv -= r * V(0, 0, 0);
+        }
+        if (zf >= (double)a.sp_zstart) {
+            R s = sin(R(0.5 * 3.14159265358979323846) * (R(zf) - a.sp_zstart) * a.sp_inv);
+            tw -= a.sp_alpha * s * s * W(0, 0, 0);
+        }
+    }
+
+    // predictor and the theta update (with the RK3 stage combination)
+    const long long qi = iidx(g, i, j, k);
+    const R dt = a.dt;
+    a.us[qi] = U(0, 0, 0) + dt * tu;
+    a.vs[qi] = V(0, 0, 0) + dt * tv;
+    a.ws[qi] = (g.bc_z == 1 && k == 0) ? R(0) : W(0, 0, 0) + dt * tw;
+    R tn = T(0, 0, 0) + dt * tt;
+    if (a.stage) tn = a.ca * a.th0[q] + a.cb * tn;  // th0 may alias th_out (stage 3): plain load
+    a.th_out[q] = tn;
+}
+
+// Smagorinsky nut = (C_s Delta_k)^2 |S| at the cell centres (src/FiniteVolume.jl:936-944,
+// strain src/Operators.jl:451-496); halos are filled by a separate launch.
+template <typename R, bool UNI>
+__global__ void __launch_bounds__(256) smagorinsky_kernel(Geo g, const R* __restrict__ u, const R* __restrict__ v,
+                                                          const R* __restrict__ w, R* __restrict__ nut, R c_s) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+    Met<R, UNI> m(g);
+    const long long q = pidx(g, i, j, k);
+    Nb<R> U{u + q, g.sy, g.sz}, V{v + q, g.sy, g.sz}, W{w + q, g.sy, g.sz};
+    R idx = R(g.idx), idy = R(g.idy), idz = m.idz(k), ido = m.idz_off(k);
+    R cf = c_s * m.filter(k);
+    R coef = cf * cf;
+    R du_dx = (U(1, 0, 0) - U(0, 0, 0)) * idx;
+    R dv_dy = (V(0, 1, 0) - V(0, 0, 0)) * idy;
+    R dw_dz = (W(0, 0, 1) - W(0, 0, 0)) * idz;
+    R du_dy = ((U(0, 1, 0) + U(1, 1, 0)) - (U(0, -1, 0) + U(1, -1, 0))) * (R(0.25) * idy);
+    R dv_dx = ((V(1, 0, 0) + V(1, 1, 0)) - (V(-1, 0, 0) + V(-1, 1, 0))) * (R(0.25) * idx);
+    R du_dz = ((U(0, 0, 1) + U(1, 0, 1)) - (U(0, 0, -1) + U(1, 0, -1))) * (R(0.25) * ido);
+    R dw_dx = ((W(1, 0, 0) + W(1, 0, 1)) - (W(-1, 0, 0) + W(-1, 0, 1))) * (R(0.25) * idx);
+    R dv_dz = ((V(0, 0, 1) + V(0, 1, 1)) - (V(0, 0, -1) + V(0, 1, -1))) * (R(0.25) * ido);
+    R dw_dy = ((W(0, 1, 0) + W(0, 1, 1)) - (W(0, -1, 0) + W(0, -1, 1))) * (R(0.25) * idy);
+    R S12 = R(0.5) * (du_dy + dv_dx), S13 = R(0.5) * (du_dz + dw_dx), S23 = R(0.5) * (dv_dz + dw_dy);
+    R S2 = R(2) * (du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz) + R(4) * (S12 * S12 + S13 * S13 + S23 * S23);
+    nut[q] = coef * sqrt(S2);
+}

@@ -1,0 +1,866 @@
+// aeolus_b200.cu -- libaeolus_b200.so: the C-ABI of include/aeolus_b200.h and
+// the per-domain orchestration of the projected SSP-RK3 step on one B200.
+//
+// One substage (src/Simulations.jl:531-650; src/Anelastic.jl:1791-1876):
+//   [SGS] smagorinsky -> nut, halo(nut)
+//   sweep           tendencies + predictor u* (interior) + theta (padded)
+//   div_fftx        divergence of u* fused with the r2c transform along x
+//   ffty            forward transform along y
+//   fftz_solve      periodic z: forward, 1/lambda, inverse   | thomas: walls in z
+//   ffty            inverse along y
+//   ifftx           c2r along x -> phi
+//   correct         u = c(u* - grad phi, u0), p = phi/dt
+//   halo            halos of u, v, w, theta for the next substage
+// The three substages of a step are captured once into a CUDA graph and
+// replayed.  State lives in three padded sets: the step starts and ends in
+// set 0 (u^n), stage 1 writes set 1, stage 2 set 2, stage 3 set 0 again.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/aeolus_b200.h"
+#include "aeo_common.cuh"
+#include "aeo_fft.cuh"
+#include "aeo_misc.cuh"
+#include "aeo_sweep.cuh"
+
+static std::string g_create_error;
+
+#define CK(call)                                                                         \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            fail(std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+            return AEO_ERR_CUDA;                                                         \
+        }                                                                                \
+    } while (0)
+
+#define CKL()                                                                            \
+    do {                                                                                 \
+        cudaError_t e_ = cudaGetLastError();                                             \
+        if (e_ != cudaSuccess) {                                                         \
+            fail(std::string("kernel launch: ") + cudaGetErrorString(e_));               \
+            return AEO_ERR_CUDA;                                                         \
+        }                                                                                \
+    } while (0)
+
+static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+static int next_pow2(int n) {
+    int p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+
+struct CoreBase {
+    aeo_config cfg{};
+    std::string err;
+    cudaStream_t st = nullptr;
+    Geo g{};
+    int launches = 0;
+    virtual ~CoreBase() {}
+    void fail(const std::string& m) { err = m; }
+    virtual aeo_status init(const double* zf, const double* wc, const double* wf, const double* thf) = 0;
+    virtual aeo_status set_field(int id, const double* host) = 0;
+    virtual aeo_status get_field(int id, double* host) = 0;
+    virtual aeo_status step_rk3(double dt, int n, bool sync) = 0;
+    virtual aeo_status step_euler(double dt, int n) = 0;
+    virtual aeo_status pressure_solve(const double* src, double* phi) = 0;
+    virtual aeo_status kinetic_energy(double* out) = 0;
+    virtual aeo_status max_divergence(double* out) = 0;
+    virtual aeo_status fill_uniform(int id, uint64_t seed, uint32_t stream, double amp, int mode) = 0;
+    virtual aeo_status project() = 0;
+    virtual aeo_status profile_step(double dt, double* ms, int ncls) = 0;
+};
+
+struct aeo_sim {
+    CoreBase* core;
+};
+
+template <typename R>
+struct Core : CoreBase {
+    // device buffers
+    std::vector<void*> allocs;
+    double* levels = nullptr;  // metric vectors
+    double *kx2 = nullptr, *ky2 = nullptr, *kz2 = nullptr;
+    double* colc = nullptr;    // column coefficients
+    ColumnCoef cc{};
+    R* P[3][4] = {};           // padded state sets (u, v, w, theta)
+    R* Q[3] = {};              // predictor (interior)
+    R* nut = nullptr;          // padded
+    R* phi = nullptr;          // interior
+    R* pres = nullptr;         // interior
+    cplx<R>* S = nullptr;      // spectrum
+    cplx<double>* dsc = nullptr;
+    cplx<R>* tw = nullptr;
+    int NT = 0;
+    double* d_stage = nullptr; // host-layout staging (device)
+    long long host_n = 0;
+    double* d_part = nullptr;
+    int* d_flag = nullptr;
+    int rows_x = 1, tpx_y = 1, tpx_z = 1;
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+    double graph_dt = 0.0;
+    bool uni = true, sgs = false, anel = false;
+    // per-kernel-class timing of one un-graphed step (aeo_profile_step)
+    bool profiling = false;
+    std::vector<std::pair<int, cudaEvent_t>> marks;
+    void mark(int cls) {
+        if (!profiling) return;
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, st);
+        marks.push_back({cls, e});
+    }
+
+    ~Core() override {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
+        for (void* p : allocs) cudaFree(p);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    template <typename T>
+    aeo_status alloc(T** p, size_t count) {
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+        if (e != cudaSuccess) {
+            fail(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+            return AEO_ERR_CUDA;
+        }
+        CK(cudaMemsetAsync(q, 0, std::max<size_t>(count, 1) * sizeof(T), st));
+        allocs.push_back(q);
+        *p = reinterpret_cast<T*>(q);
+        return AEO_OK;
+    }
+
+    long long padded_count() const { return (long long)g.sz * (g.nz + 2 * AEO_H); }
+
+    aeo_status init(const double* zfi, const double* wc, const double* wf, const double* thf) override {
+        const aeo_config& c = cfg;
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        uni = !c.stretched;
+        sgs = c.c_s != 0.0;
+        anel = c.core == AEO_CORE_ANELASTIC;
+        g.nx = c.nx; g.ny = c.ny; g.nz = c.nz;
+        g.px = c.nx + 2 * AEO_HX;
+        g.py = c.ny + 2 * AEO_H;
+        g.sy = g.px;
+        g.sz = (long long)g.px * g.py;
+        g.nin = (long long)c.nx * c.ny * c.nz;
+        g.bc_z = c.bc_z;
+        g.uniform = uni;
+        g.dx = c.lx / c.nx; g.dy = c.ly / c.ny; g.dz = c.lz / c.nz;
+        g.idx = 1 / g.dx; g.idy = 1 / g.dy; g.idx2 = 1 / (g.dx * g.dx); g.idy2 = 1 / (g.dy * g.dy);
+        g.idz = 1 / g.dz; g.idz2 = 1 / (g.dz * g.dz);
+        g.delta_u = std::pow(g.dx * g.dy * g.dz, 1.0 / 3);
+        // ---- vertical metrics over the storage levels (src/StretchedGrids.jl:345-400, :570-590)
+        const int Hz = c.hz, Nz = c.nz, NZ = Nz + 2 * Hz;
+        std::vector<double> zf(NZ + 1), zc(NZ), dzc(NZ), dzf(NZ + 1);
+        if (uni) {
+            for (int k = 0; k <= NZ; ++k) zf[k] = c.z0 + (double)(k - Hz) * g.dz;
+            for (int k = 0; k < NZ; ++k) zc[k] = c.z0 + ((double)(k - Hz) + 0.5) * g.dz;
+            for (int k = 0; k < NZ; ++k) dzc[k] = g.dz;
+            for (int k = 0; k <= NZ; ++k) dzf[k] = g.dz;
+        } else {
+            for (int k = 0; k <= Nz; ++k) zf[Hz + k] = zfi[k];
+            for (int k = Hz - 1; k >= 0; --k) zf[k] = 2 * zf[k + 1] - zf[k + 2];
+            for (int k = Hz + Nz + 1; k <= NZ; ++k) zf[k] = 2 * zf[k - 1] - zf[k - 2];
+            for (int k = 0; k < NZ; ++k) dzc[k] = zf[k + 1] - zf[k];
+            for (int k = 0; k < NZ; ++k) zc[k] = (zf[k] + zf[k + 1]) / 2;
+            dzf[0] = dzc[0];
+            for (int k = 1; k < NZ; ++k) dzf[k] = zc[k] - zc[k - 1];
+            dzf[NZ] = dzc[NZ - 1];
+        }
+        // device vectors indexed by interior level k at (k + AEO_LH); storage level K = k + Hz
+        const int L = Nz + 2 * AEO_LH + 2;
+        const int NV = 13;
+        std::vector<double> hv((size_t)NV * L, 0.0);
+        auto put = [&](int vec, int K, double val) {
+            int k = K - Hz;
+            int e = k + AEO_LH;
+            if (e >= 0 && e < L) hv[(size_t)vec * L + e] = val;
+        };
+        for (int K = 0; K < NZ; ++K) {
+            put(0, K, 1 / dzc[K]);
+            put(2, K, 2 / (dzf[K] + dzf[K + 1]));
+            put(7, K, std::pow(g.dx * g.dy * dzc[K], 1.0 / 3));
+            put(8, K, zc[K]);
+            if (K >= 1) {
+                double sm = dzc[K - 1] + dzc[K];
+                put(3, K, dzc[K] / (dzc[K - 1] + dzc[K]));
+                put(4, K, dzc[K - 1] / (dzc[K - 1] + dzc[K]));
+                put(5, K, dzc[K - 1] / sm);
+                put(6, K, dzc[K] / sm);
+            }
+        }
+        for (int K = 0; K <= NZ; ++K) {
+            put(1, K, 1 / dzf[K]);
+            put(9, K, zf[K]);
+        }
+        if (anel) {
+            for (int K = 0; K < NZ; ++K) put(10, K, wc[K]);
+            for (int K = 0; K <= NZ; ++K) put(11, K, wf[K]);
+            if (thf)
+                for (int K = 0; K <= NZ; ++K) put(12, K, thf[K]);
+        }
+        if (aeo_status s = alloc(&levels, hv.size())) return s;
+        CK(cudaMemcpyAsync(levels, hv.data(), hv.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        g.idzc = levels + 0 * L; g.idzf = levels + 1 * L; g.idz_off = levels + 2 * L;
+        g.wlo = levels + 3 * L; g.whi = levels + 4 * L; g.alo = levels + 5 * L; g.ahi = levels + 6 * L;
+        g.delta = levels + 7 * L; g.zc = levels + 8 * L; g.zf = levels + 9 * L;
+        g.wc = anel ? levels + 10 * L : nullptr;
+        g.wf = anel ? levels + 11 * L : nullptr;
+        g.thf = anel ? levels + 12 * L : nullptr;
+
+        // ---- eigenvalues and column coefficients
+        const int Nx = c.nx, Ny = c.ny, Mh = Nx / 2 + 1;
+        std::vector<double> hkx(Mh), hky(Ny), hkz(Nz);
+        if (c.solver == AEO_SOLVER_FFT) {
+            // src/PressureSolvers.jl:128-130
+            for (int m = 0; m < Mh; ++m) { double s = std::sin(M_PI * m / Nx); hkx[m] = 4 / (g.dx * g.dx) * (s * s); }
+            for (int m = 0; m < Ny; ++m) { double s = std::sin(M_PI * m / Ny); hky[m] = 4 / (g.dy * g.dy) * (s * s); }
+            for (int m = 0; m < Nz; ++m) { double s = std::sin(M_PI * m / Nz); hkz[m] = 4 / (g.dz * g.dz) * (s * s); }
+        } else {
+            // _r2r_eigen, src/PressureSolvers.jl:618-624
+            for (int m = 0; m < Mh; ++m) { int mm = std::min(m, Nx - m); double s = std::sin(M_PI * mm / Nx); hkx[m] = 4 / (g.dx * g.dx) * (s * s); }
+            for (int m = 0; m < Ny; ++m) { int mm = std::min(m, Ny - m); double s = std::sin(M_PI * mm / Ny); hky[m] = 4 / (g.dy * g.dy) * (s * s); }
+        }
+        if (aeo_status s = alloc(&kx2, Mh)) return s;
+        if (aeo_status s = alloc(&ky2, Ny)) return s;
+        if (aeo_status s = alloc(&kz2, Nz)) return s;
+        CK(cudaMemcpyAsync(kx2, hkx.data(), Mh * sizeof(double), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ky2, hky.data(), Ny * sizeof(double), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(kz2, hkz.data(), Nz * sizeof(double), cudaMemcpyHostToDevice, st));
+        if (c.solver == AEO_SOLVER_COLUMN) {
+            std::vector<double> lo(Nz), up(Nz), hw(Nz), me(Nz), io(Nz + 1), ga(Nz);
+            for (int k = 0; k < Nz; ++k) {
+                int K = Hz + k;
+                if (anel) {
+                    if (uni) {
+                        // DirectWeightedPoissonSolver, src/Anelastic.jl:1013-1019
+                        double idz2 = 1 / (g.dz * g.dz);
+                        lo[k] = k > 0 ? wf[K] * idz2 : 0.0;
+                        up[k] = k < Nz - 1 ? wf[K + 1] * idz2 : 0.0;
+                        hw[k] = wc[K]; me[k] = g.dz * g.dz; ga[k] = 1.0;
+                    } else {
+                        lo[k] = k > 0 ? wf[K] / (dzc[K] * dzf[K]) : 0.0;
+                        up[k] = k < Nz - 1 ? wf[K + 1] / (dzc[K] * dzf[K + 1]) : 0.0;
+                        hw[k] = wc[K]; me[k] = dzc[K]; ga[k] = dzc[K];
+                    }
+                } else {
+                    // ColumnTridiagonalSolver(dzc, dzf), src/PressureSolvers.jl:686-700
+                    lo[k] = k > 0 ? 1 / (dzc[K] * dzf[K]) : 0.0;
+                    up[k] = k < Nz - 1 ? 1 / (dzc[K] * dzf[K + 1]) : 0.0;
+                    hw[k] = 1.0; me[k] = dzc[K]; ga[k] = dzc[K];
+                }
+            }
+            for (int k = 0; k <= Nz; ++k) {
+                int K = Hz + k;
+                io[k] = anel ? (uni ? 1 / wf[K] : dzf[K] / wf[K]) : dzf[K];
+            }
+            double ms = 0, gs = 0;
+            for (int k = 0; k < Nz; ++k) { ms += me[k]; gs += ga[k]; }
+            if (aeo_status s = alloc(&colc, 6 * (size_t)(Nz + 1))) return s;
+            std::vector<double> hc(6 * (size_t)(Nz + 1), 0.0);
+            std::copy(lo.begin(), lo.end(), hc.begin());
+            std::copy(up.begin(), up.end(), hc.begin() + (Nz + 1));
+            std::copy(hw.begin(), hw.end(), hc.begin() + 2 * (Nz + 1));
+            std::copy(me.begin(), me.end(), hc.begin() + 3 * (Nz + 1));
+            std::copy(io.begin(), io.end(), hc.begin() + 4 * (Nz + 1));
+            std::copy(ga.begin(), ga.end(), hc.begin() + 5 * (Nz + 1));
+            CK(cudaMemcpyAsync(colc, hc.data(), hc.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+            cc.lower = colc; cc.upper = colc + (Nz + 1); cc.hw = colc + 2 * (Nz + 1);
+            cc.meas = colc + 3 * (Nz + 1); cc.iota = colc + 4 * (Nz + 1); cc.gauge = colc + 5 * (Nz + 1);
+            cc.meas_sum = ms; cc.gauge_sum = gs; cc.kx2 = kx2; cc.ky2 = ky2;
+        }
+
+        // ---- twiddles
+        NT = next_pow2(std::max(std::max(Nx, Ny), c.solver == AEO_SOLVER_FFT ? Nz : 1));
+        {
+            std::vector<cplx<R>> ht(NT);
+            for (int m = 0; m < NT; ++m) {
+                double a = -2.0 * M_PI * (double)m / (double)NT;
+                ht[m].x = (R)std::cos(a);
+                ht[m].y = (R)std::sin(a);
+            }
+            if (aeo_status s = alloc(&tw, NT)) return s;
+            CK(cudaMemcpyAsync(tw, ht.data(), NT * sizeof(cplx<R>), cudaMemcpyHostToDevice, st));
+        }
+        rows_x = std::max(1, 2048 / (Nx / 2));
+        tpx_y = std::max(1, std::min(16, 2048 / Ny));
+        tpx_z = std::max(1, std::min(16, 2048 / Nz));
+
+        // ---- fields
+        const long long np = padded_count();
+        for (int s = 0; s < 3; ++s)
+            for (int f = 0; f < 4; ++f)
+                if (aeo_status e = alloc(&P[s][f], np)) return e;
+        for (int f = 0; f < 3; ++f)
+            if (aeo_status e = alloc(&Q[f], g.nin)) return e;
+        if (sgs)
+            if (aeo_status e = alloc(&nut, np)) return e;
+        if (aeo_status e = alloc(&phi, g.nin)) return e;
+        if (aeo_status e = alloc(&pres, g.nin)) return e;
+        const long long ns = (long long)Mh * Ny * Nz;
+        if (aeo_status e = alloc(&S, ns)) return e;
+        if (c.solver == AEO_SOLVER_COLUMN) {
+            if (sizeof(R) == sizeof(double)) dsc = reinterpret_cast<cplx<double>*>(S);
+            else if (aeo_status e = alloc(&dsc, ns)) return e;
+        }
+        host_n = (long long)(c.nx + 2 * c.hx) * (c.ny + 2 * c.hy) * (c.nz + 2 * c.hz);
+        if (aeo_status e = alloc(&d_stage, std::max<long long>(host_n, g.nin))) return e;
+        if (aeo_status e = alloc(&d_part, Nz + 1)) return e;
+        if (aeo_status e = alloc(&d_flag, 1)) return e;
+        CK(cudaStreamSynchronize(st));
+        launches = 3 * (8 + (sgs ? 2 : 0));
+        return AEO_OK;
+    }
+
+    // ---- launch helpers -------------------------------------------------------------
+    dim3 blk3() const { return dim3(32, 4, 2); }
+    dim3 grd3() const { return dim3((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + 1) / 2); }
+
+    aeo_status halo(R* const* f, const int* loc, int nf) {
+        HaloSet<R> hs{};
+        for (int q = 0; q < nf; ++q) { hs.f[q] = f[q]; hs.loc[q] = loc[q]; }
+        hs.nf = nf;
+        long long n = shell_count(g);
+        halo_fill_kernel<R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, hs);
+        CKL();
+        return AEO_OK;
+    }
+
+    template <int ADV, bool SG, bool AN, bool UN>
+    void launch_sweep_t(const SweepArgs<R>& a) {
+        sweep_kernel<R, ADV, SG, AN, UN><<<grd3(), blk3(), 0, st>>>(a);
+    }
+
+    aeo_status launch_sweep(const SweepArgs<R>& a) {
+        const int adv = cfg.advection;
+        if (anel) {
+            if (uni) { if (sgs) launch_sweep_t<0, true, true, true>(a); else launch_sweep_t<0, false, true, true>(a); }
+            else { if (sgs) launch_sweep_t<0, true, true, false>(a); else launch_sweep_t<0, false, true, false>(a); }
+        } else if (!uni) {
+            if (sgs) launch_sweep_t<0, true, false, false>(a); else launch_sweep_t<0, false, false, false>(a);
+        } else if (adv == AEO_ADV_CENTRED) {
+            if (sgs) launch_sweep_t<0, true, false, true>(a); else launch_sweep_t<0, false, false, true>(a);
+        } else if (adv == AEO_ADV_WENO_JS5) {
+            if (sgs) launch_sweep_t<1, true, false, true>(a); else launch_sweep_t<1, false, false, true>(a);
+        } else {
+            if (sgs) launch_sweep_t<2, true, false, true>(a); else launch_sweep_t<2, false, false, true>(a);
+        }
+        CKL();
+        return AEO_OK;
+    }
+
+    // The pressure solve from the source (src == nullptr: divergence of Q) into phi.
+    aeo_status solve(const R* src) {
+        const int M = g.nx / 2;
+        size_t smx = (size_t)rows_x * M * sizeof(cplx<R>);
+        unsigned gx = (unsigned)((g.ny * (long long)g.nz + rows_x - 1) / rows_x);
+        if (src) {
+            if (aeo_status e = src_fftx(src)) return e;
+        } else if (anel) {
+            if (uni) div_fftx_kernel<R, true, true><<<gx, 256, smx, st>>>(g, Q[0], Q[1], Q[2], S, tw, NT, rows_x);
+            else div_fftx_kernel<R, true, false><<<gx, 256, smx, st>>>(g, Q[0], Q[1], Q[2], S, tw, NT, rows_x);
+        } else {
+            if (uni) div_fftx_kernel<R, false, true><<<gx, 256, smx, st>>>(g, Q[0], Q[1], Q[2], S, tw, NT, rows_x);
+            else div_fftx_kernel<R, false, false><<<gx, 256, smx, st>>>(g, Q[0], Q[1], Q[2], S, tw, NT, rows_x);
+        }
+        CKL();
+        mark(AEO_K_DIV_FFTX);
+        const int Mh = M + 1;
+        dim3 gy((Mh + tpx_y - 1) / tpx_y, g.nz);
+        size_t smy = (size_t)tpx_y * g.ny * sizeof(cplx<R>);
+        ffty_kernel<R, 0><<<gy, 256, smy, st>>>(g, S, tw, NT, tpx_y);
+        CKL();
+        mark(AEO_K_FFTY);
+        if (cfg.solver == AEO_SOLVER_FFT) {
+            dim3 gz((Mh + tpx_z - 1) / tpx_z, g.ny);
+            size_t smz = (size_t)tpx_z * g.nz * sizeof(cplx<R>);
+            double nrm = 1.0 / ((double)g.nx * g.ny * g.nz);
+            fftz_solve_kernel<R><<<gz, 256, smz, st>>>(g, S, tw, NT, tpx_z, kx2, ky2, kz2, nrm);
+        } else {
+            dim3 gt((Mh + 31) / 32, g.ny);
+            size_t smt = (size_t)g.nz * 32 * sizeof(double);
+            thomas_kernel<R><<<gt, 32, smt, st>>>(g, S, dsc, cc);
+        }
+        CKL();
+        mark(AEO_K_ZSOLVE);
+        ffty_kernel<R, 1><<<gy, 256, smy, st>>>(g, S, tw, NT, tpx_y);
+        CKL();
+        mark(AEO_K_FFTY);
+        R scale = cfg.solver == AEO_SOLVER_FFT ? R(1) : R(1.0 / ((double)g.nx * g.ny));
+        ifftx_kernel<R><<<gx, 256, smx, st>>>(g, S, phi, tw, NT, rows_x, scale);
+        CKL();
+        mark(AEO_K_IFFTX);
+        return AEO_OK;
+    }
+
+    // r2c of a given interior source (the standalone solve): the divergence
+    // kernel with the source in place of the velocities is the x transform of
+    // a source whose "divergence" is itself -- use a small packing kernel.
+    aeo_status src_fftx(const R* src);
+    aeo_status project() override;
+
+    aeo_status substage(int s_in, int s_out, int stage, R dt, R ca, R cb) {
+        R** in = P[s_in];
+        R** out = P[s_out];
+        if (sgs) {
+            if (uni) smagorinsky_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, in[0], in[1], in[2], nut, R(cfg.c_s));
+            else smagorinsky_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, in[0], in[1], in[2], nut, R(cfg.c_s));
+            CKL();
+            R* f[1] = {nut};
+            int l[1] = {LOC_C};
+            if (aeo_status e = halo(f, l, 1)) return e;
+            mark(AEO_K_SGS);
+        }
+        SweepArgs<R> a{};
+        a.g = g;
+        a.u = in[0]; a.v = in[1]; a.w = in[2]; a.th = in[3];
+        a.nut = nut;
+        a.th0 = P[0][3];
+        a.us = Q[0]; a.vs = Q[1]; a.ws = Q[2];
+        a.th_out = out[3];
+        a.dt = dt; a.ca = ca; a.cb = cb; a.stage = stage;
+        a.nu = R(cfg.nu); a.gacc = R(cfg.g); a.theta0 = R(cfg.theta0); a.fcor = R(cfg.f_coriolis);
+        a.pr_t = R(cfg.pr_t); a.inv_prt = R(1.0 / cfg.pr_t);
+        a.flux_bot = R(cfg.flux_bot); a.flux_top = R(cfg.flux_top);
+        a.sp_alpha = R(cfg.sponge_alpha); a.sp_zstart = R(cfg.sponge_zstart);
+        double ztop = cfg.z0 + cfg.lz;
+        a.sp_inv = R(1.0 / (ztop - cfg.sponge_zstart));
+        if (aeo_status e = launch_sweep(a)) return e;
+        mark(AEO_K_SWEEP);
+        if (aeo_status e = solve(nullptr)) return e;
+        if (uni)
+            correct_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, Q[0], Q[1], Q[2], phi, P[0][0], P[0][1], P[0][2],
+                                                               out[0], out[1], out[2], pres, R(1.0 / (double)dt), ca, cb, stage);
+        else
+            correct_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, Q[0], Q[1], Q[2], phi, P[0][0], P[0][1], P[0][2],
+                                                                out[0], out[1], out[2], pres, R(1.0 / (double)dt), ca, cb, stage);
+        CKL();
+        mark(AEO_K_CORRECT);
+        R* f[4] = {out[0], out[1], out[2], out[3]};
+        int l[4] = {LOC_FX, LOC_FY, LOC_FZ, LOC_C};
+        aeo_status hs = halo(f, l, 4);
+        mark(AEO_K_HALO);
+        return hs;
+    }
+
+    aeo_status enqueue_rk3(double dt) {
+        const R inv3 = R(1) / R(3), two3 = R(2) * inv3;
+        if (aeo_status e = substage(0, 1, 0, R(dt), R(0), R(0))) return e;
+        if (aeo_status e = substage(1, 2, 1, R(dt), R(0.75), R(0.25))) return e;
+        return substage(2, 0, 1, R(dt), inv3, two3);
+    }
+
+    aeo_status step_rk3(double dt, int n, bool sync) override {
+        if (!gexec || graph_dt != dt) {
+            if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+            if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            aeo_status e = enqueue_rk3(dt);
+            cudaGraph_t gr = nullptr;
+            cudaError_t ce = cudaStreamEndCapture(st, &gr);
+            if (e) { if (gr) cudaGraphDestroy(gr); return e; }
+            if (ce != cudaSuccess) { fail(std::string("graph capture: ") + cudaGetErrorString(ce)); return AEO_ERR_CUDA; }
+            graph = gr;
+            CK(cudaGraphInstantiate(&gexec, graph, 0));
+            graph_dt = dt;
+        }
+        for (int s = 0; s < n; ++s) CK(cudaGraphLaunch(gexec, st));
+        if (sync) {
+            CK(cudaStreamSynchronize(st));
+            return check_finite();
+        }
+        return AEO_OK;
+    }
+
+    aeo_status profile_step(double dt, double* ms, int ncls) override {
+        profiling = true;
+        marks.clear();
+        mark(-1);
+        aeo_status e = enqueue_rk3(dt);
+        profiling = false;
+        if (e) return e;
+        CK(cudaStreamSynchronize(st));
+        for (int c = 0; c < ncls; ++c) ms[c] = 0.0;
+        for (size_t q = 1; q < marks.size(); ++q) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, marks[q - 1].second, marks[q].second);
+            int c = marks[q].first;
+            if (c >= 0 && c < ncls) ms[c] += (double)t;
+        }
+        for (auto& m : marks) cudaEventDestroy(m.second);
+        marks.clear();
+        return check_finite();
+    }
+
+    aeo_status step_euler(double dt, int n) override {
+        for (int s = 0; s < n; ++s) {
+            if (aeo_status e = substage(0, 1, 0, R(dt), R(0), R(0))) return e;
+            // the Euler result becomes the state: swap sets 0 and 1
+            for (int f = 0; f < 4; ++f) std::swap(P[0][f], P[1][f]);
+            if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+            if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+        }
+        CK(cudaStreamSynchronize(st));
+        return check_finite();
+    }
+
+    aeo_status check_finite() {
+        CK(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
+        dim3 gb((g.nx + 127) / 128, g.ny, g.nz);
+        for (int f = 0; f < 4; ++f) {
+            finite_check_kernel<R><<<gb, 128, 0, st>>>(g, P[0][f], d_flag);
+            CKL();
+        }
+        int h = 0;
+        CK(cudaMemcpyAsync(&h, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (h) { fail("non-finite value in the state after the step"); return AEO_ERR_NUMERICAL; }
+        return AEO_OK;
+    }
+
+    R* field_ptr(int id, int* padded, int* loc) {
+        *padded = 1;
+        switch (id) {
+            case AEO_FIELD_U: *loc = LOC_FX; return P[0][0];
+            case AEO_FIELD_V: *loc = LOC_FY; return P[0][1];
+            case AEO_FIELD_W: *loc = LOC_FZ; return P[0][2];
+            case AEO_FIELD_THETA: *loc = LOC_C; return P[0][3];
+            case AEO_FIELD_P: *padded = 0; *loc = -1; return pres;
+            case AEO_FIELD_NUT: *loc = -1; return nut;
+            default: return nullptr;
+        }
+    }
+
+    aeo_status set_field(int id, const double* host) override {
+        int padded, loc;
+        R* d = field_ptr(id, &padded, &loc);
+        if (!d) { fail("set_field: unknown or unavailable field"); return AEO_ERR_ARGUMENT; }
+        CK(cudaMemcpyAsync(d_stage, host, host_n * sizeof(double), cudaMemcpyHostToDevice, st));
+        dim3 gb((g.nx + 127) / 128, g.ny, g.nz);
+        unpack_host_kernel<R><<<gb, 128, 0, st>>>(g, d_stage, cfg.hx, cfg.hy, cfg.hz, d, padded);
+        CKL();
+        if (padded && loc >= 0) {
+            if (loc == LOC_FZ && g.bc_z == 1) {
+                wall_face_zero_kernel<R><<<dim3((g.nx + 127) / 128, g.ny), 128, 0, st>>>(g, d);
+                CKL();
+            }
+            R* f[1] = {d};
+            int l[1] = {loc};
+            if (aeo_status e = halo(f, l, 1)) return e;
+        }
+        CK(cudaStreamSynchronize(st));
+        return AEO_OK;
+    }
+
+    aeo_status get_field(int id, double* host) override {
+        int padded, loc;
+        R* d = field_ptr(id, &padded, &loc);
+        if (!d) { fail("get_field: unknown or unavailable field"); return AEO_ERR_ARGUMENT; }
+        pack_host_kernel<R><<<(unsigned)((host_n + 255) / 256), 256, 0, st>>>(g, d_stage, cfg.hx, cfg.hy, cfg.hz, d,
+                                                                              padded, loc);
+        CKL();
+        CK(cudaMemcpyAsync(host, d_stage, host_n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return AEO_OK;
+    }
+
+    aeo_status pressure_solve(const double* src, double* out) override {
+        CK(cudaMemcpyAsync(d_stage, src, g.nin * sizeof(double), cudaMemcpyHostToDevice, st));
+        convert_kernel<R><<<(unsigned)((g.nin + 255) / 256), 256, 0, st>>>(g.nin, d_stage, Q[0]);
+        CKL();
+        if (aeo_status e = solve(Q[0])) return e;
+        convert_back_kernel<R><<<(unsigned)((g.nin + 255) / 256), 256, 0, st>>>(g.nin, phi, d_stage);
+        CKL();
+        CK(cudaMemcpyAsync(out, d_stage, g.nin * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return AEO_OK;
+    }
+
+    aeo_status kinetic_energy(double* out) override {
+        if (uni) ke_levels_kernel<R, true><<<g.nz, 256, 0, st>>>(g, P[0][0], P[0][1], P[0][2], d_part);
+        else ke_levels_kernel<R, false><<<g.nz, 256, 0, st>>>(g, P[0][0], P[0][1], P[0][2], d_part);
+        CKL();
+        std::vector<double> h(g.nz);
+        CK(cudaMemcpyAsync(h.data(), d_part, g.nz * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        double t = 0.0;
+        for (int k = 0; k < g.nz; ++k) t += h[k];
+        *out = uni ? 0.5 * t * (g.dx * g.dy * g.dz) : 0.5 * t * g.dx * g.dy;
+        return AEO_OK;
+    }
+
+    aeo_status max_divergence(double* out) override {
+        if (anel) {
+            if (uni) maxdiv_levels_kernel<R, true, true><<<g.nz, 256, 0, st>>>(g, P[0][0], P[0][1], P[0][2], d_part);
+            else maxdiv_levels_kernel<R, true, false><<<g.nz, 256, 0, st>>>(g, P[0][0], P[0][1], P[0][2], d_part);
+        } else {
+            if (uni) maxdiv_levels_kernel<R, false, true><<<g.nz, 256, 0, st>>>(g, P[0][0], P[0][1], P[0][2], d_part);
+            else maxdiv_levels_kernel<R, false, false><<<g.nz, 256, 0, st>>>(g, P[0][0], P[0][1], P[0][2], d_part);
+        }
+        CKL();
+        std::vector<double> h(g.nz);
+        CK(cudaMemcpyAsync(h.data(), d_part, g.nz * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        double m = 0.0;
+        for (int k = 0; k < g.nz; ++k) m = std::max(m, h[k]);
+        *out = m;
+        return AEO_OK;
+    }
+
+    aeo_status fill_uniform(int id, uint64_t seed, uint32_t stream, double amp, int mode) override {
+        int padded, loc;
+        R* d = field_ptr(id, &padded, &loc);
+        if (!d || loc < 0) { fail("fill_uniform: field must be u, v, w or theta"); return AEO_ERR_ARGUMENT; }
+        philox_fill_kernel<R><<<(unsigned)((g.nin + 255) / 256), 256, 0, st>>>(g, d, padded, seed, stream, amp, mode);
+        CKL();
+        if (loc == LOC_FZ && g.bc_z == 1) {
+            wall_face_zero_kernel<R><<<dim3((g.nx + 127) / 128, g.ny), 128, 0, st>>>(g, d);
+            CKL();
+        }
+        R* f[1] = {d};
+        int l[1] = {loc};
+        if (aeo_status e = halo(f, l, 1)) return e;
+        CK(cudaStreamSynchronize(st));
+        return AEO_OK;
+    }
+};
+
+// r2c of an interior source along x: pack pairs, FFT, post-process (the
+// div_fftx kernel body with the source read directly).
+template <typename R>
+__global__ void __launch_bounds__(256) src_fftx_kernel(Geo g, const R* __restrict__ src, cplx<R>* __restrict__ S,
+                                                       const cplx<R>* __restrict__ tw, int NT, int rows) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<R>* buf = reinterpret_cast<cplx<R>*>(smem_raw);
+    const int M = g.nx / 2, Mh = M + 1;
+    const long long nrows = (long long)g.ny * g.nz;
+    const long long row0 = (long long)blockIdx.x * rows;
+    for (int e = threadIdx.x; e < rows * M; e += blockDim.x) {
+        int r = e / M, n = e % M;
+        long long row = row0 + r;
+        cplx<R> z = cmk<R>(R(0), R(0));
+        if (row < nrows) z = cmk<R>(src[row * g.nx + 2 * n], src[row * g.nx + 2 * n + 1]);
+        buf[r * M + n] = z;
+    }
+    __syncthreads();
+    smem_fft<R, false, false, FFT_KB>(buf, M, rows, M, 1, tw, NT);
+    const int tstep = NT / g.nx;
+    for (int e = threadIdx.x; e < rows * Mh; e += blockDim.x) {
+        int r = e / Mh, kk = e % Mh;
+        long long row = row0 + r;
+        if (row >= nrows) continue;
+        cplx<R> a = buf[r * M + (kk == M ? 0 : kk)];
+        cplx<R> b = buf[r * M + (kk == 0 ? 0 : M - kk)];
+        R er = R(0.5) * (a.x + b.x), ei = R(0.5) * (a.y - b.y);
+        R orr = R(0.5) * (a.y + b.y), oi = R(-0.5) * (a.x - b.x);
+        cplx<R> wv = tw[(kk * tstep) & (NT - 1)];
+        S[row * Mh + kk] = cmk<R>(er + (wv.x * orr - wv.y * oi), ei + (wv.x * oi + wv.y * orr));
+    }
+}
+
+template <typename R>
+aeo_status Core<R>::src_fftx(const R* src) {
+    const int M = g.nx / 2;
+    size_t smx = (size_t)rows_x * M * sizeof(cplx<R>);
+    unsigned gx = (unsigned)((g.ny * (long long)g.nz + rows_x - 1) / rows_x);
+    src_fftx_kernel<R><<<gx, 256, smx, st>>>(g, src, S, tw, NT, rows_x);
+    CKL();
+    return AEO_OK;
+}
+
+template <typename R>
+__global__ void padded_to_interior_kernel(Geo g, const R* __restrict__ a, R* __restrict__ b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i < g.nx) b[iidx(g, i, j, k)] = a[pidx(g, i, j, k)];
+}
+
+template <typename R>
+aeo_status Core<R>::project() {
+    dim3 gb((g.nx + 127) / 128, g.ny, g.nz);
+    for (int f = 0; f < 3; ++f) {
+        padded_to_interior_kernel<R><<<gb, 128, 0, st>>>(g, P[0][f], Q[f]);
+        CKL();
+    }
+    if (aeo_status e = solve(nullptr)) return e;
+    if (uni)
+        correct_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, Q[0], Q[1], Q[2], phi, P[0][0], P[0][1], P[0][2], P[0][0],
+                                                           P[0][1], P[0][2], pres, R(1), R(0), R(0), 0);
+    else
+        correct_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, Q[0], Q[1], Q[2], phi, P[0][0], P[0][1], P[0][2], P[0][0],
+                                                            P[0][1], P[0][2], pres, R(1), R(0), R(0), 0);
+    CKL();
+    R* f[3] = {P[0][0], P[0][1], P[0][2]};
+    int l[3] = {LOC_FX, LOC_FY, LOC_FZ};
+    if (aeo_status e = halo(f, l, 3)) return e;
+    CK(cudaStreamSynchronize(st));
+    return AEO_OK;
+}
+
+// ====================================================================================
+// C-ABI
+// ====================================================================================
+
+static aeo_status validate(const aeo_config* c, const double* zf, const double* wc, const double* wf, std::string* m) {
+    if (!c) { *m = "config is NULL"; return AEO_ERR_ARGUMENT; }
+    if (c->nx < 4 || c->ny < 4 || c->nz < 2) { *m = "grid too small (nx, ny >= 4, nz >= 2)"; return AEO_ERR_ARGUMENT; }
+    if (!is_pow2(c->nx) || !is_pow2(c->ny)) { *m = "nx and ny must be powers of two"; return AEO_ERR_ARGUMENT; }
+    if (c->nx / 2 > 2048 || c->ny > 2048) { *m = "nx/2 and ny must not exceed 2048"; return AEO_ERR_ARGUMENT; }
+    if (c->bc_x != AEO_BC_PERIODIC || c->bc_y != AEO_BC_PERIODIC) { *m = "x and y must be periodic"; return AEO_ERR_ARGUMENT; }
+    if (c->bc_z != AEO_BC_PERIODIC && c->bc_z != AEO_BC_WALL) { *m = "bc_z must be periodic or wall"; return AEO_ERR_ARGUMENT; }
+    if (c->hx < 0 || c->hy < 0 || c->hz < 0 || c->hx > 8 || c->hy > 8 || c->hz > 8) { *m = "host halo widths must be in 0..8"; return AEO_ERR_ARGUMENT; }
+    if (c->solver == AEO_SOLVER_FFT) {
+        if (c->bc_z != AEO_BC_PERIODIC) { *m = "the FFT solver needs a periodic z"; return AEO_ERR_ARGUMENT; }
+        if (!is_pow2(c->nz) || c->nz > 2048) { *m = "the FFT solver needs nz a power of two <= 2048"; return AEO_ERR_ARGUMENT; }
+    } else if (c->solver == AEO_SOLVER_COLUMN) {
+        if (c->bc_z != AEO_BC_WALL) { *m = "the column solver needs walls in z"; return AEO_ERR_ARGUMENT; }
+    } else { *m = "unknown solver"; return AEO_ERR_ARGUMENT; }
+    if (c->advection < 0 || c->advection > 2) { *m = "unknown advection scheme"; return AEO_ERR_ARGUMENT; }
+    if (c->advection != AEO_ADV_CENTRED && (c->stretched || c->core == AEO_CORE_ANELASTIC)) {
+        *m = "WENO advection is defined on a uniform Boussinesq grid (src/AdvectionSchemes.jl:731)";
+        return AEO_ERR_ARGUMENT;
+    }
+    if (c->core == AEO_CORE_ANELASTIC && (!wc || !wf || c->bc_z != AEO_BC_WALL)) {
+        *m = "the anelastic core needs wc, wf and walls in z";
+        return AEO_ERR_ARGUMENT;
+    }
+    if (c->core != AEO_CORE_BOUSSINESQ && c->core != AEO_CORE_ANELASTIC) { *m = "unknown core"; return AEO_ERR_ARGUMENT; }
+    if (c->stretched && (!zf || c->bc_z != AEO_BC_WALL)) { *m = "a stretched grid needs zf and walls in z"; return AEO_ERR_ARGUMENT; }
+    if (c->precision != AEO_PREC_FP64 && c->precision != AEO_PREC_FP32_MIXED) { *m = "unknown precision"; return AEO_ERR_ARGUMENT; }
+    if (c->c_s != 0.0 && !(c->pr_t > 0.0)) { *m = "pr_t must be positive with SGS"; return AEO_ERR_ARGUMENT; }
+    return AEO_OK;
+}
+
+extern "C" {
+
+aeo_status aeo_create(const aeo_config* cfg, const double* zf, const double* wc, const double* wf, const double* thf,
+                      aeo_sim** out) {
+    if (!out) { g_create_error = "out is NULL"; return AEO_ERR_ARGUMENT; }
+    *out = nullptr;
+    std::string m;
+    if (aeo_status s = validate(cfg, zf, wc, wf, &m)) { g_create_error = m; return s; }
+    cudaError_t e = cudaSetDevice(cfg->device);
+    if (e != cudaSuccess) { g_create_error = std::string("cudaSetDevice: ") + cudaGetErrorString(e); return AEO_ERR_CUDA; }
+    CoreBase* c = cfg->precision == AEO_PREC_FP64 ? (CoreBase*)new (std::nothrow) Core<double>()
+                                                  : (CoreBase*)new (std::nothrow) Core<float>();
+    if (!c) { g_create_error = "out of host memory"; return AEO_ERR_CUDA; }
+    c->cfg = *cfg;
+    aeo_status s = c->init(zf, wc, wf, thf);
+    if (s) { g_create_error = c->err; delete c; return s; }
+    aeo_sim* h = new (std::nothrow) aeo_sim;
+    if (!h) { delete c; g_create_error = "out of host memory"; return AEO_ERR_CUDA; }
+    h->core = c;
+    *out = h;
+    return AEO_OK;
+}
+
+aeo_status aeo_destroy(aeo_sim* h) {
+    if (!h) return AEO_OK;
+    cudaSetDevice(h->core->cfg.device);
+    delete h->core;
+    delete h;
+    return AEO_OK;
+}
+
+#define ENTER(h)                                                       \
+    if (!h) return AEO_ERR_ARGUMENT;                                   \
+    if (cudaSetDevice(h->core->cfg.device) != cudaSuccess) {           \
+        h->core->fail("cudaSetDevice failed");                         \
+        return AEO_ERR_CUDA;                                           \
+    }
+
+aeo_status aeo_set_field(aeo_sim* h, int32_t field, const double* host) {
+    ENTER(h);
+    if (!host) { h->core->fail("host pointer is NULL"); return AEO_ERR_ARGUMENT; }
+    return h->core->set_field(field, host);
+}
+
+aeo_status aeo_get_field(aeo_sim* h, int32_t field, double* host) {
+    ENTER(h);
+    if (!host) { h->core->fail("host pointer is NULL"); return AEO_ERR_ARGUMENT; }
+    return h->core->get_field(field, host);
+}
+
+aeo_status aeo_step_rk3(aeo_sim* h, double dt, int32_t nsteps) {
+    ENTER(h);
+    if (!(dt > 0) || nsteps < 0) { h->core->fail("dt must be positive and nsteps >= 0"); return AEO_ERR_ARGUMENT; }
+    return h->core->step_rk3(dt, nsteps, true);
+}
+
+aeo_status aeo_step_rk3_async(aeo_sim* h, double dt, int32_t nsteps) {
+    ENTER(h);
+    if (!(dt > 0) || nsteps < 0) { h->core->fail("dt must be positive and nsteps >= 0"); return AEO_ERR_ARGUMENT; }
+    return h->core->step_rk3(dt, nsteps, false);
+}
+
+aeo_status aeo_synchronize(aeo_sim* h) {
+    ENTER(h);
+    cudaError_t e = cudaStreamSynchronize(h->core->st);
+    if (e != cudaSuccess) { h->core->fail(cudaGetErrorString(e)); return AEO_ERR_CUDA; }
+    return AEO_OK;
+}
+
+aeo_status aeo_step_euler(aeo_sim* h, double dt, int32_t nsteps) {
+    ENTER(h);
+    if (!(dt > 0) || nsteps < 0) { h->core->fail("dt must be positive and nsteps >= 0"); return AEO_ERR_ARGUMENT; }
+    return h->core->step_euler(dt, nsteps);
+}
+
+aeo_status aeo_project(aeo_sim* h) {
+    ENTER(h);
+    return h->core->project();
+}
+
+aeo_status aeo_pressure_solve(aeo_sim* h, const double* src, double* phi) {
+    ENTER(h);
+    if (!src || !phi) { h->core->fail("NULL array"); return AEO_ERR_ARGUMENT; }
+    return h->core->pressure_solve(src, phi);
+}
+
+aeo_status aeo_kinetic_energy(aeo_sim* h, double* out) {
+    ENTER(h);
+    if (!out) return AEO_ERR_ARGUMENT;
+    return h->core->kinetic_energy(out);
+}
+
+aeo_status aeo_max_divergence(aeo_sim* h, double* out) {
+    ENTER(h);
+    if (!out) return AEO_ERR_ARGUMENT;
+    return h->core->max_divergence(out);
+}
+
+aeo_status aeo_profile_step(aeo_sim* h, double dt, double* ms_per_class, int32_t nclass) {
+    ENTER(h);
+    if (!(dt > 0) || !ms_per_class || nclass < 0) { h->core->fail("bad profile arguments"); return AEO_ERR_ARGUMENT; }
+    return h->core->profile_step(dt, ms_per_class, nclass);
+}
+
+aeo_status aeo_launches_per_step(aeo_sim* h, int32_t* out) {
+    if (!h || !out) return AEO_ERR_ARGUMENT;
+    *out = h->core->launches;
+    return AEO_OK;
+}
+
+void* aeo_stream(aeo_sim* h) { return h ? (void*)h->core->st : nullptr; }
+
+aeo_status aeo_fill_uniform(aeo_sim* h, int32_t field, uint64_t seed, uint32_t stream, double amp, int32_t mode) {
+    ENTER(h);
+    return h->core->fill_uniform(field, seed, stream, amp, mode);
+}
+
+const char* aeo_last_error(const aeo_sim* h) { return h ? h->core->err.c_str() : g_create_error.c_str(); }
+
+const char* aeo_version(void) { return "aeolus_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,394 @@
+#!/usr/bin/env python
+"""bench.py -- cell-steps/s of the projected SSP-RK3 dynamical-core step.
+
+Workload (default "cbl", the dry convective boundary layer): anelastic
+core, 256 x 256 x 128 cells on 5120 m x 5120 m x 2000 m with tanh-stretched
+z (first cell 8 m), rho0(z) = 1.2 exp(-z/8000), theta 300 K to 1 km then
++3 K and 3 K/km, seeded uniform +-0.1 K theta noise in the lowest 10 levels,
+surface heat flux 0.1 K m/s, Smagorinsky C_s = 0.17 (Pr_t = 1/3), walls in
+z, FFT-xy + tridiagonal-z pressure solve, dt = 1 s.  Synthetic inputs from
+the Philox generator (no dataset exists for this case).
+
+One "step" = one projected SSP-RK3 step of the whole grid.  `value` is the
+FP32-mixed step (stencils and horizontal FFTs in FP32, the column solve and
+reductions in FP64) timed with CUDA events on the library's stream with the
+state resident in HBM; the FP64 step is measured the same way and reported
+beside it.  `e2e` is the same metric through the C-ABI with the state copied
+from pinned host memory and back every step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--workload cbl|tgv]
+
+Under torchrun every rank runs an independent replica of the workload (the
+step has no data-path collective on one domain; weak scaling) and rank 0
+prints one JSON line with the max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "aeolus.jl_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+# ----------------------------------------------------------------------------- workloads
+def workload(name):
+    from aeolus_b200 import CoreSpec, regular_grid, stretched_grid, tanh_beta_for_first_cell, tanh_faces
+    from aeolus_b200.inputs import cbl_initial, cbl_theta_profile, taylor_green
+    from aeolus_b200.reference_state import anelastic_profiles, exponential_density
+
+    if name == "cbl":
+        nx, nz, lz = 256, 128, 2000.0
+        beta = tanh_beta_for_first_cell(nz, lz, 8.0)
+        g = stretched_grid((nx, nx, nz), (5120.0, 5120.0, lz), tanh_faces(nz, lz, beta))
+        prof = anelastic_profiles(g, exponential_density(g), cbl_theta_profile(g.znodes("c")))
+
+        def spec(prec):
+            return CoreSpec(grid=g, core="anelastic", c_s=0.17, pr_t=1 / 3, flux_bot=0.1, precision=prec,
+                            wc=prof["wc"], wf=prof["wf"], thf=prof["thf"])
+
+        u, v, w, th, _ = cbl_initial(g, seed=1, noise=0.1, noise_levels=10)
+        desc = {"workload": "dry CBL, anelastic, 256x256x128, tanh z (dz1=8 m, beta=%.4f), Cs=0.17, "
+                            "F=0.1 K m/s, dt=1 s, FFT-xy + tridiagonal-z" % beta,
+                "grid": [nx, nx, nz], "dt": 1.0, "advection": "centred (W-weighted flux form)",
+                "sgs": "Smagorinsky Cs=0.17 Prt=1/3", "l2": "inputs larger than L2 (state ~0.5 GB)"}
+        return g, spec, (u, v, w, th), 1.0, desc, False
+    if name == "tgv":
+        n = 256
+        g = regular_grid((n, n, n), (2 * np.pi,) * 3)
+
+        def spec(prec):
+            return CoreSpec(grid=g, advection="weno_js5", nu=1 / 1600, precision=prec)
+
+        state = taylor_green(g, seed=1, amp=1e-3)
+        desc = {"workload": "Taylor-Green vortex 256^3 triply periodic, WENO-JS5, nu=1/1600, dt=0.01, FFT projection",
+                "grid": [n, n, n], "dt": 0.01, "l2": "inputs larger than L2"}
+        return g, spec, state, 0.01, desc, True
+    raise SystemExit(f"unknown workload {name}")
+
+
+# algorithmic bytes per cell of one launch of each kernel class (field passes
+# P, one compulsory read or write of one interior scalar field), averaged over
+# the three substages; the spectrum holds (nx/2+1)/nx complex per cell.
+def class_passes(cls, g, sgs):
+    sp = 2.0 * (g.nx // 2 + 1) / g.nx  # real words of the spectrum per cell
+    return {
+        "sweep": (8 + 9 + 9) / 3.0,            # R u,v,w,theta (+theta0); W u*,v*,w*,theta
+        "sgs": 4.0,                           # R u,v,w; W nut
+        "div_fftx": 3.0 + sp,                 # R u*,v*,w*; W spectrum
+        "ffty": 2.0 * sp,                     # R+W spectrum
+        "zsolve": 2.0 * sp,                   # R+W spectrum
+        "ifftx": sp + 1.0,                    # R spectrum; W phi
+        "correct": (8 + 11 + 11) / 3.0,       # R u*,v*,w*,phi (+u0,v0,w0); W u,v,w,p
+        "halo": 0.0,
+    }[cls]
+
+
+LAUNCHES_PER_STEP = {"sweep": 3, "sgs": 6, "div_fftx": 3, "ffty": 6, "zsolve": 3, "ifftx": 3, "correct": 3, "halo": 3}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- distributed
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------------------- timing
+def timed_steps(sim, dt, k, world):
+    import torch
+    stream = torch.cuda.ExternalStream(sim.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    sim.synchronize()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    sim.step_rk3_async(dt, k)
+    e1.record(stream)
+    sim.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    return e0.elapsed_time(e1)
+
+
+def e2e_steps(sim, state, dt, k):
+    """Through the C-ABI with host buffers: every step uploads u, v, w, theta
+    from pinned host memory, steps, and downloads them again."""
+    import torch
+    pinned = []
+    for a in state:
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = a
+        pinned.append(t.numpy())
+    outs = [torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy() for a in state]
+    stream = torch.cuda.ExternalStream(sim.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sim.synchronize()
+    e0.record(stream)
+    for _ in range(k):
+        for n, a in zip(("u", "v", "w", "theta"), pinned):
+            sim.set_field(n, a)
+        sim.step_rk3(dt, 1)
+        for n, o in zip(("u", "v", "w", "theta"), outs):
+            sim.get_field(n, o)
+    e1.record(stream)
+    sim.synchronize()
+    nbytes = sum(a.nbytes for a in pinned)
+    return e0.elapsed_time(e1) / k, nbytes, sum(o.nbytes for o in outs)
+
+
+def cpu_oracle_rate(spec, state, dt, min_seconds=10.0, max_steps=20):
+    """The oracle (CPU restatement) on the host cores, full grid."""
+    from oracle.oracle import OracleSimulation, set_threads
+    cores = os.cpu_count() or 1
+    set_threads(cores)
+    o = OracleSimulation(spec)
+    o.set_state(*state)
+    o.step_rk3(dt, 1)  # warm-up
+    n, t0 = 0, time.perf_counter()
+    while True:
+        o.step_rk3(dt, 1)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= min_seconds or n >= max_steps:
+            break
+    o.close()
+    return spec.grid.ncells * n / el, cores, n, el
+
+
+# ----------------------------------------------------------------------------- arms
+def run_reference(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    g, mkspec, state, dt, desc, _ = workload(args.workload)
+    spec = mkspec("fp64")
+    from oracle.oracle import OracleSimulation, set_threads
+    cores = os.cpu_count() or 1
+    set_threads(cores)
+    o = OracleSimulation(spec)
+    o.set_state(*state)
+    o.step_rk3(dt, max(1, args.warmup))
+    t0 = time.perf_counter()
+    o.step_rk3(dt, args.steps)
+    el = time.perf_counter() - t0
+    value = g.ncells * args.steps / el
+    line = {
+        "impl": "reference", "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": desc,
+        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} RK3 steps of the full {desc['grid']} grid after {max(1, args.warmup)} "
+                                   f"warm-up steps; the reference is Julia (not installable), this is the "
+                                   f"C/OpenMP FP64 restatement of its step"},
+        "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args):
+    world, rank, local = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    from aeolus_b200 import _lib
+    from aeolus_b200.simulation import Simulation
+
+    g, mkspec, state, dt, desc, _ = workload(args.workload)
+    hbm, hbm_kind = measured_peaks()
+    results = {}
+    for prec in ("fp32_mixed", "fp64"):
+        sim = Simulation(mkspec(prec), device=local)
+        sim.set_state(*state)
+        sim.step_rk3(dt, args.warmup)
+        prof = sim.profile_step(dt)           # per-kernel-class device time, one un-graphed step
+        sim.step_rk3(dt, 1)
+        clk = ClockSampler(local)
+        clk.start()
+        ms_total = timed_steps(sim, dt, args.steps, world)
+        clocks = clk.stop()
+        ms_total = max_over_ranks(ms_total, world)
+        ms = ms_total / args.steps
+        e2e_ms, h2d, d2h = e2e_steps(sim, state, dt, max(2, min(args.steps, 5)))
+        e2e_ms = max_over_ranks(e2e_ms, world)
+        results[prec] = dict(ms=ms, prof=prof, clocks=clocks, e2e_ms=e2e_ms, h2d=h2d, d2h=d2h,
+                             launches=sim.launches_per_step(), div=sim.max_divergence(),
+                             ke=sim.kinetic_energy())
+        sim.close()
+        del sim
+    if rank != 0:
+        barrier(world)
+        return 0
+    main = results["fp32_mixed"]
+    ncell = g.ncells
+    value = world * ncell / (main["ms"] * 1e-3)
+    sgs = True
+    # roofline of the dominant kernel class
+    prof = main["prof"]
+    dom = max(prof, key=lambda c: prof[c])
+    s = 4  # fp32 words
+    passes = class_passes(dom, g, sgs)
+    per_launch_ms = prof[dom] / LAUNCHES_PER_STEP[dom]
+    bytes_per_launch = passes * s * ncell
+    achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
+    kernels = {}
+    for c, v in prof.items():
+        if v <= 0:
+            continue
+        pl = v / LAUNCHES_PER_STEP[c]
+        b = class_passes(c, g, sgs) * s * ncell
+        kernels[c] = {"ms_per_step": round(v, 4), "share": round(v / sum(prof.values()), 4),
+                      "GBps_per_launch": round(b / (pl * 1e-3) / 1e9, 1) if b > 0 else None}
+    step_bytes = 392.0 * ncell  # FP32-mixed algorithmic bytes per cell-step
+    fp64 = results["fp64"]
+    line = {
+        "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": main["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32-mixed (FP32 stencils/FFT, FP64 column solve and reductions)",
+        "data": "synthetic (Philox-seeded CBL initial state)",
+        "config": dict(desc, parallelism=f"replicas x{world}" if world > 1 else "1 GPU"),
+        "fp64": {"value": world * ncell / (fp64["ms"] * 1e-3), "ms_per_step": fp64["ms"],
+                 "e2e": world * ncell / (fp64["e2e_ms"] * 1e-3), "max_divergence": fp64["div"]},
+        "e2e": {"value": world * ncell / (main["e2e_ms"] * 1e-3), "unit": "cell-steps/s",
+                "h2d_bytes_per_step": main["h2d"], "d2h_bytes_per_step": main["d2h"]},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm,
+                     "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_kind": hbm_kind,
+                     "bytes_per_launch": bytes_per_launch, "traffic": None},
+        "step_roofline": {"algorithmic_bytes_per_cell_step": 392, "achieved_GBps": round(
+            step_bytes / (main["ms"] * 1e-3) / 1e9, 1), "frac": round(step_bytes / (main["ms"] * 1e-3) / 1e9 / hbm, 4)},
+        "kernels": kernels,
+        "gpu_launches": main["launches"] * args.steps,
+        "clocks": main["clocks"],
+        "max_divergence": main["div"],
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        rate, cores, n, el = cpu_oracle_rate(mkspec("fp64"), state, dt)
+        line["cpu_baseline"] = {"value": rate, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+                                "sample": f"{n} RK3 steps of the full grid ({el:.1f} s), FP64 oracle, "
+                                          f"{cores} OpenMP threads"}
+    print(json.dumps(line), flush=True)
+    barrier(world)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="cbl", choices=["cbl", "tgv"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rc = run_reference(args) if args.impl == "reference" else run_b200(args)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        import torch.distributed as dist
+        if dist.is_initialized():
+            dist.destroy_process_group()
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())

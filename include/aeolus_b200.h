@@ -1,0 +1,168 @@
+/*
+ * aeolus_b200.h -- the C-ABI of libaeolus_b200.so, the B200 (sm_100a)
+ * dynamical-core step of the Aeolus.jl large-eddy-simulation model.
+ *
+ * One handle owns all device state of one domain (one simulation).  Host
+ * arrays crossing this interface are in the reference's storage layout: a
+ * Float64 field of Nx x Ny x Nz interior cells with halos (Hx, Hy, Hz) is a
+ * column-major (x fastest) array of (Nx+2Hx)(Ny+2Hy)(Nz+2Hz) doubles, i.e.
+ * the `Field.data` array of the reference (src/Fields.jl:21,
+ * src/Grids.jl:98-130), so a Julia `ccall` passes it by pointer with no
+ * reshuffle.  No host pointer is retained after a call returns.
+ *
+ * Every entry point returns an aeo_status; on failure aeo_last_error(h)
+ * describes it.  A handle is not thread-safe; distinct handles are
+ * independent.  Work is enqueued on the handle's own CUDA stream and every
+ * call below returns after that stream has synchronised.
+ *
+ * Each entry point names the reference interface it replaces.
+ */
+#ifndef AEOLUS_B200_H
+#define AEOLUS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    AEO_OK = 0,
+    AEO_ERR_ARGUMENT = 1,   /* maps to ArgumentError in the host shim */
+    AEO_ERR_CUDA = 2,       /* CUDA runtime failure (message in aeo_last_error) */
+    AEO_ERR_NUMERICAL = 3,  /* non-finite state or failed solve: NumericalFailure */
+    AEO_ERR_STATE = 4       /* call out of order (e.g. no field set yet) */
+} aeo_status;
+
+enum { AEO_BC_PERIODIC = 0, AEO_BC_WALL = 1 };
+enum { AEO_CORE_BOUSSINESQ = 0, AEO_CORE_ANELASTIC = 1 };
+enum { AEO_ADV_CENTRED = 0, AEO_ADV_WENO_JS5 = 1, AEO_ADV_WENO_Z5 = 2 };
+enum { AEO_SOLVER_FFT = 0, AEO_SOLVER_COLUMN = 1 };
+enum { AEO_PREC_FP64 = 0, AEO_PREC_FP32_MIXED = 1 };
+enum { AEO_FIELD_U = 0, AEO_FIELD_V = 1, AEO_FIELD_W = 2, AEO_FIELD_THETA = 3,
+       AEO_FIELD_P = 4, AEO_FIELD_NUT = 5 };
+
+/* Grid + physics of one domain.  Mirrors the keyword set of
+ * BoussinesqSimulation (src/Simulations.jl:232-246) and of the sound-proof
+ * MassWeightedSimulation (src/Anelastic.jl:1559), the mesh of RegularGrid /
+ * StretchedGrid (src/Grids.jl:98, src/StretchedGrids.jl:345) and the
+ * FieldBoundaryConditions kinds of src/BoundaryConditions.jl:54-74
+ * (x, y periodic; z periodic or ImpermeableWall). */
+typedef struct {
+    int32_t nx, ny, nz;        /* interior cells (nx even)                     */
+    int32_t hx, hy, hz;        /* halo widths of the HOST storage arrays       */
+    double lx, ly, lz;         /* domain extent                                */
+    double x0, y0, z0;         /* origin                                       */
+    int32_t bc_x, bc_y, bc_z;  /* AEO_BC_*; x and y must be periodic           */
+    int32_t stretched;         /* 1: zf gives the Nz+1 interior face heights   */
+    int32_t core;              /* AEO_CORE_*                                   */
+    int32_t advection;         /* AEO_ADV_* (momentum and theta)               */
+    int32_t solver;            /* AEO_SOLVER_FFT (triply periodic) or COLUMN   */
+    int32_t precision;         /* AEO_PREC_*                                   */
+    double nu;                 /* molecular viscosity / diffusivity (0 = off)  */
+    double theta0;             /* Boussinesq reference theta (0 = no buoyancy) */
+    double g;                  /* gravitational acceleration                   */
+    double f_coriolis;         /* Coriolis parameter (0 = off)                 */
+    double c_s;                /* Smagorinsky constant (0 = no SGS)            */
+    double pr_t;               /* turbulent Prandtl number                     */
+    double flux_bot, flux_top; /* prescribed wall fluxes of theta              */
+    double sponge_alpha;       /* Rayleigh sponge rate (0 = off)               */
+    double sponge_zstart;      /* sponge bottom                                */
+    int32_t device;            /* CUDA device ordinal                          */
+} aeo_config;
+
+typedef struct aeo_sim aeo_sim;
+
+/* Create a domain.  zf: Nz+1 interior face heights when cfg->stretched
+ * (StretchedGrid(stretching = (:custom, zf))), else NULL.  Anelastic core:
+ * wc (Nz+2Hz) and wf (Nz+2Hz+1) are the halo-padded constraint weights
+ * (ReferenceState.ρ̄c_pad / ρ̄f_pad, src/Anelastic.jl:232-233, :375-380) and
+ * thf (Nz+2Hz+1) the padded face reference theta (θ̄f_pad) of the buoyancy;
+ * NULL for the Boussinesq core.  Replaces the constructors
+ * BoussinesqSimulation (src/Simulations.jl:232) and the sound-proof
+ * simulation of src/Anelastic.jl:1559 together with their default pressure
+ * solvers (_default_solver, src/Simulations.jl:1137; DirectWeightedPoissonSolver,
+ * src/Anelastic.jl:997). */
+aeo_status aeo_create(const aeo_config* cfg, const double* zf, const double* wc,
+                      const double* wf, const double* thf, aeo_sim** out);
+
+/* Release the domain and all its device memory. */
+aeo_status aeo_destroy(aeo_sim* h);
+
+/* Copy a host Field.data array (storage layout, halos ignored on input) into
+ * the domain.  Replaces writes into sim.u/v/w/θ.data (src/Simulations.jl:201-206)
+ * followed by fill_state_halos! (src/Simulations.jl:1028). */
+aeo_status aeo_set_field(aeo_sim* h, int32_t field, const double* host);
+
+/* Copy a field to a host Field.data array (storage layout).  u, v, w, θ come
+ * back with halos filled from the interior by the boundary conditions
+ * (fill_halos!, src/boundary_conditions/halo_sets.jl:176); p and νt with
+ * zero halos. */
+aeo_status aeo_get_field(aeo_sim* h, int32_t field, double* host);
+
+/* nsteps projected SSP-RK3 steps of size dt: step_rk3! of the Boussinesq
+ * core (src/Simulations.jl:843-904) or of the sound-proof core
+ * (src/Anelastic.jl:1905-1948).  The whole step is one CUDA graph. */
+aeo_status aeo_step_rk3(aeo_sim* h, double dt, int32_t nsteps);
+
+/* nsteps forward-Euler projection steps: step! (src/Simulations.jl:481-650,
+ * src/Anelastic.jl:1747-1876). */
+aeo_status aeo_step_euler(aeo_sim* h, double dt, int32_t nsteps);
+
+/* The projection's Poisson solve on interior-sized arrays (Nx*Ny*Nz, x
+ * fastest): solve!(p, source, solver) / solve_source_buffer! of the
+ * AbstractPressureSolver seam (src/PressureSolvers.jl:41-80, :162-174,
+ * :712-732).  Zero-mean gauge (FFT) or the column solver's gauge. */
+aeo_status aeo_pressure_solve(aeo_sim* h, const double* src, double* phi);
+
+/* Project the current velocity onto the discretely solenoidal fields (one
+ * Chorin projection with dt = 1, p = phi): the config driver's
+ * `_project!(sim, 1.0)` of a noisy initial field
+ * (src/config/simulation_driver.jl:1316; src/Simulations.jl:711-744). */
+aeo_status aeo_project(aeo_sim* h);
+
+/* kinetic_energy (src/Simulations.jl:992-1014) and max_divergence
+ * (src/Simulations.jl:1045-1050; the W-normalised residual
+ * (1/W)∇·(W u) for the anelastic core, src/Anelastic.jl:1134-1142). */
+aeo_status aeo_kinetic_energy(aeo_sim* h, double* out);
+aeo_status aeo_max_divergence(aeo_sim* h, double* out);
+
+/* Device-resident stepping for benchmarks and graph-captured drivers: the
+ * same as aeo_step_rk3 but returns without synchronising the stream. */
+aeo_status aeo_step_rk3_async(aeo_sim* h, double dt, int32_t nsteps);
+aeo_status aeo_synchronize(aeo_sim* h);
+
+/* Kernel classes of one substage, for aeo_profile_step. */
+enum { AEO_K_SGS = 0, AEO_K_SWEEP = 1, AEO_K_DIV_FFTX = 2, AEO_K_FFTY = 3, AEO_K_ZSOLVE = 4,
+       AEO_K_IFFTX = 5, AEO_K_CORRECT = 6, AEO_K_HALO = 7, AEO_K_NCLASS = 8 };
+
+/* One RK3 step run launch by launch (not as a graph) with CUDA events
+ * recorded on the handle's stream between kernel groups; ms_per_class[c]
+ * receives the summed device time of class c over the step.  Advances the
+ * state like aeo_step_rk3.  The reference's per-stage wall times of
+ * StepRecord (src/simulations/step_record.jl:1-263) are the analogue. */
+aeo_status aeo_profile_step(aeo_sim* h, double dt, double* ms_per_class, int32_t nclass);
+
+/* Number of kernel launches one RK3 step issues (for launch accounting). */
+aeo_status aeo_launches_per_step(aeo_sim* h, int32_t* out);
+
+/* The handle's CUDA stream (a cudaStream_t) for callers that time kernels. */
+void* aeo_stream(aeo_sim* h);
+
+/* Philox4x32-10 uniform fill on the device: out[i] = amp*(2*U(seed, stream, i)-1)
+ * for i < n, written into the given field's interior in storage order
+ * (the synthetic-input generator of Backends.counter_rng, src/Backends.jl:1607-1739).
+ * mode 0 overwrites, mode 1 adds. */
+aeo_status aeo_fill_uniform(aeo_sim* h, int32_t field, uint64_t seed, uint32_t stream,
+                            double amp, int32_t mode);
+
+/* Last error message of the handle (or of the last failed aeo_create when h is NULL). */
+const char* aeo_last_error(const aeo_sim* h);
+
+/* Library version string. */
+const char* aeo_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1322 @@
+/*
+ * aeolus_oracle.c -- TEST INFRASTRUCTURE ONLY (the oracle).
+ *
+ * A CPU FP64 restatement of the Aeolus.jl dynamical-core time step, used as
+ * the checker for the CUDA library and as the timed CPU baseline.  The
+ * product path never links or calls this file.  Every function names the
+ * reference lines (path:line inside the Aeolus.jl project) it restates; the
+ * arithmetic follows the reference's expression order so that the oracle
+ * differs from the reference by round-off only.
+ *
+ * Parity pins: the reference is Julia (not installable here), so the oracle
+ * is pinned by the reference's own known-answer and analytic tests restated
+ * in tests/ (Philox4x32-10 KATs of test/backends.jl:265-276, the discrete
+ * Poisson identities of test/runtests.jl:168-260 and
+ * test/pressure_column.jl:13-117, the projection's round-off divergence,
+ * WENO design order of test/advection.jl:52-188, the TGV modified-wavenumber
+ * decay of test/ka_step.jl:138-147).
+ *
+ * Build: oracle/Makefile (gcc -O2 -fopenmp -ffp-contract=off; no fast-math,
+ * no FMA contraction, so that each operation rounds as Julia's does).
+ */
+#include "aeolus_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define LOC_C 0
+#define LOC_FX 1
+#define LOC_FY 2
+#define LOC_FZ 3
+
+typedef struct { double re, im; } cpx;
+
+typedef struct {
+    int n;          /* transform length */
+    int pow2;       /* 1 when n is a power of two */
+    cpx* tw;        /* e^{-2 pi i k / n}, k < n */
+    int* rev;       /* bit reversal (pow2 only) */
+} fft_plan;
+
+struct oc_sim {
+    oc_params p;
+    int NX, NY, NZ;
+    int64_t n;                   /* storage points */
+    /* metrics (src/FiniteVolume.jl:71-186, src/StretchedGrids.jl:560-590) */
+    int uniform;
+    double dx, dy, dz, idx, idy, idx2, idy2, idz, idz2, delta_u;
+    double *zf, *zc, *dzc, *dzf;                  /* storage levels */
+    double *idzc, *idzf, *idz_off, *wlo, *whi, *alo, *ahi, *delta;
+    /* anelastic weights (padded) */
+    double *wc, *wf, *thf;
+    /* fields (storage layout) */
+    double *u, *v, *w, *th, *pr, *nut, *kt, *phi;
+    double *tu, *tv, *tw, *tt;
+    double *u0, *v0, *w0, *th0;
+    /* pressure solver */
+    double* src;                 /* interior-sized */
+    cpx* hat;                    /* (Nx/2+1) x Ny x Nz */
+    double *kx2, *ky2, *kz2;     /* eigenvalue pieces */
+    double *lower, *upper, *hw, *meas, *iota, *gauge;
+    double meas_sum, gauge_sum;
+    fft_plan px, py, pz;         /* px: length Nx/2 (the packed r2c) */
+    cpx* twx;                    /* e^{-2 pi i k / Nx}, k <= Nx/2 */
+};
+
+#define ID(s, i, j, k) ((int64_t)(i) + (int64_t)(s)->NX * ((int64_t)(j) + (int64_t)(s)->NY * (int64_t)(k)))
+#define A(f, i, j, k) (f)[ID(s, i, j, k)]
+
+/* ------------------------------------------------------------------------- */
+/* Philox4x32-10 (src/Backends.jl:1607-1640) and the uniform fill            */
+/* ------------------------------------------------------------------------- */
+
+void oc_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 1; r <= 10; ++r) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * (uint64_t)c0;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * (uint64_t)c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        if (r < 10) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+/* The first 64-bit draw of the counter stream (seed, stream, id)
+ * (src/Backends.jl:1707-1739: key = (seed>>32, seed), counter =
+ * (block 0, stream, id lo, id hi), draw = x1<<32 | x0) mapped to [0,1) by
+ * its top 53 bits, then to [-amp, amp]. */
+static double philox_uniform(uint64_t seed, uint32_t stream, uint64_t id) {
+    uint32_t key[2] = {(uint32_t)(seed >> 32), (uint32_t)seed};
+    uint32_t ctr[4] = {0u, stream, (uint32_t)id, (uint32_t)(id >> 32)};
+    uint32_t o[4];
+    oc_philox4x32(ctr, key, o);
+    uint64_t x = ((uint64_t)o[1] << 32) | (uint64_t)o[0];
+    return (double)(x >> 11) * 0x1.0p-53;
+}
+
+void oc_uniform_fill(uint64_t seed, uint32_t stream, int64_t n, double amp, double* out) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) out[i] = amp * (2.0 * philox_uniform(seed, stream, (uint64_t)i) - 1.0);
+}
+
+void oc_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+/* ------------------------------------------------------------------------- */
+/* FFT: own radix-2 (power of two) or direct DFT (other lengths)             */
+/* ------------------------------------------------------------------------- */
+
+static void plan_init(fft_plan* pl, int n) {
+    pl->n = n;
+    pl->pow2 = (n > 0) && ((n & (n - 1)) == 0);
+    pl->tw = (cpx*)malloc(sizeof(cpx) * (size_t)(n > 0 ? n : 1));
+    for (int k = 0; k < n; ++k) {
+        double a = -2.0 * M_PI * (double)k / (double)n;
+        pl->tw[k].re = cos(a);
+        pl->tw[k].im = sin(a);
+    }
+    pl->rev = NULL;
+    if (pl->pow2) {
+        pl->rev = (int*)malloc(sizeof(int) * (size_t)n);
+        int lg = 0;
+        while ((1 << lg) < n) ++lg;
+        for (int i = 0; i < n; ++i) {
+            int r = 0;
+            for (int b = 0; b < lg; ++b) if (i & (1 << b)) r |= 1 << (lg - 1 - b);
+            pl->rev[i] = r;
+        }
+    }
+}
+
+static void plan_free(fft_plan* pl) { free(pl->tw); free(pl->rev); }
+
+/* In-place unnormalised DFT of a (length pl->n); sign -1 forward, +1 inverse.
+ * tmp: scratch of length n. */
+static void fft_c(const fft_plan* pl, cpx* a, int inverse, cpx* tmp) {
+    int n = pl->n;
+    if (n <= 1) return;
+    if (!pl->pow2) {
+        for (int k = 0; k < n; ++k) {
+            double sr = 0.0, si = 0.0;
+            for (int j = 0; j < n; ++j) {
+                int m = (int)(((int64_t)j * k) % n);
+                double wr = pl->tw[m].re, wi = inverse ? -pl->tw[m].im : pl->tw[m].im;
+                sr += a[j].re * wr - a[j].im * wi;
+                si += a[j].re * wi + a[j].im * wr;
+            }
+            tmp[k].re = sr; tmp[k].im = si;
+        }
+        memcpy(a, tmp, sizeof(cpx) * (size_t)n);
+        return;
+    }
+    for (int i = 0; i < n; ++i) {
+        int r = pl->rev[i];
+        if (r > i) { cpx t = a[i]; a[i] = a[r]; a[r] = t; }
+    }
+    for (int len = 2; len <= n; len <<= 1) {
+        int half = len >> 1, step = n / len;
+        for (int b = 0; b < n; b += len) {
+            for (int j = 0; j < half; ++j) {
+                cpx wv = pl->tw[j * step];
+                if (inverse) wv.im = -wv.im;
+                cpx x = a[b + j], y = a[b + j + half];
+                cpx t = {y.re * wv.re - y.im * wv.im, y.re * wv.im + y.im * wv.re};
+                a[b + j].re = x.re + t.re; a[b + j].im = x.im + t.im;
+                a[b + j + half].re = x.re - t.re; a[b + j + half].im = x.im - t.im;
+            }
+        }
+    }
+}
+
+/* Real-to-complex forward DFT of x (length N = 2M) to X[0..M], by the
+ * packed length-M complex transform. z: scratch M+1, tmp: scratch M. */
+static void rfft_row(const oc_sim* s, const double* x, cpx* X, cpx* z, cpx* tmp) {
+    int N = s->p.nx, M = N / 2;
+    for (int n = 0; n < M; ++n) { z[n].re = x[2 * n]; z[n].im = x[2 * n + 1]; }
+    fft_c(&s->px, z, 0, tmp);
+    z[M] = z[0];
+    for (int k = 0; k <= M; ++k) {
+        cpx a = z[k], b = z[M - k];
+        double er = 0.5 * (a.re + b.re), ei = 0.5 * (a.im - b.im);
+        double orr = 0.5 * (a.im + b.im), oi = -0.5 * (a.re - b.re);
+        cpx w = s->twx[k];
+        X[k].re = er + (w.re * orr - w.im * oi);
+        X[k].im = ei + (w.re * oi + w.im * orr);
+    }
+}
+
+/* Unnormalised complex-to-real inverse (FFTW brfft): x[n] = sum over the
+ * Hermitian spectrum of X[k] e^{+2 pi i k n / N}. */
+static void irfft_row(const oc_sim* s, const cpx* X, double* x, cpx* z, cpx* tmp) {
+    int N = s->p.nx, M = N / 2;
+    for (int k = 0; k < M; ++k) {
+        cpx a = X[k], b = X[M - k];
+        double er = a.re + b.re, ei = a.im - b.im;          /* X_k + conj X_{M-k} */
+        double dr = a.re - b.re, di = a.im + b.im;          /* X_k - conj X_{M-k} */
+        cpx w = s->twx[k];                                  /* multiply by conj(w) */
+        double orr = dr * w.re + di * w.im, oi = di * w.re - dr * w.im;
+        z[k].re = er - oi;                                  /* E + i O */
+        z[k].im = ei + orr;
+    }
+    fft_c(&s->px, z, 1, tmp);
+    for (int n = 0; n < M; ++n) { x[2 * n] = z[n].re; x[2 * n + 1] = z[n].im; }
+}
+
+/* ------------------------------------------------------------------------- */
+/* Metric accessors (src/FiniteVolume.jl:146-186)                             */
+/* ------------------------------------------------------------------------- */
+
+static inline double m_idz(const oc_sim* s, int k) { return s->uniform ? s->idz : s->idzc[k]; }
+static inline double m_idzf(const oc_sim* s, int k) { return s->uniform ? s->idz : s->idzf[k]; }
+static inline double m_idz_off(const oc_sim* s, int k) { return s->uniform ? s->idz : s->idz_off[k]; }
+static inline double m_zface(const oc_sim* s, int k, double lo, double hi) {
+    return s->uniform ? 0.5 * (lo + hi) : s->wlo[k] * lo + s->whi[k] * hi;
+}
+static inline double m_zflux(const oc_sim* s, int k, double lo, double hi) {
+    return s->uniform ? 0.5 * (lo + hi) : s->alo[k] * lo + s->ahi[k] * hi;
+}
+static inline double m_lapz(const oc_sim* s, int loc, int k, double fm, double c, double fp) {
+    if (s->uniform) return (fp - 2 * c + fm) * s->idz2;
+    if (loc == LOC_FZ) return ((fp - c) * s->idzc[k] - (c - fm) * s->idzc[k - 1]) * s->idzf[k];
+    return ((fp - c) * s->idzf[k + 1] - (c - fm) * s->idzf[k]) * s->idzc[k];
+}
+static inline double m_filter(const oc_sim* s, int k) { return s->uniform ? s->delta_u : s->delta[k]; }
+
+/* ------------------------------------------------------------------------- */
+/* Halo fills (src/boundary_conditions/halo_kernels.jl:100-140,               */
+/* src/BoundaryConditions.jl:228-258): x, then y, then z.                     */
+/* ------------------------------------------------------------------------- */
+
+static void fill_halos(oc_sim* s, double* d, int loc) {
+    int NX = s->NX, NY = s->NY, NZ = s->NZ;
+    int Hx = s->p.hx, Hy = s->p.hy, Hz = s->p.hz, Nx = s->p.nx, Ny = s->p.ny, Nz = s->p.nz;
+    /* x: periodic */
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < NZ; ++k)
+        for (int j = 0; j < NY; ++j)
+            for (int h = 1; h <= Hx; ++h) {
+                A(d, h - 1, j, k) = A(d, Nx + h - 1, j, k);
+                A(d, Hx + Nx + h - 1, j, k) = A(d, Hx + h - 1, j, k);
+            }
+    /* y: periodic */
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < NZ; ++k)
+        for (int h = 1; h <= Hy; ++h)
+            for (int i = 0; i < NX; ++i) {
+                A(d, i, h - 1, k) = A(d, i, Ny + h - 1, k);
+                A(d, i, Hy + Ny + h - 1, k) = A(d, i, Hy + h - 1, k);
+            }
+    /* z */
+    if (s->p.bc_z == OC_BC_PERIODIC) {
+#pragma omp parallel for schedule(static)
+        for (int j = 0; j < NY; ++j)
+            for (int h = 1; h <= Hz; ++h)
+                for (int i = 0; i < NX; ++i) {
+                    A(d, i, j, h - 1) = A(d, i, j, Nz + h - 1);
+                    A(d, i, j, Hz + Nz + h - 1) = A(d, i, j, Hz + h - 1);
+                }
+    } else if (loc != LOC_FZ) {
+        /* ImpermeableWall on C / FaceX / FaceY: mirror (NoFlux) */
+#pragma omp parallel for schedule(static)
+        for (int j = 0; j < NY; ++j)
+            for (int h = 1; h <= Hz; ++h)
+                for (int i = 0; i < NX; ++i) {
+                    A(d, i, j, Hz - h) = A(d, i, j, Hz + h - 1);
+                    A(d, i, j, Hz + Nz + h - 1) = A(d, i, j, Hz + Nz - h);
+                }
+    } else {
+        /* ImpermeableWall on FaceZ: wall faces zero, odd extension */
+#pragma omp parallel for schedule(static)
+        for (int j = 0; j < NY; ++j) {
+            for (int i = 0; i < NX; ++i) {
+                A(d, i, j, Hz) = 0.0;
+                if (Hz + Nz < NZ) A(d, i, j, Hz + Nz) = 0.0;
+            }
+            for (int h = 1; h <= Hz; ++h)
+                for (int i = 0; i < NX; ++i) {
+                    A(d, i, j, Hz - h) = -A(d, i, j, Hz + h);
+                    int dst = Hz + Nz + h;
+                    if (dst < NZ) A(d, i, j, dst) = -A(d, i, j, Hz + Nz - h);
+                }
+        }
+    }
+}
+
+void oc_fill_state_halos(oc_sim* s) {
+    fill_halos(s, s->u, LOC_FX);
+    fill_halos(s, s->v, LOC_FY);
+    fill_halos(s, s->w, LOC_FZ);
+    fill_halos(s, s->th, LOC_C);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Point operators                                                            */
+/* ------------------------------------------------------------------------- */
+
+/* seven-point Laplacian (src/FiniteVolume.jl:271-280) */
+static inline double lap_at(const oc_sim* s, const double* f, int i, int j, int k, int loc) {
+    double c = A(f, i, j, k);
+    return (A(f, i + 1, j, k) - 2 * c + A(f, i - 1, j, k)) * s->idx2 +
+           (A(f, i, j + 1, k) - 2 * c + A(f, i, j - 1, k)) * s->idy2 +
+           m_lapz(s, loc, k, A(f, i, j, k - 1), c, A(f, i, j, k + 1));
+}
+
+/* centred flux-form momentum advection (src/FiniteVolume.jl:730-797) */
+static inline double mom_u_at(const oc_sim* s, const double* u, const double* v, const double* w, int i, int j, int k) {
+    double uce = 0.5 * (A(u, i, j, k) + A(u, i + 1, j, k));
+    double ucw = 0.5 * (A(u, i - 1, j, k) + A(u, i, j, k));
+    double d_uu_dx = (uce * uce - ucw * ucw) * s->idx;
+    double vun = 0.5 * (A(v, i - 1, j + 1, k) + A(v, i, j + 1, k));
+    double uvn = 0.5 * (A(u, i, j, k) + A(u, i, j + 1, k));
+    double vus = 0.5 * (A(v, i - 1, j, k) + A(v, i, j, k));
+    double uvs = 0.5 * (A(u, i, j - 1, k) + A(u, i, j, k));
+    double d_vu_dy = (vun * uvn - vus * uvs) * s->idy;
+    double wut = 0.5 * (A(w, i - 1, j, k + 1) + A(w, i, j, k + 1));
+    double uwt = 0.5 * (A(u, i, j, k) + A(u, i, j, k + 1));
+    double wub = 0.5 * (A(w, i - 1, j, k) + A(w, i, j, k));
+    double uwb = 0.5 * (A(u, i, j, k - 1) + A(u, i, j, k));
+    double d_wu_dz = (wut * uwt - wub * uwb) * m_idz(s, k);
+    return d_uu_dx + d_vu_dy + d_wu_dz;
+}
+
+static inline double mom_v_at(const oc_sim* s, const double* u, const double* v, const double* w, int i, int j, int k) {
+    double uve = 0.5 * (A(u, i + 1, j - 1, k) + A(u, i + 1, j, k));
+    double vue = 0.5 * (A(v, i, j, k) + A(v, i + 1, j, k));
+    double uvw = 0.5 * (A(u, i, j - 1, k) + A(u, i, j, k));
+    double vuw = 0.5 * (A(v, i - 1, j, k) + A(v, i, j, k));
+    double d_uv_dx = (uve * vue - uvw * vuw) * s->idx;
+    double vcn = 0.5 * (A(v, i, j, k) + A(v, i, j + 1, k));
+    double vcs = 0.5 * (A(v, i, j - 1, k) + A(v, i, j, k));
+    double d_vv_dy = (vcn * vcn - vcs * vcs) * s->idy;
+    double wvt = 0.5 * (A(w, i, j - 1, k + 1) + A(w, i, j, k + 1));
+    double vwt = 0.5 * (A(v, i, j, k) + A(v, i, j, k + 1));
+    double wvb = 0.5 * (A(w, i, j - 1, k) + A(w, i, j, k));
+    double vwb = 0.5 * (A(v, i, j, k - 1) + A(v, i, j, k));
+    double d_wv_dz = (wvt * vwt - wvb * vwb) * m_idz(s, k);
+    return d_uv_dx + d_vv_dy + d_wv_dz;
+}
+
+static inline double mom_w_at(const oc_sim* s, const double* u, const double* v, const double* w, int i, int j, int k) {
+    double uwe = m_zflux(s, k, A(u, i + 1, j, k - 1), A(u, i + 1, j, k));
+    double wue = 0.5 * (A(w, i, j, k) + A(w, i + 1, j, k));
+    double uww = m_zflux(s, k, A(u, i, j, k - 1), A(u, i, j, k));
+    double wuw = 0.5 * (A(w, i - 1, j, k) + A(w, i, j, k));
+    double d_uw_dx = (uwe * wue - uww * wuw) * s->idx;
+    double vwn = m_zflux(s, k, A(v, i, j + 1, k - 1), A(v, i, j + 1, k));
+    double wvn = 0.5 * (A(w, i, j, k) + A(w, i, j + 1, k));
+    double vws = m_zflux(s, k, A(v, i, j, k - 1), A(v, i, j, k));
+    double wvs = 0.5 * (A(w, i, j - 1, k) + A(w, i, j, k));
+    double d_vw_dy = (vwn * wvn - vws * wvs) * s->idy;
+    double wct = 0.5 * (A(w, i, j, k) + A(w, i, j, k + 1));
+    double wcb = 0.5 * (A(w, i, j, k - 1) + A(w, i, j, k));
+    double d_ww_dz = (wct * wct - wcb * wcb) * m_idzf(s, k);
+    return d_uw_dx + d_vw_dy + d_ww_dz;
+}
+
+/* centred flux-form scalar advection (src/FiniteVolume.jl:1682-1693) */
+static inline double adv_centred_at(const oc_sim* s, const double* u, const double* v, const double* w,
+                                    const double* d, int i, int j, int k) {
+    double ue = A(u, i + 1, j, k) * 0.5 * (A(d, i, j, k) + A(d, i + 1, j, k));
+    double uw = A(u, i, j, k) * 0.5 * (A(d, i - 1, j, k) + A(d, i, j, k));
+    double vn = A(v, i, j + 1, k) * 0.5 * (A(d, i, j, k) + A(d, i, j + 1, k));
+    double vs = A(v, i, j, k) * 0.5 * (A(d, i, j - 1, k) + A(d, i, j, k));
+    double wt = A(w, i, j, k + 1) * 0.5 * (A(d, i, j, k) + A(d, i, j, k + 1));
+    double wb = A(w, i, j, k) * 0.5 * (A(d, i, j, k - 1) + A(d, i, j, k));
+    return (ue - uw) * s->idx + (vn - vs) * s->idy + (wt - wb) * m_idz(s, k);
+}
+
+/* W-weighted centred momentum / scalar advection (src/Anelastic.jl:1193-1306);
+ * on a stretched column the vertical metrics and the side-face volume flux of
+ * a w control volume (_zflux) replace the uniform ones -- on a uniform grid
+ * these are the reference expressions bit for bit. */
+static inline double wmom_u(const oc_sim* s, const double* u, const double* v, const double* w, int i, int j, int k) {
+    double iwc = 1 / s->wc[k], wfb = s->wf[k], wft = s->wf[k + 1];
+    double uce = 0.5 * (A(u, i, j, k) + A(u, i + 1, j, k));
+    double ucw = 0.5 * (A(u, i - 1, j, k) + A(u, i, j, k));
+    double d_uu_dx = (uce * uce - ucw * ucw) * s->idx;
+    double vun = 0.5 * (A(v, i - 1, j + 1, k) + A(v, i, j + 1, k));
+    double uvn = 0.5 * (A(u, i, j, k) + A(u, i, j + 1, k));
+    double vus = 0.5 * (A(v, i - 1, j, k) + A(v, i, j, k));
+    double uvs = 0.5 * (A(u, i, j - 1, k) + A(u, i, j, k));
+    double d_vu_dy = (vun * uvn - vus * uvs) * s->idy;
+    double wut = 0.5 * (A(w, i - 1, j, k + 1) + A(w, i, j, k + 1));
+    double uwt = 0.5 * (A(u, i, j, k) + A(u, i, j, k + 1));
+    double wub = 0.5 * (A(w, i - 1, j, k) + A(w, i, j, k));
+    double uwb = 0.5 * (A(u, i, j, k - 1) + A(u, i, j, k));
+    double d_wu_dz = (wft * wut * uwt - wfb * wub * uwb) * m_idz(s, k) * iwc;
+    return d_uu_dx + d_vu_dy + d_wu_dz;
+}
+
+static inline double wmom_v(const oc_sim* s, const double* u, const double* v, const double* w, int i, int j, int k) {
+    double iwc = 1 / s->wc[k], wfb = s->wf[k], wft = s->wf[k + 1];
+    double uve = 0.5 * (A(u, i + 1, j - 1, k) + A(u, i + 1, j, k));
+    double vue = 0.5 * (A(v, i, j, k) + A(v, i + 1, j, k));
+    double uvw = 0.5 * (A(u, i, j - 1, k) + A(u, i, j, k));
+    double vuw = 0.5 * (A(v, i - 1, j, k) + A(v, i, j, k));
+    double d_uv_dx = (uve * vue - uvw * vuw) * s->idx;
+    double vcn = 0.5 * (A(v, i, j, k) + A(v, i, j + 1, k));
+    double vcs = 0.5 * (A(v, i, j - 1, k) + A(v, i, j, k));
+    double d_vv_dy = (vcn * vcn - vcs * vcs) * s->idy;
+    double wvt = 0.5 * (A(w, i, j - 1, k + 1) + A(w, i, j, k + 1));
+    double vwt = 0.5 * (A(v, i, j, k) + A(v, i, j, k + 1));
+    double wvb = 0.5 * (A(w, i, j - 1, k) + A(w, i, j, k));
+    double vwb = 0.5 * (A(v, i, j, k - 1) + A(v, i, j, k));
+    double d_wv_dz = (wft * wvt * vwt - wfb * wvb * vwb) * m_idz(s, k) * iwc;
+    return d_uv_dx + d_vv_dy + d_wv_dz;
+}
+
+static inline double wmom_w(const oc_sim* s, const double* u, const double* v, const double* w, int i, int j, int k) {
+    double iwf = 1 / s->wf[k], wcb = s->wc[k - 1], wct = s->wc[k];
+    double uwe = m_zflux(s, k, A(u, i + 1, j, k - 1), A(u, i + 1, j, k));
+    double wue = 0.5 * (A(w, i, j, k) + A(w, i + 1, j, k));
+    double uww = m_zflux(s, k, A(u, i, j, k - 1), A(u, i, j, k));
+    double wuw = 0.5 * (A(w, i - 1, j, k) + A(w, i, j, k));
+    double d_uw_dx = (uwe * wue - uww * wuw) * s->idx;
+    double vwn = m_zflux(s, k, A(v, i, j + 1, k - 1), A(v, i, j + 1, k));
+    double wvn = 0.5 * (A(w, i, j, k) + A(w, i, j + 1, k));
+    double vws = m_zflux(s, k, A(v, i, j, k - 1), A(v, i, j, k));
+    double wvs = 0.5 * (A(w, i, j - 1, k) + A(w, i, j, k));
+    double d_vw_dy = (vwn * wvn - vws * wvs) * s->idy;
+    double wtop = 0.5 * (A(w, i, j, k) + A(w, i, j, k + 1));
+    double wbot = 0.5 * (A(w, i, j, k - 1) + A(w, i, j, k));
+    double d_ww_dz = (wct * wtop * wtop - wcb * wbot * wbot) * m_idzf(s, k) * iwf;
+    return d_uw_dx + d_vw_dy + d_ww_dz;
+}
+
+static inline double wscal(const oc_sim* s, const double* u, const double* v, const double* w, const double* f,
+                           int i, int j, int k) {
+    double iwc = 1 / s->wc[k], wfb = s->wf[k], wft = s->wf[k + 1];
+    double ue = A(u, i + 1, j, k) * 0.5 * (A(f, i, j, k) + A(f, i + 1, j, k));
+    double uw = A(u, i, j, k) * 0.5 * (A(f, i - 1, j, k) + A(f, i, j, k));
+    double vn = A(v, i, j + 1, k) * 0.5 * (A(f, i, j, k) + A(f, i, j + 1, k));
+    double vs = A(v, i, j, k) * 0.5 * (A(f, i, j - 1, k) + A(f, i, j, k));
+    double wt = wft * A(w, i, j, k + 1) * 0.5 * (A(f, i, j, k) + A(f, i, j, k + 1));
+    double wb = wfb * A(w, i, j, k) * 0.5 * (A(f, i, j, k - 1) + A(f, i, j, k));
+    return (ue - uw) * s->idx + (vn - vs) * s->idy + (wt - wb) * m_idz(s, k) * iwc;
+}
+
+/* --- WENO reconstructions (src/AdvectionSchemes.jl:105-120, :240-255,
+ *     :319-333) ------------------------------------------------------------ */
+
+static inline double beta3(double a1, double a2) { return a1 * a1 + (13.0 / 3.0) * (a2 * a2); }
+static inline double b3_m2(double v1, double v2, double v3) {
+    return beta3((v1 - 4 * v2 + 3 * v3) / 2, (v1 - 2 * v2 + v3) / 2);
+}
+static inline double b3_m1(double v1, double v2, double v3) {
+    return beta3((v3 - v1) / 2, (v1 - 2 * v2 + v3) / 2);
+}
+static inline double b3_p0(double v1, double v2, double v3) {
+    return beta3((-3 * v1 + 4 * v2 - v3) / 2, (v1 - 2 * v2 + v3) / 2);
+}
+
+static inline double weno_js5_left(double v1, double v2, double v3, double v4, double v5) {
+    double q0 = (2 * v1 - 7 * v2 + 11 * v3) / 6;
+    double q1 = (-v2 + 5 * v3 + 2 * v4) / 6;
+    double q2 = (2 * v3 + 5 * v4 - v5) / 6;
+    double b0 = b3_m2(v1, v2, v3), b1 = b3_m1(v2, v3, v4), b2 = b3_p0(v3, v4, v5);
+    double e = 1e-6;
+    double a0 = (1.0 / 10) / ((b0 + e) * (b0 + e));
+    double a1 = (6.0 / 10) / ((b1 + e) * (b1 + e));
+    double a2 = (3.0 / 10) / ((b2 + e) * (b2 + e));
+    return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
+}
+
+static inline double weno_z5_left(double v1, double v2, double v3, double v4, double v5) {
+    double q0 = (2 * v1 - 7 * v2 + 11 * v3) / 6;
+    double q1 = (-v2 + 5 * v3 + 2 * v4) / 6;
+    double q2 = (2 * v3 + 5 * v4 - v5) / 6;
+    double b0 = b3_m2(v1, v2, v3), b1 = b3_m1(v2, v3, v4), b2 = b3_p0(v3, v4, v5);
+    double eps = DBL_EPSILON * DBL_EPSILON;
+    double tau = fabs(b0 - b2);
+    double t0 = tau / (b0 + eps), t1 = tau / (b1 + eps), t2 = tau / (b2 + eps);
+    double a0 = (1.0 / 10) * (1.0 + t0 * t0);
+    double a1 = (6.0 / 10) * (1.0 + t1 * t1);
+    double a2 = (3.0 / 10) * (1.0 + t2 * t2);
+    return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
+}
+
+static inline double recon(int scheme, double v1, double v2, double v3, double v4, double v5) {
+    return scheme == OC_ADV_WENO_Z5 ? weno_z5_left(v1, v2, v3, v4, v5) : weno_js5_left(v1, v2, v3, v4, v5);
+}
+
+/* upwinded face values between cells c and c+1 along each axis
+ * (src/AdvectionSchemes.jl:623-666: mirror-symmetric selection) */
+static inline double face_x(const oc_sim* s, int sc, const double* d, int c, int j, int k, double vel) {
+    if (vel >= 0) return recon(sc, A(d, c - 2, j, k), A(d, c - 1, j, k), A(d, c, j, k), A(d, c + 1, j, k), A(d, c + 2, j, k));
+    return recon(sc, A(d, c + 3, j, k), A(d, c + 2, j, k), A(d, c + 1, j, k), A(d, c, j, k), A(d, c - 1, j, k));
+}
+static inline double face_y(const oc_sim* s, int sc, const double* d, int i, int c, int k, double vel) {
+    if (vel >= 0) return recon(sc, A(d, i, c - 2, k), A(d, i, c - 1, k), A(d, i, c, k), A(d, i, c + 1, k), A(d, i, c + 2, k));
+    return recon(sc, A(d, i, c + 3, k), A(d, i, c + 2, k), A(d, i, c + 1, k), A(d, i, c, k), A(d, i, c - 1, k));
+}
+static inline double face_z(const oc_sim* s, int sc, const double* d, int i, int j, int c, double vel) {
+    if (vel >= 0) return recon(sc, A(d, i, j, c - 2), A(d, i, j, c - 1), A(d, i, j, c), A(d, i, j, c + 1), A(d, i, j, c + 2));
+    return recon(sc, A(d, i, j, c + 3), A(d, i, j, c + 2), A(d, i, j, c + 1), A(d, i, j, c), A(d, i, j, c - 1));
+}
+
+/* flux-form reconstructed scalar advection (src/AdvectionSchemes.jl:685-699) */
+static inline double recon_scalar_at(const oc_sim* s, int sc, const double* u, const double* v, const double* w,
+                                     const double* f, int i, int j, int k) {
+    double uw = A(u, i, j, k), ue = A(u, i + 1, j, k);
+    double Fx = (ue * face_x(s, sc, f, i, j, k, ue) - uw * face_x(s, sc, f, i - 1, j, k, uw)) * s->idx;
+    double vs = A(v, i, j, k), vn = A(v, i, j + 1, k);
+    double Fy = (vn * face_y(s, sc, f, i, j, k, vn) - vs * face_y(s, sc, f, i, j - 1, k, vs)) * s->idy;
+    double wb = A(w, i, j, k), wt = A(w, i, j, k + 1);
+    double Fz = (wt * face_z(s, sc, f, i, j, k, wt) - wb * face_z(s, sc, f, i, j, k - 1, wb)) * s->idz;
+    return Fx + Fy + Fz;
+}
+
+/* reconstructed momentum advection (src/AdvectionSchemes.jl:1203-1256) */
+static inline double recon_mom_u(const oc_sim* s, int sc, const double* u, const double* v, const double* w, int i, int j, int k) {
+    double Ue = (A(u, i, j, k) + A(u, i + 1, j, k)) / 2;
+    double Uw = (A(u, i - 1, j, k) + A(u, i, j, k)) / 2;
+    double dx = (Ue * face_x(s, sc, u, i, j, k, Ue) - Uw * face_x(s, sc, u, i - 1, j, k, Uw)) * s->idx;
+    double Vn = (A(v, i - 1, j + 1, k) + A(v, i, j + 1, k)) / 2;
+    double Vs = (A(v, i - 1, j, k) + A(v, i, j, k)) / 2;
+    double dy = (Vn * face_y(s, sc, u, i, j, k, Vn) - Vs * face_y(s, sc, u, i, j - 1, k, Vs)) * s->idy;
+    double Wt = (A(w, i - 1, j, k + 1) + A(w, i, j, k + 1)) / 2;
+    double Wb = (A(w, i - 1, j, k) + A(w, i, j, k)) / 2;
+    double dz = (Wt * face_z(s, sc, u, i, j, k, Wt) - Wb * face_z(s, sc, u, i, j, k - 1, Wb)) * s->idz;
+    return dx + dy + dz;
+}
+static inline double recon_mom_v(const oc_sim* s, int sc, const double* u, const double* v, const double* w, int i, int j, int k) {
+    double Ue = (A(u, i + 1, j - 1, k) + A(u, i + 1, j, k)) / 2;
+    double Uw = (A(u, i, j - 1, k) + A(u, i, j, k)) / 2;
+    double dx = (Ue * face_x(s, sc, v, i, j, k, Ue) - Uw * face_x(s, sc, v, i - 1, j, k, Uw)) * s->idx;
+    double Vn = (A(v, i, j, k) + A(v, i, j + 1, k)) / 2;
+    double Vs = (A(v, i, j - 1, k) + A(v, i, j, k)) / 2;
+    double dy = (Vn * face_y(s, sc, v, i, j, k, Vn) - Vs * face_y(s, sc, v, i, j - 1, k, Vs)) * s->idy;
+    double Wt = (A(w, i, j - 1, k + 1) + A(w, i, j, k + 1)) / 2;
+    double Wb = (A(w, i, j - 1, k) + A(w, i, j, k)) / 2;
+    double dz = (Wt * face_z(s, sc, v, i, j, k, Wt) - Wb * face_z(s, sc, v, i, j, k - 1, Wb)) * s->idz;
+    return dx + dy + dz;
+}
+static inline double recon_mom_w(const oc_sim* s, int sc, const double* u, const double* v, const double* w, int i, int j, int k) {
+    double Ue = (A(u, i + 1, j, k - 1) + A(u, i + 1, j, k)) / 2;
+    double Uw = (A(u, i, j, k - 1) + A(u, i, j, k)) / 2;
+    double dx = (Ue * face_x(s, sc, w, i, j, k, Ue) - Uw * face_x(s, sc, w, i - 1, j, k, Uw)) * s->idx;
+    double Vn = (A(v, i, j + 1, k - 1) + A(v, i, j + 1, k)) / 2;
+    double Vs = (A(v, i, j, k - 1) + A(v, i, j, k)) / 2;
+    double dy = (Vn * face_y(s, sc, w, i, j, k, Vn) - Vs * face_y(s, sc, w, i, j - 1, k, Vs)) * s->idy;
+    double Wt = (A(w, i, j, k) + A(w, i, j, k + 1)) / 2;
+    double Wb = (A(w, i, j, k - 1) + A(w, i, j, k)) / 2;
+    double dz = (Wt * face_z(s, sc, w, i, j, k, Wt) - Wb * face_z(s, sc, w, i, j, k - 1, Wb)) * s->idz;
+    return dx + dy + dz;
+}
+
+/* --- Smagorinsky (src/FiniteVolume.jl:936-944, src/Operators.jl:451-496) -- */
+static inline double smag_at(const oc_sim* s, int i, int j, int k) {
+    const double *u = s->u, *v = s->v, *w = s->w;
+    double idx = s->idx, idy = s->idy, idz = m_idz(s, k), ido = m_idz_off(s, k);
+    double coef = (s->p.c_s * m_filter(s, k)) * (s->p.c_s * m_filter(s, k));
+    double du_dx = (A(u, i + 1, j, k) - A(u, i, j, k)) * idx;
+    double dv_dy = (A(v, i, j + 1, k) - A(v, i, j, k)) * idy;
+    double dw_dz = (A(w, i, j, k + 1) - A(w, i, j, k)) * idz;
+    double du_dy = ((A(u, i, j + 1, k) + A(u, i + 1, j + 1, k)) - (A(u, i, j - 1, k) + A(u, i + 1, j - 1, k))) * (0.25 * idy);
+    double dv_dx = ((A(v, i + 1, j, k) + A(v, i + 1, j + 1, k)) - (A(v, i - 1, j, k) + A(v, i - 1, j + 1, k))) * (0.25 * idx);
+    double du_dz = ((A(u, i, j, k + 1) + A(u, i + 1, j, k + 1)) - (A(u, i, j, k - 1) + A(u, i + 1, j, k - 1))) * (0.25 * ido);
+    double dw_dx = ((A(w, i + 1, j, k) + A(w, i + 1, j, k + 1)) - (A(w, i - 1, j, k) + A(w, i - 1, j, k + 1))) * (0.25 * idx);
+    double dv_dz = ((A(v, i, j, k + 1) + A(v, i, j + 1, k + 1)) - (A(v, i, j, k - 1) + A(v, i, j + 1, k - 1))) * (0.25 * ido);
+    double dw_dy = ((A(w, i, j + 1, k) + A(w, i, j + 1, k + 1)) - (A(w, i, j - 1, k) + A(w, i, j - 1, k + 1))) * (0.25 * idy);
+    double S11 = du_dx, S22 = dv_dy, S33 = dw_dz;
+    double S12 = 0.5 * (du_dy + dv_dx);
+    double S13 = 0.5 * (du_dz + dw_dx);
+    double S23 = 0.5 * (dv_dz + dw_dy);
+    double S2 = 2 * (S11 * S11 + S22 * S22 + S33 * S33) + 4 * (S12 * S12 + S13 * S13 + S23 * S23);
+    return coef * sqrt(S2);
+}
+
+/* eddy viscosity divergence (src/FiniteVolume.jl:969-1042, :1556-1562) */
+static inline double eddy_u(const oc_sim* s, int i, int j, int k) {
+    const double *u = s->u, *n = s->nut;
+    double idx = s->idx, idy = s->idy;
+    double fxE = A(n, i, j, k) * (A(u, i + 1, j, k) - A(u, i, j, k)) * idx;
+    double fxW = A(n, i - 1, j, k) * (A(u, i, j, k) - A(u, i - 1, j, k)) * idx;
+    double eN = 0.25 * (A(n, i - 1, j, k) + A(n, i, j, k) + A(n, i - 1, j + 1, k) + A(n, i, j + 1, k));
+    double eS = 0.25 * (A(n, i - 1, j - 1, k) + A(n, i, j - 1, k) + A(n, i - 1, j, k) + A(n, i, j, k));
+    double fyN = eN * (A(u, i, j + 1, k) - A(u, i, j, k)) * idy;
+    double fyS = eS * (A(u, i, j, k) - A(u, i, j - 1, k)) * idy;
+    double eT = 0.25 * (A(n, i - 1, j, k) + A(n, i, j, k) + A(n, i - 1, j, k + 1) + A(n, i, j, k + 1));
+    double eB = 0.25 * (A(n, i - 1, j, k - 1) + A(n, i, j, k - 1) + A(n, i - 1, j, k) + A(n, i, j, k));
+    double fzT = eT * (A(u, i, j, k + 1) - A(u, i, j, k)) * m_idzf(s, k + 1);
+    double fzB = eB * (A(u, i, j, k) - A(u, i, j, k - 1)) * m_idzf(s, k);
+    double vert = s->wc ? (s->wf[k + 1] * fzT - s->wf[k] * fzB) * m_idz(s, k) / s->wc[k] : (fzT - fzB) * m_idz(s, k);
+    return (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
+}
+
+static inline double eddy_v(const oc_sim* s, int i, int j, int k) {
+    const double *v = s->v, *n = s->nut;
+    double idx = s->idx, idy = s->idy;
+    double fyN = A(n, i, j, k) * (A(v, i, j + 1, k) - A(v, i, j, k)) * idy;
+    double fyS = A(n, i, j - 1, k) * (A(v, i, j, k) - A(v, i, j - 1, k)) * idy;
+    double eE = 0.25 * (A(n, i, j - 1, k) + A(n, i + 1, j - 1, k) + A(n, i, j, k) + A(n, i + 1, j, k));
+    double eW = 0.25 * (A(n, i - 1, j - 1, k) + A(n, i, j - 1, k) + A(n, i - 1, j, k) + A(n, i, j, k));
+    double fxE = eE * (A(v, i + 1, j, k) - A(v, i, j, k)) * idx;
+    double fxW = eW * (A(v, i, j, k) - A(v, i - 1, j, k)) * idx;
+    double eT = 0.25 * (A(n, i, j - 1, k) + A(n, i, j, k) + A(n, i, j - 1, k + 1) + A(n, i, j, k + 1));
+    double eB = 0.25 * (A(n, i, j - 1, k - 1) + A(n, i, j, k - 1) + A(n, i, j - 1, k) + A(n, i, j, k));
+    double fzT = eT * (A(v, i, j, k + 1) - A(v, i, j, k)) * m_idzf(s, k + 1);
+    double fzB = eB * (A(v, i, j, k) - A(v, i, j, k - 1)) * m_idzf(s, k);
+    double vert = s->wc ? (s->wf[k + 1] * fzT - s->wf[k] * fzB) * m_idz(s, k) / s->wc[k] : (fzT - fzB) * m_idz(s, k);
+    return (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
+}
+
+static inline double eddy_w(const oc_sim* s, int i, int j, int k) {
+    const double *w = s->w, *n = s->nut;
+    double idx = s->idx, idy = s->idy;
+    double fzT = A(n, i, j, k) * (A(w, i, j, k + 1) - A(w, i, j, k)) * m_idz(s, k);
+    double fzB = A(n, i, j, k - 1) * (A(w, i, j, k) - A(w, i, j, k - 1)) * m_idz(s, k - 1);
+    double eE = 0.25 * (A(n, i, j, k - 1) + A(n, i + 1, j, k - 1) + A(n, i, j, k) + A(n, i + 1, j, k));
+    double eW = 0.25 * (A(n, i - 1, j, k - 1) + A(n, i, j, k - 1) + A(n, i - 1, j, k) + A(n, i, j, k));
+    double fxE = eE * (A(w, i + 1, j, k) - A(w, i, j, k)) * idx;
+    double fxW = eW * (A(w, i, j, k) - A(w, i - 1, j, k)) * idx;
+    double eN = 0.25 * (A(n, i, j, k - 1) + A(n, i, j + 1, k - 1) + A(n, i, j, k) + A(n, i, j + 1, k));
+    double eS = 0.25 * (A(n, i, j - 1, k - 1) + A(n, i, j, k - 1) + A(n, i, j - 1, k) + A(n, i, j, k));
+    double fyN = eN * (A(w, i, j + 1, k) - A(w, i, j, k)) * idy;
+    double fyS = eS * (A(w, i, j, k) - A(w, i, j - 1, k)) * idy;
+    double vert = s->wc ? (s->wc[k] * fzT - s->wc[k - 1] * fzB) * m_idzf(s, k) / s->wf[k] : (fzT - fzB) * m_idzf(s, k);
+    return (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
+}
+
+/* scalar eddy diffusion: Boussinesq s*(div K grad) with K = nut, s = 1/Prt
+ * (src/FiniteVolume.jl:1280-1300); sound-proof W-weighted form with
+ * K = nut/Prt (src/FiniteVolume.jl:1473-1492). */
+static inline double eddy_scalar(const oc_sim* s, const double* d, int i, int j, int k) {
+    double idx = s->idx, idy = s->idy;
+    if (!s->wc) {
+        const double* H = s->nut;
+        double sc = 1 / s->p.pr_t;
+        double nE = 0.5 * (A(H, i, j, k) + A(H, i + 1, j, k));
+        double nW = 0.5 * (A(H, i - 1, j, k) + A(H, i, j, k));
+        double nN = 0.5 * (A(H, i, j, k) + A(H, i, j + 1, k));
+        double nS = 0.5 * (A(H, i, j - 1, k) + A(H, i, j, k));
+        double nT = 0.5 * (A(H, i, j, k) + A(H, i, j, k + 1));
+        double nB = 0.5 * (A(H, i, j, k - 1) + A(H, i, j, k));
+        double fxE = nE * (A(d, i + 1, j, k) - A(d, i, j, k)) * idx;
+        double fxW = nW * (A(d, i, j, k) - A(d, i - 1, j, k)) * idx;
+        double fyN = nN * (A(d, i, j + 1, k) - A(d, i, j, k)) * idy;
+        double fyS = nS * (A(d, i, j, k) - A(d, i, j - 1, k)) * idy;
+        double fzT = nT * (A(d, i, j, k + 1) - A(d, i, j, k)) * m_idzf(s, k + 1);
+        double fzB = nB * (A(d, i, j, k) - A(d, i, j, k - 1)) * m_idzf(s, k);
+        return sc * ((fxE - fxW) * idx + (fyN - fyS) * idy + (fzT - fzB) * m_idz(s, k));
+    }
+    const double* K = s->kt;
+    double fxE = 0.5 * (A(K, i, j, k) + A(K, i + 1, j, k)) * (A(d, i + 1, j, k) - A(d, i, j, k)) * idx;
+    double fxW = 0.5 * (A(K, i - 1, j, k) + A(K, i, j, k)) * (A(d, i, j, k) - A(d, i - 1, j, k)) * idx;
+    double fyN = 0.5 * (A(K, i, j, k) + A(K, i, j + 1, k)) * (A(d, i, j + 1, k) - A(d, i, j, k)) * idy;
+    double fyS = 0.5 * (A(K, i, j - 1, k) + A(K, i, j, k)) * (A(d, i, j, k) - A(d, i, j - 1, k)) * idy;
+    double fzT = 0.5 * (A(K, i, j, k) + A(K, i, j, k + 1)) * (A(d, i, j, k + 1) - A(d, i, j, k)) * m_idzf(s, k + 1);
+    double fzB = 0.5 * (A(K, i, j, k - 1) + A(K, i, j, k)) * (A(d, i, j, k) - A(d, i, j, k - 1)) * m_idzf(s, k);
+    double vert = (s->wf[k + 1] * fzT - s->wf[k] * fzB) * m_idz(s, k) / s->wc[k];
+    return (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
+}
+
+/* Rayleigh sponge rate (src/FiniteVolume.jl:578-592, :664-702) */
+static inline double sponge_rate(const oc_sim* s, double z) {
+    double zs = s->p.sponge_zstart, ztop = s->p.z0 + s->p.lz;
+    if (!(z >= zs)) return 0.0;
+    double inv = 1 / (ztop - zs);
+    double sn = sin(0.5 * M_PI * (z - zs) * inv);
+    return s->p.sponge_alpha * sn * sn;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Tendencies of one substage (src/Simulations.jl:548-620,                    */
+/* src/Anelastic.jl:1809-1849)                                                */
+/* ------------------------------------------------------------------------- */
+
+static void compute_tendencies(oc_sim* s) {
+    const oc_params* P = &s->p;
+    int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
+    int anel = (P->core == OC_CORE_ANELASTIC);
+    int sc = P->advection;
+    int has_visc = P->nu != 0, has_sgs = P->c_s != 0;
+    int has_buoy = anel ? (P->g != 0) : (P->theta0 != 0);
+    const double *u = s->u, *v = s->v, *w = s->w, *th = s->th;
+
+    /* 4a. Smagorinsky coefficients, then their halos (velocity BCs) */
+    if (has_sgs) {
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int k = Hz; k < Hz + Nz; ++k)
+            for (int j = Hy; j < Hy + Ny; ++j)
+                for (int i = Hx; i < Hx + Nx; ++i) A(s->nut, i, j, k) = smag_at(s, i, j, k);
+        fill_halos(s, s->nut, LOC_C);
+        if (anel)
+            for (int64_t q = 0; q < s->n; ++q) s->kt[q] = s->nut[q] / P->pr_t;
+    }
+
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = Hz; k < Hz + Nz; ++k)
+        for (int j = Hy; j < Hy + Ny; ++j)
+            for (int i = Hx; i < Hx + Nx; ++i) {
+                double tu, tv, tw, tt;
+                /* 2. advection (the tendencies start from zero) */
+                if (anel) {
+                    tu = 0.0 - wmom_u(s, u, v, w, i, j, k);
+                    tv = 0.0 - wmom_v(s, u, v, w, i, j, k);
+                    tw = 0.0 - wmom_w(s, u, v, w, i, j, k);
+                    tt = 0.0 - wscal(s, u, v, w, th, i, j, k);
+                } else if (sc == OC_ADV_CENTRED) {
+                    tu = 0.0 - mom_u_at(s, u, v, w, i, j, k);
+                    tv = 0.0 - mom_v_at(s, u, v, w, i, j, k);
+                    tw = 0.0 - mom_w_at(s, u, v, w, i, j, k);
+                    tt = 0.0 - adv_centred_at(s, u, v, w, th, i, j, k);
+                } else {
+                    tu = 0.0 - recon_mom_u(s, sc, u, v, w, i, j, k);
+                    tv = 0.0 - recon_mom_v(s, sc, u, v, w, i, j, k);
+                    tw = 0.0 - recon_mom_w(s, sc, u, v, w, i, j, k);
+                    tt = 0.0 - recon_scalar_at(s, sc, u, v, w, th, i, j, k);
+                }
+                /* 3. molecular viscosity / diffusion */
+                if (has_visc) {
+                    tu = tu + P->nu * lap_at(s, u, i, j, k, LOC_FX);
+                    tv = tv + P->nu * lap_at(s, v, i, j, k, LOC_FY);
+                    tw = tw + P->nu * lap_at(s, w, i, j, k, LOC_FZ);
+                    tt = tt + P->nu * lap_at(s, th, i, j, k, LOC_C);
+                }
+                /* 4b. SGS tendencies */
+                if (has_sgs) {
+                    tu += eddy_u(s, i, j, k);
+                    tv += eddy_v(s, i, j, k);
+                    tw += eddy_w(s, i, j, k);
+                    tt += eddy_scalar(s, th, i, j, k);
+                }
+                /* 5. buoyancy on the z faces */
+                if (has_buoy) {
+                    if (anel) {
+                        double tb = s->thf[k];
+                        double coef = P->g / tb;
+                        double thface = m_zface(s, k, A(th, i, j, k - 1), A(th, i, j, k));
+                        tw += coef * (thface - tb);
+                    } else {
+                        double thface = m_zface(s, k, A(th, i, j, k - 1), A(th, i, j, k));
+                        tw += (P->g / P->theta0) * (thface - P->theta0);
+                    }
+                }
+                /* 6. Coriolis */
+                if (P->f_coriolis != 0) {
+                    double v_at_u = 0.25 * (A(v, i - 1, j, k) + A(v, i, j, k) + A(v, i - 1, j + 1, k) + A(v, i, j + 1, k));
+                    tu += P->f_coriolis * v_at_u;
+                    double u_at_v = 0.25 * (A(u, i, j - 1, k) + A(u, i + 1, j - 1, k) + A(u, i, j, k) + A(u, i + 1, j, k));
+                    tv -= P->f_coriolis * u_at_v;
+                }
+                /* 6a. prescribed wall fluxes of theta */
+                if (k == Hz) tt += P->flux_bot * m_idz(s, Hz);
+                if (k == Hz + Nz - 1) tt -= P->flux_top * m_idz(s, Hz + Nz - 1);
+                /* 6b. Rayleigh sponge toward rest */
+                if (P->sponge_alpha != 0) {
+                    double zcen = s->zc[k], zface = s->zf[k];
+                    double rc = sponge_rate(s, zcen), rf = sponge_rate(s, zface);
+                    if (zcen >= P->sponge_zstart) { tu -= rc * (A(u, i, j, k) - 0.0); tv -= rc * (A(v, i, j, k) - 0.0); }
+                    if (zface >= P->sponge_zstart) tw -= rf * (A(w, i, j, k) - 0.0);
+                }
+                A(s->tu, i, j, k) = tu;
+                A(s->tv, i, j, k) = tv;
+                A(s->tw, i, j, k) = tw;
+                A(s->tt, i, j, k) = tt;
+            }
+}
+
+int oc_tendencies(oc_sim* s, double* tu, double* tv, double* tw, double* tt) {
+    oc_fill_state_halos(s);
+    compute_tendencies(s);
+    size_t b = sizeof(double) * (size_t)s->n;
+    if (tu) memcpy(tu, s->tu, b);
+    if (tv) memcpy(tv, s->tv, b);
+    if (tw) memcpy(tw, s->tw, b);
+    if (tt) memcpy(tt, s->tt, b);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Divergence (src/FiniteVolume.jl:312-316, :1869-1888;                       */
+/* src/Anelastic.jl:1110-1120)                                                */
+/* ------------------------------------------------------------------------- */
+
+static inline double div_at(const oc_sim* s, const double* u, const double* v, const double* w, int i, int j, int k) {
+    return (A(u, i + 1, j, k) - A(u, i, j, k)) * s->idx + (A(v, i, j + 1, k) - A(v, i, j, k)) * s->idy +
+           (A(w, i, j, k + 1) - A(w, i, j, k)) * m_idz(s, k);
+}
+static inline double wdiv_at(const oc_sim* s, const double* u, const double* v, const double* w, int i, int j, int k) {
+    double wc = s->wc[k], wfb = s->wf[k], wft = s->wf[k + 1];
+    return wc * ((A(u, i + 1, j, k) - A(u, i, j, k)) * s->idx + (A(v, i, j + 1, k) - A(v, i, j, k)) * s->idy) +
+           (wft * A(w, i, j, k + 1) - wfb * A(w, i, j, k)) * m_idz(s, k);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Pressure solvers                                                           */
+/* ------------------------------------------------------------------------- */
+
+/* Forward x-y transform of s->src into s->hat (rfft in x, DFT in y). */
+static void xy_forward(oc_sim* s) {
+    int Nx = s->p.nx, Ny = s->p.ny, Nz = s->p.nz, Mh = Nx / 2 + 1;
+#pragma omp parallel
+    {
+        int nmax = (Nx > Ny ? Nx : Ny) + 2;
+        cpx* z = (cpx*)malloc(sizeof(cpx) * (size_t)nmax);
+        cpx* tmp = (cpx*)malloc(sizeof(cpx) * (size_t)nmax);
+        cpx* col = (cpx*)malloc(sizeof(cpx) * (size_t)nmax);
+#pragma omp for collapse(2) schedule(static)
+        for (int k = 0; k < Nz; ++k)
+            for (int j = 0; j < Ny; ++j)
+                rfft_row(s, s->src + (int64_t)Nx * (j + (int64_t)Ny * k), s->hat + (int64_t)Mh * (j + (int64_t)Ny * k), z, tmp);
+#pragma omp for collapse(2) schedule(static)
+        for (int k = 0; k < Nz; ++k)
+            for (int p = 0; p < Mh; ++p) {
+                for (int j = 0; j < Ny; ++j) col[j] = s->hat[p + (int64_t)Mh * (j + (int64_t)Ny * k)];
+                fft_c(&s->py, col, 0, tmp);
+                for (int j = 0; j < Ny; ++j) s->hat[p + (int64_t)Mh * (j + (int64_t)Ny * k)] = col[j];
+            }
+        free(z); free(tmp); free(col);
+    }
+}
+
+static void xy_inverse(oc_sim* s) {
+    int Nx = s->p.nx, Ny = s->p.ny, Nz = s->p.nz, Mh = Nx / 2 + 1;
+#pragma omp parallel
+    {
+        int nmax = (Nx > Ny ? Nx : Ny) + 2;
+        cpx* z = (cpx*)malloc(sizeof(cpx) * (size_t)nmax);
+        cpx* tmp = (cpx*)malloc(sizeof(cpx) * (size_t)nmax);
+        cpx* col = (cpx*)malloc(sizeof(cpx) * (size_t)nmax);
+#pragma omp for collapse(2) schedule(static)
+        for (int k = 0; k < Nz; ++k)
+            for (int p = 0; p < Mh; ++p) {
+                for (int j = 0; j < Ny; ++j) col[j] = s->hat[p + (int64_t)Mh * (j + (int64_t)Ny * k)];
+                fft_c(&s->py, col, 1, tmp);
+                for (int j = 0; j < Ny; ++j) s->hat[p + (int64_t)Mh * (j + (int64_t)Ny * k)] = col[j];
+            }
+#pragma omp for collapse(2) schedule(static)
+        for (int k = 0; k < Nz; ++k)
+            for (int j = 0; j < Ny; ++j)
+                irfft_row(s, s->hat + (int64_t)Mh * (j + (int64_t)Ny * k), s->src + (int64_t)Nx * (j + (int64_t)Ny * k), z, tmp);
+        free(z); free(tmp); free(col);
+    }
+}
+
+/* FFTPoissonSolver (src/PressureSolvers.jl:103-174): forward x-y then z,
+ * scale by nrm/lambda (zero for the mean mode), inverse z then x-y. */
+static void solve_fft(oc_sim* s) {
+    int Nx = s->p.nx, Ny = s->p.ny, Nz = s->p.nz, Mh = Nx / 2 + 1;
+    double nrm = 1 / (double)((int64_t)Nx * Ny * Nz);
+    xy_forward(s);
+#pragma omp parallel
+    {
+        cpx* tmp = (cpx*)malloc(sizeof(cpx) * (size_t)(Nz + 1));
+        cpx* col = (cpx*)malloc(sizeof(cpx) * (size_t)(Nz + 1));
+#pragma omp for collapse(2) schedule(static)
+        for (int j = 0; j < Ny; ++j)
+            for (int p = 0; p < Mh; ++p) {
+                for (int k = 0; k < Nz; ++k) col[k] = s->hat[p + (int64_t)Mh * (j + (int64_t)Ny * k)];
+                fft_c(&s->pz, col, 0, tmp);
+                for (int k = 0; k < Nz; ++k) {
+                    double lam = -(s->kx2[p] + s->ky2[j] + s->kz2[k]);
+                    double il = lam == 0 ? 0.0 : nrm / lam;
+                    col[k].re = col[k].re * il;
+                    col[k].im = col[k].im * il;
+                }
+                fft_c(&s->pz, col, 1, tmp);
+                for (int k = 0; k < Nz; ++k) s->hat[p + (int64_t)Mh * (j + (int64_t)Ny * k)] = col[k];
+            }
+        free(tmp); free(col);
+    }
+    xy_inverse(s);
+}
+
+/* ColumnTridiagonalSolver (src/PressureSolvers.jl:591-805): x-y transform,
+ * Thomas per horizontal wavenumber with the factorisation of :650-661,
+ * the mean mode integrated (_mean_mode!, :780-805), inverse, x norm. */
+static void solve_column(oc_sim* s) {
+    int Nx = s->p.nx, Ny = s->p.ny, Nz = s->p.nz, Mh = Nx / 2 + 1;
+    double norm = 1.0 / (double)(1 * Nx * 1 * Ny);
+    xy_forward(s);
+    const double *lo = s->lower, *up = s->upper, *hw = s->hw;
+#pragma omp parallel
+    {
+        double* cp = (double*)malloc(sizeof(double) * (size_t)Nz);
+        double* id = (double*)malloc(sizeof(double) * (size_t)Nz);
+#pragma omp for collapse(2) schedule(static)
+        for (int q = 0; q < Ny; ++q)
+            for (int p = 0; p < Mh; ++p) {
+                if (p == 0 && q == 0) continue;
+                double lam = s->kx2[p] + s->ky2[q];
+                double cprev = 0.0;
+                for (int k = 0; k < Nz; ++k) {
+                    double b = -(lo[k] + up[k]) - lam * hw[k];
+                    double den = b - lo[k] * cprev;
+                    id[k] = 1 / den;
+                    cprev = up[k] / den;
+                    cp[k] = cprev;
+                }
+                cpx* c0 = s->hat + p + (int64_t)Mh * q;
+                int64_t st = (int64_t)Mh * Ny;
+                c0[0].re *= id[0];
+                c0[0].im *= id[0];
+                for (int k = 1; k < Nz; ++k) {
+                    double a = lo[k];
+                    c0[k * st].re = (c0[k * st].re - a * c0[(k - 1) * st].re) * id[k];
+                    c0[k * st].im = (c0[k * st].im - a * c0[(k - 1) * st].im) * id[k];
+                }
+                for (int k = Nz - 2; k >= 0; --k) {
+                    c0[k * st].re -= cp[k] * c0[(k + 1) * st].re;
+                    c0[k * st].im -= cp[k] * c0[(k + 1) * st].im;
+                }
+            }
+        free(cp); free(id);
+    }
+    /* the mean mode (real) */
+    {
+        int64_t st = (int64_t)Mh * Ny;
+        double* col = (double*)malloc(sizeof(double) * (size_t)Nz);
+        for (int k = 0; k < Nz; ++k) col[k] = s->hat[k * st].re;
+        double mb = 0.0;
+        for (int k = 0; k < Nz; ++k) mb += col[k] * s->meas[k];
+        mb /= s->meas_sum;
+        double F = 0.0, ph = 0.0, prev = col[0] - mb;
+        col[0] = 0.0;
+        for (int k = 1; k < Nz; ++k) {
+            F += prev * s->meas[k - 1];
+            ph += F * s->iota[k];
+            prev = col[k] - mb;
+            col[k] = ph;
+        }
+        double mp = 0.0;
+        for (int k = 0; k < Nz; ++k) mp += col[k] * s->gauge[k];
+        double sh = mp / s->gauge_sum;
+        for (int k = 0; k < Nz; ++k) { s->hat[k * st].re = col[k] - sh; s->hat[k * st].im = 0.0; }
+        free(col);
+    }
+    xy_inverse(s);
+    int64_t nin = (int64_t)Nx * Ny * Nz;
+    for (int64_t q = 0; q < nin; ++q) s->src[q] *= norm;
+}
+
+static void solve_src(oc_sim* s) {
+    if (s->p.solver == OC_SOLVER_FFT) solve_fft(s);
+    else solve_column(s);
+}
+
+int oc_pressure_solve(oc_sim* s, const double* src, double* phi) {
+    int64_t nin = (int64_t)s->p.nx * s->p.ny * s->p.nz;
+    memcpy(s->src, src, sizeof(double) * (size_t)nin);
+    solve_src(s);
+    memcpy(phi, s->src, sizeof(double) * (size_t)nin);
+    return 0;
+}
+
+/* The operator each solver inverts, on interior-sized arrays (periodic x, y;
+ * z periodic 7-point or the column coefficients with zero end fluxes). */
+int oc_apply_poisson_operator(oc_sim* s, const double* phi, double* out) {
+    int Nx = s->p.nx, Ny = s->p.ny, Nz = s->p.nz;
+#define PI3(i, j, k) phi[(int64_t)(i) + (int64_t)Nx * ((int64_t)(j) + (int64_t)Ny * (int64_t)(k))]
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                int ip = (i + 1) % Nx, im = (i + Nx - 1) % Nx, jp = (j + 1) % Ny, jm = (j + Ny - 1) % Ny;
+                double c = PI3(i, j, k);
+                double h = (PI3(ip, j, k) - 2 * c + PI3(im, j, k)) * s->idx2 + (PI3(i, jp, k) - 2 * c + PI3(i, jm, k)) * s->idy2;
+                double r;
+                if (s->p.solver == OC_SOLVER_FFT) {
+                    int kp = (k + 1) % Nz, km = (k + Nz - 1) % Nz;
+                    r = h + (PI3(i, j, kp) - 2 * c + PI3(i, j, km)) * s->idz2;
+                } else {
+                    r = s->hw[k] * h;
+                    if (k > 0) r += s->lower[k] * (PI3(i, j, k - 1) - c);
+                    if (k < Nz - 1) r += s->upper[k] * (PI3(i, j, k + 1) - c);
+                }
+                out[(int64_t)i + (int64_t)Nx * (j + (int64_t)Ny * k)] = r;
+            }
+#undef PI3
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* One projected substage (src/Simulations.jl:531-650, :711-744)              */
+/* ------------------------------------------------------------------------- */
+
+/* stage: 0 plain Euler; otherwise c(x, snap) = ca*snap + cb*x */
+static void substage(oc_sim* s, double dt, int stage, double ca, double cb) {
+    const oc_params* P = &s->p;
+    int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
+    int anel = P->core == OC_CORE_ANELASTIC;
+    oc_fill_state_halos(s);
+    compute_tendencies(s);
+    /* 7. predictor */
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = Hz; k < Hz + Nz; ++k)
+        for (int j = Hy; j < Hy + Ny; ++j)
+            for (int i = Hx; i < Hx + Nx; ++i) {
+                int64_t q = ID(s, i, j, k);
+                s->u[q] = s->u[q] + dt * s->tu[q];
+                s->v[q] = s->v[q] + dt * s->tv[q];
+                s->w[q] = s->w[q] + dt * s->tw[q];
+            }
+    /* 8. divergence into the solver's buffer */
+    fill_halos(s, s->u, LOC_FX);
+    fill_halos(s, s->v, LOC_FY);
+    fill_halos(s, s->w, LOC_FZ);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i)
+                s->src[(int64_t)i + (int64_t)Nx * (j + (int64_t)Ny * k)] =
+                    anel ? wdiv_at(s, s->u, s->v, s->w, i + Hx, j + Hy, k + Hz)
+                         : div_at(s, s->u, s->v, s->w, i + Hx, j + Hy, k + Hz);
+    /* 9. Poisson solve */
+    solve_src(s);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i)
+                A(s->phi, i + Hx, j + Hy, k + Hz) = s->src[(int64_t)i + (int64_t)Nx * (j + (int64_t)Ny * k)];
+    fill_halos(s, s->phi, LOC_C);
+    /* 10. correction, p = phi/dt, RK combination; 11. theta */
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = Hz; k < Hz + Nz; ++k)
+        for (int j = Hy; j < Hy + Ny; ++j)
+            for (int i = Hx; i < Hx + Nx; ++i) {
+                int64_t q = ID(s, i, j, k);
+                double pc = s->phi[q];
+                double un = s->u[q] - (pc - A(s->phi, i - 1, j, k)) * s->idx;
+                double vn = s->v[q] - (pc - A(s->phi, i, j - 1, k)) * s->idy;
+                double wn = s->w[q] - (pc - A(s->phi, i, j, k - 1)) * m_idzf(s, k);
+                double tn = s->th[q] + dt * s->tt[q];
+                if (stage) {
+                    un = ca * s->u0[q] + cb * un;
+                    vn = ca * s->v0[q] + cb * vn;
+                    wn = ca * s->w0[q] + cb * wn;
+                    tn = ca * s->th0[q] + cb * tn;
+                }
+                s->u[q] = un; s->v[q] = vn; s->w[q] = wn; s->th[q] = tn;
+                s->pr[q] = pc / dt;
+            }
+}
+
+/* The Chorin projection of the current velocity with dt = 1 (the config
+ * driver's `_project!(sim, 1.0)` of a noisy initial field,
+ * src/config/simulation_driver.jl:1316; steps 8-10 of src/Simulations.jl:711-744). */
+int oc_project(oc_sim* s) {
+    const oc_params* P = &s->p;
+    int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
+    int anel = P->core == OC_CORE_ANELASTIC;
+    fill_halos(s, s->u, LOC_FX);
+    fill_halos(s, s->v, LOC_FY);
+    fill_halos(s, s->w, LOC_FZ);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i)
+                s->src[(int64_t)i + (int64_t)Nx * (j + (int64_t)Ny * k)] =
+                    anel ? wdiv_at(s, s->u, s->v, s->w, i + Hx, j + Hy, k + Hz)
+                         : div_at(s, s->u, s->v, s->w, i + Hx, j + Hy, k + Hz);
+    solve_src(s);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i)
+                A(s->phi, i + Hx, j + Hy, k + Hz) = s->src[(int64_t)i + (int64_t)Nx * (j + (int64_t)Ny * k)];
+    fill_halos(s, s->phi, LOC_C);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = Hz; k < Hz + Nz; ++k)
+        for (int j = Hy; j < Hy + Ny; ++j)
+            for (int i = Hx; i < Hx + Nx; ++i) {
+                int64_t q = ID(s, i, j, k);
+                double pc = s->phi[q];
+                s->u[q] = s->u[q] - (pc - A(s->phi, i - 1, j, k)) * s->idx;
+                s->v[q] = s->v[q] - (pc - A(s->phi, i, j - 1, k)) * s->idy;
+                s->w[q] = s->w[q] - (pc - A(s->phi, i, j, k - 1)) * m_idzf(s, k);
+                s->pr[q] = pc;
+            }
+    return 0;
+}
+
+int oc_step_euler(oc_sim* s, double dt, int nsteps) {
+    for (int n = 0; n < nsteps; ++n) substage(s, dt, 0, 0.0, 0.0);
+    return 0;
+}
+
+/* SSP-RK3 of three projected substages (src/Simulations.jl:854-912) */
+int oc_step_rk3(oc_sim* s, double dt, int nsteps) {
+    size_t b = sizeof(double) * (size_t)s->n;
+    double inv3 = 1.0 / 3, two3 = 2 * inv3;
+    for (int n = 0; n < nsteps; ++n) {
+        memcpy(s->u0, s->u, b); memcpy(s->v0, s->v, b); memcpy(s->w0, s->w, b); memcpy(s->th0, s->th, b);
+        substage(s, dt, 0, 0.0, 0.0);
+        substage(s, dt, 1, 0.75, 0.25);
+        substage(s, dt, 1, inv3, two3);
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Diagnostics (src/Simulations.jl:992-1050)                                  */
+/* ------------------------------------------------------------------------- */
+
+double oc_kinetic_energy(oc_sim* s) {
+    const oc_params* P = &s->p;
+    int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
+    double* part = (double*)calloc((size_t)Nz, sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int k = Hz; k < Hz + Nz; ++k) {
+        double acc = 0.0;
+        for (int j = Hy; j < Hy + Ny; ++j)
+            for (int i = Hx; i < Hx + Nx; ++i) {
+                double uu = A(s->u, i, j, k), vv = A(s->v, i, j, k), ww = A(s->w, i, j, k);
+                if (s->uniform) acc += uu * uu + vv * vv + ww * ww;
+                else acc += (uu * uu + vv * vv) * s->dzc[k] + ww * ww * s->dzf[k];
+            }
+        part[k - Hz] = acc;
+    }
+    double tot = 0.0;
+    for (int k = 0; k < Nz; ++k) tot += part[k];
+    free(part);
+    if (s->uniform) return 0.5 * tot * (s->dx * s->dy * s->dz);
+    return 0.5 * tot * s->dx * s->dy;
+}
+
+double oc_max_divergence(oc_sim* s) {
+    const oc_params* P = &s->p;
+    int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
+    fill_halos(s, s->u, LOC_FX);
+    fill_halos(s, s->v, LOC_FY);
+    fill_halos(s, s->w, LOC_FZ);
+    double m = 0.0;
+#pragma omp parallel for collapse(2) reduction(max : m) schedule(static)
+    for (int k = Hz; k < Hz + Nz; ++k)
+        for (int j = Hy; j < Hy + Ny; ++j)
+            for (int i = Hx; i < Hx + Nx; ++i) {
+                double d = s->wc ? wdiv_at(s, s->u, s->v, s->w, i, j, k) / s->wc[k] : div_at(s, s->u, s->v, s->w, i, j, k);
+                d = fabs(d);
+                if (d > m) m = d;
+            }
+    return m;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Construction                                                               */
+/* ------------------------------------------------------------------------- */
+
+static double* dalloc(int64_t n) { return (double*)calloc((size_t)(n > 0 ? n : 1), sizeof(double)); }
+
+oc_sim* oc_create(const oc_params* p, const double* zfi, const double* wc, const double* wf, const double* thf) {
+    if (p->bc_x != OC_BC_PERIODIC || p->bc_y != OC_BC_PERIODIC) return NULL;
+    if (p->nx % 2 != 0) return NULL;
+    int H = p->hx;
+    if (p->advection != OC_ADV_CENTRED && (H < 3 || p->hy < 3 || p->hz < 3)) return NULL;
+    if (p->advection != OC_ADV_CENTRED && (p->stretched || p->core == OC_CORE_ANELASTIC)) return NULL;
+    if (p->core == OC_CORE_ANELASTIC && (!wc || !wf || p->bc_z != OC_BC_WALL)) return NULL;
+    if (p->solver == OC_SOLVER_FFT && p->bc_z != OC_BC_PERIODIC) return NULL;
+    if (p->solver == OC_SOLVER_COLUMN && p->bc_z != OC_BC_WALL) return NULL;
+    if (p->stretched && (!zfi || p->bc_z != OC_BC_WALL)) return NULL;
+    oc_sim* s = (oc_sim*)calloc(1, sizeof(oc_sim));
+    s->p = *p;
+    s->NX = p->nx + 2 * p->hx; s->NY = p->ny + 2 * p->hy; s->NZ = p->nz + 2 * p->hz;
+    s->n = (int64_t)s->NX * s->NY * s->NZ;
+    int NZ = s->NZ, Nz = p->nz, Hz = p->hz;
+    s->uniform = !p->stretched;
+    s->dx = p->lx / p->nx; s->dy = p->ly / p->ny; s->dz = p->lz / p->nz;
+    s->idx = 1 / s->dx; s->idy = 1 / s->dy; s->idx2 = 1 / (s->dx * s->dx); s->idy2 = 1 / (s->dy * s->dy);
+    s->idz = 1 / s->dz; s->idz2 = 1 / (s->dz * s->dz);
+    s->delta_u = pow(s->dx * s->dy * s->dz, 1.0 / 3);
+    /* vertical storage metrics (src/StretchedGrids.jl:345-400, :570-590) */
+    s->zf = dalloc(NZ + 1); s->zc = dalloc(NZ); s->dzc = dalloc(NZ); s->dzf = dalloc(NZ + 1);
+    s->idzc = dalloc(NZ); s->idzf = dalloc(NZ + 1); s->idz_off = dalloc(NZ);
+    s->wlo = dalloc(NZ); s->whi = dalloc(NZ); s->alo = dalloc(NZ); s->ahi = dalloc(NZ); s->delta = dalloc(NZ);
+    if (s->uniform) {
+        for (int k = 0; k < NZ + 1; ++k) s->zf[k] = p->z0 + (double)(k - Hz) * s->dz;
+        for (int k = 0; k < NZ; ++k) s->zc[k] = p->z0 + ((double)(k - Hz) + 0.5) * s->dz;
+        for (int k = 0; k < NZ; ++k) s->dzc[k] = s->dz;
+        for (int k = 0; k < NZ + 1; ++k) s->dzf[k] = s->dz;
+    } else {
+        for (int k = 0; k <= Nz; ++k) s->zf[Hz + k] = zfi[k];
+        for (int k = Hz - 1; k >= 0; --k) s->zf[k] = 2 * s->zf[k + 1] - s->zf[k + 2];
+        for (int k = Hz + Nz + 1; k <= NZ; ++k) s->zf[k] = 2 * s->zf[k - 1] - s->zf[k - 2];
+        for (int k = 0; k < NZ; ++k) s->dzc[k] = s->zf[k + 1] - s->zf[k];
+        for (int k = 0; k < NZ; ++k) s->zc[k] = (s->zf[k] + s->zf[k + 1]) / 2;
+        s->dzf[0] = s->dzc[0];
+        for (int k = 1; k < NZ; ++k) s->dzf[k] = s->zc[k] - s->zc[k - 1];
+        s->dzf[NZ] = s->dzc[NZ - 1];
+    }
+    for (int k = 0; k < NZ; ++k) s->idzc[k] = 1 / s->dzc[k];
+    for (int k = 0; k < NZ + 1; ++k) s->idzf[k] = 1 / s->dzf[k];
+    for (int k = 0; k < NZ; ++k) s->idz_off[k] = 2 / (s->dzf[k] + s->dzf[k + 1]);
+    for (int k = 1; k < NZ; ++k) {
+        s->wlo[k] = s->dzc[k] / (s->dzc[k - 1] + s->dzc[k]);
+        s->whi[k] = s->dzc[k - 1] / (s->dzc[k - 1] + s->dzc[k]);
+        double sm = s->dzc[k - 1] + s->dzc[k];
+        s->alo[k] = s->dzc[k - 1] / sm;
+        s->ahi[k] = s->dzc[k] / sm;
+    }
+    for (int k = 0; k < NZ; ++k) s->delta[k] = pow(s->dx * s->dy * s->dzc[k], 1.0 / 3);
+    if (p->core == OC_CORE_ANELASTIC) {
+        s->wc = dalloc(NZ); s->wf = dalloc(NZ + 1); s->thf = dalloc(NZ + 1);
+        memcpy(s->wc, wc, sizeof(double) * (size_t)NZ);
+        memcpy(s->wf, wf, sizeof(double) * (size_t)(NZ + 1));
+        if (thf) memcpy(s->thf, thf, sizeof(double) * (size_t)(NZ + 1));
+    }
+    int64_t n = s->n;
+    s->u = dalloc(n); s->v = dalloc(n); s->w = dalloc(n); s->th = dalloc(n); s->pr = dalloc(n);
+    s->nut = dalloc(n); s->kt = dalloc(n); s->phi = dalloc(n);
+    s->tu = dalloc(n); s->tv = dalloc(n); s->tw = dalloc(n); s->tt = dalloc(n);
+    s->u0 = dalloc(n); s->v0 = dalloc(n); s->w0 = dalloc(n); s->th0 = dalloc(n);
+    int Nx = p->nx, Ny = p->ny, Mh = Nx / 2 + 1;
+    s->src = dalloc((int64_t)Nx * Ny * Nz);
+    s->hat = (cpx*)calloc((size_t)Mh * Ny * Nz, sizeof(cpx));
+    plan_init(&s->px, Nx / 2);
+    plan_init(&s->py, Ny);
+    plan_init(&s->pz, Nz);
+    s->twx = (cpx*)malloc(sizeof(cpx) * (size_t)Mh);
+    for (int k = 0; k < Mh; ++k) {
+        double a = -2.0 * M_PI * (double)k / (double)Nx;
+        s->twx[k].re = cos(a); s->twx[k].im = sin(a);
+    }
+    /* eigenvalue pieces */
+    s->kx2 = dalloc(Mh); s->ky2 = dalloc(Ny); s->kz2 = dalloc(Nz);
+    if (p->solver == OC_SOLVER_FFT) {
+        /* src/PressureSolvers.jl:128-130 */
+        for (int m = 0; m < Mh; ++m) { double sn = sin(M_PI * m / Nx); s->kx2[m] = 4 / (s->dx * s->dx) * (sn * sn); }
+        for (int m = 0; m < Ny; ++m) { double sn = sin(M_PI * m / Ny); s->ky2[m] = 4 / (s->dy * s->dy) * (sn * sn); }
+        for (int m = 0; m < Nz; ++m) { double sn = sin(M_PI * m / Nz); s->kz2[m] = 4 / (s->dz * s->dz) * (sn * sn); }
+    } else {
+        /* _r2r_eigen, src/PressureSolvers.jl:618-624 */
+        for (int m = 0; m < Mh; ++m) { int mm = m < Nx - m ? m : Nx - m; double sn = sin(M_PI * mm / Nx); s->kx2[m] = 4 / (s->dx * s->dx) * (sn * sn); }
+        for (int m = 0; m < Ny; ++m) { int mm = m < Ny - m ? m : Ny - m; double sn = sin(M_PI * mm / Ny); s->ky2[m] = 4 / (s->dy * s->dy) * (sn * sn); }
+        /* column coefficients */
+        s->lower = dalloc(Nz); s->upper = dalloc(Nz); s->hw = dalloc(Nz);
+        s->meas = dalloc(Nz); s->iota = dalloc(Nz + 1); s->gauge = dalloc(Nz);
+        for (int k = 0; k < Nz; ++k) {
+            int K = Hz + k;                      /* storage level of cell k */
+            if (p->core == OC_CORE_ANELASTIC) {
+                if (s->uniform) {
+                    /* DirectWeightedPoissonSolver, src/Anelastic.jl:1013-1019 */
+                    double idz2 = 1 / (s->dz * s->dz);
+                    s->lower[k] = k > 0 ? s->wf[K] * idz2 : 0.0;
+                    s->upper[k] = k < Nz - 1 ? s->wf[K + 1] * idz2 : 0.0;
+                    s->hw[k] = s->wc[K];
+                    s->meas[k] = s->dz * s->dz;
+                    s->gauge[k] = 1.0;
+                } else {
+                    /* weighted operator on the stretched column */
+                    s->lower[k] = k > 0 ? s->wf[K] / (s->dzc[K] * s->dzf[K]) : 0.0;
+                    s->upper[k] = k < Nz - 1 ? s->wf[K + 1] / (s->dzc[K] * s->dzf[K + 1]) : 0.0;
+                    s->hw[k] = s->wc[K];
+                    s->meas[k] = s->dzc[K];
+                    s->gauge[k] = s->dzc[K];
+                }
+            } else {
+                /* ColumnTridiagonalSolver(dzc, dzf), src/PressureSolvers.jl:686-700 */
+                s->lower[k] = k > 0 ? 1 / (s->dzc[K] * s->dzf[K]) : 0.0;
+                s->upper[k] = k < Nz - 1 ? 1 / (s->dzc[K] * s->dzf[K + 1]) : 0.0;
+                s->hw[k] = 1.0;
+                s->meas[k] = s->dzc[K];
+                s->gauge[k] = s->dzc[K];
+            }
+        }
+        for (int k = 0; k <= Nz; ++k) {
+            int K = Hz + k;
+            if (p->core == OC_CORE_ANELASTIC)
+                s->iota[k] = s->uniform ? 1 / s->wf[K] : s->dzf[K] / s->wf[K];
+            else
+                s->iota[k] = s->dzf[K];
+        }
+        s->meas_sum = 0.0; s->gauge_sum = 0.0;
+        for (int k = 0; k < Nz; ++k) { s->meas_sum += s->meas[k]; s->gauge_sum += s->gauge[k]; }
+    }
+    return s;
+}
+
+void oc_destroy(oc_sim* s) {
+    if (!s) return;
+    double* ptrs[] = {s->zf, s->zc, s->dzc, s->dzf, s->idzc, s->idzf, s->idz_off, s->wlo, s->whi, s->alo, s->ahi,
+                      s->delta, s->wc, s->wf, s->thf, s->u, s->v, s->w, s->th, s->pr, s->nut, s->kt, s->phi,
+                      s->tu, s->tv, s->tw, s->tt, s->u0, s->v0, s->w0, s->th0, s->src, s->kx2, s->ky2, s->kz2,
+                      s->lower, s->upper, s->hw, s->meas, s->iota, s->gauge};
+    for (size_t q = 0; q < sizeof(ptrs) / sizeof(ptrs[0]); ++q) free(ptrs[q]);
+    free(s->hat); free(s->twx);
+    plan_free(&s->px); plan_free(&s->py); plan_free(&s->pz);
+    free(s);
+}
+
+int64_t oc_storage_size(const oc_sim* s) { return s->n; }
+
+static double* field_ptr(const oc_sim* s, int id) {
+    switch (id) {
+        case OC_U: return s->u;
+        case OC_V: return s->v;
+        case OC_W: return s->w;
+        case OC_THETA: return s->th;
+        case OC_P: return s->pr;
+        case OC_NUT: return s->nut;
+        case OC_PHI: return s->phi;
+        default: return NULL;
+    }
+}
+
+int oc_set_field(oc_sim* s, int id, const double* src) {
+    double* d = field_ptr(s, id);
+    if (!d) return -1;
+    memcpy(d, src, sizeof(double) * (size_t)s->n);
+    return 0;
+}
+
+int oc_get_field(const oc_sim* s, int id, double* dst) {
+    const double* d = field_ptr(s, id);
+    if (!d) return -1;
+    memcpy(dst, d, sizeof(double) * (size_t)s->n);
+    return 0;
+}

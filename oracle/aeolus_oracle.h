@@ -1,0 +1,74 @@
+/*
+ * aeolus_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU FP64 restatement of the Aeolus.jl dynamical-core step (the checker the
+ * CUDA library is compared against).  Nothing in the product path links,
+ * loads or calls this code; only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / --impl reference legs of bench.py do.
+ *
+ * Arrays crossing this interface use the reference storage layout: a field
+ * on a grid of Nx x Ny x Nz interior cells with halos (Hx, Hy, Hz) is a
+ * column-major (x fastest) array of (Nx+2Hx)(Ny+2Hy)(Nz+2Hz) doubles, the
+ * interior at 0-based indices [H, H+N).  FaceX index i is the west face of
+ * cell i, FaceY the south face, FaceZ the bottom face (src/Grids.jl:52-80).
+ */
+#ifndef AEOLUS_ORACLE_H
+#define AEOLUS_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { OC_BC_PERIODIC = 0, OC_BC_WALL = 1 };
+enum { OC_CORE_BOUSSINESQ = 0, OC_CORE_ANELASTIC = 1 };
+enum { OC_ADV_CENTRED = 0, OC_ADV_WENO_JS5 = 1, OC_ADV_WENO_Z5 = 2 };
+enum { OC_SOLVER_FFT = 0, OC_SOLVER_COLUMN = 1 };
+enum { OC_U = 0, OC_V = 1, OC_W = 2, OC_THETA = 3, OC_P = 4, OC_NUT = 5, OC_PHI = 6 };
+
+typedef struct {
+    int32_t nx, ny, nz, hx, hy, hz;
+    double lx, ly, lz, x0, y0, z0;
+    int32_t stretched;        /* 0: uniform z; 1: zf[] gives the Nz+1 interior faces */
+    int32_t bc_x, bc_y, bc_z; /* x, y: periodic only; z: periodic or wall */
+    int32_t core, advection, solver;
+    double nu, theta0, g, f_coriolis, c_s, pr_t;
+    double flux_bot, flux_top, sponge_alpha, sponge_zstart;
+} oc_params;
+
+typedef struct oc_sim oc_sim;
+
+/* zf: Nz+1 interior face heights (stretched only, else NULL).
+ * wc (Nz+2Hz), wf (Nz+2Hz+1), thf (Nz+2Hz+1): padded weights and the face
+ * reference potential temperature of the anelastic core (NULL otherwise). */
+oc_sim* oc_create(const oc_params* p, const double* zf, const double* wc,
+                  const double* wf, const double* thf);
+void oc_destroy(oc_sim* s);
+int64_t oc_storage_size(const oc_sim* s);
+int oc_set_field(oc_sim* s, int id, const double* src);
+int oc_get_field(const oc_sim* s, int id, double* dst);
+void oc_fill_state_halos(oc_sim* s);
+int oc_step_rk3(oc_sim* s, double dt, int nsteps);
+int oc_step_euler(oc_sim* s, double dt, int nsteps);
+/* Chorin projection of the current velocity (dt = 1). */
+int oc_project(oc_sim* s);
+/* Tendencies of the current state (halos filled first) into tu..tθ (storage). */
+int oc_tendencies(oc_sim* s, double* tu, double* tv, double* tw, double* tt);
+/* Solve the projection's Poisson problem: src and phi are interior-sized
+ * (Nx*Ny*Nz, x fastest). */
+int oc_pressure_solve(oc_sim* s, const double* src, double* phi);
+/* Apply the discrete operator the solver inverts (interior-sized in/out). */
+int oc_apply_poisson_operator(oc_sim* s, const double* phi, double* out);
+double oc_kinetic_energy(oc_sim* s);
+double oc_max_divergence(oc_sim* s);
+void oc_set_threads(int n);
+
+/* Philox4x32-10 block function and the uniform fill of the synthetic inputs. */
+void oc_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+void oc_uniform_fill(uint64_t seed, uint32_t stream, int64_t n, double amp, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

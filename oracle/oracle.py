@@ -1,0 +1,201 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes binding of the oracle (oracle/aeolus_oracle.c).
+
+The oracle is a CPU FP64 restatement of the reference's dynamical-core step;
+tests, `__graft_entry__.smoke()` and bench.py's CPU-baseline leg use it as the
+checker.  It takes the same `CoreSpec` as the product library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "libaeolus_oracle.so")
+
+_D = C.POINTER(C.c_double)
+
+
+class OcParams(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("hx", C.c_int32), ("hy", C.c_int32), ("hz", C.c_int32),
+        ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double),
+        ("x0", C.c_double), ("y0", C.c_double), ("z0", C.c_double),
+        ("stretched", C.c_int32), ("bc_x", C.c_int32), ("bc_y", C.c_int32), ("bc_z", C.c_int32),
+        ("core", C.c_int32), ("advection", C.c_int32), ("solver", C.c_int32),
+        ("nu", C.c_double), ("theta0", C.c_double), ("g", C.c_double), ("f_coriolis", C.c_double),
+        ("c_s", C.c_double), ("pr_t", C.c_double),
+        ("flux_bot", C.c_double), ("flux_top", C.c_double), ("sponge_alpha", C.c_double),
+        ("sponge_zstart", C.c_double),
+    ]
+
+
+_lib = None
+
+
+def build():
+    r = subprocess.run(["make", "-C", _HERE], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
+    return LIB_PATH
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        build()
+    lib = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    lib.oc_create.argtypes = [C.POINTER(OcParams), _D, _D, _D, _D]
+    lib.oc_create.restype = P
+    lib.oc_destroy.argtypes = [P]
+    lib.oc_storage_size.argtypes = [P]
+    lib.oc_storage_size.restype = C.c_int64
+    lib.oc_set_field.argtypes = [P, C.c_int, _D]
+    lib.oc_get_field.argtypes = [P, C.c_int, _D]
+    lib.oc_fill_state_halos.argtypes = [P]
+    lib.oc_step_rk3.argtypes = [P, C.c_double, C.c_int]
+    lib.oc_step_euler.argtypes = [P, C.c_double, C.c_int]
+    lib.oc_project.argtypes = [P]
+    lib.oc_tendencies.argtypes = [P, _D, _D, _D, _D]
+    lib.oc_pressure_solve.argtypes = [P, _D, _D]
+    lib.oc_apply_poisson_operator.argtypes = [P, _D, _D]
+    lib.oc_kinetic_energy.argtypes = [P]
+    lib.oc_kinetic_energy.restype = C.c_double
+    lib.oc_max_divergence.argtypes = [P]
+    lib.oc_max_divergence.restype = C.c_double
+    lib.oc_set_threads.argtypes = [C.c_int]
+    lib.oc_philox4x32.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+    lib.oc_uniform_fill.argtypes = [C.c_uint64, C.c_uint32, C.c_int64, C.c_double, _D]
+    _lib = lib
+    return lib
+
+
+FIELD_IDS = {"u": 0, "v": 1, "w": 2, "theta": 3, "p": 4, "nut": 5, "phi": 6}
+_ADV = {"centred": 0, "weno_js5": 1, "weno_z5": 2}
+_SOLV = {"fft": 0, "column": 1}
+_CORE = {"boussinesq": 0, "anelastic": 1}
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_D)
+
+
+def set_threads(n: int):
+    load().oc_set_threads(int(n))
+
+
+def philox4x32(ctr, key):
+    lib = load()
+    c = (C.c_uint32 * 4)(*ctr)
+    k = (C.c_uint32 * 2)(*key)
+    o = (C.c_uint32 * 4)()
+    lib.oc_philox4x32(c, k, o)
+    return tuple(int(x) for x in o)
+
+
+def uniform_fill(seed: int, stream: int, n: int, amp: float) -> np.ndarray:
+    out = np.empty(n)
+    load().oc_uniform_fill(seed, stream, n, amp, _p(out))
+    return out
+
+
+class OracleSimulation:
+    """The oracle's domain: same CoreSpec and storage-array interface as aeolus_b200.Simulation."""
+
+    def __init__(self, spec):
+        lib = load()
+        g = spec.grid
+        p = OcParams()
+        p.nx, p.ny, p.nz = g.size
+        p.hx, p.hy, p.hz = g.halo
+        p.lx, p.ly, p.lz = g.extent
+        p.x0, p.y0, p.z0 = g.origin
+        p.stretched = 1 if g.stretched else 0
+        p.bc_x = p.bc_y = 0
+        p.bc_z = 0 if g.bc_z == "periodic" else 1
+        p.core = _CORE[spec.core]
+        p.advection = _ADV[spec.advection]
+        p.solver = _SOLV[spec.solver]
+        p.nu, p.theta0, p.g, p.f_coriolis = spec.nu, spec.theta0, spec.g, spec.f_coriolis
+        p.c_s, p.pr_t = spec.c_s, spec.pr_t
+        p.flux_bot, p.flux_top = spec.flux_bot, spec.flux_top
+        p.sponge_alpha, p.sponge_zstart = spec.sponge_alpha, spec.sponge_zstart
+        self._keep = [g.zf, spec.wc, spec.wf, spec.thf]
+        h = lib.oc_create(C.byref(p), _p(g.zf), _p(spec.wc), _p(spec.wf), _p(spec.thf))
+        if not h:
+            raise ValueError("oracle: unsupported configuration")
+        self._h = h
+        self._lib = lib
+        self.spec = spec
+        self.grid = g
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.oc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_field(self, name, data):
+        a = np.ascontiguousarray(data, dtype=np.float64)
+        assert a.shape == self.grid.storage_shape
+        assert self._lib.oc_set_field(self._h, FIELD_IDS[name], _p(a)) == 0
+
+    def get_field(self, name):
+        out = np.empty(self.grid.storage_shape)
+        assert self._lib.oc_get_field(self._h, FIELD_IDS[name], _p(out)) == 0
+        return out
+
+    def set_state(self, u, v, w, theta):
+        for n, a in zip(("u", "v", "w", "theta"), (u, v, w, theta)):
+            self.set_field(n, a)
+
+    def get_state(self):
+        return tuple(self.get_field(n) for n in ("u", "v", "w", "theta"))
+
+    def fill_halos(self):
+        self._lib.oc_fill_state_halos(self._h)
+
+    def step_rk3(self, dt, nsteps=1):
+        assert self._lib.oc_step_rk3(self._h, float(dt), int(nsteps)) == 0
+
+    def step(self, dt, nsteps=1):
+        assert self._lib.oc_step_euler(self._h, float(dt), int(nsteps)) == 0
+
+    def project(self):
+        assert self._lib.oc_project(self._h) == 0
+
+    def tendencies(self):
+        outs = [np.empty(self.grid.storage_shape) for _ in range(4)]
+        self._lib.oc_tendencies(self._h, *[_p(o) for o in outs])
+        return outs
+
+    def pressure_solve(self, src):
+        g = self.grid
+        s = np.ascontiguousarray(src, dtype=np.float64)
+        assert s.shape == (g.nz, g.ny, g.nx)
+        out = np.empty_like(s)
+        self._lib.oc_pressure_solve(self._h, _p(s), _p(out))
+        return out
+
+    def apply_poisson_operator(self, phi):
+        p = np.ascontiguousarray(phi, dtype=np.float64)
+        out = np.empty_like(p)
+        self._lib.oc_apply_poisson_operator(self._h, _p(p), _p(out))
+        return out
+
+    def kinetic_energy(self):
+        return self._lib.oc_kinetic_energy(self._h)
+
+    def max_divergence(self):
+        return self._lib.oc_max_divergence(self._h)

@@ -1,0 +1,213 @@
+"""Parity of the CUDA step (through the C-ABI) against the FP64 oracle.
+
+Tolerances (the north-star parity bar):
+  * FP64: relative L2 per prognostic field <= 1e-11 after 1 step and
+    <= 1e-8 after 100 steps; post-projection divergence at round-off;
+  * FP32-mixed against the FP64 oracle: relative L2 <= 1e-5.
+"""
+import numpy as np
+import pytest
+
+from aeolus_b200 import CoreSpec, regular_grid, stretched_grid, tanh_beta_for_first_cell, tanh_faces
+from aeolus_b200.inputs import cbl_initial, cbl_theta_profile, philox_uniform, taylor_green
+from aeolus_b200.reference_state import anelastic_profiles, exponential_density
+from oracle.oracle import OracleSimulation
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("u", "v", "w", "theta")
+
+
+def Sim(spec):
+    from aeolus_b200.simulation import Simulation
+    return Simulation(spec)
+
+
+def rel_l2(a, b, g):
+    a = a[g.interior]
+    b = b[g.interior]
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def compare(gpu, orc, g, tol):
+    errs = {}
+    for n in FIELDS:
+        errs[n] = rel_l2(gpu.get_field(n), orc.get_field(n), g)
+    assert all(e <= tol for e in errs.values()), errs
+    return errs
+
+
+def tgv_pair(n, scheme, precision="fp64", nu=1 / 1600):
+    g = regular_grid((n, n, n), (2 * np.pi,) * 3)
+    spec = CoreSpec(grid=g, advection=scheme, nu=nu, precision=precision)
+    ospec = CoreSpec(grid=g, advection=scheme, nu=nu)
+    u, v, w, th = taylor_green(g, seed=1, amp=1e-3)
+    gs, os_ = Sim(spec), OracleSimulation(ospec)
+    for s in (gs, os_):
+        s.set_state(u, v, w, th)
+        s.project()
+    return g, gs, os_
+
+
+def cbl_spec(nx=32, nz=32, c_s=0.17, flux=0.1, precision="fp64"):
+    lz = 2000.0
+    dz1 = 8.0 * 128 / nz
+    g = stretched_grid((nx, nx, nz), (5120.0 * nx / 256, 5120.0 * nx / 256, lz),
+                       tanh_faces(nz, lz, tanh_beta_for_first_cell(nz, lz, dz1)))
+    th = cbl_theta_profile(g.znodes("c"))
+    prof = anelastic_profiles(g, exponential_density(g), th)
+    mk = lambda prec: CoreSpec(grid=g, core="anelastic", c_s=c_s, flux_bot=flux, precision=prec,
+                               wc=prof["wc"], wf=prof["wf"], thf=prof["thf"])
+    return g, mk(precision), mk("fp64")
+
+
+# ------------------------------------------------------------------ inputs --
+def test_device_philox_fill_matches_the_generator():
+    g = regular_grid((16, 8, 4), (1, 1, 1))
+    s = Sim(CoreSpec(grid=g))
+    s.fill_uniform("theta", 2026, 3, 0.5)
+    ref = 0.5 * (2 * philox_uniform(2026, 3, g.ncells) - 1)
+    assert np.array_equal(s.get_field("theta")[g.interior].ravel(), ref)
+
+
+@pytest.mark.parametrize("bc_z", ["periodic", "wall"])
+def test_halos_match_the_reference_fill(bc_z):
+    g = regular_grid((16, 8, 8), (1, 1, 1), bc_z=bc_z)
+    solver = "fft" if bc_z == "periodic" else "column"
+    s, o = Sim(CoreSpec(grid=g, solver=solver)), OracleSimulation(CoreSpec(grid=g, solver=solver))
+    rng = np.random.default_rng(0)
+    for n in FIELDS:
+        a = rng.standard_normal(g.storage_shape)
+        s.set_field(n, a)
+        o.set_field(n, a)
+    o.fill_halos()
+    for n in FIELDS:
+        assert np.array_equal(s.get_field(n), o.get_field(n)), n
+
+
+# ------------------------------------------------------------------ Poisson -
+@pytest.mark.parametrize("case", ["fft", "column", "stretched", "anelastic"])
+def test_pressure_solve_parity(case):
+    if case == "fft":
+        g = regular_grid((32, 16, 8), (2.0, 1.0, 0.5))
+        spec = CoreSpec(grid=g)
+    elif case == "column":
+        g = regular_grid((32, 16, 8), (2.0, 1.0, 0.5), bc_z="wall")
+        spec = CoreSpec(grid=g)
+    elif case == "stretched":
+        g = stretched_grid((32, 16, 12), (2.0, 1.0, 1.0), tanh_faces(12, 1.0, 1.5))
+        spec = CoreSpec(grid=g)
+    else:
+        g, spec, _ = cbl_spec(nx=16, nz=16)
+    src = np.random.default_rng(7).standard_normal((g.nz, g.ny, g.nx))
+    src -= src.mean()
+    a = Sim(spec).pressure_solve(src)
+    b = OracleSimulation(spec).pressure_solve(src)
+    assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+
+
+# ------------------------------------------------------------------ steps ---
+@pytest.mark.parametrize("scheme", ["centred", "weno_js5", "weno_z5"])
+def test_taylor_green_one_step(scheme):
+    g, gs, os_ = tgv_pair(32, scheme)
+    assert gs.max_divergence() < 1e-12
+    gs.step_rk3(0.01)
+    os_.step_rk3(0.01)
+    compare(gs, os_, g, 1e-11)
+    assert gs.max_divergence() < 1e-12
+    assert abs(gs.kinetic_energy() - os_.kinetic_energy()) <= 1e-12 * os_.kinetic_energy()
+    p_rel = rel_l2(gs.get_field("p"), os_.get_field("p"), g)
+    assert p_rel < 1e-9
+
+
+def test_taylor_green_weno5_100_steps_64():
+    g, gs, os_ = tgv_pair(64, "weno_js5")
+    gs.step_rk3(0.01, 100)
+    os_.step_rk3(0.01, 100)
+    compare(gs, os_, g, 1e-8)
+    assert gs.max_divergence() < 1e-12
+
+
+def test_euler_step_parity():
+    g, gs, os_ = tgv_pair(16, "weno_z5")
+    gs.step(0.01, 2)
+    os_.step(0.01, 2)
+    compare(gs, os_, g, 1e-11)
+
+
+def test_anelastic_cbl_parity():
+    g, spec, ospec = cbl_spec(nx=32, nz=32)
+    u, v, w, th, _ = cbl_initial(g, seed=1, noise=0.1)
+    gs, os_ = Sim(spec), OracleSimulation(ospec)
+    for s in (gs, os_):
+        s.set_state(u, v, w, th)
+    gs.step_rk3(1.0)
+    os_.step_rk3(1.0)
+    compare(gs, os_, g, 1e-11)
+    gs.step_rk3(1.0, 9)
+    os_.step_rk3(1.0, 9)
+    compare(gs, os_, g, 1e-9)
+    assert gs.max_divergence() < 1e-13
+    nut = gs.get_field("nut")[g.interior]
+    assert np.all(np.isfinite(nut)) and nut.max() > 0
+
+
+def test_boussinesq_stretched_sgs_buoyancy_parity():
+    nz = 16
+    g = stretched_grid((32, 16, nz), (640.0, 320.0, 400.0), tanh_faces(nz, 400.0, 1.5))
+    spec = CoreSpec(grid=g, nu=1e-3, theta0=300.0, c_s=0.17, flux_bot=0.05, f_coriolis=1e-4,
+                    sponge_alpha=0.01, sponge_zstart=300.0)
+    th = np.full(g.storage_shape, 300.0)
+    rng = np.random.default_rng(3)
+    th[g.interior] += 0.1 * rng.standard_normal((nz, 16, 32))
+    u = g.zeros()
+    u[g.interior] = 0.5 + 0.1 * rng.standard_normal((nz, 16, 32))
+    gs, os_ = Sim(spec), OracleSimulation(spec)
+    for s in (gs, os_):
+        s.set_state(u, g.zeros(), g.zeros(), th)
+        s.project()
+    gs.step_rk3(0.5, 3)
+    os_.step_rk3(0.5, 3)
+    compare(gs, os_, g, 1e-11)
+
+
+# ------------------------------------------------------------------ mixed ---
+def test_fp32_mixed_close_to_fp64_oracle():
+    g, gs, os_ = tgv_pair(32, "weno_js5", precision="fp32_mixed")
+    gs.step_rk3(0.01, 10)
+    os_.step_rk3(0.01, 10)
+    errs = {n: rel_l2(gs.get_field(n), os_.get_field(n), g) for n in ("u", "v", "w")}
+    assert all(e < 1e-5 for e in errs.values()), errs
+
+
+def test_fp32_mixed_anelastic_close_to_fp64():
+    g, spec, ospec = cbl_spec(nx=32, nz=32, precision="fp32_mixed")
+    u, v, w, th, _ = cbl_initial(g, seed=1, noise=0.1)
+    gs, os_ = Sim(spec), OracleSimulation(ospec)
+    for s in (gs, os_):
+        s.set_state(u, v, w, th)
+    gs.step_rk3(1.0, 5)
+    os_.step_rk3(1.0, 5)
+    assert rel_l2(gs.get_field("theta"), os_.get_field("theta"), g) < 1e-6
+    assert rel_l2(gs.get_field("w"), os_.get_field("w"), g) < 1e-3
+
+
+# ------------------------------------------------------------------ errors --
+def test_nonfinite_state_raises_numerical_failure():
+    from aeolus_b200._lib import NumericalFailure
+    g, gs, _ = tgv_pair(16, "centred")
+    th = gs.get_field("theta")
+    th[g.interior][0, 0, 0] = np.nan
+    th[3, 3, 3] = np.nan
+    gs.set_field("theta", th)
+    with pytest.raises(NumericalFailure):
+        gs.step_rk3(0.01)
+
+
+def test_bad_arguments_are_rejected():
+    g, gs, _ = tgv_pair(16, "centred")
+    with pytest.raises(ValueError):
+        gs.step_rk3(-1.0)
+    with pytest.raises(ValueError):
+        gs.set_field("u", np.zeros((3, 3, 3)))
