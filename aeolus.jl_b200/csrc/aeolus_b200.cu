@@ -637,39 +637,6 @@ struct Core : CoreBase {
     }
 };
 
-// r2c of an interior source along x: pack pairs, FFT, post-process (the
-// div_fftx kernel body with the source read directly).
-template <typename R>
-__global__ void __launch_bounds__(256) src_fftx_kernel(Geo g, const R* __restrict__ src, cplx<R>* __restrict__ S,
-                                                       const cplx<R>* __restrict__ tw, int NT, int rows) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx<R>* buf = reinterpret_cast<cplx<R>*>(smem_raw);
-    const int M = g.nx / 2, Mh = M + 1;
-    const long long nrows = (long long)g.ny * g.nz;
-    const long long row0 = (long long)blockIdx.x * rows;
-    for (int e = threadIdx.x; e < rows * M; e += blockDim.x) {
-        int r = e / M, n = e % M;
-        long long row = row0 + r;
-        cplx<R> z = cmk<R>(R(0), R(0));
-        if (row < nrows) z = cmk<R>(src[row * g.nx + 2 * n], src[row * g.nx + 2 * n + 1]);
-        buf[r * M + n] = z;
-    }
-    __syncthreads();
-    smem_fft<R, false, false, FFT_KB>(buf, M, rows, M, 1, tw, NT);
-    const int tstep = NT / g.nx;
-    for (int e = threadIdx.x; e < rows * Mh; e += blockDim.x) {
-        int r = e / Mh, kk = e % Mh;
-        long long row = row0 + r;
-        if (row >= nrows) continue;
-        cplx<R> a = buf[r * M + (kk == M ? 0 : kk)];
-        cplx<R> b = buf[r * M + (kk == 0 ? 0 : M - kk)];
-        R er = R(0.5) * (a.x + b.x), ei = R(0.5) * (a.y - b.y);
-        R orr = R(0.5) * (a.y + b.y), oi = R(-0.5) * (a.x - b.x);
-        cplx<R> wv = tw[(kk * tstep) & (NT - 1)];
-        S[row * Mh + kk] = cmk<R>(er + (wv.x * orr - wv.y * oi), ei + (wv.x * oi + wv.y * orr));
-    }
-}
-
 template <typename R>
 aeo_status Core<R>::src_fftx(const R* src) {
     const int M = g.nx / 2;
