@@ -281,7 +281,7 @@ struct ColumnCoef {
 // One warp per CTA: lane = kx, blockIdx.y = ky.  dsc: FP64 scratch column
 // storage (nz x ny x Mh complex) holding the forward-elimination values.
 template <typename R>
-__global__ void __launch_bounds__(32) thomas_kernel(Geo g, cplx<R>* __restrict__ S, cplx<double>* __restrict__ dsc,
+__global__ void __launch_bounds__(32) thomas_kernel(Geo g, cplx<R>* S, cplx<double>* dsc,  // S and dsc alias in FP64
                                                     ColumnCoef c) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* cp = reinterpret_cast<double*>(smem_raw);   // [nz][32]

@@ -33,6 +33,9 @@
 
 static std::string g_create_error;
 
+// The message aeo_last_error(NULL) returns (also set by handle-free entry points).
+void aeo_set_global_error(const std::string& m) { g_create_error = m; }
+
 #define CK(call)                                                                         \
     do {                                                                                 \
         cudaError_t e_ = (call);                                                         \
