@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libaeolus_b200.so")
 SYMBOLS = (
     "aeo_create", "aeo_destroy", "aeo_set_field", "aeo_get_field", "aeo_step_rk3", "aeo_step_euler",
     "aeo_pressure_solve", "aeo_project", "aeo_kinetic_energy", "aeo_max_divergence", "aeo_step_rk3_async",
-    "aeo_synchronize", "aeo_profile_step", "aeo_launches_per_step", "aeo_stream", "aeo_fill_uniform", "aeo_last_error",
+    "aeo_synchronize", "aeo_profile_step", "aeo_launches_per_step", "aeo_stream", "aeo_fill_uniform", "aeo_pressure_solve_column_noalloc", "aeo_last_error",
     "aeo_version",
 )
 
@@ -85,6 +85,8 @@ def load():
     lib.aeo_stream.argtypes = [P]
     lib.aeo_stream.restype = C.c_void_p
     lib.aeo_fill_uniform.argtypes = [P, C.c_int32, C.c_uint64, C.c_uint32, C.c_double, C.c_int32]
+    lib.aeo_pressure_solve_column_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                                      D, D, D, D, D, D, P, P, P]
     lib.aeo_last_error.argtypes = [P]
     lib.aeo_last_error.restype = C.c_char_p
     lib.aeo_version.restype = C.c_char_p

@@ -156,6 +156,29 @@ void* aeo_stream(aeo_sim* h);
 aeo_status aeo_fill_uniform(aeo_sim* h, int32_t field, uint64_t seed, uint32_t stream,
                             double amp, int32_t mode);
 
+/* The column pressure solve (x, y periodic; zero-flux walls in z) without a
+ * handle and without allocating device memory.  This entry point has no
+ * counterpart in the reference.  It is for callers that cannot call
+ * cudaMalloc: a host runtime whose device memory must all come from its own
+ * pool or budget, an application that reserves every byte at start-up, or
+ * a stepping loop that cannot afford cudaMalloc's implicit synchronisation.
+ * Its scratch (twiddles, eigenvalues, coefficients and the (nx/2+1)*ny*nz
+ * complex FP64 spectrum) lives in one static 32 MiB device array of this
+ * library, held by every GPU that loads it until the process exits; a grid
+ * whose scratch does not fit is rejected with AEO_ERR_ARGUMENT.  Operator:
+ * the ColumnTridiagonalSolver coefficients lower, upper, hweight, measure
+ * (nz each), inv_coupling (nz+1) and gauge (nz), host arrays; src and phi
+ * are caller-owned device arrays of nx*ny*nz doubles (x fastest).  It runs
+ * on `stream` on the current device and returns after that stream has
+ * synchronised.  The first call on a device looks up the scratch address;
+ * make that first call before any stream capture.  Calls share the scratch:
+ * calls that overlap on the GPU (other streams, other host threads) race. */
+aeo_status aeo_pressure_solve_column_noalloc(int32_t nx, int32_t ny, int32_t nz, double lx, double ly,
+                                             const double* lower, const double* upper,
+                                             const double* hweight, const double* measure,
+                                             const double* inv_coupling, const double* gauge,
+                                             const double* src, double* phi, void* stream);
+
 /* Last error message of the handle (or of the last failed aeo_create when h is NULL). */
 const char* aeo_last_error(const aeo_sim* h);
 
