@@ -38,6 +38,7 @@ struct SweepArgs {
     R dt, ca, cb;
     int stage;
     R nu, gacc, theta0, fcor, inv_prt, pr_t, flux_bot, flux_top, sp_alpha, sp_zstart, sp_inv;
+    R c_s;
 };
 
 // ---- metric accessors (src/FiniteVolume.jl:146-186) -----------------------
@@ -104,30 +105,36 @@ __device__ __forceinline__ R weno5_left(R v1, R v2, R v3, R v4, R v5) {
     return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
 }
 
-// Upwinded face value between cells c and c+1 along the axis of stride st
-// (src/AdvectionSchemes.jl:623-666); `at` points at cell c.
-template <typename R, int ADV>
-__device__ __forceinline__ R face_val(const R* __restrict__ at, long long st, R vel) {
-    if (vel >= R(0))
-        return weno5_left<R, ADV>(__ldg(at - 2 * st), __ldg(at - st), __ldg(at), __ldg(at + st), __ldg(at + 2 * st));
-    return weno5_left<R, ADV>(__ldg(at + 3 * st), __ldg(at + 2 * st), __ldg(at + st), __ldg(at), __ldg(at - st));
+// Upwinded face values between cells c and c+1 along x, y or z
+// (src/AdvectionSchemes.jl:623-666, mirror-symmetric selection): the
+// left-biased stencil c-2..c+2 for a non-negative face velocity, else the
+// mirrored right-biased c+3..c-1.
+template <typename R, int ADV, class A>
+__device__ __forceinline__ R face_x(const A& F, int c, int dj, int dk, R vel) {
+    if (vel >= R(0)) return weno5_left<R, ADV>(F(c - 2, dj, dk), F(c - 1, dj, dk), F(c, dj, dk), F(c + 1, dj, dk), F(c + 2, dj, dk));
+    return weno5_left<R, ADV>(F(c + 3, dj, dk), F(c + 2, dj, dk), F(c + 1, dj, dk), F(c, dj, dk), F(c - 1, dj, dk));
+}
+template <typename R, int ADV, class A>
+__device__ __forceinline__ R face_y(const A& F, int di, int c, int dk, R vel) {
+    if (vel >= R(0)) return weno5_left<R, ADV>(F(di, c - 2, dk), F(di, c - 1, dk), F(di, c, dk), F(di, c + 1, dk), F(di, c + 2, dk));
+    return weno5_left<R, ADV>(F(di, c + 3, dk), F(di, c + 2, dk), F(di, c + 1, dk), F(di, c, dk), F(di, c - 1, dk));
+}
+template <typename R, int ADV, class A>
+__device__ __forceinline__ R face_z(const A& F, int di, int dj, int c, R vel) {
+    if (vel >= R(0)) return weno5_left<R, ADV>(F(di, dj, c - 2), F(di, dj, c - 1), F(di, dj, c), F(di, dj, c + 1), F(di, dj, c + 2));
+    return weno5_left<R, ADV>(F(di, dj, c + 3), F(di, dj, c + 2), F(di, dj, c + 1), F(di, dj, c), F(di, dj, c - 1));
 }
 
-// ---- the sweep --------------------------------------------------------------
-template <typename R, int ADV, bool SGS, bool ANEL, bool UNI>
-__global__ void __launch_bounds__(256) sweep_kernel(SweepArgs<R> a) {
-    const Geo& g = a.g;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int j = blockIdx.y * blockDim.y + threadIdx.y;
-    int k = blockIdx.z * blockDim.z + threadIdx.z;
-    if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+// ---- the tendency at one point ------------------------------------------------
+// U, V, W, T, N are accessors (di, dj, dk) -> value around the point at level
+// k; the same arithmetic serves the direct form (global memory) and the
+// tiled form (shared-memory planes).
+template <typename R, int ADV, bool SGS, bool ANEL, bool UNI, class AU, class AN>
+__device__ __forceinline__ void sweep_point(const SweepArgs<R>& a, const Geo& g, int k, const AU& U, const AU& V,
+                                            const AU& W, const AU& T, const AN& N, R& tu, R& tv, R& tw, R& tt) {
     Met<R, UNI> m(g);
-    const long long q = pidx(g, i, j, k);
-    const long long sy = g.sy, sz = g.sz;
-    Nb<R> U{a.u + q, sy, sz}, V{a.v + q, sy, sz}, W{a.w + q, sy, sz}, T{a.th + q, sy, sz};
     const R idx = R(g.idx), idy = R(g.idy), idx2 = R(g.idx2), idy2 = R(g.idy2);
     const R h = R(0.5);
-    R tu, tv, tw, tt;
 
     if (ANEL) {
         // W-weighted centred forms (src/Anelastic.jl:1193-1306)
@@ -216,44 +223,40 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs<R> a) {
     } else {
         // WENO flux forms on a uniform grid (src/AdvectionSchemes.jl:685-699, :1203-1256)
         const R idz = R(g.idz);
-        const R* up = a.u + q;
-        const R* vp = a.v + q;
-        const R* wp = a.w + q;
-        const R* tp = a.th + q;
         {
             R Ue = (U(0, 0, 0) + U(1, 0, 0)) / R(2), Uw = (U(-1, 0, 0) + U(0, 0, 0)) / R(2);
-            R dx = (Ue * face_val<R, ADV>(up, 1, Ue) - Uw * face_val<R, ADV>(up - 1, 1, Uw)) * idx;
+            R dx = (Ue * face_x<R, ADV>(U, 0, 0, 0, Ue) - Uw * face_x<R, ADV>(U, -1, 0, 0, Uw)) * idx;
             R Vn = (V(-1, 1, 0) + V(0, 1, 0)) / R(2), Vs = (V(-1, 0, 0) + V(0, 0, 0)) / R(2);
-            R dy = (Vn * face_val<R, ADV>(up, sy, Vn) - Vs * face_val<R, ADV>(up - sy, sy, Vs)) * idy;
+            R dy = (Vn * face_y<R, ADV>(U, 0, 0, 0, Vn) - Vs * face_y<R, ADV>(U, 0, -1, 0, Vs)) * idy;
             R Wt = (W(-1, 0, 1) + W(0, 0, 1)) / R(2), Wb = (W(-1, 0, 0) + W(0, 0, 0)) / R(2);
-            R dz = (Wt * face_val<R, ADV>(up, sz, Wt) - Wb * face_val<R, ADV>(up - sz, sz, Wb)) * idz;
+            R dz = (Wt * face_z<R, ADV>(U, 0, 0, 0, Wt) - Wb * face_z<R, ADV>(U, 0, 0, -1, Wb)) * idz;
             tu = R(0) - (dx + dy + dz);
         }
         {
             R Ue = (U(1, -1, 0) + U(1, 0, 0)) / R(2), Uw = (U(0, -1, 0) + U(0, 0, 0)) / R(2);
-            R dx = (Ue * face_val<R, ADV>(vp, 1, Ue) - Uw * face_val<R, ADV>(vp - 1, 1, Uw)) * idx;
+            R dx = (Ue * face_x<R, ADV>(V, 0, 0, 0, Ue) - Uw * face_x<R, ADV>(V, -1, 0, 0, Uw)) * idx;
             R Vn = (V(0, 0, 0) + V(0, 1, 0)) / R(2), Vs = (V(0, -1, 0) + V(0, 0, 0)) / R(2);
-            R dy = (Vn * face_val<R, ADV>(vp, sy, Vn) - Vs * face_val<R, ADV>(vp - sy, sy, Vs)) * idy;
+            R dy = (Vn * face_y<R, ADV>(V, 0, 0, 0, Vn) - Vs * face_y<R, ADV>(V, 0, -1, 0, Vs)) * idy;
             R Wt = (W(0, -1, 1) + W(0, 0, 1)) / R(2), Wb = (W(0, -1, 0) + W(0, 0, 0)) / R(2);
-            R dz = (Wt * face_val<R, ADV>(vp, sz, Wt) - Wb * face_val<R, ADV>(vp - sz, sz, Wb)) * idz;
+            R dz = (Wt * face_z<R, ADV>(V, 0, 0, 0, Wt) - Wb * face_z<R, ADV>(V, 0, 0, -1, Wb)) * idz;
             tv = R(0) - (dx + dy + dz);
         }
         {
             R Ue = (U(1, 0, -1) + U(1, 0, 0)) / R(2), Uw = (U(0, 0, -1) + U(0, 0, 0)) / R(2);
-            R dx = (Ue * face_val<R, ADV>(wp, 1, Ue) - Uw * face_val<R, ADV>(wp - 1, 1, Uw)) * idx;
+            R dx = (Ue * face_x<R, ADV>(W, 0, 0, 0, Ue) - Uw * face_x<R, ADV>(W, -1, 0, 0, Uw)) * idx;
             R Vn = (V(0, 1, -1) + V(0, 1, 0)) / R(2), Vs = (V(0, 0, -1) + V(0, 0, 0)) / R(2);
-            R dy = (Vn * face_val<R, ADV>(wp, sy, Vn) - Vs * face_val<R, ADV>(wp - sy, sy, Vs)) * idy;
+            R dy = (Vn * face_y<R, ADV>(W, 0, 0, 0, Vn) - Vs * face_y<R, ADV>(W, 0, -1, 0, Vs)) * idy;
             R Wt = (W(0, 0, 0) + W(0, 0, 1)) / R(2), Wb = (W(0, 0, -1) + W(0, 0, 0)) / R(2);
-            R dz = (Wt * face_val<R, ADV>(wp, sz, Wt) - Wb * face_val<R, ADV>(wp - sz, sz, Wb)) * idz;
+            R dz = (Wt * face_z<R, ADV>(W, 0, 0, 0, Wt) - Wb * face_z<R, ADV>(W, 0, 0, -1, Wb)) * idz;
             tw = R(0) - (dx + dy + dz);
         }
         {
             R uw = U(0, 0, 0), ue = U(1, 0, 0);
-            R Fx = (ue * face_val<R, ADV>(tp, 1, ue) - uw * face_val<R, ADV>(tp - 1, 1, uw)) * idx;
+            R Fx = (ue * face_x<R, ADV>(T, 0, 0, 0, ue) - uw * face_x<R, ADV>(T, -1, 0, 0, uw)) * idx;
             R vs = V(0, 0, 0), vn = V(0, 1, 0);
-            R Fy = (vn * face_val<R, ADV>(tp, sy, vn) - vs * face_val<R, ADV>(tp - sy, sy, vs)) * idy;
+            R Fy = (vn * face_y<R, ADV>(T, 0, 0, 0, vn) - vs * face_y<R, ADV>(T, 0, -1, 0, vs)) * idy;
             R wb = W(0, 0, 0), wt = W(0, 0, 1);
-            R Fz = (wt * face_val<R, ADV>(tp, sz, wt) - wb * face_val<R, ADV>(tp - sz, sz, wb)) * idz;
+            R Fz = (wt * face_z<R, ADV>(T, 0, 0, 0, wt) - wb * face_z<R, ADV>(T, 0, 0, -1, wb)) * idz;
             tt = R(0) - (Fx + Fy + Fz);
         }
     }
@@ -277,7 +280,6 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs<R> a) {
 
     // Smagorinsky SGS fluxes (eddy viscosity from the nut array, halos filled)
     if (SGS) {
-        Nb<R> N{a.nut + q, sy, sz};
         const R q4 = R(0.25);
         {
             R fxE = N(0, 0, 0) * (U(1, 0, 0) - U(0, 0, 0)) * idx;
@@ -382,6 +384,22 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs<R> a) {
         }
     }
 
+}
+
+// ---- direct form: one thread per cell, neighbours from global memory --------------
+template <typename R, int ADV, bool SGS, bool ANEL, bool UNI>
+__global__ void __launch_bounds__(256) sweep_kernel(SweepArgs<R> a) {
+    const Geo& g = a.g;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+    const long long q = pidx(g, i, j, k);
+    const long long sy = g.sy, sz = g.sz;
+    Nb<R> U{a.u + q, sy, sz}, V{a.v + q, sy, sz}, W{a.w + q, sy, sz}, T{a.th + q, sy, sz};
+    Nb<R> N{SGS ? a.nut + q : a.u + q, sy, sz};
+    R tu, tv, tw, tt;
+    sweep_point<R, ADV, SGS, ANEL, UNI>(a, g, k, U, V, W, T, N, tu, tv, tw, tt);
     // predictor and the theta update (with the RK3 stage combination)
     const long long qi = iidx(g, i, j, k);
     const R dt = a.dt;
@@ -393,18 +411,11 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs<R> a) {
     a.th_out[q] = tn;
 }
 
-// Smagorinsky nut = (C_s Delta_k)^2 |S| at the cell centres (src/FiniteVolume.jl:936-944,
-// strain src/Operators.jl:451-496); halos are filled by a separate launch.
-template <typename R, bool UNI>
-__global__ void __launch_bounds__(256) smagorinsky_kernel(Geo g, const R* __restrict__ u, const R* __restrict__ v,
-                                                          const R* __restrict__ w, R* __restrict__ nut, R c_s) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int j = blockIdx.y * blockDim.y + threadIdx.y;
-    int k = blockIdx.z * blockDim.z + threadIdx.z;
-    if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+// Smagorinsky nut = (C_s Delta_k)^2 |S| at a cell centre (src/FiniteVolume.jl:936-944,
+// strain src/Operators.jl:451-496), accessors around the point at level k.
+template <typename R, bool UNI, class A>
+__device__ __forceinline__ R smag_point(const Geo& g, int k, R c_s, const A& U, const A& V, const A& W) {
     Met<R, UNI> m(g);
-    const long long q = pidx(g, i, j, k);
-    Nb<R> U{u + q, g.sy, g.sz}, V{v + q, g.sy, g.sz}, W{w + q, g.sy, g.sz};
     R idx = R(g.idx), idy = R(g.idy), idz = m.idz(k), ido = m.idz_off(k);
     R cf = c_s * m.filter(k);
     R coef = cf * cf;
@@ -419,5 +430,18 @@ __global__ void __launch_bounds__(256) smagorinsky_kernel(Geo g, const R* __rest
     R dw_dy = ((W(0, 1, 0) + W(0, 1, 1)) - (W(0, -1, 0) + W(0, -1, 1))) * (R(0.25) * idy);
     R S12 = R(0.5) * (du_dy + dv_dx), S13 = R(0.5) * (du_dz + dw_dx), S23 = R(0.5) * (dv_dz + dw_dy);
     R S2 = R(2) * (du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz) + R(4) * (S12 * S12 + S13 * S13 + S23 * S23);
-    nut[q] = coef * sqrt(S2);
+    return coef * sqrt(S2);
+}
+
+// The direct form: nut into a padded array (halos filled by a separate launch).
+template <typename R, bool UNI>
+__global__ void __launch_bounds__(256) smagorinsky_kernel(Geo g, const R* __restrict__ u, const R* __restrict__ v,
+                                                          const R* __restrict__ w, R* __restrict__ nut, R c_s) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+    const long long q = pidx(g, i, j, k);
+    Nb<R> U{u + q, g.sy, g.sz}, V{v + q, g.sy, g.sz}, W{w + q, g.sy, g.sz};
+    nut[q] = smag_point<R, UNI>(g, k, c_s, U, V, W);
 }

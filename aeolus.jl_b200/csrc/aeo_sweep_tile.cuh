@@ -1,0 +1,221 @@
+// aeo_sweep_tile.cuh -- the tiled form of the fused sweep for sm_100a.
+//
+// A CTA owns a 32 x 8 column tile and marches up a chunk of levels.  The
+// xy-planes of u, v, w and theta (with an xy halo) live in a shared-memory
+// ring of slots that TMA fills: one elected thread issues a 3-D tile load
+// (cp.async.bulk.tensor, no multicast) per field and level, completing on the
+// slot's mbarrier, one level ahead of the one being computed.  The
+// Smagorinsky eddy viscosity is computed in-tile for each level into a
+// three-plane ring, so the separate nut pass and its halo fill disappear.
+// Every point then runs the same sweep_point arithmetic as the direct form
+// (aeo_sweep.cuh), reading its neighbours from shared memory.
+//
+// Waits on the mbarriers are bounded: after AEO_WAIT_LIMIT polls the CTA
+// records AEO_ERR_FLAG_TMA in the error word, drains the copies it issued
+// (again bounded) and returns; the host reports the failure after the step.
+#pragma once
+
+#include <cuda.h>
+
+#include "aeo_sweep.cuh"
+
+#define AEO_WAIT_LIMIT (1u << 22)
+#define AEO_ERR_FLAG_TMA 2
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (uint32_t it = 0; it < AEO_WAIT_LIMIT; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+template <typename R, int ADV, bool SGS>
+struct TileShape {
+    static constexpr int TX = 32, TY = 8, NT = TX * TY;
+    static constexpr int HH = ADV ? 3 : 2;               // xy halo of the planes
+    static constexpr int ZL = ADV ? 3 : (SGS ? 2 : 1);   // levels below the point
+    static constexpr int ZH = ADV ? 3 : (SGS ? 2 : 1);   // levels above
+    static constexpr int NW = ZL + ZH + 1;
+    static constexpr int LOOK = 1;                       // levels loaded ahead
+    static constexpr int NS = NW + LOOK;                 // ring slots
+    static constexpr int PW = TX + 8;                    // row: x from i0-4 (16-byte aligned TMA start)
+    static constexpr int PH = TY + 2 * HH;
+    static constexpr int PSZ = PW * PH;                  // elements of one field-plane (the TMA box)
+    static constexpr int PSZA = (int)(((PSZ * sizeof(R) + 127) / 128) * 128 / sizeof(R));
+    static constexpr int NPW = TX + 2, NPH = TY + 2, NPS = NPW * NPH;  // nut plane with halo 1
+    static constexpr size_t PLANES_BYTES = (size_t)NS * 4 * PSZA * sizeof(R);
+    static constexpr size_t NUT_BYTES = SGS ? (size_t)3 * NPS * sizeof(R) : 0;
+    static constexpr size_t SMEM = PLANES_BYTES + ((NUT_BYTES + 127) / 128) * 128 + 8 * NS + 128;
+};
+
+struct TileMaps {
+    CUtensorMap u, v, w, t;
+};
+
+// accessor of one field around the thread's point: level k+dk is ring plane p[dk+ZL]
+template <typename R, int NW, int ZL, int PW>
+struct SmAcc {
+    const R* p[NW];
+    int base;
+    __device__ __forceinline__ R operator()(int di, int dj, int dk) const { return p[dk + ZL][base + dj * PW + di]; }
+};
+
+template <typename R, int NPW>
+struct NutAcc {
+    const R* p[3];  // levels k-1, k, k+1
+    int base;
+    __device__ __forceinline__ R operator()(int di, int dj, int dk) const { return p[dk + 1][base + dj * NPW + di]; }
+};
+
+template <typename R, int ADV, bool SGS, bool ANEL, bool UNI>
+__global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__ TileMaps maps, SweepArgs<R> a,
+                                                         int kchunk, int* err) {
+    using S = TileShape<R, ADV, SGS>;
+    extern __shared__ __align__(128) unsigned char smem_tile[];
+    unsigned char* sbase = reinterpret_cast<unsigned char*>(((uintptr_t)smem_tile + 127) & ~(uintptr_t)127);
+    R* planes = reinterpret_cast<R*>(sbase);
+    R* nutp = reinterpret_cast<R*>(sbase + S::PLANES_BYTES);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + S::PLANES_BYTES + ((S::NUT_BYTES + 127) / 128) * 128);
+
+    const Geo& g = a.g;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + S::TX * ty;
+    const int i0 = blockIdx.x * S::TX, j0 = blockIdx.y * S::TY;
+    const int kbeg = blockIdx.z * kchunk;
+    const int kend = min(g.nz, kbeg + kchunk);
+    const int i = i0 + tx, j = j0 + ty;
+    const bool active = i < g.nx && j < g.ny;
+    const int Lfirst = kbeg - S::ZL;             // first level held
+    const int Llast = kend - 1 + S::ZH;          // last level needed
+    const uint32_t bytes = 4u * S::PSZ * sizeof(R);
+
+    auto slot_of = [&](int L) { return (L - Lfirst) % S::NS; };
+    auto parity_of = [&](int L) { return (uint32_t)(((L - Lfirst) / S::NS) & 1); };
+    auto plane = [&](int L, int f) { return planes + ((size_t)slot_of(L) * 4 + f) * S::PSZA; };
+    auto issue = [&](int L) {
+        uint64_t* b = bars + slot_of(L);
+        mbar_expect_tx(b, bytes);
+        const int x = i0 + AEO_HX - 4, y = j0 + AEO_H - S::HH, z = L + AEO_H;
+        tma_load_3d(plane(L, 0), &maps.u, b, x, y, z);
+        tma_load_3d(plane(L, 1), &maps.v, b, x, y, z);
+        tma_load_3d(plane(L, 2), &maps.w, b, x, y, z);
+        tma_load_3d(plane(L, 3), &maps.t, b, x, y, z);
+    };
+
+    if (tid == 0) {
+        for (int s = 0; s < S::NS; ++s) mbar_init(bars + s, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    int Lissued = min(Llast, kbeg + S::ZH + S::LOOK);
+    if (tid == 0)
+        for (int L = Lfirst; L <= Lissued; ++L) issue(L);
+
+    const int vbase = (ty + S::HH) * S::PW + (tx + 4);
+    bool failed = false;
+    for (int k = kbeg; k < kend; ++k) {
+        // the levels this iteration needs
+        const int Lw0 = (k == kbeg) ? Lfirst : k + S::ZH;
+        bool ok = true;
+        for (int L = Lw0; L <= k + S::ZH; ++L) ok = ok && mbar_wait_bounded(bars + slot_of(L), parity_of(L));
+        if (__syncthreads_or(!ok)) { failed = true; break; }
+
+        SmAcc<R, S::NW, S::ZL, S::PW> U, V, W, T;
+#pragma unroll
+        for (int d = 0; d < S::NW; ++d) {
+            const int L = k - S::ZL + d;
+            U.p[d] = plane(L, 0); V.p[d] = plane(L, 1); W.p[d] = plane(L, 2); T.p[d] = plane(L, 3);
+        }
+        U.base = V.base = W.base = T.base = vbase;
+
+        NutAcc<R, S::NPW> N;
+        if (SGS) {
+            // eddy viscosity of the levels k-1 .. k+1 (first iteration) or k+1
+            const int Lz0 = (k == kbeg) ? k - 1 : k + 1;
+            for (int L = Lz0; L <= k + 1; ++L) {
+                R* np = nutp + (size_t)(((L % 3) + 3) % 3) * S::NPS;
+                const bool mirror = g.bc_z == 1 && (L < 0 || L >= g.nz);
+                if (mirror) continue;   // filled from the interior neighbour below
+                SmAcc<R, S::NW, S::ZL, S::PW> Uq, Vq, Wq;
+#pragma unroll
+                for (int d = 0; d < S::NW; ++d) {
+                    const int Ld = L - S::ZL + d;
+                    const bool inwin = Ld >= k - S::ZL && Ld <= k + S::ZH;
+                    Uq.p[d] = inwin ? plane(Ld, 0) : planes;
+                    Vq.p[d] = inwin ? plane(Ld, 1) : planes;
+                    Wq.p[d] = inwin ? plane(Ld, 2) : planes;
+                }
+                for (int e = tid; e < S::NPS; e += S::NT) {
+                    const int ci = e % S::NPW, cj = e / S::NPW;
+                    const int b = (cj - 1 + S::HH) * S::PW + (ci - 1 + 4);
+                    Uq.base = Vq.base = Wq.base = b;
+                    np[e] = smag_point<R, UNI>(g, L, R(a.c_s), Uq, Vq, Wq);
+                }
+            }
+            __syncthreads();
+            // walls: the halo levels take the mirrored interior value
+            for (int L = Lz0; L <= k + 1; ++L) {
+                if (!(g.bc_z == 1 && (L < 0 || L >= g.nz))) continue;
+                const int Ls = L < 0 ? -L - 1 : 2 * g.nz - 1 - L;
+                R* dst = nutp + (size_t)(((L % 3) + 3) % 3) * S::NPS;
+                const R* src = nutp + (size_t)(((Ls % 3) + 3) % 3) * S::NPS;
+                for (int e = tid; e < S::NPS; e += S::NT) dst[e] = src[e];
+            }
+            __syncthreads();
+            for (int d = 0; d < 3; ++d) {
+                const int L = k - 1 + d;
+                N.p[d] = nutp + (size_t)(((L % 3) + 3) % 3) * S::NPS;
+            }
+            N.base = (ty + 1) * S::NPW + (tx + 1);
+        } else {
+            N.p[0] = N.p[1] = N.p[2] = nutp;
+            N.base = 0;
+        }
+
+        if (active) {
+            R tu, tv, tw, tt;
+            sweep_point<R, ADV, SGS, ANEL, UNI>(a, g, k, U, V, W, T, N, tu, tv, tw, tt);
+            const long long qi = iidx(g, i, j, k), q = pidx(g, i, j, k);
+            const R dt = a.dt;
+            a.us[qi] = U(0, 0, 0) + dt * tu;
+            a.vs[qi] = V(0, 0, 0) + dt * tv;
+            a.ws[qi] = (g.bc_z == 1 && k == 0) ? R(0) : W(0, 0, 0) + dt * tw;
+            R tn = T(0, 0, 0) + dt * tt;
+            if (a.stage) tn = a.ca * a.th0[q] + a.cb * tn;
+            a.th_out[q] = tn;
+        }
+        __syncthreads();  // every read of level k - ZL is done: its slot can be refilled
+        const int Lnext = k + S::ZH + S::LOOK + 1;
+        if (Lnext <= Llast) {
+            if (tid == 0) issue(Lnext);
+            Lissued = Lnext;
+        }
+    }
+    if (failed) {
+        if (tid == 0) atomicOr(err, AEO_ERR_FLAG_TMA);
+        // drain the copies this CTA issued before returning (bounded)
+        for (int L = max(Lfirst, Lissued - S::NS + 1); L <= Lissued; ++L) mbar_wait_bounded(bars + slot_of(L), parity_of(L));
+    }
+}

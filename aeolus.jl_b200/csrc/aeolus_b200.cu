@@ -30,6 +30,9 @@
 #include "aeo_fft.cuh"
 #include "aeo_misc.cuh"
 #include "aeo_sweep.cuh"
+#include "aeo_sweep_tile.cuh"
+
+#include <cudaTypedefs.h>
 
 static std::string g_create_error;
 
@@ -108,6 +111,8 @@ struct Core : CoreBase {
     double* d_part = nullptr;
     int* d_flag = nullptr;
     int rows_x = 1, tpx_y = 1, tpx_z = 1;
+    TileMaps tmaps[3];          // TMA maps of the padded state sets
+    int kchunk = 32;
     cudaGraphExec_t gexec = nullptr;
     cudaGraph_t graph = nullptr;
     double graph_dt = 0.0;
@@ -322,8 +327,10 @@ struct Core : CoreBase {
         if (aeo_status e = alloc(&d_stage, std::max<long long>(host_n, g.nin))) return e;
         if (aeo_status e = alloc(&d_part, Nz + 1)) return e;
         if (aeo_status e = alloc(&d_flag, 1)) return e;
+        if (aeo_status e = make_tensor_maps()) return e;
+        kchunk = std::min(g.nz, 32);
         CK(cudaStreamSynchronize(st));
-        launches = 3 * (8 + (sgs ? 2 : 0));
+        launches = 3 * 8;
         return AEO_OK;
     }
 
@@ -341,9 +348,39 @@ struct Core : CoreBase {
         return AEO_OK;
     }
 
+    aeo_status make_tensor_maps() {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (!fn || q != cudaDriverEntryPointSuccess) { fail("cuTensorMapEncodeTiled is unavailable"); return AEO_ERR_CUDA; }
+        auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        const int HH = cfg.advection != AEO_ADV_CENTRED ? 3 : 2;
+        cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)(g.nz + 2 * AEO_H)};
+        cuuint64_t strides[2] = {(cuuint64_t)g.sy * sizeof(R), (cuuint64_t)g.sz * sizeof(R)};
+        cuuint32_t box[3] = {32 + 8, (cuuint32_t)(8 + 2 * HH), 1};
+        cuuint32_t es[3] = {1, 1, 1};
+        CUtensorMapDataType dt = sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+        for (int s = 0; s < 3; ++s) {
+            CUtensorMap* m[4] = {&tmaps[s].u, &tmaps[s].v, &tmaps[s].w, &tmaps[s].t};
+            for (int f = 0; f < 4; ++f) {
+                CUresult r = encode(m[f], dt, 3, (void*)P[s][f], dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                if (r != CUDA_SUCCESS) { fail("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")"); return AEO_ERR_CUDA; }
+            }
+        }
+        return AEO_OK;
+    }
+
+    int cur_in = 0;   // the padded set the sweep reads (set by substage)
+
     template <int ADV, bool SG, bool AN, bool UN>
     void launch_sweep_t(const SweepArgs<R>& a) {
-        sweep_kernel<R, ADV, SG, AN, UN><<<grd3(), blk3(), 0, st>>>(a);
+        using TS = TileShape<R, ADV, SG>;
+        cudaFuncSetAttribute(sweep_tile_kernel<R, ADV, SG, AN, UN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TS::SMEM);
+        dim3 grid((g.nx + TS::TX - 1) / TS::TX, (g.ny + TS::TY - 1) / TS::TY, (g.nz + kchunk - 1) / kchunk);
+        sweep_tile_kernel<R, ADV, SG, AN, UN><<<grid, dim3(TS::TX, TS::TY), TS::SMEM, st>>>(tmaps[cur_in], a, kchunk, d_flag);
     }
 
     aeo_status launch_sweep(const SweepArgs<R>& a) {
@@ -417,15 +454,7 @@ struct Core : CoreBase {
     aeo_status substage(int s_in, int s_out, int stage, R dt, R ca, R cb) {
         R** in = P[s_in];
         R** out = P[s_out];
-        if (sgs) {
-            if (uni) smagorinsky_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, in[0], in[1], in[2], nut, R(cfg.c_s));
-            else smagorinsky_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, in[0], in[1], in[2], nut, R(cfg.c_s));
-            CKL();
-            R* f[1] = {nut};
-            int l[1] = {LOC_C};
-            if (aeo_status e = halo(f, l, 1)) return e;
-            mark(AEO_K_SGS);
-        }
+        cur_in = s_in;
         SweepArgs<R> a{};
         a.g = g;
         a.u = in[0]; a.v = in[1]; a.w = in[2]; a.th = in[3];
@@ -438,6 +467,7 @@ struct Core : CoreBase {
         a.pr_t = R(cfg.pr_t); a.inv_prt = R(1.0 / cfg.pr_t);
         a.flux_bot = R(cfg.flux_bot); a.flux_top = R(cfg.flux_top);
         a.sp_alpha = R(cfg.sponge_alpha); a.sp_zstart = R(cfg.sponge_zstart);
+        a.c_s = R(cfg.c_s);
         double ztop = cfg.z0 + cfg.lz;
         a.sp_inv = R(1.0 / (ztop - cfg.sponge_zstart));
         if (aeo_status e = launch_sweep(a)) return e;
@@ -512,6 +542,7 @@ struct Core : CoreBase {
             if (aeo_status e = substage(0, 1, 0, R(dt), R(0), R(0))) return e;
             // the Euler result becomes the state: swap sets 0 and 1
             for (int f = 0; f < 4; ++f) std::swap(P[0][f], P[1][f]);
+            std::swap(tmaps[0], tmaps[1]);
             if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
             if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
         }
@@ -520,7 +551,6 @@ struct Core : CoreBase {
     }
 
     aeo_status check_finite() {
-        CK(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
         dim3 gb((g.nx + 127) / 128, g.ny, g.nz);
         for (int f = 0; f < 4; ++f) {
             finite_check_kernel<R><<<gb, 128, 0, st>>>(g, P[0][f], d_flag);
@@ -528,7 +558,9 @@ struct Core : CoreBase {
         }
         int h = 0;
         CK(cudaMemcpyAsync(&h, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
         CK(cudaStreamSynchronize(st));
+        if (h & AEO_ERR_FLAG_TMA) { fail("a tile load did not complete within its wait limit"); return AEO_ERR_CUDA; }
         if (h) { fail("non-finite value in the state after the step"); return AEO_ERR_NUMERICAL; }
         return AEO_OK;
     }
@@ -571,6 +603,12 @@ struct Core : CoreBase {
         int padded, loc;
         R* d = field_ptr(id, &padded, &loc);
         if (!d) { fail("get_field: unknown or unavailable field"); return AEO_ERR_ARGUMENT; }
+        if (id == AEO_FIELD_NUT) {
+            // the step keeps nut in shared memory: evaluate it for the current state
+            if (uni) smagorinsky_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, P[0][0], P[0][1], P[0][2], nut, R(cfg.c_s));
+            else smagorinsky_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, P[0][0], P[0][1], P[0][2], nut, R(cfg.c_s));
+            CKL();
+        }
         pack_host_kernel<R><<<(unsigned)((host_n + 255) / 256), 256, 0, st>>>(g, d_stage, cfg.hx, cfg.hy, cfg.hz, d,
                                                                               padded, loc);
         CKL();

@@ -97,7 +97,9 @@ aeo_status aeo_set_field(aeo_sim* h, int32_t field, const double* host);
 /* Copy a field to a host Field.data array (storage layout).  u, v, w, θ come
  * back with halos filled from the interior by the boundary conditions
  * (fill_halos!, src/boundary_conditions/halo_sets.jl:176); p and νt with
- * zero halos. */
+ * zero halos.  νt (the `max_νt` diagnostic, src/Simulations.jl:1058) is the
+ * Smagorinsky viscosity of the current state: the step itself keeps νt in
+ * shared memory only. */
 aeo_status aeo_get_field(aeo_sim* h, int32_t field, double* host);
 
 /* nsteps projected SSP-RK3 steps of size dt: step_rk3! of the Boussinesq
