@@ -16,7 +16,8 @@ LIB_PATH = os.path.join(_HERE, "lib", "libaeolus_b200.so")
 SYMBOLS = (
     "aeo_create", "aeo_destroy", "aeo_set_field", "aeo_get_field", "aeo_step_rk3", "aeo_step_euler",
     "aeo_pressure_solve", "aeo_project", "aeo_kinetic_energy", "aeo_max_divergence", "aeo_step_rk3_async",
-    "aeo_synchronize", "aeo_profile_step", "aeo_launches_per_step", "aeo_stream", "aeo_fill_uniform", "aeo_pressure_solve_column_noalloc", "aeo_last_error",
+    "aeo_synchronize", "aeo_profile_step", "aeo_launches_per_step", "aeo_stream", "aeo_fill_uniform",
+    "aeo_pressure_solve_column_noalloc", "aeo_step_adaptive", "aeo_cfl_diagnostics", "aeo_init_isotropic", "aeo_last_error",
     "aeo_version",
 )
 
@@ -36,6 +37,25 @@ class AeoConfig(C.Structure):
         ("device", C.c_int32),
     ]
 
+
+class AeoCfl(C.Structure):
+    """CFLConstraints + the guard limits of step_adaptive! (src/TimeIntegration.jl:127-153, :823-835)."""
+    _fields_ = [
+        ("c_advective", C.c_double), ("c_diffusive", C.c_double), ("c_buoyancy", C.c_double),
+        ("c_coriolis", C.c_double), ("dt_min", C.c_double), ("dt_max", C.c_double), ("growth_max", C.c_double),
+        ("divergence_tol", C.c_double), ("max_velocity", C.c_double), ("max_retries", C.c_int32),
+    ]
+
+
+class AeoAdaptiveStats(C.Structure):
+    _fields_ = [
+        ("dt", C.c_double), ("t_advanced", C.c_double), ("limiter", C.c_int32), ("retries", C.c_int32),
+        ("advective_rate", C.c_double), ("nut_max", C.c_double), ("brunt_vaisala", C.c_double),
+        ("max_divergence", C.c_double), ("max_speed", C.c_double),
+    ]
+
+
+LIMITERS = ("advective", "diffusive", "buoyancy", "coriolis", "sgs", "growth", "dt_min", "dt_max", "retried")
 
 _lib = None
 
@@ -87,6 +107,9 @@ def load():
     lib.aeo_fill_uniform.argtypes = [P, C.c_int32, C.c_uint64, C.c_uint32, C.c_double, C.c_int32]
     lib.aeo_pressure_solve_column_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                                       D, D, D, D, D, D, P, P, P]
+    lib.aeo_step_adaptive.argtypes = [P, C.POINTER(AeoCfl), C.c_int32, D, C.POINTER(AeoAdaptiveStats)]
+    lib.aeo_cfl_diagnostics.argtypes = [P, C.POINTER(AeoCfl), C.c_double, C.POINTER(AeoAdaptiveStats)]
+    lib.aeo_init_isotropic.argtypes = [P, C.c_double, C.c_double, C.c_uint64, C.c_double, C.c_int32, C.c_double]
     lib.aeo_last_error.argtypes = [P]
     lib.aeo_last_error.restype = C.c_char_p
     lib.aeo_version.restype = C.c_char_p

@@ -89,6 +89,90 @@ def taylor_green(grid: Grid, seed: int = 1, amp: float = 1e-3):
     return embed(grid, u), embed(grid, v), embed(grid, w), embed(grid, th)
 
 
+_SM1 = np.uint64(0x9E3779B97F4A7C15)
+_SM2 = np.uint64(0xBF58476D1CE4E5B9)
+_SM3 = np.uint64(0x94D049BB133111EB)
+
+
+def _splitmix(x):
+    """SplitMix64 (src/operators/spectra.jl:257-262) on uint64 arrays."""
+    with np.errstate(over="ignore"):
+        x = x + _SM1
+        x = (x ^ (x >> np.uint64(30))) * _SM2
+        x = (x ^ (x >> np.uint64(27))) * _SM3
+        return x ^ (x >> np.uint64(31))
+
+
+def _mode_key(seed, m1, m2, m3):
+    """The counter hash of a mode (src/operators/spectra.jl:263-264); negative
+    m wrap as two's complement (m % UInt64)."""
+    u = lambda m: np.asarray(m, dtype=np.int64).astype(np.uint64)
+    s = _splitmix(np.uint64(seed % (1 << 64)))
+    return _splitmix(_splitmix(_splitmix(s ^ u(m1)) ^ u(m2)) ^ u(m3))
+
+
+def _unit(h):
+    return ((h >> np.uint64(11)) + np.uint64(1)).astype(np.float64) * 2.0 ** -53
+
+
+def _mode_normals(h):
+    """Three complex standard normals of mode key h by Box-Muller
+    (src/operators/spectra.jl:268-275)."""
+    out = []
+    with np.errstate(over="ignore"):
+        for j in (1, 2, 3):
+            a = _splitmix(h + np.uint64(2 * j - 1))
+            b = _splitmix(h + np.uint64(2 * j))
+            rho = np.sqrt(-2 * np.log(_unit(a)))
+            phi = 2 * np.pi * _unit(b)
+            out.append((rho * np.cos(phi) + 1j * rho * np.sin(phi)) / np.sqrt(2))
+    return out
+
+
+def passot_pouquet(k, u_rms: float = 1.0, k_peak: float = 4.0):
+    """E(k) = 16 sqrt(2/pi) u_rms^2 k^4 / k_p^5 exp(-2 (k/k_p)^2) (src/operators/spectra.jl:248-253)."""
+    return 16 * np.sqrt(2 / np.pi) * u_rms ** 2 * k ** 4 / k_peak ** 5 * np.exp(-2 * (k / k_peak) ** 2)
+
+
+def isotropic_turbulence(grid: Grid, u_rms: float = 1.0, k_peak: float = 4.0, seed: int = 1, kmax: float = np.inf):
+    """`isotropic_turbulence_field!` (src/operators/spectra.jl:312-343): the
+    random-phase solenoidal field of spectrum E(k), defined in spectral space
+    (each mode's draw depends on seed and the integer mode only), evaluated
+    at each component's staggered nodes.  Triply periodic uniform grids.
+    Returns storage arrays (u, v, w)."""
+    nx, ny, nz = grid.size
+    lx, ly, lz = grid.extent
+    mx = np.fft.fftfreq(nx, 1.0 / nx).astype(np.int64)
+    my = np.fft.fftfreq(ny, 1.0 / ny).astype(np.int64)
+    mz = np.fft.fftfreq(nz, 1.0 / nz).astype(np.int64)
+    M3, M2, M1 = np.meshgrid(mz, my, mx, indexing="ij")
+    ck = (2 * np.pi / lx, 2 * np.pi / ly, 2 * np.pi / lz)
+    dV = ck[0] * ck[1] * ck[2]
+    keep = (2 * np.abs(M1) < nx) & (2 * np.abs(M2) < ny) & (2 * np.abs(M3) < nz) & ~((M1 == 0) & (M2 == 0) & (M3 == 0))
+    k1, k2, k3 = ck[0] * M1, ck[1] * M2, ck[2] * M3
+    kk2 = k1 ** 2 + k2 ** 2 + k3 ** 2
+    kk = np.sqrt(kk2)
+    keep &= kk <= kmax
+    canon = (M3 > 0) | ((M3 == 0) & ((M2 > 0) | ((M2 == 0) & (M1 > 0))))
+    sgn = np.where(canon, 1, -1)
+    r = _mode_normals(_mode_key(seed, sgn * M1, sgn * M2, sgn * M3))
+    kc = (sgn * k1, sgn * k2, sgn * k3)
+    safe = np.where(keep, kk2, 1.0)
+    kr = (kc[0] * r[0] + kc[1] * r[1] + kc[2] * r[2]) / safe
+    amp = np.sqrt(np.maximum(passot_pouquet(kk, u_rms, k_peak), 0.0) * dV / (4 * np.pi * safe))
+    x0, y0, z0 = grid.origin
+    firsts = ((x0, y0 + 0.5 * grid.dy, z0 + 0.5 * grid.dz), (x0 + 0.5 * grid.dx, y0, z0 + 0.5 * grid.dz),
+              (x0 + 0.5 * grid.dx, y0 + 0.5 * grid.dy, z0))
+    out = []
+    for j in range(3):
+        pj = r[j] - kc[j] * kr
+        uh = amp * np.where(canon, pj, np.conj(pj))
+        x1 = firsts[j]
+        A = np.where(keep, uh * np.exp(1j * (k1 * x1[0] + k2 * x1[1] + k3 * x1[2])), 0.0) * (nx * ny * nz)
+        out.append(embed(grid, np.real(np.fft.ifftn(A))))
+    return tuple(out)
+
+
 def cbl_theta_profile(z: np.ndarray, theta_ml: float = 300.0, z_inv: float = 1000.0, jump: float = 3.0,
                       lapse: float = 3e-3) -> np.ndarray:
     """Dry convective boundary layer: theta_ml up to z_inv, then a jump and a

@@ -33,6 +33,32 @@ def _ptr(a: Optional[np.ndarray]):
     return a.ctypes.data_as(_D)
 
 
+class CFLConstraints:
+    """`CFLConstraints` (src/TimeIntegration.jl:127-153) with the guard limits
+    of `step_adaptive!` (divergence_tol, max_velocity, max_retries)."""
+
+    def __init__(self, C_advective=0.5, C_diffusive=0.25, C_buoyancy=0.5, C_coriolis=0.5, dt_min=1e-8,
+                 dt_max=float("inf"), growth_max=1.1, divergence_tol=1e-6, max_velocity=float("inf"), max_retries=3):
+        if not (C_advective > 0 and C_diffusive > 0 and C_buoyancy > 0 and C_coriolis > 0):
+            raise ValueError("CFL numbers must be > 0")
+        if not (0 < dt_min <= dt_max):
+            raise ValueError("need 0 < dt_min <= dt_max")
+        if not growth_max >= 1:
+            raise ValueError("growth_max must be >= 1")
+        self.__dict__.update(locals())
+        del self.__dict__["self"]
+
+    def to_c(self):
+        return _lib.AeoCfl(self.C_advective, self.C_diffusive, self.C_buoyancy, self.C_coriolis, self.dt_min,
+                           self.dt_max, self.growth_max, self.divergence_tol, self.max_velocity, self.max_retries)
+
+
+def _stats(st) -> dict:
+    return {"dt": st.dt, "t_advanced": st.t_advanced, "limiter": _lib.LIMITERS[st.limiter], "retries": st.retries,
+            "advective_rate": st.advective_rate, "nut_max": st.nut_max, "N": st.brunt_vaisala,
+            "max_divergence": st.max_divergence, "max_speed": st.max_speed}
+
+
 class Simulation:
     def __init__(self, spec: CoreSpec, device: int = 0):
         self.spec = spec
@@ -126,6 +152,32 @@ class Simulation:
     def project(self):
         """One Chorin projection of the current velocity (dt = 1)."""
         _lib.check(self._lib.aeo_project(self._h), self._h)
+
+    def init_isotropic(self, u_rms: float = 1.0, k_peak: float = 4.0, seed: int = 1, kmax: float = 0.0,
+                       project: bool = True, target_rms: float = 0.0):
+        """`isotropic_turbulence_field!` with the Passot-Pouquet spectrum
+        (src/operators/spectra.jl:248-343) generated on the device; then an
+        optional projection and rescaling to a per-component rms."""
+        _lib.check(self._lib.aeo_init_isotropic(self._h, float(u_rms), float(k_peak), int(seed), float(kmax),
+                                                1 if project else 0, float(target_rms)), self._h)
+
+    def step_adaptive(self, constraints: "CFLConstraints" = None, nsteps: int = 1, dt_prev=None) -> dict:
+        """`step_adaptive!` (src/TimeIntegration.jl:808-938) nsteps times: the
+        CFL pick, the RK3 step and the guard run on the device; a failed guard
+        retries the step from its unchanged start with half the dt.  Returns
+        the stats of the last step (dt, limiter, ...) and the time advanced."""
+        c = (constraints or CFLConstraints()).to_c()
+        d = C.c_double(float(dt_prev) if dt_prev else 0.0)
+        st = _lib.AeoAdaptiveStats()
+        _lib.check(self._lib.aeo_step_adaptive(self._h, C.byref(c), int(nsteps), C.byref(d), C.byref(st)), self._h)
+        return _stats(st)
+
+    def cfl_diagnostics(self, constraints: "CFLConstraints" = None, dt_prev=None) -> dict:
+        """`cfl_diagnostics` + `adaptive_dt` of the current state."""
+        c = (constraints or CFLConstraints()).to_c()
+        st = _lib.AeoAdaptiveStats()
+        _lib.check(self._lib.aeo_cfl_diagnostics(self._h, C.byref(c), float(dt_prev or 0.0), C.byref(st)), self._h)
+        return _stats(st)
 
     # ---- solver seam and diagnostics ------------------------------------------
     def pressure_solve(self, src: np.ndarray) -> np.ndarray:

@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(256) correct_kernel(Geo g, const R* __restrict
                                                       const R* __restrict__ ws, const R* __restrict__ phi,
                                                       const R* u0, const R* v0,
                                                       const R* w0, R* uo, R* vo,
-                                                      R* wo, R* __restrict__ p, R inv_dt, R ca, R cb,
+                                                      R* wo, R* __restrict__ p, const double* __restrict__ dtp, R ca, R cb,
                                                       int stage) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(256) correct_kernel(Geo g, const R* __restrict
     uo[qp] = un;
     vo[qp] = vn;
     wo[qp] = wn;
-    p[qi] = pc * inv_dt;
+    p[qi] = pc / R(__ldg(dtp));  // p = phi/dt (_DivBy, src/Simulations.jl:1207-1211)
 }
 
 // ---- host-layout packing ----------------------------------------------------------
@@ -252,4 +252,10 @@ __global__ void philox_fill_kernel(Geo g, R* __restrict__ dst, int padded, uint6
     int i = (int)(t % g.nx), j = (int)((t / g.nx) % g.ny), k = (int)(t / ((long long)g.nx * g.ny));
     long long q = padded ? pidx(g, i, j, k) : t;
     dst[q] = add ? R((double)dst[q] + val) : R(val);
+}
+
+template <typename R>
+__global__ void padded_to_interior_kernel(Geo g, const R* __restrict__ a, R* __restrict__ b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i < g.nx) b[iidx(g, i, j, k)] = a[pidx(g, i, j, k)];
 }

@@ -35,7 +35,8 @@ struct SweepArgs {
     R* vs;
     R* ws;
     R* th_out;      // padded
-    R dt, ca, cb;
+    const double* dtp;  // the step's dt in device memory
+    R ca, cb;
     int stage;
     R nu, gacc, theta0, fcor, inv_prt, pr_t, flux_bot, flux_top, sp_alpha, sp_zstart, sp_inv;
     R c_s;
@@ -402,7 +403,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs<R> a) {
     sweep_point<R, ADV, SGS, ANEL, UNI>(a, g, k, U, V, W, T, N, tu, tv, tw, tt);
     // predictor and the theta update (with the RK3 stage combination)
     const long long qi = iidx(g, i, j, k);
-    const R dt = a.dt;
+    const R dt = R(__ldg(a.dtp));
     a.us[qi] = U(0, 0, 0) + dt * tu;
     a.vs[qi] = V(0, 0, 0) + dt * tv;
     a.ws[qi] = (g.bc_z == 1 && k == 0) ? R(0) : W(0, 0, 0) + dt * tw;

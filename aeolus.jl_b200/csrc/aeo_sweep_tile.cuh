@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
             R tu, tv, tw, tt;
             sweep_point<R, ADV, SGS, ANEL, UNI>(a, g, k, U, V, W, T, N, tu, tv, tw, tt);
             const long long qi = iidx(g, i, j, k), q = pidx(g, i, j, k);
-            const R dt = a.dt;
+            const R dt = R(__ldg(a.dtp));
             a.us[qi] = U(0, 0, 0) + dt * tu;
             a.vs[qi] = V(0, 0, 0) + dt * tv;
             a.ws[qi] = (g.bc_z == 1 && k == 0) ? R(0) : W(0, 0, 0) + dt * tw;

@@ -2,19 +2,24 @@
 // the per-domain orchestration of the projected SSP-RK3 step on one B200.
 //
 // One substage (src/Simulations.jl:531-650; src/Anelastic.jl:1791-1876):
-//   [SGS] smagorinsky -> nut, halo(nut)
-//   sweep           tendencies + predictor u* (interior) + theta (padded)
+//   sweep           tendencies (in-tile Smagorinsky) + predictor u* + theta
 //   div_fftx        divergence of u* fused with the r2c transform along x
 //   ffty            forward transform along y
 //   fftz_solve      periodic z: forward, 1/lambda, inverse   | thomas: walls in z
 //   ffty            inverse along y
 //   ifftx           c2r along x -> phi
-//   correct         u = c(u* - grad phi, u0), p = phi/dt
+//   correct         u = c(u* - grad phi, u^n), p = phi/dt
 //   halo            halos of u, v, w, theta for the next substage
-// The three substages of a step are captured once into a CUDA graph and
-// replayed.  State lives in three padded sets: the step starts and ends in
-// set 0 (u^n), stage 1 writes set 1, stage 2 set 2, stage 3 set 0 again.
+//
+// State lives in four padded sets.  A step reads set `cur` (u^n), writes the
+// stages into sets 2 and 3 and the result into set cur^1, so u^n stays
+// untouched until the step is accepted: the snapshot/retry of the adaptive
+// step costs nothing.  dt lives in device memory (StepScalars), written by the
+// host for fixed steps or by the on-device CFL pick for adaptive ones, so
+// each step is one CUDA graph (one per parity of `cur`, with or without the
+// pick) that is captured once and replayed.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -26,13 +31,13 @@
 #include <vector>
 
 #include "../../include/aeolus_b200.h"
+#include "aeo_adapt.cuh"
 #include "aeo_common.cuh"
 #include "aeo_fft.cuh"
+#include "aeo_init.cuh"
 #include "aeo_misc.cuh"
 #include "aeo_sweep.cuh"
 #include "aeo_sweep_tile.cuh"
-
-#include <cudaTypedefs.h>
 
 static std::string g_create_error;
 
@@ -77,12 +82,16 @@ struct CoreBase {
     virtual aeo_status get_field(int id, double* host) = 0;
     virtual aeo_status step_rk3(double dt, int n, bool sync) = 0;
     virtual aeo_status step_euler(double dt, int n) = 0;
+    virtual aeo_status step_adaptive(const aeo_cfl* c, int n, double* dt_prev, aeo_adaptive_stats* stats) = 0;
+    virtual aeo_status cfl(const aeo_cfl* c, double dt_prev, aeo_adaptive_stats* stats) = 0;
     virtual aeo_status pressure_solve(const double* src, double* phi) = 0;
     virtual aeo_status kinetic_energy(double* out) = 0;
     virtual aeo_status max_divergence(double* out) = 0;
     virtual aeo_status fill_uniform(int id, uint64_t seed, uint32_t stream, double amp, int mode) = 0;
     virtual aeo_status project() = 0;
     virtual aeo_status profile_step(double dt, double* ms, int ncls) = 0;
+    virtual aeo_status init_isotropic(double u_rms, double k_peak, uint64_t seed, double kmax, int proj,
+                                      double target_rms) = 0;
 };
 
 struct aeo_sim {
@@ -91,15 +100,16 @@ struct aeo_sim {
 
 template <typename R>
 struct Core : CoreBase {
-    // device buffers
     std::vector<void*> allocs;
     double* levels = nullptr;  // metric vectors
     double *kx2 = nullptr, *ky2 = nullptr, *kz2 = nullptr;
     double* colc = nullptr;    // column coefficients
     ColumnCoef cc{};
-    R* P[3][4] = {};           // padded state sets (u, v, w, theta)
+    R* P[4][4] = {};           // padded state sets (u, v, w, theta)
+    TileMaps tmaps[4];         // TMA maps of the padded sets
+    int cur = 0;               // the set holding the state (0 or 1)
     R* Q[3] = {};              // predictor (interior)
-    R* nut = nullptr;          // padded
+    R* nut = nullptr;          // padded, diagnostics only
     R* phi = nullptr;          // interior
     R* pres = nullptr;         // interior
     cplx<R>* S = nullptr;      // spectrum
@@ -108,14 +118,15 @@ struct Core : CoreBase {
     int NT = 0;
     double* d_stage = nullptr; // host-layout staging (device)
     long long host_n = 0;
-    double* d_part = nullptr;
+    double* d_part = nullptr;  // per-level partials (4 per level)
     int* d_flag = nullptr;
+    StepScalars* d_sc = nullptr;
     int rows_x = 1, tpx_y = 1, tpx_z = 1;
-    TileMaps tmaps[3];          // TMA maps of the padded state sets
     int kchunk = 32;
-    cudaGraphExec_t gexec = nullptr;
-    cudaGraph_t graph = nullptr;
-    double graph_dt = 0.0;
+    double dz_min = 0.0;
+    cudaGraphExec_t gexec[2][2] = {};   // [with CFL pick][parity of cur]
+    CflParams cflp{};
+    bool cflp_set = false;
     bool uni = true, sgs = false, anel = false;
     // per-kernel-class timing of one un-graphed step (aeo_profile_step)
     bool profiling = false;
@@ -129,10 +140,15 @@ struct Core : CoreBase {
     }
 
     ~Core() override {
-        if (gexec) cudaGraphExecDestroy(gexec);
-        if (graph) cudaGraphDestroy(graph);
+        drop_graphs();
         for (void* p : allocs) cudaFree(p);
         if (st) cudaStreamDestroy(st);
+    }
+
+    void drop_graphs() {
+        for (auto& a : gexec)
+            for (auto& e : a)
+                if (e) { cudaGraphExecDestroy(e); e = nullptr; }
     }
 
     template <typename T>
@@ -187,13 +203,14 @@ struct Core : CoreBase {
             for (int k = 1; k < NZ; ++k) dzf[k] = zc[k] - zc[k - 1];
             dzf[NZ] = dzc[NZ - 1];
         }
+        dz_min = dzc[Hz];
+        for (int k = Hz; k < Hz + Nz; ++k) dz_min = std::min(dz_min, dzc[k]);
         // device vectors indexed by interior level k at (k + AEO_LH); storage level K = k + Hz
         const int L = Nz + 2 * AEO_LH + 2;
         const int NV = 13;
         std::vector<double> hv((size_t)NV * L, 0.0);
         auto put = [&](int vec, int K, double val) {
-            int k = K - Hz;
-            int e = k + AEO_LH;
+            int e = K - Hz + AEO_LH;
             if (e >= 0 && e < L) hv[(size_t)vec * L + e] = val;
         };
         for (int K = 0; K < NZ; ++K) {
@@ -308,7 +325,7 @@ struct Core : CoreBase {
 
         // ---- fields
         const long long np = padded_count();
-        for (int s = 0; s < 3; ++s)
+        for (int s = 0; s < 4; ++s)
             for (int f = 0; f < 4; ++f)
                 if (aeo_status e = alloc(&P[s][f], np)) return e;
         for (int f = 0; f < 3; ++f)
@@ -325,12 +342,39 @@ struct Core : CoreBase {
         }
         host_n = (long long)(c.nx + 2 * c.hx) * (c.ny + 2 * c.hy) * (c.nz + 2 * c.hz);
         if (aeo_status e = alloc(&d_stage, std::max<long long>(host_n, g.nin))) return e;
-        if (aeo_status e = alloc(&d_part, Nz + 1)) return e;
+        if (aeo_status e = alloc(&d_part, 4 * (size_t)(Nz + 1))) return e;
         if (aeo_status e = alloc(&d_flag, 1)) return e;
+        if (aeo_status e = alloc(&d_sc, 1)) return e;
+        set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->one, 1.0);
+        CKL();
         if (aeo_status e = make_tensor_maps()) return e;
         kchunk = std::min(g.nz, 32);
         CK(cudaStreamSynchronize(st));
         launches = 3 * 8;
+        return AEO_OK;
+    }
+
+    aeo_status make_tensor_maps() {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (!fn || q != cudaDriverEntryPointSuccess) { fail("cuTensorMapEncodeTiled is unavailable"); return AEO_ERR_CUDA; }
+        auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        const int HH = cfg.advection != AEO_ADV_CENTRED ? 3 : 2;
+        cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)(g.nz + 2 * AEO_H)};
+        cuuint64_t strides[2] = {(cuuint64_t)g.sy * sizeof(R), (cuuint64_t)g.sz * sizeof(R)};
+        cuuint32_t box[3] = {32 + 8, (cuuint32_t)(8 + 2 * HH), 1};
+        cuuint32_t es[3] = {1, 1, 1};
+        CUtensorMapDataType dt = sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+        for (int s = 0; s < 4; ++s) {
+            CUtensorMap* m[4] = {&tmaps[s].u, &tmaps[s].v, &tmaps[s].w, &tmaps[s].t};
+            for (int f = 0; f < 4; ++f) {
+                CUresult r = encode(m[f], dt, 3, (void*)P[s][f], dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                if (r != CUDA_SUCCESS) { fail("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")"); return AEO_ERR_CUDA; }
+            }
+        }
         return AEO_OK;
     }
 
@@ -348,54 +392,28 @@ struct Core : CoreBase {
         return AEO_OK;
     }
 
-    aeo_status make_tensor_maps() {
-        void* fn = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
-        if (!fn || q != cudaDriverEntryPointSuccess) { fail("cuTensorMapEncodeTiled is unavailable"); return AEO_ERR_CUDA; }
-        auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-        const int HH = cfg.advection != AEO_ADV_CENTRED ? 3 : 2;
-        cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)(g.nz + 2 * AEO_H)};
-        cuuint64_t strides[2] = {(cuuint64_t)g.sy * sizeof(R), (cuuint64_t)g.sz * sizeof(R)};
-        cuuint32_t box[3] = {32 + 8, (cuuint32_t)(8 + 2 * HH), 1};
-        cuuint32_t es[3] = {1, 1, 1};
-        CUtensorMapDataType dt = sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-        for (int s = 0; s < 3; ++s) {
-            CUtensorMap* m[4] = {&tmaps[s].u, &tmaps[s].v, &tmaps[s].w, &tmaps[s].t};
-            for (int f = 0; f < 4; ++f) {
-                CUresult r = encode(m[f], dt, 3, (void*)P[s][f], dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-                if (r != CUDA_SUCCESS) { fail("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")"); return AEO_ERR_CUDA; }
-            }
-        }
-        return AEO_OK;
-    }
-
-    int cur_in = 0;   // the padded set the sweep reads (set by substage)
-
     template <int ADV, bool SG, bool AN, bool UN>
-    void launch_sweep_t(const SweepArgs<R>& a) {
+    void launch_sweep_t(int s_in, const SweepArgs<R>& a) {
         using TS = TileShape<R, ADV, SG>;
         cudaFuncSetAttribute(sweep_tile_kernel<R, ADV, SG, AN, UN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)TS::SMEM);
         dim3 grid((g.nx + TS::TX - 1) / TS::TX, (g.ny + TS::TY - 1) / TS::TY, (g.nz + kchunk - 1) / kchunk);
-        sweep_tile_kernel<R, ADV, SG, AN, UN><<<grid, dim3(TS::TX, TS::TY), TS::SMEM, st>>>(tmaps[cur_in], a, kchunk, d_flag);
+        sweep_tile_kernel<R, ADV, SG, AN, UN><<<grid, dim3(TS::TX, TS::TY), TS::SMEM, st>>>(tmaps[s_in], a, kchunk, d_flag);
     }
 
-    aeo_status launch_sweep(const SweepArgs<R>& a) {
+    aeo_status launch_sweep(int s_in, const SweepArgs<R>& a) {
         const int adv = cfg.advection;
         if (anel) {
-            if (uni) { if (sgs) launch_sweep_t<0, true, true, true>(a); else launch_sweep_t<0, false, true, true>(a); }
-            else { if (sgs) launch_sweep_t<0, true, true, false>(a); else launch_sweep_t<0, false, true, false>(a); }
+            if (uni) { if (sgs) launch_sweep_t<0, true, true, true>(s_in, a); else launch_sweep_t<0, false, true, true>(s_in, a); }
+            else { if (sgs) launch_sweep_t<0, true, true, false>(s_in, a); else launch_sweep_t<0, false, true, false>(s_in, a); }
         } else if (!uni) {
-            if (sgs) launch_sweep_t<0, true, false, false>(a); else launch_sweep_t<0, false, false, false>(a);
+            if (sgs) launch_sweep_t<0, true, false, false>(s_in, a); else launch_sweep_t<0, false, false, false>(s_in, a);
         } else if (adv == AEO_ADV_CENTRED) {
-            if (sgs) launch_sweep_t<0, true, false, true>(a); else launch_sweep_t<0, false, false, true>(a);
+            if (sgs) launch_sweep_t<0, true, false, true>(s_in, a); else launch_sweep_t<0, false, false, true>(s_in, a);
         } else if (adv == AEO_ADV_WENO_JS5) {
-            if (sgs) launch_sweep_t<1, true, false, true>(a); else launch_sweep_t<1, false, false, true>(a);
+            if (sgs) launch_sweep_t<1, true, false, true>(s_in, a); else launch_sweep_t<1, false, false, true>(s_in, a);
         } else {
-            if (sgs) launch_sweep_t<2, true, false, true>(a); else launch_sweep_t<2, false, false, true>(a);
+            if (sgs) launch_sweep_t<2, true, false, true>(s_in, a); else launch_sweep_t<2, false, false, true>(s_in, a);
         }
         CKL();
         return AEO_OK;
@@ -407,7 +425,7 @@ struct Core : CoreBase {
         size_t smx = (size_t)rows_x * M * sizeof(cplx<R>);
         unsigned gx = (unsigned)((g.ny * (long long)g.nz + rows_x - 1) / rows_x);
         if (src) {
-            if (aeo_status e = src_fftx(src)) return e;
+            src_fftx_kernel<R><<<gx, 256, smx, st>>>(g, src, S, tw, NT, rows_x);
         } else if (anel) {
             if (uni) div_fftx_kernel<R, true, true><<<gx, 256, smx, st>>>(g, Q[0], Q[1], Q[2], S, tw, NT, rows_x);
             else div_fftx_kernel<R, true, false><<<gx, 256, smx, st>>>(g, Q[0], Q[1], Q[2], S, tw, NT, rows_x);
@@ -431,6 +449,8 @@ struct Core : CoreBase {
         } else {
             dim3 gt((Mh + 31) / 32, g.ny);
             size_t smt = (size_t)g.nz * 32 * sizeof(double);
+            if (smt > 48 * 1024)
+                cudaFuncSetAttribute(thomas_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
             thomas_kernel<R><<<gt, 32, smt, st>>>(g, S, dsc, cc);
         }
         CKL();
@@ -445,24 +465,31 @@ struct Core : CoreBase {
         return AEO_OK;
     }
 
-    // r2c of a given interior source (the standalone solve): the divergence
-    // kernel with the source in place of the velocities is the x transform of
-    // a source whose "divergence" is itself -- use a small packing kernel.
-    aeo_status src_fftx(const R* src);
-    aeo_status project() override;
+    aeo_status correct(R** out, int stage, R ca, R cb, const double* dtp, int s_u0) {
+        R** u0 = P[s_u0];
+        if (uni)
+            correct_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, Q[0], Q[1], Q[2], phi, u0[0], u0[1], u0[2], out[0],
+                                                               out[1], out[2], pres, dtp, ca, cb, stage);
+        else
+            correct_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, Q[0], Q[1], Q[2], phi, u0[0], u0[1], u0[2], out[0],
+                                                                out[1], out[2], pres, dtp, ca, cb, stage);
+        CKL();
+        return AEO_OK;
+    }
 
-    aeo_status substage(int s_in, int s_out, int stage, R dt, R ca, R cb) {
-        R** in = P[s_in];
+    // One projected substage: set s_in -> set s_out; stage c(x, s) = ca*s + cb*x
+    // with the step-start set s_u0 (stages 2, 3).
+    aeo_status substage(int s_in, int s_out, int s_u0, int stage, R ca, R cb) {
         R** out = P[s_out];
-        cur_in = s_in;
         SweepArgs<R> a{};
         a.g = g;
-        a.u = in[0]; a.v = in[1]; a.w = in[2]; a.th = in[3];
-        a.nut = nut;
-        a.th0 = P[0][3];
+        a.u = P[s_in][0]; a.v = P[s_in][1]; a.w = P[s_in][2]; a.th = P[s_in][3];
+        a.nut = nullptr;
+        a.th0 = P[s_u0][3];
         a.us = Q[0]; a.vs = Q[1]; a.ws = Q[2];
         a.th_out = out[3];
-        a.dt = dt; a.ca = ca; a.cb = cb; a.stage = stage;
+        a.dtp = &d_sc->dt;
+        a.ca = ca; a.cb = cb; a.stage = stage;
         a.nu = R(cfg.nu); a.gacc = R(cfg.g); a.theta0 = R(cfg.theta0); a.fcor = R(cfg.f_coriolis);
         a.pr_t = R(cfg.pr_t); a.inv_prt = R(1.0 / cfg.pr_t);
         a.flux_bot = R(cfg.flux_bot); a.flux_top = R(cfg.flux_top);
@@ -470,16 +497,10 @@ struct Core : CoreBase {
         a.c_s = R(cfg.c_s);
         double ztop = cfg.z0 + cfg.lz;
         a.sp_inv = R(1.0 / (ztop - cfg.sponge_zstart));
-        if (aeo_status e = launch_sweep(a)) return e;
+        if (aeo_status e = launch_sweep(s_in, a)) return e;
         mark(AEO_K_SWEEP);
         if (aeo_status e = solve(nullptr)) return e;
-        if (uni)
-            correct_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, Q[0], Q[1], Q[2], phi, P[0][0], P[0][1], P[0][2],
-                                                               out[0], out[1], out[2], pres, R(1.0 / (double)dt), ca, cb, stage);
-        else
-            correct_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, Q[0], Q[1], Q[2], phi, P[0][0], P[0][1], P[0][2],
-                                                                out[0], out[1], out[2], pres, R(1.0 / (double)dt), ca, cb, stage);
-        CKL();
+        if (aeo_status e = correct(out, stage, ca, cb, &d_sc->dt, s_u0)) return e;
         mark(AEO_K_CORRECT);
         R* f[4] = {out[0], out[1], out[2], out[3]};
         int l[4] = {LOC_FX, LOC_FY, LOC_FZ, LOC_C};
@@ -488,28 +509,57 @@ struct Core : CoreBase {
         return hs;
     }
 
-    aeo_status enqueue_rk3(double dt) {
-        const R inv3 = R(1) / R(3), two3 = R(2) * inv3;
-        if (aeo_status e = substage(0, 1, 0, R(dt), R(0), R(0))) return e;
-        if (aeo_status e = substage(1, 2, 1, R(dt), R(0.75), R(0.25))) return e;
-        return substage(2, 0, 1, R(dt), inv3, two3);
+    aeo_status enqueue_pick(int s_state) {
+        R** in = P[s_state];
+        if (uni) {
+            if (sgs) cfl_levels_kernel<R, true, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), d_part);
+            else cfl_levels_kernel<R, true, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), d_part);
+        } else {
+            if (sgs) cfl_levels_kernel<R, false, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), d_part);
+            else cfl_levels_kernel<R, false, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), d_part);
+        }
+        CKL();
+        dt_pick_kernel<<<1, 32, 0, st>>>(g, cflp, d_part, d_sc);
+        CKL();
+        return AEO_OK;
     }
 
-    aeo_status step_rk3(double dt, int n, bool sync) override {
-        if (!gexec || graph_dt != dt) {
-            if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
-            if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+    // One RK3 step from set c to set c^1 (src/Simulations.jl:854-904).
+    aeo_status enqueue_rk3(int c, bool pick) {
+        if (pick)
+            if (aeo_status e = enqueue_pick(c)) return e;
+        const R inv3 = R(1) / R(3), two3 = R(2) * inv3;
+        if (aeo_status e = substage(c, 2, c, 0, R(0), R(0))) return e;
+        if (aeo_status e = substage(2, 3, c, 1, R(0.75), R(0.25))) return e;
+        return substage(3, c ^ 1, c, 1, inv3, two3);
+    }
+
+    aeo_status graph_for(bool pick, cudaGraphExec_t* out) {
+        cudaGraphExec_t& ge = gexec[pick ? 1 : 0][cur];
+        if (!ge) {
             CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            aeo_status e = enqueue_rk3(dt);
+            aeo_status e = enqueue_rk3(cur, pick);
             cudaGraph_t gr = nullptr;
             cudaError_t ce = cudaStreamEndCapture(st, &gr);
             if (e) { if (gr) cudaGraphDestroy(gr); return e; }
             if (ce != cudaSuccess) { fail(std::string("graph capture: ") + cudaGetErrorString(ce)); return AEO_ERR_CUDA; }
-            graph = gr;
-            CK(cudaGraphInstantiate(&gexec, graph, 0));
-            graph_dt = dt;
+            cudaError_t ie = cudaGraphInstantiate(&ge, gr, 0);
+            cudaGraphDestroy(gr);
+            if (ie != cudaSuccess) { ge = nullptr; fail(std::string("graph instantiate: ") + cudaGetErrorString(ie)); return AEO_ERR_CUDA; }
         }
-        for (int s = 0; s < n; ++s) CK(cudaGraphLaunch(gexec, st));
+        *out = ge;
+        return AEO_OK;
+    }
+
+    aeo_status step_rk3(double dt, int n, bool sync) override {
+        set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt, dt);
+        CKL();
+        for (int s = 0; s < n; ++s) {
+            cudaGraphExec_t ge;
+            if (aeo_status e = graph_for(false, &ge)) return e;
+            CK(cudaGraphLaunch(ge, st));
+            cur ^= 1;
+        }
         if (sync) {
             CK(cudaStreamSynchronize(st));
             return check_finite();
@@ -517,14 +567,157 @@ struct Core : CoreBase {
         return AEO_OK;
     }
 
+    aeo_status step_euler(double dt, int n) override {
+        set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt, dt);
+        CKL();
+        for (int s = 0; s < n; ++s) {
+            if (aeo_status e = substage(cur, cur ^ 1, cur, 0, R(0), R(0))) return e;
+            cur ^= 1;
+        }
+        CK(cudaStreamSynchronize(st));
+        return check_finite();
+    }
+
+    void set_cfl(const aeo_cfl* c) {
+        CflParams p{};
+        p.c_adv = c->c_advective; p.c_diff = c->c_diffusive; p.c_buoy = c->c_buoyancy; p.c_cor = c->c_coriolis;
+        p.dt_min = c->dt_min; p.dt_max = c->dt_max; p.growth = c->growth_max;
+        p.nu = cfg.nu; p.pr_t = cfg.pr_t; p.fcor = cfg.f_coriolis; p.gacc = cfg.g; p.theta0 = cfg.theta0;
+        p.dz_min = dz_min; p.sgs = sgs; p.anel = anel;
+        p.buoy = anel ? (cfg.g != 0.0) : (cfg.theta0 != 0.0);
+        if (!cflp_set || std::memcmp(&p, &cflp, sizeof(p)) != 0) {
+            cflp = p;
+            cflp_set = true;
+            for (auto& e : gexec[1])
+                if (e) { cudaGraphExecDestroy(e); e = nullptr; }
+        }
+    }
+
+    aeo_status read_scalars(StepScalars* h) {
+        CK(cudaMemcpyAsync(h, d_sc, sizeof(StepScalars), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return AEO_OK;
+    }
+
+    // the post-step guard of set s: (finite, max |div|, max speed)
+    aeo_status guard(int s, bool* finite, double* div, double* speed) {
+        R** in = P[s];
+        if (anel) {
+            if (uni) guard_levels_kernel<R, true, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], pres, d_part);
+            else guard_levels_kernel<R, true, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], pres, d_part);
+        } else {
+            if (uni) guard_levels_kernel<R, false, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], pres, d_part);
+            else guard_levels_kernel<R, false, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], pres, d_part);
+        }
+        CKL();
+        std::vector<double> h(3 * (size_t)g.nz);
+        CK(cudaMemcpyAsync(h.data(), d_part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        bool fin = true;
+        double dm = 0, sm = 0;
+        for (int k = 0; k < g.nz; ++k) {
+            fin = fin && h[3 * k] == 0.0;
+            dm = std::max(dm, h[3 * k + 1]);
+            sm = std::max(sm, h[3 * k + 2]);
+        }
+        *finite = fin;
+        *div = dm;
+        *speed = sm;
+        return AEO_OK;
+    }
+
+    aeo_status cfl(const aeo_cfl* c, double dt_prev, aeo_adaptive_stats* out) override {
+        set_cfl(c);
+        set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt_prev, dt_prev > 0 ? dt_prev : 0.0);
+        CKL();
+        if (aeo_status e = enqueue_pick(cur)) return e;
+        StepScalars h;
+        if (aeo_status e = read_scalars(&h)) return e;
+        std::memset(out, 0, sizeof(*out));
+        out->dt = h.dt;
+        out->limiter = h.limiter;
+        out->advective_rate = h.rate;
+        out->nut_max = h.nut_max;
+        out->brunt_vaisala = h.N;
+        return AEO_OK;
+    }
+
+    // step_adaptive! (src/TimeIntegration.jl:808-938): CFL pick on the
+    // device, the step, the guard; on a failed guard the state (set cur,
+    // untouched) is kept and the step retried with half the dt.
+    aeo_status step_adaptive(const aeo_cfl* c, int n, double* dt_prev_io, aeo_adaptive_stats* stats) override {
+        set_cfl(c);
+        double dt_prev = (dt_prev_io && *dt_prev_io > 0) ? *dt_prev_io : 0.0;
+        set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt_prev, dt_prev);
+        CKL();
+        aeo_adaptive_stats acc{};
+        for (int s = 0; s < n; ++s) {
+            cudaGraphExec_t ge;
+            if (aeo_status e = graph_for(true, &ge)) return e;
+            CK(cudaGraphLaunch(ge, st));
+            StepScalars h;
+            if (aeo_status e = read_scalars(&h)) return e;
+            double dt = h.dt;
+            int retries = 0;
+            while (true) {
+                bool fin;
+                double dv, sp;
+                if (aeo_status e = guard(cur ^ 1, &fin, &dv, &sp)) return e;
+                bool ok = fin && std::isfinite(dv) && dv <= c->divergence_tol && sp <= c->max_velocity;
+                int flag = 0;
+                CK(cudaMemcpyAsync(&flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                if (flag & AEO_ERR_FLAG_TMA) { fail("a tile load did not complete within its wait limit"); return AEO_ERR_CUDA; }
+                if (ok) {
+                    acc.max_divergence = dv;
+                    acc.max_speed = sp;
+                    break;
+                }
+                if (retries >= c->max_retries) {
+                    fail(std::string("step_adaptive: step failed (") + (!fin ? "nonfinite" : (dv > c->divergence_tol ? "divergence" : "velocity")) +
+                         ") after " + std::to_string(retries) + " retries; the state is the one before the step");
+                    return AEO_ERR_NUMERICAL;
+                }
+                double dt_new = std::max(dt / 2, c->dt_min);
+                if (dt_new == dt) {
+                    fail("step_adaptive: step failed at dt_min; the state is the one before the step");
+                    return AEO_ERR_NUMERICAL;
+                }
+                dt = dt_new;
+                ++retries;
+                set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt, dt);
+                CKL();
+                cudaGraphExec_t gr;
+                if (aeo_status e = graph_for(false, &gr)) return e;
+                CK(cudaGraphLaunch(gr, st));
+            }
+            cur ^= 1;
+            set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt_prev, dt);
+            CKL();
+            acc.dt = dt;
+            acc.t_advanced += dt;
+            acc.retries += retries;
+            acc.limiter = retries ? 8 : h.limiter;
+            acc.advective_rate = h.rate;
+            acc.nut_max = h.nut_max;
+            acc.brunt_vaisala = h.N;
+        }
+        if (dt_prev_io && n > 0) *dt_prev_io = acc.dt;
+        if (stats) *stats = acc;
+        return AEO_OK;
+    }
+
     aeo_status profile_step(double dt, double* ms, int ncls) override {
+        set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt, dt);
+        CKL();
         profiling = true;
         marks.clear();
         mark(-1);
-        aeo_status e = enqueue_rk3(dt);
+        aeo_status e = enqueue_rk3(cur, false);
         profiling = false;
         if (e) return e;
         CK(cudaStreamSynchronize(st));
+        cur ^= 1;
         for (int c = 0; c < ncls; ++c) ms[c] = 0.0;
         for (size_t q = 1; q < marks.size(); ++q) {
             float t = 0.f;
@@ -537,23 +730,10 @@ struct Core : CoreBase {
         return check_finite();
     }
 
-    aeo_status step_euler(double dt, int n) override {
-        for (int s = 0; s < n; ++s) {
-            if (aeo_status e = substage(0, 1, 0, R(dt), R(0), R(0))) return e;
-            // the Euler result becomes the state: swap sets 0 and 1
-            for (int f = 0; f < 4; ++f) std::swap(P[0][f], P[1][f]);
-            std::swap(tmaps[0], tmaps[1]);
-            if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
-            if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
-        }
-        CK(cudaStreamSynchronize(st));
-        return check_finite();
-    }
-
     aeo_status check_finite() {
         dim3 gb((g.nx + 127) / 128, g.ny, g.nz);
         for (int f = 0; f < 4; ++f) {
-            finite_check_kernel<R><<<gb, 128, 0, st>>>(g, P[0][f], d_flag);
+            finite_check_kernel<R><<<gb, 128, 0, st>>>(g, P[cur][f], d_flag);
             CKL();
         }
         int h = 0;
@@ -568,10 +748,10 @@ struct Core : CoreBase {
     R* field_ptr(int id, int* padded, int* loc) {
         *padded = 1;
         switch (id) {
-            case AEO_FIELD_U: *loc = LOC_FX; return P[0][0];
-            case AEO_FIELD_V: *loc = LOC_FY; return P[0][1];
-            case AEO_FIELD_W: *loc = LOC_FZ; return P[0][2];
-            case AEO_FIELD_THETA: *loc = LOC_C; return P[0][3];
+            case AEO_FIELD_U: *loc = LOC_FX; return P[cur][0];
+            case AEO_FIELD_V: *loc = LOC_FY; return P[cur][1];
+            case AEO_FIELD_W: *loc = LOC_FZ; return P[cur][2];
+            case AEO_FIELD_THETA: *loc = LOC_C; return P[cur][3];
             case AEO_FIELD_P: *padded = 0; *loc = -1; return pres;
             case AEO_FIELD_NUT: *loc = -1; return nut;
             default: return nullptr;
@@ -605,8 +785,8 @@ struct Core : CoreBase {
         if (!d) { fail("get_field: unknown or unavailable field"); return AEO_ERR_ARGUMENT; }
         if (id == AEO_FIELD_NUT) {
             // the step keeps nut in shared memory: evaluate it for the current state
-            if (uni) smagorinsky_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, P[0][0], P[0][1], P[0][2], nut, R(cfg.c_s));
-            else smagorinsky_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, P[0][0], P[0][1], P[0][2], nut, R(cfg.c_s));
+            if (uni) smagorinsky_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], nut, R(cfg.c_s));
+            else smagorinsky_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], nut, R(cfg.c_s));
             CKL();
         }
         pack_host_kernel<R><<<(unsigned)((host_n + 255) / 256), 256, 0, st>>>(g, d_stage, cfg.hx, cfg.hy, cfg.hz, d,
@@ -629,9 +809,88 @@ struct Core : CoreBase {
         return AEO_OK;
     }
 
+    // One Chorin projection of the state with dt = 1 (the config driver's
+    // _project!(sim, 1.0), src/config/simulation_driver.jl:1316).
+    aeo_status project() override {
+        dim3 gb((g.nx + 127) / 128, g.ny, g.nz);
+        for (int f = 0; f < 3; ++f) {
+            padded_to_interior_kernel<R><<<gb, 128, 0, st>>>(g, P[cur][f], Q[f]);
+            CKL();
+        }
+        if (aeo_status e = solve(nullptr)) return e;
+        if (aeo_status e = correct(P[cur], 0, R(0), R(0), &d_sc->one, cur)) return e;
+        R* f[3] = {P[cur][0], P[cur][1], P[cur][2]};
+        int l[3] = {LOC_FX, LOC_FY, LOC_FZ};
+        if (aeo_status e = halo(f, l, 3)) return e;
+        CK(cudaStreamSynchronize(st));
+        return AEO_OK;
+    }
+
+    // isotropic_turbulence_field! on the device, then the optional projection
+    // and rescaling to a target per-component rms.
+    aeo_status init_isotropic(double u_rms, double k_peak, uint64_t seed, double kmax, int proj,
+                              double target_rms) override {
+        if (cfg.solver != AEO_SOLVER_FFT || !uni) {
+            fail("init_isotropic: a triply periodic uniform grid is required (src/operators/spectra.jl:316)");
+            return AEO_ERR_ARGUMENT;
+        }
+        const int Mh = g.nx / 2 + 1, M = g.nx / 2;
+        const long long ns = (long long)Mh * g.ny * g.nz;
+        dim3 gy((Mh + tpx_y - 1) / tpx_y, g.nz);
+        size_t smy = (size_t)tpx_y * g.ny * sizeof(cplx<R>);
+        dim3 gz((Mh + tpx_z - 1) / tpx_z, g.ny);
+        size_t smz = (size_t)tpx_z * g.nz * sizeof(cplx<R>);
+        size_t smx = (size_t)rows_x * M * sizeof(cplx<R>);
+        unsigned gx = (unsigned)((g.ny * (long long)g.nz + rows_x - 1) / rows_x);
+        dim3 gb((g.nx + 127) / 128, g.ny, g.nz);
+        for (int comp = 0; comp < 3; ++comp) {
+            IsoParams p{};
+            p.u_rms = u_rms; p.k_peak = k_peak; p.kmax = kmax > 0 ? kmax : 1.0 / 0.0;
+            p.lx = cfg.lx; p.ly = cfg.ly; p.lz = cfg.lz;
+            p.x1 = cfg.x0 + (comp == 0 ? 0.0 : 0.5 * g.dx);
+            p.y1 = cfg.y0 + (comp == 1 ? 0.0 : 0.5 * g.dy);
+            p.z1 = cfg.z0 + (comp == 2 ? 0.0 : 0.5 * g.dz);
+            p.seed = seed;
+            p.comp = comp;
+            iso_modes_kernel<R><<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(g, S, p);
+            CKL();
+            fftz_inv_kernel<R><<<gz, 256, smz, st>>>(g, S, tw, NT, tpx_z);
+            CKL();
+            ffty_kernel<R, 1><<<gy, 256, smy, st>>>(g, S, tw, NT, tpx_y);
+            CKL();
+            ifftx_kernel<R><<<gx, 256, smx, st>>>(g, S, phi, tw, NT, rows_x, R(1));
+            CKL();
+            interior_to_padded_kernel<R><<<gb, 128, 0, st>>>(g, phi, P[cur][comp], R(1));
+            CKL();
+        }
+        R* f[3] = {P[cur][0], P[cur][1], P[cur][2]};
+        int l[3] = {LOC_FX, LOC_FY, LOC_FZ};
+        if (aeo_status e = halo(f, l, 3)) return e;
+        if (proj)
+            if (aeo_status e = project()) return e;
+        if (target_rms > 0) {
+            sumsq_levels_kernel<R><<<g.nz, 256, 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], d_part);
+            CKL();
+            std::vector<double> h(g.nz);
+            CK(cudaMemcpyAsync(h.data(), d_part, g.nz * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            double sum = 0.0;
+            for (int k = 0; k < g.nz; ++k) sum += h[k];
+            double rms = std::sqrt(sum / (3.0 * (double)g.nin));
+            if (!(rms > 0)) { fail("init_isotropic: the generated field is zero"); return AEO_ERR_NUMERICAL; }
+            for (int c = 0; c < 3; ++c) {
+                scale_padded_kernel<R><<<gb, 128, 0, st>>>(g, P[cur][c], target_rms / rms);
+                CKL();
+            }
+            if (aeo_status e = halo(f, l, 3)) return e;
+        }
+        CK(cudaStreamSynchronize(st));
+        return AEO_OK;
+    }
+
     aeo_status kinetic_energy(double* out) override {
-        if (uni) ke_levels_kernel<R, true><<<g.nz, 256, 0, st>>>(g, P[0][0], P[0][1], P[0][2], d_part);
-        else ke_levels_kernel<R, false><<<g.nz, 256, 0, st>>>(g, P[0][0], P[0][1], P[0][2], d_part);
+        if (uni) ke_levels_kernel<R, true><<<g.nz, 256, 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], d_part);
+        else ke_levels_kernel<R, false><<<g.nz, 256, 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], d_part);
         CKL();
         std::vector<double> h(g.nz);
         CK(cudaMemcpyAsync(h.data(), d_part, g.nz * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -643,12 +902,13 @@ struct Core : CoreBase {
     }
 
     aeo_status max_divergence(double* out) override {
+        R** s = P[cur];
         if (anel) {
-            if (uni) maxdiv_levels_kernel<R, true, true><<<g.nz, 256, 0, st>>>(g, P[0][0], P[0][1], P[0][2], d_part);
-            else maxdiv_levels_kernel<R, true, false><<<g.nz, 256, 0, st>>>(g, P[0][0], P[0][1], P[0][2], d_part);
+            if (uni) maxdiv_levels_kernel<R, true, true><<<g.nz, 256, 0, st>>>(g, s[0], s[1], s[2], d_part);
+            else maxdiv_levels_kernel<R, true, false><<<g.nz, 256, 0, st>>>(g, s[0], s[1], s[2], d_part);
         } else {
-            if (uni) maxdiv_levels_kernel<R, false, true><<<g.nz, 256, 0, st>>>(g, P[0][0], P[0][1], P[0][2], d_part);
-            else maxdiv_levels_kernel<R, false, false><<<g.nz, 256, 0, st>>>(g, P[0][0], P[0][1], P[0][2], d_part);
+            if (uni) maxdiv_levels_kernel<R, false, true><<<g.nz, 256, 0, st>>>(g, s[0], s[1], s[2], d_part);
+            else maxdiv_levels_kernel<R, false, false><<<g.nz, 256, 0, st>>>(g, s[0], s[1], s[2], d_part);
         }
         CKL();
         std::vector<double> h(g.nz);
@@ -677,44 +937,6 @@ struct Core : CoreBase {
         return AEO_OK;
     }
 };
-
-template <typename R>
-aeo_status Core<R>::src_fftx(const R* src) {
-    const int M = g.nx / 2;
-    size_t smx = (size_t)rows_x * M * sizeof(cplx<R>);
-    unsigned gx = (unsigned)((g.ny * (long long)g.nz + rows_x - 1) / rows_x);
-    src_fftx_kernel<R><<<gx, 256, smx, st>>>(g, src, S, tw, NT, rows_x);
-    CKL();
-    return AEO_OK;
-}
-
-template <typename R>
-__global__ void padded_to_interior_kernel(Geo g, const R* __restrict__ a, R* __restrict__ b) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-    if (i < g.nx) b[iidx(g, i, j, k)] = a[pidx(g, i, j, k)];
-}
-
-template <typename R>
-aeo_status Core<R>::project() {
-    dim3 gb((g.nx + 127) / 128, g.ny, g.nz);
-    for (int f = 0; f < 3; ++f) {
-        padded_to_interior_kernel<R><<<gb, 128, 0, st>>>(g, P[0][f], Q[f]);
-        CKL();
-    }
-    if (aeo_status e = solve(nullptr)) return e;
-    if (uni)
-        correct_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, Q[0], Q[1], Q[2], phi, P[0][0], P[0][1], P[0][2], P[0][0],
-                                                           P[0][1], P[0][2], pres, R(1), R(0), R(0), 0);
-    else
-        correct_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, Q[0], Q[1], Q[2], phi, P[0][0], P[0][1], P[0][2], P[0][0],
-                                                            P[0][1], P[0][2], pres, R(1), R(0), R(0), 0);
-    CKL();
-    R* f[3] = {P[0][0], P[0][1], P[0][2]};
-    int l[3] = {LOC_FX, LOC_FY, LOC_FZ};
-    if (aeo_status e = halo(f, l, 3)) return e;
-    CK(cudaStreamSynchronize(st));
-    return AEO_OK;
-}
 
 // ====================================================================================
 // C-ABI
@@ -823,6 +1045,35 @@ aeo_status aeo_step_euler(aeo_sim* h, double dt, int32_t nsteps) {
     ENTER(h);
     if (!(dt > 0) || nsteps < 0) { h->core->fail("dt must be positive and nsteps >= 0"); return AEO_ERR_ARGUMENT; }
     return h->core->step_euler(dt, nsteps);
+}
+
+aeo_status aeo_step_adaptive(aeo_sim* h, const aeo_cfl* c, int32_t nsteps, double* dt_prev,
+                             aeo_adaptive_stats* stats) {
+    ENTER(h);
+    if (!c || nsteps < 0 || !(c->c_advective > 0) || !(c->c_diffusive > 0) || !(c->c_buoyancy > 0) ||
+        !(c->c_coriolis > 0) || !(c->dt_min > 0) || !(c->dt_min <= c->dt_max) || !(c->growth_max >= 1) ||
+        c->max_retries < 0) {
+        h->core->fail("step_adaptive: invalid CFL constraints (CFLConstraints, src/TimeIntegration.jl:137-153)");
+        return AEO_ERR_ARGUMENT;
+    }
+    return h->core->step_adaptive(c, nsteps, dt_prev, stats);
+}
+
+aeo_status aeo_cfl_diagnostics(aeo_sim* h, const aeo_cfl* c, double dt_prev, aeo_adaptive_stats* out) {
+    ENTER(h);
+    if (!c || !out || !(c->c_advective > 0) || !(c->c_diffusive > 0) || !(c->dt_min > 0) || !(c->dt_min <= c->dt_max) ||
+        !(c->growth_max >= 1)) {
+        h->core->fail("cfl_diagnostics: invalid CFL constraints");
+        return AEO_ERR_ARGUMENT;
+    }
+    return h->core->cfl(c, dt_prev, out);
+}
+
+aeo_status aeo_init_isotropic(aeo_sim* h, double u_rms, double k_peak, uint64_t seed, double kmax, int32_t project,
+                              double target_rms) {
+    ENTER(h);
+    if (!(u_rms > 0) || !(k_peak > 0)) { h->core->fail("init_isotropic: u_rms and k_peak must be positive"); return AEO_ERR_ARGUMENT; }
+    return h->core->init_isotropic(u_rms, k_peak, seed, kmax, project, target_rms);
 }
 
 aeo_status aeo_project(aeo_sim* h) {

@@ -111,6 +111,43 @@ aeo_status aeo_step_rk3(aeo_sim* h, double dt, int32_t nsteps);
  * src/Anelastic.jl:1747-1876). */
 aeo_status aeo_step_euler(aeo_sim* h, double dt, int32_t nsteps);
 
+/* CFL constraints and guard limits of the adaptive step: CFLConstraints
+ * (src/TimeIntegration.jl:127-153; defaults C_advective 0.5, C_diffusive
+ * 0.25, C_buoyancy 0.5, C_coriolis 0.5, dt_min 1e-8, dt_max Inf,
+ * growth_max 1.1) and step_adaptive!'s divergence_tol (1e-6), max_velocity
+ * (Inf) and max_retries (3) (src/TimeIntegration.jl:823-835). */
+typedef struct {
+    double c_advective, c_diffusive, c_buoyancy, c_coriolis;
+    double dt_min, dt_max, growth_max;
+    double divergence_tol, max_velocity;
+    int32_t max_retries;
+} aeo_cfl;
+
+/* What an adaptive step reports: the last accepted dt, the time advanced, the
+ * limiter of the pick (0 advective, 1 diffusive, 2 buoyancy, 3 Coriolis,
+ * 4 sgs, 5 growth, 6 dt_min, 7 dt_max, 8 retried), the retries, the pick's
+ * advective rate max Σ|u_i|/Δx_i, max νt, Brunt-Väisälä frequency, and the
+ * guard's max |∇·u| and max speed of the new state. */
+typedef struct {
+    double dt, t_advanced;
+    int32_t limiter, retries;
+    double advective_rate, nut_max, brunt_vaisala, max_divergence, max_speed;
+} aeo_adaptive_stats;
+
+/* nsteps adaptive SSP-RK3 steps: step_adaptive! (src/TimeIntegration.jl:808-938)
+ * with adaptive_dt (:436-454) evaluated on the device inside the step's CUDA
+ * graph.  *dt_prev in: the previous dt (<= 0: none, no growth limit); out: the
+ * last accepted dt.  A step whose guard fails (non-finite state, divergence
+ * above the tolerance, speed above the cap) is retried from the unchanged
+ * step-start state with half the dt, up to max_retries times; then the call
+ * returns AEO_ERR_NUMERICAL with the state of the start of that step. */
+aeo_status aeo_step_adaptive(aeo_sim* h, const aeo_cfl* c, int32_t nsteps, double* dt_prev,
+                             aeo_adaptive_stats* stats);
+
+/* cfl_diagnostics + adaptive_dt of the current state (src/TimeIntegration.jl:291-454):
+ * the dt the next adaptive step would take and its limiter, without stepping. */
+aeo_status aeo_cfl_diagnostics(aeo_sim* h, const aeo_cfl* c, double dt_prev, aeo_adaptive_stats* out);
+
 /* The projection's Poisson solve on interior-sized arrays (Nx*Ny*Nz, x
  * fastest): solve!(p, source, solver) / solve_source_buffer! of the
  * AbstractPressureSolver seam (src/PressureSolvers.jl:41-80, :162-174,
@@ -122,6 +159,17 @@ aeo_status aeo_pressure_solve(aeo_sim* h, const double* src, double* phi);
  * `_project!(sim, 1.0)` of a noisy initial field
  * (src/config/simulation_driver.jl:1316; src/Simulations.jl:711-744). */
 aeo_status aeo_project(aeo_sim* h);
+
+/* Fill u, v, w with the random-phase isotropic field of the Passot-Pouquet
+ * spectrum E(k) = 16 sqrt(2/pi) u_rms^2 k^4/k_peak^5 exp(-2 (k/k_peak)^2):
+ * isotropic_turbulence_field! with PassotPouquetSpectrum
+ * (src/operators/spectra.jl:248-343; SplitMix64 mode hash, modes with
+ * |k| <= kmax, kmax <= 0 for no cut-off), generated on the device.  Then,
+ * when `project` is non-zero, one Chorin projection (aeo_project), and when
+ * target_rms > 0 a rescaling of u, v, w to that per-component rms.  Triply
+ * periodic uniform grids only. */
+aeo_status aeo_init_isotropic(aeo_sim* h, double u_rms, double k_peak, uint64_t seed, double kmax,
+                              int32_t project, double target_rms);
 
 /* kinetic_energy (src/Simulations.jl:992-1014) and max_divergence
  * (src/Simulations.jl:1045-1050; the W-normalised residual

@@ -1090,6 +1090,83 @@ int oc_step_euler(oc_sim* s, double dt, int nsteps) {
     return 0;
 }
 
+/* cfl_diagnostics + adaptive_dt (src/TimeIntegration.jl:164-185, :209-226,
+ * :291-365, :436-454): the advective rate max_cell sum |u_i|/dx_i, the
+ * diffusive (molecular + Smagorinsky) and SGS limits over the harmonic
+ * spacing of the thinnest cell, the Brunt-Vaisala limit of the plane-mean
+ * theta profile, the Coriolis limit; then the growth limit and the clamp.
+ * limiter: 0 adv, 1 diff, 2 buoy, 3 cor, 4 sgs, 5 growth, 6 dt_min, 7 dt_max. */
+double oc_adaptive_dt(oc_sim* s, const oc_cfl* c, double dt_prev, int* limiter) {
+    const oc_params* P = &s->p;
+    int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
+    int anel = P->core == OC_CORE_ANELASTIC;
+    fill_halos(s, s->u, LOC_FX);
+    fill_halos(s, s->v, LOC_FY);
+    fill_halos(s, s->w, LOC_FZ);
+    double rate = 0.0, nutm = 0.0;
+    int nanr = 0;
+    double* mean = (double*)calloc((size_t)Nz, sizeof(double));
+    for (int k = Hz; k < Hz + Nz; ++k) {
+        double acc = 0.0;
+        for (int j = Hy; j < Hy + Ny; ++j)
+            for (int i = Hx; i < Hx + Nx; ++i) {
+                double au = fmax(fabs(A(s->u, i, j, k)), fabs(A(s->u, i + 1, j, k)));
+                double av = fmax(fabs(A(s->v, i, j, k)), fabs(A(s->v, i, j + 1, k)));
+                double aw = fmax(fabs(A(s->w, i, j, k)), fabs(A(s->w, i, j, k + 1)));
+                double r = au * s->idx + av * s->idy + aw * m_idz(s, k);
+                if (isnan(r)) nanr = 1;
+                else if (r > rate) rate = r;
+                if (P->c_s != 0) {
+                    double n = smag_at(s, i, j, k);
+                    if (n > nutm) nutm = n;
+                }
+                acc += A(s->th, i, j, k);
+            }
+        mean[k - Hz] = acc / ((double)Nx * Ny);
+    }
+    const double INF = 1.0 / 0.0;
+    if (nanr) rate = NAN;
+    double dt_adv = isnan(rate) ? NAN : (rate > 0 ? c->c_adv / rate : INF);
+    double dzmin = INF;
+    for (int k = Hz; k < Hz + Nz; ++k) dzmin = fmin(dzmin, s->dzc[k]);
+    double harm = 1.0 / (1 / (s->dx * s->dx) + 1 / (s->dy * s->dy) + 1 / (dzmin * dzmin));
+    double nu_total = P->nu + nutm;
+    double dt_diff = nu_total > 0 ? c->c_diff * harm / nu_total : INF;
+    double ksgs = fmax(nutm, P->c_s != 0 ? nutm / P->pr_t : 0.0);
+    double dt_sgs = ksgs > 0 ? c->c_diff * harm / ksgs : INF;
+    int buoy = anel ? (P->g != 0) : (P->theta0 != 0);
+    double n2max = 0.0;
+    if (buoy)
+        for (int k = 1; k < Nz; ++k) {
+            double dzf = s->dzf[Hz + k];
+            double n2 = anel ? P->g * (log(mean[k]) - log(mean[k - 1])) / dzf
+                             : (P->g / P->theta0) * (mean[k] - mean[k - 1]) * (1 / dzf);
+            n2max = fmax(n2max, n2);
+        }
+    free(mean);
+    double N = sqrt(fmax(n2max, 0.0));
+    double dt_buoy = N > 0 ? c->c_buoy / N : INF;
+    double f = fabs(P->f_coriolis);
+    double dt_cor = f > 0 ? c->c_cor / f : INF;
+    double dt = dt_adv;
+    int lim = 0;
+    if (dt_diff < dt) { dt = dt_diff; lim = 1; }
+    if (dt_buoy < dt) { dt = dt_buoy; lim = 2; }
+    if (dt_cor < dt) { dt = dt_cor; lim = 3; }
+    if (dt_sgs < dt) { dt = dt_sgs; lim = 4; }
+    if (isnan(dt)) {
+        dt = c->dt_min;
+        lim = 6;
+    } else {
+        if (dt_prev > 0 && c->growth * dt_prev < dt) { dt = c->growth * dt_prev; lim = 5; }
+        if (dt < c->dt_min) lim = 6;
+        if (dt > c->dt_max) lim = 7;
+        dt = fmin(fmax(dt, c->dt_min), c->dt_max);
+    }
+    if (limiter) *limiter = lim;
+    return dt;
+}
+
 /* SSP-RK3 of three projected substages (src/Simulations.jl:854-912) */
 int oc_step_rk3(oc_sim* s, double dt, int nsteps) {
     size_t b = sizeof(double) * (size_t)s->n;
@@ -1100,6 +1177,21 @@ int oc_step_rk3(oc_sim* s, double dt, int nsteps) {
         substage(s, dt, 1, 0.75, 0.25);
         substage(s, dt, 1, inv3, two3);
     }
+    return 0;
+}
+
+/* nsteps of step_adaptive! without failures: the adaptive_dt pick, then
+ * step_rk3!.  dts (nsteps entries, may be NULL) receives the dt sequence;
+ * *dt_prev carries the growth limit in and the last dt out. */
+int oc_step_adaptive(oc_sim* s, const oc_cfl* c, int nsteps, double* dt_prev, double* dts) {
+    double dp = dt_prev ? *dt_prev : 0.0;
+    for (int n = 0; n < nsteps; ++n) {
+        double dt = oc_adaptive_dt(s, c, dp, NULL);
+        oc_step_rk3(s, dt, 1);
+        if (dts) dts[n] = dt;
+        dp = dt;
+    }
+    if (dt_prev) *dt_prev = dp;
     return 0;
 }
 

@@ -53,6 +53,11 @@ int oc_step_rk3(oc_sim* s, double dt, int nsteps);
 int oc_step_euler(oc_sim* s, double dt, int nsteps);
 /* Chorin projection of the current velocity (dt = 1). */
 int oc_project(oc_sim* s);
+
+/* CFLConstraints (src/TimeIntegration.jl:127-153) */
+typedef struct { double c_adv, c_diff, c_buoy, c_cor, dt_min, dt_max, growth; } oc_cfl;
+double oc_adaptive_dt(oc_sim* s, const oc_cfl* c, double dt_prev, int* limiter);
+int oc_step_adaptive(oc_sim* s, const oc_cfl* c, int nsteps, double* dt_prev, double* dts);
 /* Tendencies of the current state (halos filled first) into tu..tθ (storage). */
 int oc_tendencies(oc_sim* s, double* tu, double* tv, double* tw, double* tt);
 /* Solve the projection's Poisson problem: src and phi are interior-sized

@@ -33,6 +33,15 @@ class OcParams(C.Structure):
     ]
 
 
+class OcCfl(C.Structure):
+    _fields_ = [("c_adv", C.c_double), ("c_diff", C.c_double), ("c_buoy", C.c_double), ("c_cor", C.c_double),
+                ("dt_min", C.c_double), ("dt_max", C.c_double), ("growth", C.c_double)]
+
+
+def _cfl(c):
+    return OcCfl(c.C_advective, c.C_diffusive, c.C_buoyancy, c.C_coriolis, c.dt_min, c.dt_max, c.growth_max)
+
+
 _lib = None
 
 
@@ -62,6 +71,9 @@ def load():
     lib.oc_step_rk3.argtypes = [P, C.c_double, C.c_int]
     lib.oc_step_euler.argtypes = [P, C.c_double, C.c_int]
     lib.oc_project.argtypes = [P]
+    lib.oc_adaptive_dt.argtypes = [P, C.POINTER(OcCfl), C.c_double, C.POINTER(C.c_int)]
+    lib.oc_adaptive_dt.restype = C.c_double
+    lib.oc_step_adaptive.argtypes = [P, C.POINTER(OcCfl), C.c_int, C.POINTER(C.c_double), _D]
     lib.oc_tendencies.argtypes = [P, _D, _D, _D, _D]
     lib.oc_pressure_solve.argtypes = [P, _D, _D]
     lib.oc_apply_poisson_operator.argtypes = [P, _D, _D]
@@ -171,6 +183,17 @@ class OracleSimulation:
 
     def step(self, dt, nsteps=1):
         assert self._lib.oc_step_euler(self._h, float(dt), int(nsteps)) == 0
+
+    def adaptive_dt(self, constraints, dt_prev=None):
+        lim = C.c_int()
+        dt = self._lib.oc_adaptive_dt(self._h, C.byref(_cfl(constraints)), float(dt_prev or 0.0), C.byref(lim))
+        return dt, lim.value
+
+    def step_adaptive(self, constraints, nsteps=1, dt_prev=None):
+        d = C.c_double(float(dt_prev or 0.0))
+        dts = np.empty(nsteps)
+        self._lib.oc_step_adaptive(self._h, C.byref(_cfl(constraints)), int(nsteps), C.byref(d), _p(dts))
+        return dts
 
     def project(self):
         assert self._lib.oc_project(self._h) == 0

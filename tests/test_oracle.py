@@ -242,3 +242,58 @@ def test_anelastic_constraint_at_round_off_after_steps():
     o.step_rk3(1.0, 3)
     assert o.max_divergence() < 1e-13
     assert np.abs(o.get_field("w")[g.interior]).max() > 0  # the surface flux drives motion
+
+
+# ---------------------------------------------------------------- adaptive dt
+def test_adaptive_dt_advective_limit_growth_and_clamp():
+    from aeolus_b200.simulation import CFLConstraints
+    n = 16
+    g = regular_grid((n, n, n), (2 * np.pi,) * 3)
+    o = OracleSimulation(CoreSpec(grid=g, nu=0.0))
+    rng = np.random.default_rng(1)
+    st = []
+    for name in ("u", "v", "w"):
+        a = g.zeros()
+        a[g.interior] = rng.standard_normal((n, n, n))
+        o.set_field(name, a)
+        st.append(a)
+    o.fill_halos()
+    u, v, w, _ = o.get_state()
+    I = g.interior
+    hz, hy, hx = g.halo[2], g.halo[1], g.halo[0]
+    au = np.maximum(np.abs(u[I]), np.abs(u[hz:hz + n, hy:hy + n, hx + 1:hx + n + 1]))
+    av = np.maximum(np.abs(v[I]), np.abs(v[hz:hz + n, hy + 1:hy + n + 1, hx:hx + n]))
+    aw = np.maximum(np.abs(w[I]), np.abs(w[hz + 1:hz + n + 1, hy:hy + n, hx:hx + n]))
+    rate = (au / g.dx + av / g.dy + aw / g.dz).max()
+    dt, lim = o.adaptive_dt(CFLConstraints(C_advective=0.5))
+    assert abs(dt - 0.5 / rate) <= 1e-14 * dt and lim == 0
+    dt2, lim2 = o.adaptive_dt(CFLConstraints(), dt_prev=0.5 * dt)
+    assert abs(dt2 - 1.1 * 0.5 * dt) <= 1e-15 and lim2 == 5
+    dt3, lim3 = o.adaptive_dt(CFLConstraints(dt_max=0.1 * dt))
+    assert dt3 == 0.1 * dt and lim3 == 7
+
+
+def test_adaptive_dt_diffusive_limit_binds_for_viscous_flow():
+    from aeolus_b200.simulation import CFLConstraints
+    g = regular_grid((16, 16, 16), (1.0, 1.0, 1.0))
+    o = OracleSimulation(CoreSpec(grid=g, nu=1.0))
+    a = g.zeros()
+    a[g.interior] = 1e-3
+    o.set_field("u", a)
+    dt, lim = o.adaptive_dt(CFLConstraints())
+    harm = 1 / (3 / g.dx ** 2)
+    assert lim == 1 and abs(dt - 0.25 * harm / 1.0) < 1e-15
+
+
+def test_isotropic_field_is_real_with_the_target_rms_and_projects_to_round_off():
+    from aeolus_b200.inputs import isotropic_turbulence
+    g = regular_grid((32, 32, 32), (2 * np.pi,) * 3)
+    u, v, w = isotropic_turbulence(g, 1.0, 4.0, seed=1)
+    I = g.interior
+    rms = [np.sqrt((a[I] ** 2).mean()) for a in (u, v, w)]
+    assert all(0.8 < r < 1.2 for r in rms)
+    o = OracleSimulation(CoreSpec(grid=g))
+    o.set_state(u, v, w, g.zeros())
+    assert o.max_divergence() > 1e-3          # the continuous field's discrete divergence
+    o.project()
+    assert o.max_divergence() < 1e-12
