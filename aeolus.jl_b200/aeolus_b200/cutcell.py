@@ -1,0 +1,231 @@
+"""Cut-cell geometry of floor-standing box obstacles and the host side of
+the cut-cell projection (set-up work: serial loops in the reference too).
+
+Restates `cut_cell_geometry(mesh, levelset; nsub, vol_min)` and
+`_finalize_geometry` (src/CutCell.jl:243-319, :398-493):
+  * volume fractions from nsub^3 sub-samples per cell, open-area fractions
+    from nsub^2 samples per face, with the level-set convention phi > 0
+    fluid (src/CutCell.jl:265-317);
+  * the consistency sweeps: a face touching a dry cell is closed; a wetted
+    cell with no open face becomes solid; repeated up to 16 times until
+    nothing changes (:413-447);
+  * vol_eff = max(vol_frac, vol_min) on wetted cells, 0 in solid (:449-465).
+The outermost low-side storage faces are closed as in the reference (:407-411).
+
+Obstacles are axis-aligned boxes standing on the floor z0 (an urban block
+model).  Their union with the ground is the level set
+phi(x, y, z) = z - H(x, y), H the top of the tallest box whose closed
+footprint covers (x, y) (the floor elsewhere), periodic in x and y: a sample
+is fluid iff it lies strictly above H.  The per-sample test is done as a
+sorted search of the z samples, so the fractions are the reference's exact
+sample counts at any grid size.
+
+Arrays are storage-shaped (Nz+2Hz, Ny+2Hy, Nx+2Hx) and indexed [k, j, i];
+ax[k, j, i] is the west face of cell i, ay the south face, az the bottom.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .grids import Grid
+from .inputs import philox_uniform, uniform_noise
+
+
+@dataclass
+class CutCellGeometry:
+    grid: Grid
+    vol_frac: np.ndarray
+    vol_eff: np.ndarray
+    ax: np.ndarray
+    ay: np.ndarray
+    az: np.ndarray
+    is_solid: np.ndarray
+    is_small: np.ndarray
+    vol_min: float
+    nsub: int
+
+    @property
+    def fluid_interior(self) -> np.ndarray:
+        return ~self.is_solid[self.grid.interior]
+
+
+def random_boxes(grid: Grid, n: int, seed: int, footprint=(10.0, 40.0), height=(10.0, 60.0)) -> np.ndarray:
+    """n floor-standing boxes: Philox-seeded centres uniform over the
+    horizontal domain, side lengths uniform in `footprint`, heights uniform in
+    `height`.  Returns (n, 6) rows (x0, x1, y0, y1, z0, z1)."""
+    u = [philox_uniform(seed, 100 + s, n) for s in range(5)]
+    lx, ly = grid.extent[0], grid.extent[1]
+    ox, oy, oz = grid.origin
+    cx, cy = ox + u[0] * lx, oy + u[1] * ly
+    wx = footprint[0] + u[2] * (footprint[1] - footprint[0])
+    wy = footprint[0] + u[3] * (footprint[1] - footprint[0])
+    hz = height[0] + u[4] * (height[1] - height[0])
+    return np.stack([cx - wx / 2, cx + wx / 2, cy - wy / 2, cy + wy / 2, np.full(n, oz), oz + hz], axis=1)
+
+
+def _west(grid: Grid, axis: int) -> np.ndarray:
+    """_xw/_yw/_zw of every storage index (src/CutCell.jl:90-92)."""
+    n, H = grid.size[axis], grid.halo[axis]
+    d = (grid.dx, grid.dy, grid.dz)[axis]
+    return grid.origin[axis] + (np.arange(n + 2 * H) - H) * d
+
+
+def _subsamples(grid: Grid, axis: int, nsub: int) -> np.ndarray:
+    """x_w + (a - 1/2) h, h = d/nsub, a = 1..nsub, for every storage index,
+    flattened cell-major (src/CutCell.jl:266-274)."""
+    d = (grid.dx, grid.dy, grid.dz)[axis]
+    h = d * (1.0 / nsub)
+    return (_west(grid, axis)[:, None] + (np.arange(1, nsub + 1) - 0.5) * h).ravel()
+
+
+def box_heights(grid: Grid, boxes, x: np.ndarray, y: np.ndarray) -> np.ndarray:
+    """H on the lattice y (rows) x x (columns): the tallest box whose closed
+    footprint holds the point, periodic in x and y; the floor z0 elsewhere."""
+    lx, ly = grid.extent[0], grid.extent[1]
+    ox, oy, floor = grid.origin
+    X = ox + np.mod(x - ox, lx)
+    Y = oy + np.mod(y - oy, ly)
+    H = np.full((len(Y), len(X)), floor)
+    for (x0, x1, y0, y1, z0, z1) in np.asarray(boxes, dtype=np.float64).reshape(-1, 6):
+        if z0 > floor:
+            raise ValueError("boxes must stand on the floor (z0 <= grid origin z)")
+        for sx in (-lx, 0.0, lx):
+            ix = np.nonzero((X >= x0 + sx) & (X <= x1 + sx))[0]
+            if ix.size == 0:
+                continue
+            for sy in (-ly, 0.0, ly):
+                iy = np.nonzero((Y >= y0 + sy) & (Y <= y1 + sy))[0]
+                if iy.size == 0:
+                    continue
+                H[np.ix_(iy, ix)] = np.maximum(H[np.ix_(iy, ix)], z1)
+    return H
+
+
+def _fluid_counts(H: np.ndarray, zs: np.ndarray, nsub: int, nz: int) -> np.ndarray:
+    """For each level k and lattice column, the number of the level's nsub
+    z samples strictly above H: level k owns samples [k nsub, (k+1) nsub)."""
+    nle = np.searchsorted(zs, H, side="right")        # samples with z <= H
+    out = np.empty((nz,) + H.shape, dtype=np.int32)
+    for k in range(nz):
+        out[k] = nsub - np.clip(nle - k * nsub, 0, nsub)
+    return out
+
+
+def box_geometry(grid: Grid, boxes, nsub: int = 4, vol_min: float = 1e-3) -> CutCellGeometry:
+    """`cut_cell_geometry` of floor-standing boxes (src/CutCell.jl:243-319)."""
+    if nsub < 1:
+        raise ValueError("nsub must be >= 1")
+    if not 0 <= vol_min < 1:
+        raise ValueError("vol_min must lie in [0, 1)")
+    NZ, NY, NX = grid.storage_shape
+    xs, ys, zs = (_subsamples(grid, a, nsub) for a in range(3))
+    xf, yf, zf = (_west(grid, a) for a in range(3))
+    n2, n3 = float(nsub * nsub), float(nsub ** 3)
+    Hc = box_heights(grid, boxes, xs, ys)
+    vol = _fluid_counts(Hc, zs, nsub, NZ).reshape(NZ, NY, nsub, NX, nsub).sum(axis=(2, 4)) / n3
+    ax = _fluid_counts(box_heights(grid, boxes, xf, ys), zs, nsub, NZ).reshape(NZ, NY, nsub, NX).sum(axis=2) / n2
+    ay = _fluid_counts(box_heights(grid, boxes, xs, yf), zs, nsub, NZ).reshape(NZ, NY, NX, nsub).sum(axis=3) / n2
+    nle = np.searchsorted(zf, Hc, side="right")       # bottom faces with z <= H
+    az = np.stack([(nle <= k).reshape(NY, nsub, NX, nsub).sum(axis=(1, 3)) for k in range(NZ)]) / n2
+    return finalize_geometry(grid, vol, ax, ay, az, vol_min, nsub)
+
+
+def finalize_geometry(grid: Grid, vol, ax, ay, az, vol_min: float, nsub: int) -> CutCellGeometry:
+    """The robustness passes of `_finalize_geometry` (src/CutCell.jl:398-465)."""
+    vol = np.array(vol, dtype=np.float64)
+    ax, ay, az = (np.array(a, dtype=np.float64) for a in (ax, ay, az))
+    solid = ~(vol > 0)
+    ax[:, :, 0] = 0.0
+    ay[:, 0, :] = 0.0
+    az[0, :, :] = 0.0
+    for _ in range(16):
+        ax[:, :, 1:][solid[:, :, :-1] | solid[:, :, 1:]] = 0.0
+        ay[:, 1:, :][solid[:, :-1, :] | solid[:, 1:, :]] = 0.0
+        az[1:, :, :][solid[:-1, :, :] | solid[1:, :, :]] = 0.0
+        opn = ax + ay + az
+        opn[:, :, :-1] += ax[:, :, 1:]
+        opn[:, :-1, :] += ay[:, 1:, :]
+        opn[:-1, :, :] += az[1:, :, :]
+        newly = ~solid & ~(opn > 0)
+        if not newly.any():
+            break
+        solid |= newly
+        vol[newly] = 0.0
+    small = ~solid & (vol < vol_min)
+    vol_eff = np.where(solid, 0.0, np.where(vol < vol_min, vol_min, vol))
+    return CutCellGeometry(grid, vol, vol_eff, ax, ay, az, solid, small, vol_min, nsub)
+
+
+def face_coefficients(geom: CutCellGeometry, power: int = 2):
+    """Interior face coefficients a^q of the cut-cell Laplacian
+    (cutcell_laplacian!, src/CutCell.jl:735-768): cx (Nz, Ny, Nx+1),
+    cy (Nz, Ny+1, Nx), cz (Nz+1, Ny, Nx); face index i is the west face of
+    cell i, the last one the east face of the last cell."""
+    g = geom.grid
+    hx, hy, hz = g.halo
+    nx, ny, nz = g.size
+    ks, js, is_ = slice(hz, hz + nz), slice(hy, hy + ny), slice(hx, hx + nx)
+    cx = geom.ax[ks, js, hx:hx + nx + 1] ** power
+    cy = geom.ay[ks, hy:hy + ny + 1, is_] ** power
+    cz = geom.az[hz:hz + nz + 1, js, is_] ** power
+    return np.ascontiguousarray(cx), np.ascontiguousarray(cy), np.ascontiguousarray(cz)
+
+
+def cutcell_divergence(geom: CutCellGeometry, u, v, w) -> np.ndarray:
+    """`cutcell_divergence!` without the small-cell redistribution
+    (src/CutCell.jl:602-622): the aperture-weighted flux difference over
+    vol_eff, zero in solid cells; u, v, w storage arrays with filled halos.
+    Returns the interior (Nz, Ny, Nx)."""
+    g = geom.grid
+    hx, hy, hz = g.halo
+    nx, ny, nz = g.size
+    K, J, I = slice(hz, hz + nz), slice(hy, hy + ny), slice(hx, hx + nx)
+    Ip, Jp, Kp = slice(hx + 1, hx + nx + 1), slice(hy + 1, hy + ny + 1), slice(hz + 1, hz + nz + 1)
+    fx = (geom.ax[K, J, Ip] * u[K, J, Ip] - geom.ax[K, J, I] * u[K, J, I]) / g.dx
+    fy = (geom.ay[K, Jp, I] * v[K, Jp, I] - geom.ay[K, J, I] * v[K, J, I]) / g.dy
+    fz = (geom.az[Kp, J, I] * w[Kp, J, I] - geom.az[K, J, I] * w[K, J, I]) / g.dz
+    ve = geom.vol_eff[K, J, I]
+    return np.where(ve > 0, (fx + fy + fz) / np.where(ve > 0, ve, 1.0), 0.0)
+
+
+def pressure_rhs(geom: CutCellGeometry, u, v, w) -> np.ndarray:
+    """Right-hand side of the symmetric cut-cell projection: vol_eff times
+    the cut-cell divergence (vol_eff L is symmetric, src/CutCell.jl:705-716),
+    zero in the solid, zero mean over the fluid."""
+    g = geom.grid
+    ve = geom.vol_eff[g.interior]
+    b = ve * cutcell_divergence(geom, u, v, w)
+    fluid = ve > 0
+    b[fluid] -= b[fluid].mean()
+    b[~fluid] = 0.0
+    return b
+
+
+def _periodic_xy(grid: Grid, A: np.ndarray) -> None:
+    hx, hy, _ = grid.halo
+    nx, ny, _ = grid.size
+    A[:, :, :hx] = A[:, :, nx:nx + hx]
+    A[:, :, hx + nx:] = A[:, :, hx:2 * hx]
+    A[:, :hy, :] = A[:, ny:ny + hy, :]
+    A[:, hy + ny:, :] = A[:, hy:2 * hy, :]
+
+
+def urban_velocity(grid: Grid, geom: CutCellGeometry, u_ref: float = 5.0, z_ref: float = 10.0,
+                   z0: float = 0.1, noise: float = 0.5, seed: int = 1):
+    """Log-profile inflow u(z) = u_ref ln(z/z0)/ln(z_ref/z0) (zero below z0)
+    plus Philox-seeded uniform noise of amplitude `noise` on u, v, w, with
+    every closed face zeroed.  Storage arrays with periodic x/y halos and
+    zero z halos."""
+    z = grid.znodes("c")
+    prof = np.where(z > z0, np.log(np.maximum(z, z0) / z0) / np.log(z_ref / z0), 0.0) * u_ref
+    comps = (prof[:, None, None] + uniform_noise(grid, seed, 0, noise),
+             uniform_noise(grid, seed, 1, noise), uniform_noise(grid, seed, 2, noise))
+    out = []
+    for a, ap in zip(comps, (geom.ax, geom.ay, geom.az)):
+        A = grid.zeros()
+        A[grid.interior] = a * (ap[grid.interior] > 0)
+        _periodic_xy(grid, A)
+        out.append(A)
+    return tuple(out)
