@@ -12,13 +12,16 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libaeolus_b200.so")
 
-# every entry point include/aeolus_b200.h declares
+# every entry point include/aeolus_b200.h and include/aeolus_b200_mgpcg.h declare
 SYMBOLS = (
     "aeo_create", "aeo_destroy", "aeo_set_field", "aeo_get_field", "aeo_step_rk3", "aeo_step_euler",
     "aeo_pressure_solve", "aeo_project", "aeo_kinetic_energy", "aeo_max_divergence", "aeo_step_rk3_async",
     "aeo_synchronize", "aeo_profile_step", "aeo_launches_per_step", "aeo_stream", "aeo_fill_uniform",
     "aeo_pressure_solve_column_noalloc", "aeo_step_adaptive", "aeo_cfl_diagnostics", "aeo_init_isotropic", "aeo_last_error",
     "aeo_version",
+    "aeo_mg_create", "aeo_mg_destroy", "aeo_mg_levels", "aeo_mg_solve", "aeo_mg_solve_device",
+    "aeo_mg_vcycle_solve", "aeo_mg_apply", "aeo_mg_precondition", "aeo_mg_profile",
+    "aeo_mg_launches_per_iteration", "aeo_mg_last_error",
 )
 
 
@@ -53,6 +56,22 @@ class AeoAdaptiveStats(C.Structure):
         ("advective_rate", C.c_double), ("nut_max", C.c_double), ("brunt_vaisala", C.c_double),
         ("max_divergence", C.c_double), ("max_speed", C.c_double),
     ]
+
+
+class AeoMgConfig(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+        ("bc_x", C.c_int32), ("bc_y", C.c_int32), ("bc_z", C.c_int32),
+        ("precision", C.c_int32), ("precond", C.c_int32), ("flexible", C.c_int32),
+        ("tol", C.c_double), ("maxit", C.c_int32), ("nu1", C.c_int32), ("nu2", C.c_int32),
+        ("coarse_sweeps", C.c_int32), ("min_size", C.c_int32), ("device", C.c_int32),
+    ]
+
+
+class AeoMgStats(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("status", C.c_int32), ("residual", C.c_double),
+                ("bnorm", C.c_double), ("curvature", C.c_double)]
 
 
 LIMITERS = ("advective", "diffusive", "buoyancy", "coriolis", "sgs", "growth", "dt_min", "dt_max", "retried")
@@ -113,19 +132,31 @@ def load():
     lib.aeo_last_error.argtypes = [P]
     lib.aeo_last_error.restype = C.c_char_p
     lib.aeo_version.restype = C.c_char_p
+    lib.aeo_mg_create.argtypes = [C.POINTER(AeoMgConfig), D, D, D, C.POINTER(P)]
+    lib.aeo_mg_destroy.argtypes = [P]
+    lib.aeo_mg_levels.argtypes = [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    for f in (lib.aeo_mg_solve, lib.aeo_mg_vcycle_solve):
+        f.argtypes = [P, D, D, C.POINTER(AeoMgStats)]
+    lib.aeo_mg_solve_device.argtypes = [P, P, P, C.POINTER(AeoMgStats)]
+    lib.aeo_mg_apply.argtypes = [P, D, D]
+    lib.aeo_mg_precondition.argtypes = [P, D, D]
+    lib.aeo_mg_profile.argtypes = [P, C.c_int32, C.c_int32, D]
+    lib.aeo_mg_launches_per_iteration.argtypes = [P]
+    lib.aeo_mg_last_error.argtypes = [P]
+    lib.aeo_mg_last_error.restype = C.c_char_p
     for s in SYMBOLS:
         f = getattr(lib, s)
-        if s not in ("aeo_stream", "aeo_last_error", "aeo_version"):
+        if s not in ("aeo_stream", "aeo_last_error", "aeo_version", "aeo_mg_last_error"):
             f.restype = C.c_int32
     _lib = lib
     return lib
 
 
-def check(status: int, handle=None):
+def check(status: int, handle=None, mg=False):
     if status == 0:
         return
     lib = load()
-    msg = lib.aeo_last_error(handle).decode(errors="replace")
+    msg = (lib.aeo_mg_last_error if mg else lib.aeo_last_error)(handle).decode(errors="replace")
     if status == 3:
         raise NumericalFailure(status, msg)
     if status == 1:
