@@ -24,8 +24,13 @@
 //     Neumann mirror), exact for the even dimensions of every level that is
 //     not the coarsest;
 //   * the coarsest level runs all its sweeps in one thread block with its
-//     arrays in shared memory, each colour pass computed before it is
-//     written, which is the reference's halo-copy semantics at any parity;
+//     arrays in shared memory (threads own columns; colour passes in place,
+//     or double-buffered where a periodic axis of odd length would join two
+//     cells of one colour), the reference's halo-copy semantics at any parity;
+//   * face coefficients with at most 256 distinct values (the sampled
+//     apertures of a cut-cell geometry) are stored as one-byte codes into a
+//     table of the values themselves: the same operator at 3 bytes per cell
+//     instead of 12 (FP32) or 24 (FP64);
 //   * the first half-sweep of a level that starts from zero is pointwise
 //     (every neighbour is zero), so it is fused with the zeroing and with
 //     the mean projection of the level's right-hand side;
@@ -37,608 +42,23 @@
 //     right-hand side are kept.
 #include <cuda_runtime.h>
 
-#include <cfloat>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <new>
 #include <string>
 #include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/aeolus_b200_mgpcg.h"
+#include "aeo_mg_kernels.cuh"
 
 namespace {
 
-constexpr int TPB = 256;
-constexpr int RED_BLOCKS = 592;        // 4 x 148 SMs: the fixed grid of every FP64 reduction
-constexpr int COARSE_THREADS = 1024;
-constexpr int COARSE_MAX_CELLS = 16384;
-constexpr int COARSE_PER_THREAD = COARSE_MAX_CELLS / COARSE_THREADS;
+using namespace mgk;
+
 constexpr int MAX_LEVELS = 24;
-
-template <typename R> struct Eps;
-template <> struct Eps<double> { static __device__ __host__ double v() { return DBL_EPSILON; } };
-template <> struct Eps<float> { static __device__ __host__ float v() { return FLT_EPSILON; } };
-
-struct Bc { int x, y, z; };            // 0 periodic, 1 Neumann
-
-// Device scalars of one solve.  Written only by last blocks of reductions
-// and read by every block of the next kernels.
-struct PcgState {
-    double tol, n;
-    double mb, bnorm, rz, pAp, alpha, beta, m, mr, rnorm, curvature, mx, rel;
-    int iters, maxit, status, done;
-    int project, flexible;
-    unsigned counter;
-};
-
-template <typename R> struct Level {
-    int nx, ny, nz;
-    long long n;
-    R ix2, iy2, iz2;
-    R* phi;
-    R* b;
-    const R* cx;                        // nullptr: constant-coefficient Laplacian
-    const R* cy;
-    const R* cz;
-    double* bmean;                      // mean of b to subtract before use (device scalar)
-};
-
-__device__ __forceinline__ int wm(int i, int n, int bc) { return i > 0 ? i - 1 : (bc == 0 ? n - 1 : 0); }
-__device__ __forceinline__ int wp(int i, int n, int bc) { return i < n - 1 ? i + 1 : (bc == 0 ? 0 : n - 1); }
-
-// Neighbour and face indices of cell (i, j, k) of an nx x ny x nz level.
-struct Idx {
-    long long q, xm, xp, ym, yp, zm, zp, cx, cy;
-    long long sy, sz;                   // cy north offset (nx), cz top offset (nx*ny)
-};
-
-__device__ __forceinline__ Idx make_idx(int i, int j, int k, int nx, int ny, int nz, Bc bc) {
-    Idx d;
-    long long row = (long long)nx * ((long long)j + (long long)ny * k);
-    d.q = row + i;
-    d.xm = row + wm(i, nx, bc.x);
-    d.xp = row + wp(i, nx, bc.x);
-    long long pl = (long long)nx * ny * k;
-    d.ym = pl + (long long)nx * wm(j, ny, bc.y) + i;
-    d.yp = pl + (long long)nx * wp(j, ny, bc.y) + i;
-    long long cj = (long long)nx * j + i;
-    d.zm = (long long)nx * ny * wm(k, nz, bc.z) + cj;
-    d.zp = (long long)nx * ny * wp(k, nz, bc.z) + cj;
-    d.cx = (long long)i + (long long)(nx + 1) * ((long long)j + (long long)ny * k);
-    d.cy = (long long)i + (long long)nx * ((long long)j + (long long)(ny + 1) * k);
-    d.sy = nx;
-    d.sz = (long long)nx * ny;
-    return d;
-}
-
-// _Aphi of _ConstOp / _VarOp (src/Multigrid.jl:174-193) in the value type V
-// with coefficients of type C.
-template <typename V, typename C>
-__device__ __forceinline__ V aphi(const V* f, const Idx& d, const C* cx, const C* cy, const C* cz, V ix2, V iy2,
-                                  V iz2) {
-    V c = f[d.q];
-    if (cx == nullptr)
-        return (f[d.xp] - V(2) * c + f[d.xm]) * ix2 + (f[d.yp] - V(2) * c + f[d.ym]) * iy2 +
-               (f[d.zp] - V(2) * c + f[d.zm]) * iz2;
-    V fxp = V(cx[d.cx + 1]), fxm = V(cx[d.cx]);
-    V fyp = V(cy[d.cy + d.sy]), fym = V(cy[d.cy]);
-    V fzp = V(cz[d.q + d.sz]), fzm = V(cz[d.q]);
-    return (fxp * (f[d.xp] - c) - fxm * (c - f[d.xm])) * ix2 + (fyp * (f[d.yp] - c) - fym * (c - f[d.ym])) * iy2 +
-           (fzp * (f[d.zp] - c) - fzm * (c - f[d.zm])) * iz2;
-}
-
-// One RB-GS update of cell d (src/Multigrid.jl:311-336); false: a fully
-// blocked cell (|diag| < eps), left unchanged.
-template <typename R>
-__device__ __forceinline__ bool gs_value(const R* f, R bval, const Idx& d, const Level<R>& L, R* out) {
-    R off, diag;
-    if (L.cx == nullptr) {
-        diag = -R(2) * (L.ix2 + L.iy2 + L.iz2);
-        off = (f[d.xp] + f[d.xm]) * L.ix2 + (f[d.yp] + f[d.ym]) * L.iy2 + (f[d.zp] + f[d.zm]) * L.iz2;
-    } else {
-        R fxp = L.cx[d.cx + 1], fxm = L.cx[d.cx];
-        R fyp = L.cy[d.cy + d.sy], fym = L.cy[d.cy];
-        R fzp = L.cz[d.q + d.sz], fzm = L.cz[d.q];
-        diag = -((fxp + fxm) * L.ix2 + (fyp + fym) * L.iy2 + (fzp + fzm) * L.iz2);
-        if (fabs(diag) < Eps<R>::v()) return false;
-        off = (fxp * f[d.xp] + fxm * f[d.xm]) * L.ix2 + (fyp * f[d.yp] + fym * f[d.ym]) * L.iy2 +
-              (fzp * f[d.zp] + fzm * f[d.zm]) * L.iz2;
-    }
-    *out = (bval - off) / diag;
-    return true;
-}
-
-// The diagonal alone (first half-sweep from zero: every neighbour is zero)
-template <typename R>
-__device__ __forceinline__ bool gs_diag(const Idx& d, const Level<R>& L, R* diag) {
-    if (L.cx == nullptr) {
-        *diag = -R(2) * (L.ix2 + L.iy2 + L.iz2);
-        return true;
-    }
-    R fxp = L.cx[d.cx + 1], fxm = L.cx[d.cx];
-    R fyp = L.cy[d.cy + d.sy], fym = L.cy[d.cy];
-    R fzp = L.cz[d.q + d.sz], fzm = L.cz[d.q];
-    *diag = -((fxp + fxm) * L.ix2 + (fyp + fym) * L.iy2 + (fzp + fzm) * L.iz2);
-    return !(fabs(*diag) < Eps<R>::v());
-}
-
-// ---------------------------------------------------------------- reductions
-
-__device__ __forceinline__ double warp_sum(double v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// Block sum of K values, valid in thread 0; fixed order (deterministic).
-template <int K>
-__device__ __forceinline__ void block_sum(double (&v)[K]) {
-    __shared__ double sh[K][32];
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-    for (int q = 0; q < K; ++q) v[q] = warp_sum(v[q]);
-    if (l == 0)
-#pragma unroll
-        for (int q = 0; q < K; ++q) sh[q][w] = v[q];
-    __syncthreads();
-    if (w == 0) {
-#pragma unroll
-        for (int q = 0; q < K; ++q) v[q] = warp_sum(l < nw ? sh[q][l] : 0.0);
-    }
-    __syncthreads();
-}
-
-// Stores this block's partials; the last block to arrive folds all of them
-// in block order and returns true with the totals in thread 0's `tot`.
-template <int K>
-__device__ bool reduce_last(double (&v)[K], double* part, unsigned* counter, double (&tot)[K]) {
-    __shared__ bool last;
-    block_sum<K>(v);
-    const int nb = gridDim.x;
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int q = 0; q < K; ++q) part[q * nb + blockIdx.x] = v[q];
-        __threadfence();
-        unsigned t = atomicAdd(counter, 1u);
-        last = (t == (unsigned)nb - 1);
-    }
-    __syncthreads();
-    if (!last) return false;
-    __threadfence();
-    double a[K];
-#pragma unroll
-    for (int q = 0; q < K; ++q) a[q] = 0.0;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x)
-#pragma unroll
-        for (int q = 0; q < K; ++q) a[q] += __ldcg(&part[q * nb + b]);
-    block_sum<K>(a);
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int q = 0; q < K; ++q) tot[q] = a[q];
-        *counter = 0u;
-    }
-    return true;
-}
-
-// ------------------------------------------------------------ CG kernels
-// (pcg!/_pcg!, src/Backends.jl:1526-1589; definite = :negative)
-
-// sum of a -> S->mb (mode 0) or S->mx (mode 1), divided by n when the mean is projected
-__global__ void pcg_mean_kernel(const double* __restrict__ a, long long n, PcgState* S, double* part, int mode) {
-    double v[1] = {0.0};
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-        v[0] += a[q];
-    double t[1];
-    if (reduce_last<1>(v, part, &S->counter, t) && threadIdx.x == 0) {
-        double m = S->project ? t[0] / S->n : 0.0;
-        if (mode == 0) S->mb = m; else S->mx = m;
-    }
-}
-
-// r = b - mb (zero guess), x = 0; reduces (|b - mb|^2, sum r); zero rhs ends the solve
-__global__ void pcg_init_kernel(const double* __restrict__ b, double* __restrict__ r, double* __restrict__ x,
-                                long long n, PcgState* S, double* part) {
-    const double mb = S->mb;
-    double v[2] = {0.0, 0.0};
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-        double bv = b[q] - mb;
-        r[q] = bv;
-        x[q] = 0.0;
-        v[0] += bv * bv;
-        v[1] += bv;
-    }
-    double t[2];
-    if (reduce_last<2>(v, part, &S->counter, t) && threadIdx.x == 0) {
-        S->bnorm = sqrt(t[0]);
-        S->mr = S->project ? t[1] / S->n : 0.0;
-        S->iters = 0;
-        S->curvature = nan("");
-        S->rz = 0.0;
-        S->alpha = S->beta = 0.0;
-        if (S->bnorm == 0.0) {
-            S->status = AEO_MG_ZERO_RHS;
-            S->done = 3;
-        } else {
-            S->status = AEO_MG_MAXIT;
-            S->done = 0;
-        }
-    }
-}
-
-// Ap = A p with p.Ap; the last block forms alpha or flags a breakdown
-template <typename C>
-__global__ void pcg_apply_kernel(const double* __restrict__ p, double* __restrict__ Ap, const C* cx, const C* cy,
-                                 const C* cz, int nx, int ny, int nz, Bc bc, double ix2, double iy2, double iz2,
-                                 PcgState* S, double* part, int standalone) {
-    if (!standalone && S->done) return;
-    const long long n = (long long)nx * ny * nz;
-    double v[1] = {0.0};
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-        int i = (int)(q % nx);
-        long long t = q / nx;
-        int j = (int)(t % ny), k = (int)(t / ny);
-        Idx d = make_idx(i, j, k, nx, ny, nz, bc);
-        double a = aphi<double, C>(p, d, cx, cy, cz, ix2, iy2, iz2);
-        Ap[q] = a;
-        v[0] += p[q] * a;
-    }
-    double t[1];
-    if (reduce_last<1>(v, part, &S->counter, t) && threadIdx.x == 0 && !standalone) {
-        double pAp = t[0];
-        S->pAp = pAp;
-        S->curvature = pAp;
-        if (!(fabs(pAp) > DBL_EPSILON * fabs(S->rz))) {
-            S->status = AEO_MG_BREAKDOWN;
-            S->done = 2;
-        } else {
-            S->alpha = S->rz / pAp;
-        }
-    }
-}
-
-// x += alpha p, r -= alpha Ap; reduces (r.r, sum r); convergence test
-__global__ void pcg_update_kernel(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
-                                  const double* __restrict__ Ap, long long n, PcgState* S, double* part) {
-    if (S->done) return;
-    const double alpha = S->alpha;
-    double v[2] = {0.0, 0.0};
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-        x[q] = x[q] + alpha * p[q];
-        double rv = r[q] - alpha * Ap[q];
-        r[q] = rv;
-        v[0] += rv * rv;
-        v[1] += rv;
-    }
-    double t[2];
-    if (reduce_last<2>(v, part, &S->counter, t) && threadIdx.x == 0) {
-        S->iters += 1;
-        S->rnorm = sqrt(t[0]);
-        S->mr = S->project ? t[1] / S->n : 0.0;
-        if (S->rnorm <= S->tol * S->bnorm) {
-            S->status = AEO_MG_CONVERGED;
-            S->done = 1;
-        }
-    }
-}
-
-// after z = M r: (r.r, r.z, sum z, sum r, z.Ap, sum Ap); the deflation mean
-// m = sum z / n, (r.z) -= m sum r, and beta
-template <typename Z>
-__global__ void pcg_rz_kernel(const double* __restrict__ r, const Z* __restrict__ z, const double* __restrict__ Ap,
-                              long long n, PcgState* S, double* part, int first) {
-    if (S->done) return;
-    const bool flex = S->flexible && !first;
-    double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-        double rv = r[q], zv = double(z[q]);
-        v[0] += rv * rv;
-        v[1] += rv * zv;
-        v[2] += zv;
-        v[3] += rv;
-        if (flex) {
-            double a = Ap[q];
-            v[4] += zv * a;
-            v[5] += a;
-        }
-    }
-    double t[6];
-    if (reduce_last<6>(v, part, &S->counter, t) && threadIdx.x == 0) {
-        double m = S->project ? t[2] / S->n : 0.0;
-        double rzn = t[1];
-        if (S->project) rzn -= m * t[3];
-        S->m = m;
-        if (first) {
-            S->rz = rzn;
-            S->beta = 0.0;
-            S->rnorm = sqrt(t[0]);
-            if (S->rnorm <= S->tol * S->bnorm) {
-                S->status = AEO_MG_CONVERGED;
-                S->done = 1;
-            }
-        } else {
-            if (flex) {
-                double zAp = t[4] - (S->project ? m * t[5] : 0.0);
-                S->beta = -S->alpha * zAp / S->rz;
-            } else {
-                S->beta = rzn / S->rz;
-            }
-            S->rz = rzn;
-        }
-    }
-}
-
-// p = (z - m) + beta p  (p = z - m on the first pass)
-template <typename Z>
-__global__ void pcg_dir_kernel(double* __restrict__ p, const Z* __restrict__ z, long long n, const PcgState* S,
-                               int first) {
-    if (S->done) return;
-    const double m = S->m, beta = S->beta;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-        p[q] = first ? double(z[q]) - m : (double(z[q]) - m) + beta * p[q];
-}
-
-__global__ void pcg_cond_kernel(PcgState* S, cudaGraphConditionalHandle h, int mode) {
-    // mode 0: CG (continue while running and below the iteration cap);
-    // mode 1: multigrid cycles (continue while above tol and below the cap)
-    unsigned go = (S->done == 0 && S->iters < S->maxit) ? 1u : 0u;
-    if (mode == 0 && S->done == 0 && S->iters >= S->maxit) S->status = AEO_MG_MAXIT;
-    cudaGraphSetConditional(h, go);
-}
-
-__global__ void shift_kernel(double* __restrict__ x, long long n, const PcgState* S) {
-    const double m = S->mx;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-        x[q] = x[q] - m;
-}
-
-// ------------------------------------------------------- multigrid kernels
-
-// The first half-sweep of a level whose phi starts at zero: one thread per
-// pair of cells (2ih, 2ih+1) of a row.  b <- b - mean (the projection of
-// the level's right-hand side; level 0 takes b from the FP64 residual
-// r - mean r), phi <- (b - 0)/diag on colour-0 cells, 0 on colour-1 cells.
-template <typename R>
-__global__ void mg_first_kernel(Level<R> L, Bc bc, const double* __restrict__ r0, const double* mr0, const int* done) {
-    if (*done) return;
-    const int half = L.nx >> 1;
-    const long long total = (long long)half * L.ny * L.nz;
-    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= total) return;
-    int ih = (int)(t % half);
-    long long rest = t / half;
-    int j = (int)(rest % L.ny), k = (int)(rest / L.ny);
-    const double m0 = r0 ? *mr0 : 0.0;
-    const R m = r0 ? R(0) : R(*L.bmean);
-#pragma unroll
-    for (int s = 0; s < 2; ++s) {
-        int i = 2 * ih + s;
-        long long q = (long long)L.nx * ((long long)j + (long long)L.ny * k) + i;
-        R bv = r0 ? R(r0[q] - m0) : L.b[q] - m;
-        L.b[q] = bv;
-        R out = R(0);
-        if (((i + j + k) & 1) == 0) {
-            Idx d = make_idx(i, j, k, L.nx, L.ny, L.nz, bc);
-            R diag;
-            if (gs_diag<R>(d, L, &diag)) out = (bv - R(0)) / diag;
-        }
-        L.phi[q] = out;
-    }
-}
-
-// One colour pass of red-black Gauss-Seidel over an even-nx level.
-template <typename R>
-__global__ void mg_rbgs_kernel(Level<R> L, Bc bc, int colour, const int* done) {
-    if (done && *done) return;
-    const int half = L.nx >> 1;
-    const long long total = (long long)half * L.ny * L.nz;
-    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= total) return;
-    int ih = (int)(t % half);
-    long long rest = t / half;
-    int j = (int)(rest % L.ny), k = (int)(rest / L.ny);
-    int i = 2 * ih + ((j + k + colour) & 1);
-    Idx d = make_idx(i, j, k, L.nx, L.ny, L.nz, bc);
-    R v;
-    if (gs_value<R>(L.phi, L.b[d.q], d, L, &v)) L.phi[d.q] = v;
-}
-
-// Coarse b = mean of the eight fine residuals b - A phi (src/Multigrid.jl:
-// 380-406, formed here without storing the fine residual); the last block
-// stores the coarse mean that the coarse level subtracts before use.
-template <typename R>
-__global__ void mg_restrict_kernel(Level<R> F, Level<R> Cl, Bc bc, double* part, unsigned* counter, const int* done) {
-    if (done && *done) return;
-    const long long nc = Cl.n;
-    double v[1] = {0.0};
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nc; t += (long long)gridDim.x * blockDim.x) {
-        int I = (int)(t % Cl.nx);
-        long long rest = t / Cl.nx;
-        int J = (int)(rest % Cl.ny), K = (int)(rest / Cl.ny);
-        R s = R(0);
-#pragma unroll
-        for (int dk = 0; dk < 2; ++dk)
-#pragma unroll
-            for (int dj = 0; dj < 2; ++dj)
-#pragma unroll
-                for (int di = 0; di < 2; ++di) {
-                    Idx d = make_idx(2 * I + di, 2 * J + dj, 2 * K + dk, F.nx, F.ny, F.nz, bc);
-                    R rr = F.b[d.q] - aphi<R, R>(F.phi, d, F.cx, F.cy, F.cz, F.ix2, F.iy2, F.iz2);
-                    s += rr;
-                }
-        R bc_ = s * R(0.125);
-        Cl.b[t] = bc_;
-        v[0] += double(bc_);
-    }
-    double tot[1];
-    if (reduce_last<1>(v, part, counter, tot) && threadIdx.x == 0) *Cl.bmean = tot[0] / double(nc);
-}
-
-// phi_fine += trilinear (3/4, 1/4) interpolation of phi_coarse
-// (src/Multigrid.jl:412-455), the eight terms in the reference's order.
-template <typename R>
-__global__ void mg_prolong_kernel(Level<R> F, Level<R> Cl, Bc bc, const int* done) {
-    if (done && *done) return;
-    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= F.n) return;
-    int i = (int)(t % F.nx);
-    long long rest = t / F.nx;
-    int j = (int)(rest % F.ny), k = (int)(rest / F.ny);
-    int Ih = i >> 1, Jh = j >> 1, Kh = k >> 1;
-    int Ix = (i & 1) ? wp(Ih, Cl.nx, bc.x) : wm(Ih, Cl.nx, bc.x);
-    int Jy = (j & 1) ? wp(Jh, Cl.ny, bc.y) : wm(Jh, Cl.ny, bc.y);
-    int Kz = (k & 1) ? wp(Kh, Cl.nz, bc.z) : wm(Kh, Cl.nz, bc.z);
-    const R n_ = R(3) / R(4), f_ = R(1) / R(4);
-    const long long sx = 1, sy = Cl.nx, sz = (long long)Cl.nx * Cl.ny;
-    const R* P = Cl.phi;
-    long long hhh = Ih * sx + Jh * sy + Kh * sz;
-    R acc = R(0);
-    acc += (n_ * n_ * n_) * P[hhh];
-    acc += (f_ * n_ * n_) * P[Ix * sx + Jh * sy + Kh * sz];
-    acc += (n_ * f_ * n_) * P[Ih * sx + Jy * sy + Kh * sz];
-    acc += (f_ * f_ * n_) * P[Ix * sx + Jy * sy + Kh * sz];
-    acc += (n_ * n_ * f_) * P[Ih * sx + Jh * sy + Kz * sz];
-    acc += (f_ * n_ * f_) * P[Ix * sx + Jh * sy + Kz * sz];
-    acc += (n_ * f_ * f_) * P[Ih * sx + Jy * sy + Kz * sz];
-    acc += (f_ * f_ * f_) * P[Ix * sx + Jy * sy + Kz * sz];
-    F.phi[t] += acc;
-}
-
-// The coarsest level: phi = 0, b -= mean, then `sweeps` RB-GS sweeps, all
-// in one block (_solve_coarsest!, src/Multigrid.jl:681-685).  Arrays are
-// staged in shared memory when they fit.  Each colour pass computes every
-// new value before any is written, the semantics of the reference's halo
-// copy even where a periodic wrap joins two cells of one colour.
-template <typename R>
-__global__ void __launch_bounds__(COARSE_THREADS) mg_coarsest_kernel(Level<R> L, Bc bc, int sweeps, int staged,
-                                                                    const double* __restrict__ r0, const double* mr0,
-                                                                    const int* done) {
-    if (done && *done) return;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int nx = L.nx, ny = L.ny, nz = L.nz;
-    const int n = (int)L.n;
-    const int ncx = (nx + 1) * ny * nz, ncy = nx * (ny + 1) * nz, ncz = nx * ny * (nz + 1);
-    Level<R> S = L;
-    if (staged) {
-        R* base = reinterpret_cast<R*>(smem_raw);
-        S.phi = base;
-        S.b = base + n;
-        if (L.cx) {
-            R* c = base + 2 * n;
-            for (int q = threadIdx.x; q < ncx; q += blockDim.x) c[q] = L.cx[q];
-            for (int q = threadIdx.x; q < ncy; q += blockDim.x) c[ncx + q] = L.cy[q];
-            for (int q = threadIdx.x; q < ncz; q += blockDim.x) c[ncx + ncy + q] = L.cz[q];
-            S.cx = c;
-            S.cy = c + ncx;
-            S.cz = c + ncx + ncy;
-        }
-    }
-    const double m0 = r0 ? *mr0 : 0.0;
-    const R m = r0 ? R(0) : R(*L.bmean);
-    for (int q = threadIdx.x; q < n; q += blockDim.x) {
-        S.b[q] = r0 ? R(r0[q] - m0) : L.b[q] - m;
-        S.phi[q] = R(0);
-    }
-    __syncthreads();
-    R nv[COARSE_PER_THREAD];
-    for (int sw = 0; sw < sweeps; ++sw)
-        for (int colour = 0; colour < 2; ++colour) {
-#pragma unroll
-            for (int s = 0; s < COARSE_PER_THREAD; ++s) {
-                int q = threadIdx.x + s * COARSE_THREADS;
-                nv[s] = R(0);
-                if (q < n) {
-                    int i = q % nx, j = (q / nx) % ny, k = q / (nx * ny);
-                    Idx d = make_idx(i, j, k, nx, ny, nz, bc);
-                    R v = S.phi[q];
-                    if (((i + j + k) & 1) == colour) gs_value<R>(S.phi, S.b[q], d, S, &v);
-                    nv[s] = v;
-                }
-            }
-            __syncthreads();
-#pragma unroll
-            for (int s = 0; s < COARSE_PER_THREAD; ++s) {
-                int q = threadIdx.x + s * COARSE_THREADS;
-                if (q < n) S.phi[q] = nv[s];
-            }
-            __syncthreads();
-        }
-    if (staged)
-        for (int q = threadIdx.x; q < n; q += blockDim.x) L.phi[q] = S.phi[q];
-}
-
-// Level-0 right-hand side for the standalone cycles: b0 = r - mean(r)
-template <typename R>
-__global__ void mg_load_kernel(Level<R> L, const double* __restrict__ r0, const double* mr0) {
-    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= L.n) return;
-    L.b[t] = R(r0[t] - *mr0);
-    L.phi[t] = R(0);
-}
-
-// relative residual of the standalone cycles (_residual_norm!,
-// src/Multigrid.jl:780-785): |r - mean r| / |b| from sum r and sum r^2
-template <typename R>
-__global__ void mg_resnorm_kernel(Level<R> L, Bc bc, PcgState* S, double* part) {
-    if (S->done) return;
-    double v[2] = {0.0, 0.0};
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < L.n; t += (long long)gridDim.x * blockDim.x) {
-        int i = (int)(t % L.nx);
-        long long rest = t / L.nx;
-        int j = (int)(rest % L.ny), k = (int)(rest / L.ny);
-        Idx d = make_idx(i, j, k, L.nx, L.ny, L.nz, bc);
-        double rr = double(L.b[t] - aphi<R, R>(L.phi, d, L.cx, L.cy, L.cz, L.ix2, L.iy2, L.iz2));
-        v[0] += rr;
-        v[1] += rr * rr;
-    }
-    double tot[2];
-    if (reduce_last<2>(v, part, &S->counter, tot) && threadIdx.x == 0) {
-        double ss = tot[1];
-        if (S->project) ss -= tot[0] * (tot[0] / S->n);
-        S->iters += 1;
-        S->rel = sqrt(fmax(ss, 0.0)) / S->bnorm;
-        S->rnorm = S->rel;
-        if (S->rel < S->tol) {
-            S->status = AEO_MG_CONVERGED;
-            S->done = 1;
-        }
-    }
-}
-
-// phi0 -> x (FP64) after the cycles; the mean removed by shift_kernel
-template <typename R>
-__global__ void mg_store_kernel(Level<R> L, double* __restrict__ x) {
-    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= L.n) return;
-    x[t] = double(L.phi[t]);
-}
-
-// |b0| of the standalone cycles; zero rhs ends before the first cycle
-template <typename R>
-__global__ void mg_bnorm_kernel(Level<R> L, PcgState* S, double* part) {
-    double v[1] = {0.0};
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < L.n; t += (long long)gridDim.x * blockDim.x) {
-        double bv = double(L.b[t]);
-        v[0] += bv * bv;
-    }
-    double tot[1];
-    if (reduce_last<1>(v, part, &S->counter, tot) && threadIdx.x == 0) {
-        S->bnorm = sqrt(tot[0]);
-        S->iters = 0;
-        S->rel = 1.0;
-        S->curvature = nan("");
-        if (S->bnorm == 0.0) {
-            S->status = AEO_MG_ZERO_RHS;
-            S->done = 3;
-        } else {
-            S->status = AEO_MG_MAXIT;
-            S->done = 0;
-        }
-    }
-}
-
-// ------------------------------------------------------------- host side
-
-int blocks_for(long long n) { return (int)((n + TPB - 1) / TPB); }
 
 struct MgBase {
     aeo_mg_config cfg{};
@@ -716,31 +136,67 @@ void restrict_coeff(int nx, int ny, int nz, const std::vector<double>& cx, const
             }
 }
 
-template <typename R, typename CT>
+// One-byte codes of a level's face coefficients when it holds at most 256
+// distinct values (the sampled apertures of a cut-cell geometry hold at most
+// nsub^2 + 1): tab[code] is the value itself, so the coded operator is
+// exactly the given one.
+bool encode(const std::vector<double>& x, const std::vector<double>& y, const std::vector<double>& z,
+            std::vector<double>& tab, std::vector<uint8_t>& kx, std::vector<uint8_t>& ky, std::vector<uint8_t>& kz) {
+    std::unordered_map<uint64_t, uint8_t> code;
+    tab.clear();
+    auto key = [](double v) {
+        uint64_t u;
+        std::memcpy(&u, &v, 8);
+        return u;
+    };
+    for (const std::vector<double>* a : {&x, &y, &z})
+        for (double v : *a) {
+            uint64_t u = key(v);
+            if (code.find(u) != code.end()) continue;
+            if (tab.size() == 256) return false;
+            code.emplace(u, (uint8_t)tab.size());
+            tab.push_back(v);
+        }
+    auto fill = [&](const std::vector<double>& a, std::vector<uint8_t>& k) {
+        k.resize(a.size());
+        for (size_t q = 0; q < a.size(); ++q) k[q] = code[key(a[q])];
+    };
+    fill(x, kx);
+    fill(y, ky);
+    fill(z, kz);
+    return true;
+}
+
+template <typename R>
 struct Mg : MgBase {
     cudaStream_t st = nullptr, st_body = nullptr;
     Bc bc{0, 0, 0};
     int nl = 0;
-    long long n = 0;
+    int n = 0;
     Level<R> L[MAX_LEVELS];
     std::vector<void*> allocs;
-    const CT *ocx = nullptr, *ocy = nullptr, *ocz = nullptr;   // operator coefficients (FP64 or exact FP32)
+    Coef<double> opd;              // the operator's coefficients, FP64 values or codes
+    Coef<float> opf;               // ... or FP32 values when every one is exact in FP32
+    bool op_f32 = false;
+    int coded_levels = 0;
     double *b = nullptr, *x = nullptr, *r = nullptr, *p = nullptr, *Ap = nullptr;
     double* part = nullptr;
+    size_t part_cap = 0;           // doubles in `part`
     double* bmeans = nullptr;      // one device scalar per level
     PcgState* S = nullptr;
     PcgState* hS = nullptr;        // pinned host copy
     int* dzero = nullptr;          // a device flag that stays 0 (kernels run outside a solve)
     int coarse_staged = 0;
+    int coarse_inplace = 1;        // 0 when a periodic axis of the coarsest level has an odd length
     size_t coarse_smem = 0;
-    cudaGraphExec_t g_solve = nullptr, g_cycles = nullptr, g_pc = nullptr;
+    R* coarse_spare = nullptr;     // the coarsest level's second buffer when not staged
+    cudaGraphExec_t g_solve = nullptr, g_cycles = nullptr;
     int body_launches = 0;
 
     ~Mg() override {
         if (st) cudaStreamSynchronize(st);
         if (g_solve) cudaGraphExecDestroy(g_solve);
         if (g_cycles) cudaGraphExecDestroy(g_cycles);
-        if (g_pc) cudaGraphExecDestroy(g_pc);
         for (void* a : allocs) cudaFree(a);
         if (hS) cudaFreeHost(hS);
         if (st) cudaStreamDestroy(st);
@@ -756,6 +212,16 @@ struct Mg : MgBase {
         return AEO_OK;
     }
 
+    template <typename T, typename S_>
+    aeo_status upload(const T** out, const std::vector<S_>& h) {
+        T* d;
+        if (aeo_status s = dalloc(&d, h.size())) return s;
+        std::vector<T> t(h.begin(), h.end());
+        CK(cudaMemcpy(d, t.data(), sizeof(T) * t.size(), cudaMemcpyHostToDevice));
+        *out = d;
+        return AEO_OK;
+    }
+
     int nlevels() const override { return nl; }
     void level_dims(int l, int32_t* d) const override {
         d[0] = L[l].nx;
@@ -764,6 +230,21 @@ struct Mg : MgBase {
     }
     int launches_per_iteration() const override { return body_launches; }
 
+    static dim3 half_grid(const Level<R>& F) {
+        return dim3((unsigned)((F.nx / 2 + RB_X - 1) / RB_X), (unsigned)((F.ny + RB_Y - 1) / RB_Y), (unsigned)F.nz);
+    }
+    static dim3 cell_grid(const Level<R>& F) {
+        return dim3((unsigned)((F.nx + RB_X - 1) / RB_X), (unsigned)((F.ny + RB_Y - 1) / RB_Y), (unsigned)F.nz);
+    }
+    static dim3 restrict_grid(const Level<R>& F, const Level<R>& Cl) {
+        return dim3((unsigned)((F.nx + 31) / 32), (unsigned)((F.ny + 7) / 8),
+                    (unsigned)((Cl.nz + RS_PAIRS - 1) / RS_PAIRS));
+    }
+    static int row_blocks(int rows) {
+        int b = (rows + RB_Y - 1) / RB_Y;
+        return b < RED_BLOCKS ? b : RED_BLOCKS;
+    }
+
     aeo_status init(const double* cx, const double* cy, const double* cz) override {
         bc = {cfg.bc_x, cfg.bc_y, cfg.bc_z};
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -771,71 +252,63 @@ struct Mg : MgBase {
         const bool coeff = cx != nullptr;
         int nx = cfg.nx, ny = cfg.ny, nz = cfg.nz;
         double dx = cfg.dx, dy = cfg.dy, dz = cfg.dz;
-        n = (long long)nx * ny * nz;
+        n = nx * ny * nz;
         std::vector<double> hx, hy, hz;
         if (coeff) {
             hx.assign(cx, cx + (size_t)(nx + 1) * ny * nz);
             hy.assign(cy, cy + (size_t)nx * (ny + 1) * nz);
             hz.assign(cz, cz + (size_t)nx * ny * (nz + 1));
         }
-        // the operator's coefficients: FP64, or FP32 when every value is exactly representable
-        if (coeff) {
-            bool exact = sizeof(CT) == sizeof(double);
-            if (!exact) {
-                exact = true;
-                for (const std::vector<double>* v : {&hx, &hy, &hz})
-                    for (double a : *v)
-                        if (double(float(a)) != a) { exact = false; break; }
-                if (!exact) {
-                    fail("internal: FP32 operator coefficients requested for inexact values");
-                    return AEO_ERR_STATE;
-                }
-            }
-            CT *ax, *ay, *az;
-            if (aeo_status s = dalloc(&ax, hx.size())) return s;
-            if (aeo_status s = dalloc(&ay, hy.size())) return s;
-            if (aeo_status s = dalloc(&az, hz.size())) return s;
-            std::vector<CT> t;
-            t.assign(hx.begin(), hx.end());
-            CK(cudaMemcpy(ax, t.data(), sizeof(CT) * t.size(), cudaMemcpyHostToDevice));
-            t.assign(hy.begin(), hy.end());
-            CK(cudaMemcpy(ay, t.data(), sizeof(CT) * t.size(), cudaMemcpyHostToDevice));
-            t.assign(hz.begin(), hz.end());
-            CK(cudaMemcpy(az, t.data(), sizeof(CT) * t.size(), cudaMemcpyHostToDevice));
-            ocx = ax; ocy = ay; ocz = az;
-        }
-        // the hierarchy (src/Multigrid.jl:572-591)
         if (aeo_status s = dalloc(&bmeans, MAX_LEVELS)) return s;
         CK(cudaMemset(bmeans, 0, sizeof(double) * MAX_LEVELS));
-        std::vector<double> Cx, Cy, Cz;
+        std::vector<double> Cx, Cy, Cz, tab;
+        std::vector<uint8_t> kx, ky, kz;
+        // the hierarchy (src/Multigrid.jl:572-591)
         while (true) {
             Level<R>& V = L[nl];
             V.nx = nx; V.ny = ny; V.nz = nz;
-            V.n = (long long)nx * ny * nz;
+            V.n = nx * ny * nz;
             V.ix2 = R(1) / (R(dx) * R(dx));   // one(T) / dx^2 (src/Multigrid.jl:162-164)
             V.iy2 = R(1) / (R(dy) * R(dy));
             V.iz2 = R(1) / (R(dz) * R(dz));
             if (aeo_status s = dalloc(&V.phi, V.n)) return s;
             if (aeo_status s = dalloc(&V.b, V.n)) return s;
             V.bmean = bmeans + nl;
-            V.cx = V.cy = V.cz = nullptr;
+            V.c = Coef<R>();
             if (coeff) {
-                if (nl == 0 && std::is_same<R, CT>::value) {
-                    V.cx = reinterpret_cast<const R*>(ocx);
-                    V.cy = reinterpret_cast<const R*>(ocy);
-                    V.cz = reinterpret_cast<const R*>(ocz);
+                if (encode(hx, hy, hz, tab, kx, ky, kz)) {
+                    if (aeo_status s = upload(&V.c.kx, kx)) return s;
+                    if (aeo_status s = upload(&V.c.ky, ky)) return s;
+                    if (aeo_status s = upload(&V.c.kz, kz)) return s;
+                    if (aeo_status s = upload(&V.c.tab, tab)) return s;
+                    ++coded_levels;
+                    if (nl == 0) {
+                        opd.kx = V.c.kx; opd.ky = V.c.ky; opd.kz = V.c.kz;
+                        if (aeo_status s = upload(&opd.tab, tab)) return s;
+                    }
                 } else {
-                    R *ax, *ay, *az;
-                    if (aeo_status s = dalloc(&ax, hx.size())) return s;
-                    if (aeo_status s = dalloc(&ay, hy.size())) return s;
-                    if (aeo_status s = dalloc(&az, hz.size())) return s;
-                    std::vector<R> t(hx.begin(), hx.end());
-                    CK(cudaMemcpy(ax, t.data(), sizeof(R) * t.size(), cudaMemcpyHostToDevice));
-                    t.assign(hy.begin(), hy.end());
-                    CK(cudaMemcpy(ay, t.data(), sizeof(R) * t.size(), cudaMemcpyHostToDevice));
-                    t.assign(hz.begin(), hz.end());
-                    CK(cudaMemcpy(az, t.data(), sizeof(R) * t.size(), cudaMemcpyHostToDevice));
-                    V.cx = ax; V.cy = ay; V.cz = az;
+                    if (aeo_status s = upload(&V.c.cx, hx)) return s;
+                    if (aeo_status s = upload(&V.c.cy, hy)) return s;
+                    if (aeo_status s = upload(&V.c.cz, hz)) return s;
+                    if (nl == 0) {
+                        bool exact = std::is_same<R, float>::value;
+                        for (const std::vector<double>* v : {&hx, &hy, &hz})
+                            for (size_t q = 0; exact && q < v->size(); ++q) exact = double(float((*v)[q])) == (*v)[q];
+                        if (exact) {
+                            op_f32 = true;
+                            opf.cx = reinterpret_cast<const float*>(V.c.cx);
+                            opf.cy = reinterpret_cast<const float*>(V.c.cy);
+                            opf.cz = reinterpret_cast<const float*>(V.c.cz);
+                        } else if (std::is_same<R, double>::value) {
+                            opd.cx = reinterpret_cast<const double*>(V.c.cx);
+                            opd.cy = reinterpret_cast<const double*>(V.c.cy);
+                            opd.cz = reinterpret_cast<const double*>(V.c.cz);
+                        } else {
+                            if (aeo_status s = upload(&opd.cx, hx)) return s;
+                            if (aeo_status s = upload(&opd.cy, hy)) return s;
+                            if (aeo_status s = upload(&opd.cz, hz)) return s;
+                        }
+                    }
                 }
             }
             ++nl;
@@ -857,19 +330,28 @@ struct Mg : MgBase {
                  std::to_string(COARSE_MAX_CELLS) + " one block solves: give nx, ny, nz more factors of two");
             return AEO_ERR_ARGUMENT;
         }
-        size_t cb = sizeof(R) * (2 * (size_t)C.n + (coeff ? (size_t)(C.nx + 1) * C.ny * C.nz +
+        size_t cb = sizeof(R) * (3 * (size_t)C.n + (coeff ? (size_t)(C.nx + 1) * C.ny * C.nz +
                                                           (size_t)C.nx * (C.ny + 1) * C.nz +
                                                           (size_t)C.nx * C.ny * (C.nz + 1) : 0));
         coarse_staged = cb <= 200 * 1024;
+        coarse_inplace = !((cfg.bc_x == AEO_MG_PERIODIC && C.nx % 2) || (cfg.bc_y == AEO_MG_PERIODIC && C.ny % 2) ||
+                           (cfg.bc_z == AEO_MG_PERIODIC && C.nz % 2));
         coarse_smem = coarse_staged ? cb : 0;
         if (coarse_smem > 48 * 1024)
             CK(cudaFuncSetAttribute(mg_coarsest_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_smem));
+        if (aeo_status s = dalloc(&coarse_spare, C.n)) return s;
         if (aeo_status s = dalloc(&b, n)) return s;
         if (aeo_status s = dalloc(&x, n)) return s;
         if (aeo_status s = dalloc(&r, n)) return s;
         if (aeo_status s = dalloc(&p, n)) return s;
         if (aeo_status s = dalloc(&Ap, n)) return s;
-        if (aeo_status s = dalloc(&part, (size_t)RED_BLOCKS * 8)) return s;
+        part_cap = (size_t)RED_BLOCKS * 8;
+        for (int l = 0; l + 1 < nl; ++l) {
+            dim3 g = restrict_grid(L[l], L[l + 1]);
+            size_t nb = (size_t)g.x * g.y * g.z;
+            if (nb > part_cap) part_cap = nb;
+        }
+        if (aeo_status s = dalloc(&part, part_cap)) return s;
         if (aeo_status s = dalloc(&S, 1)) return s;
         if (aeo_status s = dalloc(&dzero, 1)) return s;
         CK(cudaMemset(dzero, 0, sizeof(int)));
@@ -878,19 +360,23 @@ struct Mg : MgBase {
         h0.tol = cfg.tol;
         h0.n = double(n);
         h0.maxit = cfg.maxit;
-        h0.project = (cfg.bc_x == 0 || cfg.bc_x == 1) && (cfg.bc_y == 0 || cfg.bc_y == 1) &&
-                     (cfg.bc_z == 0 || cfg.bc_z == 1);
+        h0.project = 1;            // periodic / Neumann on every axis: always singular
         h0.flexible = cfg.flexible;
         CK(cudaMemcpy(S, &h0, sizeof(PcgState), cudaMemcpyHostToDevice));
-        CK(cudaMemset(part, 0, sizeof(double) * RED_BLOCKS * 8));
+        CK(cudaMemset(part, 0, sizeof(double) * part_cap));
         return AEO_OK;
     }
 
-    // ---- launch helpers (stream s) ----
     aeo_status launch_apply(cudaStream_t s, const double* in, double* out, int standalone) {
         const double ix2 = 1.0 / (cfg.dx * cfg.dx), iy2 = 1.0 / (cfg.dy * cfg.dy), iz2 = 1.0 / (cfg.dz * cfg.dz);
-        pcg_apply_kernel<CT><<<RED_BLOCKS, TPB, 0, s>>>(in, out, ocx, ocy, ocz, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2,
-                                                        iz2, S, part, standalone);
+        const dim3 blk(RB_X, RB_Y);
+        const int nb = row_blocks(cfg.ny * cfg.nz);
+        if (op_f32)
+            pcg_apply_kernel<float><<<nb, blk, 0, s>>>(in, out, opf, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2, iz2, S,
+                                                       part, standalone);
+        else
+            pcg_apply_kernel<double><<<nb, blk, 0, s>>>(in, out, opd, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2, iz2, S,
+                                                        part, standalone);
         CKL();
         return AEO_OK;
     }
@@ -901,62 +387,62 @@ struct Mg : MgBase {
         return c;
     }
 
-    // One V-cycle from phi = 0 with level-0 right-hand side r0 - mean (mg_vcycle!,
-    // src/Multigrid.jl:706-739).  from_zero = false: level 0 keeps its phi and b
-    // (the standalone cycles).
+    aeo_status launch_coarsest(cudaStream_t s, Level<R>& C, const double* r0, const int* done) {
+        mg_coarsest_kernel<R><<<1, COARSE_THREADS, coarse_smem, s>>>(C, coarse_spare, bc, cfg.coarse_sweeps,
+                                                                     coarse_staged, coarse_inplace, r0, &S->mr, done);
+        CKL();
+        return AEO_OK;
+    }
+
+    // One V-cycle from phi = 0 with level-0 right-hand side r0 - mean
+    // (mg_vcycle!, src/Multigrid.jl:706-739); from_zero = false: level 0
+    // keeps its phi and b (the standalone cycles).
     aeo_status launch_vcycle(cudaStream_t s, const double* r0, bool from_zero, const int* done) {
         const double* mr = &S->mr;
+        const dim3 blk(RB_X, RB_Y);
         if (nl == 1) {
             if (!from_zero) {
-                fail("internal: standalone cycles on a one-level hierarchy");
-                return AEO_ERR_STATE;
+                fail("standalone multigrid cycles need at least two levels");
+                return AEO_ERR_ARGUMENT;
             }
-            mg_coarsest_kernel<R><<<1, COARSE_THREADS, coarse_smem, s>>>(L[0], bc, cfg.coarse_sweeps, coarse_staged,
-                                                                         r0, mr, done);
-            CKL();
-            return AEO_OK;
+            return launch_coarsest(s, L[0], r0, done);
         }
         for (int l = 0; l < nl - 1; ++l) {
             Level<R>& F = L[l];
-            const int hb = blocks_for((long long)(F.nx / 2) * F.ny * F.nz);
+            const dim3 hg = half_grid(F);
             int sw0 = 0;
             if (l > 0 || from_zero) {
-                mg_first_kernel<R><<<hb, TPB, 0, s>>>(F, bc, l == 0 ? r0 : nullptr, mr, done);
+                mg_first_kernel<R><<<hg, blk, 0, s>>>(F, bc, l == 0 ? r0 : nullptr, mr, done);
                 CKL();
-                mg_rbgs_kernel<R><<<hb, TPB, 0, s>>>(F, bc, 1, done);
+                mg_rbgs_kernel<R><<<hg, blk, 0, s>>>(F, bc, 1, done);
                 CKL();
                 sw0 = 1;
             }
             for (int sw = sw0; sw < cfg.nu1; ++sw)
                 for (int c = 0; c < 2; ++c) {
-                    mg_rbgs_kernel<R><<<hb, TPB, 0, s>>>(F, bc, c, done);
+                    mg_rbgs_kernel<R><<<hg, blk, 0, s>>>(F, bc, c, done);
                     CKL();
                 }
             Level<R>& Cl = L[l + 1];
-            int rb = blocks_for(Cl.n);
-            if (rb > RED_BLOCKS) rb = RED_BLOCKS;
-            mg_restrict_kernel<R><<<rb, TPB, 0, s>>>(F, Cl, bc, part, &S->counter, done);
+            mg_restrict_kernel<R><<<restrict_grid(F, Cl), dim3(32, 8, 2), 0, s>>>(F, Cl, bc, part, &S->counter, done);
             CKL();
         }
-        Level<R>& C = L[nl - 1];
-        mg_coarsest_kernel<R><<<1, COARSE_THREADS, coarse_smem, s>>>(C, bc, cfg.coarse_sweeps, coarse_staged, nullptr,
-                                                                     mr, done);
-        CKL();
+        if (aeo_status q = launch_coarsest(s, L[nl - 1], nullptr, done)) return q;
         for (int l = nl - 2; l >= 0; --l) {
             Level<R>& F = L[l];
-            mg_prolong_kernel<R><<<blocks_for(F.n), TPB, 0, s>>>(F, L[l + 1], bc, done);
+            mg_prolong_kernel<R><<<cell_grid(F), blk, 0, s>>>(F, L[l + 1], bc, done);
             CKL();
-            const int hb = blocks_for((long long)(F.nx / 2) * F.ny * F.nz);
+            const dim3 hg = half_grid(F);
             for (int sw = 0; sw < cfg.nu2; ++sw)
                 for (int c = 0; c < 2; ++c) {
-                    mg_rbgs_kernel<R><<<hb, TPB, 0, s>>>(F, bc, c, done);
+                    mg_rbgs_kernel<R><<<hg, blk, 0, s>>>(F, bc, c, done);
                     CKL();
                 }
         }
         return AEO_OK;
     }
 
-    // the preconditioned residual z: level-0 phi, or r itself for plain CG
+    // z: level-0 phi after the cycle, or r itself for plain CG
     aeo_status launch_rz_dir(cudaStream_t s, int first) {
         if (cfg.precond == AEO_PC_VCYCLE) {
             pcg_rz_kernel<R><<<RED_BLOCKS, TPB, 0, s>>>(r, L[0].phi, Ap, n, S, part, first);
@@ -985,8 +471,9 @@ struct Mg : MgBase {
         return AEO_OK;
     }
 
-    // Adds a WHILE node on `hdl` to the graph being captured on `st`, captures
-    // `body` into its body graph on st_body, and continues the capture after it.
+    // Adds a WHILE node on `hdl` to the graph being captured on `st`,
+    // captures `body` into its body graph on st_body, and continues the
+    // capture after it.
     template <typename F>
     aeo_status capture_while(cudaGraphConditionalHandle hdl, F body) {
         cudaStreamCaptureStatus cs;
@@ -1040,9 +527,9 @@ struct Mg : MgBase {
         return AEO_OK;
     }
 
-    // The solve graph: prologue, WHILE(one CG iteration), mean shift.  The
-    // loop's condition is set by pcg_cond_kernel before the loop and at the
-    // end of every iteration.
+    // The solve graph: prologue, WHILE(one CG iteration), the mean shift.
+    // The loop condition is set by pcg_cond_kernel before the loop and at
+    // the end of every iteration.
     aeo_status build_solve() {
         CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
         aeo_status s = [&]() -> aeo_status {
@@ -1074,19 +561,13 @@ struct Mg : MgBase {
                     return AEO_OK;
                 }))
                 return q;
-            if (S_project()) {
-                pcg_mean_kernel<<<RED_BLOCKS, TPB, 0, st>>>(x, n, S, part, 1);
-                CKL();
-                shift_kernel<<<RED_BLOCKS, TPB, 0, st>>>(x, n, S);
-                CKL();
-            }
+            pcg_mean_kernel<<<RED_BLOCKS, TPB, 0, st>>>(x, n, S, part, 1);
+            CKL();
+            shift_kernel<<<RED_BLOCKS, TPB, 0, st>>>(x, n, S);
+            CKL();
             return AEO_OK;
         }();
         return end_capture(&g_solve, s);
-    }
-
-    bool S_project() const {
-        return (cfg.bc_x == 0 || cfg.bc_x == 1) && (cfg.bc_y == 0 || cfg.bc_y == 1) && (cfg.bc_z == 0 || cfg.bc_z == 1);
     }
 
     aeo_status stats_out(aeo_mg_stats* o, bool relative) {
@@ -1123,7 +604,8 @@ struct Mg : MgBase {
             if (aeo_status q = make_handle(&hdl)) return q;
             pcg_mean_kernel<<<RED_BLOCKS, TPB, 0, st>>>(b, n, S, part, 0);
             CKL();
-            mg_load_kernel_launch(st);
+            // b0 = b - mean(b) (_load_rhs!), phi0 = 0
+            mg_load_kernel<R><<<RED_BLOCKS, TPB, 0, st>>>(L[0], b, &S->mb);
             CKL();
             mg_bnorm_kernel<R><<<RED_BLOCKS, TPB, 0, st>>>(L[0], S, part);
             CKL();
@@ -1131,29 +613,22 @@ struct Mg : MgBase {
             CKL();
             if (aeo_status q = capture_while(hdl, [&](cudaStream_t sb) -> aeo_status {
                     if (aeo_status q2 = launch_vcycle(sb, nullptr, false, &S->done)) return q2;
-                    mg_resnorm_kernel<R><<<RED_BLOCKS, TPB, 0, sb>>>(L[0], bc, S, part);
+                    mg_resnorm_kernel<R><<<row_blocks(cfg.ny * cfg.nz), dim3(RB_X, RB_Y), 0, sb>>>(L[0], bc, S, part);
                     CKL();
                     pcg_cond_kernel<<<1, 1, 0, sb>>>(S, hdl, 1);
                     CKL();
                     return AEO_OK;
                 }))
                 return q;
-            mg_store_kernel<R><<<blocks_for(n), TPB, 0, st>>>(L[0], x);
+            mg_store_kernel<R><<<RED_BLOCKS, TPB, 0, st>>>(L[0], x);
             CKL();
-            if (S_project()) {
-                pcg_mean_kernel<<<RED_BLOCKS, TPB, 0, st>>>(x, n, S, part, 1);
-                CKL();
-                shift_kernel<<<RED_BLOCKS, TPB, 0, st>>>(x, n, S);
-                CKL();
-            }
+            pcg_mean_kernel<<<RED_BLOCKS, TPB, 0, st>>>(x, n, S, part, 1);
+            CKL();
+            shift_kernel<<<RED_BLOCKS, TPB, 0, st>>>(x, n, S);
+            CKL();
             return AEO_OK;
         }();
         return end_capture(&g_cycles, s);
-    }
-
-    void mg_load_kernel_launch(cudaStream_t s) {
-        // b0 = b - mean(b) (the loaded right-hand side, _load_rhs!), phi0 = 0
-        mg_load_kernel<R><<<blocks_for(n), TPB, 0, s>>>(L[0], b, &S->mb);
     }
 
     aeo_status cycles(const double* bin, double* xout, aeo_mg_stats* o) override {
@@ -1173,8 +648,8 @@ struct Mg : MgBase {
         return AEO_OK;
     }
 
-    // z = M r: the load of r with its mean (as the solve's prologue), one cycle,
-    // then z - mean(z) on the host side of the copy
+    // z = M r: r loaded with its mean removed (as in the solve), one cycle,
+    // then z - mean(z) (the deflated preconditioner of the reference)
     aeo_status precondition(const double* rin, double* zout) override {
         if (cfg.precond != AEO_PC_VCYCLE) {
             std::memcpy(zout, rin, sizeof(double) * n);
@@ -1184,19 +659,16 @@ struct Mg : MgBase {
             CKL();
             pcg_init_kernel<<<RED_BLOCKS, TPB, 0, st>>>(b, r, x, n, S, part);
             CKL();
-            // pcg_init stored mean(r) in S->mr; the cycle runs even for a zero r
             if (aeo_status s = launch_vcycle(st, r, true, dzero)) return s;
             std::vector<R> hz((size_t)n);
             CK(cudaMemcpyAsync(hz.data(), L[0].phi, sizeof(R) * n, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
-            for (long long q = 0; q < n; ++q) zout[q] = double(hz[q]);
+            for (int q = 0; q < n; ++q) zout[q] = double(hz[q]);
         }
-        if (S_project()) {
-            double s = 0;
-            for (long long q = 0; q < n; ++q) s += zout[q];
-            s /= double(n);
-            for (long long q = 0; q < n; ++q) zout[q] -= s;
-        }
+        double s = 0;
+        for (int q = 0; q < n; ++q) s += zout[q];
+        s /= double(n);
+        for (int q = 0; q < n; ++q) zout[q] -= s;
         return AEO_OK;
     }
 
@@ -1208,19 +680,18 @@ struct Mg : MgBase {
         cudaEvent_t e0, e1;
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
-        int* dz = dzero;
         auto run = [&]() -> aeo_status {
             switch (what) {
             case 0: CK(cudaGraphLaunch(g_solve, st)); return AEO_OK;
             case 1: {
                 Level<R>& F = L[0];
                 if (F.nx % 2) { fail("profile: odd finest nx"); return AEO_ERR_ARGUMENT; }
-                mg_rbgs_kernel<R><<<blocks_for((long long)(F.nx / 2) * F.ny * F.nz), TPB, 0, st>>>(F, bc, 0, dz);
+                mg_rbgs_kernel<R><<<half_grid(F), dim3(RB_X, RB_Y), 0, st>>>(F, bc, 0, dzero);
                 CKL();
                 return AEO_OK;
             }
             case 2: return launch_apply(st, p, Ap, 1);
-            case 3: return launch_vcycle(st, r, true, dz);
+            case 3: return launch_vcycle(st, r, true, dzero);
             default: fail("profile: unknown part"); return AEO_ERR_ARGUMENT;
             }
         };
@@ -1233,7 +704,7 @@ struct Mg : MgBase {
         CK(cudaEventSynchronize(e1));
         float t = 0;
         CK(cudaEventElapsedTime(&t, e0, e1));
-        *ms = double(t) / (reps > 0 ? reps : 1);
+        *ms = double(t) / reps;
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         return AEO_OK;
@@ -1271,22 +742,12 @@ aeo_status aeo_mg_create(const aeo_mg_config* c, const double* cx, const double*
         g_mg_error = "invalid tol / maxit / sweep counts (nu1 >= 1)";
         return AEO_ERR_ARGUMENT;
     }
-    long long ncell = (long long)c->nx * c->ny * c->nz;
-    if (ncell > (1LL << 31)) { g_mg_error = "grid above 2^31 cells"; return AEO_ERR_ARGUMENT; }
+    long long ncell = (long long)(c->nx + 1) * (c->ny + 1) * (c->nz + 1);
+    if (ncell >= (1LL << 30)) { g_mg_error = "grid at or above 2^30 cells"; return AEO_ERR_ARGUMENT; }
     if (cudaSetDevice(c->device) != cudaSuccess) { g_mg_error = "cudaSetDevice failed"; return AEO_ERR_CUDA; }
-    bool exact32 = false;
-    if (c->precision == AEO_PREC_FP32_MIXED && cx) {
-        exact32 = true;
-        const long long nxs = (long long)(c->nx + 1) * c->ny * c->nz, nys = (long long)c->nx * (c->ny + 1) * c->nz,
-                        nzs = (long long)c->nx * c->ny * (c->nz + 1);
-        for (long long q = 0; q < nxs && exact32; ++q) exact32 = double(float(cx[q])) == cx[q];
-        for (long long q = 0; q < nys && exact32; ++q) exact32 = double(float(cy[q])) == cy[q];
-        for (long long q = 0; q < nzs && exact32; ++q) exact32 = double(float(cz[q])) == cz[q];
-    }
     MgBase* m = nullptr;
-    if (c->precision == AEO_PREC_FP64) m = new (std::nothrow) Mg<double, double>();
-    else if (exact32) m = new (std::nothrow) Mg<float, float>();
-    else m = new (std::nothrow) Mg<float, double>();
+    if (c->precision == AEO_PREC_FP64) m = new (std::nothrow) Mg<double>();
+    else m = new (std::nothrow) Mg<float>();
     if (!m) { g_mg_error = "out of host memory"; return AEO_ERR_CUDA; }
     m->cfg = *c;
     if (aeo_status s = m->init(cx, cy, cz)) {

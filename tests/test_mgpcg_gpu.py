@@ -67,6 +67,27 @@ def test_one_vcycle_matches_the_oracle(bc):
     assert rel(zg, zo) < 1e-11
 
 
+@pytest.mark.parametrize("n,bc,precision", [
+    ((40, 24, 10), ("periodic",) * 3, "fp64"),          # coarsest 20 x 12 x 5: an odd periodic axis
+    ((64, 64, 12), ("periodic", "periodic", "neumann"), "fp64"),   # coarsest 32 x 32 x 6 outside shared memory
+    ((64, 64, 12), ("periodic", "periodic", "neumann"), "fp32_mixed"),
+])
+def test_coarsest_level_variants_match_the_oracle(n, bc, precision):
+    rng = np.random.default_rng(8)
+    nx, ny, nz = n
+    cx, cy, cz = (0.2 + rng.random(s) for s in ((nz, ny, nx + 1), (nz, ny + 1, nx), (nz + 1, ny, nx)))
+    cx[..., -1] = cx[..., 0]
+    cy[:, -1, :] = cy[:, 0, :]
+    if bc[2] == "periodic":
+        cz[-1] = cz[0]
+    b = rng.standard_normal((nz, ny, nx))
+    g = MG(n, (1.0, 1.0, 1.0), coeffs=(cx, cy, cz), bc=bc, precision=precision)
+    o = OracleMGPCG(n, (1.0, 1.0, 1.0), coeffs=(cx, cy, cz), bc=bc)
+    assert g.level_dims() == [o.level_dims(l) for l in range(o.nlevels)]
+    zg, zo = g.precondition(b), o.precondition(b)
+    assert rel(zg, zo) < (1e-11 if precision == "fp64" else 1e-5)
+
+
 def test_cutcell_mgcg_solve_matches_the_oracle():
     coeffs, b = ref_case()
     g = MG(REF_N, REF_H, coeffs=coeffs, tol=1e-10)
