@@ -494,12 +494,16 @@ __global__ void mg_prolong_kernel(Level<R> F, Level<R> Cl, Bc bc, const int* don
 // the other colour copied, so every update sees the values from before the
 // pass.  One barrier per pass.  phi, b and the coefficients are staged in
 // shared memory when they fit.
+// With `mat` (set-up, staged only) block j runs the same sweeps on the unit
+// right-hand side e_j and stores the result as column j of the n x n
+// row-major matrix of the whole coarsest solve (see mg_coarse_matvec_kernel).
 template <typename R>
 __global__ void __launch_bounds__(COARSE_THREADS) mg_coarsest_kernel(Level<R> L, R* spare, Bc bc, int sweeps,
                                                                     int staged, int inplace,
                                                                     const double* __restrict__ r0, const double* mr0,
-                                                                    const int* done) {
+                                                                    const int* done, R* mat) {
     if (*done) return;
+    const int unit = mat ? (int)blockIdx.x : -1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nx = L.nx, ny = L.ny, nz = L.nz, n = L.n;
     const int ncx = (nx + 1) * ny * nz, ncy = nx * (ny + 1) * nz, ncz = nx * ny * (nz + 1);
@@ -524,10 +528,10 @@ __global__ void __launch_bounds__(COARSE_THREADS) mg_coarsest_kernel(Level<R> L,
             cz = c + ncx + ncy;
         }
     }
-    const double m0 = r0 ? *mr0 : 0.0;
-    const R m = r0 ? R(0) : R(*L.bmean);
+    const double m0 = (r0 && unit < 0) ? *mr0 : 0.0;
+    const R m = (r0 || unit >= 0) ? R(0) : R(*L.bmean);
     for (int q = t; q < n; q += nt) {
-        bb[q] = r0 ? R(r0[q] - m0) : L.b[q] - m;
+        bb[q] = unit >= 0 ? R(q == unit ? 1 : 0) : (r0 ? R(r0[q] - m0) : L.b[q] - m);
         A[q] = R(0);
     }
     __syncthreads();
@@ -591,8 +595,121 @@ __global__ void __launch_bounds__(COARSE_THREADS) mg_coarsest_kernel(Level<R> L,
                 B = tmp;
             }
         }
-    if (A != L.phi)
+    if (unit >= 0) {
+        for (int q = t; q < n; q += nt) mat[(size_t)q * n + unit] = A[q];
+    } else if (A != L.phi) {
         for (int q = t; q < n; q += nt) L.phi[q] = A[q];
+    }
+}
+
+// The coarsest solve as one dense product phi = M (b - mean b), M the n x n
+// matrix of the sweeps above (a linear map of the right-hand side, built
+// once per coefficient field): the same result up to the order of the sums,
+// with the n^2 values read from L2 by all SMs instead of 2 * sweeps
+// dependent passes on one.  One warp per row, FP64 accumulation, fixed order.
+template <typename R>
+__global__ void mg_coarse_matvec_kernel(Level<R> L, const R* __restrict__ mat, const double* __restrict__ r0,
+                                        const double* mr0, const int* done) {
+    if (*done) return;
+    const int n = L.n;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const double m0 = r0 ? *mr0 : 0.0;
+    const R m = r0 ? R(0) : R(*L.bmean);
+    const R* Mr = mat + (size_t)row * n;
+    double acc = 0.0;
+    for (int j = lane; j < n; j += 32) {
+        const R bj = r0 ? R(r0[j] - m0) : L.b[j] - m;
+        acc += double(Mr[j]) * double(bj);
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) L.phi[row] = R(acc);
+}
+
+// The coarsest level when its columns are short (nz <= COL_NZ), fit one
+// block (nx ny <= 1024 threads) and no periodic axis has an odd length: one
+// thread per (x, y) column keeps the column's phi and b in registers, so the
+// vertical neighbours never leave the thread; phi is mirrored in shared
+// memory for the lateral neighbours, which are always of the other colour.
+// The same sweeps and arithmetic as mg_coarsest_kernel, in place.
+constexpr int COL_NZ = 8;
+template <typename R, int MAXT>
+__global__ void __launch_bounds__(MAXT) mg_coarsest_col_kernel(Level<R> L, Bc bc, int sweeps,
+                                                                        const double* __restrict__ r0,
+                                                                        const double* mr0, const int* done) {
+    if (*done) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nx = L.nx, ny = L.ny, nz = L.nz, n = L.n, ncol = nx * ny;
+    const int ncx = (nx + 1) * ny * nz, ncy = nx * (ny + 1) * nz, ncz = nx * ny * (nz + 1);
+    const int nt = blockDim.x, t = threadIdx.x;
+    const bool var = L.c.var();
+    R* A = reinterpret_cast<R*>(smem_raw);
+    R* bv = A + n;
+    R* cx = bv + n;
+    R* cy = cx + ncx;
+    R* cz = cy + ncy;
+    if (var) {
+        for (int q = t; q < ncx; q += nt) cx[q] = L.c.x(q);
+        for (int q = t; q < ncy; q += nt) cy[q] = L.c.y(q);
+        for (int q = t; q < ncz; q += nt) cz[q] = L.c.z(q);
+    }
+    for (int q = t; q < n; q += nt) A[q] = R(0);
+    const bool act = t < ncol;
+    const int col = act ? t : 0;
+    const int i = col % nx, j = col / nx;
+    const double m0 = r0 ? *mr0 : 0.0;
+    const R m = r0 ? R(0) : R(*L.bmean);
+    for (int q = t; q < n; q += nt) bv[q] = r0 ? R(r0[q] - m0) : L.b[q] - m;
+    R ph[COL_NZ];
+#pragma unroll
+    for (int k = 0; k < COL_NZ; ++k) ph[k] = R(0);
+    const int oxm = wm(i, nx, bc.x) - i, oxp = wp(i, nx, bc.x) - i;
+    const int oym = (wm(j, ny, bc.y) - j) * nx, oyp = (wp(j, ny, bc.y) - j) * nx;
+    const int cxb = i + (nx + 1) * j, cyb = i + nx * j;
+    const R ix2 = L.ix2, iy2 = L.iy2, iz2 = L.iz2;
+    const R cdiag = -R(2) * (ix2 + iy2 + iz2);
+    const bool zper = bc.z == 0;
+    __syncthreads();
+    for (int sw = 0; sw < sweeps; ++sw)
+        for (int colour = 0; colour < 2; ++colour) {
+            if (act) {
+                R top = ph[0];
+#pragma unroll
+                for (int k = 1; k < COL_NZ; ++k)
+                    if (k == nz - 1) top = ph[k];
+#pragma unroll
+                for (int k = 0; k < COL_NZ; ++k) {
+                    if (k >= nz || ((i + j + k) & 1) != colour) continue;
+                    const int q = col + ncol * k;
+                    const R vzm = k > 0 ? ph[k > 0 ? k - 1 : 0] : (zper ? top : ph[0]);
+                    const R vzp = k < nz - 1 ? ph[k + 1 < COL_NZ ? k + 1 : COL_NZ - 1] : (zper ? ph[0] : ph[k]);
+                    R off, diag;
+                    bool upd = true;
+                    if (!var) {
+                        diag = cdiag;
+                        off = (A[q + oxp] + A[q + oxm]) * ix2 + (A[q + oyp] + A[q + oym]) * iy2 + (vzp + vzm) * iz2;
+                    } else {
+                        const int ax = cxb + (nx + 1) * ny * k, ay = cyb + nx * (ny + 1) * k;
+                        const R fxp = cx[ax + 1], fxm = cx[ax], fyp = cy[ay + nx], fym = cy[ay];
+                        const R fzp = cz[q + ncol], fzm = cz[q];
+                        diag = -((fxp + fxm) * ix2 + (fyp + fym) * iy2 + (fzp + fzm) * iz2);
+                        upd = !(fabs(diag) < Eps<R>::v());
+                        off = (fxp * A[q + oxp] + fxm * A[q + oxm]) * ix2 + (fyp * A[q + oyp] + fym * A[q + oym]) * iy2 +
+                              (fzp * vzp + fzm * vzm) * iz2;
+                    }
+                    if (upd) {
+                        const R v = (bv[q] - off) / diag;
+                        ph[k] = v;
+                        A[q] = v;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    if (act)
+#pragma unroll
+        for (int k = 0; k < COL_NZ; ++k)
+            if (k < nz) L.phi[col + ncol * k] = ph[k];
 }
 
 // level-0 right-hand side of the standalone cycles: b0 = b - mean(b), phi0 = 0

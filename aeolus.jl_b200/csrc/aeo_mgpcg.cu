@@ -190,6 +190,10 @@ struct Mg : MgBase {
     int coarse_inplace = 1;        // 0 when a periodic axis of the coarsest level has an odd length
     size_t coarse_smem = 0;
     R* coarse_spare = nullptr;     // the coarsest level's second buffer when not staged
+    R* coarse_mat = nullptr;       // the coarsest solve as a dense n x n matrix (nullptr: run the sweeps)
+    int coarse_col = 0;            // the register-column coarsest kernel applies
+    int coarse_col_threads = 0;
+    size_t coarse_col_smem = 0;
     cudaGraphExec_t g_solve = nullptr, g_cycles = nullptr;
     int body_launches = 0;
 
@@ -337,9 +341,33 @@ struct Mg : MgBase {
         coarse_inplace = !((cfg.bc_x == AEO_MG_PERIODIC && C.nx % 2) || (cfg.bc_y == AEO_MG_PERIODIC && C.ny % 2) ||
                            (cfg.bc_z == AEO_MG_PERIODIC && C.nz % 2));
         coarse_smem = coarse_staged ? cb : 0;
+        coarse_col_smem = sizeof(R) * (2 * (size_t)C.n + (coeff ? (size_t)(C.nx + 1) * C.ny * C.nz +
+                                                             (size_t)C.nx * (C.ny + 1) * C.nz +
+                                                             (size_t)C.nx * C.ny * (C.nz + 1) : 0));
+        coarse_col = coarse_inplace && C.nz <= COL_NZ && C.nx * C.ny <= COARSE_THREADS && coarse_col_smem <= 225 * 1024;
+        coarse_col_threads = ((C.nx * C.ny + 31) / 32) * 32;
+        if (coarse_col && coarse_col_smem > 48 * 1024) {
+            CK(cudaFuncSetAttribute(mg_coarsest_col_kernel<R, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)coarse_col_smem));
+            CK(cudaFuncSetAttribute(mg_coarsest_col_kernel<R, COARSE_THREADS>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_col_smem));
+        }
         if (coarse_smem > 48 * 1024)
             CK(cudaFuncSetAttribute(mg_coarsest_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_smem));
         if (aeo_status s = dalloc(&coarse_spare, C.n)) return s;
+        // the coarsest solve as a matrix, when its sweeps fit shared memory and
+        // the matrix is modest: one block per unit right-hand side
+        if (coarse_staged && (size_t)C.n * C.n * sizeof(R) <= (size_t(512) << 20) && cfg.coarse_sweeps > 0) {
+            if (aeo_status s = dalloc(&coarse_mat, (size_t)C.n * C.n)) return s;
+            int* dz = nullptr;
+            if (aeo_status s = dalloc(&dz, 1)) return s;
+            CK(cudaMemset(dz, 0, sizeof(int)));
+            mg_coarsest_kernel<R><<<C.n, COARSE_THREADS, coarse_smem, st>>>(L[nl - 1], coarse_spare, bc,
+                                                                            cfg.coarse_sweeps, 1, coarse_inplace,
+                                                                            nullptr, nullptr, dz, coarse_mat);
+            CKL();
+            CK(cudaStreamSynchronize(st));
+        }
         if (aeo_status s = dalloc(&b, n)) return s;
         if (aeo_status s = dalloc(&x, n)) return s;
         if (aeo_status s = dalloc(&r, n)) return s;
@@ -388,8 +416,24 @@ struct Mg : MgBase {
     }
 
     aeo_status launch_coarsest(cudaStream_t s, Level<R>& C, const double* r0, const int* done) {
+        if (coarse_mat) {
+            mg_coarse_matvec_kernel<R><<<(C.n + 7) / 8, 256, 0, s>>>(C, coarse_mat, r0, &S->mr, done);
+            CKL();
+            return AEO_OK;
+        }
+        if (coarse_col) {
+            if (coarse_col_threads <= 256)
+                mg_coarsest_col_kernel<R, 256><<<1, coarse_col_threads, coarse_col_smem, s>>>(C, bc, cfg.coarse_sweeps,
+                                                                                             r0, &S->mr, done);
+            else
+                mg_coarsest_col_kernel<R, COARSE_THREADS><<<1, coarse_col_threads, coarse_col_smem, s>>>(
+                    C, bc, cfg.coarse_sweeps, r0, &S->mr, done);
+            CKL();
+            return AEO_OK;
+        }
         mg_coarsest_kernel<R><<<1, COARSE_THREADS, coarse_smem, s>>>(C, coarse_spare, bc, cfg.coarse_sweeps,
-                                                                     coarse_staged, coarse_inplace, r0, &S->mr, done);
+                                                                     coarse_staged, coarse_inplace, r0, &S->mr, done,
+                                                                     nullptr);
         CKL();
         return AEO_OK;
     }
@@ -692,6 +736,14 @@ struct Mg : MgBase {
             }
             case 2: return launch_apply(st, p, Ap, 1);
             case 3: return launch_vcycle(st, r, true, dzero);
+            case 4: return launch_coarsest(st, L[nl - 1], nl == 1 ? r : nullptr, dzero);
+            case 5: {
+                if (nl < 2) { fail("profile: one level, no restriction"); return AEO_ERR_ARGUMENT; }
+                mg_restrict_kernel<R><<<restrict_grid(L[0], L[1]), dim3(32, 8, 2), 0, st>>>(L[0], L[1], bc, part,
+                                                                                         &S->counter, dzero);
+                CKL();
+                return AEO_OK;
+            }
             default: fail("profile: unknown part"); return AEO_ERR_ARGUMENT;
             }
         };

@@ -91,7 +91,8 @@ aeo_status aeo_mg_precondition(aeo_mg* h, const double* r, double* z);
 /* Device time of `reps` back-to-back launches of one part, after warm-up:
  * what = 0 the whole solve of the right-hand side of the last solve call,
  * 1 one red-black colour pass on the finest level, 2 the operator with its
- * p.Ap reduction, 3 one preconditioner application.  ms_out: mean ms. */
+ * p.Ap reduction, 3 one preconditioner application, 4 the coarsest-level
+ * solve, 5 the residual restriction of the finest level.  ms_out: mean ms. */
 aeo_status aeo_mg_profile(aeo_mg* h, int32_t what, int32_t reps, double* ms_out);
 /* kernel launches of one CG iteration (graph body) */
 int32_t aeo_mg_launches_per_iteration(const aeo_mg* h);
