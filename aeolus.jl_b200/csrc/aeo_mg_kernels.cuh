@@ -16,7 +16,6 @@ constexpr int RED_BLOCKS = 592;        // 4 x 148 SMs: the fixed grid of every F
 constexpr int COARSE_THREADS = 1024;
 constexpr int COARSE_MAX_CELLS = 16384;
 constexpr int RB_X = 32, RB_Y = 8;     // block of the 3-D stencil grids
-constexpr int RS_PAIRS = 4;            // fine plane pairs one restriction block walks up z
 
 enum { MG_CONVERGED = 0, MG_MAXIT = 1, MG_BREAKDOWN = 2, MG_ZERO_RHS = 3 };
 
@@ -57,6 +56,7 @@ template <typename R> struct Level {
     R ix2, iy2, iz2;
     R* phi;
     R* b;
+    R* r;                               // residual (every level but the coarsest)
     Coef<R> c;
     double* bmean;                      // mean of b to subtract before use (device scalar)
 };
@@ -410,48 +410,40 @@ __global__ void mg_rbgs_kernel(Level<R> L, Bc bc, int colour, const int* done) {
     if (gs_value<R>(L.phi, L.b[d.q], d, L, &v)) L.phi[d.q] = v;
 }
 
-// Coarse b = mean of the eight fine residuals b - A phi (src/Multigrid.jl:
-// 380-406), the fine residual formed here and never stored.  A block of
-// 32 x 8 x 2 threads holds one fine residual each for a 32 x 8 x 2 fine tile
-// (16 x 4 coarse cells) and walks RS_PAIRS such tiles up z; the eight
-// children of a coarse cell are summed in the reference's order.  The last
-// block stores the coarse mean that the coarse level subtracts before use.
+// r = b - A phi on a level (_compute_residual!, src/Multigrid.jl:281-285):
+// one thread per cell, a 3-D grid.
 template <typename R>
-__global__ void __launch_bounds__(512) mg_restrict_kernel(Level<R> F, Level<R> Cl, Bc bc, double* part,
-                                                          unsigned* counter, const int* done) {
+__global__ void mg_residual_kernel(Level<R> F, Bc bc, const int* done) {
     if (*done) return;
-    __shared__ R rs[2][8][33];
-    const int tx = threadIdx.x, ty = threadIdx.y, tz = threadIdx.z;
-    const int i = blockIdx.x * 32 + tx, j = blockIdx.y * 8 + ty;
-    const int t = tid();
-    const int I = blockIdx.x * 16 + (t & 15), J = blockIdx.y * 4 + ((t >> 4) & 3);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+    if (i >= F.nx || j >= F.ny) return;
+    Idx d = make_idx(i, j, k, F.nx, F.ny, F.nz, bc);
+    F.r[d.q] = F.b[d.q] - aphi<R, R>(F.phi, d, F.c, F.ix2, F.iy2, F.iz2);
+}
+
+// Coarse b = mean of the eight fine residuals (src/Multigrid.jl:380-406),
+// summed in the reference's order; one thread per coarse cell on a 3-D
+// grid.  The last block stores the coarse mean that the coarse level
+// subtracts before use.
+template <typename R>
+__global__ void mg_restrict_kernel(Level<R> F, Level<R> Cl, double* part, unsigned* counter, const int* done) {
+    if (*done) return;
+    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y, K = blockIdx.z;
     double v[1] = {0.0};
-    for (int pr = 0; pr < RS_PAIRS; ++pr) {
-        const int K = blockIdx.z * RS_PAIRS + pr;
-        if (K >= Cl.nz) break;
-        const int k = 2 * K + tz;
-        R rr = R(0);
-        if (i < F.nx && j < F.ny) {
-            Idx d = make_idx(i, j, k, F.nx, F.ny, F.nz, bc);
-            rr = F.b[d.q] - aphi<R, R>(F.phi, d, F.c, F.ix2, F.iy2, F.iz2);
-        }
-        rs[tz][ty][tx] = rr;
-        __syncthreads();
-        if (t < 64 && I < Cl.nx && J < Cl.ny) {
-            const int a = 2 * (t & 15), c = 2 * ((t >> 4) & 3);
-            R s = rs[0][c][a];
-            s += rs[0][c][a + 1];
-            s += rs[0][c + 1][a];
-            s += rs[0][c + 1][a + 1];
-            s += rs[1][c][a];
-            s += rs[1][c][a + 1];
-            s += rs[1][c + 1][a];
-            s += rs[1][c + 1][a + 1];
-            const R bcv = s * R(0.125);
-            Cl.b[Cl.nx * (J + Cl.ny * K) + I] = bcv;
-            v[0] += double(bcv);
-        }
-        __syncthreads();
+    if (I < Cl.nx && J < Cl.ny) {
+        const int sy = F.nx, sz = F.nx * F.ny;
+        const R* r = F.r + (2 * I) + sy * (2 * J) + sz * (2 * K);
+        R s = r[0];
+        s += r[1];
+        s += r[sy];
+        s += r[sy + 1];
+        s += r[sz];
+        s += r[sz + 1];
+        s += r[sz + sy];
+        s += r[sz + sy + 1];
+        const R bcv = s * R(0.125);
+        Cl.b[Cl.nx * (J + Cl.ny * K) + I] = bcv;
+        v[0] = double(bcv);
     }
     double tot[1];
     if (reduce_last<1>(v, part, counter, tot) && tid() == 0) *Cl.bmean = tot[0] / double(Cl.n);

@@ -34,7 +34,10 @@
 //   * the first half-sweep of a level that starts from zero is pointwise
 //     (every neighbour is zero), so it is fused with the zeroing and with
 //     the mean projection of the level's right-hand side;
-//   * the fine residual is never stored: it is formed inside the restriction.
+//   * the coarsest solve (nu sweeps of RB-GS from zero, a linear map of its
+//     right-hand side) is precomputed once per coefficient field as a dense
+//     matrix, built by running the sweeps on every unit vector, and applied
+//     as one L2-resident matrix-vector product on all SMs;
 //   * the mean projections the reference applies to phi after smoothing and
 //     prolongation shift phi by a constant; RB-GS, the residual and the
 //     prolongation commute with constant shifts and the CG deflation removes
@@ -240,10 +243,7 @@ struct Mg : MgBase {
     static dim3 cell_grid(const Level<R>& F) {
         return dim3((unsigned)((F.nx + RB_X - 1) / RB_X), (unsigned)((F.ny + RB_Y - 1) / RB_Y), (unsigned)F.nz);
     }
-    static dim3 restrict_grid(const Level<R>& F, const Level<R>& Cl) {
-        return dim3((unsigned)((F.nx + 31) / 32), (unsigned)((F.ny + 7) / 8),
-                    (unsigned)((Cl.nz + RS_PAIRS - 1) / RS_PAIRS));
-    }
+    static dim3 restrict_grid(const Level<R>& Cl) { return cell_grid(Cl); }
     static int row_blocks(int rows) {
         int b = (rows + RB_Y - 1) / RB_Y;
         return b < RED_BLOCKS ? b : RED_BLOCKS;
@@ -277,6 +277,7 @@ struct Mg : MgBase {
             V.iz2 = R(1) / (R(dz) * R(dz));
             if (aeo_status s = dalloc(&V.phi, V.n)) return s;
             if (aeo_status s = dalloc(&V.b, V.n)) return s;
+            V.r = nullptr;
             V.bmean = bmeans + nl;
             V.c = Coef<R>();
             if (coeff) {
@@ -325,6 +326,7 @@ struct Mg : MgBase {
                 restrict_coeff(nx, ny, nz, hx, hy, hz, cnx, cny, cnz, Cx, Cy, Cz);
                 hx.swap(Cx); hy.swap(Cy); hz.swap(Cz);
             }
+            if (aeo_status s = dalloc(&V.r, V.n)) return s;
             nx = cnx; ny = cny; nz = cnz;
             dx *= 2; dy *= 2; dz *= 2;
         }
@@ -375,7 +377,7 @@ struct Mg : MgBase {
         if (aeo_status s = dalloc(&Ap, n)) return s;
         part_cap = (size_t)RED_BLOCKS * 8;
         for (int l = 0; l + 1 < nl; ++l) {
-            dim3 g = restrict_grid(L[l], L[l + 1]);
+            dim3 g = restrict_grid(L[l + 1]);
             size_t nb = (size_t)g.x * g.y * g.z;
             if (nb > part_cap) part_cap = nb;
         }
@@ -411,7 +413,7 @@ struct Mg : MgBase {
 
     int vcycle_launches() const {
         int c = 1;   // coarsest
-        for (int l = 0; l < nl - 1; ++l) c += 2 * cfg.nu1 + 2 * cfg.nu2 + 2;
+        for (int l = 0; l < nl - 1; ++l) c += 2 * cfg.nu1 + 2 * cfg.nu2 + 3;
         return c;
     }
 
@@ -468,7 +470,9 @@ struct Mg : MgBase {
                     CKL();
                 }
             Level<R>& Cl = L[l + 1];
-            mg_restrict_kernel<R><<<restrict_grid(F, Cl), dim3(32, 8, 2), 0, s>>>(F, Cl, bc, part, &S->counter, done);
+            mg_residual_kernel<R><<<cell_grid(F), blk, 0, s>>>(F, bc, done);
+            CKL();
+            mg_restrict_kernel<R><<<restrict_grid(Cl), blk, 0, s>>>(F, Cl, part, &S->counter, done);
             CKL();
         }
         if (aeo_status q = launch_coarsest(s, L[nl - 1], nullptr, done)) return q;
@@ -739,8 +743,10 @@ struct Mg : MgBase {
             case 4: return launch_coarsest(st, L[nl - 1], nl == 1 ? r : nullptr, dzero);
             case 5: {
                 if (nl < 2) { fail("profile: one level, no restriction"); return AEO_ERR_ARGUMENT; }
-                mg_restrict_kernel<R><<<restrict_grid(L[0], L[1]), dim3(32, 8, 2), 0, st>>>(L[0], L[1], bc, part,
-                                                                                         &S->counter, dzero);
+                mg_residual_kernel<R><<<cell_grid(L[0]), dim3(RB_X, RB_Y), 0, st>>>(L[0], bc, dzero);
+                CKL();
+                mg_restrict_kernel<R><<<restrict_grid(L[1]), dim3(RB_X, RB_Y), 0, st>>>(L[0], L[1], part, &S->counter,
+                                                                                      dzero);
                 CKL();
                 return AEO_OK;
             }
