@@ -102,10 +102,13 @@ class MGPreconditionedCG:
                 "relative_residual": st.residual if relative else (0.0 if st.bnorm == 0 else st.residual / st.bnorm),
                 "curvature": st.curvature}
 
-    def solve(self, b):
-        """x = A^-1 b by MG-preconditioned CG (solve!, src/Multigrid.jl:955-967)."""
+    def solve(self, b, out=None):
+        """x = A^-1 b by MG-preconditioned CG (solve!, src/Multigrid.jl:955-967).
+        `out`: an optional C-contiguous float64 array (e.g. pinned) for x."""
         b = self._arr(b)
-        x = np.empty(self.shape)
+        x = np.empty(self.shape) if out is None else out
+        if x.shape != self.shape or x.dtype != np.float64 or not x.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of the grid's shape")
         st = L.AeoMgStats()
         self._chk(L.load().aeo_mg_solve(self._h, _p(b), _p(x), C.byref(st)))
         self.last_stats = self._stats(st, False)
