@@ -22,6 +22,9 @@ SYMBOLS = (
     "aeo_mg_create", "aeo_mg_destroy", "aeo_mg_levels", "aeo_mg_solve", "aeo_mg_solve_device",
     "aeo_mg_vcycle_solve", "aeo_mg_apply", "aeo_mg_precondition", "aeo_mg_profile",
     "aeo_mg_launches_per_iteration", "aeo_mg_last_error",
+    "aeo_unet_param_count", "aeo_unet_create", "aeo_unet_destroy", "aeo_unet_set_params", "aeo_unet_get_params",
+    "aeo_unet_set_mask", "aeo_unet_set_out_scale", "aeo_unet_apply", "aeo_unet_gradients", "aeo_unet_train_step",
+    "aeo_unet_activation", "aeo_unet_profile", "aeo_unet_last_error",
 )
 
 
@@ -144,19 +147,36 @@ def load():
     lib.aeo_mg_launches_per_iteration.argtypes = [P]
     lib.aeo_mg_last_error.argtypes = [P]
     lib.aeo_mg_last_error.restype = C.c_char_p
+    F = C.POINTER(C.c_float)
+    lib.aeo_unet_param_count.restype = C.c_int64
+    lib.aeo_unet_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_int32, C.POINTER(P)]
+    lib.aeo_unet_destroy.argtypes = [P]
+    lib.aeo_unet_set_params.argtypes = [P, F]
+    lib.aeo_unet_get_params.argtypes = [P, F, F]
+    lib.aeo_unet_set_mask.argtypes = [P, F]
+    lib.aeo_unet_set_out_scale.argtypes = [P, C.c_double]
+    lib.aeo_unet_apply.argtypes = [P, D, D]
+    lib.aeo_unet_gradients.argtypes = [P, D, D, D]
+    lib.aeo_unet_train_step.argtypes = [P, D, D, C.c_double, D]
+    lib.aeo_unet_activation.argtypes = [P, C.c_int32, F]
+    lib.aeo_unet_profile.argtypes = [P, C.c_int32, C.c_int32, D]
+    lib.aeo_unet_last_error.argtypes = [P]
+    lib.aeo_unet_last_error.restype = C.c_char_p
     for s in SYMBOLS:
         f = getattr(lib, s)
-        if s not in ("aeo_stream", "aeo_last_error", "aeo_version", "aeo_mg_last_error"):
+        if s not in ("aeo_stream", "aeo_last_error", "aeo_version", "aeo_mg_last_error", "aeo_unet_last_error",
+                     "aeo_unet_param_count"):
             f.restype = C.c_int32
     _lib = lib
     return lib
 
 
-def check(status: int, handle=None, mg=False):
+def check(status: int, handle=None, mg=False, unet=False):
     if status == 0:
         return
     lib = load()
-    msg = (lib.aeo_mg_last_error if mg else lib.aeo_last_error)(handle).decode(errors="replace")
+    f = lib.aeo_unet_last_error if unet else (lib.aeo_mg_last_error if mg else lib.aeo_last_error)
+    msg = f(handle).decode(errors="replace")
     if status == 3:
         raise NumericalFailure(status, msg)
     if status == 1:

@@ -1,0 +1,577 @@
+// aeo_unet_kernels.cuh -- kernels of the learned U-Net preconditioner
+// (included by aeo_unet.cu).
+//
+// Tensors are channels-last bfloat16 arrays (cell-major, C channels of a
+// cell contiguous, cell = x + nx (y + ny z)); the grid is periodic in x and
+// y and zero outside z.  A 3x3x3 convolution is an implicit GEMM on the
+// tcgen05 tensor cores: M = 128 output cells, N = C_out, K = 27 taps x C_in,
+// BF16 operands from shared memory, the FP32 accumulator in TMEM.
+//
+// Tiles of 128 cells: mode 0 takes a 128-cell x segment of one row
+// (nx % 128 == 0); mode 1 takes 128 / nx whole rows (128 % nx == 0).  The
+// input tile with its one-cell halo is staged once in shared memory as
+// K-major planes of 16-byte rows (8 channels of one cell), so that the A
+// operand of every tap is the same canonical layout at another start
+// address: mode 0 keeps a halo-ed row per (dz, dy) and shifts by dx within
+// it; mode 1 keeps, per (dz, dx), rows rotated by dx (periodic) and stacked,
+// so that a dy shift is a whole-row offset.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "aeo_tc.cuh"
+
+namespace un {
+
+constexpr int TM = 128;                 // cells per tile (the MMA M)
+constexpr int CONV_THREADS = 128;
+constexpr uint32_t WAIT_LIMIT = 1u << 26;   // mbarrier polls before a kernel gives up
+
+typedef __nv_bfloat16 bf16;
+
+struct Tiles {
+    int nx, ny, nz;
+    int mode, rows, tx, ntiles;
+    int np, pitch;                      // staged planes per 8-channel chunk, 16-byte rows per plane
+};
+
+inline Tiles make_tiles(int nx, int ny, int nz) {
+    Tiles T{};
+    T.nx = nx; T.ny = ny; T.nz = nz;
+    if (nx % TM == 0) {
+        T.mode = 0; T.rows = 1; T.tx = nx / TM; T.ntiles = T.tx * ny * nz;
+        T.np = 9; T.pitch = TM + 2;
+    } else {
+        T.mode = 1; T.rows = TM / nx; T.tx = ny / T.rows; T.ntiles = T.tx * nz;
+        T.np = 9 * (T.rows + 2); T.pitch = nx;
+    }
+    return T;
+}
+
+__device__ __forceinline__ void tile_origin(const Tiles& T, int tile, int& x0, int& j0, int& k) {
+    if (T.mode == 0) {
+        const int xt = tile % T.tx, rest = tile / T.tx;
+        x0 = xt * TM; j0 = rest % T.ny; k = rest / T.ny;
+    } else {
+        x0 = 0; j0 = (tile % T.tx) * T.rows; k = tile / T.tx;
+    }
+}
+
+// cell of tile row m
+__device__ __forceinline__ int cell_of(const Tiles& T, int x0, int j0, int k, int m) {
+    if (T.mode == 0) return (k * T.ny + j0) * T.nx + x0 + m;
+    return (k * T.ny + j0 + m / T.nx) * T.nx + m % T.nx;
+}
+
+// staged plane and first cell of tap t = (dz+1)*9 + (dy+1)*3 + (dx+1)
+__device__ __forceinline__ void tap_plane(const Tiles& T, int t, int& P, int& xs) {
+    const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+    if (T.mode == 0) { P = (dz + 1) * 3 + (dy + 1); xs = 1 + dx; }
+    else { P = ((dz + 1) * 3 + (dx + 1)) * (T.rows + 2) + 1 + dy; xs = 0; }
+}
+
+// The input tile with its halo into shared memory: row (c, P, x) at
+// ((c * np + P) * pitch + x) * 16 bytes.
+template <int CIN>
+__device__ __forceinline__ void stage_input(const Tiles& T, const uint4* __restrict__ in, uint4* sA, int x0, int j0,
+                                            int k) {
+    constexpr int NCH = CIN / 8;
+    const int per = T.np * T.pitch;
+    for (int it = threadIdx.x; it < NCH * per; it += blockDim.x) {
+        const int c = it / per, rem = it - c * per;
+        const int P = rem / T.pitch, x = rem - P * T.pitch;
+        int dz, gx, gy;
+        if (T.mode == 0) {
+            dz = P / 3 - 1;
+            gx = x0 - 1 + x;
+            gy = j0 + (P % 3) - 1;
+        } else {
+            const int nyr = T.rows + 2, yr = P % nyr, q = P / nyr;
+            dz = q / 3 - 1;
+            gx = x + (q % 3) - 1;
+            gy = j0 - 1 + yr;
+        }
+        gx = gx < 0 ? gx + T.nx : (gx >= T.nx ? gx - T.nx : gx);
+        gy = gy < 0 ? gy + T.ny : (gy >= T.ny ? gy - T.ny : gy);
+        const int gz = k + dz;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (gz >= 0 && gz < T.nz) v = in[((size_t)(gz * T.ny + gy) * T.nx + gx) * NCH + c];
+        sA[it] = v;
+    }
+}
+
+struct ConvArgs {
+    Tiles T;
+    const bf16* in;        // (n, CIN)
+    const uint4* wimg;     // weights in the shared-memory image [chunk][tap][co][8]
+    const float* bias;     // COUT or nullptr
+    const bf16* add;       // (n, COUT) added before the activation, or nullptr
+    const bf16* gate;      // (n, COUT): result *= (gate > 0), or nullptr
+    bf16* out;             // (n, COUT) or nullptr
+    float* out0;           // channel 0 in FP32 (times out0_scale * out0_mask), or nullptr
+    const float* out0_mask;
+    const double* out0_scale;
+    int relu;
+    int* err;
+};
+
+template <int CIN, int COUT>
+constexpr size_t conv_smem_weights() { return (size_t)(CIN / 8) * 27 * COUT * 16; }
+
+// out = act(conv(in) + bias + add) * gate, per the flags.
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(CONV_THREADS) conv_fwd_kernel(ConvArgs a) {
+    static_assert(CIN % 16 == 0 && (COUT == 16 || COUT == 32), "CIN multiple of 16, COUT 16 or 32");
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr int NCH = CIN / 8;
+    constexpr int WROWS = NCH * 27 * COUT;
+    __shared__ uint64_t mbar;
+    __shared__ uint32_t tslot;
+    const Tiles& T = a.T;
+    uint4* sB = reinterpret_cast<uint4*>(smem);
+    uint4* sA = sB + WROWS;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = threadIdx.x; i < WROWS; i += blockDim.x) sB[i] = a.wimg[i];
+    if (threadIdx.x == 0) tc::mbar_init(&mbar, 1);
+    if (warp == 0) tc::tmem_alloc(&tslot, 32);
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = tslot;
+    const uint32_t idesc = tc::idesc_bf16(COUT, false, false);
+    const uint32_t lboA = (uint32_t)(T.np * T.pitch * 16), lboB = 27u * COUT * 16u;
+    const uint32_t aBase = tc::smem_u32(sA), bBase = tc::smem_u32(sB);
+    uint32_t phase = 0;
+    bool failed = false;
+    for (int tile = blockIdx.x; tile < T.ntiles; tile += gridDim.x) {
+        int x0, j0, k;
+        tile_origin(T, tile, x0, j0, k);
+        stage_input<CIN>(T, reinterpret_cast<const uint4*>(a.in), sA, x0, j0, k);
+        tc::fence_async_smem();
+        tc::fence_before();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tc::fence_after();
+#pragma unroll 1
+            for (int t = 0; t < 27; ++t) {
+                int P, xs;
+                tap_plane(T, t, P, xs);
+#pragma unroll
+                for (int ks = 0; ks < CIN / 16; ++ks) {
+                    const uint32_t aa = aBase + (uint32_t)(((2 * ks * T.np + P) * T.pitch + xs) * 16);
+                    const uint32_t bb = bBase + (uint32_t)((2 * ks * 27 + t) * COUT * 16);
+                    tc::mma_bf16(tmem, tc::sdesc(aa, lboA, 128), tc::sdesc(bb, lboB, 128), idesc,
+                                 (t | ks) ? 1u : 0u);
+                }
+            }
+            tc::commit(&mbar);
+        }
+        const bool ok = tc::mbar_wait(&mbar, phase, WAIT_LIMIT);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        tc::fence_after();
+        // epilogue: warp w holds tile rows 32w..32w+31 in its TMEM lane quarter
+        const int m = warp * 32 + lane;
+        const int cell = cell_of(T, x0, j0, k, m);
+        float v[COUT];
+        {
+            float h[16];
+            tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16), h);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) v[q] = h[q];
+            if constexpr (COUT == 32) {
+                tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + 16u, h);
+#pragma unroll
+                for (int q = 0; q < 16; ++q) v[16 + q] = h[q];
+            }
+        }
+        if (a.bias)
+#pragma unroll
+            for (int q = 0; q < COUT; ++q) v[q] += a.bias[q];
+        if (a.add) {
+            const uint4* ap = reinterpret_cast<const uint4*>(a.add + (size_t)cell * COUT);
+#pragma unroll
+            for (int u = 0; u < COUT / 8; ++u) {
+                uint4 w = ap[u];
+                const bf16* e = reinterpret_cast<const bf16*>(&w);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) v[8 * u + q] += __bfloat162float(e[q]);
+            }
+        }
+        if (a.relu)
+#pragma unroll
+            for (int q = 0; q < COUT; ++q) v[q] = fmaxf(v[q], 0.0f);
+        if (a.gate) {
+            const uint4* gp = reinterpret_cast<const uint4*>(a.gate + (size_t)cell * COUT);
+#pragma unroll
+            for (int u = 0; u < COUT / 8; ++u) {
+                uint4 w = gp[u];
+                const bf16* e = reinterpret_cast<const bf16*>(&w);
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (!(__bfloat162float(e[q]) > 0.0f)) v[8 * u + q] = 0.0f;
+            }
+        }
+        if (a.out) {
+            uint4* op = reinterpret_cast<uint4*>(a.out + (size_t)cell * COUT);
+#pragma unroll
+            for (int u = 0; u < COUT / 8; ++u) {
+                uint4 w;
+                bf16* e = reinterpret_cast<bf16*>(&w);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) e[q] = __float2bfloat16_rn(v[8 * u + q]);
+                op[u] = w;
+            }
+        }
+        if (a.out0) {
+            float s = a.out0_scale ? (float)*a.out0_scale : 1.0f;
+            if (a.out0_mask) s *= a.out0_mask[cell];
+            a.out0[cell] = v[0] * s;
+        }
+        tc::fence_before();
+        __syncthreads();
+    }
+    if (failed) {
+        if (threadIdx.x == 0) atomicExch(a.err, 1);
+        tc::mbar_wait(&mbar, phase ^ 1u, WAIT_LIMIT);   // the outstanding MMAs, bounded
+    }
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 32);
+}
+
+struct WgradArgs {
+    Tiles T;
+    const bf16* x;         // (n, CIN) layer input
+    const bf16* g;         // (n, COUT) gradient of the layer's pre-activation
+    float* dW;             // [27][COUT][CIN], accumulated
+    float* db;             // [COUT], accumulated
+    int* err;
+};
+
+template <int CIN> constexpr int wg_mtiles() { return (27 * (CIN / 8) + 15) / 16; }
+template <int CIN, int COUT> constexpr uint32_t wg_tmem_cols() {
+    return wg_mtiles<CIN>() * COUT <= 32 ? 32u : wg_mtiles<CIN>() * COUT <= 64 ? 64u
+         : wg_mtiles<CIN>() * COUT <= 128 ? 128u : 256u;
+}
+
+// dW[t][co][ci] += sum over cells of x[nbr_t(cell), ci] g[cell, co] and
+// db[co] += sum g[cell, co]: per tile a GEMM D[(t, ci) x co] over K = the
+// tile's 128 cells, both operands MN-major, the (t, ci) rows in M-tiles of
+// 16 eight-channel planes materialised from the staged input.  Each CTA
+// accumulates over its tiles in TMEM and adds its sums to dW at the end.
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(CONV_THREADS) conv_wgrad_kernel(WgradArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr int NCH = CIN / 8, NCO = COUT / 8, NMT = wg_mtiles<CIN>();
+    constexpr uint32_t NCOL = wg_tmem_cols<CIN, COUT>();
+    __shared__ uint64_t mbar;
+    __shared__ uint32_t tslot;
+    const Tiles& T = a.T;
+    uint4* sG = reinterpret_cast<uint4*>(smem);          // NCO planes x 128 rows
+    uint4* sM = sG + NCO * TM;                           // 16 planes x 128 rows
+    uint4* sA = sM + 16 * TM;                            // staged input
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) tc::mbar_init(&mbar, 1);
+    if (warp == 0) tc::tmem_alloc(&tslot, NCOL);
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = tslot;
+    const uint32_t idesc = tc::idesc_bf16(COUT, true, true);
+    const uint32_t mBase = tc::smem_u32(sM), gBase = tc::smem_u32(sG);
+    uint32_t phase = 0;
+    bool failed = false, any = false;
+    float dbacc = 0.0f;
+    for (int tile = blockIdx.x; tile < T.ntiles && !failed; tile += gridDim.x) {
+        int x0, j0, k;
+        tile_origin(T, tile, x0, j0, k);
+        stage_input<CIN>(T, reinterpret_cast<const uint4*>(a.x), sA, x0, j0, k);
+        for (int it = threadIdx.x; it < NCO * TM; it += blockDim.x) {
+            const int c = it / TM, m = it - c * TM;
+            sG[it] = reinterpret_cast<const uint4*>(a.g)[(size_t)cell_of(T, x0, j0, k, m) * NCO + c];
+        }
+        __syncthreads();
+        if (threadIdx.x < COUT) {
+            const int c = threadIdx.x / 8, e = threadIdx.x % 8;
+            const bf16* gp = reinterpret_cast<const bf16*>(sG + c * TM);
+            for (int m = 0; m < TM; ++m) dbacc += __bfloat162float(gp[m * 8 + e]);
+        }
+        for (int mt = 0; mt < NMT; ++mt) {
+            for (int it = threadIdx.x; it < 16 * TM; it += blockDim.x) {
+                const int gl = it / TM, m = it - gl * TM;
+                const int G = mt * 16 + gl;
+                uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                if (G < 27 * NCH) {
+                    const int t = G / NCH, c = G - t * NCH;
+                    int P, xs;
+                    tap_plane(T, t, P, xs);
+                    v = sA[(c * T.np + P) * T.pitch + xs + m];
+                }
+                sM[it] = v;
+            }
+            tc::fence_async_smem();
+            tc::fence_before();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                tc::fence_after();
+#pragma unroll
+                for (int kk = 0; kk < TM / 16; ++kk) {
+                    const uint64_t ad = tc::sdesc(mBase + kk * 256u, 128u, (uint32_t)TM * 16u);
+                    const uint64_t bd = tc::sdesc(gBase + kk * 256u, 128u, (uint32_t)TM * 16u);
+                    tc::mma_bf16(tmem + (uint32_t)(mt * COUT), ad, bd, idesc, (any || kk) ? 1u : 0u);
+                }
+                tc::commit(&mbar);
+            }
+            const bool ok = tc::mbar_wait(&mbar, phase, WAIT_LIMIT);
+            phase ^= 1u;
+            if (__syncthreads_or(!ok)) {
+                failed = true;
+                break;
+            }
+        }
+        any = true;
+    }
+    if (failed) {
+        if (threadIdx.x == 0) atomicExch(a.err, 1);
+        tc::mbar_wait(&mbar, phase ^ 1u, WAIT_LIMIT);
+    } else if (any) {
+        tc::fence_after();
+        if (threadIdx.x < COUT) atomicAdd(&a.db[threadIdx.x], dbacc);
+        const int m = warp * 32 + lane;
+        for (int mt = 0; mt < NMT; ++mt) {
+            float v[COUT];
+            float h[16];
+            tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(mt * COUT), h);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) v[q] = h[q];
+            if constexpr (COUT == 32) {
+                tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(mt * COUT + 16), h);
+#pragma unroll
+                for (int q = 0; q < 16; ++q) v[16 + q] = h[q];
+            }
+            const int G = mt * 16 + m / 8;
+            if (G < 27 * NCH) {
+                const int t = G / NCH, ci = (G % NCH) * 8 + m % 8;
+#pragma unroll
+                for (int co = 0; co < COUT; ++co) atomicAdd(&a.dW[((size_t)t * COUT + co) * CIN + ci], v[co]);
+            }
+        }
+    }
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, NCOL);
+}
+
+// ---------------------------------------------------------------- helpers
+
+#define GS(i, n) for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)(n); \
+                      i += (long long)gridDim.x * blockDim.x)
+
+// Forward image [c][t][co][8] of W[t][co][ci] (FP32 master) in BF16; with
+// `transpose` the image of the transposed, flipped convolution that maps an
+// output gradient back to the input: W'[t'][ci][co] = W[26 - t'][co][ci].
+__global__ void weight_image_kernel(const float* __restrict__ W, bf16* __restrict__ img, int cin, int cout,
+                                    int transpose) {
+    const int ci_img = transpose ? cout : cin, co_img = transpose ? cin : cout;
+    const int n = 27 * ci_img * co_img;
+    GS(q, n) {
+        // img index: ((c * 27 + t) * co_img + o) * 8 + e, input channel i = 8c + e
+        const int e = (int)(q % 8);
+        long long r = q / 8;
+        const int o = (int)(r % co_img);
+        r /= co_img;
+        const int t = (int)(r % 27);
+        const int c = (int)(r / 27);
+        const int i = 8 * c + e;
+        float w = transpose ? W[((size_t)(26 - t) * cout + i) * cin + o] : W[((size_t)t * cout + o) * cin + i];
+        img[q] = __float2bfloat16_rn(w);
+    }
+}
+
+// network input: channel 0 = r * s (s = sqrt(n_fluid)/|r| from *scale), 1 = fluid mask
+__global__ void input_kernel(const double* __restrict__ r, const float* __restrict__ mask, const double* scale,
+                             bf16* __restrict__ x, long long n) {
+    const float s = (float)*scale;
+    GS(q, n) {
+        uint4 w0 = make_uint4(0u, 0u, 0u, 0u), w1 = w0;
+        bf16* e = reinterpret_cast<bf16*>(&w0);
+        e[0] = __float2bfloat16_rn((float)r[q] * s);
+        e[1] = __float2bfloat16_rn(mask[q]);
+        uint4* xp = reinterpret_cast<uint4*>(x + q * 16);
+        xp[0] = w0;
+        xp[1] = w1;
+    }
+}
+
+// coarse = mean of the 8 fine children (2x2x2 pooling), C channels
+__global__ void pool_kernel(const bf16* __restrict__ f, bf16* __restrict__ c, int nx, int ny, int nz, int C) {
+    const int cx = nx / 2, cy = ny / 2, cz = nz / 2;
+    const long long n = (long long)cx * cy * cz * C;
+    GS(q, n) {
+        const int ch = (int)(q % C);
+        long long cell = q / C;
+        const int I = (int)(cell % cx), J = (int)((cell / cx) % cy), K = (int)(cell / ((long long)cx * cy));
+        float s = 0.0f;
+#pragma unroll
+        for (int d = 0; d < 8; ++d) {
+            const int i = 2 * I + (d & 1), j = 2 * J + ((d >> 1) & 1), k = 2 * K + (d >> 2);
+            s += __bfloat162float(f[(((size_t)k * ny + j) * nx + i) * C + ch]);
+        }
+        c[q] = __float2bfloat16_rn(s * 0.125f);
+    }
+}
+
+// fine = coarse[parent] + skip (nearest upsampling with an additive skip)
+__global__ void up_add_kernel(const bf16* __restrict__ c, const bf16* __restrict__ skip, bf16* __restrict__ f, int nx,
+                              int ny, int nz, int C) {
+    const long long n = (long long)nx * ny * nz * C;
+    GS(q, n) {
+        const int ch = (int)(q % C);
+        long long cell = q / C;
+        const int i = (int)(cell % nx), j = (int)((cell / nx) % ny), k = (int)(cell / ((long long)nx * ny));
+        const size_t p = (((size_t)(k / 2) * (ny / 2) + j / 2) * (nx / 2) + i / 2) * C + ch;
+        f[q] = __float2bfloat16_rn(__bfloat162float(c[p]) + __bfloat162float(skip[q]));
+    }
+}
+
+// coarse gradient of nearest upsampling (sum of the 8 children), times (act > 0)
+__global__ void up_back_gate_kernel(const bf16* __restrict__ gf, const bf16* __restrict__ act, bf16* __restrict__ gc,
+                                    int nx, int ny, int nz, int C) {
+    const int cx = nx / 2, cy = ny / 2, cz = nz / 2;
+    const long long n = (long long)cx * cy * cz * C;
+    GS(q, n) {
+        const int ch = (int)(q % C);
+        long long cell = q / C;
+        const int I = (int)(cell % cx), J = (int)((cell / cx) % cy), K = (int)(cell / ((long long)cx * cy));
+        float s = 0.0f;
+#pragma unroll
+        for (int d = 0; d < 8; ++d) {
+            const int i = 2 * I + (d & 1), j = 2 * J + ((d >> 1) & 1), k = 2 * K + (d >> 2);
+            s += __bfloat162float(gf[(((size_t)k * ny + j) * nx + i) * C + ch]);
+        }
+        gc[q] = __bfloat162float(act[q]) > 0.0f ? __float2bfloat16_rn(s) : __float2bfloat16_rn(0.0f);
+    }
+}
+
+// fine gradient = (skip gradient + pooled-coarse gradient / 8) * (act > 0)
+__global__ void pool_back_add_gate_kernel(const bf16* __restrict__ gskip, const bf16* __restrict__ gc,
+                                          const bf16* __restrict__ act, bf16* __restrict__ gf, int nx, int ny, int nz,
+                                          int C) {
+    const long long n = (long long)nx * ny * nz * C;
+    GS(q, n) {
+        const int ch = (int)(q % C);
+        long long cell = q / C;
+        const int i = (int)(cell % nx), j = (int)((cell / nx) % ny), k = (int)(cell / ((long long)nx * ny));
+        const size_t p = (((size_t)(k / 2) * (ny / 2) + j / 2) * (nx / 2) + i / 2) * C + ch;
+        const float v = __bfloat162float(gskip[q]) + 0.125f * __bfloat162float(gc[p]);
+        gf[q] = __bfloat162float(act[q]) > 0.0f ? __float2bfloat16_rn(v) : __float2bfloat16_rn(0.0f);
+    }
+}
+
+// the output-layer gradient image: channel 0 = g (FP32 field), the rest 0
+__global__ void grad_out_kernel(const float* __restrict__ g, bf16* __restrict__ gimg, long long n) {
+    GS(q, n) {
+        uint4 w0 = make_uint4(0u, 0u, 0u, 0u), w1 = w0;
+        reinterpret_cast<bf16*>(&w0)[0] = __float2bfloat16_rn(g[q]);
+        uint4* p = reinterpret_cast<uint4*>(gimg + q * 16);
+        p[0] = w0;
+        p[1] = w1;
+    }
+}
+
+// sums over fluid cells of z and e, both brought to the network's output
+// units by *tscale, and the fluid count
+__global__ void loss_sums_kernel(const float* __restrict__ z, const double* __restrict__ e, const float* __restrict__ mask,
+                                 const double* tscale, double* sums, long long n) {
+    double sz = 0.0, se = 0.0, sn = 0.0;
+    const double ts = *tscale;
+    GS(q, n) {
+        if (mask[q] > 0.0f) {
+            sz += z[q] * ts;
+            se += e[q] * ts;
+            sn += 1.0;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sz += __shfl_down_sync(0xffffffffu, sz, o);
+        se += __shfl_down_sync(0xffffffffu, se, o);
+        sn += __shfl_down_sync(0xffffffffu, sn, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&sums[0], sz);
+        atomicAdd(&sums[1], se);
+        atomicAdd(&sums[2], sn);
+    }
+}
+
+// in network units (z' = z tscale, e' = e tscale): d = (z' - mean z') -
+// (e' - mean e') on fluid cells; loss += d^2 / n_f, g = dloss/dz' = 2 d / n_f
+__global__ void loss_grad_kernel(const float* __restrict__ z, const double* __restrict__ e,
+                                 const float* __restrict__ mask, const double* tscale, double* sums,
+                                 float* __restrict__ g, long long n) {
+    const double nf = sums[2] > 0.0 ? sums[2] : 1.0;
+    const double mz = sums[0] / nf, me = sums[1] / nf, ts = *tscale;
+    double l = 0.0;
+    GS(q, n) {
+        float gv = 0.0f;
+        if (mask[q] > 0.0f) {
+            const double d = (z[q] * ts - mz) - (e[q] * ts - me);
+            l += d * d;
+            gv = (float)(2.0 * d / nf);
+        }
+        g[q] = gv;
+    }
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&sums[3], l / nf);
+}
+
+// Adam on the FP32 master parameters (Kingma & Ba 2015), gradients zeroed after use
+__global__ void adam_kernel(float* __restrict__ p, float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                            long long n, float lr, float b1, float b2, float eps, float c1, float c2) {
+    GS(q, n) {
+        const float gq = g[q];
+        const float mq = b1 * m[q] + (1.0f - b1) * gq;
+        const float vq = b2 * v[q] + (1.0f - b2) * gq * gq;
+        m[q] = mq;
+        v[q] = vq;
+        p[q] -= lr * (mq / c1) / (sqrtf(vq / c2) + eps);
+        g[q] = 0.0f;
+    }
+}
+
+// s = sqrt(n_fluid) / |r|, from a reduction of r^2 over fluid cells
+__global__ void rscale_kernel(const double* __restrict__ r, const float* __restrict__ mask, double* acc, long long n) {
+    double s = 0.0, c = 0.0;
+    GS(q, n) {
+        if (mask[q] > 0.0f) {
+            s += r[q] * r[q];
+            c += 1.0;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, o);
+        c += __shfl_down_sync(0xffffffffu, c, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&acc[0], s);
+        atomicAdd(&acc[1], c);
+    }
+}
+
+// scale[0] = sqrt(n_f / sum r^2) (network input scale); scale[1] = out_scale / scale[0]
+// (network output -> error); scale[2] = 1 / scale[1] (error -> training target)
+__global__ void rscale_final_kernel(const double* acc, double* scale, const double* out_scale) {
+    const double s = acc[0] > 0.0 ? sqrt(acc[1] / acc[0]) : 1.0;
+    scale[0] = s;
+    scale[1] = *out_scale / s;
+    scale[2] = s / *out_scale;
+}
+
+#undef GS
+
+}  // namespace un
