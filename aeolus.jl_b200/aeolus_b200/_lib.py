@@ -21,7 +21,7 @@ SYMBOLS = (
     "aeo_version",
     "aeo_mg_create", "aeo_mg_destroy", "aeo_mg_levels", "aeo_mg_solve", "aeo_mg_solve_device",
     "aeo_mg_vcycle_solve", "aeo_mg_apply", "aeo_mg_precondition", "aeo_mg_profile",
-    "aeo_mg_launches_per_iteration", "aeo_mg_last_error",
+    "aeo_mg_launches_per_iteration", "aeo_mg_last_error", "aeo_mg_set_learned", "aeo_mg_solve_harvest",
     "aeo_unet_param_count", "aeo_unet_create", "aeo_unet_destroy", "aeo_unet_set_params", "aeo_unet_get_params",
     "aeo_unet_set_mask", "aeo_unet_set_out_scale", "aeo_unet_apply", "aeo_unet_gradients", "aeo_unet_train_step",
     "aeo_unet_activation", "aeo_unet_profile", "aeo_unet_last_error",
@@ -74,7 +74,7 @@ class AeoMgConfig(C.Structure):
 
 class AeoMgStats(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("status", C.c_int32), ("residual", C.c_double),
-                ("bnorm", C.c_double), ("curvature", C.c_double)]
+                ("bnorm", C.c_double), ("curvature", C.c_double), ("fallback_at", C.c_int32)]
 
 
 LIMITERS = ("advective", "diffusive", "buoyancy", "coriolis", "sgs", "growth", "dt_min", "dt_max", "retried")
@@ -147,6 +147,8 @@ def load():
     lib.aeo_mg_launches_per_iteration.argtypes = [P]
     lib.aeo_mg_last_error.argtypes = [P]
     lib.aeo_mg_last_error.restype = C.c_char_p
+    lib.aeo_mg_set_learned.argtypes = [P, P, C.c_double]
+    lib.aeo_mg_solve_harvest.argtypes = [P, D, D, C.POINTER(AeoMgStats), D, D, C.c_int32, C.POINTER(C.c_int32)]
     F = C.POINTER(C.c_float)
     lib.aeo_unet_param_count.restype = C.c_int64
     lib.aeo_unet_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_int32, C.POINTER(P)]

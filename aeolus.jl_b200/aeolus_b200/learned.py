@@ -1,0 +1,86 @@
+"""Training the learned U-Net preconditioner on residual -> error pairs
+harvested from plain (multigrid-preconditioned) CG solves of cut-cell urban
+pressure problems, and using it in flexible CG.
+
+    pairs = harvest_pairs(problems, cap=12)          # [(r_k, e_k)]
+    net = train_unet(shape, pairs, steps=2000)
+    mg.set_learned(net)                              # flexible CG with the network
+
+A pair (r_k, e_k) is the residual after k CG iterations and the error
+x* - x_k of that iterate against the converged solution, so A e_k = r_k.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .cutcell import box_geometry, face_coefficients, pressure_rhs, random_boxes, urban_velocity
+from .grids import regular_grid
+from .multigrid import MGPreconditionedCG
+from .unet import UNet, error_scale
+
+
+def urban_geometry(n, seed, nboxes, delta=2.0):
+    """The grid and cut-cell geometry of `nboxes` floor-standing boxes from
+    `seed` on n cells of `delta` metres."""
+    g = regular_grid(n, tuple(delta * v for v in n), halo=(3, 3, 3), bc_z="wall")
+    return g, box_geometry(g, random_boxes(g, nboxes, seed=seed), nsub=4)
+
+
+def urban_rhs(g, geom, noise_seed):
+    """The right-hand side from a log-profile inflow with seeded noise."""
+    u, v, w = urban_velocity(g, geom, seed=noise_seed)
+    return pressure_rhs(geom, u, v, w)
+
+
+def urban_problem(n, seed, nboxes, delta=2.0, noise_seed=None):
+    """Face coefficients, right-hand side and fluid mask of the cut-cell
+    urban pressure problem (noise from `noise_seed`, default `seed`)."""
+    g, geom = urban_geometry(n, seed, nboxes, delta)
+    fluid = (~geom.is_solid[g.interior]).astype(np.float32)
+    return face_coefficients(geom), urban_rhs(g, geom, seed if noise_seed is None else noise_seed), fluid
+
+
+def harvest_pairs(n, seeds, rhs_per_geometry, nboxes, cap=12, delta=2.0, tol=1e-8):
+    """Residual -> error pairs (with the fluid mask of their geometry) from
+    plain MG-preconditioned CG solves: for each geometry seed,
+    `rhs_per_geometry` right-hand sides with fresh noise seeds."""
+    out = []
+    for s in seeds:
+        g, geom = urban_geometry(n, s, nboxes, delta)
+        fluid = (~geom.is_solid[g.interior]).astype(np.float32)
+        mg = MGPreconditionedCG(n, (delta,) * 3, coeffs=face_coefficients(geom), tol=tol)
+        for q in range(rhs_per_geometry):
+            b = urban_rhs(g, geom, 1000 * s + q)
+            x, st, pairs = mg.solve_harvest(b, cap)
+            out.extend((r, e, fluid) for r, e in pairs if np.linalg.norm(r) > 0)
+    return out
+
+
+def train_unet(n, pairs, steps, lr=1e-3, seed=0, net=None, lr_final=1e-4):
+    """Adam on the pairs (cycled in a seeded random order), the learning rate
+    decaying geometrically from lr to lr_final.  Returns (net, losses)."""
+    if net is None:
+        net = UNet(n, seed=seed)
+    net.set_out_scale(error_scale([(r, e) for r, e, _ in pairs]))
+    rng = np.random.default_rng(seed)
+    order = rng.permutation(len(pairs))
+    losses = []
+    mask_id = None
+    for it in range(steps):
+        r, e, fluid = pairs[order[it % len(pairs)]]
+        if mask_id is not id(fluid):
+            net.set_mask(fluid)
+            mask_id = id(fluid)
+        a = lr * (lr_final / lr) ** (it / max(steps - 1, 1))
+        losses.append(net.train_step(r, e, a))
+    return net, np.array(losses)
+
+
+def transfer(net, n, fluid):
+    """The trained weights and output scale on a network for another grid
+    (the convolutions are size-independent), with that grid's fluid mask."""
+    other = UNet(n)
+    other.set_params(net.params())
+    other.set_mask(fluid)
+    other.set_out_scale(net.out_scale)
+    return other

@@ -20,7 +20,7 @@ import numpy as np
 from . import _lib as L
 
 BCS = {"periodic": 0, "neumann": 1}
-PRECONDITIONERS = {"identity": 0, "vcycle": 1}
+PRECONDITIONERS = {"identity": 0, "vcycle": 1}   # "learned": see MGPreconditionedCG.set_learned
 PRECISIONS = {"fp64": 0, "fp32_mixed": 1}
 STATUS = {0: "converged", 1: "maxit", 2: "breakdown", 3: "zero_rhs"}
 
@@ -100,7 +100,7 @@ class MGPreconditionedCG:
         return {"iterations": st.iterations, "status": STATUS[st.status], "residual": st.residual,
                 "bnorm": st.bnorm,
                 "relative_residual": st.residual if relative else (0.0 if st.bnorm == 0 else st.residual / st.bnorm),
-                "curvature": st.curvature}
+                "curvature": st.curvature, "fallback_at": st.fallback_at}
 
     def solve(self, b, out=None):
         """x = A^-1 b by MG-preconditioned CG (solve!, src/Multigrid.jl:955-967).
@@ -113,6 +113,29 @@ class MGPreconditionedCG:
         self._chk(L.load().aeo_mg_solve(self._h, _p(b), _p(x), C.byref(st)))
         self.last_stats = self._stats(st, False)
         return x, self.last_stats
+
+    def set_learned(self, net, stagnation=0.9):
+        """Precondition flexible CG with the learned U-Net `net` (an
+        aeolus_b200.unet.UNet of this grid, its mask set); None restores the
+        V-cycle.  A solve falls back to the V-cycle for its remaining
+        iterations after two iterations in a row whose residual fell by less
+        than `stagnation`."""
+        self._chk(L.load().aeo_mg_set_learned(self._h, net.handle if net is not None else None, float(stagnation)))
+        self._net = net
+
+    def solve_harvest(self, b, cap=16):
+        """solve() that also returns the residuals r_k and iterates x_k of the
+        CG iterations: (x, stats, [(r_k, x - x_k)]), residual -> error pairs."""
+        b = self._arr(b)
+        x = np.empty(self.shape)
+        rh = np.empty((cap,) + self.shape)
+        xh = np.empty((cap,) + self.shape)
+        cnt = C.c_int32()
+        st = L.AeoMgStats()
+        self._chk(L.load().aeo_mg_solve_harvest(self._h, _p(b), _p(x), C.byref(st), _p(rh), _p(xh), int(cap),
+                                                C.byref(cnt)))
+        self.last_stats = self._stats(st, False)
+        return x, self.last_stats, [(rh[k], x - xh[k]) for k in range(cnt.value)]
 
     def solve_device(self, b_ptr: int, x_ptr: int):
         """The same on FP64 device arrays (raw device pointers)."""

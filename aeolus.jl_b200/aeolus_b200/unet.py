@@ -61,6 +61,7 @@ class UNet:
         L.check(lib.aeo_unet_create(nx, ny, nz, int(seed), int(device), C.byref(h)), None, unet=True)
         self._h = h
         self.nparams = int(lib.aeo_unet_param_count())
+        self.out_scale = 1.0
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -105,6 +106,7 @@ class UNet:
 
     def set_out_scale(self, s):
         self._chk(L.load().aeo_unet_set_out_scale(self._h, float(s)))
+        self.out_scale = float(s)
 
     def apply(self, r):
         r = self._arr(r)

@@ -32,6 +32,11 @@ struct PcgState {
     int iters, maxit, status, done;
     int project, flexible;
     unsigned counter;
+    // learned preconditioner: in use (learned), at set-up (learned_init), the
+    // iteration it was dropped at (-1: never), slow iterations in a row, the
+    // previous residual norm and the stagnation ratio
+    int learned, learned_init, fallback_at, slow;
+    double rprev, stag;
 };
 
 // Face coefficients of one level: value arrays, or one-byte codes into a
@@ -234,6 +239,9 @@ __global__ void pcg_init_kernel(const double* __restrict__ b, double* __restrict
         S->curvature = nan("");
         S->rz = 0.0;
         S->alpha = S->beta = 0.0;
+        S->learned = S->learned_init;
+        S->fallback_at = -1;
+        S->slow = 0;
         if (S->bnorm == 0.0) {
             S->status = MG_ZERO_RHS;
             S->done = 3;
@@ -331,6 +339,7 @@ __global__ void pcg_rz_kernel(const double* __restrict__ r, const Z* __restrict_
             S->rz = rzn;
             S->beta = 0.0;
             S->rnorm = sqrt(t[0]);
+            S->rprev = S->rnorm;
             if (S->rnorm <= S->tol * S->bnorm) {
                 S->status = MG_CONVERGED;
                 S->done = 1;
@@ -360,6 +369,37 @@ __global__ void pcg_cond_kernel(PcgState* S, cudaGraphConditionalHandle h, int m
     unsigned go = (S->done == 0 && S->iters < S->maxit) ? 1u : 0u;
     if (mode == 0 && S->done == 0 && S->iters >= S->maxit) S->status = MG_MAXIT;
     cudaGraphSetConditional(h, go);
+}
+
+// The preconditioner of the next application (the IF node's value): the
+// learned network while it keeps the residual falling; from the second
+// iteration in a row whose residual fell by less than the stagnation ratio
+// on, the multigrid cycle for the rest of the solve.
+__global__ void pcg_select_kernel(PcgState* S, cudaGraphConditionalHandle h) {
+    if (S->done == 0 && S->learned) {
+        if (S->rnorm > S->stag * S->rprev) {
+            if (++S->slow >= 2) {
+                S->learned = 0;
+                S->fallback_at = S->iters;
+            }
+        } else {
+            S->slow = 0;
+        }
+    }
+    S->rprev = S->rnorm;
+    cudaGraphSetConditional(h, (S->done == 0 && S->learned) ? 1u : 0u);
+}
+
+// the iterate and residual after `iters` updates into slot iters of the
+// history (residual -> error training pairs of the plain solve)
+__global__ void pcg_harvest_kernel(const double* __restrict__ x, const double* __restrict__ r, double* __restrict__ hx,
+                                   double* __restrict__ hr, int n, int cap, const PcgState* S) {
+    const int slot = S->iters;
+    if (slot >= cap) return;
+    GRID_STRIDE(q, n) {
+        hx[(size_t)slot * n + q] = x[q];
+        hr[(size_t)slot * n + q] = r[q];
+    }
 }
 
 __global__ void shift_kernel(double* __restrict__ x, int n, const PcgState* S) {

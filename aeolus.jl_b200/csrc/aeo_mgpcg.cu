@@ -55,7 +55,13 @@
 #include <vector>
 
 #include "../../include/aeolus_b200_mgpcg.h"
+#include "../../include/aeolus_b200_unet.h"
 #include "aeo_mg_kernels.cuh"
+
+// the learned preconditioner's forward pass on a device residual (aeo_unet.cu)
+aeo_status aeo_unet_forward_on(aeo_unet* h, const double* r_dev, cudaStream_t s);
+const float* aeo_unet_output(const aeo_unet* h);
+long long aeo_unet_cells(const aeo_unet* h);
 
 namespace {
 
@@ -77,6 +83,9 @@ struct MgBase {
     virtual int nlevels() const = 0;
     virtual void level_dims(int l, int32_t* d) const = 0;
     virtual int launches_per_iteration() const = 0;
+    virtual aeo_status set_learned(aeo_unet* net, double stag) = 0;
+    virtual aeo_status harvest(const double* b, double* x, aeo_mg_stats* st, double* rh, double* xh, int cap,
+                               int* count) = 0;
 };
 
 #define CK(call)                                                                         \
@@ -172,7 +181,12 @@ bool encode(const std::vector<double>& x, const std::vector<double>& y, const st
 
 template <typename R>
 struct Mg : MgBase {
-    cudaStream_t st = nullptr, st_body = nullptr;
+    cudaStream_t st = nullptr, st_body = nullptr, st_br[2] = {nullptr, nullptr};
+    aeo_unet* net = nullptr;       // the learned preconditioner (AEO_PC_LEARNED)
+    double* hist_x = nullptr;      // harvest history, `hist_cap` slots of n
+    double* hist_r = nullptr;
+    int hist_cap = 0;
+    cudaGraphExec_t g_harvest = nullptr;
     Bc bc{0, 0, 0};
     int nl = 0;
     int n = 0;
@@ -204,10 +218,15 @@ struct Mg : MgBase {
         if (st) cudaStreamSynchronize(st);
         if (g_solve) cudaGraphExecDestroy(g_solve);
         if (g_cycles) cudaGraphExecDestroy(g_cycles);
+        if (g_harvest) cudaGraphExecDestroy(g_harvest);
         for (void* a : allocs) cudaFree(a);
+        if (hist_x) cudaFree(hist_x);
+        if (hist_r) cudaFree(hist_r);
         if (hS) cudaFreeHost(hS);
         if (st) cudaStreamDestroy(st);
         if (st_body) cudaStreamDestroy(st_body);
+        for (cudaStream_t b_ : st_br)
+            if (b_) cudaStreamDestroy(b_);
     }
 
     template <typename T>
@@ -253,6 +272,8 @@ struct Mg : MgBase {
         bc = {cfg.bc_x, cfg.bc_y, cfg.bc_z};
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&st_body, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&st_br[0], cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&st_br[1], cudaStreamNonBlocking));
         const bool coeff = cx != nullptr;
         int nx = cfg.nx, ny = cfg.ny, nz = cfg.nz;
         double dx = cfg.dx, dy = cfg.dy, dz = cfg.dz;
@@ -490,9 +511,15 @@ struct Mg : MgBase {
         return AEO_OK;
     }
 
-    // z: level-0 phi after the cycle, or r itself for plain CG
-    aeo_status launch_rz_dir(cudaStream_t s, int first) {
-        if (cfg.precond == AEO_PC_VCYCLE) {
+    // z: level-0 phi after the cycle, the network's output, or r itself for plain CG
+    aeo_status launch_rz_dir(cudaStream_t s, int first, int pc = -1) {
+        if (pc < 0) pc = cfg.precond;
+        if (pc == AEO_PC_LEARNED) {
+            const float* zf = aeo_unet_output(net);
+            pcg_rz_kernel<float><<<RED_BLOCKS, TPB, 0, s>>>(r, zf, Ap, n, S, part, first);
+            CKL();
+            pcg_dir_kernel<float><<<RED_BLOCKS, TPB, 0, s>>>(p, zf, n, S, first);
+        } else if (pc == AEO_PC_VCYCLE) {
             pcg_rz_kernel<R><<<RED_BLOCKS, TPB, 0, s>>>(r, L[0].phi, Ap, n, S, part, first);
             CKL();
             pcg_dir_kernel<R><<<RED_BLOCKS, TPB, 0, s>>>(p, L[0].phi, n, S, first);
@@ -519,16 +546,31 @@ struct Mg : MgBase {
         return AEO_OK;
     }
 
-    // Adds a WHILE node on `hdl` to the graph being captured on `st`,
-    // captures `body` into its body graph on st_body, and continues the
-    // capture after it.
-    template <typename F>
-    aeo_status capture_while(cudaGraphConditionalHandle hdl, F body) {
+    // A conditional handle on the graph being captured on `s`, value `dflt`
+    // at every launch until a kernel sets it.
+    aeo_status make_handle_on(cudaStream_t s, cudaGraphConditionalHandle* hdl, unsigned dflt) {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, nullptr, nullptr));
+        if (cs != cudaStreamCaptureStatusActive) {
+            fail("internal: stream is not capturing");
+            return AEO_ERR_STATE;
+        }
+        CK(cudaGraphConditionalHandleCreate(hdl, g, dflt, cudaGraphCondAssignDefault));
+        return AEO_OK;
+    }
+
+    // Adds a conditional node (WHILE with one body, or IF with one or two) on
+    // `hdl` to the graph being captured on `s`, captures body i on stream
+    // bs[i], and continues the capture on `s` after the node.
+    template <typename F0, typename F1>
+    aeo_status capture_cond(cudaStream_t s, cudaGraphConditionalHandle hdl, cudaGraphConditionalNodeType type,
+                            int nbodies, const cudaStream_t* bs, F0 body0, F1 body1) {
         cudaStreamCaptureStatus cs;
         cudaGraph_t g = nullptr;
         const cudaGraphNode_t* deps = nullptr;
         size_t ndeps = 0;
-        CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps));
+        CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &ndeps));
         if (cs != cudaStreamCaptureStatusActive) {
             fail("internal: stream is not capturing");
             return AEO_ERR_STATE;
@@ -536,23 +578,54 @@ struct Mg : MgBase {
         cudaGraphNodeParams cp = {};
         cp.type = cudaGraphNodeTypeConditional;
         cp.conditional.handle = hdl;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
+        cp.conditional.type = type;
+        cp.conditional.size = (unsigned)nbodies;
         cudaGraphNode_t node;
         std::vector<cudaGraphNode_t> dv(deps, deps + ndeps);
         CK(cudaGraphAddNode(&node, g, dv.data(), dv.size(), &cp));
-        cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
-        CK(cudaStreamBeginCaptureToGraph(st_body, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-        aeo_status bs = body(st_body);
-        cudaGraph_t out = nullptr;
-        cudaError_t e = cudaStreamEndCapture(st_body, &out);
-        if (bs) return bs;
-        if (e != cudaSuccess) {
-            fail(std::string("cudaStreamEndCapture(body): ") + cudaGetErrorString(e));
-            return AEO_ERR_CUDA;
+        for (int i = 0; i < nbodies; ++i) {
+            cudaGraph_t bodyg = cp.conditional.phGraph_out[i];
+            CK(cudaStreamBeginCaptureToGraph(bs[i], bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+            aeo_status q = i == 0 ? body0(bs[i]) : body1(bs[i]);
+            cudaGraph_t out = nullptr;
+            cudaError_t e = cudaStreamEndCapture(bs[i], &out);
+            if (q) return q;
+            if (e != cudaSuccess) {
+                fail(std::string("cudaStreamEndCapture(body): ") + cudaGetErrorString(e));
+                return AEO_ERR_CUDA;
+            }
         }
-        CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+        CK(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
         return AEO_OK;
+    }
+
+    template <typename F>
+    aeo_status capture_while(cudaGraphConditionalHandle hdl, F body) {
+        return capture_cond(st, hdl, cudaGraphCondTypeWhile, 1, &st_body, body,
+                            [](cudaStream_t) -> aeo_status { return AEO_OK; });
+    }
+
+    // the preconditioner application of the body: the network or, after a
+    // stagnation, the multigrid cycle, chosen on the device by an IF node
+    aeo_status launch_learned_pc(cudaStream_t sb, int* count) {
+        cudaGraphConditionalHandle h2;
+        if (aeo_status q = make_handle_on(sb, &h2, 1)) return q;
+        pcg_select_kernel<<<1, 1, 0, sb>>>(S, h2);
+        CKL();
+        *count += 1;
+        return capture_cond(
+            sb, h2, cudaGraphCondTypeIf, 2, st_br,
+            [&](cudaStream_t s0) -> aeo_status {
+                if (aeo_status q = aeo_unet_forward_on(net, r, s0)) {
+                    fail("learned preconditioner: forward pass could not be captured");
+                    return q;
+                }
+                return launch_rz_dir(s0, 0, AEO_PC_LEARNED);
+            },
+            [&](cudaStream_t s1) -> aeo_status {
+                if (aeo_status q = launch_vcycle(s1, r, true, &S->done)) return q;
+                return launch_rz_dir(s1, 0, AEO_PC_VCYCLE);
+            });
     }
 
     aeo_status end_capture(cudaGraphExec_t* ex, aeo_status s) {
@@ -578,7 +651,7 @@ struct Mg : MgBase {
     // The solve graph: prologue, WHILE(one CG iteration), the mean shift.
     // The loop condition is set by pcg_cond_kernel before the loop and at
     // the end of every iteration.
-    aeo_status build_solve() {
+    aeo_status build_solve(bool harvest = false) {
         CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
         aeo_status s = [&]() -> aeo_status {
             cudaGraphConditionalHandle hdl;
@@ -587,8 +660,14 @@ struct Mg : MgBase {
             CKL();
             pcg_init_kernel<<<RED_BLOCKS, TPB, 0, st>>>(b, r, x, n, S, part);
             CKL();
+            if (harvest) {
+                pcg_harvest_kernel<<<RED_BLOCKS, TPB, 0, st>>>(x, r, hist_x, hist_r, n, hist_cap, S);
+                CKL();
+            }
             if (cfg.precond == AEO_PC_VCYCLE)
                 if (aeo_status q = launch_vcycle(st, r, true, &S->done)) return q;
+            if (cfg.precond == AEO_PC_LEARNED)
+                if (aeo_status q = aeo_unet_forward_on(net, r, st)) return q;
             if (aeo_status q = launch_rz_dir(st, 1)) return q;
             pcg_cond_kernel<<<1, 1, 0, st>>>(S, hdl, 0);
             CKL();
@@ -598,14 +677,25 @@ struct Mg : MgBase {
                     pcg_update_kernel<<<RED_BLOCKS, TPB, 0, sb>>>(x, r, p, Ap, n, S, part);
                     CKL();
                     c0 += 2;
-                    if (cfg.precond == AEO_PC_VCYCLE) {
-                        if (aeo_status q2 = launch_vcycle(sb, r, true, &S->done)) return q2;
-                        c0 += vcycle_launches();
+                    if (harvest) {
+                        pcg_harvest_kernel<<<RED_BLOCKS, TPB, 0, sb>>>(x, r, hist_x, hist_r, n, hist_cap, S);
+                        CKL();
+                        c0 += 1;
                     }
-                    if (aeo_status q2 = launch_rz_dir(sb, 0)) return q2;
+                    if (cfg.precond == AEO_PC_LEARNED) {
+                        if (aeo_status q2 = launch_learned_pc(sb, &c0)) return q2;
+                        c0 += 2;
+                    } else {
+                        if (cfg.precond == AEO_PC_VCYCLE) {
+                            if (aeo_status q2 = launch_vcycle(sb, r, true, &S->done)) return q2;
+                            c0 += vcycle_launches();
+                        }
+                        if (aeo_status q2 = launch_rz_dir(sb, 0)) return q2;
+                        c0 += 2;
+                    }
                     pcg_cond_kernel<<<1, 1, 0, sb>>>(S, hdl, 0);
                     CKL();
-                    body_launches = c0 + 3;
+                    body_launches = c0 + 1;
                     return AEO_OK;
                 }))
                 return q;
@@ -615,7 +705,7 @@ struct Mg : MgBase {
             CKL();
             return AEO_OK;
         }();
-        return end_capture(&g_solve, s);
+        return end_capture(harvest ? &g_harvest : &g_solve, s);
     }
 
     aeo_status stats_out(aeo_mg_stats* o, bool relative) {
@@ -627,6 +717,7 @@ struct Mg : MgBase {
             o->residual = relative ? hS->rel : hS->rnorm;
             o->bnorm = hS->bnorm;
             o->curvature = hS->curvature;
+            o->fallback_at = hS->fallback_at;
             if (hS->status == AEO_MG_ZERO_RHS) o->residual = 0.0;
         }
         return AEO_OK;
@@ -699,7 +790,14 @@ struct Mg : MgBase {
     // z = M r: r loaded with its mean removed (as in the solve), one cycle,
     // then z - mean(z) (the deflated preconditioner of the reference)
     aeo_status precondition(const double* rin, double* zout) override {
-        if (cfg.precond != AEO_PC_VCYCLE) {
+        if (cfg.precond == AEO_PC_LEARNED) {
+            CK(cudaMemcpyAsync(r, rin, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+            if (aeo_status s = aeo_unet_forward_on(net, r, st)) return s;
+            std::vector<float> hz((size_t)n);
+            CK(cudaMemcpyAsync(hz.data(), aeo_unet_output(net), sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            for (int q = 0; q < n; ++q) zout[q] = double(hz[q]);
+        } else if (cfg.precond != AEO_PC_VCYCLE) {
             std::memcpy(zout, rin, sizeof(double) * n);
         } else {
             CK(cudaMemcpyAsync(b, rin, sizeof(double) * n, cudaMemcpyHostToDevice, st));
@@ -717,6 +815,58 @@ struct Mg : MgBase {
         for (int q = 0; q < n; ++q) s += zout[q];
         s /= double(n);
         for (int q = 0; q < n; ++q) zout[q] -= s;
+        return AEO_OK;
+    }
+
+    void drop_graphs() {
+        if (g_solve) cudaGraphExecDestroy(g_solve);
+        if (g_harvest) cudaGraphExecDestroy(g_harvest);
+        g_solve = g_harvest = nullptr;
+    }
+
+    aeo_status set_learned(aeo_unet* nn, double stag) override {
+        if (nn && aeo_unet_cells(nn) != (long long)n) {
+            fail("set_learned: the network's grid differs from the solver's");
+            return AEO_ERR_ARGUMENT;
+        }
+        CK(cudaStreamSynchronize(st));
+        drop_graphs();
+        net = nn;
+        cfg.precond = nn ? AEO_PC_LEARNED : AEO_PC_VCYCLE;
+        PcgState h0{};
+        CK(cudaMemcpy(&h0, S, sizeof(PcgState), cudaMemcpyDeviceToHost));
+        h0.learned_init = nn ? 1 : 0;
+        h0.stag = stag;
+        h0.flexible = nn ? 1 : cfg.flexible;
+        CK(cudaMemcpy(S, &h0, sizeof(PcgState), cudaMemcpyHostToDevice));
+        return AEO_OK;
+    }
+
+    aeo_status harvest(const double* bin, double* xout, aeo_mg_stats* o, double* rh, double* xh, int cap,
+                       int* count) override {
+        if (cap != hist_cap) {
+            CK(cudaStreamSynchronize(st));
+            if (hist_x) cudaFree(hist_x);
+            if (hist_r) cudaFree(hist_r);
+            hist_x = hist_r = nullptr;
+            hist_cap = 0;
+            if (g_harvest) cudaGraphExecDestroy(g_harvest);
+            g_harvest = nullptr;
+            CK(cudaMalloc(&hist_x, sizeof(double) * (size_t)cap * n));
+            CK(cudaMalloc(&hist_r, sizeof(double) * (size_t)cap * n));
+            hist_cap = cap;
+        }
+        if (!g_harvest)
+            if (aeo_status s = build_solve(true)) return s;
+        CK(cudaMemcpyAsync(b, bin, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+        CK(cudaGraphLaunch(g_harvest, st));
+        CK(cudaMemcpyAsync(xout, x, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        if (aeo_status s = stats_out(o, false)) return s;
+        const int c = hS->iters + 1 < cap ? hS->iters + 1 : cap;
+        CK(cudaMemcpyAsync(rh, hist_r, sizeof(double) * (size_t)c * n, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(xh, hist_x, sizeof(double) * (size_t)c * n, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        *count = c;
         return AEO_OK;
     }
 
@@ -880,6 +1030,25 @@ aeo_status aeo_mg_profile(aeo_mg* h, int32_t what, int32_t reps, double* ms) {
 }
 
 int32_t aeo_mg_launches_per_iteration(const aeo_mg* h) { return h ? h->core->launches_per_iteration() : 0; }
+
+aeo_status aeo_mg_set_learned(aeo_mg* h, aeo_unet* net, double stagnation) {
+    MG_ENTER(h);
+    if (net && !(stagnation > 0 && stagnation <= 1)) {
+        h->core->fail("set_learned: the stagnation ratio lies in (0, 1]");
+        return AEO_ERR_ARGUMENT;
+    }
+    return h->core->set_learned(net, stagnation);
+}
+
+aeo_status aeo_mg_solve_harvest(aeo_mg* h, const double* b, double* x, aeo_mg_stats* st, double* r_hist,
+                                double* x_hist, int32_t cap, int32_t* count) {
+    MG_ENTER(h);
+    if (!b || !x || !r_hist || !x_hist || !count || cap < 1) {
+        h->core->fail("solve_harvest: NULL array or cap < 1");
+        return AEO_ERR_ARGUMENT;
+    }
+    return h->core->harvest(b, x, st, r_hist, x_hist, cap, count);
+}
 
 const char* aeo_mg_last_error(const aeo_mg* h) { return h ? h->core->err.c_str() : g_mg_error.c_str(); }
 

@@ -36,8 +36,9 @@ extern "C" {
 
 enum { AEO_MG_PERIODIC = 0, AEO_MG_NEUMANN = 1 };
 /* preconditioner of the CG iteration: none (plain CG), one multigrid cycle
- * per application (the reference's MGPreconditionedCG) */
-enum { AEO_PC_IDENTITY = 0, AEO_PC_VCYCLE = 1 };
+ * per application (the reference's MGPreconditionedCG), or the learned U-Net
+ * of aeolus_b200_unet.h (set by aeo_mg_set_learned; no reference counterpart) */
+enum { AEO_PC_IDENTITY = 0, AEO_PC_VCYCLE = 1, AEO_PC_LEARNED = 2 };
 /* solve status (the reference's :converged, :maxit, :breakdown, :zero_rhs) */
 enum { AEO_MG_CONVERGED = 0, AEO_MG_MAXIT = 1, AEO_MG_BREAKDOWN = 2, AEO_MG_ZERO_RHS = 3 };
 
@@ -65,9 +66,12 @@ typedef struct {
     double residual;           /* ||r|| of the last iterate (relative for aeo_mg_vcycle_solve) */
     double bnorm;              /* ||b - mean(b)|| */
     double curvature;          /* the last p.Ap formed (NaN if none) */
+    int32_t fallback_at;       /* learned preconditioner: the iteration it was dropped for the
+                                  multigrid cycle after stagnating, -1 if never */
 } aeo_mg_stats;
 
 typedef struct aeo_mg aeo_mg;
+struct aeo_unet;
 
 /* cx, cy, cz: host face coefficients, or all NULL for the constant-coefficient
  * Laplacian.  Fails with AEO_ERR_ARGUMENT when the coarsest level exceeds
@@ -94,6 +98,20 @@ aeo_status aeo_mg_precondition(aeo_mg* h, const double* r, double* z);
  * p.Ap reduction, 3 one preconditioner application, 4 the coarsest-level
  * solve, 5 the residual restriction of the finest level.  ms_out: mean ms. */
 aeo_status aeo_mg_profile(aeo_mg* h, int32_t what, int32_t reps, double* ms_out);
+/* The learned preconditioner (no reference counterpart): `net` (same grid;
+ * NULL detaches it) preconditions flexible CG from the next solve on.  When
+ * an iteration's residual falls by less than `stagnation` (ratio of norms)
+ * twice in a row, the solve switches to the multigrid cycle for its
+ * remaining iterations, on the device inside the solve graph; every solve
+ * still stops at ||r|| <= tol ||b||. */
+aeo_status aeo_mg_set_learned(aeo_mg* h, struct aeo_unet* net, double stagnation);
+/* aeo_mg_solve that also returns its residuals and iterates: slot k of
+ * r_hist / x_hist (cap slots of nx*ny*nz doubles each) holds r_k and x_k
+ * after k updates (slot 0: b - mean b and 0); *count = the slots filled.
+ * The pairs (r_k, x - x_k) are residual -> error pairs of this solve (no
+ * reference counterpart: the training data of the learned preconditioner). */
+aeo_status aeo_mg_solve_harvest(aeo_mg* h, const double* b, double* x, aeo_mg_stats* stats, double* r_hist,
+                                double* x_hist, int32_t cap, int32_t* count);
 /* kernel launches of one CG iteration (graph body) */
 int32_t aeo_mg_launches_per_iteration(const aeo_mg* h);
 const char* aeo_mg_last_error(const aeo_mg* h);
