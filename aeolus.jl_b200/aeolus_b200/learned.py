@@ -76,6 +76,38 @@ def train_unet(n, pairs, steps, lr=1e-3, seed=0, net=None, lr_final=1e-4):
     return net, np.array(losses)
 
 
+def train_streaming(n, seeds, rhs_per_geometry, nboxes, pairs_total, cap=12, lr=1e-3, lr_final=1e-4, seed=0,
+                    delta=2.0, warm_pairs=None):
+    """Harvest and train geometry by geometry (the pairs of one geometry in
+    memory at a time): each harvested pair is used for one Adam step, up to
+    `pairs_total` steps.  The output scale comes from the first geometry's
+    pairs (or `warm_pairs`).  Returns (net, losses, pairs used)."""
+    net = UNet(n, seed=seed)
+    losses, used = [], 0
+    rng = np.random.default_rng(seed)
+    for gi, s in enumerate(seeds):
+        g, geom = urban_geometry(n, s, nboxes, delta)
+        fluid = (~geom.is_solid[g.interior]).astype(np.float32)
+        mg = MGPreconditionedCG(n, (delta,) * 3, coeffs=face_coefficients(geom), tol=1e-8)
+        pairs = []
+        for q in range(rhs_per_geometry):
+            _, _, ps = mg.solve_harvest(urban_rhs(g, geom, 1000 * s + q), cap)
+            pairs.extend(p for p in ps if np.linalg.norm(p[0]) > 0)
+        if gi == 0:
+            net.set_out_scale(error_scale(warm_pairs or pairs))
+        net.set_mask(fluid)
+        for k in rng.permutation(len(pairs)):
+            if used >= pairs_total:
+                break
+            a = lr * (lr_final / lr) ** (used / max(pairs_total - 1, 1))
+            losses.append(net.train_step(pairs[k][0], pairs[k][1], a))
+            used += 1
+        del pairs, mg
+        if used >= pairs_total:
+            break
+    return net, np.array(losses), used
+
+
 def transfer(net, n, fluid):
     """The trained weights and output scale on a network for another grid
     (the convolutions are size-independent), with that grid's fluid mask."""

@@ -68,9 +68,16 @@ int grid_for(long long n, int tpb = 256) {
     return (int)(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
 }
 
+constexpr size_t SMEM_CAP = 227 * 1024;
+
+template <int CIN>
+size_t stage_bytes(const Tiles& T) { return (size_t)(CIN / 8) * T.np * T.pitch * 16; }
+// two staging buffers when they fit, else one
+template <int CIN, int COUT>
+bool fwd_dbuf(const Tiles& T) { return un::conv_smem_weights<CIN, COUT>() + 2 * stage_bytes<CIN>(T) <= SMEM_CAP; }
 template <int CIN, int COUT>
 size_t fwd_smem(const Tiles& T) {
-    return un::conv_smem_weights<CIN, COUT>() + (size_t)(CIN / 8) * T.np * T.pitch * 16;
+    return un::conv_smem_weights<CIN, COUT>() + (fwd_dbuf<CIN, COUT>(T) ? 2 : 1) * stage_bytes<CIN>(T);
 }
 template <int CIN, int COUT>
 size_t wg_smem(const Tiles& T) {
@@ -180,7 +187,7 @@ struct aeo_unet {
         if (aeo_status s = dalloc(&rbuf, n0)) return s;
         if (aeo_status s = dalloc(&ebuf, n0)) return s;
         if (aeo_status s = dalloc(&scale, 4)) return s;
-        if (aeo_status s = dalloc(&acc, 8)) return s;
+        if (aeo_status s = dalloc(&acc, 10)) return s;
         if (aeo_status s = dalloc(&derr, 1)) return s;
         CK(cudaMemset(derr, 0, sizeof(int)));
         std::vector<float> ones((size_t)n0, 1.0f);
@@ -203,7 +210,7 @@ struct aeo_unet {
             w3232 = std::max(w3232, wg_smem<32, 32>(T[l]));
             w3216 = std::max(w3216, wg_smem<32, 16>(T[l]));
         }
-        const size_t cap = 227 * 1024;
+        const size_t cap = SMEM_CAP;
         for (size_t v : {f1616, f1632, f3232, f3216, w1616, w1632, w3232, w3216})
             if (v > cap) {
                 err = "U-Net tile needs more shared memory than a block has";
@@ -262,6 +269,10 @@ struct aeo_unet {
         a.out0_scale = out0_scale;
         a.relu = relu;
         a.err = derr;
+        if (ci == 16 && co == 16) a.dbuf = fwd_dbuf<16, 16>(Tl);
+        else if (ci == 16 && co == 32) a.dbuf = fwd_dbuf<16, 32>(Tl);
+        else if (ci == 32 && co == 32) a.dbuf = fwd_dbuf<32, 32>(Tl);
+        else a.dbuf = fwd_dbuf<32, 16>(Tl);
         const int gsz = conv_grid(Tl);
         if (ci == 16 && co == 16) un::conv_fwd_kernel<16, 16><<<gsz, un::CONV_THREADS, fwd_smem<16, 16>(Tl), st>>>(a);
         else if (ci == 16 && co == 32) un::conv_fwd_kernel<16, 32><<<gsz, un::CONV_THREADS, fwd_smem<16, 32>(Tl), st>>>(a);
@@ -330,7 +341,7 @@ struct aeo_unet {
     // gradients of the loss against the error e (FP64 field) into G
     aeo_status backward(const double* e) {
         const int nx1 = nx / 2, ny1 = ny / 2, nz1 = nz / 2;
-        CK(cudaMemsetAsync(acc + 4, 0, sizeof(double) * 4, st));
+        CK(cudaMemsetAsync(acc + 4, 0, sizeof(double) * 5, st));
         un::loss_sums_kernel<<<grid_for(n[0]), 256, 0, st>>>(z, e, mask, scale + 2, acc + 4, n[0]);
         CKL();
         // the loss is on the network's raw output: undo the output scale in z
@@ -493,10 +504,10 @@ aeo_status aeo_unet_gradients(aeo_unet* h, const double* r, const double* e, dou
     CK(cudaMemcpyAsync(h->ebuf, e, sizeof(double) * h->n[0], cudaMemcpyHostToDevice, h->st));
     if (aeo_status s = h->forward_(h->rbuf)) return s;
     if (aeo_status s = h->backward(h->ebuf)) return s;
-    double hl[4];
+    double hl[5];
     CK(cudaMemcpyAsync(hl, h->acc + 4, sizeof(hl), cudaMemcpyDeviceToHost, h->st));
     if (aeo_status s = h->check_err()) return s;
-    if (loss) *loss = hl[3];
+    if (loss) *loss = hl[4];
     return AEO_OK;
 }
 

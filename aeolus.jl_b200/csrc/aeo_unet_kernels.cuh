@@ -72,33 +72,47 @@ __device__ __forceinline__ void tap_plane(const Tiles& T, int t, int& P, int& xs
     else { P = ((dz + 1) * 3 + (dx + 1)) * (T.rows + 2) + 1 + dy; xs = 0; }
 }
 
-// The input tile with its halo into shared memory: row (c, P, x) at
-// ((c * np + P) * pitch + x) * 16 bytes.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    const uint32_t d = tc::smem_u32(dst);
+    const int n = valid ? 16 : 0;                 // 0: zero-fill the 16 bytes
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
+
+// The input tile with its halo into shared memory, row (c, P, x) at
+// ((c * np + P) * pitch + x) * 16 bytes: one warp per run of a plane (a
+// halo-ed row segment in mode 0, a dx-rotated row in mode 1), lanes along
+// x; asynchronous 16-byte copies (cp.async), zero-filled outside z.
 template <int CIN>
 __device__ __forceinline__ void stage_input(const Tiles& T, const uint4* __restrict__ in, uint4* sA, int x0, int j0,
                                             int k) {
     constexpr int NCH = CIN / 8;
-    const int per = T.np * T.pitch;
-    for (int it = threadIdx.x; it < NCH * per; it += blockDim.x) {
-        const int c = it / per, rem = it - c * per;
-        const int P = rem / T.pitch, x = rem - P * T.pitch;
-        int dz, gx, gy;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+    for (int run = warp; run < NCH * T.np; run += nwarp) {
+        const int c = run / T.np, P = run - c * T.np;
+        int dz, gy, xoff;
         if (T.mode == 0) {
             dz = P / 3 - 1;
-            gx = x0 - 1 + x;
             gy = j0 + (P % 3) - 1;
+            xoff = x0 - 1;
         } else {
             const int nyr = T.rows + 2, yr = P % nyr, q = P / nyr;
             dz = q / 3 - 1;
-            gx = x + (q % 3) - 1;
             gy = j0 - 1 + yr;
+            xoff = (q % 3) - 1;
         }
-        gx = gx < 0 ? gx + T.nx : (gx >= T.nx ? gx - T.nx : gx);
         gy = gy < 0 ? gy + T.ny : (gy >= T.ny ? gy - T.ny : gy);
         const int gz = k + dz;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        if (gz >= 0 && gz < T.nz) v = in[((size_t)(gz * T.ny + gy) * T.nx + gx) * NCH + c];
-        sA[it] = v;
+        const bool zin = gz >= 0 && gz < T.nz;
+        const uint4* row = in + ((size_t)((zin ? gz : 0) * T.ny + gy) * T.nx) * NCH + c;
+        uint4* dst = sA + (size_t)run * T.pitch;
+        for (int x = lane; x < T.pitch; x += 32) {
+            int gx = xoff + x;
+            gx = gx < 0 ? gx + T.nx : (gx >= T.nx ? gx - T.nx : gx);
+            cp_async16(dst + x, row + (size_t)gx * NCH, zin);
+        }
     }
 }
 
@@ -114,6 +128,7 @@ struct ConvArgs {
     const float* out0_mask;
     const double* out0_scale;
     int relu;
+    int dbuf;              // two staging buffers (the next tile loads while this one multiplies)
     int* err;
 };
 
@@ -131,7 +146,9 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_fwd_kernel(ConvArgs a) {
     __shared__ uint32_t tslot;
     const Tiles& T = a.T;
     uint4* sB = reinterpret_cast<uint4*>(smem);
-    uint4* sA = sB + WROWS;
+    uint4* sAbuf[2];
+    sAbuf[0] = sB + WROWS;
+    sAbuf[1] = a.dbuf ? sAbuf[0] + (size_t)NCH * T.np * T.pitch : sAbuf[0];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int i = threadIdx.x; i < WROWS; i += blockDim.x) sB[i] = a.wimg[i];
     if (threadIdx.x == 0) tc::mbar_init(&mbar, 1);
@@ -142,13 +159,32 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_fwd_kernel(ConvArgs a) {
     const uint32_t tmem = tslot;
     const uint32_t idesc = tc::idesc_bf16(COUT, false, false);
     const uint32_t lboA = (uint32_t)(T.np * T.pitch * 16), lboB = 27u * COUT * 16u;
-    const uint32_t aBase = tc::smem_u32(sA), bBase = tc::smem_u32(sB);
+    const uint32_t bBase = tc::smem_u32(sB);
     uint32_t phase = 0;
     bool failed = false;
-    for (int tile = blockIdx.x; tile < T.ntiles; tile += gridDim.x) {
+    const uint4* inp = reinterpret_cast<const uint4*>(a.in);
+    int it = 0;
+    if (blockIdx.x < T.ntiles) {
+        int x0, j0, k;
+        tile_origin(T, blockIdx.x, x0, j0, k);
+        stage_input<CIN>(T, inp, sAbuf[0], x0, j0, k);
+    }
+    cp_async_commit();
+    for (int tile = blockIdx.x; tile < T.ntiles; tile += gridDim.x, ++it) {
         int x0, j0, k;
         tile_origin(T, tile, x0, j0, k);
-        stage_input<CIN>(T, reinterpret_cast<const uint4*>(a.in), sA, x0, j0, k);
+        uint4* sA = sAbuf[it & 1];
+        const uint32_t aBase = tc::smem_u32(sA);
+        const int nxt = tile + gridDim.x;
+        if (a.dbuf && nxt < T.ntiles) {
+            int x1, j1, k1;
+            tile_origin(T, nxt, x1, j1, k1);
+            stage_input<CIN>(T, inp, sAbuf[(it + 1) & 1], x1, j1, k1);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
         tc::fence_async_smem();
         tc::fence_before();
         __syncthreads();
@@ -235,7 +271,14 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_fwd_kernel(ConvArgs a) {
         }
         tc::fence_before();
         __syncthreads();
+        if (!a.dbuf && nxt < T.ntiles) {
+            int x1, j1, k1;
+            tile_origin(T, nxt, x1, j1, k1);
+            stage_input<CIN>(T, inp, sAbuf[0], x1, j1, k1);
+            cp_async_commit();
+        }
     }
+    cp_async_wait<0>();
     if (failed) {
         if (threadIdx.x == 0) atomicExch(a.err, 1);
         tc::mbar_wait(&mbar, phase ^ 1u, WAIT_LIMIT);   // the outstanding MMAs, bounded
@@ -291,6 +334,8 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_wgrad_kernel(WgradArgs a) {
         int x0, j0, k;
         tile_origin(T, tile, x0, j0, k);
         stage_input<CIN>(T, reinterpret_cast<const uint4*>(a.x), sA, x0, j0, k);
+        cp_async_commit();
+        cp_async_wait<0>();
         for (int it = threadIdx.x; it < NCO * TM; it += blockDim.x) {
             const int c = it / TM, m = it - c * TM;
             sG[it] = reinterpret_cast<const uint4*>(a.g)[(size_t)cell_of(T, x0, j0, k, m) * NCO + c];
@@ -484,16 +529,20 @@ __global__ void grad_out_kernel(const float* __restrict__ g, bf16* __restrict__ 
     }
 }
 
-// sums over fluid cells of z and e, both brought to the network's output
-// units by *tscale, and the fluid count
+// Sums over fluid cells: z in network units (z * zs, zs = *tscale), the raw
+// error e, the count and e^2.  The loss compares the mean-free network
+// output with the mean-free error scaled to unit RMS on the fluid: flexible
+// CG is invariant to the scale of each preconditioner application, so only
+// the error's shape is learned, whatever its magnitude.
 __global__ void loss_sums_kernel(const float* __restrict__ z, const double* __restrict__ e, const float* __restrict__ mask,
                                  const double* tscale, double* sums, long long n) {
-    double sz = 0.0, se = 0.0, sn = 0.0;
-    const double ts = *tscale;
+    double sz = 0.0, se = 0.0, sn = 0.0, see = 0.0;
+    const double zs = *tscale;
     GS(q, n) {
         if (mask[q] > 0.0f) {
-            sz += z[q] * ts;
-            se += e[q] * ts;
+            sz += z[q] * zs;
+            se += e[q];
+            see += e[q] * e[q];
             sn += 1.0;
         }
     }
@@ -501,33 +550,36 @@ __global__ void loss_sums_kernel(const float* __restrict__ z, const double* __re
         sz += __shfl_down_sync(0xffffffffu, sz, o);
         se += __shfl_down_sync(0xffffffffu, se, o);
         sn += __shfl_down_sync(0xffffffffu, sn, o);
+        see += __shfl_down_sync(0xffffffffu, see, o);
     }
     if ((threadIdx.x & 31) == 0) {
         atomicAdd(&sums[0], sz);
         atomicAdd(&sums[1], se);
         atomicAdd(&sums[2], sn);
+        atomicAdd(&sums[3], see);
     }
 }
 
-// in network units (z' = z tscale, e' = e tscale): d = (z' - mean z') -
-// (e' - mean e') on fluid cells; loss += d^2 / n_f, g = dloss/dz' = 2 d / n_f
+// d = (z' - mean z') - (e' - mean e') on fluid cells, z' = z tscale, e' = e
+// scaled to unit RMS; loss += d^2 / n_f; g = dloss/dz' = 2 d / n_f
 __global__ void loss_grad_kernel(const float* __restrict__ z, const double* __restrict__ e,
                                  const float* __restrict__ mask, const double* tscale, double* sums,
                                  float* __restrict__ g, long long n) {
     const double nf = sums[2] > 0.0 ? sums[2] : 1.0;
-    const double mz = sums[0] / nf, me = sums[1] / nf, ts = *tscale;
+    const double es = sums[3] > 0.0 ? sqrt(nf / sums[3]) : 1.0;
+    const double mz = sums[0] / nf, me = sums[1] * es / nf, zs = *tscale;
     double l = 0.0;
     GS(q, n) {
         float gv = 0.0f;
         if (mask[q] > 0.0f) {
-            const double d = (z[q] * ts - mz) - (e[q] * ts - me);
+            const double d = (z[q] * zs - mz) - (e[q] * es - me);
             l += d * d;
             gv = (float)(2.0 * d / nf);
         }
         g[q] = gv;
     }
     for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(&sums[3], l / nf);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&sums[4], l / nf);
 }
 
 // Adam on the FP32 master parameters (Kingma & Ba 2015), gradients zeroed after use

@@ -48,7 +48,9 @@ aeo_status aeo_unet_set_out_scale(aeo_unet* h, double out_scale);
 aeo_status aeo_unet_apply(aeo_unet* h, const double* r, double* z);
 /* forward and backward on one pair (r, e = A^-1 r), gradients replaced (not
  * accumulated across calls); loss = mean over fluid cells of the squared
- * difference of the mean-free output and target in network units */
+ * difference of the mean-free network output and the mean-free error scaled
+ * to unit RMS on the fluid (flexible CG is invariant to the scale of each
+ * preconditioner application, so only the error's shape is learned) */
 aeo_status aeo_unet_gradients(aeo_unet* h, const double* r, const double* e, double* loss);
 /* aeo_unet_gradients then one Adam step (beta 0.9 / 0.999, eps 1e-8) */
 aeo_status aeo_unet_train_step(aeo_unet* h, const double* r, const double* e, double lr, double* loss);

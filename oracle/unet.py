@@ -169,9 +169,10 @@ def forward(P, x):
 
 def loss_and_grad_out(out, target, mask):
     """L = sum over fluid cells of (z - mean z - (e - mean e))^2 / n_fluid,
-    z the raw output, e the target in network units (the error times
-    s / out_scale); returns (L, dL/dz)."""
+    z the raw output, e the error scaled to unit RMS on the fluid; returns
+    (L, dL/dz)."""
     f = mask > 0
+    target = target * np.sqrt(f.sum() / (target[f].astype(np.float64) ** 2).sum())
     nf = max(int(f.sum()), 1)
     z = np.where(f, out, 0.0)
     e = np.where(f, target, 0.0)
