@@ -417,6 +417,7 @@ def run_b200_urban(args):
         "parts_ms": {k: round(v, 4) for k, v in m["parts"].items()},
         "gpu_launches": (m["st"]["iterations"] + 1) * m["lpi"] * args.steps,
         "clocks": m["clocks"],
+        "learned": learned_pcg(coeffs, b, args),
     }
     if world == 1 and not args.no_cpu_baseline:
         from oracle.mgpcg import OracleMGPCG
@@ -429,6 +430,39 @@ def run_b200_urban(args):
     print(json.dumps(line), flush=True)
     barrier(world)
     return 0
+
+
+def learned_pcg(coeffs, b, args):
+    """The learned U-Net preconditioner on the urban problem: trained on the
+    GPU on 2000 residual -> error pairs harvested from plain MG-preconditioned
+    CG solves of 128 x 128 x 48 problems at the same 2 m spacing (20 training
+    geometries of 10 boxes, seeds 101..120, 10 right-hand sides each), then
+    used in flexible CG on the test geometry (seed 1, not seen in training).
+    Compared with CG without a preconditioner (the method without the
+    network) and with the multigrid preconditioner."""
+    from aeolus_b200.learned import train_streaming, transfer, urban_geometry
+    from aeolus_b200.multigrid import MGPreconditionedCG
+    t0 = time.perf_counter()
+    net, losses, used = train_streaming((128, 128, 48), seeds=range(101, 121), rhs_per_geometry=10, nboxes=10,
+                                        pairs_total=2000)
+    train_s = time.perf_counter() - t0
+    g, geom = urban_geometry(URBAN_N, 1, 40)
+    fluid = (~geom.is_solid[g.interior]).astype(np.float32)
+    big = transfer(net, URBAN_N, fluid)
+    out = {"training": {"pairs": used, "seconds": round(train_s, 1), "loss_first50": float(losses[:50].mean()),
+                        "loss_last50": float(losses[-50:].mean()), "grid": [128, 128, 48],
+                        "step_ms": net.profile("train", 5)},
+           "unet_forward_ms": big.profile("forward", 10)}
+    for name, pc in (("learned", "vcycle"), ("plain_cg", "identity"), ("mg", "vcycle")):
+        s = MGPreconditionedCG(URBAN_N, (URBAN_H,) * 3, coeffs=coeffs, tol=1e-8, precision="fp32_mixed", maxit=4000,
+                               precond=pc)
+        if name == "learned":
+            s.set_learned(big, stagnation=0.9)
+        x, st = s.solve(b)
+        out[name] = {"ms": s.profile("solve", 3), "iterations": st["iterations"],
+                     "relative_residual": st["relative_residual"], "status": st["status"],
+                     "fallback_at": st["fallback_at"]}
+    return out
 
 
 def run_b200(args):
