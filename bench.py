@@ -17,14 +17,18 @@ beside it.  `e2e` is the same metric through the C-ABI with the state copied
 from pinned host memory and back every step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--workload cbl|tgv|urban]
+                  [--workload cbl|tgv|urban|hit]
 
 The default line also carries "pcg": the other half of the headline metric,
 the time to a 1e-8 relative residual of the cut-cell urban pressure problem
 (256 x 256 x 96 at 2 m, 40 floor-standing boxes, multigrid-preconditioned CG
 in FP64 and FP32-mixed).  `--workload urban` reports that solve as the line's
 own metric (ms to 1e-8, lower is better) with its roofline, e2e and CPU
-baseline.
+baseline.  `--workload hit` is the decaying isotropic turbulence of 512^3
+cells (WENO-Z5, no SGS, adaptive dt at CFL 0.5): the FP64 run steps
+adaptively, the FP32-mixed run repeats its dt sequence, and the line reports
+the FP32-mixed cell-steps/s beside the FP64 rate with the fields' relative L2
+difference and the kinetic-energy difference after `--hit-steps` steps.
 
 Under torchrun every rank runs an independent replica of the workload (the
 step has no data-path collective on one domain; weak scaling) and rank 0
@@ -465,6 +469,136 @@ def learned_pcg(coeffs, b, args):
     return out
 
 
+def run_reference_hit(args):
+    """The oracle (all host cores) on the HIT workload: the field generated on
+    the host by the same spectral construction, projected, then timed steps
+    at the first adaptive dt (each step is a bounded sample of the workload)."""
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    from aeolus_b200 import CoreSpec, regular_grid
+    from aeolus_b200.inputs import isotropic_turbulence
+    from aeolus_b200.simulation import CFLConstraints
+    from oracle.oracle import OracleSimulation, set_threads
+    n = args.hit_n
+    g = regular_grid((n, n, n), (2 * np.pi,) * 3)
+    cores = os.cpu_count() or 1
+    set_threads(cores)
+    o = OracleSimulation(CoreSpec(grid=g, advection="weno_z5", nu=0.0))
+    u, v, w = isotropic_turbulence(g, 1.0, 4.0, seed=1)
+    o.set_state(u, v, w, g.zeros())
+    del u, v, w
+    o.project()
+    dt, _ = o.adaptive_dt(CFLConstraints(C_advective=0.5, growth_max=1.1))
+    k = max(1, min(args.steps, 2))
+    t0 = time.perf_counter()
+    o.step_rk3(dt, k)
+    el = time.perf_counter() - t0
+    value = g.ncells * k / el
+    line = {"impl": "reference", "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s",
+            "n_gpus": args.gpus, "steps": k, "warmup": 0, "ms_per_step": 1e3 * el / k, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"decaying isotropic turbulence {n}^3, WENO-Z5, no SGS", "grid": [n, n, n]},
+            "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+                             "sample": f"{k} RK3 steps of the full grid at the first adaptive dt, FP64 oracle"},
+            "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200_hit(args):
+    world, rank, local = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    from aeolus_b200 import CoreSpec, regular_grid
+    from aeolus_b200.simulation import CFLConstraints, Simulation
+    n = args.hit_n
+    g = regular_grid((n, n, n), (2 * np.pi,) * 3)
+
+    def spec(prec):
+        return CoreSpec(grid=g, advection="weno_z5", nu=0.0, precision=prec)
+
+    hbm, hbm_kind = measured_peaks()
+    s64 = Simulation(spec("fp64"), device=local)
+    s64.init_isotropic(u_rms=1.0, k_peak=4.0, seed=1, project=True, target_rms=1.0)
+    state0 = s64.get_state()
+    ke0 = s64.kinetic_energy()
+    c = CFLConstraints(C_advective=0.5, growth_max=1.1)
+    dts, dt_prev = [], None
+    for _ in range(args.hit_steps):
+        st = s64.step_adaptive(c, 1, dt_prev)
+        dts.append(st["dt"])
+        dt_prev = st["dt"]
+    fin64 = [s64.get_field(f)[g.interior] for f in ("u", "v", "w")]
+    ke64, div64 = s64.kinetic_energy(), s64.max_divergence()
+    s32 = Simulation(spec("fp32_mixed"), device=local)
+    s32.set_state(*state0)
+    for dt in dts:
+        s32.step_rk3(dt, 1)
+    fin32 = [s32.get_field(f)[g.interior] for f in ("u", "v", "w")]
+    ke32, div32 = s32.kinetic_energy(), s32.max_divergence()
+    rel = {f: float(np.linalg.norm(a - b) / np.linalg.norm(b)) for f, a, b in zip("uvw", fin32, fin64)}
+    del fin32, fin64
+    # rates: fixed-dt steps (the captured graph) at the last dt, and adaptive steps
+    dt = dts[-1]
+    res = {}
+    for name, sim in (("fp32_mixed", s32), ("fp64", s64)):
+        sim.step_rk3(dt, args.warmup)
+        clk = ClockSampler(local)
+        clk.start()
+        ms = timed_steps(sim, dt, args.steps, world) / args.steps
+        clocks = clk.stop()
+        prof = sim.profile_step(dt)
+        import torch as _t
+        e0, e1 = _t.cuda.Event(enable_timing=True), _t.cuda.Event(enable_timing=True)
+        ka = max(3, min(args.steps, 10))
+        # the guard's divergence bound is the reference's FP64 round-off bound (1e-6);
+        # an FP32 projection leaves ~1e-7 relative to the velocity gradients
+        ca = c if name == "fp64" else CFLConstraints(C_advective=0.5, growth_max=1.1, divergence_tol=1e-2)
+        sim.synchronize()
+        e0.record(_t.cuda.ExternalStream(sim.stream))
+        sim.step_adaptive(ca, ka, dt)
+        e1.record(_t.cuda.ExternalStream(sim.stream))
+        sim.synchronize()
+        res[name] = {"ms": max_over_ranks(ms, world), "clocks": clocks, "prof": prof,
+                     "adaptive_ms": e0.elapsed_time(e1) / ka, "launches": sim.launches_per_step()}
+    if rank != 0:
+        barrier(world)
+        return 0
+    ncell = g.ncells
+    m = res["fp32_mixed"]
+    prof = m["prof"]
+    per_launch_ms = prof["sweep"] / LAUNCHES_PER_STEP["sweep"]
+    sweep_bytes = class_passes("sweep", g, False) * 4 * ncell
+    ach = sweep_bytes / (per_launch_ms * 1e-3) / 1e9
+    line = {
+        "metric": "cell-steps/s", "value": world * ncell / (m["ms"] * 1e-3), "unit": "cell-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32-mixed (FP32 stencils/FFT, FP64 reductions)", "data": "synthetic (Passot-Pouquet spectrum, seed 1)",
+        "config": {"workload": f"decaying isotropic turbulence {n}^3, triply periodic, WENO-Z5, no SGS, nu = 0, "
+                               f"adaptive dt CFL 0.5 (growth 1.1), E(k) ~ k^4 exp(-2 (k/4)^2), u_rms = 1",
+                   "grid": [n, n, n], "l2": "inputs larger than L2",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "fp64": {"value": world * ncell / (res["fp64"]["ms"] * 1e-3), "ms_per_step": res["fp64"]["ms"],
+                 "adaptive_ms_per_step": res["fp64"]["adaptive_ms"]},
+        "adaptive_ms_per_step": m["adaptive_ms"],
+        "fp32_vs_fp64": {"steps": args.hit_steps, "relative_l2": rel, "ke_fp64": ke64, "ke_fp32": ke32,
+                         "ke_initial": ke0, "ke_relative_difference": abs(ke32 - ke64) / ke64,
+                         "ke_decay_relative_difference": abs((ke0 - ke32) - (ke0 - ke64)) / (ke0 - ke64)
+                         if ke0 != ke64 else None, "max_divergence_fp64": div64, "max_divergence_fp32": div32,
+                         "t_end": float(np.sum(dts))},
+        "roofline": {"bound": "hbm", "kernel": "sweep", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(ach / hbm, 4), "peak_kind": hbm_kind, "bytes_per_launch": sweep_bytes,
+                     "traffic": None},
+        "gpu_launches": m["launches"] * args.steps,
+        "clocks": m["clocks"],
+    }
+    print(json.dumps(line), flush=True)
+    barrier(world)
+    return 0
+
+
 def run_b200(args):
     world, rank, local = dist_setup()
     import torch
@@ -563,13 +697,17 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="cbl", choices=["cbl", "tgv", "urban"])
+    ap.add_argument("--workload", default="cbl", choices=["cbl", "tgv", "urban", "hit"])
+    ap.add_argument("--hit-n", type=int, default=512)
+    ap.add_argument("--hit-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.workload == "urban":
         rc = run_reference_urban(args) if args.impl == "reference" else run_b200_urban(args)
+    elif args.workload == "hit":
+        rc = run_reference_hit(args) if args.impl == "reference" else run_b200_hit(args)
     else:
         rc = run_reference(args) if args.impl == "reference" else run_b200(args)
     if int(os.environ.get("WORLD_SIZE", "1")) > 1:
