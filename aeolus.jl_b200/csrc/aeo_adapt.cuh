@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(256) cfl_levels_kernel(Geo g, const R* __restr
         r = fmax(r, rate);
         if (SGS) {
             Nb<R> U{u + q, g.sy, g.sz}, V{v + q, g.sy, g.sz}, W{w + q, g.sy, g.sz};
-            nm = fmax(nm, (double)smag_point<R, UNI>(g, k, c_s, U, V, W));
+            nm = fmax(nm, (double)smag_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, U, V, W));
         }
         ts += (double)th[q];
     }

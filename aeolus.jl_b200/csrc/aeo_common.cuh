@@ -71,6 +71,9 @@ struct Geo {
     const double* wc;
     const double* wf;
     const double* thf;
+    // the per-level factors in the working precision (rows LV_*, entry k + AEO_LH)
+    const void* lvr;
+    int lvn;   // row stride
 };
 
 __device__ __forceinline__ long long pidx(const Geo& g, int i, int j, int k) {
@@ -126,5 +129,53 @@ __device__ __forceinline__ R ld_mapped_interior(const Geo& g, const R* __restric
     R v = __ldg(a + iidx(g, wrapi(i, g.nx), wrapi(j, g.ny), kk));
     return s > 0 ? v : -v;
 }
+
+// ---- metric accessors (src/FiniteVolume.jl:146-186) -----------------------
+// Per-level factors in the working precision: row f holds the factor of level
+// k at entry k + AEO_LH.  The engine builds the rows once from its FP64
+// metric vectors (the reciprocals and g/theta_f rounded exactly as the
+// division in R would round them; the sponge rates from the profile), so a
+// kernel reads each factor with one load instead of an FP64 load, a
+// conversion and, for the reciprocals, a division per point.
+enum {
+    LV_IDZC = 0, LV_IDZF, LV_IDZOFF, LV_WLO, LV_WHI, LV_ALO, LV_AHI, LV_DELTA,
+    LV_WC, LV_WF, LV_IWC, LV_IWF, LV_THF, LV_GTHF, LV_SPC, LV_SPF, LV_N
+};
+
+template <typename R, bool UNI>
+struct Met {
+    const Geo& g;
+    const R* t;        // row f, level k at t[f * stride + k + off]
+    int stride, off;
+    __device__ __forceinline__ explicit Met(const Geo& gg)
+        : g(gg), t(static_cast<const R*>(gg.lvr)), stride(gg.lvn), off(AEO_LH) {}
+    __device__ __forceinline__ Met(const Geo& gg, const R* tab, int s, int o) : g(gg), t(tab), stride(s), off(o) {}
+    __device__ __forceinline__ R lv(int f, int k) const { return t[f * stride + k + off]; }
+    __device__ __forceinline__ R idz(int k) const { return UNI ? R(g.idz) : lv(LV_IDZC, k); }
+    __device__ __forceinline__ R idzf(int k) const { return UNI ? R(g.idz) : lv(LV_IDZF, k); }
+    __device__ __forceinline__ R idz_off(int k) const { return UNI ? R(g.idz) : lv(LV_IDZOFF, k); }
+    __device__ __forceinline__ R zface(int k, R lo, R hi) const {
+        return UNI ? R(0.5) * (lo + hi) : lv(LV_WLO, k) * lo + lv(LV_WHI, k) * hi;
+    }
+    __device__ __forceinline__ R zflux(int k, R lo, R hi) const {
+        return UNI ? R(0.5) * (lo + hi) : lv(LV_ALO, k) * lo + lv(LV_AHI, k) * hi;
+    }
+    __device__ __forceinline__ R lapz(int loc, int k, R fm, R c, R fp) const {
+        if (UNI) return (fp - R(2) * c + fm) * R(g.idz2);
+        if (loc == LOC_FZ) return ((fp - c) * lv(LV_IDZC, k) - (c - fm) * lv(LV_IDZC, k - 1)) * lv(LV_IDZF, k);
+        return ((fp - c) * lv(LV_IDZF, k + 1) - (c - fm) * lv(LV_IDZF, k)) * lv(LV_IDZC, k);
+    }
+    __device__ __forceinline__ R filter(int k) const { return UNI ? R(g.delta_u) : lv(LV_DELTA, k); }
+    // sound-proof weights
+    __device__ __forceinline__ R wc(int k) const { return lv(LV_WC, k); }
+    __device__ __forceinline__ R wf(int k) const { return lv(LV_WF, k); }
+    __device__ __forceinline__ R iwc(int k) const { return lv(LV_IWC, k); }
+    __device__ __forceinline__ R iwf(int k) const { return lv(LV_IWF, k); }
+    __device__ __forceinline__ R thf(int k) const { return lv(LV_THF, k); }
+    __device__ __forceinline__ R gthf(int k) const { return lv(LV_GTHF, k); }
+    // Rayleigh sponge rates at the centre and the bottom face of level k
+    __device__ __forceinline__ R spc(int k) const { return lv(LV_SPC, k); }
+    __device__ __forceinline__ R spf(int k) const { return lv(LV_SPF, k); }
+};
 
 #define AEO_CHECK_LAUNCH() ((void)0)

@@ -87,15 +87,16 @@ __global__ void __launch_bounds__(256) fftz_inv_kernel(Geo g, cplx<R>* __restric
     const int j = blockIdx.y, p0 = blockIdx.x * tpx;
     const long long sk = (long long)g.ny * Mh;
     const long long base = (long long)j * Mh;
+    const int lt = __ffs(tpx) - 1;
     for (int e = threadIdx.x; e < g.nz * tpx; e += blockDim.x) {
-        int kz = e / tpx, c = e % tpx, p = p0 + c;
-        buf[kz * tpx + c] = p < Mh ? S[base + kz * sk + p] : cmk<R>(R(0), R(0));
+        const int kz = e >> lt, c = e & (tpx - 1), p = p0 + c;
+        buf[e] = p < Mh ? S[base + kz * sk + p] : cmk<R>(R(0), R(0));
     }
     __syncthreads();
-    smem_fft<R, true, true, FFT_KB>(buf, g.nz, tpx, 1, tpx, tw, NT);
+    smem_fft<R, true, true, FFT_KB>(buf, __ffs(g.nz) - 1, __ffs(tpx) - 1, 1, tpx, tw, NT);
     for (int e = threadIdx.x; e < g.nz * tpx; e += blockDim.x) {
-        int kz = e / tpx, c = e % tpx, p = p0 + c;
-        if (p < Mh) S[base + kz * sk + p] = buf[kz * tpx + c];
+        const int kz = e >> lt, c = e & (tpx - 1), p = p0 + c;
+        if (p < Mh) S[base + kz * sk + p] = buf[e];
     }
 }
 

@@ -87,9 +87,9 @@ extern "C" aeo_status aeo_pressure_solve_column_noalloc(int32_t nx, int32_t ny, 
         aeo_set_global_error("pressure_solve_column_noalloc: NULL argument");
         return AEO_ERR_ARGUMENT;
     }
-    if (!pow2(nx) || !pow2(ny) || nx < 4 || ny < 4 || nx / 2 > 2048 || ny > 2048 || nz < 1 || nz > 896) {
+    if (!pow2(nx) || !pow2(ny) || nx < 4 || ny < 4 || nx / 2 > 2048 || ny > 2048 || nz < 1 || nz > AEO_COLUMN_NZ_MAX) {
         aeo_set_global_error("pressure_solve_column_noalloc: nx, ny must be powers of two (4 <= nx <= 4096, "
-                             "4 <= ny <= 2048) and 1 <= nz <= 896");
+                             "4 <= ny <= 2048) and 1 <= nz <= " + std::to_string(AEO_COLUMN_NZ_MAX));
         return AEO_ERR_ARGUMENT;
     }
     if (lower[0] != 0.0 || upper[nz - 1] != 0.0 || !(lx > 0) || !(ly > 0)) {
@@ -163,8 +163,7 @@ extern "C" aeo_status aeo_pressure_solve_column_noalloc(int32_t nx, int32_t ny, 
     size_t smx = (size_t)rows * M * sizeof(cplx<double>);
     dim3 gy((Mh + tpx - 1) / tpx, nz);
     size_t smy = (size_t)tpx * ny * sizeof(cplx<double>);
-    dim3 gt((Mh + 31) / 32, ny);
-    size_t smt = (size_t)nz * 32 * sizeof(double);
+    size_t smt = thomas_smem(g);
     if (smt > 48 * 1024) {
         e = cudaFuncSetAttribute(thomas_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
         if (e != cudaSuccess) {
@@ -174,7 +173,7 @@ extern "C" aeo_status aeo_pressure_solve_column_noalloc(int32_t nx, int32_t ny, 
     }
     src_fftx_kernel<double><<<gx, 256, smx, st>>>(g, src, S, tw, NT, rows);
     ffty_kernel<double, 0><<<gy, 256, smy, st>>>(g, S, tw, NT, tpx);
-    thomas_kernel<double><<<gt, 32, smt, st>>>(g, S, S, cc);
+    thomas_kernel<double><<<thomas_blocks(g), 32, smt, st>>>(g, S, S, cc);
     ffty_kernel<double, 1><<<gy, 256, smy, st>>>(g, S, tw, NT, tpx);
     ifftx_kernel<double><<<gx, 256, smx, st>>>(g, S, phi, tw, NT, rows, 1.0 / ((double)nx * ny));
     e = cudaGetLastError();

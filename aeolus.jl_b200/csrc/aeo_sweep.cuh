@@ -42,28 +42,6 @@ struct SweepArgs {
     R c_s;
 };
 
-// ---- metric accessors (src/FiniteVolume.jl:146-186) -----------------------
-template <typename R, bool UNI>
-struct Met {
-    const Geo& g;
-    __device__ Met(const Geo& gg) : g(gg) {}
-    __device__ __forceinline__ R idz(int k) const { return UNI ? R(g.idz) : R(lvl(g.idzc, k)); }
-    __device__ __forceinline__ R idzf(int k) const { return UNI ? R(g.idz) : R(lvl(g.idzf, k)); }
-    __device__ __forceinline__ R idz_off(int k) const { return UNI ? R(g.idz) : R(lvl(g.idz_off, k)); }
-    __device__ __forceinline__ R zface(int k, R lo, R hi) const {
-        return UNI ? R(0.5) * (lo + hi) : R(lvl(g.wlo, k)) * lo + R(lvl(g.whi, k)) * hi;
-    }
-    __device__ __forceinline__ R zflux(int k, R lo, R hi) const {
-        return UNI ? R(0.5) * (lo + hi) : R(lvl(g.alo, k)) * lo + R(lvl(g.ahi, k)) * hi;
-    }
-    __device__ __forceinline__ R lapz(int loc, int k, R fm, R c, R fp) const {
-        if (UNI) return (fp - R(2) * c + fm) * R(g.idz2);
-        if (loc == LOC_FZ) return ((fp - c) * R(lvl(g.idzc, k)) - (c - fm) * R(lvl(g.idzc, k - 1))) * R(lvl(g.idzf, k));
-        return ((fp - c) * R(lvl(g.idzf, k + 1)) - (c - fm) * R(lvl(g.idzf, k))) * R(lvl(g.idzc, k));
-    }
-    __device__ __forceinline__ R filter(int k) const { return UNI ? R(g.delta_u) : R(lvl(g.delta, k)); }
-};
-
 // padded-array accessor around the thread's point
 template <typename R>
 struct Nb {
@@ -130,16 +108,16 @@ __device__ __forceinline__ R face_z(const A& F, int di, int dj, int c, R vel) {
 // U, V, W, T, N are accessors (di, dj, dk) -> value around the point at level
 // k; the same arithmetic serves the direct form (global memory) and the
 // tiled form (shared-memory planes).
-template <typename R, int ADV, bool SGS, bool ANEL, bool UNI, class AU, class AN>
-__device__ __forceinline__ void sweep_point(const SweepArgs<R>& a, const Geo& g, int k, const AU& U, const AU& V,
-                                            const AU& W, const AU& T, const AN& N, R& tu, R& tv, R& tw, R& tt) {
-    Met<R, UNI> m(g);
+template <typename R, int ADV, bool SGS, bool ANEL, bool UNI, class AU, class AV, class AW, class AT, class AN>
+__device__ __forceinline__ void sweep_point(const Met<R, UNI>& m, const SweepArgs<R>& a, const Geo& g, int k,
+                                            const AU& U, const AV& V, const AW& W, const AT& T, const AN& N, R& tu,
+                                            R& tv, R& tw, R& tt) {
     const R idx = R(g.idx), idy = R(g.idy), idx2 = R(g.idx2), idy2 = R(g.idy2);
     const R h = R(0.5);
 
     if (ANEL) {
         // W-weighted centred forms (src/Anelastic.jl:1193-1306)
-        R iwc = R(1) / R(lvl(g.wc, k)), wfb = R(lvl(g.wf, k)), wft = R(lvl(g.wf, k + 1));
+        R iwc = m.iwc(k), wfb = m.wf(k), wft = m.wf(k + 1);
         {
             R uce = h * (U(0, 0, 0) + U(1, 0, 0)), ucw = h * (U(-1, 0, 0) + U(0, 0, 0));
             R d_uu_dx = (uce * uce - ucw * ucw) * idx;
@@ -163,7 +141,7 @@ __device__ __forceinline__ void sweep_point(const SweepArgs<R>& a, const Geo& g,
             tv = R(0) - (d_uv_dx + d_vv_dy + d_wv_dz);
         }
         {
-            R iwf = R(1) / R(lvl(g.wf, k)), wcb = R(lvl(g.wc, k - 1)), wct = R(lvl(g.wc, k));
+            R iwf = m.iwf(k), wcb = m.wc(k - 1), wct = m.wc(k);
             R uwe = m.zflux(k, U(1, 0, -1), U(1, 0, 0)), wue = h * (W(0, 0, 0) + W(1, 0, 0));
             R uww = m.zflux(k, U(0, 0, -1), U(0, 0, 0)), wuw = h * (W(-1, 0, 0) + W(0, 0, 0));
             R d_uw_dx = (uwe * wue - uww * wuw) * idx;
@@ -293,7 +271,7 @@ __device__ __forceinline__ void sweep_point(const SweepArgs<R>& a, const Geo& g,
             R eB = q4 * (N(-1, 0, -1) + N(0, 0, -1) + N(-1, 0, 0) + N(0, 0, 0));
             R fzT = eT * (U(0, 0, 1) - U(0, 0, 0)) * m.idzf(k + 1);
             R fzB = eB * (U(0, 0, 0) - U(0, 0, -1)) * m.idzf(k);
-            R vert = ANEL ? (R(lvl(g.wf, k + 1)) * fzT - R(lvl(g.wf, k)) * fzB) * m.idz(k) / R(lvl(g.wc, k))
+            R vert = ANEL ? (m.wf(k + 1) * fzT - m.wf(k) * fzB) * m.idz(k) * m.iwc(k)
                           : (fzT - fzB) * m.idz(k);
             tu += (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
         }
@@ -308,7 +286,7 @@ __device__ __forceinline__ void sweep_point(const SweepArgs<R>& a, const Geo& g,
             R eB = q4 * (N(0, -1, -1) + N(0, 0, -1) + N(0, -1, 0) + N(0, 0, 0));
             R fzT = eT * (V(0, 0, 1) - V(0, 0, 0)) * m.idzf(k + 1);
             R fzB = eB * (V(0, 0, 0) - V(0, 0, -1)) * m.idzf(k);
-            R vert = ANEL ? (R(lvl(g.wf, k + 1)) * fzT - R(lvl(g.wf, k)) * fzB) * m.idz(k) / R(lvl(g.wc, k))
+            R vert = ANEL ? (m.wf(k + 1) * fzT - m.wf(k) * fzB) * m.idz(k) * m.iwc(k)
                           : (fzT - fzB) * m.idz(k);
             tv += (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
         }
@@ -323,7 +301,7 @@ __device__ __forceinline__ void sweep_point(const SweepArgs<R>& a, const Geo& g,
             R eS = q4 * (N(0, -1, -1) + N(0, 0, -1) + N(0, -1, 0) + N(0, 0, 0));
             R fyN = eN * (W(0, 1, 0) - W(0, 0, 0)) * idy;
             R fyS = eS * (W(0, 0, 0) - W(0, -1, 0)) * idy;
-            R vert = ANEL ? (R(lvl(g.wc, k)) * fzT - R(lvl(g.wc, k - 1)) * fzB) * m.idzf(k) / R(lvl(g.wf, k))
+            R vert = ANEL ? (m.wc(k) * fzT - m.wc(k - 1) * fzB) * m.idzf(k) * m.iwf(k)
                           : (fzT - fzB) * m.idzf(k);
             tw += (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
         }
@@ -336,16 +314,16 @@ __device__ __forceinline__ void sweep_point(const SweepArgs<R>& a, const Geo& g,
             R fzT = nT * (T(0, 0, 1) - T(0, 0, 0)) * m.idzf(k + 1), fzB = nB * (T(0, 0, 0) - T(0, 0, -1)) * m.idzf(k);
             tt += a.inv_prt * ((fxE - fxW) * idx + (fyN - fyS) * idy + (fzT - fzB) * m.idz(k));
         } else {
-            // kappa = nut / Pr_t, the W-weighted form
-            R pr = a.pr_t;
-            R K0 = N(0, 0, 0) / pr;
-            R fxE = h * (K0 + N(1, 0, 0) / pr) * (T(1, 0, 0) - T(0, 0, 0)) * idx;
-            R fxW = h * (N(-1, 0, 0) / pr + K0) * (T(0, 0, 0) - T(-1, 0, 0)) * idx;
-            R fyN = h * (K0 + N(0, 1, 0) / pr) * (T(0, 1, 0) - T(0, 0, 0)) * idy;
-            R fyS = h * (N(0, -1, 0) / pr + K0) * (T(0, 0, 0) - T(0, -1, 0)) * idy;
-            R fzT = h * (K0 + N(0, 0, 1) / pr) * (T(0, 0, 1) - T(0, 0, 0)) * m.idzf(k + 1);
-            R fzB = h * (N(0, 0, -1) / pr + K0) * (T(0, 0, 0) - T(0, 0, -1)) * m.idzf(k);
-            R vert = (R(lvl(g.wf, k + 1)) * fzT - R(lvl(g.wf, k)) * fzB) * m.idz(k) / R(lvl(g.wc, k));
+            // kappa = nut / Pr_t, the W-weighted form (1/Pr_t applied once per face)
+            const R hk = h * a.inv_prt;
+            const R N0 = N(0, 0, 0);
+            R fxE = hk * (N0 + N(1, 0, 0)) * (T(1, 0, 0) - T(0, 0, 0)) * idx;
+            R fxW = hk * (N(-1, 0, 0) + N0) * (T(0, 0, 0) - T(-1, 0, 0)) * idx;
+            R fyN = hk * (N0 + N(0, 1, 0)) * (T(0, 1, 0) - T(0, 0, 0)) * idy;
+            R fyS = hk * (N(0, -1, 0) + N0) * (T(0, 0, 0) - T(0, -1, 0)) * idy;
+            R fzT = hk * (N0 + N(0, 0, 1)) * (T(0, 0, 1) - T(0, 0, 0)) * m.idzf(k + 1);
+            R fzB = hk * (N(0, 0, -1) + N0) * (T(0, 0, 0) - T(0, 0, -1)) * m.idzf(k);
+            R vert = (m.wf(k + 1) * fzT - m.wf(k) * fzB) * m.idz(k) * m.iwc(k);
             tt += (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
         }
     }
@@ -353,8 +331,8 @@ __device__ __forceinline__ void sweep_point(const SweepArgs<R>& a, const Geo& g,
     // buoyancy on the z faces
     if (ANEL) {
         if (a.gacc != R(0)) {
-            R tb = R(lvl(g.thf, k));
-            R coef = a.gacc / tb;
+            R tb = m.thf(k);
+            R coef = m.gthf(k);   // g / theta_f
             tw += coef * (m.zface(k, T(0, 0, -1), T(0, 0, 0)) - tb);
         }
     } else if (a.theta0 != R(0)) {
@@ -370,21 +348,14 @@ __device__ __forceinline__ void sweep_point(const SweepArgs<R>& a, const Geo& g,
     // prescribed wall fluxes of theta
     if (k == 0) tt += a.flux_bot * m.idz(0);
     if (k == g.nz - 1) tt -= a.flux_top * m.idz(g.nz - 1);
-    // Rayleigh sponge toward rest
+    // Rayleigh sponge toward rest: the per-level rates alpha sin^2(pi/2 (z - z_s)/(z_top - z_s))
+    // above z_s, zero below (src/FiniteVolume.jl:578-702)
     if (a.sp_alpha != R(0)) {
-        double zc = lvl(g.zc, k), zf = lvl(g.zf, k);
-        if (zc >= (double)a.sp_zstart) {
-            R s = sin(R(0.5 * 3.14159265358979323846) * (R(zc) - a.sp_zstart) * a.sp_inv);
-            R r = a.sp_alpha * s * s;
-            tu -= r * U(0, 0, 0);
-            tv -= r * V(0, 0, 0);
-        }
-        if (zf >= (double)a.sp_zstart) {
-            R s = sin(R(0.5 * 3.14159265358979323846) * (R(zf) - a.sp_zstart) * a.sp_inv);
-            tw -= a.sp_alpha * s * s * W(0, 0, 0);
-        }
+        const R rc = m.spc(k), rf = m.spf(k);
+        tu -= rc * U(0, 0, 0);
+        tv -= rc * V(0, 0, 0);
+        tw -= rf * W(0, 0, 0);
     }
-
 }
 
 // ---- direct form: one thread per cell, neighbours from global memory --------------
@@ -400,7 +371,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs<R> a) {
     Nb<R> U{a.u + q, sy, sz}, V{a.v + q, sy, sz}, W{a.w + q, sy, sz}, T{a.th + q, sy, sz};
     Nb<R> N{SGS ? a.nut + q : a.u + q, sy, sz};
     R tu, tv, tw, tt;
-    sweep_point<R, ADV, SGS, ANEL, UNI>(a, g, k, U, V, W, T, N, tu, tv, tw, tt);
+    sweep_point<R, ADV, SGS, ANEL, UNI>(Met<R, UNI>(g), a, g, k, U, V, W, T, N, tu, tv, tw, tt);
     // predictor and the theta update (with the RK3 stage combination)
     const long long qi = iidx(g, i, j, k);
     const R dt = R(__ldg(a.dtp));
@@ -414,9 +385,9 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs<R> a) {
 
 // Smagorinsky nut = (C_s Delta_k)^2 |S| at a cell centre (src/FiniteVolume.jl:936-944,
 // strain src/Operators.jl:451-496), accessors around the point at level k.
-template <typename R, bool UNI, class A>
-__device__ __forceinline__ R smag_point(const Geo& g, int k, R c_s, const A& U, const A& V, const A& W) {
-    Met<R, UNI> m(g);
+template <typename R, bool UNI, class AU, class AV, class AW>
+__device__ __forceinline__ R smag_point(const Met<R, UNI>& m, const Geo& g, int k, R c_s, const AU& U, const AV& V,
+                                        const AW& W) {
     R idx = R(g.idx), idy = R(g.idy), idz = m.idz(k), ido = m.idz_off(k);
     R cf = c_s * m.filter(k);
     R coef = cf * cf;
@@ -444,5 +415,5 @@ __global__ void __launch_bounds__(256) smagorinsky_kernel(Geo g, const R* __rest
     if (i >= g.nx || j >= g.ny || k >= g.nz) return;
     const long long q = pidx(g, i, j, k);
     Nb<R> U{u + q, g.sy, g.sz}, V{v + q, g.sy, g.sz}, W{w + q, g.sy, g.sz};
-    nut[q] = smag_point<R, UNI>(g, k, c_s, U, V, W);
+    nut[q] = smag_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, U, V, W);
 }

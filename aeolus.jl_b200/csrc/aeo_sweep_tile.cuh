@@ -67,27 +67,32 @@ struct TileShape {
     static constexpr int PSZA = (int)(((PSZ * sizeof(R) + 127) / 128) * 128 / sizeof(R));
     static constexpr int NPW = TX + 2, NPH = TY + 2, NPS = NPW * NPH;  // nut plane with halo 1
     static constexpr size_t PLANES_BYTES = (size_t)NS * 4 * PSZA * sizeof(R);
-    static constexpr size_t NUT_BYTES = SGS ? (size_t)3 * NPS * sizeof(R) : 0;
-    static constexpr size_t SMEM = PLANES_BYTES + ((NUT_BYTES + 127) / 128) * 128 + 8 * NS + 128;
+    static constexpr size_t NUT_BYTES = SGS ? (((size_t)3 * NPS * sizeof(R) + 127) / 128) * 128 : 0;
+    static constexpr size_t BAR_BYTES = 128;
+    static_assert(NS * 8 <= (int)BAR_BYTES, "mbarrier block");
+    // + the chunk's per-level factors, LV_N rows of (kchunk + 2 AEO_LH), + alignment slack
+    static size_t smem(int kchunk) {
+        return PLANES_BYTES + NUT_BYTES + BAR_BYTES + (size_t)LV_N * (kchunk + 2 * AEO_LH) * sizeof(R) + 128;
+    }
 };
 
 struct TileMaps {
     CUtensorMap u, v, w, t;
 };
 
-// accessor of one field around the thread's point: level k+dk is ring plane p[dk+ZL]
-template <typename R, int NW, int ZL, int PW>
+// Accessor of one field around the thread's point: level k+dk is the ring
+// plane lp[dk+ZL] (pointers at the thread's point, field 0), field f sits
+// FOFS elements further.  Every index but the plane pointer is a constant.
+template <typename R, int ZL, int PW, int FOFS>
 struct SmAcc {
-    const R* p[NW];
-    int base;
-    __device__ __forceinline__ R operator()(int di, int dj, int dk) const { return p[dk + ZL][base + dj * PW + di]; }
+    const R* const* lp;
+    __device__ __forceinline__ R operator()(int di, int dj, int dk) const { return lp[dk + ZL][FOFS + dj * PW + di]; }
 };
 
 template <typename R, int NPW>
 struct NutAcc {
-    const R* p[3];  // levels k-1, k, k+1
-    int base;
-    __device__ __forceinline__ R operator()(int di, int dj, int dk) const { return p[dk + 1][base + dj * NPW + di]; }
+    const R* p[3];  // levels k-1, k, k+1 at the thread's point
+    __device__ __forceinline__ R operator()(int di, int dj, int dk) const { return p[dk + 1][dj * NPW + di]; }
 };
 
 template <typename R, int ADV, bool SGS, bool ANEL, bool UNI>
@@ -95,10 +100,13 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
                                                          int kchunk, int* err) {
     using S = TileShape<R, ADV, SGS>;
     extern __shared__ __align__(128) unsigned char smem_tile[];
-    unsigned char* sbase = reinterpret_cast<unsigned char*>(((uintptr_t)smem_tile + 127) & ~(uintptr_t)127);
+    // offsets from the shared array itself keep every pointer below in the
+    // shared state space (plain ld.shared with constant offsets)
+    unsigned char* sbase = smem_tile + ((128u - (smem_u32(smem_tile) & 127u)) & 127u);
     R* planes = reinterpret_cast<R*>(sbase);
     R* nutp = reinterpret_cast<R*>(sbase + S::PLANES_BYTES);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + S::PLANES_BYTES + ((S::NUT_BYTES + 127) / 128) * 128);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + S::PLANES_BYTES + S::NUT_BYTES);
+    R* lvs = reinterpret_cast<R*>(sbase + S::PLANES_BYTES + S::NUT_BYTES + S::BAR_BYTES);
 
     const Geo& g = a.g;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + S::TX * ty;
@@ -113,26 +121,38 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
 
     auto slot_of = [&](int L) { return (L - Lfirst) % S::NS; };
     auto parity_of = [&](int L) { return (uint32_t)(((L - Lfirst) / S::NS) & 1); };
-    auto plane = [&](int L, int f) { return planes + ((size_t)slot_of(L) * 4 + f) * S::PSZA; };
+    auto plane = [&](int L) { return planes + (size_t)slot_of(L) * 4 * S::PSZA; };
     auto issue = [&](int L) {
         uint64_t* b = bars + slot_of(L);
         mbar_expect_tx(b, bytes);
         const int x = i0 + AEO_HX - 4, y = j0 + AEO_H - S::HH, z = L + AEO_H;
-        tma_load_3d(plane(L, 0), &maps.u, b, x, y, z);
-        tma_load_3d(plane(L, 1), &maps.v, b, x, y, z);
-        tma_load_3d(plane(L, 2), &maps.w, b, x, y, z);
-        tma_load_3d(plane(L, 3), &maps.t, b, x, y, z);
+        R* d = plane(L);
+        tma_load_3d(d, &maps.u, b, x, y, z);
+        tma_load_3d(d + S::PSZA, &maps.v, b, x, y, z);
+        tma_load_3d(d + 2 * S::PSZA, &maps.w, b, x, y, z);
+        tma_load_3d(d + 3 * S::PSZA, &maps.t, b, x, y, z);
     };
 
     if (tid == 0) {
         for (int s = 0; s < S::NS; ++s) mbar_init(bars + s, 1);
         fence_mbar_init();
     }
+    // the chunk's per-level factors: level k of row f at lvs[f * nlt + k + AEO_LH - kbeg]
+    const int nlt = kend - kbeg + 2 * AEO_LH;
+    {
+        const R* src = static_cast<const R*>(g.lvr);
+        for (int e = tid; e < LV_N * nlt; e += S::NT) {
+            const int f = e / nlt, kk = e - f * nlt;
+            lvs[e] = src[(size_t)f * g.lvn + kbeg + kk];
+        }
+    }
     __syncthreads();
+    const Met<R, UNI> m(g, lvs, nlt, AEO_LH - kbeg);
     int Lissued = min(Llast, kbeg + S::ZH + S::LOOK);
     if (tid == 0)
         for (int L = Lfirst; L <= Lissued; ++L) issue(L);
 
+    const R dt = R(__ldg(a.dtp));
     const int vbase = (ty + S::HH) * S::PW + (tx + 4);
     bool failed = false;
     for (int k = kbeg; k < kend; ++k) {
@@ -141,76 +161,73 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
         bool ok = true;
         for (int L = Lw0; L <= k + S::ZH; ++L) ok = ok && mbar_wait_bounded(bars + slot_of(L), parity_of(L));
         if (__syncthreads_or(!ok)) { failed = true; break; }
-
-        SmAcc<R, S::NW, S::ZL, S::PW> U, V, W, T;
-#pragma unroll
-        for (int d = 0; d < S::NW; ++d) {
-            const int L = k - S::ZL + d;
-            U.p[d] = plane(L, 0); V.p[d] = plane(L, 1); W.p[d] = plane(L, 2); T.p[d] = plane(L, 3);
+        // every thread is past level k-1: the slot of level k-1-ZL takes level k+ZH+LOOK
+        if (k > kbeg) {
+            const int Ln = k + S::ZH + S::LOOK;
+            if (Ln <= Llast) {
+                if (tid == 0) issue(Ln);
+                Lissued = Ln;
+            }
         }
-        U.base = V.base = W.base = T.base = vbase;
+
+        const R* lp[S::NW];
+#pragma unroll
+        for (int d = 0; d < S::NW; ++d) lp[d] = plane(k - S::ZL + d) + vbase;
+        const SmAcc<R, S::ZL, S::PW, 0> U{lp};
+        const SmAcc<R, S::ZL, S::PW, S::PSZA> V{lp};
+        const SmAcc<R, S::ZL, S::PW, 2 * S::PSZA> W{lp};
+        const SmAcc<R, S::ZL, S::PW, 3 * S::PSZA> T{lp};
 
         NutAcc<R, S::NPW> N;
         if (SGS) {
             // eddy viscosity of the levels k-1 .. k+1 (first iteration) or k+1
             const int Lz0 = (k == kbeg) ? k - 1 : k + 1;
+            bool mirror = false;
             for (int L = Lz0; L <= k + 1; ++L) {
-                R* np = nutp + (size_t)(((L % 3) + 3) % 3) * S::NPS;
-                const bool mirror = g.bc_z == 1 && (L < 0 || L >= g.nz);
-                if (mirror) continue;   // filled from the interior neighbour below
-                SmAcc<R, S::NW, S::ZL, S::PW> Uq, Vq, Wq;
+                if (g.bc_z == 1 && (L < 0 || L >= g.nz)) { mirror = true; continue; }  // from the level inside
+                R* np = nutp + (size_t)((L + 3) % 3) * S::NPS;
+                const R* sp[3];
 #pragma unroll
-                for (int d = 0; d < S::NW; ++d) {
-                    const int Ld = L - S::ZL + d;
-                    const bool inwin = Ld >= k - S::ZL && Ld <= k + S::ZH;
-                    Uq.p[d] = inwin ? plane(Ld, 0) : planes;
-                    Vq.p[d] = inwin ? plane(Ld, 1) : planes;
-                    Wq.p[d] = inwin ? plane(Ld, 2) : planes;
-                }
+                for (int d = 0; d < 3; ++d) sp[d] = plane(L - 1 + d);
                 for (int e = tid; e < S::NPS; e += S::NT) {
-                    const int ci = e % S::NPW, cj = e / S::NPW;
+                    const int cj = e / S::NPW, ci = e - cj * S::NPW;
                     const int b = (cj - 1 + S::HH) * S::PW + (ci - 1 + 4);
-                    Uq.base = Vq.base = Wq.base = b;
-                    np[e] = smag_point<R, UNI>(g, L, R(a.c_s), Uq, Vq, Wq);
+                    const R* q[3] = {sp[0] + b, sp[1] + b, sp[2] + b};
+                    const SmAcc<R, 1, S::PW, 0> Uq{q};
+                    const SmAcc<R, 1, S::PW, S::PSZA> Vq{q};
+                    const SmAcc<R, 1, S::PW, 2 * S::PSZA> Wq{q};
+                    np[e] = smag_point<R, UNI>(m, g, L, R(a.c_s), Uq, Vq, Wq);
                 }
             }
             __syncthreads();
-            // walls: the halo levels take the mirrored interior value
-            for (int L = Lz0; L <= k + 1; ++L) {
-                if (!(g.bc_z == 1 && (L < 0 || L >= g.nz))) continue;
-                const int Ls = L < 0 ? -L - 1 : 2 * g.nz - 1 - L;
-                R* dst = nutp + (size_t)(((L % 3) + 3) % 3) * S::NPS;
-                const R* src = nutp + (size_t)(((Ls % 3) + 3) % 3) * S::NPS;
-                for (int e = tid; e < S::NPS; e += S::NT) dst[e] = src[e];
+            if (mirror) {
+                // walls: the halo levels take the mirrored interior value
+                for (int L = Lz0; L <= k + 1; ++L) {
+                    if (!(g.bc_z == 1 && (L < 0 || L >= g.nz))) continue;
+                    const int Ls = L < 0 ? -L - 1 : 2 * g.nz - 1 - L;
+                    R* dst = nutp + (size_t)((L + 3) % 3) * S::NPS;
+                    const R* src = nutp + (size_t)((Ls + 3) % 3) * S::NPS;
+                    for (int e = tid; e < S::NPS; e += S::NT) dst[e] = src[e];
+                }
+                __syncthreads();
             }
-            __syncthreads();
-            for (int d = 0; d < 3; ++d) {
-                const int L = k - 1 + d;
-                N.p[d] = nutp + (size_t)(((L % 3) + 3) % 3) * S::NPS;
-            }
-            N.base = (ty + 1) * S::NPW + (tx + 1);
+            const int nb = (ty + 1) * S::NPW + (tx + 1);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) N.p[d] = nutp + (size_t)((k - 1 + d + 3) % 3) * S::NPS + nb;
         } else {
             N.p[0] = N.p[1] = N.p[2] = nutp;
-            N.base = 0;
         }
 
         if (active) {
             R tu, tv, tw, tt;
-            sweep_point<R, ADV, SGS, ANEL, UNI>(a, g, k, U, V, W, T, N, tu, tv, tw, tt);
+            sweep_point<R, ADV, SGS, ANEL, UNI>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt);
             const long long qi = iidx(g, i, j, k), q = pidx(g, i, j, k);
-            const R dt = R(__ldg(a.dtp));
             a.us[qi] = U(0, 0, 0) + dt * tu;
             a.vs[qi] = V(0, 0, 0) + dt * tv;
             a.ws[qi] = (g.bc_z == 1 && k == 0) ? R(0) : W(0, 0, 0) + dt * tw;
             R tn = T(0, 0, 0) + dt * tt;
             if (a.stage) tn = a.ca * a.th0[q] + a.cb * tn;
             a.th_out[q] = tn;
-        }
-        __syncthreads();  // every read of level k - ZL is done: its slot can be refilled
-        const int Lnext = k + S::ZH + S::LOOK + 1;
-        if (Lnext <= Llast) {
-            if (tid == 0) issue(Lnext);
-            Lissued = Lnext;
         }
     }
     if (failed) {

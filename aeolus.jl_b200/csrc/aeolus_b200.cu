@@ -102,6 +102,7 @@ template <typename R>
 struct Core : CoreBase {
     std::vector<void*> allocs;
     double* levels = nullptr;  // metric vectors
+    R* levels_r = nullptr;     // per-level factors in the working precision (rows LV_*)
     double *kx2 = nullptr, *ky2 = nullptr, *kz2 = nullptr;
     double* colc = nullptr;    // column coefficients
     ColumnCoef cc{};
@@ -244,6 +245,44 @@ struct Core : CoreBase {
         g.wc = anel ? levels + 10 * L : nullptr;
         g.wf = anel ? levels + 11 * L : nullptr;
         g.thf = anel ? levels + 12 * L : nullptr;
+        // the same factors in R, with the reciprocals, g/theta_f and the sponge
+        // rates folded in (each rounded as the division or product in R rounds it)
+        {
+            std::vector<R> hr((size_t)LV_N * L, R(0));
+            auto row = [&](int v, int e) { return hv[(size_t)v * L + e]; };
+            const R zs = R(c.sponge_zstart), al = R(c.sponge_alpha);
+            const R sinv = R(1.0 / (c.z0 + c.lz - c.sponge_zstart));
+            auto rate = [&](double z) -> R {
+                if (c.sponge_alpha == 0.0 || !(z >= (double)zs)) return R(0);
+                R arg = R(0.5 * 3.14159265358979323846) * (R(z) - zs) * sinv;
+                R sn = R(std::sin((double)arg));
+                return al * sn * sn;
+            };
+            for (int e = 0; e < L; ++e) {
+                auto put_r = [&](int f, R v) { hr[(size_t)f * L + e] = v; };
+                put_r(LV_IDZC, R(row(0, e)));
+                put_r(LV_IDZF, R(row(1, e)));
+                put_r(LV_IDZOFF, R(row(2, e)));
+                put_r(LV_WLO, R(row(3, e)));
+                put_r(LV_WHI, R(row(4, e)));
+                put_r(LV_ALO, R(row(5, e)));
+                put_r(LV_AHI, R(row(6, e)));
+                put_r(LV_DELTA, R(row(7, e)));
+                const R wcr = R(row(10, e)), wfr = R(row(11, e)), thr = R(row(12, e));
+                put_r(LV_WC, wcr);
+                put_r(LV_WF, wfr);
+                put_r(LV_IWC, wcr != R(0) ? R(1) / wcr : R(0));
+                put_r(LV_IWF, wfr != R(0) ? R(1) / wfr : R(0));
+                put_r(LV_THF, thr);
+                put_r(LV_GTHF, thr != R(0) ? R(c.g) / thr : R(0));
+                put_r(LV_SPC, rate(row(8, e)));
+                put_r(LV_SPF, rate(row(9, e)));
+            }
+            if (aeo_status s = alloc(&levels_r, hr.size())) return s;
+            CK(cudaMemcpyAsync(levels_r, hr.data(), hr.size() * sizeof(R), cudaMemcpyHostToDevice, st));
+            g.lvr = levels_r;
+            g.lvn = L;
+        }
 
         // ---- eigenvalues and column coefficients
         const int Nx = c.nx, Ny = c.ny, Mh = Nx / 2 + 1;
@@ -395,10 +434,10 @@ struct Core : CoreBase {
     template <int ADV, bool SG, bool AN, bool UN>
     void launch_sweep_t(int s_in, const SweepArgs<R>& a) {
         using TS = TileShape<R, ADV, SG>;
-        cudaFuncSetAttribute(sweep_tile_kernel<R, ADV, SG, AN, UN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)TS::SMEM);
+        const size_t sm = TS::smem(kchunk);
+        cudaFuncSetAttribute(sweep_tile_kernel<R, ADV, SG, AN, UN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         dim3 grid((g.nx + TS::TX - 1) / TS::TX, (g.ny + TS::TY - 1) / TS::TY, (g.nz + kchunk - 1) / kchunk);
-        sweep_tile_kernel<R, ADV, SG, AN, UN><<<grid, dim3(TS::TX, TS::TY), TS::SMEM, st>>>(tmaps[s_in], a, kchunk, d_flag);
+        sweep_tile_kernel<R, ADV, SG, AN, UN><<<grid, dim3(TS::TX, TS::TY), sm, st>>>(tmaps[s_in], a, kchunk, d_flag);
     }
 
     aeo_status launch_sweep(int s_in, const SweepArgs<R>& a) {
@@ -447,11 +486,10 @@ struct Core : CoreBase {
             double nrm = 1.0 / ((double)g.nx * g.ny * g.nz);
             fftz_solve_kernel<R><<<gz, 256, smz, st>>>(g, S, tw, NT, tpx_z, kx2, ky2, kz2, nrm);
         } else {
-            dim3 gt((Mh + 31) / 32, g.ny);
-            size_t smt = (size_t)g.nz * 32 * sizeof(double);
+            size_t smt = thomas_smem(g);
             if (smt > 48 * 1024)
                 cudaFuncSetAttribute(thomas_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
-            thomas_kernel<R><<<gt, 32, smt, st>>>(g, S, dsc, cc);
+            thomas_kernel<R><<<thomas_blocks(g), 32, smt, st>>>(g, S, dsc, cc);
         }
         CKL();
         mark(AEO_K_ZSOLVE);
@@ -955,6 +993,7 @@ static aeo_status validate(const aeo_config* c, const double* zf, const double* 
         if (!is_pow2(c->nz) || c->nz > 2048) { *m = "the FFT solver needs nz a power of two <= 2048"; return AEO_ERR_ARGUMENT; }
     } else if (c->solver == AEO_SOLVER_COLUMN) {
         if (c->bc_z != AEO_BC_WALL) { *m = "the column solver needs walls in z"; return AEO_ERR_ARGUMENT; }
+        if (c->nz > AEO_COLUMN_NZ_MAX) { *m = "the column solver needs nz <= " + std::to_string(AEO_COLUMN_NZ_MAX); return AEO_ERR_ARGUMENT; }
     } else { *m = "unknown solver"; return AEO_ERR_ARGUMENT; }
     if (c->advection < 0 || c->advection > 2) { *m = "unknown advection scheme"; return AEO_ERR_ARGUMENT; }
     if (c->advection != AEO_ADV_CENTRED && (c->stretched || c->core == AEO_CORE_ANELASTIC)) {
