@@ -7,9 +7,10 @@
 // spectrum S is stored [kz][ky][kx] with kx in [0, nx/2] (the r2c half
 // spectrum of x), complex of the state precision.
 //
-//   div_fftx   divergence of the predicted velocity (plain, or W-weighted for
-//              the sound-proof core) fused with the r2c transform along x
+//   div        divergence of the predicted velocity (plain, or W-weighted for
+//              the sound-proof core), one cell per thread
 //              (src/FiniteVolume.jl:1869-1888, src/Anelastic.jl:1110-1120)
+//   src_fftx   r2c transform along x of an interior source (the divergence)
 //   ffty       complex transform along y (forward or inverse)
 //   fftz_solve periodic z: forward transform, scale by nrm/lambda (zero mean
 //              mode), inverse transform -- one pass (src/PressureSolvers.jl:128-138,
@@ -19,103 +20,174 @@
 //              integrated (src/PressureSolvers.jl:650-661, :754-805)
 //   ifftx      c2r along x into the potential phi (interior array)
 //
-// The transforms are Stockham autosort FFTs (radix-4 passes, a radix-2 pass
-// when log2 n is odd) on lines held in shared memory; twiddles come from one
-// table tw[m] = exp(-2 pi i m / NT) with NT the largest transform length.
+// The transforms are Stockham autosort FFTs on lines held in shared memory,
+// each pass an in-register DFT of radix 16, 8 or 4; the inter-pass twiddles
+// come from one table tw[m] = exp(-2 pi i m / NT) with NT the largest
+// transform length.
 #pragma once
 
 #include "aeo_common.cuh"
 
-// Batched in-place Stockham FFT in shared memory.  Line l, element e lives
-// at buf[l*ls + e*es]; n = 2^logn points per line, 2^lognl lines.
-// LINE_FAST: consecutive threads take consecutive lines (strided lines,
-// es > 1); otherwise consecutive elements of a line.  KB bounds the
-// butterflies a thread holds per pass (checked by the host).  Every size is a
-// power of two, so all index arithmetic is shifts and masks.
-template <typename R, bool INV, bool LINE_FAST, int KB>
-__device__ __forceinline__ void smem_fft(cplx<R>* buf, int logn, int lognl, int ls, int es,
-                                         const cplx<R>* __restrict__ tw, int NT) {
-    const int nthr = blockDim.x * blockDim.y * blockDim.z;
-    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
-    const int logNT = __ffs(NT) - 1;
-    for (int logNs = 0; logNs < logn;) {
-        const int lr = (logn - logNs >= 2) ? 2 : 1;    // radix 4, or 2 for the last pass of an odd log n
-        const int RR = 1 << lr;
-        const int lognb = logn - lr, nb = 1 << lognb;  // butterflies per line
-        const int total = nb << lognl;
-        const int Ns = 1 << logNs;
-        const int tsh = logNT - lr - logNs;            // twiddle step NT / (RR Ns) as a shift
-        cplx<R> v[KB][4];
-        int jj[KB], ll[KB];
+// Launch shape of every transform CTA: a CTA holds at most 2048 points (the
+// host sizes rows / column tiles so), PTS per thread: 128 threads x 16 points
+// (radix up to 16) in FP32, 256 x 8 (radix up to 8) in FP64, where 16
+// complex doubles would not fit the register budget.
+template <typename R>
+struct FftCfg {
+    static constexpr int THREADS = sizeof(R) == 8 ? 256 : 128;
+    static constexpr int PTS = 2048 / THREADS;
+    static constexpr int MAXLR = PTS == 16 ? 4 : 3;
+    static constexpr int MINB = sizeof(R) == 8 ? 2 : 4;   // CTAs per SM compiled for (128 registers)
+};
+#define FFT_THREADS(R) (FftCfg<R>::THREADS)
+#define FFT_MINB(R) (FftCfg<R>::MINB)
+
+// exp(-2 pi i m / 16), m = 0..15: the exact values of cos and sin at
+// multiples of pi/8 (cos pi/8 = sqrt(2 + sqrt 2)/2, cos pi/4 = sqrt(2)/2,
+// cos 3pi/8 = sqrt(2 - sqrt 2)/2), so every in-register DFT of R | 16 points
+// uses constants, not table loads.
+__device__ __forceinline__ double w16_re(int m) {
+    constexpr double c[16] = {1.0, 0.92387953251128675613, 0.70710678118654752440, 0.38268343236508977173,
+                              0.0, -0.38268343236508977173, -0.70710678118654752440, -0.92387953251128675613,
+                              -1.0, -0.92387953251128675613, -0.70710678118654752440, -0.38268343236508977173,
+                              0.0, 0.38268343236508977173, 0.70710678118654752440, 0.92387953251128675613};
+    return c[m & 15];
+}
+__device__ __forceinline__ double w16_im(int m) { return -w16_re((m + 12) & 15); }   // -sin(2 pi m / 16)
+
+// In-register DFT of R points (natural order in and out), decimation in time:
+// y_q = sum_r v_r W_R^{rq}, W_R = exp(-+2 pi i / R).
+template <typename R, int N, bool INV>
+__device__ __forceinline__ void dft_reg(cplx<R>* v) {
+    if constexpr (N == 1) {
+        return;
+    } else if constexpr (N == 2) {
+        const cplx<R> a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else {
+        constexpr int H = N / 2;
+        cplx<R> e[H], o[H];
 #pragma unroll
-        for (int s = 0; s < KB; ++s) {
-            int b = tid + s * nthr;
-            if (b < total) {
-                int l, j;
-                if (LINE_FAST) { l = b & ((1 << lognl) - 1); j = b >> lognl; }
-                else { l = b >> lognb; j = b & (nb - 1); }
-                jj[s] = j;
-                ll[s] = l;
-                cplx<R>* base = buf + l * ls;
-                if (RR == 4) {
-#pragma unroll
-                    for (int r = 0; r < 4; ++r) v[s][r] = base[(j + r * nb) * es];
-                } else {
-                    v[s][0] = base[j * es];
-                    v[s][1] = base[(j + nb) * es];
-                }
-            }
+        for (int i = 0; i < H; ++i) {
+            e[i] = v[2 * i];
+            o[i] = v[2 * i + 1];
         }
-        __syncthreads();
+        dft_reg<R, H, INV>(e);
+        dft_reg<R, H, INV>(o);
 #pragma unroll
-        for (int s = 0; s < KB; ++s) {
-            int b = tid + s * nthr;
-            if (b < total) {
-                int j = jj[s], l = ll[s];
-                int k = j & (Ns - 1);
-                if (Ns > 1) {
-#pragma unroll
-                    for (int r = 1; r < 4; ++r) {
-                        if (r < RR) {
-                            int m = ((r * k) << tsh) & (NT - 1);
-                            cplx<R> wv = tw[m];
-                            if (INV) wv.y = -wv.y;
-                            v[s][r] = cmul(v[s][r], wv);
-                        }
-                    }
-                }
-                cplx<R> y0, y1, y2, y3;
-                if (RR == 4) {
-                    cplx<R> b0 = cadd(v[s][0], v[s][2]), b1 = csub(v[s][0], v[s][2]);
-                    cplx<R> b2 = cadd(v[s][1], v[s][3]), b3 = csub(v[s][1], v[s][3]);
-                    // forward: y1 = b1 - i b3, y3 = b1 + i b3; inverse the opposite
-                    cplx<R> ib3 = cmk<R>(-b3.y, b3.x);
-                    y0 = cadd(b0, b2);
-                    y2 = csub(b0, b2);
-                    y1 = INV ? cadd(b1, ib3) : csub(b1, ib3);
-                    y3 = INV ? csub(b1, ib3) : cadd(b1, ib3);
-                } else {
-                    y0 = cadd(v[s][0], v[s][1]);
-                    y1 = csub(v[s][0], v[s][1]);
-                    y2 = y0;
-                    y3 = y1;
-                }
-                int o = ((j - k) << lr) + k;
-                cplx<R>* base = buf + l * ls;
-                base[o * es] = y0;
-                base[(o + Ns) * es] = y1;
-                if (RR == 4) {
-                    base[(o + 2 * Ns) * es] = y2;
-                    base[(o + 3 * Ns) * es] = y3;
-                }
+        for (int k = 0; k < H; ++k) {
+            cplx<R> t = o[k];
+            const int m = k * (16 / N);              // W_N^k = W_16^m
+            if (m == 4) {                            // -i (forward) / +i (inverse)
+                t = INV ? cmk<R>(-t.y, t.x) : cmk<R>(t.y, -t.x);
+            } else if (m != 0) {
+                const R wr = R(w16_re(m)), wi = INV ? R(-w16_im(m)) : R(w16_im(m));
+                t = cmk<R>(t.x * wr - t.y * wi, t.x * wi + t.y * wr);
             }
+            v[k] = cadd(e[k], t);
+            v[k + H] = csub(e[k], t);
         }
-        __syncthreads();
-        logNs += lr;
     }
 }
 
-constexpr int FFT_KB = 4;
+// Row-contiguous lines (es = 1) are stored skewed, element e at e + e/16, so
+// that the stride-R writes of a radix-R pass fall in distinct banks; a line
+// of M elements then spans M + M/16 slots; one more holds a raw half
+// spectrum's M + 1 bins before the c2r pre-process.
+__host__ __device__ __forceinline__ int xrow(int M) { return M + (M >> 4) + 1; }
+template <bool SKEW>
+__device__ __forceinline__ int sk16(int e) { return SKEW ? e + (e >> 4) : e; }
+
+// One Stockham pass of radix 2^LR over all lines: butterfly j of a line reads
+// x[j + r n/R], applies the twiddles W_{R Ns}^{r k} (k = j mod Ns), does the
+// R-point DFT in registers and writes y[(j - k) R + k + q Ns].  A thread
+// holds FftCfg::PTS / R butterflies; everything but the in-place stores happens
+// before the barrier, so only the results and their offsets live across it.
+template <typename R, int LR, bool INV, bool LINE_FAST, bool SKEW = !LINE_FAST>
+__device__ __forceinline__ void fft_pass(cplx<R>* buf, int logn, int lognl, int ls, int es, int logNs,
+                                         const cplx<R>* __restrict__ tw, int NT, int logNT) {
+    constexpr int RR = 1 << LR, KB = FftCfg<R>::PTS / RR;
+    const int nthr = blockDim.x;
+    const int tid = threadIdx.x;
+    const int lognb = logn - LR, nb = 1 << lognb;
+    const int total = nb << lognl;
+    const int Ns = 1 << logNs;
+    const int tsh = logNT - LR - logNs;
+    asm volatile("" ::: "memory");   // keep this variant's loads below the radix dispatch
+    cplx<R> v[KB][RR];
+    int oo[KB];   // output offset of butterfly s (-1: none)
+#pragma unroll
+    for (int s = 0; s < KB; ++s) {
+        const int b = tid + s * nthr;
+        oo[s] = -1;
+        if (b < total) {
+            int l, j;
+            if (LINE_FAST) { l = b & ((1 << lognl) - 1); j = b >> lognl; }
+            else { l = b >> lognb; j = b & (nb - 1); }
+            const int k = j & (Ns - 1);
+            const cplx<R>* base = buf + l * ls;
+            v[s][0] = base[sk16<SKEW>(j) * es];
+#pragma unroll
+            for (int r = 1; r < RR; ++r) {
+                v[s][r] = base[sk16<SKEW>(j + r * nb) * es];
+                if (logNs > 0) {
+                    cplx<R> wv = tw[((r * k) << tsh) & (NT - 1)];
+                    if (INV) wv.y = -wv.y;
+                    v[s][r] = cmul(v[s][r], wv);
+                }
+            }
+            dft_reg<R, RR, INV>(v[s]);
+            // SKEW: the line offset and the first output index, packed (both < 2^15)
+            oo[s] = SKEW ? ((l * ls) | ((((j - k) << LR) + k) << 16)) : l * ls + (((j - k) << LR) + k) * es;
+        }
+    }
+    __syncthreads();
+    const int st = Ns * es;
+#pragma unroll
+    for (int s = 0; s < KB; ++s) {
+        if (oo[s] >= 0) {
+            if (SKEW) {
+                const int lo = oo[s] & 0xFFFF, o = oo[s] >> 16;
+#pragma unroll
+                for (int q = 0; q < RR; ++q) buf[lo + sk16<true>(o + q * Ns)] = v[s][q];
+            } else {
+#pragma unroll
+                for (int q = 0; q < RR; ++q) buf[oo[s] + q * st] = v[s][q];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Batched in-place Stockham FFT in shared memory.  Line l, element e lives
+// at buf[l*ls + e*es]; n = 2^logn points per line, 2^lognl lines, at most
+// FftCfg::PTS points per thread.  LINE_FAST: consecutive threads take
+// consecutive lines (strided lines, es > 1); otherwise consecutive elements
+// of a line.  The passes have radix 2^2 .. 2^MAXLR (ceil(logn / MAXLR)
+// passes, the logs spread evenly, larger first; radix 2 only for a 2-point
+// line), so all index arithmetic is shifts and masks and each pass's DFT
+// lives in registers.
+template <typename R, bool INV, bool LINE_FAST>
+__device__ __forceinline__ void smem_fft(cplx<R>* buf, int logn, int lognl, int ls, int es,
+                                         const cplx<R>* __restrict__ tw, int NT) {
+    constexpr int MAXLR = FftCfg<R>::MAXLR;
+    const int logNT = __ffs(NT) - 1;
+    if (logn == 1) {
+        fft_pass<R, 1, INV, LINE_FAST>(buf, logn, lognl, ls, es, 0, tw, NT, logNT);
+        return;
+    }
+    const int np = (logn + MAXLR - 1) / MAXLR;
+    int logNs = 0;
+    for (int pass = 0; pass < np; ++pass) {
+        const int rest = logn - logNs, left = np - pass;
+        const int lr = (rest + left - 1) / left;
+        if (MAXLR >= 4 && lr == 4) fft_pass<R, (MAXLR >= 4 ? 4 : 3), INV, LINE_FAST>(buf, logn, lognl, ls, es, logNs, tw, NT, logNT);
+        else if (lr == 3) fft_pass<R, 3, INV, LINE_FAST>(buf, logn, lognl, ls, es, logNs, tw, NT, logNT);
+        else fft_pass<R, 2, INV, LINE_FAST>(buf, logn, lognl, ls, es, logNs, tw, NT, logNT);
+        logNs += lr;
+    }
+}
 
 // ---- divergence + r2c along x --------------------------------------------------
 // The neighbours i+1, j+1, k+1 are plain loads inside the domain; only the
@@ -138,83 +210,97 @@ __device__ __forceinline__ R div_point(const Geo& g, const Met<R, UNI>& m, const
 // The r2c post-process of bin kk from the packed M-point transform of one row.
 template <typename R>
 __device__ __forceinline__ cplx<R> r2c_bin(const cplx<R>* rowbuf, int M, int kk, cplx<R> wv) {
-    const cplx<R> a = rowbuf[kk == M ? 0 : kk];
-    const cplx<R> b = rowbuf[kk == 0 ? 0 : M - kk];
+    const cplx<R> a = rowbuf[sk16<true>(kk == M ? 0 : kk)];
+    const cplx<R> b = rowbuf[sk16<true>(kk == 0 ? 0 : M - kk)];
     const R er = R(0.5) * (a.x + b.x), ei = R(0.5) * (a.y - b.y);
     const R orr = R(0.5) * (a.y + b.y), oi = R(-0.5) * (a.x - b.x);
     return cmk<R>(er + (wv.x * orr - wv.y * oi), ei + (wv.x * oi + wv.y * orr));
 }
 
-// One CTA transforms `rows` x-rows (row = j + ny*k).  M = nx/2; rows, M and
-// ny are powers of two.
+// The divergence of the predicted velocity at every interior cell (the
+// source of the pressure solve), one cell per thread; src_fftx transforms it.
 template <typename R, bool ANEL, bool UNI>
-__global__ void __launch_bounds__(256) div_fftx_kernel(Geo g, const R* __restrict__ us, const R* __restrict__ vs,
-                                                       const R* __restrict__ ws, cplx<R>* __restrict__ S,
-                                                       const cplx<R>* __restrict__ tw, int NT, int rows) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx<R>* buf = reinterpret_cast<cplx<R>*>(smem_raw);
-    const int M = g.nx / 2, Mh = M + 1, lM = __ffs(M) - 1, lny = __ffs(g.ny) - 1;
-    const long long nrows = (long long)g.ny * g.nz;
-    const long long row0 = (long long)blockIdx.x * rows;
-    const int tid = threadIdx.x, nthr = blockDim.x;
-    const Met<R, UNI> m(g);
-    for (int e = tid; e < (rows << lM); e += nthr) {
-        const int r = e >> lM, n = e & (M - 1);
-        const long long row = row0 + r;
-        cplx<R> z = cmk<R>(R(0), R(0));
-        if (row < nrows) {
-            const int j = (int)(row & (g.ny - 1)), k = (int)(row >> lny);
-            z.x = div_point<R, ANEL, UNI>(g, m, us, vs, ws, 2 * n, j, k);
-            z.y = div_point<R, ANEL, UNI>(g, m, us, vs, ws, 2 * n + 1, j, k);
-        }
-        buf[e] = z;
-    }
-    __syncthreads();
-    smem_fft<R, false, false, FFT_KB>(buf, lM, __ffs(rows) - 1, M, 1, tw, NT);
-    const int tstep = NT / g.nx;
-    for (int e = tid; e < (rows << lM); e += nthr) {
-        const int r = e >> lM, kk = e & (M - 1);
-        const long long row = row0 + r;
-        if (row < nrows) S[row * Mh + kk] = r2c_bin(buf + r * M, M, kk, tw[(kk * tstep) & (NT - 1)]);
-    }
-    for (int r = tid; r < rows; r += nthr) {   // the Nyquist bin, twiddle exactly -1
-        const long long row = row0 + r;
-        if (row < nrows) S[row * Mh + M] = r2c_bin(buf + r * M, M, M, cmk<R>(R(-1), R(0)));
-    }
+__global__ void __launch_bounds__(256) div_kernel(Geo g, const R* __restrict__ us, const R* __restrict__ vs,
+                                                  const R* __restrict__ ws, R* __restrict__ out) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.nin) return;
+    const int lnx = __ffs(g.nx) - 1, lny = __ffs(g.ny) - 1;
+    const int i = (int)(q & (g.nx - 1)), j = (int)((q >> lnx) & (g.ny - 1)), k = (int)(q >> (lnx + lny));
+    out[q] = div_point<R, ANEL, UNI>(g, Met<R, UNI>(g), us, vs, ws, i, j, k);
 }
 
 // ---- c2r along x into phi ---------------------------------------------------------
+// The pre-process of output bin kk from the half-spectrum bins a = X_kk and
+// b = X_{M-kk} of a row (the inverse of r2c_bin's packing).
 template <typename R>
-__global__ void __launch_bounds__(256) ifftx_kernel(Geo g, const cplx<R>* __restrict__ S, R* __restrict__ phi,
+__device__ __forceinline__ cplx<R> c2r_pre(cplx<R> a, cplx<R> b, cplx<R> wv) {
+    const R er = a.x + b.x, ei = a.y - b.y;
+    const R dr = a.x - b.x, di = a.y + b.y;
+    const R orr = dr * wv.x + di * wv.y, oi = di * wv.x - dr * wv.y;
+    return cmk<R>(er - oi, ei + orr);
+}
+
+// The CTA stages its rows' half spectra with one coalesced load per bin,
+// pre-processes the bin pairs (u, M-u) (unit 0 of a row: bins 0 and M/2) in
+// registers, writes the packed M-point lines skewed, runs the inverse FFT
+// and stores the real pairs.
+template <typename R>
+__global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) ifftx_kernel(Geo g, const cplx<R>* __restrict__ S, R* __restrict__ phi,
                                                     const cplx<R>* __restrict__ tw, int NT, int rows, R scale) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<R>* buf = reinterpret_cast<cplx<R>*>(smem_raw);
-    const int M = g.nx / 2, Mh = M + 1, lM = __ffs(M) - 1;
+    constexpr int UPT = FftCfg<R>::PTS / 2;
+    const int M = g.nx / 2, Mh = M + 1, lM = __ffs(M) - 1, LS = xrow(M);
     const long long nrows = (long long)g.ny * g.nz;
     const long long row0 = (long long)blockIdx.x * rows;
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int tstep = NT / g.nx;
+#pragma unroll 16
     for (int e = tid; e < (rows << lM); e += nthr) {
         const int r = e >> lM, kk = e & (M - 1);
         const long long row = row0 + r;
-        cplx<R> z = cmk<R>(R(0), R(0));
-        if (row < nrows) {
-            cplx<R> a = S[row * Mh + kk], b = S[row * Mh + (M - kk)];
-            R er = a.x + b.x, ei = a.y - b.y;
-            R dr = a.x - b.x, di = a.y + b.y;
-            cplx<R> wv = tw[(kk * tstep) & (NT - 1)];
-            R orr = dr * wv.x + di * wv.y, oi = di * wv.x - dr * wv.y;
-            z = cmk<R>(er - oi, ei + orr);
-        }
-        buf[e] = z;
+        buf[r * LS + kk] = row < nrows ? S[row * Mh + kk] : cmk<R>(R(0), R(0));
+    }
+    for (int r = tid; r < rows; r += nthr) {
+        const long long row = row0 + r;
+        buf[r * LS + M] = row < nrows ? S[row * Mh + M] : cmk<R>(R(0), R(0));
     }
     __syncthreads();
-    smem_fft<R, true, false, FFT_KB>(buf, lM, __ffs(rows) - 1, M, 1, tw, NT);
+    const int lH = lM - 1, H = M >> 1;
+    const int nunits = rows << lH;
+    cplx<R> z0[UPT], z1[UPT];
+    int pos[UPT];
+#pragma unroll
+    for (int s = 0; s < UPT; ++s) {
+        const int e = tid + s * nthr;
+        pos[s] = -1;
+        if (e < nunits) {
+            const int r = e >> lH, u = e & (H - 1);
+            const cplx<R>* rb = buf + r * LS;
+            const cplx<R> a = rb[u], b = rb[M - u];
+            z0[s] = c2r_pre(a, b, tw[(u * tstep) & (NT - 1)]);
+            if (u == 0) z1[s] = c2r_pre(rb[H], rb[H], tw[(H * tstep) & (NT - 1)]);
+            else z1[s] = c2r_pre(b, a, tw[((M - u) * tstep) & (NT - 1)]);
+            pos[s] = (r << 16) | u;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < UPT; ++s) {
+        if (pos[s] >= 0) {
+            const int r = pos[s] >> 16, u = pos[s] & 0xFFFF;
+            cplx<R>* rb = buf + r * LS;
+            rb[sk16<true>(u)] = z0[s];
+            rb[sk16<true>(u == 0 ? H : M - u)] = z1[s];
+        }
+    }
+    __syncthreads();
+    smem_fft<R, true, false>(buf, lM, __ffs(rows) - 1, LS, 1, tw, NT);
     for (int e = tid; e < (rows << lM); e += nthr) {
         const int r = e >> lM, n = e & (M - 1);
         const long long row = row0 + r;
         if (row >= nrows) continue;
-        const cplx<R> z = buf[e];
+        const cplx<R> z = buf[r * LS + sk16<true>(n)];
         phi[row * g.nx + 2 * n] = z.x * scale;
         phi[row * g.nx + 2 * n + 1] = z.y * scale;
     }
@@ -223,7 +309,7 @@ __global__ void __launch_bounds__(256) ifftx_kernel(Geo g, const cplx<R>* __rest
 // ---- complex transform along y (MODE 0 forward, 1 inverse) ----------------------
 // CTA: tile of `tpx` consecutive kx columns at one kz, all ky.
 template <typename R, int MODE>
-__global__ void __launch_bounds__(256) ffty_kernel(Geo g, cplx<R>* __restrict__ S, const cplx<R>* __restrict__ tw,
+__global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) ffty_kernel(Geo g, cplx<R>* __restrict__ S, const cplx<R>* __restrict__ tw,
                                                    int NT, int tpx) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<R>* buf = reinterpret_cast<cplx<R>*>(smem_raw);
@@ -232,12 +318,13 @@ __global__ void __launch_bounds__(256) ffty_kernel(Geo g, cplx<R>* __restrict__ 
     const int tid = threadIdx.x, nthr = blockDim.x;
     const long long base = (long long)k * g.ny * Mh;
     const int lt = __ffs(tpx) - 1;
+#pragma unroll 16
     for (int e = tid; e < g.ny * tpx; e += nthr) {
         const int jj = e >> lt, c = e & (tpx - 1), p = p0 + c;
         buf[e] = p < Mh ? S[base + (long long)jj * Mh + p] : cmk<R>(R(0), R(0));
     }
     __syncthreads();
-    smem_fft<R, MODE == 1, true, FFT_KB>(buf, __ffs(g.ny) - 1, __ffs(tpx) - 1, 1, tpx, tw, NT);
+    smem_fft<R, MODE == 1, true>(buf, __ffs(g.ny) - 1, __ffs(tpx) - 1, 1, tpx, tw, NT);
     for (int e = tid; e < g.ny * tpx; e += nthr) {
         const int jj = e >> lt, c = e & (tpx - 1), p = p0 + c;
         if (p < Mh) S[base + (long long)jj * Mh + p] = buf[e];
@@ -246,7 +333,7 @@ __global__ void __launch_bounds__(256) ffty_kernel(Geo g, cplx<R>* __restrict__ 
 
 // ---- periodic z: forward, scale by nrm/lambda, inverse -------------------------
 template <typename R>
-__global__ void __launch_bounds__(256) fftz_solve_kernel(Geo g, cplx<R>* __restrict__ S, const cplx<R>* __restrict__ tw,
+__global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) fftz_solve_kernel(Geo g, cplx<R>* __restrict__ S, const cplx<R>* __restrict__ tw,
                                                          int NT, int tpx, const double* __restrict__ kx2,
                                                          const double* __restrict__ ky2, const double* __restrict__ kz2,
                                                          double nrm) {
@@ -258,12 +345,13 @@ __global__ void __launch_bounds__(256) fftz_solve_kernel(Geo g, cplx<R>* __restr
     const long long sk = (long long)g.ny * Mh;
     const long long base = (long long)j * Mh;
     const int lt = __ffs(tpx) - 1;
+#pragma unroll 16
     for (int e = tid; e < g.nz * tpx; e += nthr) {
         const int kz = e >> lt, c = e & (tpx - 1), p = p0 + c;
         buf[e] = p < Mh ? S[base + kz * sk + p] : cmk<R>(R(0), R(0));
     }
     __syncthreads();
-    smem_fft<R, false, true, FFT_KB>(buf, __ffs(g.nz) - 1, __ffs(tpx) - 1, 1, tpx, tw, NT);
+    smem_fft<R, false, true>(buf, __ffs(g.nz) - 1, __ffs(tpx) - 1, 1, tpx, tw, NT);
     for (int e = tid; e < g.nz * tpx; e += nthr) {
         const int kz = e >> lt, c = e & (tpx - 1), p = p0 + c;
         if (p < Mh) {
@@ -274,7 +362,7 @@ __global__ void __launch_bounds__(256) fftz_solve_kernel(Geo g, cplx<R>* __restr
         }
     }
     __syncthreads();
-    smem_fft<R, true, true, FFT_KB>(buf, __ffs(g.nz) - 1, __ffs(tpx) - 1, 1, tpx, tw, NT);
+    smem_fft<R, true, true>(buf, __ffs(g.nz) - 1, __ffs(tpx) - 1, 1, tpx, tw, NT);
     for (int e = tid; e < g.nz * tpx; e += nthr) {
         const int kz = e >> lt, c = e & (tpx - 1), p = p0 + c;
         if (p < Mh) S[base + kz * sk + p] = buf[e];
@@ -299,11 +387,13 @@ struct ColumnCoef {
 // streams its column through a shared-memory ring with cp.async, THOMAS_PF
 // levels ahead of the recurrence, and waits (cp.async.wait_group) for exactly
 // the level it needs, so the loads overlap the FP64 recurrence instead of
-// exposing one memory latency per level.  The modified upper diagonal c'_k
-// sits in shared memory [nz][32] after the ring, followed by the three
-// coefficient vectors of the diagonals; the forward-elimination values d'_k go to
-// dsc, an FP64 column scratch of the spectrum's layout (dsc may alias S when
-// S is FP64: d'_k overwrites the level it came from after that level was read).
+// exposing one memory latency per level.  The forward-elimination values d'_k
+// go to dsc, an FP64 column scratch of the spectrum's layout (dsc may alias S
+// when S is FP64: d'_k overwrites the level it came from after that level
+// was read).  The modified upper diagonal c'_k goes either to an FP64 scratch
+// of the same layout (CPG: streamed back with d'_k, so a CTA needs only its
+// rings and every column warp of the grid is resident at once) or to shared
+// memory [nz][32] (no scratch: the allocation-free entry).
 constexpr int THOMAS_PF = 16;
 // the largest nz whose column state fits a CTA's 227 KB of shared memory
 #define AEO_COLUMN_NZ_MAX 800
@@ -329,16 +419,23 @@ __device__ __forceinline__ void thomas_wait() { asm volatile("cp.async.wait_grou
 inline unsigned thomas_blocks(const Geo& g) {
     return 1u + (unsigned)(((long long)g.ny * (g.nx / 2 + 1) + 31) / 32);
 }
-// the ring [THOMAS_PF][32] of cplx<double>, then c' [nz][32] and lower, upper, h [nz] each
-inline size_t thomas_smem(const Geo& g) {
-    return (size_t)g.nz * 35 * sizeof(double) + (size_t)THOMAS_PF * 32 * 2 * sizeof(double);
+// Shared memory: the d' ring [THOMAS_PF][32] of cplx<double>, then (CPG) the
+// c' ring [THOMAS_PF][32] of double or (shared c') c' [nz][32], then the
+// lower, upper and h vectors [nz] each; at least the mean mode's 5 nz + 1.
+inline size_t thomas_smem(const Geo& g, bool cpg) {
+    const size_t ring = (size_t)THOMAS_PF * 32 * 2 * sizeof(double);
+    const size_t cols = cpg ? (size_t)THOMAS_PF * 32 * sizeof(double) + (size_t)g.nz * 3 * sizeof(double)
+                            : (size_t)g.nz * 35 * sizeof(double);
+    const size_t mean = (size_t)(5 * g.nz + 1) * sizeof(double);
+    return ring + (cols > mean ? cols : mean);
 }
 
-template <typename R>
-__global__ void __launch_bounds__(32) thomas_kernel(Geo g, cplx<R>* S, cplx<double>* dsc, ColumnCoef c) {
+template <typename R, bool CPG>
+__global__ void __launch_bounds__(32) thomas_kernel(Geo g, cplx<R>* S, cplx<double>* dsc, double* cpg, ColumnCoef c) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx<double>* ring = reinterpret_cast<cplx<double>*>(smem_raw);   // [THOMAS_PF][32], 16-byte entries
-    double* cp = reinterpret_cast<double*>(ring + THOMAS_PF * 32);     // [nz][32]
+    constexpr int D = THOMAS_PF;
+    cplx<double>* ring = reinterpret_cast<cplx<double>*>(smem_raw);   // [D][32], 16-byte entries
+    double* after = reinterpret_cast<double*>(ring + D * 32);
     const int Mh = g.nx / 2 + 1;
     const int lane = threadIdx.x;
     const long long sk = (long long)g.ny * Mh;
@@ -349,7 +446,7 @@ __global__ void __launch_bounds__(32) thomas_kernel(Geo g, cplx<R>* S, cplx<doub
         // sums and the double integration in the reference's order, the
         // warp writes the gauged profile back (the serial loops read shared
         // memory only)
-        double* sv = cp;             // [nz] the column's real parts
+        double* sv = after;          // [nz] the column's real parts
         double* ph = sv + nz;        // [nz] the integrated profile
         double* me = ph + nz;        // [nz] measures
         double* io = me + nz;        // [nz + 1] iota
@@ -382,10 +479,12 @@ __global__ void __launch_bounds__(32) thomas_kernel(Geo g, cplx<R>* S, cplx<doub
         for (int k = lane; k < nz; k += 32) S[k * sk] = cmk<R>(R(ph[k] - sh), R(0));
         return;
     }
-    // the diagonals' per-level coefficients, staged once
-    double* s_lo = cp + 32 * nz;
+    double* cring = after;                              // CPG: [D][32] c' ring
+    double* cp = after;                                 // shared c': [nz][32]
+    double* s_lo = CPG ? after + D * 32 : after + 32 * nz;
     double* s_up = s_lo + nz;
     double* s_hw = s_up + nz;
+    // the diagonals' per-level coefficients, staged once
     for (int k = lane; k < nz; k += 32) {
         s_lo[k] = c.lower[k];
         s_up[k] = c.upper[k];
@@ -396,7 +495,6 @@ __global__ void __launch_bounds__(32) thomas_kernel(Geo g, cplx<R>* S, cplx<doub
     if (col == 0 || col >= sk) return;
     const int p = (int)(col % Mh), j = (int)(col / Mh);
     const double lam = c.kx2[p] + c.ky2[j];
-    constexpr int D = THOMAS_PF;
     // forward elimination: level k waits in slot k % D; the copy of level
     // k + D - 1 goes to the slot read one level earlier
     cplx<R>* rs = reinterpret_cast<cplx<R>*>(ring);   // this lane's entries at [slot * 32 + lane]
@@ -417,29 +515,36 @@ __global__ void __launch_bounds__(32) thomas_kernel(Geo g, cplx<R>* S, cplx<doub
         const double den = b - lo * cprev;
         const double id = 1.0 / den;
         cprev = up * id;
-        cp[k * 32 + lane] = cprev;
         dr = ((double)s.x - lo * dr) * id;   // lo = 0 at k = 0
         di = ((double)s.y - lo * di) * id;
-        if (k < nz - 1) dsc[col + (long long)k * sk] = cmk<double>(dr, di);
+        if (k < nz - 1) {
+            if (CPG) cpg[col + (long long)k * sk] = cprev;
+            else cp[k * 32 + lane] = cprev;
+            dsc[col + (long long)k * sk] = cmk<double>(dr, di);
+        }
     }
     thomas_wait<0>();
     S[col + (long long)(nz - 1) * sk] = cmk<R>(R(dr), R(di));
-    // back substitution over k = nz-2 .. 0, the d' values streamed alike
-    // (slot t holds level nz-2-t modulo D)
+    // back substitution over k = nz-2 .. 0, the d' (and c') values streamed
+    // alike (slot t holds level nz-2-t modulo D)
+    auto fetch = [&](int slot, int k) {
+        thomas_cp16(ring + slot * 32 + lane, dsc + col + (long long)k * sk);
+        if (CPG) thomas_cp8(cring + slot * 32 + lane, cpg + col + (long long)k * sk);
+    };
 #pragma unroll
     for (int q = 0; q < D - 1; ++q) {
         const int k = nz - 2 - q;
-        if (k >= 0) thomas_cp16(ring + q * 32 + lane, dsc + col + (long long)k * sk);
+        if (k >= 0) fetch(q, k);
         thomas_commit();
     }
     for (int t = 0; t <= nz - 2; ++t) {
         const int k = nz - 2 - t;
         const int tn = t + D - 1, kn = nz - 2 - tn;
-        if (kn >= 0) thomas_cp16(ring + (tn % D) * 32 + lane, dsc + col + (long long)kn * sk);
+        if (kn >= 0) fetch(tn % D, kn);
         thomas_commit();
         thomas_wait<D - 1>();
         const cplx<double> d = ring[(t % D) * 32 + lane];
-        const double cc = cp[k * 32 + lane];
+        const double cc = CPG ? cring[(t % D) * 32 + lane] : cp[k * 32 + lane];
         dr = d.x - cc * dr;
         di = d.y - cc * di;
         S[col + (long long)k * sk] = cmk<R>(R(dr), R(di));
@@ -447,34 +552,34 @@ __global__ void __launch_bounds__(32) thomas_kernel(Geo g, cplx<R>* S, cplx<doub
     thomas_wait<0>();
 }
 
-// r2c of an interior source along x: pack pairs, FFT, post-process (the
-// div_fftx kernel body with the source read directly).
+// r2c of an interior source along x: pack pairs, FFT, post-process.
 template <typename R>
-__global__ void __launch_bounds__(256) src_fftx_kernel(Geo g, const R* __restrict__ src, cplx<R>* __restrict__ S,
+__global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) src_fftx_kernel(Geo g, const R* __restrict__ src, cplx<R>* __restrict__ S,
                                                        const cplx<R>* __restrict__ tw, int NT, int rows) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<R>* buf = reinterpret_cast<cplx<R>*>(smem_raw);
-    const int M = g.nx / 2, Mh = M + 1, lM = __ffs(M) - 1;
+    const int M = g.nx / 2, Mh = M + 1, lM = __ffs(M) - 1, LS = xrow(M);
     const long long nrows = (long long)g.ny * g.nz;
     const long long row0 = (long long)blockIdx.x * rows;
     const int tid = threadIdx.x, nthr = blockDim.x;
+#pragma unroll 16
     for (int e = tid; e < (rows << lM); e += nthr) {
         const int r = e >> lM, n = e & (M - 1);
         const long long row = row0 + r;
         cplx<R> z = cmk<R>(R(0), R(0));
         if (row < nrows) z = cmk<R>(src[row * g.nx + 2 * n], src[row * g.nx + 2 * n + 1]);
-        buf[e] = z;
+        buf[r * LS + sk16<true>(n)] = z;
     }
     __syncthreads();
-    smem_fft<R, false, false, FFT_KB>(buf, lM, __ffs(rows) - 1, M, 1, tw, NT);
+    smem_fft<R, false, false>(buf, lM, __ffs(rows) - 1, LS, 1, tw, NT);
     const int tstep = NT / g.nx;
     for (int e = tid; e < (rows << lM); e += nthr) {
         const int r = e >> lM, kk = e & (M - 1);
         const long long row = row0 + r;
-        if (row < nrows) S[row * Mh + kk] = r2c_bin(buf + r * M, M, kk, tw[(kk * tstep) & (NT - 1)]);
+        if (row < nrows) S[row * Mh + kk] = r2c_bin(buf + r * LS, M, kk, tw[(kk * tstep) & (NT - 1)]);
     }
-    for (int r = tid; r < rows; r += nthr) {   // the Nyquist bin
+    for (int r = tid; r < rows; r += nthr) {   // the Nyquist bin, twiddle exactly -1
         const long long row = row0 + r;
-        if (row < nrows) S[row * Mh + M] = r2c_bin(buf + r * M, M, M, tw[(M * tstep) & (NT - 1)]);
+        if (row < nrows) S[row * Mh + M] = r2c_bin(buf + r * LS, M, M, cmk<R>(R(-1), R(0)));
     }
 }

@@ -79,7 +79,7 @@ __global__ void iso_modes_kernel(Geo g, cplx<R>* __restrict__ S, IsoParams p) {
 
 // inverse complex transform along z of the spectrum (the field generator's z pass)
 template <typename R>
-__global__ void __launch_bounds__(256) fftz_inv_kernel(Geo g, cplx<R>* __restrict__ S, const cplx<R>* __restrict__ tw,
+__global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) fftz_inv_kernel(Geo g, cplx<R>* __restrict__ S, const cplx<R>* __restrict__ tw,
                                                        int NT, int tpx) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<R>* buf = reinterpret_cast<cplx<R>*>(smem_raw);
@@ -88,12 +88,13 @@ __global__ void __launch_bounds__(256) fftz_inv_kernel(Geo g, cplx<R>* __restric
     const long long sk = (long long)g.ny * Mh;
     const long long base = (long long)j * Mh;
     const int lt = __ffs(tpx) - 1;
+#pragma unroll 16
     for (int e = threadIdx.x; e < g.nz * tpx; e += blockDim.x) {
         const int kz = e >> lt, c = e & (tpx - 1), p = p0 + c;
         buf[e] = p < Mh ? S[base + kz * sk + p] : cmk<R>(R(0), R(0));
     }
     __syncthreads();
-    smem_fft<R, true, true, FFT_KB>(buf, __ffs(g.nz) - 1, __ffs(tpx) - 1, 1, tpx, tw, NT);
+    smem_fft<R, true, true>(buf, __ffs(g.nz) - 1, __ffs(tpx) - 1, 1, tpx, tw, NT);
     for (int e = threadIdx.x; e < g.nz * tpx; e += blockDim.x) {
         const int kz = e >> lt, c = e & (tpx - 1), p = p0 + c;
         if (p < Mh) S[base + kz * sk + p] = buf[e];

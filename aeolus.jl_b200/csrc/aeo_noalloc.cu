@@ -160,22 +160,22 @@ extern "C" aeo_status aeo_pressure_solve_column_noalloc(int32_t nx, int32_t ny, 
     const int rows = 2048 / M > 1 ? 2048 / M : 1;
     const int tpx = 2048 / ny > 16 ? 16 : (2048 / ny > 1 ? 2048 / ny : 1);
     unsigned gx = (unsigned)(((long long)ny * nz + rows - 1) / rows);
-    size_t smx = (size_t)rows * M * sizeof(cplx<double>);
+    size_t smx = (size_t)rows * xrow(M) * sizeof(cplx<double>);
     dim3 gy((Mh + tpx - 1) / tpx, nz);
     size_t smy = (size_t)tpx * ny * sizeof(cplx<double>);
-    size_t smt = thomas_smem(g);
+    size_t smt = thomas_smem(g, false);
     if (smt > 48 * 1024) {
-        e = cudaFuncSetAttribute(thomas_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
+        e = cudaFuncSetAttribute(thomas_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
         if (e != cudaSuccess) {
             aeo_set_global_error(std::string("pressure_solve_column_noalloc: ") + cudaGetErrorString(e));
             return AEO_ERR_CUDA;
         }
     }
-    src_fftx_kernel<double><<<gx, 256, smx, st>>>(g, src, S, tw, NT, rows);
-    ffty_kernel<double, 0><<<gy, 256, smy, st>>>(g, S, tw, NT, tpx);
-    thomas_kernel<double><<<thomas_blocks(g), 32, smt, st>>>(g, S, S, cc);
-    ffty_kernel<double, 1><<<gy, 256, smy, st>>>(g, S, tw, NT, tpx);
-    ifftx_kernel<double><<<gx, 256, smx, st>>>(g, S, phi, tw, NT, rows, 1.0 / ((double)nx * ny));
+    src_fftx_kernel<double><<<gx, FFT_THREADS(double), smx, st>>>(g, src, S, tw, NT, rows);
+    ffty_kernel<double, 0><<<gy, FFT_THREADS(double), smy, st>>>(g, S, tw, NT, tpx);
+    thomas_kernel<double, false><<<thomas_blocks(g), 32, smt, st>>>(g, S, S, nullptr, cc);
+    ffty_kernel<double, 1><<<gy, FFT_THREADS(double), smy, st>>>(g, S, tw, NT, tpx);
+    ifftx_kernel<double><<<gx, FFT_THREADS(double), smx, st>>>(g, S, phi, tw, NT, rows, 1.0 / ((double)nx * ny));
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {

@@ -3,7 +3,7 @@
 //
 // One substage (src/Simulations.jl:531-650; src/Anelastic.jl:1791-1876):
 //   sweep           tendencies (in-tile Smagorinsky) + predictor u* + theta
-//   div_fftx        divergence of u* fused with the r2c transform along x
+//   div, src_fftx   divergence of u* (into phi's storage), r2c transform along x
 //   ffty            forward transform along y
 //   fftz_solve      periodic z: forward, 1/lambda, inverse   | thomas: walls in z
 //   ffty            inverse along y
@@ -115,6 +115,7 @@ struct Core : CoreBase {
     R* pres = nullptr;         // interior
     cplx<R>* S = nullptr;      // spectrum
     cplx<double>* dsc = nullptr;
+    double* cps = nullptr;     // the column solve's c' scratch (spectrum layout)
     cplx<R>* tw = nullptr;
     int NT = 0;
     double* d_stage = nullptr; // host-layout staging (device)
@@ -378,6 +379,7 @@ struct Core : CoreBase {
         if (c.solver == AEO_SOLVER_COLUMN) {
             if (sizeof(R) == sizeof(double)) dsc = reinterpret_cast<cplx<double>*>(S);
             else if (aeo_status e = alloc(&dsc, ns)) return e;
+            if (aeo_status e = alloc(&cps, ns)) return e;
         }
         host_n = (long long)(c.nx + 2 * c.hx) * (c.ny + 2 * c.hy) * (c.nz + 2 * c.hz);
         if (aeo_status e = alloc(&d_stage, std::max<long long>(host_n, g.nin))) return e;
@@ -389,7 +391,7 @@ struct Core : CoreBase {
         if (aeo_status e = make_tensor_maps()) return e;
         kchunk = std::min(g.nz, 32);
         CK(cudaStreamSynchronize(st));
-        launches = 3 * 8;
+        launches = 3 * 9;
         return AEO_OK;
     }
 
@@ -461,43 +463,46 @@ struct Core : CoreBase {
     // The pressure solve from the source (src == nullptr: divergence of Q) into phi.
     aeo_status solve(const R* src) {
         const int M = g.nx / 2;
-        size_t smx = (size_t)rows_x * M * sizeof(cplx<R>);
+        size_t smx = (size_t)rows_x * xrow(M) * sizeof(cplx<R>);
         unsigned gx = (unsigned)((g.ny * (long long)g.nz + rows_x - 1) / rows_x);
         if (src) {
-            src_fftx_kernel<R><<<gx, 256, smx, st>>>(g, src, S, tw, NT, rows_x);
-        } else if (anel) {
-            if (uni) div_fftx_kernel<R, true, true><<<gx, 256, smx, st>>>(g, Q[0], Q[1], Q[2], S, tw, NT, rows_x);
-            else div_fftx_kernel<R, true, false><<<gx, 256, smx, st>>>(g, Q[0], Q[1], Q[2], S, tw, NT, rows_x);
+            src_fftx_kernel<R><<<gx, FFT_THREADS(R), smx, st>>>(g, src, S, tw, NT, rows_x);
         } else {
-            if (uni) div_fftx_kernel<R, false, true><<<gx, 256, smx, st>>>(g, Q[0], Q[1], Q[2], S, tw, NT, rows_x);
-            else div_fftx_kernel<R, false, false><<<gx, 256, smx, st>>>(g, Q[0], Q[1], Q[2], S, tw, NT, rows_x);
+            // the divergence into phi (overwritten by the c2r at the end), then its r2c
+            const unsigned gd = (unsigned)((g.nin + 255) / 256);
+            if (anel && uni) div_kernel<R, true, true><<<gd, 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi);
+            else if (anel) div_kernel<R, true, false><<<gd, 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi);
+            else if (uni) div_kernel<R, false, true><<<gd, 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi);
+            else div_kernel<R, false, false><<<gd, 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi);
+            CKL();
+            src_fftx_kernel<R><<<gx, FFT_THREADS(R), smx, st>>>(g, phi, S, tw, NT, rows_x);
         }
         CKL();
         mark(AEO_K_DIV_FFTX);
         const int Mh = M + 1;
         dim3 gy((Mh + tpx_y - 1) / tpx_y, g.nz);
         size_t smy = (size_t)tpx_y * g.ny * sizeof(cplx<R>);
-        ffty_kernel<R, 0><<<gy, 256, smy, st>>>(g, S, tw, NT, tpx_y);
+        ffty_kernel<R, 0><<<gy, FFT_THREADS(R), smy, st>>>(g, S, tw, NT, tpx_y);
         CKL();
         mark(AEO_K_FFTY);
         if (cfg.solver == AEO_SOLVER_FFT) {
             dim3 gz((Mh + tpx_z - 1) / tpx_z, g.ny);
             size_t smz = (size_t)tpx_z * g.nz * sizeof(cplx<R>);
             double nrm = 1.0 / ((double)g.nx * g.ny * g.nz);
-            fftz_solve_kernel<R><<<gz, 256, smz, st>>>(g, S, tw, NT, tpx_z, kx2, ky2, kz2, nrm);
+            fftz_solve_kernel<R><<<gz, FFT_THREADS(R), smz, st>>>(g, S, tw, NT, tpx_z, kx2, ky2, kz2, nrm);
         } else {
-            size_t smt = thomas_smem(g);
+            size_t smt = thomas_smem(g, true);
             if (smt > 48 * 1024)
-                cudaFuncSetAttribute(thomas_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
-            thomas_kernel<R><<<thomas_blocks(g), 32, smt, st>>>(g, S, dsc, cc);
+                cudaFuncSetAttribute(thomas_kernel<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
+            thomas_kernel<R, true><<<thomas_blocks(g), 32, smt, st>>>(g, S, dsc, cps, cc);
         }
         CKL();
         mark(AEO_K_ZSOLVE);
-        ffty_kernel<R, 1><<<gy, 256, smy, st>>>(g, S, tw, NT, tpx_y);
+        ffty_kernel<R, 1><<<gy, FFT_THREADS(R), smy, st>>>(g, S, tw, NT, tpx_y);
         CKL();
         mark(AEO_K_FFTY);
         R scale = cfg.solver == AEO_SOLVER_FFT ? R(1) : R(1.0 / ((double)g.nx * g.ny));
-        ifftx_kernel<R><<<gx, 256, smx, st>>>(g, S, phi, tw, NT, rows_x, scale);
+        ifftx_kernel<R><<<gx, FFT_THREADS(R), smx, st>>>(g, S, phi, tw, NT, rows_x, scale);
         CKL();
         mark(AEO_K_IFFTX);
         return AEO_OK;
@@ -878,7 +883,7 @@ struct Core : CoreBase {
         size_t smy = (size_t)tpx_y * g.ny * sizeof(cplx<R>);
         dim3 gz((Mh + tpx_z - 1) / tpx_z, g.ny);
         size_t smz = (size_t)tpx_z * g.nz * sizeof(cplx<R>);
-        size_t smx = (size_t)rows_x * M * sizeof(cplx<R>);
+        size_t smx = (size_t)rows_x * xrow(M) * sizeof(cplx<R>);
         unsigned gx = (unsigned)((g.ny * (long long)g.nz + rows_x - 1) / rows_x);
         dim3 gb((g.nx + 127) / 128, g.ny, g.nz);
         for (int comp = 0; comp < 3; ++comp) {
@@ -892,11 +897,11 @@ struct Core : CoreBase {
             p.comp = comp;
             iso_modes_kernel<R><<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(g, S, p);
             CKL();
-            fftz_inv_kernel<R><<<gz, 256, smz, st>>>(g, S, tw, NT, tpx_z);
+            fftz_inv_kernel<R><<<gz, FFT_THREADS(R), smz, st>>>(g, S, tw, NT, tpx_z);
             CKL();
-            ffty_kernel<R, 1><<<gy, 256, smy, st>>>(g, S, tw, NT, tpx_y);
+            ffty_kernel<R, 1><<<gy, FFT_THREADS(R), smy, st>>>(g, S, tw, NT, tpx_y);
             CKL();
-            ifftx_kernel<R><<<gx, 256, smx, st>>>(g, S, phi, tw, NT, rows_x, R(1));
+            ifftx_kernel<R><<<gx, FFT_THREADS(R), smx, st>>>(g, S, phi, tw, NT, rows_x, R(1));
             CKL();
             interior_to_padded_kernel<R><<<gb, 128, 0, st>>>(g, phi, P[cur][comp], R(1));
             CKL();

@@ -138,7 +138,7 @@ def class_passes(cls, g, sgs):
     return {
         "sweep": (8 + 9 + 9) / 3.0,            # R u,v,w,theta (+theta0); W u*,v*,w*,theta
         "sgs": 4.0,                           # R u,v,w; W nut
-        "div_fftx": 3.0 + sp,                 # R u*,v*,w*; W spectrum
+        "div_fftx": 3.0 + sp,                 # R u*,v*,w*; W spectrum (the divergence + r2c pair)
         "ffty": 2.0 * sp,                     # R+W spectrum
         "zsolve": 2.0 * sp,                   # R+W spectrum
         "ifftx": sp + 1.0,                    # R spectrum; W phi
