@@ -178,4 +178,26 @@ struct Met {
     __device__ __forceinline__ R spf(int k) const { return lv(LV_SPF, k); }
 };
 
+// N = 16 / sizeof(R) consecutive values as one 16-byte access (the caller
+// guarantees 16-byte alignment: an x-offset that is a multiple of N in an
+// array whose rows hold a multiple of N values).
+template <typename R>
+struct Vec16 {
+    static constexpr int N = 16 / (int)sizeof(R);
+};
+__device__ __forceinline__ void vld(const float* p, float (&v)[4]) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void vld(const double* p, double (&v)[2]) {
+    const double2 t = *reinterpret_cast<const double2*>(p);
+    v[0] = t.x; v[1] = t.y;
+}
+__device__ __forceinline__ void vst(float* p, const float (&v)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void vst(double* p, const double (&v)[2]) {
+    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+}
+
 #define AEO_CHECK_LAUNCH() ((void)0)

@@ -189,22 +189,51 @@ __device__ __forceinline__ void smem_fft(cplx<R>* buf, int logn, int lognl, int 
     }
 }
 
-// ---- divergence + r2c along x --------------------------------------------------
-// The neighbours i+1, j+1, k+1 are plain loads inside the domain; only the
-// last cell of a row, column or level goes through the boundary map.
+// ---- divergence ------------------------------------------------------------------
+// The divergence of the predicted velocity (the source of the pressure solve)
+// for N = 16/sizeof(R) x-consecutive cells per thread, 16-byte loads and
+// stores.  The east, north and top neighbours follow the boundary maps:
+// periodic x and y, and in z periodic or the zero wall face.
 template <typename R, bool ANEL, bool UNI>
-__device__ __forceinline__ R div_point(const Geo& g, const Met<R, UNI>& m, const R* __restrict__ us,
-                                       const R* __restrict__ vs, const R* __restrict__ ws, int i, int j, int k) {
-    const long long q = iidx(g, i, j, k);
-    const R up = i + 1 < g.nx ? __ldg(us + q + 1) : ld_mapped_interior(g, us, i + 1, j, k, LOC_FX);
-    const R vp = j + 1 < g.ny ? __ldg(vs + q + g.nx) : ld_mapped_interior(g, vs, i, j + 1, k, LOC_FY);
-    const R wp = k + 1 < g.nz ? __ldg(ws + q + (long long)g.nx * g.ny) : ld_mapped_interior(g, ws, i, j, k + 1, LOC_FZ);
-    const R idz = m.idz(k);
-    if (ANEL) {
-        const R wc = m.wc(k), wfb = m.wf(k), wft = m.wf(k + 1);
-        return wc * ((up - __ldg(us + q)) * R(g.idx) + (vp - __ldg(vs + q)) * R(g.idy)) + (wft * wp - wfb * __ldg(ws + q)) * idz;
+__global__ void __launch_bounds__(256) div_kernel(Geo g, const R* __restrict__ us, const R* __restrict__ vs,
+                                                  const R* __restrict__ ws, R* __restrict__ out) {
+    constexpr int N = Vec16<R>::N;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.nin / N) return;
+    const long long q = t * N;
+    const int lnx = __ffs(g.nx) - 1, lny = __ffs(g.ny) - 1;
+    const int i0 = (int)(q & (g.nx - 1)), j = (int)((q >> lnx) & (g.ny - 1)), k = (int)(q >> (lnx + lny));
+    const long long pl = (long long)g.nx * g.ny;
+    const Met<R, UNI> m(g);
+    R uc[N], vc[N], wc[N], vn[N], wn[N];
+    vld(us + q, uc);
+    const R ue = __ldg(us + (i0 + N < g.nx ? q + N : q + N - g.nx));
+    vld(vs + q, vc);
+    vld(vs + (j + 1 < g.ny ? q + g.nx : q - (long long)(g.ny - 1) * g.nx), vn);
+    vld(ws + q, wc);
+    if (k + 1 < g.nz) vld(ws + q + pl, wn);
+    else if (g.bc_z == 0) vld(ws + q - (long long)(g.nz - 1) * pl, wn);
+    else {
+#pragma unroll
+        for (int n = 0; n < N; ++n) wn[n] = R(0);   // the top wall face
     }
-    return (up - __ldg(us + q)) * R(g.idx) + (vp - __ldg(vs + q)) * R(g.idy) + (wp - __ldg(ws + q)) * idz;
+    const R idx = R(g.idx), idy = R(g.idy), idz = m.idz(k);
+    R d[N];
+    if (ANEL) {
+        const R wcv = m.wc(k), wfb = m.wf(k), wft = m.wf(k + 1);
+#pragma unroll
+        for (int n = 0; n < N; ++n) {
+            const R up = n + 1 < N ? uc[n + 1] : ue;
+            d[n] = wcv * ((up - uc[n]) * idx + (vn[n] - vc[n]) * idy) + (wft * wn[n] - wfb * wc[n]) * idz;
+        }
+    } else {
+#pragma unroll
+        for (int n = 0; n < N; ++n) {
+            const R up = n + 1 < N ? uc[n + 1] : ue;
+            d[n] = (up - uc[n]) * idx + (vn[n] - vc[n]) * idy + (wn[n] - wc[n]) * idz;
+        }
+    }
+    vst(out + q, d);
 }
 
 // The r2c post-process of bin kk from the packed M-point transform of one row.
@@ -215,18 +244,6 @@ __device__ __forceinline__ cplx<R> r2c_bin(const cplx<R>* rowbuf, int M, int kk,
     const R er = R(0.5) * (a.x + b.x), ei = R(0.5) * (a.y - b.y);
     const R orr = R(0.5) * (a.y + b.y), oi = R(-0.5) * (a.x - b.x);
     return cmk<R>(er + (wv.x * orr - wv.y * oi), ei + (wv.x * oi + wv.y * orr));
-}
-
-// The divergence of the predicted velocity at every interior cell (the
-// source of the pressure solve), one cell per thread; src_fftx transforms it.
-template <typename R, bool ANEL, bool UNI>
-__global__ void __launch_bounds__(256) div_kernel(Geo g, const R* __restrict__ us, const R* __restrict__ vs,
-                                                  const R* __restrict__ ws, R* __restrict__ out) {
-    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= g.nin) return;
-    const int lnx = __ffs(g.nx) - 1, lny = __ffs(g.ny) - 1;
-    const int i = (int)(q & (g.nx - 1)), j = (int)((q >> lnx) & (g.ny - 1)), k = (int)(q >> (lnx + lny));
-    out[q] = div_point<R, ANEL, UNI>(g, Met<R, UNI>(g), us, vs, ws, i, j, k);
 }
 
 // ---- c2r along x into phi ---------------------------------------------------------

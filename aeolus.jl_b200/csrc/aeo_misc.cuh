@@ -76,6 +76,9 @@ __global__ void wall_face_zero_kernel(Geo g, R* w) {
 // ---- the projection's correction (src/FiniteVolume.jl:1823-1849) ---------------
 // u = c(u* - d(phi)/dx, u0) (likewise v, w), p = phi/dt; c(x, s) = ca*s + cb*x
 // in RK3 stages 2 and 3 (_Lin2r, src/Simulations.jl:1194-1198).
+// N = 16/sizeof(R) x-consecutive cells per thread, 16-byte loads and stores;
+// the west, south and bottom neighbours of phi follow the centred-field
+// maps: periodic x and y, in z periodic or the wall mirror.
 template <typename R, bool UNI>
 __global__ void __launch_bounds__(256) correct_kernel(Geo g, const R* __restrict__ us, const R* __restrict__ vs,
                                                       const R* __restrict__ ws, const R* __restrict__ phi,
@@ -83,28 +86,51 @@ __global__ void __launch_bounds__(256) correct_kernel(Geo g, const R* __restrict
                                                       const R* w0, R* uo, R* vo,
                                                       R* wo, R* __restrict__ p, const double* __restrict__ dtp, R ca, R cb,
                                                       int stage) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int j = blockIdx.y * blockDim.y + threadIdx.y;
-    int k = blockIdx.z * blockDim.z + threadIdx.z;
-    if (i >= g.nx || j >= g.ny || k >= g.nz) return;
-    const long long qi = iidx(g, i, j, k), qp = pidx(g, i, j, k);
-    R pc = __ldg(phi + qi);
-    R pw = ld_mapped_interior(g, phi, i - 1, j, k, LOC_C);
-    R ps = ld_mapped_interior(g, phi, i, j - 1, k, LOC_C);
-    R pb = ld_mapped_interior(g, phi, i, j, k - 1, LOC_C);
-    R idzf = UNI ? R(g.idz) : R(lvl(g.idzf, k));
-    R un = __ldg(us + qi) - (pc - pw) * R(g.idx);
-    R vn = __ldg(vs + qi) - (pc - ps) * R(g.idy);
-    R wn = __ldg(ws + qi) - (pc - pb) * idzf;
-    if (stage) {
-        un = ca * u0[qp] + cb * un;
-        vn = ca * v0[qp] + cb * vn;
-        wn = ca * w0[qp] + cb * wn;
+    constexpr int N = Vec16<R>::N;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.nin / N) return;
+    const long long qi = t * N;
+    const int lnx = __ffs(g.nx) - 1, lny = __ffs(g.ny) - 1;
+    const int i0 = (int)(qi & (g.nx - 1)), j = (int)((qi >> lnx) & (g.ny - 1)), k = (int)(qi >> (lnx + lny));
+    const long long qp = pidx(g, i0, j, k), pl = (long long)g.nx * g.ny;
+    R pc[N], ps[N], pb[N];
+    vld(phi + qi, pc);
+    const R pwl = __ldg(phi + (i0 > 0 ? qi - 1 : qi + g.nx - 1));
+    vld(phi + (j > 0 ? qi - g.nx : qi + (long long)(g.ny - 1) * g.nx), ps);
+    // k - 1 = -1: periodic wrap, or the wall mirror (level 0 itself)
+    vld(phi + (k > 0 ? qi - pl : (g.bc_z == 0 ? qi + (long long)(g.nz - 1) * pl : qi)), pb);
+    const R idzf = UNI ? R(g.idz) : Met<R, UNI>(g).idzf(k);
+    R uc[N], vc[N], wc[N];
+    vld(us + qi, uc);
+    vld(vs + qi, vc);
+    vld(ws + qi, wc);
+    R un[N], vn[N], wn[N];
+#pragma unroll
+    for (int n = 0; n < N; ++n) {
+        const R pw = n > 0 ? pc[n - 1] : pwl;
+        un[n] = uc[n] - (pc[n] - pw) * R(g.idx);
+        vn[n] = vc[n] - (pc[n] - ps[n]) * R(g.idy);
+        wn[n] = wc[n] - (pc[n] - pb[n]) * idzf;
     }
-    uo[qp] = un;
-    vo[qp] = vn;
-    wo[qp] = wn;
-    p[qi] = pc / R(__ldg(dtp));  // p = phi/dt (_DivBy, src/Simulations.jl:1207-1211)
+    if (stage) {
+        R a0[N];
+        vld(u0 + qp, a0);
+#pragma unroll
+        for (int n = 0; n < N; ++n) un[n] = ca * a0[n] + cb * un[n];
+        vld(v0 + qp, a0);
+#pragma unroll
+        for (int n = 0; n < N; ++n) vn[n] = ca * a0[n] + cb * vn[n];
+        vld(w0 + qp, a0);
+#pragma unroll
+        for (int n = 0; n < N; ++n) wn[n] = ca * a0[n] + cb * wn[n];
+    }
+    vst(uo + qp, un);
+    vst(vo + qp, vn);
+    vst(wo + qp, wn);
+    const R dt = R(__ldg(dtp));
+#pragma unroll
+    for (int n = 0; n < N; ++n) pc[n] = pc[n] / dt;   // p = phi/dt (_DivBy, src/Simulations.jl:1207-1211)
+    vst(p + qi, pc);
 }
 
 // ---- host-layout packing ----------------------------------------------------------

@@ -422,6 +422,8 @@ struct Core : CoreBase {
     // ---- launch helpers -------------------------------------------------------------
     dim3 blk3() const { return dim3(32, 4, 2); }
     dim3 grd3() const { return dim3((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + 1) / 2); }
+    // 256-thread blocks over the interior, 16 / sizeof(R) x-consecutive cells a thread
+    unsigned gvec() const { return (unsigned)((g.nin / Vec16<R>::N + 255) / 256); }
 
     aeo_status halo(R* const* f, const int* loc, int nf) {
         HaloSet<R> hs{};
@@ -469,11 +471,10 @@ struct Core : CoreBase {
             src_fftx_kernel<R><<<gx, FFT_THREADS(R), smx, st>>>(g, src, S, tw, NT, rows_x);
         } else {
             // the divergence into phi (overwritten by the c2r at the end), then its r2c
-            const unsigned gd = (unsigned)((g.nin + 255) / 256);
-            if (anel && uni) div_kernel<R, true, true><<<gd, 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi);
-            else if (anel) div_kernel<R, true, false><<<gd, 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi);
-            else if (uni) div_kernel<R, false, true><<<gd, 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi);
-            else div_kernel<R, false, false><<<gd, 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi);
+            if (anel && uni) div_kernel<R, true, true><<<gvec(), 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi);
+            else if (anel) div_kernel<R, true, false><<<gvec(), 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi);
+            else if (uni) div_kernel<R, false, true><<<gvec(), 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi);
+            else div_kernel<R, false, false><<<gvec(), 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi);
             CKL();
             src_fftx_kernel<R><<<gx, FFT_THREADS(R), smx, st>>>(g, phi, S, tw, NT, rows_x);
         }
@@ -511,10 +512,10 @@ struct Core : CoreBase {
     aeo_status correct(R** out, int stage, R ca, R cb, const double* dtp, int s_u0) {
         R** u0 = P[s_u0];
         if (uni)
-            correct_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, Q[0], Q[1], Q[2], phi, u0[0], u0[1], u0[2], out[0],
+            correct_kernel<R, true><<<gvec(), 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi, u0[0], u0[1], u0[2], out[0],
                                                                out[1], out[2], pres, dtp, ca, cb, stage);
         else
-            correct_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, Q[0], Q[1], Q[2], phi, u0[0], u0[1], u0[2], out[0],
+            correct_kernel<R, false><<<gvec(), 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi, u0[0], u0[1], u0[2], out[0],
                                                                 out[1], out[2], pres, dtp, ca, cb, stage);
         CKL();
         return AEO_OK;
