@@ -59,8 +59,11 @@ struct TileShape {
     static constexpr int ZL = ADV ? 3 : (SGS ? 2 : 1);   // levels below the point
     static constexpr int ZH = ADV ? 3 : (SGS ? 2 : 1);   // levels above
     static constexpr int NW = ZL + ZH + 1;
-    static constexpr int LOOK = 1;                       // levels loaded ahead
-    static constexpr int NS = NW + LOOK;                 // ring slots
+    // ring slots: FP32 rounds the window + 1 up to a power of two (slot
+    // arithmetic is a mask; the extra slots load further ahead), FP64 keeps
+    // window + 1 so that two CTAs fit an SM
+    static constexpr int NS = sizeof(R) == 8 ? NW + 1 : (NW + 1 <= 4 ? 4 : (NW + 1 <= 8 ? 8 : 16));
+    static constexpr int LOOK = NS - NW;                 // levels loaded ahead
     static constexpr int PW = TX + 8;                    // row: x from i0-4 (16-byte aligned TMA start)
     static constexpr int PH = TY + 2 * HH;
     static constexpr int PSZ = PW * PH;                  // elements of one field-plane (the TMA box)
@@ -70,10 +73,11 @@ struct TileShape {
     static constexpr size_t NUT_BYTES = SGS ? (((size_t)3 * NPS * sizeof(R) + 127) / 128) * 128 : 0;
     static constexpr size_t BAR_BYTES = 128;
     static_assert(NS * 8 <= (int)BAR_BYTES, "mbarrier block");
-    // + the chunk's per-level factors, LV_N rows of (kchunk + 2 AEO_LH), + alignment slack
-    static size_t smem(int kchunk) {
-        return PLANES_BYTES + NUT_BYTES + BAR_BYTES + (size_t)LV_N * (kchunk + 2 * AEO_LH) * sizeof(R) + 128;
-    }
+    static_assert(TX == 32 && NPS == TX * NPH + 2 * NPH, "the eddy-viscosity loop maps warps to 32-column rows");
+    // + the chunk's per-level factors, LV_N rows of NLT (a chunk has at most
+    // KCH levels), + alignment slack
+    static constexpr int KCH = 32, NLT = KCH + 2 * AEO_LH;
+    static constexpr size_t SMEM = PLANES_BYTES + NUT_BYTES + BAR_BYTES + (size_t)LV_N * NLT * sizeof(R) + 128;
 };
 
 struct TileMaps {
@@ -137,17 +141,18 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
         for (int s = 0; s < S::NS; ++s) mbar_init(bars + s, 1);
         fence_mbar_init();
     }
-    // the chunk's per-level factors: level k of row f at lvs[f * nlt + k + AEO_LH - kbeg]
+    // the chunk's per-level factors: level k of row f at lvs[f * NLT + k + AEO_LH - kbeg]
+    // (a compile-time row stride: every factor is one ld.shared off the level's base)
     const int nlt = kend - kbeg + 2 * AEO_LH;
     {
         const R* src = static_cast<const R*>(g.lvr);
-        for (int e = tid; e < LV_N * nlt; e += S::NT) {
-            const int f = e / nlt, kk = e - f * nlt;
-            lvs[e] = src[(size_t)f * g.lvn + kbeg + kk];
+        for (int e = tid; e < LV_N * S::NLT; e += S::NT) {
+            const int f = e / S::NLT, kk = e - f * S::NLT;
+            if (kk < nlt) lvs[e] = src[(size_t)f * g.lvn + kbeg + kk];
         }
     }
     __syncthreads();
-    const Met<R, UNI> m(g, lvs, nlt, AEO_LH - kbeg);
+    const Met<R, UNI> m(g, lvs, S::NLT, AEO_LH - kbeg);
     int Lissued = min(Llast, kbeg + S::ZH + S::LOOK);
     if (tid == 0)
         for (int L = Lfirst; L <= Lissued; ++L) issue(L);
@@ -158,8 +163,11 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
     for (int k = kbeg; k < kend; ++k) {
         // the levels this iteration needs
         const int Lw0 = (k == kbeg) ? Lfirst : k + S::ZH;
+        // one warp polls the mbarriers; the CTA barrier then releases the
+        // others (it orders the copies the poll observed before their reads)
         bool ok = true;
-        for (int L = Lw0; L <= k + S::ZH; ++L) ok = ok && mbar_wait_bounded(bars + slot_of(L), parity_of(L));
+        if (tid < 32)
+            for (int L = Lw0; L <= k + S::ZH; ++L) ok = ok && mbar_wait_bounded(bars + slot_of(L), parity_of(L));
         if (__syncthreads_or(!ok)) { failed = true; break; }
         // every thread is past level k-1: the slot of level k-1-ZL takes level k+ZH+LOOK
         if (k > kbeg) {
@@ -189,14 +197,18 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
                 const R* sp[3];
 #pragma unroll
                 for (int d = 0; d < 3; ++d) sp[d] = plane(L - 1 + d);
+                // warps take whole rows of the tile's 32 columns (contiguous,
+                // conflict-free), the two edge columns come last
                 for (int e = tid; e < S::NPS; e += S::NT) {
-                    const int cj = e / S::NPW, ci = e - cj * S::NPW;
+                    int cj, ci;
+                    if (e < S::TX * S::NPH) { cj = e >> 5; ci = (e & 31) + 1; }
+                    else { const int x = e - S::TX * S::NPH; cj = x >> 1; ci = (x & 1) ? S::NPW - 1 : 0; }
                     const int b = (cj - 1 + S::HH) * S::PW + (ci - 1 + 4);
                     const R* q[3] = {sp[0] + b, sp[1] + b, sp[2] + b};
                     const SmAcc<R, 1, S::PW, 0> Uq{q};
                     const SmAcc<R, 1, S::PW, S::PSZA> Vq{q};
                     const SmAcc<R, 1, S::PW, 2 * S::PSZA> Wq{q};
-                    np[e] = smag_point<R, UNI>(m, g, L, R(a.c_s), Uq, Vq, Wq);
+                    np[cj * S::NPW + ci] = smag_point<R, UNI>(m, g, L, R(a.c_s), Uq, Vq, Wq);
                 }
             }
             __syncthreads();

@@ -389,7 +389,7 @@ struct Core : CoreBase {
         set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->one, 1.0);
         CKL();
         if (aeo_status e = make_tensor_maps()) return e;
-        kchunk = std::min(g.nz, 32);
+        kchunk = std::min(g.nz, TileShape<R, 0, false>::KCH);
         CK(cudaStreamSynchronize(st));
         launches = 3 * 9;
         return AEO_OK;
@@ -438,7 +438,7 @@ struct Core : CoreBase {
     template <int ADV, bool SG, bool AN, bool UN>
     void launch_sweep_t(int s_in, const SweepArgs<R>& a) {
         using TS = TileShape<R, ADV, SG>;
-        const size_t sm = TS::smem(kchunk);
+        const size_t sm = TS::SMEM;
         cudaFuncSetAttribute(sweep_tile_kernel<R, ADV, SG, AN, UN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         dim3 grid((g.nx + TS::TX - 1) / TS::TX, (g.ny + TS::TY - 1) / TS::TY, (g.nz + kchunk - 1) / kchunk);
         sweep_tile_kernel<R, ADV, SG, AN, UN><<<grid, dim3(TS::TX, TS::TY), sm, st>>>(tmaps[s_in], a, kchunk, d_flag);
