@@ -154,16 +154,26 @@ struct Met {
     __device__ __forceinline__ R idz(int k) const { return UNI ? R(g.idz) : lv(LV_IDZC, k); }
     __device__ __forceinline__ R idzf(int k) const { return UNI ? R(g.idz) : lv(LV_IDZF, k); }
     __device__ __forceinline__ R idz_off(int k) const { return UNI ? R(g.idz) : lv(LV_IDZOFF, k); }
-    __device__ __forceinline__ R zface(int k, R lo, R hi) const {
-        return UNI ? R(0.5) * (lo + hi) : lv(LV_WLO, k) * lo + lv(LV_WHI, k) * hi;
+    // the mixing helpers take the value type of the caller: R, or a pair of
+    // FP32 lanes (the factors broadcast)
+    template <typename V>
+    __device__ __forceinline__ V zface(int k, V lo, V hi) const {
+        if constexpr (UNI) return V(R(0.5)) * (lo + hi);
+        else return V(lv(LV_WLO, k)) * lo + V(lv(LV_WHI, k)) * hi;
     }
-    __device__ __forceinline__ R zflux(int k, R lo, R hi) const {
-        return UNI ? R(0.5) * (lo + hi) : lv(LV_ALO, k) * lo + lv(LV_AHI, k) * hi;
+    template <typename V>
+    __device__ __forceinline__ V zflux(int k, V lo, V hi) const {
+        if constexpr (UNI) return V(R(0.5)) * (lo + hi);
+        else return V(lv(LV_ALO, k)) * lo + V(lv(LV_AHI, k)) * hi;
     }
-    __device__ __forceinline__ R lapz(int loc, int k, R fm, R c, R fp) const {
-        if (UNI) return (fp - R(2) * c + fm) * R(g.idz2);
-        if (loc == LOC_FZ) return ((fp - c) * lv(LV_IDZC, k) - (c - fm) * lv(LV_IDZC, k - 1)) * lv(LV_IDZF, k);
-        return ((fp - c) * lv(LV_IDZF, k + 1) - (c - fm) * lv(LV_IDZF, k)) * lv(LV_IDZC, k);
+    template <typename V>
+    __device__ __forceinline__ V lapz(int loc, int k, V fm, V c, V fp) const {
+        if constexpr (UNI) {
+            return (fp - V(R(2)) * c + fm) * V(R(g.idz2));
+        } else {
+            if (loc == LOC_FZ) return ((fp - c) * V(lv(LV_IDZC, k)) - (c - fm) * V(lv(LV_IDZC, k - 1))) * V(lv(LV_IDZF, k));
+            return ((fp - c) * V(lv(LV_IDZF, k + 1)) - (c - fm) * V(lv(LV_IDZF, k))) * V(lv(LV_IDZC, k));
+        }
     }
     __device__ __forceinline__ R filter(int k) const { return UNI ? R(g.delta_u) : lv(LV_DELTA, k); }
     // sound-proof weights

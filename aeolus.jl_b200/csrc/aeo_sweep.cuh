@@ -107,223 +107,226 @@ __device__ __forceinline__ R face_z(const A& F, int di, int dj, int c, R vel) {
 // ---- the tendency at one point ------------------------------------------------
 // U, V, W, T, N are accessors (di, dj, dk) -> value around the point at level
 // k; the same arithmetic serves the direct form (global memory) and the
-// tiled form (shared-memory planes).
-template <typename R, int ADV, bool SGS, bool ANEL, bool UNI, class AU, class AV, class AW, class AT, class AN>
+// tiled form (shared-memory planes).  VT is the value type: R, or a pair of
+// FP32 lanes (F2) for two x-adjacent cells of the paired sweep (the
+// centred forms only).
+template <typename R, int ADV, bool SGS, bool ANEL, bool UNI, class AU, class AV, class AW, class AT, class AN,
+          typename VT>
 __device__ __forceinline__ void sweep_point(const Met<R, UNI>& m, const SweepArgs<R>& a, const Geo& g, int k,
-                                            const AU& U, const AV& V, const AW& W, const AT& T, const AN& N, R& tu,
-                                            R& tv, R& tw, R& tt) {
-    const R idx = R(g.idx), idy = R(g.idy), idx2 = R(g.idx2), idy2 = R(g.idy2);
-    const R h = R(0.5);
+                                            const AU& U, const AV& V, const AW& W, const AT& T, const AN& N, VT& tu,
+                                            VT& tv, VT& tw, VT& tt) {
+    const VT idx = VT(g.idx), idy = VT(g.idy), idx2 = VT(g.idx2), idy2 = VT(g.idy2);
+    const VT h = VT(0.5);
 
-    if (ANEL) {
+    if constexpr (ANEL) {
         // W-weighted centred forms (src/Anelastic.jl:1193-1306)
-        R iwc = m.iwc(k), wfb = m.wf(k), wft = m.wf(k + 1);
+        VT iwc = m.iwc(k), wfb = m.wf(k), wft = m.wf(k + 1);
         {
-            R uce = h * (U(0, 0, 0) + U(1, 0, 0)), ucw = h * (U(-1, 0, 0) + U(0, 0, 0));
-            R d_uu_dx = (uce * uce - ucw * ucw) * idx;
-            R vun = h * (V(-1, 1, 0) + V(0, 1, 0)), uvn = h * (U(0, 0, 0) + U(0, 1, 0));
-            R vus = h * (V(-1, 0, 0) + V(0, 0, 0)), uvs = h * (U(0, -1, 0) + U(0, 0, 0));
-            R d_vu_dy = (vun * uvn - vus * uvs) * idy;
-            R wut = h * (W(-1, 0, 1) + W(0, 0, 1)), uwt = h * (U(0, 0, 0) + U(0, 0, 1));
-            R wub = h * (W(-1, 0, 0) + W(0, 0, 0)), uwb = h * (U(0, 0, -1) + U(0, 0, 0));
-            R d_wu_dz = (wft * wut * uwt - wfb * wub * uwb) * m.idz(k) * iwc;
-            tu = R(0) - (d_uu_dx + d_vu_dy + d_wu_dz);
+            VT uce = h * (U(0, 0, 0) + U(1, 0, 0)), ucw = h * (U(-1, 0, 0) + U(0, 0, 0));
+            VT d_uu_dx = (uce * uce - ucw * ucw) * idx;
+            VT vun = h * (V(-1, 1, 0) + V(0, 1, 0)), uvn = h * (U(0, 0, 0) + U(0, 1, 0));
+            VT vus = h * (V(-1, 0, 0) + V(0, 0, 0)), uvs = h * (U(0, -1, 0) + U(0, 0, 0));
+            VT d_vu_dy = (vun * uvn - vus * uvs) * idy;
+            VT wut = h * (W(-1, 0, 1) + W(0, 0, 1)), uwt = h * (U(0, 0, 0) + U(0, 0, 1));
+            VT wub = h * (W(-1, 0, 0) + W(0, 0, 0)), uwb = h * (U(0, 0, -1) + U(0, 0, 0));
+            VT d_wu_dz = (wft * wut * uwt - wfb * wub * uwb) * m.idz(k) * iwc;
+            tu = VT(0) - (d_uu_dx + d_vu_dy + d_wu_dz);
         }
         {
-            R uve = h * (U(1, -1, 0) + U(1, 0, 0)), vue = h * (V(0, 0, 0) + V(1, 0, 0));
-            R uvw = h * (U(0, -1, 0) + U(0, 0, 0)), vuw = h * (V(-1, 0, 0) + V(0, 0, 0));
-            R d_uv_dx = (uve * vue - uvw * vuw) * idx;
-            R vcn = h * (V(0, 0, 0) + V(0, 1, 0)), vcs = h * (V(0, -1, 0) + V(0, 0, 0));
-            R d_vv_dy = (vcn * vcn - vcs * vcs) * idy;
-            R wvt = h * (W(0, -1, 1) + W(0, 0, 1)), vwt = h * (V(0, 0, 0) + V(0, 0, 1));
-            R wvb = h * (W(0, -1, 0) + W(0, 0, 0)), vwb = h * (V(0, 0, -1) + V(0, 0, 0));
-            R d_wv_dz = (wft * wvt * vwt - wfb * wvb * vwb) * m.idz(k) * iwc;
-            tv = R(0) - (d_uv_dx + d_vv_dy + d_wv_dz);
+            VT uve = h * (U(1, -1, 0) + U(1, 0, 0)), vue = h * (V(0, 0, 0) + V(1, 0, 0));
+            VT uvw = h * (U(0, -1, 0) + U(0, 0, 0)), vuw = h * (V(-1, 0, 0) + V(0, 0, 0));
+            VT d_uv_dx = (uve * vue - uvw * vuw) * idx;
+            VT vcn = h * (V(0, 0, 0) + V(0, 1, 0)), vcs = h * (V(0, -1, 0) + V(0, 0, 0));
+            VT d_vv_dy = (vcn * vcn - vcs * vcs) * idy;
+            VT wvt = h * (W(0, -1, 1) + W(0, 0, 1)), vwt = h * (V(0, 0, 0) + V(0, 0, 1));
+            VT wvb = h * (W(0, -1, 0) + W(0, 0, 0)), vwb = h * (V(0, 0, -1) + V(0, 0, 0));
+            VT d_wv_dz = (wft * wvt * vwt - wfb * wvb * vwb) * m.idz(k) * iwc;
+            tv = VT(0) - (d_uv_dx + d_vv_dy + d_wv_dz);
         }
         {
-            R iwf = m.iwf(k), wcb = m.wc(k - 1), wct = m.wc(k);
-            R uwe = m.zflux(k, U(1, 0, -1), U(1, 0, 0)), wue = h * (W(0, 0, 0) + W(1, 0, 0));
-            R uww = m.zflux(k, U(0, 0, -1), U(0, 0, 0)), wuw = h * (W(-1, 0, 0) + W(0, 0, 0));
-            R d_uw_dx = (uwe * wue - uww * wuw) * idx;
-            R vwn = m.zflux(k, V(0, 1, -1), V(0, 1, 0)), wvn = h * (W(0, 0, 0) + W(0, 1, 0));
-            R vws = m.zflux(k, V(0, 0, -1), V(0, 0, 0)), wvs = h * (W(0, -1, 0) + W(0, 0, 0));
-            R d_vw_dy = (vwn * wvn - vws * wvs) * idy;
-            R wtop = h * (W(0, 0, 0) + W(0, 0, 1)), wbot = h * (W(0, 0, -1) + W(0, 0, 0));
-            R d_ww_dz = (wct * wtop * wtop - wcb * wbot * wbot) * m.idzf(k) * iwf;
-            tw = R(0) - (d_uw_dx + d_vw_dy + d_ww_dz);
+            VT iwf = m.iwf(k), wcb = m.wc(k - 1), wct = m.wc(k);
+            VT uwe = m.zflux(k, U(1, 0, -1), U(1, 0, 0)), wue = h * (W(0, 0, 0) + W(1, 0, 0));
+            VT uww = m.zflux(k, U(0, 0, -1), U(0, 0, 0)), wuw = h * (W(-1, 0, 0) + W(0, 0, 0));
+            VT d_uw_dx = (uwe * wue - uww * wuw) * idx;
+            VT vwn = m.zflux(k, V(0, 1, -1), V(0, 1, 0)), wvn = h * (W(0, 0, 0) + W(0, 1, 0));
+            VT vws = m.zflux(k, V(0, 0, -1), V(0, 0, 0)), wvs = h * (W(0, -1, 0) + W(0, 0, 0));
+            VT d_vw_dy = (vwn * wvn - vws * wvs) * idy;
+            VT wtop = h * (W(0, 0, 0) + W(0, 0, 1)), wbot = h * (W(0, 0, -1) + W(0, 0, 0));
+            VT d_ww_dz = (wct * wtop * wtop - wcb * wbot * wbot) * m.idzf(k) * iwf;
+            tw = VT(0) - (d_uw_dx + d_vw_dy + d_ww_dz);
         }
         {
-            R ue = U(1, 0, 0) * h * (T(0, 0, 0) + T(1, 0, 0)), uw = U(0, 0, 0) * h * (T(-1, 0, 0) + T(0, 0, 0));
-            R vn = V(0, 1, 0) * h * (T(0, 0, 0) + T(0, 1, 0)), vs = V(0, 0, 0) * h * (T(0, -1, 0) + T(0, 0, 0));
-            R wt = wft * W(0, 0, 1) * h * (T(0, 0, 0) + T(0, 0, 1)), wb = wfb * W(0, 0, 0) * h * (T(0, 0, -1) + T(0, 0, 0));
-            tt = R(0) - ((ue - uw) * idx + (vn - vs) * idy + (wt - wb) * m.idz(k) * iwc);
+            VT ue = U(1, 0, 0) * h * (T(0, 0, 0) + T(1, 0, 0)), uw = U(0, 0, 0) * h * (T(-1, 0, 0) + T(0, 0, 0));
+            VT vn = V(0, 1, 0) * h * (T(0, 0, 0) + T(0, 1, 0)), vs = V(0, 0, 0) * h * (T(0, -1, 0) + T(0, 0, 0));
+            VT wt = wft * W(0, 0, 1) * h * (T(0, 0, 0) + T(0, 0, 1)), wb = wfb * W(0, 0, 0) * h * (T(0, 0, -1) + T(0, 0, 0));
+            tt = VT(0) - ((ue - uw) * idx + (vn - vs) * idy + (wt - wb) * m.idz(k) * iwc);
         }
-    } else if (ADV == 0) {
+    } else if constexpr (ADV == 0) {
         // centred flux form (src/FiniteVolume.jl:730-797, :1682-1693)
         {
-            R uce = h * (U(0, 0, 0) + U(1, 0, 0)), ucw = h * (U(-1, 0, 0) + U(0, 0, 0));
-            R d_uu_dx = (uce * uce - ucw * ucw) * idx;
-            R vun = h * (V(-1, 1, 0) + V(0, 1, 0)), uvn = h * (U(0, 0, 0) + U(0, 1, 0));
-            R vus = h * (V(-1, 0, 0) + V(0, 0, 0)), uvs = h * (U(0, -1, 0) + U(0, 0, 0));
-            R d_vu_dy = (vun * uvn - vus * uvs) * idy;
-            R wut = h * (W(-1, 0, 1) + W(0, 0, 1)), uwt = h * (U(0, 0, 0) + U(0, 0, 1));
-            R wub = h * (W(-1, 0, 0) + W(0, 0, 0)), uwb = h * (U(0, 0, -1) + U(0, 0, 0));
-            R d_wu_dz = (wut * uwt - wub * uwb) * m.idz(k);
-            tu = R(0) - (d_uu_dx + d_vu_dy + d_wu_dz);
+            VT uce = h * (U(0, 0, 0) + U(1, 0, 0)), ucw = h * (U(-1, 0, 0) + U(0, 0, 0));
+            VT d_uu_dx = (uce * uce - ucw * ucw) * idx;
+            VT vun = h * (V(-1, 1, 0) + V(0, 1, 0)), uvn = h * (U(0, 0, 0) + U(0, 1, 0));
+            VT vus = h * (V(-1, 0, 0) + V(0, 0, 0)), uvs = h * (U(0, -1, 0) + U(0, 0, 0));
+            VT d_vu_dy = (vun * uvn - vus * uvs) * idy;
+            VT wut = h * (W(-1, 0, 1) + W(0, 0, 1)), uwt = h * (U(0, 0, 0) + U(0, 0, 1));
+            VT wub = h * (W(-1, 0, 0) + W(0, 0, 0)), uwb = h * (U(0, 0, -1) + U(0, 0, 0));
+            VT d_wu_dz = (wut * uwt - wub * uwb) * m.idz(k);
+            tu = VT(0) - (d_uu_dx + d_vu_dy + d_wu_dz);
         }
         {
-            R uve = h * (U(1, -1, 0) + U(1, 0, 0)), vue = h * (V(0, 0, 0) + V(1, 0, 0));
-            R uvw = h * (U(0, -1, 0) + U(0, 0, 0)), vuw = h * (V(-1, 0, 0) + V(0, 0, 0));
-            R d_uv_dx = (uve * vue - uvw * vuw) * idx;
-            R vcn = h * (V(0, 0, 0) + V(0, 1, 0)), vcs = h * (V(0, -1, 0) + V(0, 0, 0));
-            R d_vv_dy = (vcn * vcn - vcs * vcs) * idy;
-            R wvt = h * (W(0, -1, 1) + W(0, 0, 1)), vwt = h * (V(0, 0, 0) + V(0, 0, 1));
-            R wvb = h * (W(0, -1, 0) + W(0, 0, 0)), vwb = h * (V(0, 0, -1) + V(0, 0, 0));
-            R d_wv_dz = (wvt * vwt - wvb * vwb) * m.idz(k);
-            tv = R(0) - (d_uv_dx + d_vv_dy + d_wv_dz);
+            VT uve = h * (U(1, -1, 0) + U(1, 0, 0)), vue = h * (V(0, 0, 0) + V(1, 0, 0));
+            VT uvw = h * (U(0, -1, 0) + U(0, 0, 0)), vuw = h * (V(-1, 0, 0) + V(0, 0, 0));
+            VT d_uv_dx = (uve * vue - uvw * vuw) * idx;
+            VT vcn = h * (V(0, 0, 0) + V(0, 1, 0)), vcs = h * (V(0, -1, 0) + V(0, 0, 0));
+            VT d_vv_dy = (vcn * vcn - vcs * vcs) * idy;
+            VT wvt = h * (W(0, -1, 1) + W(0, 0, 1)), vwt = h * (V(0, 0, 0) + V(0, 0, 1));
+            VT wvb = h * (W(0, -1, 0) + W(0, 0, 0)), vwb = h * (V(0, 0, -1) + V(0, 0, 0));
+            VT d_wv_dz = (wvt * vwt - wvb * vwb) * m.idz(k);
+            tv = VT(0) - (d_uv_dx + d_vv_dy + d_wv_dz);
         }
         {
-            R uwe = m.zflux(k, U(1, 0, -1), U(1, 0, 0)), wue = h * (W(0, 0, 0) + W(1, 0, 0));
-            R uww = m.zflux(k, U(0, 0, -1), U(0, 0, 0)), wuw = h * (W(-1, 0, 0) + W(0, 0, 0));
-            R d_uw_dx = (uwe * wue - uww * wuw) * idx;
-            R vwn = m.zflux(k, V(0, 1, -1), V(0, 1, 0)), wvn = h * (W(0, 0, 0) + W(0, 1, 0));
-            R vws = m.zflux(k, V(0, 0, -1), V(0, 0, 0)), wvs = h * (W(0, -1, 0) + W(0, 0, 0));
-            R d_vw_dy = (vwn * wvn - vws * wvs) * idy;
-            R wct = h * (W(0, 0, 0) + W(0, 0, 1)), wcb = h * (W(0, 0, -1) + W(0, 0, 0));
-            R d_ww_dz = (wct * wct - wcb * wcb) * m.idzf(k);
-            tw = R(0) - (d_uw_dx + d_vw_dy + d_ww_dz);
+            VT uwe = m.zflux(k, U(1, 0, -1), U(1, 0, 0)), wue = h * (W(0, 0, 0) + W(1, 0, 0));
+            VT uww = m.zflux(k, U(0, 0, -1), U(0, 0, 0)), wuw = h * (W(-1, 0, 0) + W(0, 0, 0));
+            VT d_uw_dx = (uwe * wue - uww * wuw) * idx;
+            VT vwn = m.zflux(k, V(0, 1, -1), V(0, 1, 0)), wvn = h * (W(0, 0, 0) + W(0, 1, 0));
+            VT vws = m.zflux(k, V(0, 0, -1), V(0, 0, 0)), wvs = h * (W(0, -1, 0) + W(0, 0, 0));
+            VT d_vw_dy = (vwn * wvn - vws * wvs) * idy;
+            VT wct = h * (W(0, 0, 0) + W(0, 0, 1)), wcb = h * (W(0, 0, -1) + W(0, 0, 0));
+            VT d_ww_dz = (wct * wct - wcb * wcb) * m.idzf(k);
+            tw = VT(0) - (d_uw_dx + d_vw_dy + d_ww_dz);
         }
         {
-            R ue = U(1, 0, 0) * h * (T(0, 0, 0) + T(1, 0, 0)), uw = U(0, 0, 0) * h * (T(-1, 0, 0) + T(0, 0, 0));
-            R vn = V(0, 1, 0) * h * (T(0, 0, 0) + T(0, 1, 0)), vs = V(0, 0, 0) * h * (T(0, -1, 0) + T(0, 0, 0));
-            R wt = W(0, 0, 1) * h * (T(0, 0, 0) + T(0, 0, 1)), wb = W(0, 0, 0) * h * (T(0, 0, -1) + T(0, 0, 0));
-            tt = R(0) - ((ue - uw) * idx + (vn - vs) * idy + (wt - wb) * m.idz(k));
+            VT ue = U(1, 0, 0) * h * (T(0, 0, 0) + T(1, 0, 0)), uw = U(0, 0, 0) * h * (T(-1, 0, 0) + T(0, 0, 0));
+            VT vn = V(0, 1, 0) * h * (T(0, 0, 0) + T(0, 1, 0)), vs = V(0, 0, 0) * h * (T(0, -1, 0) + T(0, 0, 0));
+            VT wt = W(0, 0, 1) * h * (T(0, 0, 0) + T(0, 0, 1)), wb = W(0, 0, 0) * h * (T(0, 0, -1) + T(0, 0, 0));
+            tt = VT(0) - ((ue - uw) * idx + (vn - vs) * idy + (wt - wb) * m.idz(k));
         }
     } else {
         // WENO flux forms on a uniform grid (src/AdvectionSchemes.jl:685-699, :1203-1256)
-        const R idz = R(g.idz);
+        const VT idz = VT(g.idz);
         {
-            R Ue = (U(0, 0, 0) + U(1, 0, 0)) / R(2), Uw = (U(-1, 0, 0) + U(0, 0, 0)) / R(2);
-            R dx = (Ue * face_x<R, ADV>(U, 0, 0, 0, Ue) - Uw * face_x<R, ADV>(U, -1, 0, 0, Uw)) * idx;
-            R Vn = (V(-1, 1, 0) + V(0, 1, 0)) / R(2), Vs = (V(-1, 0, 0) + V(0, 0, 0)) / R(2);
-            R dy = (Vn * face_y<R, ADV>(U, 0, 0, 0, Vn) - Vs * face_y<R, ADV>(U, 0, -1, 0, Vs)) * idy;
-            R Wt = (W(-1, 0, 1) + W(0, 0, 1)) / R(2), Wb = (W(-1, 0, 0) + W(0, 0, 0)) / R(2);
-            R dz = (Wt * face_z<R, ADV>(U, 0, 0, 0, Wt) - Wb * face_z<R, ADV>(U, 0, 0, -1, Wb)) * idz;
-            tu = R(0) - (dx + dy + dz);
+            VT Ue = (U(0, 0, 0) + U(1, 0, 0)) / VT(2), Uw = (U(-1, 0, 0) + U(0, 0, 0)) / VT(2);
+            VT dx = (Ue * face_x<VT, ADV>(U, 0, 0, 0, Ue) - Uw * face_x<VT, ADV>(U, -1, 0, 0, Uw)) * idx;
+            VT Vn = (V(-1, 1, 0) + V(0, 1, 0)) / VT(2), Vs = (V(-1, 0, 0) + V(0, 0, 0)) / VT(2);
+            VT dy = (Vn * face_y<VT, ADV>(U, 0, 0, 0, Vn) - Vs * face_y<VT, ADV>(U, 0, -1, 0, Vs)) * idy;
+            VT Wt = (W(-1, 0, 1) + W(0, 0, 1)) / VT(2), Wb = (W(-1, 0, 0) + W(0, 0, 0)) / VT(2);
+            VT dz = (Wt * face_z<VT, ADV>(U, 0, 0, 0, Wt) - Wb * face_z<VT, ADV>(U, 0, 0, -1, Wb)) * idz;
+            tu = VT(0) - (dx + dy + dz);
         }
         {
-            R Ue = (U(1, -1, 0) + U(1, 0, 0)) / R(2), Uw = (U(0, -1, 0) + U(0, 0, 0)) / R(2);
-            R dx = (Ue * face_x<R, ADV>(V, 0, 0, 0, Ue) - Uw * face_x<R, ADV>(V, -1, 0, 0, Uw)) * idx;
-            R Vn = (V(0, 0, 0) + V(0, 1, 0)) / R(2), Vs = (V(0, -1, 0) + V(0, 0, 0)) / R(2);
-            R dy = (Vn * face_y<R, ADV>(V, 0, 0, 0, Vn) - Vs * face_y<R, ADV>(V, 0, -1, 0, Vs)) * idy;
-            R Wt = (W(0, -1, 1) + W(0, 0, 1)) / R(2), Wb = (W(0, -1, 0) + W(0, 0, 0)) / R(2);
-            R dz = (Wt * face_z<R, ADV>(V, 0, 0, 0, Wt) - Wb * face_z<R, ADV>(V, 0, 0, -1, Wb)) * idz;
-            tv = R(0) - (dx + dy + dz);
+            VT Ue = (U(1, -1, 0) + U(1, 0, 0)) / VT(2), Uw = (U(0, -1, 0) + U(0, 0, 0)) / VT(2);
+            VT dx = (Ue * face_x<VT, ADV>(V, 0, 0, 0, Ue) - Uw * face_x<VT, ADV>(V, -1, 0, 0, Uw)) * idx;
+            VT Vn = (V(0, 0, 0) + V(0, 1, 0)) / VT(2), Vs = (V(0, -1, 0) + V(0, 0, 0)) / VT(2);
+            VT dy = (Vn * face_y<VT, ADV>(V, 0, 0, 0, Vn) - Vs * face_y<VT, ADV>(V, 0, -1, 0, Vs)) * idy;
+            VT Wt = (W(0, -1, 1) + W(0, 0, 1)) / VT(2), Wb = (W(0, -1, 0) + W(0, 0, 0)) / VT(2);
+            VT dz = (Wt * face_z<VT, ADV>(V, 0, 0, 0, Wt) - Wb * face_z<VT, ADV>(V, 0, 0, -1, Wb)) * idz;
+            tv = VT(0) - (dx + dy + dz);
         }
         {
-            R Ue = (U(1, 0, -1) + U(1, 0, 0)) / R(2), Uw = (U(0, 0, -1) + U(0, 0, 0)) / R(2);
-            R dx = (Ue * face_x<R, ADV>(W, 0, 0, 0, Ue) - Uw * face_x<R, ADV>(W, -1, 0, 0, Uw)) * idx;
-            R Vn = (V(0, 1, -1) + V(0, 1, 0)) / R(2), Vs = (V(0, 0, -1) + V(0, 0, 0)) / R(2);
-            R dy = (Vn * face_y<R, ADV>(W, 0, 0, 0, Vn) - Vs * face_y<R, ADV>(W, 0, -1, 0, Vs)) * idy;
-            R Wt = (W(0, 0, 0) + W(0, 0, 1)) / R(2), Wb = (W(0, 0, -1) + W(0, 0, 0)) / R(2);
-            R dz = (Wt * face_z<R, ADV>(W, 0, 0, 0, Wt) - Wb * face_z<R, ADV>(W, 0, 0, -1, Wb)) * idz;
-            tw = R(0) - (dx + dy + dz);
+            VT Ue = (U(1, 0, -1) + U(1, 0, 0)) / VT(2), Uw = (U(0, 0, -1) + U(0, 0, 0)) / VT(2);
+            VT dx = (Ue * face_x<VT, ADV>(W, 0, 0, 0, Ue) - Uw * face_x<VT, ADV>(W, -1, 0, 0, Uw)) * idx;
+            VT Vn = (V(0, 1, -1) + V(0, 1, 0)) / VT(2), Vs = (V(0, 0, -1) + V(0, 0, 0)) / VT(2);
+            VT dy = (Vn * face_y<VT, ADV>(W, 0, 0, 0, Vn) - Vs * face_y<VT, ADV>(W, 0, -1, 0, Vs)) * idy;
+            VT Wt = (W(0, 0, 0) + W(0, 0, 1)) / VT(2), Wb = (W(0, 0, -1) + W(0, 0, 0)) / VT(2);
+            VT dz = (Wt * face_z<VT, ADV>(W, 0, 0, 0, Wt) - Wb * face_z<VT, ADV>(W, 0, 0, -1, Wb)) * idz;
+            tw = VT(0) - (dx + dy + dz);
         }
         {
-            R uw = U(0, 0, 0), ue = U(1, 0, 0);
-            R Fx = (ue * face_x<R, ADV>(T, 0, 0, 0, ue) - uw * face_x<R, ADV>(T, -1, 0, 0, uw)) * idx;
-            R vs = V(0, 0, 0), vn = V(0, 1, 0);
-            R Fy = (vn * face_y<R, ADV>(T, 0, 0, 0, vn) - vs * face_y<R, ADV>(T, 0, -1, 0, vs)) * idy;
-            R wb = W(0, 0, 0), wt = W(0, 0, 1);
-            R Fz = (wt * face_z<R, ADV>(T, 0, 0, 0, wt) - wb * face_z<R, ADV>(T, 0, 0, -1, wb)) * idz;
-            tt = R(0) - (Fx + Fy + Fz);
+            VT uw = U(0, 0, 0), ue = U(1, 0, 0);
+            VT Fx = (ue * face_x<VT, ADV>(T, 0, 0, 0, ue) - uw * face_x<VT, ADV>(T, -1, 0, 0, uw)) * idx;
+            VT vs = V(0, 0, 0), vn = V(0, 1, 0);
+            VT Fy = (vn * face_y<VT, ADV>(T, 0, 0, 0, vn) - vs * face_y<VT, ADV>(T, 0, -1, 0, vs)) * idy;
+            VT wb = W(0, 0, 0), wt = W(0, 0, 1);
+            VT Fz = (wt * face_z<VT, ADV>(T, 0, 0, 0, wt) - wb * face_z<VT, ADV>(T, 0, 0, -1, wb)) * idz;
+            tt = VT(0) - (Fx + Fy + Fz);
         }
     }
 
     // molecular viscosity / diffusion
     if (a.nu != R(0)) {
-        R c;
+        VT c;
         c = U(0, 0, 0);
-        tu = tu + a.nu * ((U(1, 0, 0) - R(2) * c + U(-1, 0, 0)) * idx2 + (U(0, 1, 0) - R(2) * c + U(0, -1, 0)) * idy2 +
+        tu = tu + a.nu * ((U(1, 0, 0) - VT(2) * c + U(-1, 0, 0)) * idx2 + (U(0, 1, 0) - VT(2) * c + U(0, -1, 0)) * idy2 +
                           m.lapz(LOC_FX, k, U(0, 0, -1), c, U(0, 0, 1)));
         c = V(0, 0, 0);
-        tv = tv + a.nu * ((V(1, 0, 0) - R(2) * c + V(-1, 0, 0)) * idx2 + (V(0, 1, 0) - R(2) * c + V(0, -1, 0)) * idy2 +
+        tv = tv + a.nu * ((V(1, 0, 0) - VT(2) * c + V(-1, 0, 0)) * idx2 + (V(0, 1, 0) - VT(2) * c + V(0, -1, 0)) * idy2 +
                           m.lapz(LOC_FY, k, V(0, 0, -1), c, V(0, 0, 1)));
         c = W(0, 0, 0);
-        tw = tw + a.nu * ((W(1, 0, 0) - R(2) * c + W(-1, 0, 0)) * idx2 + (W(0, 1, 0) - R(2) * c + W(0, -1, 0)) * idy2 +
+        tw = tw + a.nu * ((W(1, 0, 0) - VT(2) * c + W(-1, 0, 0)) * idx2 + (W(0, 1, 0) - VT(2) * c + W(0, -1, 0)) * idy2 +
                           m.lapz(LOC_FZ, k, W(0, 0, -1), c, W(0, 0, 1)));
         c = T(0, 0, 0);
-        tt = tt + a.nu * ((T(1, 0, 0) - R(2) * c + T(-1, 0, 0)) * idx2 + (T(0, 1, 0) - R(2) * c + T(0, -1, 0)) * idy2 +
+        tt = tt + a.nu * ((T(1, 0, 0) - VT(2) * c + T(-1, 0, 0)) * idx2 + (T(0, 1, 0) - VT(2) * c + T(0, -1, 0)) * idy2 +
                           m.lapz(LOC_C, k, T(0, 0, -1), c, T(0, 0, 1)));
     }
 
     // Smagorinsky SGS fluxes (eddy viscosity from the nut array, halos filled)
     if (SGS) {
-        const R q4 = R(0.25);
+        const VT q4 = VT(0.25);
         {
-            R fxE = N(0, 0, 0) * (U(1, 0, 0) - U(0, 0, 0)) * idx;
-            R fxW = N(-1, 0, 0) * (U(0, 0, 0) - U(-1, 0, 0)) * idx;
-            R eN = q4 * (N(-1, 0, 0) + N(0, 0, 0) + N(-1, 1, 0) + N(0, 1, 0));
-            R eS = q4 * (N(-1, -1, 0) + N(0, -1, 0) + N(-1, 0, 0) + N(0, 0, 0));
-            R fyN = eN * (U(0, 1, 0) - U(0, 0, 0)) * idy;
-            R fyS = eS * (U(0, 0, 0) - U(0, -1, 0)) * idy;
-            R eT = q4 * (N(-1, 0, 0) + N(0, 0, 0) + N(-1, 0, 1) + N(0, 0, 1));
-            R eB = q4 * (N(-1, 0, -1) + N(0, 0, -1) + N(-1, 0, 0) + N(0, 0, 0));
-            R fzT = eT * (U(0, 0, 1) - U(0, 0, 0)) * m.idzf(k + 1);
-            R fzB = eB * (U(0, 0, 0) - U(0, 0, -1)) * m.idzf(k);
-            R vert = ANEL ? (m.wf(k + 1) * fzT - m.wf(k) * fzB) * m.idz(k) * m.iwc(k)
+            VT fxE = N(0, 0, 0) * (U(1, 0, 0) - U(0, 0, 0)) * idx;
+            VT fxW = N(-1, 0, 0) * (U(0, 0, 0) - U(-1, 0, 0)) * idx;
+            VT eN = q4 * (N(-1, 0, 0) + N(0, 0, 0) + N(-1, 1, 0) + N(0, 1, 0));
+            VT eS = q4 * (N(-1, -1, 0) + N(0, -1, 0) + N(-1, 0, 0) + N(0, 0, 0));
+            VT fyN = eN * (U(0, 1, 0) - U(0, 0, 0)) * idy;
+            VT fyS = eS * (U(0, 0, 0) - U(0, -1, 0)) * idy;
+            VT eT = q4 * (N(-1, 0, 0) + N(0, 0, 0) + N(-1, 0, 1) + N(0, 0, 1));
+            VT eB = q4 * (N(-1, 0, -1) + N(0, 0, -1) + N(-1, 0, 0) + N(0, 0, 0));
+            VT fzT = eT * (U(0, 0, 1) - U(0, 0, 0)) * m.idzf(k + 1);
+            VT fzB = eB * (U(0, 0, 0) - U(0, 0, -1)) * m.idzf(k);
+            VT vert = ANEL ? (m.wf(k + 1) * fzT - m.wf(k) * fzB) * m.idz(k) * m.iwc(k)
                           : (fzT - fzB) * m.idz(k);
             tu += (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
         }
         {
-            R fyN = N(0, 0, 0) * (V(0, 1, 0) - V(0, 0, 0)) * idy;
-            R fyS = N(0, -1, 0) * (V(0, 0, 0) - V(0, -1, 0)) * idy;
-            R eE = q4 * (N(0, -1, 0) + N(1, -1, 0) + N(0, 0, 0) + N(1, 0, 0));
-            R eW = q4 * (N(-1, -1, 0) + N(0, -1, 0) + N(-1, 0, 0) + N(0, 0, 0));
-            R fxE = eE * (V(1, 0, 0) - V(0, 0, 0)) * idx;
-            R fxW = eW * (V(0, 0, 0) - V(-1, 0, 0)) * idx;
-            R eT = q4 * (N(0, -1, 0) + N(0, 0, 0) + N(0, -1, 1) + N(0, 0, 1));
-            R eB = q4 * (N(0, -1, -1) + N(0, 0, -1) + N(0, -1, 0) + N(0, 0, 0));
-            R fzT = eT * (V(0, 0, 1) - V(0, 0, 0)) * m.idzf(k + 1);
-            R fzB = eB * (V(0, 0, 0) - V(0, 0, -1)) * m.idzf(k);
-            R vert = ANEL ? (m.wf(k + 1) * fzT - m.wf(k) * fzB) * m.idz(k) * m.iwc(k)
+            VT fyN = N(0, 0, 0) * (V(0, 1, 0) - V(0, 0, 0)) * idy;
+            VT fyS = N(0, -1, 0) * (V(0, 0, 0) - V(0, -1, 0)) * idy;
+            VT eE = q4 * (N(0, -1, 0) + N(1, -1, 0) + N(0, 0, 0) + N(1, 0, 0));
+            VT eW = q4 * (N(-1, -1, 0) + N(0, -1, 0) + N(-1, 0, 0) + N(0, 0, 0));
+            VT fxE = eE * (V(1, 0, 0) - V(0, 0, 0)) * idx;
+            VT fxW = eW * (V(0, 0, 0) - V(-1, 0, 0)) * idx;
+            VT eT = q4 * (N(0, -1, 0) + N(0, 0, 0) + N(0, -1, 1) + N(0, 0, 1));
+            VT eB = q4 * (N(0, -1, -1) + N(0, 0, -1) + N(0, -1, 0) + N(0, 0, 0));
+            VT fzT = eT * (V(0, 0, 1) - V(0, 0, 0)) * m.idzf(k + 1);
+            VT fzB = eB * (V(0, 0, 0) - V(0, 0, -1)) * m.idzf(k);
+            VT vert = ANEL ? (m.wf(k + 1) * fzT - m.wf(k) * fzB) * m.idz(k) * m.iwc(k)
                           : (fzT - fzB) * m.idz(k);
             tv += (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
         }
         {
-            R fzT = N(0, 0, 0) * (W(0, 0, 1) - W(0, 0, 0)) * m.idz(k);
-            R fzB = N(0, 0, -1) * (W(0, 0, 0) - W(0, 0, -1)) * m.idz(k - 1);
-            R eE = q4 * (N(0, 0, -1) + N(1, 0, -1) + N(0, 0, 0) + N(1, 0, 0));
-            R eW = q4 * (N(-1, 0, -1) + N(0, 0, -1) + N(-1, 0, 0) + N(0, 0, 0));
-            R fxE = eE * (W(1, 0, 0) - W(0, 0, 0)) * idx;
-            R fxW = eW * (W(0, 0, 0) - W(-1, 0, 0)) * idx;
-            R eN = q4 * (N(0, 0, -1) + N(0, 1, -1) + N(0, 0, 0) + N(0, 1, 0));
-            R eS = q4 * (N(0, -1, -1) + N(0, 0, -1) + N(0, -1, 0) + N(0, 0, 0));
-            R fyN = eN * (W(0, 1, 0) - W(0, 0, 0)) * idy;
-            R fyS = eS * (W(0, 0, 0) - W(0, -1, 0)) * idy;
-            R vert = ANEL ? (m.wc(k) * fzT - m.wc(k - 1) * fzB) * m.idzf(k) * m.iwf(k)
+            VT fzT = N(0, 0, 0) * (W(0, 0, 1) - W(0, 0, 0)) * m.idz(k);
+            VT fzB = N(0, 0, -1) * (W(0, 0, 0) - W(0, 0, -1)) * m.idz(k - 1);
+            VT eE = q4 * (N(0, 0, -1) + N(1, 0, -1) + N(0, 0, 0) + N(1, 0, 0));
+            VT eW = q4 * (N(-1, 0, -1) + N(0, 0, -1) + N(-1, 0, 0) + N(0, 0, 0));
+            VT fxE = eE * (W(1, 0, 0) - W(0, 0, 0)) * idx;
+            VT fxW = eW * (W(0, 0, 0) - W(-1, 0, 0)) * idx;
+            VT eN = q4 * (N(0, 0, -1) + N(0, 1, -1) + N(0, 0, 0) + N(0, 1, 0));
+            VT eS = q4 * (N(0, -1, -1) + N(0, 0, -1) + N(0, -1, 0) + N(0, 0, 0));
+            VT fyN = eN * (W(0, 1, 0) - W(0, 0, 0)) * idy;
+            VT fyS = eS * (W(0, 0, 0) - W(0, -1, 0)) * idy;
+            VT vert = ANEL ? (m.wc(k) * fzT - m.wc(k - 1) * fzB) * m.idzf(k) * m.iwf(k)
                           : (fzT - fzB) * m.idzf(k);
             tw += (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
         }
         if (!ANEL) {
-            R nE = h * (N(0, 0, 0) + N(1, 0, 0)), nW = h * (N(-1, 0, 0) + N(0, 0, 0));
-            R nN = h * (N(0, 0, 0) + N(0, 1, 0)), nS = h * (N(0, -1, 0) + N(0, 0, 0));
-            R nT = h * (N(0, 0, 0) + N(0, 0, 1)), nB = h * (N(0, 0, -1) + N(0, 0, 0));
-            R fxE = nE * (T(1, 0, 0) - T(0, 0, 0)) * idx, fxW = nW * (T(0, 0, 0) - T(-1, 0, 0)) * idx;
-            R fyN = nN * (T(0, 1, 0) - T(0, 0, 0)) * idy, fyS = nS * (T(0, 0, 0) - T(0, -1, 0)) * idy;
-            R fzT = nT * (T(0, 0, 1) - T(0, 0, 0)) * m.idzf(k + 1), fzB = nB * (T(0, 0, 0) - T(0, 0, -1)) * m.idzf(k);
+            VT nE = h * (N(0, 0, 0) + N(1, 0, 0)), nW = h * (N(-1, 0, 0) + N(0, 0, 0));
+            VT nN = h * (N(0, 0, 0) + N(0, 1, 0)), nS = h * (N(0, -1, 0) + N(0, 0, 0));
+            VT nT = h * (N(0, 0, 0) + N(0, 0, 1)), nB = h * (N(0, 0, -1) + N(0, 0, 0));
+            VT fxE = nE * (T(1, 0, 0) - T(0, 0, 0)) * idx, fxW = nW * (T(0, 0, 0) - T(-1, 0, 0)) * idx;
+            VT fyN = nN * (T(0, 1, 0) - T(0, 0, 0)) * idy, fyS = nS * (T(0, 0, 0) - T(0, -1, 0)) * idy;
+            VT fzT = nT * (T(0, 0, 1) - T(0, 0, 0)) * m.idzf(k + 1), fzB = nB * (T(0, 0, 0) - T(0, 0, -1)) * m.idzf(k);
             tt += a.inv_prt * ((fxE - fxW) * idx + (fyN - fyS) * idy + (fzT - fzB) * m.idz(k));
         } else {
             // kappa = nut / Pr_t, the W-weighted form (1/Pr_t applied once per face)
-            const R hk = h * a.inv_prt;
-            const R N0 = N(0, 0, 0);
-            R fxE = hk * (N0 + N(1, 0, 0)) * (T(1, 0, 0) - T(0, 0, 0)) * idx;
-            R fxW = hk * (N(-1, 0, 0) + N0) * (T(0, 0, 0) - T(-1, 0, 0)) * idx;
-            R fyN = hk * (N0 + N(0, 1, 0)) * (T(0, 1, 0) - T(0, 0, 0)) * idy;
-            R fyS = hk * (N(0, -1, 0) + N0) * (T(0, 0, 0) - T(0, -1, 0)) * idy;
-            R fzT = hk * (N0 + N(0, 0, 1)) * (T(0, 0, 1) - T(0, 0, 0)) * m.idzf(k + 1);
-            R fzB = hk * (N(0, 0, -1) + N0) * (T(0, 0, 0) - T(0, 0, -1)) * m.idzf(k);
-            R vert = (m.wf(k + 1) * fzT - m.wf(k) * fzB) * m.idz(k) * m.iwc(k);
+            const VT hk = h * a.inv_prt;
+            const VT N0 = N(0, 0, 0);
+            VT fxE = hk * (N0 + N(1, 0, 0)) * (T(1, 0, 0) - T(0, 0, 0)) * idx;
+            VT fxW = hk * (N(-1, 0, 0) + N0) * (T(0, 0, 0) - T(-1, 0, 0)) * idx;
+            VT fyN = hk * (N0 + N(0, 1, 0)) * (T(0, 1, 0) - T(0, 0, 0)) * idy;
+            VT fyS = hk * (N(0, -1, 0) + N0) * (T(0, 0, 0) - T(0, -1, 0)) * idy;
+            VT fzT = hk * (N0 + N(0, 0, 1)) * (T(0, 0, 1) - T(0, 0, 0)) * m.idzf(k + 1);
+            VT fzB = hk * (N(0, 0, -1) + N0) * (T(0, 0, 0) - T(0, 0, -1)) * m.idzf(k);
+            VT vert = (m.wf(k + 1) * fzT - m.wf(k) * fzB) * m.idz(k) * m.iwc(k);
             tt += (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
         }
     }
@@ -331,8 +334,8 @@ __device__ __forceinline__ void sweep_point(const Met<R, UNI>& m, const SweepArg
     // buoyancy on the z faces
     if (ANEL) {
         if (a.gacc != R(0)) {
-            R tb = m.thf(k);
-            R coef = m.gthf(k);   // g / theta_f
+            VT tb = m.thf(k);
+            VT coef = m.gthf(k);   // g / theta_f
             tw += coef * (m.zface(k, T(0, 0, -1), T(0, 0, 0)) - tb);
         }
     } else if (a.theta0 != R(0)) {
@@ -340,9 +343,9 @@ __device__ __forceinline__ void sweep_point(const Met<R, UNI>& m, const SweepArg
     }
     // Coriolis
     if (a.fcor != R(0)) {
-        R v_at_u = R(0.25) * (V(-1, 0, 0) + V(0, 0, 0) + V(-1, 1, 0) + V(0, 1, 0));
+        VT v_at_u = VT(0.25) * (V(-1, 0, 0) + V(0, 0, 0) + V(-1, 1, 0) + V(0, 1, 0));
         tu += a.fcor * v_at_u;
-        R u_at_v = R(0.25) * (U(0, -1, 0) + U(1, -1, 0) + U(0, 0, 0) + U(1, 0, 0));
+        VT u_at_v = VT(0.25) * (U(0, -1, 0) + U(1, -1, 0) + U(0, 0, 0) + U(1, 0, 0));
         tv -= a.fcor * u_at_v;
     }
     // prescribed wall fluxes of theta
@@ -351,7 +354,7 @@ __device__ __forceinline__ void sweep_point(const Met<R, UNI>& m, const SweepArg
     // Rayleigh sponge toward rest: the per-level rates alpha sin^2(pi/2 (z - z_s)/(z_top - z_s))
     // above z_s, zero below (src/FiniteVolume.jl:578-702)
     if (a.sp_alpha != R(0)) {
-        const R rc = m.spc(k), rf = m.spf(k);
+        const VT rc = m.spc(k), rf = m.spf(k);
         tu -= rc * U(0, 0, 0);
         tv -= rc * V(0, 0, 0);
         tw -= rf * W(0, 0, 0);
@@ -386,23 +389,24 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs<R> a) {
 // Smagorinsky nut = (C_s Delta_k)^2 |S| at a cell centre (src/FiniteVolume.jl:936-944,
 // strain src/Operators.jl:451-496), accessors around the point at level k.
 template <typename R, bool UNI, class AU, class AV, class AW>
-__device__ __forceinline__ R smag_point(const Met<R, UNI>& m, const Geo& g, int k, R c_s, const AU& U, const AV& V,
-                                        const AW& W) {
-    R idx = R(g.idx), idy = R(g.idy), idz = m.idz(k), ido = m.idz_off(k);
-    R cf = c_s * m.filter(k);
-    R coef = cf * cf;
-    R du_dx = (U(1, 0, 0) - U(0, 0, 0)) * idx;
-    R dv_dy = (V(0, 1, 0) - V(0, 0, 0)) * idy;
-    R dw_dz = (W(0, 0, 1) - W(0, 0, 0)) * idz;
-    R du_dy = ((U(0, 1, 0) + U(1, 1, 0)) - (U(0, -1, 0) + U(1, -1, 0))) * (R(0.25) * idy);
-    R dv_dx = ((V(1, 0, 0) + V(1, 1, 0)) - (V(-1, 0, 0) + V(-1, 1, 0))) * (R(0.25) * idx);
-    R du_dz = ((U(0, 0, 1) + U(1, 0, 1)) - (U(0, 0, -1) + U(1, 0, -1))) * (R(0.25) * ido);
-    R dw_dx = ((W(1, 0, 0) + W(1, 0, 1)) - (W(-1, 0, 0) + W(-1, 0, 1))) * (R(0.25) * idx);
-    R dv_dz = ((V(0, 0, 1) + V(0, 1, 1)) - (V(0, 0, -1) + V(0, 1, -1))) * (R(0.25) * ido);
-    R dw_dy = ((W(0, 1, 0) + W(0, 1, 1)) - (W(0, -1, 0) + W(0, -1, 1))) * (R(0.25) * idy);
-    R S12 = R(0.5) * (du_dy + dv_dx), S13 = R(0.5) * (du_dz + dw_dx), S23 = R(0.5) * (dv_dz + dw_dy);
-    R S2 = R(2) * (du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz) + R(4) * (S12 * S12 + S13 * S13 + S23 * S23);
-    return coef * sqrt(S2);
+__device__ __forceinline__ auto smag_point(const Met<R, UNI>& m, const Geo& g, int k, R c_s, const AU& U, const AV& V,
+                                           const AW& W) {
+    using VT = decltype(U(0, 0, 0));   // R, or a pair of FP32 lanes
+    const R idx = R(g.idx), idy = R(g.idy), idz = m.idz(k), ido = m.idz_off(k);
+    const R cf = c_s * m.filter(k);
+    const R coef = cf * cf;
+    VT du_dx = (U(1, 0, 0) - U(0, 0, 0)) * idx;
+    VT dv_dy = (V(0, 1, 0) - V(0, 0, 0)) * idy;
+    VT dw_dz = (W(0, 0, 1) - W(0, 0, 0)) * idz;
+    VT du_dy = ((U(0, 1, 0) + U(1, 1, 0)) - (U(0, -1, 0) + U(1, -1, 0))) * (R(0.25) * idy);
+    VT dv_dx = ((V(1, 0, 0) + V(1, 1, 0)) - (V(-1, 0, 0) + V(-1, 1, 0))) * (R(0.25) * idx);
+    VT du_dz = ((U(0, 0, 1) + U(1, 0, 1)) - (U(0, 0, -1) + U(1, 0, -1))) * (R(0.25) * ido);
+    VT dw_dx = ((W(1, 0, 0) + W(1, 0, 1)) - (W(-1, 0, 0) + W(-1, 0, 1))) * (R(0.25) * idx);
+    VT dv_dz = ((V(0, 0, 1) + V(0, 1, 1)) - (V(0, 0, -1) + V(0, 1, -1))) * (R(0.25) * ido);
+    VT dw_dy = ((W(0, 1, 0) + W(0, 1, 1)) - (W(0, -1, 0) + W(0, -1, 1))) * (R(0.25) * idy);
+    VT S12 = R(0.5) * (du_dy + dv_dx), S13 = R(0.5) * (du_dz + dw_dx), S23 = R(0.5) * (dv_dz + dw_dy);
+    VT S2 = R(2) * (du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz) + R(4) * (S12 * S12 + S13 * S13 + S23 * S23);
+    return VT(coef * sqrt(S2));
 }
 
 // The direct form: nut into a padded array (halos filled by a separate launch).

@@ -37,6 +37,7 @@
 #include "aeo_init.cuh"
 #include "aeo_misc.cuh"
 #include "aeo_sweep.cuh"
+#include "aeo_sweep_pair.cuh"
 #include "aeo_sweep_tile.cuh"
 
 static std::string g_create_error;
@@ -108,6 +109,7 @@ struct Core : CoreBase {
     ColumnCoef cc{};
     R* P[4][4] = {};           // padded state sets (u, v, w, theta)
     TileMaps tmaps[4];         // TMA maps of the padded sets
+    bool pair = false;         // FP32 centred: the paired sweep (64-cell tiles, 72-wide plane boxes)
     int cur = 0;               // the set holding the state (0 or 1)
     R* Q[3] = {};              // predictor (interior)
     R* nut = nullptr;          // padded, diagnostics only
@@ -402,9 +404,10 @@ struct Core : CoreBase {
         if (!fn || q != cudaDriverEntryPointSuccess) { fail("cuTensorMapEncodeTiled is unavailable"); return AEO_ERR_CUDA; }
         auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
         const int HH = cfg.advection != AEO_ADV_CENTRED ? 3 : 2;
+        pair = sizeof(R) == sizeof(float) && cfg.advection == AEO_ADV_CENTRED;
         cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)(g.nz + 2 * AEO_H)};
         cuuint64_t strides[2] = {(cuuint64_t)g.sy * sizeof(R), (cuuint64_t)g.sz * sizeof(R)};
-        cuuint32_t box[3] = {32 + 8, (cuuint32_t)(8 + 2 * HH), 1};
+        cuuint32_t box[3] = {pair ? 64u + 8u : 32u + 8u, (cuuint32_t)(8 + 2 * HH), 1};
         cuuint32_t es[3] = {1, 1, 1};
         CUtensorMapDataType dt = sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
         for (int s = 0; s < 4; ++s) {
@@ -437,6 +440,17 @@ struct Core : CoreBase {
 
     template <int ADV, bool SG, bool AN, bool UN>
     void launch_sweep_t(int s_in, const SweepArgs<R>& a) {
+        if constexpr (ADV == 0 && sizeof(R) == sizeof(float)) {
+            if (pair) {
+                using PS = PairShape<SG>;
+                cudaFuncSetAttribute(sweep_pair_kernel<SG, AN, UN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)PS::SMEM);
+                dim3 grid((g.nx + PS::TX - 1) / PS::TX, (g.ny + PS::TY - 1) / PS::TY, (g.nz + kchunk - 1) / kchunk);
+                sweep_pair_kernel<SG, AN, UN><<<grid, dim3(PS::TXT, PS::TY), PS::SMEM, st>>>(tmaps[s_in], a, kchunk,
+                                                                                           d_flag);
+                return;
+            }
+        }
         using TS = TileShape<R, ADV, SG>;
         const size_t sm = TS::SMEM;
         cudaFuncSetAttribute(sweep_tile_kernel<R, ADV, SG, AN, UN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
