@@ -56,30 +56,40 @@ struct Nb {
 template <typename R>
 __device__ __forceinline__ R beta3(R a1, R a2) { return a1 * a1 + R(13.0 / 3.0) * (a2 * a2); }
 
+// a / b for the nonlinear weights: FP32 uses the two-instruction division
+// (2 ulp; the denominators b_i + eps and (b_i + eps)^2 lie in the normal
+// range), FP64 the IEEE one
+template <typename R>
+__device__ __forceinline__ R wdiv(R a, R b) {
+    if constexpr (sizeof(R) == 4) return __fdividef(a, b);
+    else return a / b;
+}
+
 template <typename R, int ADV>
 __device__ __forceinline__ R weno5_left(R v1, R v2, R v3, R v4, R v5) {
-    R q0 = (R(2) * v1 - R(7) * v2 + R(11) * v3) / R(6);
-    R q1 = (-v2 + R(5) * v3 + R(2) * v4) / R(6);
-    R q2 = (R(2) * v3 + R(5) * v4 - v5) / R(6);
-    R d2a = (v1 - R(2) * v2 + v3) / R(2);
-    R d2b = (v2 - R(2) * v3 + v4) / R(2);
-    R d2c = (v3 - R(2) * v4 + v5) / R(2);
-    R b0 = beta3<R>((v1 - R(4) * v2 + R(3) * v3) / R(2), d2a);
-    R b1 = beta3<R>((v4 - v2) / R(2), d2b);
-    R b2 = beta3<R>((R(-3) * v3 + R(4) * v4 - v5) / R(2), d2c);
+    const R s6 = R(1.0 / 6.0);
+    R q0 = (R(2) * v1 - R(7) * v2 + R(11) * v3) * s6;
+    R q1 = (-v2 + R(5) * v3 + R(2) * v4) * s6;
+    R q2 = (R(2) * v3 + R(5) * v4 - v5) * s6;
+    R d2a = (v1 - R(2) * v2 + v3) * R(0.5);
+    R d2b = (v2 - R(2) * v3 + v4) * R(0.5);
+    R d2c = (v3 - R(2) * v4 + v5) * R(0.5);
+    R b0 = beta3<R>((v1 - R(4) * v2 + R(3) * v3) * R(0.5), d2a);
+    R b1 = beta3<R>((v4 - v2) * R(0.5), d2b);
+    R b2 = beta3<R>((R(-3) * v3 + R(4) * v4 - v5) * R(0.5), d2c);
     R a0, a1, a2;
     if (ADV == 2) {  // WENO-Z5, p = 2, eps = eps(T)^2
         const R eps = sizeof(R) == 8 ? R(4.930380657631324e-32) : R(1.4210854715202004e-14);
         R tau = fabs(b0 - b2);
-        R t0 = tau / (b0 + eps), t1 = tau / (b1 + eps), t2 = tau / (b2 + eps);
+        R t0 = wdiv(tau, b0 + eps), t1 = wdiv(tau, b1 + eps), t2 = wdiv(tau, b2 + eps);
         a0 = R(0.1) * (R(1) + t0 * t0);
         a1 = R(0.6) * (R(1) + t1 * t1);
         a2 = R(0.3) * (R(1) + t2 * t2);
     } else {         // WENO-JS5, eps = 1e-6
         const R e = R(1e-6);
-        a0 = R(0.1) / ((b0 + e) * (b0 + e));
-        a1 = R(0.6) / ((b1 + e) * (b1 + e));
-        a2 = R(0.3) / ((b2 + e) * (b2 + e));
+        a0 = wdiv(R(0.1), (b0 + e) * (b0 + e));
+        a1 = wdiv(R(0.6), (b1 + e) * (b1 + e));
+        a2 = wdiv(R(0.3), (b2 + e) * (b2 + e));
     }
     return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
 }
@@ -87,22 +97,37 @@ __device__ __forceinline__ R weno5_left(R v1, R v2, R v3, R v4, R v5) {
 // Upwinded face values between cells c and c+1 along x, y or z
 // (src/AdvectionSchemes.jl:623-666, mirror-symmetric selection): the
 // left-biased stencil c-2..c+2 for a non-negative face velocity, else the
-// mirrored right-biased c+3..c-1.
+// mirrored right-biased c+3..c-1.  The six values are loaded once and the
+// stencil is selected by the sign, so a warp whose faces see both signs runs
+// one reconstruction, not two.
+template <typename R, int ADV>
+__device__ __forceinline__ R weno_upwind(bool pos, R f0, R f1, R f2, R f3, R f4, R f5) {
+    return weno5_left<R, ADV>(pos ? f0 : f5, pos ? f1 : f4, pos ? f2 : f3, pos ? f3 : f2, pos ? f4 : f1);
+}
 template <typename R, int ADV, class A>
 __device__ __forceinline__ R face_x(const A& F, int c, int dj, int dk, R vel) {
-    if (vel >= R(0)) return weno5_left<R, ADV>(F(c - 2, dj, dk), F(c - 1, dj, dk), F(c, dj, dk), F(c + 1, dj, dk), F(c + 2, dj, dk));
-    return weno5_left<R, ADV>(F(c + 3, dj, dk), F(c + 2, dj, dk), F(c + 1, dj, dk), F(c, dj, dk), F(c - 1, dj, dk));
+    return weno_upwind<R, ADV>(vel >= R(0), F(c - 2, dj, dk), F(c - 1, dj, dk), F(c, dj, dk), F(c + 1, dj, dk),
+                               F(c + 2, dj, dk), F(c + 3, dj, dk));
 }
 template <typename R, int ADV, class A>
 __device__ __forceinline__ R face_y(const A& F, int di, int c, int dk, R vel) {
-    if (vel >= R(0)) return weno5_left<R, ADV>(F(di, c - 2, dk), F(di, c - 1, dk), F(di, c, dk), F(di, c + 1, dk), F(di, c + 2, dk));
-    return weno5_left<R, ADV>(F(di, c + 3, dk), F(di, c + 2, dk), F(di, c + 1, dk), F(di, c, dk), F(di, c - 1, dk));
+    return weno_upwind<R, ADV>(vel >= R(0), F(di, c - 2, dk), F(di, c - 1, dk), F(di, c, dk), F(di, c + 1, dk),
+                               F(di, c + 2, dk), F(di, c + 3, dk));
 }
 template <typename R, int ADV, class A>
 __device__ __forceinline__ R face_z(const A& F, int di, int dj, int c, R vel) {
-    if (vel >= R(0)) return weno5_left<R, ADV>(F(di, dj, c - 2), F(di, dj, c - 1), F(di, dj, c), F(di, dj, c + 1), F(di, dj, c + 2));
-    return weno5_left<R, ADV>(F(di, dj, c + 3), F(di, dj, c + 2), F(di, dj, c + 1), F(di, dj, c), F(di, dj, c - 1));
+    return weno_upwind<R, ADV>(vel >= R(0), F(di, dj, c - 2), F(di, dj, c - 1), F(di, dj, c), F(di, dj, c + 1),
+                               F(di, dj, c + 2), F(di, dj, c + 3));
 }
+
+// The z fluxes of the WENO forms at the top face of a level are the bottom
+// fluxes of the level above (same velocities, same stencil values): a
+// thread marching up a column carries them instead of recomputing them.
+template <typename VT>
+struct ZCarry {
+    VT f[4];     // w-weighted top-face fluxes of u, v, w, theta
+    bool valid;  // f holds the bottom fluxes of this level
+};
 
 // ---- the tendency at one point ------------------------------------------------
 // U, V, W, T, N are accessors (di, dj, dk) -> value around the point at level
@@ -114,7 +139,7 @@ template <typename R, int ADV, bool SGS, bool ANEL, bool UNI, class AU, class AV
           typename VT>
 __device__ __forceinline__ void sweep_point(const Met<R, UNI>& m, const SweepArgs<R>& a, const Geo& g, int k,
                                             const AU& U, const AV& V, const AW& W, const AT& T, const AN& N, VT& tu,
-                                            VT& tv, VT& tw, VT& tt) {
+                                            VT& tv, VT& tw, VT& tt, ZCarry<VT>* zc = nullptr) {
     const VT idx = VT(g.idx), idy = VT(g.idy), idx2 = VT(g.idx2), idy2 = VT(g.idy2);
     const VT h = VT(0.5);
 
@@ -211,7 +236,10 @@ __device__ __forceinline__ void sweep_point(const Met<R, UNI>& m, const SweepArg
             VT Vn = (V(-1, 1, 0) + V(0, 1, 0)) / VT(2), Vs = (V(-1, 0, 0) + V(0, 0, 0)) / VT(2);
             VT dy = (Vn * face_y<VT, ADV>(U, 0, 0, 0, Vn) - Vs * face_y<VT, ADV>(U, 0, -1, 0, Vs)) * idy;
             VT Wt = (W(-1, 0, 1) + W(0, 0, 1)) / VT(2), Wb = (W(-1, 0, 0) + W(0, 0, 0)) / VT(2);
-            VT dz = (Wt * face_z<VT, ADV>(U, 0, 0, 0, Wt) - Wb * face_z<VT, ADV>(U, 0, 0, -1, Wb)) * idz;
+            const VT ft = Wt * face_z<VT, ADV>(U, 0, 0, 0, Wt);
+            const VT fb = (zc && zc->valid) ? zc->f[0] : VT(Wb * face_z<VT, ADV>(U, 0, 0, -1, Wb));
+            if (zc) zc->f[0] = ft;
+            VT dz = (ft - fb) * idz;
             tu = VT(0) - (dx + dy + dz);
         }
         {
@@ -220,7 +248,10 @@ __device__ __forceinline__ void sweep_point(const Met<R, UNI>& m, const SweepArg
             VT Vn = (V(0, 0, 0) + V(0, 1, 0)) / VT(2), Vs = (V(0, -1, 0) + V(0, 0, 0)) / VT(2);
             VT dy = (Vn * face_y<VT, ADV>(V, 0, 0, 0, Vn) - Vs * face_y<VT, ADV>(V, 0, -1, 0, Vs)) * idy;
             VT Wt = (W(0, -1, 1) + W(0, 0, 1)) / VT(2), Wb = (W(0, -1, 0) + W(0, 0, 0)) / VT(2);
-            VT dz = (Wt * face_z<VT, ADV>(V, 0, 0, 0, Wt) - Wb * face_z<VT, ADV>(V, 0, 0, -1, Wb)) * idz;
+            const VT ft = Wt * face_z<VT, ADV>(V, 0, 0, 0, Wt);
+            const VT fb = (zc && zc->valid) ? zc->f[1] : VT(Wb * face_z<VT, ADV>(V, 0, 0, -1, Wb));
+            if (zc) zc->f[1] = ft;
+            VT dz = (ft - fb) * idz;
             tv = VT(0) - (dx + dy + dz);
         }
         {
@@ -229,7 +260,10 @@ __device__ __forceinline__ void sweep_point(const Met<R, UNI>& m, const SweepArg
             VT Vn = (V(0, 1, -1) + V(0, 1, 0)) / VT(2), Vs = (V(0, 0, -1) + V(0, 0, 0)) / VT(2);
             VT dy = (Vn * face_y<VT, ADV>(W, 0, 0, 0, Vn) - Vs * face_y<VT, ADV>(W, 0, -1, 0, Vs)) * idy;
             VT Wt = (W(0, 0, 0) + W(0, 0, 1)) / VT(2), Wb = (W(0, 0, -1) + W(0, 0, 0)) / VT(2);
-            VT dz = (Wt * face_z<VT, ADV>(W, 0, 0, 0, Wt) - Wb * face_z<VT, ADV>(W, 0, 0, -1, Wb)) * idz;
+            const VT ft = Wt * face_z<VT, ADV>(W, 0, 0, 0, Wt);
+            const VT fb = (zc && zc->valid) ? zc->f[2] : VT(Wb * face_z<VT, ADV>(W, 0, 0, -1, Wb));
+            if (zc) zc->f[2] = ft;
+            VT dz = (ft - fb) * idz;
             tw = VT(0) - (dx + dy + dz);
         }
         {
@@ -238,7 +272,10 @@ __device__ __forceinline__ void sweep_point(const Met<R, UNI>& m, const SweepArg
             VT vs = V(0, 0, 0), vn = V(0, 1, 0);
             VT Fy = (vn * face_y<VT, ADV>(T, 0, 0, 0, vn) - vs * face_y<VT, ADV>(T, 0, -1, 0, vs)) * idy;
             VT wb = W(0, 0, 0), wt = W(0, 0, 1);
-            VT Fz = (wt * face_z<VT, ADV>(T, 0, 0, 0, wt) - wb * face_z<VT, ADV>(T, 0, 0, -1, wb)) * idz;
+            const VT ft = wt * face_z<VT, ADV>(T, 0, 0, 0, wt);
+            const VT fb = (zc && zc->valid) ? zc->f[3] : VT(wb * face_z<VT, ADV>(T, 0, 0, -1, wb));
+            if (zc) zc->f[3] = ft;
+            VT Fz = (ft - fb) * idz;
             tt = VT(0) - (Fx + Fy + Fz);
         }
     }

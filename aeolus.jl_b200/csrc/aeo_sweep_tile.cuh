@@ -159,6 +159,8 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
 
     const R dt = R(__ldg(a.dtp));
     const int vbase = (ty + S::HH) * S::PW + (tx + 4);
+    ZCarry<R> zc;   // the WENO z fluxes carried up the column
+    zc.valid = false;
     bool failed = false;
     for (int k = kbeg; k < kend; ++k) {
         // the levels this iteration needs
@@ -232,7 +234,8 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
 
         if (active) {
             R tu, tv, tw, tt;
-            sweep_point<R, ADV, SGS, ANEL, UNI>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt);
+            sweep_point<R, ADV, SGS, ANEL, UNI>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt, ADV ? &zc : nullptr);
+            zc.valid = true;
             const long long qi = iidx(g, i, j, k), q = pidx(g, i, j, k);
             a.us[qi] = U(0, 0, 0) + dt * tu;
             a.vs[qi] = V(0, 0, 0) + dt * tv;
