@@ -129,14 +129,48 @@ struct ZCarry {
     bool valid;  // f holds the bottom fluxes of this level
 };
 
+// The WENO advective fluxes of field f (0 u, 1 v, 2 w, 3 theta) through the
+// west x-face, the south y-face and the top z-face of the point the
+// accessors are centred on (src/AdvectionSchemes.jl:1203-1256): the
+// advecting velocity interpolated to the face times the upwinded face value.
+// F is the accessor of field f itself.
+template <typename R, int ADV, class AU, class AF>
+__device__ __forceinline__ R weno_xflux(int f, const AU& U, const AF& F) {
+    R vel;
+    if (f == 0) vel = (U(-1, 0, 0) + U(0, 0, 0)) / R(2);
+    else if (f == 1) vel = (U(0, -1, 0) + U(0, 0, 0)) / R(2);
+    else if (f == 2) vel = (U(0, 0, -1) + U(0, 0, 0)) / R(2);
+    else vel = U(0, 0, 0);
+    return vel * face_x<R, ADV>(F, -1, 0, 0, vel);
+}
+template <typename R, int ADV, class AV, class AF>
+__device__ __forceinline__ R weno_yflux(int f, const AV& V, const AF& F) {
+    R vel;
+    if (f == 0) vel = (V(-1, 0, 0) + V(0, 0, 0)) / R(2);
+    else if (f == 1) vel = (V(0, -1, 0) + V(0, 0, 0)) / R(2);
+    else if (f == 2) vel = (V(0, 0, -1) + V(0, 0, 0)) / R(2);
+    else vel = V(0, 0, 0);
+    return vel * face_y<R, ADV>(F, 0, -1, 0, vel);
+}
+// S = 0: the top z-face; S = -1: the bottom one (the top face one level down)
+template <typename R, int ADV, int S, class AW, class AF>
+__device__ __forceinline__ R weno_zflux(int f, const AW& W, const AF& F) {
+    R vel;
+    if (f == 0) vel = (W(-1, 0, 1 + S) + W(0, 0, 1 + S)) / R(2);
+    else if (f == 1) vel = (W(0, -1, 1 + S) + W(0, 0, 1 + S)) / R(2);
+    else if (f == 2) vel = (W(0, 0, S) + W(0, 0, 1 + S)) / R(2);
+    else vel = W(0, 0, 1 + S);
+    return vel * face_z<R, ADV>(F, 0, 0, S, vel);
+}
+
 // ---- the tendency at one point ------------------------------------------------
 // U, V, W, T, N are accessors (di, dj, dk) -> value around the point at level
 // k; the same arithmetic serves the direct form (global memory) and the
 // tiled form (shared-memory planes).  VT is the value type: R, or a pair of
 // FP32 lanes (F2) for two x-adjacent cells of the paired sweep (the
 // centred forms only).
-template <typename R, int ADV, bool SGS, bool ANEL, bool UNI, class AU, class AV, class AW, class AT, class AN,
-          typename VT>
+template <typename R, int ADV, bool SGS, bool ANEL, bool UNI, bool EXT = false, class AU, class AV, class AW,
+          class AT, class AN, typename VT>
 __device__ __forceinline__ void sweep_point(const Met<R, UNI>& m, const SweepArgs<R>& a, const Geo& g, int k,
                                             const AU& U, const AV& V, const AW& W, const AT& T, const AN& N, VT& tu,
                                             VT& tv, VT& tw, VT& tt, ZCarry<VT>* zc = nullptr) {
@@ -227,8 +261,9 @@ __device__ __forceinline__ void sweep_point(const Met<R, UNI>& m, const SweepArg
             VT wt = W(0, 0, 1) * h * (T(0, 0, 0) + T(0, 0, 1)), wb = W(0, 0, 0) * h * (T(0, 0, -1) + T(0, 0, 0));
             tt = VT(0) - ((ue - uw) * idx + (vn - vs) * idy + (wt - wb) * m.idz(k));
         }
-    } else {
-        // WENO flux forms on a uniform grid (src/AdvectionSchemes.jl:685-699, :1203-1256)
+    } else if constexpr (!EXT) {
+        // WENO flux forms on a uniform grid (src/AdvectionSchemes.jl:685-699, :1203-1256);
+        // EXT: the caller computed them (face fluxes shared between cells) into tu..tt
         const VT idz = VT(g.idz);
         {
             VT Ue = (U(0, 0, 0) + U(1, 0, 0)) / VT(2), Uw = (U(-1, 0, 0) + U(0, 0, 0)) / VT(2);

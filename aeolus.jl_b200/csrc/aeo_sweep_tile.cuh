@@ -71,13 +71,24 @@ struct TileShape {
     static constexpr int NPW = TX + 2, NPH = TY + 2, NPS = NPW * NPH;  // nut plane with halo 1
     static constexpr size_t PLANES_BYTES = (size_t)NS * 4 * PSZA * sizeof(R);
     static constexpr size_t NUT_BYTES = SGS ? (((size_t)3 * NPS * sizeof(R) + 127) / 128) * 128 : 0;
+    // WENO in FP64: the x- and y-face fluxes of the level's tile, [4][TY][TX+1] and
+    // [4][TY+1][TX], computed once per face; FP32 reconstructions are cheap
+    // enough that recomputing a face in both cells (straight-line code, no
+    // extra barrier) is faster
+    static constexpr bool SHARE = ADV > 0 && sizeof(R) == 8;
+    static constexpr int FXN = TY * (TX + 1), FYN = (TY + 1) * TX;
+    static constexpr int FPF = 576;                      // face entries per field: x 264 padded to 288, y 288
+    static constexpr size_t FLUX_BYTES = SHARE ? (((size_t)4 * (FXN + FYN) * sizeof(R) + 127) / 128) * 128 : 0;
     static constexpr size_t BAR_BYTES = 128;
     static_assert(NS * 8 <= (int)BAR_BYTES, "mbarrier block");
     static_assert(TX == 32 && NPS == TX * NPH + 2 * NPH, "the eddy-viscosity loop maps warps to 32-column rows");
     // + the chunk's per-level factors, LV_N rows of NLT (a chunk has at most
     // KCH levels), + alignment slack
     static constexpr int KCH = 32, NLT = KCH + 2 * AEO_LH;
-    static constexpr size_t SMEM = PLANES_BYTES + NUT_BYTES + BAR_BYTES + (size_t)LV_N * NLT * sizeof(R) + 128;
+    static constexpr size_t SMEM =
+        PLANES_BYTES + NUT_BYTES + FLUX_BYTES + BAR_BYTES + (size_t)LV_N * NLT * sizeof(R) + 128;
+    static_assert(!ADV || (FPF % 32 == 0 && FXN <= FPF / 2 && FYN == FPF / 2 && (4 * FPF) % NT == 0),
+                  "one field per warp in the face phase");
 };
 
 struct TileMaps {
@@ -91,6 +102,14 @@ template <typename R, int ZL, int PW, int FOFS>
 struct SmAcc {
     const R* const* lp;
     __device__ __forceinline__ R operator()(int di, int dj, int dk) const { return lp[dk + ZL][FOFS + dj * PW + di]; }
+};
+
+// the same with the field offset a (warp-uniform) runtime value
+template <typename R, int ZL, int PW>
+struct SmAccF {
+    const R* const* lp;
+    int fofs;
+    __device__ __forceinline__ R operator()(int di, int dj, int dk) const { return lp[dk + ZL][fofs + dj * PW + di]; }
 };
 
 template <typename R, int NPW>
@@ -109,8 +128,10 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
     unsigned char* sbase = smem_tile + ((128u - (smem_u32(smem_tile) & 127u)) & 127u);
     R* planes = reinterpret_cast<R*>(sbase);
     R* nutp = reinterpret_cast<R*>(sbase + S::PLANES_BYTES);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + S::PLANES_BYTES + S::NUT_BYTES);
-    R* lvs = reinterpret_cast<R*>(sbase + S::PLANES_BYTES + S::NUT_BYTES + S::BAR_BYTES);
+    R* fxs = reinterpret_cast<R*>(sbase + S::PLANES_BYTES + S::NUT_BYTES);   // WENO face fluxes
+    R* fys = fxs + 4 * S::FXN;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + S::PLANES_BYTES + S::NUT_BYTES + S::FLUX_BYTES);
+    R* lvs = reinterpret_cast<R*>(sbase + S::PLANES_BYTES + S::NUT_BYTES + S::FLUX_BYTES + S::BAR_BYTES);
 
     const Geo& g = a.g;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + S::TX * ty;
@@ -232,10 +253,65 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
             N.p[0] = N.p[1] = N.p[2] = nutp;
         }
 
+        R tu, tv, tw, tt;
+        if constexpr (S::SHARE) {
+            // face phase: every x- and y-face flux of the tile once (a face is
+            // shared by the two cells beside it); one field per warp
+            const R* lp0[S::NW];
+#pragma unroll
+            for (int d = 0; d < S::NW; ++d) lp0[d] = plane(k - S::ZL + d);
+#pragma unroll 3
+            for (int q = 0; q < 4 * S::FPF / S::NT; ++q) {
+                // branch-free: an x face and a y face differ only in the stencil
+                // stride and the advecting field (u or v); the second velocity
+                // point depends on the field only (f is warp-uniform, so is isx)
+                const int e = tid + q * S::NT;
+                const int f = e / S::FPF, r = e - f * S::FPF;
+                const bool isx = r < S::FPF / 2;
+                int rr = isx ? r : r - S::FPF / 2;
+                const bool valid = !isx || rr < S::FXN;
+                rr = valid ? rr : 0;
+                const int fjx = rr / (S::TX + 1), fjy = rr / S::TX;
+                const int fj = isx ? fjx : fjy;
+                const int fi = isx ? rr - fjx * (S::TX + 1) : rr - fjy * S::TX;
+                const int fb = (fj + S::HH) * S::PW + (fi + 4);
+                const int st = isx ? 1 : S::PW;
+                const int vofs = isx ? 0 : S::PSZA;
+                const R* p0 = lp0[S::ZL] + fb;
+                const R* p1 = (f == 2 ? lp0[S::ZL - 1] : lp0[S::ZL]) + fb + vofs + (f == 0 ? -1 : (f == 1 ? -S::PW : 0));
+                const R a0 = p0[vofs], a1 = *p1;
+                const R vel = f == 3 ? a0 : (a1 + a0) / R(2);
+                const R* pf = p0 + f * S::PSZA;
+                const R flux = vel * weno_upwind<R, ADV>(vel >= R(0), pf[-3 * st], pf[-2 * st], pf[-st], pf[0], pf[st],
+                                                        pf[2 * st]);
+                if (valid) {
+                    if (isx) fxs[f * S::FXN + fj * (S::TX + 1) + fi] = flux;
+                    else fys[f * S::FYN + fj * S::TX + fi] = flux;
+                }
+            }
+            __syncthreads();
+            if (active) {
+                // cell phase: differences of the shared fluxes, the z fluxes carried up the column
+                const R idx = R(g.idx), idy = R(g.idy), idz = R(g.idz);
+                R adv[4];
+#pragma unroll
+                for (int f = 0; f < 4; ++f) {
+                    const SmAccF<R, S::ZL, S::PW> F{lp, f * S::PSZA};
+                    const R ft = weno_zflux<R, ADV, 0>(f, W, F);
+                    const R fb = zc.valid ? zc.f[f] : weno_zflux<R, ADV, -1>(f, W, F);
+                    zc.f[f] = ft;
+                    const R* fx = fxs + f * S::FXN + ty * (S::TX + 1) + tx;
+                    const R* fy = fys + f * S::FYN + ty * S::TX + tx;
+                    adv[f] = R(0) - ((fx[1] - fx[0]) * idx + (fy[S::TX] - fy[0]) * idy + (ft - fb) * idz);
+                }
+                zc.valid = true;
+                tu = adv[0]; tv = adv[1]; tw = adv[2]; tt = adv[3];
+            }
+        }
         if (active) {
-            R tu, tv, tw, tt;
-            sweep_point<R, ADV, SGS, ANEL, UNI>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt, ADV ? &zc : nullptr);
-            zc.valid = true;
+            sweep_point<R, ADV, SGS, ANEL, UNI, S::SHARE>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt,
+                                                          (ADV > 0 && !S::SHARE) ? &zc : nullptr);
+            if (ADV > 0 && !S::SHARE) zc.valid = true;
             const long long qi = iidx(g, i, j, k), q = pidx(g, i, j, k);
             a.us[qi] = U(0, 0, 0) + dt * tu;
             a.vs[qi] = V(0, 0, 0) + dt * tv;
