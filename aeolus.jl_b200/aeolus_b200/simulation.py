@@ -189,6 +189,37 @@ class Simulation:
         _lib.check(self._lib.aeo_pressure_solve(self._h, _ptr(s), _ptr(out)), self._h)
         return out
 
+    # ---- the PCG pressure solver (solver="pcg") --------------------------------
+    def set_pcg(self, apertures=None, tol: float = 1e-8, maxit: int = 200):
+        """The cut-cell face apertures (ax, ay, az) of shapes (nz, ny, nx+1),
+        (nz, ny+1, nx), (nz+1, ny, nx) in [0, 1] (None: every face open) and
+        the CG tolerance / iteration cap of every projection's solve."""
+        g = self.grid
+        if apertures is None:
+            _lib.check(self._lib.aeo_set_pcg(self._h, None, None, None, float(tol), int(maxit)), self._h)
+            return
+        ax, ay, az = (np.ascontiguousarray(a, dtype=np.float64) for a in apertures)
+        if ax.shape != (g.nz, g.ny, g.nx + 1) or ay.shape != (g.nz, g.ny + 1, g.nx) or az.shape != (g.nz + 1, g.ny, g.nx):
+            raise ValueError("apertures must be (nz, ny, nx+1), (nz, ny+1, nx), (nz+1, ny, nx)")
+        self._apertures = (ax, ay, az)
+        _lib.check(self._lib.aeo_set_pcg(self._h, _ptr(ax), _ptr(ay), _ptr(az), float(tol), int(maxit)), self._h)
+
+    def pcg_stats(self) -> dict:
+        """The last projection's solve: iterations, status, ||r||, ||b||."""
+        it, stt = C.c_int32(), C.c_int32()
+        r, b = C.c_double(), C.c_double()
+        _lib.check(self._lib.aeo_pcg_stats(self._h, C.byref(it), C.byref(stt), C.byref(r), C.byref(b)), self._h)
+        from .multigrid import STATUS
+        return {"iterations": it.value, "status": STATUS.get(stt.value, stt.value), "residual": r.value,
+                "bnorm": b.value, "relative_residual": r.value / b.value if b.value > 0 else 0.0}
+
+    def set_learned(self, net=None, stagnation: float = 0.9):
+        """The learned U-Net preconditioner of every projection's solve (None:
+        back to the multigrid cycle); kept alive by this object."""
+        self._net = net
+        _lib.check(self._lib.aeo_pcg_set_learned(self._h, net.handle if net is not None else None, float(stagnation)),
+                   self._h)
+
     def kinetic_energy(self) -> float:
         v = C.c_double()
         _lib.check(self._lib.aeo_kinetic_energy(self._h, C.byref(v)), self._h)

@@ -16,7 +16,7 @@ from .grids import PERIODIC, WALL, Grid
 
 CORES = {"boussinesq": 0, "anelastic": 1}
 ADVECTION = {"centred": 0, "weno_js5": 1, "weno_z5": 2}
-SOLVERS = {"fft": 0, "column": 1}
+SOLVERS = {"fft": 0, "column": 1, "pcg": 2}
 PRECISIONS = {"fp64": 0, "fp32_mixed": 1}
 FIELDS = {"u": 0, "v": 1, "w": 2, "theta": 3, "p": 4, "nut": 5}
 
@@ -54,6 +54,8 @@ class CoreSpec:
             self.solver = "fft" if self.grid.bc_z == PERIODIC else "column"
         if self.solver not in SOLVERS:
             raise ValueError(f"solver must be one of {list(SOLVERS)}, got {self.solver!r}")
+        if self.solver == "pcg" and (self.core != "boussinesq" or self.grid.stretched):
+            raise ValueError("the PCG pressure solver projects a Boussinesq domain of uniform spacing")
         if self.sponge_zstart is None:
             self.sponge_zstart = self.grid.origin[2] + self.grid.extent[2]
         if self.core == "anelastic":

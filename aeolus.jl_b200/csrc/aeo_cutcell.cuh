@@ -1,0 +1,128 @@
+// aeo_cutcell.cuh -- the projection of the stepping engine with the
+// multigrid-preconditioned CG pressure solver (solver = AEO_SOLVER_PCG) on
+// cut-cell face apertures.
+//
+// With apertures a in [0, 1] on every face (a = 0: blocked), the projection
+// solves A phi = b with
+//   b        = sum over the cell's faces of (+-) a u* / h   (the aperture-weighted divergence),
+//   A phi    = sum over the cell's faces of a^2 (phi_nbr - phi) / h^2,
+// the a^2-weighted Laplacian of the MG-PCG handle, and corrects
+//   u = u* - a (phi+ - phi-) / h    on every face,
+// so that the aperture-weighted divergence of u is A phi - b = 0 to the
+// solve's tolerance, and the velocity of a blocked face is zero after every
+// projection (apply_cutcell_velocity_bc!, src/CutCell.jl:852-880).  b is
+// cutcell_divergence! times vol_eff (the symmetric right-hand side) and the
+// correction is cutcell_gradient_x/y/z! (src/CutCell.jl:602-700); with every
+// aperture 1 this is the projection of MGPreconditionedCG as the Boussinesq
+// pressure solver (the urban :mg_cg slot, src/components/urban/pressure_solver.jl:126).
+//
+// Apertures live in the face layout of aeolus_b200_mgpcg.h: ax (nx+1) per
+// row, ay (ny+1) rows per level, az (nz+1) levels; face index i is the west
+// (south, bottom) face of cell i.
+#pragma once
+
+#include "aeo_common.cuh"
+
+// b = the aperture-weighted divergence of (u*, v*, w*) (interior arrays), in FP64
+template <typename R>
+__global__ void __launch_bounds__(256) cc_div_kernel(Geo g, const R* __restrict__ us, const R* __restrict__ vs,
+                                                     const R* __restrict__ ws, const R* __restrict__ ax,
+                                                     const R* __restrict__ ay, const R* __restrict__ az,
+                                                     double* __restrict__ b) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.nin) return;
+    const int lnx = __ffs(g.nx) - 1, lny = __ffs(g.ny) - 1;
+    const int i = (int)(q & (g.nx - 1)), j = (int)((q >> lnx) & (g.ny - 1)), k = (int)(q >> (lnx + lny));
+    const long long pl = (long long)g.nx * g.ny;
+    const long long xr = (long long)(g.nx + 1) * (j + (long long)g.ny * k);
+    const long long yr = (long long)g.nx * (j + (long long)(g.ny + 1) * k);
+    const R aw = ax[xr + i], ae = ax[xr + i + 1];
+    const R as = ay[yr + i], an = ay[yr + g.nx + i];
+    const R ab = az[q], at = az[q + pl];
+    const R uw = us[q], ue = us[i + 1 < g.nx ? q + 1 : q + 1 - g.nx];
+    const R vsv = vs[q], vn = vs[j + 1 < g.ny ? q + g.nx : q - (long long)(g.ny - 1) * g.nx];
+    const R wb = ws[q];
+    const R wt = k + 1 < g.nz ? ws[q + pl] : (g.bc_z == 0 ? ws[q - (long long)(g.nz - 1) * pl] : R(0));
+    // in FP64 whatever R is: a fluid region the obstacles seal off from the rest
+    // adds a null space whose right-hand side sums to zero only to the
+    // rounding of this sum, and CG drifts along it unless that rounding is FP64's
+    b[q] = ((double)ae * ue - (double)aw * uw) * g.idx + ((double)an * vn - (double)as * vsv) * g.idy +
+           ((double)at * wt - (double)ab * wb) * g.idz;
+}
+
+// u = c(u* - a d(phi), u^n) on every face (0 on a blocked one), p = phi/dt;
+// c(x, s) = ca*s + cb*x in RK3 stages 2 and 3 (as correct_kernel)
+template <typename R>
+__global__ void __launch_bounds__(256) cc_correct_kernel(Geo g, const R* __restrict__ us, const R* __restrict__ vs,
+                                                         const R* __restrict__ ws, const double* __restrict__ phi,
+                                                         const R* __restrict__ ax, const R* __restrict__ ay,
+                                                         const R* __restrict__ az, const R* u0, const R* v0,
+                                                         const R* w0, R* uo, R* vo, R* wo, R* __restrict__ p,
+                                                         const double* __restrict__ dtp, R ca, R cb, int stage) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.nin) return;
+    const int lnx = __ffs(g.nx) - 1, lny = __ffs(g.ny) - 1;
+    const int i = (int)(q & (g.nx - 1)), j = (int)((q >> lnx) & (g.ny - 1)), k = (int)(q >> (lnx + lny));
+    const long long pl = (long long)g.nx * g.ny;
+    const double pc = phi[q];
+    const double pw = phi[i > 0 ? q - 1 : q + g.nx - 1];
+    const double ps = phi[j > 0 ? q - g.nx : q + (long long)(g.ny - 1) * g.nx];
+    // k - 1 = -1: periodic wrap, or the wall mirror (the bottom face is blocked there)
+    const double pb = phi[k > 0 ? q - pl : (g.bc_z == 0 ? q + (long long)(g.nz - 1) * pl : q)];
+    const R aw = ax[(long long)(g.nx + 1) * (j + (long long)g.ny * k) + i];
+    const R as = ay[(long long)g.nx * (j + (long long)(g.ny + 1) * k) + i];
+    const R ab = az[q];
+    R un = aw > R(0) ? us[q] - aw * R((pc - pw) * g.idx) : R(0);
+    R vn = as > R(0) ? vs[q] - as * R((pc - ps) * g.idy) : R(0);
+    R wn = ab > R(0) ? ws[q] - ab * R((pc - pb) * g.idz) : R(0);
+    const long long qp = pidx(g, i, j, k);
+    if (stage) {
+        un = ca * u0[qp] + cb * un;
+        vn = ca * v0[qp] + cb * vn;
+        wn = ca * w0[qp] + cb * wn;
+    }
+    uo[qp] = un;
+    vo[qp] = vn;
+    wo[qp] = wn;
+    p[q] = R(pc / __ldg(dtp));   // p = phi/dt (_DivBy, src/Simulations.jl:1207-1211)
+}
+
+// y[i] = x[i] in FP64 (the seam-2 source into the solver's right-hand side)
+template <typename R>
+__global__ void to_f64_kernel(long long n, const R* __restrict__ x, double* __restrict__ y) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) y[q] = (double)x[q];
+}
+template <typename R>
+__global__ void from_f64_kernel(long long n, const double* __restrict__ x, R* __restrict__ y) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) y[q] = R(x[q]);
+}
+
+// per level: max |aperture-weighted divergence| of the padded state (halos filled)
+template <typename R>
+__global__ void __launch_bounds__(256) cc_maxdiv_levels_kernel(Geo g, const R* __restrict__ u,
+                                                               const R* __restrict__ v, const R* __restrict__ w,
+                                                               const R* __restrict__ ax, const R* __restrict__ ay,
+                                                               const R* __restrict__ az, double* __restrict__ part) {
+    __shared__ double red[256];
+    const int k = blockIdx.x;
+    double acc = 0.0;
+    for (int e = threadIdx.x; e < g.nx * g.ny; e += blockDim.x) {
+        const int i = e % g.nx, j = e / g.nx;
+        const long long q = pidx(g, i, j, k), qi = iidx(g, i, j, k);
+        const long long xr = (long long)(g.nx + 1) * (j + (long long)g.ny * k);
+        const long long yr = (long long)g.nx * (j + (long long)(g.ny + 1) * k);
+        const double du = ((double)ax[xr + i + 1] * (double)u[q + 1] - (double)ax[xr + i] * (double)u[q]) * g.idx;
+        const double dv = ((double)ay[yr + g.nx + i] * (double)v[q + g.sy] - (double)ay[yr + i] * (double)v[q]) * g.idy;
+        const double dw = ((double)az[qi + (long long)g.nx * g.ny] * (double)w[q + g.sz] - (double)az[qi] * (double)w[q]) * g.idz;
+        acc = fmax(acc, fabs(du + dv + dw));
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[k] = red[0];
+}

@@ -1,0 +1,14 @@
+// aeo_mg_internal.h -- the multigrid-preconditioned CG handle as the pressure
+// solver of the stepping engine (C++ linkage, not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/aeolus_b200_mgpcg.h"
+
+// the handle's device right-hand side b and solution x (nx*ny*nz FP64 each)
+aeo_status aeo_mg_buffers(aeo_mg* h, double** b, double** x);
+// x = A^-1 b (zero first guess), enqueued on s: no host synchronisation
+aeo_status aeo_mg_launch(aeo_mg* h, cudaStream_t s);
+// the statistics of the last solve (synchronises the device)
+aeo_status aeo_mg_read_stats(aeo_mg* h, aeo_mg_stats* o);

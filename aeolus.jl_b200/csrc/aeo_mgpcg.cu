@@ -86,6 +86,11 @@ struct MgBase {
     virtual aeo_status set_learned(aeo_unet* net, double stag) = 0;
     virtual aeo_status harvest(const double* b, double* x, aeo_mg_stats* st, double* rh, double* xh, int cap,
                                int* count) = 0;
+    // the stepping engine's use: the device right-hand side and solution
+    // buffers, the solve enqueued on the caller's stream, the last statistics
+    virtual void buffers(double** b, double** x) = 0;
+    virtual aeo_status launch_on(cudaStream_t s) = 0;
+    virtual aeo_status last_stats(aeo_mg_stats* o) = 0;
 };
 
 #define CK(call)                                                                         \
@@ -202,6 +207,7 @@ struct Mg : MgBase {
     double* bmeans = nullptr;      // one device scalar per level
     PcgState* S = nullptr;
     PcgState* hS = nullptr;        // pinned host copy
+    cudaEvent_t ev_own = nullptr;  // orders this handle's stream before a launch on another
     int* dzero = nullptr;          // a device flag that stays 0 (kernels run outside a solve)
     int coarse_staged = 0;
     int coarse_inplace = 1;        // 0 when a periodic axis of the coarsest level has an odd length
@@ -223,6 +229,7 @@ struct Mg : MgBase {
         if (hist_x) cudaFree(hist_x);
         if (hist_r) cudaFree(hist_r);
         if (hS) cudaFreeHost(hS);
+        if (ev_own) cudaEventDestroy(ev_own);
         if (st) cudaStreamDestroy(st);
         if (st_body) cudaStreamDestroy(st_body);
         for (cudaStream_t b_ : st_br)
@@ -723,6 +730,31 @@ struct Mg : MgBase {
         return AEO_OK;
     }
 
+    void buffers(double** bo, double** xo) override {
+        *bo = b;
+        *xo = x;
+    }
+    // x = A^-1 b from the rhs buffer into the solution buffer, ordered on s
+    // (the graph is captured once on this handle's stream; a graph launch
+    // runs on any stream)
+    aeo_status launch_on(cudaStream_t s) override {
+        if (!g_solve)
+            if (aeo_status q = build_solve()) return q;
+        if (s != st) {
+            // everything this handle queued on its own stream (set-up, the
+            // coarsest map, weight changes) precedes the solve on s
+            if (!ev_own) CK(cudaEventCreateWithFlags(&ev_own, cudaEventDisableTiming));
+            CK(cudaEventRecord(ev_own, st));
+            CK(cudaStreamWaitEvent(s, ev_own, 0));
+        }
+        CK(cudaGraphLaunch(g_solve, s));
+        return AEO_OK;
+    }
+    aeo_status last_stats(aeo_mg_stats* o) override {
+        CK(cudaDeviceSynchronize());
+        return stats_out(o, false);
+    }
+
     aeo_status solve(const double* bin, double* xout, bool device, aeo_mg_stats* o) override {
         if (!g_solve)
             if (aeo_status s = build_solve()) return s;
@@ -1053,3 +1085,18 @@ aeo_status aeo_mg_solve_harvest(aeo_mg* h, const double* b, double* x, aeo_mg_st
 const char* aeo_mg_last_error(const aeo_mg* h) { return h ? h->core->err.c_str() : g_mg_error.c_str(); }
 
 }  // extern "C"
+
+// ---- internal (C++ linkage) entry points of the stepping engine (aeolus_b200.cu)
+aeo_status aeo_mg_buffers(aeo_mg* h, double** b, double** x) {
+    if (!h || !b || !x) return AEO_ERR_ARGUMENT;
+    h->core->buffers(b, x);
+    return AEO_OK;
+}
+aeo_status aeo_mg_launch(aeo_mg* h, cudaStream_t s) {
+    if (!h) return AEO_ERR_ARGUMENT;
+    return h->core->launch_on(s);
+}
+aeo_status aeo_mg_read_stats(aeo_mg* h, aeo_mg_stats* o) {
+    if (!h || !o) return AEO_ERR_ARGUMENT;
+    return h->core->last_stats(o);
+}

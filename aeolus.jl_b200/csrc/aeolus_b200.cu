@@ -32,7 +32,9 @@
 
 #include "../../include/aeolus_b200.h"
 #include "aeo_adapt.cuh"
+#include "aeo_mg_internal.h"
 #include "aeo_common.cuh"
+#include "aeo_cutcell.cuh"
 #include "aeo_fft.cuh"
 #include "aeo_init.cuh"
 #include "aeo_misc.cuh"
@@ -93,6 +95,9 @@ struct CoreBase {
     virtual aeo_status profile_step(double dt, double* ms, int ncls) = 0;
     virtual aeo_status init_isotropic(double u_rms, double k_peak, uint64_t seed, double kmax, int proj,
                                       double target_rms) = 0;
+    virtual aeo_status set_pcg(const double* ax, const double* ay, const double* az, double tol, int maxit) = 0;
+    virtual aeo_status pcg_stats(aeo_mg_stats* o) = 0;
+    virtual aeo_status pcg_set_learned(aeo_unet* net, double stagnation) = 0;
 };
 
 struct aeo_sim {
@@ -120,6 +125,14 @@ struct Core : CoreBase {
     double* cps = nullptr;     // the column solve's c' scratch (spectrum layout)
     cplx<R>* tw = nullptr;
     int NT = 0;
+    // solver = AEO_SOLVER_PCG: the MG-PCG handle (a^2 faces), its device rhs and
+    // solution, and the face apertures (aeo_cutcell.cuh)
+    bool pcg = false;
+    aeo_mg* mg = nullptr;
+    double *mg_b = nullptr, *mg_x = nullptr;
+    R *apx = nullptr, *apy = nullptr, *apz = nullptr;
+    double pcg_tol = 1e-8;
+    int pcg_maxit = 200;
     double* d_stage = nullptr; // host-layout staging (device)
     long long host_n = 0;
     double* d_part = nullptr;  // per-level partials (4 per level)
@@ -144,7 +157,9 @@ struct Core : CoreBase {
     }
 
     ~Core() override {
+        if (st) cudaStreamSynchronize(st);   // solves of the MG-PCG handle may be in flight on st
         drop_graphs();
+        if (mg) aeo_mg_destroy(mg);
         for (void* p : allocs) cudaFree(p);
         if (st) cudaStreamDestroy(st);
     }
@@ -383,6 +398,13 @@ struct Core : CoreBase {
             else if (aeo_status e = alloc(&dsc, ns)) return e;
             if (aeo_status e = alloc(&cps, ns)) return e;
         }
+        if (c.solver == AEO_SOLVER_PCG) {
+            pcg = true;
+            if (aeo_status e = alloc(&apx, (size_t)(Nx + 1) * Ny * Nz)) return e;
+            if (aeo_status e = alloc(&apy, (size_t)Nx * (Ny + 1) * Nz)) return e;
+            if (aeo_status e = alloc(&apz, (size_t)Nx * Ny * (Nz + 1))) return e;
+            if (aeo_status e = make_pcg(nullptr, nullptr, nullptr)) return e;
+        }
         host_n = (long long)(c.nx + 2 * c.hx) * (c.ny + 2 * c.hy) * (c.nz + 2 * c.hz);
         if (aeo_status e = alloc(&d_stage, std::max<long long>(host_n, g.nin))) return e;
         if (aeo_status e = alloc(&d_part, 4 * (size_t)(Nz + 1))) return e;
@@ -394,6 +416,86 @@ struct Core : CoreBase {
         kchunk = std::min(g.nz, TileShape<R, 0, false>::KCH);
         CK(cudaStreamSynchronize(st));
         launches = 3 * 9;
+        return AEO_OK;
+    }
+
+    // The apertures (host FP64 in the face layout of aeolus_b200_mgpcg.h, NULL:
+    // every face open; the wall faces of a bounded z are blocked whatever is
+    // given), their device copies, and the MG-PCG handle of the a^2 operator.
+    aeo_status make_pcg(const double* axh, const double* ayh, const double* azh) {
+        const int Nx = g.nx, Ny = g.ny, Nz = g.nz;
+        const size_t n[3] = {(size_t)(Nx + 1) * Ny * Nz, (size_t)Nx * (Ny + 1) * Nz, (size_t)Nx * Ny * (Nz + 1)};
+        const double* src[3] = {axh, ayh, azh};
+        std::vector<double> a[3], c2[3];
+        for (int d = 0; d < 3; ++d) {
+            a[d].assign(n[d], 1.0);
+            if (src[d]) std::copy(src[d], src[d] + n[d], a[d].begin());
+            for (double v : a[d])
+                if (!(v >= 0.0 && v <= 1.0)) { fail("set_pcg: apertures must lie in [0, 1]"); return AEO_ERR_ARGUMENT; }
+        }
+        if (g.bc_z == 1)
+            for (size_t q = 0; q < (size_t)Nx * Ny; ++q) {
+                a[2][q] = 0.0;
+                a[2][(size_t)Nz * Nx * Ny + q] = 0.0;
+            }
+        R* dst[3] = {apx, apy, apz};
+        for (int d = 0; d < 3; ++d) {
+            std::vector<R> ar(n[d]);
+            c2[d].resize(n[d]);
+            for (size_t q = 0; q < n[d]; ++q) {
+                ar[q] = R(a[d][q]);
+                c2[d][q] = a[d][q] * a[d][q];
+            }
+            CK(cudaMemcpyAsync(dst[d], ar.data(), n[d] * sizeof(R), cudaMemcpyHostToDevice, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        aeo_mg_config mc{};
+        mc.nx = Nx; mc.ny = Ny; mc.nz = Nz;
+        mc.dx = g.dx; mc.dy = g.dy; mc.dz = g.dz;
+        mc.bc_x = AEO_MG_PERIODIC; mc.bc_y = AEO_MG_PERIODIC;
+        mc.bc_z = g.bc_z == 1 ? AEO_MG_NEUMANN : AEO_MG_PERIODIC;
+        mc.precision = cfg.precision;
+        mc.precond = AEO_PC_VCYCLE;
+        mc.flexible = cfg.precision == AEO_PREC_FP64 ? 0 : 1;
+        mc.tol = pcg_tol;
+        mc.maxit = pcg_maxit;
+        mc.nu1 = 2; mc.nu2 = 2; mc.coarse_sweeps = 50; mc.min_size = 4;
+        mc.device = cfg.device;
+        CK(cudaStreamSynchronize(st));   // no solve of the old handle in flight
+        if (mg) { aeo_mg_destroy(mg); mg = nullptr; }
+        if (aeo_status e = aeo_mg_create(&mc, c2[0].data(), c2[1].data(), c2[2].data(), &mg)) {
+            fail(std::string("the MG-PCG pressure solver: ") + aeo_mg_last_error(nullptr));
+            return e;
+        }
+        aeo_mg_buffers(mg, &mg_b, &mg_x);
+        return AEO_OK;
+    }
+
+    aeo_status set_pcg(const double* ax, const double* ay, const double* az, double tol, int maxit) override {
+        if (!pcg) { fail("set_pcg: the domain was not created with solver = AEO_SOLVER_PCG"); return AEO_ERR_STATE; }
+        if (!(tol > 0) || maxit < 1) { fail("set_pcg: tol > 0 and maxit >= 1 required"); return AEO_ERR_ARGUMENT; }
+        if ((ax == nullptr) != (ay == nullptr) || (ax == nullptr) != (az == nullptr)) {
+            fail("set_pcg: give all three aperture arrays or none");
+            return AEO_ERR_ARGUMENT;
+        }
+        pcg_tol = tol;
+        pcg_maxit = maxit;
+        return make_pcg(ax, ay, az);
+    }
+
+    aeo_status pcg_stats(aeo_mg_stats* o) override {
+        if (!pcg) { fail("pcg_stats: the domain was not created with solver = AEO_SOLVER_PCG"); return AEO_ERR_STATE; }
+        CK(cudaStreamSynchronize(st));
+        return aeo_mg_read_stats(mg, o);
+    }
+
+    aeo_status pcg_set_learned(aeo_unet* net, double stagnation) override {
+        if (!pcg) { fail("pcg_set_learned: the domain was not created with solver = AEO_SOLVER_PCG"); return AEO_ERR_STATE; }
+        CK(cudaStreamSynchronize(st));
+        if (aeo_status e = aeo_mg_set_learned(mg, net, stagnation)) {
+            fail(std::string("pcg_set_learned: ") + aeo_mg_last_error(mg));
+            return e;
+        }
         return AEO_OK;
     }
 
@@ -478,6 +580,23 @@ struct Core : CoreBase {
 
     // The pressure solve from the source (src == nullptr: divergence of Q) into phi.
     aeo_status solve(const R* src) {
+        if (pcg) {
+            const unsigned gb = (unsigned)((g.nin + 255) / 256);
+            if (src) to_f64_kernel<R><<<gb, 256, 0, st>>>(g.nin, src, mg_b);
+            else cc_div_kernel<R><<<gb, 256, 0, st>>>(g, Q[0], Q[1], Q[2], apx, apy, apz, mg_b);
+            CKL();
+            mark(AEO_K_DIV_FFTX);
+            if (aeo_status e = aeo_mg_launch(mg, st)) {
+                fail(std::string("the MG-PCG pressure solve: ") + aeo_mg_last_error(mg));
+                return e;
+            }
+            mark(AEO_K_ZSOLVE);
+            if (src) {
+                from_f64_kernel<R><<<gb, 256, 0, st>>>(g.nin, mg_x, phi);
+                CKL();
+            }
+            return AEO_OK;
+        }
         const int M = g.nx / 2;
         size_t smx = (size_t)rows_x * xrow(M) * sizeof(cplx<R>);
         unsigned gx = (unsigned)((g.ny * (long long)g.nz + rows_x - 1) / rows_x);
@@ -525,6 +644,13 @@ struct Core : CoreBase {
 
     aeo_status correct(R** out, int stage, R ca, R cb, const double* dtp, int s_u0) {
         R** u0 = P[s_u0];
+        if (pcg) {
+            cc_correct_kernel<R><<<(unsigned)((g.nin + 255) / 256), 256, 0, st>>>(
+                g, Q[0], Q[1], Q[2], mg_x, apx, apy, apz, u0[0], u0[1], u0[2], out[0], out[1], out[2], pres, dtp, ca,
+                cb, stage);
+            CKL();
+            return AEO_OK;
+        }
         if (uni)
             correct_kernel<R, true><<<gvec(), 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi, u0[0], u0[1], u0[2], out[0],
                                                                out[1], out[2], pres, dtp, ca, cb, stage);
@@ -592,6 +718,17 @@ struct Core : CoreBase {
         return substage(3, c ^ 1, c, 1, inv3, two3);
     }
 
+    // One step on the stream: the captured graph, or (solver = PCG, whose solve
+    // is itself a graph with conditional nodes that a capture cannot contain)
+    // the launches themselves.
+    aeo_status launch_step(bool pick) {
+        if (pcg) return enqueue_rk3(cur, pick);
+        cudaGraphExec_t ge;
+        if (aeo_status e = graph_for(pick, &ge)) return e;
+        CK(cudaGraphLaunch(ge, st));
+        return AEO_OK;
+    }
+
     aeo_status graph_for(bool pick, cudaGraphExec_t* out) {
         cudaGraphExec_t& ge = gexec[pick ? 1 : 0][cur];
         if (!ge) {
@@ -613,9 +750,7 @@ struct Core : CoreBase {
         set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt, dt);
         CKL();
         for (int s = 0; s < n; ++s) {
-            cudaGraphExec_t ge;
-            if (aeo_status e = graph_for(false, &ge)) return e;
-            CK(cudaGraphLaunch(ge, st));
+            if (aeo_status e = launch_step(false)) return e;
             cur ^= 1;
         }
         if (sync) {
@@ -710,9 +845,7 @@ struct Core : CoreBase {
         CKL();
         aeo_adaptive_stats acc{};
         for (int s = 0; s < n; ++s) {
-            cudaGraphExec_t ge;
-            if (aeo_status e = graph_for(true, &ge)) return e;
-            CK(cudaGraphLaunch(ge, st));
+            if (aeo_status e = launch_step(true)) return e;
             StepScalars h;
             if (aeo_status e = read_scalars(&h)) return e;
             double dt = h.dt;
@@ -745,9 +878,7 @@ struct Core : CoreBase {
                 ++retries;
                 set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt, dt);
                 CKL();
-                cudaGraphExec_t gr;
-                if (aeo_status e = graph_for(false, &gr)) return e;
-                CK(cudaGraphLaunch(gr, st));
+                if (aeo_status e = launch_step(false)) return e;
             }
             cur ^= 1;
             set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt_prev, dt);
@@ -961,6 +1092,17 @@ struct Core : CoreBase {
 
     aeo_status max_divergence(double* out) override {
         R** s = P[cur];
+        if (pcg) {
+            cc_maxdiv_levels_kernel<R><<<g.nz, 256, 0, st>>>(g, s[0], s[1], s[2], apx, apy, apz, d_part);
+            CKL();
+            std::vector<double> h((size_t)g.nz);
+            CK(cudaMemcpyAsync(h.data(), d_part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            double m = 0.0;
+            for (double v : h) m = std::max(m, v);
+            *out = m;
+            return AEO_OK;
+        }
         if (anel) {
             if (uni) maxdiv_levels_kernel<R, true, true><<<g.nz, 256, 0, st>>>(g, s[0], s[1], s[2], d_part);
             else maxdiv_levels_kernel<R, true, false><<<g.nz, 256, 0, st>>>(g, s[0], s[1], s[2], d_part);
@@ -1014,6 +1156,12 @@ static aeo_status validate(const aeo_config* c, const double* zf, const double* 
     } else if (c->solver == AEO_SOLVER_COLUMN) {
         if (c->bc_z != AEO_BC_WALL) { *m = "the column solver needs walls in z"; return AEO_ERR_ARGUMENT; }
         if (c->nz > AEO_COLUMN_NZ_MAX) { *m = "the column solver needs nz <= " + std::to_string(AEO_COLUMN_NZ_MAX); return AEO_ERR_ARGUMENT; }
+    } else if (c->solver == AEO_SOLVER_PCG) {
+        if (c->stretched) { *m = "the PCG pressure solver needs a uniform z (one multigrid spacing per axis)"; return AEO_ERR_ARGUMENT; }
+        if (c->core != AEO_CORE_BOUSSINESQ) {
+            *m = "the PCG pressure solver projects the Boussinesq core (the sound-proof cores take the direct weighted solver)";
+            return AEO_ERR_ARGUMENT;
+        }
     } else { *m = "unknown solver"; return AEO_ERR_ARGUMENT; }
     if (c->advection < 0 || c->advection > 2) { *m = "unknown advection scheme"; return AEO_ERR_ARGUMENT; }
     if (c->advection != AEO_ADV_CENTRED && (c->stretched || c->core == AEO_CORE_ANELASTIC)) {
@@ -1144,6 +1292,27 @@ aeo_status aeo_pressure_solve(aeo_sim* h, const double* src, double* phi) {
     ENTER(h);
     if (!src || !phi) { h->core->fail("NULL array"); return AEO_ERR_ARGUMENT; }
     return h->core->pressure_solve(src, phi);
+}
+
+aeo_status aeo_set_pcg(aeo_sim* h, const double* ax, const double* ay, const double* az, double tol, int32_t maxit) {
+    ENTER(h);
+    return h->core->set_pcg(ax, ay, az, tol, maxit);
+}
+
+aeo_status aeo_pcg_stats(aeo_sim* h, int32_t* iterations, int32_t* status, double* residual, double* bnorm) {
+    ENTER(h);
+    aeo_mg_stats o{};
+    if (aeo_status e = h->core->pcg_stats(&o)) return e;
+    if (iterations) *iterations = o.iterations;
+    if (status) *status = o.status;
+    if (residual) *residual = o.residual;
+    if (bnorm) *bnorm = o.bnorm;
+    return AEO_OK;
+}
+
+aeo_status aeo_pcg_set_learned(aeo_sim* h, struct aeo_unet* net, double stagnation) {
+    ENTER(h);
+    return h->core->pcg_set_learned(net, stagnation);
 }
 
 aeo_status aeo_kinetic_energy(aeo_sim* h, double* out) {

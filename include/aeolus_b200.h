@@ -37,7 +37,7 @@ typedef enum {
 enum { AEO_BC_PERIODIC = 0, AEO_BC_WALL = 1 };
 enum { AEO_CORE_BOUSSINESQ = 0, AEO_CORE_ANELASTIC = 1 };
 enum { AEO_ADV_CENTRED = 0, AEO_ADV_WENO_JS5 = 1, AEO_ADV_WENO_Z5 = 2 };
-enum { AEO_SOLVER_FFT = 0, AEO_SOLVER_COLUMN = 1 };
+enum { AEO_SOLVER_FFT = 0, AEO_SOLVER_COLUMN = 1, AEO_SOLVER_PCG = 2 };
 enum { AEO_PREC_FP64 = 0, AEO_PREC_FP32_MIXED = 1 };
 enum { AEO_FIELD_U = 0, AEO_FIELD_V = 1, AEO_FIELD_W = 2, AEO_FIELD_THETA = 3,
        AEO_FIELD_P = 4, AEO_FIELD_NUT = 5 };
@@ -57,7 +57,8 @@ typedef struct {
     int32_t stretched;         /* 1: zf gives the Nz+1 interior face heights   */
     int32_t core;              /* AEO_CORE_*                                   */
     int32_t advection;         /* AEO_ADV_* (momentum and theta)               */
-    int32_t solver;            /* AEO_SOLVER_FFT (triply periodic) or COLUMN   */
+    int32_t solver;            /* AEO_SOLVER_FFT (triply periodic), COLUMN, or
+                                  PCG (Boussinesq, uniform z: aeo_set_pcg)      */
     int32_t precision;         /* AEO_PREC_*                                   */
     double nu;                 /* molecular viscosity / diffusivity (0 = off)  */
     double theta0;             /* Boussinesq reference theta (0 = no buoyancy) */
@@ -228,6 +229,33 @@ aeo_status aeo_pressure_solve_column_noalloc(int32_t nx, int32_t ny, int32_t nz,
                                              const double* hweight, const double* measure,
                                              const double* inv_coupling, const double* gauge,
                                              const double* src, double* phi, void* stream);
+
+/* The pressure solve of a domain created with solver = AEO_SOLVER_PCG:
+ * conjugate gradients preconditioned by one multigrid V(2,2) cycle
+ * (MGPreconditionedCG, src/Multigrid.jl:893-967, the urban :mg_cg slot of
+ * src/components/urban/pressure_solver.jl:126) on cut-cell face apertures.
+ * ax ((nx+1)*ny*nz), ay (nx*(ny+1)*nz), az (nx*ny*(nz+1)): host FP64
+ * apertures in [0, 1] in the face layout of aeolus_b200_mgpcg.h (face i the
+ * west / south / bottom face of cell i), all NULL for every face open; the
+ * wall faces of a bounded z are blocked whatever is given.  The projection
+ * solves the a^2-weighted Laplacian against the aperture-weighted
+ * divergence of the predictor (cutcell_divergence! times vol_eff,
+ * src/CutCell.jl:602-623) and corrects with the aperture-scaled gradient
+ * (cutcell_gradient_x/y/z!, :666-700), so a blocked face carries no velocity
+ * (apply_cutcell_velocity_bc!, :852-880) and the aperture-weighted
+ * divergence after a projection is the solve's residual.  Every solve runs
+ * to ||r|| <= tol ||b|| or maxit iterations (defaults 1e-8, 200); steps of
+ * such a domain are launched kernel by kernel (the solve is itself a graph
+ * with a device-side loop).  aeo_max_divergence reports the aperture-weighted
+ * divergence on these domains.  No reference counterpart for the learned
+ * preconditioner (aeo_pcg_set_learned: the U-Net of aeolus_b200_unet.h with
+ * its stagnation fallback to the cycle; net NULL switches back). */
+struct aeo_unet;
+aeo_status aeo_set_pcg(aeo_sim* h, const double* ax, const double* ay, const double* az, double tol, int32_t maxit);
+/* the statistics of the last projection's solve (iterations, AEO_MG_* status,
+ * ||r||, ||b - mean(b)||); synchronises the handle's stream */
+aeo_status aeo_pcg_stats(aeo_sim* h, int32_t* iterations, int32_t* status, double* residual, double* bnorm);
+aeo_status aeo_pcg_set_learned(aeo_sim* h, struct aeo_unet* net, double stagnation);
 
 /* Last error message of the handle (or of the last failed aeo_create when h is NULL). */
 const char* aeo_last_error(const aeo_sim* h);

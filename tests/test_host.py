@@ -93,3 +93,12 @@ def test_spec_validation():
         CoreSpec(grid=g, core="anelastic")
     assert CoreSpec(grid=g).solver == "fft"
     assert CoreSpec(grid=regular_grid((16, 16, 16), (1, 1, 1), bc_z="wall")).solver == "column"
+
+
+def test_pcg_solver_needs_a_uniform_boussinesq_domain():
+    from aeolus_b200 import CoreSpec, regular_grid, stretched_grid, tanh_faces
+    g = regular_grid((32, 32, 16), (64.0, 64.0, 32.0), halo=(3, 3, 3), bc_z="wall")
+    assert CoreSpec(grid=g, solver="pcg").solver == "pcg"
+    gs = stretched_grid((32, 32, 16), (64.0, 64.0, 400.0), tanh_faces(16, 400.0, 1.5))
+    with pytest.raises(ValueError):
+        CoreSpec(grid=gs, solver="pcg")
