@@ -103,13 +103,18 @@ def box_heights(grid: Grid, boxes, x: np.ndarray, y: np.ndarray) -> np.ndarray:
     return H
 
 
-def _fluid_counts(H: np.ndarray, zs: np.ndarray, nsub: int, nz: int) -> np.ndarray:
-    """For each level k and lattice column, the number of the level's nsub
-    z samples strictly above H: level k owns samples [k nsub, (k+1) nsub)."""
-    nle = np.searchsorted(zs, H, side="right")        # samples with z <= H
-    out = np.empty((nz,) + H.shape, dtype=np.int32)
-    for k in range(nz):
-        out[k] = nsub - np.clip(nle - k * nsub, 0, nsub)
+def _level_fractions(nle: np.ndarray, nsub: int, nz: int, fold, norm: float) -> np.ndarray:
+    """Fluid fraction of every level from nle, the number of z samples at or
+    below H of each sample column: level k owns samples [k nsub, (k+1) nsub),
+    and fold sums a level's per-column counts over the samples of each cell
+    or face.  Levels above the tallest H are all fluid, so only the levels
+    the obstacles reach are counted (one level at a time)."""
+    top = min(nz, int(nle.max()) // nsub + 1)
+    first = fold(nsub - np.clip(nle, 0, nsub))
+    out = np.ones((nz,) + first.shape)
+    out[0] = first / norm
+    for k in range(1, top):
+        out[k] = fold(nsub - np.clip(nle - k * nsub, 0, nsub)) / norm
     return out
 
 
@@ -124,12 +129,53 @@ def box_geometry(grid: Grid, boxes, nsub: int = 4, vol_min: float = 1e-3) -> Cut
     xf, yf, zf = (_west(grid, a) for a in range(3))
     n2, n3 = float(nsub * nsub), float(nsub ** 3)
     Hc = box_heights(grid, boxes, xs, ys)
-    vol = _fluid_counts(Hc, zs, nsub, NZ).reshape(NZ, NY, nsub, NX, nsub).sum(axis=(2, 4)) / n3
-    ax = _fluid_counts(box_heights(grid, boxes, xf, ys), zs, nsub, NZ).reshape(NZ, NY, nsub, NX).sum(axis=2) / n2
-    ay = _fluid_counts(box_heights(grid, boxes, xs, yf), zs, nsub, NZ).reshape(NZ, NY, NX, nsub).sum(axis=3) / n2
+
+    def below(H):
+        return np.searchsorted(zs, H, side="right")    # samples with z <= H
+
+    vol = _level_fractions(below(Hc), nsub, NZ, lambda c: c.reshape(NY, nsub, NX, nsub).sum(axis=(1, 3)), n3)
+    ax = _level_fractions(below(box_heights(grid, boxes, xf, ys)), nsub, NZ,
+                          lambda c: c.reshape(NY, nsub, NX).sum(axis=1), n2)
+    ay = _level_fractions(below(box_heights(grid, boxes, xs, yf)), nsub, NZ,
+                          lambda c: c.reshape(NY, NX, nsub).sum(axis=2), n2)
     nle = np.searchsorted(zf, Hc, side="right")       # bottom faces with z <= H
-    az = np.stack([(nle <= k).reshape(NY, nsub, NX, nsub).sum(axis=(1, 3)) for k in range(NZ)]) / n2
+    az = np.ones((NZ, NY, NX))
+    for k in range(min(NZ, int(nle.max()) + 1)):
+        az[k] = (nle <= k).reshape(NY, nsub, NX, nsub).sum(axis=(1, 3)) / n2
     return finalize_geometry(grid, vol, ax, ay, az, vol_min, nsub)
+
+
+def box_solid_mask(grid: Grid, boxes) -> np.ndarray:
+    """The SolidMask of floor-standing boxes: a cell is solid when its centre
+    lies below the top of a box whose closed footprint holds it (the
+    predicate of mark_solid!, src/IBM.jl:51-63), evaluated on every storage
+    cell, so the x and y halos hold the periodic images and the levels below
+    the floor are solid (mark_solid! marks the interior only; the halo cells
+    only decide the faces on the domain boundary, which are periodic partners
+    or walls)."""
+    xc, yc, zc = (_subsamples(grid, a, 1) for a in range(3))
+    H = box_heights(grid, boxes, xc, yc)
+    return zc[:, None, None] < H[None, :, :]
+
+
+def staircase_geometry(grid: Grid, mask: np.ndarray, vol_min: float = 1e-3) -> CutCellGeometry:
+    """`cut_cell_geometry(mesh, sm::SolidMask)` (src/CutCell.jl:334-352): 0/1
+    volume fractions and apertures (a face is open when both its cells are
+    fluid), then the consistency passes, so the cut-cell operators are the
+    Cartesian ones with blocked faces.  This is the obstacle model of the
+    urban cases (their `geom.sm` solid mask)."""
+    mask = np.asarray(mask, dtype=bool)
+    if mask.shape != grid.storage_shape:
+        raise ValueError(f"mask shape {mask.shape} != storage shape {grid.storage_shape}")
+    vol = np.where(mask, 0.0, 1.0)
+    fl = ~mask
+    ax = np.zeros(grid.storage_shape)
+    ay = np.zeros(grid.storage_shape)
+    az = np.zeros(grid.storage_shape)
+    ax[:, :, 1:] = fl[:, :, :-1] & fl[:, :, 1:]
+    ay[:, 1:, :] = fl[:, :-1, :] & fl[:, 1:, :]
+    az[1:, :, :] = fl[:-1, :, :] & fl[1:, :, :]
+    return finalize_geometry(grid, vol, ax, ay, az, vol_min, 1)
 
 
 def finalize_geometry(grid: Grid, vol, ax, ay, az, vol_min: float, nsub: int) -> CutCellGeometry:

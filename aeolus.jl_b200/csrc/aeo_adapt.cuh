@@ -23,6 +23,7 @@ struct StepScalars {
 struct CflParams {
     double c_adv, c_diff, c_buoy, c_cor, dt_min, dt_max, growth;
     double nu, pr_t, fcor, gacc, theta0, dz_min;
+    double th_off;   // the stored offset of theta (plane means are of theta - th_off)
     int sgs, buoy, anel;
 };
 
@@ -83,7 +84,7 @@ __global__ void dt_pick_kernel(Geo g, CflParams c, const double* __restrict__ pa
         nanr = nanr || isnan(r);
         rate = fmax(rate, r);
         nutm = fmax(nutm, part[4 * k + 1]);
-        double mean = part[4 * k + 2];
+        double mean = part[4 * k + 2] + c.th_off;
         if (k > 0 && c.buoy) {
             double dzf = g.uniform ? g.dz : 1.0 / lvl(g.idzf, k);
             double n2 = c.anel ? c.gacc * (log(mean) - log(prev)) / dzf

@@ -83,6 +83,7 @@ struct MgBase {
     virtual int nlevels() const = 0;
     virtual void level_dims(int l, int32_t* d) const = 0;
     virtual int launches_per_iteration() const = 0;
+    virtual int launches_per_solve(int iterations) const = 0;
     virtual aeo_status set_learned(aeo_unet* net, double stag) = 0;
     virtual aeo_status harvest(const double* b, double* x, aeo_mg_stats* st, double* rh, double* xh, int cap,
                                int* count) = 0;
@@ -90,6 +91,8 @@ struct MgBase {
     // buffers, the solve enqueued on the caller's stream, the last statistics
     virtual void buffers(double** b, double** x) = 0;
     virtual aeo_status launch_on(cudaStream_t s) = 0;
+    virtual aeo_status enqueue_on(cudaStream_t s) = 0;
+    virtual aeo_status order_before(cudaStream_t s) = 0;
     virtual aeo_status last_stats(aeo_mg_stats* o) = 0;
 };
 
@@ -219,6 +222,7 @@ struct Mg : MgBase {
     size_t coarse_col_smem = 0;
     cudaGraphExec_t g_solve = nullptr, g_cycles = nullptr;
     int body_launches = 0;
+    int prologue_launches = 0;
 
     ~Mg() override {
         if (st) cudaStreamSynchronize(st);
@@ -262,6 +266,12 @@ struct Mg : MgBase {
         d[2] = L[l].nz;
     }
     int launches_per_iteration() const override { return body_launches; }
+    // kernels of one solve graph launch of `iterations` CG iterations: the
+    // prologue, the loop bodies and the two of the mean shift (the U-Net's own
+    // kernels in a learned prologue are not counted)
+    int launches_per_solve(int iterations) const override {
+        return prologue_launches + iterations * body_launches + 2;
+    }
 
     static dim3 half_grid(const Level<R>& F) {
         return dim3((unsigned)((F.nx / 2 + RB_X - 1) / RB_X), (unsigned)((F.ny + RB_Y - 1) / RB_Y), (unsigned)F.nz);
@@ -660,25 +670,34 @@ struct Mg : MgBase {
     // the end of every iteration.
     aeo_status build_solve(bool harvest = false) {
         CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
-        aeo_status s = [&]() -> aeo_status {
-            cudaGraphConditionalHandle hdl;
-            if (aeo_status q = make_handle(&hdl)) return q;
-            pcg_mean_kernel<<<RED_BLOCKS, TPB, 0, st>>>(b, n, S, part, 0);
+        aeo_status s = capture_solve(st, harvest);
+        return end_capture(harvest ? &g_harvest : &g_solve, s);
+    }
+
+    // The solve's nodes captured on `s` (a stream capturing into this
+    // handle's graph or into the caller's: the conditional nodes go into
+    // whichever graph `s` is capturing).
+    aeo_status capture_solve(cudaStream_t s0, bool harvest) {
+        cudaGraphConditionalHandle hdl;
+        if (aeo_status q = make_handle_on(s0, &hdl, 0)) return q;
+        pcg_mean_kernel<<<RED_BLOCKS, TPB, 0, s0>>>(b, n, S, part, 0);
+        CKL();
+        pcg_init_kernel<<<RED_BLOCKS, TPB, 0, s0>>>(b, r, x, n, S, part);
+        CKL();
+        if (harvest) {
+            pcg_harvest_kernel<<<RED_BLOCKS, TPB, 0, s0>>>(x, r, hist_x, hist_r, n, hist_cap, S);
             CKL();
-            pcg_init_kernel<<<RED_BLOCKS, TPB, 0, st>>>(b, r, x, n, S, part);
-            CKL();
-            if (harvest) {
-                pcg_harvest_kernel<<<RED_BLOCKS, TPB, 0, st>>>(x, r, hist_x, hist_r, n, hist_cap, S);
-                CKL();
-            }
-            if (cfg.precond == AEO_PC_VCYCLE)
-                if (aeo_status q = launch_vcycle(st, r, true, &S->done)) return q;
-            if (cfg.precond == AEO_PC_LEARNED)
-                if (aeo_status q = aeo_unet_forward_on(net, r, st)) return q;
-            if (aeo_status q = launch_rz_dir(st, 1)) return q;
-            pcg_cond_kernel<<<1, 1, 0, st>>>(S, hdl, 0);
-            CKL();
-            if (aeo_status q = capture_while(hdl, [&](cudaStream_t sb) -> aeo_status {
+        }
+        if (cfg.precond == AEO_PC_VCYCLE)
+            if (aeo_status q = launch_vcycle(s0, r, true, &S->done)) return q;
+        if (cfg.precond == AEO_PC_LEARNED)
+            if (aeo_status q = aeo_unet_forward_on(net, r, s0)) return q;
+        if (aeo_status q = launch_rz_dir(s0, 1)) return q;
+        pcg_cond_kernel<<<1, 1, 0, s0>>>(S, hdl, 0);
+        CKL();
+        if (!harvest) prologue_launches = 5 + (cfg.precond == AEO_PC_VCYCLE ? vcycle_launches() : 0);
+        if (aeo_status q = capture_cond(s0, hdl, cudaGraphCondTypeWhile, 1, &st_body,
+                [&](cudaStream_t sb) -> aeo_status {
                     int c0 = 0;
                     if (aeo_status q2 = launch_apply(sb, p, Ap, 0)) return q2;
                     pcg_update_kernel<<<RED_BLOCKS, TPB, 0, sb>>>(x, r, p, Ap, n, S, part);
@@ -704,15 +723,14 @@ struct Mg : MgBase {
                     CKL();
                     body_launches = c0 + 1;
                     return AEO_OK;
-                }))
-                return q;
-            pcg_mean_kernel<<<RED_BLOCKS, TPB, 0, st>>>(x, n, S, part, 1);
-            CKL();
-            shift_kernel<<<RED_BLOCKS, TPB, 0, st>>>(x, n, S);
-            CKL();
-            return AEO_OK;
-        }();
-        return end_capture(harvest ? &g_harvest : &g_solve, s);
+                },
+                [](cudaStream_t) -> aeo_status { return AEO_OK; }))
+            return q;
+        pcg_mean_kernel<<<RED_BLOCKS, TPB, 0, s0>>>(x, n, S, part, 1);
+        CKL();
+        shift_kernel<<<RED_BLOCKS, TPB, 0, s0>>>(x, n, S);
+        CKL();
+        return AEO_OK;
     }
 
     aeo_status stats_out(aeo_mg_stats* o, bool relative) {
@@ -748,6 +766,22 @@ struct Mg : MgBase {
             CK(cudaStreamWaitEvent(s, ev_own, 0));
         }
         CK(cudaGraphLaunch(g_solve, s));
+        return AEO_OK;
+    }
+    // x = A^-1 b on s: captured inline when s is capturing (the caller's
+    // graph then holds the loop), else the handle's own solve graph
+    aeo_status enqueue_on(cudaStream_t s) override {
+        cudaStreamCaptureStatus cs;
+        CK(cudaStreamIsCapturing(s, &cs));
+        if (cs == cudaStreamCaptureStatusActive) return capture_solve(s, false);
+        return launch_on(s);
+    }
+    // everything this handle queued on its own stream precedes what s runs next
+    aeo_status order_before(cudaStream_t s) override {
+        if (s == st) return AEO_OK;
+        if (!ev_own) CK(cudaEventCreateWithFlags(&ev_own, cudaEventDisableTiming));
+        CK(cudaEventRecord(ev_own, st));
+        CK(cudaStreamWaitEvent(s, ev_own, 0));
         return AEO_OK;
     }
     aeo_status last_stats(aeo_mg_stats* o) override {
@@ -1099,4 +1133,15 @@ aeo_status aeo_mg_launch(aeo_mg* h, cudaStream_t s) {
 aeo_status aeo_mg_read_stats(aeo_mg* h, aeo_mg_stats* o) {
     if (!h || !o) return AEO_ERR_ARGUMENT;
     return h->core->last_stats(o);
+}
+aeo_status aeo_mg_enqueue(aeo_mg* h, cudaStream_t s) {
+    if (!h) return AEO_ERR_ARGUMENT;
+    return h->core->enqueue_on(s);
+}
+aeo_status aeo_mg_order_before(aeo_mg* h, cudaStream_t s) {
+    if (!h) return AEO_ERR_ARGUMENT;
+    return h->core->order_before(s);
+}
+int aeo_mg_launches_per_solve(const aeo_mg* h, int iterations) {
+    return h ? h->core->launches_per_solve(iterations) : 0;
 }

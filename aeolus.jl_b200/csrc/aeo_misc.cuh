@@ -137,21 +137,22 @@ __global__ void __launch_bounds__(256) correct_kernel(Geo g, const R* __restrict
 // Host storage (reference layout, halos hh) <-> device padded interior.
 template <typename R>
 __global__ void unpack_host_kernel(Geo g, const double* __restrict__ hsrc, int hx, int hy, int hz,
-                                   R* __restrict__ dst, int padded) {
+                                   R* __restrict__ dst, int padded, double off) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int j = blockIdx.y, k = blockIdx.z;
     if (i >= g.nx) return;
     long long HX = g.nx + 2LL * hx, HY = g.ny + 2LL * hy;
-    double v = hsrc[(i + hx) + HX * ((j + hy) + HY * (long long)(k + hz))];
+    double v = hsrc[(i + hx) + HX * ((j + hy) + HY * (long long)(k + hz))] - off;
     if (padded) dst[pidx(g, i, j, k)] = R(v);
     else dst[iidx(g, i, j, k)] = R(v);
 }
 
 // Fill the whole host storage array from the device interior through the
-// composite boundary map (loc < 0: halos zero).
+// composite boundary map (loc < 0: halos zero); `off` is added back to every
+// mapped value (the stored offset of theta, 0 otherwise).
 template <typename R>
 __global__ void pack_host_kernel(Geo g, double* __restrict__ hdst, int hx, int hy, int hz,
-                                 const R* __restrict__ src, int padded, int loc) {
+                                 const R* __restrict__ src, int padded, int loc, double off) {
     long long HX = g.nx + 2LL * hx, HY = g.ny + 2LL * hy, HZ = g.nz + 2LL * hz;
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= HX * HY * HZ) return;
@@ -167,7 +168,7 @@ __global__ void pack_host_kernel(Geo g, double* __restrict__ hdst, int hx, int h
         if (s != 0) {
             int ii = inside ? i : wrapi(i, g.nx), jj = inside ? j : wrapi(j, g.ny);
             R r = padded ? src[pidx(g, ii, jj, kk)] : src[iidx(g, ii, jj, kk)];
-            v = s > 0 ? (double)r : -(double)r;
+            v = (s > 0 ? (double)r : -(double)r) + off;
         }
     }
     hdst[t] = v;
@@ -267,7 +268,7 @@ __device__ __forceinline__ void philox4x32(uint32_t c[4], uint32_t k0, uint32_t 
 // (seed, stream, id): its top 53 bits over 2^53.
 template <typename R>
 __global__ void philox_fill_kernel(Geo g, R* __restrict__ dst, int padded, uint64_t seed, uint32_t stream, double amp,
-                                   int add) {
+                                   int add, double off) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= g.nin) return;
     uint32_t c[4] = {0u, stream, (uint32_t)t, (uint32_t)((unsigned long long)t >> 32)};
@@ -277,7 +278,7 @@ __global__ void philox_fill_kernel(Geo g, R* __restrict__ dst, int padded, uint6
     double val = amp * (2.0 * u01 - 1.0);
     int i = (int)(t % g.nx), j = (int)((t / g.nx) % g.ny), k = (int)(t / ((long long)g.nx * g.ny));
     long long q = padded ? pidx(g, i, j, k) : t;
-    dst[q] = add ? R((double)dst[q] + val) : R(val);
+    dst[q] = add ? R((double)dst[q] + val) : R(val - off);
 }
 
 template <typename R>

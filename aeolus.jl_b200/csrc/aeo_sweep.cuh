@@ -39,6 +39,7 @@ struct SweepArgs {
     R ca, cb;
     int stage;
     R nu, gacc, theta0, fcor, inv_prt, pr_t, flux_bot, flux_top, sp_alpha, sp_zstart, sp_inv;
+    R bref;         // theta0 in stored units (theta is held as theta - offset)
     R c_s;
 };
 
@@ -411,7 +412,7 @@ __device__ __forceinline__ void sweep_point(const Met<R, UNI>& m, const SweepArg
             tw += coef * (m.zface(k, T(0, 0, -1), T(0, 0, 0)) - tb);
         }
     } else if (a.theta0 != R(0)) {
-        tw += (a.gacc / a.theta0) * (m.zface(k, T(0, 0, -1), T(0, 0, 0)) - a.theta0);
+        tw += (a.gacc / a.theta0) * (m.zface(k, T(0, 0, -1), T(0, 0, 0)) - a.bref);
     }
     // Coriolis
     if (a.fcor != R(0)) {

@@ -79,6 +79,8 @@ struct CoreBase {
     Geo g{};
     int launches = 0;
     virtual ~CoreBase() {}
+    // kernels of one RK3 step (solver = PCG: with the last solve's iteration count)
+    virtual int step_launches() { return launches; }
     void fail(const std::string& m) { err = m; }
     virtual aeo_status init(const double* zf, const double* wc, const double* wf, const double* thf) = 0;
     virtual aeo_status set_field(int id, const double* host) = 0;
@@ -113,6 +115,10 @@ struct Core : CoreBase {
     double* colc = nullptr;    // column coefficients
     ColumnCoef cc{};
     R* P[4][4] = {};           // padded state sets (u, v, w, theta)
+    // theta is held as theta - th_off: the reference value (theta0, or the
+    // anelastic theta_f at the surface) in FP32, so the stored numbers are the
+    // few-kelvin deviations and keep FP32's relative precision; 0 in FP64
+    double th_off = 0.0;
     TileMaps tmaps[4];         // TMA maps of the padded sets
     bool pair = false;         // FP32 centred: the paired sweep (64-cell tiles, 72-wide plane boxes)
     int cur = 0;               // the set holding the state (0 or 1)
@@ -192,6 +198,7 @@ struct Core : CoreBase {
         uni = !c.stretched;
         sgs = c.c_s != 0.0;
         anel = c.core == AEO_CORE_ANELASTIC;
+        if (sizeof(R) == sizeof(float)) th_off = anel ? (thf ? thf[c.hz] : 0.0) : c.theta0;
         g.nx = c.nx; g.ny = c.ny; g.nz = c.nz;
         g.px = c.nx + 2 * AEO_HX;
         g.py = c.ny + 2 * AEO_H;
@@ -291,7 +298,7 @@ struct Core : CoreBase {
                 put_r(LV_WF, wfr);
                 put_r(LV_IWC, wcr != R(0) ? R(1) / wcr : R(0));
                 put_r(LV_IWF, wfr != R(0) ? R(1) / wfr : R(0));
-                put_r(LV_THF, thr);
+                put_r(LV_THF, R(row(12, e) - th_off));   // the buoyancy's reference in stored units
                 put_r(LV_GTHF, thr != R(0) ? R(c.g) / thr : R(0));
                 put_r(LV_SPC, rate(row(8, e)));
                 put_r(LV_SPF, rate(row(9, e)));
@@ -462,6 +469,7 @@ struct Core : CoreBase {
         mc.nu1 = 2; mc.nu2 = 2; mc.coarse_sweeps = 50; mc.min_size = 4;
         mc.device = cfg.device;
         CK(cudaStreamSynchronize(st));   // no solve of the old handle in flight
+        drop_graphs();                   // the step graphs hold the old handle's nodes
         if (mg) { aeo_mg_destroy(mg); mg = nullptr; }
         if (aeo_status e = aeo_mg_create(&mc, c2[0].data(), c2[1].data(), c2[2].data(), &mg)) {
             fail(std::string("the MG-PCG pressure solver: ") + aeo_mg_last_error(nullptr));
@@ -483,6 +491,14 @@ struct Core : CoreBase {
         return make_pcg(ax, ay, az);
     }
 
+    // a PCG substage: sweep, cc_div, the solve graph, cc_correct, halo fill
+    int step_launches() override {
+        if (!pcg) return launches;
+        aeo_mg_stats o{};
+        if (cudaStreamSynchronize(st) != cudaSuccess || aeo_mg_read_stats(mg, &o)) return 0;
+        return 3 * (4 + aeo_mg_launches_per_solve(mg, o.iterations));
+    }
+
     aeo_status pcg_stats(aeo_mg_stats* o) override {
         if (!pcg) { fail("pcg_stats: the domain was not created with solver = AEO_SOLVER_PCG"); return AEO_ERR_STATE; }
         CK(cudaStreamSynchronize(st));
@@ -492,6 +508,7 @@ struct Core : CoreBase {
     aeo_status pcg_set_learned(aeo_unet* net, double stagnation) override {
         if (!pcg) { fail("pcg_set_learned: the domain was not created with solver = AEO_SOLVER_PCG"); return AEO_ERR_STATE; }
         CK(cudaStreamSynchronize(st));
+        drop_graphs();   // the solve's loop body changes with the preconditioner
         if (aeo_status e = aeo_mg_set_learned(mg, net, stagnation)) {
             fail(std::string("pcg_set_learned: ") + aeo_mg_last_error(mg));
             return e;
@@ -586,7 +603,7 @@ struct Core : CoreBase {
             else cc_div_kernel<R><<<gb, 256, 0, st>>>(g, Q[0], Q[1], Q[2], apx, apy, apz, mg_b);
             CKL();
             mark(AEO_K_DIV_FFTX);
-            if (aeo_status e = aeo_mg_launch(mg, st)) {
+            if (aeo_status e = aeo_mg_enqueue(mg, st)) {
                 fail(std::string("the MG-PCG pressure solve: ") + aeo_mg_last_error(mg));
                 return e;
             }
@@ -675,6 +692,7 @@ struct Core : CoreBase {
         a.dtp = &d_sc->dt;
         a.ca = ca; a.cb = cb; a.stage = stage;
         a.nu = R(cfg.nu); a.gacc = R(cfg.g); a.theta0 = R(cfg.theta0); a.fcor = R(cfg.f_coriolis);
+        a.bref = R(cfg.theta0 - th_off);
         a.pr_t = R(cfg.pr_t); a.inv_prt = R(1.0 / cfg.pr_t);
         a.flux_bot = R(cfg.flux_bot); a.flux_top = R(cfg.flux_top);
         a.sp_alpha = R(cfg.sponge_alpha); a.sp_zstart = R(cfg.sponge_zstart);
@@ -718,13 +736,16 @@ struct Core : CoreBase {
         return substage(3, c ^ 1, c, 1, inv3, two3);
     }
 
-    // One step on the stream: the captured graph, or (solver = PCG, whose solve
-    // is itself a graph with conditional nodes that a capture cannot contain)
-    // the launches themselves.
+    // One step on the stream: the captured graph (solver = PCG: with the three
+    // CG solves inside it as conditional WHILE nodes).
     aeo_status launch_step(bool pick) {
-        if (pcg) return enqueue_rk3(cur, pick);
         cudaGraphExec_t ge;
         if (aeo_status e = graph_for(pick, &ge)) return e;
+        if (pcg)
+            if (aeo_status e = aeo_mg_order_before(mg, st)) {
+                fail(std::string("the MG-PCG pressure solve: ") + aeo_mg_last_error(mg));
+                return e;
+            }
         CK(cudaGraphLaunch(ge, st));
         return AEO_OK;
     }
@@ -732,7 +753,11 @@ struct Core : CoreBase {
     aeo_status graph_for(bool pick, cudaGraphExec_t* out) {
         cudaGraphExec_t& ge = gexec[pick ? 1 : 0][cur];
         if (!ge) {
-            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            // PCG: the handle's set-up work is complete before its nodes are
+            // captured; the conditional-node capture of its CG loop runs in
+            // relaxed mode, as the handle's own solve graph
+            if (pcg) CK(cudaDeviceSynchronize());
+            CK(cudaStreamBeginCapture(st, pcg ? cudaStreamCaptureModeRelaxed : cudaStreamCaptureModeThreadLocal));
             aeo_status e = enqueue_rk3(cur, pick);
             cudaGraph_t gr = nullptr;
             cudaError_t ce = cudaStreamEndCapture(st, &gr);
@@ -776,6 +801,7 @@ struct Core : CoreBase {
         p.c_adv = c->c_advective; p.c_diff = c->c_diffusive; p.c_buoy = c->c_buoyancy; p.c_cor = c->c_coriolis;
         p.dt_min = c->dt_min; p.dt_max = c->dt_max; p.growth = c->growth_max;
         p.nu = cfg.nu; p.pr_t = cfg.pr_t; p.fcor = cfg.f_coriolis; p.gacc = cfg.g; p.theta0 = cfg.theta0;
+        p.th_off = th_off;
         p.dz_min = dz_min; p.sgs = sgs; p.anel = anel;
         p.buoy = anel ? (cfg.g != 0.0) : (cfg.theta0 != 0.0);
         if (!cflp_set || std::memcmp(&p, &cflp, sizeof(p)) != 0) {
@@ -953,7 +979,8 @@ struct Core : CoreBase {
         if (!d) { fail("set_field: unknown or unavailable field"); return AEO_ERR_ARGUMENT; }
         CK(cudaMemcpyAsync(d_stage, host, host_n * sizeof(double), cudaMemcpyHostToDevice, st));
         dim3 gb((g.nx + 127) / 128, g.ny, g.nz);
-        unpack_host_kernel<R><<<gb, 128, 0, st>>>(g, d_stage, cfg.hx, cfg.hy, cfg.hz, d, padded);
+        unpack_host_kernel<R><<<gb, 128, 0, st>>>(g, d_stage, cfg.hx, cfg.hy, cfg.hz, d, padded,
+                                                  id == AEO_FIELD_THETA ? th_off : 0.0);
         CKL();
         if (padded && loc >= 0) {
             if (loc == LOC_FZ && g.bc_z == 1) {
@@ -979,7 +1006,8 @@ struct Core : CoreBase {
             CKL();
         }
         pack_host_kernel<R><<<(unsigned)((host_n + 255) / 256), 256, 0, st>>>(g, d_stage, cfg.hx, cfg.hy, cfg.hz, d,
-                                                                              padded, loc);
+                                                                              padded, loc,
+                                                                              id == AEO_FIELD_THETA ? th_off : 0.0);
         CKL();
         CK(cudaMemcpyAsync(host, d_stage, host_n * sizeof(double), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -1124,7 +1152,8 @@ struct Core : CoreBase {
         int padded, loc;
         R* d = field_ptr(id, &padded, &loc);
         if (!d || loc < 0) { fail("fill_uniform: field must be u, v, w or theta"); return AEO_ERR_ARGUMENT; }
-        philox_fill_kernel<R><<<(unsigned)((g.nin + 255) / 256), 256, 0, st>>>(g, d, padded, seed, stream, amp, mode);
+        philox_fill_kernel<R><<<(unsigned)((g.nin + 255) / 256), 256, 0, st>>>(g, d, padded, seed, stream, amp, mode,
+                                                                               id == AEO_FIELD_THETA ? th_off : 0.0);
         CKL();
         if (loc == LOC_FZ && g.bc_z == 1) {
             wall_face_zero_kernel<R><<<dim3((g.nx + 127) / 128, g.ny), 128, 0, st>>>(g, d);
@@ -1335,7 +1364,7 @@ aeo_status aeo_profile_step(aeo_sim* h, double dt, double* ms_per_class, int32_t
 
 aeo_status aeo_launches_per_step(aeo_sim* h, int32_t* out) {
     if (!h || !out) return AEO_ERR_ARGUMENT;
-    *out = h->core->launches;
+    *out = h->core->step_launches();
     return AEO_OK;
 }
 

@@ -17,7 +17,7 @@ beside it.  `e2e` is the same metric through the C-ABI with the state copied
 from pinned host memory and back every step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--workload cbl|tgv|urban|hit]
+                  [--workload cbl|tgv|urban|hit|urban_step]
 
 The default line also carries "pcg": the other half of the headline metric,
 the time to a 1e-8 relative residual of the cut-cell urban pressure problem
@@ -29,6 +29,14 @@ cells (WENO-Z5, no SGS, adaptive dt at CFL 0.5): the FP64 run steps
 adaptively, the FP32-mixed run repeats its dt sequence, and the line reports
 the FP32-mixed cell-steps/s beside the FP64 rate with the fields' relative L2
 difference and the kinetic-energy difference after `--hit-steps` steps.
+
+`--workload urban_step` is the large urban convective case: 1024 x 1024 x
+192 cells of 2 m, 600 seeded floor-standing boxes, surface heat flux
+0.15 K m/s, WENO-JS5 with Smagorinsky, the projection by the
+multigrid-preconditioned CG on the cut-cell apertures to a 1e-8 relative
+residual; FP32-mixed against FP64 (cell-steps/s, CG iterations and solve
+time, field error after `--urban-steps` steps), with the learned U-Net
+preconditioner in the FP32-mixed run when `--learned` is given.
 
 Under torchrun every rank runs an independent replica of the workload (the
 step has no data-path collective on one domain; weak scaling) and rank 0
@@ -599,6 +607,207 @@ def run_b200_hit(args):
     return 0
 
 
+URBAN_STEP_N = (1024, 1024, 192)
+
+
+def urban_step_case(n, nboxes, seed=1):
+    """The large urban convective case: n cells of 2 m (walls in z), `nboxes`
+    floor-standing boxes (Philox-seeded centres, footprints U(10, 40) m,
+    heights U(10, 60) m) as a solid mask (a cell is solid when its centre is
+    inside a box) and its staircase geometry (0/1 apertures, the obstacle
+    model of the urban cases), Boussinesq with theta0 =
+    300 K, surface heat flux 0.15 K m/s, WENO-JS5 advection with Smagorinsky
+    C_s = 0.17, the projection by the multigrid-preconditioned CG on the
+    cut-cell apertures.  Initial state: at rest, theta = 300 K plus seeded
+    uniform +-0.1 K noise in the lowest 10 levels.  Returns the grid, the
+    apertures, the fluid mask, a spec maker, the state and a description."""
+    from aeolus_b200 import CoreSpec, regular_grid
+    from aeolus_b200.cutcell import box_solid_mask, face_coefficients, random_boxes, staircase_geometry
+    from aeolus_b200.inputs import philox_uniform
+    g = regular_grid(n, tuple(URBAN_H * v for v in n), halo=(3, 3, 3), bc_z="wall")
+    geom = staircase_geometry(g, box_solid_mask(g, random_boxes(g, nboxes, seed=seed)))
+    ap = face_coefficients(geom, power=1)
+    fluid = ~geom.is_solid[g.interior]
+    del geom
+    nx, ny, nz = n
+    kn = min(10, nz)
+    th = np.full(g.storage_shape, 300.0)
+    hx, hy, hz = g.halo
+    th[hz:hz + kn, hy:hy + ny, hx:hx + nx] += (
+        0.1 * (2.0 * philox_uniform(seed, 3, nx * ny * kn) - 1.0)).reshape(kn, ny, nx)
+    zero = g.zeros()
+    state = (zero, zero, zero, th)
+
+    def mkspec(prec):
+        return CoreSpec(grid=g, advection="weno_js5", c_s=0.17, nu=0.0, theta0=300.0, flux_bot=0.15,
+                        solver="pcg", precision=prec)
+
+    desc = {"workload": f"urban convective {nx}x{ny}x{nz} at 2 m, {nboxes} boxes (seed {seed}, footprints "
+                        "U(10,40) m, heights U(10,60) m, staircase solid mask), heated surface 0.15 K m/s, "
+                        "Boussinesq, WENO-JS5 + "
+                        "Smagorinsky 0.17, MG-preconditioned CG projection on cut-cell apertures to 1e-8, dt = 1 s",
+            "grid": [nx, ny, nz], "solid_fraction": round(float(1.0 - fluid.mean()), 4),
+            "l2": "inputs larger than L2"}
+    return g, ap, fluid, mkspec, state, desc
+
+
+def urban_step_learned(sim, n, fluid, dt, k):
+    """The learned U-Net preconditioner in the FP32-mixed step: trained on the
+    GPU as for the urban pressure problem (2000 residual -> error pairs of
+    128 x 128 x 48 problems, seeds 101..120), transferred to this grid with
+    its fluid mask; k steps timed, the last solve's statistics."""
+    import torch
+    from aeolus_b200.learned import train_streaming, transfer
+    t0 = time.perf_counter()
+    net, losses, used = train_streaming((128, 128, 48), seeds=range(101, 121), rhs_per_geometry=10, nboxes=10,
+                                        pairs_total=2000)
+    train_s = time.perf_counter() - t0
+    big = transfer(net, n, fluid.astype(np.float32))
+    sim.set_learned(big, 0.9)
+    sim.step_rk3(dt, 1)
+    stream = torch.cuda.ExternalStream(sim.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sim.synchronize()
+    e0.record(stream)
+    sim.step_rk3_async(dt, k)
+    e1.record(stream)
+    sim.synchronize()
+    ms = e0.elapsed_time(e1) / k
+    prof = sim.profile_step(dt)
+    st = sim.pcg_stats()
+    sim.set_learned(None)
+    return {"ms_per_step": ms, "solve_ms": prof["zsolve"] / 3, "iterations_last_solve": st["iterations"],
+            "status": st["status"], "relative_residual": st["relative_residual"],
+            "training": {"pairs": used, "seconds": round(train_s, 1),
+                         "loss_first50": float(losses[:50].mean()), "loss_last50": float(losses[-50:].mean())},
+            "unet_forward_ms": big.profile("forward", 3)}
+
+
+def run_b200_urban_step(args):
+    world, rank, local = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    from aeolus_b200.simulation import Simulation
+    n = tuple(args.urban_n) if args.urban_n else URBAN_STEP_N
+    nboxes = args.urban_boxes
+    t0 = time.perf_counter()
+    g, ap, fluid, mkspec, state, desc = urban_step_case(n, nboxes)
+    setup_s = time.perf_counter() - t0
+    hbm, hbm_kind = measured_peaks()
+    dt, S = 1.0, args.urban_steps
+    fields = ("u", "v", "w", "theta")
+    res, ref = {}, None
+    for prec in ("fp64", "fp32_mixed"):
+        sim = Simulation(mkspec(prec), device=local)
+        sim.set_pcg(ap, tol=1e-8, maxit=500)
+        sim.set_state(*state)
+        sim.project()
+        # the trajectory: S steps from the common initial state
+        ms_traj = timed_steps(sim, dt, S, world) / S
+        fin = [sim.get_field(f)[g.interior].copy() for f in fields]
+        ke, div = sim.kinetic_energy(), sim.max_divergence()
+        if ref is None:
+            ref = fin
+            rel = None
+        else:
+            rel = {f: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)) for f, a, b in zip(fields, fin, ref)}
+        del fin
+        sim.step_rk3(dt, args.warmup)
+        clk = ClockSampler(local)
+        clk.start()
+        ms = max_over_ranks(timed_steps(sim, dt, args.steps, world) / args.steps, world)
+        clocks = clk.stop()
+        prof = sim.profile_step(dt)
+        st = sim.pcg_stats()
+        launches = sim.launches_per_step()
+        e2e_ms, h2d, d2h = e2e_steps(sim, state, dt, 2)
+        out = dict(ms=ms, ms_traj=ms_traj, prof=prof, st=st, launches=launches, clocks=clocks, rel=rel, ke=ke,
+                   div=div, e2e_ms=max_over_ranks(e2e_ms, world), h2d=h2d, d2h=d2h)
+        if prec == "fp32_mixed" and args.learned:
+            out["learned"] = urban_step_learned(sim, n, fluid, dt, max(2, min(args.steps, 5)))
+        res[prec] = out
+        sim.close()
+        del sim
+    del ref
+    if rank != 0:
+        barrier(world)
+        return 0
+    ncell = g.ncells
+    m, d = res["fp32_mixed"], res["fp64"]
+    prof = m["prof"]
+    per_launch_ms = prof["sweep"] / LAUNCHES_PER_STEP["sweep"]
+    sweep_bytes = class_passes("sweep", g, True) * 4 * ncell
+    ach = sweep_bytes / (per_launch_ms * 1e-3) / 1e9
+
+    def solve(r):
+        return {"ms_per_solve": round(r["prof"]["zsolve"] / 3, 3), "iterations_last_solve": r["st"]["iterations"],
+                "status": r["st"]["status"], "relative_residual": r["st"]["relative_residual"]}
+
+    line = {
+        "metric": "cell-steps/s", "value": world * ncell / (m["ms"] * 1e-3), "unit": "cell-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32-mixed (FP32 stencils and multigrid cycle; FP64 CG vectors, operator, reductions)",
+        "data": "synthetic (Philox-seeded boxes and theta noise)",
+        "config": dict(desc, parallelism=f"replicas x{world}" if world > 1 else "1 GPU"),
+        "pcg": solve(m),
+        "fp64": {"value": world * ncell / (d["ms"] * 1e-3), "ms_per_step": d["ms"], "pcg": solve(d),
+                 "e2e": world * ncell / (d["e2e_ms"] * 1e-3), "max_divergence": d["div"]},
+        "fp32_vs_fp64": {"steps": S, "relative_l2": m["rel"], "ke_fp64": d["ke"], "ke_fp32": m["ke"],
+                         "max_divergence_fp32": m["div"], "max_divergence_fp64": d["div"],
+                         "trajectory_ms_per_step": {"fp32_mixed": m["ms_traj"], "fp64": d["ms_traj"]}},
+        "kernels_ms_per_step": {k: round(v, 3) for k, v in prof.items() if v > 0},
+        "e2e": {"value": world * ncell / (m["e2e_ms"] * 1e-3), "unit": "cell-steps/s",
+                "h2d_bytes_per_step": m["h2d"], "d2h_bytes_per_step": m["d2h"]},
+        "roofline": {"bound": "hbm", "kernel": "sweep", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(ach / hbm, 4), "peak_kind": hbm_kind, "bytes_per_launch": sweep_bytes,
+                     "traffic": None},
+        "gpu_launches": m["launches"] * args.steps,
+        "clocks": m["clocks"],
+        "setup_seconds": round(setup_s, 1),
+        "learned": m.get("learned"),
+    }
+    print(json.dumps(line), flush=True)
+    barrier(world)
+    return 0
+
+
+def run_reference_urban_step(args):
+    """The oracle's cut-cell step (all host threads for the stencils, the
+    serial multigrid CG) on a bounded sample of the urban convective case:
+    128 x 128 x 48 cells of 2 m holding the case's box density (9 boxes),
+    one warm-up step and min(steps, 2) timed steps."""
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    from oracle.oracle import OracleSimulation, set_threads
+    n = (128, 128, 48)
+    g, ap, fluid, mkspec, state, desc = urban_step_case(n, 9)
+    cores = os.cpu_count() or 1
+    set_threads(cores)
+    o = OracleSimulation(mkspec("fp64"))
+    o.set_pcg(ap, tol=1e-8, maxit=500)
+    o.set_state(*state)
+    o.project()
+    o.step_rk3(1.0, 1)
+    k = max(1, min(args.steps, 2))
+    t0 = time.perf_counter()
+    o.step_rk3(1.0, k)
+    el = time.perf_counter() - t0
+    rate = g.ncells * k / el
+    line = {
+        "impl": "reference", "metric": "cell-steps/s", "value": rate, "unit": "cell-steps/s", "n_gpus": args.gpus,
+        "steps": k, "warmup": 1, "ms_per_step": 1e3 * el / k, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": dict(desc, sample=list(n)),
+        "cpu_baseline": {"value": rate, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+                         "sample": f"{k} steps of a 128x128x48 sample (9 boxes) after one warm-up, FP64 oracle, "
+                                   f"{cores} OpenMP threads for the stencils, serial multigrid CG"},
+        "e2e": {"value": rate, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_b200(args):
     world, rank, local = dist_setup()
     import torch
@@ -697,15 +906,21 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="cbl", choices=["cbl", "tgv", "urban", "hit"])
+    ap.add_argument("--workload", default="cbl", choices=["cbl", "tgv", "urban", "hit", "urban_step"])
     ap.add_argument("--hit-n", type=int, default=512)
     ap.add_argument("--hit-steps", type=int, default=100)
+    ap.add_argument("--urban-n", type=int, nargs=3, default=None)
+    ap.add_argument("--urban-boxes", type=int, default=600)
+    ap.add_argument("--urban-steps", type=int, default=10)
+    ap.add_argument("--learned", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.workload == "urban":
         rc = run_reference_urban(args) if args.impl == "reference" else run_b200_urban(args)
+    elif args.workload == "urban_step":
+        rc = run_reference_urban_step(args) if args.impl == "reference" else run_b200_urban_step(args)
     elif args.workload == "hit":
         rc = run_reference_hit(args) if args.impl == "reference" else run_b200_hit(args)
     else:

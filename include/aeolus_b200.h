@@ -194,7 +194,9 @@ enum { AEO_K_SGS = 0, AEO_K_SWEEP = 1, AEO_K_DIV_FFTX = 2, AEO_K_FFTY = 3, AEO_K
  * StepRecord (src/simulations/step_record.jl:1-263) are the analogue. */
 aeo_status aeo_profile_step(aeo_sim* h, double dt, double* ms_per_class, int32_t nclass);
 
-/* Number of kernel launches one RK3 step issues (for launch accounting). */
+/* Number of kernel launches one RK3 step issues (for launch accounting).
+   solver = AEO_SOLVER_PCG: counted with the iteration count of the last
+   pressure solve for all three substages (synchronises the stream). */
 aeo_status aeo_launches_per_step(aeo_sim* h, int32_t* out);
 
 /* The handle's CUDA stream (a cudaStream_t) for callers that time kernels. */

@@ -20,6 +20,7 @@
  * no FMA contraction, so that each operation rounds as Julia's does).
  */
 #include "aeolus_oracle.h"
+#include "mgpcg_oracle.h"
 
 #include <float.h>
 #include <math.h>
@@ -66,6 +67,10 @@ struct oc_sim {
     double meas_sum, gauge_sum;
     fft_plan px, py, pz;         /* px: length Nx/2 (the packed r2c) */
     cpx* twx;                    /* e^{-2 pi i k / Nx}, k <= Nx/2 */
+    /* solver = PCG: face apertures (interior face layout), the CG of the a^2 operator */
+    double *apx, *apy, *apz, *cgx;
+    ocg* cg;
+    ocg_stats cg_st;
 };
 
 #define ID(s, i, j, k) ((int64_t)(i) + (int64_t)(s)->NX * ((int64_t)(j) + (int64_t)(s)->NY * (int64_t)(k)))
@@ -990,6 +995,67 @@ int oc_apply_poisson_operator(oc_sim* s, const double* phi, double* out) {
 /* ------------------------------------------------------------------------- */
 
 /* stage: 0 plain Euler; otherwise c(x, snap) = ca*snap + cb*x */
+/* The cut-cell projection (solver = PCG; src/CutCell.jl:602-700, 852-880):
+ * b = sum over the faces of (+-) a u* / h (u* in the storage arrays, halos
+ * filled), phi = A^-1 b by MGPreconditionedCG with the a^2 face coefficients
+ * (src/Multigrid.jl:893-967) into cgx. */
+static void cc_solve(oc_sim* s) {
+    const oc_params* P = &s->p;
+    int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
+    int64_t pl = (int64_t)Nx * Ny;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                int64_t qi = i + (int64_t)Nx * (j + (int64_t)Ny * k);
+                int64_t xr = (int64_t)(Nx + 1) * (j + (int64_t)Ny * k), yr = (int64_t)Nx * (j + (int64_t)(Ny + 1) * k);
+                int I = i + Hx, J = j + Hy, K = k + Hz;
+                double aw = s->apx[xr + i], ae = s->apx[xr + i + 1];
+                double as = s->apy[yr + i], an = s->apy[yr + Nx + i];
+                double ab = s->apz[qi], at = s->apz[qi + pl];
+                s->src[qi] = (ae * A(s->u, I + 1, J, K) - aw * A(s->u, I, J, K)) * s->idx +
+                             (an * A(s->v, I, J + 1, K) - as * A(s->v, I, J, K)) * s->idy +
+                             (at * A(s->w, I, J, K + 1) - ab * A(s->w, I, J, K)) * s->idz;
+            }
+    ocg_solve(s->cg, s->src, s->cgx, &s->cg_st);
+}
+
+/* u = c(u* - a d(phi), u^n) on every face (0 on a blocked one), theta =
+ * c(theta + dt t_theta, theta^n) (with_theta), p = phi/dt; c(x, s) = ca s + cb x
+ * in stages 2 and 3. */
+static void cc_correct(oc_sim* s, double dt, int stage, double ca, double cb, int with_theta) {
+    const oc_params* P = &s->p;
+    int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
+    int64_t pl = (int64_t)Nx * Ny;
+    const double* phi = s->cgx;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                int64_t qi = i + (int64_t)Nx * (j + (int64_t)Ny * k);
+                int64_t q = ID(s, i + Hx, j + Hy, k + Hz);
+                double pc = phi[qi];
+                double pw = phi[i > 0 ? qi - 1 : qi + Nx - 1];
+                double ps = phi[j > 0 ? qi - Nx : qi + (int64_t)(Ny - 1) * Nx];
+                double pb = phi[k > 0 ? qi - pl : (P->bc_z == OC_BC_PERIODIC ? qi + (int64_t)(Nz - 1) * pl : qi)];
+                double aw = s->apx[(int64_t)(Nx + 1) * (j + (int64_t)Ny * k) + i];
+                double as = s->apy[(int64_t)Nx * (j + (int64_t)(Ny + 1) * k) + i];
+                double ab = s->apz[qi];
+                double un = aw > 0 ? s->u[q] - aw * ((pc - pw) * s->idx) : 0.0;
+                double vn = as > 0 ? s->v[q] - as * ((pc - ps) * s->idy) : 0.0;
+                double wn = ab > 0 ? s->w[q] - ab * ((pc - pb) * s->idz) : 0.0;
+                double tn = with_theta ? s->th[q] + dt * s->tt[q] : s->th[q];
+                if (stage) {
+                    un = ca * s->u0[q] + cb * un;
+                    vn = ca * s->v0[q] + cb * vn;
+                    wn = ca * s->w0[q] + cb * wn;
+                    tn = ca * s->th0[q] + cb * tn;
+                }
+                s->u[q] = un; s->v[q] = vn; s->w[q] = wn; s->th[q] = tn;
+                s->pr[q] = pc / dt;
+            }
+}
+
 static void substage(oc_sim* s, double dt, int stage, double ca, double cb) {
     const oc_params* P = &s->p;
     int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
@@ -1010,6 +1076,11 @@ static void substage(oc_sim* s, double dt, int stage, double ca, double cb) {
     fill_halos(s, s->u, LOC_FX);
     fill_halos(s, s->v, LOC_FY);
     fill_halos(s, s->w, LOC_FZ);
+    if (P->solver == OC_SOLVER_PCG) {
+        cc_solve(s);
+        cc_correct(s, dt, stage, ca, cb, 1);
+        return;
+    }
 #pragma omp parallel for collapse(2) schedule(static)
     for (int k = 0; k < Nz; ++k)
         for (int j = 0; j < Ny; ++j)
@@ -1057,6 +1128,11 @@ int oc_project(oc_sim* s) {
     fill_halos(s, s->u, LOC_FX);
     fill_halos(s, s->v, LOC_FY);
     fill_halos(s, s->w, LOC_FZ);
+    if (P->solver == OC_SOLVER_PCG) {
+        cc_solve(s);
+        cc_correct(s, 1.0, 0, 0.0, 0.0, 0);
+        return 0;
+    }
 #pragma omp parallel for collapse(2) schedule(static)
     for (int k = 0; k < Nz; ++k)
         for (int j = 0; j < Ny; ++j)
@@ -1232,7 +1308,17 @@ double oc_max_divergence(oc_sim* s) {
     for (int k = Hz; k < Hz + Nz; ++k)
         for (int j = Hy; j < Hy + Ny; ++j)
             for (int i = Hx; i < Hx + Nx; ++i) {
-                double d = s->wc ? wdiv_at(s, s->u, s->v, s->w, i, j, k) / s->wc[k] : div_at(s, s->u, s->v, s->w, i, j, k);
+                double d;
+                if (P->solver == OC_SOLVER_PCG) {
+                    int64_t qi = (i - Hx) + (int64_t)Nx * ((j - Hy) + (int64_t)Ny * (k - Hz));
+                    int64_t xr = (int64_t)(Nx + 1) * ((j - Hy) + (int64_t)Ny * (k - Hz));
+                    int64_t yr = (int64_t)Nx * ((j - Hy) + (int64_t)(Ny + 1) * (k - Hz));
+                    d = (s->apx[xr + i - Hx + 1] * A(s->u, i + 1, j, k) - s->apx[xr + i - Hx] * A(s->u, i, j, k)) * s->idx +
+                        (s->apy[yr + Nx + i - Hx] * A(s->v, i, j + 1, k) - s->apy[yr + i - Hx] * A(s->v, i, j, k)) * s->idy +
+                        (s->apz[qi + (int64_t)Nx * Ny] * A(s->w, i, j, k + 1) - s->apz[qi] * A(s->w, i, j, k)) * s->idz;
+                } else {
+                    d = s->wc ? wdiv_at(s, s->u, s->v, s->w, i, j, k) / s->wc[k] : div_at(s, s->u, s->v, s->w, i, j, k);
+                }
                 d = fabs(d);
                 if (d > m) m = d;
             }
@@ -1255,6 +1341,7 @@ oc_sim* oc_create(const oc_params* p, const double* zfi, const double* wc, const
     if (p->solver == OC_SOLVER_FFT && p->bc_z != OC_BC_PERIODIC) return NULL;
     if (p->solver == OC_SOLVER_COLUMN && p->bc_z != OC_BC_WALL) return NULL;
     if (p->stretched && (!zfi || p->bc_z != OC_BC_WALL)) return NULL;
+    if (p->solver == OC_SOLVER_PCG && (p->stretched || p->core != OC_CORE_BOUSSINESQ)) return NULL;
     oc_sim* s = (oc_sim*)calloc(1, sizeof(oc_sim));
     s->p = *p;
     s->NX = p->nx + 2 * p->hx; s->NY = p->ny + 2 * p->hy; s->NZ = p->nz + 2 * p->hz;
@@ -1369,7 +1456,68 @@ oc_sim* oc_create(const oc_params* p, const double* zfi, const double* wc, const
         s->meas_sum = 0.0; s->gauge_sum = 0.0;
         for (int k = 0; k < Nz; ++k) { s->meas_sum += s->meas[k]; s->gauge_sum += s->gauge[k]; }
     }
+    if (p->solver == OC_SOLVER_PCG) {
+        s->cgx = dalloc((int64_t)Nx * Ny * Nz);
+        if (oc_set_apertures(s, NULL, NULL, NULL, 1e-8, 200)) {
+            oc_destroy(s);
+            return NULL;
+        }
+    }
     return s;
+}
+
+int oc_set_apertures(oc_sim* s, const double* ax, const double* ay, const double* az, double tol, int maxit) {
+    const oc_params* P = &s->p;
+    if (P->solver != OC_SOLVER_PCG || !(tol > 0) || maxit < 1) return -1;
+    if ((ax == NULL) != (ay == NULL) || (ax == NULL) != (az == NULL)) return -1;
+    int Nx = P->nx, Ny = P->ny, Nz = P->nz;
+    int64_t n[3] = {(int64_t)(Nx + 1) * Ny * Nz, (int64_t)Nx * (Ny + 1) * Nz, (int64_t)Nx * Ny * (Nz + 1)};
+    const double* in[3] = {ax, ay, az};
+    double* a[3];
+    double* c2[3];
+    for (int d = 0; d < 3; ++d) {
+        a[d] = dalloc(n[d]);
+        c2[d] = dalloc(n[d]);
+        for (int64_t q = 0; q < n[d]; ++q) a[d][q] = in[d] ? in[d][q] : 1.0;
+    }
+    int bad = 0;
+    for (int d = 0; d < 3; ++d)
+        for (int64_t q = 0; q < n[d]; ++q)
+            if (!(a[d][q] >= 0.0 && a[d][q] <= 1.0)) bad = 1;
+    if (P->bc_z == OC_BC_WALL)
+        for (int64_t q = 0; q < (int64_t)Nx * Ny; ++q) {
+            a[2][q] = 0.0;
+            a[2][(int64_t)Nz * Nx * Ny + q] = 0.0;
+        }
+    for (int d = 0; d < 3; ++d)
+        for (int64_t q = 0; q < n[d]; ++q) c2[d][q] = a[d][q] * a[d][q];
+    ocg* cg = NULL;
+    if (!bad) {
+        ocg_params prm = {Nx, Ny, Nz, s->dx, s->dy, s->dz, OCG_BC_PERIODIC, OCG_BC_PERIODIC,
+                          P->bc_z == OC_BC_WALL ? OCG_BC_NEUMANN : OCG_BC_PERIODIC, tol, maxit,
+                          2, 2, 50, 4, 1, OCG_PC_VCYCLE};
+        cg = ocg_create(&prm, c2[0], c2[1], c2[2]);
+    }
+    for (int d = 0; d < 3; ++d) free(c2[d]);
+    if (!cg) {
+        for (int d = 0; d < 3; ++d) free(a[d]);
+        return -1;
+    }
+    free(s->apx); free(s->apy); free(s->apz);
+    if (s->cg) ocg_destroy(s->cg);
+    s->apx = a[0]; s->apy = a[1]; s->apz = a[2];
+    s->cg = cg;
+    memset(&s->cg_st, 0, sizeof(s->cg_st));
+    return 0;
+}
+
+int oc_pcg_stats(const oc_sim* s, int* iterations, int* status, double* residual, double* bnorm) {
+    if (s->p.solver != OC_SOLVER_PCG) return -1;
+    if (iterations) *iterations = s->cg_st.iterations;
+    if (status) *status = s->cg_st.status;
+    if (residual) *residual = s->cg_st.residual;
+    if (bnorm) *bnorm = s->cg_st.bnorm;
+    return 0;
 }
 
 void oc_destroy(oc_sim* s) {
@@ -1380,6 +1528,8 @@ void oc_destroy(oc_sim* s) {
                       s->lower, s->upper, s->hw, s->meas, s->iota, s->gauge};
     for (size_t q = 0; q < sizeof(ptrs) / sizeof(ptrs[0]); ++q) free(ptrs[q]);
     free(s->hat); free(s->twx);
+    free(s->apx); free(s->apy); free(s->apz); free(s->cgx);
+    if (s->cg) ocg_destroy(s->cg);
     plan_free(&s->px); plan_free(&s->py); plan_free(&s->pz);
     free(s);
 }

@@ -24,7 +24,7 @@ extern "C" {
 enum { OC_BC_PERIODIC = 0, OC_BC_WALL = 1 };
 enum { OC_CORE_BOUSSINESQ = 0, OC_CORE_ANELASTIC = 1 };
 enum { OC_ADV_CENTRED = 0, OC_ADV_WENO_JS5 = 1, OC_ADV_WENO_Z5 = 2 };
-enum { OC_SOLVER_FFT = 0, OC_SOLVER_COLUMN = 1 };
+enum { OC_SOLVER_FFT = 0, OC_SOLVER_COLUMN = 1, OC_SOLVER_PCG = 2 };
 enum { OC_U = 0, OC_V = 1, OC_W = 2, OC_THETA = 3, OC_P = 4, OC_NUT = 5, OC_PHI = 6 };
 
 typedef struct {
@@ -66,7 +66,18 @@ int oc_pressure_solve(oc_sim* s, const double* src, double* phi);
 /* Apply the discrete operator the solver inverts (interior-sized in/out). */
 int oc_apply_poisson_operator(oc_sim* s, const double* phi, double* out);
 double oc_kinetic_energy(oc_sim* s);
+/* max |divergence|; solver = OC_SOLVER_PCG: the aperture-weighted one */
 double oc_max_divergence(oc_sim* s);
+/* solver = OC_SOLVER_PCG (uniform Boussinesq grid): the face apertures in
+ * [0, 1] in the interior face layout of mgpcg_oracle.h (all NULL: every face
+ * open; the wall faces of a bounded z are blocked whatever is given) and the
+ * multigrid-preconditioned CG's relative tolerance and iteration cap.  The
+ * projection solves sum_faces a^2 (phi_nbr - phi) / h^2 = the
+ * aperture-weighted divergence and corrects u = u* - a d(phi) on every face
+ * (zero on a blocked face).  0 on success. */
+int oc_set_apertures(oc_sim* s, const double* ax, const double* ay, const double* az, double tol, int maxit);
+/* iterations, status (mgpcg_oracle.h OCG_*), ||r|| and ||b|| of the last solve */
+int oc_pcg_stats(const oc_sim* s, int* iterations, int* status, double* residual, double* bnorm);
 void oc_set_threads(int n);
 
 /* Philox4x32-10 block function and the uniform fill of the synthetic inputs. */

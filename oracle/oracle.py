@@ -82,6 +82,9 @@ def load():
     lib.oc_max_divergence.argtypes = [P]
     lib.oc_max_divergence.restype = C.c_double
     lib.oc_set_threads.argtypes = [C.c_int]
+    lib.oc_set_apertures.argtypes = [P, _D, _D, _D, C.c_double, C.c_int]
+    lib.oc_pcg_stats.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                 C.POINTER(C.c_double)]
     lib.oc_philox4x32.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     lib.oc_uniform_fill.argtypes = [C.c_uint64, C.c_uint32, C.c_int64, C.c_double, _D]
     _lib = lib
@@ -90,7 +93,8 @@ def load():
 
 FIELD_IDS = {"u": 0, "v": 1, "w": 2, "theta": 3, "p": 4, "nut": 5, "phi": 6}
 _ADV = {"centred": 0, "weno_js5": 1, "weno_z5": 2}
-_SOLV = {"fft": 0, "column": 1}
+_SOLV = {"fft": 0, "column": 1, "pcg": 2}
+_PCG_STATUS = {0: "converged", 1: "maxit", 2: "breakdown", 3: "zero_rhs"}
 _CORE = {"boussinesq": 0, "anelastic": 1}
 
 
@@ -216,6 +220,28 @@ class OracleSimulation:
         out = np.empty_like(p)
         self._lib.oc_apply_poisson_operator(self._h, _p(p), _p(out))
         return out
+
+    def set_pcg(self, apertures=None, tol=1e-8, maxit=200):
+        """solver = "pcg": the face apertures (ax, ay, az) in the interior face
+        layout (None: every face open) and the CG tolerance and cap."""
+        if apertures is None:
+            ptrs = (None, None, None)
+        else:
+            g = self.grid
+            nx, ny, nz = g.size
+            a = [np.ascontiguousarray(x, dtype=np.float64) for x in apertures]
+            assert a[0].shape == (nz, ny, nx + 1) and a[1].shape == (nz, ny + 1, nx) and a[2].shape == (nz + 1, ny, nx)
+            self._ap = a
+            ptrs = tuple(_p(x) for x in a)
+        if self._lib.oc_set_apertures(self._h, *ptrs, float(tol), int(maxit)) != 0:
+            raise ValueError("oracle: set_pcg rejected (solver, tolerance or apertures)")
+
+    def pcg_stats(self):
+        it, stt = C.c_int(), C.c_int()
+        r, b = C.c_double(), C.c_double()
+        assert self._lib.oc_pcg_stats(self._h, C.byref(it), C.byref(stt), C.byref(r), C.byref(b)) == 0
+        return {"iterations": it.value, "status": _PCG_STATUS[stt.value], "residual": r.value, "bnorm": b.value,
+                "relative_residual": 0.0 if b.value == 0 else r.value / b.value}
 
     def kinetic_energy(self):
         return self._lib.oc_kinetic_energy(self._h)
