@@ -170,8 +170,9 @@ class MGPreconditionedCG:
     def profile(self, what: str, reps: int = 20) -> float:
         """Mean device ms of one part: "solve", "rbgs" (one finest colour
         pass), "apply" (operator + p.Ap), "vcycle", "coarsest" (the
-        coarsest-level sweeps), "restrict" (finest residual restriction)."""
-        code = {"solve": 0, "rbgs": 1, "apply": 2, "vcycle": 3, "coarsest": 4, "restrict": 5}[what]
+        coarsest-level sweeps), "restrict" (finest residual restriction),
+        "sweep" (one whole finest red-black sweep as the cycle runs it)."""
+        code = {"solve": 0, "rbgs": 1, "apply": 2, "vcycle": 3, "coarsest": 4, "restrict": 5, "sweep": 6}[what]
         ms = C.c_double()
         self._chk(L.load().aeo_mg_profile(self._h, code, int(reps), C.byref(ms)))
         return ms.value

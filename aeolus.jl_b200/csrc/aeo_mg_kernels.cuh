@@ -12,7 +12,7 @@
 namespace mgk {
 
 constexpr int TPB = 256;
-constexpr int RED_BLOCKS = 592;        // 4 x 148 SMs: the fixed grid of every FP64 reduction
+constexpr int RED_BLOCKS = 1184;       // 8 x 148 SMs (2048 threads an SM): the fixed grid of every FP64 reduction
 constexpr int COARSE_THREADS = 1024;
 constexpr int COARSE_MAX_CELLS = 16384;
 constexpr int RB_X = 32, RB_Y = 8;     // block of the 3-D stencil grids
@@ -107,24 +107,56 @@ __device__ __forceinline__ V aphi(const V* f, const Idx& d, const Coef<C>& cf, V
            (fzp * (f[d.zp] - c) - fzm * (c - f[d.zm])) * iz2;
 }
 
-// One RB-GS update (src/Multigrid.jl:311-336); false for a fully blocked
-// cell (|diag| < eps), which keeps its value.
-template <typename R>
-__device__ __forceinline__ bool gs_value(const R* f, R bval, const Idx& d, const Level<R>& L, R* out) {
-    R off, diag;
-    if (!L.c.var()) {
-        diag = -R(2) * (L.ix2 + L.iy2 + L.iz2);
-        off = (f[d.xp] + f[d.xm]) * L.ix2 + (f[d.yp] + f[d.ym]) * L.iy2 + (f[d.zp] + f[d.zm]) * L.iz2;
-    } else {
-        R fxp = L.c.x(d.cx + 1), fxm = L.c.x(d.cx);
-        R fyp = L.c.y(d.cy + d.sy), fym = L.c.y(d.cy);
-        R fzp = L.c.z(d.q + d.sz), fzm = L.c.z(d.q);
-        diag = -((fxp + fxm) * L.ix2 + (fyp + fym) * L.iy2 + (fzp + fzm) * L.iz2);
-        if (fabs(diag) < Eps<R>::v()) return false;
-        off = (fxp * f[d.xp] + fxm * f[d.xm]) * L.ix2 + (fyp * f[d.yp] + fym * f[d.ym]) * L.iy2 +
-              (fzp * f[d.zp] + fzm * f[d.zm]) * L.iz2;
+// The coefficient form of a level, as a kernel template parameter: the
+// constant-coefficient Laplacian, one-byte codes into the level's value
+// table (staged in shared memory), or per-face values.
+enum { CF_CONST = 0, CF_CODES = 1, CF_VALUES = 2 };
+
+template <typename R, int CF>
+__device__ __forceinline__ R face_coef(const R* vals, const unsigned char* codes, const R* stab, int f) {
+    if (CF == CF_CODES) return stab[codes[f]];
+    return vals[f];
+}
+
+// The six neighbours of cell q = (i, j, k): the interior steps, or at a
+// boundary the periodic wrap / the Neumann mirror (the cell itself) -- the
+// maps of make_idx, formed from q with adds and selects.
+struct Nbr {
+    int xm, xp, ym, yp, zm, zp;
+};
+__device__ __forceinline__ Nbr nbr_of(int q, int i, int j, int k, int nx, int ny, int nz, int pl, Bc bc) {
+    Nbr n;
+    n.xm = i > 0 ? q - 1 : (bc.x == 0 ? q + nx - 1 : q);
+    n.xp = i < nx - 1 ? q + 1 : (bc.x == 0 ? q - (nx - 1) : q);
+    n.ym = j > 0 ? q - nx : (bc.y == 0 ? q + (ny - 1) * nx : q);
+    n.yp = j < ny - 1 ? q + nx : (bc.y == 0 ? q - (ny - 1) * nx : q);
+    n.zm = k > 0 ? q - pl : (bc.z == 0 ? q + (nz - 1) * pl : q);
+    n.zp = k < nz - 1 ? q + pl : (bc.z == 0 ? q - (nz - 1) * pl : q);
+    return n;
+}
+
+// the smoother's division: IEEE in FP64 (the reference's arithmetic); the
+// FP32 cycle (a preconditioner of FP64 CG) divides with the fast reciprocal
+// (within 2 ulp)
+__device__ __forceinline__ double gs_div(double a, double b) { return a / b; }
+__device__ __forceinline__ float gs_div(float a, float b) { return __fdividef(a, b); }
+
+// One RB-GS update (src/Multigrid.jl:311-336) from the six neighbour values
+// and face coefficients; false for a fully blocked cell (|diag| < eps),
+// which keeps its value.
+template <typename R, int CF>
+__device__ __forceinline__ bool gs_vals(R nxp, R nxm, R nyp, R nym, R nzp, R nzm, R fxp, R fxm, R fyp, R fym, R fzp,
+                                        R fzm, R bval, R ix2, R iy2, R iz2, R* out) {
+    if (CF == CF_CONST) {
+        const R diag = -R(2) * (ix2 + iy2 + iz2);
+        const R off = (nxp + nxm) * ix2 + (nyp + nym) * iy2 + (nzp + nzm) * iz2;
+        *out = gs_div(bval - off, diag);
+        return true;
     }
-    *out = (bval - off) / diag;
+    const R diag = -((fxp + fxm) * ix2 + (fyp + fym) * iy2 + (fzp + fzm) * iz2);
+    if (fabs(diag) < Eps<R>::v()) return false;
+    const R off = (fxp * nxp + fxm * nxm) * ix2 + (fyp * nyp + fym * nym) * iy2 + (fzp * nzp + fzm * nzm) * iz2;
+    *out = gs_div(bval - off, diag);
     return true;
 }
 
@@ -254,20 +286,44 @@ __global__ void pcg_init_kernel(const double* __restrict__ b, double* __restrict
 
 // Ap = A p with p.Ap; the last block forms alpha or flags a breakdown.
 // Block (32, 8): lanes along x, warps over rows, rows looped on a fixed grid.
-template <typename C>
-__global__ void pcg_apply_kernel(const double* __restrict__ p, double* __restrict__ Ap, Coef<C> cf, int nx, int ny,
-                                 int nz, Bc bc, double ix2, double iy2, double iz2, PcgState* S, double* part,
-                                 int standalone) {
+// The coefficient form is a template parameter (codes: the table, padded to
+// 256 entries, staged in shared memory); the arithmetic of aphi in FP64.
+template <typename C, int CF>
+__global__ void __launch_bounds__(RB_X * RB_Y) pcg_apply_kernel(const double* __restrict__ p, double* __restrict__ Ap,
+                                                               Coef<C> cf, int nx, int ny, int nz, Bc bc, double ix2,
+                                                               double iy2, double iz2, PcgState* S, double* part,
+                                                               int standalone) {
+    __shared__ double stab[CF == CF_CODES ? 256 : 1];
     if (!standalone && S->done) return;
+    if (CF == CF_CODES) {
+        for (int q = tid(); q < 256; q += nthreads()) stab[q] = double(cf.tab[q]);
+        __syncthreads();
+    }
     double v[1] = {0.0};
-    const int nrows = ny * nz;
+    const int nrows = ny * nz, pl = nx * ny;
     for (int row = blockIdx.x * blockDim.y + threadIdx.y; row < nrows; row += gridDim.x * blockDim.y) {
         const int j = row % ny, k = row / ny;
         for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-            Idx d = make_idx(i, j, k, nx, ny, nz, bc);
-            double a = aphi<double, C>(p, d, cf, ix2, iy2, iz2);
-            Ap[d.q] = a;
-            v[0] += p[d.q] * a;
+            const int q = i + nx * row;
+            const Nbr n = nbr_of(q, i, j, k, nx, ny, nz, pl, bc);
+            const double c = p[q];
+            double a;
+            if (CF == CF_CONST) {
+                a = (p[n.xp] - 2.0 * c + p[n.xm]) * ix2 + (p[n.yp] - 2.0 * c + p[n.ym]) * iy2 +
+                    (p[n.zp] - 2.0 * c + p[n.zm]) * iz2;
+            } else {
+                const int fx = q + j + ny * k, fy = q + nx * k;
+                const double fxm = CF == CF_CODES ? stab[cf.kx[fx]] : double(cf.cx[fx]);
+                const double fxp = CF == CF_CODES ? stab[cf.kx[fx + 1]] : double(cf.cx[fx + 1]);
+                const double fym = CF == CF_CODES ? stab[cf.ky[fy]] : double(cf.cy[fy]);
+                const double fyp = CF == CF_CODES ? stab[cf.ky[fy + nx]] : double(cf.cy[fy + nx]);
+                const double fzm = CF == CF_CODES ? stab[cf.kz[q]] : double(cf.cz[q]);
+                const double fzp = CF == CF_CODES ? stab[cf.kz[q + pl]] : double(cf.cz[q + pl]);
+                a = (fxp * (p[n.xp] - c) - fxm * (c - p[n.xm])) * ix2 + (fyp * (p[n.yp] - c) - fym * (c - p[n.ym])) * iy2 +
+                    (fzp * (p[n.zp] - c) - fzm * (c - p[n.zm])) * iz2;
+            }
+            Ap[q] = a;
+            v[0] += c * a;
         }
     }
     double t[1];
@@ -438,27 +494,105 @@ __global__ void mg_first_kernel(Level<R> L, Bc bc, const double* __restrict__ r0
     }
 }
 
-// One colour pass of red-black Gauss-Seidel over an even-nx level.
-template <typename R>
-__global__ void mg_rbgs_kernel(Level<R> L, Bc bc, int colour, const int* done) {
+// One colour pass of red-black Gauss-Seidel over an even-nx level.  A
+// thread owns an x-pair of cells and marches RB_K levels up their column:
+// the pair is one vector load per level and stays in registers as the
+// z-neighbours of the next level and the x-neighbour of the updated cell
+// (the pair's other cell), so an update loads the pair above, the x
+// neighbour outside the pair, the two y neighbours, b and its face
+// coefficients; every neighbour is of the other colour, so the pass has no
+// order.  The coefficient form is a template parameter (codes: the level's
+// table, padded to 256 entries, staged in shared memory); K = 1 on levels too
+// small to fill the GPU with K-level columns.
+
+template <typename R> struct Vec2;
+template <> struct Vec2<float> { using T = float2; };
+template <> struct Vec2<double> { using T = double2; };
+
+template <typename R, int CF, int RB_K>
+__global__ void __launch_bounds__(RB_X * RB_Y) mg_rbgs_kernel(Level<R> L, Bc bc, int colour, const int* done) {
+    __shared__ R stab[CF == CF_CODES ? 256 : 1];
     if (*done) return;
-    const int ih = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
-    if (ih >= (L.nx >> 1) || j >= L.ny) return;
-    const int i = 2 * ih + ((j + k + colour) & 1);
-    Idx d = make_idx(i, j, k, L.nx, L.ny, L.nz, bc);
-    R v;
-    if (gs_value<R>(L.phi, L.b[d.q], d, L, &v)) L.phi[d.q] = v;
+    if (CF == CF_CODES) {
+        for (int q = tid(); q < 256; q += nthreads()) stab[q] = L.c.tab[q];
+        __syncthreads();
+    }
+    using V2 = typename Vec2<R>::T;
+    const int ih = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k0 = blockIdx.z * RB_K;
+    const int nx = L.nx, ny = L.ny, nz = L.nz, pl = nx * ny;
+    if (ih >= (nx >> 1) || j >= ny) return;
+    const int i0 = 2 * ih, row0 = i0 + nx * j;
+    // in-plane neighbours outside the pair (-1 / 0: the Neumann mirror, the cell itself)
+    const int xl = i0 > 0 ? row0 - 1 : (bc.x == 0 ? row0 + nx - 1 : -1);
+    const int xr = i0 + 2 < nx ? row0 + 2 : (bc.x == 0 ? row0 + 2 - nx : -1);
+    const int dym = j > 0 ? -nx : (bc.y == 0 ? (ny - 1) * nx : 0);
+    const int dyp = j < ny - 1 ? nx : (bc.y == 0 ? -(ny - 1) * nx : 0);
+    const R* __restrict__ f = L.phi;
+    auto pair_at = [&](int k) { return *reinterpret_cast<const V2*>(f + (size_t)k * pl + row0); };
+    V2 pc = pair_at(k0);
+    V2 pm = k0 > 0 ? pair_at(k0 - 1) : (bc.z == 0 ? pair_at(nz - 1) : pc);
+#pragma unroll
+    for (int kk = 0; kk < RB_K; ++kk) {
+        const int k = k0 + kk;
+        if (k >= nz) break;
+        const V2 pp = k + 1 < nz ? pair_at(k + 1) : (bc.z == 0 ? pair_at(0) : pc);
+        const int a = (j + k + colour) & 1;   // the pair's cell of this colour
+        const int q = k * pl + row0 + a;
+        const R c = a ? pc.y : pc.x;
+        const R nxm = a ? pc.x : (xl >= 0 ? f[k * pl + xl] : c);
+        const R nxp = a ? (xr >= 0 ? f[k * pl + xr] : c) : pc.y;
+        const R nym = dym ? f[q + dym] : c;
+        const R nyp = dyp ? f[q + dyp] : c;
+        const R nzm = a ? pm.y : pm.x, nzp = a ? pp.y : pp.x;
+        R fxp = R(0), fxm = R(0), fyp = R(0), fym = R(0), fzp = R(0), fzm = R(0);
+        if (CF != CF_CONST) {
+            const int fx = q + j + ny * k, fy = q + nx * k;   // (nx+1)(j + ny k) + i, nx(j + (ny+1) k) + i
+            fxm = face_coef<R, CF>(L.c.cx, L.c.kx, stab, fx);
+            fxp = face_coef<R, CF>(L.c.cx, L.c.kx, stab, fx + 1);
+            fym = face_coef<R, CF>(L.c.cy, L.c.ky, stab, fy);
+            fyp = face_coef<R, CF>(L.c.cy, L.c.ky, stab, fy + nx);
+            fzm = face_coef<R, CF>(L.c.cz, L.c.kz, stab, q);
+            fzp = face_coef<R, CF>(L.c.cz, L.c.kz, stab, q + pl);
+        }
+        R v;
+        if (gs_vals<R, CF>(nxp, nxm, nyp, nym, nzp, nzm, fxp, fxm, fyp, fym, fzp, fzm, L.b[q], L.ix2, L.iy2, L.iz2, &v))
+            L.phi[q] = v;
+        pm = pc;
+        pc = pp;
+    }
 }
 
 // r = b - A phi on a level (_compute_residual!, src/Multigrid.jl:281-285):
-// one thread per cell, a 3-D grid.
-template <typename R>
-__global__ void mg_residual_kernel(Level<R> F, Bc bc, const int* done) {
+// one thread per cell, a 3-D grid; the arithmetic of aphi.
+template <typename R, int CF>
+__global__ void __launch_bounds__(RB_X * RB_Y) mg_residual_kernel(Level<R> F, Bc bc, const int* done) {
+    __shared__ R stab[CF == CF_CODES ? 256 : 1];
     if (*done) return;
+    if (CF == CF_CODES) {
+        for (int q = tid(); q < 256; q += nthreads()) stab[q] = F.c.tab[q];
+        __syncthreads();
+    }
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
-    if (i >= F.nx || j >= F.ny) return;
-    Idx d = make_idx(i, j, k, F.nx, F.ny, F.nz, bc);
-    F.r[d.q] = F.b[d.q] - aphi<R, R>(F.phi, d, F.c, F.ix2, F.iy2, F.iz2);
+    const int nx = F.nx, ny = F.ny, nz = F.nz, pl = nx * ny;
+    if (i >= nx || j >= ny) return;
+    const int q = i + nx * (j + ny * k);
+    const Nbr n = nbr_of(q, i, j, k, nx, ny, nz, pl, bc);
+    const R* __restrict__ f = F.phi;
+    const R c = f[q];
+    R a;
+    if (CF == CF_CONST) {
+        a = (f[n.xp] - R(2) * c + f[n.xm]) * F.ix2 + (f[n.yp] - R(2) * c + f[n.ym]) * F.iy2 +
+            (f[n.zp] - R(2) * c + f[n.zm]) * F.iz2;
+    } else {
+        const int fx = q + j + ny * k, fy = q + nx * k;
+        const R fxm = face_coef<R, CF>(F.c.cx, F.c.kx, stab, fx), fxp = face_coef<R, CF>(F.c.cx, F.c.kx, stab, fx + 1);
+        const R fym = face_coef<R, CF>(F.c.cy, F.c.ky, stab, fy), fyp = face_coef<R, CF>(F.c.cy, F.c.ky, stab, fy + nx);
+        const R fzm = face_coef<R, CF>(F.c.cz, F.c.kz, stab, q), fzp = face_coef<R, CF>(F.c.cz, F.c.kz, stab, q + pl);
+        a = (fxp * (f[n.xp] - c) - fxm * (c - f[n.xm])) * F.ix2 + (fyp * (f[n.yp] - c) - fym * (c - f[n.ym])) * F.iy2 +
+            (fzp * (f[n.zp] - c) - fzm * (c - f[n.zm])) * F.iz2;
+    }
+    F.r[q] = F.b[q] - a;
 }
 
 // Coarse b = mean of the eight fine residuals (src/Multigrid.jl:380-406),

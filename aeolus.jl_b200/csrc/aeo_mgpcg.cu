@@ -323,11 +323,13 @@ struct Mg : MgBase {
                     if (aeo_status s = upload(&V.c.kx, kx)) return s;
                     if (aeo_status s = upload(&V.c.ky, ky)) return s;
                     if (aeo_status s = upload(&V.c.kz, kz)) return s;
-                    if (aeo_status s = upload(&V.c.tab, tab)) return s;
+                    std::vector<double> tab256(tab);
+                    tab256.resize(256, 0.0);   // the smoothers stage all 256 entries in shared memory
+                    if (aeo_status s = upload(&V.c.tab, tab256)) return s;
                     ++coded_levels;
                     if (nl == 0) {
                         opd.kx = V.c.kx; opd.ky = V.c.ky; opd.kz = V.c.kz;
-                        if (aeo_status s = upload(&opd.tab, tab)) return s;
+                        if (aeo_status s = upload(&opd.tab, tab256)) return s;
                     }
                 } else {
                     if (aeo_status s = upload(&V.c.cx, hx)) return s;
@@ -440,11 +442,17 @@ struct Mg : MgBase {
         const dim3 blk(RB_X, RB_Y);
         const int nb = row_blocks(cfg.ny * cfg.nz);
         if (op_f32)
-            pcg_apply_kernel<float><<<nb, blk, 0, s>>>(in, out, opf, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2, iz2, S,
-                                                       part, standalone);
+            pcg_apply_kernel<float, CF_VALUES><<<nb, blk, 0, s>>>(in, out, opf, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2,
+                                                                  iz2, S, part, standalone);
+        else if (opd.kx)
+            pcg_apply_kernel<double, CF_CODES><<<nb, blk, 0, s>>>(in, out, opd, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2,
+                                                                  iz2, S, part, standalone);
+        else if (opd.cx)
+            pcg_apply_kernel<double, CF_VALUES><<<nb, blk, 0, s>>>(in, out, opd, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2,
+                                                                   iz2, S, part, standalone);
         else
-            pcg_apply_kernel<double><<<nb, blk, 0, s>>>(in, out, opd, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2, iz2, S,
-                                                        part, standalone);
+            pcg_apply_kernel<double, CF_CONST><<<nb, blk, 0, s>>>(in, out, opd, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2,
+                                                                  iz2, S, part, standalone);
         CKL();
         return AEO_OK;
     }
@@ -498,18 +506,14 @@ struct Mg : MgBase {
             if (l > 0 || from_zero) {
                 mg_first_kernel<R><<<hg, blk, 0, s>>>(F, bc, l == 0 ? r0 : nullptr, mr, done);
                 CKL();
-                mg_rbgs_kernel<R><<<hg, blk, 0, s>>>(F, bc, 1, done);
-                CKL();
+                if (aeo_status q = launch_rbgs(s, F, 1, done)) return q;
                 sw0 = 1;
             }
             for (int sw = sw0; sw < cfg.nu1; ++sw)
-                for (int c = 0; c < 2; ++c) {
-                    mg_rbgs_kernel<R><<<hg, blk, 0, s>>>(F, bc, c, done);
-                    CKL();
-                }
+                for (int c = 0; c < 2; ++c)
+                    if (aeo_status q = launch_rbgs(s, F, c, done)) return q;
             Level<R>& Cl = L[l + 1];
-            mg_residual_kernel<R><<<cell_grid(F), blk, 0, s>>>(F, bc, done);
-            CKL();
+            if (aeo_status q = launch_residual(s, F, done)) return q;
             mg_restrict_kernel<R><<<restrict_grid(Cl), blk, 0, s>>>(F, Cl, part, &S->counter, done);
             CKL();
         }
@@ -518,13 +522,37 @@ struct Mg : MgBase {
             Level<R>& F = L[l];
             mg_prolong_kernel<R><<<cell_grid(F), blk, 0, s>>>(F, L[l + 1], bc, done);
             CKL();
-            const dim3 hg = half_grid(F);
             for (int sw = 0; sw < cfg.nu2; ++sw)
-                for (int c = 0; c < 2; ++c) {
-                    mg_rbgs_kernel<R><<<hg, blk, 0, s>>>(F, bc, c, done);
-                    CKL();
-                }
+                for (int c = 0; c < 2; ++c)
+                    if (aeo_status q = launch_rbgs(s, F, c, done)) return q;
         }
+        return AEO_OK;
+    }
+
+    // one colour pass / the residual of level F in its coefficient form
+    // columns of 8 levels a thread where that still leaves 8 blocks an SM
+    aeo_status launch_rbgs(cudaStream_t s, const Level<R>& F, int colour, const int* done) {
+        const unsigned bx = (unsigned)((F.nx / 2 + RB_X - 1) / RB_X), by = (unsigned)((F.ny + RB_Y - 1) / RB_Y);
+        const bool col = (size_t)bx * by * ((F.nz + 7) / 8) >= 8 * 148;
+        const dim3 hg(bx, by, (unsigned)(col ? (F.nz + 7) / 8 : F.nz)), blk(RB_X, RB_Y);
+        if (col) {
+            if (F.c.kx) mg_rbgs_kernel<R, CF_CODES, 8><<<hg, blk, 0, s>>>(F, bc, colour, done);
+            else if (F.c.cx) mg_rbgs_kernel<R, CF_VALUES, 8><<<hg, blk, 0, s>>>(F, bc, colour, done);
+            else mg_rbgs_kernel<R, CF_CONST, 8><<<hg, blk, 0, s>>>(F, bc, colour, done);
+        } else {
+            if (F.c.kx) mg_rbgs_kernel<R, CF_CODES, 1><<<hg, blk, 0, s>>>(F, bc, colour, done);
+            else if (F.c.cx) mg_rbgs_kernel<R, CF_VALUES, 1><<<hg, blk, 0, s>>>(F, bc, colour, done);
+            else mg_rbgs_kernel<R, CF_CONST, 1><<<hg, blk, 0, s>>>(F, bc, colour, done);
+        }
+        CKL();
+        return AEO_OK;
+    }
+    aeo_status launch_residual(cudaStream_t s, const Level<R>& F, const int* done) {
+        const dim3 g = cell_grid(F), blk(RB_X, RB_Y);
+        if (F.c.kx) mg_residual_kernel<R, CF_CODES><<<g, blk, 0, s>>>(F, bc, done);
+        else if (F.c.cx) mg_residual_kernel<R, CF_VALUES><<<g, blk, 0, s>>>(F, bc, done);
+        else mg_residual_kernel<R, CF_CONST><<<g, blk, 0, s>>>(F, bc, done);
+        CKL();
         return AEO_OK;
     }
 
@@ -950,21 +978,23 @@ struct Mg : MgBase {
             case 1: {
                 Level<R>& F = L[0];
                 if (F.nx % 2) { fail("profile: odd finest nx"); return AEO_ERR_ARGUMENT; }
-                mg_rbgs_kernel<R><<<half_grid(F), dim3(RB_X, RB_Y), 0, st>>>(F, bc, 0, dzero);
-                CKL();
-                return AEO_OK;
+                return launch_rbgs(st, F, 0, dzero);
             }
             case 2: return launch_apply(st, p, Ap, 1);
             case 3: return launch_vcycle(st, r, true, dzero);
             case 4: return launch_coarsest(st, L[nl - 1], nl == 1 ? r : nullptr, dzero);
             case 5: {
                 if (nl < 2) { fail("profile: one level, no restriction"); return AEO_ERR_ARGUMENT; }
-                mg_residual_kernel<R><<<cell_grid(L[0]), dim3(RB_X, RB_Y), 0, st>>>(L[0], bc, dzero);
-                CKL();
+                if (aeo_status q = launch_residual(st, L[0], dzero)) return q;
                 mg_restrict_kernel<R><<<restrict_grid(L[1]), dim3(RB_X, RB_Y), 0, st>>>(L[0], L[1], part, &S->counter,
                                                                                       dzero);
                 CKL();
                 return AEO_OK;
+            }
+            case 6: {
+                if (nl < 2) { fail("profile: one level, no smoothing sweep"); return AEO_ERR_ARGUMENT; }
+                if (aeo_status q = launch_rbgs(st, L[0], 0, dzero)) return q;
+                return launch_rbgs(st, L[0], 1, dzero);
             }
             default: fail("profile: unknown part"); return AEO_ERR_ARGUMENT;
             }

@@ -395,7 +395,7 @@ def run_b200_urban(args):
         barrier(world)
         clocks = clk.stop()
         ms = max_over_ranks(ms, world)
-        parts = {p: s.profile(p, 20) for p in ("vcycle", "apply", "rbgs", "restrict", "coarsest")}
+        parts = {p: s.profile(p, 20) for p in ("vcycle", "apply", "sweep", "rbgs", "restrict", "coarsest")}
         # e2e: the C-ABI call with pinned host arrays, copies inside
         bh = torch.empty(b.shape, dtype=torch.float64, pin_memory=True).numpy()
         bh[...] = b

@@ -96,7 +96,9 @@ aeo_status aeo_mg_precondition(aeo_mg* h, const double* r, double* z);
  * what = 0 the whole solve of the right-hand side of the last solve call,
  * 1 one red-black colour pass on the finest level, 2 the operator with its
  * p.Ap reduction, 3 one preconditioner application, 4 the coarsest-level
- * solve, 5 the residual restriction of the finest level.  ms_out: mean ms. */
+ * solve, 5 the residual restriction of the finest level, 6 one whole
+ * red-black sweep of the finest level as the cycle runs it (one fused pass,
+ * or the two colour passes).  ms_out: mean ms. */
 aeo_status aeo_mg_profile(aeo_mg* h, int32_t what, int32_t reps, double* ms_out);
 /* The learned preconditioner (no reference counterpart): `net` (same grid;
  * NULL detaches it) preconditions flexible CG from the next solve on.  When

@@ -88,6 +88,24 @@ def test_coarsest_level_variants_match_the_oracle(n, bc, precision):
     assert rel(zg, zo) < (1e-11 if precision == "fp64" else 1e-5)
 
 
+@pytest.mark.parametrize("coded,bc,nu,precision", [
+    (True, ("periodic", "periodic", "neumann"), (2, 2), "fp64"),
+    (True, ("periodic", "periodic", "neumann"), (2, 2), "fp32_mixed"),
+    (True, ("neumann", "neumann", "neumann"), (3, 1), "fp64"),
+    (False, ("periodic", "periodic", "neumann"), (2, 2), "fp64"),
+])
+def test_large_level_vcycle_matches_the_oracle(coded, bc, nu, precision):
+    """One V-cycle at 128 x 128 x 48 in each coefficient form of the smoother
+    (one-byte codes on the finest level, per-face values below it, or the
+    constant Laplacian), periodic or mirrored sides, and odd sweep counts."""
+    n = (128, 128, 48)
+    coeffs, b = urban_problem(n, seed=5, nboxes=10) if coded else (None, np.random.default_rng(6).standard_normal(n[::-1]))
+    g = MG(n, (2.0,) * 3, coeffs=coeffs, bc=bc, nu1=nu[0], nu2=nu[1], precision=precision)
+    o = OracleMGPCG(n, (2.0,) * 3, coeffs=coeffs, bc=bc, nu1=nu[0], nu2=nu[1])
+    zg, zo = g.precondition(b), o.precondition(b)
+    assert rel(zg, zo) < (1e-11 if precision == "fp64" else 1e-5)
+
+
 def test_cutcell_mgcg_solve_matches_the_oracle():
     coeffs, b = ref_case()
     g = MG(REF_N, REF_H, coeffs=coeffs, tol=1e-10)
