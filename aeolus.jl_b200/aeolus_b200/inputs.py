@@ -192,3 +192,45 @@ def cbl_initial(grid: Grid, seed: int = 1, noise: float = 0.1, noise_levels: int
     th[:nz_noise] += pert[:nz_noise]
     z = np.zeros((grid.nz, grid.ny, grid.nx))
     return embed(grid, z), embed(grid, z), embed(grid, z), embed(grid, th), prof
+
+
+def storage_from_interior(grid: Grid, interior: np.ndarray, wall_face: bool = False) -> np.ndarray:
+    """A storage array from its interior values with the halos filled:
+    periodic in x and y; in z periodic, or at walls the mirror (zero
+    gradient), or for a z-face field zero on the two wall faces and zero
+    beyond them."""
+    hx, hy, hz = grid.halo
+    a = np.pad(interior, ((0, 0), (hy, hy), (hx, hx)), mode="wrap")
+    if grid.bc_z == "periodic":
+        a = np.pad(a, ((hz, hz), (0, 0), (0, 0)), mode="wrap")
+    elif wall_face:
+        a = np.pad(a, ((hz, hz), (0, 0), (0, 0)), mode="constant")
+        a[hz] = 0.0
+        a[hz + grid.nz] = 0.0
+    else:
+        a = np.pad(a, ((hz, hz), (0, 0), (0, 0)), mode="symmetric")
+    return np.ascontiguousarray(a)
+
+
+def tracer_case(grid: Grid, seed: int, cfl: float = 0.9, sharp: bool = True):
+    """Inputs of the positivity-preserving advection: seeded normal face
+    velocities scaled so that sum_d max|u_d| dt/dx_d = cfl at dt = 1, and a
+    non-negative field -- a smooth positive background with, when sharp,
+    random zero cells, a zero slab and a unit block (where the limiter acts).
+    Returns storage arrays u, v, w, phi (halos filled) and dt."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = grid.size
+    vel = [rng.standard_normal((nz, ny, nx)) for _ in range(3)]
+    rate = sum(np.abs(a).max() / h for a, h in zip(vel, (grid.dx, grid.dy, grid.dz)))
+    vel = [a * (cfl / rate) for a in vel]
+    x = (np.arange(nx) + 0.5) / nx
+    y = (np.arange(ny) + 0.5) / ny
+    z = (np.arange(nz) + 0.5) / nz
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    phi = 1.5 + np.sin(2 * np.pi * X) * np.cos(2 * np.pi * Y) * np.cos(2 * np.pi * Z)
+    if sharp:
+        phi = np.where(rng.random((nz, ny, nx)) < 0.15, 0.0, phi)
+        phi[nz // 4:nz // 2, ny // 4:ny // 2, nx // 4:nx // 2] = 1.0
+        phi[:, :, :nx // 8] = 0.0
+    return (storage_from_interior(grid, vel[0]), storage_from_interior(grid, vel[1]),
+            storage_from_interior(grid, vel[2], wall_face=True), storage_from_interior(grid, phi), 1.0)

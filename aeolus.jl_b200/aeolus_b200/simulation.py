@@ -189,6 +189,38 @@ class Simulation:
         _lib.check(self._lib.aeo_pressure_solve(self._h, _ptr(s), _ptr(out)), self._h)
         return out
 
+    # ---- positivity-preserving scalar advection -----------------------------------
+    def advect_positive(self, u, v, w, phi, dt: float, scheme: str = "weno_z5", tend=None,
+                        accumulate: bool = True) -> np.ndarray:
+        """advect_positive! (src/AdvectionSchemes.jl:1141-1160): tend (a copy;
+        zeros when None) with -div(u phi) added (accumulate) or written, the
+        face fluxes limited so that phi + dt*tend stays non-negative under the
+        first-order CFL condition.  Storage arrays with filled halos (>= 3)."""
+        g = self.grid
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (u, v, w, phi)]
+        for a in arrs:
+            if a.shape != g.storage_shape:
+                raise ValueError(f"arrays must have the storage shape {g.storage_shape}")
+        if scheme not in ("weno_js5", "weno_z5"):
+            raise ValueError("scheme must be weno_js5 or weno_z5")
+        out = np.zeros(g.storage_shape) if tend is None else np.array(tend, dtype=np.float64, copy=True)
+        if out.shape != g.storage_shape:
+            raise ValueError(f"tend must have the storage shape {g.storage_shape}")
+        _lib.check(self._lib.aeo_advect_positive(self._h, *[_ptr(a) for a in arrs], _ptr(out), float(dt),
+                                                 ADVECTION[scheme], int(bool(accumulate))), self._h)
+        return out
+
+    def advect_positive_device(self, u, v, w, phi, tend, dt: float, scheme: str = "weno_z5",
+                               accumulate: bool = True):
+        """The same on device arrays (integer addresses, or objects with a
+        data_ptr() such as torch tensors) of the working precision in the
+        storage layout, enqueued on the domain's stream."""
+        def addr(a):
+            return C.c_void_p(a.data_ptr() if hasattr(a, "data_ptr") else int(a))
+        _lib.check(self._lib.aeo_advect_positive_device(self._h, addr(u), addr(v), addr(w), addr(phi), addr(tend),
+                                                        float(dt), ADVECTION[scheme], int(bool(accumulate))),
+                   self._h)
+
     # ---- the PCG pressure solver (solver="pcg") --------------------------------
     def set_pcg(self, apertures=None, tol: float = 1e-8, maxit: int = 200):
         """The cut-cell face apertures (ax, ay, az) of shapes (nz, ny, nx+1),

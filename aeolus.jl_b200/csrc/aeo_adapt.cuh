@@ -18,6 +18,7 @@ struct StepScalars {
     int limiter;      // 0 advective, 1 diffusive, 2 buoyancy, 3 Coriolis, 4 sgs, 5 growth, 6 dt_min, 7 dt_max
     int pad;
     double rate, nut_max, N;   // the pick's diagnostics
+    double pos_dt;             // the dt of the positivity-limited advection (aeo_advect_positive)
 };
 
 struct CflParams {

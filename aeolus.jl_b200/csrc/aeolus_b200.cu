@@ -35,6 +35,7 @@
 #include "aeo_mg_internal.h"
 #include "aeo_common.cuh"
 #include "aeo_cutcell.cuh"
+#include "aeo_positive.cuh"
 #include "aeo_fft.cuh"
 #include "aeo_init.cuh"
 #include "aeo_misc.cuh"
@@ -90,6 +91,8 @@ struct CoreBase {
     virtual aeo_status step_adaptive(const aeo_cfl* c, int n, double* dt_prev, aeo_adaptive_stats* stats) = 0;
     virtual aeo_status cfl(const aeo_cfl* c, double dt_prev, aeo_adaptive_stats* stats) = 0;
     virtual aeo_status pressure_solve(const double* src, double* phi) = 0;
+    virtual aeo_status advect_positive(const void* u, const void* v, const void* w, const void* phi, void* tend,
+                                       double dt, int scheme, int accumulate, bool host) = 0;
     virtual aeo_status kinetic_energy(double* out) = 0;
     virtual aeo_status max_divergence(double* out) = 0;
     virtual aeo_status fill_uniform(int id, uint64_t seed, uint32_t stream, double amp, int mode) = 0;
@@ -1026,6 +1029,73 @@ struct Core : CoreBase {
         return AEO_OK;
     }
 
+    // advect_positive! on caller arrays in the reference storage layout: device
+    // arrays of the working precision (host = false, enqueued on the stream),
+    // or host FP64 arrays staged through the device (host = true, synchronous)
+    R *pos_fx = nullptr, *pos_fy = nullptr, *pos_fz = nullptr, *pos_r = nullptr, *pos_st = nullptr;
+    aeo_status advect_positive(const void* u, const void* v, const void* w, const void* phi, void* tend, double dt,
+                               int scheme, int accumulate, bool host) override {
+        if (scheme != AEO_ADV_WENO_JS5 && scheme != AEO_ADV_WENO_Z5) {
+            fail("advect_positive: scheme must be WENO-JS5 or WENO-Z5");
+            return AEO_ERR_ARGUMENT;
+        }
+        if (!uni) { fail("advect_positive: a uniform grid is required (the WENO stencils assume it)"); return AEO_ERR_ARGUMENT; }
+        if (cfg.hx < 3 || cfg.hy < 3 || cfg.hz < 3) { fail("advect_positive: halos >= 3 required"); return AEO_ERR_ARGUMENT; }
+        if (!(dt >= 0)) { fail("advect_positive: dt >= 0 required"); return AEO_ERR_ARGUMENT; }
+        if (!pos_fx) {
+            if (aeo_status e = alloc(&pos_fx, (size_t)(g.nx + 1) * g.ny * g.nz)) return e;
+            if (aeo_status e = alloc(&pos_fy, (size_t)g.nx * (g.ny + 1) * g.nz)) return e;
+            if (aeo_status e = alloc(&pos_fz, (size_t)g.nx * g.ny * (g.nz + 1))) return e;
+            if (aeo_status e = alloc(&pos_r, (size_t)g.nin)) return e;
+        }
+        const R* a[4] = {static_cast<const R*>(u), static_cast<const R*>(v), static_cast<const R*>(w),
+                         static_cast<const R*>(phi)};
+        R* t = static_cast<R*>(tend);
+        const unsigned hb = (unsigned)((host_n + 255) / 256);
+        if (host) {
+            if (!pos_st)
+                if (aeo_status e = alloc(&pos_st, 5 * (size_t)host_n)) return e;
+            const double* hs[5] = {static_cast<const double*>(u), static_cast<const double*>(v),
+                                   static_cast<const double*>(w), static_cast<const double*>(phi),
+                                   static_cast<const double*>(tend)};
+            for (int f = 0; f < 5; ++f) {
+                if (f == 4 && !accumulate) break;
+                CK(cudaMemcpyAsync(d_stage, hs[f], host_n * sizeof(double), cudaMemcpyHostToDevice, st));
+                convert_kernel<R><<<hb, 256, 0, st>>>(host_n, d_stage, pos_st + f * host_n);
+                CKL();
+            }
+            for (int f = 0; f < 4; ++f) a[f] = pos_st + f * host_n;
+            t = pos_st + 4 * host_n;
+        }
+        set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->pos_dt, dt);
+        CKL();
+        PosGeo pg{};
+        pg.nx = g.nx; pg.ny = g.ny; pg.nz = g.nz;
+        pg.hx = cfg.hx; pg.hy = cfg.hy; pg.hz = cfg.hz;
+        pg.sx = 1;
+        pg.sy = g.nx + 2LL * cfg.hx;
+        pg.sz = pg.sy * (g.ny + 2LL * cfg.hy);
+        pg.idx = g.idx; pg.idy = g.idy; pg.idz = g.idz;
+        const dim3 gf((unsigned)((g.nx + 1 + 127) / 128), (unsigned)(g.ny + 1), (unsigned)(g.nz + 1));
+        if (scheme == AEO_ADV_WENO_Z5)
+            pos_flux_kernel<R, AEO_ADV_WENO_Z5><<<gf, 128, 0, st>>>(pg, a[0], a[1], a[2], a[3], pos_fx, pos_fy, pos_fz);
+        else
+            pos_flux_kernel<R, AEO_ADV_WENO_JS5><<<gf, 128, 0, st>>>(pg, a[0], a[1], a[2], a[3], pos_fx, pos_fy, pos_fz);
+        CKL();
+        const dim3 gc((unsigned)((g.nx + 127) / 128), (unsigned)g.ny, (unsigned)g.nz);
+        pos_ratio_kernel<R><<<gc, 128, 0, st>>>(pg, a[0], a[1], a[2], a[3], pos_fx, pos_fy, pos_fz, &d_sc->pos_dt, pos_r);
+        CKL();
+        pos_apply_kernel<R><<<gc, 128, 0, st>>>(pg, a[0], a[1], a[2], a[3], pos_fx, pos_fy, pos_fz, pos_r, t, accumulate);
+        CKL();
+        if (host) {
+            convert_back_kernel<R><<<hb, 256, 0, st>>>(host_n, t, d_stage);
+            CKL();
+            CK(cudaMemcpyAsync(tend, d_stage, host_n * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        return AEO_OK;
+    }
+
     // One Chorin projection of the state with dt = 1 (the config driver's
     // _project!(sim, 1.0), src/config/simulation_driver.jl:1316).
     aeo_status project() override {
@@ -1321,6 +1391,20 @@ aeo_status aeo_pressure_solve(aeo_sim* h, const double* src, double* phi) {
     ENTER(h);
     if (!src || !phi) { h->core->fail("NULL array"); return AEO_ERR_ARGUMENT; }
     return h->core->pressure_solve(src, phi);
+}
+
+aeo_status aeo_advect_positive(aeo_sim* h, const double* u, const double* v, const double* w, const double* phi,
+                               double* tend, double dt, int32_t scheme, int32_t accumulate) {
+    ENTER(h);
+    if (!u || !v || !w || !phi || !tend) { h->core->fail("NULL array"); return AEO_ERR_ARGUMENT; }
+    return h->core->advect_positive(u, v, w, phi, tend, dt, scheme, accumulate, true);
+}
+
+aeo_status aeo_advect_positive_device(aeo_sim* h, const void* u, const void* v, const void* w, const void* phi,
+                                      void* tend, double dt, int32_t scheme, int32_t accumulate) {
+    ENTER(h);
+    if (!u || !v || !w || !phi || !tend) { h->core->fail("NULL array"); return AEO_ERR_ARGUMENT; }
+    return h->core->advect_positive(u, v, w, phi, tend, dt, scheme, accumulate, false);
 }
 
 aeo_status aeo_set_pcg(aeo_sim* h, const double* ax, const double* ay, const double* az, double tol, int32_t maxit) {

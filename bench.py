@@ -17,7 +17,7 @@ beside it.  `e2e` is the same metric through the C-ABI with the state copied
 from pinned host memory and back every step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--workload cbl|tgv|urban|hit|urban_step]
+                  [--workload cbl|tgv|urban|hit|urban_step|tracer]
 
 The default line also carries "pcg": the other half of the headline metric,
 the time to a 1e-8 relative residual of the cut-cell urban pressure problem
@@ -607,6 +607,109 @@ def run_b200_hit(args):
     return 0
 
 
+def run_tracer(args):
+    """Positivity-preserving WENO-Z5 tracer advection (advect_positive!) on
+    device arrays in the reference storage layout: 256^3 triply periodic,
+    random face velocities at a first-order CFL of 0.9, a non-negative field
+    with zero regions and blocks (the limiter active); FP32-mixed and FP64;
+    the oracle on a 128^3 sample on the host cores as the CPU baseline (the
+    reference arm prints only that)."""
+    import torch
+    from aeolus_b200 import CoreSpec, regular_grid
+    from aeolus_b200.inputs import tracer_case as case
+
+    def grid(n):
+        return regular_grid(n, (1.0, 1.0, 1.0), halo=(3, 3, 3), bc_z="periodic")
+
+    def spec(g, precision="fp64"):
+        return CoreSpec(grid=g, advection="weno_z5", precision=precision)
+
+    n = args.tracer_n
+    g = grid((n, n, n))
+    u, v, w, phi, dt = case(g, 1)
+    ncell = g.ncells
+    line = {"metric": "cell-updates/s", "unit": "cell-updates/s", "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "data": "synthetic (seeded velocities and field)",
+            "config": {"workload": f"advect_positive WENO-Z5 tracer, {n}^3 triply periodic, first-order CFL 0.9, "
+                                   "limiter active (zero regions and blocks)", "grid": [n, n, n],
+                       "l2": "inputs larger than L2"}}
+    if args.impl == "reference":
+        from oracle.oracle import OracleSimulation, set_threads
+        cores = os.cpu_count() or 1
+        set_threads(cores)
+        gs = grid((128, 128, 128))
+        us, vs, ws, ps, _ = case(gs, 1)
+        o = OracleSimulation(spec(gs))
+        o.advect_positive(us, vs, ws, ps, dt)
+        k = max(1, min(args.steps, 3))
+        t0 = time.perf_counter()
+        for _ in range(k):
+            o.advect_positive(us, vs, ws, ps, dt)
+        el = (time.perf_counter() - t0) / k
+        rate = gs.ncells / el
+        line.update({"impl": "reference", "value": rate, "n_gpus": args.gpus, "steps": k, "warmup": 1,
+                     "ms_per_step": 1e3 * el, "dtype": "f64",
+                     "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+                                      "sample": f"{k} calls on a 128^3 sample of the workload, FP64 oracle, "
+                                                f"{cores} OpenMP threads"},
+                     "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                             "d2h_bytes_per_step": 0}})
+        print(json.dumps(line), flush=True)
+        return 0
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    from aeolus_b200.simulation import Simulation
+    hbm, hbm_kind = measured_peaks()
+    res = {}
+    for prec, dtype, word in (("fp32_mixed", torch.float32, 4), ("fp64", torch.float64, 8)):
+        s = Simulation(spec(g, prec), device=local)
+        dev = [torch.from_numpy(a).to(dtype).cuda() for a in (u, v, w, phi)]
+        tend = torch.zeros(g.storage_shape, dtype=dtype, device="cuda")
+        stream = torch.cuda.ExternalStream(s.stream)
+        for _ in range(args.warmup):
+            s.advect_positive_device(*dev, tend, dt)
+        clk = ClockSampler(local)
+        clk.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.synchronize()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            s.advect_positive_device(*dev, tend, dt)
+        e1.record(stream)
+        s.synchronize()
+        clocks = clk.stop()
+        ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+        # e2e: the host-array entry point (u, v, w, phi, tend up, tend down)
+        t0 = time.perf_counter()
+        ke = max(2, min(args.steps, 5))
+        out = np.zeros(g.storage_shape)
+        for _ in range(ke):
+            out = s.advect_positive(u, v, w, phi, dt, tend=out)
+        e2e_ms = 1e3 * (time.perf_counter() - t0) / ke
+        res[prec] = dict(ms=ms, e2e_ms=e2e_ms, clocks=clocks, word=word)
+        s.close()
+    if rank != 0:
+        return 0
+    m = res["fp32_mixed"]
+    # algorithmic bytes: read u, v, w, phi and tend, write tend (the fluxes and
+    # ratios between the three kernels are the implementation's own traffic)
+    byts = 6 * m["word"] * ncell
+    ach = byts / (m["ms"] * 1e-3) / 1e9
+    hb = 5 * 8 * int(np.prod(g.storage_shape))
+    line.update({"value": world * ncell / (m["ms"] * 1e-3), "n_gpus": world, "steps": args.steps,
+                 "warmup": args.warmup, "ms_per_step": m["ms"], "dtype": "f32 (FP32 arithmetic on FP32 arrays)",
+                 "fp64": {"value": world * ncell / (res["fp64"]["ms"] * 1e-3), "ms_per_step": res["fp64"]["ms"]},
+                 "e2e": {"value": ncell / (m["e2e_ms"] * 1e-3), "unit": "cell-updates/s",
+                         "h2d_bytes_per_step": hb, "d2h_bytes_per_step": 8 * int(np.prod(g.storage_shape))},
+                 "roofline": {"bound": "hbm", "kernel": "advect_positive (three kernels, whole call)",
+                              "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s", "frac": round(ach / hbm, 4),
+                              "peak_kind": hbm_kind, "bytes_per_launch": byts, "traffic": None},
+                 "gpu_launches": 3 * args.steps, "clocks": m["clocks"]})
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 URBAN_STEP_N = (1024, 1024, 192)
 
 
@@ -906,7 +1009,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="cbl", choices=["cbl", "tgv", "urban", "hit", "urban_step"])
+    ap.add_argument("--workload", default="cbl", choices=["cbl", "tgv", "urban", "hit", "urban_step", "tracer"])
+    ap.add_argument("--tracer-n", type=int, default=256)
     ap.add_argument("--hit-n", type=int, default=512)
     ap.add_argument("--hit-steps", type=int, default=100)
     ap.add_argument("--urban-n", type=int, nargs=3, default=None)
@@ -919,6 +1023,8 @@ def main():
         args.warmup = 3
     if args.workload == "urban":
         rc = run_reference_urban(args) if args.impl == "reference" else run_b200_urban(args)
+    elif args.workload == "tracer":
+        rc = run_tracer(args)
     elif args.workload == "urban_step":
         rc = run_reference_urban_step(args) if args.impl == "reference" else run_b200_urban_step(args)
     elif args.workload == "hit":

@@ -194,6 +194,24 @@ enum { AEO_K_SGS = 0, AEO_K_SWEEP = 1, AEO_K_DIV_FFTX = 2, AEO_K_FFTY = 3, AEO_K
  * StepRecord (src/simulations/step_record.jl:1-263) are the analogue. */
 aeo_status aeo_profile_step(aeo_sim* h, double dt, double* ms_per_class, int32_t nclass);
 
+/* Positivity-preserving scalar advection: replaces
+ *   advect_positive!(tend, u, v, w, phi, dt; scheme, accumulate)
+ *                                   src/AdvectionSchemes.jl:1141-1160
+ * with the limiter of apply_positivity_limiter! (:998-1098, upwind low-order
+ * fluxes, the one-layer periodic wrap of the ratio: no boundary conditions).
+ * Adds (accumulate = 1) or writes -div(u phi) into the interior of tend so
+ * that phi + dt * tend stays >= 0 where phi >= 0 and sum |u_d| dt/dx_d <= 1.
+ * u, v, w, phi, tend are arrays of the domain's storage layout (the layout of
+ * aeo_set_field), halos filled, hx, hy, hz >= 3; scheme AEO_ADV_WENO_JS5 or
+ * AEO_ADV_WENO_Z5; a uniform grid.  The host form takes FP64 host arrays and
+ * synchronises; the device form takes device arrays of the domain's working
+ * precision (double for AEO_PREC_FP64, float for AEO_PREC_FP32_MIXED) and is
+ * enqueued on the domain's stream (aeo_stream). */
+aeo_status aeo_advect_positive(aeo_sim* h, const double* u, const double* v, const double* w, const double* phi,
+                               double* tend, double dt, int32_t scheme, int32_t accumulate);
+aeo_status aeo_advect_positive_device(aeo_sim* h, const void* u, const void* v, const void* w, const void* phi,
+                                      void* tend, double dt, int32_t scheme, int32_t accumulate);
+
 /* Number of kernel launches one RK3 step issues (for launch accounting).
    solver = AEO_SOLVER_PCG: counted with the iteration count of the last
    pressure solve for all three substages (synchronises the stream). */

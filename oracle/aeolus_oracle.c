@@ -1275,6 +1275,117 @@ int oc_step_adaptive(oc_sim* s, const oc_cfl* c, int nsteps, double* dt_prev, do
 /* Diagnostics (src/Simulations.jl:992-1050)                                  */
 /* ------------------------------------------------------------------------- */
 
+/* ------------------------------------------------------------------------- */
+/* Positivity-preserving scalar advection (advect_positive!,                   */
+/* src/AdvectionSchemes.jl:1100-1160, the limiter :1015-1098)                  */
+/* ------------------------------------------------------------------------- */
+
+/* Adds (accumulate) or writes -div(u phi) to tend (storage arrays of the
+ * domain's layout, halos of u, v, w and phi filled, halo >= 3): the
+ * reconstructed face fluxes F = vel * face value (WENO-JS5 / WENO-Z5,
+ * _reconstructed_fluxes! :868-892), the first-order upwind fluxes L
+ * (_upwind_fluxes! :899-909), the antidiffusive outflow ratio of every cell
+ * (_b_limit_ratio! :1015-1043), its one-layer periodic wrap
+ * (_wrap_one_layer! :951-958, the default without boundary conditions), the
+ * limited fluxes L + c (F - L) with c the donor's ratio (_b_limit_x/y/z!
+ * :1045-1071) and their divergence (_b_flux_div! :911-926).  Uniform grids. */
+int oc_advect_positive(oc_sim* s, const double* u, const double* v, const double* w, const double* phi,
+                       double* tend, double dt, int scheme, int accumulate) {
+    const oc_params* P = &s->p;
+    if (!s->uniform || (scheme != OC_ADV_WENO_JS5 && scheme != OC_ADV_WENO_Z5)) return -1;
+    if (P->hx < 3 || P->hy < 3 || P->hz < 3) return -1;
+    int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
+    int64_t n = s->n;
+    double *Fx = (double*)calloc((size_t)n, sizeof(double)), *Fy = (double*)calloc((size_t)n, sizeof(double));
+    double *Fz = (double*)calloc((size_t)n, sizeof(double)), *Lx = (double*)calloc((size_t)n, sizeof(double));
+    double *Ly = (double*)calloc((size_t)n, sizeof(double)), *Lz = (double*)calloc((size_t)n, sizeof(double));
+    double* R = (double*)calloc((size_t)n, sizeof(double));
+    /* face fluxes over the interior faces plus the closing face of each axis */
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = Hz; k <= Hz + Nz; ++k)
+        for (int j = Hy; j <= Hy + Ny; ++j)
+            for (int i = Hx; i <= Hx + Nx; ++i) {
+                int64_t q = ID(s, i, j, k);
+                if (j < Hy + Ny && k < Hz + Nz) {
+                    double vel = u[q];
+                    Fx[q] = vel * face_x(s, scheme, phi, i - 1, j, k, vel);
+                    Lx[q] = vel * (vel >= 0 ? A(phi, i - 1, j, k) : phi[q]);
+                }
+                if (i < Hx + Nx && k < Hz + Nz) {
+                    double vel = v[q];
+                    Fy[q] = vel * face_y(s, scheme, phi, i, j - 1, k, vel);
+                    Ly[q] = vel * (vel >= 0 ? A(phi, i, j - 1, k) : phi[q]);
+                }
+                if (i < Hx + Nx && j < Hy + Ny) {
+                    double vel = w[q];
+                    Fz[q] = vel * face_z(s, scheme, phi, i, j, k - 1, vel);
+                    Lz[q] = vel * (vel >= 0 ? A(phi, i, j, k - 1) : phi[q]);
+                }
+            }
+    const double z = 0.0, idx = s->idx, idy = s->idy, idz = s->idz;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = Hz; k < Hz + Nz; ++k)
+        for (int j = Hy; j < Hy + Ny; ++j)
+            for (int i = Hx; i < Hx + Nx; ++i) {
+                double lxe = A(Lx, i + 1, j, k), lxw = A(Lx, i, j, k);
+                double lyn = A(Ly, i, j + 1, k), lys = A(Ly, i, j, k);
+                double lzt = A(Lz, i, j, k + 1), lzb = A(Lz, i, j, k);
+                double axe = A(Fx, i + 1, j, k) - lxe, axw = A(Fx, i, j, k) - lxw;
+                double ayn = A(Fy, i, j + 1, k) - lyn, ays = A(Fy, i, j, k) - lys;
+                double azt = A(Fz, i, j, k + 1) - lzt, azb = A(Fz, i, j, k) - lzb;
+                double Pm = dt * ((fmax(axe, z) + fmax(-axw, z)) * idx + (fmax(ayn, z) + fmax(-ays, z)) * idy +
+                                  (fmax(azt, z) + fmax(-azb, z)) * idz);
+                double div_lo = (lxe - lxw) * idx + (lyn - lys) * idy + (lzt - lzb) * idz;
+                double Q = fmax(A(phi, i, j, k) - dt * div_lo, z);
+                A(R, i, j, k) = Pm > z ? fmin(1.0, Q / Pm) : 1.0;
+            }
+    /* one-layer periodic wrap of the ratio, x then y then z */
+    for (int k = Hz; k < Hz + Nz; ++k)
+        for (int j = Hy; j < Hy + Ny; ++j) {
+            A(R, Hx - 1, j, k) = A(R, Hx + Nx - 1, j, k);
+            A(R, Hx + Nx, j, k) = A(R, Hx, j, k);
+        }
+    for (int k = Hz; k < Hz + Nz; ++k)
+        for (int i = Hx; i < Hx + Nx; ++i) {
+            A(R, i, Hy - 1, k) = A(R, i, Hy + Ny - 1, k);
+            A(R, i, Hy + Ny, k) = A(R, i, Hy, k);
+        }
+    for (int j = Hy; j < Hy + Ny; ++j)
+        for (int i = Hx; i < Hx + Nx; ++i) {
+            A(R, i, j, Hz - 1) = A(R, i, j, Hz + Nz - 1);
+            A(R, i, j, Hz + Nz) = A(R, i, j, Hz);
+        }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = Hz; k <= Hz + Nz; ++k)
+        for (int j = Hy; j <= Hy + Ny; ++j)
+            for (int i = Hx; i <= Hx + Nx; ++i) {
+                int64_t q = ID(s, i, j, k);
+                if (j < Hy + Ny && k < Hz + Nz) {
+                    double a = Fx[q] - Lx[q], c = a >= z ? A(R, i - 1, j, k) : R[q];
+                    Fx[q] = Lx[q] + c * a;
+                }
+                if (i < Hx + Nx && k < Hz + Nz) {
+                    double a = Fy[q] - Ly[q], c = a >= z ? A(R, i, j - 1, k) : R[q];
+                    Fy[q] = Ly[q] + c * a;
+                }
+                if (i < Hx + Nx && j < Hy + Ny) {
+                    double a = Fz[q] - Lz[q], c = a >= z ? A(R, i, j, k - 1) : R[q];
+                    Fz[q] = Lz[q] + c * a;
+                }
+            }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = Hz; k < Hz + Nz; ++k)
+        for (int j = Hy; j < Hy + Ny; ++j)
+            for (int i = Hx; i < Hx + Nx; ++i) {
+                int64_t q = ID(s, i, j, k);
+                double d = (A(Fx, i + 1, j, k) - Fx[q]) * idx + (A(Fy, i, j + 1, k) - Fy[q]) * idy +
+                           (A(Fz, i, j, k + 1) - Fz[q]) * idz;
+                tend[q] = accumulate ? tend[q] - d : -d;
+            }
+    free(Fx); free(Fy); free(Fz); free(Lx); free(Ly); free(Lz); free(R);
+    return 0;
+}
+
 double oc_kinetic_energy(oc_sim* s) {
     const oc_params* P = &s->p;
     int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;

@@ -79,6 +79,12 @@ int oc_set_apertures(oc_sim* s, const double* ax, const double* ay, const double
 /* iterations, status (mgpcg_oracle.h OCG_*), ||r|| and ||b|| of the last solve */
 int oc_pcg_stats(const oc_sim* s, int* iterations, int* status, double* residual, double* bnorm);
 void oc_set_threads(int n);
+/* advect_positive! (src/AdvectionSchemes.jl:1100-1160): add (accumulate) or
+ * write -div(u phi) with the positivity limiter; storage arrays of the
+ * domain's layout with filled halos (>= 3); scheme OC_ADV_WENO_JS5 or
+ * OC_ADV_WENO_Z5; uniform grids.  0 on success. */
+int oc_advect_positive(oc_sim* s, const double* u, const double* v, const double* w, const double* phi,
+                       double* tend, double dt, int scheme, int accumulate);
 
 /* Philox4x32-10 block function and the uniform fill of the synthetic inputs. */
 void oc_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);

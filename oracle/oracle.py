@@ -82,6 +82,7 @@ def load():
     lib.oc_max_divergence.argtypes = [P]
     lib.oc_max_divergence.restype = C.c_double
     lib.oc_set_threads.argtypes = [C.c_int]
+    lib.oc_advect_positive.argtypes = [P, _D, _D, _D, _D, _D, C.c_double, C.c_int, C.c_int]
     lib.oc_set_apertures.argtypes = [P, _D, _D, _D, C.c_double, C.c_int]
     lib.oc_pcg_stats.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double),
                                  C.POINTER(C.c_double)]
@@ -242,6 +243,21 @@ class OracleSimulation:
         assert self._lib.oc_pcg_stats(self._h, C.byref(it), C.byref(stt), C.byref(r), C.byref(b)) == 0
         return {"iterations": it.value, "status": _PCG_STATUS[stt.value], "residual": r.value, "bnorm": b.value,
                 "relative_residual": 0.0 if b.value == 0 else r.value / b.value}
+
+    def advect_positive(self, u, v, w, phi, dt, scheme="weno_z5", tend=None, accumulate=True):
+        """advect_positive!: tend (a copy, zeros if None) with -div(u phi)
+        added (accumulate) or written, the positivity limiter applied; storage
+        arrays with filled halos."""
+        g = self.grid
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (u, v, w, phi)]
+        for a in arrs:
+            assert a.shape == g.storage_shape
+        out = np.zeros(g.storage_shape) if tend is None else np.array(tend, dtype=np.float64, copy=True)
+        rc = self._lib.oc_advect_positive(self._h, *[_p(a) for a in arrs], _p(out), float(dt), _ADV[scheme],
+                                          int(bool(accumulate)))
+        if rc != 0:
+            raise ValueError("oracle: advect_positive needs a uniform grid, halo >= 3 and a WENO scheme")
+        return out
 
     def kinetic_energy(self):
         return self._lib.oc_kinetic_energy(self._h)
