@@ -189,6 +189,19 @@ class Simulation:
         _lib.check(self._lib.aeo_pressure_solve(self._h, _ptr(s), _ptr(out)), self._h)
         return out
 
+    # ---- the implicit IBM correction ------------------------------------------------
+    def set_ibm(self, mask=None, tau: float = 0.0):
+        """implicit_ibm_correction! after every predictor (src/IBM.jl:295-300):
+        a storage-shaped solid mask (None switches it off) and tau (0: the
+        faces of solid cells are zeroed)."""
+        if mask is None:
+            _lib.check(self._lib.aeo_set_ibm(self._h, None, float(tau)), self._h)
+            return
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        if m.shape != self.grid.storage_shape:
+            raise ValueError(f"mask must have the storage shape {self.grid.storage_shape}")
+        _lib.check(self._lib.aeo_set_ibm(self._h, m.ctypes.data_as(C.c_void_p), float(tau)), self._h)
+
     # ---- positivity-preserving scalar advection -----------------------------------
     def advect_positive(self, u, v, w, phi, dt: float, scheme: str = "weno_z5", tend=None,
                         accumulate: bool = True) -> np.ndarray:

@@ -126,3 +126,41 @@ __global__ void __launch_bounds__(256) cc_maxdiv_levels_kernel(Geo g, const R* _
     }
     if (threadIdx.x == 0) part[k] = red[0];
 }
+
+// implicit_ibm_correction! (src/IBM.jl:295-300) as the post-predictor term
+// (src/Simulations.jl:624-628) on the interior predictor faces: a face is
+// scaled by 1/(1 + dt/tau) (0 for tau = 0) once per solid cell it touches --
+// the cell above it along its axis and, but for the first face of a row
+// (whose low neighbour lies beyond the interior, where the halo fill that
+// follows the hook replaces the scaled copy), the cell below.
+template <typename R>
+__global__ void __launch_bounds__(256) ibm_kernel(Geo g, R* __restrict__ us, R* __restrict__ vs, R* __restrict__ ws,
+                                                  const unsigned char* __restrict__ mask,
+                                                  const double* __restrict__ dtp, double tau) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.nin) return;
+    const int lnx = __ffs(g.nx) - 1, lny = __ffs(g.ny) - 1;
+    const int i = (int)(q & (g.nx - 1)), j = (int)((q >> lnx) & (g.ny - 1)), k = (int)(q >> (lnx + lny));
+    const long long pl = (long long)g.nx * g.ny;
+    const int mc = mask[q];
+    const int nu = mc + (i > 0 ? mask[q - 1] : 0);
+    const int nv = mc + (j > 0 ? mask[q - g.nx] : 0);
+    const int nw = mc + (k > 0 ? mask[q - pl] : 0);
+    if ((nu | nv | nw) == 0) return;
+    const R f = tau > 0 ? R(1.0 / (1.0 + *dtp / tau)) : R(0);
+    if (nu) {
+        R v = us[q] * f;
+        if (nu > 1) v = v * f;
+        us[q] = v;
+    }
+    if (nv) {
+        R v = vs[q] * f;
+        if (nv > 1) v = v * f;
+        vs[q] = v;
+    }
+    if (nw) {
+        R v = ws[q] * f;
+        if (nw > 1) v = v * f;
+        ws[q] = v;
+    }
+}

@@ -103,6 +103,7 @@ struct CoreBase {
     virtual aeo_status set_pcg(const double* ax, const double* ay, const double* az, double tol, int maxit) = 0;
     virtual aeo_status pcg_stats(aeo_mg_stats* o) = 0;
     virtual aeo_status pcg_set_learned(aeo_unet* net, double stagnation) = 0;
+    virtual aeo_status set_ibm(const uint8_t* mask, double tau) = 0;
 };
 
 struct aeo_sim {
@@ -502,6 +503,37 @@ struct Core : CoreBase {
         return 3 * (4 + aeo_mg_launches_per_solve(mg, o.iterations));
     }
 
+    // the implicit IBM correction after every predictor (aeo_set_ibm)
+    unsigned char* ibm_mask = nullptr;
+    unsigned char* ibm_alloc = nullptr;
+    double ibm_tau = 0.0;
+    aeo_status set_ibm(const uint8_t* mask, double tau) override {
+        if (pcg) { fail("set_ibm: the PCG solver takes obstacles as apertures (aeo_set_pcg)"); return AEO_ERR_STATE; }
+        if (!(tau >= 0)) { fail("set_ibm: tau >= 0 required"); return AEO_ERR_ARGUMENT; }
+        CK(cudaStreamSynchronize(st));
+        drop_graphs();   // the step graphs gain or lose the correction
+        if (!mask) {
+            ibm_mask = nullptr;
+            launches = 3 * 9;
+            return AEO_OK;
+        }
+        std::vector<unsigned char> m((size_t)g.nin);
+        const long long HX = cfg.nx + 2LL * cfg.hx, HY = cfg.ny + 2LL * cfg.hy;
+        for (int k = 0; k < g.nz; ++k)
+            for (int j = 0; j < g.ny; ++j)
+                for (int i = 0; i < g.nx; ++i)
+                    m[(size_t)i + (size_t)g.nx * ((size_t)j + (size_t)g.ny * k)] =
+                        mask[(i + cfg.hx) + HX * ((j + cfg.hy) + HY * (long long)(k + cfg.hz))] ? 1 : 0;
+        if (!ibm_alloc)
+            if (aeo_status e = alloc(&ibm_alloc, (size_t)g.nin)) return e;
+        CK(cudaMemcpyAsync(ibm_alloc, m.data(), m.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        ibm_mask = ibm_alloc;
+        ibm_tau = tau;
+        launches = 3 * 10;
+        return AEO_OK;
+    }
+
     aeo_status pcg_stats(aeo_mg_stats* o) override {
         if (!pcg) { fail("pcg_stats: the domain was not created with solver = AEO_SOLVER_PCG"); return AEO_ERR_STATE; }
         CK(cudaStreamSynchronize(st));
@@ -703,6 +735,11 @@ struct Core : CoreBase {
         double ztop = cfg.z0 + cfg.lz;
         a.sp_inv = R(1.0 / (ztop - cfg.sponge_zstart));
         if (aeo_status e = launch_sweep(s_in, a)) return e;
+        if (ibm_mask) {
+            ibm_kernel<R><<<(unsigned)((g.nin + 255) / 256), 256, 0, st>>>(g, Q[0], Q[1], Q[2], ibm_mask, &d_sc->dt,
+                                                                         ibm_tau);
+            CKL();
+        }
         mark(AEO_K_SWEEP);
         if (aeo_status e = solve(nullptr)) return e;
         if (aeo_status e = correct(out, stage, ca, cb, &d_sc->dt, s_u0)) return e;
@@ -1405,6 +1442,11 @@ aeo_status aeo_advect_positive_device(aeo_sim* h, const void* u, const void* v, 
     ENTER(h);
     if (!u || !v || !w || !phi || !tend) { h->core->fail("NULL array"); return AEO_ERR_ARGUMENT; }
     return h->core->advect_positive(u, v, w, phi, tend, dt, scheme, accumulate, false);
+}
+
+aeo_status aeo_set_ibm(aeo_sim* h, const uint8_t* mask, double tau) {
+    ENTER(h);
+    return h->core->set_ibm(mask, tau);
 }
 
 aeo_status aeo_set_pcg(aeo_sim* h, const double* ax, const double* ay, const double* az, double tol, int32_t maxit) {

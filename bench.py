@@ -170,18 +170,61 @@ def measured_peaks():
 
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event reasons sampled during the timed region:
+    read-only NVML queries every 2 ms from a thread (the GPU found by its PCI
+    address), so even a timed region of a few milliseconds has samples;
+    nvidia-smi at 100 ms when NVML is not importable."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown", 0x8),
+             ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+             ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+             ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap", 0x4))
 
     def __init__(self, device):
         self.device = device
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.sm = []
+        self.smax = None
+        self.reasons = set()
+
+    def _nvml_sample(self):
+        m = self.nvml
+        self.sm.append(float(m.nvmlDeviceGetClockInfo(self.h, m.NVML_CLOCK_SM)))
+        r = m.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        for name, const, bit in self.NAMES:
+            if r & getattr(m, const, bit):
+                self.reasons.add(name)
+
+    def _poll(self):
+        while not self.halt.is_set():
+            try:
+                self._nvml_sample()
+            except Exception:
+                return
+            time.sleep(0.002)
 
     def start(self):
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            p = torch.cuda.get_device_properties(self.device)
+            bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+            self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            self.nvml = pynvml
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self._nvml_sample()
+            self.halt = threading.Event()
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                           "-lms", "100", "-i", str(self.device)], stdout=subprocess.PIPE,
@@ -196,6 +239,15 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml:
+            self.halt.set()
+            self.t.join(timeout=5)
+            try:
+                self._nvml_sample()
+            except Exception:
+                pass
+            return {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.smax,
+                    "reasons": sorted(self.reasons), "samples": len(self.sm), "source": "nvml, 2 ms"}
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -204,7 +256,7 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        names = [n for n, _, _ in self.NAMES]
         for l in self.lines:
             f = [x.strip() for x in l.split(",")]
             if len(f) < 9:
@@ -218,7 +270,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 100 ms"}
 
 
 # ----------------------------------------------------------------------------- distributed

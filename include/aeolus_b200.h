@@ -194,6 +194,16 @@ enum { AEO_K_SGS = 0, AEO_K_SWEEP = 1, AEO_K_DIV_FFTX = 2, AEO_K_FFTY = 3, AEO_K
  * StepRecord (src/simulations/step_record.jl:1-263) are the analogue. */
 aeo_status aeo_profile_step(aeo_sim* h, double dt, double* ms_per_class, int32_t nclass);
 
+/* The implicit immersed-boundary correction after every predictor: replaces
+ *   step!/step_rk3!(sim, dt; post_predictor! = (s, dt) -> implicit_ibm_correction!(s, sm; tau, dt = dt))
+ *                                   src/IBM.jl:295-300, src/Simulations.jl:624-628
+ * mask: storage-shaped bytes (the SolidMask of src/IBM.jl:33, nonzero =
+ * solid; the interior cells count), NULL switches the correction off.  Every
+ * predictor face of a solid cell is scaled by 1/(1 + dt/tau), once per solid
+ * cell it touches (tau = 0: zeroed).  Not with AEO_SOLVER_PCG (obstacles are
+ * apertures there). */
+aeo_status aeo_set_ibm(aeo_sim* h, const uint8_t* mask, double tau);
+
 /* Positivity-preserving scalar advection: replaces
  *   advect_positive!(tend, u, v, w, phi, dt; scheme, accumulate)
  *                                   src/AdvectionSchemes.jl:1141-1160

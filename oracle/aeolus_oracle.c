@@ -67,6 +67,9 @@ struct oc_sim {
     double meas_sum, gauge_sum;
     fft_plan px, py, pz;         /* px: length Nx/2 (the packed r2c) */
     cpx* twx;                    /* e^{-2 pi i k / Nx}, k <= Nx/2 */
+    /* the implicit IBM correction: solid cells (interior, x fastest) and tau */
+    unsigned char* ibm;
+    double ibm_tau;
     /* solver = PCG: face apertures (interior face layout), the CG of the a^2 operator */
     double *apx, *apy, *apz, *cgx;
     ocg* cg;
@@ -1056,6 +1059,49 @@ static void cc_correct(oc_sim* s, double dt, int stage, double ca, double cb, in
             }
 }
 
+/* implicit_ibm_correction! (src/IBM.jl:295-300) as the post-predictor hook
+ * (src/Simulations.jl:624-628): every face of a solid interior cell scaled by
+ * 1/(1 + dt/tau) (0 for tau = 0), once per solid cell it touches.  The halo
+ * fill that follows replaces the faces beyond the interior with periodic
+ * images, so an interior face counts the solid cell on its high side and, for
+ * all but the first face of a row, the one on its low side. */
+static void ibm_correct(oc_sim* s, double dt) {
+    const oc_params* P = &s->p;
+    int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
+    const double f = s->ibm_tau > 0 ? 1 / (1 + dt / s->ibm_tau) : 0.0;
+    const unsigned char* m = s->ibm;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                int64_t c = i + (int64_t)Nx * (j + (int64_t)Ny * k);
+                int64_t q = ID(s, i + Hx, j + Hy, k + Hz);
+                int nu = m[c] + (i > 0 ? m[c - 1] : 0);
+                int nv = m[c] + (j > 0 ? m[c - Nx] : 0);
+                int nw = m[c] + (k > 0 ? m[c - (int64_t)Nx * Ny] : 0);
+                for (int r = 0; r < nu; ++r) s->u[q] *= f;
+                for (int r = 0; r < nv; ++r) s->v[q] *= f;
+                for (int r = 0; r < nw; ++r) s->w[q] *= f;
+            }
+}
+
+int oc_set_ibm(oc_sim* s, const unsigned char* mask, double tau) {
+    const oc_params* P = &s->p;
+    if (!(tau >= 0) || P->solver == OC_SOLVER_PCG) return -1;
+    free(s->ibm);
+    s->ibm = NULL;
+    if (!mask) return 0;
+    int64_t nin = (int64_t)P->nx * P->ny * P->nz;
+    s->ibm = (unsigned char*)malloc((size_t)nin);
+    for (int k = 0; k < P->nz; ++k)
+        for (int j = 0; j < P->ny; ++j)
+            for (int i = 0; i < P->nx; ++i)
+                s->ibm[i + (int64_t)P->nx * (j + (int64_t)P->ny * k)] =
+                    mask[ID(s, i + P->hx, j + P->hy, k + P->hz)] ? 1 : 0;
+    s->ibm_tau = tau;
+    return 0;
+}
+
 static void substage(oc_sim* s, double dt, int stage, double ca, double cb) {
     const oc_params* P = &s->p;
     int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
@@ -1072,6 +1118,7 @@ static void substage(oc_sim* s, double dt, int stage, double ca, double cb) {
                 s->v[q] = s->v[q] + dt * s->tv[q];
                 s->w[q] = s->w[q] + dt * s->tw[q];
             }
+    if (s->ibm) ibm_correct(s, dt);
     /* 8. divergence into the solver's buffer */
     fill_halos(s, s->u, LOC_FX);
     fill_halos(s, s->v, LOC_FY);
@@ -1639,7 +1686,7 @@ void oc_destroy(oc_sim* s) {
                       s->lower, s->upper, s->hw, s->meas, s->iota, s->gauge};
     for (size_t q = 0; q < sizeof(ptrs) / sizeof(ptrs[0]); ++q) free(ptrs[q]);
     free(s->hat); free(s->twx);
-    free(s->apx); free(s->apy); free(s->apz); free(s->cgx);
+    free(s->apx); free(s->apy); free(s->apz); free(s->cgx); free(s->ibm);
     if (s->cg) ocg_destroy(s->cg);
     plan_free(&s->px); plan_free(&s->py); plan_free(&s->pz);
     free(s);

@@ -76,6 +76,11 @@ double oc_max_divergence(oc_sim* s);
  * aperture-weighted divergence and corrects u = u* - a d(phi) on every face
  * (zero on a blocked face).  0 on success. */
 int oc_set_apertures(oc_sim* s, const double* ax, const double* ay, const double* az, double tol, int maxit);
+/* the implicit IBM correction after every predictor (implicit_ibm_correction!,
+ * src/IBM.jl:295-300): mask storage-shaped, nonzero = solid (interior cells
+ * count), NULL switches it off; tau >= 0 (0: the faces are zeroed); not with
+ * OC_SOLVER_PCG.  0 on success. */
+int oc_set_ibm(oc_sim* s, const unsigned char* mask, double tau);
 /* iterations, status (mgpcg_oracle.h OCG_*), ||r|| and ||b|| of the last solve */
 int oc_pcg_stats(const oc_sim* s, int* iterations, int* status, double* residual, double* bnorm);
 void oc_set_threads(int n);

@@ -82,6 +82,7 @@ def load():
     lib.oc_max_divergence.argtypes = [P]
     lib.oc_max_divergence.restype = C.c_double
     lib.oc_set_threads.argtypes = [C.c_int]
+    lib.oc_set_ibm.argtypes = [P, C.c_void_p, C.c_double]
     lib.oc_advect_positive.argtypes = [P, _D, _D, _D, _D, _D, C.c_double, C.c_int, C.c_int]
     lib.oc_set_apertures.argtypes = [P, _D, _D, _D, C.c_double, C.c_int]
     lib.oc_pcg_stats.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double),
@@ -221,6 +222,19 @@ class OracleSimulation:
         out = np.empty_like(p)
         self._lib.oc_apply_poisson_operator(self._h, _p(p), _p(out))
         return out
+
+    def set_ibm(self, mask=None, tau=0.0):
+        """The implicit IBM correction after every predictor: a storage-shaped
+        solid mask (None: off) and tau (0: blocked faces zeroed)."""
+        if mask is None:
+            ptr = None
+        else:
+            m = np.ascontiguousarray(mask, dtype=np.uint8)
+            assert m.shape == self.grid.storage_shape
+            self._ibm = m
+            ptr = m.ctypes.data_as(C.c_void_p)
+        if self._lib.oc_set_ibm(self._h, ptr, float(tau)) != 0:
+            raise ValueError("oracle: set_ibm rejected (tau < 0, or the PCG solver)")
 
     def set_pcg(self, apertures=None, tol=1e-8, maxit=200):
         """solver = "pcg": the face apertures (ax, ay, az) in the interior face
