@@ -41,7 +41,7 @@ class AeoConfig(C.Structure):
         ("nu", C.c_double), ("theta0", C.c_double), ("g", C.c_double), ("f_coriolis", C.c_double),
         ("c_s", C.c_double), ("pr_t", C.c_double), ("flux_bot", C.c_double), ("flux_top", C.c_double),
         ("sponge_alpha", C.c_double), ("sponge_zstart", C.c_double),
-        ("device", C.c_int32),
+        ("device", C.c_int32), ("sgs_model", C.c_int32),
     ]
 
 

@@ -74,6 +74,9 @@ struct Geo {
     // the per-level factors in the working precision (rows LV_*, entry k + AEO_LH)
     const void* lvr;
     int lvn;   // row stride
+    // the SGS closure when c_s > 0: 0 Smagorinsky, 1 Vreman (coefficient 2.5 c_s^2)
+    int sgs_model;
+    double sgs_cv;
 };
 
 __device__ __forceinline__ long long pidx(const Geo& g, int i, int j, int k) {

@@ -51,3 +51,8 @@ __device__ __forceinline__ F2& operator-=(F2& x, F2 y) { return x = x - y; }
 __device__ __forceinline__ F2& operator-=(F2& x, F2M y) { return x = x - y; }
 
 __device__ __forceinline__ F2 sqrt(F2 x) { return F2(sqrtf(x.v.x), sqrtf(x.v.y)); }
+
+// c sqrt(b / a) where a > 0, else 0, lane by lane
+__device__ __forceinline__ F2 sqrt_ratio_or_zero(F2 b, F2 a, float c) {
+    return F2(a.v.x > 0.f ? c * sqrtf(b.v.x / a.v.x) : 0.f, a.v.y > 0.f ? c * sqrtf(b.v.y / a.v.y) : 0.f);
+}

@@ -459,8 +459,17 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs<R> a) {
     a.th_out[q] = tn;
 }
 
+template <typename R>
+__device__ __forceinline__ R sqrt_ratio_or_zero(R b, R a, R c) {
+    return a > R(0) ? c * sqrt(b / a) : R(0);
+}
+
 // Smagorinsky nut = (C_s Delta_k)^2 |S| at a cell centre (src/FiniteVolume.jl:936-944,
-// strain src/Operators.jl:451-496), accessors around the point at level k.
+// strain src/Operators.jl:451-496), accessors around the point at level k; or,
+// with g.sgs_model = 1, Vreman's nut = c sqrt(B_beta / alpha:alpha) from the
+// same gradient tensor, B_beta in the Cauchy-Binet form over the rows a_m =
+// d_m u (_vreman_point / _vreman_body!, src/operators/sgs_amd_vreman.jl:93-100,
+// :293-298; uniform grids).
 template <typename R, bool UNI, class AU, class AV, class AW>
 __device__ __forceinline__ auto smag_point(const Met<R, UNI>& m, const Geo& g, int k, R c_s, const AU& U, const AV& V,
                                            const AW& W) {
@@ -477,6 +486,20 @@ __device__ __forceinline__ auto smag_point(const Met<R, UNI>& m, const Geo& g, i
     VT dw_dx = ((W(1, 0, 0) + W(1, 0, 1)) - (W(-1, 0, 0) + W(-1, 0, 1))) * (R(0.25) * idx);
     VT dv_dz = ((V(0, 0, 1) + V(0, 1, 1)) - (V(0, 0, -1) + V(0, 1, -1))) * (R(0.25) * ido);
     VT dw_dy = ((W(0, 1, 0) + W(0, 1, 1)) - (W(0, -1, 0) + W(0, -1, 1))) * (R(0.25) * idy);
+    if (g.sgs_model == 1) {
+        const R d2x = R(g.dx * g.dx), d2y = R(g.dy * g.dy), d2z = R(g.dz * g.dz);
+        // |a_m x a_n|^2 of the rows a1 = d_x u, a2 = d_y u, a3 = d_z u
+        VT c12a = dv_dx * dw_dy - dw_dx * dv_dy, c12b = dw_dx * du_dy - du_dx * dw_dy, c12c = du_dx * dv_dy - dv_dx * du_dy;
+        VT c13a = dv_dx * dw_dz - dw_dx * dv_dz, c13b = dw_dx * du_dz - du_dx * dw_dz, c13c = du_dx * dv_dz - dv_dx * du_dz;
+        VT c23a = dv_dy * dw_dz - dw_dy * dv_dz, c23b = dw_dy * du_dz - du_dy * dw_dz, c23c = du_dy * dv_dz - dv_dy * du_dz;
+        VT x12 = c12a * c12a + c12b * c12b + c12c * c12c;
+        VT x13 = c13a * c13a + c13b * c13b + c13c * c13c;
+        VT x23 = c23a * c23a + c23b * c23b + c23c * c23c;
+        VT Bb = VT(d2x * d2y) * x12 + VT(d2x * d2z) * x13 + VT(d2y * d2z) * x23;
+        VT aa = du_dx * du_dx + du_dy * du_dy + du_dz * du_dz + dv_dx * dv_dx + dv_dy * dv_dy + dv_dz * dv_dz +
+                dw_dx * dw_dx + dw_dy * dw_dy + dw_dz * dw_dz;
+        return sqrt_ratio_or_zero(Bb, aa, R(g.sgs_cv));
+    }
     VT S12 = R(0.5) * (du_dy + dv_dx), S13 = R(0.5) * (du_dz + dw_dx), S23 = R(0.5) * (dv_dz + dw_dy);
     VT S2 = R(2) * (du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz) + R(4) * (S12 * S12 + S13 * S13 + S23 * S23);
     return VT(coef * sqrt(S2));

@@ -202,6 +202,8 @@ struct Core : CoreBase {
         uni = !c.stretched;
         sgs = c.c_s != 0.0;
         anel = c.core == AEO_CORE_ANELASTIC;
+        g.sgs_model = c.sgs_model;
+        g.sgs_cv = 2.5 * c.c_s * c.c_s;
         if (sizeof(R) == sizeof(float)) th_off = anel ? (thf ? thf[c.hz] : 0.0) : c.theta0;
         g.nx = c.nx; g.ny = c.ny; g.nz = c.nz;
         g.px = c.nx + 2 * AEO_HX;
@@ -1312,6 +1314,14 @@ static aeo_status validate(const aeo_config* c, const double* zf, const double* 
     if (c->stretched && (!zf || c->bc_z != AEO_BC_WALL)) { *m = "a stretched grid needs zf and walls in z"; return AEO_ERR_ARGUMENT; }
     if (c->precision != AEO_PREC_FP64 && c->precision != AEO_PREC_FP32_MIXED) { *m = "unknown precision"; return AEO_ERR_ARGUMENT; }
     if (c->c_s != 0.0 && !(c->pr_t > 0.0)) { *m = "pr_t must be positive with SGS"; return AEO_ERR_ARGUMENT; }
+    if (c->sgs_model != AEO_SGS_SMAGORINSKY && c->sgs_model != AEO_SGS_VREMAN) {
+        *m = "unknown SGS closure";
+        return AEO_ERR_ARGUMENT;
+    }
+    if (c->sgs_model == AEO_SGS_VREMAN && c->stretched) {
+        *m = "the Vreman closure takes a uniform grid (src/operators/sgs_amd_vreman.jl:280-284)";
+        return AEO_ERR_ARGUMENT;
+    }
     return AEO_OK;
 }
 

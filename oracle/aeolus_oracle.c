@@ -584,6 +584,22 @@ static inline double smag_at(const oc_sim* s, int i, int j, int k) {
     double S12 = 0.5 * (du_dy + dv_dx);
     double S13 = 0.5 * (du_dz + dw_dx);
     double S23 = 0.5 * (dv_dz + dw_dy);
+    if (s->p.sgs_model == OC_SGS_VREMAN) {
+        /* Vreman (2004): c sqrt(B_beta / alpha:alpha), c = 2.5 C_s^2, B_beta in the
+         * Cauchy-Binet form over the rows a_m = d_m u (_vreman_point,
+         * src/operators/sgs_amd_vreman.jl:93-100; _vreman_body! :293-298) */
+        double a1[3] = {du_dx, dv_dx, dw_dx}, a2[3] = {du_dy, dv_dy, dw_dy}, a3[3] = {du_dz, dv_dz, dw_dz};
+        double d2x = s->dx * s->dx, d2y = s->dy * s->dy, d2z = s->dz * s->dz;
+#define CROSS2(a, b) ((a[1] * b[2] - a[2] * b[1]) * (a[1] * b[2] - a[2] * b[1]) + \
+                      (a[2] * b[0] - a[0] * b[2]) * (a[2] * b[0] - a[0] * b[2]) + \
+                      (a[0] * b[1] - a[1] * b[0]) * (a[0] * b[1] - a[1] * b[0]))
+        double Bb = d2x * d2y * CROSS2(a1, a2) + d2x * d2z * CROSS2(a1, a3) + d2y * d2z * CROSS2(a2, a3);
+#undef CROSS2
+        double aa = du_dx * du_dx + du_dy * du_dy + du_dz * du_dz + dv_dx * dv_dx + dv_dy * dv_dy + dv_dz * dv_dz +
+                    dw_dx * dw_dx + dw_dy * dw_dy + dw_dz * dw_dz;
+        double c = 2.5 * s->p.c_s * s->p.c_s;
+        return aa > 0 ? c * sqrt(Bb / aa) : 0.0;
+    }
     double S2 = 2 * (S11 * S11 + S22 * S22 + S33 * S33) + 4 * (S12 * S12 + S13 * S13 + S23 * S23);
     return coef * sqrt(S2);
 }
@@ -1500,6 +1516,7 @@ oc_sim* oc_create(const oc_params* p, const double* zfi, const double* wc, const
     if (p->solver == OC_SOLVER_COLUMN && p->bc_z != OC_BC_WALL) return NULL;
     if (p->stretched && (!zfi || p->bc_z != OC_BC_WALL)) return NULL;
     if (p->solver == OC_SOLVER_PCG && (p->stretched || p->core != OC_CORE_BOUSSINESQ)) return NULL;
+    if (p->sgs_model == OC_SGS_VREMAN && p->stretched) return NULL;
     oc_sim* s = (oc_sim*)calloc(1, sizeof(oc_sim));
     s->p = *p;
     s->NX = p->nx + 2 * p->hx; s->NY = p->ny + 2 * p->hy; s->NZ = p->nz + 2 * p->hz;

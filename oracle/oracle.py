@@ -29,7 +29,7 @@ class OcParams(C.Structure):
         ("nu", C.c_double), ("theta0", C.c_double), ("g", C.c_double), ("f_coriolis", C.c_double),
         ("c_s", C.c_double), ("pr_t", C.c_double),
         ("flux_bot", C.c_double), ("flux_top", C.c_double), ("sponge_alpha", C.c_double),
-        ("sponge_zstart", C.c_double),
+        ("sponge_zstart", C.c_double), ("sgs_model", C.c_int32),
     ]
 
 
@@ -144,6 +144,7 @@ class OracleSimulation:
         p.c_s, p.pr_t = spec.c_s, spec.pr_t
         p.flux_bot, p.flux_top = spec.flux_bot, spec.flux_top
         p.sponge_alpha, p.sponge_zstart = spec.sponge_alpha, spec.sponge_zstart
+        p.sgs_model = {"smagorinsky": 0, "vreman": 1}[spec.sgs]
         self._keep = [g.zf, spec.wc, spec.wf, spec.thf]
         h = lib.oc_create(C.byref(p), _p(g.zf), _p(spec.wc), _p(spec.wf), _p(spec.thf))
         if not h:

@@ -150,8 +150,12 @@ def test_training_lowers_the_loss_on_poisson_pairs():
     net.set_mask(np.ones((nz, ny, nx), dtype=np.float32))
     net.set_out_scale(error_scale(pairs))
     first = np.mean([net.gradients(r, e) for r, e in pairs])
-    for epoch in range(12):
-        for r, e in pairs:
-            net.train_step(r, e, lr=2e-3)
+    # the learning rate decays geometrically as in train_streaming: per-pair
+    # Adam steps at a constant rate leave the last epoch's loss wandering, and
+    # the weight-gradient sums are FP32 atomics (not bit-reproducible)
+    nstep = 12 * len(pairs)
+    for q in range(nstep):
+        r, e = pairs[q % len(pairs)]
+        net.train_step(r, e, lr=2e-3 * (0.05 ** (q / (nstep - 1))))
     last = np.mean([net.gradients(r, e) for r, e in pairs])
     assert last < 0.7 * first, (first, last)
