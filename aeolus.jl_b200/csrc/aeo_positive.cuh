@@ -45,29 +45,35 @@ template <typename R>
 __device__ __forceinline__ R pos_beta(R a1, R a2) {
     return a1 * a1 + (R(13) / R(3)) * (a2 * a2);
 }
+// the weight divisions: IEEE in FP64; in FP32 the two-instruction
+// reciprocal-multiply (within 2 ulp; the denominators are normal numbers)
+__device__ __forceinline__ double pos_div(double a, double b) { return a / b; }
+__device__ __forceinline__ float pos_div(float a, float b) { return __fdividef(a, b); }
+
 template <typename R, int S>
 __device__ __forceinline__ R pos_recon(R v1, R v2, R v3, R v4, R v5) {
-    const R q0 = (R(2) * v1 - R(7) * v2 + R(11) * v3) / R(6);
-    const R q1 = (-v2 + R(5) * v3 + R(2) * v4) / R(6);
-    const R q2 = (R(2) * v3 + R(5) * v4 - v5) / R(6);
-    const R b0 = pos_beta<R>((v1 - R(4) * v2 + R(3) * v3) / R(2), (v1 - R(2) * v2 + v3) / R(2));
-    const R b1 = pos_beta<R>((v4 - v2) / R(2), (v2 - R(2) * v3 + v4) / R(2));
-    const R b2 = pos_beta<R>((-R(3) * v3 + R(4) * v4 - v5) / R(2), (v3 - R(2) * v4 + v5) / R(2));
+    const R sixth = R(1) / R(6), half = R(0.5);
+    const R q0 = (R(2) * v1 - R(7) * v2 + R(11) * v3) * sixth;
+    const R q1 = (-v2 + R(5) * v3 + R(2) * v4) * sixth;
+    const R q2 = (R(2) * v3 + R(5) * v4 - v5) * sixth;
+    const R b0 = pos_beta<R>((v1 - R(4) * v2 + R(3) * v3) * half, (v1 - R(2) * v2 + v3) * half);
+    const R b1 = pos_beta<R>((v4 - v2) * half, (v2 - R(2) * v3 + v4) * half);
+    const R b2 = pos_beta<R>((-R(3) * v3 + R(4) * v4 - v5) * half, (v3 - R(2) * v4 + v5) * half);
     R a0, a1, a2;
     if (S == AEO_ADV_WENO_JS5) {
         const R e = R(1e-6);
-        a0 = (R(1) / R(10)) / ((b0 + e) * (b0 + e));
-        a1 = (R(6) / R(10)) / ((b1 + e) * (b1 + e));
-        a2 = (R(3) / R(10)) / ((b2 + e) * (b2 + e));
+        a0 = pos_div(R(0.1), (b0 + e) * (b0 + e));
+        a1 = pos_div(R(0.6), (b1 + e) * (b1 + e));
+        a2 = pos_div(R(0.3), (b2 + e) * (b2 + e));
     } else {   // p = 2, eps = eps(T)^2
         const R eps = sizeof(R) == 8 ? R(4.930380657631324e-32) : R(1.4210854715202004e-14);
         const R tau = fabs(b0 - b2);
-        const R t0 = tau / (b0 + eps), t1 = tau / (b1 + eps), t2 = tau / (b2 + eps);
-        a0 = (R(1) / R(10)) * (R(1) + t0 * t0);
-        a1 = (R(6) / R(10)) * (R(1) + t1 * t1);
-        a2 = (R(3) / R(10)) * (R(1) + t2 * t2);
+        const R t0 = pos_div(tau, b0 + eps), t1 = pos_div(tau, b1 + eps), t2 = pos_div(tau, b2 + eps);
+        a0 = R(0.1) * (R(1) + t0 * t0);
+        a1 = R(0.6) * (R(1) + t1 * t1);
+        a2 = R(0.3) * (R(1) + t2 * t2);
     }
-    return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
+    return pos_div(a0 * q0 + a1 * q1 + a2 * q2, a0 + a1 + a2);
 }
 
 // the face value between cells c and c+1 (c at p, the axis stride s): the
