@@ -283,8 +283,11 @@ def dist_setup():
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        backend = "gloo"
+        if torch.cuda.is_available():   # one rank per GPU; gloo for the host-only (CPU) runs
+            torch.cuda.set_device(local)
+            backend = "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
@@ -299,7 +302,7 @@ def max_over_ranks(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -686,6 +689,9 @@ def run_tracer(args):
                                    "limiter active (zero regions and blocks)", "grid": [n, n, n],
                        "l2": "inputs larger than L2"}}
     if args.impl == "reference":
+        world, rank, _ = dist_setup()
+        if rank != 0:
+            return 0
         from oracle.oracle import OracleSimulation, set_threads
         cores = os.cpu_count() or 1
         set_threads(cores)
