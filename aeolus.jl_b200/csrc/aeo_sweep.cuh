@@ -464,6 +464,94 @@ __device__ __forceinline__ R sqrt_ratio_or_zero(R b, R a, R c) {
     return a > R(0) ? c * sqrt(b / a) : R(0);
 }
 
+// The sigma-model operator D = s3 (s1 - s2)(s2 - s3) / s1^2 of the velocity
+// gradient g (rows g_a = d u_a / d x_b), clipped at zero (sigma_operator,
+// src/operators/sigma_closure.jl:130-196): the eigenvalues of g^T g in closed
+// form -- the trigonometric solution in the deviator, then, where the smaller
+// gap is under 1 % of the spread, the simple eigenvalue deflated through the
+// largest cross product of two rows of G - lambda I and the close pair
+// recomputed from the 2 x 2 compression (_sym3_eigvals :48-97) -- and s3 from
+// the determinant (exactly zero for a gradient of rank <= 2).  Out of line:
+// the closed form is long and only the sigma closure calls it.
+template <typename R>
+__device__ __noinline__ R sigma_operator(R g11, R g12, R g13, R g21, R g22, R g23, R g31, R g32, R g33) {
+    const R G11 = g11 * g11 + g21 * g21 + g31 * g31, G22 = g12 * g12 + g22 * g22 + g32 * g32;
+    const R G33 = g13 * g13 + g23 * g23 + g33 * g33;
+    const R G12 = g11 * g12 + g21 * g22 + g31 * g32, G13 = g11 * g13 + g21 * g23 + g31 * g33;
+    const R G23 = g12 * g13 + g22 * g23 + g32 * g33;
+    const R m = (G11 + G22 + G33) / R(3);
+    const R a = G11 - m, b = G22 - m, c = G33 - m;
+    const R off2 = G12 * G12 + G13 * G13 + G23 * G23;
+    const R al1 = (a * a + b * b + c * c + R(2) * off2) / R(6);
+    R l1 = m, l2 = m;
+    if (al1 > R(0)) {
+        const R detd = a * (b * c - G23 * G23) - G12 * (G12 * c - G23 * G13) + G13 * (G12 * G23 - b * G13);
+        const R al2 = detd / R(2);
+        const R r = fmin(fmax(al2 / (al1 * sqrt(al1)), R(-1)), R(1));
+        R sp, cp;
+        sincos(acos(r) / R(3), &sp, &cp);
+        const R s = R(2) * sqrt(al1);
+        l1 = m + s * cp;
+        const R l3 = m - s * (cp + sqrt(R(3)) * sp) / R(2);
+        l2 = R(3) * m - l1 - l3;
+        if (!(fmin(l1 - l2, l2 - l3) >= R(0.01) * (l1 - l3))) {
+            const bool top = (l1 - l2) >= (l2 - l3);
+            const R iso = top ? l1 : l3;
+            const R r1x = G11 - iso, r1y = G12, r1z = G13;
+            const R r2x = G12, r2y = G22 - iso, r2z = G23;
+            const R r3x = G13, r3y = G23, r3z = G33 - iso;
+            // cross products of the rows; the largest is the simple eigenvector
+            R vx = r1y * r2z - r1z * r2y, vy = r1z * r2x - r1x * r2z, vz = r1x * r2y - r1y * r2x;
+            R nv = vx * vx + vy * vy + vz * vz;
+            {
+                const R cx = r1y * r3z - r1z * r3y, cy = r1z * r3x - r1x * r3z, cz = r1x * r3y - r1y * r3x;
+                const R n = cx * cx + cy * cy + cz * cz;
+                if (n > nv) { vx = cx; vy = cy; vz = cz; nv = n; }
+            }
+            {
+                const R cx = r2y * r3z - r2z * r3y, cy = r2z * r3x - r2x * r3z, cz = r2x * r3y - r2y * r3x;
+                const R n = cx * cx + cy * cy + cz * cz;
+                if (n > nv) { vx = cx; vy = cy; vz = cz; nv = n; }
+            }
+            if (nv > R(0)) {
+                const R inv = sqrt(nv);
+                vx = vx / inv; vy = vy / inv; vz = vz / inv;
+                const R ax = fabs(vx), ay = fabs(vy), az = fabs(vz);
+                const R tx = (ax <= ay && ax <= az) ? R(1) : R(0);
+                const R ty = (ax <= ay && ax <= az) ? R(0) : (ay <= az ? R(1) : R(0));
+                const R tz = (ax <= ay && ax <= az) ? R(0) : (ay <= az ? R(0) : R(1));
+                R e1x = vy * tz - vz * ty, e1y = vz * tx - vx * tz, e1z = vx * ty - vy * tx;
+                const R ne = sqrt(e1x * e1x + e1y * e1y + e1z * e1z);
+                e1x = e1x / ne; e1y = e1y / ne; e1z = e1z / ne;
+                const R e2x = vy * e1z - vz * e1y, e2y = vz * e1x - vx * e1z, e2z = vx * e1y - vy * e1x;
+                const R Gvx = G11 * vx + G12 * vy + G13 * vz, Gvy = G12 * vx + G22 * vy + G23 * vz,
+                        Gvz = G13 * vx + G23 * vy + G33 * vz;
+                const R G1x = G11 * e1x + G12 * e1y + G13 * e1z, G1y = G12 * e1x + G22 * e1y + G23 * e1z,
+                        G1z = G13 * e1x + G23 * e1y + G33 * e1z;
+                const R G2x = G11 * e2x + G12 * e2y + G13 * e2z, G2y = G12 * e2x + G22 * e2y + G23 * e2z,
+                        G2z = G13 * e2x + G23 * e2y + G33 * e2z;
+                const R liso = vx * Gvx + vy * Gvy + vz * Gvz;
+                const R pp = e1x * G1x + e1y * G1y + e1z * G1z;
+                const R qq = e1x * G2x + e1y * G2y + e1z * G2z;
+                const R rr = e2x * G2x + e2y * G2y + e2z * G2z;
+                const R h = sqrt((pp - rr) * (pp - rr) + R(4) * qq * qq) / R(2);
+                const R mp = (pp + rr) / R(2) + h, mm = (pp + rr) / R(2) - h;
+                if (top) { l1 = fmax(liso, mp); l2 = mp; }
+                else { l1 = mp; l2 = mm; }
+            }
+        }
+    }
+    const R s1 = sqrt(fmax(l1, R(0)));
+    if (!(s1 > R(0))) return R(0);
+    const R s2 = sqrt(fmax(l2, R(0)));
+    const R detg = g11 * (g22 * g33 - g23 * g32) - g12 * (g21 * g33 - g23 * g31) + g13 * (g21 * g32 - g22 * g31);
+    const R pr = s1 * s2;
+    const R s3 = pr > R(0) ? fabs(detg) / pr : R(0);
+    const R d12 = fmax(l1 - l2, R(0)) / (s1 + s2);
+    return fmax(s3 * d12 * (s2 - s3) / (s1 * s1), R(0));
+}
+
+
 // Smagorinsky nut = (C_s Delta_k)^2 |S| at a cell centre (src/FiniteVolume.jl:936-944,
 // strain src/Operators.jl:451-496), accessors around the point at level k; or,
 // with g.sgs_model = 1, Vreman's nut = c sqrt(B_beta / alpha:alpha) from the
@@ -486,6 +574,9 @@ __device__ __forceinline__ auto smag_point(const Met<R, UNI>& m, const Geo& g, i
     VT dw_dx = ((W(1, 0, 0) + W(1, 0, 1)) - (W(-1, 0, 0) + W(-1, 0, 1))) * (R(0.25) * idx);
     VT dv_dz = ((V(0, 0, 1) + V(0, 1, 1)) - (V(0, 0, -1) + V(0, 1, -1))) * (R(0.25) * ido);
     VT dw_dy = ((W(0, 1, 0) + W(0, 1, 1)) - (W(0, -1, 0) + W(0, -1, 1))) * (R(0.25) * idy);
+    if (g.sgs_model == 2)   // sigma model: (C_sigma Delta)^2 D_sigma (compute_sigma_nut!, sigma_closure.jl:208-222)
+        return VT(VT(coef) * sigma_operator(VT(du_dx), VT(du_dy), VT(du_dz), VT(dv_dx), VT(dv_dy), VT(dv_dz),
+                                            VT(dw_dx), VT(dw_dy), VT(dw_dz)));
     if (g.sgs_model == 1) {
         const R d2x = R(g.dx * g.dx), d2y = R(g.dy * g.dy), d2z = R(g.dz * g.dz);
         // |a_m x a_n|^2 of the rows a1 = d_x u, a2 = d_y u, a3 = d_z u

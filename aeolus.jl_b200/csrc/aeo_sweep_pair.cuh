@@ -14,7 +14,15 @@
 #pragma once
 
 #include "aeo_f2.cuh"
+
 #include "aeo_sweep_tile.cuh"
+
+// the sigma-model operator lane by lane (the closed-form eigenproblem has no
+// paired form)
+__device__ __forceinline__ F2 sigma_operator(F2 g11, F2 g12, F2 g13, F2 g21, F2 g22, F2 g23, F2 g31, F2 g32, F2 g33) {
+    return F2(sigma_operator<float>(g11.v.x, g12.v.x, g13.v.x, g21.v.x, g22.v.x, g23.v.x, g31.v.x, g32.v.x, g33.v.x),
+              sigma_operator<float>(g11.v.y, g12.v.y, g13.v.y, g21.v.y, g22.v.y, g23.v.y, g31.v.y, g32.v.y, g33.v.y));
+}
 
 template <bool SGS>
 struct PairShape {

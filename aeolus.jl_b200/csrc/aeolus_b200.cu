@@ -1314,12 +1314,13 @@ static aeo_status validate(const aeo_config* c, const double* zf, const double* 
     if (c->stretched && (!zf || c->bc_z != AEO_BC_WALL)) { *m = "a stretched grid needs zf and walls in z"; return AEO_ERR_ARGUMENT; }
     if (c->precision != AEO_PREC_FP64 && c->precision != AEO_PREC_FP32_MIXED) { *m = "unknown precision"; return AEO_ERR_ARGUMENT; }
     if (c->c_s != 0.0 && !(c->pr_t > 0.0)) { *m = "pr_t must be positive with SGS"; return AEO_ERR_ARGUMENT; }
-    if (c->sgs_model != AEO_SGS_SMAGORINSKY && c->sgs_model != AEO_SGS_VREMAN) {
+    if (c->sgs_model != AEO_SGS_SMAGORINSKY && c->sgs_model != AEO_SGS_VREMAN && c->sgs_model != AEO_SGS_SIGMA) {
         *m = "unknown SGS closure";
         return AEO_ERR_ARGUMENT;
     }
-    if (c->sgs_model == AEO_SGS_VREMAN && c->stretched) {
-        *m = "the Vreman closure takes a uniform grid (src/operators/sgs_amd_vreman.jl:280-284)";
+    if (c->sgs_model != AEO_SGS_SMAGORINSKY && c->stretched) {
+        *m = "the Vreman and sigma closures take a uniform grid (src/operators/sgs_amd_vreman.jl:280-284, "
+             "src/operators/sigma_closure.jl:208-212)";
         return AEO_ERR_ARGUMENT;
     }
     return AEO_OK;

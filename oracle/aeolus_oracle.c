@@ -566,6 +566,85 @@ static inline double recon_mom_w(const oc_sim* s, int sc, const double* u, const
     return dx + dy + dz;
 }
 
+/* sigma_operator (src/operators/sigma_closure.jl:130-196): the eigenvalues of
+ * g^T g by _sym3_eigvals (:48-97: the trigonometric solution in the
+ * deviator; where the smaller gap is under 1 % of the spread, the simple
+ * eigenvalue deflated through the largest cross product of two rows of
+ * G - lambda I and the close pair from the 2 x 2 compression), s3 from the
+ * determinant, D = s3 (s1 - s2)(s2 - s3) / s1^2 clipped at zero. */
+static double sigma_op(double g11, double g12, double g13, double g21, double g22, double g23, double g31,
+                       double g32, double g33) {
+    double G11 = g11 * g11 + g21 * g21 + g31 * g31, G22 = g12 * g12 + g22 * g22 + g32 * g32;
+    double G33 = g13 * g13 + g23 * g23 + g33 * g33;
+    double G12 = g11 * g12 + g21 * g22 + g31 * g32, G13 = g11 * g13 + g21 * g23 + g31 * g33;
+    double G23 = g12 * g13 + g22 * g23 + g32 * g33;
+    double m = (G11 + G22 + G33) / 3;
+    double a = G11 - m, b = G22 - m, c = G33 - m;
+    double off2 = G12 * G12 + G13 * G13 + G23 * G23;
+    double al1 = (a * a + b * b + c * c + 2 * off2) / 6;
+    double l1 = m, l2 = m;
+    if (al1 > 0) {
+        double detd = a * (b * c - G23 * G23) - G12 * (G12 * c - G23 * G13) + G13 * (G12 * G23 - b * G13);
+        double al2 = detd / 2;
+        double r = al2 / (al1 * sqrt(al1));
+        r = r < -1 ? -1 : (r > 1 ? 1 : r);
+        double ph = acos(r) / 3, sp = sin(ph), cp = cos(ph);
+        double sv = 2 * sqrt(al1);
+        l1 = m + sv * cp;
+        double l3 = m - sv * (cp + sqrt(3.0) * sp) / 2;
+        l2 = 3 * m - l1 - l3;
+        double gap = (l1 - l2) < (l2 - l3) ? (l1 - l2) : (l2 - l3);
+        if (!(gap >= 0.01 * (l1 - l3))) {
+            int top = (l1 - l2) >= (l2 - l3);
+            double iso = top ? l1 : l3;
+            double r1[3] = {G11 - iso, G12, G13}, r2[3] = {G12, G22 - iso, G23}, r3[3] = {G13, G23, G33 - iso};
+            double cr[3][3] = {{r1[1] * r2[2] - r1[2] * r2[1], r1[2] * r2[0] - r1[0] * r2[2], r1[0] * r2[1] - r1[1] * r2[0]},
+                               {r1[1] * r3[2] - r1[2] * r3[1], r1[2] * r3[0] - r1[0] * r3[2], r1[0] * r3[1] - r1[1] * r3[0]},
+                               {r2[1] * r3[2] - r2[2] * r3[1], r2[2] * r3[0] - r2[0] * r3[2], r2[0] * r3[1] - r2[1] * r3[0]}};
+            int best = 0;
+            double nv = cr[0][0] * cr[0][0] + cr[0][1] * cr[0][1] + cr[0][2] * cr[0][2];
+            for (int q = 1; q < 3; ++q) {
+                double n = cr[q][0] * cr[q][0] + cr[q][1] * cr[q][1] + cr[q][2] * cr[q][2];
+                if (n > nv) { nv = n; best = q; }
+            }
+            if (nv > 0) {
+                double sn = sqrt(nv);
+                double v[3] = {cr[best][0] / sn, cr[best][1] / sn, cr[best][2] / sn};
+                double ax = fabs(v[0]), ay = fabs(v[1]), az = fabs(v[2]);
+                double t[3] = {0, 0, 0};
+                if (ax <= ay && ax <= az) t[0] = 1; else if (ay <= az) t[1] = 1; else t[2] = 1;
+                double e1[3] = {v[1] * t[2] - v[2] * t[1], v[2] * t[0] - v[0] * t[2], v[0] * t[1] - v[1] * t[0]};
+                double ne = sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+                e1[0] /= ne; e1[1] /= ne; e1[2] /= ne;
+                double e2[3] = {v[1] * e1[2] - v[2] * e1[1], v[2] * e1[0] - v[0] * e1[2], v[0] * e1[1] - v[1] * e1[0]};
+#define SYMMUL(x, o) do { o[0] = G11 * x[0] + G12 * x[1] + G13 * x[2]; \
+                          o[1] = G12 * x[0] + G22 * x[1] + G23 * x[2]; \
+                          o[2] = G13 * x[0] + G23 * x[1] + G33 * x[2]; } while (0)
+                double Gv[3], Ge1[3], Ge2[3];
+                SYMMUL(v, Gv); SYMMUL(e1, Ge1); SYMMUL(e2, Ge2);
+#undef SYMMUL
+                double liso = v[0] * Gv[0] + v[1] * Gv[1] + v[2] * Gv[2];
+                double pp = e1[0] * Ge1[0] + e1[1] * Ge1[1] + e1[2] * Ge1[2];
+                double qq = e1[0] * Ge2[0] + e1[1] * Ge2[1] + e1[2] * Ge2[2];
+                double rr = e2[0] * Ge2[0] + e2[1] * Ge2[1] + e2[2] * Ge2[2];
+                double h = sqrt((pp - rr) * (pp - rr) + 4 * qq * qq) / 2;
+                double mp = (pp + rr) / 2 + h, mm = (pp + rr) / 2 - h;
+                if (top) { l1 = liso > mp ? liso : mp; l2 = mp; }
+                else { l1 = mp; l2 = mm; }
+            }
+        }
+    }
+    double s1 = sqrt(l1 > 0 ? l1 : 0);
+    if (!(s1 > 0)) return 0.0;
+    double s2 = sqrt(l2 > 0 ? l2 : 0);
+    double detg = g11 * (g22 * g33 - g23 * g32) - g12 * (g21 * g33 - g23 * g31) + g13 * (g21 * g32 - g22 * g31);
+    double pr = s1 * s2;
+    double s3 = pr > 0 ? fabs(detg) / pr : 0.0;
+    double d12 = (l1 - l2 > 0 ? l1 - l2 : 0) / (s1 + s2);
+    double D = s3 * d12 * (s2 - s3) / (s1 * s1);
+    return D > 0 ? D : 0.0;
+}
+
 /* --- Smagorinsky (src/FiniteVolume.jl:936-944, src/Operators.jl:451-496) -- */
 static inline double smag_at(const oc_sim* s, int i, int j, int k) {
     const double *u = s->u, *v = s->v, *w = s->w;
@@ -584,6 +663,8 @@ static inline double smag_at(const oc_sim* s, int i, int j, int k) {
     double S12 = 0.5 * (du_dy + dv_dx);
     double S13 = 0.5 * (du_dz + dw_dx);
     double S23 = 0.5 * (dv_dz + dw_dy);
+    if (s->p.sgs_model == OC_SGS_SIGMA)   /* (C_sigma Delta)^2 D_sigma, compute_sigma_nut! (sigma_closure.jl:208-222) */
+        return coef * sigma_op(du_dx, du_dy, du_dz, dv_dx, dv_dy, dv_dz, dw_dx, dw_dy, dw_dz);
     if (s->p.sgs_model == OC_SGS_VREMAN) {
         /* Vreman (2004): c sqrt(B_beta / alpha:alpha), c = 2.5 C_s^2, B_beta in the
          * Cauchy-Binet form over the rows a_m = d_m u (_vreman_point,
@@ -1516,7 +1597,7 @@ oc_sim* oc_create(const oc_params* p, const double* zfi, const double* wc, const
     if (p->solver == OC_SOLVER_COLUMN && p->bc_z != OC_BC_WALL) return NULL;
     if (p->stretched && (!zfi || p->bc_z != OC_BC_WALL)) return NULL;
     if (p->solver == OC_SOLVER_PCG && (p->stretched || p->core != OC_CORE_BOUSSINESQ)) return NULL;
-    if (p->sgs_model == OC_SGS_VREMAN && p->stretched) return NULL;
+    if ((p->sgs_model == OC_SGS_VREMAN || p->sgs_model == OC_SGS_SIGMA) && p->stretched) return NULL;
     oc_sim* s = (oc_sim*)calloc(1, sizeof(oc_sim));
     s->p = *p;
     s->NX = p->nx + 2 * p->hx; s->NY = p->ny + 2 * p->hy; s->NZ = p->nz + 2 * p->hz;
