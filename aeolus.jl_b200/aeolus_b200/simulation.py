@@ -125,6 +125,22 @@ class Simulation:
         _lib.check(self._lib.aeo_get_field(self._h, FIELDS[name], _ptr(out)), self._h)
         return out
 
+    def set_field_f32(self, name: str, data: np.ndarray):
+        """set_field from an FP32 host array (half the bytes)."""
+        a = np.ascontiguousarray(data, dtype=np.float32)
+        if a.shape != self.grid.storage_shape:
+            raise ValueError(f"{name}: expected storage shape {self.grid.storage_shape}, got {a.shape}")
+        _lib.check(self._lib.aeo_set_field_f32(self._h, FIELDS[name], a.ctypes.data_as(C.c_void_p)), self._h)
+
+    def get_field_f32(self, name: str, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """get_field into an FP32 host array."""
+        if out is None:
+            out = np.empty(self.grid.storage_shape, dtype=np.float32)
+        if out.dtype != np.float32 or out.shape != self.grid.storage_shape or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float32 array of the storage shape")
+        _lib.check(self._lib.aeo_get_field_f32(self._h, FIELDS[name], out.ctypes.data_as(C.c_void_p)), self._h)
+        return out
+
     def set_state(self, u, v, w, theta):
         self.set_field("u", u)
         self.set_field("v", v)

@@ -135,14 +135,14 @@ __global__ void __launch_bounds__(256) correct_kernel(Geo g, const R* __restrict
 
 // ---- host-layout packing ----------------------------------------------------------
 // Host storage (reference layout, halos hh) <-> device padded interior.
-template <typename R>
-__global__ void unpack_host_kernel(Geo g, const double* __restrict__ hsrc, int hx, int hy, int hz,
+template <typename R, typename S = double>
+__global__ void unpack_host_kernel(Geo g, const S* __restrict__ hsrc, int hx, int hy, int hz,
                                    R* __restrict__ dst, int padded, double off) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int j = blockIdx.y, k = blockIdx.z;
     if (i >= g.nx) return;
     long long HX = g.nx + 2LL * hx, HY = g.ny + 2LL * hy;
-    double v = hsrc[(i + hx) + HX * ((j + hy) + HY * (long long)(k + hz))] - off;
+    double v = (double)hsrc[(i + hx) + HX * ((j + hy) + HY * (long long)(k + hz))] - off;
     if (padded) dst[pidx(g, i, j, k)] = R(v);
     else dst[iidx(g, i, j, k)] = R(v);
 }
@@ -150,8 +150,8 @@ __global__ void unpack_host_kernel(Geo g, const double* __restrict__ hsrc, int h
 // Fill the whole host storage array from the device interior through the
 // composite boundary map (loc < 0: halos zero); `off` is added back to every
 // mapped value (the stored offset of theta, 0 otherwise).
-template <typename R>
-__global__ void pack_host_kernel(Geo g, double* __restrict__ hdst, int hx, int hy, int hz,
+template <typename R, typename S = double>
+__global__ void pack_host_kernel(Geo g, S* __restrict__ hdst, int hx, int hy, int hz,
                                  const R* __restrict__ src, int padded, int loc, double off) {
     long long HX = g.nx + 2LL * hx, HY = g.ny + 2LL * hy, HZ = g.nz + 2LL * hz;
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -171,7 +171,7 @@ __global__ void pack_host_kernel(Geo g, double* __restrict__ hdst, int hx, int h
             v = (s > 0 ? (double)r : -(double)r) + off;
         }
     }
-    hdst[t] = v;
+    hdst[t] = S(v);
 }
 
 // interior-sized double <-> interior R

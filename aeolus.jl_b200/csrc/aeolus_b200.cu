@@ -86,6 +86,8 @@ struct CoreBase {
     virtual aeo_status init(const double* zf, const double* wc, const double* wf, const double* thf) = 0;
     virtual aeo_status set_field(int id, const double* host) = 0;
     virtual aeo_status get_field(int id, double* host) = 0;
+    virtual aeo_status set_field_f32(int id, const float* host) = 0;
+    virtual aeo_status get_field_f32(int id, float* host) = 0;
     virtual aeo_status step_rk3(double dt, int n, bool sync) = 0;
     virtual aeo_status step_euler(double dt, int n) = 0;
     virtual aeo_status step_adaptive(const aeo_cfl* c, int n, double* dt_prev, aeo_adaptive_stats* stats) = 0;
@@ -1015,14 +1017,23 @@ struct Core : CoreBase {
         }
     }
 
-    aeo_status set_field(int id, const double* host) override {
+    aeo_status set_field(int id, const double* host) override { return set_field_t<double>(id, host); }
+    aeo_status get_field(int id, double* host) override { return get_field_t<double>(id, host); }
+    aeo_status set_field_f32(int id, const float* host) override { return set_field_t<float>(id, host); }
+    aeo_status get_field_f32(int id, float* host) override { return get_field_t<float>(id, host); }
+
+    // the host array (FP64 or FP32, the reference storage layout) through the
+    // staging buffer into the device field, and back
+    template <typename S>
+    aeo_status set_field_t(int id, const S* host) {
         int padded, loc;
         R* d = field_ptr(id, &padded, &loc);
         if (!d) { fail("set_field: unknown or unavailable field"); return AEO_ERR_ARGUMENT; }
-        CK(cudaMemcpyAsync(d_stage, host, host_n * sizeof(double), cudaMemcpyHostToDevice, st));
+        S* stage = reinterpret_cast<S*>(d_stage);
+        CK(cudaMemcpyAsync(stage, host, host_n * sizeof(S), cudaMemcpyHostToDevice, st));
         dim3 gb((g.nx + 127) / 128, g.ny, g.nz);
-        unpack_host_kernel<R><<<gb, 128, 0, st>>>(g, d_stage, cfg.hx, cfg.hy, cfg.hz, d, padded,
-                                                  id == AEO_FIELD_THETA ? th_off : 0.0);
+        unpack_host_kernel<R, S><<<gb, 128, 0, st>>>(g, stage, cfg.hx, cfg.hy, cfg.hz, d, padded,
+                                                     id == AEO_FIELD_THETA ? th_off : 0.0);
         CKL();
         if (padded && loc >= 0) {
             if (loc == LOC_FZ && g.bc_z == 1) {
@@ -1037,7 +1048,8 @@ struct Core : CoreBase {
         return AEO_OK;
     }
 
-    aeo_status get_field(int id, double* host) override {
+    template <typename S>
+    aeo_status get_field_t(int id, S* host) {
         int padded, loc;
         R* d = field_ptr(id, &padded, &loc);
         if (!d) { fail("get_field: unknown or unavailable field"); return AEO_ERR_ARGUMENT; }
@@ -1047,11 +1059,12 @@ struct Core : CoreBase {
             else smagorinsky_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], nut, R(cfg.c_s));
             CKL();
         }
-        pack_host_kernel<R><<<(unsigned)((host_n + 255) / 256), 256, 0, st>>>(g, d_stage, cfg.hx, cfg.hy, cfg.hz, d,
-                                                                              padded, loc,
-                                                                              id == AEO_FIELD_THETA ? th_off : 0.0);
+        S* stage = reinterpret_cast<S*>(d_stage);
+        pack_host_kernel<R, S><<<(unsigned)((host_n + 255) / 256), 256, 0, st>>>(g, stage, cfg.hx, cfg.hy, cfg.hz, d,
+                                                                                 padded, loc,
+                                                                                 id == AEO_FIELD_THETA ? th_off : 0.0);
         CKL();
-        CK(cudaMemcpyAsync(host, d_stage, host_n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(host, stage, host_n * sizeof(S), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         return AEO_OK;
     }
@@ -1374,6 +1387,18 @@ aeo_status aeo_get_field(aeo_sim* h, int32_t field, double* host) {
     ENTER(h);
     if (!host) { h->core->fail("host pointer is NULL"); return AEO_ERR_ARGUMENT; }
     return h->core->get_field(field, host);
+}
+
+aeo_status aeo_set_field_f32(aeo_sim* h, int32_t field, const float* host) {
+    ENTER(h);
+    if (!host) { h->core->fail("host pointer is NULL"); return AEO_ERR_ARGUMENT; }
+    return h->core->set_field_f32(field, host);
+}
+
+aeo_status aeo_get_field_f32(aeo_sim* h, int32_t field, float* host) {
+    ENTER(h);
+    if (!host) { h->core->fail("host pointer is NULL"); return AEO_ERR_ARGUMENT; }
+    return h->core->get_field_f32(field, host);
 }
 
 aeo_status aeo_step_rk3(aeo_sim* h, double dt, int32_t nsteps) {

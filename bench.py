@@ -324,26 +324,31 @@ def timed_steps(sim, dt, k, world):
     return e0.elapsed_time(e1)
 
 
-def e2e_steps(sim, state, dt, k):
+def e2e_steps(sim, state, dt, k, f32=False):
     """Through the C-ABI with host buffers: every step uploads u, v, w, theta
-    from pinned host memory, steps, and downloads them again."""
+    from pinned host memory, steps, and downloads them again -- FP64 host
+    arrays, or with f32 the FP32 ones of aeo_set_field_f32 / aeo_get_field_f32
+    (an FP32-mixed domain's host mirror)."""
     import torch
+    dt_host = torch.float32 if f32 else torch.float64
     pinned = []
     for a in state:
-        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        t = torch.empty(a.shape, dtype=dt_host, pin_memory=True)
         t.numpy()[...] = a
         pinned.append(t.numpy())
-    outs = [torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy() for a in state]
+    outs = [torch.empty(a.shape, dtype=dt_host, pin_memory=True).numpy() for a in state]
+    put = sim.set_field_f32 if f32 else sim.set_field
+    get = sim.get_field_f32 if f32 else sim.get_field
     stream = torch.cuda.ExternalStream(sim.stream)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     sim.synchronize()
     e0.record(stream)
     for _ in range(k):
         for n, a in zip(("u", "v", "w", "theta"), pinned):
-            sim.set_field(n, a)
+            put(n, a)
         sim.step_rk3(dt, 1)
         for n, o in zip(("u", "v", "w", "theta"), outs):
-            sim.get_field(n, o)
+            get(n, o)
     e1.record(stream)
     sim.synchronize()
     nbytes = sum(a.nbytes for a in pinned)
@@ -881,7 +886,7 @@ def run_b200_urban_step(args):
         prof = sim.profile_step(dt)
         st = sim.pcg_stats()
         launches = sim.launches_per_step()
-        e2e_ms, h2d, d2h = e2e_steps(sim, state, dt, 2)
+        e2e_ms, h2d, d2h = e2e_steps(sim, state, dt, 2, f32=prec == "fp32_mixed")
         out = dict(ms=ms, ms_traj=ms_traj, prof=prof, st=st, launches=launches, clocks=clocks, rel=rel, ke=ke,
                    div=div, e2e_ms=max_over_ranks(e2e_ms, world), h2d=h2d, d2h=d2h)
         if prec == "fp32_mixed" and args.learned:
@@ -991,7 +996,7 @@ def run_b200(args):
         clocks = clk.stop()
         ms_total = max_over_ranks(ms_total, world)
         ms = ms_total / args.steps
-        e2e_ms, h2d, d2h = e2e_steps(sim, state, dt, max(2, min(args.steps, 5)))
+        e2e_ms, h2d, d2h = e2e_steps(sim, state, dt, max(2, min(args.steps, 5)), f32=prec == "fp32_mixed")
         e2e_ms = max_over_ranks(e2e_ms, world)
         results[prec] = dict(ms=ms, prof=prof, clocks=clocks, e2e_ms=e2e_ms, h2d=h2d, d2h=d2h,
                              launches=sim.launches_per_step(), div=sim.max_divergence(),

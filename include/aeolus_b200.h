@@ -111,6 +111,12 @@ aeo_status aeo_set_field(aeo_sim* h, int32_t field, const double* host);
  * Smagorinsky viscosity of the current state: the step itself keeps νt in
  * shared memory only. */
 aeo_status aeo_get_field(aeo_sim* h, int32_t field, double* host);
+/* The same with FP32 host arrays (half the host<->device bytes; the values
+ * are the FP32 roundings of the FP64 ones, exact for an FP32-mixed domain's
+ * stored state).  No reference counterpart: a Float32 host mirror of the
+ * fields for AEO_PREC_FP32_MIXED domains. */
+aeo_status aeo_set_field_f32(aeo_sim* h, int32_t field, const float* host);
+aeo_status aeo_get_field_f32(aeo_sim* h, int32_t field, float* host);
 
 /* nsteps projected SSP-RK3 steps of size dt: step_rk3! of the Boussinesq
  * core (src/Simulations.jl:843-904) or of the sound-proof core
