@@ -20,7 +20,7 @@ import numpy as np
 from . import _lib as L
 
 BCS = {"periodic": 0, "neumann": 1}
-PRECONDITIONERS = {"identity": 0, "vcycle": 1}   # "learned": see MGPreconditionedCG.set_learned
+PRECONDITIONERS = {"identity": 0, "vcycle": 1, "jacobi": 3}   # "learned": see MGPreconditionedCG.set_learned
 PRECISIONS = {"fp64": 0, "fp32_mixed": 1}
 STATUS = {0: "converged", 1: "maxit", 2: "breakdown", 3: "zero_rhs"}
 

@@ -420,6 +420,14 @@ __global__ void pcg_dir_kernel(double* __restrict__ p, const Z* __restrict__ z, 
     GRID_STRIDE(q, n) p[q] = first ? double(z[q]) - m : (double(z[q]) - m) + beta * p[q];
 }
 
+// z = r / diag(A), the Jacobi preconditioner (1/diag precomputed; 0 on a
+// fully blocked cell)
+__global__ void pcg_jacobi_kernel(double* __restrict__ z, const double* __restrict__ r,
+                                  const double* __restrict__ invd, int n, const PcgState* S) {
+    if (S->done) return;
+    GRID_STRIDE(q, n) z[q] = r[q] * invd[q];
+}
+
 // the loop condition of the WHILE node: mode 0 CG, mode 1 multigrid cycles
 __global__ void pcg_cond_kernel(PcgState* S, cudaGraphConditionalHandle h, int mode) {
     unsigned go = (S->done == 0 && S->iters < S->maxit) ? 1u : 0u;

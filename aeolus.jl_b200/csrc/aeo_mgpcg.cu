@@ -191,6 +191,9 @@ template <typename R>
 struct Mg : MgBase {
     cudaStream_t st = nullptr, st_body = nullptr, st_br[2] = {nullptr, nullptr};
     aeo_unet* net = nullptr;       // the learned preconditioner (AEO_PC_LEARNED)
+    double* invd = nullptr;        // AEO_PC_JACOBI: 1 / the operator's diagonal (0 on a fully blocked cell)
+    double* zj = nullptr;          // ... and z = r / diag
+    std::vector<double> h_invd;
     double* hist_x = nullptr;      // harvest history, `hist_cap` slots of n
     double* hist_r = nullptr;
     int hist_cap = 0;
@@ -295,6 +298,29 @@ struct Mg : MgBase {
         int nx = cfg.nx, ny = cfg.ny, nz = cfg.nz;
         double dx = cfg.dx, dy = cfg.dy, dz = cfg.dz;
         n = nx * ny * nz;
+        if (cfg.precond == AEO_PC_JACOBI) {
+            // the diagonal of the fine operator: -sum over the faces of c / h^2,
+            // a Neumann boundary face (whose mirror neighbour is the cell itself)
+            // contributing nothing
+            h_invd.assign((size_t)n, 0.0);
+            const double ix2 = 1.0 / (dx * dx), iy2 = 1.0 / (dy * dy), iz2 = 1.0 / (dz * dz);
+            auto C3 = [&](const double* c, size_t f) { return c ? c[f] : 1.0; };
+            for (int k = 0; k < nz; ++k)
+                for (int j = 0; j < ny; ++j)
+                    for (int i = 0; i < nx; ++i) {
+                        const size_t q = (size_t)i + (size_t)nx * (j + (size_t)ny * k);
+                        const size_t xr = (size_t)(nx + 1) * (j + (size_t)ny * k) + i;
+                        const size_t yr = (size_t)nx * (j + (size_t)(ny + 1) * k) + i;
+                        double sum = 0.0;
+                        if (!(i == 0 && cfg.bc_x == AEO_MG_NEUMANN)) sum += C3(cx, xr) * ix2;
+                        if (!(i == nx - 1 && cfg.bc_x == AEO_MG_NEUMANN)) sum += C3(cx, xr + 1) * ix2;
+                        if (!(j == 0 && cfg.bc_y == AEO_MG_NEUMANN)) sum += C3(cy, yr) * iy2;
+                        if (!(j == ny - 1 && cfg.bc_y == AEO_MG_NEUMANN)) sum += C3(cy, yr + nx) * iy2;
+                        if (!(k == 0 && cfg.bc_z == AEO_MG_NEUMANN)) sum += C3(cz, q) * iz2;
+                        if (!(k == nz - 1 && cfg.bc_z == AEO_MG_NEUMANN)) sum += C3(cz, q + (size_t)nx * ny) * iz2;
+                        h_invd[q] = sum > 0.0 ? -1.0 / sum : 0.0;
+                    }
+        }
         std::vector<double> hx, hy, hz;
         if (coeff) {
             hx.assign(cx, cx + (size_t)(nx + 1) * ny * nz);
@@ -415,6 +441,11 @@ struct Mg : MgBase {
         if (aeo_status s = dalloc(&r, n)) return s;
         if (aeo_status s = dalloc(&p, n)) return s;
         if (aeo_status s = dalloc(&Ap, n)) return s;
+        if (cfg.precond == AEO_PC_JACOBI) {
+            if (aeo_status s = dalloc(&invd, n)) return s;
+            if (aeo_status s = dalloc(&zj, n)) return s;
+            CK(cudaMemcpy(invd, h_invd.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        }
         part_cap = (size_t)RED_BLOCKS * 8;
         for (int l = 0; l + 1 < nl; ++l) {
             dim3 g = restrict_grid(L[l + 1]);
@@ -568,6 +599,12 @@ struct Mg : MgBase {
             pcg_rz_kernel<R><<<RED_BLOCKS, TPB, 0, s>>>(r, L[0].phi, Ap, n, S, part, first);
             CKL();
             pcg_dir_kernel<R><<<RED_BLOCKS, TPB, 0, s>>>(p, L[0].phi, n, S, first);
+        } else if (pc == AEO_PC_JACOBI) {
+            pcg_jacobi_kernel<<<RED_BLOCKS, TPB, 0, s>>>(zj, r, invd, n, S);
+            CKL();
+            pcg_rz_kernel<double><<<RED_BLOCKS, TPB, 0, s>>>(r, zj, Ap, n, S, part, first);
+            CKL();
+            pcg_dir_kernel<double><<<RED_BLOCKS, TPB, 0, s>>>(p, zj, n, S, first);
         } else {
             pcg_rz_kernel<double><<<RED_BLOCKS, TPB, 0, s>>>(r, r, Ap, n, S, part, first);
             CKL();
@@ -723,7 +760,9 @@ struct Mg : MgBase {
         if (aeo_status q = launch_rz_dir(s0, 1)) return q;
         pcg_cond_kernel<<<1, 1, 0, s0>>>(S, hdl, 0);
         CKL();
-        if (!harvest) prologue_launches = 5 + (cfg.precond == AEO_PC_VCYCLE ? vcycle_launches() : 0);
+        if (!harvest)
+            prologue_launches = 5 + (cfg.precond == AEO_PC_VCYCLE ? vcycle_launches() : 0) +
+                                (cfg.precond == AEO_PC_JACOBI ? 1 : 0);
         if (aeo_status q = capture_cond(s0, hdl, cudaGraphCondTypeWhile, 1, &st_body,
                 [&](cudaStream_t sb) -> aeo_status {
                     int c0 = 0;
@@ -745,7 +784,7 @@ struct Mg : MgBase {
                             c0 += vcycle_launches();
                         }
                         if (aeo_status q2 = launch_rz_dir(sb, 0)) return q2;
-                        c0 += 2;
+                        c0 += cfg.precond == AEO_PC_JACOBI ? 3 : 2;
                     }
                     pcg_cond_kernel<<<1, 1, 0, sb>>>(S, hdl, 0);
                     CKL();
@@ -891,6 +930,8 @@ struct Mg : MgBase {
             CK(cudaMemcpyAsync(hz.data(), aeo_unet_output(net), sizeof(float) * n, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             for (int q = 0; q < n; ++q) zout[q] = double(hz[q]);
+        } else if (cfg.precond == AEO_PC_JACOBI) {
+            for (int q = 0; q < n; ++q) zout[q] = rin[q] * h_invd[q];
         } else if (cfg.precond != AEO_PC_VCYCLE) {
             std::memcpy(zout, rin, sizeof(double) * n);
         } else {
@@ -1041,7 +1082,10 @@ aeo_status aeo_mg_create(const aeo_mg_config* c, const double* cx, const double*
         return AEO_ERR_ARGUMENT;
     }
     if (c->precision != AEO_PREC_FP64 && c->precision != AEO_PREC_FP32_MIXED) { g_mg_error = "unknown precision"; return AEO_ERR_ARGUMENT; }
-    if (c->precond != AEO_PC_IDENTITY && c->precond != AEO_PC_VCYCLE) { g_mg_error = "unknown preconditioner"; return AEO_ERR_ARGUMENT; }
+    if (c->precond != AEO_PC_IDENTITY && c->precond != AEO_PC_VCYCLE && c->precond != AEO_PC_JACOBI) {
+        g_mg_error = "unknown preconditioner";
+        return AEO_ERR_ARGUMENT;
+    }
     if (!(c->tol >= 0) || c->maxit < 0 || c->nu1 < 1 || c->nu2 < 0 || c->coarse_sweeps < 0 || c->min_size < 1) {
         g_mg_error = "invalid tol / maxit / sweep counts (nu1 >= 1)";
         return AEO_ERR_ARGUMENT;

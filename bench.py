@@ -511,7 +511,8 @@ def learned_pcg(coeffs, b, args):
     geometries of 10 boxes, seeds 101..120, 10 right-hand sides each), then
     used in flexible CG on the test geometry (seed 1, not seen in training).
     Compared with CG without a preconditioner (the method without the
-    network) and with the multigrid preconditioner."""
+    network), with Jacobi-preconditioned CG (the density-weighted projection's
+    solver) and with the multigrid preconditioner."""
     from aeolus_b200.learned import train_streaming, transfer, urban_geometry
     from aeolus_b200.multigrid import MGPreconditionedCG
     t0 = time.perf_counter()
@@ -525,7 +526,7 @@ def learned_pcg(coeffs, b, args):
                         "loss_last50": float(losses[-50:].mean()), "grid": [128, 128, 48],
                         "step_ms": net.profile("train", 5)},
            "unet_forward_ms": big.profile("forward", 10)}
-    for name, pc in (("learned", "vcycle"), ("plain_cg", "identity"), ("mg", "vcycle")):
+    for name, pc in (("learned", "vcycle"), ("plain_cg", "identity"), ("jacobi_cg", "jacobi"), ("mg", "vcycle")):
         s = MGPreconditionedCG(URBAN_N, (URBAN_H,) * 3, coeffs=coeffs, tol=1e-8, precision="fp32_mixed", maxit=4000,
                                precond=pc)
         if name == "learned":

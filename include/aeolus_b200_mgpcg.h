@@ -38,7 +38,10 @@ enum { AEO_MG_PERIODIC = 0, AEO_MG_NEUMANN = 1 };
 /* preconditioner of the CG iteration: none (plain CG), one multigrid cycle
  * per application (the reference's MGPreconditionedCG), or the learned U-Net
  * of aeolus_b200_unet.h (set by aeo_mg_set_learned; no reference counterpart) */
-enum { AEO_PC_IDENTITY = 0, AEO_PC_VCYCLE = 1, AEO_PC_LEARNED = 2 };
+enum { AEO_PC_IDENTITY = 0, AEO_PC_VCYCLE = 1, AEO_PC_LEARNED = 2, AEO_PC_JACOBI = 3 };
+/* AEO_PC_JACOBI: z = r / diag(A) (the Jacobi-preconditioned CG of the
+ * density-weighted projection, DensityWeightedPoissonSolver,
+ * src/components/urban/pressure_solver.jl:18-20) */
 /* solve status (the reference's :converged, :maxit, :breakdown, :zero_rhs) */
 enum { AEO_MG_CONVERGED = 0, AEO_MG_MAXIT = 1, AEO_MG_BREAKDOWN = 2, AEO_MG_ZERO_RHS = 3 };
 
