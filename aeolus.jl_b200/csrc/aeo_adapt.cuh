@@ -28,15 +28,16 @@ struct CflParams {
     int sgs, buoy, anel;
 };
 
-// Per level: max advective rate, max nut (SGS), sum of theta.
+// Per level: max advective rate, max nut (SGS), sum of theta, max kappa_t
+// (the AMD closure's own; 0 otherwise).
 template <typename R, bool UNI, bool SGS>
 __global__ void __launch_bounds__(256) cfl_levels_kernel(Geo g, const R* __restrict__ u, const R* __restrict__ v,
                                                          const R* __restrict__ w, const R* __restrict__ th, R c_s,
-                                                         double* __restrict__ part) {
-    __shared__ double rmax[256], nmax[256], tsum[256];
+                                                         R bg, R pr_t, double* __restrict__ part) {
+    __shared__ double rmax[256], nmax[256], tsum[256], kmax[256];
     const int k = blockIdx.x;
     const double iz = UNI ? g.idz : lvl(g.idzc, k);
-    double r = 0.0, nm = 0.0, ts = 0.0;
+    double r = 0.0, nm = 0.0, ts = 0.0, km = 0.0;
     bool nanr = false;
     for (int e = threadIdx.x; e < g.nx * g.ny; e += blockDim.x) {
         const int i = e % g.nx, j = e / g.nx;
@@ -49,13 +50,21 @@ __global__ void __launch_bounds__(256) cfl_levels_kernel(Geo g, const R* __restr
         r = fmax(r, rate);
         if (SGS) {
             Nb<R> U{u + q, g.sy, g.sz}, V{v + q, g.sy, g.sz}, W{w + q, g.sy, g.sz};
-            nm = fmax(nm, (double)smag_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, U, V, W));
+            if (g.sgs_model == 3) {
+                Nb<R> T{th + q, g.sy, g.sz};
+                const NuKappa<R> nk = amd_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, bg, pr_t, U, V, W, T);
+                nm = fmax(nm, (double)nk.nu);
+                km = fmax(km, (double)nk.ka);
+            } else {
+                nm = fmax(nm, (double)smag_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, U, V, W));
+            }
         }
         ts += (double)th[q];
     }
     rmax[threadIdx.x] = nanr ? NAN : r;
     nmax[threadIdx.x] = nm;
     tsum[threadIdx.x] = ts;
+    kmax[threadIdx.x] = km;
     __syncthreads();
     for (int s = blockDim.x / 2; s > 0; s >>= 1) {
         if (threadIdx.x < s) {
@@ -63,6 +72,7 @@ __global__ void __launch_bounds__(256) cfl_levels_kernel(Geo g, const R* __restr
             rmax[threadIdx.x] = (isnan(a) || isnan(b)) ? NAN : fmax(a, b);
             nmax[threadIdx.x] = fmax(nmax[threadIdx.x], nmax[threadIdx.x + s]);
             tsum[threadIdx.x] += tsum[threadIdx.x + s];
+            kmax[threadIdx.x] = fmax(kmax[threadIdx.x], kmax[threadIdx.x + s]);
         }
         __syncthreads();
     }
@@ -70,7 +80,7 @@ __global__ void __launch_bounds__(256) cfl_levels_kernel(Geo g, const R* __restr
         part[4 * k + 0] = rmax[0];
         part[4 * k + 1] = nmax[0];
         part[4 * k + 2] = tsum[0] / ((double)g.nx * g.ny);
-        part[4 * k + 3] = 0.0;
+        part[4 * k + 3] = kmax[0];
     }
 }
 
@@ -78,13 +88,14 @@ __global__ void __launch_bounds__(256) cfl_levels_kernel(Geo g, const R* __restr
 __global__ void dt_pick_kernel(Geo g, CflParams c, const double* __restrict__ part, StepScalars* s) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const double INF = 1.0 / 0.0;
-    double rate = 0.0, nutm = 0.0, n2max = 0.0, prev = 0.0;
+    double rate = 0.0, nutm = 0.0, ktm = 0.0, n2max = 0.0, prev = 0.0;
     bool nanr = false;
     for (int k = 0; k < g.nz; ++k) {
         double r = part[4 * k];
         nanr = nanr || isnan(r);
         rate = fmax(rate, r);
         nutm = fmax(nutm, part[4 * k + 1]);
+        ktm = fmax(ktm, part[4 * k + 3]);
         double mean = part[4 * k + 2] + c.th_off;
         if (k > 0 && c.buoy) {
             double dzf = g.uniform ? g.dz : 1.0 / lvl(g.idzf, k);
@@ -100,7 +111,8 @@ __global__ void dt_pick_kernel(Geo g, CflParams c, const double* __restrict__ pa
     double harm = 1.0 / (dx2 + dy2 + dz2);
     double nu_total = c.nu + nutm;
     double dt_diff = nu_total > 0 ? c.c_diff * harm / nu_total : INF;
-    double kt = c.sgs ? nutm / c.pr_t : 0.0;
+    // kappa_t: nut / Pr_t, or the AMD closure's own (max(nu_t, kappa_t) binds, src/TimeIntegration.jl:322-335)
+    double kt = c.sgs ? (g.sgs_model == 3 ? ktm : nutm / c.pr_t) : 0.0;
     double ksgs = fmax(nutm, kt);
     double dt_sgs = ksgs > 0 ? c.c_diff * harm / ksgs : INF;
     double N = sqrt(fmax(n2max, 0.0));

@@ -41,6 +41,8 @@ struct SweepArgs {
     R nu, gacc, theta0, fcor, inv_prt, pr_t, flux_bot, flux_top, sp_alpha, sp_zstart, sp_inv;
     R bref;         // theta0 in stored units (theta is held as theta - offset)
     R c_s;
+    R sgs_bg;       // g / theta0 of the AMD closure's buoyancy term (0: none)
+    int kofs;       // the AMD closure: its kappa_t sits kofs elements past nut_t (0: kappa_t = nut_t / Pr_t)
 };
 
 // padded-array accessor around the thread's point
@@ -51,6 +53,7 @@ struct Nb {
     __device__ __forceinline__ R operator()(int di, int dj, int dk) const {
         return __ldg(p + di + (long long)dj * sy + (long long)dk * sz);
     }
+    __device__ __forceinline__ Nb shifted(int o) const { return Nb{p + o, sy, sz}; }
 };
 
 // ---- WENO reconstructions (src/AdvectionSchemes.jl:105-120, :240-255, :319-333)
@@ -170,8 +173,8 @@ __device__ __forceinline__ R weno_zflux(int f, const AW& W, const AF& F) {
 // tiled form (shared-memory planes).  VT is the value type: R, or a pair of
 // FP32 lanes (F2) for two x-adjacent cells of the paired sweep (the
 // centred forms only).
-template <typename R, int ADV, bool SGS, bool ANEL, bool UNI, bool EXT = false, class AU, class AV, class AW,
-          class AT, class AN, typename VT>
+template <typename R, int ADV, bool SGS, bool ANEL, bool UNI, bool EXT = false, bool AMD = false, class AU, class AV,
+          class AW, class AT, class AN, typename VT>
 __device__ __forceinline__ void sweep_point(const Met<R, UNI>& m, const SweepArgs<R>& a, const Geo& g, int k,
                                             const AU& U, const AV& V, const AW& W, const AT& T, const AN& N, VT& tu,
                                             VT& tv, VT& tw, VT& tt, ZCarry<VT>* zc = nullptr) {
@@ -382,9 +385,11 @@ __device__ __forceinline__ void sweep_point(const Met<R, UNI>& m, const SweepArg
             tw += (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
         }
         if (!ANEL) {
-            VT nE = h * (N(0, 0, 0) + N(1, 0, 0)), nW = h * (N(-1, 0, 0) + N(0, 0, 0));
-            VT nN = h * (N(0, 0, 0) + N(0, 1, 0)), nS = h * (N(0, -1, 0) + N(0, 0, 0));
-            VT nT = h * (N(0, 0, 0) + N(0, 0, 1)), nB = h * (N(0, 0, -1) + N(0, 0, 0));
+            // K = nut (scaled by 1/Pr_t), or the AMD closure's own kappa_t (inv_prt = 1)
+            const AN K = AMD ? N.shifted(a.kofs) : N;
+            VT nE = h * (K(0, 0, 0) + K(1, 0, 0)), nW = h * (K(-1, 0, 0) + K(0, 0, 0));
+            VT nN = h * (K(0, 0, 0) + K(0, 1, 0)), nS = h * (K(0, -1, 0) + K(0, 0, 0));
+            VT nT = h * (K(0, 0, 0) + K(0, 0, 1)), nB = h * (K(0, 0, -1) + K(0, 0, 0));
             VT fxE = nE * (T(1, 0, 0) - T(0, 0, 0)) * idx, fxW = nW * (T(0, 0, 0) - T(-1, 0, 0)) * idx;
             VT fyN = nN * (T(0, 1, 0) - T(0, 0, 0)) * idy, fyS = nS * (T(0, 0, 0) - T(0, -1, 0)) * idy;
             VT fzT = nT * (T(0, 0, 1) - T(0, 0, 0)) * m.idzf(k + 1), fzB = nB * (T(0, 0, 0) - T(0, 0, -1)) * m.idzf(k);
@@ -596,15 +601,82 @@ __device__ __forceinline__ auto smag_point(const Met<R, UNI>& m, const Geo& g, i
     return VT(coef * sqrt(S2));
 }
 
+// The anisotropic minimum-dissipation closure at one point (_amd_point,
+// _amd_scalar_point and _amd_body!, src/operators/sgs_amd_vreman.jl:54-90,
+// :204-212; Rozema et al. 2015, Abkar & Moin 2017), from g_ab = du_a/dx_b, the
+// centred theta gradient t, the squared spacings d2, bg = g / theta0 and the
+// Poincare constant C:
+//   nu_t = C max(0, -(d_k du_i)(d_k du_j) S_ij + bg (d_k dw)(d_k dtheta) min(1, 1/Ri)) / du:du,
+//   kappa_t = C max(0, -(d_k du_i)(d_k dtheta) dtheta_i) / |grad theta|^2,
+// with (d_k da)(d_k db) = sum_k d2_k da_k db_k, Ri = |bg| |grad theta| / du:du,
+// nu_t = 0 where du:du = 0 and kappa_t = nu_t / Pr_t where grad theta = 0.
+template <class T>
+struct NuKappa {
+    T nu, ka;
+};
+
+template <typename R>
+__device__ __noinline__ NuKappa<R> amd_lane(R ux, R uy, R uz, R vx, R vy, R vz, R wx, R wy, R wz, R tx, R ty, R tz,
+                                            R d2x, R d2y, R d2z, R bg, R C, R pr_t) {
+    auto sdot = [&](R a1, R a2, R a3, R b1, R b2, R b3) { return d2x * a1 * b1 + d2y * a2 * b2 + d2z * a3 * b3; };
+    const R S12 = R(0.5) * (uy + vx), S13 = R(0.5) * (uz + wx), S23 = R(0.5) * (vz + wy);
+    const R P = sdot(ux, uy, uz, ux, uy, uz) * ux + sdot(vx, vy, vz, vx, vy, vz) * vy +
+                sdot(wx, wy, wz, wx, wy, wz) * wz +
+                R(2) * (sdot(ux, uy, uz, vx, vy, vz) * S12 + sdot(ux, uy, uz, wx, wy, wz) * S13 +
+                        sdot(vx, vy, vz, wx, wy, wz) * S23);
+    const R B = bg * sdot(wx, wy, wz, tx, ty, tz);
+    const R D = ux * ux + uy * uy + uz * uz + vx * vx + vy * vy + vz * vz + wx * wx + wy * wy + wz * wz;
+    const R kd = tx * tx + ty * ty + tz * tz;
+    const R N2 = fabs(bg) * sqrt(kd);
+    const R Bw = D >= N2 ? B : B * (D / N2);
+    const R Q = sdot(ux, uy, uz, tx, ty, tz) * tx + sdot(vx, vy, vz, tx, ty, tz) * ty + sdot(wx, wy, wz, tx, ty, tz) * tz;
+    const R nn = -P + Bw;
+    NuKappa<R> o;
+    o.nu = D > R(0) ? C * fmax(R(0), nn) / D : R(0);
+    o.ka = kd > R(0) ? C * fmax(R(0), -Q) / kd : o.nu / pr_t;
+    return o;
+}
+
+// the velocity gradient of smag_point and the theta gradient (centred over two
+// cells, _scalar_gradient_at, src/operators/sgs_amd_vreman.jl:18-25) around
+// the point at level k; uniform grids
+template <typename R, bool UNI, class AU, class AV, class AW, class AT>
+__device__ __forceinline__ auto amd_point(const Met<R, UNI>& m, const Geo& g, int k, R C, R bg, R pr_t, const AU& U,
+                                          const AV& V, const AW& W, const AT& T) {
+    using VT = decltype(U(0, 0, 0));
+    const R idx = R(g.idx), idy = R(g.idy), idz = m.idz(k), ido = m.idz_off(k);
+    VT du_dx = (U(1, 0, 0) - U(0, 0, 0)) * idx;
+    VT dv_dy = (V(0, 1, 0) - V(0, 0, 0)) * idy;
+    VT dw_dz = (W(0, 0, 1) - W(0, 0, 0)) * idz;
+    VT du_dy = ((U(0, 1, 0) + U(1, 1, 0)) - (U(0, -1, 0) + U(1, -1, 0))) * (R(0.25) * idy);
+    VT dv_dx = ((V(1, 0, 0) + V(1, 1, 0)) - (V(-1, 0, 0) + V(-1, 1, 0))) * (R(0.25) * idx);
+    VT du_dz = ((U(0, 0, 1) + U(1, 0, 1)) - (U(0, 0, -1) + U(1, 0, -1))) * (R(0.25) * ido);
+    VT dw_dx = ((W(1, 0, 0) + W(1, 0, 1)) - (W(-1, 0, 0) + W(-1, 0, 1))) * (R(0.25) * idx);
+    VT dv_dz = ((V(0, 0, 1) + V(0, 1, 1)) - (V(0, 0, -1) + V(0, 1, -1))) * (R(0.25) * ido);
+    VT dw_dy = ((W(0, 1, 0) + W(0, 1, 1)) - (W(0, -1, 0) + W(0, -1, 1))) * (R(0.25) * idy);
+    VT tx = (T(1, 0, 0) - T(-1, 0, 0)) * (R(0.5) * idx);
+    VT ty = (T(0, 1, 0) - T(0, -1, 0)) * (R(0.5) * idy);
+    VT tz = (T(0, 0, 1) - T(0, 0, -1)) * (R(0.5) * idz);
+    return amd_lane(VT(du_dx), VT(du_dy), VT(du_dz), VT(dv_dx), VT(dv_dy), VT(dv_dz), VT(dw_dx), VT(dw_dy), VT(dw_dz),
+                    VT(tx), VT(ty), VT(tz), VT(R(g.dx * g.dx)), VT(R(g.dy * g.dy)), VT(R(g.dz * g.dz)), VT(bg), VT(C),
+                    VT(pr_t));
+}
+
 // The direct form: nut into a padded array (halos filled by a separate launch).
 template <typename R, bool UNI>
 __global__ void __launch_bounds__(256) smagorinsky_kernel(Geo g, const R* __restrict__ u, const R* __restrict__ v,
-                                                          const R* __restrict__ w, R* __restrict__ nut, R c_s) {
+                                                          const R* __restrict__ w, const R* __restrict__ th,
+                                                          R* __restrict__ nut, R c_s, R bg, R pr_t) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int j = blockIdx.y * blockDim.y + threadIdx.y;
     int k = blockIdx.z * blockDim.z + threadIdx.z;
     if (i >= g.nx || j >= g.ny || k >= g.nz) return;
     const long long q = pidx(g, i, j, k);
     Nb<R> U{u + q, g.sy, g.sz}, V{v + q, g.sy, g.sz}, W{w + q, g.sy, g.sz};
-    nut[q] = smag_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, U, V, W);
+    if (g.sgs_model == 3) {
+        Nb<R> T{th + q, g.sy, g.sz};
+        nut[q] = amd_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, bg, pr_t, U, V, W, T).nu;
+    } else {
+        nut[q] = smag_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, U, V, W);
+    }
 }

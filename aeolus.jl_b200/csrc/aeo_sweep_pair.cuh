@@ -17,6 +17,19 @@
 
 #include "aeo_sweep_tile.cuh"
 
+// the AMD closure lane by lane
+__device__ __forceinline__ NuKappa<F2> amd_lane(F2 ux, F2 uy, F2 uz, F2 vx, F2 vy, F2 vz, F2 wx, F2 wy, F2 wz, F2 tx,
+                                                F2 ty, F2 tz, F2 d2x, F2 d2y, F2 d2z, F2 bg, F2 C, F2 pr_t) {
+    const NuKappa<float> a = amd_lane<float>(ux.v.x, uy.v.x, uz.v.x, vx.v.x, vy.v.x, vz.v.x, wx.v.x, wy.v.x, wz.v.x,
+                                             tx.v.x, ty.v.x, tz.v.x, d2x.v.x, d2y.v.x, d2z.v.x, bg.v.x, C.v.x, pr_t.v.x);
+    const NuKappa<float> b = amd_lane<float>(ux.v.y, uy.v.y, uz.v.y, vx.v.y, vy.v.y, vz.v.y, wx.v.y, wy.v.y, wz.v.y,
+                                             tx.v.y, ty.v.y, tz.v.y, d2x.v.y, d2y.v.y, d2z.v.y, bg.v.y, C.v.y, pr_t.v.y);
+    NuKappa<F2> o;
+    o.nu = F2(a.nu, b.nu);
+    o.ka = F2(a.ka, b.ka);
+    return o;
+}
+
 // the sigma-model operator lane by lane (the closed-form eigenproblem has no
 // paired form)
 __device__ __forceinline__ F2 sigma_operator(F2 g11, F2 g12, F2 g13, F2 g21, F2 g22, F2 g23, F2 g31, F2 g32, F2 g33) {
@@ -42,6 +55,10 @@ struct PairShape {
     static constexpr size_t BAR_BYTES = 128;
     static constexpr int KCH = 32, NLT = KCH + 2 * AEO_LH;
     static constexpr size_t SMEM = PLANES_BYTES + NUT_BYTES + BAR_BYTES + (size_t)LV_N * NLT * sizeof(float) + 128;
+    // the AMD closure's kappa_t planes (the nut planes' layout) after the rest
+    static constexpr size_t KT_BYTE = ((SMEM - 128 + 127) / 128) * 128;
+    static constexpr int KT_OFS = (int)((KT_BYTE - PLANES_BYTES) / sizeof(float));   // elements past nutp
+    static constexpr size_t SMEM_AMD = KT_BYTE + NUT_BYTES + 128;
     static_assert(NS * 8 <= (int)BAR_BYTES, "mbarrier block");
     static_assert(TXT == 32 && NPAIR == TXT + 2, "the eddy-viscosity loop maps warps to 32-pair rows");
     static_assert(PW % 2 == 0 && PSZA % 2 == 0 && NPW % 2 == 0, "pairs stay 8-byte aligned");
@@ -74,9 +91,10 @@ struct PairNut {
         const float2 lo = ld2(dk, o - 1), hi = ld2(dk, o + 1);
         return F2(lo.y, hi.x);
     }
+    __device__ __forceinline__ PairNut shifted(int o) const { return PairNut{{p[0] + o, p[1] + o, p[2] + o}}; }
 };
 
-template <bool SGS, bool ANEL, bool UNI>
+template <bool SGS, bool ANEL, bool UNI, bool AMD = false>
 __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(const __grid_constant__ TileMaps maps, SweepArgs<float> a,
                                                             int kchunk, int* err) {
     using S = PairShape<SGS>;
@@ -178,8 +196,15 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(const __grid_constan
                     const PairAcc<1, S::PW, 0> Uq{q};
                     const PairAcc<1, S::PW, S::PSZA> Vq{q};
                     const PairAcc<1, S::PW, 2 * S::PSZA> Wq{q};
-                    const F2 nv = smag_point<R, UNI>(m, g, L, R(a.c_s), Uq, Vq, Wq);
-                    *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nv.v;
+                    if constexpr (AMD) {
+                        const PairAcc<1, S::PW, 3 * S::PSZA> Tq{q};
+                        const NuKappa<F2> nk = amd_point<R, UNI>(m, g, L, R(a.c_s), a.sgs_bg, a.pr_t, Uq, Vq, Wq, Tq);
+                        *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nk.nu.v;
+                        *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc + S::KT_OFS) = nk.ka.v;
+                    } else {
+                        const F2 nv = smag_point<R, UNI>(m, g, L, R(a.c_s), Uq, Vq, Wq);
+                        *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nv.v;
+                    }
                 }
             }
             __syncthreads();
@@ -190,6 +215,8 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(const __grid_constan
                     float* dst = nutp + (size_t)((L + 3) % 3) * S::NPS;
                     const float* src = nutp + (size_t)((Ls + 3) % 3) * S::NPS;
                     for (int e = tid; e < S::NPS; e += S::NT) dst[e] = src[e];
+                    if (AMD)
+                        for (int e = tid; e < S::NPS; e += S::NT) dst[e + S::KT_OFS] = src[e + S::KT_OFS];
                 }
                 __syncthreads();
             }
@@ -203,7 +230,7 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(const __grid_constan
 
         if (active) {
             F2 tu, tv, tw, tt;
-            sweep_point<R, 0, SGS, ANEL, UNI>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt);
+            sweep_point<R, 0, SGS, ANEL, UNI, false, AMD>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt);
             const long long qi = iidx(g, i, j, k), q = pidx(g, i, j, k);
             const F2 fdt(dt);
             *reinterpret_cast<float2*>(a.us + qi) = (U(0, 0, 0) + fdt * tu).v;

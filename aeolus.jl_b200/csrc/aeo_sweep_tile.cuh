@@ -87,6 +87,10 @@ struct TileShape {
     static constexpr int KCH = 32, NLT = KCH + 2 * AEO_LH;
     static constexpr size_t SMEM =
         PLANES_BYTES + NUT_BYTES + FLUX_BYTES + BAR_BYTES + (size_t)LV_N * NLT * sizeof(R) + 128;
+    // the AMD closure's kappa_t planes (the nut planes' layout) after the rest
+    static constexpr size_t KT_BYTE = ((SMEM - 128 + 127) / 128) * 128;
+    static constexpr int KT_OFS = (int)((KT_BYTE - PLANES_BYTES) / sizeof(R));   // elements past nutp
+    static constexpr size_t SMEM_AMD = KT_BYTE + NUT_BYTES + 128;
     static_assert(!ADV || (FPF % 32 == 0 && FXN <= FPF / 2 && FYN == FPF / 2 && (4 * FPF) % NT == 0),
                   "one field per warp in the face phase");
 };
@@ -116,9 +120,12 @@ template <typename R, int NPW>
 struct NutAcc {
     const R* p[3];  // levels k-1, k, k+1 at the thread's point
     __device__ __forceinline__ R operator()(int di, int dj, int dk) const { return p[dk + 1][dj * NPW + di]; }
+    __device__ __forceinline__ NutAcc shifted(int o) const { return NutAcc{{p[0] + o, p[1] + o, p[2] + o}}; }
 };
 
-template <typename R, int ADV, bool SGS, bool ANEL, bool UNI>
+// AMD: the anisotropic minimum-dissipation closure (its kappa_t planes KT_OFS
+// elements past the nut planes)
+template <typename R, int ADV, bool SGS, bool ANEL, bool UNI, bool AMD = false>
 __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__ TileMaps maps, SweepArgs<R> a,
                                                          int kchunk, int* err) {
     using S = TileShape<R, ADV, SGS>;
@@ -231,7 +238,14 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
                     const SmAcc<R, 1, S::PW, 0> Uq{q};
                     const SmAcc<R, 1, S::PW, S::PSZA> Vq{q};
                     const SmAcc<R, 1, S::PW, 2 * S::PSZA> Wq{q};
-                    np[cj * S::NPW + ci] = smag_point<R, UNI>(m, g, L, R(a.c_s), Uq, Vq, Wq);
+                    if constexpr (AMD) {
+                        const SmAcc<R, 1, S::PW, 3 * S::PSZA> Tq{q};
+                        const NuKappa<R> nk = amd_point<R, UNI>(m, g, L, R(a.c_s), a.sgs_bg, a.pr_t, Uq, Vq, Wq, Tq);
+                        np[cj * S::NPW + ci] = nk.nu;
+                        np[cj * S::NPW + ci + S::KT_OFS] = nk.ka;
+                    } else {
+                        np[cj * S::NPW + ci] = smag_point<R, UNI>(m, g, L, R(a.c_s), Uq, Vq, Wq);
+                    }
                 }
             }
             __syncthreads();
@@ -243,6 +257,8 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
                     R* dst = nutp + (size_t)((L + 3) % 3) * S::NPS;
                     const R* src = nutp + (size_t)((Ls + 3) % 3) * S::NPS;
                     for (int e = tid; e < S::NPS; e += S::NT) dst[e] = src[e];
+                    if (AMD)
+                        for (int e = tid; e < S::NPS; e += S::NT) dst[e + S::KT_OFS] = src[e + S::KT_OFS];
                 }
                 __syncthreads();
             }
@@ -309,8 +325,8 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
             }
         }
         if (active) {
-            sweep_point<R, ADV, SGS, ANEL, UNI, S::SHARE>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt,
-                                                          (ADV > 0 && !S::SHARE) ? &zc : nullptr);
+            sweep_point<R, ADV, SGS, ANEL, UNI, S::SHARE, AMD>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt,
+                                                               (ADV > 0 && !S::SHARE) ? &zc : nullptr);
             if (ADV > 0 && !S::SHARE) zc.valid = true;
             const long long qi = iidx(g, i, j, k), q = pidx(g, i, j, k);
             a.us[qi] = U(0, 0, 0) + dt * tu;

@@ -157,6 +157,9 @@ struct Core : CoreBase {
     CflParams cflp{};
     bool cflp_set = false;
     bool uni = true, sgs = false, anel = false;
+    bool amd() const { return sgs && cfg.sgs_model == AEO_SGS_AMD; }
+    // g / theta0 of the AMD closure's buoyancy term (0 without buoyancy)
+    R amd_bg() const { return R(amd() && cfg.theta0 != 0.0 ? cfg.g / cfg.theta0 : 0.0); }
     // per-kernel-class timing of one un-graphed step (aeo_profile_step)
     bool profiling = false;
     std::vector<std::pair<int, cudaEvent_t>> marks;
@@ -601,18 +604,40 @@ struct Core : CoreBase {
         if constexpr (ADV == 0 && sizeof(R) == sizeof(float)) {
             if (pair) {
                 using PS = PairShape<SG>;
+                dim3 grid((g.nx + PS::TX - 1) / PS::TX, (g.ny + PS::TY - 1) / PS::TY, (g.nz + kchunk - 1) / kchunk);
+                if constexpr (SG && !AN && UN) {
+                    if (amd()) {
+                        SweepArgs<R> b = a;
+                        b.kofs = PS::KT_OFS;
+                        cudaFuncSetAttribute(sweep_pair_kernel<SG, AN, UN, true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PS::SMEM_AMD);
+                        sweep_pair_kernel<SG, AN, UN, true><<<grid, dim3(PS::TXT, PS::TY), PS::SMEM_AMD, st>>>(
+                            tmaps[s_in], b, kchunk, d_flag);
+                        return;
+                    }
+                }
                 cudaFuncSetAttribute(sweep_pair_kernel<SG, AN, UN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)PS::SMEM);
-                dim3 grid((g.nx + PS::TX - 1) / PS::TX, (g.ny + PS::TY - 1) / PS::TY, (g.nz + kchunk - 1) / kchunk);
                 sweep_pair_kernel<SG, AN, UN><<<grid, dim3(PS::TXT, PS::TY), PS::SMEM, st>>>(tmaps[s_in], a, kchunk,
                                                                                            d_flag);
                 return;
             }
         }
         using TS = TileShape<R, ADV, SG>;
+        dim3 grid((g.nx + TS::TX - 1) / TS::TX, (g.ny + TS::TY - 1) / TS::TY, (g.nz + kchunk - 1) / kchunk);
+        if constexpr (SG && !AN && UN) {
+            if (amd()) {
+                SweepArgs<R> b = a;
+                b.kofs = TS::KT_OFS;
+                cudaFuncSetAttribute(sweep_tile_kernel<R, ADV, SG, AN, UN, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS::SMEM_AMD);
+                sweep_tile_kernel<R, ADV, SG, AN, UN, true><<<grid, dim3(TS::TX, TS::TY), TS::SMEM_AMD, st>>>(
+                    tmaps[s_in], b, kchunk, d_flag);
+                return;
+            }
+        }
         const size_t sm = TS::SMEM;
         cudaFuncSetAttribute(sweep_tile_kernel<R, ADV, SG, AN, UN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        dim3 grid((g.nx + TS::TX - 1) / TS::TX, (g.ny + TS::TY - 1) / TS::TY, (g.nz + kchunk - 1) / kchunk);
         sweep_tile_kernel<R, ADV, SG, AN, UN><<<grid, dim3(TS::TX, TS::TY), sm, st>>>(tmaps[s_in], a, kchunk, d_flag);
     }
 
@@ -732,7 +757,11 @@ struct Core : CoreBase {
         a.ca = ca; a.cb = cb; a.stage = stage;
         a.nu = R(cfg.nu); a.gacc = R(cfg.g); a.theta0 = R(cfg.theta0); a.fcor = R(cfg.f_coriolis);
         a.bref = R(cfg.theta0 - th_off);
-        a.pr_t = R(cfg.pr_t); a.inv_prt = R(1.0 / cfg.pr_t);
+        a.pr_t = R(cfg.pr_t);
+        // the AMD closure brings its own kappa_t (the flux takes it unscaled)
+        // and a buoyancy term with g / theta0
+        a.inv_prt = amd() ? R(1) : R(1.0 / cfg.pr_t);
+        a.sgs_bg = amd_bg();
         a.flux_bot = R(cfg.flux_bot); a.flux_top = R(cfg.flux_top);
         a.sp_alpha = R(cfg.sponge_alpha); a.sp_zstart = R(cfg.sponge_zstart);
         a.c_s = R(cfg.c_s);
@@ -758,11 +787,11 @@ struct Core : CoreBase {
     aeo_status enqueue_pick(int s_state) {
         R** in = P[s_state];
         if (uni) {
-            if (sgs) cfl_levels_kernel<R, true, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), d_part);
-            else cfl_levels_kernel<R, true, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), d_part);
+            if (sgs) cfl_levels_kernel<R, true, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_part);
+            else cfl_levels_kernel<R, true, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_part);
         } else {
-            if (sgs) cfl_levels_kernel<R, false, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), d_part);
-            else cfl_levels_kernel<R, false, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), d_part);
+            if (sgs) cfl_levels_kernel<R, false, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_part);
+            else cfl_levels_kernel<R, false, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_part);
         }
         CKL();
         dt_pick_kernel<<<1, 32, 0, st>>>(g, cflp, d_part, d_sc);
@@ -1055,8 +1084,8 @@ struct Core : CoreBase {
         if (!d) { fail("get_field: unknown or unavailable field"); return AEO_ERR_ARGUMENT; }
         if (id == AEO_FIELD_NUT) {
             // the step keeps nut in shared memory: evaluate it for the current state
-            if (uni) smagorinsky_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], nut, R(cfg.c_s));
-            else smagorinsky_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], nut, R(cfg.c_s));
+            if (uni) smagorinsky_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], P[cur][3], nut, R(cfg.c_s), amd_bg(), R(cfg.pr_t));
+            else smagorinsky_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], P[cur][3], nut, R(cfg.c_s), amd_bg(), R(cfg.pr_t));
             CKL();
         }
         S* stage = reinterpret_cast<S*>(d_stage);
@@ -1327,13 +1356,18 @@ static aeo_status validate(const aeo_config* c, const double* zf, const double* 
     if (c->stretched && (!zf || c->bc_z != AEO_BC_WALL)) { *m = "a stretched grid needs zf and walls in z"; return AEO_ERR_ARGUMENT; }
     if (c->precision != AEO_PREC_FP64 && c->precision != AEO_PREC_FP32_MIXED) { *m = "unknown precision"; return AEO_ERR_ARGUMENT; }
     if (c->c_s != 0.0 && !(c->pr_t > 0.0)) { *m = "pr_t must be positive with SGS"; return AEO_ERR_ARGUMENT; }
-    if (c->sgs_model != AEO_SGS_SMAGORINSKY && c->sgs_model != AEO_SGS_VREMAN && c->sgs_model != AEO_SGS_SIGMA) {
+    if (c->sgs_model != AEO_SGS_SMAGORINSKY && c->sgs_model != AEO_SGS_VREMAN && c->sgs_model != AEO_SGS_SIGMA &&
+        c->sgs_model != AEO_SGS_AMD) {
         *m = "unknown SGS closure";
         return AEO_ERR_ARGUMENT;
     }
     if (c->sgs_model != AEO_SGS_SMAGORINSKY && c->stretched) {
-        *m = "the Vreman and sigma closures take a uniform grid (src/operators/sgs_amd_vreman.jl:280-284, "
-             "src/operators/sigma_closure.jl:208-212)";
+        *m = "the Vreman, sigma and AMD closures take a uniform grid (src/operators/sgs_amd_vreman.jl:102-107, "
+             ":280-284, src/operators/sigma_closure.jl:208-212)";
+        return AEO_ERR_ARGUMENT;
+    }
+    if (c->sgs_model == AEO_SGS_AMD && c->c_s != 0.0 && c->core != AEO_CORE_BOUSSINESQ) {
+        *m = "the AMD closure is built for the Boussinesq core";
         return AEO_ERR_ARGUMENT;
     }
     return AEO_OK;

@@ -645,6 +645,47 @@ static double sigma_op(double g11, double g12, double g13, double g21, double g2
     return D > 0 ? D : 0.0;
 }
 
+/* --- AMD: anisotropic minimum dissipation (_amd_point, _amd_scalar_point,
+ * _amd_body!, src/operators/sgs_amd_vreman.jl:54-90, :204-212), from the
+ * velocity gradient of smag_at (g_ab = du_a/dx_b) and the centred theta
+ * gradient (_scalar_gradient_at, :18-25); bg = g/theta0 (0 without
+ * buoyancy). nu_t into *nu, theta's own kappa_t into *ka. */
+static void amd_at(const oc_sim* s, int i, int j, int k, double* nu, double* ka) {
+    const double *u = s->u, *v = s->v, *w = s->w, *t = s->th;
+    double idx = s->idx, idy = s->idy, idz = m_idz(s, k), ido = m_idz_off(s, k);
+    double g[3][3];
+    g[0][0] = (A(u, i + 1, j, k) - A(u, i, j, k)) * idx;
+    g[1][1] = (A(v, i, j + 1, k) - A(v, i, j, k)) * idy;
+    g[2][2] = (A(w, i, j, k + 1) - A(w, i, j, k)) * idz;
+    g[0][1] = ((A(u, i, j + 1, k) + A(u, i + 1, j + 1, k)) - (A(u, i, j - 1, k) + A(u, i + 1, j - 1, k))) * (0.25 * idy);
+    g[1][0] = ((A(v, i + 1, j, k) + A(v, i + 1, j + 1, k)) - (A(v, i - 1, j, k) + A(v, i - 1, j + 1, k))) * (0.25 * idx);
+    g[0][2] = ((A(u, i, j, k + 1) + A(u, i + 1, j, k + 1)) - (A(u, i, j, k - 1) + A(u, i + 1, j, k - 1))) * (0.25 * ido);
+    g[2][0] = ((A(w, i + 1, j, k) + A(w, i + 1, j, k + 1)) - (A(w, i - 1, j, k) + A(w, i - 1, j, k + 1))) * (0.25 * idx);
+    g[1][2] = ((A(v, i, j, k + 1) + A(v, i, j + 1, k + 1)) - (A(v, i, j, k - 1) + A(v, i, j + 1, k - 1))) * (0.25 * ido);
+    g[2][1] = ((A(w, i, j + 1, k) + A(w, i, j + 1, k + 1)) - (A(w, i, j - 1, k) + A(w, i, j - 1, k + 1))) * (0.25 * idy);
+    double gt[3] = {(A(t, i + 1, j, k) - A(t, i - 1, j, k)) * (0.5 * idx),
+                    (A(t, i, j + 1, k) - A(t, i, j - 1, k)) * (0.5 * idy),
+                    (A(t, i, j, k + 1) - A(t, i, j, k - 1)) * (0.5 * idz)};
+    double d2[3] = {s->dx * s->dx, s->dy * s->dy, s->dz * s->dz};
+    double bg = s->p.theta0 != 0 ? s->p.g / s->p.theta0 : 0.0;
+#define SDOT(a, b) (d2[0] * (a)[0] * (b)[0] + d2[1] * (a)[1] * (b)[1] + d2[2] * (a)[2] * (b)[2])
+    double S12 = 0.5 * (g[0][1] + g[1][0]), S13 = 0.5 * (g[0][2] + g[2][0]), S23 = 0.5 * (g[1][2] + g[2][1]);
+    double P = SDOT(g[0], g[0]) * g[0][0] + SDOT(g[1], g[1]) * g[1][1] + SDOT(g[2], g[2]) * g[2][2] +
+               2 * (SDOT(g[0], g[1]) * S12 + SDOT(g[0], g[2]) * S13 + SDOT(g[1], g[2]) * S23);
+    double B = bg * SDOT(g[2], gt);
+    double D = 0;
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) D += g[a][b] * g[a][b];
+    double kd = gt[0] * gt[0] + gt[1] * gt[1] + gt[2] * gt[2];
+    double N2 = fabs(bg) * sqrt(kd);
+    double Bw = D >= N2 ? B : B * (D / N2);           /* B min(1, 1/Ri) */
+    double Q = SDOT(g[0], gt) * gt[0] + SDOT(g[1], gt) * gt[1] + SDOT(g[2], gt) * gt[2];
+#undef SDOT
+    double C = s->p.c_s, nn = -P + Bw;
+    *nu = D > 0 ? C * fmax(0.0, nn) / D : 0.0;
+    *ka = kd > 0 ? C * fmax(0.0, -Q) / kd : *nu / s->p.pr_t;
+}
+
 /* --- Smagorinsky (src/FiniteVolume.jl:936-944, src/Operators.jl:451-496) -- */
 static inline double smag_at(const oc_sim* s, int i, int j, int k) {
     const double *u = s->u, *v = s->v, *w = s->w;
@@ -659,6 +700,11 @@ static inline double smag_at(const oc_sim* s, int i, int j, int k) {
     double dw_dx = ((A(w, i + 1, j, k) + A(w, i + 1, j, k + 1)) - (A(w, i - 1, j, k) + A(w, i - 1, j, k + 1))) * (0.25 * idx);
     double dv_dz = ((A(v, i, j, k + 1) + A(v, i, j + 1, k + 1)) - (A(v, i, j, k - 1) + A(v, i, j + 1, k - 1))) * (0.25 * ido);
     double dw_dy = ((A(w, i, j + 1, k) + A(w, i, j + 1, k + 1)) - (A(w, i, j - 1, k) + A(w, i, j - 1, k + 1))) * (0.25 * idy);
+    if (s->p.sgs_model == OC_SGS_AMD) {
+        double nu, ka;
+        amd_at(s, i, j, k, &nu, &ka);
+        return nu;
+    }
     double S11 = du_dx, S22 = dv_dy, S33 = dw_dz;
     double S12 = 0.5 * (du_dy + dv_dx);
     double S13 = 0.5 * (du_dz + dw_dx);
@@ -743,8 +789,11 @@ static inline double eddy_w(const oc_sim* s, int i, int j, int k) {
 static inline double eddy_scalar(const oc_sim* s, const double* d, int i, int j, int k) {
     double idx = s->idx, idy = s->idy;
     if (!s->wc) {
-        const double* H = s->nut;
-        double sc = 1 / s->p.pr_t;
+        /* the AMD closure: its own kappa_t, unscaled (AMDClosure,
+         * src/operators/sgs_amd_vreman.jl:325-354) */
+        const int amd = s->p.sgs_model == OC_SGS_AMD;
+        const double* H = amd ? s->kt : s->nut;
+        double sc = amd ? 1.0 : 1 / s->p.pr_t;
         double nE = 0.5 * (A(H, i, j, k) + A(H, i + 1, j, k));
         double nW = 0.5 * (A(H, i - 1, j, k) + A(H, i, j, k));
         double nN = 0.5 * (A(H, i, j, k) + A(H, i, j + 1, k));
@@ -798,8 +847,12 @@ static void compute_tendencies(oc_sim* s) {
 #pragma omp parallel for collapse(2) schedule(static)
         for (int k = Hz; k < Hz + Nz; ++k)
             for (int j = Hy; j < Hy + Ny; ++j)
-                for (int i = Hx; i < Hx + Nx; ++i) A(s->nut, i, j, k) = smag_at(s, i, j, k);
+                for (int i = Hx; i < Hx + Nx; ++i) {
+                    if (P->sgs_model == OC_SGS_AMD) amd_at(s, i, j, k, &A(s->nut, i, j, k), &A(s->kt, i, j, k));
+                    else A(s->nut, i, j, k) = smag_at(s, i, j, k);
+                }
         fill_halos(s, s->nut, LOC_C);
+        if (P->sgs_model == OC_SGS_AMD) fill_halos(s, s->kt, LOC_C);
         if (anel)
             for (int64_t q = 0; q < s->n; ++q) s->kt[q] = s->nut[q] / P->pr_t;
     }
@@ -1323,7 +1376,7 @@ double oc_adaptive_dt(oc_sim* s, const oc_cfl* c, double dt_prev, int* limiter) 
     fill_halos(s, s->u, LOC_FX);
     fill_halos(s, s->v, LOC_FY);
     fill_halos(s, s->w, LOC_FZ);
-    double rate = 0.0, nutm = 0.0;
+    double rate = 0.0, nutm = 0.0, ktm = 0.0;
     int nanr = 0;
     double* mean = (double*)calloc((size_t)Nz, sizeof(double));
     for (int k = Hz; k < Hz + Nz; ++k) {
@@ -1337,8 +1390,11 @@ double oc_adaptive_dt(oc_sim* s, const oc_cfl* c, double dt_prev, int* limiter) 
                 if (isnan(r)) nanr = 1;
                 else if (r > rate) rate = r;
                 if (P->c_s != 0) {
-                    double n = smag_at(s, i, j, k);
+                    double n, kk = 0.0;
+                    if (P->sgs_model == OC_SGS_AMD) amd_at(s, i, j, k, &n, &kk);
+                    else n = smag_at(s, i, j, k);
                     if (n > nutm) nutm = n;
+                    if (kk > ktm) ktm = kk;
                 }
                 acc += A(s->th, i, j, k);
             }
@@ -1352,7 +1408,8 @@ double oc_adaptive_dt(oc_sim* s, const oc_cfl* c, double dt_prev, int* limiter) 
     double harm = 1.0 / (1 / (s->dx * s->dx) + 1 / (s->dy * s->dy) + 1 / (dzmin * dzmin));
     double nu_total = P->nu + nutm;
     double dt_diff = nu_total > 0 ? c->c_diff * harm / nu_total : INF;
-    double ksgs = fmax(nutm, P->c_s != 0 ? nutm / P->pr_t : 0.0);
+    /* max(nu_t, kappa_t), kappa_t the AMD closure's own (src/TimeIntegration.jl:322-335) */
+    double ksgs = fmax(nutm, P->c_s != 0 ? (P->sgs_model == OC_SGS_AMD ? ktm : nutm / P->pr_t) : 0.0);
     double dt_sgs = ksgs > 0 ? c->c_diff * harm / ksgs : INF;
     int buoy = anel ? (P->g != 0) : (P->theta0 != 0);
     double n2max = 0.0;
@@ -1597,7 +1654,9 @@ oc_sim* oc_create(const oc_params* p, const double* zfi, const double* wc, const
     if (p->solver == OC_SOLVER_COLUMN && p->bc_z != OC_BC_WALL) return NULL;
     if (p->stretched && (!zfi || p->bc_z != OC_BC_WALL)) return NULL;
     if (p->solver == OC_SOLVER_PCG && (p->stretched || p->core != OC_CORE_BOUSSINESQ)) return NULL;
-    if ((p->sgs_model == OC_SGS_VREMAN || p->sgs_model == OC_SGS_SIGMA) && p->stretched) return NULL;
+    if ((p->sgs_model == OC_SGS_VREMAN || p->sgs_model == OC_SGS_SIGMA || p->sgs_model == OC_SGS_AMD) && p->stretched)
+        return NULL;
+    if (p->sgs_model == OC_SGS_AMD && p->c_s != 0 && p->core != OC_CORE_BOUSSINESQ) return NULL;
     oc_sim* s = (oc_sim*)calloc(1, sizeof(oc_sim));
     s->p = *p;
     s->NX = p->nx + 2 * p->hx; s->NY = p->ny + 2 * p->hy; s->NZ = p->nz + 2 * p->hz;
@@ -1800,6 +1859,7 @@ static double* field_ptr(const oc_sim* s, int id) {
         case OC_THETA: return s->th;
         case OC_P: return s->pr;
         case OC_NUT: return s->nut;
+        case OC_KT: return s->kt;
         case OC_PHI: return s->phi;
         default: return NULL;
     }

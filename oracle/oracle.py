@@ -93,7 +93,7 @@ def load():
     return lib
 
 
-FIELD_IDS = {"u": 0, "v": 1, "w": 2, "theta": 3, "p": 4, "nut": 5, "phi": 6}
+FIELD_IDS = {"u": 0, "v": 1, "w": 2, "theta": 3, "p": 4, "nut": 5, "phi": 6, "kt": 7}
 _ADV = {"centred": 0, "weno_js5": 1, "weno_z5": 2}
 _SOLV = {"fft": 0, "column": 1, "pcg": 2}
 _PCG_STATUS = {0: "converged", 1: "maxit", 2: "breakdown", 3: "zero_rhs"}
@@ -144,7 +144,7 @@ class OracleSimulation:
         p.c_s, p.pr_t = spec.c_s, spec.pr_t
         p.flux_bot, p.flux_top = spec.flux_bot, spec.flux_top
         p.sponge_alpha, p.sponge_zstart = spec.sponge_alpha, spec.sponge_zstart
-        p.sgs_model = {"smagorinsky": 0, "vreman": 1, "sigma": 2}[spec.sgs]
+        p.sgs_model = {"smagorinsky": 0, "vreman": 1, "sigma": 2, "amd": 3}[spec.sgs]
         self._keep = [g.zf, spec.wc, spec.wf, spec.thf]
         h = lib.oc_create(C.byref(p), _p(g.zf), _p(spec.wc), _p(spec.wf), _p(spec.thf))
         if not h:
