@@ -16,7 +16,7 @@ from .grids import PERIODIC, WALL, Grid
 
 CORES = {"boussinesq": 0, "anelastic": 1}
 ADVECTION = {"centred": 0, "weno_js5": 1, "weno_z5": 2}
-SGS_MODELS = {"smagorinsky": 0, "vreman": 1, "sigma": 2, "amd": 3}
+SGS_MODELS = {"smagorinsky": 0, "vreman": 1, "sigma": 2, "amd": 3, "dynamic": 4}
 SOLVERS = {"fft": 0, "column": 1, "pcg": 2}
 PRECISIONS = {"fp64": 0, "fp32_mixed": 1}
 FIELDS = {"u": 0, "v": 1, "w": 2, "theta": 3, "p": 4, "nut": 5}
@@ -36,7 +36,8 @@ class CoreSpec:
     c_s: float = 0.0
     sgs: str = "smagorinsky"            # the closure when c_s > 0: smagorinsky, vreman (c = 2.5 c_s^2),
                                         # sigma (c_s is C_sigma, 1.35 in the reference) or amd (c_s is the
-                                        # AMD constant C, 0.3 in the reference; its own kappa_t)
+                                        # AMD constant C, 0.3 in the reference; its own kappa_t) or dynamic
+                                        # (Germano-Lilly, plane-averaged; c_s is the clip cs_max, 0.5)
     pr_t: float = 1.0 / 3.0
     flux_bot: float = 0.0
     flux_top: float = 0.0
@@ -86,9 +87,11 @@ class CoreSpec:
             raise ValueError("pr_t must be positive")
         if self.sgs not in SGS_MODELS:
             raise ValueError(f"sgs must be one of {list(SGS_MODELS)}, got {self.sgs!r}")
-        if self.sgs in ("vreman", "sigma", "amd") and self.grid.stretched:
+        if self.sgs in ("vreman", "sigma", "amd", "dynamic") and self.grid.stretched:
             raise ValueError("the Vreman, sigma and AMD closures take a RegularGrid only (compute_vreman_nut!, "
                              "src/operators/sgs_amd_vreman.jl:280-284; compute_amd_coefficients!, :102-107; "
                              "compute_sigma_nut!, src/operators/sigma_closure.jl:208-212)")
+        if self.sgs == "dynamic" and self.c_s != 0 and min(self.grid.halo) < 2:
+            raise ValueError("the dynamic Smagorinsky closure needs halos of at least 2 (src/Operators.jl:556-557)")
         if self.sgs == "amd" and self.c_s != 0 and self.core != "boussinesq":
             raise ValueError("the AMD closure is built for the Boussinesq core")

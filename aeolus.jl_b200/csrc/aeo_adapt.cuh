@@ -9,6 +9,7 @@
 #pragma once
 
 #include "aeo_sweep.cuh"
+#include "aeo_dynamic.cuh"
 
 // Scalars of the step that live in device memory (read by the stage kernels).
 struct StepScalars {
@@ -33,7 +34,8 @@ struct CflParams {
 template <typename R, bool UNI, bool SGS>
 __global__ void __launch_bounds__(256) cfl_levels_kernel(Geo g, const R* __restrict__ u, const R* __restrict__ v,
                                                          const R* __restrict__ w, const R* __restrict__ th, R c_s,
-                                                         R bg, R pr_t, double* __restrict__ part) {
+                                                         R bg, R pr_t, const double* __restrict__ cs2, double dd2,
+                                                         double* __restrict__ part) {
     __shared__ double rmax[256], nmax[256], tsum[256], kmax[256];
     const int k = blockIdx.x;
     const double iz = UNI ? g.idz : lvl(g.idzc, k);
@@ -50,7 +52,9 @@ __global__ void __launch_bounds__(256) cfl_levels_kernel(Geo g, const R* __restr
         r = fmax(r, rate);
         if (SGS) {
             Nb<R> U{u + q, g.sy, g.sz}, V{v + q, g.sy, g.sz}, W{w + q, g.sy, g.sz};
-            if (g.sgs_model == 3) {
+            if (g.sgs_model == 4) {   // dynamic Smagorinsky: cs2(k) Delta^2 |S|
+                nm = fmax(nm, (double)(R(cs2[k] * dd2) * strain_at<R, UNI>(Met<R, UNI>(g), g, k, U, V, W, (R*)nullptr)));
+            } else if (g.sgs_model == 3) {
                 Nb<R> T{th + q, g.sy, g.sz};
                 const NuKappa<R> nk = amd_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, bg, pr_t, U, V, W, T);
                 nm = fmax(nm, (double)nk.nu);

@@ -42,6 +42,8 @@ struct SweepArgs {
     R bref;         // theta0 in stored units (theta is held as theta - offset)
     R c_s;
     R sgs_bg;       // g / theta0 of the AMD closure's buoyancy term (0: none)
+    const double* cs2;  // the dynamic Smagorinsky coefficient per level
+    double dyn_d2;      // ... and its Delta^2 = (dx dy dz)^(2/3)
     int kofs;       // the AMD closure: its kappa_t sits kofs elements past nut_t (0: kappa_t = nut_t / Pr_t)
 };
 
@@ -662,18 +664,46 @@ __device__ __forceinline__ auto amd_point(const Met<R, UNI>& m, const Geo& g, in
                     VT(pr_t));
 }
 
+// |S| = sqrt(2 S:S) from the velocity-gradient stencil of smag_point
+// (_strain_at, src/Operators.jl:488-496), with the six strain components
+template <typename R, bool UNI, class AU, class AV, class AW>
+__device__ __forceinline__ auto strain_at(const Met<R, UNI>& m, const Geo& g, int k, const AU& U, const AV& V,
+                                          const AW& W, decltype(U(0, 0, 0))* S6) {
+    using VT = decltype(U(0, 0, 0));
+    const R idx = R(g.idx), idy = R(g.idy), idz = m.idz(k), ido = m.idz_off(k);
+    VT du_dx = (U(1, 0, 0) - U(0, 0, 0)) * idx;
+    VT dv_dy = (V(0, 1, 0) - V(0, 0, 0)) * idy;
+    VT dw_dz = (W(0, 0, 1) - W(0, 0, 0)) * idz;
+    VT du_dy = ((U(0, 1, 0) + U(1, 1, 0)) - (U(0, -1, 0) + U(1, -1, 0))) * (R(0.25) * idy);
+    VT dv_dx = ((V(1, 0, 0) + V(1, 1, 0)) - (V(-1, 0, 0) + V(-1, 1, 0))) * (R(0.25) * idx);
+    VT du_dz = ((U(0, 0, 1) + U(1, 0, 1)) - (U(0, 0, -1) + U(1, 0, -1))) * (R(0.25) * ido);
+    VT dw_dx = ((W(1, 0, 0) + W(1, 0, 1)) - (W(-1, 0, 0) + W(-1, 0, 1))) * (R(0.25) * idx);
+    VT dv_dz = ((V(0, 0, 1) + V(0, 1, 1)) - (V(0, 0, -1) + V(0, 1, -1))) * (R(0.25) * ido);
+    VT dw_dy = ((W(0, 1, 0) + W(0, 1, 1)) - (W(0, -1, 0) + W(0, -1, 1))) * (R(0.25) * idy);
+    VT S12 = R(0.5) * (du_dy + dv_dx), S13 = R(0.5) * (du_dz + dw_dx), S23 = R(0.5) * (dv_dz + dw_dy);
+    VT S2 = R(2) * (du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz) + R(4) * (S12 * S12 + S13 * S13 + S23 * S23);
+    if (S6) {
+        S6[0] = du_dx; S6[1] = dv_dy; S6[2] = dw_dz;
+        S6[3] = S12; S6[4] = S13; S6[5] = S23;
+    }
+    return VT(sqrt(S2));
+}
+
 // The direct form: nut into a padded array (halos filled by a separate launch).
 template <typename R, bool UNI>
 __global__ void __launch_bounds__(256) smagorinsky_kernel(Geo g, const R* __restrict__ u, const R* __restrict__ v,
                                                           const R* __restrict__ w, const R* __restrict__ th,
-                                                          R* __restrict__ nut, R c_s, R bg, R pr_t) {
+                                                          R* __restrict__ nut, R c_s, R bg, R pr_t,
+                                                          const double* __restrict__ cs2, double dd2) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int j = blockIdx.y * blockDim.y + threadIdx.y;
     int k = blockIdx.z * blockDim.z + threadIdx.z;
     if (i >= g.nx || j >= g.ny || k >= g.nz) return;
     const long long q = pidx(g, i, j, k);
     Nb<R> U{u + q, g.sy, g.sz}, V{v + q, g.sy, g.sz}, W{w + q, g.sy, g.sz};
-    if (g.sgs_model == 3) {
+    if (g.sgs_model == 4) {
+        nut[q] = R(cs2[k] * dd2) * strain_at<R, UNI>(Met<R, UNI>(g), g, k, U, V, W, (R*)nullptr);
+    } else if (g.sgs_model == 3) {
         Nb<R> T{th + q, g.sy, g.sz};
         nut[q] = amd_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, bg, pr_t, U, V, W, T).nu;
     } else {

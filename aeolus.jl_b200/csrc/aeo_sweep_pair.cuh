@@ -94,7 +94,7 @@ struct PairNut {
     __device__ __forceinline__ PairNut shifted(int o) const { return PairNut{{p[0] + o, p[1] + o, p[2] + o}}; }
 };
 
-template <bool SGS, bool ANEL, bool UNI, bool AMD = false>
+template <bool SGS, bool ANEL, bool UNI, int CLOS = 0>   // CLOS: as in sweep_tile_kernel
 __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(const __grid_constant__ TileMaps maps, SweepArgs<float> a,
                                                             int kchunk, int* err) {
     using S = PairShape<SGS>;
@@ -196,7 +196,11 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(const __grid_constan
                     const PairAcc<1, S::PW, 0> Uq{q};
                     const PairAcc<1, S::PW, S::PSZA> Vq{q};
                     const PairAcc<1, S::PW, 2 * S::PSZA> Wq{q};
-                    if constexpr (AMD) {
+                    if constexpr (CLOS == 2) {
+                        const F2 c = F2(float(dyn_cs2_at(g, a.cs2, L) * a.dyn_d2));
+                        const F2 nv = c * strain_at<R, UNI>(m, g, L, Uq, Vq, Wq, (F2*)nullptr);
+                        *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nv.v;
+                    } else if constexpr (CLOS == 1) {
                         const PairAcc<1, S::PW, 3 * S::PSZA> Tq{q};
                         const NuKappa<F2> nk = amd_point<R, UNI>(m, g, L, R(a.c_s), a.sgs_bg, a.pr_t, Uq, Vq, Wq, Tq);
                         *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nk.nu.v;
@@ -215,7 +219,7 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(const __grid_constan
                     float* dst = nutp + (size_t)((L + 3) % 3) * S::NPS;
                     const float* src = nutp + (size_t)((Ls + 3) % 3) * S::NPS;
                     for (int e = tid; e < S::NPS; e += S::NT) dst[e] = src[e];
-                    if (AMD)
+                    if (CLOS == 1)
                         for (int e = tid; e < S::NPS; e += S::NT) dst[e + S::KT_OFS] = src[e + S::KT_OFS];
                 }
                 __syncthreads();
@@ -230,7 +234,7 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(const __grid_constan
 
         if (active) {
             F2 tu, tv, tw, tt;
-            sweep_point<R, 0, SGS, ANEL, UNI, false, AMD>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt);
+            sweep_point<R, 0, SGS, ANEL, UNI, false, CLOS == 1>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt);
             const long long qi = iidx(g, i, j, k), q = pidx(g, i, j, k);
             const F2 fdt(dt);
             *reinterpret_cast<float2*>(a.us + qi) = (U(0, 0, 0) + fdt * tu).v;

@@ -18,6 +18,7 @@
 #include <cuda.h>
 
 #include "aeo_sweep.cuh"
+#include "aeo_dynamic.cuh"
 
 #define AEO_WAIT_LIMIT (1u << 22)
 #define AEO_ERR_FLAG_TMA 2
@@ -123,9 +124,10 @@ struct NutAcc {
     __device__ __forceinline__ NutAcc shifted(int o) const { return NutAcc{{p[0] + o, p[1] + o, p[2] + o}}; }
 };
 
-// AMD: the anisotropic minimum-dissipation closure (its kappa_t planes KT_OFS
-// elements past the nut planes)
-template <typename R, int ADV, bool SGS, bool ANEL, bool UNI, bool AMD = false>
+// CLOS: the closure of the coefficient pass: 0 the static ones (smag_point),
+// 1 the anisotropic minimum-dissipation closure (its kappa_t planes KT_OFS
+// elements past the nut planes), 2 dynamic Smagorinsky (cs2 per level)
+template <typename R, int ADV, bool SGS, bool ANEL, bool UNI, int CLOS = 0>
 __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__ TileMaps maps, SweepArgs<R> a,
                                                          int kchunk, int* err) {
     using S = TileShape<R, ADV, SGS>;
@@ -238,7 +240,10 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
                     const SmAcc<R, 1, S::PW, 0> Uq{q};
                     const SmAcc<R, 1, S::PW, S::PSZA> Vq{q};
                     const SmAcc<R, 1, S::PW, 2 * S::PSZA> Wq{q};
-                    if constexpr (AMD) {
+                    if constexpr (CLOS == 2) {
+                        const R c = R(dyn_cs2_at(g, a.cs2, L) * a.dyn_d2);
+                        np[cj * S::NPW + ci] = c * strain_at<R, UNI>(m, g, L, Uq, Vq, Wq, (R*)nullptr);
+                    } else if constexpr (CLOS == 1) {
                         const SmAcc<R, 1, S::PW, 3 * S::PSZA> Tq{q};
                         const NuKappa<R> nk = amd_point<R, UNI>(m, g, L, R(a.c_s), a.sgs_bg, a.pr_t, Uq, Vq, Wq, Tq);
                         np[cj * S::NPW + ci] = nk.nu;
@@ -257,7 +262,7 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
                     R* dst = nutp + (size_t)((L + 3) % 3) * S::NPS;
                     const R* src = nutp + (size_t)((Ls + 3) % 3) * S::NPS;
                     for (int e = tid; e < S::NPS; e += S::NT) dst[e] = src[e];
-                    if (AMD)
+                    if (CLOS == 1)
                         for (int e = tid; e < S::NPS; e += S::NT) dst[e + S::KT_OFS] = src[e + S::KT_OFS];
                 }
                 __syncthreads();
@@ -325,7 +330,7 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
             }
         }
         if (active) {
-            sweep_point<R, ADV, SGS, ANEL, UNI, S::SHARE, AMD>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt,
+            sweep_point<R, ADV, SGS, ANEL, UNI, S::SHARE, CLOS == 1>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt,
                                                                (ADV > 0 && !S::SHARE) ? &zc : nullptr);
             if (ADV > 0 && !S::SHARE) zc.valid = true;
             const long long qi = iidx(g, i, j, k), q = pidx(g, i, j, k);

@@ -158,6 +158,28 @@ struct Core : CoreBase {
     bool cflp_set = false;
     bool uni = true, sgs = false, anel = false;
     bool amd() const { return sgs && cfg.sgs_model == AEO_SGS_AMD; }
+    bool dyn() const { return sgs && cfg.sgs_model == AEO_SGS_DYNAMIC; }
+    // the dynamic Smagorinsky workspace: the ten pass-1 fields, the per-block
+    // partials of LM and MM, the per-level coefficient
+    DynWs<R> dws{};
+    double* d_cs2 = nullptr;
+    double* d_dynpart = nullptr;
+    int dyn_nb = 0;
+    double dyn_d2 = 0.0;   // Delta^2 = (dx dy dz)^(2/3)
+    // the kernels of the dynamic coefficient of the state in `in` (3 launches)
+    aeo_status enqueue_dynamic(R* const* in) {
+        const long long ns = (long long)dws.sx * dws.sy * (g.nz + 2);
+        germano_pass1_kernel<R><<<(unsigned)std::min<long long>((ns + 255) / 256, 148LL * 16), 256, 0, st>>>(
+            g, in[0], in[1], in[2], dws);
+        CKL();
+        germano_pass2_kernel<R><<<dim3((unsigned)dyn_nb, (unsigned)g.nz), 256, 0, st>>>(
+            g, dws, R(1.0 / 27), R(dyn_d2), R(9.0), d_dynpart);
+        CKL();
+        germano_level_kernel<<<(g.nz + 127) / 128, 128, 0, st>>>(g.nz, dyn_nb, d_dynpart, cfg.c_s * cfg.c_s, d_cs2);
+        CKL();
+        return AEO_OK;
+    }
+    int dyn_launches() const { return dyn() ? 3 : 0; }
     // g / theta0 of the AMD closure's buoyancy term (0 without buoyancy)
     R amd_bg() const { return R(amd() && cfg.theta0 != 0.0 ? cfg.g / cfg.theta0 : 0.0); }
     // per-kernel-class timing of one un-graphed step (aeo_profile_step)
@@ -426,6 +448,17 @@ struct Core : CoreBase {
         host_n = (long long)(c.nx + 2 * c.hx) * (c.ny + 2 * c.hy) * (c.nz + 2 * c.hz);
         if (aeo_status e = alloc(&d_stage, std::max<long long>(host_n, g.nin))) return e;
         if (aeo_status e = alloc(&d_part, 4 * (size_t)(Nz + 1))) return e;
+        if (dyn()) {
+            dws.sx = g.nx + 2;
+            dws.sy = g.ny + 2;
+            const size_t ns = (size_t)dws.sx * dws.sy * (g.nz + 2);
+            for (int f = 0; f < DYN_N; ++f)
+                if (aeo_status e = alloc(&dws.f[f], ns)) return e;
+            dyn_nb = (g.nx * g.ny + 255) / 256;
+            if (aeo_status e = alloc(&d_dynpart, 2 * (size_t)dyn_nb * g.nz)) return e;
+            if (aeo_status e = alloc(&d_cs2, (size_t)g.nz)) return e;
+            dyn_d2 = std::pow(g.dx * g.dy * g.dz, 2.0 / 3.0);
+        }
         if (aeo_status e = alloc(&d_flag, 1)) return e;
         if (aeo_status e = alloc(&d_sc, 1)) return e;
         set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->one, 1.0);
@@ -433,7 +466,7 @@ struct Core : CoreBase {
         if (aeo_status e = make_tensor_maps()) return e;
         kchunk = std::min(g.nz, TileShape<R, 0, false>::KCH);
         CK(cudaStreamSynchronize(st));
-        launches = 3 * 9;
+        launches = 3 * (9 + dyn_launches());
         return AEO_OK;
     }
 
@@ -507,7 +540,7 @@ struct Core : CoreBase {
         if (!pcg) return launches;
         aeo_mg_stats o{};
         if (cudaStreamSynchronize(st) != cudaSuccess || aeo_mg_read_stats(mg, &o)) return 0;
-        return 3 * (4 + aeo_mg_launches_per_solve(mg, o.iterations));
+        return 3 * (4 + dyn_launches() + aeo_mg_launches_per_solve(mg, o.iterations));
     }
 
     // the implicit IBM correction after every predictor (aeo_set_ibm)
@@ -521,7 +554,7 @@ struct Core : CoreBase {
         drop_graphs();   // the step graphs gain or lose the correction
         if (!mask) {
             ibm_mask = nullptr;
-            launches = 3 * 9;
+            launches = 3 * (9 + dyn_launches());
             return AEO_OK;
         }
         std::vector<unsigned char> m((size_t)g.nin);
@@ -537,7 +570,7 @@ struct Core : CoreBase {
         CK(cudaStreamSynchronize(st));
         ibm_mask = ibm_alloc;
         ibm_tau = tau;
-        launches = 3 * 10;
+        launches = 3 * (10 + dyn_launches());
         return AEO_OK;
     }
 
@@ -609,10 +642,19 @@ struct Core : CoreBase {
                     if (amd()) {
                         SweepArgs<R> b = a;
                         b.kofs = PS::KT_OFS;
-                        cudaFuncSetAttribute(sweep_pair_kernel<SG, AN, UN, true>,
+                        cudaFuncSetAttribute(sweep_pair_kernel<SG, AN, UN, 1>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PS::SMEM_AMD);
-                        sweep_pair_kernel<SG, AN, UN, true><<<grid, dim3(PS::TXT, PS::TY), PS::SMEM_AMD, st>>>(
+                        sweep_pair_kernel<SG, AN, UN, 1><<<grid, dim3(PS::TXT, PS::TY), PS::SMEM_AMD, st>>>(
                             tmaps[s_in], b, kchunk, d_flag);
+                        return;
+                    }
+                }
+                if constexpr (SG && UN) {
+                    if (dyn()) {
+                        cudaFuncSetAttribute(sweep_pair_kernel<SG, AN, UN, 2>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PS::SMEM);
+                        sweep_pair_kernel<SG, AN, UN, 2><<<grid, dim3(PS::TXT, PS::TY), PS::SMEM, st>>>(
+                            tmaps[s_in], a, kchunk, d_flag);
                         return;
                     }
                 }
@@ -629,10 +671,19 @@ struct Core : CoreBase {
             if (amd()) {
                 SweepArgs<R> b = a;
                 b.kofs = TS::KT_OFS;
-                cudaFuncSetAttribute(sweep_tile_kernel<R, ADV, SG, AN, UN, true>,
+                cudaFuncSetAttribute(sweep_tile_kernel<R, ADV, SG, AN, UN, 1>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS::SMEM_AMD);
-                sweep_tile_kernel<R, ADV, SG, AN, UN, true><<<grid, dim3(TS::TX, TS::TY), TS::SMEM_AMD, st>>>(
+                sweep_tile_kernel<R, ADV, SG, AN, UN, 1><<<grid, dim3(TS::TX, TS::TY), TS::SMEM_AMD, st>>>(
                     tmaps[s_in], b, kchunk, d_flag);
+                return;
+            }
+        }
+        if constexpr (SG && UN) {
+            if (dyn()) {
+                cudaFuncSetAttribute(sweep_tile_kernel<R, ADV, SG, AN, UN, 2>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS::SMEM);
+                sweep_tile_kernel<R, ADV, SG, AN, UN, 2><<<grid, dim3(TS::TX, TS::TY), TS::SMEM, st>>>(
+                    tmaps[s_in], a, kchunk, d_flag);
                 return;
             }
         }
@@ -762,6 +813,10 @@ struct Core : CoreBase {
         // and a buoyancy term with g / theta0
         a.inv_prt = amd() ? R(1) : R(1.0 / cfg.pr_t);
         a.sgs_bg = amd_bg();
+        a.cs2 = d_cs2;
+        a.dyn_d2 = dyn_d2;
+        if (dyn())
+            if (aeo_status e = enqueue_dynamic(P[s_in])) return e;
         a.flux_bot = R(cfg.flux_bot); a.flux_top = R(cfg.flux_top);
         a.sp_alpha = R(cfg.sponge_alpha); a.sp_zstart = R(cfg.sponge_zstart);
         a.c_s = R(cfg.c_s);
@@ -786,12 +841,14 @@ struct Core : CoreBase {
 
     aeo_status enqueue_pick(int s_state) {
         R** in = P[s_state];
+        if (dyn())
+            if (aeo_status e = enqueue_dynamic(in)) return e;
         if (uni) {
-            if (sgs) cfl_levels_kernel<R, true, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_part);
-            else cfl_levels_kernel<R, true, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_part);
+            if (sgs) cfl_levels_kernel<R, true, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_part);
+            else cfl_levels_kernel<R, true, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_part);
         } else {
-            if (sgs) cfl_levels_kernel<R, false, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_part);
-            else cfl_levels_kernel<R, false, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_part);
+            if (sgs) cfl_levels_kernel<R, false, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_part);
+            else cfl_levels_kernel<R, false, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_part);
         }
         CKL();
         dt_pick_kernel<<<1, 32, 0, st>>>(g, cflp, d_part, d_sc);
@@ -1084,8 +1141,10 @@ struct Core : CoreBase {
         if (!d) { fail("get_field: unknown or unavailable field"); return AEO_ERR_ARGUMENT; }
         if (id == AEO_FIELD_NUT) {
             // the step keeps nut in shared memory: evaluate it for the current state
-            if (uni) smagorinsky_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], P[cur][3], nut, R(cfg.c_s), amd_bg(), R(cfg.pr_t));
-            else smagorinsky_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], P[cur][3], nut, R(cfg.c_s), amd_bg(), R(cfg.pr_t));
+            if (dyn())
+                if (aeo_status e = enqueue_dynamic(P[cur])) return e;
+            if (uni) smagorinsky_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], P[cur][3], nut, R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2);
+            else smagorinsky_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], P[cur][3], nut, R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2);
             CKL();
         }
         S* stage = reinterpret_cast<S*>(d_stage);
@@ -1357,13 +1416,17 @@ static aeo_status validate(const aeo_config* c, const double* zf, const double* 
     if (c->precision != AEO_PREC_FP64 && c->precision != AEO_PREC_FP32_MIXED) { *m = "unknown precision"; return AEO_ERR_ARGUMENT; }
     if (c->c_s != 0.0 && !(c->pr_t > 0.0)) { *m = "pr_t must be positive with SGS"; return AEO_ERR_ARGUMENT; }
     if (c->sgs_model != AEO_SGS_SMAGORINSKY && c->sgs_model != AEO_SGS_VREMAN && c->sgs_model != AEO_SGS_SIGMA &&
-        c->sgs_model != AEO_SGS_AMD) {
+        c->sgs_model != AEO_SGS_AMD && c->sgs_model != AEO_SGS_DYNAMIC) {
         *m = "unknown SGS closure";
         return AEO_ERR_ARGUMENT;
     }
     if (c->sgs_model != AEO_SGS_SMAGORINSKY && c->stretched) {
-        *m = "the Vreman, sigma and AMD closures take a uniform grid (src/operators/sgs_amd_vreman.jl:102-107, "
-             ":280-284, src/operators/sigma_closure.jl:208-212)";
+        *m = "the Vreman, sigma, AMD and dynamic closures take a uniform grid (src/operators/sgs_amd_vreman.jl:102-107, "
+             ":280-284, src/operators/sigma_closure.jl:208-212, src/Operators.jl:555)";
+        return AEO_ERR_ARGUMENT;
+    }
+    if (c->sgs_model == AEO_SGS_DYNAMIC && c->c_s != 0.0 && (c->hx < 2 || c->hy < 2 || c->hz < 2)) {
+        *m = "the dynamic Smagorinsky closure needs host halos of at least 2 (src/Operators.jl:556-557)";
         return AEO_ERR_ARGUMENT;
     }
     if (c->sgs_model == AEO_SGS_AMD && c->c_s != 0.0 && c->core != AEO_CORE_BOUSSINESQ) {

@@ -74,6 +74,10 @@ struct oc_sim {
     double *apx, *apy, *apz, *cgx;
     ocg* cg;
     ocg_stats cg_st;
+    /* dynamic Smagorinsky: the ten pass-1 fields on the interior + one shell,
+     * LM and MM (interior), the per-level coefficient */
+    double* dyn[10];
+    double *dyn_lm, *dyn_mm, *cs2;
 };
 
 #define ID(s, i, j, k) ((int64_t)(i) + (int64_t)(s)->NX * ((int64_t)(j) + (int64_t)(s)->NY * (int64_t)(k)))
@@ -686,6 +690,93 @@ static void amd_at(const oc_sim* s, int i, int j, int k, double* nu, double* ka)
     *ka = kd > 0 ? C * fmax(0.0, -Q) / kd : *nu / s->p.pr_t;
 }
 
+/* --- dynamic Smagorinsky (compute_dynamic_smagorinsky_nut!, plane
+ * averaging, filter ratio 3, clip c_s^2; src/Operators.jl:548-900): pass 1
+ * (_germano_pass1_body!) the cell-centred velocity, strain and |S| on the
+ * interior + one shell; pass 2 (_germano_pass2_body!, _germano_LM_MM) the
+ * 3x3x3 box sums (z outer, x inner) and L^d:M, M:M; the plane sums (j outer,
+ * i inner) and the clip (_plane_cs2_body!) into s->cs2. */
+static double* dalloc(int64_t n);
+static void dyn_coefficients(oc_sim* s) {
+    const oc_params* P = &s->p;
+    int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
+    int SX = Nx + 2, SY = Ny + 2, SZ = Nz + 2;
+    size_t ns = (size_t)SX * SY * SZ, ni = (size_t)Nx * Ny * Nz;
+    if (!s->dyn[0]) {
+        for (int f = 0; f < 10; ++f) s->dyn[f] = dalloc((int64_t)ns);
+        s->dyn_lm = dalloc((int64_t)ni); s->dyn_mm = dalloc((int64_t)ni); s->cs2 = dalloc(Nz);
+    }
+    const double *u = s->u, *v = s->v, *w = s->w;
+    double idx = s->idx, idy = s->idy, idz = s->idz;
+#define SH(li, lj, lk) ((size_t)(li) + (size_t)SX * ((size_t)(lj) + (size_t)SY * (size_t)(lk)))
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int lk = 0; lk < SZ; ++lk)
+        for (int lj = 0; lj < SY; ++lj)
+            for (int li = 0; li < SX; ++li) {
+                int i = Hx - 1 + li, j = Hy - 1 + lj, k = Hz - 1 + lk;
+                size_t e = SH(li, lj, lk);
+                s->dyn[0][e] = 0.5 * (A(u, i, j, k) + A(u, i + 1, j, k));
+                s->dyn[1][e] = 0.5 * (A(v, i, j, k) + A(v, i, j + 1, k));
+                s->dyn[2][e] = 0.5 * (A(w, i, j, k) + A(w, i, j, k + 1));
+                double du_dx = (A(u, i + 1, j, k) - A(u, i, j, k)) * idx;
+                double dv_dy = (A(v, i, j + 1, k) - A(v, i, j, k)) * idy;
+                double dw_dz = (A(w, i, j, k + 1) - A(w, i, j, k)) * idz;
+                double du_dy = ((A(u, i, j + 1, k) + A(u, i + 1, j + 1, k)) - (A(u, i, j - 1, k) + A(u, i + 1, j - 1, k))) * (0.25 * idy);
+                double dv_dx = ((A(v, i + 1, j, k) + A(v, i + 1, j + 1, k)) - (A(v, i - 1, j, k) + A(v, i - 1, j + 1, k))) * (0.25 * idx);
+                double du_dz = ((A(u, i, j, k + 1) + A(u, i + 1, j, k + 1)) - (A(u, i, j, k - 1) + A(u, i + 1, j, k - 1))) * (0.25 * idz);
+                double dw_dx = ((A(w, i + 1, j, k) + A(w, i + 1, j, k + 1)) - (A(w, i - 1, j, k) + A(w, i - 1, j, k + 1))) * (0.25 * idx);
+                double dv_dz = ((A(v, i, j, k + 1) + A(v, i, j + 1, k + 1)) - (A(v, i, j, k - 1) + A(v, i, j + 1, k - 1))) * (0.25 * idz);
+                double dw_dy = ((A(w, i, j + 1, k) + A(w, i, j + 1, k + 1)) - (A(w, i, j - 1, k) + A(w, i, j - 1, k + 1))) * (0.25 * idy);
+                double S12 = 0.5 * (du_dy + dv_dx), S13 = 0.5 * (du_dz + dw_dx), S23 = 0.5 * (dv_dz + dw_dy);
+                double S2 = 2 * (du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz) + 4 * (S12 * S12 + S13 * S13 + S23 * S23);
+                s->dyn[3][e] = du_dx; s->dyn[4][e] = dv_dy; s->dyn[5][e] = dw_dz;
+                s->dyn[6][e] = S12; s->dyn[7][e] = S13; s->dyn[8][e] = S23;
+                s->dyn[9][e] = sqrt(S2);
+            }
+    const double d2 = pow(s->dx * s->dy * s->dz, 2.0 / 3.0), a2 = 9.0, inv = 1.0 / 27;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                double t[21] = {0};
+                for (int c = 0; c < 3; ++c)
+                    for (int b = 0; b < 3; ++b)
+                        for (int a = 0; a < 3; ++a) {
+                            size_t e = SH(i + a, j + b, k + c);
+                            double uu = s->dyn[0][e], vv = s->dyn[1][e], ww = s->dyn[2][e], ms = s->dyn[9][e];
+                            t[0] += uu; t[1] += vv; t[2] += ww;
+                            t[3] += uu * uu; t[4] += vv * vv; t[5] += ww * ww;
+                            t[6] += uu * vv; t[7] += uu * ww; t[8] += vv * ww;
+                            for (int q = 0; q < 6; ++q) { t[9 + q] += s->dyn[3 + q][e]; t[15 + q] += ms * s->dyn[3 + q][e]; }
+                        }
+                double Ut = t[0] * inv, Vt = t[1] * inv, Wt = t[2] * inv;
+                double L11 = t[3] * inv - Ut * Ut, L22 = t[4] * inv - Vt * Vt, L33 = t[5] * inv - Wt * Wt;
+                double L12 = t[6] * inv - Ut * Vt, L13 = t[7] * inv - Ut * Wt, L23 = t[8] * inv - Vt * Wt;
+                double tr = (L11 + L22 + L33) / 3;
+                L11 -= tr; L22 -= tr; L33 -= tr;
+                double A11 = t[9] * inv, A22 = t[10] * inv, A33 = t[11] * inv;
+                double A12 = t[12] * inv, A13 = t[13] * inv, A23 = t[14] * inv;
+                double magSt = sqrt(2 * (A11 * A11 + A22 * A22 + A33 * A33) + 4 * (A12 * A12 + A13 * A13 + A23 * A23));
+                double c1 = 2 * d2 * a2 * magSt, c2 = 2 * d2 * inv;
+                double M11 = c2 * t[15] - c1 * A11, M22 = c2 * t[16] - c1 * A22, M33 = c2 * t[17] - c1 * A33;
+                double M12 = c2 * t[18] - c1 * A12, M13 = c2 * t[19] - c1 * A13, M23 = c2 * t[20] - c1 * A23;
+                size_t q = (size_t)i + (size_t)Nx * ((size_t)j + (size_t)Ny * k);
+                s->dyn_lm[q] = L11 * M11 + L22 * M22 + L33 * M33 + 2 * (L12 * M12 + L13 * M13 + L23 * M23);
+                s->dyn_mm[q] = M11 * M11 + M22 * M22 + M33 * M33 + 2 * (M12 * M12 + M13 * M13 + M23 * M23);
+            }
+#undef SH
+    double cmax = P->c_s * P->c_s;
+    for (int k = 0; k < Nz; ++k) {
+        double lm = 0, mm = 0;
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                size_t q = (size_t)i + (size_t)Nx * ((size_t)j + (size_t)Ny * k);
+                lm += s->dyn_lm[q]; mm += s->dyn_mm[q];
+            }
+        s->cs2[k] = mm > 0 ? fmin(fmax(lm / mm, 0.0), cmax) : 0.0;
+    }
+}
+
 /* --- Smagorinsky (src/FiniteVolume.jl:936-944, src/Operators.jl:451-496) -- */
 static inline double smag_at(const oc_sim* s, int i, int j, int k) {
     const double *u = s->u, *v = s->v, *w = s->w;
@@ -728,6 +819,8 @@ static inline double smag_at(const oc_sim* s, int i, int j, int k) {
         return aa > 0 ? c * sqrt(Bb / aa) : 0.0;
     }
     double S2 = 2 * (S11 * S11 + S22 * S22 + S33 * S33) + 4 * (S12 * S12 + S13 * S13 + S23 * S23);
+    if (s->p.sgs_model == OC_SGS_DYNAMIC)   /* cs2(k) Delta^2 |S| (_dynamic_nut_body!), dyn_coefficients first */
+        return s->cs2[k - s->p.hz] * pow(s->dx * s->dy * s->dz, 2.0 / 3.0) * sqrt(S2);
     return coef * sqrt(S2);
 }
 
@@ -843,6 +936,7 @@ static void compute_tendencies(oc_sim* s) {
     const double *u = s->u, *v = s->v, *w = s->w, *th = s->th;
 
     /* 4a. Smagorinsky coefficients, then their halos (velocity BCs) */
+    if (has_sgs && P->sgs_model == OC_SGS_DYNAMIC) dyn_coefficients(s);
     if (has_sgs) {
 #pragma omp parallel for collapse(2) schedule(static)
         for (int k = Hz; k < Hz + Nz; ++k)
@@ -1376,6 +1470,7 @@ double oc_adaptive_dt(oc_sim* s, const oc_cfl* c, double dt_prev, int* limiter) 
     fill_halos(s, s->u, LOC_FX);
     fill_halos(s, s->v, LOC_FY);
     fill_halos(s, s->w, LOC_FZ);
+    if (P->c_s != 0 && P->sgs_model == OC_SGS_DYNAMIC) dyn_coefficients(s);
     double rate = 0.0, nutm = 0.0, ktm = 0.0;
     int nanr = 0;
     double* mean = (double*)calloc((size_t)Nz, sizeof(double));
@@ -1654,7 +1749,8 @@ oc_sim* oc_create(const oc_params* p, const double* zfi, const double* wc, const
     if (p->solver == OC_SOLVER_COLUMN && p->bc_z != OC_BC_WALL) return NULL;
     if (p->stretched && (!zfi || p->bc_z != OC_BC_WALL)) return NULL;
     if (p->solver == OC_SOLVER_PCG && (p->stretched || p->core != OC_CORE_BOUSSINESQ)) return NULL;
-    if ((p->sgs_model == OC_SGS_VREMAN || p->sgs_model == OC_SGS_SIGMA || p->sgs_model == OC_SGS_AMD) && p->stretched)
+    if ((p->sgs_model == OC_SGS_VREMAN || p->sgs_model == OC_SGS_SIGMA || p->sgs_model == OC_SGS_AMD ||
+         p->sgs_model == OC_SGS_DYNAMIC) && p->stretched)
         return NULL;
     if (p->sgs_model == OC_SGS_AMD && p->c_s != 0 && p->core != OC_CORE_BOUSSINESQ) return NULL;
     oc_sim* s = (oc_sim*)calloc(1, sizeof(oc_sim));
@@ -1844,6 +1940,8 @@ void oc_destroy(oc_sim* s) {
     for (size_t q = 0; q < sizeof(ptrs) / sizeof(ptrs[0]); ++q) free(ptrs[q]);
     free(s->hat); free(s->twx);
     free(s->apx); free(s->apy); free(s->apz); free(s->cgx); free(s->ibm);
+    for (int f = 0; f < 10; ++f) free(s->dyn[f]);
+    free(s->dyn_lm); free(s->dyn_mm); free(s->cs2);
     if (s->cg) ocg_destroy(s->cg);
     plan_free(&s->px); plan_free(&s->py); plan_free(&s->pz);
     free(s);
