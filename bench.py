@@ -60,9 +60,14 @@ for _p in (ROOT, PKG):
 import numpy as np  # noqa: E402
 
 HBM_FALLBACK_GBS = 6650.0
+# DRAM bytes (read + write) of one sweep launch of the CBL 256x256x128 FP32-mixed
+# step, from an ncu capture of `python bench.py --steps 2 --warmup 3`
+# (profiles/sweep_pair_kernel_cbl256_fp32.md)
+CBL_SWEEP_DRAM_BYTES = 157088256 + 95768576
 
 
 # ----------------------------------------------------------------------------- workloads
+
 def workload(name):
     from aeolus_b200 import CoreSpec, regular_grid, stretched_grid, tanh_beta_for_first_cell, tanh_faces
     from aeolus_b200.inputs import cbl_initial, cbl_theta_profile, taylor_green
@@ -1047,7 +1052,9 @@ def run_b200(args):
                 "h2d_bytes_per_step": main["h2d"], "d2h_bytes_per_step": main["d2h"]},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm,
                      "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_kind": hbm_kind,
-                     "bytes_per_launch": bytes_per_launch, "traffic": None},
+                     "bytes_per_launch": bytes_per_launch, "traffic": CBL_SWEEP_DRAM_BYTES,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one sweep launch of "
+                                       "this workload (profiles/sweep_pair_kernel_cbl256_fp32.md)"},
         "step_roofline": {"algorithmic_bytes_per_cell_step": 392, "achieved_GBps": round(
             step_bytes / (main["ms"] * 1e-3) / 1e9, 1), "frac": round(step_bytes / (main["ms"] * 1e-3) / 1e9 / hbm, 4)},
         "kernels": kernels,
