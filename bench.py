@@ -64,6 +64,9 @@ HBM_FALLBACK_GBS = 6650.0
 # step, from an ncu capture of `python bench.py --steps 2 --warmup 3`
 # (profiles/sweep_pair_kernel_cbl256_fp32.md)
 CBL_SWEEP_DRAM_BYTES = 157088256 + 95768576
+# ... and of one finest red-black colour pass of the urban 256x256x96 FP32-mixed
+# solve (profiles/mg_vcycle_urban256x256x96_fp32.md): 69.4 MB read + 1.3 MB written
+URBAN_RBGS_DRAM_BYTES = 70.7e6
 
 
 # ----------------------------------------------------------------------------- workloads
@@ -490,7 +493,10 @@ def run_b200_urban(args):
         "e2e": {"value": m["e2e"], "unit": "ms", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n + 64},
         "roofline": {"bound": "hbm", "kernel": "mg_rbgs_kernel (finest level, one colour pass)",
                      "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s", "frac": round(ach / hbm, 4),
-                     "peak_kind": hbm_kind, "bytes_per_launch": rb_bytes, "traffic": None},
+                     "peak_kind": hbm_kind, "bytes_per_launch": rb_bytes,
+                     "traffic": URBAN_RBGS_DRAM_BYTES if tuple(URBAN_N) == (256, 256, 96) else None,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one finest colour "
+                                       "pass at 256x256x96 (profiles/mg_vcycle_urban256x256x96_fp32.md)"},
         "parts_ms": {k: round(v, 4) for k, v in m["parts"].items()},
         "gpu_launches": (m["st"]["iterations"] + 1) * m["lpi"] * args.steps,
         "clocks": m["clocks"],
