@@ -46,6 +46,19 @@ __device__ __forceinline__ cplx<R> cmul(cplx<R> a, cplx<R> b) {
 template <typename R>
 __device__ __forceinline__ cplx<R> cconj(cplx<R> a) { return cmk<R>(a.x, -a.y); }
 
+// The RK3 stage combination c(x, s) = ca*s + cb*x (_Lin2r,
+// src/Simulations.jl:1194-1198).  FP64 evaluates it as written, as the
+// reference does.  FP32 evaluates x + ca*(s - x), whose two weights sum to
+// one exactly: with ca = fl(1/3) and cb = fl(2/3) the written form's weights
+// sum to 1 + 3.0e-8, which scales every field by that factor once per step
+// (a kinetic-energy drift of 6e-8 per step, the size of a whole step's
+// physical decay in a weakly dissipative flow).
+template <typename R>
+__device__ __forceinline__ R rk_combine(R ca, R cb, R s, R x) {
+    if constexpr (sizeof(R) == 4) return fmaf(ca, s - x, x);
+    else return ca * s + cb * x;
+}
+
 // Geometry of one domain, passed by value to every kernel.
 struct Geo {
     int nx, ny, nz;

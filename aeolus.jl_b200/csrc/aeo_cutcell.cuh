@@ -77,9 +77,9 @@ __global__ void __launch_bounds__(256) cc_correct_kernel(Geo g, const R* __restr
     R wn = ab > R(0) ? ws[q] - ab * R((pc - pb) * g.idz) : R(0);
     const long long qp = pidx(g, i, j, k);
     if (stage) {
-        un = ca * u0[qp] + cb * un;
-        vn = ca * v0[qp] + cb * vn;
-        wn = ca * w0[qp] + cb * wn;
+        un = rk_combine(ca, cb, u0[qp], un);
+        vn = rk_combine(ca, cb, v0[qp], vn);
+        wn = rk_combine(ca, cb, w0[qp], wn);
     }
     uo[qp] = un;
     vo[qp] = vn;

@@ -56,3 +56,7 @@ __device__ __forceinline__ F2 sqrt(F2 x) { return F2(sqrtf(x.v.x), sqrtf(x.v.y))
 __device__ __forceinline__ F2 sqrt_ratio_or_zero(F2 b, F2 a, float c) {
     return F2(a.v.x > 0.f ? c * sqrtf(b.v.x / a.v.x) : 0.f, a.v.y > 0.f ? c * sqrtf(b.v.y / a.v.y) : 0.f);
 }
+
+// the FP32 RK3 stage combination x + ca*(s - x) on a pair (rk_combine of
+// aeo_common.cuh: weights that sum to one exactly)
+__device__ __forceinline__ F2 rk_combine(float ca, float, F2 s, F2 x) { return x + F2(ca) * (s - x); }

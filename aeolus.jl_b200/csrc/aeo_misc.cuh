@@ -116,13 +116,13 @@ __global__ void __launch_bounds__(256) correct_kernel(Geo g, const R* __restrict
         R a0[N];
         vld(u0 + qp, a0);
 #pragma unroll
-        for (int n = 0; n < N; ++n) un[n] = ca * a0[n] + cb * un[n];
+        for (int n = 0; n < N; ++n) un[n] = rk_combine(ca, cb, a0[n], un[n]);
         vld(v0 + qp, a0);
 #pragma unroll
-        for (int n = 0; n < N; ++n) vn[n] = ca * a0[n] + cb * vn[n];
+        for (int n = 0; n < N; ++n) vn[n] = rk_combine(ca, cb, a0[n], vn[n]);
         vld(w0 + qp, a0);
 #pragma unroll
-        for (int n = 0; n < N; ++n) wn[n] = ca * a0[n] + cb * wn[n];
+        for (int n = 0; n < N; ++n) wn[n] = rk_combine(ca, cb, a0[n], wn[n]);
     }
     vst(uo + qp, un);
     vst(vo + qp, vn);

@@ -15,7 +15,6 @@
 // array until the process exits.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "../../include/aeolus_b200.h"
@@ -23,8 +22,6 @@
 #include "aeo_fft.cuh"
 
 #define AEO_NOALLOC_SCRATCH_BYTES (32u << 20)   // 32 MiB per device
-#define AEO_NOALLOC_MAX_DEVICES 64
-
 static __device__ __align__(256) unsigned char aeo_noalloc_scratch[AEO_NOALLOC_SCRATCH_BYTES];
 
 // defined in aeolus_b200.cu: the message aeo_last_error(NULL) returns
@@ -32,24 +29,20 @@ void aeo_set_global_error(const std::string& m);
 
 namespace {
 
-std::mutex g_mu;
-void* g_scratch[AEO_NOALLOC_MAX_DEVICES] = {};
-
-// The device address of the static scratch on the current device, looked up
-// once per device.  In host code the symbol is only a host-side stand-in,
-// never a device address: kernels get this pointer instead.
-aeo_status scratch_address(int dev, unsigned char** out) {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, aeo_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            aeo_set_global_error(std::string("cudaGetSymbolAddress(aeo_noalloc_scratch): ") + cudaGetErrorString(e));
-            return AEO_ERR_CUDA;
-        }
-        g_scratch[dev] = p;
+// The device address of the static scratch on the current device.  In host
+// code the symbol is only a host-side stand-in, never a device address:
+// kernels get this pointer instead.  It is looked up on every call (the
+// lookup allocates nothing), so a pointer never outlives the context it
+// belongs to: after a cudaDeviceReset the next call finds the array of the
+// new context.
+aeo_status scratch_address(unsigned char** out) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, aeo_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        aeo_set_global_error(std::string("cudaGetSymbolAddress(aeo_noalloc_scratch): ") + cudaGetErrorString(e));
+        return AEO_ERR_CUDA;
     }
-    *out = reinterpret_cast<unsigned char*>(g_scratch[dev]);
+    *out = reinterpret_cast<unsigned char*>(p);
     return AEO_OK;
 }
 
@@ -113,15 +106,28 @@ extern "C" aeo_status aeo_pressure_solve_column_noalloc(int32_t nx, int32_t ny, 
                              " (32 MiB: (nx/2+1)*ny*nz*16 bytes plus tables must fit)");
         return AEO_ERR_ARGUMENT;
     }
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= AEO_NOALLOC_MAX_DEVICES) {
-        aeo_set_global_error(std::string("pressure_solve_column_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    // the call copies pageable host arrays and synchronises the stream, which
+    // would invalidate a capture in progress: refuse a capturing stream
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess) {
+        aeo_set_global_error(std::string("pressure_solve_column_noalloc: cudaStreamIsCapturing: ") + cudaGetErrorString(e));
         return AEO_ERR_CUDA;
     }
+    if (cap != cudaStreamCaptureStatusNone) {
+        aeo_set_global_error("pressure_solve_column_noalloc: the stream is capturing a graph; call it outside a capture");
+        return AEO_ERR_ARGUMENT;
+    }
+    double ms = 0, gs = 0;
+    for (int k = 0; k < nz; ++k) { ms += measure[k]; gs += gauge[k]; }
+    if (!(ms != 0.0) || !(gs != 0.0)) {
+        aeo_set_global_error("pressure_solve_column_noalloc: the sums of measure and of gauge must be nonzero "
+                             "(the mean mode divides by them)");
+        return AEO_ERR_ARGUMENT;
+    }
     unsigned char* base = nullptr;
-    if (aeo_status s = scratch_address(dev, &base)) return s;
-    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (aeo_status sa = scratch_address(&base)) return sa;
 
     cplx<double>* tw = reinterpret_cast<cplx<double>*>(base);
     double* kx2 = reinterpret_cast<double*>(base + b_tw);
@@ -141,9 +147,6 @@ extern "C" aeo_status aeo_pressure_solve_column_noalloc(int32_t nx, int32_t ny, 
             return AEO_ERR_CUDA;
         }
     }
-    double ms = 0, gs = 0;
-    for (int k = 0; k < nz; ++k) { ms += measure[k]; gs += gauge[k]; }
-
     Geo g{};
     g.nx = nx; g.ny = ny; g.nz = nz;
     g.nin = (long long)nx * ny * nz;

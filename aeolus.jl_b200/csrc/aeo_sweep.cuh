@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs<R> a) {
     a.vs[qi] = V(0, 0, 0) + dt * tv;
     a.ws[qi] = (g.bc_z == 1 && k == 0) ? R(0) : W(0, 0, 0) + dt * tw;
     R tn = T(0, 0, 0) + dt * tt;
-    if (a.stage) tn = a.ca * a.th0[q] + a.cb * tn;  // th0 may alias th_out (stage 3): plain load
+    if (a.stage) tn = rk_combine(a.ca, a.cb, a.th0[q], tn);  // th0 may alias th_out (stage 3): plain load
     a.th_out[q] = tn;
 }
 

@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(const __grid_constan
             *reinterpret_cast<float2*>(a.ws + qi) =
                 (g.bc_z == 1 && k == 0) ? make_float2(0.f, 0.f) : (W(0, 0, 0) + fdt * tw).v;
             F2 tn = T(0, 0, 0) + fdt * tt;
-            if (a.stage) tn = a.ca * F2(*reinterpret_cast<const float2*>(a.th0 + q)) + a.cb * tn;
+            if (a.stage) tn = rk_combine(a.ca, a.cb, F2(*reinterpret_cast<const float2*>(a.th0 + q)), tn);
             *reinterpret_cast<float2*>(a.th_out + q) = tn.v;
         }
     }

@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
             a.vs[qi] = V(0, 0, 0) + dt * tv;
             a.ws[qi] = (g.bc_z == 1 && k == 0) ? R(0) : W(0, 0, 0) + dt * tw;
             R tn = T(0, 0, 0) + dt * tt;
-            if (a.stage) tn = a.ca * a.th0[q] + a.cb * tn;
+            if (a.stage) tn = rk_combine(a.ca, a.cb, a.th0[q], tn);
             a.th_out[q] = tn;
         }
     }

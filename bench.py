@@ -363,10 +363,22 @@ def e2e_steps(sim, state, dt, k, f32=False):
     return e0.elapsed_time(e1) / k, nbytes, sum(o.nbytes for o in outs)
 
 
-def cpu_oracle_rate(spec, state, dt, min_seconds=10.0, max_steps=20):
-    """The oracle (CPU restatement) on the host cores, full grid."""
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def cpu_oracle_rate(spec, state, dt, min_seconds=10.0, max_steps=20, threads=None):
+    """The oracle (CPU restatement) on the host cores (all of them, or
+    `threads`), full grid."""
     from oracle.oracle import OracleSimulation, set_threads
-    cores = os.cpu_count() or 1
+    cores = threads or os.cpu_count() or 1
     set_threads(cores)
     o = OracleSimulation(spec)
     o.set_state(*state)
@@ -586,40 +598,77 @@ def run_reference_hit(args):
     return 0
 
 
-def run_b200_hit(args):
-    world, rank, local = dist_setup()
+def precision_comparison(s32, s64, g, theta_ref=None):
+    """FP32-mixed against FP64 after the same steps from the same state: per
+    prognostic field the relative L2 difference, the max abs difference and
+    that max relative to the FP64 field's max; theta also as its departure
+    from `theta_ref` (the initial profile), whose differences are not hidden
+    behind the 300 K level; kinetic energies and max divergences."""
+    rel, mx, mxr = {}, {}, {}
+    names = ("u", "v", "w") + (("theta",) if theta_ref is not None else ())
+    for f in names:
+        a, b = s32.get_field(f)[g.interior], s64.get_field(f)[g.interior]
+        keys = [(f, a, b)]
+        if f == "theta":
+            keys.append(("theta_departure", a - theta_ref, b - theta_ref))
+        for k, x, y in keys:
+            d = np.abs(x - y)
+            ny_ = float(np.linalg.norm(y))
+            rel[k] = float(np.linalg.norm(x - y) / ny_) if ny_ > 0 else float(np.linalg.norm(x - y))
+            mx[k] = float(d.max())
+            ym = float(np.abs(y).max())
+            mxr[k] = mx[k] / ym if ym > 0 else mx[k]
+        del a, b, keys
+    return {"relative_l2": rel, "max_abs": mx, "max_relative": mxr,
+            "ke_fp64": s64.kinetic_energy(), "ke_fp32": s32.kinetic_energy(),
+            "max_divergence_fp64": s64.max_divergence(), "max_divergence_fp32": s32.max_divergence()}
+
+
+def ke_change(cmp, ke0_64, ke0_32):
+    """Kinetic-energy drift of the FP32-mixed run against FP64: the relative
+    difference of the final energies and of the energy change over the run
+    (the decay of a decaying flow, the growth of a convecting one)."""
+    k64, k32 = cmp["ke_fp64"], cmp["ke_fp32"]
+    d64, d32 = k64 - ke0_64, k32 - ke0_32
+    cmp.update({"ke_initial_fp64": ke0_64, "ke_initial_fp32": ke0_32,
+                "ke_relative_difference": abs(k32 - k64) / abs(k64) if k64 else None,
+                "ke_change_fp64": d64, "ke_change_fp32": d32,
+                "ke_change_relative_difference": abs(d32 - d64) / abs(d64) if d64 else None})
+    return cmp
+
+
+def hit_run(n, nsteps, args, local, world):
+    """Config 3, decaying isotropic turbulence on n^3 cells: the FP64 run steps
+    adaptively (CFL 0.5, growth 1.1) for `nsteps` steps, the FP32-mixed run
+    repeats its dt sequence from the same start, the two are compared; then
+    both are timed at the last dt (the captured graph) and adaptively."""
     import torch
-    torch.cuda.set_device(local)
     from aeolus_b200 import CoreSpec, regular_grid
     from aeolus_b200.simulation import CFLConstraints, Simulation
-    n = args.hit_n
     g = regular_grid((n, n, n), (2 * np.pi,) * 3)
 
     def spec(prec):
         return CoreSpec(grid=g, advection="weno_z5", nu=0.0, precision=prec)
 
-    hbm, hbm_kind = measured_peaks()
     s64 = Simulation(spec("fp64"), device=local)
     s64.init_isotropic(u_rms=1.0, k_peak=4.0, seed=1, project=True, target_rms=1.0)
     state0 = s64.get_state()
     ke0 = s64.kinetic_energy()
     c = CFLConstraints(C_advective=0.5, growth_max=1.1)
     dts, dt_prev = [], None
-    for _ in range(args.hit_steps):
+    for _ in range(nsteps):
         st = s64.step_adaptive(c, 1, dt_prev)
         dts.append(st["dt"])
         dt_prev = st["dt"]
-    fin64 = [s64.get_field(f)[g.interior] for f in ("u", "v", "w")]
-    ke64, div64 = s64.kinetic_energy(), s64.max_divergence()
     s32 = Simulation(spec("fp32_mixed"), device=local)
     s32.set_state(*state0)
+    del state0
+    ke0_32 = s32.kinetic_energy()
     for dt in dts:
         s32.step_rk3(dt, 1)
-    fin32 = [s32.get_field(f)[g.interior] for f in ("u", "v", "w")]
-    ke32, div32 = s32.kinetic_energy(), s32.max_divergence()
-    rel = {f: float(np.linalg.norm(a - b) / np.linalg.norm(b)) for f, a, b in zip("uvw", fin32, fin64)}
-    del fin32, fin64
-    # rates: fixed-dt steps (the captured graph) at the last dt, and adaptive steps
+    cmp = ke_change(precision_comparison(s32, s64, g), ke0, ke0_32)
+    cmp["ke_decay_relative_difference"] = cmp["ke_change_relative_difference"]
+    cmp.update({"steps": nsteps, "t_end": float(np.sum(dts)), "dt_first": dts[0], "dt_last": dts[-1]})
     dt = dts[-1]
     res = {}
     for name, sim in (("fp32_mixed", s32), ("fp64", s64)):
@@ -629,19 +678,30 @@ def run_b200_hit(args):
         ms = timed_steps(sim, dt, args.steps, world) / args.steps
         clocks = clk.stop()
         prof = sim.profile_step(dt)
-        import torch as _t
-        e0, e1 = _t.cuda.Event(enable_timing=True), _t.cuda.Event(enable_timing=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ka = max(3, min(args.steps, 10))
         # the guard's divergence bound is the reference's FP64 round-off bound (1e-6);
         # an FP32 projection leaves ~1e-7 relative to the velocity gradients
         ca = c if name == "fp64" else CFLConstraints(C_advective=0.5, growth_max=1.1, divergence_tol=1e-2)
         sim.synchronize()
-        e0.record(_t.cuda.ExternalStream(sim.stream))
+        e0.record(torch.cuda.ExternalStream(sim.stream))
         sim.step_adaptive(ca, ka, dt)
-        e1.record(_t.cuda.ExternalStream(sim.stream))
+        e1.record(torch.cuda.ExternalStream(sim.stream))
         sim.synchronize()
         res[name] = {"ms": max_over_ranks(ms, world), "clocks": clocks, "prof": prof,
                      "adaptive_ms": e0.elapsed_time(e1) / ka, "launches": sim.launches_per_step()}
+    s32.close()
+    s64.close()
+    return g, cmp, res
+
+
+def run_b200_hit(args):
+    world, rank, local = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    n = args.hit_n
+    hbm, hbm_kind = measured_peaks()
+    g, cmp, res = hit_run(n, args.hit_steps, args, local, world)
     if rank != 0:
         barrier(world)
         return 0
@@ -663,11 +723,7 @@ def run_b200_hit(args):
         "fp64": {"value": world * ncell / (res["fp64"]["ms"] * 1e-3), "ms_per_step": res["fp64"]["ms"],
                  "adaptive_ms_per_step": res["fp64"]["adaptive_ms"]},
         "adaptive_ms_per_step": m["adaptive_ms"],
-        "fp32_vs_fp64": {"steps": args.hit_steps, "relative_l2": rel, "ke_fp64": ke64, "ke_fp32": ke32,
-                         "ke_initial": ke0, "ke_relative_difference": abs(ke32 - ke64) / ke64,
-                         "ke_decay_relative_difference": abs((ke0 - ke32) - (ke0 - ke64)) / (ke0 - ke64)
-                         if ke0 != ke64 else None, "max_divergence_fp64": div64, "max_divergence_fp32": div32,
-                         "t_end": float(np.sum(dts))},
+        "fp32_vs_fp64": cmp,
         "roofline": {"bound": "hbm", "kernel": "sweep", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
                      "frac": round(ach / hbm, 4), "peak_kind": hbm_kind, "bytes_per_launch": sweep_bytes,
                      "traffic": None},
@@ -1008,19 +1064,51 @@ def run_b200(args):
         clocks = clk.stop()
         ms_total = max_over_ranks(ms_total, world)
         ms = ms_total / args.steps
-        e2e_ms, h2d, d2h = e2e_steps(sim, state, dt, max(2, min(args.steps, 5)), f32=prec == "fp32_mixed")
+        # e2e through the reference's binding: Float64 Field.data host arrays
+        ke2e = max(2, min(args.steps, 5))
+        e2e_ms, h2d, d2h = e2e_steps(sim, state, dt, ke2e)
         e2e_ms = max_over_ranks(e2e_ms, world)
-        results[prec] = dict(ms=ms, prof=prof, clocks=clocks, e2e_ms=e2e_ms, h2d=h2d, d2h=d2h,
-                             launches=sim.launches_per_step(), div=sim.max_divergence(),
-                             ke=sim.kinetic_energy())
+        r = dict(ms=ms, prof=prof, clocks=clocks, e2e_ms=e2e_ms, h2d=h2d, d2h=d2h,
+                 launches=sim.launches_per_step(), div=sim.max_divergence(), ke=sim.kinetic_energy())
+        if prec == "fp32_mixed":   # and through the FP32 host mirror of an FP32-mixed domain
+            e2e32_ms, h2d32, d2h32 = e2e_steps(sim, state, dt, ke2e, f32=True)
+            r.update(e2e32_ms=max_over_ranks(e2e32_ms, world), h2d32=h2d32, d2h32=d2h32)
+        results[prec] = r
         sim.close()
         del sim
+    # FP32-mixed against FP64 over the configured run (500 steps of 1 s)
+    sims = {p: Simulation(mkspec(p), device=local) for p in ("fp64", "fp32_mixed")}
+    for sim in sims.values():
+        sim.set_state(*state)
+    ke0 = {p: sim.kinetic_energy() for p, sim in sims.items()}
+    for sim in sims.values():
+        sim.step_rk3(dt, args.cbl_steps)
+    theta_ref = state[3][g.interior]
+    cbl_cmp = ke_change(precision_comparison(sims["fp32_mixed"], sims["fp64"], g, theta_ref=theta_ref),
+                        ke0["fp64"], ke0["fp32_mixed"])
+    cbl_cmp["ke_growth_relative_difference"] = cbl_cmp["ke_change_relative_difference"]
+    cbl_cmp.update({"steps": args.cbl_steps, "t_end": dt * args.cbl_steps})
+    for sim in sims.values():
+        sim.close()
+    del sims
     # the other half of the metric: PCG time to 1e-8 on the urban problem
     coeffs, b, udesc = urban_problem()
     pcg = pcg_solves(coeffs, b, reps=max(3, min(args.steps, 10)))
     for v in pcg.values():
         v["ms"] = max_over_ranks(v["ms"], world)
         del v["handle"]
+    # config 3 beside it: decaying isotropic turbulence, FP32-mixed against FP64
+    hit = None
+    if args.hit_steps > 0:
+        hg, hcmp, hres = hit_run(args.hit_n, args.hit_steps, args, local, world)
+        hit = {"config": f"decaying isotropic turbulence {args.hit_n}^3, WENO-Z5, no SGS, nu = 0, adaptive dt "
+                         f"CFL 0.5 (growth 1.1), Passot-Pouquet spectrum k_p = 4, u_rms = 1, seed 1",
+               "value": world * hg.ncells / (hres["fp32_mixed"]["ms"] * 1e-3), "unit": "cell-steps/s",
+               "ms_per_step": hres["fp32_mixed"]["ms"],
+               "fp64": {"value": world * hg.ncells / (hres["fp64"]["ms"] * 1e-3), "ms_per_step": hres["fp64"]["ms"]},
+               "adaptive_ms_per_step": {"fp32_mixed": hres["fp32_mixed"]["adaptive_ms"],
+                                        "fp64": hres["fp64"]["adaptive_ms"]},
+               "fp32_vs_fp64": hcmp, "clocks": hres["fp32_mixed"]["clocks"]}
     if rank != 0:
         barrier(world)
         return 0
@@ -1055,7 +1143,13 @@ def run_b200(args):
         "fp64": {"value": world * ncell / (fp64["ms"] * 1e-3), "ms_per_step": fp64["ms"],
                  "e2e": world * ncell / (fp64["e2e_ms"] * 1e-3), "max_divergence": fp64["div"]},
         "e2e": {"value": world * ncell / (main["e2e_ms"] * 1e-3), "unit": "cell-steps/s",
-                "h2d_bytes_per_step": main["h2d"], "d2h_bytes_per_step": main["d2h"]},
+                "h2d_bytes_per_step": main["h2d"], "d2h_bytes_per_step": main["d2h"],
+                "host_arrays": "Float64 storage arrays (the reference's Field.data) through aeo_set_field / "
+                               "aeo_get_field, pinned"},
+        "e2e_fp32_host": {"value": world * ncell / (main["e2e32_ms"] * 1e-3), "unit": "cell-steps/s",
+                          "h2d_bytes_per_step": main["h2d32"], "d2h_bytes_per_step": main["d2h32"],
+                          "host_arrays": "Float32 mirrors through aeo_set_field_f32 / aeo_get_field_f32"},
+        "fp32_vs_fp64": cbl_cmp,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm,
                      "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_kind": hbm_kind,
                      "bytes_per_launch": bytes_per_launch, "traffic": CBL_SWEEP_DRAM_BYTES,
@@ -1069,12 +1163,17 @@ def run_b200(args):
         "max_divergence": main["div"],
         "pcg": {"metric": "PCG time-to-1e-8", "unit": "ms", "config": udesc,
                 "plain_fp32_mixed": pcg["fp32_mixed"], "plain_fp64": pcg["fp64"], "learned": None},
+        "hit": hit,
     }
     if world == 1 and not args.no_cpu_baseline:
         rate, cores, n, el = cpu_oracle_rate(mkspec("fp64"), state, dt)
+        rate1, _, n1, el1 = cpu_oracle_rate(mkspec("fp64"), state, dt, threads=1, min_seconds=8.0, max_steps=2)
         line["cpu_baseline"] = {"value": rate, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+                                "cpu_model": cpu_model(),
                                 "sample": f"{n} RK3 steps of the full grid ({el:.1f} s), FP64 oracle, "
-                                          f"{cores} OpenMP threads"}
+                                          f"{cores} OpenMP threads",
+                                "one_thread": {"value": rate1, "sample": f"{n1} RK3 steps of the full grid "
+                                                                         f"({el1:.1f} s), 1 thread"}}
     print(json.dumps(line), flush=True)
     barrier(world)
     return 0
@@ -1089,7 +1188,8 @@ def main():
     ap.add_argument("--workload", default="cbl", choices=["cbl", "tgv", "urban", "hit", "urban_step", "tracer"])
     ap.add_argument("--tracer-n", type=int, default=256)
     ap.add_argument("--hit-n", type=int, default=512)
-    ap.add_argument("--hit-steps", type=int, default=100)
+    ap.add_argument("--hit-steps", type=int, default=200)
+    ap.add_argument("--cbl-steps", type=int, default=500)
     ap.add_argument("--urban-n", type=int, nargs=3, default=None)
     ap.add_argument("--urban-boxes", type=int, default=600)
     ap.add_argument("--urban-steps", type=int, default=10)

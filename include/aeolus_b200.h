@@ -276,10 +276,17 @@ aeo_status aeo_fill_uniform(aeo_sim* h, int32_t field, uint64_t seed, uint32_t s
  * the ColumnTridiagonalSolver coefficients lower, upper, hweight, measure
  * (nz each), inv_coupling (nz+1) and gauge (nz), host arrays; src and phi
  * are caller-owned device arrays of nx*ny*nz doubles (x fastest).  It runs
- * on `stream` on the current device and returns after that stream has
- * synchronised.  The first call on a device looks up the scratch address;
- * make that first call before any stream capture.  Calls share the scratch:
- * calls that overlap on the GPU (other streams, other host threads) race. */
+ * on `stream` on the current device: it copies the six host coefficient
+ * arrays to the scratch, launches the solve and returns after that stream
+ * has synchronised; a stream that is capturing a graph is refused with
+ * AEO_ERR_ARGUMENT, as are a zero sum of measure or of gauge.  Every call
+ * looks up the scratch array's device address on the current device (the
+ * lookup allocates nothing, and after a cudaDeviceReset it finds the array
+ * of the new context);
+ * the first call on a device also loads the library's device code there,
+ * so make that first call before any stream capture begins on the device.
+ * Calls share the scratch: calls that overlap on the GPU (other streams,
+ * other host threads) race. */
 aeo_status aeo_pressure_solve_column_noalloc(int32_t nx, int32_t ny, int32_t nz, double lx, double ly,
                                              const double* lower, const double* upper,
                                              const double* hweight, const double* measure,
