@@ -5,14 +5,17 @@ reference is Julia, which is not installed) and writes:
   philox4x32_10_kat.json  the Random123 known-answer vectors of
                           test/backends.jl:269-273 (Philox4x32-10)
 
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py /path/to/Aeolus.jl
+   or: AEOLUS_REFERENCE=/path/to/Aeolus.jl python tests/golden/make_golden.py
 """
 import json
 import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("AEOLUS_REFERENCE")
+if not REF:
+    sys.exit("usage: make_golden.py /path/to/Aeolus.jl (or set AEOLUS_REFERENCE)")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
