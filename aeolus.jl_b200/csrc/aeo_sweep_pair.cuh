@@ -7,10 +7,18 @@
 // shared load (an odd offset takes the halves of the two aligned pairs
 // around it, which its even neighbours load anyway).
 //
-// A CTA owns 64 x 8 cells (32 x 8 threads) and marches up a chunk of levels;
-// the planes of u, v, w and theta (x from i0-4, 72 wide, y halo 2) come by
-// TMA into a ring one level ahead; the Smagorinsky eddy viscosity of each
-// new level is computed in-tile on pairs (tile x -2 .. 65, y -1 .. 8).
+// A tile is 64 x 8 cells (32 x 8 threads).  The kernel is persistent: it is
+// launched with as many CTAs as the SMs hold (two per SM) and CTA c takes
+// the c-th of that many equal contiguous ranges of the (tile, level) items,
+// tile-major, so every CTA does the same number of levels (no partial last
+// wave) in one or a few column segments.  In a segment the CTA marches up
+// the column: the planes of u, v, w and theta (x from i0-4, 72 wide, y halo
+// 2) come by TMA into a ring loaded one level ahead of what the level in
+// hand reads; every thread polls the slot's mbarrier itself (bounded).  With
+// an SGS closure the eddy viscosity of level k+2 is formed on cell pairs
+// (tile x -2 .. 65, y -1 .. 8) in the same pass as the sweep of level k,
+// into a ring of four planes, so one CTA barrier per level orders both the
+// eddy-viscosity planes and the reuse of the ring slots.
 #pragma once
 
 #include "aeo_f2.cuh"
@@ -41,9 +49,12 @@ template <bool SGS>
 struct PairShape {
     static constexpr int TXT = 32, TX = 2 * TXT, TY = 8, NT = TXT * TY;
     static constexpr int HH = 2;
-    static constexpr int ZL = SGS ? 2 : 1, ZH = SGS ? 2 : 1;
-    static constexpr int NW = ZL + ZH + 1;
-    static constexpr int NS = NW + 1;                    // one level ahead (two CTAs per SM)
+    // levels read while level k is swept: k-1 .. k+1, and with SGS the
+    // velocities k+1 .. k+3 of the eddy viscosity of level k+2
+    static constexpr int ZH = SGS ? 3 : 1;
+    static constexpr int NW = ZH + 2;                    // k-1 .. k+ZH
+    static constexpr int NS = NW + 1;                    // one level in flight
+    static constexpr int NNU = 4;                        // eddy-viscosity planes k-1 .. k+2
     static constexpr int PW = TX + 8;                    // x from i0-4: 16-byte aligned TMA start
     static constexpr int PH = TY + 2 * HH;
     static constexpr int PSZ = PW * PH;
@@ -51,17 +62,20 @@ struct PairShape {
     static constexpr int NPW = TX + 4, NPH = TY + 2, NPS = NPW * NPH;   // nut plane: x -2 .. 65, y -1 .. 8
     static constexpr int NPAIR = NPW / 2;                // nut pairs per row
     static constexpr size_t PLANES_BYTES = (size_t)NS * 4 * PSZA * sizeof(float);
-    static constexpr size_t NUT_BYTES = SGS ? (((size_t)3 * NPS * sizeof(float) + 127) / 128) * 128 : 0;
+    static constexpr size_t NUT_BYTES = SGS ? (((size_t)NNU * NPS * sizeof(float) + 127) / 128) * 128 : 0;
     static constexpr size_t BAR_BYTES = 128;
-    static constexpr int KCH = 32, NLT = KCH + 2 * AEO_LH;
+    // a column segment has at most KCH levels (the per-level factor table)
+    static constexpr int KCH = 64, NLT = KCH + 2 * AEO_LH;
     static constexpr size_t SMEM = PLANES_BYTES + NUT_BYTES + BAR_BYTES + (size_t)LV_N * NLT * sizeof(float) + 128;
     // the AMD closure's kappa_t planes (the nut planes' layout) after the rest
     static constexpr size_t KT_BYTE = ((SMEM - 128 + 127) / 128) * 128;
     static constexpr int KT_OFS = (int)((KT_BYTE - PLANES_BYTES) / sizeof(float));   // elements past nutp
     static constexpr size_t SMEM_AMD = KT_BYTE + NUT_BYTES + 128;
+    static constexpr int CTAS_PER_SM = 2;
     static_assert(NS * 8 <= (int)BAR_BYTES, "mbarrier block");
     static_assert(TXT == 32 && NPAIR == TXT + 2, "the eddy-viscosity loop maps warps to 32-pair rows");
     static_assert(PW % 2 == 0 && PSZA % 2 == 0 && NPW % 2 == 0, "pairs stay 8-byte aligned");
+    static_assert(SMEM_AMD + 1024 <= 228 * 1024 / CTAS_PER_SM, "two CTAs an SM");
 };
 
 // Pair accessor: (di, dj, dk) -> the values at x and x+1 (x = the thread's
@@ -94,9 +108,42 @@ struct PairNut {
     __device__ __forceinline__ PairNut shifted(int o) const { return PairNut{{p[0] + o, p[1] + o, p[2] + o}}; }
 };
 
+// The eddy viscosity (and the AMD closure's kappa_t) of level L on the nut
+// plane np, from the ring planes of levels L-1, L, L+1: warps take rows of
+// the 32 interior pairs, the two edge pairs of every row come last.
+template <int CLOS, bool UNI, class S>
+__device__ __forceinline__ void pair_nut_plane(const Met<float, UNI>& m, const SweepArgs<float>& a, const Geo& g,
+                                               int L, const float* const* sp, float* np, int tid) {
+    using R = float;
+    for (int e = tid; e < S::NPAIR * S::NPH; e += S::NT) {
+        int cj, pc;
+        if (e < S::TXT * S::NPH) { cj = e >> 5; pc = (e & 31) + 1; }
+        else { const int x = e - S::TXT * S::NPH; cj = x >> 1; pc = (x & 1) ? S::NPAIR - 1 : 0; }
+        // the pair's first cell sits at tile x = 2 pc - 2, plane x = 2 pc + 2
+        const int b = (cj - 1 + S::HH) * S::PW + 2 * pc + 2;
+        const float* q[3] = {sp[0] + b, sp[1] + b, sp[2] + b};
+        const PairAcc<1, S::PW, 0> Uq{q};
+        const PairAcc<1, S::PW, S::PSZA> Vq{q};
+        const PairAcc<1, S::PW, 2 * S::PSZA> Wq{q};
+        if constexpr (CLOS == 2) {
+            const F2 c = F2(float(dyn_cs2_at(g, a.cs2, L) * a.dyn_d2));
+            const F2 nv = c * strain_at<R, UNI>(m, g, L, Uq, Vq, Wq, (F2*)nullptr);
+            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nv.v;
+        } else if constexpr (CLOS == 1) {
+            const PairAcc<1, S::PW, 3 * S::PSZA> Tq{q};
+            const NuKappa<F2> nk = amd_point<R, UNI>(m, g, L, R(a.c_s), a.sgs_bg, a.pr_t, Uq, Vq, Wq, Tq);
+            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nk.nu.v;
+            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc + S::KT_OFS) = nk.ka.v;
+        } else {
+            const F2 nv = smag_point<R, UNI>(m, g, L, R(a.c_s), Uq, Vq, Wq);
+            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nv.v;
+        }
+    }
+}
+
 template <bool SGS, bool ANEL, bool UNI, int CLOS = 0>   // CLOS: as in sweep_tile_kernel
 __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(const __grid_constant__ TileMaps maps, SweepArgs<float> a,
-                                                            int kchunk, int* err) {
+                                                            int ntx, int items, int* err) {
     using S = PairShape<SGS>;
     using R = float;
     extern __shared__ __align__(128) unsigned char smem_tile[];
@@ -108,146 +155,162 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(const __grid_constan
 
     const Geo& g = a.g;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + S::TXT * ty;
-    const int i0 = blockIdx.x * S::TX, j0 = blockIdx.y * S::TY;
-    const int kbeg = blockIdx.z * kchunk;
-    const int kend = min(g.nz, kbeg + kchunk);
-    const int i = i0 + 2 * tx, j = j0 + ty;
-    const bool active = i < g.nx && j < g.ny;   // nx is even: the pair is whole
-    const int Lfirst = kbeg - S::ZL;
-    const int Llast = kend - 1 + S::ZH;
     const uint32_t bytes = 4u * S::PSZ * sizeof(float);
-
-    auto slot_of = [&](int L) { return (L - Lfirst) % S::NS; };
-    auto parity_of = [&](int L) { return (uint32_t)(((L - Lfirst) / S::NS) & 1); };
-    auto plane = [&](int L) { return planes + (size_t)slot_of(L) * 4 * S::PSZA; };
-    auto issue = [&](int L) {
-        uint64_t* b = bars + slot_of(L);
-        mbar_expect_tx(b, bytes);
-        const int x = i0 + AEO_HX - 4, y = j0 + AEO_H - S::HH, z = L + AEO_H;
-        float* d = plane(L);
-        tma_load_3d(d, &maps.u, b, x, y, z);
-        tma_load_3d(d + S::PSZA, &maps.v, b, x, y, z);
-        tma_load_3d(d + 2 * S::PSZA, &maps.w, b, x, y, z);
-        tma_load_3d(d + 3 * S::PSZA, &maps.t, b, x, y, z);
-    };
+    const int w0 = (int)((long long)items * blockIdx.x / gridDim.x);
+    const int w1 = (int)((long long)items * (blockIdx.x + 1) / gridDim.x);
+    const R dt = R(__ldg(a.dtp));
+    const int vbase = (ty + S::HH) * S::PW + 4 + 2 * tx;
+    const int nb = (ty + 1) * S::NPW + 2 * tx + 2;    // the thread's pair on a nut plane
+    auto nut_plane = [&](int L) { return nutp + (size_t)(L & (S::NNU - 1)) * S::NPS; };
 
     if (tid == 0) {
         for (int s = 0; s < S::NS; ++s) mbar_init(bars + s, 1);
         fence_mbar_init();
     }
-    const int nlt = kend - kbeg + 2 * AEO_LH;
-    {
-        const float* src = static_cast<const float*>(g.lvr);
-        for (int e = tid; e < LV_N * S::NLT; e += S::NT) {
-            const int f = e / S::NLT, kk = e - f * S::NLT;
-            if (kk < nlt) lvs[e] = src[(size_t)f * g.lvn + kbeg + kk];
-        }
-    }
-    __syncthreads();
-    const Met<R, UNI> m(g, lvs, S::NLT, AEO_LH - kbeg);
-    int Lissued = min(Llast, kbeg + S::ZH + 1);
-    if (tid == 0)
-        for (int L = Lfirst; L <= Lissued; ++L) issue(L);
-
-    const R dt = R(__ldg(a.dtp));
-    const int vbase = (ty + S::HH) * S::PW + 4 + 2 * tx;
+    // loads issued before the segment in hand: the ring position and
+    // mbarrier phase of every load follow from this count
+    uint32_t seq0 = 0;
     bool failed = false;
-    for (int k = kbeg; k < kend; ++k) {
-        const int Lw0 = (k == kbeg) ? Lfirst : k + S::ZH;
-        bool ok = true;
-        if (tid < 32)
-            for (int L = Lw0; L <= k + S::ZH; ++L) ok = ok && mbar_wait_bounded(bars + slot_of(L), parity_of(L));
-        if (__syncthreads_or(!ok)) { failed = true; break; }
-        // every thread is past level k-1: the slot of level k-1-ZL takes level k+ZH+1
-        if (k > kbeg) {
-            const int Ln = k + S::ZH + 1;
-            if (Ln <= Llast) {
-                if (tid == 0) issue(Ln);
-                Lissued = Ln;
+    int Lfirst = 0;
+    for (int w = w0; w < w1;) {
+        const int tile = w / g.nz;
+        const int kbeg = w - tile * g.nz;
+        const int kend = min(min(g.nz, kbeg + S::KCH), w1 - tile * g.nz);
+        w = tile * g.nz + kend;
+        const int i0 = (tile % ntx) * S::TX, j0 = (tile / ntx) * S::TY;
+        const int i = i0 + 2 * tx, j = j0 + ty;
+        const bool active = i < g.nx && j < g.ny;   // nx is even: the pair is whole
+        Lfirst = kbeg - (SGS ? 2 : 1);
+        const int Llast = kend + (SGS ? 1 : 0);
+        auto seq_of = [&](int L) { return seq0 + (uint32_t)(L - Lfirst); };
+        auto slot_of = [&](int L) { return (int)(seq_of(L) % S::NS); };
+        auto parity_of = [&](int L) { return (uint32_t)((seq_of(L) / S::NS) & 1u); };
+        auto plane = [&](int L) { return planes + (size_t)slot_of(L) * 4 * S::PSZA; };
+        auto issue = [&](int L) {
+            uint64_t* b = bars + slot_of(L);
+            mbar_expect_tx(b, bytes);
+            const int x = i0 + AEO_HX - 4, y = j0 + AEO_H - S::HH, z = L + AEO_H;
+            float* d = plane(L);
+            tma_load_3d(d, &maps.u, b, x, y, z);
+            tma_load_3d(d + S::PSZA, &maps.v, b, x, y, z);
+            tma_load_3d(d + 2 * S::PSZA, &maps.w, b, x, y, z);
+            tma_load_3d(d + 3 * S::PSZA, &maps.t, b, x, y, z);
+        };
+        auto wait_upto = [&](int Lo, int Hi) {   // this thread waits for the planes Lo..Hi
+            bool ok = true;
+            for (int L = Lo; L <= Hi; ++L) ok = ok && mbar_wait_bounded(bars + slot_of(L), parity_of(L));
+            return ok;
+        };
+
+        // the previous segment is done with the ring and the factor table
+        __syncthreads();
+        if (tid == 0)
+            for (int L = Lfirst; L <= min(Llast, Lfirst + S::NS - 1); ++L) issue(L);
+        int kfail = kbeg;   // the level at which a wait gave up
+        const int nlt = kend - kbeg + 2 * AEO_LH;
+        {
+            const float* src = static_cast<const float*>(g.lvr);
+            for (int e = tid; e < LV_N * S::NLT; e += S::NT) {
+                const int f = e / S::NLT, kk = e - f * S::NLT;
+                if (kk < nlt) lvs[e] = src[(size_t)f * g.lvn + kbeg + kk];
             }
         }
+        __syncthreads();
+        const Met<R, UNI> m(g, lvs, S::NLT, AEO_LH - kbeg);
 
-        const float* lp[S::NW];
-#pragma unroll
-        for (int d = 0; d < S::NW; ++d) lp[d] = plane(k - S::ZL + d) + vbase;
-        const PairAcc<S::ZL, S::PW, 0> U{lp};
-        const PairAcc<S::ZL, S::PW, S::PSZA> V{lp};
-        const PairAcc<S::ZL, S::PW, 2 * S::PSZA> W{lp};
-        const PairAcc<S::ZL, S::PW, 3 * S::PSZA> T{lp};
-
-        PairNut<S::NPW> N;
-        if (SGS) {
-            const int Lz0 = (k == kbeg) ? k - 1 : k + 1;
-            bool mirror = false;
-            for (int L = Lz0; L <= k + 1; ++L) {
-                if (g.bc_z == 1 && (L < 0 || L >= g.nz)) { mirror = true; continue; }
-                float* np = nutp + (size_t)((L + 3) % 3) * S::NPS;
-                const float* sp[3];
-#pragma unroll
-                for (int d = 0; d < 3; ++d) sp[d] = plane(L - 1 + d);
-                // warps take rows of the 32 interior pairs, the two edge pairs come last
-                for (int e = tid; e < S::NPAIR * S::NPH; e += S::NT) {
-                    int cj, pc;
-                    if (e < S::TXT * S::NPH) { cj = e >> 5; pc = (e & 31) + 1; }
-                    else { const int x = e - S::TXT * S::NPH; cj = x >> 1; pc = (x & 1) ? S::NPAIR - 1 : 0; }
-                    // the pair's first cell sits at tile x = 2 pc - 2, plane x = 2 pc + 2
-                    const int b = (cj - 1 + S::HH) * S::PW + 2 * pc + 2;
-                    const float* q[3] = {sp[0] + b, sp[1] + b, sp[2] + b};
-                    const PairAcc<1, S::PW, 0> Uq{q};
-                    const PairAcc<1, S::PW, S::PSZA> Vq{q};
-                    const PairAcc<1, S::PW, 2 * S::PSZA> Wq{q};
-                    if constexpr (CLOS == 2) {
-                        const F2 c = F2(float(dyn_cs2_at(g, a.cs2, L) * a.dyn_d2));
-                        const F2 nv = c * strain_at<R, UNI>(m, g, L, Uq, Vq, Wq, (F2*)nullptr);
-                        *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nv.v;
-                    } else if constexpr (CLOS == 1) {
-                        const PairAcc<1, S::PW, 3 * S::PSZA> Tq{q};
-                        const NuKappa<F2> nk = amd_point<R, UNI>(m, g, L, R(a.c_s), a.sgs_bg, a.pr_t, Uq, Vq, Wq, Tq);
-                        *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nk.nu.v;
-                        *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc + S::KT_OFS) = nk.ka.v;
-                    } else {
-                        const F2 nv = smag_point<R, UNI>(m, g, L, R(a.c_s), Uq, Vq, Wq);
-                        *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nv.v;
-                    }
-                }
+        // the planes of the first level (and with SGS the eddy viscosity of
+        // levels kbeg-1 .. kbeg+1) before the first sweep
+        bool ok = wait_upto(Lfirst, min(Llast, kbeg + (SGS ? 2 : 1)));
+        if (SGS && ok)
+            for (int L = kbeg - 1; L <= kbeg + 1; ++L) {
+                if (g.bc_z == 1 && (L < 0 || L >= g.nz)) continue;
+                const float* sp[3] = {plane(L - 1), plane(L), plane(L + 1)};
+                pair_nut_plane<CLOS, UNI, S>(m, a, g, L, sp, nut_plane(L), tid);
+            }
+        failed = __syncthreads_or(!ok);
+        if (SGS && !failed && g.bc_z == 1 && (kbeg == 0 || kbeg + 1 >= g.nz)) {
+            // the wall mirrors: level -1 takes level 0, level nz takes nz-1
+            for (int L = kbeg - 1; L <= kbeg + 1; ++L) {
+                if (L >= 0 && L < g.nz) continue;
+                const int Ls = L < 0 ? -L - 1 : 2 * g.nz - 1 - L;
+                float* dst = nut_plane(L);
+                const float* srcp = nut_plane(Ls);
+                for (int e = tid; e < S::NPS; e += S::NT) dst[e] = srcp[e];
+                if (CLOS == 1)
+                    for (int e = tid; e < S::NPS; e += S::NT) dst[e + S::KT_OFS] = srcp[e + S::KT_OFS];
             }
             __syncthreads();
-            if (mirror) {
-                for (int L = Lz0; L <= k + 1; ++L) {
-                    if (!(g.bc_z == 1 && (L < 0 || L >= g.nz))) continue;
-                    const int Ls = L < 0 ? -L - 1 : 2 * g.nz - 1 - L;
-                    float* dst = nutp + (size_t)((L + 3) % 3) * S::NPS;
-                    const float* src = nutp + (size_t)((Ls + 3) % 3) * S::NPS;
-                    for (int e = tid; e < S::NPS; e += S::NT) dst[e] = src[e];
-                    if (CLOS == 1)
-                        for (int e = tid; e < S::NPS; e += S::NT) dst[e + S::KT_OFS] = src[e + S::KT_OFS];
-                }
-                __syncthreads();
-            }
-            // the thread's pair: nut row ty + 1, column 2 tx + 2
-            const int nb = (ty + 1) * S::NPW + 2 * tx + 2;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) N.p[d] = nutp + (size_t)((k - 1 + d + 3) % 3) * S::NPS + nb;
-        } else {
-            N.p[0] = N.p[1] = N.p[2] = nutp;
         }
 
-        if (active) {
-            F2 tu, tv, tw, tt;
-            sweep_point<R, 0, SGS, ANEL, UNI, false, CLOS == 1>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt);
-            const long long qi = iidx(g, i, j, k), q = pidx(g, i, j, k);
-            const F2 fdt(dt);
-            *reinterpret_cast<float2*>(a.us + qi) = (U(0, 0, 0) + fdt * tu).v;
-            *reinterpret_cast<float2*>(a.vs + qi) = (V(0, 0, 0) + fdt * tv).v;
-            *reinterpret_cast<float2*>(a.ws + qi) =
-                (g.bc_z == 1 && k == 0) ? make_float2(0.f, 0.f) : (W(0, 0, 0) + fdt * tw).v;
-            F2 tn = T(0, 0, 0) + fdt * tt;
-            if (a.stage) tn = rk_combine(a.ca, a.cb, F2(*reinterpret_cast<const float2*>(a.th0 + q)), tn);
-            *reinterpret_cast<float2*>(a.th_out + q) = tn.v;
+        for (int k = kbeg; k < kend && !failed; ++k) {
+            if (k > kbeg) {
+                // every thread is past level k-1: its planes and nut planes are
+                // free, and the nut plane of level k+1 is visible
+                if (__syncthreads_or(!ok)) { failed = true; kfail = k - 1; break; }
+            }
+            // the slot of level k-2 (read last by level k-1 or the prologue)
+            // takes level k-2+NS
+            const int Ln = k - 2 + S::NS;
+            if (tid == 0 && k - 2 >= Lfirst && Ln <= Llast) issue(Ln);
+            // the one new plane this level reads (the prologue waited for the rest)
+            const int Lneed = k + S::ZH;
+            if (Lneed <= Llast && (SGS || k > kbeg)) ok = mbar_wait_bounded(bars + slot_of(Lneed), parity_of(Lneed));
+
+            // the step-start theta of the pair (stages 2, 3), loaded before the
+            // eddy-viscosity pass so that its latency hides behind it
+            float2 th0v = make_float2(0.f, 0.f);
+            if (a.stage && active) th0v = *reinterpret_cast<const float2*>(a.th0 + pidx(g, i, j, k));
+
+            if (SGS && k + 2 <= kend) {
+                const int L = k + 2;
+                if (g.bc_z == 1 && L >= g.nz) {
+                    // the wall mirror: level nz takes level nz-1 (formed a level ago)
+                    float* dst = nut_plane(L);
+                    const float* srcp = nut_plane(2 * g.nz - 1 - L);
+                    for (int e = tid; e < S::NPS; e += S::NT) dst[e] = srcp[e];
+                    if (CLOS == 1)
+                        for (int e = tid; e < S::NPS; e += S::NT) dst[e + S::KT_OFS] = srcp[e + S::KT_OFS];
+                } else if (ok) {
+                    const float* sp[3] = {plane(L - 1), plane(L), plane(L + 1)};
+                    pair_nut_plane<CLOS, UNI, S>(m, a, g, L, sp, nut_plane(L), tid);
+                }
+            }
+
+            const float* lp[3] = {plane(k - 1) + vbase, plane(k) + vbase, plane(k + 1) + vbase};
+            const PairAcc<1, S::PW, 0> U{lp};
+            const PairAcc<1, S::PW, S::PSZA> V{lp};
+            const PairAcc<1, S::PW, 2 * S::PSZA> W{lp};
+            const PairAcc<1, S::PW, 3 * S::PSZA> T{lp};
+            PairNut<S::NPW> N;
+            if (SGS) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) N.p[d] = nut_plane(k - 1 + d) + nb;
+            } else {
+                N.p[0] = N.p[1] = N.p[2] = nutp;
+            }
+            if (active) {
+                F2 tu, tv, tw, tt;
+                sweep_point<R, 0, SGS, ANEL, UNI, false, CLOS == 1>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt);
+                const long long qi = iidx(g, i, j, k), q = pidx(g, i, j, k);
+                const F2 fdt(dt);
+                *reinterpret_cast<float2*>(a.us + qi) = (U(0, 0, 0) + fdt * tu).v;
+                *reinterpret_cast<float2*>(a.vs + qi) = (V(0, 0, 0) + fdt * tv).v;
+                *reinterpret_cast<float2*>(a.ws + qi) =
+                    (g.bc_z == 1 && k == 0) ? make_float2(0.f, 0.f) : (W(0, 0, 0) + fdt * tw).v;
+                F2 tn = T(0, 0, 0) + fdt * tt;
+                if (a.stage) tn = rk_combine(a.ca, a.cb, F2(th0v), tn);
+                *reinterpret_cast<float2*>(a.th_out + q) = tn.v;
+            }
         }
-    }
-    if (failed) {
-        if (tid == 0) atomicOr(err, AEO_ERR_FLAG_TMA);
-        for (int L = max(Lfirst, Lissued - S::NS + 1); L <= Lissued; ++L) mbar_wait_bounded(bars + slot_of(L), parity_of(L));
+        if (!failed && __syncthreads_or(!ok)) { failed = true; kfail = kend - 1; }   // the last level's wait
+        if (failed) {
+            // drain the copies this segment issued by level kfail (bounded) before the CTA exits
+            if (tid == 0) atomicOr(err, AEO_ERR_FLAG_TMA);
+            const int Lissued = min(Llast, max(Lfirst + S::NS - 1, kfail - 2 + S::NS));
+            for (int L = max(Lfirst, Lissued - S::NS + 1); L <= Lissued; ++L)
+                mbar_wait_bounded(bars + slot_of(L), parity_of(L));
+            break;
+        }
+        seq0 += (uint32_t)(Llast - Lfirst + 1);
     }
 }

@@ -152,6 +152,7 @@ struct Core : CoreBase {
     StepScalars* d_sc = nullptr;
     int rows_x = 1, tpx_y = 1, tpx_z = 1;
     int kchunk = 32;
+    int nsm = 148;           // SMs of the device (the persistent sweep's grid)
     double dz_min = 0.0;
     cudaGraphExec_t gexec[2][2] = {};   // [with CFL pick][parity of cur]
     CflParams cflp{};
@@ -465,6 +466,7 @@ struct Core : CoreBase {
         CKL();
         if (aeo_status e = make_tensor_maps()) return e;
         kchunk = std::min(g.nz, TileShape<R, 0, false>::KCH);
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cfg.device));
         CK(cudaStreamSynchronize(st));
         launches = 3 * (9 + dyn_launches());
         return AEO_OK;
@@ -637,7 +639,10 @@ struct Core : CoreBase {
         if constexpr (ADV == 0 && sizeof(R) == sizeof(float)) {
             if (pair) {
                 using PS = PairShape<SG>;
-                dim3 grid((g.nx + PS::TX - 1) / PS::TX, (g.ny + PS::TY - 1) / PS::TY, (g.nz + kchunk - 1) / kchunk);
+                // persistent: the SMs' worth of CTAs, each an equal range of (tile, level) items
+                const int ntx = (g.nx + PS::TX - 1) / PS::TX, nty = (g.ny + PS::TY - 1) / PS::TY;
+                const int items = ntx * nty * g.nz;
+                const dim3 grid((unsigned)std::min(items, PS::CTAS_PER_SM * nsm));
                 if constexpr (SG && !AN && UN) {
                     if (amd()) {
                         SweepArgs<R> b = a;
@@ -645,7 +650,7 @@ struct Core : CoreBase {
                         cudaFuncSetAttribute(sweep_pair_kernel<SG, AN, UN, 1>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PS::SMEM_AMD);
                         sweep_pair_kernel<SG, AN, UN, 1><<<grid, dim3(PS::TXT, PS::TY), PS::SMEM_AMD, st>>>(
-                            tmaps[s_in], b, kchunk, d_flag);
+                            tmaps[s_in], b, ntx, items, d_flag);
                         return;
                     }
                 }
@@ -654,14 +659,14 @@ struct Core : CoreBase {
                         cudaFuncSetAttribute(sweep_pair_kernel<SG, AN, UN, 2>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PS::SMEM);
                         sweep_pair_kernel<SG, AN, UN, 2><<<grid, dim3(PS::TXT, PS::TY), PS::SMEM, st>>>(
-                            tmaps[s_in], a, kchunk, d_flag);
+                            tmaps[s_in], a, ntx, items, d_flag);
                         return;
                     }
                 }
                 cudaFuncSetAttribute(sweep_pair_kernel<SG, AN, UN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)PS::SMEM);
-                sweep_pair_kernel<SG, AN, UN><<<grid, dim3(PS::TXT, PS::TY), PS::SMEM, st>>>(tmaps[s_in], a, kchunk,
-                                                                                           d_flag);
+                sweep_pair_kernel<SG, AN, UN><<<grid, dim3(PS::TXT, PS::TY), PS::SMEM, st>>>(tmaps[s_in], a, ntx,
+                                                                                           items, d_flag);
                 return;
             }
         }
