@@ -153,9 +153,25 @@ def box_solid_mask(grid: Grid, boxes) -> np.ndarray:
     the floor are solid (mark_solid! marks the interior only; the halo cells
     only decide the faces on the domain boundary, which are periodic partners
     or walls)."""
-    xc, yc, zc = (_subsamples(grid, a, 1) for a in range(3))
+    xc, yc = (_subsamples(grid, a, 1) for a in range(2))
     H = box_heights(grid, boxes, xc, yc)
-    return zc[:, None, None] < H[None, :, :]
+    return storage_zc(grid)[:, None, None] < H[None, :, :]
+
+
+def storage_zc(grid: Grid) -> np.ndarray:
+    """Cell-centre heights of every storage level: uniform, or on a stretched
+    column from its faces, the halo faces continued linearly (the halo
+    levels mirror the first and last cells, src/StretchedGrids.jl:345-360)."""
+    if grid.zf is None:
+        return _subsamples(grid, 2, 1)
+    H, nz = grid.halo[2], grid.nz
+    zf = np.empty(nz + 2 * H + 1)
+    zf[H:H + nz + 1] = grid.zf
+    for k in range(H - 1, -1, -1):
+        zf[k] = 2 * zf[k + 1] - zf[k + 2]
+    for k in range(H + nz + 1, nz + 2 * H + 1):
+        zf[k] = 2 * zf[k - 1] - zf[k - 2]
+    return 0.5 * (zf[:-1] + zf[1:])
 
 
 def staircase_geometry(grid: Grid, mask: np.ndarray, vol_min: float = 1e-3) -> CutCellGeometry:

@@ -59,8 +59,6 @@ class CoreSpec:
             self.solver = "fft" if self.grid.bc_z == PERIODIC else "column"
         if self.solver not in SOLVERS:
             raise ValueError(f"solver must be one of {list(SOLVERS)}, got {self.solver!r}")
-        if self.solver == "pcg" and (self.core != "boussinesq" or self.grid.stretched):
-            raise ValueError("the PCG pressure solver projects a Boussinesq domain of uniform spacing")
         if self.sponge_zstart is None:
             self.sponge_zstart = self.grid.origin[2] + self.grid.extent[2]
         if self.core == "anelastic":

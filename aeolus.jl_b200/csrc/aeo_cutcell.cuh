@@ -16,6 +16,19 @@
 // aperture 1 this is the projection of MGPreconditionedCG as the Boussinesq
 // pressure solver (the urban :mg_cg slot, src/components/urban/pressure_solver.jl:126).
 //
+// On the sound-proof core and on a stretched column the same projection
+// carries the density weights W_c, W_f (DensityWeightedPoissonSolver,
+// src/Anelastic.jl:734-793: W_c on x and y faces, W_f on z faces) and the
+// column metrics, in the symmetric form the multigrid hierarchy takes (one
+// spacing h_z = L_z / N_z per axis): every equation is multiplied by
+// dz_c[k] / h_z, so
+//   b     = dz_c/h_z (W_c (a u)_x + W_c (a v)_y) + (W_f a w)_z / h_z   (differences over the cell),
+//   A phi = sum of c (phi_nbr - phi) / h^2,  c = W_c a^2 dz_c / h_z (x, y faces), W_f a^2 h_z / dz_f (z faces),
+//   w     = w* - a (phi_k - phi_k-1) / dz_f   (u, v as before),
+// and after the projection the aperture- and density-weighted divergence
+// D(W a u) vanishes to the solve's tolerance (the a = 1 case is the direct
+// weighted solve's constraint, src/Anelastic.jl:987-1021).
+//
 // Apertures live in the face layout of aeolus_b200_mgpcg.h: ax (nx+1) per
 // row, ay (ny+1) rows per level, az (nz+1) levels; face index i is the west
 // (south, bottom) face of cell i.
@@ -23,8 +36,9 @@
 
 #include "aeo_common.cuh"
 
-// b = the aperture-weighted divergence of (u*, v*, w*) (interior arrays), in FP64
-template <typename R>
+// b = the aperture-weighted divergence of (u*, v*, w*) (interior arrays), in
+// FP64; ANEL: density-weighted, !UNI: on the stretched column (symmetric form)
+template <typename R, bool ANEL = false, bool UNI = true>
 __global__ void __launch_bounds__(256) cc_div_kernel(Geo g, const R* __restrict__ us, const R* __restrict__ vs,
                                                      const R* __restrict__ ws, const R* __restrict__ ax,
                                                      const R* __restrict__ ay, const R* __restrict__ az,
@@ -46,13 +60,21 @@ __global__ void __launch_bounds__(256) cc_div_kernel(Geo g, const R* __restrict_
     // in FP64 whatever R is: a fluid region the obstacles seal off from the rest
     // adds a null space whose right-hand side sums to zero only to the
     // rounding of this sum, and CG drifts along it unless that rounding is FP64's
-    b[q] = ((double)ae * ue - (double)aw * uw) * g.idx + ((double)an * vn - (double)as * vsv) * g.idy +
-           ((double)at * wt - (double)ab * wb) * g.idz;
+    if constexpr (!ANEL && UNI) {
+        b[q] = ((double)ae * ue - (double)aw * uw) * g.idx + ((double)an * vn - (double)as * vsv) * g.idy +
+               ((double)at * wt - (double)ab * wb) * g.idz;
+    } else {
+        const double wc = ANEL ? lvl(g.wc, k) : 1.0;
+        const double wfb = ANEL ? lvl(g.wf, k) : 1.0, wft = ANEL ? lvl(g.wf, k + 1) : 1.0;
+        const double sc = UNI ? 1.0 : g.idz / lvl(g.idzc, k);   // dz_c / h_z
+        b[q] = wc * sc * (((double)ae * ue - (double)aw * uw) * g.idx + ((double)an * vn - (double)as * vsv) * g.idy) +
+               (wft * ((double)at * wt) - wfb * ((double)ab * wb)) * g.idz;
+    }
 }
 
 // u = c(u* - a d(phi), u^n) on every face (0 on a blocked one), p = phi/dt;
 // c(x, s) = ca*s + cb*x in RK3 stages 2 and 3 (as correct_kernel)
-template <typename R>
+template <typename R, bool UNI = true>
 __global__ void __launch_bounds__(256) cc_correct_kernel(Geo g, const R* __restrict__ us, const R* __restrict__ vs,
                                                          const R* __restrict__ ws, const double* __restrict__ phi,
                                                          const R* __restrict__ ax, const R* __restrict__ ay,
@@ -74,7 +96,7 @@ __global__ void __launch_bounds__(256) cc_correct_kernel(Geo g, const R* __restr
     const R ab = az[q];
     R un = aw > R(0) ? us[q] - aw * R((pc - pw) * g.idx) : R(0);
     R vn = as > R(0) ? vs[q] - as * R((pc - ps) * g.idy) : R(0);
-    R wn = ab > R(0) ? ws[q] - ab * R((pc - pb) * g.idz) : R(0);
+    R wn = ab > R(0) ? ws[q] - ab * R((pc - pb) * (UNI ? g.idz : lvl(g.idzf, k))) : R(0);
     const long long qp = pidx(g, i, j, k);
     if (stage) {
         un = rk_combine(ca, cb, u0[qp], un);
@@ -99,8 +121,9 @@ __global__ void from_f64_kernel(long long n, const double* __restrict__ x, R* __
     if (q < n) y[q] = R(x[q]);
 }
 
-// per level: max |aperture-weighted divergence| of the padded state (halos filled)
-template <typename R>
+// per level: max |aperture-weighted divergence| of the padded state (halos
+// filled); ANEL: (1/W_c) D(W a u), the weighted constraint
+template <typename R, bool ANEL = false, bool UNI = true>
 __global__ void __launch_bounds__(256) cc_maxdiv_levels_kernel(Geo g, const R* __restrict__ u,
                                                                const R* __restrict__ v, const R* __restrict__ w,
                                                                const R* __restrict__ ax, const R* __restrict__ ay,
@@ -115,7 +138,13 @@ __global__ void __launch_bounds__(256) cc_maxdiv_levels_kernel(Geo g, const R* _
         const long long yr = (long long)g.nx * (j + (long long)(g.ny + 1) * k);
         const double du = ((double)ax[xr + i + 1] * (double)u[q + 1] - (double)ax[xr + i] * (double)u[q]) * g.idx;
         const double dv = ((double)ay[yr + g.nx + i] * (double)v[q + g.sy] - (double)ay[yr + i] * (double)v[q]) * g.idy;
-        const double dw = ((double)az[qi + (long long)g.nx * g.ny] * (double)w[q + g.sz] - (double)az[qi] * (double)w[q]) * g.idz;
+        const double idz = UNI ? g.idz : lvl(g.idzc, k);
+        double dw;
+        if (ANEL)
+            dw = (lvl(g.wf, k + 1) * ((double)az[qi + (long long)g.nx * g.ny] * (double)w[q + g.sz]) -
+                  lvl(g.wf, k) * ((double)az[qi] * (double)w[q])) * idz / lvl(g.wc, k);
+        else
+            dw = ((double)az[qi + (long long)g.nx * g.ny] * (double)w[q + g.sz] - (double)az[qi] * (double)w[q]) * idz;
         acc = fmax(acc, fabs(du + dv + dw));
     }
     red[threadIdx.x] = acc;

@@ -243,13 +243,41 @@ __global__ void __launch_bounds__(256) maxdiv_levels_kernel(Geo g, const R* __re
     if (threadIdx.x == 0) part[k] = red[0];
 }
 
-// non-finite check of the state (status word for the host)
+// The loop of the multi-step graph: a conditional WHILE node whose body is two
+// RK3 steps runs while step pairs remain (the count in device memory).
+__global__ void steps_set_kernel(int* left, int pairs) { *left = pairs; }
+__global__ void steps_begin_kernel(const int* left, cudaGraphConditionalHandle h) {
+    cudaGraphSetConditional(h, *left > 0 ? 1u : 0u);
+}
+__global__ void steps_next_kernel(int* left, cudaGraphConditionalHandle h) {
+    const int n = *left - 1;
+    *left = n;
+    cudaGraphSetConditional(h, n > 0 ? 1u : 0u);
+}
+
+// non-finite check of the four state fields (status word for the host): a
+// grid-stride pass over the interiors, N = 16/sizeof(R) x-consecutive values a
+// 16-byte load; one flag update per block
 template <typename R>
-__global__ void finite_check_kernel(Geo g, const R* __restrict__ a, int* __restrict__ flag) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-    if (i >= g.nx) return;
-    R v = a[pidx(g, i, j, k)];
-    if (!isfinite((double)v)) atomicOr(flag, 1);
+__global__ void __launch_bounds__(256) finite_check_kernel(Geo g, const R* __restrict__ f0, const R* __restrict__ f1,
+                                                           const R* __restrict__ f2, const R* __restrict__ f3,
+                                                           int* __restrict__ flag) {
+    constexpr int N = Vec16<R>::N;
+    const long long per = g.nin / N;   // vectors of one field (nx is a multiple of N)
+    const int lnx = __ffs(g.nx) - 1, lny = __ffs(g.ny) - 1;
+    bool bad = false;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < 4 * per;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int f = (int)(t / per);
+        const long long qi = (t - f * per) * N;
+        const int i0 = (int)(qi & (g.nx - 1)), j = (int)((qi >> lnx) & (g.ny - 1)), k = (int)(qi >> (lnx + lny));
+        const R* a = f == 0 ? f0 : (f == 1 ? f1 : (f == 2 ? f2 : f3));
+        R v[N];
+        vld(a + pidx(g, i0, j, k), v);
+#pragma unroll
+        for (int n = 0; n < N; ++n) bad = bad || !isfinite(v[n]);
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
 }
 
 // ---- Philox4x32-10 (src/Backends.jl:1607-1640) ------------------------------------

@@ -153,8 +153,16 @@ struct Core : CoreBase {
     int rows_x = 1, tpx_y = 1, tpx_z = 1;
     int kchunk = 32;
     int nsm = 148;           // SMs of the device (the persistent sweep's grid)
+    // interior column metrics and weights on the host (the PCG operator's coefficients):
+    // dz_c per level, dz_f per face, W_c, W_f (1 on the Boussinesq core)
+    std::vector<double> h_dzc, h_dzf, h_wc, h_wf;
     double dz_min = 0.0;
     cudaGraphExec_t gexec[2][2] = {};   // [with CFL pick][parity of cur]
+    // n steps as one launch: a WHILE node over pairs of steps [parity of cur],
+    // its body captured on st_loop, the pair count in d_steps
+    cudaGraphExec_t gmulti[2] = {};
+    cudaStream_t st_loop = nullptr;
+    int* d_steps = nullptr;
     CflParams cflp{};
     bool cflp_set = false;
     bool uni = true, sgs = false, anel = false;
@@ -199,6 +207,7 @@ struct Core : CoreBase {
         drop_graphs();
         if (mg) aeo_mg_destroy(mg);
         for (void* p : allocs) cudaFree(p);
+        if (st_loop) cudaStreamDestroy(st_loop);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -206,6 +215,8 @@ struct Core : CoreBase {
         for (auto& a : gexec)
             for (auto& e : a)
                 if (e) { cudaGraphExecDestroy(e); e = nullptr; }
+        for (auto& e : gmulti)
+            if (e) { cudaGraphExecDestroy(e); e = nullptr; }
     }
 
     template <typename T>
@@ -227,6 +238,7 @@ struct Core : CoreBase {
     aeo_status init(const double* zfi, const double* wc, const double* wf, const double* thf) override {
         const aeo_config& c = cfg;
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&st_loop, cudaStreamNonBlocking));
         uni = !c.stretched;
         sgs = c.c_s != 0.0;
         anel = c.core == AEO_CORE_ANELASTIC;
@@ -262,6 +274,14 @@ struct Core : CoreBase {
             dzf[0] = dzc[0];
             for (int k = 1; k < NZ; ++k) dzf[k] = zc[k] - zc[k - 1];
             dzf[NZ] = dzc[NZ - 1];
+        }
+        h_dzc.assign(dzc.begin() + Hz, dzc.begin() + Hz + Nz);
+        h_dzf.assign(dzf.begin() + Hz, dzf.begin() + Hz + Nz + 1);
+        h_wc.assign(Nz, 1.0);
+        h_wf.assign(Nz + 1, 1.0);
+        if (anel) {
+            for (int k = 0; k < Nz; ++k) h_wc[k] = wc[Hz + k];
+            for (int k = 0; k <= Nz; ++k) h_wf[k] = wf[Hz + k];
         }
         dz_min = dzc[Hz];
         for (int k = Hz; k < Hz + Nz; ++k) dz_min = std::min(dz_min, dzc[k]);
@@ -461,6 +481,7 @@ struct Core : CoreBase {
             dyn_d2 = std::pow(g.dx * g.dy * g.dz, 2.0 / 3.0);
         }
         if (aeo_status e = alloc(&d_flag, 1)) return e;
+        if (aeo_status e = alloc(&d_steps, 1)) return e;
         if (aeo_status e = alloc(&d_sc, 1)) return e;
         set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->one, 1.0);
         CKL();
@@ -492,12 +513,26 @@ struct Core : CoreBase {
                 a[2][(size_t)Nz * Nx * Ny + q] = 0.0;
             }
         R* dst[3] = {apx, apy, apz};
+        // c = a^2 on the uniform Boussinesq column; with density weights or a
+        // stretched column, the symmetric form (aeo_cutcell.cuh): W_c a^2 dz_c/h_z
+        // on x and y faces, W_f a^2 h_z/dz_f on z faces
+        const bool weighted = anel || !uni;
+        const size_t rowx = (size_t)(Nx + 1) * Ny, rowy = (size_t)Nx * (Ny + 1), rowz = (size_t)Nx * Ny;
         for (int d = 0; d < 3; ++d) {
             std::vector<R> ar(n[d]);
             c2[d].resize(n[d]);
             for (size_t q = 0; q < n[d]; ++q) {
                 ar[q] = R(a[d][q]);
                 c2[d][q] = a[d][q] * a[d][q];
+                if (weighted) {
+                    if (d < 2) {
+                        const int k = (int)(q / (d == 0 ? rowx : rowy));
+                        c2[d][q] *= h_wc[k] * (h_dzc[k] / g.dz);
+                    } else {
+                        const int k = (int)(q / rowz);
+                        c2[d][q] *= h_wf[k] * (g.dz / h_dzf[k]);
+                    }
+                }
             }
             CK(cudaMemcpyAsync(dst[d], ar.data(), n[d] * sizeof(R), cudaMemcpyHostToDevice, st));
             CK(cudaStreamSynchronize(st));
@@ -720,6 +755,9 @@ struct Core : CoreBase {
         if (pcg) {
             const unsigned gb = (unsigned)((g.nin + 255) / 256);
             if (src) to_f64_kernel<R><<<gb, 256, 0, st>>>(g.nin, src, mg_b);
+            else if (anel && uni) cc_div_kernel<R, true, true><<<gb, 256, 0, st>>>(g, Q[0], Q[1], Q[2], apx, apy, apz, mg_b);
+            else if (anel) cc_div_kernel<R, true, false><<<gb, 256, 0, st>>>(g, Q[0], Q[1], Q[2], apx, apy, apz, mg_b);
+            else if (!uni) cc_div_kernel<R, false, false><<<gb, 256, 0, st>>>(g, Q[0], Q[1], Q[2], apx, apy, apz, mg_b);
             else cc_div_kernel<R><<<gb, 256, 0, st>>>(g, Q[0], Q[1], Q[2], apx, apy, apz, mg_b);
             CKL();
             mark(AEO_K_DIV_FFTX);
@@ -782,9 +820,14 @@ struct Core : CoreBase {
     aeo_status correct(R** out, int stage, R ca, R cb, const double* dtp, int s_u0) {
         R** u0 = P[s_u0];
         if (pcg) {
-            cc_correct_kernel<R><<<(unsigned)((g.nin + 255) / 256), 256, 0, st>>>(
-                g, Q[0], Q[1], Q[2], mg_x, apx, apy, apz, u0[0], u0[1], u0[2], out[0], out[1], out[2], pres, dtp, ca,
-                cb, stage);
+            if (uni)
+                cc_correct_kernel<R, true><<<(unsigned)((g.nin + 255) / 256), 256, 0, st>>>(
+                    g, Q[0], Q[1], Q[2], mg_x, apx, apy, apz, u0[0], u0[1], u0[2], out[0], out[1], out[2], pres, dtp,
+                    ca, cb, stage);
+            else
+                cc_correct_kernel<R, false><<<(unsigned)((g.nin + 255) / 256), 256, 0, st>>>(
+                    g, Q[0], Q[1], Q[2], mg_x, apx, apy, apz, u0[0], u0[1], u0[2], out[0], out[1], out[2], pres, dtp,
+                    ca, cb, stage);
             CKL();
             return AEO_OK;
         }
@@ -906,9 +949,84 @@ struct Core : CoreBase {
         return AEO_OK;
     }
 
+    // The graph of n steps: WHILE(pairs left) { step cur -> cur^1; step cur^1 -> cur }.
+    aeo_status multi_graph_for(cudaGraphExec_t* out) {
+        cudaGraphExec_t& ge = gmulti[cur];
+        if (!ge) {
+            if (pcg) CK(cudaDeviceSynchronize());   // as graph_for: the handle's set-up is complete
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+            aeo_status e = AEO_OK;
+            cudaError_t ce = cudaSuccess;
+            cudaStreamCaptureStatus cs;
+            cudaGraph_t g0 = nullptr;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t nd = 0;
+            cudaGraphConditionalHandle h{};
+            cudaGraphNode_t node{};
+            ce = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g0, nullptr, nullptr);
+            if (ce == cudaSuccess) ce = cudaGraphConditionalHandleCreate(&h, g0, 0, cudaGraphCondAssignDefault);
+            if (ce == cudaSuccess) {
+                steps_begin_kernel<<<1, 1, 0, st>>>(d_steps, h);
+                ce = cudaGetLastError();
+            }
+            if (ce == cudaSuccess) ce = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g0, &deps, &nd);
+            cudaGraphNodeParams cp = {};
+            if (ce == cudaSuccess) {
+                cp.type = cudaGraphNodeTypeConditional;
+                cp.conditional.handle = h;
+                cp.conditional.type = cudaGraphCondTypeWhile;
+                cp.conditional.size = 1;
+                std::vector<cudaGraphNode_t> dv(deps, deps + nd);
+                ce = cudaGraphAddNode(&node, g0, dv.data(), dv.size(), &cp);
+            }
+            if (ce == cudaSuccess)
+                ce = cudaStreamBeginCaptureToGraph(st_loop, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                   cudaStreamCaptureModeRelaxed);
+            if (ce == cudaSuccess) {
+                // the body: every launch of the two steps goes to st_loop
+                std::swap(st, st_loop);
+                e = enqueue_rk3(cur, false);
+                if (!e) e = enqueue_rk3(cur ^ 1, false);
+                if (!e) {
+                    steps_next_kernel<<<1, 1, 0, st>>>(d_steps, h);
+                    if (cudaGetLastError() != cudaSuccess) { fail("multi-step graph: loop kernel"); e = AEO_ERR_CUDA; }
+                }
+                std::swap(st, st_loop);
+                cudaGraph_t bg = nullptr;
+                cudaError_t be = cudaStreamEndCapture(st_loop, &bg);
+                if (be != cudaSuccess && !e) { fail(std::string("multi-step body capture: ") + cudaGetErrorString(be)); e = AEO_ERR_CUDA; }
+                if (!e) ce = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+            }
+            cudaGraph_t gr = nullptr;
+            cudaError_t ee = cudaStreamEndCapture(st, &gr);
+            if (!e && ce != cudaSuccess) { fail(std::string("multi-step graph: ") + cudaGetErrorString(ce)); e = AEO_ERR_CUDA; }
+            if (!e && ee != cudaSuccess) { fail(std::string("multi-step graph capture: ") + cudaGetErrorString(ee)); e = AEO_ERR_CUDA; }
+            if (e) { if (gr) cudaGraphDestroy(gr); return e; }
+            cudaError_t ie = cudaGraphInstantiate(&ge, gr, 0);
+            cudaGraphDestroy(gr);
+            if (ie != cudaSuccess) { ge = nullptr; fail(std::string("multi-step graph instantiate: ") + cudaGetErrorString(ie)); return AEO_ERR_CUDA; }
+        }
+        *out = ge;
+        return AEO_OK;
+    }
+
     aeo_status step_rk3(double dt, int n, bool sync) override {
         set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt, dt);
         CKL();
+        if (n >= 2) {
+            // the pairs of steps as one launch of the multi-step graph
+            cudaGraphExec_t ge;
+            if (aeo_status e = multi_graph_for(&ge)) return e;
+            steps_set_kernel<<<1, 1, 0, st>>>(d_steps, n / 2);
+            CKL();
+            if (pcg)
+                if (aeo_status e = aeo_mg_order_before(mg, st)) {
+                    fail(std::string("the MG-PCG pressure solve: ") + aeo_mg_last_error(mg));
+                    return e;
+                }
+            CK(cudaGraphLaunch(ge, st));
+            n -= 2 * (n / 2);   // the state is back in set cur
+        }
         for (int s = 0; s < n; ++s) {
             if (aeo_status e = launch_step(false)) return e;
             cur ^= 1;
@@ -1081,11 +1199,10 @@ struct Core : CoreBase {
     }
 
     aeo_status check_finite() {
-        dim3 gb((g.nx + 127) / 128, g.ny, g.nz);
-        for (int f = 0; f < 4; ++f) {
-            finite_check_kernel<R><<<gb, 128, 0, st>>>(g, P[cur][f], d_flag);
-            CKL();
-        }
+        const long long vecs = 4 * (g.nin / Vec16<R>::N);
+        const unsigned nb = (unsigned)std::min<long long>((vecs + 255) / 256, 8LL * nsm);
+        finite_check_kernel<R><<<nb, 256, 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], P[cur][3], d_flag);
+        CKL();
         int h = 0;
         CK(cudaMemcpyAsync(&h, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
@@ -1336,7 +1453,10 @@ struct Core : CoreBase {
     aeo_status max_divergence(double* out) override {
         R** s = P[cur];
         if (pcg) {
-            cc_maxdiv_levels_kernel<R><<<g.nz, 256, 0, st>>>(g, s[0], s[1], s[2], apx, apy, apz, d_part);
+            if (anel && uni) cc_maxdiv_levels_kernel<R, true, true><<<g.nz, 256, 0, st>>>(g, s[0], s[1], s[2], apx, apy, apz, d_part);
+            else if (anel) cc_maxdiv_levels_kernel<R, true, false><<<g.nz, 256, 0, st>>>(g, s[0], s[1], s[2], apx, apy, apz, d_part);
+            else if (!uni) cc_maxdiv_levels_kernel<R, false, false><<<g.nz, 256, 0, st>>>(g, s[0], s[1], s[2], apx, apy, apz, d_part);
+            else cc_maxdiv_levels_kernel<R><<<g.nz, 256, 0, st>>>(g, s[0], s[1], s[2], apx, apy, apz, d_part);
             CKL();
             std::vector<double> h((size_t)g.nz);
             CK(cudaMemcpyAsync(h.data(), d_part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1401,11 +1521,8 @@ static aeo_status validate(const aeo_config* c, const double* zf, const double* 
         if (c->bc_z != AEO_BC_WALL) { *m = "the column solver needs walls in z"; return AEO_ERR_ARGUMENT; }
         if (c->nz > AEO_COLUMN_NZ_MAX) { *m = "the column solver needs nz <= " + std::to_string(AEO_COLUMN_NZ_MAX); return AEO_ERR_ARGUMENT; }
     } else if (c->solver == AEO_SOLVER_PCG) {
-        if (c->stretched) { *m = "the PCG pressure solver needs a uniform z (one multigrid spacing per axis)"; return AEO_ERR_ARGUMENT; }
-        if (c->core != AEO_CORE_BOUSSINESQ) {
-            *m = "the PCG pressure solver projects the Boussinesq core (the sound-proof cores take the direct weighted solver)";
-            return AEO_ERR_ARGUMENT;
-        }
+        // any core and column: the density weights and the stretched metric
+        // enter the multigrid operator in its symmetric form (aeo_cutcell.cuh)
     } else { *m = "unknown solver"; return AEO_ERR_ARGUMENT; }
     if (c->advection < 0 || c->advection > 2) { *m = "unknown advection scheme"; return AEO_ERR_ARGUMENT; }
     if (c->advection != AEO_ADV_CENTRED && (c->stretched || c->core == AEO_CORE_ANELASTIC)) {

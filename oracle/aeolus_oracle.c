@@ -1245,7 +1245,12 @@ int oc_apply_poisson_operator(oc_sim* s, const double* phi, double* out) {
 /* The cut-cell projection (solver = PCG; src/CutCell.jl:602-700, 852-880):
  * b = sum over the faces of (+-) a u* / h (u* in the storage arrays, halos
  * filled), phi = A^-1 b by MGPreconditionedCG with the a^2 face coefficients
- * (src/Multigrid.jl:893-967) into cgx. */
+ * (src/Multigrid.jl:893-967) into cgx.  On the sound-proof core the flux
+ * carries the density weights of DensityWeightedPoissonSolver
+ * (src/Anelastic.jl:734-793: W_c on x and y faces, W_f on z faces), and on a
+ * stretched column the z-difference is over dz_c; the equation of cell k is
+ * taken times dz_c[k] / h_z (the symmetric form of the operator built in
+ * oc_set_apertures), h_z = L_z / N_z. */
 static void cc_solve(oc_sim* s) {
     const oc_params* P = &s->p;
     int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
@@ -1260,9 +1265,19 @@ static void cc_solve(oc_sim* s) {
                 double aw = s->apx[xr + i], ae = s->apx[xr + i + 1];
                 double as = s->apy[yr + i], an = s->apy[yr + Nx + i];
                 double ab = s->apz[qi], at = s->apz[qi + pl];
-                s->src[qi] = (ae * A(s->u, I + 1, J, K) - aw * A(s->u, I, J, K)) * s->idx +
-                             (an * A(s->v, I, J + 1, K) - as * A(s->v, I, J, K)) * s->idy +
-                             (at * A(s->w, I, J, K + 1) - ab * A(s->w, I, J, K)) * s->idz;
+                if (P->core != OC_CORE_ANELASTIC && s->uniform) {
+                    s->src[qi] = (ae * A(s->u, I + 1, J, K) - aw * A(s->u, I, J, K)) * s->idx +
+                                 (an * A(s->v, I, J + 1, K) - as * A(s->v, I, J, K)) * s->idy +
+                                 (at * A(s->w, I, J, K + 1) - ab * A(s->w, I, J, K)) * s->idz;
+                } else {
+                    double wcc = P->core == OC_CORE_ANELASTIC ? s->wc[K] : 1.0;
+                    double wfb = P->core == OC_CORE_ANELASTIC ? s->wf[K] : 1.0;
+                    double wft = P->core == OC_CORE_ANELASTIC ? s->wf[K + 1] : 1.0;
+                    double sc = s->uniform ? 1.0 : s->dzc[K] / s->dz;
+                    s->src[qi] = wcc * sc * ((ae * A(s->u, I + 1, J, K) - aw * A(s->u, I, J, K)) * s->idx +
+                                             (an * A(s->v, I, J + 1, K) - as * A(s->v, I, J, K)) * s->idy) +
+                                 (wft * (at * A(s->w, I, J, K + 1)) - wfb * (ab * A(s->w, I, J, K))) / s->dz;
+                }
             }
     ocg_solve(s->cg, s->src, s->cgx, &s->cg_st);
 }
@@ -1290,7 +1305,7 @@ static void cc_correct(oc_sim* s, double dt, int stage, double ca, double cb, in
                 double ab = s->apz[qi];
                 double un = aw > 0 ? s->u[q] - aw * ((pc - pw) * s->idx) : 0.0;
                 double vn = as > 0 ? s->v[q] - as * ((pc - ps) * s->idy) : 0.0;
-                double wn = ab > 0 ? s->w[q] - ab * ((pc - pb) * s->idz) : 0.0;
+                double wn = ab > 0 ? s->w[q] - ab * ((pc - pb) * m_idzf(s, k + Hz)) : 0.0;
                 double tn = with_theta ? s->th[q] + dt * s->tt[q] : s->th[q];
                 if (stage) {
                     un = ca * s->u0[q] + cb * un;
@@ -1720,9 +1735,14 @@ double oc_max_divergence(oc_sim* s) {
                     int64_t qi = (i - Hx) + (int64_t)Nx * ((j - Hy) + (int64_t)Ny * (k - Hz));
                     int64_t xr = (int64_t)(Nx + 1) * ((j - Hy) + (int64_t)Ny * (k - Hz));
                     int64_t yr = (int64_t)Nx * ((j - Hy) + (int64_t)(Ny + 1) * (k - Hz));
+                    double dw;
+                    if (P->core == OC_CORE_ANELASTIC)
+                        dw = (s->wf[k + 1] * (s->apz[qi + (int64_t)Nx * Ny] * A(s->w, i, j, k + 1)) -
+                              s->wf[k] * (s->apz[qi] * A(s->w, i, j, k))) * m_idz(s, k) / s->wc[k];
+                    else
+                        dw = (s->apz[qi + (int64_t)Nx * Ny] * A(s->w, i, j, k + 1) - s->apz[qi] * A(s->w, i, j, k)) * m_idz(s, k);
                     d = (s->apx[xr + i - Hx + 1] * A(s->u, i + 1, j, k) - s->apx[xr + i - Hx] * A(s->u, i, j, k)) * s->idx +
-                        (s->apy[yr + Nx + i - Hx] * A(s->v, i, j + 1, k) - s->apy[yr + i - Hx] * A(s->v, i, j, k)) * s->idy +
-                        (s->apz[qi + (int64_t)Nx * Ny] * A(s->w, i, j, k + 1) - s->apz[qi] * A(s->w, i, j, k)) * s->idz;
+                        (s->apy[yr + Nx + i - Hx] * A(s->v, i, j + 1, k) - s->apy[yr + i - Hx] * A(s->v, i, j, k)) * s->idy + dw;
                 } else {
                     d = s->wc ? wdiv_at(s, s->u, s->v, s->w, i, j, k) / s->wc[k] : div_at(s, s->u, s->v, s->w, i, j, k);
                 }
@@ -1748,7 +1768,6 @@ oc_sim* oc_create(const oc_params* p, const double* zfi, const double* wc, const
     if (p->solver == OC_SOLVER_FFT && p->bc_z != OC_BC_PERIODIC) return NULL;
     if (p->solver == OC_SOLVER_COLUMN && p->bc_z != OC_BC_WALL) return NULL;
     if (p->stretched && (!zfi || p->bc_z != OC_BC_WALL)) return NULL;
-    if (p->solver == OC_SOLVER_PCG && (p->stretched || p->core != OC_CORE_BOUSSINESQ)) return NULL;
     if ((p->sgs_model == OC_SGS_VREMAN || p->sgs_model == OC_SGS_SIGMA || p->sgs_model == OC_SGS_AMD ||
          p->sgs_model == OC_SGS_DYNAMIC) && p->stretched)
         return NULL;
@@ -1902,6 +1921,22 @@ int oc_set_apertures(oc_sim* s, const double* ax, const double* ay, const double
         }
     for (int d = 0; d < 3; ++d)
         for (int64_t q = 0; q < n[d]; ++q) c2[d][q] = a[d][q] * a[d][q];
+    if (P->core == OC_CORE_ANELASTIC || !s->uniform) {
+        /* the symmetric form of the density-weighted operator on the column:
+         * W_c a^2 dz_c / h_z on x and y faces, W_f a^2 h_z / dz_f on z faces */
+        int Hz = P->hz, anel = P->core == OC_CORE_ANELASTIC;
+        for (int d = 0; d < 2; ++d) {
+            int64_t row = d == 0 ? (int64_t)(Nx + 1) * Ny : (int64_t)Nx * (Ny + 1);
+            for (int64_t q = 0; q < n[d]; ++q) {
+                int K = Hz + (int)(q / row);
+                c2[d][q] *= (anel ? s->wc[K] : 1.0) * (s->dzc[K] / s->dz);
+            }
+        }
+        for (int64_t q = 0; q < n[2]; ++q) {
+            int K = Hz + (int)(q / ((int64_t)Nx * Ny));
+            c2[2][q] *= (anel ? s->wf[K] : 1.0) * (s->dz / s->dzf[K]);
+        }
+    }
     ocg* cg = NULL;
     if (!bad) {
         ocg_params prm = {Nx, Ny, Nz, s->dx, s->dy, s->dz, OCG_BC_PERIODIC, OCG_BC_PERIODIC,

@@ -95,10 +95,17 @@ def test_spec_validation():
     assert CoreSpec(grid=regular_grid((16, 16, 16), (1, 1, 1), bc_z="wall")).solver == "column"
 
 
-def test_pcg_solver_needs_a_uniform_boussinesq_domain():
+def test_pcg_solver_takes_any_core_and_column():
+    """The cut-cell MG-PCG projection carries the density weights and the
+    stretched metric in its operator, so every core and column accepts it;
+    WENO advection stays on uniform Boussinesq grids."""
     from aeolus_b200 import CoreSpec, regular_grid, stretched_grid, tanh_faces
+    from aeolus_b200.reference_state import anelastic_profiles, exponential_density
     g = regular_grid((32, 32, 16), (64.0, 64.0, 32.0), halo=(3, 3, 3), bc_z="wall")
     assert CoreSpec(grid=g, solver="pcg").solver == "pcg"
     gs = stretched_grid((32, 32, 16), (64.0, 64.0, 400.0), tanh_faces(16, 400.0, 1.5))
+    assert CoreSpec(grid=gs, solver="pcg").solver == "pcg"
+    prof = anelastic_profiles(gs, exponential_density(gs), 300.0 + 0 * gs.znodes("c"))
+    assert CoreSpec(grid=gs, core="anelastic", solver="pcg", wc=prof["wc"], wf=prof["wf"]).solver == "pcg"
     with pytest.raises(ValueError):
-        CoreSpec(grid=gs, solver="pcg")
+        CoreSpec(grid=gs, solver="pcg", advection="weno_js5")
