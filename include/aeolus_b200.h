@@ -59,7 +59,7 @@ typedef struct {
     int32_t core;              /* AEO_CORE_*                                   */
     int32_t advection;         /* AEO_ADV_* (momentum and theta)               */
     int32_t solver;            /* AEO_SOLVER_FFT (triply periodic), COLUMN, or
-                                  PCG (Boussinesq, uniform z: aeo_set_pcg)      */
+                                  PCG (any core and column: aeo_set_pcg)        */
     int32_t precision;         /* AEO_PREC_*                                   */
     double nu;                 /* molecular viscosity / diffusivity (0 = off)  */
     double theta0;             /* Boussinesq reference theta (0 = no buoyancy) */
@@ -131,7 +131,10 @@ aeo_status aeo_get_field_f32(aeo_sim* h, int32_t field, float* host);
 
 /* nsteps projected SSP-RK3 steps of size dt: step_rk3! of the Boussinesq
  * core (src/Simulations.jl:843-904) or of the sound-proof core
- * (src/Anelastic.jl:1905-1948).  The whole step is one CUDA graph. */
+ * (src/Anelastic.jl:1905-1948).  The whole step is one CUDA graph; with
+ * nsteps >= 2 the pairs of steps run as one launch of a graph whose
+ * conditional WHILE node loops over a two-step body (an odd last step is
+ * launched on its own), bit-identical to single steps. */
 aeo_status aeo_step_rk3(aeo_sim* h, double dt, int32_t nsteps);
 
 /* nsteps forward-Euler projection steps: step! (src/Simulations.jl:481-650,
@@ -306,11 +309,17 @@ aeo_status aeo_pressure_solve_column_noalloc(int32_t nx, int32_t ny, int32_t nz,
  * src/CutCell.jl:602-623) and corrects with the aperture-scaled gradient
  * (cutcell_gradient_x/y/z!, :666-700), so a blocked face carries no velocity
  * (apply_cutcell_velocity_bc!, :852-880) and the aperture-weighted
- * divergence after a projection is the solve's residual.  Every solve runs
- * to ||r|| <= tol ||b|| or maxit iterations (defaults 1e-8, 200); steps of
- * such a domain are launched kernel by kernel (the solve is itself a graph
- * with a device-side loop).  aeo_max_divergence reports the aperture-weighted
- * divergence on these domains.  No reference counterpart for the learned
+ * divergence after a projection is the solve's residual.  On the
+ * sound-proof core the fluxes carry the density weights of
+ * DensityWeightedPoissonSolver (src/Anelastic.jl:734-793: W_c on x and y
+ * faces, W_f on z faces; the :density_weighted_cg slot,
+ * src/components/urban/pressure_solver.jl:182-191) and on a stretched column
+ * the z metrics, both in the symmetric form the multigrid hierarchy takes
+ * (every equation times dz_c/h_z, h_z = lz/nz).  Every solve runs to
+ * ||r|| <= tol ||b|| or maxit iterations (defaults 1e-8, 200); the solve's
+ * CG loop is a conditional node inside the step's graph.  aeo_max_divergence
+ * reports the aperture-weighted (density-weighted) divergence on these
+ * domains.  No reference counterpart for the learned
  * preconditioner (aeo_pcg_set_learned: the U-Net of aeolus_b200_unet.h with
  * its stagnation fallback to the cycle; net NULL switches back). */
 struct aeo_unet;
