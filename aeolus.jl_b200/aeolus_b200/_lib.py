@@ -26,6 +26,8 @@ SYMBOLS = (
     "aeo_unet_param_count", "aeo_unet_create", "aeo_unet_destroy", "aeo_unet_set_params", "aeo_unet_get_params",
     "aeo_unet_set_mask", "aeo_unet_set_out_scale", "aeo_unet_apply", "aeo_unet_gradients", "aeo_unet_train_step",
     "aeo_unet_activation", "aeo_unet_profile", "aeo_unet_last_error",
+    "aeo_ghost_create", "aeo_ghost_destroy", "aeo_ghost_reconstruct", "aeo_ghost_reconstruct_host",
+    "aeo_ghost_wall_stress", "aeo_ghost_wall_stress_host", "aeo_ghost_last_error",
 )
 
 
@@ -174,20 +176,31 @@ def load():
     lib.aeo_unet_profile.argtypes = [P, C.c_int32, C.c_int32, D]
     lib.aeo_unet_last_error.argtypes = [P]
     lib.aeo_unet_last_error.restype = C.c_char_p
+    I64 = C.POINTER(C.c_int64)
+    lib.aeo_ghost_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int64, I64, I64, D, D, D, D,
+                                     C.POINTER(C.c_uint8), C.c_int32, C.POINTER(P)]
+    lib.aeo_ghost_destroy.argtypes = [P]
+    lib.aeo_ghost_reconstruct.argtypes = [P, P, C.c_int32, C.c_int32, C.c_double, C.c_double, P]
+    lib.aeo_ghost_reconstruct_host.argtypes = [P, D, C.c_int32, C.c_double, C.c_double]
+    lib.aeo_ghost_wall_stress.argtypes = [P, P, P, P, P, P, P, C.c_int32, D, C.c_double, C.c_double, P, P, P]
+    lib.aeo_ghost_wall_stress_host.argtypes = [P, D, D, D, D, D, D, C.c_int32, D, C.c_double, C.c_double, D, D]
+    lib.aeo_ghost_last_error.argtypes = [P]
+    lib.aeo_ghost_last_error.restype = C.c_char_p
     for s in SYMBOLS:
         f = getattr(lib, s)
         if s not in ("aeo_stream", "aeo_last_error", "aeo_version", "aeo_mg_last_error", "aeo_unet_last_error",
-                     "aeo_unet_param_count"):
+                     "aeo_unet_param_count", "aeo_ghost_last_error"):
             f.restype = C.c_int32
     _lib = lib
     return lib
 
 
-def check(status: int, handle=None, mg=False, unet=False):
+def check(status: int, handle=None, mg=False, unet=False, ghost=False):
     if status == 0:
         return
     lib = load()
-    f = lib.aeo_unet_last_error if unet else (lib.aeo_mg_last_error if mg else lib.aeo_last_error)
+    f = (lib.aeo_ghost_last_error if ghost else lib.aeo_unet_last_error if unet else
+         (lib.aeo_mg_last_error if mg else lib.aeo_last_error))
     msg = f(handle).decode(errors="replace")
     if status == 3:
         raise NumericalFailure(status, msg)

@@ -26,6 +26,7 @@ ax[k, j, i] is the west face of cell i, ay the south face, az the bottom.
 from __future__ import annotations
 
 from dataclasses import dataclass
+from typing import Callable, Optional
 
 import numpy as np
 
@@ -45,6 +46,16 @@ class CutCellGeometry:
     is_small: np.ndarray
     vol_min: float
     nsub: int
+    # the small cells' merge partners (flat storage index, -1 none), the cut
+    # cells, and from a level set its cell-centre values, the unit normals
+    # into the fluid and the wetted area of every cut cell
+    merge_target: Optional[np.ndarray] = None
+    is_cut: Optional[np.ndarray] = None
+    phi: Optional[np.ndarray] = None
+    nx: Optional[np.ndarray] = None
+    ny: Optional[np.ndarray] = None
+    nz: Optional[np.ndarray] = None
+    area: Optional[np.ndarray] = None
 
     @property
     def fluid_interior(self) -> np.ndarray:
@@ -194,8 +205,88 @@ def staircase_geometry(grid: Grid, mask: np.ndarray, vol_min: float = 1e-3) -> C
     return finalize_geometry(grid, vol, ax, ay, az, vol_min, 1)
 
 
-def finalize_geometry(grid: Grid, vol, ax, ay, az, vol_min: float, nsub: int) -> CutCellGeometry:
-    """The robustness passes of `_finalize_geometry` (src/CutCell.jl:398-465)."""
+def _storage_coord(grid: Grid, axis: int, face: bool) -> np.ndarray:
+    """Cell-centre (face=False) or west-face coordinate of every storage index
+    along `axis` of a uniform grid (_xc/_xw, src/CutCell.jl:90-92)."""
+    n, H = grid.size[axis], grid.halo[axis]
+    d = (grid.dx, grid.dy, grid.dz)[axis]
+    return grid.origin[axis] + (np.arange(n + 2 * H) - H + (0.0 if face else 0.5)) * d
+
+
+def cut_cell_geometry(grid: Grid, levelset: Callable, nsub: int = 4, vol_min: float = 1e-3) -> CutCellGeometry:
+    """`cut_cell_geometry(mesh, levelset; nsub, vol_min)` (src/CutCell.jl:243-319)
+    for a level set phi(x, y, z) (phi > 0 fluid) that takes numpy arrays:
+    phi at every storage cell centre, volume fractions from nsub^3 sub-samples
+    per cell and open-area fractions from nsub^2 per face, then the
+    robustness passes, the small-cell merge partners, the normals and the
+    wetted areas (_finalize_geometry)."""
+    if grid.zf is not None:
+        raise ValueError("cut_cell_geometry takes a uniform (RegularGrid) column")
+    if nsub < 1:
+        raise ValueError("nsub must be >= 1")
+    if not 0 <= vol_min < 1:
+        raise ValueError("vol_min must lie in [0, 1)")
+    xc, yc, zc = (_storage_coord(grid, a, False) for a in range(3))
+    xw, yw, zw = (_storage_coord(grid, a, True) for a in range(3))
+    h = (grid.dx / nsub, grid.dy / nsub, grid.dz / nsub)
+    off = (np.arange(nsub) + 0.5)
+
+    def ls(x, y, z):
+        return np.asarray(levelset(x[None, None, :], y[None, :, None], z[:, None, None]), dtype=np.float64) * \
+            np.ones((len(z), len(y), len(x)))
+
+    phi = ls(xc, yc, zc)
+    vol = np.zeros(phi.shape)
+    for c in off:
+        for b in off:
+            for a in off:
+                vol += ls(xw + a * h[0], yw + b * h[1], zw + c * h[2]) > 0
+    vol /= nsub ** 3
+    ax = np.zeros(phi.shape)
+    ay = np.zeros(phi.shape)
+    az = np.zeros(phi.shape)
+    for c in off:
+        for b in off:
+            ax += ls(xw, yw + b * h[1], zw + c * h[2]) > 0
+    for c in off:
+        for a in off:
+            ay += ls(xw + a * h[0], yw, zw + c * h[2]) > 0
+    for b in off:
+        for a in off:
+            az += ls(xw + a * h[0], yw + b * h[1], zw) > 0
+    ax /= nsub ** 2
+    ay /= nsub ** 2
+    az /= nsub ** 2
+    return finalize_geometry(grid, vol, ax, ay, az, vol_min, nsub, phi=phi)
+
+
+def normal_from(phi: np.ndarray, grid: Grid, k, j, i):
+    """`_normal_from` (src/CutCell.jl:126-139): the unit normal into the fluid
+    from central differences of phi (one-sided at the array edges) and
+    |grad phi|; (0, 0, 1, 1) where the gradient vanishes.  Vectorised over
+    index arrays k, j, i."""
+    n3, n2, n1 = phi.shape
+    k, j, i = (np.asarray(a) for a in (k, j, i))
+    ip, im = np.minimum(i + 1, n1 - 1), np.maximum(i - 1, 0)
+    jp, jm = np.minimum(j + 1, n2 - 1), np.maximum(j - 1, 0)
+    kp, km = np.minimum(k + 1, n3 - 1), np.maximum(k - 1, 0)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        gx = np.where(ip == im, 0.0, (phi[k, j, ip] - phi[k, j, im]) / ((ip - im) * grid.dx))
+        gy = np.where(jp == jm, 0.0, (phi[k, jp, i] - phi[k, jm, i]) / ((jp - jm) * grid.dy))
+        gz = np.where(kp == km, 0.0, (phi[kp, j, i] - phi[km, j, i]) / ((kp - km) * grid.dz))
+        mag = np.sqrt(gx * gx + gy * gy + gz * gz)
+        bad = ~(mag > 0) | ~np.isfinite(mag)
+        safe = np.where(bad, 1.0, mag)
+        return (np.where(bad, 0.0, gx / safe), np.where(bad, 0.0, gy / safe), np.where(bad, 1.0, gz / safe),
+                np.where(bad, 1.0, mag))
+
+
+def finalize_geometry(grid: Grid, vol, ax, ay, az, vol_min: float, nsub: int, phi=None) -> CutCellGeometry:
+    """The robustness passes of `_finalize_geometry` (src/CutCell.jl:398-465),
+    the merge partner of every small cell (the open neighbour of largest
+    volume fraction, the first in the order -x, +x, -y, +y, -z, +z on a tie;
+    :467-491) and, with a level set, the wetted area from the aperture
+    balance and the normal of every cut cell (:493-504)."""
     vol = np.array(vol, dtype=np.float64)
     ax, ay, az = (np.array(a, dtype=np.float64) for a in (ax, ay, az))
     solid = ~(vol > 0)
@@ -216,8 +307,39 @@ def finalize_geometry(grid: Grid, vol, ax, ay, az, vol_min: float, nsub: int) ->
         solid |= newly
         vol[newly] = 0.0
     small = ~solid & (vol < vol_min)
+    cut = ~solid & (vol < 1.0)
     vol_eff = np.where(solid, 0.0, np.where(vol < vol_min, vol_min, vol))
-    return CutCellGeometry(grid, vol, vol_eff, ax, ay, az, solid, small, vol_min, nsub)
+    n3, n2, n1 = vol.shape
+    target = np.full(vol.shape, -1, dtype=np.int64)
+    for k, j, i in zip(*np.nonzero(small)):
+        best, bestv = -1, 0.0
+        for ap, i2, j2, k2 in ((ax[k, j, i] if i > 0 else 0.0, i - 1, j, k),
+                               (ax[k, j, i + 1] if i < n1 - 1 else 0.0, i + 1, j, k),
+                               (ay[k, j, i] if j > 0 else 0.0, i, j - 1, k),
+                               (ay[k, j + 1, i] if j < n2 - 1 else 0.0, i, j + 1, k),
+                               (az[k, j, i] if k > 0 else 0.0, i, j, k - 1),
+                               (az[k + 1, j, i] if k < n3 - 1 else 0.0, i, j, k + 1)):
+            if not ap > 0 or not (0 <= i2 < n1 and 0 <= j2 < n2 and 0 <= k2 < n3):
+                continue
+            if vol[k2, j2, i2] > bestv:
+                bestv, best = vol[k2, j2, i2], (k2 * n2 + j2) * n1 + i2
+        target[k, j, i] = best
+    geom = CutCellGeometry(grid, vol, vol_eff, ax, ay, az, solid, small, vol_min, nsub,
+                           merge_target=target, is_cut=cut)
+    if phi is not None:
+        axp = np.zeros(vol.shape); axp[:, :, :-1] = ax[:, :, 1:]
+        ayp = np.zeros(vol.shape); ayp[:, :-1, :] = ay[:, 1:, :]
+        azp = np.zeros(vol.shape); azp[:-1, :, :] = az[1:, :, :]
+        sx = (axp - ax) * (grid.dy * grid.dz)
+        sy = (ayp - ay) * (grid.dx * grid.dz)
+        sz = (azp - az) * (grid.dx * grid.dy)
+        geom.area = np.where(cut, np.sqrt(sx * sx + sy * sy + sz * sz), 0.0)
+        geom.phi = np.asarray(phi, dtype=np.float64)
+        geom.nx, geom.ny, geom.nz = np.zeros(vol.shape), np.zeros(vol.shape), np.zeros(vol.shape)
+        kk, jj, ii = np.nonzero(cut)
+        gx, gy, gz, _ = normal_from(geom.phi, grid, kk, jj, ii)
+        geom.nx[cut], geom.ny[cut], geom.nz[cut] = gx, gy, gz
+    return geom
 
 
 def face_coefficients(geom: CutCellGeometry, power: int = 2):
@@ -235,11 +357,15 @@ def face_coefficients(geom: CutCellGeometry, power: int = 2):
     return np.ascontiguousarray(cx), np.ascontiguousarray(cy), np.ascontiguousarray(cz)
 
 
-def cutcell_divergence(geom: CutCellGeometry, u, v, w) -> np.ndarray:
-    """`cutcell_divergence!` without the small-cell redistribution
-    (src/CutCell.jl:602-622): the aperture-weighted flux difference over
-    vol_eff, zero in solid cells; u, v, w storage arrays with filled halos.
-    Returns the interior (Nz, Ny, Nx)."""
+def cutcell_divergence(geom: CutCellGeometry, u, v, w, redistribute: bool = False) -> np.ndarray:
+    """`cutcell_divergence!` (src/CutCell.jl:602-622): the aperture-weighted
+    flux difference over vol_eff, zero in solid cells; u, v, w storage arrays
+    with filled halos.  With `redistribute`, `_redistribute_small_cells!`
+    (:624-644): every small cell and its merge partner take their cluster's
+    volume-weighted mean, one small cell after another in storage order (a
+    partner shared by several small cells accumulates them in turn), which
+    conserves the sum of vol_eff times the divergence.  Returns the interior
+    (Nz, Ny, Nx)."""
     g = geom.grid
     hx, hy, hz = g.halo
     nx, ny, nz = g.size
@@ -249,7 +375,25 @@ def cutcell_divergence(geom: CutCellGeometry, u, v, w) -> np.ndarray:
     fy = (geom.ay[K, Jp, I] * v[K, Jp, I] - geom.ay[K, J, I] * v[K, J, I]) / g.dy
     fz = (geom.az[Kp, J, I] * w[Kp, J, I] - geom.az[K, J, I] * w[K, J, I]) / g.dz
     ve = geom.vol_eff[K, J, I]
-    return np.where(ve > 0, (fx + fy + fz) / np.where(ve > 0, ve, 1.0), 0.0)
+    div = np.where(ve > 0, (fx + fy + fz) / np.where(ve > 0, ve, 1.0), 0.0)
+    if not redistribute or geom.merge_target is None or not geom.is_small[K, J, I].any():
+        return div
+    full = np.zeros(geom.vol_eff.shape)
+    full[K, J, I] = div
+    flat, vef = full.ravel(), geom.vol_eff.ravel()
+    inside = np.zeros(full.shape, dtype=bool)
+    inside[K, J, I] = True
+    for q in np.flatnonzero((geom.is_small & inside).ravel()):
+        t = geom.merge_target.ravel()[q]
+        if t < 0:
+            continue
+        vt = vef[q] + vef[t]
+        if not vt > 0:
+            continue
+        d = (vef[q] * flat[q] + vef[t] * flat[t]) / vt
+        flat[q] = d
+        flat[t] = d
+    return full[K, J, I]
 
 
 def pressure_rhs(geom: CutCellGeometry, u, v, w) -> np.ndarray:
