@@ -263,19 +263,21 @@ __global__ void __launch_bounds__(256) finite_check_kernel(Geo g, const R* __res
                                                            const R* __restrict__ f2, const R* __restrict__ f3,
                                                            int* __restrict__ flag) {
     constexpr int N = Vec16<R>::N;
-    const long long per = g.nin / N;   // vectors of one field (nx is a multiple of N)
+    const int per = (int)(g.nin / N);   // vectors of one field (nx is a multiple of N)
     const int lnx = __ffs(g.nx) - 1, lny = __ffs(g.ny) - 1;
+    const int stride = gridDim.x * blockDim.x;
     bool bad = false;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < 4 * per;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int f = (int)(t / per);
-        const long long qi = (t - f * per) * N;
-        const int i0 = (int)(qi & (g.nx - 1)), j = (int)((qi >> lnx) & (g.ny - 1)), k = (int)(qi >> (lnx + lny));
-        const R* a = f == 0 ? f0 : (f == 1 ? f1 : (f == 2 ? f2 : f3));
-        R v[N];
-        vld(a + pidx(g, i0, j, k), v);
 #pragma unroll
-        for (int n = 0; n < N; ++n) bad = bad || !isfinite(v[n]);
+    for (int f = 0; f < 4; ++f) {
+        const R* a = f == 0 ? f0 : (f == 1 ? f1 : (f == 2 ? f2 : f3));
+        for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < per; t += stride) {
+            const long long qi = (long long)t * N;
+            const int i0 = (int)(qi & (g.nx - 1)), j = (int)((qi >> lnx) & (g.ny - 1)), k = (int)(qi >> (lnx + lny));
+            R v[N];
+            vld(a + pidx(g, i0, j, k), v);
+#pragma unroll
+            for (int n = 0; n < N; ++n) bad = bad || !isfinite(v[n]);
+        }
     }
     if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
 }

@@ -41,6 +41,7 @@
 #include "aeo_misc.cuh"
 #include "aeo_sweep.cuh"
 #include "aeo_sweep_pair.cuh"
+#include "aeo_sweep_wpair.cuh"
 #include "aeo_sweep_tile.cuh"
 
 static std::string g_create_error;
@@ -152,6 +153,8 @@ struct Core : CoreBase {
     StepScalars* d_sc = nullptr;
     int rows_x = 1, tpx_y = 1, tpx_z = 1;
     int kchunk = 32;
+    int wchunk = 32;         // levels a CTA of the paired WENO sweep marches
+    int fin_per_sm = 4;      // resident CTAs of the finite check an SM
     int nsm = 148;           // SMs of the device (the persistent sweep's grid)
     // interior column metrics and weights on the host (the PCG operator's coefficients):
     // dz_c per level, dz_f per face, W_c, W_f (1 on the Boussinesq core)
@@ -488,6 +491,22 @@ struct Core : CoreBase {
         if (aeo_status e = make_tensor_maps()) return e;
         kchunk = std::min(g.nz, TileShape<R, 0, false>::KCH);
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cfg.device));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fin_per_sm, finite_check_kernel<R>, 256, 0));
+        fin_per_sm = std::max(fin_per_sm, 1);
+        {
+            // the paired WENO sweep: the chunk length that minimises whole waves x
+            // (levels + the 6-plane start of a chunk)
+            const long long tiles = (long long)((g.nx + WPairShape::TX - 1) / WPairShape::TX) *
+                                    ((g.ny + WPairShape::TY - 1) / WPairShape::TY);
+            const long long slots = (long long)WPairShape::CTAS_PER_SM * nsm;
+            long long best = -1;
+            for (int c : {16, 32, 64}) {
+                const int kc = std::min(c, g.nz);
+                const long long waves = (tiles * ((g.nz + kc - 1) / kc) + slots - 1) / slots;
+                const long long cost = waves * (kc + 6);
+                if (best < 0 || cost < best) { best = cost; wchunk = kc; }
+            }
+        }
         CK(cudaStreamSynchronize(st));
         launches = 3 * (9 + dyn_launches());
         return AEO_OK;
@@ -704,6 +723,14 @@ struct Core : CoreBase {
                                                                                            items, d_flag);
                 return;
             }
+        }
+        if constexpr (ADV > 0 && !SG && !AN && UN && sizeof(R) == sizeof(float)) {
+            // FP32 WENO without a closure: cell pairs, every face once
+            using WS = WPairShape;
+            const dim3 grid((g.nx + WS::TX - 1) / WS::TX, (g.ny + WS::TY - 1) / WS::TY, (g.nz + wchunk - 1) / wchunk);
+            cudaFuncSetAttribute(sweep_wpair_kernel<ADV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WS::SMEM);
+            sweep_wpair_kernel<ADV><<<grid, dim3(WS::TXT, WS::TY), WS::SMEM, st>>>(tmaps[s_in], a, wchunk, d_flag);
+            return;
         }
         using TS = TileShape<R, ADV, SG>;
         dim3 grid((g.nx + TS::TX - 1) / TS::TX, (g.ny + TS::TY - 1) / TS::TY, (g.nz + kchunk - 1) / kchunk);
@@ -1199,8 +1226,9 @@ struct Core : CoreBase {
     }
 
     aeo_status check_finite() {
-        const long long vecs = 4 * (g.nin / Vec16<R>::N);
-        const unsigned nb = (unsigned)std::min<long long>((vecs + 255) / 256, 8LL * nsm);
+        // one resident wave: every CTA loops over its share of each field
+        const long long vecs = g.nin / Vec16<R>::N;
+        const unsigned nb = (unsigned)std::min<long long>((vecs + 255) / 256, (long long)fin_per_sm * nsm);
         finite_check_kernel<R><<<nb, 256, 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], P[cur][3], d_flag);
         CKL();
         int h = 0;
