@@ -63,7 +63,7 @@ HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes (read + write) of one sweep launch of the CBL 256x256x128 FP32-mixed
 # step, from an ncu capture of `python bench.py --steps 2 --warmup 3`
 # (profiles/sweep_pair_kernel_cbl256_fp32.md)
-CBL_SWEEP_DRAM_BYTES = 157088256 + 95768576
+CBL_SWEEP_DRAM_BYTES = 315824640 + 109399552
 # ... and of one finest red-black colour pass of the urban 256x256x96 FP32-mixed
 # solve (profiles/mg_vcycle_urban256x256x96_fp32.md): 69.4 MB read + 1.3 MB written
 URBAN_RBGS_DRAM_BYTES = 70.7e6
@@ -1133,6 +1133,14 @@ def run_b200(args):
                "adaptive_ms_per_step": {"fp32_mixed": hres["fp32_mixed"]["adaptive_ms"],
                                         "fp64": hres["fp64"]["adaptive_ms"]},
                "fp32_vs_fp64": hcmp, "clocks": hres["fp32_mixed"]["clocks"]}
+        hprof = hres["fp32_mixed"]["prof"]
+        if hprof.get("sweep", 0) > 0:
+            hb = class_passes("sweep", hg, False) * 4 * hg.ncells
+            hach = hb / (hprof["sweep"] / LAUNCHES_PER_STEP["sweep"] * 1e-3) / 1e9
+            hbm_h, hbm_kind_h = measured_peaks()
+            hit["roofline"] = {"bound": "hbm", "kernel": "sweep (sweep_wpair_kernel)", "achieved": round(hach, 1),
+                               "peak": hbm_h, "unit": "GB/s", "frac": round(hach / hbm_h, 4),
+                               "peak_kind": hbm_kind_h, "bytes_per_launch": hb}
     if rank != 0:
         barrier(world)
         return 0

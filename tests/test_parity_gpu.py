@@ -181,14 +181,16 @@ def test_fp32_mixed_close_to_fp64_oracle():
     assert all(e < 1e-5 for e in errs.values()), errs
 
 
-def test_fp32_mixed_anelastic_close_to_fp64():
+@pytest.mark.parametrize("nz", [64, 160])
+def test_fp32_mixed_anelastic_close_to_fp64(nz):
     """The dry CBL (noise in the lowest 10 levels, as the bench workload) on a
-    64 x 64 x 64 tanh column: after 50 steps of 1 s the convection has grown w
+    64 x 64 x nz tanh column: after 50 steps of 1 s the convection has grown w
     well above the FP32 round-off of the first steps, and every prognostic
     field of the FP32-mixed step is within 1e-5 (relative L2) of the FP64
     oracle; theta is compared as its departure from the initial profile, and
-    the kinetic energy the convection has built up to 1e-6."""
-    g, spec, ospec = cbl_spec(nx=64, nz=64, precision="fp32_mixed")
+    the kinetic energy the convection has built up to 1e-6.  With nz = 160
+    the persistent paired sweep runs three chunk rows of levels (64, 64, 32)."""
+    g, spec, ospec = cbl_spec(nx=64, nz=nz, precision="fp32_mixed")
     u, v, w, th, _ = cbl_initial(g, seed=1, noise=0.1, noise_levels=10)
     gs, os_ = Sim(spec), OracleSimulation(ospec)
     for s in (gs, os_):
