@@ -405,16 +405,24 @@ struct ColumnCoef {
 // levels ahead of the recurrence, and waits (cp.async.wait_group) for exactly
 // the level it needs, so the loads overlap the FP64 recurrence instead of
 // exposing one memory latency per level.  The forward-elimination values d'_k
-// go to dsc, an FP64 column scratch of the spectrum's layout (dsc may alias S
-// when S is FP64: d'_k overwrites the level it came from after that level
-// was read).  The modified upper diagonal c'_k goes either to an FP64 scratch
-// of the same layout (CPG: streamed back with d'_k, so a CTA needs only its
-// rings and every column warp of the grid is resident at once) or to shared
-// memory [nz][32] (no scratch: the allocation-free entry).
+// go to dsc, a column scratch of the spectrum's layout in precision RD (dsc
+// may alias S when RD is S's type: d'_k overwrites the level it came from
+// after that level was read).  The modified upper diagonal c'_k goes either
+// to an RD scratch of the same layout (CPG: streamed back with d'_k, so a CTA
+// needs only its rings and every column warp of the grid is resident at
+// once) or to shared memory [nz][32] (no scratch: the allocation-free entry).
+// The recurrence itself runs in FP64 whatever RD is; the FP32-mixed step
+// stores d' and c' in FP32 in place (S and an FP32 c' array), so the stored
+// intermediates carry the rounding of the FP32 spectrum they came from and
+// the solve moves 40 bytes an element instead of 64.
 constexpr int THOMAS_PF = 16;
 // the largest nz whose column state fits a CTA's 227 KB of shared memory
 #define AEO_COLUMN_NZ_MAX 800
 
+__device__ __forceinline__ void thomas_cp4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
 __device__ __forceinline__ void thomas_cp8(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
                  : "memory");
@@ -425,7 +433,8 @@ __device__ __forceinline__ void thomas_cp16(void* dst, const void* src) {
 }
 template <int N>
 __device__ __forceinline__ void thomas_cp(void* dst, const void* src) {
-    if (N == 8) thomas_cp8(dst, src);
+    if (N == 4) thomas_cp4(dst, src);
+    else if (N == 8) thomas_cp8(dst, src);
     else thomas_cp16(dst, src);
 }
 __device__ __forceinline__ void thomas_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
@@ -447,8 +456,41 @@ inline size_t thomas_smem(const Geo& g, bool cpg) {
     return ring + (cols > mean ? cols : mean);
 }
 
-template <typename R, bool CPG>
-__global__ void __launch_bounds__(32) thomas_kernel(Geo g, cplx<R>* S, cplx<double>* dsc, double* cpg, ColumnCoef c) {
+// The elimination factors of every non-mean column, once per grid: the
+// multiplier m_k = 1 / (b_k - lo_k c'_{k-1}) of level k and c'_k = up_k m_k,
+// in precision RD at the spectrum's layout (mtab, ctab).  They depend on the
+// column's coefficients and its eigenvalue kx^2 + ky^2 only, so the solves
+// of a run stream them instead of recomputing the division chain; the FP64
+// arithmetic and its order are those of the solve kernel's own elimination,
+// so an FP64 table reproduces it exactly.
+template <typename RD>
+__global__ void __launch_bounds__(256) thomas_factor_kernel(Geo g, RD* __restrict__ mtab, RD* __restrict__ ctab,
+                                                            ColumnCoef c) {
+    const int Mh = g.nx / 2 + 1;
+    const long long sk = (long long)g.ny * Mh;
+    const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col == 0 || col >= sk) return;
+    const int p = (int)(col % Mh), j = (int)(col / Mh);
+    const double lam = c.kx2[p] + c.ky2[j];
+    double cprev = 0.0;
+    for (int k = 0; k < g.nz; ++k) {
+        const double lo = c.lower[k], up = c.upper[k];
+        const double b = -(lo + up) - lam * c.hw[k];
+        const double den = b - lo * cprev;
+        const double id = 1.0 / den;
+        cprev = up * id;
+        mtab[col + (long long)k * sk] = RD(id);
+        if (k < g.nz - 1) ctab[col + (long long)k * sk] = RD(cprev);
+    }
+}
+
+// FAC: the elimination factors come from thomas_factor_kernel's tables
+// (mtab; cpg holds c'), streamed through the c' ring in the forward pass, so
+// the recurrence is two multiply-adds a level and writes no c'.
+template <typename R, bool CPG, typename RD = double, bool FAC = false>
+__global__ void __launch_bounds__(32) thomas_kernel(Geo g, cplx<R>* S, cplx<RD>* dsc, RD* cpg, ColumnCoef c,
+                                                    const RD* __restrict__ mtab = nullptr) {
+    static_assert(!FAC || CPG, "the factored solve streams c' from its table");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int D = THOMAS_PF;
     cplx<double>* ring = reinterpret_cast<cplx<double>*>(smem_raw);   // [D][32], 16-byte entries
@@ -496,7 +538,7 @@ __global__ void __launch_bounds__(32) thomas_kernel(Geo g, cplx<R>* S, cplx<doub
         for (int k = lane; k < nz; k += 32) S[k * sk] = cmk<R>(R(ph[k] - sh), R(0));
         return;
     }
-    double* cring = after;                              // CPG: [D][32] c' ring
+    RD* cring = reinterpret_cast<RD*>(after);           // CPG: [D][32] c' ring
     double* cp = after;                                 // shared c': [nz][32]
     double* s_lo = CPG ? after + D * 32 : after + 32 * nz;
     double* s_up = s_lo + nz;
@@ -517,36 +559,51 @@ __global__ void __launch_bounds__(32) thomas_kernel(Geo g, cplx<R>* S, cplx<doub
     cplx<R>* rs = reinterpret_cast<cplx<R>*>(ring);   // this lane's entries at [slot * 32 + lane]
 #pragma unroll
     for (int q = 0; q < D - 1; ++q) {
-        if (q < nz) thomas_cp<sizeof(cplx<R>)>(rs + q * 32 + lane, S + col + q * sk);
+        if (q < nz) {
+            thomas_cp<sizeof(cplx<R>)>(rs + q * 32 + lane, S + col + q * sk);
+            if (FAC) thomas_cp<sizeof(RD)>(cring + q * 32 + lane, mtab + col + q * sk);
+        }
         thomas_commit();
     }
     double cprev = 0.0, dr = 0.0, di = 0.0;
     for (int k = 0; k < nz; ++k) {
         const int kn = k + D - 1;
-        if (kn < nz) thomas_cp<sizeof(cplx<R>)>(rs + (kn % D) * 32 + lane, S + col + (long long)kn * sk);
+        if (kn < nz) {
+            thomas_cp<sizeof(cplx<R>)>(rs + (kn % D) * 32 + lane, S + col + (long long)kn * sk);
+            if (FAC) thomas_cp<sizeof(RD)>(cring + (kn % D) * 32 + lane, mtab + col + (long long)kn * sk);
+        }
         thomas_commit();
         thomas_wait<D - 1>();   // level k has landed
         const cplx<R> s = rs[(k % D) * 32 + lane];
-        const double lo = s_lo[k], up = s_up[k];
-        const double b = -(lo + up) - lam * s_hw[k];
-        const double den = b - lo * cprev;
-        const double id = 1.0 / den;
-        cprev = up * id;
+        const double lo = s_lo[k];
+        double id;
+        if constexpr (FAC) {
+            id = (double)cring[(k % D) * 32 + lane];
+        } else {
+            const double up = s_up[k];
+            const double b = -(lo + up) - lam * s_hw[k];
+            const double den = b - lo * cprev;
+            id = 1.0 / den;
+            cprev = up * id;
+        }
         dr = ((double)s.x - lo * dr) * id;   // lo = 0 at k = 0
         di = ((double)s.y - lo * di) * id;
         if (k < nz - 1) {
-            if (CPG) cpg[col + (long long)k * sk] = cprev;
-            else cp[k * 32 + lane] = cprev;
-            dsc[col + (long long)k * sk] = cmk<double>(dr, di);
+            if (!FAC) {
+                if (CPG) cpg[col + (long long)k * sk] = RD(cprev);
+                else cp[k * 32 + lane] = cprev;
+            }
+            dsc[col + (long long)k * sk] = cmk<RD>(RD(dr), RD(di));
         }
     }
     thomas_wait<0>();
     S[col + (long long)(nz - 1) * sk] = cmk<R>(R(dr), R(di));
     // back substitution over k = nz-2 .. 0, the d' (and c') values streamed
     // alike (slot t holds level nz-2-t modulo D)
+    cplx<RD>* dring = reinterpret_cast<cplx<RD>*>(ring);
     auto fetch = [&](int slot, int k) {
-        thomas_cp16(ring + slot * 32 + lane, dsc + col + (long long)k * sk);
-        if (CPG) thomas_cp8(cring + slot * 32 + lane, cpg + col + (long long)k * sk);
+        thomas_cp<sizeof(cplx<RD>)>(dring + slot * 32 + lane, dsc + col + (long long)k * sk);
+        if (CPG) thomas_cp<sizeof(RD)>(cring + slot * 32 + lane, cpg + col + (long long)k * sk);
     };
 #pragma unroll
     for (int q = 0; q < D - 1; ++q) {
@@ -560,10 +617,10 @@ __global__ void __launch_bounds__(32) thomas_kernel(Geo g, cplx<R>* S, cplx<doub
         if (kn >= 0) fetch(tn % D, kn);
         thomas_commit();
         thomas_wait<D - 1>();
-        const cplx<double> d = ring[(t % D) * 32 + lane];
-        const double cc = CPG ? cring[(t % D) * 32 + lane] : cp[k * 32 + lane];
-        dr = d.x - cc * dr;
-        di = d.y - cc * di;
+        const cplx<RD> d = dring[(t % D) * 32 + lane];
+        const double cc = CPG ? (double)cring[(t % D) * 32 + lane] : cp[k * 32 + lane];
+        dr = (double)d.x - cc * dr;
+        di = (double)d.y - cc * di;
         S[col + (long long)k * sk] = cmk<R>(R(dr), R(di));
     }
     thomas_wait<0>();

@@ -168,7 +168,7 @@ extern "C" aeo_status aeo_pressure_solve_column_noalloc(int32_t nx, int32_t ny, 
     size_t smy = (size_t)tpx * ny * sizeof(cplx<double>);
     size_t smt = thomas_smem(g, false);
     if (smt > 48 * 1024) {
-        e = cudaFuncSetAttribute(thomas_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
+        e = cudaFuncSetAttribute(thomas_kernel<double, false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
         if (e != cudaSuccess) {
             aeo_set_global_error(std::string("pressure_solve_column_noalloc: ") + cudaGetErrorString(e));
             return AEO_ERR_CUDA;
@@ -176,7 +176,7 @@ extern "C" aeo_status aeo_pressure_solve_column_noalloc(int32_t nx, int32_t ny, 
     }
     src_fftx_kernel<double><<<gx, FFT_THREADS(double), smx, st>>>(g, src, S, tw, NT, rows);
     ffty_kernel<double, 0><<<gy, FFT_THREADS(double), smy, st>>>(g, S, tw, NT, tpx);
-    thomas_kernel<double, false><<<thomas_blocks(g), 32, smt, st>>>(g, S, S, nullptr, cc);
+    thomas_kernel<double, false, double><<<thomas_blocks(g), 32, smt, st>>>(g, S, S, nullptr, cc);
     ffty_kernel<double, 1><<<gy, FFT_THREADS(double), smy, st>>>(g, S, tw, NT, tpx);
     ifftx_kernel<double><<<gx, FFT_THREADS(double), smx, st>>>(g, S, phi, tw, NT, rows, 1.0 / ((double)nx * ny));
     e = cudaGetLastError();

@@ -134,7 +134,6 @@ struct Core : CoreBase {
     R* phi = nullptr;          // interior
     R* pres = nullptr;         // interior
     cplx<R>* S = nullptr;      // spectrum
-    cplx<double>* dsc = nullptr;
     double* cps = nullptr;     // the column solve's c' scratch (spectrum layout)
     cplx<R>* tw = nullptr;
     int NT = 0;
@@ -458,9 +457,12 @@ struct Core : CoreBase {
         const long long ns = (long long)Mh * Ny * Nz;
         if (aeo_status e = alloc(&S, ns)) return e;
         if (c.solver == AEO_SOLVER_COLUMN) {
-            if (sizeof(R) == sizeof(double)) dsc = reinterpret_cast<cplx<double>*>(S);
-            else if (aeo_status e = alloc(&dsc, ns)) return e;
-            if (aeo_status e = alloc(&cps, ns)) return e;
+            // the elimination factors m and c' of every column in the working precision
+            if (aeo_status e = alloc(&cps, sizeof(R) == sizeof(double) ? 2 * ns : ns)) return e;
+            R* ftab = reinterpret_cast<R*>(cps);
+            const long long cols = (long long)Ny * Mh;
+            thomas_factor_kernel<R><<<(unsigned)((cols + 255) / 256), 256, 0, st>>>(g, ftab, ftab + ns, cc);
+            CKL();
         }
         if (c.solver == AEO_SOLVER_PCG) {
             pcg = true;
@@ -829,8 +831,12 @@ struct Core : CoreBase {
         } else {
             size_t smt = thomas_smem(g, true);
             if (smt > 48 * 1024)
-                cudaFuncSetAttribute(thomas_kernel<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smt);
-            thomas_kernel<R, true><<<thomas_blocks(g), 32, smt, st>>>(g, S, dsc, cps, cc);
+                cudaFuncSetAttribute(thomas_kernel<R, true, R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smt);
+            // d' in place in S; the factors m and c' from the tables made at set-up
+            R* ftab = reinterpret_cast<R*>(cps);
+            const long long ns = (long long)(g.nx / 2 + 1) * g.ny * g.nz;
+            thomas_kernel<R, true, R, true><<<thomas_blocks(g), 32, smt, st>>>(g, S, S, ftab + ns, cc, ftab);
         }
         CKL();
         mark(AEO_K_ZSOLVE);
