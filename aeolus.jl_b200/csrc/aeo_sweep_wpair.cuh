@@ -31,7 +31,7 @@
 #pragma once
 
 #include "aeo_f2.cuh"
-#include "aeo_sweep_tile.cuh"
+#include "aeo_sweep_pair.cuh"   // PairAcc, PairNut (and the tile machinery)
 
 __device__ __forceinline__ F2 ld2s(const float* p) { return F2(*reinterpret_cast<const float2*>(p)); }
 __device__ __forceinline__ float2 ldf2(const float* p) { return *reinterpret_cast<const float2*>(p); }
@@ -51,13 +51,17 @@ __device__ __forceinline__ F2 f2pick(bool px, bool py, F2 a, F2 b) {
 // weno5_left (aeo_sweep.cuh) on two faces
 template <int ADV>
 __device__ __forceinline__ F2 weno5_left_f2(F2 v1, F2 v2, F2 v3, F2 v4, F2 v5) {
-    const F2 s6(float(1.0 / 6.0)), two(2.f), half(0.5f), c133(float(13.0 / 3.0));
-    const F2 q0 = F2(two * v1 - F2(7.f) * v2 + F2(11.f) * v3) * s6;
-    const F2 q1 = F2(F2(5.f) * v3 - v2 + two * v4) * s6;
-    const F2 q2 = F2(two * v3 + F2(5.f) * v4 - v5) * s6;
-    const F2 d2a = F2(v1 - two * v2 + v3) * half;
-    const F2 d2b = F2(v2 - two * v3 + v4) * half;
-    const F2 d2c = F2(v3 - two * v4 + v5) * half;
+    // the candidate values and second differences with the 1/6 and 1/2 folded
+    // into the coefficients (one rounding fewer than the scalar form's)
+    const F2 half(0.5f), c133(float(13.0 / 3.0));
+    const F2 c13(float(1.0 / 3.0)), c16(float(1.0 / 6.0)), c56(float(5.0 / 6.0)), c76(float(7.0 / 6.0)),
+        c116(float(11.0 / 6.0));
+    const F2 q0 = c13 * v1 - c76 * v2 + c116 * v3;
+    const F2 q1 = c56 * v3 - c16 * v2 + c13 * v4;
+    const F2 q2 = c13 * v3 + c56 * v4 - c16 * v5;
+    const F2 d2a = half * (v1 + v3) - v2;
+    const F2 d2b = half * (v2 + v4) - v3;
+    const F2 d2c = half * (v3 + v5) - v4;
     const F2 e0 = F2(v1 - F2(4.f) * v2 + F2(3.f) * v3) * half;
     const F2 e1 = (v4 - v2) * half;
     const F2 e2 = F2(F2(4.f) * v4 - F2(3.f) * v3 - v5) * half;
@@ -223,7 +227,7 @@ __global__ void __launch_bounds__(128, 3) sweep_wpair_kernel(const __grid_consta
         {
             const float* pk = pl[3];
             const float* pkm = pl[2];
-#pragma unroll 1
+#pragma unroll 2
             for (int w = warp; w < S::NYW; w += S::NWARP) {
                 const int row = 2 * w + hrow, f = row / (S::TY + 1), fj = row - f * (S::TY + 1);
                 const int b = (fj + S::HH) * S::PW + 4 + 2 * pc;
@@ -231,7 +235,7 @@ __global__ void __launch_bounds__(128, 3) sweep_wpair_kernel(const __grid_consta
                     face_item<ADV, false>(pk, pkm, f, b).v;
             }
             // (started two warps on, so that the edge warp lands on a warp with four y items)
-#pragma unroll 1
+#pragma unroll 2
             for (int w = (warp + 2) % S::NWARP; w <= S::NXW; w += S::NWARP) {
                 int f, fj, fi;
                 if (w < S::NXW) {

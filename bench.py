@@ -1121,6 +1121,8 @@ def run_b200(args):
     for v in pcg.values():
         v["ms"] = max_over_ranks(v["ms"], world)
         del v["handle"]
+    # the learned preconditioner on the same problem (trained in this run), beside the plain solves
+    learned = None if args.no_learned else learned_pcg(coeffs, b, args)
     # config 3 beside it: decaying isotropic turbulence, FP32-mixed against FP64
     hit = None
     if args.hit_steps > 0:
@@ -1194,7 +1196,7 @@ def run_b200(args):
         "clocks": main["clocks"],
         "max_divergence": main["div"],
         "pcg": {"metric": "PCG time-to-1e-8", "unit": "ms", "config": udesc,
-                "plain_fp32_mixed": pcg["fp32_mixed"], "plain_fp64": pcg["fp64"], "learned": None},
+                "plain_fp32_mixed": pcg["fp32_mixed"], "plain_fp64": pcg["fp64"], "learned": learned},
         "hit": hit,
     }
     if world == 1 and not args.no_cpu_baseline:
@@ -1228,6 +1230,7 @@ def main():
     ap.add_argument("--urban-core", default="anelastic", choices=["anelastic", "boussinesq"])
     ap.add_argument("--learned", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
