@@ -189,6 +189,104 @@ __device__ __forceinline__ void smem_fft(cplx<R>* buf, int logn, int lognl, int 
     }
 }
 
+// ---- compile-time lengths -----------------------------------------------------------
+// The same Stockham passes with the length n = 2^LOGN and the line count
+// 2^LOGL (n 2^LOGL = 2048 points a CTA) known at compile time: every shift,
+// mask and offset of the index arithmetic folds to a constant, the pass
+// schedule unrolls, and the inter-pass twiddles come from a table of the n
+// roots W_n^m staged in shared memory by the kernel (twn).  The pass
+// schedule is smem_fft's (ceil(rest / passes left), largest first).
+template <int LOGN, int MAXLR>
+struct FftPlan {
+    static constexpr int NP = (LOGN + MAXLR - 1) / MAXLR;
+    static constexpr int ns(int p) {   // log2 Ns before pass p
+        int l = 0;
+        for (int q = 0; q < p; ++q) l += (LOGN - l + (NP - q) - 1) / (NP - q);
+        return l;
+    }
+    static constexpr int lr(int p) { return (LOGN - ns(p) + (NP - p) - 1) / (NP - p); }
+};
+
+template <typename R, int LR, bool INV, bool LINE_FAST, int LOGN, int LOGL, int LOGNS>
+__device__ __forceinline__ void fft_pass_ct(cplx<R>* buf, const cplx<R>* twn) {
+    constexpr bool SKEW = !LINE_FAST;
+    constexpr int NTHR = FftCfg<R>::THREADS;
+    constexpr int RR = 1 << LR, KB = FftCfg<R>::PTS / RR;
+    constexpr int LOGNB = LOGN - LR, NB = 1 << LOGNB;
+    constexpr int TOTAL = NB << LOGL;
+    constexpr int NS = 1 << LOGNS;
+    constexpr int ES = LINE_FAST ? (1 << LOGL) : 1;
+    constexpr int LS = LINE_FAST ? 1 : ((1 << LOGN) + ((1 << LOGN) >> 4) + 1);
+    constexpr int TSH = LOGN - LR - LOGNS;
+    static_assert(KB * NTHR == TOTAL, "every butterfly of the pass has a thread slot");
+    const int tid = threadIdx.x;
+    cplx<R> v[KB][RR];
+    int oo[KB];
+#pragma unroll
+    for (int s = 0; s < KB; ++s) {
+        const int b = tid + s * NTHR;
+        int l, j;
+        if (LINE_FAST) { l = b & ((1 << LOGL) - 1); j = b >> LOGL; }
+        else { l = b >> LOGNB; j = b & (NB - 1); }
+        const int k = j & (NS - 1);
+        const cplx<R>* base = buf + l * LS;
+#pragma unroll
+        for (int r = 0; r < RR; ++r) {
+            v[s][r] = base[sk16<SKEW>(j + r * NB) * ES];
+            if (LOGNS > 0 && r > 0) {
+                cplx<R> wv = twn[((r * k) << TSH) & ((1 << LOGN) - 1)];
+                if (INV) wv.y = -wv.y;
+                v[s][r] = cmul(v[s][r], wv);
+            }
+        }
+        dft_reg<R, RR, INV>(v[s]);
+        oo[s] = l * LS + (SKEW ? 0 : (((j - k) << LR) + k) * ES);
+        if (SKEW) oo[s] |= ((((j - k) << LR) + k) << 16);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < KB; ++s) {
+        if (SKEW) {
+            const int lo = oo[s] & 0xFFFF, o = oo[s] >> 16;
+#pragma unroll
+            for (int q = 0; q < RR; ++q) buf[lo + sk16<true>(o + q * NS)] = v[s][q];
+        } else {
+#pragma unroll
+            for (int q = 0; q < RR; ++q) buf[oo[s] + q * NS * ES] = v[s][q];
+        }
+    }
+    __syncthreads();
+}
+
+template <typename R, bool INV, bool LINE_FAST, int LOGN, int LOGL, int P = 0>
+__device__ __forceinline__ void smem_fft_ct(cplx<R>* buf, const cplx<R>* twn) {
+    using PL = FftPlan<LOGN, FftCfg<R>::MAXLR>;
+    if constexpr (P < PL::NP) {
+        fft_pass_ct<R, PL::lr(P), INV, LINE_FAST, LOGN, LOGL, PL::ns(P)>(buf, twn);
+        smem_fft_ct<R, INV, LINE_FAST, LOGN, LOGL, P + 1>(buf, twn);
+    }
+}
+
+// The transform of a kernel: compile-time lengths (LOGN > 0; the lines fill
+// the CTA's 2048 points) or the general form.
+template <typename R, bool INV, bool LINE_FAST, int LOGN>
+__device__ __forceinline__ void run_fft(cplx<R>* buf, int logn, int lognl, int ls, int es,
+                                        const cplx<R>* __restrict__ tw, int NT, const cplx<R>* twn) {
+    if constexpr (LOGN > 0) smem_fft_ct<R, INV, LINE_FAST, LOGN, 11 - LOGN>(buf, twn);
+    else smem_fft<R, INV, LINE_FAST>(buf, logn, lognl, ls, es, tw, NT);
+}
+// Stage the roots W_n^m, m < n = 2^LOGN, from the NT-point table (NT >= n).
+template <typename R, int LOGN>
+__device__ __forceinline__ void stage_roots(cplx<R>* twn, const cplx<R>* __restrict__ tw, int NT) {
+    if constexpr (LOGN > 0) {
+        const int sh = (__ffs(NT) - 1) - LOGN;
+        for (int m = threadIdx.x; m < (1 << LOGN); m += blockDim.x) twn[m] = tw[m << sh];
+    }
+}
+// the extra shared memory of a compile-time-length kernel
+template <typename R>
+inline size_t roots_smem(int logn) { return (logn >= 7 && logn <= 9) ? ((size_t)1 << logn) * sizeof(cplx<R>) : 0; }
+
 // ---- divergence ------------------------------------------------------------------
 // The divergence of the predicted velocity (the source of the pressure solve)
 // for N = 16/sizeof(R) x-consecutive cells per thread, 16-byte loads and
@@ -261,13 +359,16 @@ __device__ __forceinline__ cplx<R> c2r_pre(cplx<R> a, cplx<R> b, cplx<R> wv) {
 // pre-processes the bin pairs (u, M-u) (unit 0 of a row: bins 0 and M/2) in
 // registers, writes the packed M-point lines skewed, runs the inverse FFT
 // and stores the real pairs.
-template <typename R>
+template <typename R, int LOGN = 0>
 __global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) ifftx_kernel(Geo g, const cplx<R>* __restrict__ S, R* __restrict__ phi,
                                                     const cplx<R>* __restrict__ tw, int NT, int rows, R scale) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<R>* buf = reinterpret_cast<cplx<R>*>(smem_raw);
     constexpr int UPT = FftCfg<R>::PTS / 2;
-    const int M = g.nx / 2, Mh = M + 1, lM = __ffs(M) - 1, LS = xrow(M);
+    const int M = LOGN > 0 ? (1 << LOGN) : g.nx / 2, Mh = M + 1, lM = LOGN > 0 ? LOGN : __ffs(M) - 1, LS = xrow(M);
+    if (LOGN > 0) rows = 1 << (11 - LOGN);
+    cplx<R>* twn = buf + rows * LS;
+    stage_roots<R, LOGN>(twn, tw, NT);
     const long long nrows = (long long)g.ny * g.nz;
     const long long row0 = (long long)blockIdx.x * rows;
     const int tid = threadIdx.x, nthr = blockDim.x;
@@ -312,7 +413,7 @@ __global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) ifftx_kernel(Geo 
         }
     }
     __syncthreads();
-    smem_fft<R, true, false>(buf, lM, __ffs(rows) - 1, LS, 1, tw, NT);
+    run_fft<R, true, false, LOGN>(buf, lM, __ffs(rows) - 1, LS, 1, tw, NT, twn);
     for (int e = tid; e < (rows << lM); e += nthr) {
         const int r = e >> lM, n = e & (M - 1);
         const long long row = row0 + r;
@@ -325,11 +426,14 @@ __global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) ifftx_kernel(Geo 
 
 // ---- complex transform along y (MODE 0 forward, 1 inverse) ----------------------
 // CTA: tile of `tpx` consecutive kx columns at one kz, all ky.
-template <typename R, int MODE>
+template <typename R, int MODE, int LOGN = 0>
 __global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) ffty_kernel(Geo g, cplx<R>* __restrict__ S, const cplx<R>* __restrict__ tw,
                                                    int NT, int tpx) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<R>* buf = reinterpret_cast<cplx<R>*>(smem_raw);
+    if (LOGN > 0) tpx = 1 << (11 - LOGN);
+    cplx<R>* twn = buf + g.ny * tpx;
+    stage_roots<R, LOGN>(twn, tw, NT);
     const int Mh = g.nx / 2 + 1;
     const int k = blockIdx.y, p0 = blockIdx.x * tpx;
     const int tid = threadIdx.x, nthr = blockDim.x;
@@ -341,7 +445,7 @@ __global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) ffty_kernel(Geo g
         buf[e] = p < Mh ? S[base + (long long)jj * Mh + p] : cmk<R>(R(0), R(0));
     }
     __syncthreads();
-    smem_fft<R, MODE == 1, true>(buf, __ffs(g.ny) - 1, __ffs(tpx) - 1, 1, tpx, tw, NT);
+    run_fft<R, MODE == 1, true, LOGN>(buf, __ffs(g.ny) - 1, __ffs(tpx) - 1, 1, tpx, tw, NT, twn);
     for (int e = tid; e < g.ny * tpx; e += nthr) {
         const int jj = e >> lt, c = e & (tpx - 1), p = p0 + c;
         if (p < Mh) S[base + (long long)jj * Mh + p] = buf[e];
@@ -349,13 +453,16 @@ __global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) ffty_kernel(Geo g
 }
 
 // ---- periodic z: forward, scale by nrm/lambda, inverse -------------------------
-template <typename R>
+template <typename R, int LOGN = 0>
 __global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) fftz_solve_kernel(Geo g, cplx<R>* __restrict__ S, const cplx<R>* __restrict__ tw,
                                                          int NT, int tpx, const double* __restrict__ kx2,
                                                          const double* __restrict__ ky2, const double* __restrict__ kz2,
                                                          double nrm) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<R>* buf = reinterpret_cast<cplx<R>*>(smem_raw);
+    if (LOGN > 0) tpx = 1 << (11 - LOGN);
+    cplx<R>* twn = buf + g.nz * tpx;
+    stage_roots<R, LOGN>(twn, tw, NT);
     const int Mh = g.nx / 2 + 1;
     const int j = blockIdx.y, p0 = blockIdx.x * tpx;
     const int tid = threadIdx.x, nthr = blockDim.x;
@@ -368,7 +475,7 @@ __global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) fftz_solve_kernel
         buf[e] = p < Mh ? S[base + kz * sk + p] : cmk<R>(R(0), R(0));
     }
     __syncthreads();
-    smem_fft<R, false, true>(buf, __ffs(g.nz) - 1, __ffs(tpx) - 1, 1, tpx, tw, NT);
+    run_fft<R, false, true, LOGN>(buf, __ffs(g.nz) - 1, __ffs(tpx) - 1, 1, tpx, tw, NT, twn);
     for (int e = tid; e < g.nz * tpx; e += nthr) {
         const int kz = e >> lt, c = e & (tpx - 1), p = p0 + c;
         if (p < Mh) {
@@ -379,7 +486,7 @@ __global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) fftz_solve_kernel
         }
     }
     __syncthreads();
-    smem_fft<R, true, true>(buf, __ffs(g.nz) - 1, __ffs(tpx) - 1, 1, tpx, tw, NT);
+    run_fft<R, true, true, LOGN>(buf, __ffs(g.nz) - 1, __ffs(tpx) - 1, 1, tpx, tw, NT, twn);
     for (int e = tid; e < g.nz * tpx; e += nthr) {
         const int kz = e >> lt, c = e & (tpx - 1), p = p0 + c;
         if (p < Mh) S[base + kz * sk + p] = buf[e];
@@ -627,12 +734,15 @@ __global__ void __launch_bounds__(32) thomas_kernel(Geo g, cplx<R>* S, cplx<RD>*
 }
 
 // r2c of an interior source along x: pack pairs, FFT, post-process.
-template <typename R>
+template <typename R, int LOGN = 0>
 __global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) src_fftx_kernel(Geo g, const R* __restrict__ src, cplx<R>* __restrict__ S,
                                                        const cplx<R>* __restrict__ tw, int NT, int rows) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<R>* buf = reinterpret_cast<cplx<R>*>(smem_raw);
-    const int M = g.nx / 2, Mh = M + 1, lM = __ffs(M) - 1, LS = xrow(M);
+    const int M = LOGN > 0 ? (1 << LOGN) : g.nx / 2, Mh = M + 1, lM = LOGN > 0 ? LOGN : __ffs(M) - 1, LS = xrow(M);
+    if (LOGN > 0) rows = 1 << (11 - LOGN);
+    cplx<R>* twn = buf + rows * LS;
+    stage_roots<R, LOGN>(twn, tw, NT);
     const long long nrows = (long long)g.ny * g.nz;
     const long long row0 = (long long)blockIdx.x * rows;
     const int tid = threadIdx.x, nthr = blockDim.x;
@@ -645,7 +755,7 @@ __global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) src_fftx_kernel(G
         buf[r * LS + sk16<true>(n)] = z;
     }
     __syncthreads();
-    smem_fft<R, false, false>(buf, lM, __ffs(rows) - 1, LS, 1, tw, NT);
+    run_fft<R, false, false, LOGN>(buf, lM, __ffs(rows) - 1, LS, 1, tw, NT, twn);
     const int tstep = NT / g.nx;
     for (int e = tid; e < (rows << lM); e += nthr) {
         const int r = e >> lM, kk = e & (M - 1);

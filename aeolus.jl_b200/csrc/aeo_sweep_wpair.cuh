@@ -51,14 +51,14 @@ __device__ __forceinline__ F2 f2pick(bool px, bool py, F2 a, F2 b) {
 // weno5_left (aeo_sweep.cuh) on two faces
 template <int ADV>
 __device__ __forceinline__ F2 weno5_left_f2(F2 v1, F2 v2, F2 v3, F2 v4, F2 v5) {
-    // the candidate values and second differences with the 1/6 and 1/2 folded
-    // into the coefficients (one rounding fewer than the scalar form's)
-    const F2 half(0.5f), c133(float(13.0 / 3.0));
-    const F2 c13(float(1.0 / 3.0)), c16(float(1.0 / 6.0)), c56(float(5.0 / 6.0)), c76(float(7.0 / 6.0)),
-        c116(float(11.0 / 6.0));
-    const F2 q0 = c13 * v1 - c76 * v2 + c116 * v3;
-    const F2 q1 = c56 * v3 - c16 * v2 + c13 * v4;
-    const F2 q2 = c13 * v3 + c56 * v4 - c16 * v5;
+    // the candidate values as the integer combinations over 6 (rounded
+    // coefficients 1/3, 7/6, 11/6 would not sum to one, and a uniform field
+    // would reconstruct with a bias that drifts the kinetic energy); the half
+    // second differences with the 1/2 folded in (exact for a uniform field)
+    const F2 s6(float(1.0 / 6.0)), two(2.f), half(0.5f), c133(float(13.0 / 3.0));
+    const F2 q0 = F2(two * v1 - F2(7.f) * v2 + F2(11.f) * v3) * s6;
+    const F2 q1 = F2(F2(5.f) * v3 - v2 + two * v4) * s6;
+    const F2 q2 = F2(two * v3 + F2(5.f) * v4 - v5) * s6;
     const F2 d2a = half * (v1 + v3) - v2;
     const F2 d2b = half * (v2 + v4) - v3;
     const F2 d2c = half * (v3 + v5) - v4;

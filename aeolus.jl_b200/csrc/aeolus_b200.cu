@@ -42,6 +42,17 @@
 #include "aeo_sweep.cuh"
 #include "aeo_sweep_pair.cuh"
 #include "aeo_sweep_wpair.cuh"
+
+// A transform kernel at a compile-time length 2^LG (128, 256 or 512 points:
+// the lines fill the CTA's 2048 points) or its general form (LG = 0).
+#define AEO_FFT_LEN(L, CALL)                                  \
+    switch (L) {                                              \
+        case 7: { constexpr int LG = 7; CALL; } break;        \
+        case 8: { constexpr int LG = 8; CALL; } break;        \
+        case 9: { constexpr int LG = 9; CALL; } break;        \
+        default: { constexpr int LG = 0; CALL; } break;       \
+    }
+static inline int ilog2i(int n) { int l = 0; while ((1 << (l + 1)) <= n) ++l; return l; }
 #include "aeo_sweep_tile.cuh"
 
 static std::string g_create_error;
@@ -804,8 +815,10 @@ struct Core : CoreBase {
         const int M = g.nx / 2;
         size_t smx = (size_t)rows_x * xrow(M) * sizeof(cplx<R>);
         unsigned gx = (unsigned)((g.ny * (long long)g.nz + rows_x - 1) / rows_x);
+        const int lgx = ilog2i(M), lgy = ilog2i(g.ny), lgz = ilog2i(g.nz);
         if (src) {
-            src_fftx_kernel<R><<<gx, FFT_THREADS(R), smx, st>>>(g, src, S, tw, NT, rows_x);
+            AEO_FFT_LEN(lgx, (src_fftx_kernel<R, LG><<<gx, FFT_THREADS(R), smx + roots_smem<R>(LG), st>>>(
+                                 g, src, S, tw, NT, rows_x)));
         } else {
             // the divergence into phi (overwritten by the c2r at the end), then its r2c
             if (anel && uni) div_kernel<R, true, true><<<gvec(), 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi);
@@ -813,21 +826,23 @@ struct Core : CoreBase {
             else if (uni) div_kernel<R, false, true><<<gvec(), 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi);
             else div_kernel<R, false, false><<<gvec(), 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi);
             CKL();
-            src_fftx_kernel<R><<<gx, FFT_THREADS(R), smx, st>>>(g, phi, S, tw, NT, rows_x);
+            AEO_FFT_LEN(lgx, (src_fftx_kernel<R, LG><<<gx, FFT_THREADS(R), smx + roots_smem<R>(LG), st>>>(
+                                 g, phi, S, tw, NT, rows_x)));
         }
         CKL();
         mark(AEO_K_DIV_FFTX);
         const int Mh = M + 1;
         dim3 gy((Mh + tpx_y - 1) / tpx_y, g.nz);
         size_t smy = (size_t)tpx_y * g.ny * sizeof(cplx<R>);
-        ffty_kernel<R, 0><<<gy, FFT_THREADS(R), smy, st>>>(g, S, tw, NT, tpx_y);
+        AEO_FFT_LEN(lgy, (ffty_kernel<R, 0, LG><<<gy, FFT_THREADS(R), smy + roots_smem<R>(LG), st>>>(g, S, tw, NT, tpx_y)));
         CKL();
         mark(AEO_K_FFTY);
         if (cfg.solver == AEO_SOLVER_FFT) {
             dim3 gz((Mh + tpx_z - 1) / tpx_z, g.ny);
             size_t smz = (size_t)tpx_z * g.nz * sizeof(cplx<R>);
             double nrm = 1.0 / ((double)g.nx * g.ny * g.nz);
-            fftz_solve_kernel<R><<<gz, FFT_THREADS(R), smz, st>>>(g, S, tw, NT, tpx_z, kx2, ky2, kz2, nrm);
+            AEO_FFT_LEN(lgz, (fftz_solve_kernel<R, LG><<<gz, FFT_THREADS(R), smz + roots_smem<R>(LG), st>>>(
+                                 g, S, tw, NT, tpx_z, kx2, ky2, kz2, nrm)));
         } else {
             size_t smt = thomas_smem(g, true);
             if (smt > 48 * 1024)
@@ -840,11 +855,12 @@ struct Core : CoreBase {
         }
         CKL();
         mark(AEO_K_ZSOLVE);
-        ffty_kernel<R, 1><<<gy, FFT_THREADS(R), smy, st>>>(g, S, tw, NT, tpx_y);
+        AEO_FFT_LEN(lgy, (ffty_kernel<R, 1, LG><<<gy, FFT_THREADS(R), smy + roots_smem<R>(LG), st>>>(g, S, tw, NT, tpx_y)));
         CKL();
         mark(AEO_K_FFTY);
         R scale = cfg.solver == AEO_SOLVER_FFT ? R(1) : R(1.0 / ((double)g.nx * g.ny));
-        ifftx_kernel<R><<<gx, FFT_THREADS(R), smx, st>>>(g, S, phi, tw, NT, rows_x, scale);
+        AEO_FFT_LEN(lgx, (ifftx_kernel<R, LG><<<gx, FFT_THREADS(R), smx + roots_smem<R>(LG), st>>>(
+                             g, S, phi, tw, NT, rows_x, scale)));
         CKL();
         mark(AEO_K_IFFTX);
         return AEO_OK;
