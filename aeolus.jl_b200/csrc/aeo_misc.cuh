@@ -58,12 +58,23 @@ __global__ void __launch_bounds__(256) halo_fill_kernel(Geo g, HaloSet<R> hs) {
     int i, j, k;
     shell_point(g, t, &i, &j, &k);
     int ii = wrapi(i, g.nx), jj = wrapi(j, g.ny);
-    for (int f = 0; f < hs.nf; ++f) {
-        int kk;
-        int s = zmap(g, k, hs.loc[f], &kk);
-        R v = s == 0 ? R(0) : hs.f[f][pidx(g, ii, jj, kk)];
-        hs.f[f][pidx(g, i, j, k)] = s < 0 ? -v : v;
+    // every field's source first, then the stores: the loads do not wait for
+    // the stores of the fields before them (the arrays could alias, as far as
+    // the compiler knows), so one memory latency a point instead of one a field
+    R v[5];
+#pragma unroll
+    for (int f = 0; f < 5; ++f) {
+        if (f < hs.nf) {
+            int kk;
+            const int s = zmap(g, k, hs.loc[f], &kk);
+            v[f] = s == 0 ? R(0) : hs.f[f][pidx(g, ii, jj, kk)];
+            if (s < 0) v[f] = -v[f];
+        }
     }
+    const long long q = pidx(g, i, j, k);
+#pragma unroll
+    for (int f = 0; f < 5; ++f)
+        if (f < hs.nf) hs.f[f][q] = v[f];
 }
 
 // The wall face of w (interior k = 0) is zero after every fill.
