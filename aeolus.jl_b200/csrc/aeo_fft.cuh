@@ -734,9 +734,42 @@ __global__ void __launch_bounds__(32) thomas_kernel(Geo g, cplx<R>* S, cplx<RD>*
 }
 
 // r2c of an interior source along x: pack pairs, FFT, post-process.
-template <typename R, int LOGN = 0>
+// DIV: the source is the divergence of the predicted velocity (us, vs, ws:
+// interior arrays), formed while the rows are staged with div_kernel's
+// arithmetic (plain, or W-weighted for the sound-proof core), instead of
+// being read from src: the divergence never goes to memory.
+template <typename R, bool ANEL, bool UNI>
+__device__ __forceinline__ cplx<R> div_pair(const Geo& g, const R* __restrict__ us, const R* __restrict__ vs,
+                                            const R* __restrict__ ws, long long row, int i0) {
+    const int j = (int)(row % g.ny), k = (int)(row / g.ny);
+    const long long q = row * g.nx + i0, pl = (long long)g.nx * g.ny;
+    const Met<R, UNI> m(g);
+    const R uc0 = __ldg(us + q), uc1 = __ldg(us + q + 1);
+    const R ue = __ldg(us + (i0 + 2 < g.nx ? q + 2 : q + 2 - g.nx));
+    const long long qn = j + 1 < g.ny ? q + g.nx : q - (long long)(g.ny - 1) * g.nx;
+    const R vc0 = __ldg(vs + q), vc1 = __ldg(vs + q + 1), vn0 = __ldg(vs + qn), vn1 = __ldg(vs + qn + 1);
+    const R wc0 = __ldg(ws + q), wc1 = __ldg(ws + q + 1);
+    R wn0 = R(0), wn1 = R(0);   // the top wall face
+    if (k + 1 < g.nz) { wn0 = __ldg(ws + q + pl); wn1 = __ldg(ws + q + pl + 1); }
+    else if (g.bc_z == 0) {
+        const long long qb = q - (long long)(g.nz - 1) * pl;
+        wn0 = __ldg(ws + qb); wn1 = __ldg(ws + qb + 1);
+    }
+    const R idx = R(g.idx), idy = R(g.idy), idz = m.idz(k);
+    if (ANEL) {
+        const R wcv = m.wc(k), wfb = m.wf(k), wft = m.wf(k + 1);
+        return cmk<R>(wcv * ((uc1 - uc0) * idx + (vn0 - vc0) * idy) + (wft * wn0 - wfb * wc0) * idz,
+                      wcv * ((ue - uc1) * idx + (vn1 - vc1) * idy) + (wft * wn1 - wfb * wc1) * idz);
+    }
+    return cmk<R>((uc1 - uc0) * idx + (vn0 - vc0) * idy + (wn0 - wc0) * idz,
+                  (ue - uc1) * idx + (vn1 - vc1) * idy + (wn1 - wc1) * idz);
+}
+
+template <typename R, int LOGN = 0, int DIV = 0>   // DIV: 0 src; 1 plain, 2 W-weighted divergence (+4: stretched)
 __global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) src_fftx_kernel(Geo g, const R* __restrict__ src, cplx<R>* __restrict__ S,
-                                                       const cplx<R>* __restrict__ tw, int NT, int rows) {
+                                                       const cplx<R>* __restrict__ tw, int NT, int rows,
+                                                       const R* __restrict__ us = nullptr, const R* __restrict__ vs = nullptr,
+                                                       const R* __restrict__ ws = nullptr) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<R>* buf = reinterpret_cast<cplx<R>*>(smem_raw);
     const int M = LOGN > 0 ? (1 << LOGN) : g.nx / 2, Mh = M + 1, lM = LOGN > 0 ? LOGN : __ffs(M) - 1, LS = xrow(M);
@@ -751,7 +784,10 @@ __global__ void __launch_bounds__(FFT_THREADS(R), FFT_MINB(R)) src_fftx_kernel(G
         const int r = e >> lM, n = e & (M - 1);
         const long long row = row0 + r;
         cplx<R> z = cmk<R>(R(0), R(0));
-        if (row < nrows) z = cmk<R>(src[row * g.nx + 2 * n], src[row * g.nx + 2 * n + 1]);
+        if (row < nrows) {
+            if constexpr (DIV == 0) z = cmk<R>(src[row * g.nx + 2 * n], src[row * g.nx + 2 * n + 1]);
+            else z = div_pair<R, (DIV & 3) == 2, (DIV & 4) == 0>(g, us, vs, ws, row, 2 * n);
+        }
         buf[r * LS + sk16<true>(n)] = z;
     }
     __syncthreads();

@@ -819,6 +819,18 @@ struct Core : CoreBase {
         if (src) {
             AEO_FFT_LEN(lgx, (src_fftx_kernel<R, LG><<<gx, FFT_THREADS(R), smx + roots_smem<R>(LG), st>>>(
                                  g, src, S, tw, NT, rows_x)));
+        } else if (lgx >= 7 && lgx <= 9) {
+            // the divergence formed in the r2c's staging (it never goes to memory)
+            const int dv = (anel ? 2 : 1) | (uni ? 0 : 4);
+#define AEO_SRC_DIV(D) AEO_FFT_LEN(lgx, (src_fftx_kernel<R, LG, D><<<gx, FFT_THREADS(R), smx + roots_smem<R>(LG), st>>>( \
+                                             g, nullptr, S, tw, NT, rows_x, Q[0], Q[1], Q[2])))
+            switch (dv) {
+                case 1: AEO_SRC_DIV(1); break;
+                case 2: AEO_SRC_DIV(2); break;
+                case 5: AEO_SRC_DIV(5); break;
+                default: AEO_SRC_DIV(6); break;
+            }
+#undef AEO_SRC_DIV
         } else {
             // the divergence into phi (overwritten by the c2r at the end), then its r2c
             if (anel && uni) div_kernel<R, true, true><<<gvec(), 256, 0, st>>>(g, Q[0], Q[1], Q[2], phi);
