@@ -22,7 +22,7 @@ import numpy as np
 from . import _lib
 from .grids import PERIODIC, WALL, Grid
 from .reference_state import anelastic_profiles
-from .spec import ADVECTION, CORES, FIELDS, PRECISIONS, SGS_MODELS, SOLVERS, CoreSpec
+from .spec import ADVECTION, CORES, FIELDS, PRECISIONS, SGS_MODELS, SOLVERS, CoreSpec, sgs_model_code
 
 _D = C.POINTER(C.c_double)
 
@@ -75,7 +75,7 @@ class Simulation:
         cfg.stretched = 1 if g.stretched else 0
         cfg.core = CORES[spec.core]
         cfg.advection = ADVECTION[spec.advection]
-        cfg.sgs_model = SGS_MODELS[spec.sgs]
+        cfg.sgs_model = sgs_model_code(spec)
         cfg.solver = SOLVERS[spec.solver]
         cfg.precision = PRECISIONS[spec.precision]
         cfg.nu, cfg.theta0, cfg.g, cfg.f_coriolis = spec.nu, spec.theta0, spec.g, spec.f_coriolis

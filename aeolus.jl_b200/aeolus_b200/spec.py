@@ -38,6 +38,8 @@ class CoreSpec:
                                         # sigma (c_s is C_sigma, 1.35 in the reference) or amd (c_s is the
                                         # AMD constant C, 0.3 in the reference; its own kappa_t) or dynamic
                                         # (Germano-Lilly, plane-averaged; c_s is the clip cs_max, 0.5)
+    averaging: str = "plane"            # the dynamic closure's <.>: "plane" (each level) or "local" (each
+                                        # cell its own clipped ratio; DynamicSmagorinsky(averaging = :local))
     pr_t: float = 1.0 / 3.0
     flux_bot: float = 0.0
     flux_top: float = 0.0
@@ -85,6 +87,8 @@ class CoreSpec:
             raise ValueError("pr_t must be positive")
         if self.sgs not in SGS_MODELS:
             raise ValueError(f"sgs must be one of {list(SGS_MODELS)}, got {self.sgs!r}")
+        if self.averaging not in ("plane", "local"):
+            raise ValueError(f"averaging must be 'plane' or 'local', got {self.averaging!r} (src/Operators.jl:558-559)")
         if self.sgs in ("vreman", "sigma", "amd", "dynamic") and self.grid.stretched:
             raise ValueError("the Vreman, sigma and AMD closures take a RegularGrid only (compute_vreman_nut!, "
                              "src/operators/sgs_amd_vreman.jl:280-284; compute_amd_coefficients!, :102-107; "
@@ -93,3 +97,11 @@ class CoreSpec:
             raise ValueError("the dynamic Smagorinsky closure needs halos of at least 2 (src/Operators.jl:556-557)")
         if self.sgs == "amd" and self.c_s != 0 and self.core != "boussinesq":
             raise ValueError("the AMD closure is built for the Boussinesq core")
+
+
+def sgs_model_code(spec) -> int:
+    """The C-ABI's AEO_SGS_* of a spec (the dynamic closure with :local
+    averaging is its own code)."""
+    if spec.sgs == "dynamic" and spec.averaging == "local":
+        return 5
+    return SGS_MODELS[spec.sgs]

@@ -35,7 +35,7 @@ template <typename R, bool UNI, bool SGS>
 __global__ void __launch_bounds__(256) cfl_levels_kernel(Geo g, const R* __restrict__ u, const R* __restrict__ v,
                                                          const R* __restrict__ w, const R* __restrict__ th, R c_s,
                                                          R bg, R pr_t, const double* __restrict__ cs2, double dd2,
-                                                         double* __restrict__ part) {
+                                                         double* __restrict__ part, const R* __restrict__ cs2f = nullptr) {
     __shared__ double rmax[256], nmax[256], tsum[256], kmax[256];
     const int k = blockIdx.x;
     const double iz = UNI ? g.idz : lvl(g.idzc, k);
@@ -53,7 +53,8 @@ __global__ void __launch_bounds__(256) cfl_levels_kernel(Geo g, const R* __restr
         if (SGS) {
             Nb<R> U{u + q, g.sy, g.sz}, V{v + q, g.sy, g.sz}, W{w + q, g.sy, g.sz};
             if (g.sgs_model == 4) {   // dynamic Smagorinsky: cs2(k) Delta^2 |S|
-                nm = fmax(nm, (double)(R(cs2[k] * dd2) * strain_at<R, UNI>(Met<R, UNI>(g), g, k, U, V, W, (R*)nullptr)));
+                nm = fmax(nm, (double)(R(dyn_cs2_cell(g, cs2, cs2f, i, j, k) * dd2) *
+                                       strain_at<R, UNI>(Met<R, UNI>(g), g, k, U, V, W, (R*)nullptr)));
             } else if (g.sgs_model == 3) {
                 Nb<R> T{th + q, g.sy, g.sz};
                 const NuKappa<R> nk = amd_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, bg, pr_t, U, V, W, T);

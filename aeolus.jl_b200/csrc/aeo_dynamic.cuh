@@ -10,7 +10,9 @@
 // sums the 21 test-filtered quantities over each interior cell's box (z
 // outer, x inner), forms L^d_ij M_ij and M_ij M_ij and reduces them per level
 // chunk; the level pass adds the chunks and clips LM / MM. The sweep then
-// evaluates nu_t = cs2(k) Delta^2 |S| in its coefficient pass.
+// evaluates nu_t = cs2(k) Delta^2 |S| in its coefficient pass.  With the
+// :local averaging pass 2 writes each cell's clipped LM / MM instead (a
+// padded field with filled halos) and nu_t = cs2(i, j, k) Delta^2 |S|.
 #pragma once
 
 #include "aeo_sweep.cuh"
@@ -49,9 +51,13 @@ __global__ void __launch_bounds__(256) germano_pass1_kernel(Geo g, const R* __re
 
 // Pass 2 (_germano_pass2_body! / _germano_LM_MM): blocks of 256 cells of one
 // level (grid.y = level); per block the sums of LM and MM into part.
-template <typename R>
+// LOCAL (averaging = :local, _local_cs2_body!): every interior cell's own
+// clipped ratio goes to the padded field cs2f (its halos filled afterwards
+// like a cell-centred field's) and no partials are written.
+template <typename R, bool LOCAL = false>
 __global__ void __launch_bounds__(256) germano_pass2_kernel(Geo g, DynWs<R> ws, R inv27, R d2, R a2,
-                                                            double* __restrict__ part) {
+                                                            double* __restrict__ part, R* __restrict__ cs2f = nullptr,
+                                                            double cs2max = 0.0) {
     __shared__ double slm[256], smm[256];
     const int k = blockIdx.y;
     const int e = blockIdx.x * 256 + threadIdx.x;
@@ -90,7 +96,9 @@ __global__ void __launch_bounds__(256) germano_pass2_kernel(Geo g, DynWs<R> ws, 
         const R M12 = c2 * t[18] - c1 * A12, M13 = c2 * t[19] - c1 * A13, M23 = c2 * t[20] - c1 * A23;
         lmv = L11 * M11 + L22 * M22 + L33 * M33 + R(2) * (L12 * M12 + L13 * M13 + L23 * M23);
         mmv = M11 * M11 + M22 * M22 + M33 * M33 + R(2) * (M12 * M12 + M13 * M13 + M23 * M23);
+        if (LOCAL) cs2f[pidx(g, i, j, k)] = R(mmv > 0 ? fmin(fmax(lmv / mmv, 0.0), cs2max) : 0.0);
     }
+    if (LOCAL) return;
     slm[threadIdx.x] = lmv;
     smm[threadIdx.x] = mmv;
     __syncthreads();
@@ -123,4 +131,10 @@ __global__ void germano_level_kernel(int nz, int nb, const double* __restrict__ 
 // the coefficient of level k (a halo level of a periodic z wraps)
 __device__ __forceinline__ double dyn_cs2_at(const Geo& g, const double* cs2, int k) {
     return cs2[k < 0 ? k + g.nz : (k >= g.nz ? k - g.nz : k)];
+}
+// the coefficient of cell (i, j, k): the padded per-cell field of the :local
+// averaging (halos filled), else the level's
+template <typename R>
+__device__ __forceinline__ double dyn_cs2_cell(const Geo& g, const double* cs2, const R* cs2f, int i, int j, int k) {
+    return cs2f ? (double)cs2f[pidx(g, i, j, k)] : dyn_cs2_at(g, cs2, k);
 }

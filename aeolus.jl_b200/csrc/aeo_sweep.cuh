@@ -43,6 +43,7 @@ struct SweepArgs {
     R c_s;
     R sgs_bg;       // g / theta0 of the AMD closure's buoyancy term (0: none)
     const double* cs2;  // the dynamic Smagorinsky coefficient per level
+    const R* cs2f;      // ... or per cell (averaging = :local; padded, halos filled; else nullptr)
     double dyn_d2;      // ... and its Delta^2 = (dx dy dz)^(2/3)
     int kofs;       // the AMD closure: its kappa_t sits kofs elements past nut_t (0: kappa_t = nut_t / Pr_t)
 };
@@ -694,7 +695,8 @@ template <typename R, bool UNI>
 __global__ void __launch_bounds__(256) smagorinsky_kernel(Geo g, const R* __restrict__ u, const R* __restrict__ v,
                                                           const R* __restrict__ w, const R* __restrict__ th,
                                                           R* __restrict__ nut, R c_s, R bg, R pr_t,
-                                                          const double* __restrict__ cs2, double dd2) {
+                                                          const double* __restrict__ cs2, double dd2,
+                                                          const R* __restrict__ cs2f = nullptr) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int j = blockIdx.y * blockDim.y + threadIdx.y;
     int k = blockIdx.z * blockDim.z + threadIdx.z;
@@ -702,7 +704,7 @@ __global__ void __launch_bounds__(256) smagorinsky_kernel(Geo g, const R* __rest
     const long long q = pidx(g, i, j, k);
     Nb<R> U{u + q, g.sy, g.sz}, V{v + q, g.sy, g.sz}, W{w + q, g.sy, g.sz};
     if (g.sgs_model == 4) {
-        nut[q] = R(cs2[k] * dd2) * strain_at<R, UNI>(Met<R, UNI>(g), g, k, U, V, W, (R*)nullptr);
+        nut[q] = R(dyn_cs2_cell(g, cs2, cs2f, i, j, k) * dd2) * strain_at<R, UNI>(Met<R, UNI>(g), g, k, U, V, W, (R*)nullptr);
     } else if (g.sgs_model == 3) {
         Nb<R> T{th + q, g.sy, g.sz};
         nut[q] = amd_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, bg, pr_t, U, V, W, T).nu;

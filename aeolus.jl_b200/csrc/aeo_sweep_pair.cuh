@@ -113,7 +113,7 @@ struct PairNut {
 // the 32 interior pairs, the two edge pairs of every row come last.
 template <int CLOS, bool UNI, class S>
 __device__ __forceinline__ void pair_nut_plane(const Met<float, UNI>& m, const SweepArgs<float>& a, const Geo& g,
-                                               int L, const float* const* sp, float* np, int tid) {
+                                               int L, const float* const* sp, float* np, int tid, int i0, int j0) {
     using R = float;
     for (int e = tid; e < S::NPAIR * S::NPH; e += S::NT) {
         int cj, pc;
@@ -126,7 +126,10 @@ __device__ __forceinline__ void pair_nut_plane(const Met<float, UNI>& m, const S
         const PairAcc<1, S::PW, S::PSZA> Vq{q};
         const PairAcc<1, S::PW, 2 * S::PSZA> Wq{q};
         if constexpr (CLOS == 2) {
-            const F2 c = F2(float(dyn_cs2_at(g, a.cs2, L) * a.dyn_d2));
+            // the pair's cells: global x = i0 + 2 pc - 2 (even), y = j0 + cj - 1
+            const F2 c = a.cs2f ? F2(*reinterpret_cast<const float2*>(a.cs2f + pidx(g, i0 + 2 * pc - 2, j0 + cj - 1, L))) *
+                                      F2(float(a.dyn_d2))
+                                : F2(float(dyn_cs2_at(g, a.cs2, L) * a.dyn_d2));
             const F2 nv = c * strain_at<R, UNI>(m, g, L, Uq, Vq, Wq, (F2*)nullptr);
             *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nv.v;
         } else if constexpr (CLOS == 1) {
@@ -225,7 +228,7 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(const __grid_constan
             for (int L = kbeg - 1; L <= kbeg + 1; ++L) {
                 if (g.bc_z == 1 && (L < 0 || L >= g.nz)) continue;
                 const float* sp[3] = {plane(L - 1), plane(L), plane(L + 1)};
-                pair_nut_plane<CLOS, UNI, S>(m, a, g, L, sp, nut_plane(L), tid);
+                pair_nut_plane<CLOS, UNI, S>(m, a, g, L, sp, nut_plane(L), tid, i0, j0);
             }
         failed = __syncthreads_or(!ok);
         if (SGS && !failed && g.bc_z == 1 && (kbeg == 0 || kbeg + 1 >= g.nz)) {
@@ -272,7 +275,7 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(const __grid_constan
                         for (int e = tid; e < S::NPS; e += S::NT) dst[e + S::KT_OFS] = srcp[e + S::KT_OFS];
                 } else if (ok) {
                     const float* sp[3] = {plane(L - 1), plane(L), plane(L + 1)};
-                    pair_nut_plane<CLOS, UNI, S>(m, a, g, L, sp, nut_plane(L), tid);
+                    pair_nut_plane<CLOS, UNI, S>(m, a, g, L, sp, nut_plane(L), tid, i0, j0);
                 }
             }
 

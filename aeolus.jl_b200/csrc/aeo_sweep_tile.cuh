@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
                     const SmAcc<R, 1, S::PW, S::PSZA> Vq{q};
                     const SmAcc<R, 1, S::PW, 2 * S::PSZA> Wq{q};
                     if constexpr (CLOS == 2) {
-                        const R c = R(dyn_cs2_at(g, a.cs2, L) * a.dyn_d2);
+                        const R c = R(dyn_cs2_cell(g, a.cs2, a.cs2f, i0 + ci - 1, j0 + cj - 1, L) * a.dyn_d2);
                         np[cj * S::NPW + ci] = c * strain_at<R, UNI>(m, g, L, Uq, Vq, Wq, (R*)nullptr);
                     } else if constexpr (CLOS == 1) {
                         const SmAcc<R, 1, S::PW, 3 * S::PSZA> Tq{q};

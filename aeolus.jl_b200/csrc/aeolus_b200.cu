@@ -180,11 +180,13 @@ struct Core : CoreBase {
     bool cflp_set = false;
     bool uni = true, sgs = false, anel = false;
     bool amd() const { return sgs && cfg.sgs_model == AEO_SGS_AMD; }
-    bool dyn() const { return sgs && cfg.sgs_model == AEO_SGS_DYNAMIC; }
+    bool dyn() const { return sgs && (cfg.sgs_model == AEO_SGS_DYNAMIC || cfg.sgs_model == AEO_SGS_DYNAMIC_LOCAL); }
+    bool dyn_local() const { return sgs && cfg.sgs_model == AEO_SGS_DYNAMIC_LOCAL; }
     // the dynamic Smagorinsky workspace: the ten pass-1 fields, the per-block
     // partials of LM and MM, the per-level coefficient
     DynWs<R> dws{};
     double* d_cs2 = nullptr;
+    R* d_cs2f = nullptr;       // the per-cell coefficient of the :local averaging (padded)
     double* d_dynpart = nullptr;
     int dyn_nb = 0;
     double dyn_d2 = 0.0;   // Delta^2 = (dx dy dz)^(2/3)
@@ -194,6 +196,14 @@ struct Core : CoreBase {
         germano_pass1_kernel<R><<<(unsigned)std::min<long long>((ns + 255) / 256, 148LL * 16), 256, 0, st>>>(
             g, in[0], in[1], in[2], dws);
         CKL();
+        if (dyn_local()) {
+            germano_pass2_kernel<R, true><<<dim3((unsigned)dyn_nb, (unsigned)g.nz), 256, 0, st>>>(
+                g, dws, R(1.0 / 27), R(dyn_d2), R(9.0), d_dynpart, d_cs2f, cfg.c_s * cfg.c_s);
+            CKL();
+            R* f[1] = {d_cs2f};
+            int l[1] = {LOC_C};
+            return halo(f, l, 1);
+        }
         germano_pass2_kernel<R><<<dim3((unsigned)dyn_nb, (unsigned)g.nz), 256, 0, st>>>(
             g, dws, R(1.0 / 27), R(dyn_d2), R(9.0), d_dynpart);
         CKL();
@@ -255,7 +265,7 @@ struct Core : CoreBase {
         uni = !c.stretched;
         sgs = c.c_s != 0.0;
         anel = c.core == AEO_CORE_ANELASTIC;
-        g.sgs_model = c.sgs_model;
+        g.sgs_model = c.sgs_model == AEO_SGS_DYNAMIC_LOCAL ? AEO_SGS_DYNAMIC : c.sgs_model;   // devices: cs2f set
         g.sgs_cv = 2.5 * c.c_s * c.c_s;
         if (sizeof(R) == sizeof(float)) th_off = anel ? (thf ? thf[c.hz] : 0.0) : c.theta0;
         g.nx = c.nx; g.ny = c.ny; g.nz = c.nz;
@@ -494,6 +504,8 @@ struct Core : CoreBase {
             dyn_nb = (g.nx * g.ny + 255) / 256;
             if (aeo_status e = alloc(&d_dynpart, 2 * (size_t)dyn_nb * g.nz)) return e;
             if (aeo_status e = alloc(&d_cs2, (size_t)g.nz)) return e;
+            if (dyn_local())
+                if (aeo_status e = alloc(&d_cs2f, padded_count())) return e;
             dyn_d2 = std::pow(g.dx * g.dy * g.dz, 2.0 / 3.0);
         }
         if (aeo_status e = alloc(&d_flag, 1)) return e;
@@ -923,6 +935,7 @@ struct Core : CoreBase {
         a.inv_prt = amd() ? R(1) : R(1.0 / cfg.pr_t);
         a.sgs_bg = amd_bg();
         a.cs2 = d_cs2;
+        a.cs2f = d_cs2f;
         a.dyn_d2 = dyn_d2;
         if (dyn())
             if (aeo_status e = enqueue_dynamic(P[s_in])) return e;
@@ -953,11 +966,11 @@ struct Core : CoreBase {
         if (dyn())
             if (aeo_status e = enqueue_dynamic(in)) return e;
         if (uni) {
-            if (sgs) cfl_levels_kernel<R, true, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_part);
-            else cfl_levels_kernel<R, true, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_part);
+            if (sgs) cfl_levels_kernel<R, true, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_part, d_cs2f);
+            else cfl_levels_kernel<R, true, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_part, d_cs2f);
         } else {
-            if (sgs) cfl_levels_kernel<R, false, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_part);
-            else cfl_levels_kernel<R, false, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_part);
+            if (sgs) cfl_levels_kernel<R, false, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_part, d_cs2f);
+            else cfl_levels_kernel<R, false, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_part, d_cs2f);
         }
         CKL();
         dt_pick_kernel<<<1, 32, 0, st>>>(g, cflp, d_part, d_sc);
@@ -1327,8 +1340,8 @@ struct Core : CoreBase {
             // the step keeps nut in shared memory: evaluate it for the current state
             if (dyn())
                 if (aeo_status e = enqueue_dynamic(P[cur])) return e;
-            if (uni) smagorinsky_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], P[cur][3], nut, R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2);
-            else smagorinsky_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], P[cur][3], nut, R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2);
+            if (uni) smagorinsky_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], P[cur][3], nut, R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_cs2f);
+            else smagorinsky_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], P[cur][3], nut, R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_cs2f);
             CKL();
         }
         S* stage = reinterpret_cast<S*>(d_stage);
@@ -1600,7 +1613,7 @@ static aeo_status validate(const aeo_config* c, const double* zf, const double* 
     if (c->precision != AEO_PREC_FP64 && c->precision != AEO_PREC_FP32_MIXED) { *m = "unknown precision"; return AEO_ERR_ARGUMENT; }
     if (c->c_s != 0.0 && !(c->pr_t > 0.0)) { *m = "pr_t must be positive with SGS"; return AEO_ERR_ARGUMENT; }
     if (c->sgs_model != AEO_SGS_SMAGORINSKY && c->sgs_model != AEO_SGS_VREMAN && c->sgs_model != AEO_SGS_SIGMA &&
-        c->sgs_model != AEO_SGS_AMD && c->sgs_model != AEO_SGS_DYNAMIC) {
+        c->sgs_model != AEO_SGS_AMD && c->sgs_model != AEO_SGS_DYNAMIC && c->sgs_model != AEO_SGS_DYNAMIC_LOCAL) {
         *m = "unknown SGS closure";
         return AEO_ERR_ARGUMENT;
     }
@@ -1609,7 +1622,8 @@ static aeo_status validate(const aeo_config* c, const double* zf, const double* 
              ":280-284, src/operators/sigma_closure.jl:208-212, src/Operators.jl:555)";
         return AEO_ERR_ARGUMENT;
     }
-    if (c->sgs_model == AEO_SGS_DYNAMIC && c->c_s != 0.0 && (c->hx < 2 || c->hy < 2 || c->hz < 2)) {
+    if ((c->sgs_model == AEO_SGS_DYNAMIC || c->sgs_model == AEO_SGS_DYNAMIC_LOCAL) && c->c_s != 0.0 &&
+        (c->hx < 2 || c->hy < 2 || c->hz < 2)) {
         *m = "the dynamic Smagorinsky closure needs host halos of at least 2 (src/Operators.jl:556-557)";
         return AEO_ERR_ARGUMENT;
     }

@@ -39,7 +39,8 @@ enum { AEO_CORE_BOUSSINESQ = 0, AEO_CORE_ANELASTIC = 1 };
 enum { AEO_ADV_CENTRED = 0, AEO_ADV_WENO_JS5 = 1, AEO_ADV_WENO_Z5 = 2 };
 enum { AEO_SOLVER_FFT = 0, AEO_SOLVER_COLUMN = 1, AEO_SOLVER_PCG = 2 };
 enum { AEO_PREC_FP64 = 0, AEO_PREC_FP32_MIXED = 1 };
-enum { AEO_SGS_SMAGORINSKY = 0, AEO_SGS_VREMAN = 1, AEO_SGS_SIGMA = 2, AEO_SGS_AMD = 3, AEO_SGS_DYNAMIC = 4 };
+enum { AEO_SGS_SMAGORINSKY = 0, AEO_SGS_VREMAN = 1, AEO_SGS_SIGMA = 2, AEO_SGS_AMD = 3, AEO_SGS_DYNAMIC = 4,
+       AEO_SGS_DYNAMIC_LOCAL = 5 };
 enum { AEO_FIELD_U = 0, AEO_FIELD_V = 1, AEO_FIELD_W = 2, AEO_FIELD_THETA = 3,
        AEO_FIELD_P = 4, AEO_FIELD_NUT = 5 };
 
@@ -88,7 +89,10 @@ typedef struct {
                                   test filter 3x3x3 with width ratio 3) with
                                   c_s = the clip cs_max (0.5 in the reference;
                                   DynamicSmagorinsky,
-                                  src/Operators.jl:497-900). Vreman, sigma,
+                                  src/Operators.jl:497-900), or the same with
+                                  averaging = :local (each cell its own
+                                  clipped ratio, _local_cs2_body!,
+                                  src/Operators.jl:873-880). Vreman, sigma,
                                   AMD and dynamic on uniform grids           */
 } aeo_config;
 

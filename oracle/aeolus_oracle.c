@@ -766,6 +766,11 @@ static void dyn_coefficients(oc_sim* s) {
             }
 #undef SH
     double cmax = P->c_s * P->c_s;
+    if (P->sgs_model == OC_SGS_DYNAMIC_LOCAL) {   /* _local_cs2_body!: each cell's own ratio, clipped */
+        for (size_t q = 0; q < ni; ++q)
+            s->dyn_lm[q] = s->dyn_mm[q] > 0 ? fmin(fmax(s->dyn_lm[q] / s->dyn_mm[q], 0.0), cmax) : 0.0;
+        return;
+    }
     for (int k = 0; k < Nz; ++k) {
         double lm = 0, mm = 0;
         for (int j = 0; j < Ny; ++j)
@@ -821,6 +826,11 @@ static inline double smag_at(const oc_sim* s, int i, int j, int k) {
     double S2 = 2 * (S11 * S11 + S22 * S22 + S33 * S33) + 4 * (S12 * S12 + S13 * S13 + S23 * S23);
     if (s->p.sgs_model == OC_SGS_DYNAMIC)   /* cs2(k) Delta^2 |S| (_dynamic_nut_body!), dyn_coefficients first */
         return s->cs2[k - s->p.hz] * pow(s->dx * s->dy * s->dz, 2.0 / 3.0) * sqrt(S2);
+    if (s->p.sgs_model == OC_SGS_DYNAMIC_LOCAL) {   /* cs2(i, j, k): the clipped ratios left in dyn_lm */
+        const oc_params* P = &s->p;
+        size_t q = (size_t)(i - P->hx) + (size_t)P->nx * ((size_t)(j - P->hy) + (size_t)P->ny * (size_t)(k - P->hz));
+        return s->dyn_lm[q] * pow(s->dx * s->dy * s->dz, 2.0 / 3.0) * sqrt(S2);
+    }
     return coef * sqrt(S2);
 }
 
@@ -936,7 +946,7 @@ static void compute_tendencies(oc_sim* s) {
     const double *u = s->u, *v = s->v, *w = s->w, *th = s->th;
 
     /* 4a. Smagorinsky coefficients, then their halos (velocity BCs) */
-    if (has_sgs && P->sgs_model == OC_SGS_DYNAMIC) dyn_coefficients(s);
+    if (has_sgs && (P->sgs_model == OC_SGS_DYNAMIC || P->sgs_model == OC_SGS_DYNAMIC_LOCAL)) dyn_coefficients(s);
     if (has_sgs) {
 #pragma omp parallel for collapse(2) schedule(static)
         for (int k = Hz; k < Hz + Nz; ++k)
@@ -1485,7 +1495,7 @@ double oc_adaptive_dt(oc_sim* s, const oc_cfl* c, double dt_prev, int* limiter) 
     fill_halos(s, s->u, LOC_FX);
     fill_halos(s, s->v, LOC_FY);
     fill_halos(s, s->w, LOC_FZ);
-    if (P->c_s != 0 && P->sgs_model == OC_SGS_DYNAMIC) dyn_coefficients(s);
+    if (P->c_s != 0 && (P->sgs_model == OC_SGS_DYNAMIC || P->sgs_model == OC_SGS_DYNAMIC_LOCAL)) dyn_coefficients(s);
     double rate = 0.0, nutm = 0.0, ktm = 0.0;
     int nanr = 0;
     double* mean = (double*)calloc((size_t)Nz, sizeof(double));
@@ -1769,7 +1779,7 @@ oc_sim* oc_create(const oc_params* p, const double* zfi, const double* wc, const
     if (p->solver == OC_SOLVER_COLUMN && p->bc_z != OC_BC_WALL) return NULL;
     if (p->stretched && (!zfi || p->bc_z != OC_BC_WALL)) return NULL;
     if ((p->sgs_model == OC_SGS_VREMAN || p->sgs_model == OC_SGS_SIGMA || p->sgs_model == OC_SGS_AMD ||
-         p->sgs_model == OC_SGS_DYNAMIC) && p->stretched)
+         p->sgs_model == OC_SGS_DYNAMIC || p->sgs_model == OC_SGS_DYNAMIC_LOCAL) && p->stretched)
         return NULL;
     if (p->sgs_model == OC_SGS_AMD && p->c_s != 0 && p->core != OC_CORE_BOUSSINESQ) return NULL;
     oc_sim* s = (oc_sim*)calloc(1, sizeof(oc_sim));

@@ -26,7 +26,8 @@ enum { OC_CORE_BOUSSINESQ = 0, OC_CORE_ANELASTIC = 1 };
 enum { OC_ADV_CENTRED = 0, OC_ADV_WENO_JS5 = 1, OC_ADV_WENO_Z5 = 2 };
 enum { OC_SOLVER_FFT = 0, OC_SOLVER_COLUMN = 1, OC_SOLVER_PCG = 2 };
 enum { OC_U = 0, OC_V = 1, OC_W = 2, OC_THETA = 3, OC_P = 4, OC_NUT = 5, OC_PHI = 6, OC_KT = 7 };
-enum { OC_SGS_SMAGORINSKY = 0, OC_SGS_VREMAN = 1, OC_SGS_SIGMA = 2, OC_SGS_AMD = 3, OC_SGS_DYNAMIC = 4 };
+enum { OC_SGS_SMAGORINSKY = 0, OC_SGS_VREMAN = 1, OC_SGS_SIGMA = 2, OC_SGS_AMD = 3, OC_SGS_DYNAMIC = 4,
+       OC_SGS_DYNAMIC_LOCAL = 5 };   /* 5: averaging = :local, src/Operators.jl:873-880 */
 
 typedef struct {
     int32_t nx, ny, nz, hx, hy, hz;

@@ -145,6 +145,8 @@ class OracleSimulation:
         p.flux_bot, p.flux_top = spec.flux_bot, spec.flux_top
         p.sponge_alpha, p.sponge_zstart = spec.sponge_alpha, spec.sponge_zstart
         p.sgs_model = {"smagorinsky": 0, "vreman": 1, "sigma": 2, "amd": 3, "dynamic": 4}[spec.sgs]
+        if spec.sgs == "dynamic" and getattr(spec, "averaging", "plane") == "local":
+            p.sgs_model = 5
         self._keep = [g.zf, spec.wc, spec.wf, spec.thf]
         h = lib.oc_create(C.byref(p), _p(g.zf), _p(spec.wc), _p(spec.wf), _p(spec.thf))
         if not h:

@@ -10,8 +10,8 @@ field; with a small cs_max the clip binds and nu_t is the static
 Smagorinsky nu_t of C_s = cs_max on every level the clip caps (and zero on
 the levels of net backscatter).  GPU (`-m gpu`):
 steps with the dynamic closure match the oracle to 1e-11 (FP64; walls and
-periodic z) and FP32-mixed to 1e-5; the nu_t diagnostic and the adaptive dt
-match the oracle.
+periodic z; plane and local averaging) and FP32-mixed to 1e-5; the nu_t
+diagnostic and the adaptive dt match the oracle.
 """
 import numpy as np
 import pytest
@@ -28,8 +28,9 @@ def grid(bc_z="wall"):
     return regular_grid((16, 16, 16), (1.0, 1.0, 0.5), halo=(3, 3, 3), bc_z=bc_z)
 
 
-def spec(g, sgs="dynamic", advection="centred", precision="fp64", c_s=CS_MAX):
-    return CoreSpec(grid=g, c_s=c_s, sgs=sgs, theta0=TH0, advection=advection, precision=precision)
+def spec(g, sgs="dynamic", advection="centred", precision="fp64", c_s=CS_MAX, averaging="plane"):
+    return CoreSpec(grid=g, c_s=c_s, sgs=sgs, theta0=TH0, advection=advection, precision=precision,
+                    averaging=averaging)
 
 
 def state(g, seed=5, amp=1.0):
@@ -49,9 +50,10 @@ def state(g, seed=5, amp=1.0):
     return u, v, w, th
 
 
-def dynamic_numpy(g, u, v, w, cs_max):
-    """_germano_pass1 / _germano_pass2 / _plane_cs2_body! / _dynamic_nut_body!
-    on storage arrays with filled halos: nu_t on the interior."""
+def dynamic_numpy(g, u, v, w, cs_max, local=False):
+    """_germano_pass1 / _germano_pass2 / _plane_cs2_body! (local:
+    _local_cs2_body!) / _dynamic_nut_body! on storage arrays with filled
+    halos: nu_t on the interior."""
     hx, hy, hz = g.halo
     nx, ny, nz = g.size
 
@@ -88,6 +90,9 @@ def dynamic_numpy(g, u, v, w, cs_max):
     M = [2 * d2 * (t[15 + c] - 9.0 * magSt * A[c]) for c in range(6)]
     LM = L[0] * M[0] + L[1] * M[1] + L[2] * M[2] + 2 * (L[3] * M[3] + L[4] * M[4] + L[5] * M[5])
     MM = M[0] ** 2 + M[1] ** 2 + M[2] ** 2 + 2 * (M[3] ** 2 + M[4] ** 2 + M[5] ** 2)
+    if local:
+        cs2 = np.where(MM > 0, np.clip(LM / np.where(MM > 0, MM, 1.0), 0.0, cs_max ** 2), 0.0)
+        return cs2 * d2 * ms[1:-1, 1:-1, 1:-1], cs2
     lm, mm = LM.sum(axis=(1, 2)), MM.sum(axis=(1, 2))
     cs2 = np.where(mm > 0, np.clip(lm / np.where(mm > 0, mm, 1.0), 0.0, cs_max ** 2), 0.0)
     return cs2[:, None, None] * d2 * ms[1:-1, 1:-1, 1:-1], cs2
@@ -102,6 +107,21 @@ def test_oracle_nut_is_the_dynamic_procedure():
     ref, cs2 = dynamic_numpy(g, *(o.get_field(n) for n in ("u", "v", "w")), CS_MAX)
     assert np.count_nonzero(cs2) >= len(cs2) // 2 and cs2.max() < CS_MAX ** 2
     assert np.abs(nut - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_oracle_nut_with_local_averaging():
+    """averaging = :local (src/Operators.jl:521-522, 873-880): every cell its
+    own clipped L^d:M / M:M; noisy, so some cells clip at cs_max^2 and some at 0."""
+    g = grid()
+    o = OracleSimulation(spec(g, averaging="local"))
+    o.set_state(*state(g))
+    o.tendencies()
+    nut = o.get_field("nut")[g.interior]
+    ref, cs2 = dynamic_numpy(g, *(o.get_field(n) for n in ("u", "v", "w")), CS_MAX, local=True)
+    assert np.count_nonzero(cs2 == 0) > 0 and np.count_nonzero((cs2 > 0) & (cs2 < CS_MAX ** 2)) > cs2.size // 4
+    assert np.abs(nut - ref).max() <= 1e-12 * np.abs(ref).max()
+    with pytest.raises(ValueError):
+        spec(g, averaging="box")
 
 
 def test_the_clip_gives_the_static_closure():
@@ -132,13 +152,16 @@ def test_dynamic_needs_a_uniform_grid_and_halos_of_two():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("advection,bc_z", [("centred", "wall"), ("weno_js5", "wall"), ("centred", "periodic")])
-def test_gpu_dynamic_steps_match_the_oracle(advection, bc_z):
+@pytest.mark.parametrize("advection,bc_z,averaging", [("centred", "wall", "plane"), ("weno_js5", "wall", "plane"),
+                                                      ("centred", "periodic", "plane"), ("centred", "wall", "local"),
+                                                      ("weno_js5", "wall", "local"), ("centred", "periodic", "local")])
+def test_gpu_dynamic_steps_match_the_oracle(advection, bc_z, averaging):
     from aeolus_b200.simulation import Simulation
     g = grid(bc_z)
     st = state(g)
-    sims = [OracleSimulation(spec(g, advection=advection)), Simulation(spec(g, advection=advection)),
-            Simulation(spec(g, advection=advection, precision="fp32_mixed"))]
+    kw = dict(advection=advection, averaging=averaging)
+    sims = [OracleSimulation(spec(g, **kw)), Simulation(spec(g, **kw)),
+            Simulation(spec(g, precision="fp32_mixed", **kw))]
     out = []
     for s in sims:
         s.set_state(*st)
@@ -153,16 +176,17 @@ def test_gpu_dynamic_steps_match_the_oracle(advection, bc_z):
     e32 = {n: np.linalg.norm(g32[n] - g64[n]) / np.linalg.norm(g64[n]) for n in FIELDS}
     assert all(e <= 1e-5 for e in e32.values()), e32
     nut = sims[1].get_field("nut")[g.interior]
-    ref, _ = dynamic_numpy(g, *(sims[1].get_field(n) for n in ("u", "v", "w")), CS_MAX)
+    ref, _ = dynamic_numpy(g, *(sims[1].get_field(n) for n in ("u", "v", "w")), CS_MAX, local=averaging == "local")
     assert np.abs(nut - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
 @pytest.mark.gpu
-def test_gpu_dynamic_adaptive_dt_matches_the_oracle():
+@pytest.mark.parametrize("averaging", ["plane", "local"])
+def test_gpu_dynamic_adaptive_dt_matches_the_oracle(averaging):
     from aeolus_b200._lib import LIMITERS
     from aeolus_b200.simulation import CFLConstraints, Simulation
     g = grid()
-    sp = spec(g, c_s=30.0)
+    sp = spec(g, c_s=30.0, averaging=averaging)
     s, o = Simulation(sp), OracleSimulation(sp)
     for x in (s, o):
         x.set_state(*state(g, amp=0.05))
