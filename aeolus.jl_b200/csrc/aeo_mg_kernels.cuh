@@ -114,8 +114,10 @@ enum { CF_CONST = 0, CF_CODES = 1, CF_VALUES = 2 };
 
 template <typename R, int CF>
 __device__ __forceinline__ R face_coef(const R* vals, const unsigned char* codes, const R* stab, int f) {
-    if (CF == CF_CODES) return stab[codes[f]];
-    return vals[f];
+    // read-only for every kernel that takes them: the non-coherent path, which
+    // the compiler may also schedule ahead of the kernel's own stores
+    if (CF == CF_CODES) return stab[__ldg(codes + f)];
+    return __ldg(vals + f);
 }
 
 // The six neighbours of cell q = (i, j, k): the interior steps, or at a
@@ -537,7 +539,21 @@ __global__ void __launch_bounds__(RB_X * RB_Y) mg_rbgs_kernel(Level<R> L, Bc bc,
     const int dym = j > 0 ? -nx : (bc.y == 0 ? (ny - 1) * nx : 0);
     const int dyp = j < ny - 1 ? nx : (bc.y == 0 ? -(ny - 1) * nx : 0);
     const R* __restrict__ f = L.phi;
-    auto pair_at = [&](int k) { return *reinterpret_cast<const V2*>(f + (size_t)k * pl + row0); };
+    // the coefficient codes / values and b through restrict pointers: no store
+    // of this kernel (phi's colour) touches them, so the loads of the levels
+    // ahead need not wait for the stores of the levels before (the byte codes
+    // could alias phi as far as the compiler knows)
+    const unsigned char* __restrict__ ckx = L.c.kx;
+    const unsigned char* __restrict__ cky = L.c.ky;
+    const unsigned char* __restrict__ ckz = L.c.kz;
+    const R* __restrict__ ccx = L.c.cx;
+    const R* __restrict__ ccy = L.c.cy;
+    const R* __restrict__ ccz = L.c.cz;
+    const R* __restrict__ bb = L.b;
+    // phi through the non-coherent path as well: a colour pass reads only the
+    // other colour's cells and the cells this thread itself writes (before it
+    // writes them), so no value read here changes during the pass
+    auto pair_at = [&](int k) { return __ldg(reinterpret_cast<const V2*>(f + (size_t)k * pl + row0)); };
     V2 pc = pair_at(k0);
     V2 pm = k0 > 0 ? pair_at(k0 - 1) : (bc.z == 0 ? pair_at(nz - 1) : pc);
 #pragma unroll
@@ -548,23 +564,23 @@ __global__ void __launch_bounds__(RB_X * RB_Y) mg_rbgs_kernel(Level<R> L, Bc bc,
         const int a = (j + k + colour) & 1;   // the pair's cell of this colour
         const int q = k * pl + row0 + a;
         const R c = a ? pc.y : pc.x;
-        const R nxm = a ? pc.x : (xl >= 0 ? f[k * pl + xl] : c);
-        const R nxp = a ? (xr >= 0 ? f[k * pl + xr] : c) : pc.y;
-        const R nym = dym ? f[q + dym] : c;
-        const R nyp = dyp ? f[q + dyp] : c;
+        const R nxm = a ? pc.x : (xl >= 0 ? __ldg(f + k * pl + xl) : c);
+        const R nxp = a ? (xr >= 0 ? __ldg(f + k * pl + xr) : c) : pc.y;
+        const R nym = dym ? __ldg(f + q + dym) : c;
+        const R nyp = dyp ? __ldg(f + q + dyp) : c;
         const R nzm = a ? pm.y : pm.x, nzp = a ? pp.y : pp.x;
         R fxp = R(0), fxm = R(0), fyp = R(0), fym = R(0), fzp = R(0), fzm = R(0);
         if (CF != CF_CONST) {
             const int fx = q + j + ny * k, fy = q + nx * k;   // (nx+1)(j + ny k) + i, nx(j + (ny+1) k) + i
-            fxm = face_coef<R, CF>(L.c.cx, L.c.kx, stab, fx);
-            fxp = face_coef<R, CF>(L.c.cx, L.c.kx, stab, fx + 1);
-            fym = face_coef<R, CF>(L.c.cy, L.c.ky, stab, fy);
-            fyp = face_coef<R, CF>(L.c.cy, L.c.ky, stab, fy + nx);
-            fzm = face_coef<R, CF>(L.c.cz, L.c.kz, stab, q);
-            fzp = face_coef<R, CF>(L.c.cz, L.c.kz, stab, q + pl);
+            fxm = face_coef<R, CF>(ccx, ckx, stab, fx);
+            fxp = face_coef<R, CF>(ccx, ckx, stab, fx + 1);
+            fym = face_coef<R, CF>(ccy, cky, stab, fy);
+            fyp = face_coef<R, CF>(ccy, cky, stab, fy + nx);
+            fzm = face_coef<R, CF>(ccz, ckz, stab, q);
+            fzp = face_coef<R, CF>(ccz, ckz, stab, q + pl);
         }
         R v;
-        if (gs_vals<R, CF>(nxp, nxm, nyp, nym, nzp, nzm, fxp, fxm, fyp, fym, fzp, fzm, L.b[q], L.ix2, L.iy2, L.iz2, &v))
+        if (gs_vals<R, CF>(nxp, nxm, nyp, nym, nzp, nzm, fxp, fxm, fyp, fym, fzp, fzm, __ldg(bb + q), L.ix2, L.iy2, L.iz2, &v))
             L.phi[q] = v;
         pm = pc;
         pc = pp;
