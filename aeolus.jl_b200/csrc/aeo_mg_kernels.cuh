@@ -15,6 +15,13 @@ constexpr int TPB = 256;
 constexpr int RED_BLOCKS = 1184;       // 8 x 148 SMs (2048 threads an SM): the fixed grid of every FP64 reduction
 constexpr int COARSE_THREADS = 1024;
 constexpr int COARSE_MAX_CELLS = 16384;
+// Programmatic dependent launch: a kernel launched with the programmatic
+// stream serialisation attribute may start while the kernel before it is
+// finishing; it waits here, before its first read of anything an earlier
+// kernel wrote, for that kernel's completion and memory (a no-op when the
+// launch had no such attribute).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 constexpr int RB_X = 32, RB_Y = 8;     // block of the 3-D stencil grids
 
 enum { MG_CONVERGED = 0, MG_MAXIT = 1, MG_BREAKDOWN = 2, MG_ZERO_RHS = 3 };
@@ -295,6 +302,7 @@ __global__ void __launch_bounds__(RB_X * RB_Y) pcg_apply_kernel(const double* __
                                                                Coef<C> cf, int nx, int ny, int nz, Bc bc, double ix2,
                                                                double iy2, double iz2, PcgState* S, double* part,
                                                                int standalone) {
+    pdl_wait();
     __shared__ double stab[CF == CF_CODES ? 256 : 1];
     if (!standalone && S->done) return;
     if (CF == CF_CODES) {
@@ -308,21 +316,23 @@ __global__ void __launch_bounds__(RB_X * RB_Y) pcg_apply_kernel(const double* __
         for (int i = threadIdx.x; i < nx; i += blockDim.x) {
             const int q = i + nx * row;
             const Nbr n = nbr_of(q, i, j, k, nx, ny, nz, pl, bc);
-            const double c = p[q];
+            // p and the coefficients are read-only here: the non-coherent path
+            const double c = __ldg(p + q);
+            const double pxp = __ldg(p + n.xp), pxm = __ldg(p + n.xm), pyp = __ldg(p + n.yp), pym = __ldg(p + n.ym);
+            const double pzp = __ldg(p + n.zp), pzm = __ldg(p + n.zm);
             double a;
             if (CF == CF_CONST) {
-                a = (p[n.xp] - 2.0 * c + p[n.xm]) * ix2 + (p[n.yp] - 2.0 * c + p[n.ym]) * iy2 +
-                    (p[n.zp] - 2.0 * c + p[n.zm]) * iz2;
+                a = (pxp - 2.0 * c + pxm) * ix2 + (pyp - 2.0 * c + pym) * iy2 + (pzp - 2.0 * c + pzm) * iz2;
             } else {
                 const int fx = q + j + ny * k, fy = q + nx * k;
-                const double fxm = CF == CF_CODES ? stab[cf.kx[fx]] : double(cf.cx[fx]);
-                const double fxp = CF == CF_CODES ? stab[cf.kx[fx + 1]] : double(cf.cx[fx + 1]);
-                const double fym = CF == CF_CODES ? stab[cf.ky[fy]] : double(cf.cy[fy]);
-                const double fyp = CF == CF_CODES ? stab[cf.ky[fy + nx]] : double(cf.cy[fy + nx]);
-                const double fzm = CF == CF_CODES ? stab[cf.kz[q]] : double(cf.cz[q]);
-                const double fzp = CF == CF_CODES ? stab[cf.kz[q + pl]] : double(cf.cz[q + pl]);
-                a = (fxp * (p[n.xp] - c) - fxm * (c - p[n.xm])) * ix2 + (fyp * (p[n.yp] - c) - fym * (c - p[n.ym])) * iy2 +
-                    (fzp * (p[n.zp] - c) - fzm * (c - p[n.zm])) * iz2;
+                const double fxm = CF == CF_CODES ? stab[__ldg(cf.kx + fx)] : double(__ldg(cf.cx + fx));
+                const double fxp = CF == CF_CODES ? stab[__ldg(cf.kx + fx + 1)] : double(__ldg(cf.cx + fx + 1));
+                const double fym = CF == CF_CODES ? stab[__ldg(cf.ky + fy)] : double(__ldg(cf.cy + fy));
+                const double fyp = CF == CF_CODES ? stab[__ldg(cf.ky + fy + nx)] : double(__ldg(cf.cy + fy + nx));
+                const double fzm = CF == CF_CODES ? stab[__ldg(cf.kz + q)] : double(__ldg(cf.cz + q));
+                const double fzp = CF == CF_CODES ? stab[__ldg(cf.kz + q + pl)] : double(__ldg(cf.cz + q + pl));
+                a = (fxp * (pxp - c) - fxm * (c - pxm)) * ix2 + (fyp * (pyp - c) - fym * (c - pym)) * iy2 +
+                    (fzp * (pzp - c) - fzm * (c - pzm)) * iz2;
             }
             Ap[q] = a;
             v[0] += c * a;
@@ -345,6 +355,7 @@ __global__ void __launch_bounds__(RB_X * RB_Y) pcg_apply_kernel(const double* __
 // x += alpha p, r -= alpha Ap; (r.r, sum r); the convergence test
 __global__ void pcg_update_kernel(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
                                   const double* __restrict__ Ap, int n, PcgState* S, double* part) {
+    pdl_wait();
     if (S->done) return;
     const double alpha = S->alpha;
     double v[2] = {0.0, 0.0};
@@ -372,6 +383,7 @@ __global__ void pcg_update_kernel(double* __restrict__ x, double* __restrict__ r
 template <typename Z>
 __global__ void pcg_rz_kernel(const double* __restrict__ r, const Z* __restrict__ z, const double* __restrict__ Ap,
                               int n, PcgState* S, double* part, int first) {
+    pdl_wait();
     if (S->done) return;
     const bool flex = S->flexible && !first;
     double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -417,6 +429,7 @@ __global__ void pcg_rz_kernel(const double* __restrict__ r, const Z* __restrict_
 // p = (z - m) + beta p  (p = z - m on the first pass)
 template <typename Z>
 __global__ void pcg_dir_kernel(double* __restrict__ p, const Z* __restrict__ z, int n, const PcgState* S, int first) {
+    pdl_wait();
     if (S->done) return;
     const double m = S->m, beta = S->beta;
     GRID_STRIDE(q, n) p[q] = first ? double(z[q]) - m : (double(z[q]) - m) + beta * p[q];
@@ -426,6 +439,7 @@ __global__ void pcg_dir_kernel(double* __restrict__ p, const Z* __restrict__ z, 
 // fully blocked cell)
 __global__ void pcg_jacobi_kernel(double* __restrict__ z, const double* __restrict__ r,
                                   const double* __restrict__ invd, int n, const PcgState* S) {
+    pdl_wait();
     if (S->done) return;
     GRID_STRIDE(q, n) z[q] = r[q] * invd[q];
 }
@@ -483,6 +497,7 @@ __global__ void shift_kernel(double* __restrict__ x, int n, const PcgState* S) {
 // One thread per pair of cells (2ih, 2ih+1).
 template <typename R>
 __global__ void mg_first_kernel(Level<R> L, Bc bc, const double* __restrict__ r0, const double* mr0, const int* done) {
+    pdl_wait();
     if (*done) return;
     const int ih = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
     if (ih >= (L.nx >> 1) || j >= L.ny) return;
@@ -521,6 +536,7 @@ template <> struct Vec2<double> { using T = double2; };
 
 template <typename R, int CF, int RB_K>
 __global__ void __launch_bounds__(RB_X * RB_Y) mg_rbgs_kernel(Level<R> L, Bc bc, int colour, const int* done) {
+    pdl_wait();
     __shared__ R stab[CF == CF_CODES ? 256 : 1];
     if (*done) return;
     if (CF == CF_CODES) {
@@ -591,6 +607,7 @@ __global__ void __launch_bounds__(RB_X * RB_Y) mg_rbgs_kernel(Level<R> L, Bc bc,
 // one thread per cell, a 3-D grid; the arithmetic of aphi.
 template <typename R, int CF>
 __global__ void __launch_bounds__(RB_X * RB_Y) mg_residual_kernel(Level<R> F, Bc bc, const int* done) {
+    pdl_wait();
     __shared__ R stab[CF == CF_CODES ? 256 : 1];
     if (*done) return;
     if (CF == CF_CODES) {
@@ -625,6 +642,7 @@ __global__ void __launch_bounds__(RB_X * RB_Y) mg_residual_kernel(Level<R> F, Bc
 // subtracts before use.
 template <typename R>
 __global__ void mg_restrict_kernel(Level<R> F, Level<R> Cl, double* part, unsigned* counter, const int* done) {
+    pdl_wait();
     if (*done) return;
     const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y, K = blockIdx.z;
     double v[1] = {0.0};
@@ -651,6 +669,7 @@ __global__ void mg_restrict_kernel(Level<R> F, Level<R> Cl, double* part, unsign
 // (src/Multigrid.jl:412-455), the eight terms in the reference's order.
 template <typename R>
 __global__ void mg_prolong_kernel(Level<R> F, Level<R> Cl, Bc bc, const int* done) {
+    pdl_wait();
     if (*done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
     if (i >= F.nx || j >= F.ny) return;
@@ -692,6 +711,7 @@ __global__ void __launch_bounds__(COARSE_THREADS) mg_coarsest_kernel(Level<R> L,
                                                                     int staged, int inplace,
                                                                     const double* __restrict__ r0, const double* mr0,
                                                                     const int* done, R* mat) {
+    pdl_wait();
     if (*done) return;
     const int unit = mat ? (int)blockIdx.x : -1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -800,6 +820,7 @@ __global__ void __launch_bounds__(COARSE_THREADS) mg_coarsest_kernel(Level<R> L,
 template <typename R>
 __global__ void mg_coarse_matvec_kernel(Level<R> L, const R* __restrict__ mat, const double* __restrict__ r0,
                                         const double* mr0, const int* done) {
+    pdl_wait();
     if (*done) return;
     const int n = L.n;
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
@@ -827,6 +848,7 @@ template <typename R, int MAXT>
 __global__ void __launch_bounds__(MAXT) mg_coarsest_col_kernel(Level<R> L, Bc bc, int sweeps,
                                                                         const double* __restrict__ r0,
                                                                         const double* mr0, const int* done) {
+    pdl_wait();
     if (*done) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nx = L.nx, ny = L.ny, nz = L.nz, n = L.n, ncol = nx * ny;

@@ -46,6 +46,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstdint>
 #include <cstring>
 #include <new>
@@ -57,6 +58,24 @@
 #include "../../include/aeolus_b200_mgpcg.h"
 #include "../../include/aeolus_b200_unet.h"
 #include "aeo_mg_kernels.cuh"
+
+// Launch with programmatic stream serialisation (the kernel may start while
+// the one before it drains, and waits in pdl_wait for its completion), unless
+// the handle turned it off.
+#define AEO_PDL_LAUNCH(KERN, GRID, BLOCK, SMEM, STREAM, ...)                                        \
+    do {                                                                                          \
+        cudaLaunchConfig_t lc_{};                                                                 \
+        lc_.gridDim = dim3(GRID);                                                                 \
+        lc_.blockDim = dim3(BLOCK);                                                               \
+        lc_.dynamicSmemBytes = (size_t)(SMEM);                                                    \
+        lc_.stream = (STREAM);                                                                    \
+        cudaLaunchAttribute la_[1];                                                               \
+        la_[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;                           \
+        la_[0].val.programmaticStreamSerializationAllowed = pdl_on ? 1 : 0;                       \
+        lc_.attrs = la_;                                                                          \
+        lc_.numAttrs = 1;                                                                         \
+        cudaLaunchKernelEx(&lc_, KERN, __VA_ARGS__);                                              \
+    } while (0)
 
 // the learned preconditioner's forward pass on a device residual (aeo_unet.cu)
 aeo_status aeo_unet_forward_on(aeo_unet* h, const double* r_dev, cudaStream_t s);
@@ -221,6 +240,7 @@ struct Mg : MgBase {
     R* coarse_spare = nullptr;     // the coarsest level's second buffer when not staged
     R* coarse_mat = nullptr;       // the coarsest solve as a dense n x n matrix (nullptr: run the sweeps)
     int coarse_col = 0;            // the register-column coarsest kernel applies
+    bool pdl_on = true;            // programmatic launches of the cycle and CG kernels
     int coarse_col_threads = 0;
     size_t coarse_col_smem = 0;
     cudaGraphExec_t g_solve = nullptr, g_cycles = nullptr;
@@ -473,16 +493,16 @@ struct Mg : MgBase {
         const dim3 blk(RB_X, RB_Y);
         const int nb = row_blocks(cfg.ny * cfg.nz);
         if (op_f32)
-            pcg_apply_kernel<float, CF_VALUES><<<nb, blk, 0, s>>>(in, out, opf, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2,
+            AEO_PDL_LAUNCH((pcg_apply_kernel<float, CF_VALUES>), nb, blk, 0, s, in, out, opf, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2,
                                                                   iz2, S, part, standalone);
         else if (opd.kx)
-            pcg_apply_kernel<double, CF_CODES><<<nb, blk, 0, s>>>(in, out, opd, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2,
+            AEO_PDL_LAUNCH((pcg_apply_kernel<double, CF_CODES>), nb, blk, 0, s, in, out, opd, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2,
                                                                   iz2, S, part, standalone);
         else if (opd.cx)
-            pcg_apply_kernel<double, CF_VALUES><<<nb, blk, 0, s>>>(in, out, opd, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2,
+            AEO_PDL_LAUNCH((pcg_apply_kernel<double, CF_VALUES>), nb, blk, 0, s, in, out, opd, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2,
                                                                    iz2, S, part, standalone);
         else
-            pcg_apply_kernel<double, CF_CONST><<<nb, blk, 0, s>>>(in, out, opd, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2,
+            AEO_PDL_LAUNCH((pcg_apply_kernel<double, CF_CONST>), nb, blk, 0, s, in, out, opd, cfg.nx, cfg.ny, cfg.nz, bc, ix2, iy2,
                                                                   iz2, S, part, standalone);
         CKL();
         return AEO_OK;
@@ -496,16 +516,16 @@ struct Mg : MgBase {
 
     aeo_status launch_coarsest(cudaStream_t s, Level<R>& C, const double* r0, const int* done) {
         if (coarse_mat) {
-            mg_coarse_matvec_kernel<R><<<(C.n + 7) / 8, 256, 0, s>>>(C, coarse_mat, r0, &S->mr, done);
+            AEO_PDL_LAUNCH((mg_coarse_matvec_kernel<R>), (C.n + 7) / 8, 256, 0, s, C, coarse_mat, r0, &S->mr, done);
             CKL();
             return AEO_OK;
         }
         if (coarse_col) {
             if (coarse_col_threads <= 256)
-                mg_coarsest_col_kernel<R, 256><<<1, coarse_col_threads, coarse_col_smem, s>>>(C, bc, cfg.coarse_sweeps,
+                AEO_PDL_LAUNCH((mg_coarsest_col_kernel<R, 256>), 1, coarse_col_threads, coarse_col_smem, s, C, bc, cfg.coarse_sweeps,
                                                                                              r0, &S->mr, done);
             else
-                mg_coarsest_col_kernel<R, COARSE_THREADS><<<1, coarse_col_threads, coarse_col_smem, s>>>(
+                AEO_PDL_LAUNCH((mg_coarsest_col_kernel<R, COARSE_THREADS>), 1, coarse_col_threads, coarse_col_smem, s, 
                     C, bc, cfg.coarse_sweeps, r0, &S->mr, done);
             CKL();
             return AEO_OK;
@@ -535,7 +555,7 @@ struct Mg : MgBase {
             const dim3 hg = half_grid(F);
             int sw0 = 0;
             if (l > 0 || from_zero) {
-                mg_first_kernel<R><<<hg, blk, 0, s>>>(F, bc, l == 0 ? r0 : nullptr, mr, done);
+                AEO_PDL_LAUNCH((mg_first_kernel<R>), hg, blk, 0, s, F, bc, l == 0 ? r0 : nullptr, mr, done);
                 CKL();
                 if (aeo_status q = launch_rbgs(s, F, 1, done)) return q;
                 sw0 = 1;
@@ -545,13 +565,13 @@ struct Mg : MgBase {
                     if (aeo_status q = launch_rbgs(s, F, c, done)) return q;
             Level<R>& Cl = L[l + 1];
             if (aeo_status q = launch_residual(s, F, done)) return q;
-            mg_restrict_kernel<R><<<restrict_grid(Cl), blk, 0, s>>>(F, Cl, part, &S->counter, done);
+            AEO_PDL_LAUNCH((mg_restrict_kernel<R>), restrict_grid(Cl), blk, 0, s, F, Cl, part, &S->counter, done);
             CKL();
         }
         if (aeo_status q = launch_coarsest(s, L[nl - 1], nullptr, done)) return q;
         for (int l = nl - 2; l >= 0; --l) {
             Level<R>& F = L[l];
-            mg_prolong_kernel<R><<<cell_grid(F), blk, 0, s>>>(F, L[l + 1], bc, done);
+            AEO_PDL_LAUNCH((mg_prolong_kernel<R>), cell_grid(F), blk, 0, s, F, L[l + 1], bc, done);
             CKL();
             for (int sw = 0; sw < cfg.nu2; ++sw)
                 for (int c = 0; c < 2; ++c)
@@ -567,22 +587,22 @@ struct Mg : MgBase {
         const bool col = (size_t)bx * by * ((F.nz + 7) / 8) >= 8 * 148;
         const dim3 hg(bx, by, (unsigned)(col ? (F.nz + 7) / 8 : F.nz)), blk(RB_X, RB_Y);
         if (col) {
-            if (F.c.kx) mg_rbgs_kernel<R, CF_CODES, 8><<<hg, blk, 0, s>>>(F, bc, colour, done);
-            else if (F.c.cx) mg_rbgs_kernel<R, CF_VALUES, 8><<<hg, blk, 0, s>>>(F, bc, colour, done);
-            else mg_rbgs_kernel<R, CF_CONST, 8><<<hg, blk, 0, s>>>(F, bc, colour, done);
+            if (F.c.kx) AEO_PDL_LAUNCH((mg_rbgs_kernel<R, CF_CODES, 8>), hg, blk, 0, s, F, bc, colour, done);
+            else if (F.c.cx) AEO_PDL_LAUNCH((mg_rbgs_kernel<R, CF_VALUES, 8>), hg, blk, 0, s, F, bc, colour, done);
+            else AEO_PDL_LAUNCH((mg_rbgs_kernel<R, CF_CONST, 8>), hg, blk, 0, s, F, bc, colour, done);
         } else {
-            if (F.c.kx) mg_rbgs_kernel<R, CF_CODES, 1><<<hg, blk, 0, s>>>(F, bc, colour, done);
-            else if (F.c.cx) mg_rbgs_kernel<R, CF_VALUES, 1><<<hg, blk, 0, s>>>(F, bc, colour, done);
-            else mg_rbgs_kernel<R, CF_CONST, 1><<<hg, blk, 0, s>>>(F, bc, colour, done);
+            if (F.c.kx) AEO_PDL_LAUNCH((mg_rbgs_kernel<R, CF_CODES, 1>), hg, blk, 0, s, F, bc, colour, done);
+            else if (F.c.cx) AEO_PDL_LAUNCH((mg_rbgs_kernel<R, CF_VALUES, 1>), hg, blk, 0, s, F, bc, colour, done);
+            else AEO_PDL_LAUNCH((mg_rbgs_kernel<R, CF_CONST, 1>), hg, blk, 0, s, F, bc, colour, done);
         }
         CKL();
         return AEO_OK;
     }
     aeo_status launch_residual(cudaStream_t s, const Level<R>& F, const int* done) {
         const dim3 g = cell_grid(F), blk(RB_X, RB_Y);
-        if (F.c.kx) mg_residual_kernel<R, CF_CODES><<<g, blk, 0, s>>>(F, bc, done);
-        else if (F.c.cx) mg_residual_kernel<R, CF_VALUES><<<g, blk, 0, s>>>(F, bc, done);
-        else mg_residual_kernel<R, CF_CONST><<<g, blk, 0, s>>>(F, bc, done);
+        if (F.c.kx) AEO_PDL_LAUNCH((mg_residual_kernel<R, CF_CODES>), g, blk, 0, s, F, bc, done);
+        else if (F.c.cx) AEO_PDL_LAUNCH((mg_residual_kernel<R, CF_VALUES>), g, blk, 0, s, F, bc, done);
+        else AEO_PDL_LAUNCH((mg_residual_kernel<R, CF_CONST>), g, blk, 0, s, F, bc, done);
         CKL();
         return AEO_OK;
     }
@@ -592,23 +612,23 @@ struct Mg : MgBase {
         if (pc < 0) pc = cfg.precond;
         if (pc == AEO_PC_LEARNED) {
             const float* zf = aeo_unet_output(net);
-            pcg_rz_kernel<float><<<RED_BLOCKS, TPB, 0, s>>>(r, zf, Ap, n, S, part, first);
+            AEO_PDL_LAUNCH((pcg_rz_kernel<float>), RED_BLOCKS, TPB, 0, s, r, zf, Ap, n, S, part, first);
             CKL();
-            pcg_dir_kernel<float><<<RED_BLOCKS, TPB, 0, s>>>(p, zf, n, S, first);
+            AEO_PDL_LAUNCH((pcg_dir_kernel<float>), RED_BLOCKS, TPB, 0, s, p, zf, n, S, first);
         } else if (pc == AEO_PC_VCYCLE) {
-            pcg_rz_kernel<R><<<RED_BLOCKS, TPB, 0, s>>>(r, L[0].phi, Ap, n, S, part, first);
+            AEO_PDL_LAUNCH((pcg_rz_kernel<R>), RED_BLOCKS, TPB, 0, s, r, L[0].phi, Ap, n, S, part, first);
             CKL();
-            pcg_dir_kernel<R><<<RED_BLOCKS, TPB, 0, s>>>(p, L[0].phi, n, S, first);
+            AEO_PDL_LAUNCH((pcg_dir_kernel<R>), RED_BLOCKS, TPB, 0, s, p, L[0].phi, n, S, first);
         } else if (pc == AEO_PC_JACOBI) {
-            pcg_jacobi_kernel<<<RED_BLOCKS, TPB, 0, s>>>(zj, r, invd, n, S);
+            AEO_PDL_LAUNCH((pcg_jacobi_kernel), RED_BLOCKS, TPB, 0, s, zj, r, invd, n, S);
             CKL();
-            pcg_rz_kernel<double><<<RED_BLOCKS, TPB, 0, s>>>(r, zj, Ap, n, S, part, first);
+            AEO_PDL_LAUNCH((pcg_rz_kernel<double>), RED_BLOCKS, TPB, 0, s, r, zj, Ap, n, S, part, first);
             CKL();
-            pcg_dir_kernel<double><<<RED_BLOCKS, TPB, 0, s>>>(p, zj, n, S, first);
+            AEO_PDL_LAUNCH((pcg_dir_kernel<double>), RED_BLOCKS, TPB, 0, s, p, zj, n, S, first);
         } else {
-            pcg_rz_kernel<double><<<RED_BLOCKS, TPB, 0, s>>>(r, r, Ap, n, S, part, first);
+            AEO_PDL_LAUNCH((pcg_rz_kernel<double>), RED_BLOCKS, TPB, 0, s, r, r, Ap, n, S, part, first);
             CKL();
-            pcg_dir_kernel<double><<<RED_BLOCKS, TPB, 0, s>>>(p, r, n, S, first);
+            AEO_PDL_LAUNCH((pcg_dir_kernel<double>), RED_BLOCKS, TPB, 0, s, p, r, n, S, first);
         }
         CKL();
         return AEO_OK;
@@ -767,7 +787,7 @@ struct Mg : MgBase {
                 [&](cudaStream_t sb) -> aeo_status {
                     int c0 = 0;
                     if (aeo_status q2 = launch_apply(sb, p, Ap, 0)) return q2;
-                    pcg_update_kernel<<<RED_BLOCKS, TPB, 0, sb>>>(x, r, p, Ap, n, S, part);
+                    AEO_PDL_LAUNCH((pcg_update_kernel), RED_BLOCKS, TPB, 0, sb, x, r, p, Ap, n, S, part);
                     CKL();
                     c0 += 2;
                     if (harvest) {
@@ -1027,7 +1047,7 @@ struct Mg : MgBase {
             case 5: {
                 if (nl < 2) { fail("profile: one level, no restriction"); return AEO_ERR_ARGUMENT; }
                 if (aeo_status q = launch_residual(st, L[0], dzero)) return q;
-                mg_restrict_kernel<R><<<restrict_grid(L[1]), dim3(RB_X, RB_Y), 0, st>>>(L[0], L[1], part, &S->counter,
+                AEO_PDL_LAUNCH((mg_restrict_kernel<R>), restrict_grid(L[1]), dim3(RB_X, RB_Y), 0, st, L[0], L[1], part, &S->counter,
                                                                                       dzero);
                 CKL();
                 return AEO_OK;
