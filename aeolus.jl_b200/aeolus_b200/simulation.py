@@ -22,7 +22,7 @@ import numpy as np
 from . import _lib
 from .grids import PERIODIC, WALL, Grid
 from .reference_state import anelastic_profiles
-from .spec import ADVECTION, CORES, FIELDS, PRECISIONS, SGS_MODELS, SOLVERS, CoreSpec, sgs_model_code
+from .spec import ADVECTION, CORES, FIELDS, PRECISIONS, SGS_MODELS, SOLVERS, CoreSpec, sgs_buoyancy_levels, sgs_model_code
 
 _D = C.POINTER(C.c_double)
 
@@ -89,6 +89,10 @@ class Simulation:
         _lib.check(st, None)
         self._h = h
         self._lib = lib
+        bg = sgs_buoyancy_levels(spec)
+        if bg is not None:
+            bg = np.ascontiguousarray(bg, dtype=np.float64)
+            _lib.check(lib.aeo_set_sgs_buoyancy(h, _ptr(bg)), h)
 
     # ---- lifecycle ------------------------------------------------------------
     def close(self):

@@ -48,6 +48,8 @@ class CoreSpec:
     wc: Optional[np.ndarray] = field(default=None, repr=False)
     wf: Optional[np.ndarray] = field(default=None, repr=False)
     thf: Optional[np.ndarray] = field(default=None, repr=False)
+    thc: Optional[np.ndarray] = field(default=None, repr=False)   # theta_bar at the Nz cell centres (the
+                                        # AMD closure's buoyancy g/theta_bar(z) on the sound-proof core)
 
     def __post_init__(self):
         if self.core not in CORES:
@@ -95,8 +97,13 @@ class CoreSpec:
                              "compute_sigma_nut!, src/operators/sigma_closure.jl:208-212)")
         if self.sgs == "dynamic" and self.c_s != 0 and min(self.grid.halo) < 2:
             raise ValueError("the dynamic Smagorinsky closure needs halos of at least 2 (src/Operators.jl:556-557)")
-        if self.sgs == "amd" and self.c_s != 0 and self.core != "boussinesq":
-            raise ValueError("the AMD closure is built for the Boussinesq core")
+        if self.sgs == "amd" and self.c_s != 0 and self.core == "anelastic":
+            if self.thc is None:
+                raise ValueError("the AMD closure on the sound-proof core needs thc, theta_bar at the cell centres "
+                                 "(its buoyancy parameter g/theta_bar(z_k), src/operators/sgs_amd_vreman.jl:331-345)")
+            self.thc = np.ascontiguousarray(self.thc, dtype=np.float64)
+            if self.thc.shape != (self.grid.nz,) or np.any(self.thc <= 0):
+                raise ValueError(f"thc needs {self.grid.nz} positive values")
 
 
 def sgs_model_code(spec) -> int:
@@ -105,3 +112,11 @@ def sgs_model_code(spec) -> int:
     if spec.sgs == "dynamic" and spec.averaging == "local":
         return 5
     return SGS_MODELS[spec.sgs]
+
+
+def sgs_buoyancy_levels(spec):
+    """The AMD closure's per-level buoyancy parameter g/theta_bar(z_k) of a
+    sound-proof spec (None where the closure takes g/theta0 or is off)."""
+    if spec.sgs == "amd" and spec.c_s != 0 and spec.core == "anelastic":
+        return spec.g / spec.thc
+    return None

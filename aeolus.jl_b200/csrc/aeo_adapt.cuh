@@ -34,7 +34,7 @@ struct CflParams {
 template <typename R, bool UNI, bool SGS>
 __global__ void __launch_bounds__(256) cfl_levels_kernel(Geo g, const R* __restrict__ u, const R* __restrict__ v,
                                                          const R* __restrict__ w, const R* __restrict__ th, R c_s,
-                                                         R bg, R pr_t, const double* __restrict__ cs2, double dd2,
+                                                         R pr_t, const double* __restrict__ cs2, double dd2,
                                                          double* __restrict__ part, const R* __restrict__ cs2f = nullptr) {
     __shared__ double rmax[256], nmax[256], tsum[256], kmax[256];
     const int k = blockIdx.x;
@@ -57,7 +57,8 @@ __global__ void __launch_bounds__(256) cfl_levels_kernel(Geo g, const R* __restr
                                        strain_at<R, UNI>(Met<R, UNI>(g), g, k, U, V, W, (R*)nullptr)));
             } else if (g.sgs_model == 3) {
                 Nb<R> T{th + q, g.sy, g.sz};
-                const NuKappa<R> nk = amd_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, bg, pr_t, U, V, W, T);
+                const Met<R, UNI> m(g);
+                const NuKappa<R> nk = amd_point<R, UNI>(m, g, k, c_s, m.lv(LV_BGC, k), pr_t, U, V, W, T);
                 nm = fmax(nm, (double)nk.nu);
                 km = fmax(km, (double)nk.ka);
             } else {

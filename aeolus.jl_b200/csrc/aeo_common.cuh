@@ -155,7 +155,9 @@ __device__ __forceinline__ R ld_mapped_interior(const Geo& g, const R* __restric
 // conversion and, for the reciprocals, a division per point.
 enum {
     LV_IDZC = 0, LV_IDZF, LV_IDZOFF, LV_WLO, LV_WHI, LV_ALO, LV_AHI, LV_DELTA,
-    LV_WC, LV_WF, LV_IWC, LV_IWF, LV_THF, LV_GTHF, LV_SPC, LV_SPF, LV_N
+    LV_WC, LV_WF, LV_IWC, LV_IWF, LV_THF, LV_GTHF, LV_SPC, LV_SPF,
+    LV_BGC,   // the AMD closure's buoyancy parameter of the level: g/theta0, or g/theta_bar(z_k) (sound-proof core)
+    LV_N
 };
 
 template <typename R, bool UNI>

@@ -41,7 +41,6 @@ struct SweepArgs {
     R nu, gacc, theta0, fcor, inv_prt, pr_t, flux_bot, flux_top, sp_alpha, sp_zstart, sp_inv;
     R bref;         // theta0 in stored units (theta is held as theta - offset)
     R c_s;
-    R sgs_bg;       // g / theta0 of the AMD closure's buoyancy term (0: none)
     const double* cs2;  // the dynamic Smagorinsky coefficient per level
     const R* cs2f;      // ... or per cell (averaging = :local; padded, halos filled; else nullptr)
     double dyn_d2;      // ... and its Delta^2 = (dx dy dz)^(2/3)
@@ -398,15 +397,17 @@ __device__ __forceinline__ void sweep_point(const Met<R, UNI>& m, const SweepArg
             VT fzT = nT * (T(0, 0, 1) - T(0, 0, 0)) * m.idzf(k + 1), fzB = nB * (T(0, 0, 0) - T(0, 0, -1)) * m.idzf(k);
             tt += a.inv_prt * ((fxE - fxW) * idx + (fyN - fyS) * idy + (fzT - fzB) * m.idz(k));
         } else {
-            // kappa = nut / Pr_t, the W-weighted form (1/Pr_t applied once per face)
+            // kappa = nut / Pr_t, the W-weighted form (1/Pr_t applied once per face), or
+            // the AMD closure's own kappa_t (inv_prt = 1)
+            const AN K = AMD ? N.shifted(a.kofs) : N;
             const VT hk = h * a.inv_prt;
-            const VT N0 = N(0, 0, 0);
-            VT fxE = hk * (N0 + N(1, 0, 0)) * (T(1, 0, 0) - T(0, 0, 0)) * idx;
-            VT fxW = hk * (N(-1, 0, 0) + N0) * (T(0, 0, 0) - T(-1, 0, 0)) * idx;
-            VT fyN = hk * (N0 + N(0, 1, 0)) * (T(0, 1, 0) - T(0, 0, 0)) * idy;
-            VT fyS = hk * (N(0, -1, 0) + N0) * (T(0, 0, 0) - T(0, -1, 0)) * idy;
-            VT fzT = hk * (N0 + N(0, 0, 1)) * (T(0, 0, 1) - T(0, 0, 0)) * m.idzf(k + 1);
-            VT fzB = hk * (N(0, 0, -1) + N0) * (T(0, 0, 0) - T(0, 0, -1)) * m.idzf(k);
+            const VT N0 = K(0, 0, 0);
+            VT fxE = hk * (N0 + K(1, 0, 0)) * (T(1, 0, 0) - T(0, 0, 0)) * idx;
+            VT fxW = hk * (K(-1, 0, 0) + N0) * (T(0, 0, 0) - T(-1, 0, 0)) * idx;
+            VT fyN = hk * (N0 + K(0, 1, 0)) * (T(0, 1, 0) - T(0, 0, 0)) * idy;
+            VT fyS = hk * (K(0, -1, 0) + N0) * (T(0, 0, 0) - T(0, -1, 0)) * idy;
+            VT fzT = hk * (N0 + K(0, 0, 1)) * (T(0, 0, 1) - T(0, 0, 0)) * m.idzf(k + 1);
+            VT fzB = hk * (K(0, 0, -1) + N0) * (T(0, 0, 0) - T(0, 0, -1)) * m.idzf(k);
             VT vert = (m.wf(k + 1) * fzT - m.wf(k) * fzB) * m.idz(k) * m.iwc(k);
             tt += (fxE - fxW) * idx + (fyN - fyS) * idy + vert;
         }
@@ -694,7 +695,7 @@ __device__ __forceinline__ auto strain_at(const Met<R, UNI>& m, const Geo& g, in
 template <typename R, bool UNI>
 __global__ void __launch_bounds__(256) smagorinsky_kernel(Geo g, const R* __restrict__ u, const R* __restrict__ v,
                                                           const R* __restrict__ w, const R* __restrict__ th,
-                                                          R* __restrict__ nut, R c_s, R bg, R pr_t,
+                                                          R* __restrict__ nut, R c_s, R pr_t,
                                                           const double* __restrict__ cs2, double dd2,
                                                           const R* __restrict__ cs2f = nullptr) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -707,7 +708,8 @@ __global__ void __launch_bounds__(256) smagorinsky_kernel(Geo g, const R* __rest
         nut[q] = R(dyn_cs2_cell(g, cs2, cs2f, i, j, k) * dd2) * strain_at<R, UNI>(Met<R, UNI>(g), g, k, U, V, W, (R*)nullptr);
     } else if (g.sgs_model == 3) {
         Nb<R> T{th + q, g.sy, g.sz};
-        nut[q] = amd_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, bg, pr_t, U, V, W, T).nu;
+        const Met<R, UNI> m(g);
+        nut[q] = amd_point<R, UNI>(m, g, k, c_s, m.lv(LV_BGC, k), pr_t, U, V, W, T).nu;
     } else {
         nut[q] = smag_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, U, V, W);
     }

@@ -134,7 +134,7 @@ __device__ __forceinline__ void pair_nut_plane(const Met<float, UNI>& m, const S
             *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nv.v;
         } else if constexpr (CLOS == 1) {
             const PairAcc<1, S::PW, 3 * S::PSZA> Tq{q};
-            const NuKappa<F2> nk = amd_point<R, UNI>(m, g, L, R(a.c_s), a.sgs_bg, a.pr_t, Uq, Vq, Wq, Tq);
+            const NuKappa<F2> nk = amd_point<R, UNI>(m, g, L, R(a.c_s), m.lv(LV_BGC, L), a.pr_t, Uq, Vq, Wq, Tq);
             *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nk.nu.v;
             *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc + S::KT_OFS) = nk.ka.v;
         } else {

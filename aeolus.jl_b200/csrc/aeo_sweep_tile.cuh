@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
                         np[cj * S::NPW + ci] = c * strain_at<R, UNI>(m, g, L, Uq, Vq, Wq, (R*)nullptr);
                     } else if constexpr (CLOS == 1) {
                         const SmAcc<R, 1, S::PW, 3 * S::PSZA> Tq{q};
-                        const NuKappa<R> nk = amd_point<R, UNI>(m, g, L, R(a.c_s), a.sgs_bg, a.pr_t, Uq, Vq, Wq, Tq);
+                        const NuKappa<R> nk = amd_point<R, UNI>(m, g, L, R(a.c_s), m.lv(LV_BGC, L), a.pr_t, Uq, Vq, Wq, Tq);
                         np[cj * S::NPW + ci] = nk.nu;
                         np[cj * S::NPW + ci + S::KT_OFS] = nk.ka;
                     } else {

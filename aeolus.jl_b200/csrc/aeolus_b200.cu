@@ -118,6 +118,7 @@ struct CoreBase {
     virtual aeo_status pcg_stats(aeo_mg_stats* o) = 0;
     virtual aeo_status pcg_set_learned(aeo_unet* net, double stagnation) = 0;
     virtual aeo_status set_ibm(const uint8_t* mask, double tau) = 0;
+    virtual aeo_status set_sgs_buoyancy(const double* bg) = 0;
 };
 
 struct aeo_sim {
@@ -214,6 +215,29 @@ struct Core : CoreBase {
     int dyn_launches() const { return dyn() ? 3 : 0; }
     // g / theta0 of the AMD closure's buoyancy term (0 without buoyancy)
     R amd_bg() const { return R(amd() && cfg.theta0 != 0.0 ? cfg.g / cfg.theta0 : 0.0); }
+    // the AMD closure on the sound-proof core takes its per-level buoyancy
+    // parameter g/theta_bar(z_k) from aeo_set_sgs_buoyancy before the first step
+    bool bg_levels_set = false;
+    aeo_status sgs_ready() {
+        if (amd() && anel && !bg_levels_set) {
+            fail("the AMD closure on the sound-proof core needs its per-level buoyancy parameter g/theta_bar "
+                 "(aeo_set_sgs_buoyancy) before a step");
+            return AEO_ERR_STATE;
+        }
+        return AEO_OK;
+    }
+    aeo_status set_sgs_buoyancy(const double* bgv) override {
+        if (!bgv) { fail("set_sgs_buoyancy: NULL levels"); return AEO_ERR_ARGUMENT; }
+        for (int k = 0; k < g.nz; ++k)
+            if (!std::isfinite(bgv[k])) { fail("set_sgs_buoyancy: non-finite level value"); return AEO_ERR_ARGUMENT; }
+        // the row of the working-precision table, halo entries from the nearest level
+        std::vector<R> row((size_t)g.lvn);
+        for (int e = 0; e < g.lvn; ++e) row[e] = R(bgv[std::min(std::max(e - AEO_LH, 0), g.nz - 1)]);
+        CK(cudaStreamSynchronize(st));
+        CK(cudaMemcpy(levels_r + (size_t)LV_BGC * g.lvn, row.data(), row.size() * sizeof(R), cudaMemcpyHostToDevice));
+        bg_levels_set = true;
+        return AEO_OK;
+    }
     // per-kernel-class timing of one un-graphed step (aeo_profile_step)
     bool profiling = false;
     std::vector<std::pair<int, cudaEvent_t>> marks;
@@ -379,6 +403,7 @@ struct Core : CoreBase {
                 put_r(LV_GTHF, thr != R(0) ? R(c.g) / thr : R(0));
                 put_r(LV_SPC, rate(row(8, e)));
                 put_r(LV_SPF, rate(row(9, e)));
+                put_r(LV_BGC, amd_bg());   // the sound-proof core's levels come from aeo_set_sgs_buoyancy
             }
             if (aeo_status s = alloc(&levels_r, hr.size())) return s;
             CK(cudaMemcpyAsync(levels_r, hr.data(), hr.size() * sizeof(R), cudaMemcpyHostToDevice, st));
@@ -722,7 +747,7 @@ struct Core : CoreBase {
                 const int ntx = (g.nx + PS::TX - 1) / PS::TX, nty = (g.ny + PS::TY - 1) / PS::TY;
                 const int items = ntx * nty * g.nz;
                 const dim3 grid((unsigned)std::min(items, PS::CTAS_PER_SM * nsm));
-                if constexpr (SG && !AN && UN) {
+                if constexpr (SG && UN) {
                     if (amd()) {
                         SweepArgs<R> b = a;
                         b.kofs = PS::KT_OFS;
@@ -759,7 +784,7 @@ struct Core : CoreBase {
         }
         using TS = TileShape<R, ADV, SG>;
         dim3 grid((g.nx + TS::TX - 1) / TS::TX, (g.ny + TS::TY - 1) / TS::TY, (g.nz + kchunk - 1) / kchunk);
-        if constexpr (SG && !AN && UN) {
+        if constexpr (SG && UN) {
             if (amd()) {
                 SweepArgs<R> b = a;
                 b.kofs = TS::KT_OFS;
@@ -933,7 +958,6 @@ struct Core : CoreBase {
         // the AMD closure brings its own kappa_t (the flux takes it unscaled)
         // and a buoyancy term with g / theta0
         a.inv_prt = amd() ? R(1) : R(1.0 / cfg.pr_t);
-        a.sgs_bg = amd_bg();
         a.cs2 = d_cs2;
         a.cs2f = d_cs2f;
         a.dyn_d2 = dyn_d2;
@@ -966,11 +990,11 @@ struct Core : CoreBase {
         if (dyn())
             if (aeo_status e = enqueue_dynamic(in)) return e;
         if (uni) {
-            if (sgs) cfl_levels_kernel<R, true, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_part, d_cs2f);
-            else cfl_levels_kernel<R, true, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_part, d_cs2f);
+            if (sgs) cfl_levels_kernel<R, true, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), R(cfg.pr_t), d_cs2, dyn_d2, d_part, d_cs2f);
+            else cfl_levels_kernel<R, true, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), R(cfg.pr_t), d_cs2, dyn_d2, d_part, d_cs2f);
         } else {
-            if (sgs) cfl_levels_kernel<R, false, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_part, d_cs2f);
-            else cfl_levels_kernel<R, false, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_part, d_cs2f);
+            if (sgs) cfl_levels_kernel<R, false, true><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), R(cfg.pr_t), d_cs2, dyn_d2, d_part, d_cs2f);
+            else cfl_levels_kernel<R, false, false><<<g.nz, 256, 0, st>>>(g, in[0], in[1], in[2], in[3], R(cfg.c_s), R(cfg.pr_t), d_cs2, dyn_d2, d_part, d_cs2f);
         }
         CKL();
         dt_pick_kernel<<<1, 32, 0, st>>>(g, cflp, d_part, d_sc);
@@ -1085,6 +1109,7 @@ struct Core : CoreBase {
     }
 
     aeo_status step_rk3(double dt, int n, bool sync) override {
+        if (aeo_status e = sgs_ready()) return e;
         set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt, dt);
         CKL();
         if (n >= 2) {
@@ -1113,6 +1138,7 @@ struct Core : CoreBase {
     }
 
     aeo_status step_euler(double dt, int n) override {
+        if (aeo_status e = sgs_ready()) return e;
         set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt, dt);
         CKL();
         for (int s = 0; s < n; ++s) {
@@ -1173,6 +1199,7 @@ struct Core : CoreBase {
     }
 
     aeo_status cfl(const aeo_cfl* c, double dt_prev, aeo_adaptive_stats* out) override {
+        if (aeo_status e = sgs_ready()) return e;
         set_cfl(c);
         set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt_prev, dt_prev > 0 ? dt_prev : 0.0);
         CKL();
@@ -1192,6 +1219,7 @@ struct Core : CoreBase {
     // device, the step, the guard; on a failed guard the state (set cur,
     // untouched) is kept and the step retried with half the dt.
     aeo_status step_adaptive(const aeo_cfl* c, int n, double* dt_prev_io, aeo_adaptive_stats* stats) override {
+        if (aeo_status e = sgs_ready()) return e;
         set_cfl(c);
         double dt_prev = (dt_prev_io && *dt_prev_io > 0) ? *dt_prev_io : 0.0;
         set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt_prev, dt_prev);
@@ -1250,6 +1278,7 @@ struct Core : CoreBase {
     }
 
     aeo_status profile_step(double dt, double* ms, int ncls) override {
+        if (aeo_status e = sgs_ready()) return e;
         set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt, dt);
         CKL();
         profiling = true;
@@ -1340,8 +1369,8 @@ struct Core : CoreBase {
             // the step keeps nut in shared memory: evaluate it for the current state
             if (dyn())
                 if (aeo_status e = enqueue_dynamic(P[cur])) return e;
-            if (uni) smagorinsky_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], P[cur][3], nut, R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_cs2f);
-            else smagorinsky_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], P[cur][3], nut, R(cfg.c_s), amd_bg(), R(cfg.pr_t), d_cs2, dyn_d2, d_cs2f);
+            if (uni) smagorinsky_kernel<R, true><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], P[cur][3], nut, R(cfg.c_s), R(cfg.pr_t), d_cs2, dyn_d2, d_cs2f);
+            else smagorinsky_kernel<R, false><<<grd3(), blk3(), 0, st>>>(g, P[cur][0], P[cur][1], P[cur][2], P[cur][3], nut, R(cfg.c_s), R(cfg.pr_t), d_cs2, dyn_d2, d_cs2f);
             CKL();
         }
         S* stage = reinterpret_cast<S*>(d_stage);
@@ -1627,10 +1656,6 @@ static aeo_status validate(const aeo_config* c, const double* zf, const double* 
         *m = "the dynamic Smagorinsky closure needs host halos of at least 2 (src/Operators.jl:556-557)";
         return AEO_ERR_ARGUMENT;
     }
-    if (c->sgs_model == AEO_SGS_AMD && c->c_s != 0.0 && c->core != AEO_CORE_BOUSSINESQ) {
-        *m = "the AMD closure is built for the Boussinesq core";
-        return AEO_ERR_ARGUMENT;
-    }
     return AEO_OK;
 }
 
@@ -1778,6 +1803,11 @@ aeo_status aeo_advect_positive_device(aeo_sim* h, const void* u, const void* v, 
 aeo_status aeo_set_ibm(aeo_sim* h, const uint8_t* mask, double tau) {
     ENTER(h);
     return h->core->set_ibm(mask, tau);
+}
+
+aeo_status aeo_set_sgs_buoyancy(aeo_sim* h, const double* bg) {
+    ENTER(h);
+    return h->core->set_sgs_buoyancy(bg);
 }
 
 aeo_status aeo_set_pcg(aeo_sim* h, const double* ax, const double* ay, const double* az, double tol, int32_t maxit) {

@@ -300,6 +300,15 @@ aeo_status aeo_pressure_solve_column_noalloc(int32_t nx, int32_t ny, int32_t nz,
                                              const double* inv_coupling, const double* gauge,
                                              const double* src, double* phi, void* stream);
 
+/* The AMD closure's buoyancy parameter of every interior level, Nz values:
+ * g / theta_bar(z_k) of the sound-proof core's reference state at the cell
+ * centres (sgs_buoyancy_parameter / _LevelBuoyancy,
+ * src/operators/sgs_amd_vreman.jl:331-345, which AMDClosure passes to
+ * compute_amd_coefficients!, :346-351).  Required before the first step of
+ * an anelastic domain with the AMD closure (AEO_ERR_STATE otherwise); the
+ * Boussinesq core uses g / theta0 and needs no call. */
+aeo_status aeo_set_sgs_buoyancy(aeo_sim* h, const double* bg);
+
 /* The pressure solve of a domain created with solver = AEO_SOLVER_PCG:
  * conjugate gradients preconditioned by one multigrid V(2,2) cycle
  * (MGPreconditionedCG, src/Multigrid.jl:893-967, the urban :mg_cg slot of

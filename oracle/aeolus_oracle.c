@@ -78,6 +78,7 @@ struct oc_sim {
      * LM and MM (interior), the per-level coefficient */
     double* dyn[10];
     double *dyn_lm, *dyn_mm, *cs2;
+    double* amd_bg;   /* g/theta_bar(z_k) of the sound-proof core's AMD closure (interior levels), or NULL */
 };
 
 #define ID(s, i, j, k) ((int64_t)(i) + (int64_t)(s)->NX * ((int64_t)(j) + (int64_t)(s)->NY * (int64_t)(k)))
@@ -671,7 +672,8 @@ static void amd_at(const oc_sim* s, int i, int j, int k, double* nu, double* ka)
                     (A(t, i, j + 1, k) - A(t, i, j - 1, k)) * (0.5 * idy),
                     (A(t, i, j, k + 1) - A(t, i, j, k - 1)) * (0.5 * idz)};
     double d2[3] = {s->dx * s->dx, s->dy * s->dy, s->dz * s->dz};
-    double bg = s->p.theta0 != 0 ? s->p.g / s->p.theta0 : 0.0;
+    double bg = s->p.core == OC_CORE_ANELASTIC ? (s->amd_bg ? s->amd_bg[k - s->p.hz] : 0.0)
+                                               : (s->p.theta0 != 0 ? s->p.g / s->p.theta0 : 0.0);
 #define SDOT(a, b) (d2[0] * (a)[0] * (b)[0] + d2[1] * (a)[1] * (b)[1] + d2[2] * (a)[2] * (b)[2])
     double S12 = 0.5 * (g[0][1] + g[1][0]), S13 = 0.5 * (g[0][2] + g[2][0]), S23 = 0.5 * (g[1][2] + g[2][1]);
     double P = SDOT(g[0], g[0]) * g[0][0] + SDOT(g[1], g[1]) * g[1][1] + SDOT(g[2], g[2]) * g[2][2] +
@@ -957,7 +959,7 @@ static void compute_tendencies(oc_sim* s) {
                 }
         fill_halos(s, s->nut, LOC_C);
         if (P->sgs_model == OC_SGS_AMD) fill_halos(s, s->kt, LOC_C);
-        if (anel)
+        if (anel && P->sgs_model != OC_SGS_AMD)   /* the AMD closure keeps its own kappa_t */
             for (int64_t q = 0; q < s->n; ++q) s->kt[q] = s->nut[q] / P->pr_t;
     }
 
@@ -1781,7 +1783,6 @@ oc_sim* oc_create(const oc_params* p, const double* zfi, const double* wc, const
     if ((p->sgs_model == OC_SGS_VREMAN || p->sgs_model == OC_SGS_SIGMA || p->sgs_model == OC_SGS_AMD ||
          p->sgs_model == OC_SGS_DYNAMIC || p->sgs_model == OC_SGS_DYNAMIC_LOCAL) && p->stretched)
         return NULL;
-    if (p->sgs_model == OC_SGS_AMD && p->c_s != 0 && p->core != OC_CORE_BOUSSINESQ) return NULL;
     oc_sim* s = (oc_sim*)calloc(1, sizeof(oc_sim));
     s->p = *p;
     s->NX = p->nx + 2 * p->hx; s->NY = p->ny + 2 * p->hy; s->NZ = p->nz + 2 * p->hz;
@@ -1906,6 +1907,13 @@ oc_sim* oc_create(const oc_params* p, const double* zfi, const double* wc, const
     return s;
 }
 
+int oc_set_sgs_buoyancy(oc_sim* s, const double* bg) {
+    if (!bg) return -1;
+    if (!s->amd_bg) s->amd_bg = dalloc(s->p.nz);
+    for (int k = 0; k < s->p.nz; ++k) s->amd_bg[k] = bg[k];
+    return 0;
+}
+
 int oc_set_apertures(oc_sim* s, const double* ax, const double* ay, const double* az, double tol, int maxit) {
     const oc_params* P = &s->p;
     if (P->solver != OC_SOLVER_PCG || !(tol > 0) || maxit < 1) return -1;
@@ -1986,7 +1994,7 @@ void oc_destroy(oc_sim* s) {
     free(s->hat); free(s->twx);
     free(s->apx); free(s->apy); free(s->apz); free(s->cgx); free(s->ibm);
     for (int f = 0; f < 10; ++f) free(s->dyn[f]);
-    free(s->dyn_lm); free(s->dyn_mm); free(s->cs2);
+    free(s->dyn_lm); free(s->dyn_mm); free(s->cs2); free(s->amd_bg);
     if (s->cg) ocg_destroy(s->cg);
     plan_free(&s->px); plan_free(&s->py); plan_free(&s->pz);
     free(s);

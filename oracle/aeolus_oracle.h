@@ -81,6 +81,9 @@ double oc_max_divergence(oc_sim* s);
  * aperture-weighted divergence and corrects u = u* - a d(phi) on every face
  * (zero on a blocked face).  0 on success. */
 int oc_set_apertures(oc_sim* s, const double* ax, const double* ay, const double* az, double tol, int maxit);
+/* the AMD closure's buoyancy parameter g/theta_bar(z_k) of the Nz interior
+ * levels (the sound-proof core; src/operators/sgs_amd_vreman.jl:331-345) */
+int oc_set_sgs_buoyancy(oc_sim* s, const double* bg);
 /* the implicit IBM correction after every predictor (implicit_ibm_correction!,
  * src/IBM.jl:295-300): mask storage-shaped, nonzero = solid (interior cells
  * count), NULL switches it off; tau >= 0 (0: the faces are zeroed); not with

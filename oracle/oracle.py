@@ -85,6 +85,7 @@ def load():
     lib.oc_set_ibm.argtypes = [P, C.c_void_p, C.c_double]
     lib.oc_advect_positive.argtypes = [P, _D, _D, _D, _D, _D, C.c_double, C.c_int, C.c_int]
     lib.oc_set_apertures.argtypes = [P, _D, _D, _D, C.c_double, C.c_int]
+    lib.oc_set_sgs_buoyancy.argtypes = [P, _D]
     lib.oc_pcg_stats.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double),
                                  C.POINTER(C.c_double)]
     lib.oc_philox4x32.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
@@ -155,6 +156,9 @@ class OracleSimulation:
         self._lib = lib
         self.spec = spec
         self.grid = g
+        if spec.sgs == "amd" and spec.c_s != 0 and spec.core == "anelastic":
+            self._bg = np.ascontiguousarray(spec.g / spec.thc, dtype=np.float64)
+            self._lib.oc_set_sgs_buoyancy(self._h, _p(self._bg))
 
     def close(self):
         if getattr(self, "_h", None):

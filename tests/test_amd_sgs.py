@@ -7,10 +7,11 @@ nu_t / Pr_t fallback where the theta gradient vanishes, the constant C = c_s.
 Oracle (CPU): nu_t and kappa_t equal a numpy statement of _amd_point on a
 random stratified field; nu_t is exactly zero in a pure shear flow u(z) (the
 closure's laminar-flow property) where Smagorinsky's is not; kappa_t is
-unchanged by theta -> a theta + b.  GPU (`-m gpu`): steps with the AMD
-closure match the oracle to 1e-11 (FP64; theta compared as its departure from
-theta0) and FP32-mixed to 1e-5; the adaptive dt with the eddy coefficients
-binding matches the oracle's pick to 1e-12.
+unchanged by theta -> a theta + b; on the sound-proof core the buoyancy
+parameter is g/theta_bar(z_k) of each level.  GPU (`-m gpu`): steps with the
+AMD closure match the oracle to 1e-11 (FP64; theta compared as its departure
+from theta0), on both cores, and FP32-mixed to 1e-5; the adaptive dt with the
+eddy coefficients binding matches the oracle's pick to 1e-12.
 """
 import numpy as np
 import pytest
@@ -129,7 +130,19 @@ def test_kappa_is_invariant_under_an_affine_theta():
     assert np.abs(k1 - k0).max() <= 1e-12 * np.abs(k0).max()
 
 
-def test_amd_needs_a_uniform_grid_and_the_boussinesq_core():
+def anelastic_spec(g, advection="centred", precision="fp64"):
+    """The sound-proof core on the uniform wall-bounded grid: an exponential
+    density and a stable theta_bar profile; the AMD buoyancy parameter is
+    g/theta_bar(z_k) of the cell centres (sgs_buoyancy_parameter,
+    src/operators/sgs_amd_vreman.jl:331-345)."""
+    from aeolus_b200.reference_state import anelastic_profiles, exponential_density
+    thc = 250.0 + 200.0 * g.znodes("c")
+    prof = anelastic_profiles(g, exponential_density(g), thc)
+    return CoreSpec(grid=g, core="anelastic", c_s=C_AMD, sgs="amd", advection=advection, precision=precision,
+                    wc=prof["wc"], wf=prof["wf"], thf=prof["thf"], thc=thc)
+
+
+def test_amd_needs_a_uniform_grid_and_centre_theta_on_the_sound_proof_core():
     from aeolus_b200 import stretched_grid, tanh_faces
     g = stretched_grid((16, 16, 16), (1.0, 1.0, 0.5), tanh_faces(16, 0.5, 1.5), halo=(3, 3, 3))
     with pytest.raises(ValueError):
@@ -137,6 +150,24 @@ def test_amd_needs_a_uniform_grid_and_the_boussinesq_core():
     n = 16
     with pytest.raises(ValueError):
         CoreSpec(grid=grid(), core="anelastic", c_s=C_AMD, sgs="amd", wc=np.ones(n + 6), wf=np.ones(n + 7))
+    assert anelastic_spec(grid()).thc.shape == (n,)
+
+
+def test_oracle_amd_on_the_sound_proof_core_uses_the_level_buoyancy():
+    """nu_t and kappa_t of the sound-proof core are the AMD point with the
+    buoyancy parameter of each level, g/theta_bar(z_k)."""
+    g = grid()
+    sp = anelastic_spec(g)
+    o = OracleSimulation(sp)
+    o.set_state(*state(g))
+    o.tendencies()
+    nut, kt = o.get_field("nut")[g.interior], o.get_field("kt")[g.interior]
+    f = [o.get_field(n) for n in FIELDS]
+    nu, ka = amd_numpy(g, *f, C_AMD, sp.pr_t, (sp.g / sp.thc)[:, None, None])
+    assert np.abs(nut - nu).max() <= 1e-12 * np.abs(nu).max()
+    assert np.abs(kt - ka).max() <= 1e-12 * np.abs(ka).max()
+    nu0, _ = amd_numpy(g, *f, C_AMD, sp.pr_t, sp.g / TH0)
+    assert np.abs(nu - nu0).max() > 1e-7 * np.abs(nu).max()   # the level values matter
 
 
 @pytest.mark.gpu
@@ -163,6 +194,39 @@ def test_gpu_amd_steps_match_the_oracle(advection):
     sp = spec(g)
     nut = sims[1].get_field("nut")[g.interior]
     nu, _ = amd_numpy(g, *(sims[1].get_field(n) for n in FIELDS), C_AMD, sp.pr_t, sp.g / TH0)
+    assert np.abs(nut - nu).max() <= 1e-12 * np.abs(nu).max()
+
+
+@pytest.mark.gpu
+def test_gpu_amd_on_the_sound_proof_core_matches_the_oracle():
+    """theta starts on the reference profile plus a stable 2 K/m and noise;
+    compared as its departure from theta_bar(z).  FP32 stores theta -
+    theta_bar(bottom face): a stored range of ~100 K against a ~1 K
+    departure, so theta's FP32 bar is 1e-4 (the velocities' 1e-5)."""
+    from aeolus_b200.simulation import Simulation
+    g = grid()
+    u, v, w, th = state(g)
+    sp = anelastic_spec(g)
+    thb = np.broadcast_to(sp.thc[:, None, None], (g.nz, g.ny, g.nx))
+    th = th.copy()
+    th[g.interior] += thb - TH0
+    sims = [OracleSimulation(sp), Simulation(anelastic_spec(g)), Simulation(anelastic_spec(g, precision="fp32_mixed"))]
+    out = []
+    for s in sims:
+        s.set_state(u, v, w, th)
+        s.project()   # the flux form's theta tendency depends on theta's storage offset unless div(W u) = 0
+        s.step_rk3(2e-3, 3)
+        f = {n: s.get_field(n)[g.interior] for n in FIELDS}
+        f["theta"] = f["theta"] - thb
+        out.append(f)
+    ora, g64, g32 = out
+    e64 = {n: np.linalg.norm(g64[n] - ora[n]) / np.linalg.norm(ora[n]) for n in FIELDS}
+    assert all(e <= 1e-11 for e in e64.values()), e64
+    e32 = {n: np.linalg.norm(g32[n] - g64[n]) / np.linalg.norm(g64[n]) for n in FIELDS}
+    assert all(e <= (1e-4 if n == "theta" else 1e-5) for n, e in e32.items()), e32
+    sp = anelastic_spec(g)
+    nut = sims[1].get_field("nut")[g.interior]
+    nu, _ = amd_numpy(g, *(sims[1].get_field(n) for n in FIELDS), C_AMD, sp.pr_t, (sp.g / sp.thc)[:, None, None])
     assert np.abs(nut - nu).max() <= 1e-12 * np.abs(nu).max()
 
 
