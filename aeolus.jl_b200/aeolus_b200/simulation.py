@@ -93,6 +93,9 @@ class Simulation:
         if bg is not None:
             bg = np.ascontiguousarray(bg, dtype=np.float64)
             _lib.check(lib.aeo_set_sgs_buoyancy(h, _ptr(bg)), h)
+        if spec.sgs == "lagrangian" and spec.c_s != 0:
+            mt = spec.lag_memory_time
+            _lib.check(lib.aeo_set_lagrangian(h, spec.lag_c0, spec.lag_theta, 0.0 if mt is None else mt), h)
 
     # ---- lifecycle ------------------------------------------------------------
     def close(self):
@@ -115,6 +118,25 @@ class Simulation:
     @property
     def handle(self):
         return self._h
+
+    # ---- the closure's memory (sgs_state / restore_sgs_state!) -----------------
+    def sgs_state(self):
+        """The Lagrangian closure's committed memory: (I_LM, I_MM, U, V, W) as
+        (nz, ny, nx) arrays and the initialised flag
+        (src/operators/lagrangian_sgs.jl:372-381)."""
+        g = self.grid
+        n = g.nx * g.ny * g.nz
+        out = np.empty(5 * n + 1)
+        _lib.check(self._lib.aeo_get_sgs_state(self._h, _ptr(out)), self._h)
+        return tuple(out[f * n:(f + 1) * n].reshape(g.nz, g.ny, g.nx).copy() for f in range(5)) + (bool(out[5 * n]),)
+
+    def set_sgs_state(self, state):
+        g = self.grid
+        arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in state[:5]]
+        if any(a.shape != (g.nz, g.ny, g.nx) for a in arrs):
+            raise ValueError(f"sgs state: five {(g.nz, g.ny, g.nx)} arrays and the initialised flag expected")
+        a = np.concatenate([x.ravel() for x in arrs] + [np.array([1.0 if state[5] else 0.0])])
+        _lib.check(self._lib.aeo_set_sgs_state(self._h, _ptr(a)), self._h)
 
     # ---- fields ---------------------------------------------------------------
     def set_field(self, name: str, data: np.ndarray):

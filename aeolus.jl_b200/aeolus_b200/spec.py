@@ -16,7 +16,7 @@ from .grids import PERIODIC, WALL, Grid
 
 CORES = {"boussinesq": 0, "anelastic": 1}
 ADVECTION = {"centred": 0, "weno_js5": 1, "weno_z5": 2}
-SGS_MODELS = {"smagorinsky": 0, "vreman": 1, "sigma": 2, "amd": 3, "dynamic": 4}
+SGS_MODELS = {"smagorinsky": 0, "vreman": 1, "sigma": 2, "amd": 3, "dynamic": 4, "lagrangian": 6}
 SOLVERS = {"fft": 0, "column": 1, "pcg": 2}
 PRECISIONS = {"fp64": 0, "fp32_mixed": 1}
 FIELDS = {"u": 0, "v": 1, "w": 2, "theta": 3, "p": 4, "nut": 5}
@@ -40,6 +40,11 @@ class CoreSpec:
                                         # (Germano-Lilly, plane-averaged; c_s is the clip cs_max, 0.5)
     averaging: str = "plane"            # the dynamic closure's <.>: "plane" (each level) or "local" (each
                                         # cell its own clipped ratio; DynamicSmagorinsky(averaging = :local))
+    # sgs = "lagrangian" (LagrangianDynamicSmagorinsky; c_s is the clip cs_max, 0.5): the initial
+    # coefficient C0, the time-scale factor theta and a fixed memory_time (None: MLC96's T)
+    lag_c0: float = 0.16
+    lag_theta: float = 1.5
+    lag_memory_time: Optional[float] = None
     pr_t: float = 1.0 / 3.0
     flux_bot: float = 0.0
     flux_top: float = 0.0
@@ -91,12 +96,19 @@ class CoreSpec:
             raise ValueError(f"sgs must be one of {list(SGS_MODELS)}, got {self.sgs!r}")
         if self.averaging not in ("plane", "local"):
             raise ValueError(f"averaging must be 'plane' or 'local', got {self.averaging!r} (src/Operators.jl:558-559)")
-        if self.sgs in ("vreman", "sigma", "amd", "dynamic") and self.grid.stretched:
+        if self.sgs in ("vreman", "sigma", "amd", "dynamic", "lagrangian") and self.grid.stretched:
             raise ValueError("the Vreman, sigma and AMD closures take a RegularGrid only (compute_vreman_nut!, "
                              "src/operators/sgs_amd_vreman.jl:280-284; compute_amd_coefficients!, :102-107; "
                              "compute_sigma_nut!, src/operators/sigma_closure.jl:208-212)")
-        if self.sgs == "dynamic" and self.c_s != 0 and min(self.grid.halo) < 2:
-            raise ValueError("the dynamic Smagorinsky closure needs halos of at least 2 (src/Operators.jl:556-557)")
+        if self.sgs in ("dynamic", "lagrangian") and self.c_s != 0 and min(self.grid.halo) < 2:
+            raise ValueError("the dynamic Smagorinsky closures need halos of at least 2 (src/Operators.jl:556-557, "
+                             "src/operators/lagrangian_sgs.jl:170-171)")
+        if self.sgs == "lagrangian":
+            if not (self.lag_c0 > 0 and self.lag_theta > 0):
+                raise ValueError("lag_c0 and lag_theta must be positive")
+            if self.lag_memory_time is not None and not self.lag_memory_time > 0:
+                raise ValueError(f"memory_time must be positive (or None for MLC96's T), got {self.lag_memory_time} "
+                                 "(src/operators/lagrangian_sgs.jl:172-173)")
         if self.sgs == "amd" and self.c_s != 0 and self.core == "anelastic":
             if self.thc is None:
                 raise ValueError("the AMD closure on the sound-proof core needs thc, theta_bar at the cell centres "

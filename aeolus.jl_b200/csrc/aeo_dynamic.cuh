@@ -12,7 +12,9 @@
 // chunk; the level pass adds the chunks and clips LM / MM. The sweep then
 // evaluates nu_t = cs2(k) Delta^2 |S| in its coefficient pass.  With the
 // :local averaging pass 2 writes each cell's clipped LM / MM instead (a
-// padded field with filled halos) and nu_t = cs2(i, j, k) Delta^2 |S|.
+// padded field with filled halos) and nu_t = cs2(i, j, k) Delta^2 |S|; the
+// Lagrangian closure runs passes 1 and 2 once per step, after it, to
+// commit its memories, whose clipped ratio is the next step's cs2(i, j, k).
 #pragma once
 
 #include "aeo_sweep.cuh"
@@ -49,15 +51,136 @@ __global__ void __launch_bounds__(256) germano_pass1_kernel(Geo g, const R* __re
     }
 }
 
+// The Lagrangian averaging (LagrangianDynamicSmagorinsky,
+// src/operators/lagrangian_sgs.jl): two sets of five interior arrays (x
+// fastest) -- I_LM, I_MM and the cell-centred velocity u^n the memory was
+// committed with -- one committed, the other written by the next commit.
+// state[0] is the committed set, state[1] is 1 once the memory is
+// initialised; both change only in lag_flip_kernel, after the commit.
+template <typename R>
+struct LagArgs {
+    R* mem[2][5];
+    int* state;
+    const double* dtp;     // the step's dt
+    double idx, idy, idz;  // 1 / dx, 1 / dy, 1 / dz
+    double theta_delta;    // theta (dx dy dz)^(1/3)
+    double memory_time;    // > 0: the fixed relaxation time, else MLC96's T
+    double c02;            // C0^2
+    double cs2max;
+};
+
+// _wrapidx (lagrangian_sgs.jl:392): the 1-based index n wrapped (periodic)
+// or clamped to [1, N], returned 0-based
+__device__ __forceinline__ int lag_wrap(int n, int N, bool per) {
+    if (per) { const int r = (n - 1) % N; return r < 0 ? r + N : r; }
+    return min(max(n, 1), N) - 1;
+}
+
+// One cell's commit (advance_sgs! :306-355 with _upstream_n :406-436 and
+// _relax_pairs! :545-568): the first commit sets I_MM = MM, I_LM = C0^2 MM;
+// later ones interpolate the committed memories trilinearly at the departure
+// point x - u^n dt (1-based fractional indices as the reference, clamped to
+// [1, N] across a wall) and relax toward this step's identity with epsilon =
+// (dt/T) / (1 + dt/T), T = theta Delta (max(lm, 1e-8 mm) mm)^(-1/8) (1 where
+// the upstream mm is 0; the fixed memory_time if given), I_LM clipped at 0.
+// u^n becomes this state's cell-centred velocity; cs2f (padded) gets the new
+// memory's clipped ratio (_local_cs2_body!).
+template <typename R>
+__device__ __forceinline__ void lag_commit_cell(const Geo& g, const DynWs<R>& ws, const LagArgs<R>& L, R* cs2f,
+                                                int i, int j, int k, double lmc, double mmc) {
+    const int cs = L.state[0];
+    R* const* old = L.mem[cs];
+    R* const* nw = L.mem[cs ^ 1];
+    const long long q = iidx(g, i, j, k);
+    double nlm, nmm;
+    if (!L.state[1]) {
+        nmm = mmc;
+        nlm = L.c02 * mmc;
+    } else {
+        const double dt = *L.dtp;
+        const double x = (double)(i + 1) - (double)old[2][q] * (dt * L.idx);
+        const double y = (double)(j + 1) - (double)old[3][q] * (dt * L.idy);
+        double z = (double)(k + 1) - (double)old[4][q] * (dt * L.idz);
+        const bool pz = g.bc_z == 0;
+        if (!pz) z = fmin(fmax(z, 1.0), (double)g.nz);
+        const double fx0 = floor(x), fy0 = floor(y), fz0 = floor(z);
+        const int x0 = (int)fx0, y0 = (int)fy0, z0 = (int)fz0;
+        const double fx = x - fx0, fy = y - fy0, fz = z - fz0;
+        double lm = 0.0, mm = 0.0;
+#pragma unroll
+        for (int dk = 0; dk <= 1; ++dk) {
+            const int c = lag_wrap(z0 + dk, g.nz, pz);
+#pragma unroll
+            for (int dj = 0; dj <= 1; ++dj) {
+                const int b = lag_wrap(y0 + dj, g.ny, true);
+#pragma unroll
+                for (int di = 0; di <= 1; ++di) {
+                    const int a = lag_wrap(x0 + di, g.nx, true);
+                    const double wgt = (di == 0 ? 1 - fx : fx) * (dj == 0 ? 1 - fy : fy) * (dk == 0 ? 1 - fz : fz);
+                    const long long r = iidx(g, a, b, c);
+                    lm += wgt * (double)old[0][r];
+                    mm += wgt * (double)old[1][r];
+                }
+            }
+        }
+        double eps;
+        if (L.memory_time > 0) {
+            eps = (dt / L.memory_time) / (1 + dt / L.memory_time);
+        } else if (mm > 0) {
+            const double Tl = L.theta_delta * pow(fmax(lm, 1e-8 * mm) * mm, -0.125);
+            eps = (dt / Tl) / (1 + dt / Tl);
+        } else {
+            eps = 1.0;
+        }
+        nlm = fmax(eps * lmc + (1 - eps) * lm, 0.0);
+        nmm = eps * mmc + (1 - eps) * mm;
+    }
+    const R slm = R(nlm), smm = R(nmm);
+    nw[0][q] = slm;
+    nw[1][q] = smm;
+    const long long sh = (long long)(i + 1) + (long long)ws.sx * ((j + 1) + (long long)ws.sy * (k + 1));
+    nw[2][q] = ws.f[DYN_UC][sh];
+    nw[3][q] = ws.f[DYN_VC][sh];
+    nw[4][q] = ws.f[DYN_WC][sh];
+    cs2f[pidx(g, i, j, k)] = R(smm > R(0) ? fmin(fmax((double)slm / (double)smm, 0.0), L.cs2max) : 0.0);
+}
+
+// After a commit: the written set becomes the committed one.
+__global__ void lag_flip_kernel(int* state) {
+    state[0] ^= 1;
+    state[1] = 1;
+}
+
+// The coefficient of the committed memory into the padded field cs2f (its
+// halos filled afterwards): min(C0^2, cs_max^2) before the first commit.
+template <typename R>
+__global__ void __launch_bounds__(256) lag_coefficient_kernel(Geo g, LagArgs<R> L, R* __restrict__ cs2f) {
+    const R* lm = L.mem[L.state[0]][0];
+    const R* mm = L.mem[L.state[0]][1];
+    const bool init = L.state[1] != 0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < g.nin;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(e % g.nx);
+        const long long r = e / g.nx;
+        const int j = (int)(r % g.ny), k = (int)(r / g.ny);
+        double c;
+        if (!init) c = fmin(L.c02, L.cs2max);
+        else c = mm[e] > R(0) ? fmin(fmax((double)lm[e] / (double)mm[e], 0.0), L.cs2max) : 0.0;
+        cs2f[pidx(g, i, j, k)] = R(c);
+    }
+}
+
 // Pass 2 (_germano_pass2_body! / _germano_LM_MM): blocks of 256 cells of one
 // level (grid.y = level); per block the sums of LM and MM into part.
-// LOCAL (averaging = :local, _local_cs2_body!): every interior cell's own
+// MODE 1 (averaging = :local, _local_cs2_body!): every interior cell's own
 // clipped ratio goes to the padded field cs2f (its halos filled afterwards
-// like a cell-centred field's) and no partials are written.
-template <typename R, bool LOCAL = false>
+// like a cell-centred field's) and no partials are written.  MODE 2 (the
+// Lagrangian commit): every cell's LM and MM enter its memory update
+// (lag_commit_cell), which writes cs2f.
+template <typename R, int MODE = 0>
 __global__ void __launch_bounds__(256) germano_pass2_kernel(Geo g, DynWs<R> ws, R inv27, R d2, R a2,
                                                             double* __restrict__ part, R* __restrict__ cs2f = nullptr,
-                                                            double cs2max = 0.0) {
+                                                            double cs2max = 0.0, LagArgs<R> lag = {}) {
     __shared__ double slm[256], smm[256];
     const int k = blockIdx.y;
     const int e = blockIdx.x * 256 + threadIdx.x;
@@ -96,9 +219,10 @@ __global__ void __launch_bounds__(256) germano_pass2_kernel(Geo g, DynWs<R> ws, 
         const R M12 = c2 * t[18] - c1 * A12, M13 = c2 * t[19] - c1 * A13, M23 = c2 * t[20] - c1 * A23;
         lmv = L11 * M11 + L22 * M22 + L33 * M33 + R(2) * (L12 * M12 + L13 * M13 + L23 * M23);
         mmv = M11 * M11 + M22 * M22 + M33 * M33 + R(2) * (M12 * M12 + M13 * M13 + M23 * M23);
-        if (LOCAL) cs2f[pidx(g, i, j, k)] = R(mmv > 0 ? fmin(fmax(lmv / mmv, 0.0), cs2max) : 0.0);
+        if (MODE == 1) cs2f[pidx(g, i, j, k)] = R(mmv > 0 ? fmin(fmax(lmv / mmv, 0.0), cs2max) : 0.0);
+        if (MODE == 2) lag_commit_cell<R>(g, ws, lag, cs2f, i, j, k, lmv, mmv);
     }
-    if (LOCAL) return;
+    if (MODE != 0) return;
     slm[threadIdx.x] = lmv;
     smm[threadIdx.x] = mmv;
     __syncthreads();

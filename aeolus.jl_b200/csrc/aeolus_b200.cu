@@ -119,6 +119,9 @@ struct CoreBase {
     virtual aeo_status pcg_set_learned(aeo_unet* net, double stagnation) = 0;
     virtual aeo_status set_ibm(const uint8_t* mask, double tau) = 0;
     virtual aeo_status set_sgs_buoyancy(const double* bg) = 0;
+    virtual aeo_status set_lagrangian(double c0, double theta, double memory_time) = 0;
+    virtual aeo_status get_sgs_state(double* out) = 0;
+    virtual aeo_status set_sgs_state(const double* in) = 0;
 };
 
 struct aeo_sim {
@@ -183,6 +186,9 @@ struct Core : CoreBase {
     bool amd() const { return sgs && cfg.sgs_model == AEO_SGS_AMD; }
     bool dyn() const { return sgs && (cfg.sgs_model == AEO_SGS_DYNAMIC || cfg.sgs_model == AEO_SGS_DYNAMIC_LOCAL); }
     bool dyn_local() const { return sgs && cfg.sgs_model == AEO_SGS_DYNAMIC_LOCAL; }
+    bool lag() const { return sgs && cfg.sgs_model == AEO_SGS_LAGRANGIAN; }
+    // the sweeps' dynamic coefficient (per level, or per cell in cs2f)
+    bool dyncl() const { return dyn() || lag(); }
     // the dynamic Smagorinsky workspace: the ten pass-1 fields, the per-block
     // partials of LM and MM, the per-level coefficient
     DynWs<R> dws{};
@@ -213,6 +219,85 @@ struct Core : CoreBase {
         return AEO_OK;
     }
     int dyn_launches() const { return dyn() ? 3 : 0; }
+    // the Lagrangian closure: its memories (two sets, LagArgs), the committed
+    // set and initialised flag on the device (and a copy of them taken before
+    // an adaptive step, put back when the step is retried), C0, theta, the
+    // fixed memory time (0: MLC96's T)
+    LagArgs<R> lagA{};
+    int* d_lag_state = nullptr;
+    double lag_c0 = 0.16, lag_theta = 1.5, lag_mt = 0.0;
+    int lag_launches() const { return lag() ? 4 : 0; }   // per step
+    // advance_sgs! of the state in `in` (halos filled): passes 1 and 2 with
+    // the memory update, the coefficient's halos, the flip
+    aeo_status enqueue_lag_commit(R* const* in) {
+        const long long ns = (long long)dws.sx * dws.sy * (g.nz + 2);
+        germano_pass1_kernel<R><<<(unsigned)std::min<long long>((ns + 255) / 256, 148LL * 16), 256, 0, st>>>(
+            g, in[0], in[1], in[2], dws);
+        CKL();
+        germano_pass2_kernel<R, 2><<<dim3((unsigned)dyn_nb, (unsigned)g.nz), 256, 0, st>>>(
+            g, dws, R(1.0 / 27), R(dyn_d2), R(9.0), d_dynpart, d_cs2f, cfg.c_s * cfg.c_s, lagA);
+        CKL();
+        R* f[1] = {d_cs2f};
+        int l[1] = {LOC_C};
+        if (aeo_status e = halo(f, l, 1)) return e;
+        lag_flip_kernel<<<1, 1, 0, st>>>(d_lag_state);
+        CKL();
+        return AEO_OK;
+    }
+    // the coefficient of the committed memory (set-up, new parameters, a restored state)
+    aeo_status lag_refresh() {
+        lagA.c02 = lag_c0 * lag_c0;
+        lagA.theta_delta = lag_theta * std::cbrt(g.dx * g.dy * g.dz);
+        lagA.memory_time = lag_mt;
+        lag_coefficient_kernel<R><<<(unsigned)std::min<long long>((g.nin + 255) / 256, 148LL * 16), 256, 0, st>>>(
+            g, lagA, d_cs2f);
+        CKL();
+        R* f[1] = {d_cs2f};
+        int l[1] = {LOC_C};
+        if (aeo_status e = halo(f, l, 1)) return e;
+        CK(cudaStreamSynchronize(st));
+        return AEO_OK;
+    }
+    aeo_status set_lagrangian(double c0, double theta, double memory_time) override {
+        if (!lag()) { fail("set_lagrangian: the domain's closure is not the Lagrangian dynamic one"); return AEO_ERR_STATE; }
+        if (!(c0 > 0) || !(theta > 0) || !std::isfinite(c0) || !std::isfinite(theta) || !(memory_time >= 0) ||
+            !std::isfinite(memory_time)) {
+            fail("set_lagrangian: c0 > 0, theta > 0 and memory_time >= 0 (0: MLC96's T) required");
+            return AEO_ERR_ARGUMENT;
+        }
+        CK(cudaStreamSynchronize(st));
+        drop_graphs();   // the parameters are captured by value
+        lag_c0 = c0; lag_theta = theta; lag_mt = memory_time;
+        return lag_refresh();
+    }
+    // sgs_state / restore_sgs_state! (src/operators/lagrangian_sgs.jl:372-381)
+    aeo_status sgs_state(double* out, bool get) {
+        if (!lag()) { fail("sgs_state: the domain's closure keeps no memory"); return AEO_ERR_STATE; }
+        if (!out) { fail("sgs_state: NULL array"); return AEO_ERR_ARGUMENT; }
+        CK(cudaStreamSynchronize(st));
+        int hs[2];
+        CK(cudaMemcpy(hs, d_lag_state, sizeof(hs), cudaMemcpyDeviceToHost));
+        std::vector<R> tmp((size_t)g.nin);
+        for (int f = 0; f < 5; ++f) {
+            double* o = out + (size_t)f * g.nin;
+            if (get) {
+                CK(cudaMemcpy(tmp.data(), lagA.mem[hs[0]][f], tmp.size() * sizeof(R), cudaMemcpyDeviceToHost));
+                for (size_t q = 0; q < tmp.size(); ++q) o[q] = (double)tmp[q];
+            } else {
+                for (size_t q = 0; q < tmp.size(); ++q) tmp[q] = R(o[q]);
+                CK(cudaMemcpy(lagA.mem[hs[0]][f], tmp.data(), tmp.size() * sizeof(R), cudaMemcpyHostToDevice));
+            }
+        }
+        if (get) {
+            out[5 * (size_t)g.nin] = hs[1] ? 1.0 : 0.0;
+            return AEO_OK;
+        }
+        hs[1] = out[5 * (size_t)g.nin] != 0.0;
+        CK(cudaMemcpy(d_lag_state, hs, sizeof(hs), cudaMemcpyHostToDevice));
+        return lag_refresh();
+    }
+    aeo_status get_sgs_state(double* out) override { return sgs_state(out, true); }
+    aeo_status set_sgs_state(const double* in) override { return sgs_state(const_cast<double*>(in), false); }
     // g / theta0 of the AMD closure's buoyancy term (0 without buoyancy)
     R amd_bg() const { return R(amd() && cfg.theta0 != 0.0 ? cfg.g / cfg.theta0 : 0.0); }
     // the AMD closure on the sound-proof core takes its per-level buoyancy
@@ -289,7 +374,8 @@ struct Core : CoreBase {
         uni = !c.stretched;
         sgs = c.c_s != 0.0;
         anel = c.core == AEO_CORE_ANELASTIC;
-        g.sgs_model = c.sgs_model == AEO_SGS_DYNAMIC_LOCAL ? AEO_SGS_DYNAMIC : c.sgs_model;   // devices: cs2f set
+        g.sgs_model = (c.sgs_model == AEO_SGS_DYNAMIC_LOCAL || c.sgs_model == AEO_SGS_LAGRANGIAN) ? AEO_SGS_DYNAMIC
+                                                                                                  : c.sgs_model;   // devices: cs2f set
         g.sgs_cv = 2.5 * c.c_s * c.c_s;
         if (sizeof(R) == sizeof(float)) th_off = anel ? (thf ? thf[c.hz] : 0.0) : c.theta0;
         g.nx = c.nx; g.ny = c.ny; g.nz = c.nz;
@@ -520,7 +606,7 @@ struct Core : CoreBase {
         host_n = (long long)(c.nx + 2 * c.hx) * (c.ny + 2 * c.hy) * (c.nz + 2 * c.hz);
         if (aeo_status e = alloc(&d_stage, std::max<long long>(host_n, g.nin))) return e;
         if (aeo_status e = alloc(&d_part, 4 * (size_t)(Nz + 1))) return e;
-        if (dyn()) {
+        if (dyncl()) {
             dws.sx = g.nx + 2;
             dws.sy = g.ny + 2;
             const size_t ns = (size_t)dws.sx * dws.sy * (g.nz + 2);
@@ -529,15 +615,28 @@ struct Core : CoreBase {
             dyn_nb = (g.nx * g.ny + 255) / 256;
             if (aeo_status e = alloc(&d_dynpart, 2 * (size_t)dyn_nb * g.nz)) return e;
             if (aeo_status e = alloc(&d_cs2, (size_t)g.nz)) return e;
-            if (dyn_local())
+            if (dyn_local() || lag())
                 if (aeo_status e = alloc(&d_cs2f, padded_count())) return e;
             dyn_d2 = std::pow(g.dx * g.dy * g.dz, 2.0 / 3.0);
+        }
+        if (lag()) {
+            for (int b = 0; b < 2; ++b)
+                for (int f = 0; f < 5; ++f)
+                    if (aeo_status e = alloc(&lagA.mem[b][f], (size_t)g.nin)) return e;
+            if (aeo_status e = alloc(&d_lag_state, 4)) return e;   // [0, 1] live, [2, 3] the copy
+            lagA.state = d_lag_state;
+            lagA.idx = 1.0 / g.dx; lagA.idy = 1.0 / g.dy; lagA.idz = 1.0 / g.dz;
+            lagA.cs2max = cfg.c_s * cfg.c_s;
         }
         if (aeo_status e = alloc(&d_flag, 1)) return e;
         if (aeo_status e = alloc(&d_steps, 1)) return e;
         if (aeo_status e = alloc(&d_sc, 1)) return e;
         set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->one, 1.0);
         CKL();
+        if (lag()) {
+            lagA.dtp = &d_sc->dt;
+            if (aeo_status e = lag_refresh()) return e;
+        }
         if (aeo_status e = make_tensor_maps()) return e;
         kchunk = std::min(g.nz, TileShape<R, 0, false>::KCH);
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cfg.device));
@@ -558,7 +657,7 @@ struct Core : CoreBase {
             }
         }
         CK(cudaStreamSynchronize(st));
-        launches = 3 * (9 + dyn_launches());
+        launches = 3 * (9 + dyn_launches()) + lag_launches();
         return AEO_OK;
     }
 
@@ -646,7 +745,7 @@ struct Core : CoreBase {
         if (!pcg) return launches;
         aeo_mg_stats o{};
         if (cudaStreamSynchronize(st) != cudaSuccess || aeo_mg_read_stats(mg, &o)) return 0;
-        return 3 * (4 + dyn_launches() + aeo_mg_launches_per_solve(mg, o.iterations));
+        return 3 * (4 + dyn_launches() + aeo_mg_launches_per_solve(mg, o.iterations)) + lag_launches();
     }
 
     // the implicit IBM correction after every predictor (aeo_set_ibm)
@@ -660,7 +759,7 @@ struct Core : CoreBase {
         drop_graphs();   // the step graphs gain or lose the correction
         if (!mask) {
             ibm_mask = nullptr;
-            launches = 3 * (9 + dyn_launches());
+            launches = 3 * (9 + dyn_launches()) + lag_launches();
             return AEO_OK;
         }
         std::vector<unsigned char> m((size_t)g.nin);
@@ -676,7 +775,7 @@ struct Core : CoreBase {
         CK(cudaStreamSynchronize(st));
         ibm_mask = ibm_alloc;
         ibm_tau = tau;
-        launches = 3 * (10 + dyn_launches());
+        launches = 3 * (10 + dyn_launches()) + lag_launches();
         return AEO_OK;
     }
 
@@ -759,7 +858,7 @@ struct Core : CoreBase {
                     }
                 }
                 if constexpr (SG && UN) {
-                    if (dyn()) {
+                    if (dyncl()) {
                         cudaFuncSetAttribute(sweep_pair_kernel<SG, AN, UN, 2>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PS::SMEM);
                         sweep_pair_kernel<SG, AN, UN, 2><<<grid, dim3(PS::TXT, PS::TY), PS::SMEM, st>>>(
@@ -796,7 +895,7 @@ struct Core : CoreBase {
             }
         }
         if constexpr (SG && UN) {
-            if (dyn()) {
+            if (dyncl()) {
                 cudaFuncSetAttribute(sweep_tile_kernel<R, ADV, SG, AN, UN, 2>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS::SMEM);
                 sweep_tile_kernel<R, ADV, SG, AN, UN, 2><<<grid, dim3(TS::TX, TS::TY), TS::SMEM, st>>>(
@@ -1009,7 +1108,16 @@ struct Core : CoreBase {
         const R inv3 = R(1) / R(3), two3 = R(2) * inv3;
         if (aeo_status e = substage(c, 2, c, 0, R(0), R(0))) return e;
         if (aeo_status e = substage(2, 3, c, 1, R(0.75), R(0.25))) return e;
-        return substage(3, c ^ 1, c, 1, inv3, two3);
+        if (aeo_status e = substage(3, c ^ 1, c, 1, inv3, two3)) return e;
+        return commit_sgs(c ^ 1);
+    }
+
+    // the closure's once-per-step commit (advance_sgs!), after the projection
+    aeo_status commit_sgs(int s_state) {
+        if (!lag()) return AEO_OK;
+        aeo_status e = enqueue_lag_commit(P[s_state]);
+        mark(AEO_K_SGS);
+        return e;
     }
 
     // One step on the stream: the captured graph (solver = PCG: with the three
@@ -1143,6 +1251,7 @@ struct Core : CoreBase {
         CKL();
         for (int s = 0; s < n; ++s) {
             if (aeo_status e = substage(cur, cur ^ 1, cur, 0, R(0), R(0))) return e;
+            if (aeo_status e = commit_sgs(cur ^ 1)) return e;
             cur ^= 1;
         }
         CK(cudaStreamSynchronize(st));
@@ -1226,6 +1335,8 @@ struct Core : CoreBase {
         CKL();
         aeo_adaptive_stats acc{};
         for (int s = 0; s < n; ++s) {
+            // the closure's memory as committed before the step: a retry starts from it
+            if (lag()) CK(cudaMemcpyAsync(d_lag_state + 2, d_lag_state, 2 * sizeof(int), cudaMemcpyDeviceToDevice, st));
             if (aeo_status e = launch_step(true)) return e;
             StepScalars h;
             if (aeo_status e = read_scalars(&h)) return e;
@@ -1244,6 +1355,11 @@ struct Core : CoreBase {
                     acc.max_divergence = dv;
                     acc.max_speed = sp;
                     break;
+                }
+                if (lag()) {
+                    // the committed memory and its coefficient again (the failed commit wrote cs2f)
+                    CK(cudaMemcpyAsync(d_lag_state, d_lag_state + 2, 2 * sizeof(int), cudaMemcpyDeviceToDevice, st));
+                    if (aeo_status e = lag_refresh()) return e;
                 }
                 if (retries >= c->max_retries) {
                     fail(std::string("step_adaptive: step failed (") + (!fin ? "nonfinite" : (dv > c->divergence_tol ? "divergence" : "velocity")) +
@@ -1642,7 +1758,8 @@ static aeo_status validate(const aeo_config* c, const double* zf, const double* 
     if (c->precision != AEO_PREC_FP64 && c->precision != AEO_PREC_FP32_MIXED) { *m = "unknown precision"; return AEO_ERR_ARGUMENT; }
     if (c->c_s != 0.0 && !(c->pr_t > 0.0)) { *m = "pr_t must be positive with SGS"; return AEO_ERR_ARGUMENT; }
     if (c->sgs_model != AEO_SGS_SMAGORINSKY && c->sgs_model != AEO_SGS_VREMAN && c->sgs_model != AEO_SGS_SIGMA &&
-        c->sgs_model != AEO_SGS_AMD && c->sgs_model != AEO_SGS_DYNAMIC && c->sgs_model != AEO_SGS_DYNAMIC_LOCAL) {
+        c->sgs_model != AEO_SGS_AMD && c->sgs_model != AEO_SGS_DYNAMIC && c->sgs_model != AEO_SGS_DYNAMIC_LOCAL &&
+        c->sgs_model != AEO_SGS_LAGRANGIAN) {
         *m = "unknown SGS closure";
         return AEO_ERR_ARGUMENT;
     }
@@ -1651,9 +1768,10 @@ static aeo_status validate(const aeo_config* c, const double* zf, const double* 
              ":280-284, src/operators/sigma_closure.jl:208-212, src/Operators.jl:555)";
         return AEO_ERR_ARGUMENT;
     }
-    if ((c->sgs_model == AEO_SGS_DYNAMIC || c->sgs_model == AEO_SGS_DYNAMIC_LOCAL) && c->c_s != 0.0 &&
-        (c->hx < 2 || c->hy < 2 || c->hz < 2)) {
-        *m = "the dynamic Smagorinsky closure needs host halos of at least 2 (src/Operators.jl:556-557)";
+    if ((c->sgs_model == AEO_SGS_DYNAMIC || c->sgs_model == AEO_SGS_DYNAMIC_LOCAL || c->sgs_model == AEO_SGS_LAGRANGIAN) &&
+        c->c_s != 0.0 && (c->hx < 2 || c->hy < 2 || c->hz < 2)) {
+        *m = "the dynamic Smagorinsky closures need host halos of at least 2 (src/Operators.jl:556-557, "
+             "src/operators/lagrangian_sgs.jl:170-171)";
         return AEO_ERR_ARGUMENT;
     }
     return AEO_OK;
@@ -1808,6 +1926,21 @@ aeo_status aeo_set_ibm(aeo_sim* h, const uint8_t* mask, double tau) {
 aeo_status aeo_set_sgs_buoyancy(aeo_sim* h, const double* bg) {
     ENTER(h);
     return h->core->set_sgs_buoyancy(bg);
+}
+
+aeo_status aeo_set_lagrangian(aeo_sim* h, double c0, double theta, double memory_time) {
+    ENTER(h);
+    return h->core->set_lagrangian(c0, theta, memory_time);
+}
+
+aeo_status aeo_get_sgs_state(aeo_sim* h, double* out) {
+    ENTER(h);
+    return h->core->get_sgs_state(out);
+}
+
+aeo_status aeo_set_sgs_state(aeo_sim* h, const double* in) {
+    ENTER(h);
+    return h->core->set_sgs_state(in);
 }
 
 aeo_status aeo_set_pcg(aeo_sim* h, const double* ax, const double* ay, const double* az, double tol, int32_t maxit) {

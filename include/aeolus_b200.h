@@ -40,7 +40,7 @@ enum { AEO_ADV_CENTRED = 0, AEO_ADV_WENO_JS5 = 1, AEO_ADV_WENO_Z5 = 2 };
 enum { AEO_SOLVER_FFT = 0, AEO_SOLVER_COLUMN = 1, AEO_SOLVER_PCG = 2 };
 enum { AEO_PREC_FP64 = 0, AEO_PREC_FP32_MIXED = 1 };
 enum { AEO_SGS_SMAGORINSKY = 0, AEO_SGS_VREMAN = 1, AEO_SGS_SIGMA = 2, AEO_SGS_AMD = 3, AEO_SGS_DYNAMIC = 4,
-       AEO_SGS_DYNAMIC_LOCAL = 5 };
+       AEO_SGS_DYNAMIC_LOCAL = 5, AEO_SGS_LAGRANGIAN = 6 };
 enum { AEO_FIELD_U = 0, AEO_FIELD_V = 1, AEO_FIELD_W = 2, AEO_FIELD_THETA = 3,
        AEO_FIELD_P = 4, AEO_FIELD_NUT = 5 };
 
@@ -84,7 +84,8 @@ typedef struct {
                                   the reference) and its own kappa_t
                                   (AMDClosure / compute_amd_coefficients!,
                                   src/operators/sgs_amd_vreman.jl:109-212,
-                                  :325-354; Boussinesq core); or dynamic
+                                  :325-354; g / theta_bar(z) on the sound-
+                                  proof core, aeo_set_sgs_buoyancy); or dynamic
                                   Smagorinsky (Germano-Lilly, plane-averaged,
                                   test filter 3x3x3 with width ratio 3) with
                                   c_s = the clip cs_max (0.5 in the reference;
@@ -92,8 +93,11 @@ typedef struct {
                                   src/Operators.jl:497-900), or the same with
                                   averaging = :local (each cell its own
                                   clipped ratio, _local_cs2_body!,
-                                  src/Operators.jl:873-880). Vreman, sigma,
-                                  AMD and dynamic on uniform grids           */
+                                  src/Operators.jl:873-880), or the
+                                  Lagrangian dynamic closure with c_s =
+                                  cs_max (LagrangianDynamicSmagorinsky,
+                                  aeo_set_lagrangian). Vreman, sigma, AMD,
+                                  dynamic and Lagrangian on uniform grids    */
 } aeo_config;
 
 typedef struct aeo_sim aeo_sim;
@@ -308,6 +312,25 @@ aeo_status aeo_pressure_solve_column_noalloc(int32_t nx, int32_t ny, int32_t nz,
  * an anelastic domain with the AMD closure (AEO_ERR_STATE otherwise); the
  * Boussinesq core uses g / theta0 and needs no call. */
 aeo_status aeo_set_sgs_buoyancy(aeo_sim* h, const double* bg);
+
+/* The Lagrangian dynamic closure (sgs_model = AEO_SGS_LAGRANGIAN;
+ * LagrangianDynamicSmagorinsky(mesh; C0, theta, memory_time),
+ * src/operators/lagrangian_sgs.jl:163-199, the scale-invariant model with
+ * cadence 1 and no mask; c_s is cs_max): the initial coefficient C0 (0.16),
+ * the time-scale factor theta (1.5) and a fixed memory_time (0: MLC96's T =
+ * theta Delta (I_LM I_MM)^(-1/8)).  A new domain has the defaults; the call
+ * recomputes the coefficient of the committed memory.  AEO_ERR_STATE on a
+ * domain with another closure. */
+aeo_status aeo_set_lagrangian(aeo_sim* h, double c0, double theta, double memory_time);
+
+/* sgs_state / restore_sgs_state! of the Lagrangian closure
+ * (src/operators/lagrangian_sgs.jl:372-381): 5 Nx Ny Nz + 1 doubles -- the
+ * committed I_LM, I_MM and the cell-centred u, v, w the memory was committed
+ * with (interior arrays, x fastest), then the initialised flag (0 / 1).
+ * Setting it recomputes the coefficient the next step uses.  AEO_ERR_STATE on
+ * a domain whose closure keeps no memory. */
+aeo_status aeo_get_sgs_state(aeo_sim* h, double* out);
+aeo_status aeo_set_sgs_state(aeo_sim* h, const double* in);
 
 /* The pressure solve of a domain created with solver = AEO_SOLVER_PCG:
  * conjugate gradients preconditioned by one multigrid V(2,2) cycle

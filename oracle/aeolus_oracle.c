@@ -79,6 +79,12 @@ struct oc_sim {
     double* dyn[10];
     double *dyn_lm, *dyn_mm, *cs2;
     double* amd_bg;   /* g/theta_bar(z_k) of the sound-proof core's AMD closure (interior levels), or NULL */
+    /* the Lagrangian closure: the memories I_LM, I_MM and the cell-centred
+     * velocity of the memory (interior, x fastest), the coefficient of the
+     * committed memory, the scratch of the relaxation, its parameters */
+    double *lag_ilm, *lag_imm, *lag_up, *lag_vp, *lag_wp, *lag_cs2, *lag_nlm, *lag_nmm;
+    int lag_init;
+    double lag_c0, lag_theta, lag_mt;
 };
 
 #define ID(s, i, j, k) ((int64_t)(i) + (int64_t)(s)->NX * ((int64_t)(j) + (int64_t)(s)->NY * (int64_t)(k)))
@@ -767,6 +773,7 @@ static void dyn_coefficients(oc_sim* s) {
                 s->dyn_mm[q] = M11 * M11 + M22 * M22 + M33 * M33 + 2 * (M12 * M12 + M13 * M13 + M23 * M23);
             }
 #undef SH
+    if (P->sgs_model == OC_SGS_LAGRANGIAN) return;   /* the identity's LM, MM feed the memories */
     double cmax = P->c_s * P->c_s;
     if (P->sgs_model == OC_SGS_DYNAMIC_LOCAL) {   /* _local_cs2_body!: each cell's own ratio, clipped */
         for (size_t q = 0; q < ni; ++q)
@@ -782,6 +789,111 @@ static void dyn_coefficients(oc_sim* s) {
             }
         s->cs2[k] = mm > 0 ? fmin(fmax(lm / mm, 0.0), cmax) : 0.0;
     }
+}
+
+/* --- Lagrangian dynamic Smagorinsky (LagrangianDynamicSmagorinsky,
+ * src/operators/lagrangian_sgs.jl; Meneveau, Lund & Cabot 1996): the
+ * scale-invariant model, cadence 1, no mask.  The coefficient of a step is
+ * that of the committed memory (sgs_viscosity!, :214-236): min(C0^2,
+ * cs_max^2) before the first commit, then _local_cs2_body!(I_LM, I_MM). */
+static void lag_coefficient(oc_sim* s) {
+    const oc_params* P = &s->p;
+    size_t ni = (size_t)P->nx * P->ny * P->nz;
+    double cmax = P->c_s * P->c_s;
+    for (size_t q = 0; q < ni; ++q) {
+        if (!s->lag_init) { s->lag_cs2[q] = fmin(s->lag_c0 * s->lag_c0, cmax); continue; }
+        double mm = s->lag_imm[q];
+        s->lag_cs2[q] = mm > 0 ? fmin(fmax(s->lag_ilm[q] / mm, 0.0), cmax) : 0.0;
+    }
+}
+
+static void lag_alloc(oc_sim* s) {
+    if (s->lag_ilm) return;
+    int64_t ni = (int64_t)s->p.nx * s->p.ny * s->p.nz;
+    s->lag_ilm = dalloc(ni); s->lag_imm = dalloc(ni); s->lag_up = dalloc(ni); s->lag_vp = dalloc(ni);
+    s->lag_wp = dalloc(ni); s->lag_cs2 = dalloc(ni); s->lag_nlm = dalloc(ni); s->lag_nmm = dalloc(ni);
+    s->lag_init = 0;
+    if (s->lag_c0 == 0) { s->lag_c0 = 0.16; s->lag_theta = 1.5; s->lag_mt = 0.0; }
+    lag_coefficient(s);
+}
+
+/* _wrapidx (lagrangian_sgs.jl:392): the 1-based index n wrapped (periodic) or
+ * clamped to [1, N]; returned 0-based */
+static inline int lag_wrap(int n, int N, int per) {
+    if (per) return ((n - 1) % N + N) % N;
+    return (n < 1 ? 1 : (n > N ? N : n)) - 1;
+}
+
+/* advance_sgs! (lagrangian_sgs.jl:306-355): the Germano identity at the state
+ * after the step (velocity halos filled first); the first commit sets I_MM =
+ * MM, I_LM = C0^2 MM, later ones relax along the pathlines
+ * (_lagrangian_relax! / _relax_body! / _relax_pairs!, :478-568): the
+ * departure point x - u^n dt of every cell (1-based fractional cell indices,
+ * clamped to [1, N] across a wall, _upstream_n :406-436), the trilinear
+ * interpolation of the old memories (dk, dj, di order), the time scale T =
+ * theta Delta (max(lm, 1e-8 mm) mm)^(-1/8) (epsilon = 1 where mm = 0, or the
+ * fixed memory_time), I_LM clipped at 0; then u^n is the new cell-centred
+ * velocity. */
+static void lag_commit(oc_sim* s, double dt) {
+    const oc_params* P = &s->p;
+    int Nx = P->nx, Ny = P->ny, Nz = P->nz;
+    int SX = Nx + 2, SY = Ny + 2;
+    size_t ni = (size_t)Nx * Ny * Nz;
+    lag_alloc(s);
+    fill_halos(s, s->u, LOC_FX);
+    fill_halos(s, s->v, LOC_FY);
+    fill_halos(s, s->w, LOC_FZ);
+    dyn_coefficients(s);
+    if (!s->lag_init) {
+        double c02 = s->lag_c0 * s->lag_c0;
+        for (size_t q = 0; q < ni; ++q) { s->lag_imm[q] = s->dyn_mm[q]; s->lag_ilm[q] = c02 * s->dyn_mm[q]; }
+        s->lag_init = 1;
+    } else {
+        double Delta = pow(s->dx * s->dy * s->dz, 1.0 / 3);
+        double cx = dt / s->dx, cy = dt / s->dy, cz = dt / s->dz;
+        double mt = s->lag_mt, th = s->lag_theta;
+        double efix = mt > 0 ? (dt / mt) / (1 + dt / mt) : 0.0;
+        int pz = P->bc_z == OC_BC_PERIODIC;
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int k = 0; k < Nz; ++k)
+            for (int j = 0; j < Ny; ++j)
+                for (int i = 0; i < Nx; ++i) {
+                    size_t q = (size_t)i + (size_t)Nx * ((size_t)j + (size_t)Ny * k);
+                    double x = (i + 1) - s->lag_up[q] * cx, y = (j + 1) - s->lag_vp[q] * cy;
+                    double z = (k + 1) - s->lag_wp[q] * cz;
+                    if (!pz) z = z < 1 ? 1.0 : (z > Nz ? (double)Nz : z);
+                    int x0 = (int)floor(x), y0 = (int)floor(y), z0 = (int)floor(z);
+                    double fx = x - x0, fy = y - y0, fz = z - z0;
+                    double lm = 0.0, mm = 0.0;
+                    for (int dk = 0; dk <= 1; ++dk)
+                        for (int dj = 0; dj <= 1; ++dj)
+                            for (int di = 0; di <= 1; ++di) {
+                                int a = lag_wrap(x0 + di, Nx, 1), b = lag_wrap(y0 + dj, Ny, 1), c = lag_wrap(z0 + dk, Nz, pz);
+                                double wgt = (di == 0 ? 1 - fx : fx) * (dj == 0 ? 1 - fy : fy) * (dk == 0 ? 1 - fz : fz);
+                                size_t r = (size_t)a + (size_t)Nx * ((size_t)b + (size_t)Ny * c);
+                                lm += wgt * s->lag_ilm[r];
+                                mm += wgt * s->lag_imm[r];
+                            }
+                    double eps;
+                    if (mt > 0) eps = efix;
+                    else if (mm > 0) {
+                        double Tl = th * Delta * pow(fmax(lm, 1e-8 * mm) * mm, -1.0 / 8);
+                        eps = (dt / Tl) / (1 + dt / Tl);
+                    } else eps = 1.0;
+                    s->lag_nlm[q] = fmax(eps * s->dyn_lm[q] + (1 - eps) * lm, 0.0);
+                    s->lag_nmm[q] = eps * s->dyn_mm[q] + (1 - eps) * mm;
+                }
+        memcpy(s->lag_ilm, s->lag_nlm, ni * sizeof(double));
+        memcpy(s->lag_imm, s->lag_nmm, ni * sizeof(double));
+    }
+    for (int k = 0; k < Nz; ++k)
+        for (int j = 0; j < Ny; ++j)
+            for (int i = 0; i < Nx; ++i) {
+                size_t q = (size_t)i + (size_t)Nx * ((size_t)j + (size_t)Ny * k);
+                size_t e = (size_t)(i + 1) + (size_t)SX * ((size_t)(j + 1) + (size_t)SY * (size_t)(k + 1));
+                s->lag_up[q] = s->dyn[0][e]; s->lag_vp[q] = s->dyn[1][e]; s->lag_wp[q] = s->dyn[2][e];
+            }
+    lag_coefficient(s);
 }
 
 /* --- Smagorinsky (src/FiniteVolume.jl:936-944, src/Operators.jl:451-496) -- */
@@ -828,10 +940,12 @@ static inline double smag_at(const oc_sim* s, int i, int j, int k) {
     double S2 = 2 * (S11 * S11 + S22 * S22 + S33 * S33) + 4 * (S12 * S12 + S13 * S13 + S23 * S23);
     if (s->p.sgs_model == OC_SGS_DYNAMIC)   /* cs2(k) Delta^2 |S| (_dynamic_nut_body!), dyn_coefficients first */
         return s->cs2[k - s->p.hz] * pow(s->dx * s->dy * s->dz, 2.0 / 3.0) * sqrt(S2);
-    if (s->p.sgs_model == OC_SGS_DYNAMIC_LOCAL) {   /* cs2(i, j, k): the clipped ratios left in dyn_lm */
+    if (s->p.sgs_model == OC_SGS_DYNAMIC_LOCAL || s->p.sgs_model == OC_SGS_LAGRANGIAN) {
+        /* cs2(i, j, k): the clipped ratios left in dyn_lm, or the committed memory's */
         const oc_params* P = &s->p;
         size_t q = (size_t)(i - P->hx) + (size_t)P->nx * ((size_t)(j - P->hy) + (size_t)P->ny * (size_t)(k - P->hz));
-        return s->dyn_lm[q] * pow(s->dx * s->dy * s->dz, 2.0 / 3.0) * sqrt(S2);
+        double c2 = P->sgs_model == OC_SGS_LAGRANGIAN ? s->lag_cs2[q] : s->dyn_lm[q];
+        return c2 * pow(s->dx * s->dy * s->dz, 2.0 / 3.0) * sqrt(S2);
     }
     return coef * sqrt(S2);
 }
@@ -1480,7 +1594,10 @@ int oc_project(oc_sim* s) {
 }
 
 int oc_step_euler(oc_sim* s, double dt, int nsteps) {
-    for (int n = 0; n < nsteps; ++n) substage(s, dt, 0, 0.0, 0.0);
+    for (int n = 0; n < nsteps; ++n) {
+        substage(s, dt, 0, 0.0, 0.0);
+        if (s->p.c_s != 0 && s->p.sgs_model == OC_SGS_LAGRANGIAN) lag_commit(s, dt);   /* once per step */
+    }
     return 0;
 }
 
@@ -1575,6 +1692,7 @@ int oc_step_rk3(oc_sim* s, double dt, int nsteps) {
         substage(s, dt, 0, 0.0, 0.0);
         substage(s, dt, 1, 0.75, 0.25);
         substage(s, dt, 1, inv3, two3);
+        if (s->p.c_s != 0 && s->p.sgs_model == OC_SGS_LAGRANGIAN) lag_commit(s, dt);   /* once per step */
     }
     return 0;
 }
@@ -1781,7 +1899,8 @@ oc_sim* oc_create(const oc_params* p, const double* zfi, const double* wc, const
     if (p->solver == OC_SOLVER_COLUMN && p->bc_z != OC_BC_WALL) return NULL;
     if (p->stretched && (!zfi || p->bc_z != OC_BC_WALL)) return NULL;
     if ((p->sgs_model == OC_SGS_VREMAN || p->sgs_model == OC_SGS_SIGMA || p->sgs_model == OC_SGS_AMD ||
-         p->sgs_model == OC_SGS_DYNAMIC || p->sgs_model == OC_SGS_DYNAMIC_LOCAL) && p->stretched)
+         p->sgs_model == OC_SGS_DYNAMIC || p->sgs_model == OC_SGS_DYNAMIC_LOCAL || p->sgs_model == OC_SGS_LAGRANGIAN) &&
+        p->stretched)
         return NULL;
     oc_sim* s = (oc_sim*)calloc(1, sizeof(oc_sim));
     s->p = *p;
@@ -1897,6 +2016,7 @@ oc_sim* oc_create(const oc_params* p, const double* zfi, const double* wc, const
         s->meas_sum = 0.0; s->gauge_sum = 0.0;
         for (int k = 0; k < Nz; ++k) { s->meas_sum += s->meas[k]; s->gauge_sum += s->gauge[k]; }
     }
+    if (p->c_s != 0 && p->sgs_model == OC_SGS_LAGRANGIAN) lag_alloc(s);
     if (p->solver == OC_SOLVER_PCG) {
         s->cgx = dalloc((int64_t)Nx * Ny * Nz);
         if (oc_set_apertures(s, NULL, NULL, NULL, 1e-8, 200)) {
@@ -1905,6 +2025,35 @@ oc_sim* oc_create(const oc_params* p, const double* zfi, const double* wc, const
         }
     }
     return s;
+}
+
+int oc_set_lagrangian(oc_sim* s, double c0, double theta, double memory_time) {
+    if (s->p.sgs_model != OC_SGS_LAGRANGIAN || !(c0 > 0) || !(theta > 0)) return -1;
+    lag_alloc(s);
+    s->lag_c0 = c0; s->lag_theta = theta; s->lag_mt = memory_time > 0 ? memory_time : 0.0;
+    lag_coefficient(s);
+    return 0;
+}
+
+int oc_get_sgs_state(const oc_sim* s, double* out) {
+    if (s->p.sgs_model != OC_SGS_LAGRANGIAN || !out) return -1;
+    size_t ni = (size_t)s->p.nx * s->p.ny * s->p.nz;
+    const double* a[5] = {s->lag_ilm, s->lag_imm, s->lag_up, s->lag_vp, s->lag_wp};
+    for (int f = 0; f < 5; ++f)
+        for (size_t q = 0; q < ni; ++q) out[f * ni + q] = a[f] ? a[f][q] : 0.0;
+    out[5 * ni] = s->lag_init;
+    return 0;
+}
+
+int oc_set_sgs_state(oc_sim* s, const double* in) {
+    if (s->p.sgs_model != OC_SGS_LAGRANGIAN || !in) return -1;
+    lag_alloc(s);
+    size_t ni = (size_t)s->p.nx * s->p.ny * s->p.nz;
+    double* a[5] = {s->lag_ilm, s->lag_imm, s->lag_up, s->lag_vp, s->lag_wp};
+    for (int f = 0; f < 5; ++f) memcpy(a[f], in + f * ni, ni * sizeof(double));
+    s->lag_init = in[5 * ni] != 0;
+    lag_coefficient(s);
+    return 0;
 }
 
 int oc_set_sgs_buoyancy(oc_sim* s, const double* bg) {
@@ -1995,6 +2144,8 @@ void oc_destroy(oc_sim* s) {
     free(s->apx); free(s->apy); free(s->apz); free(s->cgx); free(s->ibm);
     for (int f = 0; f < 10; ++f) free(s->dyn[f]);
     free(s->dyn_lm); free(s->dyn_mm); free(s->cs2); free(s->amd_bg);
+    free(s->lag_ilm); free(s->lag_imm); free(s->lag_up); free(s->lag_vp); free(s->lag_wp);
+    free(s->lag_cs2); free(s->lag_nlm); free(s->lag_nmm);
     if (s->cg) ocg_destroy(s->cg);
     plan_free(&s->px); plan_free(&s->py); plan_free(&s->pz);
     free(s);

@@ -27,7 +27,8 @@ enum { OC_ADV_CENTRED = 0, OC_ADV_WENO_JS5 = 1, OC_ADV_WENO_Z5 = 2 };
 enum { OC_SOLVER_FFT = 0, OC_SOLVER_COLUMN = 1, OC_SOLVER_PCG = 2 };
 enum { OC_U = 0, OC_V = 1, OC_W = 2, OC_THETA = 3, OC_P = 4, OC_NUT = 5, OC_PHI = 6, OC_KT = 7 };
 enum { OC_SGS_SMAGORINSKY = 0, OC_SGS_VREMAN = 1, OC_SGS_SIGMA = 2, OC_SGS_AMD = 3, OC_SGS_DYNAMIC = 4,
-       OC_SGS_DYNAMIC_LOCAL = 5 };   /* 5: averaging = :local, src/Operators.jl:873-880 */
+       OC_SGS_DYNAMIC_LOCAL = 5,     /* 5: averaging = :local, src/Operators.jl:873-880 */
+       OC_SGS_LAGRANGIAN = 6 };      /* 6: LagrangianDynamicSmagorinsky, src/operators/lagrangian_sgs.jl */
 
 typedef struct {
     int32_t nx, ny, nz, hx, hy, hz;
@@ -84,6 +85,15 @@ int oc_set_apertures(oc_sim* s, const double* ax, const double* ay, const double
 /* the AMD closure's buoyancy parameter g/theta_bar(z_k) of the Nz interior
  * levels (the sound-proof core; src/operators/sgs_amd_vreman.jl:331-345) */
 int oc_set_sgs_buoyancy(oc_sim* s, const double* bg);
+/* the Lagrangian closure's C0 (0.16), theta (1.5) and memory_time (<= 0:
+ * MLC96's T), src/operators/lagrangian_sgs.jl:163-199 */
+int oc_set_lagrangian(oc_sim* s, double c0, double theta, double memory_time);
+/* sgs_state / restore_sgs_state! of the Lagrangian closure
+ * (src/operators/lagrangian_sgs.jl:372-381): 5 Nx Ny Nz + 1 values, I_LM,
+ * I_MM and the cell-centred u, v, w of the memory (x fastest), then the
+ * initialised flag (0 / 1).  0 on success. */
+int oc_get_sgs_state(const oc_sim* s, double* out);
+int oc_set_sgs_state(oc_sim* s, const double* in);
 /* the implicit IBM correction after every predictor (implicit_ibm_correction!,
  * src/IBM.jl:295-300): mask storage-shaped, nonzero = solid (interior cells
  * count), NULL switches it off; tau >= 0 (0: the faces are zeroed); not with

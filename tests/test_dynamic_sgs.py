@@ -50,10 +50,11 @@ def state(g, seed=5, amp=1.0):
     return u, v, w, th
 
 
-def dynamic_numpy(g, u, v, w, cs_max, local=False):
+def dynamic_numpy(g, u, v, w, cs_max, local=False, parts=False):
     """_germano_pass1 / _germano_pass2 / _plane_cs2_body! (local:
     _local_cs2_body!) / _dynamic_nut_body! on storage arrays with filled
-    halos: nu_t on the interior."""
+    halos: nu_t on the interior (parts: each cell's LM, MM, |S| and its
+    cell-centred velocity instead)."""
     hx, hy, hz = g.halo
     nx, ny, nz = g.size
 
@@ -90,6 +91,9 @@ def dynamic_numpy(g, u, v, w, cs_max, local=False):
     M = [2 * d2 * (t[15 + c] - 9.0 * magSt * A[c]) for c in range(6)]
     LM = L[0] * M[0] + L[1] * M[1] + L[2] * M[2] + 2 * (L[3] * M[3] + L[4] * M[4] + L[5] * M[5])
     MM = M[0] ** 2 + M[1] ** 2 + M[2] ** 2 + 2 * (M[3] ** 2 + M[4] ** 2 + M[5] ** 2)
+    if parts:
+        inner = (slice(1, -1),) * 3
+        return LM, MM, ms[inner], (Uc[inner], Vc[inner], Wc[inner])
     if local:
         cs2 = np.where(MM > 0, np.clip(LM / np.where(MM > 0, MM, 1.0), 0.0, cs_max ** 2), 0.0)
         return cs2 * d2 * ms[1:-1, 1:-1, 1:-1], cs2
