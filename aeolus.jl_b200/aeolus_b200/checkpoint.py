@@ -4,8 +4,9 @@ write_checkpoint and the restart, src/io/checkpoint.jl:346-473).
 A payload is a self-contained dict: the format tag and version, the mesh
 record, the simulation time, copies of the prognostic storage fields (u, v,
 w, theta and the pressure, halos included), the scalar parameters of the
-CoreSpec, the closure name, the stepper state (the last accepted dt of an
-adaptive run) and free-form extras. `buffers` (the fields of an earlier
+CoreSpec, the closure name and its state (the Lagrangian closure's
+memories, sgs_state / restore_sgs_state!), the stepper state (the last
+accepted dt of an adaptive run) and free-form extras. `buffers` (the fields of an earlier
 payload of the same domain) are refilled in place, so a run that keeps its
 last good state (a rollback snapshot) allocates once.
 
@@ -28,6 +29,20 @@ import numpy as np
 CHECKPOINT_FORMAT = "aeolus_b200.checkpoint"
 CHECKPOINT_VERSION = 1
 FIELDS = ("u", "v", "w", "theta", "p")
+CLOSURE_ARRAYS = ("I_LM", "I_MM", "U", "V", "W")
+
+
+def closure_state(sim) -> Optional[Dict[str, Any]]:
+    """checkpoint_state of the run's closure (a copy of sgs_state): the
+    Lagrangian closure's memories and its initialised flag, None for the
+    closures that keep no state."""
+    spec = sim.spec
+    if spec.c_s == 0 or spec.sgs != "lagrangian":
+        return None
+    st = sim.sgs_state()
+    out: Dict[str, Any] = {k: np.array(a, dtype=np.float64, copy=True) for k, a in zip(CLOSURE_ARRAYS, st[:5])}
+    out["initialised"] = bool(st[5])
+    return out
 
 
 def mesh_record(grid) -> Dict[str, Any]:
@@ -74,6 +89,7 @@ def checkpoint_payload(sim, t: float = 0.0, stepper: Optional[Dict[str, Any]] = 
         "fields": fields,
         "parameters": parameters(spec),
         "closure_type": spec.sgs if spec.c_s != 0 else "",
+        "closure": closure_state(sim),
         "stepper": None if stepper is None else dict(stepper),
         "extra": {} if extra is None else dict(extra),
     }
@@ -97,9 +113,13 @@ def write_checkpoint(path: str, payload: Dict[str, Any]) -> str:
     (write_checkpoint, src/io/checkpoint.jl:400-417)."""
     d = os.path.dirname(os.path.abspath(path))
     os.makedirs(d, exist_ok=True)
-    head = {k: v for k, v in payload.items() if k != "fields"}
+    head = {k: v for k, v in payload.items() if k not in ("fields", "closure")}
     head["field_names"] = sorted(payload["fields"])
     arrays = {"field_" + k: v for k, v in payload["fields"].items()}
+    cl = payload.get("closure")
+    head["closure"] = None if cl is None else {"initialised": bool(cl["initialised"])}
+    if cl is not None:
+        arrays.update({"closure_" + k: cl[k] for k in CLOSURE_ARRAYS})
     tmp = path + ".tmp"
     with open(tmp, "wb") as f:
         np.savez(f, header=np.frombuffer(json.dumps(head).encode(), dtype=np.uint8), **arrays)
@@ -114,6 +134,8 @@ def read_checkpoint(path: str) -> Dict[str, Any]:
         if head.get("format") != CHECKPOINT_FORMAT:
             raise ValueError(f"{path}: not a checkpoint of this format ({head.get('format')!r})")
         fields = {k: np.array(z["field_" + k]) for k in head.pop("field_names")}
+        if head.get("closure") is not None:
+            head["closure"].update({k: np.array(z["closure_" + k]) for k in CLOSURE_ARRAYS})
     head["fields"] = fields
     return head
 
@@ -144,6 +166,19 @@ def restore(sim, payload, check_parameters: bool = True):
     missing = [n for n in FIELDS if n not in payload["fields"]]
     if missing:
         raise ValueError(f"checkpoint lacks the fields {missing}")
+    mine = sim.spec.sgs if sim.spec.c_s != 0 else ""
+    if payload.get("closure_type", "") != mine:
+        raise ValueError(f"the checkpoint's closure is {payload.get('closure_type')!r}, the domain's {mine!r}")
+    cl = payload.get("closure")
+    if (cl is None) != (closure_state_kind(sim) is None):
+        raise ValueError("the checkpoint's closure state does not fit the domain's closure")
     for name in FIELDS:
         sim.set_field(name, np.ascontiguousarray(payload["fields"][name], dtype=np.float64))
+    if cl is not None:
+        sim.set_sgs_state(tuple(cl[k] for k in CLOSURE_ARRAYS) + (bool(cl["initialised"]),))
     return payload["t"], payload["stepper"]
+
+
+def closure_state_kind(sim) -> Optional[str]:
+    """The kind of state the domain's closure keeps (None: none)."""
+    return "lagrangian" if sim.spec.c_s != 0 and sim.spec.sgs == "lagrangian" else None

@@ -20,9 +20,9 @@ from aeolus_b200.checkpoint import (FIELDS, checkpoint, checkpoint_payload, read
 from oracle.oracle import OracleSimulation
 
 
-def spec(n=16, c_s=0.17, advection="weno_js5"):
+def spec(n=16, c_s=0.17, advection="weno_js5", sgs="smagorinsky"):
     g = regular_grid((n, n, n), (1.0, 1.0, 0.5), halo=(3, 3, 3), bc_z="wall")
-    return CoreSpec(grid=g, c_s=c_s, theta0=300.0, advection=advection, nu=1e-4)
+    return CoreSpec(grid=g, c_s=c_s, theta0=300.0, advection=advection, nu=1e-4, sgs=sgs)
 
 
 def state(g, seed=3):
@@ -37,8 +37,8 @@ def state(g, seed=3):
     return u, v, w, th
 
 
-def restart_matches(make, tmp_path):
-    sp = spec()
+def restart_matches(make, tmp_path, sp=None):
+    sp = sp or spec()
     a = make(sp)
     a.set_state(*state(sp.grid))
     a.project()
@@ -53,6 +53,9 @@ def restart_matches(make, tmp_path):
     b.step_rk3(2e-3, 2)
     for n in ("u", "v", "w", "theta"):
         assert np.array_equal(a.get_field(n), b.get_field(n)), n
+    if sp.sgs == "lagrangian":
+        for x, y in zip(a.sgs_state(), b.sgs_state()):
+            assert np.array_equal(x, y)
 
 
 def test_written_checkpoint_reads_back(tmp_path):
@@ -73,6 +76,17 @@ def test_written_checkpoint_reads_back(tmp_path):
 
 def test_restart_continues_the_run_exactly(tmp_path):
     restart_matches(OracleSimulation, str(tmp_path))
+
+
+def test_restart_with_the_lagrangian_memories(tmp_path):
+    """the closure's state (checkpoint_state = sgs_state) travels with the
+    fields: the restarted run continues the memories bit for bit"""
+    restart_matches(OracleSimulation, tmp_path, spec(c_s=0.5, sgs="lagrangian"))
+    a = OracleSimulation(spec(c_s=0.5, sgs="lagrangian"))
+    a.set_state(*state(a.grid))
+    p = checkpoint(a, os.path.join(tmp_path, "lag.ckpt"))
+    with pytest.raises(ValueError):
+        restore(OracleSimulation(spec()), p, check_parameters=False)
 
 
 def test_checkpoint_of_another_domain_is_refused(tmp_path):
@@ -105,6 +119,7 @@ def test_buffers_are_refilled_in_place():
 
 
 @pytest.mark.gpu
-def test_gpu_restart_continues_the_run_exactly(tmp_path):
+@pytest.mark.parametrize("sgs,c_s", [("smagorinsky", 0.17), ("lagrangian", 0.5)])
+def test_gpu_restart_continues_the_run_exactly(tmp_path, sgs, c_s):
     from aeolus_b200.simulation import Simulation
-    restart_matches(Simulation, str(tmp_path))
+    restart_matches(Simulation, str(tmp_path), spec(c_s=c_s, sgs=sgs))
