@@ -34,11 +34,14 @@ CLOSURE_ARRAYS = ("I_LM", "I_MM", "U", "V", "W")
 
 def closure_state(sim) -> Optional[Dict[str, Any]]:
     """checkpoint_state of the run's closure (a copy of sgs_state): the
-    Lagrangian closure's memories and its initialised flag, None for the
-    closures that keep no state."""
+    Lagrangian closure's memories and its initialised flag, the TKE
+    closure's e, None for the closures that keep no state."""
     spec = sim.spec
-    if spec.c_s == 0 or spec.sgs != "lagrangian":
+    kind = closure_state_kind(sim)
+    if kind is None:
         return None
+    if kind == "tke":
+        return {"e": np.array(sim.sgs_state(), dtype=np.float64, copy=True)}
     st = sim.sgs_state()
     out: Dict[str, Any] = {k: np.array(a, dtype=np.float64, copy=True) for k, a in zip(CLOSURE_ARRAYS, st[:5])}
     out["initialised"] = bool(st[5])
@@ -117,9 +120,10 @@ def write_checkpoint(path: str, payload: Dict[str, Any]) -> str:
     head["field_names"] = sorted(payload["fields"])
     arrays = {"field_" + k: v for k, v in payload["fields"].items()}
     cl = payload.get("closure")
-    head["closure"] = None if cl is None else {"initialised": bool(cl["initialised"])}
+    head["closure"] = None if cl is None else {k: v for k, v in cl.items() if not isinstance(v, np.ndarray)}
     if cl is not None:
-        arrays.update({"closure_" + k: cl[k] for k in CLOSURE_ARRAYS})
+        head["closure"]["arrays"] = sorted(k for k, v in cl.items() if isinstance(v, np.ndarray))
+        arrays.update({"closure_" + k: v for k, v in cl.items() if isinstance(v, np.ndarray)})
     tmp = path + ".tmp"
     with open(tmp, "wb") as f:
         np.savez(f, header=np.frombuffer(json.dumps(head).encode(), dtype=np.uint8), **arrays)
@@ -135,7 +139,7 @@ def read_checkpoint(path: str) -> Dict[str, Any]:
             raise ValueError(f"{path}: not a checkpoint of this format ({head.get('format')!r})")
         fields = {k: np.array(z["field_" + k]) for k in head.pop("field_names")}
         if head.get("closure") is not None:
-            head["closure"].update({k: np.array(z["closure_" + k]) for k in CLOSURE_ARRAYS})
+            head["closure"].update({k: np.array(z["closure_" + k]) for k in head["closure"].pop("arrays")})
     head["fields"] = fields
     return head
 
@@ -175,10 +179,15 @@ def restore(sim, payload, check_parameters: bool = True):
     for name in FIELDS:
         sim.set_field(name, np.ascontiguousarray(payload["fields"][name], dtype=np.float64))
     if cl is not None:
-        sim.set_sgs_state(tuple(cl[k] for k in CLOSURE_ARRAYS) + (bool(cl["initialised"]),))
+        if closure_state_kind(sim) == "tke":
+            sim.set_sgs_state(cl["e"])
+        else:
+            sim.set_sgs_state(tuple(cl[k] for k in CLOSURE_ARRAYS) + (bool(cl["initialised"]),))
     return payload["t"], payload["stepper"]
 
 
 def closure_state_kind(sim) -> Optional[str]:
     """The kind of state the domain's closure keeps (None: none)."""
-    return "lagrangian" if sim.spec.c_s != 0 and sim.spec.sgs == "lagrangian" else None
+    if sim.spec.c_s == 0 or sim.spec.sgs not in ("lagrangian", "tke"):
+        return None
+    return sim.spec.sgs

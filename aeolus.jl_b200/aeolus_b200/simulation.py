@@ -96,6 +96,11 @@ class Simulation:
         if spec.sgs == "lagrangian" and spec.c_s != 0:
             mt = spec.lag_memory_time
             _lib.check(lib.aeo_set_lagrangian(h, spec.lag_c0, spec.lag_theta, 0.0 if mt is None else mt), h)
+        if spec.sgs == "tke" and spec.c_s != 0:
+            _lib.check(lib.aeo_set_tke(h, spec.tke_c_eps0, spec.tke_c_eps1, spec.tke_c_l,
+                                       1 if spec.tke_dissipation == "exact" else 0), h)
+            if spec.tke_e0:
+                self.set_sgs_state(np.full((g.nz, g.ny, g.nx), float(spec.tke_e0)))
 
     # ---- lifecycle ------------------------------------------------------------
     def close(self):
@@ -126,12 +131,22 @@ class Simulation:
         (src/operators/lagrangian_sgs.jl:372-381)."""
         g = self.grid
         n = g.nx * g.ny * g.nz
+        if self.spec.sgs == "tke":       # e on the interior
+            out = np.empty(n)
+            _lib.check(self._lib.aeo_get_sgs_state(self._h, _ptr(out)), self._h)
+            return out.reshape(g.nz, g.ny, g.nx)
         out = np.empty(5 * n + 1)
         _lib.check(self._lib.aeo_get_sgs_state(self._h, _ptr(out)), self._h)
         return tuple(out[f * n:(f + 1) * n].reshape(g.nz, g.ny, g.nx).copy() for f in range(5)) + (bool(out[5 * n]),)
 
     def set_sgs_state(self, state):
         g = self.grid
+        if self.spec.sgs == "tke":
+            a = np.ascontiguousarray(state, dtype=np.float64)
+            if a.shape != (g.nz, g.ny, g.nx):
+                raise ValueError(f"sgs state: e of shape {(g.nz, g.ny, g.nx)} expected")
+            _lib.check(self._lib.aeo_set_sgs_state(self._h, _ptr(a)), self._h)
+            return
         arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in state[:5]]
         if any(a.shape != (g.nz, g.ny, g.nx) for a in arrs):
             raise ValueError(f"sgs state: five {(g.nz, g.ny, g.nx)} arrays and the initialised flag expected")

@@ -16,7 +16,7 @@ from .grids import PERIODIC, WALL, Grid
 
 CORES = {"boussinesq": 0, "anelastic": 1}
 ADVECTION = {"centred": 0, "weno_js5": 1, "weno_z5": 2}
-SGS_MODELS = {"smagorinsky": 0, "vreman": 1, "sigma": 2, "amd": 3, "dynamic": 4, "lagrangian": 6}
+SGS_MODELS = {"smagorinsky": 0, "vreman": 1, "sigma": 2, "amd": 3, "dynamic": 4, "lagrangian": 6, "tke": 7}
 SOLVERS = {"fft": 0, "column": 1, "pcg": 2}
 PRECISIONS = {"fp64": 0, "fp32_mixed": 1}
 FIELDS = {"u": 0, "v": 1, "w": 2, "theta": 3, "p": 4, "nut": 5}
@@ -45,6 +45,13 @@ class CoreSpec:
     lag_c0: float = 0.16
     lag_theta: float = 1.5
     lag_memory_time: Optional[float] = None
+    # sgs = "tke" (TKEClosure, Deardorff 1980 / Moeng 1984; c_s is c_k, 0.1): c_eps0, c_eps1, c_l, the
+    # dissipation form ("semi_implicit" or "exact") and a uniform initial e (m^2 s^-2)
+    tke_c_eps0: float = 0.19
+    tke_c_eps1: float = 0.51
+    tke_c_l: float = 0.76
+    tke_dissipation: str = "semi_implicit"
+    tke_e0: float = 0.0
     pr_t: float = 1.0 / 3.0
     flux_bot: float = 0.0
     flux_top: float = 0.0
@@ -96,13 +103,22 @@ class CoreSpec:
             raise ValueError(f"sgs must be one of {list(SGS_MODELS)}, got {self.sgs!r}")
         if self.averaging not in ("plane", "local"):
             raise ValueError(f"averaging must be 'plane' or 'local', got {self.averaging!r} (src/Operators.jl:558-559)")
-        if self.sgs in ("vreman", "sigma", "amd", "dynamic", "lagrangian") and self.grid.stretched:
+        if self.sgs in ("vreman", "sigma", "amd", "dynamic", "lagrangian", "tke") and self.grid.stretched:
             raise ValueError("the Vreman, sigma and AMD closures take a RegularGrid only (compute_vreman_nut!, "
                              "src/operators/sgs_amd_vreman.jl:280-284; compute_amd_coefficients!, :102-107; "
                              "compute_sigma_nut!, src/operators/sigma_closure.jl:208-212)")
         if self.sgs in ("dynamic", "lagrangian") and self.c_s != 0 and min(self.grid.halo) < 2:
             raise ValueError("the dynamic Smagorinsky closures need halos of at least 2 (src/Operators.jl:556-557, "
                              "src/operators/lagrangian_sgs.jl:170-171)")
+        if self.sgs == "tke" and self.c_s != 0:
+            if self.core != "boussinesq" or min(self.grid.halo) < 3:
+                raise ValueError("the TKE closure runs on the Boussinesq core (theta0 its buoyancy reference) with "
+                                 "halos >= 3 (the WENO-Z5 transport of e, src/PrognosticSGS.jl:354-356)")
+            if self.tke_dissipation not in ("semi_implicit", "exact"):
+                raise ValueError(f"dissipation must be 'semi_implicit' or 'exact', got {self.tke_dissipation!r} "
+                                 "(src/PrognosticSGS.jl:332-333)")
+            if not (self.tke_c_eps0 >= 0 and self.tke_c_eps1 >= 0 and self.tke_c_l > 0 and self.tke_e0 >= 0):
+                raise ValueError("c_eps0, c_eps1 >= 0, c_l > 0 and e0 >= 0 required")
         if self.sgs == "lagrangian":
             if not (self.lag_c0 > 0 and self.lag_theta > 0):
                 raise ValueError("lag_c0 and lag_theta must be positive")

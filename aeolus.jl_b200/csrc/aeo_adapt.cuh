@@ -61,6 +61,10 @@ __global__ void __launch_bounds__(256) cfl_levels_kernel(Geo g, const R* __restr
                 const NuKappa<R> nk = amd_point<R, UNI>(m, g, k, c_s, m.lv(LV_BGC, k), pr_t, U, V, W, T);
                 nm = fmax(nm, (double)nk.nu);
                 km = fmax(km, (double)nk.ka);
+            } else if (g.sgs_model == 7) {   // the TKE closure's nu_t and kappa_t
+                const NuKappa<R> nk = tke_point<R>(g, i, j, k, th[q - g.sz], th[q], th[q + g.sz]);
+                nm = fmax(nm, (double)nk.nu);
+                km = fmax(km, (double)nk.ka);
             } else {
                 nm = fmax(nm, (double)smag_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, U, V, W));
             }
@@ -118,7 +122,7 @@ __global__ void dt_pick_kernel(Geo g, CflParams c, const double* __restrict__ pa
     double nu_total = c.nu + nutm;
     double dt_diff = nu_total > 0 ? c.c_diff * harm / nu_total : INF;
     // kappa_t: nut / Pr_t, or the AMD closure's own (max(nu_t, kappa_t) binds, src/TimeIntegration.jl:322-335)
-    double kt = c.sgs ? (g.sgs_model == 3 ? ktm : nutm / c.pr_t) : 0.0;
+    double kt = c.sgs ? ((g.sgs_model == 3 || g.sgs_model == 7) ? ktm : nutm / c.pr_t) : 0.0;
     double ksgs = fmax(nutm, kt);
     double dt_sgs = ksgs > 0 ? c.c_diff * harm / ksgs : INF;
     double N = sqrt(fmax(n2max, 0.0));

@@ -90,6 +90,11 @@ struct Geo {
     // the SGS closure when c_s > 0: 0 Smagorinsky, 1 Vreman (coefficient 2.5 c_s^2)
     int sgs_model;
     double sgs_cv;
+    // the TKE closure (sgs_model 7): its e (padded, working precision, halos
+    // filled), c_k, c_l, Delta = (dx dy dz)^(1/3), g / theta0 (0 without
+    // buoyancy)
+    const void* tke;
+    double tke_ck, tke_cl, tke_delta, tke_bg;
 };
 
 __device__ __forceinline__ long long pidx(const Geo& g, int i, int j, int k) {

@@ -619,6 +619,25 @@ struct NuKappa {
     T nu, ka;
 };
 
+// The Deardorff (1980) / Moeng (1984) coefficients of the TKE closure at
+// cell (i, j, k) (TKEClosure: _coefficients_body!, tke_length_scale,
+// tke_eddy_coefficients, src/PrognosticSGS.jl:93-110, :135-139, :432-454):
+// N^2 = (g/theta0) (theta_face_above - theta_face_below) / dz with the faces
+// the two-cell means (buoyancy_frequency_squared!,
+// src/operators/stratification.jl:124-135), l = min(Delta, c_l sqrt(e) / N)
+// where N^2 > 0 (else Delta), nu_t = c_k l sqrt(e), kappa_t = (1 + 2 l /
+// Delta) nu_t; e of the committed step (the padded field g.tke).
+template <typename R>
+__device__ __forceinline__ NuKappa<R> tke_point(const Geo& g, int i, int j, int k, R tlo, R tc, R thi) {
+    const R e = __ldg(static_cast<const R*>(g.tke) + pidx(g, i, j, k));
+    const R N2 = R(g.tke_bg) * ((R(0.5) * (tc + thi)) - (R(0.5) * (tlo + tc))) * R(g.idz);
+    const R D = R(g.tke_delta);
+    const R sq = sqrt(fmax(e, R(0)));
+    const R l = N2 > R(0) ? fmin(D, R(g.tke_cl) * sq / sqrt(N2)) : D;
+    const R nu = R(g.tke_ck) * l * sq;
+    return NuKappa<R>{nu, (R(1) + R(2) * l / D) * nu};
+}
+
 template <typename R>
 __device__ __noinline__ NuKappa<R> amd_lane(R ux, R uy, R uz, R vx, R vy, R vz, R wx, R wy, R wz, R tx, R ty, R tz,
                                             R d2x, R d2y, R d2z, R bg, R C, R pr_t) {
@@ -710,6 +729,8 @@ __global__ void __launch_bounds__(256) smagorinsky_kernel(Geo g, const R* __rest
         Nb<R> T{th + q, g.sy, g.sz};
         const Met<R, UNI> m(g);
         nut[q] = amd_point<R, UNI>(m, g, k, c_s, m.lv(LV_BGC, k), pr_t, U, V, W, T).nu;
+    } else if (g.sgs_model == 7) {
+        nut[q] = tke_point<R>(g, i, j, k, th[q - g.sz], th[q], th[q + g.sz]).nu;
     } else {
         nut[q] = smag_point<R, UNI>(Met<R, UNI>(g), g, k, c_s, U, V, W);
     }

@@ -137,6 +137,15 @@ __device__ __forceinline__ void pair_nut_plane(const Met<float, UNI>& m, const S
             const NuKappa<F2> nk = amd_point<R, UNI>(m, g, L, R(a.c_s), m.lv(LV_BGC, L), a.pr_t, Uq, Vq, Wq, Tq);
             *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nk.nu.v;
             *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc + S::KT_OFS) = nk.ka.v;
+        } else if constexpr (CLOS == 3) {
+            // the TKE closure, cell by cell: the pair's cells x = i0 + 2 pc - 2 (+1), y = j0 + cj - 1
+            const PairAcc<1, S::PW, 3 * S::PSZA> Tq{q};
+            const F2 lo = Tq(0, 0, -1), c = Tq(0, 0, 0), hi = Tq(0, 0, 1);
+            const int gi = i0 + 2 * pc - 2, gj = j0 + cj - 1;
+            const NuKappa<float> n0 = tke_point<float>(g, gi, gj, L, lo.v.x, c.v.x, hi.v.x);
+            const NuKappa<float> n1 = tke_point<float>(g, gi + 1, gj, L, lo.v.y, c.v.y, hi.v.y);
+            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = make_float2(n0.nu, n1.nu);
+            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc + S::KT_OFS) = make_float2(n0.ka, n1.ka);
         } else {
             const F2 nv = smag_point<R, UNI>(m, g, L, R(a.c_s), Uq, Vq, Wq);
             *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nv.v;
@@ -239,7 +248,7 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(const __grid_constan
                 float* dst = nut_plane(L);
                 const float* srcp = nut_plane(Ls);
                 for (int e = tid; e < S::NPS; e += S::NT) dst[e] = srcp[e];
-                if (CLOS == 1)
+                if (CLOS == 1 || CLOS == 3)
                     for (int e = tid; e < S::NPS; e += S::NT) dst[e + S::KT_OFS] = srcp[e + S::KT_OFS];
             }
             __syncthreads();
@@ -271,7 +280,7 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(const __grid_constan
                     float* dst = nut_plane(L);
                     const float* srcp = nut_plane(2 * g.nz - 1 - L);
                     for (int e = tid; e < S::NPS; e += S::NT) dst[e] = srcp[e];
-                    if (CLOS == 1)
+                    if (CLOS == 1 || CLOS == 3)
                         for (int e = tid; e < S::NPS; e += S::NT) dst[e + S::KT_OFS] = srcp[e + S::KT_OFS];
                 } else if (ok) {
                     const float* sp[3] = {plane(L - 1), plane(L), plane(L + 1)};
@@ -293,7 +302,7 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(const __grid_constan
             }
             if (active) {
                 F2 tu, tv, tw, tt;
-                sweep_point<R, 0, SGS, ANEL, UNI, false, CLOS == 1>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt);
+                sweep_point<R, 0, SGS, ANEL, UNI, false, CLOS == 1 || CLOS == 3>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt);
                 const long long qi = iidx(g, i, j, k), q = pidx(g, i, j, k);
                 const F2 fdt(dt);
                 *reinterpret_cast<float2*>(a.us + qi) = (U(0, 0, 0) + fdt * tu).v;

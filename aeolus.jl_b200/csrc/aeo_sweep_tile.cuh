@@ -126,7 +126,8 @@ struct NutAcc {
 
 // CLOS: the closure of the coefficient pass: 0 the static ones (smag_point),
 // 1 the anisotropic minimum-dissipation closure (its kappa_t planes KT_OFS
-// elements past the nut planes), 2 dynamic Smagorinsky (cs2 per level)
+// elements past the nut planes), 2 dynamic Smagorinsky (cs2 per level or
+// cell), 3 the TKE closure (tke_point; its kappa_t planes as the AMD's)
 template <typename R, int ADV, bool SGS, bool ANEL, bool UNI, int CLOS = 0>
 __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__ TileMaps maps, SweepArgs<R> a,
                                                          int kchunk, int* err) {
@@ -248,6 +249,11 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
                         const NuKappa<R> nk = amd_point<R, UNI>(m, g, L, R(a.c_s), m.lv(LV_BGC, L), a.pr_t, Uq, Vq, Wq, Tq);
                         np[cj * S::NPW + ci] = nk.nu;
                         np[cj * S::NPW + ci + S::KT_OFS] = nk.ka;
+                    } else if constexpr (CLOS == 3) {
+                        const SmAcc<R, 1, S::PW, 3 * S::PSZA> Tq{q};
+                        const NuKappa<R> nk = tke_point<R>(g, i0 + ci - 1, j0 + cj - 1, L, Tq(0, 0, -1), Tq(0, 0, 0), Tq(0, 0, 1));
+                        np[cj * S::NPW + ci] = nk.nu;
+                        np[cj * S::NPW + ci + S::KT_OFS] = nk.ka;
                     } else {
                         np[cj * S::NPW + ci] = smag_point<R, UNI>(m, g, L, R(a.c_s), Uq, Vq, Wq);
                     }
@@ -262,7 +268,7 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
                     R* dst = nutp + (size_t)((L + 3) % 3) * S::NPS;
                     const R* src = nutp + (size_t)((Ls + 3) % 3) * S::NPS;
                     for (int e = tid; e < S::NPS; e += S::NT) dst[e] = src[e];
-                    if (CLOS == 1)
+                    if (CLOS == 1 || CLOS == 3)
                         for (int e = tid; e < S::NPS; e += S::NT) dst[e + S::KT_OFS] = src[e + S::KT_OFS];
                 }
                 __syncthreads();
@@ -330,7 +336,7 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
             }
         }
         if (active) {
-            sweep_point<R, ADV, SGS, ANEL, UNI, S::SHARE, CLOS == 1>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt,
+            sweep_point<R, ADV, SGS, ANEL, UNI, S::SHARE, CLOS == 1 || CLOS == 3>(m, a, g, k, U, V, W, T, N, tu, tv, tw, tt,
                                                                (ADV > 0 && !S::SHARE) ? &zc : nullptr);
             if (ADV > 0 && !S::SHARE) zc.valid = true;
             const long long qi = iidx(g, i, j, k), q = pidx(g, i, j, k);

@@ -40,6 +40,7 @@
 #include "aeo_init.cuh"
 #include "aeo_misc.cuh"
 #include "aeo_sweep.cuh"
+#include "aeo_tke.cuh"
 #include "aeo_sweep_pair.cuh"
 #include "aeo_sweep_wpair.cuh"
 
@@ -122,6 +123,7 @@ struct CoreBase {
     virtual aeo_status set_lagrangian(double c0, double theta, double memory_time) = 0;
     virtual aeo_status get_sgs_state(double* out) = 0;
     virtual aeo_status set_sgs_state(const double* in) = 0;
+    virtual aeo_status set_tke(double c_eps0, double c_eps1, double c_l, int exact) = 0;
 };
 
 struct aeo_sim {
@@ -187,6 +189,9 @@ struct Core : CoreBase {
     bool dyn() const { return sgs && (cfg.sgs_model == AEO_SGS_DYNAMIC || cfg.sgs_model == AEO_SGS_DYNAMIC_LOCAL); }
     bool dyn_local() const { return sgs && cfg.sgs_model == AEO_SGS_DYNAMIC_LOCAL; }
     bool lag() const { return sgs && cfg.sgs_model == AEO_SGS_LAGRANGIAN; }
+    bool tke() const { return sgs && cfg.sgs_model == AEO_SGS_TKE; }
+    // the closures whose kappa_t is their own (the sweeps' kappa_t planes)
+    bool own_kappa() const { return amd() || tke(); }
     // the sweeps' dynamic coefficient (per level, or per cell in cs2f)
     bool dyncl() const { return dyn() || lag(); }
     // the dynamic Smagorinsky workspace: the ten pass-1 fields, the per-block
@@ -296,8 +301,97 @@ struct Core : CoreBase {
         CK(cudaMemcpy(d_lag_state, hs, sizeof(hs), cudaMemcpyHostToDevice));
         return lag_refresh();
     }
-    aeo_status get_sgs_state(double* out) override { return sgs_state(out, true); }
-    aeo_status set_sgs_state(const double* in) override { return sgs_state(const_cast<double*>(in), false); }
+    aeo_status get_sgs_state(double* out) override {
+        return tke() ? tke_state(out, true) : sgs_state(out, true);
+    }
+    aeo_status set_sgs_state(const double* in) override {
+        return tke() ? tke_state(const_cast<double*>(in), false) : sgs_state(const_cast<double*>(in), false);
+    }
+
+    // the TKE closure: e (padded, halos filled), K = 2 nu_t and the transport
+    // tendency of the commit (padded), the copy of e an adaptive step can
+    // return to, the coefficients
+    R *d_tke = nullptr, *d_tk2 = nullptr, *d_tkt = nullptr, *d_tke_keep = nullptr;
+    TkeArgs tkeA{};
+    int tke_launches() const { return tke() ? 8 : 0; }   // per step
+    aeo_status set_tke(double c_eps0, double c_eps1, double c_l, int exact) override {
+        if (!tke()) { fail("set_tke: the domain's closure is not the TKE closure"); return AEO_ERR_STATE; }
+        if (!(c_eps0 >= 0) || !(c_eps1 >= 0) || !(c_l > 0) || !std::isfinite(c_eps0) || !std::isfinite(c_eps1) ||
+            !std::isfinite(c_l)) {
+            fail("set_tke: c_eps0 >= 0, c_eps1 >= 0 and c_l > 0 required");
+            return AEO_ERR_ARGUMENT;
+        }
+        CK(cudaStreamSynchronize(st));
+        drop_graphs();   // the coefficients are captured by value
+        tkeA.ce0 = c_eps0; tkeA.ce1 = c_eps1; tkeA.cl = c_l; tkeA.exact = exact != 0;
+        g.tke_cl = c_l;
+        return AEO_OK;
+    }
+    // advance_sgs! of the TKE closure for the state in `in` (halos filled)
+    aeo_status enqueue_tke_commit(R* const* in) {
+        const unsigned nb = (unsigned)std::min<long long>((g.nin + 255) / 256, 148LL * 16);
+        tke_coef_kernel<R><<<nb, 256, 0, st>>>(g, tkeA, d_tke, in[3], d_tk2);
+        CKL();
+        R* f[2] = {d_tk2, d_tke};
+        int l[2] = {LOC_C, LOC_C};
+        if (aeo_status e = halo(f, l, 2)) return e;
+        PosGeo pg{};
+        pg.nx = g.nx; pg.ny = g.ny; pg.nz = g.nz;
+        pg.hx = AEO_HX; pg.hy = AEO_H; pg.hz = AEO_H;
+        pg.sx = 1; pg.sy = g.sy; pg.sz = g.sz;
+        pg.idx = g.idx; pg.idy = g.idy; pg.idz = g.idz;
+        const dim3 gf((unsigned)((g.nx + 1 + 127) / 128), (unsigned)(g.ny + 1), (unsigned)(g.nz + 1));
+        pos_flux_kernel<R, AEO_ADV_WENO_Z5><<<gf, 128, 0, st>>>(pg, in[0], in[1], in[2], d_tke, pos_fx, pos_fy, pos_fz);
+        CKL();
+        const dim3 gc((unsigned)((g.nx + 127) / 128), (unsigned)g.ny, (unsigned)g.nz);
+        pos_ratio_kernel<R><<<gc, 128, 0, st>>>(pg, in[0], in[1], in[2], d_tke, pos_fx, pos_fy, pos_fz, &d_sc->dt, pos_r);
+        CKL();
+        pos_apply_kernel<R><<<gc, 128, 0, st>>>(pg, in[0], in[1], in[2], d_tke, pos_fx, pos_fy, pos_fz, pos_r, d_tkt, 0);
+        CKL();
+        tke_update_kernel<R><<<(unsigned)((g.nin + 127) / 128), 128, 0, st>>>(g, tkeA, d_tke, d_tk2, in[3], in[0], in[1],
+                                                                              in[2], &d_sc->dt, d_tkt);
+        CKL();
+        tke_copy_kernel<R><<<nb, 256, 0, st>>>(g, d_tkt, d_tke);
+        CKL();
+        R* fe[1] = {d_tke};
+        int le[1] = {LOC_C};
+        return halo(fe, le, 1);
+    }
+    // the TKE closure's sgs_state / restore_sgs_state! (src/PrognosticSGS.jl:1174-1197): e on the interior
+    aeo_status tke_state(double* io, bool get) {
+        if (!io) { fail("sgs_state: NULL array"); return AEO_ERR_ARGUMENT; }
+        CK(cudaStreamSynchronize(st));
+        if (get) return get_padded(d_tke, io);
+        for (long long q = 0; q < g.nin; ++q)
+            if (!(io[q] >= 0) || !std::isfinite(io[q])) { fail("set_sgs_state: e must be finite and >= 0"); return AEO_ERR_ARGUMENT; }
+        if (aeo_status e = put_padded(d_tke, io)) return e;
+        R* f[1] = {d_tke};
+        int l[1] = {LOC_C};
+        if (aeo_status e = halo(f, l, 1)) return e;
+        CK(cudaStreamSynchronize(st));
+        return AEO_OK;
+    }
+    // an interior array (x fastest, FP64 on the host) to / from a padded device field
+    aeo_status put_padded(R* dst, const double* h) {
+        std::vector<R> tmp((size_t)g.nin);
+        for (size_t q = 0; q < tmp.size(); ++q) tmp[q] = R(h[q]);
+        CK(cudaMemcpyAsync(d_stage, tmp.data(), tmp.size() * sizeof(R), cudaMemcpyHostToDevice, st));
+        dim3 gb((g.nx + 127) / 128, g.ny, g.nz);
+        interior_to_padded_kernel<R><<<gb, 128, 0, st>>>(g, reinterpret_cast<const R*>(d_stage), dst, R(1));
+        CKL();
+        CK(cudaStreamSynchronize(st));
+        return AEO_OK;
+    }
+    aeo_status get_padded(const R* src, double* h) {
+        dim3 gb((g.nx + 127) / 128, g.ny, g.nz);
+        padded_to_interior_kernel<R><<<gb, 128, 0, st>>>(g, src, reinterpret_cast<R*>(d_stage));
+        CKL();
+        std::vector<R> tmp((size_t)g.nin);
+        CK(cudaMemcpyAsync(tmp.data(), d_stage, tmp.size() * sizeof(R), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (size_t q = 0; q < tmp.size(); ++q) h[q] = (double)tmp[q];
+        return AEO_OK;
+    }
     // g / theta0 of the AMD closure's buoyancy term (0 without buoyancy)
     R amd_bg() const { return R(amd() && cfg.theta0 != 0.0 ? cfg.g / cfg.theta0 : 0.0); }
     // the AMD closure on the sound-proof core takes its per-level buoyancy
@@ -619,6 +713,25 @@ struct Core : CoreBase {
                 if (aeo_status e = alloc(&d_cs2f, padded_count())) return e;
             dyn_d2 = std::pow(g.dx * g.dy * g.dz, 2.0 / 3.0);
         }
+        if (tke()) {
+            if (aeo_status e = alloc(&d_tke, padded_count())) return e;
+            if (aeo_status e = alloc(&d_tk2, padded_count())) return e;
+            if (aeo_status e = alloc(&d_tkt, padded_count())) return e;
+            if (aeo_status e = alloc(&d_tke_keep, padded_count())) return e;
+            if (aeo_status e = alloc(&pos_fx, (size_t)(g.nx + 1) * g.ny * g.nz)) return e;
+            if (aeo_status e = alloc(&pos_fy, (size_t)g.nx * (g.ny + 1) * g.nz)) return e;
+            if (aeo_status e = alloc(&pos_fz, (size_t)g.nx * g.ny * (g.nz + 1))) return e;
+            if (aeo_status e = alloc(&pos_r, (size_t)g.nin)) return e;
+            const bool buoy = cfg.theta0 > 0 && cfg.g > 0;
+            tkeA.ck = cfg.c_s; tkeA.ce0 = 0.19; tkeA.ce1 = 0.51; tkeA.cl = 0.76;
+            tkeA.delta = std::pow(g.dx * g.dy * g.dz, 1.0 / 3);
+            tkeA.bg = buoy ? cfg.g / cfg.theta0 : 0.0;
+            tkeA.pb1 = buoy ? cfg.g / cfg.theta0 * cfg.flux_bot / 2 : 0.0;
+            tkeA.pb2 = buoy ? cfg.g / cfg.theta0 * cfg.flux_top / 2 : 0.0;
+            tkeA.exact = 0;
+            g.tke = d_tke;
+            g.tke_ck = tkeA.ck; g.tke_cl = tkeA.cl; g.tke_delta = tkeA.delta; g.tke_bg = tkeA.bg;
+        }
         if (lag()) {
             for (int b = 0; b < 2; ++b)
                 for (int f = 0; f < 5; ++f)
@@ -657,7 +770,7 @@ struct Core : CoreBase {
             }
         }
         CK(cudaStreamSynchronize(st));
-        launches = 3 * (9 + dyn_launches()) + lag_launches();
+        launches = 3 * (9 + dyn_launches()) + lag_launches() + tke_launches();
         return AEO_OK;
     }
 
@@ -745,7 +858,7 @@ struct Core : CoreBase {
         if (!pcg) return launches;
         aeo_mg_stats o{};
         if (cudaStreamSynchronize(st) != cudaSuccess || aeo_mg_read_stats(mg, &o)) return 0;
-        return 3 * (4 + dyn_launches() + aeo_mg_launches_per_solve(mg, o.iterations)) + lag_launches();
+        return 3 * (4 + dyn_launches() + aeo_mg_launches_per_solve(mg, o.iterations)) + lag_launches() + tke_launches();
     }
 
     // the implicit IBM correction after every predictor (aeo_set_ibm)
@@ -759,7 +872,7 @@ struct Core : CoreBase {
         drop_graphs();   // the step graphs gain or lose the correction
         if (!mask) {
             ibm_mask = nullptr;
-            launches = 3 * (9 + dyn_launches()) + lag_launches();
+            launches = 3 * (9 + dyn_launches()) + lag_launches() + tke_launches();
             return AEO_OK;
         }
         std::vector<unsigned char> m((size_t)g.nin);
@@ -775,7 +888,7 @@ struct Core : CoreBase {
         CK(cudaStreamSynchronize(st));
         ibm_mask = ibm_alloc;
         ibm_tau = tau;
-        launches = 3 * (10 + dyn_launches()) + lag_launches();
+        launches = 3 * (10 + dyn_launches()) + lag_launches() + tke_launches();
         return AEO_OK;
     }
 
@@ -857,6 +970,17 @@ struct Core : CoreBase {
                         return;
                     }
                 }
+                if constexpr (SG && !AN && UN) {
+                    if (tke()) {
+                        SweepArgs<R> b = a;
+                        b.kofs = PS::KT_OFS;
+                        cudaFuncSetAttribute(sweep_pair_kernel<SG, AN, UN, 3>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PS::SMEM_AMD);
+                        sweep_pair_kernel<SG, AN, UN, 3><<<grid, dim3(PS::TXT, PS::TY), PS::SMEM_AMD, st>>>(
+                            tmaps[s_in], b, ntx, items, d_flag);
+                        return;
+                    }
+                }
                 if constexpr (SG && UN) {
                     if (dyncl()) {
                         cudaFuncSetAttribute(sweep_pair_kernel<SG, AN, UN, 2>,
@@ -890,6 +1014,17 @@ struct Core : CoreBase {
                 cudaFuncSetAttribute(sweep_tile_kernel<R, ADV, SG, AN, UN, 1>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS::SMEM_AMD);
                 sweep_tile_kernel<R, ADV, SG, AN, UN, 1><<<grid, dim3(TS::TX, TS::TY), TS::SMEM_AMD, st>>>(
+                    tmaps[s_in], b, kchunk, d_flag);
+                return;
+            }
+        }
+        if constexpr (SG && !AN && UN) {
+            if (tke()) {
+                SweepArgs<R> b = a;
+                b.kofs = TS::KT_OFS;
+                cudaFuncSetAttribute(sweep_tile_kernel<R, ADV, SG, AN, UN, 3>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS::SMEM_AMD);
+                sweep_tile_kernel<R, ADV, SG, AN, UN, 3><<<grid, dim3(TS::TX, TS::TY), TS::SMEM_AMD, st>>>(
                     tmaps[s_in], b, kchunk, d_flag);
                 return;
             }
@@ -1056,7 +1191,7 @@ struct Core : CoreBase {
         a.pr_t = R(cfg.pr_t);
         // the AMD closure brings its own kappa_t (the flux takes it unscaled)
         // and a buoyancy term with g / theta0
-        a.inv_prt = amd() ? R(1) : R(1.0 / cfg.pr_t);
+        a.inv_prt = own_kappa() ? R(1) : R(1.0 / cfg.pr_t);
         a.cs2 = d_cs2;
         a.cs2f = d_cs2f;
         a.dyn_d2 = dyn_d2;
@@ -1114,8 +1249,8 @@ struct Core : CoreBase {
 
     // the closure's once-per-step commit (advance_sgs!), after the projection
     aeo_status commit_sgs(int s_state) {
-        if (!lag()) return AEO_OK;
-        aeo_status e = enqueue_lag_commit(P[s_state]);
+        if (!lag() && !tke()) return AEO_OK;
+        aeo_status e = lag() ? enqueue_lag_commit(P[s_state]) : enqueue_tke_commit(P[s_state]);
         mark(AEO_K_SGS);
         return e;
     }
@@ -1337,6 +1472,7 @@ struct Core : CoreBase {
         for (int s = 0; s < n; ++s) {
             // the closure's memory as committed before the step: a retry starts from it
             if (lag()) CK(cudaMemcpyAsync(d_lag_state + 2, d_lag_state, 2 * sizeof(int), cudaMemcpyDeviceToDevice, st));
+            if (tke()) CK(cudaMemcpyAsync(d_tke_keep, d_tke, padded_count() * sizeof(R), cudaMemcpyDeviceToDevice, st));
             if (aeo_status e = launch_step(true)) return e;
             StepScalars h;
             if (aeo_status e = read_scalars(&h)) return e;
@@ -1361,6 +1497,7 @@ struct Core : CoreBase {
                     CK(cudaMemcpyAsync(d_lag_state, d_lag_state + 2, 2 * sizeof(int), cudaMemcpyDeviceToDevice, st));
                     if (aeo_status e = lag_refresh()) return e;
                 }
+                if (tke()) CK(cudaMemcpyAsync(d_tke, d_tke_keep, padded_count() * sizeof(R), cudaMemcpyDeviceToDevice, st));
                 if (retries >= c->max_retries) {
                     fail(std::string("step_adaptive: step failed (") + (!fin ? "nonfinite" : (dv > c->divergence_tol ? "divergence" : "velocity")) +
                          ") after " + std::to_string(retries) + " retries; the state is the one before the step");
@@ -1759,13 +1896,19 @@ static aeo_status validate(const aeo_config* c, const double* zf, const double* 
     if (c->c_s != 0.0 && !(c->pr_t > 0.0)) { *m = "pr_t must be positive with SGS"; return AEO_ERR_ARGUMENT; }
     if (c->sgs_model != AEO_SGS_SMAGORINSKY && c->sgs_model != AEO_SGS_VREMAN && c->sgs_model != AEO_SGS_SIGMA &&
         c->sgs_model != AEO_SGS_AMD && c->sgs_model != AEO_SGS_DYNAMIC && c->sgs_model != AEO_SGS_DYNAMIC_LOCAL &&
-        c->sgs_model != AEO_SGS_LAGRANGIAN) {
+        c->sgs_model != AEO_SGS_LAGRANGIAN && c->sgs_model != AEO_SGS_TKE) {
         *m = "unknown SGS closure";
         return AEO_ERR_ARGUMENT;
     }
     if (c->sgs_model != AEO_SGS_SMAGORINSKY && c->stretched) {
         *m = "the Vreman, sigma, AMD and dynamic closures take a uniform grid (src/operators/sgs_amd_vreman.jl:102-107, "
              ":280-284, src/operators/sigma_closure.jl:208-212, src/Operators.jl:555)";
+        return AEO_ERR_ARGUMENT;
+    }
+    if (c->sgs_model == AEO_SGS_TKE && c->c_s != 0.0 &&
+        (c->core != AEO_CORE_BOUSSINESQ || c->hx < 3 || c->hy < 3 || c->hz < 3)) {
+        *m = "the TKE closure runs on the Boussinesq core (theta0 its buoyancy reference) with host halos >= 3 "
+             "(the WENO-Z5 transport of e, src/PrognosticSGS.jl:354-356)";
         return AEO_ERR_ARGUMENT;
     }
     if ((c->sgs_model == AEO_SGS_DYNAMIC || c->sgs_model == AEO_SGS_DYNAMIC_LOCAL || c->sgs_model == AEO_SGS_LAGRANGIAN) &&
@@ -1931,6 +2074,11 @@ aeo_status aeo_set_sgs_buoyancy(aeo_sim* h, const double* bg) {
 aeo_status aeo_set_lagrangian(aeo_sim* h, double c0, double theta, double memory_time) {
     ENTER(h);
     return h->core->set_lagrangian(c0, theta, memory_time);
+}
+
+aeo_status aeo_set_tke(aeo_sim* h, double c_eps0, double c_eps1, double c_l, int32_t exact) {
+    ENTER(h);
+    return h->core->set_tke(c_eps0, c_eps1, c_l, exact);
 }
 
 aeo_status aeo_get_sgs_state(aeo_sim* h, double* out) {

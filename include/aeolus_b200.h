@@ -40,7 +40,7 @@ enum { AEO_ADV_CENTRED = 0, AEO_ADV_WENO_JS5 = 1, AEO_ADV_WENO_Z5 = 2 };
 enum { AEO_SOLVER_FFT = 0, AEO_SOLVER_COLUMN = 1, AEO_SOLVER_PCG = 2 };
 enum { AEO_PREC_FP64 = 0, AEO_PREC_FP32_MIXED = 1 };
 enum { AEO_SGS_SMAGORINSKY = 0, AEO_SGS_VREMAN = 1, AEO_SGS_SIGMA = 2, AEO_SGS_AMD = 3, AEO_SGS_DYNAMIC = 4,
-       AEO_SGS_DYNAMIC_LOCAL = 5, AEO_SGS_LAGRANGIAN = 6 };
+       AEO_SGS_DYNAMIC_LOCAL = 5, AEO_SGS_LAGRANGIAN = 6, AEO_SGS_TKE = 7 };
 enum { AEO_FIELD_U = 0, AEO_FIELD_V = 1, AEO_FIELD_W = 2, AEO_FIELD_THETA = 3,
        AEO_FIELD_P = 4, AEO_FIELD_NUT = 5 };
 
@@ -96,8 +96,11 @@ typedef struct {
                                   src/Operators.jl:873-880), or the
                                   Lagrangian dynamic closure with c_s =
                                   cs_max (LagrangianDynamicSmagorinsky,
-                                  aeo_set_lagrangian). Vreman, sigma, AMD,
-                                  dynamic and Lagrangian on uniform grids    */
+                                  aeo_set_lagrangian), or the prognostic-TKE
+                                  closure with c_s = c_k (0.1; TKEClosure,
+                                  aeo_set_tke; Boussinesq core, halos >= 3).
+                                  Vreman, sigma, AMD, dynamic, Lagrangian
+                                  and TKE on uniform grids                   */
 } aeo_config;
 
 typedef struct aeo_sim aeo_sim;
@@ -323,13 +326,27 @@ aeo_status aeo_set_sgs_buoyancy(aeo_sim* h, const double* bg);
  * domain with another closure. */
 aeo_status aeo_set_lagrangian(aeo_sim* h, double c0, double theta, double memory_time);
 
-/* sgs_state / restore_sgs_state! of the Lagrangian closure
- * (src/operators/lagrangian_sgs.jl:372-381): 5 Nx Ny Nz + 1 doubles -- the
- * committed I_LM, I_MM and the cell-centred u, v, w the memory was committed
- * with (interior arrays, x fastest), then the initialised flag (0 / 1).
- * Setting it recomputes the coefficient the next step uses.  AEO_ERR_STATE on
- * a domain whose closure keeps no memory. */
+/* sgs_state / restore_sgs_state! of the closures with a memory.  The
+ * Lagrangian closure (src/operators/lagrangian_sgs.jl:372-381): 5 Nx Ny Nz + 1
+ * doubles -- the committed I_LM, I_MM and the cell-centred u, v, w the memory
+ * was committed with (interior arrays, x fastest), then the initialised flag
+ * (0 / 1); setting it recomputes the coefficient the next step uses.  The TKE
+ * closure (src/PrognosticSGS.jl:1174-1197): e on the interior, Nx Ny Nz
+ * doubles >= 0 (its initial value; a new domain has e = 0, a fixed point of
+ * the TKE equation).  AEO_ERR_STATE on a domain whose closure keeps no
+ * memory. */
 aeo_status aeo_get_sgs_state(aeo_sim* h, double* out);
+
+/* The TKE closure (sgs_model = AEO_SGS_TKE; TKEClosure(mesh; c_k, c_eps0,
+ * c_eps1, c_l, dissipation), src/PrognosticSGS.jl:326-375, without a mask,
+ * wall cap, first-level factor or surface value; c_s is c_k): c_eps0 (0.19),
+ * c_eps1 (0.51), c_l (0.76) and the dissipation form (0 :semi_implicit, 1
+ * :exact).  e is committed once per step after the projection (advance_sgs!,
+ * :978-1002): WENO-Z5 flux-limited transport, div(2 nu_t grad e), the shear
+ * production of the discrete dual of the momentum operator, the buoyancy
+ * production (with (g/theta0) F / 2 of the surface heat fluxes in the wall
+ * levels) and the implicit sinks.  AEO_ERR_STATE on another closure. */
+aeo_status aeo_set_tke(aeo_sim* h, double c_eps0, double c_eps1, double c_l, int32_t exact);
 aeo_status aeo_set_sgs_state(aeo_sim* h, const double* in);
 
 /* The pressure solve of a domain created with solver = AEO_SOLVER_PCG:

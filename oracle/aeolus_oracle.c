@@ -85,6 +85,11 @@ struct oc_sim {
     double *lag_ilm, *lag_imm, *lag_up, *lag_vp, *lag_wp, *lag_cs2, *lag_nlm, *lag_nmm;
     int lag_init;
     double lag_c0, lag_theta, lag_mt;
+    /* the TKE closure: e, 2 nu_t and the transport tendency (storage
+     * arrays), the new e (interior), the coefficients */
+    double *tke_e, *tke_k2, *tke_tend, *tke_new;
+    double tke_ce0, tke_ce1, tke_cl;
+    int tke_exact;
 };
 
 #define ID(s, i, j, k) ((int64_t)(i) + (int64_t)(s)->NX * ((int64_t)(j) + (int64_t)(s)->NY * (int64_t)(k)))
@@ -896,6 +901,223 @@ static void lag_commit(oc_sim* s, double dt) {
     lag_coefficient(s);
 }
 
+/* --- Deardorff TKE closure (TKEClosure, src/PrognosticSGS.jl; Deardorff
+ * 1980, Moeng 1984): Boussinesq core, uniform grid, no mask / wall cap /
+ * first-level factor / surface value, dry N^2. --------------------------- */
+static void tke_alloc(oc_sim* s) {
+    if (s->tke_e) return;
+    s->tke_e = dalloc(s->n); s->tke_k2 = dalloc(s->n); s->tke_tend = dalloc(s->n);
+    s->tke_new = dalloc((int64_t)s->p.nx * s->p.ny * s->p.nz);
+    s->tke_ce0 = 0.19; s->tke_ce1 = 0.51; s->tke_cl = 0.76; s->tke_exact = 0;
+}
+
+/* N^2 of cell (i, j, k): (g/theta0) (theta_face_above - theta_face_below) / dz
+ * with the faces the two-cell means (buoyancy_frequency_squared!,
+ * src/operators/stratification.jl:124-135; TurbulenceStability.jl:129-130) */
+static inline double tke_n2(const oc_sim* s, int i, int j, int k) {
+    const oc_params* P = &s->p;
+    if (!(P->theta0 > 0 && P->g > 0)) return 0.0;
+    const double* th = s->th;
+    double below = 0.5 * (A(th, i, j, k - 1) + A(th, i, j, k)), above = 0.5 * (A(th, i, j, k) + A(th, i, j, k + 1));
+    return (P->g / P->theta0) * (above - below) * (1 / s->dz);
+}
+
+/* tke_length_scale (src/PrognosticSGS.jl:93-110): l and s = sqrt(e) / l */
+static inline void tke_length(const oc_sim* s, double e, double N2, double* l, double* sr) {
+    double Delta = pow(s->dx * s->dy * s->dz, 1.0 / 3), cl = s->tke_cl;
+    double sq = sqrt(fmax(e, 0.0)), lmax = Delta;
+    int stable = N2 > 0;
+    double N = sqrt(fmax(N2, 0.0));
+    *l = stable ? fmin(lmax, cl * sq / N) : lmax;
+    *sr = stable ? fmax(sq / lmax, N / cl) : sq / lmax;
+}
+
+/* nu_t = c_k l sqrt(e), kappa_t = (1 + 2 l / Delta) nu_t of the committed e and
+ * the current N^2 (_coefficients_body! / tke_eddy_coefficients, :432-454, :135-139) */
+static void tke_at(const oc_sim* s, int i, int j, int k, double* nu, double* ka) {
+    double Delta = pow(s->dx * s->dy * s->dz, 1.0 / 3);
+    double e = A(s->tke_e, i, j, k), l, sr;
+    tke_length(s, e, tke_n2(s, i, j, k), &l, &sr);
+    double v = s->p.c_s * l * sqrt(fmax(e, 0.0));
+    *nu = v;
+    *ka = (1 + 2 * l / Delta) * v;
+}
+
+/* The share of D destined for storage cell (I, J, K) from the velocity points
+ * around it (_dual_raw, src/PrognosticSGS.jl:589-632, with the flux shares
+ * :541-560 on a RegularGrid): each flux nu dq / h of the momentum operator
+ * gives -u_p (+-flux) / h to the cells of its nu.  Points outside the
+ * interior box give nothing. */
+static double dual_raw(const oc_sim* s, int I, int J, int K) {
+    const oc_params* P = &s->p;
+    const double *u = s->u, *v = s->v, *w = s->w;
+    const double ix2 = 1 / (s->dx * s->dx), iy2 = 1 / (s->dy * s->dy), iz2 = 1 / (s->dz * s->dz);
+    int i1 = P->hx, i2 = P->hx + P->nx - 1, j1 = P->hy, j2 = P->hy + P->ny - 1, k1 = P->hz, k2 = P->hz + P->nz - 1;
+#define IN(i, j, k) ((i) >= i1 && (i) <= i2 && (j) >= j1 && (j) <= j2 && (k) >= k1 && (k) <= k2)
+#define UX_E(i, j, k) (IN(i, j, k) ? -A(u, i, j, k) * (A(u, i + 1, j, k) - A(u, i, j, k)) * ix2 : 0.0)
+#define UX_W(i, j, k) (IN(i, j, k) ? A(u, i, j, k) * (A(u, i, j, k) - A(u, i - 1, j, k)) * ix2 : 0.0)
+#define UY_N(i, j, k) (IN(i, j, k) ? 0.25 * (-A(u, i, j, k) * (A(u, i, j + 1, k) - A(u, i, j, k)) * iy2) : 0.0)
+#define UY_S(i, j, k) (IN(i, j, k) ? 0.25 * (A(u, i, j, k) * (A(u, i, j, k) - A(u, i, j - 1, k)) * iy2) : 0.0)
+#define UZ_T(i, j, k) (IN(i, j, k) ? 0.25 * (-A(u, i, j, k) * (A(u, i, j, k + 1) - A(u, i, j, k)) * iz2) : 0.0)
+#define UZ_B(i, j, k) (IN(i, j, k) ? 0.25 * (A(u, i, j, k) * (A(u, i, j, k) - A(u, i, j, k - 1)) * iz2) : 0.0)
+#define VY_N(i, j, k) (IN(i, j, k) ? -A(v, i, j, k) * (A(v, i, j + 1, k) - A(v, i, j, k)) * iy2 : 0.0)
+#define VY_S(i, j, k) (IN(i, j, k) ? A(v, i, j, k) * (A(v, i, j, k) - A(v, i, j - 1, k)) * iy2 : 0.0)
+#define VX_E(i, j, k) (IN(i, j, k) ? 0.25 * (-A(v, i, j, k) * (A(v, i + 1, j, k) - A(v, i, j, k)) * ix2) : 0.0)
+#define VX_W(i, j, k) (IN(i, j, k) ? 0.25 * (A(v, i, j, k) * (A(v, i, j, k) - A(v, i - 1, j, k)) * ix2) : 0.0)
+#define VZ_T(i, j, k) (IN(i, j, k) ? 0.25 * (-A(v, i, j, k) * (A(v, i, j, k + 1) - A(v, i, j, k)) * iz2) : 0.0)
+#define VZ_B(i, j, k) (IN(i, j, k) ? 0.25 * (A(v, i, j, k) * (A(v, i, j, k) - A(v, i, j, k - 1)) * iz2) : 0.0)
+#define WZ_T(i, j, k) (IN(i, j, k) ? -A(w, i, j, k) * (A(w, i, j, k + 1) - A(w, i, j, k)) * iz2 : 0.0)
+#define WZ_B(i, j, k) (IN(i, j, k) ? A(w, i, j, k) * (A(w, i, j, k) - A(w, i, j, k - 1)) * iz2 : 0.0)
+#define WX_E(i, j, k) (IN(i, j, k) ? 0.25 * (-A(w, i, j, k) * (A(w, i + 1, j, k) - A(w, i, j, k)) * ix2) : 0.0)
+#define WX_W(i, j, k) (IN(i, j, k) ? 0.25 * (A(w, i, j, k) * (A(w, i, j, k) - A(w, i - 1, j, k)) * ix2) : 0.0)
+#define WY_N(i, j, k) (IN(i, j, k) ? 0.25 * (-A(w, i, j, k) * (A(w, i, j + 1, k) - A(w, i, j, k)) * iy2) : 0.0)
+#define WY_S(i, j, k) (IN(i, j, k) ? 0.25 * (A(w, i, j, k) * (A(w, i, j, k) - A(w, i, j - 1, k)) * iy2) : 0.0)
+    double d = UX_E(I, J, K) + UX_W(I + 1, J, K);
+    d += (UY_N(I + 1, J, K) + UY_N(I, J, K)) + (UY_N(I + 1, J - 1, K) + UY_N(I, J - 1, K));
+    d += (UY_S(I + 1, J + 1, K) + UY_S(I, J + 1, K)) + (UY_S(I + 1, J, K) + UY_S(I, J, K));
+    d += (UZ_T(I + 1, J, K) + UZ_T(I, J, K)) + (UZ_T(I + 1, J, K - 1) + UZ_T(I, J, K - 1));
+    d += (UZ_B(I + 1, J, K + 1) + UZ_B(I, J, K + 1)) + (UZ_B(I + 1, J, K) + UZ_B(I, J, K));
+    d += VY_N(I, J, K) + VY_S(I, J + 1, K);
+    d += (VX_E(I, J + 1, K) + VX_E(I - 1, J + 1, K)) + (VX_E(I, J, K) + VX_E(I - 1, J, K));
+    d += (VX_W(I + 1, J + 1, K) + VX_W(I, J + 1, K)) + (VX_W(I + 1, J, K) + VX_W(I, J, K));
+    d += (VZ_T(I, J + 1, K) + VZ_T(I, J, K)) + (VZ_T(I, J + 1, K - 1) + VZ_T(I, J, K - 1));
+    d += (VZ_B(I, J + 1, K + 1) + VZ_B(I, J, K + 1)) + (VZ_B(I, J + 1, K) + VZ_B(I, J, K));
+    d += WZ_T(I, J, K) + WZ_B(I, J, K + 1);
+    d += (WX_E(I, J, K + 1) + WX_E(I - 1, J, K + 1)) + (WX_E(I, J, K) + WX_E(I - 1, J, K));
+    d += (WX_W(I + 1, J, K + 1) + WX_W(I, J, K + 1)) + (WX_W(I + 1, J, K) + WX_W(I, J, K));
+    d += (WY_N(I, J, K + 1) + WY_N(I, J - 1, K + 1)) + (WY_N(I, J, K) + WY_N(I, J - 1, K));
+    d += (WY_S(I, J + 1, K + 1) + WY_S(I, J, K + 1)) + (WY_S(I, J + 1, K) + WY_S(I, J, K));
+#undef IN
+#undef UX_E
+#undef UX_W
+#undef UY_N
+#undef UY_S
+#undef UZ_T
+#undef UZ_B
+#undef VY_N
+#undef VY_S
+#undef VX_E
+#undef VX_W
+#undef VZ_T
+#undef VZ_B
+#undef WZ_T
+#undef WZ_B
+#undef WX_E
+#undef WX_W
+#undef WY_N
+#undef WY_S
+    return d;
+}
+
+/* _fold_src (src/PrognosticSGS.jl:639-640): source n (1 itself, 2 the low halo
+ * layer, 3 the high one) of storage index I along a direction whose low /
+ * high halo layers H, H+N+1 are copies of lo / hi; -1 = none */
+static inline int fold_src(int I, int H, int N, int lo, int hi, int n) {
+    return n == 1 ? I : (n == 2 ? (lo == I ? H - 1 : -1) : (hi == I ? H + N : -1));
+}
+
+/* D of interior storage cell (I, J, K) (dual_strain!, _dual_strain_body!,
+ * :642-665): the shares of every source the halo fold assigns to it.  The
+ * halo images: periodic (H+N-1, H), a wall mirror (H, H+N-1) (0-based). */
+static double dual_strain(const oc_sim* s, int I, int J, int K) {
+    const oc_params* P = &s->p;
+    int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
+    int lox = Hx + Nx - 1, hix = Hx, loy = Hy + Ny - 1, hiy = Hy;
+    int pz = P->bc_z == OC_BC_PERIODIC;
+    int loz = pz ? Hz + Nz - 1 : Hz, hiz = pz ? Hz : Hz + Nz - 1;
+    double acc = 0.0;
+    for (int nz = 1; nz <= 3; ++nz) {
+        int sz = fold_src(K, Hz, Nz, loz, hiz, nz);
+        if (sz < 0) continue;
+        for (int ny = 1; ny <= 3; ++ny) {
+            int sy = fold_src(J, Hy, Ny, loy, hiy, ny);
+            if (sy < 0) continue;
+            for (int nx = 1; nx <= 3; ++nx) {
+                int sx = fold_src(I, Hx, Nx, lox, hix, nx);
+                if (sx < 0) continue;
+                acc += dual_raw(s, sx, sy, sz);
+            }
+        }
+    }
+    return acc;
+}
+
+/* advance_sgs! of the TKE closure (src/PrognosticSGS.jl:978-1002) over an
+ * accepted step: the coefficients of e^n and the new N^2, K = 2 nu_t with
+ * filled halos, D, the flux-limited WENO-Z5 transport of e
+ * (advect_positive!, accumulate = false) plus div(2 nu_t grad e), then the
+ * update of every cell (_tke_update_body, :1077-1145): e* = e + dt (T + P_s
+ * + max(P_b, 0)), clipped at 0, and the sinks (dissipation c_eps s e, the
+ * buoyant destruction) linearised implicit, or with the exact dissipation
+ * step (e*^(-1/2) + c_eps dt / (2 l))^(-2).  A prescribed surface heat flux
+ * adds (g/theta0) F / 2 to the first / last level (_surface_buoyancy). */
+static void tke_commit(oc_sim* s, double dt) {
+    const oc_params* P = &s->p;
+    int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
+    fill_halos(s, s->u, LOC_FX);
+    fill_halos(s, s->v, LOC_FY);
+    fill_halos(s, s->w, LOC_FZ);
+    fill_halos(s, s->th, LOC_C);
+    double Delta = pow(s->dx * s->dy * s->dz, 1.0 / 3);
+    for (int k = Hz; k < Hz + Nz; ++k)
+        for (int j = Hy; j < Hy + Ny; ++j)
+            for (int i = Hx; i < Hx + Nx; ++i) {
+                double nu, ka;
+                tke_at(s, i, j, k, &nu, &ka);
+                A(s->tke_k2, i, j, k) = 2 * nu;
+            }
+    fill_halos(s, s->tke_k2, LOC_C);
+    fill_halos(s, s->tke_e, LOC_C);
+    oc_advect_positive(s, s->u, s->v, s->w, s->tke_e, s->tke_tend, dt, OC_ADV_WENO_Z5, 0);
+    int buoy = P->theta0 > 0 && P->g > 0;
+    double pb1 = buoy ? P->g / P->theta0 * P->flux_bot / 2 : 0.0, pb2 = buoy ? P->g / P->theta0 * P->flux_top / 2 : 0.0;
+    const double* e0 = s->tke_e;
+    const double* K2 = s->tke_k2;
+    const double ck = P->c_s, tiny = 2.2250738585072014e-308;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = Hz; k < Hz + Nz; ++k)
+        for (int j = Hy; j < Hy + Ny; ++j)
+            for (int i = Hx; i < Hx + Nx; ++i) {
+                /* the diffusion of e with K = 2 nu_t (_b_eddy_scalar!, src/FiniteVolume.jl:1280-1300) */
+                double nE = 0.5 * (A(K2, i, j, k) + A(K2, i + 1, j, k)), nW = 0.5 * (A(K2, i - 1, j, k) + A(K2, i, j, k));
+                double nN = 0.5 * (A(K2, i, j, k) + A(K2, i, j + 1, k)), nS = 0.5 * (A(K2, i, j - 1, k) + A(K2, i, j, k));
+                double nT = 0.5 * (A(K2, i, j, k) + A(K2, i, j, k + 1)), nB = 0.5 * (A(K2, i, j, k - 1) + A(K2, i, j, k));
+                double fxE = nE * (A(e0, i + 1, j, k) - A(e0, i, j, k)) * s->idx;
+                double fxW = nW * (A(e0, i, j, k) - A(e0, i - 1, j, k)) * s->idx;
+                double fyN = nN * (A(e0, i, j + 1, k) - A(e0, i, j, k)) * s->idy;
+                double fyS = nS * (A(e0, i, j, k) - A(e0, i, j - 1, k)) * s->idy;
+                double fzT = nT * (A(e0, i, j, k + 1) - A(e0, i, j, k)) * s->idz;
+                double fzB = nB * (A(e0, i, j, k) - A(e0, i, j, k - 1)) * s->idz;
+                double tr = A(s->tke_tend, i, j, k) +
+                            1.0 * ((fxE - fxW) * s->idx + (fyN - fyS) * s->idy + (fzT - fzB) * s->idz);
+                double e = A(e0, i, j, k), N2 = tke_n2(s, i, j, k), l, sr;
+                tke_length(s, e, N2, &l, &sr);
+                double ce = (s->tke_ce0 + s->tke_ce1 * l / Delta) * 1.0;
+                double nu = A(K2, i, j, k) / 2;
+                double Ps = nu * dual_strain(s, i, j, k) + 0.0;
+                double kv = (1 + 2 * l / Delta) * nu;
+                int kk = k - Hz + 1;
+                double Psf = (kk == 1 ? pb1 : 0.0) + (kk == Nz ? pb2 : 0.0);
+                double src = Ps + (N2 < 0 ? -kv * N2 : 0.0) + fmax(Psf, 0.0);
+                double rb = ((N2 > 0) && (sr > 0) ? (1 + 2 * l / Delta) * ck * N2 / sr : 0.0) +
+                            (Psf < 0 ? -Psf / fmax(e, tiny) : 0.0);
+                double es = e + dt * (tr + src);
+                if (es < 0) es = 0.0;
+                double R = ce * sr + rb;
+                double en = es / (1 + dt * R);
+                if (s->tke_exact && l > 0 && es > 0) {
+                    double a = 1 / (1 / sqrt(es) + ce * dt / (2 * l));
+                    en = (a * a) / (1 + dt * rb);
+                }
+                s->tke_new[(size_t)(i - Hx) + (size_t)Nx * ((size_t)(j - Hy) + (size_t)Ny * (k - Hz))] = en;
+            }
+    for (int k = Hz; k < Hz + Nz; ++k)
+        for (int j = Hy; j < Hy + Ny; ++j)
+            for (int i = Hx; i < Hx + Nx; ++i)
+                A(s->tke_e, i, j, k) = s->tke_new[(size_t)(i - Hx) + (size_t)Nx * ((size_t)(j - Hy) + (size_t)Ny * (k - Hz))];
+    fill_halos(s, s->tke_e, LOC_C);
+}
+
 /* --- Smagorinsky (src/FiniteVolume.jl:936-944, src/Operators.jl:451-496) -- */
 static inline double smag_at(const oc_sim* s, int i, int j, int k) {
     const double *u = s->u, *v = s->v, *w = s->w;
@@ -1010,7 +1232,7 @@ static inline double eddy_scalar(const oc_sim* s, const double* d, int i, int j,
     if (!s->wc) {
         /* the AMD closure: its own kappa_t, unscaled (AMDClosure,
          * src/operators/sgs_amd_vreman.jl:325-354) */
-        const int amd = s->p.sgs_model == OC_SGS_AMD;
+        const int amd = s->p.sgs_model == OC_SGS_AMD || s->p.sgs_model == OC_SGS_TKE;
         const double* H = amd ? s->kt : s->nut;
         double sc = amd ? 1.0 : 1 / s->p.pr_t;
         double nE = 0.5 * (A(H, i, j, k) + A(H, i + 1, j, k));
@@ -1069,11 +1291,12 @@ static void compute_tendencies(oc_sim* s) {
             for (int j = Hy; j < Hy + Ny; ++j)
                 for (int i = Hx; i < Hx + Nx; ++i) {
                     if (P->sgs_model == OC_SGS_AMD) amd_at(s, i, j, k, &A(s->nut, i, j, k), &A(s->kt, i, j, k));
+                    else if (P->sgs_model == OC_SGS_TKE) tke_at(s, i, j, k, &A(s->nut, i, j, k), &A(s->kt, i, j, k));
                     else A(s->nut, i, j, k) = smag_at(s, i, j, k);
                 }
         fill_halos(s, s->nut, LOC_C);
-        if (P->sgs_model == OC_SGS_AMD) fill_halos(s, s->kt, LOC_C);
-        if (anel && P->sgs_model != OC_SGS_AMD)   /* the AMD closure keeps its own kappa_t */
+        if (P->sgs_model == OC_SGS_AMD || P->sgs_model == OC_SGS_TKE) fill_halos(s, s->kt, LOC_C);
+        if (anel && P->sgs_model != OC_SGS_AMD && P->sgs_model != OC_SGS_TKE)   /* AMD and TKE keep their own kappa_t */
             for (int64_t q = 0; q < s->n; ++q) s->kt[q] = s->nut[q] / P->pr_t;
     }
 
@@ -1597,6 +1820,7 @@ int oc_step_euler(oc_sim* s, double dt, int nsteps) {
     for (int n = 0; n < nsteps; ++n) {
         substage(s, dt, 0, 0.0, 0.0);
         if (s->p.c_s != 0 && s->p.sgs_model == OC_SGS_LAGRANGIAN) lag_commit(s, dt);   /* once per step */
+        if (s->p.c_s != 0 && s->p.sgs_model == OC_SGS_TKE) tke_commit(s, dt);
     }
     return 0;
 }
@@ -1615,6 +1839,7 @@ double oc_adaptive_dt(oc_sim* s, const oc_cfl* c, double dt_prev, int* limiter) 
     fill_halos(s, s->v, LOC_FY);
     fill_halos(s, s->w, LOC_FZ);
     if (P->c_s != 0 && (P->sgs_model == OC_SGS_DYNAMIC || P->sgs_model == OC_SGS_DYNAMIC_LOCAL)) dyn_coefficients(s);
+    if (P->c_s != 0 && P->sgs_model == OC_SGS_TKE) fill_halos(s, s->th, LOC_C);
     double rate = 0.0, nutm = 0.0, ktm = 0.0;
     int nanr = 0;
     double* mean = (double*)calloc((size_t)Nz, sizeof(double));
@@ -1631,6 +1856,7 @@ double oc_adaptive_dt(oc_sim* s, const oc_cfl* c, double dt_prev, int* limiter) 
                 if (P->c_s != 0) {
                     double n, kk = 0.0;
                     if (P->sgs_model == OC_SGS_AMD) amd_at(s, i, j, k, &n, &kk);
+                    else if (P->sgs_model == OC_SGS_TKE) tke_at(s, i, j, k, &n, &kk);
                     else n = smag_at(s, i, j, k);
                     if (n > nutm) nutm = n;
                     if (kk > ktm) ktm = kk;
@@ -1648,7 +1874,8 @@ double oc_adaptive_dt(oc_sim* s, const oc_cfl* c, double dt_prev, int* limiter) 
     double nu_total = P->nu + nutm;
     double dt_diff = nu_total > 0 ? c->c_diff * harm / nu_total : INF;
     /* max(nu_t, kappa_t), kappa_t the AMD closure's own (src/TimeIntegration.jl:322-335) */
-    double ksgs = fmax(nutm, P->c_s != 0 ? (P->sgs_model == OC_SGS_AMD ? ktm : nutm / P->pr_t) : 0.0);
+    double ksgs = fmax(nutm, P->c_s != 0 ? ((P->sgs_model == OC_SGS_AMD || P->sgs_model == OC_SGS_TKE) ? ktm : nutm / P->pr_t)
+                                         : 0.0);
     double dt_sgs = ksgs > 0 ? c->c_diff * harm / ksgs : INF;
     int buoy = anel ? (P->g != 0) : (P->theta0 != 0);
     double n2max = 0.0;
@@ -1693,6 +1920,7 @@ int oc_step_rk3(oc_sim* s, double dt, int nsteps) {
         substage(s, dt, 1, 0.75, 0.25);
         substage(s, dt, 1, inv3, two3);
         if (s->p.c_s != 0 && s->p.sgs_model == OC_SGS_LAGRANGIAN) lag_commit(s, dt);   /* once per step */
+        if (s->p.c_s != 0 && s->p.sgs_model == OC_SGS_TKE) tke_commit(s, dt);
     }
     return 0;
 }
@@ -1899,8 +2127,12 @@ oc_sim* oc_create(const oc_params* p, const double* zfi, const double* wc, const
     if (p->solver == OC_SOLVER_COLUMN && p->bc_z != OC_BC_WALL) return NULL;
     if (p->stretched && (!zfi || p->bc_z != OC_BC_WALL)) return NULL;
     if ((p->sgs_model == OC_SGS_VREMAN || p->sgs_model == OC_SGS_SIGMA || p->sgs_model == OC_SGS_AMD ||
-         p->sgs_model == OC_SGS_DYNAMIC || p->sgs_model == OC_SGS_DYNAMIC_LOCAL || p->sgs_model == OC_SGS_LAGRANGIAN) &&
+         p->sgs_model == OC_SGS_DYNAMIC || p->sgs_model == OC_SGS_DYNAMIC_LOCAL || p->sgs_model == OC_SGS_LAGRANGIAN ||
+         p->sgs_model == OC_SGS_TKE) &&
         p->stretched)
+        return NULL;
+    /* the TKE closure: the Boussinesq core (theta0 its buoyancy reference), WENO-Z5 transport of e (halos >= 3) */
+    if (p->c_s != 0 && p->sgs_model == OC_SGS_TKE && (p->core != OC_CORE_BOUSSINESQ || p->hx < 3 || p->hy < 3 || p->hz < 3))
         return NULL;
     oc_sim* s = (oc_sim*)calloc(1, sizeof(oc_sim));
     s->p = *p;
@@ -2017,6 +2249,7 @@ oc_sim* oc_create(const oc_params* p, const double* zfi, const double* wc, const
         for (int k = 0; k < Nz; ++k) { s->meas_sum += s->meas[k]; s->gauge_sum += s->gauge[k]; }
     }
     if (p->c_s != 0 && p->sgs_model == OC_SGS_LAGRANGIAN) lag_alloc(s);
+    if (p->c_s != 0 && p->sgs_model == OC_SGS_TKE) tke_alloc(s);
     if (p->solver == OC_SOLVER_PCG) {
         s->cgx = dalloc((int64_t)Nx * Ny * Nz);
         if (oc_set_apertures(s, NULL, NULL, NULL, 1e-8, 200)) {
@@ -2035,9 +2268,24 @@ int oc_set_lagrangian(oc_sim* s, double c0, double theta, double memory_time) {
     return 0;
 }
 
+int oc_set_tke(oc_sim* s, double c_eps0, double c_eps1, double c_l, int exact) {
+    if (s->p.sgs_model != OC_SGS_TKE || s->p.c_s == 0 || !(c_eps0 >= 0) || !(c_eps1 >= 0) || !(c_l > 0)) return -1;
+    tke_alloc(s);
+    s->tke_ce0 = c_eps0; s->tke_ce1 = c_eps1; s->tke_cl = c_l; s->tke_exact = exact != 0;
+    return 0;
+}
+
 int oc_get_sgs_state(const oc_sim* s, double* out) {
-    if (s->p.sgs_model != OC_SGS_LAGRANGIAN || !out) return -1;
     size_t ni = (size_t)s->p.nx * s->p.ny * s->p.nz;
+    if (s->p.sgs_model == OC_SGS_TKE && s->tke_e && out) {
+        const oc_params* P = &s->p;
+        for (int k = 0; k < P->nz; ++k)
+            for (int j = 0; j < P->ny; ++j)
+                for (int i = 0; i < P->nx; ++i)
+                    out[(size_t)i + (size_t)P->nx * ((size_t)j + (size_t)P->ny * k)] = A(s->tke_e, i + P->hx, j + P->hy, k + P->hz);
+        return 0;
+    }
+    if (s->p.sgs_model != OC_SGS_LAGRANGIAN || !out) return -1;
     const double* a[5] = {s->lag_ilm, s->lag_imm, s->lag_up, s->lag_vp, s->lag_wp};
     for (int f = 0; f < 5; ++f)
         for (size_t q = 0; q < ni; ++q) out[f * ni + q] = a[f] ? a[f][q] : 0.0;
@@ -2046,6 +2294,15 @@ int oc_get_sgs_state(const oc_sim* s, double* out) {
 }
 
 int oc_set_sgs_state(oc_sim* s, const double* in) {
+    if (s->p.sgs_model == OC_SGS_TKE && s->tke_e && in) {
+        const oc_params* P = &s->p;
+        for (int k = 0; k < P->nz; ++k)
+            for (int j = 0; j < P->ny; ++j)
+                for (int i = 0; i < P->nx; ++i)
+                    A(s->tke_e, i + P->hx, j + P->hy, k + P->hz) = in[(size_t)i + (size_t)P->nx * ((size_t)j + (size_t)P->ny * k)];
+        fill_halos(s, s->tke_e, LOC_C);
+        return 0;
+    }
     if (s->p.sgs_model != OC_SGS_LAGRANGIAN || !in) return -1;
     lag_alloc(s);
     size_t ni = (size_t)s->p.nx * s->p.ny * s->p.nz;
@@ -2146,6 +2403,7 @@ void oc_destroy(oc_sim* s) {
     free(s->dyn_lm); free(s->dyn_mm); free(s->cs2); free(s->amd_bg);
     free(s->lag_ilm); free(s->lag_imm); free(s->lag_up); free(s->lag_vp); free(s->lag_wp);
     free(s->lag_cs2); free(s->lag_nlm); free(s->lag_nmm);
+    free(s->tke_e); free(s->tke_k2); free(s->tke_tend); free(s->tke_new);
     if (s->cg) ocg_destroy(s->cg);
     plan_free(&s->px); plan_free(&s->py); plan_free(&s->pz);
     free(s);

@@ -28,7 +28,8 @@ enum { OC_SOLVER_FFT = 0, OC_SOLVER_COLUMN = 1, OC_SOLVER_PCG = 2 };
 enum { OC_U = 0, OC_V = 1, OC_W = 2, OC_THETA = 3, OC_P = 4, OC_NUT = 5, OC_PHI = 6, OC_KT = 7 };
 enum { OC_SGS_SMAGORINSKY = 0, OC_SGS_VREMAN = 1, OC_SGS_SIGMA = 2, OC_SGS_AMD = 3, OC_SGS_DYNAMIC = 4,
        OC_SGS_DYNAMIC_LOCAL = 5,     /* 5: averaging = :local, src/Operators.jl:873-880 */
-       OC_SGS_LAGRANGIAN = 6 };      /* 6: LagrangianDynamicSmagorinsky, src/operators/lagrangian_sgs.jl */
+       OC_SGS_LAGRANGIAN = 6,        /* 6: LagrangianDynamicSmagorinsky, src/operators/lagrangian_sgs.jl */
+       OC_SGS_TKE = 7 };             /* 7: TKEClosure (Deardorff 1980), src/PrognosticSGS.jl; c_s is c_k */
 
 typedef struct {
     int32_t nx, ny, nz, hx, hy, hz;
@@ -93,6 +94,10 @@ int oc_set_lagrangian(oc_sim* s, double c0, double theta, double memory_time);
  * I_MM and the cell-centred u, v, w of the memory (x fastest), then the
  * initialised flag (0 / 1).  0 on success. */
 int oc_get_sgs_state(const oc_sim* s, double* out);
+/* the TKE closure's c_eps0 (0.19), c_eps1 (0.51), c_l (0.76) and dissipation
+ * form (0 :semi_implicit, 1 :exact), src/PrognosticSGS.jl:326-375; its
+ * sgs_state is e on the interior (Nx Ny Nz values, x fastest) */
+int oc_set_tke(oc_sim* s, double c_eps0, double c_eps1, double c_l, int exact);
 int oc_set_sgs_state(oc_sim* s, const double* in);
 /* the implicit IBM correction after every predictor (implicit_ibm_correction!,
  * src/IBM.jl:295-300): mask storage-shaped, nonzero = solid (interior cells

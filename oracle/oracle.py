@@ -87,6 +87,7 @@ def load():
     lib.oc_set_apertures.argtypes = [P, _D, _D, _D, C.c_double, C.c_int]
     lib.oc_set_sgs_buoyancy.argtypes = [P, _D]
     lib.oc_set_lagrangian.argtypes = [P, C.c_double, C.c_double, C.c_double]
+    lib.oc_set_tke.argtypes = [P, C.c_double, C.c_double, C.c_double, C.c_int]
     lib.oc_get_sgs_state.argtypes = [P, _D]
     lib.oc_set_sgs_state.argtypes = [P, _D]
     lib.oc_pcg_stats.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double),
@@ -148,7 +149,7 @@ class OracleSimulation:
         p.c_s, p.pr_t = spec.c_s, spec.pr_t
         p.flux_bot, p.flux_top = spec.flux_bot, spec.flux_top
         p.sponge_alpha, p.sponge_zstart = spec.sponge_alpha, spec.sponge_zstart
-        p.sgs_model = {"smagorinsky": 0, "vreman": 1, "sigma": 2, "amd": 3, "dynamic": 4, "lagrangian": 6}[spec.sgs]
+        p.sgs_model = {"smagorinsky": 0, "vreman": 1, "sigma": 2, "amd": 3, "dynamic": 4, "lagrangian": 6, "tke": 7}[spec.sgs]
         if spec.sgs == "dynamic" and getattr(spec, "averaging", "plane") == "local":
             p.sgs_model = 5
         self._keep = [g.zf, spec.wc, spec.wf, spec.thf]
@@ -166,17 +167,31 @@ class OracleSimulation:
             mt = spec.lag_memory_time
             assert self._lib.oc_set_lagrangian(self._h, spec.lag_c0, spec.lag_theta, 0.0 if mt is None else mt) == 0
 
+        if spec.sgs == "tke" and spec.c_s != 0:
+            assert self._lib.oc_set_tke(self._h, spec.tke_c_eps0, spec.tke_c_eps1, spec.tke_c_l,
+                                        1 if spec.tke_dissipation == "exact" else 0) == 0
+            if spec.tke_e0:
+                self.set_sgs_state(np.full((g.nz, g.ny, g.nx), float(spec.tke_e0)))
+
     def sgs_state(self):
         """The Lagrangian closure's memory: (I_LM, I_MM, U, V, W) as (nz, ny, nx)
-        arrays and the initialised flag."""
+        arrays and the initialised flag; the TKE closure's: e (nz, ny, nx)."""
         g = self.grid
         n = g.nx * g.ny * g.nz
+        if self.spec.sgs == "tke":
+            out = np.empty(n)
+            assert self._lib.oc_get_sgs_state(self._h, _p(out)) == 0
+            return out.reshape(g.nz, g.ny, g.nx)
         out = np.empty(5 * n + 1)
         assert self._lib.oc_get_sgs_state(self._h, _p(out)) == 0
         arrs = tuple(out[f * n:(f + 1) * n].reshape(g.nz, g.ny, g.nx).copy() for f in range(5))
         return arrs + (bool(out[5 * n]),)
 
     def set_sgs_state(self, state):
+        if self.spec.sgs == "tke":
+            a = np.ascontiguousarray(state, dtype=np.float64).ravel()
+            assert self._lib.oc_set_sgs_state(self._h, _p(a)) == 0
+            return
         a = np.concatenate([np.ascontiguousarray(x, dtype=np.float64).ravel() for x in state[:5]] +
                            [np.array([1.0 if state[5] else 0.0])])
         assert self._lib.oc_set_sgs_state(self._h, _p(a)) == 0

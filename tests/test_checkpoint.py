@@ -20,9 +20,9 @@ from aeolus_b200.checkpoint import (FIELDS, checkpoint, checkpoint_payload, read
 from oracle.oracle import OracleSimulation
 
 
-def spec(n=16, c_s=0.17, advection="weno_js5", sgs="smagorinsky"):
+def spec(n=16, c_s=0.17, advection="weno_js5", sgs="smagorinsky", **kw):
     g = regular_grid((n, n, n), (1.0, 1.0, 0.5), halo=(3, 3, 3), bc_z="wall")
-    return CoreSpec(grid=g, c_s=c_s, theta0=300.0, advection=advection, nu=1e-4, sgs=sgs)
+    return CoreSpec(grid=g, c_s=c_s, theta0=300.0, advection=advection, nu=1e-4, sgs=sgs, **kw)
 
 
 def state(g, seed=3):
@@ -56,6 +56,8 @@ def restart_matches(make, tmp_path, sp=None):
     if sp.sgs == "lagrangian":
         for x, y in zip(a.sgs_state(), b.sgs_state()):
             assert np.array_equal(x, y)
+    if sp.sgs == "tke":
+        assert np.array_equal(a.sgs_state(), b.sgs_state())
 
 
 def test_written_checkpoint_reads_back(tmp_path):
@@ -89,6 +91,10 @@ def test_restart_with_the_lagrangian_memories(tmp_path):
         restore(OracleSimulation(spec()), p, check_parameters=False)
 
 
+def test_restart_with_the_tke(tmp_path):
+    restart_matches(OracleSimulation, tmp_path, spec(c_s=0.1, sgs="tke", tke_e0=0.01))
+
+
 def test_checkpoint_of_another_domain_is_refused(tmp_path):
     sp = spec()
     o = OracleSimulation(sp)
@@ -119,7 +125,7 @@ def test_buffers_are_refilled_in_place():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("sgs,c_s", [("smagorinsky", 0.17), ("lagrangian", 0.5)])
-def test_gpu_restart_continues_the_run_exactly(tmp_path, sgs, c_s):
+@pytest.mark.parametrize("sgs,c_s,kw", [("smagorinsky", 0.17, {}), ("lagrangian", 0.5, {}), ("tke", 0.1, {"tke_e0": 0.01})])
+def test_gpu_restart_continues_the_run_exactly(tmp_path, sgs, c_s, kw):
     from aeolus_b200.simulation import Simulation
-    restart_matches(Simulation, str(tmp_path), spec(c_s=c_s, sgs=sgs))
+    restart_matches(Simulation, str(tmp_path), spec(c_s=c_s, sgs=sgs, **kw))
