@@ -6,6 +6,9 @@ pressure problems, and using it in flexible CG.
     net = train_unet(shape, pairs, steps=2000)
     mg.set_learned(net)                              # flexible CG with the network
 
+    sim = urban_flow(n, seed, nboxes)                # the urban setup as a stepped flow
+    net, losses, used = train_from_run(sim, steps=200, dt=0.2, cap=10)   # its own snapshots
+
 A pair (r_k, e_k) is the residual after k CG iterations and the error
 x* - x_k of that iterate against the converged solution, so A e_k = r_k.
 """
@@ -15,6 +18,7 @@ import numpy as np
 
 from .cutcell import box_geometry, face_coefficients, pressure_rhs, random_boxes, urban_velocity
 from .grids import regular_grid
+from .spec import CoreSpec
 from .multigrid import MGPreconditionedCG
 from .unet import UNet, error_scale
 
@@ -116,3 +120,53 @@ def transfer(net, n, fluid):
     other.set_mask(fluid)
     other.set_out_scale(net.out_scale)
     return other
+
+
+def urban_flow(n, seed, nboxes, delta=2.0, precision="fp64", noise_seed=None, device=0):
+    """The cut-cell urban setup as a stepped flow: the Boussinesq core on n
+    cells of `delta` metres (periodic in x and y, walls in z), WENO-JS5 with
+    Smagorinsky C_s = 0.17, no buoyancy, every projection the plain
+    MG-preconditioned CG on the boxes' fractional face apertures to 1e-8;
+    started from the log-profile inflow (5 m/s at 10 m, z0 = 0.1 m) with
+    +-0.5 m/s noise from `noise_seed` (default `seed`), projected.  Returns
+    (simulation, grid, geometry)."""
+    from .simulation import Simulation
+    g, geom = urban_geometry(n, seed, nboxes, delta)
+    spec = CoreSpec(grid=g, advection="weno_js5", c_s=0.17, nu=0.0, solver="pcg", precision=precision)
+    sim = Simulation(spec, device=device)
+    sim.set_pcg(face_coefficients(geom, power=1), tol=1e-8, maxit=500)
+    u, v, w = urban_velocity(g, geom, seed=seed if noise_seed is None else noise_seed)
+    sim.set_state(u, v, w, g.zeros())
+    sim.project()
+    return sim, g, geom
+
+
+def train_from_run(sim, steps, dt, cap=10, lr=1e-3, lr_final=1e-4, seed=0, net=None, fluid=None):
+    """Train on the run's own snapshots: `steps` projected RK3 steps of `sim`
+    (a PCG-projected simulation with the plain preconditioner), after each
+    step the right-hand side of its last projection solved again by the plain
+    MG-preconditioned CG with its first `cap` residual -> error pairs
+    recorded (Simulation.pcg_harvest), each pair used at once for one Adam
+    step (the rate decaying geometrically from lr to lr_final over the
+    expected steps * cap pairs).  The output scale comes from the first
+    step's pairs.  Returns (net, losses, pairs used)."""
+    g = sim.grid
+    n = (g.nx, g.ny, g.nz)
+    if net is None:
+        net = UNet(n, seed=seed)
+    if fluid is not None:
+        net.set_mask(np.asarray(fluid, dtype=np.float32))
+    rng = np.random.default_rng(seed)
+    total = max(steps * cap - 1, 1)
+    losses, used = [], 0
+    for it in range(steps):
+        sim.step_rk3(dt, 1)
+        _, _, pairs = sim.pcg_harvest(cap)
+        pairs = [p for p in pairs if np.linalg.norm(p[0]) > 0]
+        if it == 0:
+            net.set_out_scale(error_scale(pairs))
+        for k in rng.permutation(len(pairs)):
+            a = lr * (lr_final / lr) ** (min(used, total) / total)
+            losses.append(net.train_step(pairs[k][0], pairs[k][1], a))
+            used += 1
+    return net, np.array(losses), used

@@ -323,6 +323,20 @@ class Simulation:
         _lib.check(self._lib.aeo_pcg_set_learned(self._h, net.handle if net is not None else None, float(stagnation)),
                    self._h)
 
+    def pcg_harvest(self, cap: int = 10):
+        """Residual -> error pairs from the run's own snapshot: the right-hand
+        side b of the last projection's solve, solved again from zero by the
+        plain MG-preconditioned CG.  Returns (b, x, [(r_k, x - x_k)]) as
+        interior (nz, ny, nx) FP64 arrays, A (x - x_k) = r_k."""
+        g = self.grid
+        shape = (g.nz, g.ny, g.nx)
+        b, x = np.empty(shape), np.empty(shape)
+        rh, xh = np.empty((cap,) + shape), np.empty((cap,) + shape)
+        cnt = C.c_int32()
+        _lib.check(self._lib.aeo_pcg_harvest(self._h, int(cap), _ptr(b), _ptr(x), _ptr(rh), _ptr(xh), C.byref(cnt)),
+                   self._h)
+        return b, x, [(rh[k], x - xh[k]) for k in range(cnt.value)]
+
     def kinetic_energy(self) -> float:
         v = C.c_double()
         _lib.check(self._lib.aeo_kinetic_energy(self._h, C.byref(v)), self._h)

@@ -220,6 +220,14 @@ struct aeo_unet {
         CK(cudaFuncSetAttribute(un::conv_fwd_kernel<16, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f1632));
         CK(cudaFuncSetAttribute(un::conv_fwd_kernel<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f3232));
         CK(cudaFuncSetAttribute(un::conv_fwd_kernel<32, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f3216));
+        CK(cudaFuncSetAttribute(un::conv_ring_kernel<16, 16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)un::RingShape<16, 16, 2>::smem));
+        CK(cudaFuncSetAttribute(un::conv_ring_kernel<16, 32, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)un::RingShape<16, 32, 1>::smem));
+        CK(cudaFuncSetAttribute(un::conv_ring_kernel<32, 32, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)un::RingShape<32, 32, 1>::smem));
+        CK(cudaFuncSetAttribute(un::conv_ring_kernel<32, 16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)un::RingShape<32, 16, 1>::smem));
         CK(cudaFuncSetAttribute(un::conv_wgrad_kernel<16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w1616));
         CK(cudaFuncSetAttribute(un::conv_wgrad_kernel<16, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w1632));
         CK(cudaFuncSetAttribute(un::conv_wgrad_kernel<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w3232));
@@ -249,6 +257,16 @@ struct aeo_unet {
         return Tl.ntiles < g ? Tl.ntiles : g;
     }
 
+    // the ring kernel on x-segment tiles: two CTAs an SM where the ring and
+    // the weights fit twice, contiguous tile ranges of equal length
+    template <int CIN, int COUT, int PF>
+    void ring(const Tiles& Tl, const un::ConvArgs& a) {
+        constexpr size_t sm = un::RingShape<CIN, COUT, PF>::smem;
+        const int per_sm = sm <= 113 * 1024 ? 2 : 1;
+        const int g = Tl.ntiles < sms * per_sm ? Tl.ntiles : sms * per_sm;
+        un::conv_ring_kernel<CIN, COUT, PF><<<g, un::CONV_THREADS, sm, st>>>(a);
+    }
+
     // one convolution (forward, or transposed with the backward image)
     aeo_status conv(int l, bool transposed, const bf16* in, bf16* out, const float* b, const bf16* add,
                     const bf16* gate, int relu, float* out0 = nullptr, const float* out0_mask = nullptr,
@@ -269,6 +287,14 @@ struct aeo_unet {
         a.out0_scale = out0_scale;
         a.relu = relu;
         a.err = derr;
+        if (Tl.mode == 0 && Tl.ny >= 3) {   // x-segment tiles, ny >= prefetch + 1: the pipelined ring kernel
+            if (ci == 16 && co == 16) ring<16, 16, 2>(Tl, a);
+            else if (ci == 16 && co == 32) ring<16, 32, 1>(Tl, a);
+            else if (ci == 32 && co == 32) ring<32, 32, 1>(Tl, a);
+            else ring<32, 16, 1>(Tl, a);
+            CKL();
+            return AEO_OK;
+        }
         if (ci == 16 && co == 16) a.dbuf = fwd_dbuf<16, 16>(Tl);
         else if (ci == 16 && co == 32) a.dbuf = fwd_dbuf<16, 32>(Tl);
         else if (ci == 32 && co == 32) a.dbuf = fwd_dbuf<32, 32>(Tl);

@@ -132,6 +132,69 @@ struct ConvArgs {
     int* err;
 };
 
+// The epilogue of one output cell: its COUT accumulators from the thread's
+// TMEM lane (tacc = the accumulator's address with the lane quarter of the
+// calling warp), + bias + add, ReLU, * gate, stored as BF16 and/or channel 0
+// in FP32.
+template <int COUT>
+__device__ __forceinline__ void conv_epilogue(const ConvArgs& a, uint32_t tacc, int cell) {
+    float v[COUT];
+    {
+        float h[16];
+        tc::tmem_ld16(tacc, h);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = h[q];
+        if constexpr (COUT == 32) {
+            tc::tmem_ld16(tacc + 16u, h);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) v[16 + q] = h[q];
+        }
+    }
+    if (a.bias)
+#pragma unroll
+        for (int q = 0; q < COUT; ++q) v[q] += a.bias[q];
+    if (a.add) {
+        const uint4* ap = reinterpret_cast<const uint4*>(a.add + (size_t)cell * COUT);
+#pragma unroll
+        for (int u = 0; u < COUT / 8; ++u) {
+            uint4 w = ap[u];
+            const bf16* e = reinterpret_cast<const bf16*>(&w);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v[8 * u + q] += __bfloat162float(e[q]);
+        }
+    }
+    if (a.relu)
+#pragma unroll
+        for (int q = 0; q < COUT; ++q) v[q] = fmaxf(v[q], 0.0f);
+    if (a.gate) {
+        const uint4* gp = reinterpret_cast<const uint4*>(a.gate + (size_t)cell * COUT);
+#pragma unroll
+        for (int u = 0; u < COUT / 8; ++u) {
+            uint4 w = gp[u];
+            const bf16* e = reinterpret_cast<const bf16*>(&w);
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (!(__bfloat162float(e[q]) > 0.0f)) v[8 * u + q] = 0.0f;
+        }
+    }
+    if (a.out) {
+        uint4* op = reinterpret_cast<uint4*>(a.out + (size_t)cell * COUT);
+#pragma unroll
+        for (int u = 0; u < COUT / 8; ++u) {
+            uint4 w;
+            bf16* e = reinterpret_cast<bf16*>(&w);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) e[q] = __float2bfloat16_rn(v[8 * u + q]);
+            op[u] = w;
+        }
+    }
+    if (a.out0) {
+        float s = a.out0_scale ? (float)*a.out0_scale : 1.0f;
+        if (a.out0_mask) s *= a.out0_mask[cell];
+        a.out0[cell] = v[0] * s;
+    }
+}
+
 template <int CIN, int COUT>
 constexpr size_t conv_smem_weights() { return (size_t)(CIN / 8) * 27 * COUT * 16; }
 
@@ -212,63 +275,7 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_fwd_kernel(ConvArgs a) {
         }
         tc::fence_after();
         // epilogue: warp w holds tile rows 32w..32w+31 in its TMEM lane quarter
-        const int m = warp * 32 + lane;
-        const int cell = cell_of(T, x0, j0, k, m);
-        float v[COUT];
-        {
-            float h[16];
-            tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16), h);
-#pragma unroll
-            for (int q = 0; q < 16; ++q) v[q] = h[q];
-            if constexpr (COUT == 32) {
-                tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + 16u, h);
-#pragma unroll
-                for (int q = 0; q < 16; ++q) v[16 + q] = h[q];
-            }
-        }
-        if (a.bias)
-#pragma unroll
-            for (int q = 0; q < COUT; ++q) v[q] += a.bias[q];
-        if (a.add) {
-            const uint4* ap = reinterpret_cast<const uint4*>(a.add + (size_t)cell * COUT);
-#pragma unroll
-            for (int u = 0; u < COUT / 8; ++u) {
-                uint4 w = ap[u];
-                const bf16* e = reinterpret_cast<const bf16*>(&w);
-#pragma unroll
-                for (int q = 0; q < 8; ++q) v[8 * u + q] += __bfloat162float(e[q]);
-            }
-        }
-        if (a.relu)
-#pragma unroll
-            for (int q = 0; q < COUT; ++q) v[q] = fmaxf(v[q], 0.0f);
-        if (a.gate) {
-            const uint4* gp = reinterpret_cast<const uint4*>(a.gate + (size_t)cell * COUT);
-#pragma unroll
-            for (int u = 0; u < COUT / 8; ++u) {
-                uint4 w = gp[u];
-                const bf16* e = reinterpret_cast<const bf16*>(&w);
-#pragma unroll
-                for (int q = 0; q < 8; ++q)
-                    if (!(__bfloat162float(e[q]) > 0.0f)) v[8 * u + q] = 0.0f;
-            }
-        }
-        if (a.out) {
-            uint4* op = reinterpret_cast<uint4*>(a.out + (size_t)cell * COUT);
-#pragma unroll
-            for (int u = 0; u < COUT / 8; ++u) {
-                uint4 w;
-                bf16* e = reinterpret_cast<bf16*>(&w);
-#pragma unroll
-                for (int q = 0; q < 8; ++q) e[q] = __float2bfloat16_rn(v[8 * u + q]);
-                op[u] = w;
-            }
-        }
-        if (a.out0) {
-            float s = a.out0_scale ? (float)*a.out0_scale : 1.0f;
-            if (a.out0_mask) s *= a.out0_mask[cell];
-            a.out0[cell] = v[0] * s;
-        }
+        conv_epilogue<COUT>(a, tmem + ((uint32_t)(warp * 32) << 16), cell_of(T, x0, j0, k, warp * 32 + lane));
         tc::fence_before();
         __syncthreads();
         if (!a.dbuf && nxt < T.ntiles) {
@@ -285,6 +292,174 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_fwd_kernel(ConvArgs a) {
     }
     __syncthreads();
     if (warp == 0) tc::tmem_dealloc(tmem, 32);
+}
+
+// ---------------------------------------------------------------- ring kernel
+//
+// The forward convolution of x-segment tiles (nx a multiple of 128) as a
+// pipeline.  A CTA takes a contiguous range of tiles ordered y fastest
+// (tile = (k * tx + xt) * ny + j), so consecutive tiles share two of their
+// three y rows: the staged input is a ring of R "entries", an entry being
+// one y row of the column's three z planes (dz = -1, 0, +1) with its x halo,
+// K-major 16-byte rows (8 channels of a cell) as in stage_input.  A tile
+// pushes one entry (row j + 1), or three at the start of a column; tile i's
+// rows are the entries q_i - 2, q_i - 1, q_i (q_i the stream index of its
+// last entry), held in slots q mod R.  While the tensor core runs the 27
+// taps of tile i into one of two TMEM accumulators, the CTA drains tile
+// i - 1 from the other and loads the entries of tile i + PF.  An entry
+// overwrites the slot of stream index q - R; with at most one column start
+// among PF consecutive tiles (ny >= PF + 1), q_{i+PF} - q_i <= PF + 2, so
+// R = PF + 5 keeps every slot that tile i reads intact, and tile i - 1's
+// slots are reused only after its MMAs completed.
+template <int CIN, int COUT, int PF>
+struct RingShape {
+    static constexpr int NCH = CIN / 8;
+    static constexpr int R = PF + 5;
+    static constexpr int PITCH = TM + 2;
+    static constexpr size_t slot_rows = (size_t)3 * NCH * PITCH;          // 16-byte rows per entry
+    static constexpr size_t smem = conv_smem_weights<CIN, COUT>() + (size_t)R * slot_rows * 16;
+    static constexpr uint32_t tmem_cols = 2 * COUT < 32 ? 32u : (uint32_t)(2 * COUT);
+};
+
+// one entry: row jj of the column (k, x0) for dz = -1, 0, +1, every chunk,
+// cells x0 - 1 .. x0 + 128 (periodic in x), zero outside z; consecutive
+// threads copy consecutive 16 bytes of the source row
+template <int CIN, int COUT, int PF>
+__device__ __forceinline__ void ring_load_entry(const Tiles& T, const uint4* __restrict__ in, uint4* sR, int slot,
+                                                int k, int x0, int jj) {
+    using RS = RingShape<CIN, COUT, PF>;
+    constexpr int NCH = RS::NCH, PITCH = RS::PITCH, R = RS::R;
+    constexpr int TOTAL = 3 * NCH * PITCH;
+    for (int idx = threadIdx.x; idx < TOTAL; idx += blockDim.x) {
+        const int c = idx % NCH, rest = idx / NCH;
+        const int x = rest % PITCH, d = rest / PITCH;
+        const int gz = k + d - 1;
+        const bool zin = gz >= 0 && gz < T.nz;
+        int gx = x0 - 1 + x;
+        gx = gx < 0 ? gx + T.nx : (gx >= T.nx ? gx - T.nx : gx);
+        const uint4* src = in + ((size_t)((zin ? gz : 0) * T.ny + jj) * T.nx + gx) * NCH + c;
+        cp_async16(sR + ((size_t)((c * R + slot) * 3 + d)) * PITCH + x, src, zin);
+    }
+}
+
+// out = act(conv(in) + bias + add) * gate, per the flags (mode 0 tiles).
+template <int CIN, int COUT, int PF>
+__global__ void __launch_bounds__(CONV_THREADS) conv_ring_kernel(ConvArgs a) {
+    static_assert(CIN % 16 == 0 && (COUT == 16 || COUT == 32), "CIN multiple of 16, COUT 16 or 32");
+    static_assert(PF >= 1 && PF <= 4, "prefetch depth 1..4");
+    using RS = RingShape<CIN, COUT, PF>;
+    constexpr int NCH = RS::NCH, R = RS::R, PITCH = RS::PITCH;
+    constexpr int WROWS = NCH * 27 * COUT;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t mbar[2];
+    __shared__ uint32_t tslot;
+    const Tiles& T = a.T;
+    uint4* sB = reinterpret_cast<uint4*>(smem);
+    uint4* sR = sB + WROWS;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t0 = (int)((long long)T.ntiles * blockIdx.x / gridDim.x);
+    const int cnt = (int)((long long)T.ntiles * (blockIdx.x + 1) / gridDim.x) - t0;
+    for (int i = threadIdx.x; i < WROWS; i += blockDim.x) sB[i] = a.wimg[i];
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&mbar[0], 1);
+        tc::mbar_init(&mbar[1], 1);
+    }
+    if (warp == 0) tc::tmem_alloc(&tslot, RS::tmem_cols);
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = tslot;
+    const uint32_t idesc = tc::idesc_bf16(COUT, false, false);
+    constexpr uint32_t lboA = (uint32_t)(R * 3 * PITCH * 16), lboB = 27u * COUT * 16u;
+    const uint32_t aBase = tc::smem_u32(sR), bBase = tc::smem_u32(sB);
+    const uint4* inp = reinterpret_cast<const uint4*>(a.in);
+    int ql = -1;                        // stream index of the last entry loaded
+    auto load_tile = [&](int iu) {
+        const int tau = t0 + iu;
+        const int j = tau % T.ny, col = tau / T.ny;
+        const int k = col / T.tx, x0 = (col - k * T.tx) * TM;
+        const bool fresh = iu == 0 || j == 0;
+        for (int dy = fresh ? -1 : 1; dy <= 1; ++dy) {
+            int jj = j + dy;
+            jj = jj < 0 ? jj + T.ny : (jj >= T.ny ? jj - T.ny : jj);
+            ++ql;
+            ring_load_entry<CIN, COUT, PF>(T, inp, sR, ql % R, k, x0, jj);
+        }
+    };
+#pragma unroll 1
+    for (int iu = 0; iu < PF; ++iu) {
+        if (iu < cnt) load_tile(iu);
+        cp_async_commit();
+    }
+    int qm = -1;                        // stream index of the last entry of the tile in the MMA
+    int issued = 0, drained = 0;
+    bool failed = false;
+#pragma unroll 1
+    for (int i = 0; i < cnt; ++i) {
+        const int tau = t0 + i;
+        qm += (i == 0 || tau % T.ny == 0) ? 3 : 1;
+        cp_async_wait<PF - 1>();        // tile i's entries (the group committed PF groups ago)
+        tc::fence_async_smem();
+        tc::fence_before();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tc::fence_after();
+            const uint32_t dacc = tmem + (uint32_t)((i & 1) * COUT);
+#pragma unroll 1
+            for (int t = 0; t < 27; ++t) {
+                const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;      // each 0..2 (offset + 1)
+                const int slot = (qm - 2 + dy) % R;
+#pragma unroll
+                for (int ks = 0; ks < CIN / 16; ++ks) {
+                    const uint32_t aa = aBase + (uint32_t)((((2 * ks * R + slot) * 3 + dz) * PITCH + dx) * 16);
+                    const uint32_t bb = bBase + (uint32_t)((2 * ks * 27 + t) * COUT * 16);
+                    tc::mma_bf16(dacc, tc::sdesc(aa, lboA, 128), tc::sdesc(bb, lboB, 128), idesc,
+                                 (t | ks) ? 1u : 0u);
+                }
+            }
+            tc::commit(&mbar[i & 1]);
+        }
+        ++issued;
+        if (i > 0) {
+            const int ip = i - 1;
+            const bool ok = tc::mbar_wait(&mbar[ip & 1], (uint32_t)((ip >> 1) & 1), WAIT_LIMIT);
+            if (__syncthreads_or(!ok)) {
+                failed = true;
+                break;
+            }
+            ++drained;
+            tc::fence_after();
+            const int tp = tau - 1, jp = tp % T.ny, colp = tp / T.ny;
+            const int kp = colp / T.tx, x0p = (colp - kp * T.tx) * TM;
+            conv_epilogue<COUT>(a, tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((ip & 1) * COUT),
+                                (kp * T.ny + jp) * T.nx + x0p + warp * 32 + lane);
+        }
+        if (i + PF < cnt) load_tile(i + PF);
+        cp_async_commit();
+    }
+    if (!failed && cnt > 0) {
+        const int ip = cnt - 1;
+        const bool ok = tc::mbar_wait(&mbar[ip & 1], (uint32_t)((ip >> 1) & 1), WAIT_LIMIT);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+        } else {
+            ++drained;
+            tc::fence_after();
+            const int tp = t0 + ip, jp = tp % T.ny, colp = tp / T.ny;
+            const int kp = colp / T.tx, x0p = (colp - kp * T.tx) * TM;
+            conv_epilogue<COUT>(a, tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((ip & 1) * COUT),
+                                (kp * T.ny + jp) * T.nx + x0p + warp * 32 + lane);
+        }
+    }
+    cp_async_wait<0>();
+    if (failed) {
+        if (threadIdx.x == 0) atomicExch(a.err, 1);
+        // the MMAs still in flight (at most two tiles), bounded
+        for (int u = drained; u < issued; ++u) tc::mbar_wait(&mbar[u & 1], (uint32_t)((u >> 1) & 1), WAIT_LIMIT);
+    }
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, RS::tmem_cols);
 }
 
 struct WgradArgs {

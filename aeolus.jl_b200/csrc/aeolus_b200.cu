@@ -118,6 +118,7 @@ struct CoreBase {
     virtual aeo_status set_pcg(const double* ax, const double* ay, const double* az, double tol, int maxit) = 0;
     virtual aeo_status pcg_stats(aeo_mg_stats* o) = 0;
     virtual aeo_status pcg_set_learned(aeo_unet* net, double stagnation) = 0;
+    virtual aeo_status pcg_harvest(int cap, double* b, double* x, double* rh, double* xh, int* count) = 0;
     virtual aeo_status set_ibm(const uint8_t* mask, double tau) = 0;
     virtual aeo_status set_sgs_buoyancy(const double* bg) = 0;
     virtual aeo_status set_lagrangian(double c0, double theta, double memory_time) = 0;
@@ -161,6 +162,7 @@ struct Core : CoreBase {
     double *mg_b = nullptr, *mg_x = nullptr;
     R *apx = nullptr, *apy = nullptr, *apz = nullptr;
     double pcg_tol = 1e-8;
+    bool pcg_learned = false;
     int pcg_maxit = 200;
     double* d_stage = nullptr; // host-layout staging (device)
     long long host_n = 0;
@@ -904,6 +906,28 @@ struct Core : CoreBase {
         drop_graphs();   // the solve's loop body changes with the preconditioner
         if (aeo_status e = aeo_mg_set_learned(mg, net, stagnation)) {
             fail(std::string("pcg_set_learned: ") + aeo_mg_last_error(mg));
+            return e;
+        }
+        pcg_learned = net != nullptr;
+        return AEO_OK;
+    }
+
+    // The right-hand side of the last projection's solve (the run's own
+    // snapshot), solved again from zero by the plain MG-preconditioned CG with
+    // the residual and iterate of its first `cap` iterations recorded.
+    aeo_status pcg_harvest(int cap, double* b, double* x, double* rh, double* xh, int* count) override {
+        if (!pcg) { fail("pcg_harvest: the domain was not created with solver = AEO_SOLVER_PCG"); return AEO_ERR_STATE; }
+        if (pcg_learned) {
+            fail("pcg_harvest: pairs come from plain solves; switch the learned preconditioner off first");
+            return AEO_ERR_STATE;
+        }
+        CK(cudaStreamSynchronize(st));
+        aeo_mg_stats o{};
+        if (aeo_status e = aeo_mg_read_stats(mg, &o)) { fail(std::string("pcg_harvest: ") + aeo_mg_last_error(mg)); return e; }
+        if (!(o.bnorm > 0)) { fail("pcg_harvest: no projection with a non-zero right-hand side has run yet"); return AEO_ERR_STATE; }
+        CK(cudaMemcpy(b, mg_b, sizeof(double) * (size_t)g.nin, cudaMemcpyDeviceToHost));
+        if (aeo_status e = aeo_mg_solve_harvest(mg, b, x, &o, rh, xh, cap, count)) {
+            fail(std::string("pcg_harvest: ") + aeo_mg_last_error(mg));
             return e;
         }
         return AEO_OK;
@@ -2110,6 +2134,16 @@ aeo_status aeo_pcg_stats(aeo_sim* h, int32_t* iterations, int32_t* status, doubl
 aeo_status aeo_pcg_set_learned(aeo_sim* h, struct aeo_unet* net, double stagnation) {
     ENTER(h);
     return h->core->pcg_set_learned(net, stagnation);
+}
+
+aeo_status aeo_pcg_harvest(aeo_sim* h, int32_t cap, double* b, double* x, double* r_hist, double* x_hist,
+                           int32_t* count) {
+    ENTER(h);
+    if (!b || !x || !r_hist || !x_hist || !count || cap < 1) {
+        h->core->fail("pcg_harvest: NULL array or cap < 1");
+        return AEO_ERR_ARGUMENT;
+    }
+    return h->core->pcg_harvest(cap, b, x, r_hist, x_hist, count);
 }
 
 aeo_status aeo_kinetic_energy(aeo_sim* h, double* out) {

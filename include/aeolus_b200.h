@@ -381,6 +381,17 @@ aeo_status aeo_set_pcg(aeo_sim* h, const double* ax, const double* ay, const dou
  * ||r||, ||b - mean(b)||); synchronises the handle's stream */
 aeo_status aeo_pcg_stats(aeo_sim* h, int32_t* iterations, int32_t* status, double* residual, double* bnorm);
 aeo_status aeo_pcg_set_learned(aeo_sim* h, struct aeo_unet* net, double stagnation);
+/* Residual -> error pairs from the run's own snapshots (no reference
+ * counterpart; it feeds the learned preconditioner): b receives the
+ * right-hand side of the last projection's solve (the predictor's cut-cell
+ * divergence of the last substage, nx*ny*nz FP64, x fastest), which the
+ * plain MG-preconditioned CG solves again from a zero guess; x receives its
+ * converged solution, r_hist / x_hist (cap * nx*ny*nz each) the residual
+ * r_k and iterate x_k of iterations k = 0 .. count-1, so that A (x - x_k) =
+ * r_k.  AEO_ERR_STATE while a learned preconditioner is set or before a
+ * projection has run; synchronises the handle's stream. */
+aeo_status aeo_pcg_harvest(aeo_sim* h, int32_t cap, double* b, double* x, double* r_hist, double* x_hist,
+                           int32_t* count);
 
 /* Last error message of the handle (or of the last failed aeo_create when h is NULL). */
 const char* aeo_last_error(const aeo_sim* h);
