@@ -323,6 +323,21 @@ class Simulation:
         _lib.check(self._lib.aeo_pcg_set_learned(self._h, net.handle if net is not None else None, float(stagnation)),
                    self._h)
 
+    def set_open_boundaries(self, obc=None):
+        """Open lateral faces from an OpenBoundarySet
+        (open_boundary.open_boundary_conditions) on this domain's grid; None
+        closes them again (periodic x and y)."""
+        if obc is None:
+            _lib.check(self._lib.aeo_set_open(self._h, 0, 0, None, None, None), self._h)
+            self._open = None
+            return
+        if obc.grid.size != self.grid.size or obc.grid.halo != self.grid.halo:
+            raise ValueError("the open boundaries were built for another grid")
+        xp, yp, modes = obc.packed()
+        _lib.check(self._lib.aeo_set_open(self._h, int(obc.open_x), int(obc.open_y), _ptr(xp), _ptr(yp),
+                                          modes.ctypes.data_as(C.POINTER(C.c_int32))), self._h)
+        self._open = obc
+
     def pcg_harvest(self, cap: int = 10):
         """Residual -> error pairs from the run's own snapshot: the right-hand
         side b of the last projection's solve, solved again from zero by the

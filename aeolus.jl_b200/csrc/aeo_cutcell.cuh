@@ -42,7 +42,10 @@ template <typename R, bool ANEL = false, bool UNI = true>
 __global__ void __launch_bounds__(256) cc_div_kernel(Geo g, const R* __restrict__ us, const R* __restrict__ vs,
                                                      const R* __restrict__ ws, const R* __restrict__ ax,
                                                      const R* __restrict__ ay, const R* __restrict__ az,
-                                                     double* __restrict__ b) {
+                                                     double* __restrict__ b, const R* __restrict__ bw = nullptr,
+                                                     const R* __restrict__ be = nullptr,
+                                                     const R* __restrict__ bs = nullptr,
+                                                     const R* __restrict__ bn = nullptr) {
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= g.nin) return;
     const int lnx = __ffs(g.nx) - 1, lny = __ffs(g.ny) - 1;
@@ -53,8 +56,18 @@ __global__ void __launch_bounds__(256) cc_div_kernel(Geo g, const R* __restrict_
     const R aw = ax[xr + i], ae = ax[xr + i + 1];
     const R as = ay[yr + i], an = ay[yr + g.nx + i];
     const R ab = az[q], at = az[q + pl];
-    const R uw = us[q], ue = us[i + 1 < g.nx ? q + 1 : q + 1 - g.nx];
-    const R vsv = vs[q], vn = vs[j + 1 < g.ny ? q + g.nx : q - (long long)(g.ny - 1) * g.nx];
+    R uw = us[q], ue = us[i + 1 < g.nx ? q + 1 : q + 1 - g.nx];
+    R vsv = vs[q], vn = vs[j + 1 < g.ny ? q + g.nx : q - (long long)(g.ny - 1) * g.nx];
+    // open faces: the boundary faces carry the planes' (mass-corrected) normal
+    // velocities, which the fill writes into u* before the projection
+    if (bw) {
+        if (i == 0) uw = bw[(long long)k * g.ny + j];
+        if (i == g.nx - 1) ue = be[(long long)k * g.ny + j];
+    }
+    if (bs) {
+        if (j == 0) vsv = bs[(long long)k * g.nx + i];
+        if (j == g.ny - 1) vn = bn[(long long)k * g.nx + i];
+    }
     const R wb = ws[q];
     const R wt = k + 1 < g.nz ? ws[q + pl] : (g.bc_z == 0 ? ws[q - (long long)(g.nz - 1) * pl] : R(0));
     // in FP64 whatever R is: a fluid region the obstacles seal off from the rest
@@ -80,22 +93,28 @@ __global__ void __launch_bounds__(256) cc_correct_kernel(Geo g, const R* __restr
                                                          const R* __restrict__ ax, const R* __restrict__ ay,
                                                          const R* __restrict__ az, const R* u0, const R* v0,
                                                          const R* w0, R* uo, R* vo, R* wo, R* __restrict__ p,
-                                                         const double* __restrict__ dtp, R ca, R cb, int stage) {
+                                                         const double* __restrict__ dtp, R ca, R cb, int stage,
+                                                         const R* __restrict__ bw = nullptr,
+                                                         const R* __restrict__ bs = nullptr) {
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= g.nin) return;
     const int lnx = __ffs(g.nx) - 1, lny = __ffs(g.ny) - 1;
     const int i = (int)(q & (g.nx - 1)), j = (int)((q >> lnx) & (g.ny - 1)), k = (int)(q >> (lnx + lny));
     const long long pl = (long long)g.nx * g.ny;
     const double pc = phi[q];
-    const double pw = phi[i > 0 ? q - 1 : q + g.nx - 1];
-    const double ps = phi[j > 0 ? q - g.nx : q + (long long)(g.ny - 1) * g.nx];
+    // a west / south open face: phi's mirror halo (d phi / dn = 0) leaves the
+    // prescribed boundary-face velocity as the fill wrote it
+    const bool ow = bw && i == 0, os = bs && j == 0;
+    const double pw = ow ? pc : phi[i > 0 ? q - 1 : q + g.nx - 1];
+    const double ps = os ? pc : phi[j > 0 ? q - g.nx : q + (long long)(g.ny - 1) * g.nx];
     // k - 1 = -1: periodic wrap, or the wall mirror (the bottom face is blocked there)
     const double pb = phi[k > 0 ? q - pl : (g.bc_z == 0 ? q + (long long)(g.nz - 1) * pl : q)];
     const R aw = ax[(long long)(g.nx + 1) * (j + (long long)g.ny * k) + i];
     const R as = ay[(long long)g.nx * (j + (long long)(g.ny + 1) * k) + i];
     const R ab = az[q];
-    R un = aw > R(0) ? us[q] - aw * R((pc - pw) * g.idx) : R(0);
-    R vn = as > R(0) ? vs[q] - as * R((pc - ps) * g.idy) : R(0);
+    const R ustar = ow ? bw[(long long)k * g.ny + j] : us[q], vstar = os ? bs[(long long)k * g.nx + i] : vs[q];
+    R un = aw > R(0) ? ustar - aw * R((pc - pw) * g.idx) : R(0);
+    R vn = as > R(0) ? vstar - as * R((pc - ps) * g.idy) : R(0);
     R wn = ab > R(0) ? ws[q] - ab * R((pc - pb) * (UNI ? g.idz : lvl(g.idzf, k))) : R(0);
     const long long qp = pidx(g, i, j, k);
     if (stage) {

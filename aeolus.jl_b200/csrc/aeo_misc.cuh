@@ -77,6 +77,105 @@ __global__ void __launch_bounds__(256) halo_fill_kernel(Geo g, HaloSet<R> hs) {
         if (f < hs.nf) hs.f[f][q] = v[f];
 }
 
+// ---- open lateral faces (src/boundary_conditions/open_boundary.jl:722-807) -------
+// The plane buffers of the open faces in the reference's storage extents
+// (halo H = AEO_H on every axis): x planes [field][side][NZ][NY][L], y planes
+// [field][side][NZ][L][NX] (field u, v, w, theta; side 0 west/south, 1
+// east/north; NZ, NY, NX the storage extents; layer = storage index along the
+// normal on the low side, storage index - (H + N) on the high side, L = H + 1
+// so the low side holds the normal velocity's boundary face, interior 0).
+// mode[f] = 1: the field takes the zero-gradient mirror on open faces, as
+// every field without a plane does (pid < 0: the pressure, nu_t, closure
+// state).  The boundary-face values of the normal velocities, bw/be [k][j]
+// and bs/bn [k][i] (interior), feed the projection.
+template <typename R>
+struct OpenSet {
+    const R* xp;
+    const R* yp;
+    const R* bw;
+    const R* be;
+    const R* bs;
+    const R* bn;
+    int ox, oy, L;
+    int mode[4];
+};
+
+// The composite map of the reference's fill order (x, then y, then z) with
+// open faces: z first (the z fill copies whole x-y planes), then y (an open y
+// face copies its plane over every x, halos included), then x.
+template <typename R>
+__device__ __forceinline__ R open_halo_value(const Geo& g, const OpenSet<R>& ob, const R* f, int loc, int pid, int i,
+                                             int j, int k) {
+    int kk;
+    const int s = zmap(g, k, loc, &kk);
+    if (s == 0) return R(0);
+    const bool plane = pid >= 0 && ob.mode[pid] == 0;
+    const int NX = g.nx + 2 * AEO_H, NY = g.ny + 2 * AEO_H, NZ = g.nz + 2 * AEO_H;
+    R v;
+    int ii = i, jj = j;
+    if (j < 0 || j >= g.ny) {
+        if (ob.oy) {
+            if (plane) {
+                const int side = j >= g.ny, l = side ? j - g.ny : j + AEO_H;
+                v = ob.yp[((((size_t)(pid * 2 + side) * NZ + kk + AEO_H) * ob.L + l) * NX) + i + AEO_H];
+                return s > 0 ? v : -v;
+            }
+            jj = j < 0 ? -1 - j : 2 * g.ny - 1 - j;
+        } else {
+            jj = wrapi(j, g.ny);
+        }
+    }
+    if (i < 0 || i >= g.nx) {
+        if (ob.ox) {
+            if (plane) {
+                const int side = i >= g.nx, l = side ? i - g.nx : i + AEO_H;
+                v = ob.xp[((((size_t)(pid * 2 + side) * NZ + kk + AEO_H) * NY + jj + AEO_H) * ob.L) + l];
+                return s > 0 ? v : -v;
+            }
+            ii = i < 0 ? -1 - i : 2 * g.nx - 1 - i;
+        } else {
+            ii = wrapi(i, g.nx);
+        }
+    }
+    v = f[pidx(g, ii, jj, kk)];
+    return s > 0 ? v : -v;
+}
+
+// The boundary face of a normal velocity on a west / south open face lies in
+// the interior (index 0) and takes the plane's value on every fill
+// (_open_range, src/boundary_conditions/open_boundary.jl:46-51): u[0, j, k]
+// (axis 0) or v[i, 0, k] (axis 1) over the interior of the two other axes.
+template <typename R>
+__global__ void open_face_kernel(Geo g, R* f, OpenSet<R> ob, int axis) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+    const int NX = g.nx + 2 * AEO_H, NY = g.ny + 2 * AEO_H, NZ = g.nz + 2 * AEO_H;
+    if (axis == 0) {
+        if (a >= g.ny) return;
+        f[pidx(g, 0, a, k)] = ob.xp[((((size_t)0 * NZ + k + AEO_H) * NY + a + AEO_H) * ob.L) + AEO_H];
+    } else {
+        if (a >= g.nx) return;
+        f[pidx(g, a, 0, k)] = ob.yp[((((size_t)(1 * 2) * NZ + k + AEO_H) * ob.L + AEO_H) * NX) + a + AEO_H];
+    }
+}
+
+// halo_fill_kernel with open faces; pid[f] the plane of field f (-1: none)
+template <typename R>
+__global__ void __launch_bounds__(256) open_halo_fill_kernel(Geo g, HaloSet<R> hs, OpenSet<R> ob, int4 pid4) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= shell_count(g)) return;
+    int i, j, k;
+    shell_point(g, t, &i, &j, &k);
+    const int pid[4] = {pid4.x, pid4.y, pid4.z, pid4.w};
+    R v[4];
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+        if (f < hs.nf) v[f] = open_halo_value(g, ob, hs.f[f], hs.loc[f], pid[f], i, j, k);
+    const long long q = pidx(g, i, j, k);
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+        if (f < hs.nf) hs.f[f][q] = v[f];
+}
+
 // The wall face of w (interior k = 0) is zero after every fill.
 template <typename R>
 __global__ void wall_face_zero_kernel(Geo g, R* w) {

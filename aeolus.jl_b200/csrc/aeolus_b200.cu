@@ -119,6 +119,7 @@ struct CoreBase {
     virtual aeo_status pcg_stats(aeo_mg_stats* o) = 0;
     virtual aeo_status pcg_set_learned(aeo_unet* net, double stagnation) = 0;
     virtual aeo_status pcg_harvest(int cap, double* b, double* x, double* rh, double* xh, int* count) = 0;
+    virtual aeo_status set_open(int ox, int oy, const double* xp, const double* yp, const int* modes) = 0;
     virtual aeo_status set_ibm(const uint8_t* mask, double tau) = 0;
     virtual aeo_status set_sgs_buoyancy(const double* bg) = 0;
     virtual aeo_status set_lagrangian(double c0, double theta, double memory_time) = 0;
@@ -163,6 +164,10 @@ struct Core : CoreBase {
     R *apx = nullptr, *apy = nullptr, *apz = nullptr;
     double pcg_tol = 1e-8;
     bool pcg_learned = false;
+    std::vector<double> h_ap[3];   // the apertures the PCG operator was built from
+    // open lateral faces (aeo_set_open): plane buffers and boundary-face values
+    bool open_x = false, open_y = false;
+    OpenSet<R> ob{};
     int pcg_maxit = 200;
     double* d_stage = nullptr; // host-layout staging (device)
     long long host_n = 0;
@@ -795,6 +800,7 @@ struct Core : CoreBase {
                 a[2][q] = 0.0;
                 a[2][(size_t)Nz * Nx * Ny + q] = 0.0;
             }
+        for (int d = 0; d < 3; ++d) h_ap[d] = a[d];
         R* dst[3] = {apx, apy, apz};
         // c = a^2 on the uniform Boussinesq column; with density weights or a
         // stretched column, the symmetric form (aeo_cutcell.cuh): W_c a^2 dz_c/h_z
@@ -820,10 +826,20 @@ struct Core : CoreBase {
             CK(cudaMemcpyAsync(dst[d], ar.data(), n[d] * sizeof(R), cudaMemcpyHostToDevice, st));
             CK(cudaStreamSynchronize(st));
         }
+        // open faces: the operator couples nothing across them (the Neumann
+        // condition of phi, src/boundary_conditions/open_boundary.jl:485-531);
+        // the divergence keeps their apertures (the prescribed flux)
+        if (open_x)
+            for (size_t r = 0; r < (size_t)Ny * Nz; ++r) c2[0][r * (Nx + 1)] = c2[0][r * (Nx + 1) + Nx] = 0.0;
+        if (open_y)
+            for (int k = 0; k < Nz; ++k)
+                for (int i = 0; i < Nx; ++i)
+                    c2[1][(size_t)k * (Ny + 1) * Nx + i] = c2[1][((size_t)k * (Ny + 1) + Ny) * Nx + i] = 0.0;
         aeo_mg_config mc{};
         mc.nx = Nx; mc.ny = Ny; mc.nz = Nz;
         mc.dx = g.dx; mc.dy = g.dy; mc.dz = g.dz;
-        mc.bc_x = AEO_MG_PERIODIC; mc.bc_y = AEO_MG_PERIODIC;
+        mc.bc_x = open_x ? AEO_MG_NEUMANN : AEO_MG_PERIODIC;
+        mc.bc_y = open_y ? AEO_MG_NEUMANN : AEO_MG_PERIODIC;
         mc.bc_z = g.bc_z == 1 ? AEO_MG_NEUMANN : AEO_MG_PERIODIC;
         mc.precision = cfg.precision;
         mc.precond = AEO_PC_VCYCLE;
@@ -933,6 +949,76 @@ struct Core : CoreBase {
         return AEO_OK;
     }
 
+    // Open lateral faces (open_boundary_conditions,
+    // src/boundary_conditions/open_boundary.jl:532-638): the plane buffers in
+    // the layout of OpenSet (host FP64), per-field modes (0 plane, 1 mirror);
+    // the PCG operator is rebuilt with the Neumann condition on the open axes
+    // and the state's halos refilled.
+    aeo_status set_open(int ox, int oy, const double* xp, const double* yp, const int* modes) override {
+        if (!pcg) { fail("set_open: open faces need the PCG projection (solver = AEO_SOLVER_PCG)"); return AEO_ERR_STATE; }
+        if (anel || !uni) { fail("set_open: open faces are built on the uniform Boussinesq core"); return AEO_ERR_STATE; }
+        if (g.bc_z != 1) { fail("set_open: open lateral faces need walls in z"); return AEO_ERR_STATE; }
+        if (sgs) { fail("set_open: open faces are built without an SGS closure (c_s = 0)"); return AEO_ERR_STATE; }
+        if ((ox && !xp) || (oy && !yp) || ((ox || oy) && !modes)) { fail("set_open: NULL plane array"); return AEO_ERR_ARGUMENT; }
+        if (ox || oy)
+            for (int f = 0; f < 4; ++f)
+                if (modes[f] != 0 && !(f == 3 && modes[f] == 1)) {
+                    fail("set_open: the velocities take their planes (mode 0), theta its plane or the mirror (1)");
+                    return AEO_ERR_ARGUMENT;
+                }
+        CK(cudaStreamSynchronize(st));
+        drop_graphs();
+        const int H = AEO_H, NX = g.nx + 2 * H, NY = g.ny + 2 * H, NZ = g.nz + 2 * H, L = H + 1;
+        const size_t nxp = (size_t)8 * NZ * NY * L, nyp = (size_t)8 * NZ * L * NX;
+        if (!ob.xp) {
+            R *a = nullptr, *b = nullptr, *c = nullptr, *d = nullptr, *e = nullptr, *f = nullptr;
+            if (aeo_status x = alloc(&a, nxp)) return x;
+            if (aeo_status x = alloc(&b, nyp)) return x;
+            if (aeo_status x = alloc(&c, (size_t)g.ny * g.nz)) return x;
+            if (aeo_status x = alloc(&d, (size_t)g.ny * g.nz)) return x;
+            if (aeo_status x = alloc(&e, (size_t)g.nx * g.nz)) return x;
+            if (aeo_status x = alloc(&f, (size_t)g.nx * g.nz)) return x;
+            ob.xp = a; ob.yp = b; ob.bw = c; ob.be = d; ob.bs = e; ob.bn = f;
+        }
+        ob.L = L;
+        for (int f = 0; f < 4; ++f) ob.mode[f] = (ox || oy) ? modes[f] : 0;
+        // theta is stored as its deviation from th_off
+        auto conv = [&](const double* src, size_t n, size_t per_field) {
+            std::vector<R> out(n, R(0));
+            if (src)
+                for (size_t q = 0; q < n; ++q) out[q] = R(src[q] - (q / per_field == 3 ? th_off : 0.0));
+            return out;
+        };
+        std::vector<R> hx = conv(ox ? xp : nullptr, nxp, nxp / 4), hy = conv(oy ? yp : nullptr, nyp, nyp / 4);
+        std::vector<R> bw((size_t)g.ny * g.nz), be(bw.size()), bs((size_t)g.nx * g.nz), bn(bs.size());
+        for (int k = 0; k < g.nz; ++k) {
+            for (int j = 0; j < g.ny; ++j) {
+                bw[(size_t)k * g.ny + j] = hx[(((size_t)0 * NZ + k + H) * NY + j + H) * L + H];
+                be[(size_t)k * g.ny + j] = hx[(((size_t)1 * NZ + k + H) * NY + j + H) * L + 0];
+            }
+            for (int i = 0; i < g.nx; ++i) {
+                bs[(size_t)k * g.nx + i] = hy[(((size_t)2 * NZ + k + H) * L + H) * NX + i + H];
+                bn[(size_t)k * g.nx + i] = hy[(((size_t)3 * NZ + k + H) * L + 0) * NX + i + H];
+            }
+        }
+        CK(cudaMemcpy((void*)ob.xp, hx.data(), nxp * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy((void*)ob.yp, hy.data(), nyp * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy((void*)ob.bw, bw.data(), bw.size() * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy((void*)ob.be, be.data(), be.size() * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy((void*)ob.bs, bs.data(), bs.size() * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy((void*)ob.bn, bn.data(), bn.size() * sizeof(R), cudaMemcpyHostToDevice));
+        ob.ox = ox ? 1 : 0;
+        ob.oy = oy ? 1 : 0;
+        open_x = ox != 0;
+        open_y = oy != 0;
+        if (aeo_status e = make_pcg(h_ap[0].data(), h_ap[1].data(), h_ap[2].data())) return e;
+        R* f[4] = {P[cur][0], P[cur][1], P[cur][2], P[cur][3]};
+        int l[4] = {LOC_FX, LOC_FY, LOC_FZ, LOC_C};
+        if (aeo_status e = halo(f, l, 4)) return e;
+        CK(cudaStreamSynchronize(st));
+        return AEO_OK;
+    }
+
     aeo_status make_tensor_maps() {
         void* fn = nullptr;
         cudaDriverEntryPointQueryResult q;
@@ -965,6 +1051,37 @@ struct Core : CoreBase {
     unsigned gvec() const { return (unsigned)((g.nin / Vec16<R>::N + 255) / 256); }
 
     aeo_status halo(R* const* f, const int* loc, int nf) {
+        if (open_x || open_y) {
+            for (int b = 0; b < nf; b += 4) {
+                HaloSet<R> hs{};
+                int pid[4] = {-1, -1, -1, -1};
+                const int m = std::min(4, nf - b);
+                for (int q = 0; q < m; ++q) {
+                    hs.f[q] = f[b + q];
+                    hs.loc[q] = loc[b + q];
+                    for (int c = 0; c < 4; ++c)
+                        for (int s4 = 0; s4 < 4; ++s4)
+                            if (f[b + q] && f[b + q] == P[s4][c]) pid[q] = c;
+                    // the boundary face of the normal velocity (interior index 0)
+                    if (pid[q] == 0 && open_x) {
+                        open_face_kernel<R><<<dim3((unsigned)((g.ny + 127) / 128), (unsigned)g.nz), 128, 0, st>>>(
+                            g, f[b + q], ob, 0);
+                        CKL();
+                    }
+                    if (pid[q] == 1 && open_y) {
+                        open_face_kernel<R><<<dim3((unsigned)((g.nx + 127) / 128), (unsigned)g.nz), 128, 0, st>>>(
+                            g, f[b + q], ob, 1);
+                        CKL();
+                    }
+                }
+                hs.nf = m;
+                const long long n = shell_count(g);
+                open_halo_fill_kernel<R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
+                    g, hs, ob, make_int4(pid[0], pid[1], pid[2], pid[3]));
+                CKL();
+            }
+            return AEO_OK;
+        }
         HaloSet<R> hs{};
         for (int q = 0; q < nf; ++q) { hs.f[q] = f[q]; hs.loc[q] = loc[q]; }
         hs.nf = nf;
@@ -1093,7 +1210,9 @@ struct Core : CoreBase {
             else if (anel && uni) cc_div_kernel<R, true, true><<<gb, 256, 0, st>>>(g, Q[0], Q[1], Q[2], apx, apy, apz, mg_b);
             else if (anel) cc_div_kernel<R, true, false><<<gb, 256, 0, st>>>(g, Q[0], Q[1], Q[2], apx, apy, apz, mg_b);
             else if (!uni) cc_div_kernel<R, false, false><<<gb, 256, 0, st>>>(g, Q[0], Q[1], Q[2], apx, apy, apz, mg_b);
-            else cc_div_kernel<R><<<gb, 256, 0, st>>>(g, Q[0], Q[1], Q[2], apx, apy, apz, mg_b);
+            else cc_div_kernel<R><<<gb, 256, 0, st>>>(g, Q[0], Q[1], Q[2], apx, apy, apz, mg_b,
+                                                       open_x ? ob.bw : nullptr, open_x ? ob.be : nullptr,
+                                                       open_y ? ob.bs : nullptr, open_y ? ob.bn : nullptr);
             CKL();
             mark(AEO_K_DIV_FFTX);
             if (aeo_status e = aeo_mg_enqueue(mg, st)) {
@@ -1179,7 +1298,7 @@ struct Core : CoreBase {
             if (uni)
                 cc_correct_kernel<R, true><<<(unsigned)((g.nin + 255) / 256), 256, 0, st>>>(
                     g, Q[0], Q[1], Q[2], mg_x, apx, apy, apz, u0[0], u0[1], u0[2], out[0], out[1], out[2], pres, dtp,
-                    ca, cb, stage);
+                    ca, cb, stage, open_x ? ob.bw : nullptr, open_y ? ob.bs : nullptr);
             else
                 cc_correct_kernel<R, false><<<(unsigned)((g.nin + 255) / 256), 256, 0, st>>>(
                     g, Q[0], Q[1], Q[2], mg_x, apx, apy, apz, u0[0], u0[1], u0[2], out[0], out[1], out[2], pres, dtp,
@@ -2134,6 +2253,12 @@ aeo_status aeo_pcg_stats(aeo_sim* h, int32_t* iterations, int32_t* status, doubl
 aeo_status aeo_pcg_set_learned(aeo_sim* h, struct aeo_unet* net, double stagnation) {
     ENTER(h);
     return h->core->pcg_set_learned(net, stagnation);
+}
+
+aeo_status aeo_set_open(aeo_sim* h, int32_t open_x, int32_t open_y, const double* x_planes, const double* y_planes,
+                        const int32_t* modes) {
+    ENTER(h);
+    return h->core->set_open(open_x, open_y, x_planes, y_planes, modes);
 }
 
 aeo_status aeo_pcg_harvest(aeo_sim* h, int32_t cap, double* b, double* x, double* r_hist, double* x_hist,

@@ -381,6 +381,26 @@ aeo_status aeo_set_pcg(aeo_sim* h, const double* ax, const double* ay, const dou
  * ||r||, ||b - mean(b)||); synchronises the handle's stream */
 aeo_status aeo_pcg_stats(aeo_sim* h, int32_t* iterations, int32_t* status, double* residual, double* bnorm);
 aeo_status aeo_pcg_set_learned(aeo_sim* h, struct aeo_unet* net, double stagnation);
+/* Open lateral faces: Dirichlet halos from boundary data, the replacement of
+ * OpenBoundary / open_boundary_conditions(mesh, data; x, y, ...) and its halo
+ * fills (src/boundary_conditions/open_boundary.jl:485-638, :722-807).
+ * open_x / open_y open both faces of an axis (the other axis stays
+ * periodic); bottom and top stay walls.  x_planes: [field][side][NZ][NY][H+1],
+ * y_planes: [field][side][NZ][H+1][NX] (FP64; field u, v, w, theta; side 0
+ * west/south, 1 east/north; NX, NY, NZ the storage extents Nx+2H, Ny+2H,
+ * Nz+2H; layer = storage index along the face normal on the low side, that
+ * index - (H + N) on the high side, so the low side's layer H is the normal
+ * velocity's boundary face, interior index 0): the data at those storage
+ * points with the normal velocities already mass-corrected
+ * (correct_boundary_mass_flux!, :1024-1083).  modes[4]: 0 the field takes its
+ * plane, 1 the zero-gradient mirror (theta only: scalar_halo = :mirror); every
+ * other field (the pressure) takes the mirror, so the projection's phi has
+ * d phi / dn = 0 there and leaves the prescribed normal velocity unchanged.
+ * Needs solver = AEO_SOLVER_PCG on the uniform Boussinesq core with walls in z
+ * and no SGS closure; the planes are steady (the step does not refresh them).
+ * open_x = open_y = 0 closes the faces again. */
+aeo_status aeo_set_open(aeo_sim* h, int32_t open_x, int32_t open_y, const double* x_planes, const double* y_planes,
+                        const int32_t* modes);
 /* Residual -> error pairs from the run's own snapshots (no reference
  * counterpart; it feeds the learned preconditioner): b receives the
  * right-hand side of the last projection's solve (the predictor's cut-cell

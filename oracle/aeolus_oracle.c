@@ -90,6 +90,13 @@ struct oc_sim {
     double *tke_e, *tke_k2, *tke_tend, *tke_new;
     double tke_ce0, tke_ce1, tke_cl;
     int tke_exact;
+    /* open lateral faces: the plane buffers (x: [f][side][NZ][NY][L], y:
+     * [f][side][NZ][L][NX], f = u, v, w, theta), the per-field modes */
+    int open_x, open_y, oL;
+    double *oxp, *oyp;
+    int omode[4];
+    double cg_tol;
+    int cg_maxit;
 };
 
 #define ID(s, i, j, k) ((int64_t)(i) + (int64_t)(s)->NX * ((int64_t)(j) + (int64_t)(s)->NY * (int64_t)(k)))
@@ -265,9 +272,38 @@ static inline double m_filter(const oc_sim* s, int k) { return s->uniform ? s->d
 /* src/BoundaryConditions.jl:228-258): x, then y, then z.                     */
 /* ------------------------------------------------------------------------- */
 
+/* The plane of field d on the open faces (u, v, w, theta with mode 0), or -1:
+ * the mirror (_plane_name / _fill_open_face!,
+ * src/boundary_conditions/open_boundary.jl:726-772). */
+static int open_pid(const oc_sim* s, const double* d) {
+    int f = d == s->u ? 0 : d == s->v ? 1 : d == s->w ? 2 : d == s->th ? 3 : -1;
+    return f >= 0 && s->omode[f] == 0 ? f : -1;
+}
+
 static void fill_halos(oc_sim* s, double* d, int loc) {
     int NX = s->NX, NY = s->NY, NZ = s->NZ;
     int Hx = s->p.hx, Hy = s->p.hy, Hz = s->p.hz, Nx = s->p.nx, Ny = s->p.ny, Nz = s->p.nz;
+    int pid = open_pid(s, d), L = s->oL;
+    if (s->open_x) {
+        /* x: open faces (_fill_x!, :781-785): the plane's slab -- with the
+         * boundary face of u on the west (interior 0) -- or the mirror */
+        int nw = pid == 0 ? Hx + 1 : Hx;
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int k = 0; k < NZ; ++k)
+            for (int j = 0; j < NY; ++j) {
+                if (pid >= 0) {
+                    const double* pw = s->oxp + (((int64_t)(pid * 2 + 0) * NZ + k) * NY + j) * L;
+                    const double* pe = s->oxp + (((int64_t)(pid * 2 + 1) * NZ + k) * NY + j) * L;
+                    for (int l = 0; l < nw; ++l) A(d, l, j, k) = pw[l];
+                    for (int l = 0; l < Hx; ++l) A(d, Hx + Nx + l, j, k) = pe[l];
+                } else {
+                    for (int h = 1; h <= Hx; ++h) {
+                        A(d, Hx - h, j, k) = A(d, Hx + h - 1, j, k);
+                        A(d, Hx + Nx + h - 1, j, k) = A(d, Hx + Nx - h, j, k);
+                    }
+                }
+            }
+    } else {
     /* x: periodic */
 #pragma omp parallel for collapse(2) schedule(static)
     for (int k = 0; k < NZ; ++k)
@@ -276,6 +312,25 @@ static void fill_halos(oc_sim* s, double* d, int loc) {
                 A(d, h - 1, j, k) = A(d, Nx + h - 1, j, k);
                 A(d, Hx + Nx + h - 1, j, k) = A(d, Hx + h - 1, j, k);
             }
+    }
+    if (s->open_y) {
+        int ns = pid == 1 ? Hy + 1 : Hy;
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int k = 0; k < NZ; ++k)
+            for (int i = 0; i < NX; ++i) {
+                if (pid >= 0) {
+                    for (int l = 0; l < ns; ++l)
+                        A(d, i, l, k) = s->oyp[(((int64_t)(pid * 2 + 0) * NZ + k) * L + l) * NX + i];
+                    for (int l = 0; l < Hy; ++l)
+                        A(d, i, Hy + Ny + l, k) = s->oyp[(((int64_t)(pid * 2 + 1) * NZ + k) * L + l) * NX + i];
+                } else {
+                    for (int h = 1; h <= Hy; ++h) {
+                        A(d, i, Hy - h, k) = A(d, i, Hy + h - 1, k);
+                        A(d, i, Hy + Ny + h - 1, k) = A(d, i, Hy + Ny - h, k);
+                    }
+                }
+            }
+    } else {
     /* y: periodic */
 #pragma omp parallel for collapse(2) schedule(static)
     for (int k = 0; k < NZ; ++k)
@@ -284,6 +339,7 @@ static void fill_halos(oc_sim* s, double* d, int loc) {
                 A(d, i, h - 1, k) = A(d, i, Ny + h - 1, k);
                 A(d, i, Hy + Ny + h - 1, k) = A(d, i, Hy + h - 1, k);
             }
+    }
     /* z */
     if (s->p.bc_z == OC_BC_PERIODIC) {
 #pragma omp parallel for schedule(static)
@@ -1646,8 +1702,9 @@ static void cc_correct(oc_sim* s, double dt, int stage, double ca, double cb, in
                 int64_t qi = i + (int64_t)Nx * (j + (int64_t)Ny * k);
                 int64_t q = ID(s, i + Hx, j + Hy, k + Hz);
                 double pc = phi[qi];
-                double pw = phi[i > 0 ? qi - 1 : qi + Nx - 1];
-                double ps = phi[j > 0 ? qi - Nx : qi + (int64_t)(Ny - 1) * Nx];
+                /* phi's halo is the mirror on an open face (d phi / dn = 0) */
+                double pw = i > 0 ? phi[qi - 1] : (s->open_x ? pc : phi[qi + Nx - 1]);
+                double ps = j > 0 ? phi[qi - Nx] : (s->open_y ? pc : phi[qi + (int64_t)(Ny - 1) * Nx]);
                 double pb = phi[k > 0 ? qi - pl : (P->bc_z == OC_BC_PERIODIC ? qi + (int64_t)(Nz - 1) * pl : qi)];
                 double aw = s->apx[(int64_t)(Nx + 1) * (j + (int64_t)Ny * k) + i];
                 double as = s->apy[(int64_t)Nx * (j + (int64_t)(Ny + 1) * k) + i];
@@ -2345,6 +2402,13 @@ int oc_set_apertures(oc_sim* s, const double* ax, const double* ay, const double
         }
     for (int d = 0; d < 3; ++d)
         for (int64_t q = 0; q < n[d]; ++q) c2[d][q] = a[d][q] * a[d][q];
+    /* open faces: no coupling across (the Neumann condition of phi) */
+    if (s->open_x)
+        for (int64_t r = 0; r < (int64_t)Ny * Nz; ++r) c2[0][r * (Nx + 1)] = c2[0][r * (Nx + 1) + Nx] = 0.0;
+    if (s->open_y)
+        for (int k = 0; k < Nz; ++k)
+            for (int i = 0; i < Nx; ++i)
+                c2[1][(int64_t)k * (Ny + 1) * Nx + i] = c2[1][((int64_t)k * (Ny + 1) + Ny) * Nx + i] = 0.0;
     if (P->core == OC_CORE_ANELASTIC || !s->uniform) {
         /* the symmetric form of the density-weighted operator on the column:
          * W_c a^2 dz_c / h_z on x and y faces, W_f a^2 h_z / dz_f on z faces */
@@ -2363,7 +2427,8 @@ int oc_set_apertures(oc_sim* s, const double* ax, const double* ay, const double
     }
     ocg* cg = NULL;
     if (!bad) {
-        ocg_params prm = {Nx, Ny, Nz, s->dx, s->dy, s->dz, OCG_BC_PERIODIC, OCG_BC_PERIODIC,
+        ocg_params prm = {Nx, Ny, Nz, s->dx, s->dy, s->dz, s->open_x ? OCG_BC_NEUMANN : OCG_BC_PERIODIC,
+                          s->open_y ? OCG_BC_NEUMANN : OCG_BC_PERIODIC,
                           P->bc_z == OC_BC_WALL ? OCG_BC_NEUMANN : OCG_BC_PERIODIC, tol, maxit,
                           2, 2, 50, 4, 1, OCG_PC_VCYCLE};
         cg = ocg_create(&prm, c2[0], c2[1], c2[2]);
@@ -2377,7 +2442,47 @@ int oc_set_apertures(oc_sim* s, const double* ax, const double* ay, const double
     if (s->cg) ocg_destroy(s->cg);
     s->apx = a[0]; s->apy = a[1]; s->apz = a[2];
     s->cg = cg;
+    s->cg_tol = tol;
+    s->cg_maxit = maxit;
     memset(&s->cg_st, 0, sizeof(s->cg_st));
+    return 0;
+}
+
+/* Open lateral faces (open_boundary_conditions and the halo fills of
+ * src/boundary_conditions/open_boundary.jl:532-807): copies of the planes
+ * (the layout of aeo_set_open), the modes; the CG rebuilt on the domain's
+ * apertures with the Neumann condition on the open axes.  open_x = open_y = 0
+ * closes them. */
+int oc_set_open(oc_sim* s, int open_x, int open_y, const double* xp, const double* yp, const int* modes) {
+    const oc_params* P = &s->p;
+    if (P->solver != OC_SOLVER_PCG || P->core == OC_CORE_ANELASTIC || !s->uniform || P->bc_z != OC_BC_WALL ||
+        P->c_s != 0.0)
+        return -1;
+    if ((open_x && !xp) || (open_y && !yp) || ((open_x || open_y) && !modes)) return -1;
+    int L = (P->hx > P->hy ? P->hx : P->hy) + 1;
+    int64_t nxp = (int64_t)8 * s->NZ * s->NY * L, nyp = (int64_t)8 * s->NZ * L * s->NX;
+    free(s->oxp); free(s->oyp);
+    s->oxp = dalloc(nxp);
+    s->oyp = dalloc(nyp);
+    if (open_x) memcpy(s->oxp, xp, sizeof(double) * nxp);
+    if (open_y) memcpy(s->oyp, yp, sizeof(double) * nyp);
+    for (int f = 0; f < 4; ++f) s->omode[f] = (open_x || open_y) ? modes[f] : 0;
+    s->oL = L;
+    s->open_x = open_x != 0;
+    s->open_y = open_y != 0;
+    /* the operator on the current apertures (the wall faces already closed) */
+    int64_t n[3] = {(int64_t)(P->nx + 1) * P->ny * P->nz, (int64_t)P->nx * (P->ny + 1) * P->nz,
+                    (int64_t)P->nx * P->ny * (P->nz + 1)};
+    double* a[3];
+    for (int d = 0; d < 3; ++d) {
+        const double* src = d == 0 ? s->apx : d == 1 ? s->apy : s->apz;
+        a[d] = dalloc(n[d]);
+        for (int64_t q = 0; q < n[d]; ++q) a[d][q] = src ? src[q] : 1.0;
+    }
+    int r = oc_set_apertures(s, a[0], a[1], a[2], s->cg ? s->cg_tol : 1e-8, s->cg ? s->cg_maxit : 200);
+    for (int d = 0; d < 3; ++d) free(a[d]);
+    if (r) return r;
+    oc_fill_state_halos(s);
     return 0;
 }
 
@@ -2398,7 +2503,7 @@ void oc_destroy(oc_sim* s) {
                       s->lower, s->upper, s->hw, s->meas, s->iota, s->gauge};
     for (size_t q = 0; q < sizeof(ptrs) / sizeof(ptrs[0]); ++q) free(ptrs[q]);
     free(s->hat); free(s->twx);
-    free(s->apx); free(s->apy); free(s->apz); free(s->cgx); free(s->ibm);
+    free(s->apx); free(s->apy); free(s->apz); free(s->cgx); free(s->ibm); free(s->oxp); free(s->oyp);
     for (int f = 0; f < 10; ++f) free(s->dyn[f]);
     free(s->dyn_lm); free(s->dyn_mm); free(s->cs2); free(s->amd_bg);
     free(s->lag_ilm); free(s->lag_imm); free(s->lag_up); free(s->lag_vp); free(s->lag_wp);

@@ -106,6 +106,8 @@ int oc_set_sgs_state(oc_sim* s, const double* in);
 int oc_set_ibm(oc_sim* s, const unsigned char* mask, double tau);
 /* iterations, status (mgpcg_oracle.h OCG_*), ||r|| and ||b|| of the last solve */
 int oc_pcg_stats(const oc_sim* s, int* iterations, int* status, double* residual, double* bnorm);
+/* open lateral faces: planes in the layout of aeo_set_open (FP64), modes[4] */
+int oc_set_open(oc_sim* s, int open_x, int open_y, const double* xp, const double* yp, const int* modes);
 void oc_set_threads(int n);
 /* advect_positive! (src/AdvectionSchemes.jl:1100-1160): add (accumulate) or
  * write -div(u phi) with the positivity limiter; storage arrays of the

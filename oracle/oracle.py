@@ -85,6 +85,7 @@ def load():
     lib.oc_set_ibm.argtypes = [P, C.c_void_p, C.c_double]
     lib.oc_advect_positive.argtypes = [P, _D, _D, _D, _D, _D, C.c_double, C.c_int, C.c_int]
     lib.oc_set_apertures.argtypes = [P, _D, _D, _D, C.c_double, C.c_int]
+    lib.oc_set_open.argtypes = [P, C.c_int, C.c_int, _D, _D, C.POINTER(C.c_int)]
     lib.oc_set_sgs_buoyancy.argtypes = [P, _D]
     lib.oc_set_lagrangian.argtypes = [P, C.c_double, C.c_double, C.c_double]
     lib.oc_set_tke.argtypes = [P, C.c_double, C.c_double, C.c_double, C.c_int]
@@ -293,6 +294,20 @@ class OracleSimulation:
             ptrs = tuple(_p(x) for x in a)
         if self._lib.oc_set_apertures(self._h, *ptrs, float(tol), int(maxit)) != 0:
             raise ValueError("oracle: set_pcg rejected (solver, tolerance or apertures)")
+
+    def set_open_boundaries(self, obc=None):
+        """Open lateral faces from an OpenBoundarySet (None closes them)."""
+        if obc is None:
+            if self._lib.oc_set_open(self._h, 0, 0, None, None, None) != 0:
+                raise ValueError("oracle: set_open rejected")
+            return
+        xp, yp, modes = obc.packed()
+        m = np.ascontiguousarray(modes, dtype=np.int32)
+        self._open = (xp, yp, m)
+        if self._lib.oc_set_open(self._h, int(obc.open_x), int(obc.open_y), _p(xp), _p(yp),
+                                 m.ctypes.data_as(C.POINTER(C.c_int))) != 0:
+            raise ValueError("oracle: set_open rejected (needs the PCG solver on the uniform Boussinesq core, "
+                             "walls in z, no SGS closure)")
 
     def pcg_stats(self):
         it, stt = C.c_int(), C.c_int()
