@@ -66,6 +66,7 @@ struct Geo {
     long long sy, sz;      // padded strides of j and k
     long long nin;         // nx*ny*nz
     int bc_z;              // 0 periodic, 1 wall
+    int ox, oy;            // open x / y faces (aeo_set_open): fields without planes take the mirror there
     int uniform;           // 1: uniform z metrics
     double dx, dy, dz;
     double idx, idy, idx2, idy2, idz, idz2, delta_u;
@@ -96,6 +97,14 @@ struct Geo {
     const void* tke;
     double tke_ck, tke_cl, tke_delta, tke_bg;
 };
+
+// The cell whose value a closure field takes at (i, j) on open faces: the
+// zero-gradient mirror of the reference's halo fill
+// (src/boundary_conditions/open_boundary.jl:54-58) across an open x or y face.
+__device__ __forceinline__ int open_src(int open, int i, int n) {
+    if (!open) return i;
+    return i < 0 ? -1 - i : (i >= n ? 2 * n - 1 - i : i);
+}
 
 __device__ __forceinline__ long long pidx(const Geo& g, int i, int j, int k) {
     return (long long)(i + AEO_HX) + (long long)(j + AEO_H) * g.sy + (long long)(k + AEO_H) * g.sz;

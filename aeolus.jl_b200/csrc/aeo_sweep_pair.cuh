@@ -119,36 +119,43 @@ __device__ __forceinline__ void pair_nut_plane(const Met<float, UNI>& m, const S
         int cj, pc;
         if (e < S::TXT * S::NPH) { cj = e >> 5; pc = (e & 31) + 1; }
         else { const int x = e - S::TXT * S::NPH; cj = x >> 1; pc = (x & 1) ? S::NPAIR - 1 : 0; }
-        // the pair's first cell sits at tile x = 2 pc - 2, plane x = 2 pc + 2
-        const int b = (cj - 1 + S::HH) * S::PW + 2 * pc + 2;
+        // the pair's first cell sits at tile x = 2 pc - 2, plane x = 2 pc + 2;
+        // open faces: a pair beyond one takes the mirrored pair, reversed
+        // (cells -2, -1 the values of 1, 0; nx, nx + 1 those of nx - 1, nx - 2)
+        int gx = i0 + 2 * pc - 2;
+        bool rev = false;
+        if (g.ox && (gx < 0 || gx >= g.nx)) { gx = gx < 0 ? -2 - gx : 2 * g.nx - 2 - gx; rev = true; }
+        const int gy = open_src(g.oy, j0 + cj - 1, g.ny);
+        const int b = (gy - j0 + S::HH) * S::PW + (gx - i0) + 4;
         const float* q[3] = {sp[0] + b, sp[1] + b, sp[2] + b};
         const PairAcc<1, S::PW, 0> Uq{q};
         const PairAcc<1, S::PW, S::PSZA> Vq{q};
         const PairAcc<1, S::PW, 2 * S::PSZA> Wq{q};
         if constexpr (CLOS == 2) {
             // the pair's cells: global x = i0 + 2 pc - 2 (even), y = j0 + cj - 1
-            const F2 c = a.cs2f ? F2(*reinterpret_cast<const float2*>(a.cs2f + pidx(g, i0 + 2 * pc - 2, j0 + cj - 1, L))) *
+            const F2 c = a.cs2f ? F2(*reinterpret_cast<const float2*>(a.cs2f + pidx(g, gx, gy, L))) *
                                       F2(float(a.dyn_d2))
                                 : F2(float(dyn_cs2_at(g, a.cs2, L) * a.dyn_d2));
             const F2 nv = c * strain_at<R, UNI>(m, g, L, Uq, Vq, Wq, (F2*)nullptr);
-            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nv.v;
+            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = rev ? make_float2(nv.v.y, nv.v.x) : nv.v;
         } else if constexpr (CLOS == 1) {
             const PairAcc<1, S::PW, 3 * S::PSZA> Tq{q};
             const NuKappa<F2> nk = amd_point<R, UNI>(m, g, L, R(a.c_s), m.lv(LV_BGC, L), a.pr_t, Uq, Vq, Wq, Tq);
-            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nk.nu.v;
-            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc + S::KT_OFS) = nk.ka.v;
+            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = rev ? make_float2(nk.nu.v.y, nk.nu.v.x) : nk.nu.v;
+            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc + S::KT_OFS) =
+                rev ? make_float2(nk.ka.v.y, nk.ka.v.x) : nk.ka.v;
         } else if constexpr (CLOS == 3) {
             // the TKE closure, cell by cell: the pair's cells x = i0 + 2 pc - 2 (+1), y = j0 + cj - 1
             const PairAcc<1, S::PW, 3 * S::PSZA> Tq{q};
             const F2 lo = Tq(0, 0, -1), c = Tq(0, 0, 0), hi = Tq(0, 0, 1);
-            const int gi = i0 + 2 * pc - 2, gj = j0 + cj - 1;
-            const NuKappa<float> n0 = tke_point<float>(g, gi, gj, L, lo.v.x, c.v.x, hi.v.x);
-            const NuKappa<float> n1 = tke_point<float>(g, gi + 1, gj, L, lo.v.y, c.v.y, hi.v.y);
-            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = make_float2(n0.nu, n1.nu);
-            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc + S::KT_OFS) = make_float2(n0.ka, n1.ka);
+            const NuKappa<float> n0 = tke_point<float>(g, gx, gy, L, lo.v.x, c.v.x, hi.v.x);
+            const NuKappa<float> n1 = tke_point<float>(g, gx + 1, gy, L, lo.v.y, c.v.y, hi.v.y);
+            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = rev ? make_float2(n1.nu, n0.nu) : make_float2(n0.nu, n1.nu);
+            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc + S::KT_OFS) =
+                rev ? make_float2(n1.ka, n0.ka) : make_float2(n0.ka, n1.ka);
         } else {
             const F2 nv = smag_point<R, UNI>(m, g, L, R(a.c_s), Uq, Vq, Wq);
-            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = nv.v;
+            *reinterpret_cast<float2*>(np + cj * S::NPW + 2 * pc) = rev ? make_float2(nv.v.y, nv.v.x) : nv.v;
         }
     }
 }

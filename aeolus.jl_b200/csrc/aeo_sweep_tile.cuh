@@ -236,13 +236,15 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
                     int cj, ci;
                     if (e < S::TX * S::NPH) { cj = e >> 5; ci = (e & 31) + 1; }
                     else { const int x = e - S::TX * S::NPH; cj = x >> 1; ci = (x & 1) ? S::NPW - 1 : 0; }
-                    const int b = (cj - 1 + S::HH) * S::PW + (ci - 1 + 4);
+                    // open faces: a ring cell beyond one takes the mirrored cell's value
+                    const int gi = open_src(g.ox, i0 + ci - 1, g.nx), gj = open_src(g.oy, j0 + cj - 1, g.ny);
+                    const int b = (gj - j0 + S::HH) * S::PW + (gi - i0 + 4);
                     const R* q[3] = {sp[0] + b, sp[1] + b, sp[2] + b};
                     const SmAcc<R, 1, S::PW, 0> Uq{q};
                     const SmAcc<R, 1, S::PW, S::PSZA> Vq{q};
                     const SmAcc<R, 1, S::PW, 2 * S::PSZA> Wq{q};
                     if constexpr (CLOS == 2) {
-                        const R c = R(dyn_cs2_cell(g, a.cs2, a.cs2f, i0 + ci - 1, j0 + cj - 1, L) * a.dyn_d2);
+                        const R c = R(dyn_cs2_cell(g, a.cs2, a.cs2f, gi, gj, L) * a.dyn_d2);
                         np[cj * S::NPW + ci] = c * strain_at<R, UNI>(m, g, L, Uq, Vq, Wq, (R*)nullptr);
                     } else if constexpr (CLOS == 1) {
                         const SmAcc<R, 1, S::PW, 3 * S::PSZA> Tq{q};
@@ -251,7 +253,7 @@ __global__ void __launch_bounds__(256) sweep_tile_kernel(const __grid_constant__
                         np[cj * S::NPW + ci + S::KT_OFS] = nk.ka;
                     } else if constexpr (CLOS == 3) {
                         const SmAcc<R, 1, S::PW, 3 * S::PSZA> Tq{q};
-                        const NuKappa<R> nk = tke_point<R>(g, i0 + ci - 1, j0 + cj - 1, L, Tq(0, 0, -1), Tq(0, 0, 0), Tq(0, 0, 1));
+                        const NuKappa<R> nk = tke_point<R>(g, gi, gj, L, Tq(0, 0, -1), Tq(0, 0, 0), Tq(0, 0, 1));
                         np[cj * S::NPW + ci] = nk.nu;
                         np[cj * S::NPW + ci + S::KT_OFS] = nk.ka;
                     } else {

@@ -958,7 +958,10 @@ struct Core : CoreBase {
         if (!pcg) { fail("set_open: open faces need the PCG projection (solver = AEO_SOLVER_PCG)"); return AEO_ERR_STATE; }
         if (anel || !uni) { fail("set_open: open faces are built on the uniform Boussinesq core"); return AEO_ERR_STATE; }
         if (g.bc_z != 1) { fail("set_open: open lateral faces need walls in z"); return AEO_ERR_STATE; }
-        if (sgs) { fail("set_open: open faces are built without an SGS closure (c_s = 0)"); return AEO_ERR_STATE; }
+        if (sgs && cfg.sgs_model >= AEO_SGS_DYNAMIC) {
+            fail("set_open: open faces take the static SGS closures (Smagorinsky, Vreman, sigma, AMD)");
+            return AEO_ERR_STATE;
+        }
         if ((ox && !xp) || (oy && !yp) || ((ox || oy) && !modes)) { fail("set_open: NULL plane array"); return AEO_ERR_ARGUMENT; }
         if (ox || oy)
             for (int f = 0; f < 4; ++f)
@@ -1011,6 +1014,8 @@ struct Core : CoreBase {
         ob.oy = oy ? 1 : 0;
         open_x = ox != 0;
         open_y = oy != 0;
+        g.ox = ob.ox;     // the sweeps' closure fields take the mirror across open faces
+        g.oy = ob.oy;
         if (aeo_status e = make_pcg(h_ap[0].data(), h_ap[1].data(), h_ap[2].data())) return e;
         R* f[4] = {P[cur][0], P[cur][1], P[cur][2], P[cur][3]};
         int l[4] = {LOC_FX, LOC_FY, LOC_FZ, LOC_C};

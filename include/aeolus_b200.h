@@ -396,8 +396,10 @@ aeo_status aeo_pcg_set_learned(aeo_sim* h, struct aeo_unet* net, double stagnati
  * plane, 1 the zero-gradient mirror (theta only: scalar_halo = :mirror); every
  * other field (the pressure) takes the mirror, so the projection's phi has
  * d phi / dn = 0 there and leaves the prescribed normal velocity unchanged.
- * Needs solver = AEO_SOLVER_PCG on the uniform Boussinesq core with walls in z
- * and no SGS closure; the planes are steady (the step does not refresh them).
+ * Needs solver = AEO_SOLVER_PCG on the uniform Boussinesq core with walls in z;
+ * of the SGS closures the static ones (Smagorinsky, Vreman, sigma, AMD), whose
+ * nu_t takes the mirror across the open faces; the planes are steady (the
+ * step does not refresh them).
  * open_x = open_y = 0 closes the faces again. */
 aeo_status aeo_set_open(aeo_sim* h, int32_t open_x, int32_t open_y, const double* x_planes, const double* y_planes,
                         const int32_t* modes);

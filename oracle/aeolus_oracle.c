@@ -2456,7 +2456,8 @@ int oc_set_apertures(oc_sim* s, const double* ax, const double* ay, const double
 int oc_set_open(oc_sim* s, int open_x, int open_y, const double* xp, const double* yp, const int* modes) {
     const oc_params* P = &s->p;
     if (P->solver != OC_SOLVER_PCG || P->core == OC_CORE_ANELASTIC || !s->uniform || P->bc_z != OC_BC_WALL ||
-        P->c_s != 0.0)
+        (P->c_s != 0.0 && (P->sgs_model == OC_SGS_DYNAMIC || P->sgs_model == OC_SGS_DYNAMIC_LOCAL ||
+                           P->sgs_model == OC_SGS_LAGRANGIAN || P->sgs_model == OC_SGS_TKE)))
         return -1;
     if ((open_x && !xp) || (open_y && !yp) || ((open_x || open_y) && !modes)) return -1;
     int L = (P->hx > P->hy ? P->hx : P->hy) + 1;

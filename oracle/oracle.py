@@ -307,7 +307,7 @@ class OracleSimulation:
         if self._lib.oc_set_open(self._h, int(obc.open_x), int(obc.open_y), _p(xp), _p(yp),
                                  m.ctypes.data_as(C.POINTER(C.c_int))) != 0:
             raise ValueError("oracle: set_open rejected (needs the PCG solver on the uniform Boussinesq core, "
-                             "walls in z, no SGS closure)")
+                             "walls in z, a static SGS closure if any)")
 
     def pcg_stats(self):
         it, stt = C.c_int(), C.c_int()

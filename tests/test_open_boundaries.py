@@ -15,9 +15,11 @@ CPU (host and oracle):
   matching data stays uniform over steps (the stepped check the reference
   describes and cut from its suite, :1-10).
 GPU (-m gpu): the CUDA step with open x, and open x and y, over floor-standing
-boxes matches the oracle (FP64, relative L2 <= 1e-10 per field after 3
-steps at tol 1e-12; FP32-mixed within 1e-5 of FP64), keeps the boundary
-faces and the uniform wind."""
+boxes, with and without Smagorinsky (whose eddy viscosity takes the mirror
+across open faces, as the reference's nu_t halo fill gives it), matches the
+oracle (FP64, relative L2 <= 1e-10 per field after 3 steps at tol 1e-12;
+FP32-mixed within 1e-5 of FP64, the paired FP32 sweep included), keeps the
+boundary faces and the uniform wind."""
 import numpy as np
 import pytest
 
@@ -105,8 +107,8 @@ def start_state(g, seed, fluid):
     return u, v, w, th
 
 
-def spec(g, advection="centred", precision="fp64"):
-    return CoreSpec(grid=g, nu=1e-3, theta0=300.0, advection=advection, solver="pcg", precision=precision)
+def spec(g, advection="centred", precision="fp64", c_s=0.0):
+    return CoreSpec(grid=g, nu=1e-3, theta0=300.0, advection=advection, solver="pcg", precision=precision, c_s=c_s)
 
 
 def open_divergence(g, ap, u, v, w):
@@ -129,7 +131,7 @@ def test_oracle_open_projection_keeps_the_faces_and_the_constraint():
     g, geom, ap = box_case()
     fluid = (~geom.is_solid[g.interior]).astype(float)
     obc = open_boundary_conditions(g, inflow(), x="open", y="periodic")
-    o = OracleSimulation(spec(g))
+    o = OracleSimulation(spec(g, c_s=0.17))
     o.set_pcg(ap, tol=1e-12, maxit=500)
     o.set_open_boundaries(obc)
     o.set_state(*start_state(g, 5, fluid))
@@ -172,14 +174,16 @@ def rel_l2(a, b, g):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("y,advection", [("periodic", "centred"), ("open", "weno_js5")])
-def test_open_step_matches_the_oracle(y, advection):
+@pytest.mark.parametrize("y,advection,c_s", [("periodic", "centred", 0.0), ("open", "weno_js5", 0.0),
+                                             ("open", "centred", 0.17), ("periodic", "weno_js5", 0.17)])
+def test_open_step_matches_the_oracle(y, advection, c_s):
+    # with Smagorinsky the eddy viscosity takes the mirror across the open faces
     from aeolus_b200.simulation import Simulation
     from oracle.oracle import OracleSimulation
     g, geom, ap = box_case()
     fluid = (~geom.is_solid[g.interior]).astype(float)
     obc = open_boundary_conditions(g, inflow(), x="open", y=y)
-    sp = spec(g, advection)
+    sp = spec(g, advection, c_s=c_s)
     gpu, ora = Simulation(sp), OracleSimulation(sp)
     st = start_state(g, 7, fluid)
     for s in (gpu, ora):
@@ -202,7 +206,9 @@ def test_open_step_matches_the_oracle(y, advection):
 
 
 @pytest.mark.gpu
-def test_open_step_fp32_mixed_close_to_fp64():
+@pytest.mark.parametrize("advection,c_s", [("weno_js5", 0.0), ("centred", 0.17)])
+def test_open_step_fp32_mixed_close_to_fp64(advection, c_s):
+    # FP32 centred with Smagorinsky runs the paired sweep
     from aeolus_b200.simulation import Simulation
     g, geom, ap = box_case(3)
     fluid = (~geom.is_solid[g.interior]).astype(float)
@@ -210,7 +216,7 @@ def test_open_step_fp32_mixed_close_to_fp64():
     st = start_state(g, 9, fluid)
     out = {}
     for prec in ("fp64", "fp32_mixed"):
-        s = Simulation(spec(g, "weno_js5", prec))
+        s = Simulation(spec(g, advection, prec, c_s))
         s.set_pcg(ap, tol=1e-10, maxit=500)
         s.set_open_boundaries(obc)
         s.set_state(*st)
