@@ -22,11 +22,15 @@ net boundary flux vanishes.
 Built here: open x and/or y faces over a wall bottom and a wall (rigid-lid)
 top, on the uniform Boussinesq core with the PCG projection; steady data
 (`ProfileBoundaryData`, :336-408, and `FunctionBoundaryData` evaluated at one
-time, :330-380); outflow `:dirichlet` (every point takes the data); normal
-halo `:value`; scalar halo `:value` or `:mirror`; corrections `:uniform`,
-`:outflow_only` and `:none`.  The buffers are static, so the correction is
-applied once here (the reference applies the same correction to the same
-data before every projection).
+time, :330-380); outflow `:dirichlet` (every point takes the data) or
+`:convective` per side (src/boundary_conditions/outflow.jl: an outflow point
+is advanced by the radiation equation with the outward normal velocity as
+phase speed, on the device before every projection); normal halo `:value`;
+scalar halo `:value` or `:mirror`; corrections `:uniform`, `:outflow_only`
+and `:none`.  Dirichlet buffers are static, so their correction is applied
+once here (the reference applies the same correction to the same data
+before every projection); with a radiating face the step redoes data,
+radiation and correction before every projection.
 """
 from __future__ import annotations
 
@@ -130,13 +134,70 @@ class OpenBoundarySet:
     """Every plane of the open faces of one domain, the correction mode and
     the ledger of the last correction (`OpenBoundaryState`, :445-485)."""
 
-    def __init__(self, grid: Grid, planes, correction: str, open_x: bool, open_y: bool):
+    def __init__(self, grid: Grid, planes, correction: str, open_x: bool, open_y: bool, outflow=None):
         self.grid = grid
         self.planes = planes
         self.correction = correction
         self.open_x = open_x
         self.open_y = open_y
+        self.outflow = dict(outflow or {})          # side -> "dirichlet" | "convective"
         self.ledger = {"Q": 0.0, "residual": 0.0, "delta": 0.0}
+        for p in planes:
+            p.raw = p.data.copy()                    # the data before the correction
+
+    def mark_solids(self, solid):
+        """Where a solid obstacle touches the open faces (`mark_open_boundary_solids!`,
+        src/boundary_conditions/open_boundary.jl:809-868): `solid` a storage-shaped
+        bool array ([k, j, i], True = solid).  A boundary point is solid when an
+        interior cell it borders is (the cell next to the face; for a
+        component staggered along the face either of its two cells); solid
+        points take zero velocity in every layer (_apply_solid_values!,
+        :870-900) and leave the mass-flux correction.  The planes are refilled
+        from the data and corrected again."""
+        g = self.grid
+        solid = np.asarray(solid, dtype=bool)
+        if solid.shape != g.storage_shape:
+            raise ValueError(f"the solid mask must have the storage shape {g.storage_shape}")
+        H = g.halo
+        N = g.size
+        for p in self.planes:
+            ax = p.axis
+            t1, t2 = (1, 2) if ax == 0 else (0, 2)
+            nl = _NORMAL[p.name]
+            cell = H[ax] + N[ax] - 1 if p.high else H[ax]
+            fl = np.zeros((N[t1], N[t2]), dtype=bool)
+            for da in ((0, -1) if nl == t1 else (0,)):
+                for db in ((0, -1) if nl == t2 else (0,)):
+                    I = [None, None, None]
+                    I[ax] = cell
+                    I[t1] = slice(H[t1] + da, H[t1] + N[t1] + da)
+                    I[t2] = slice(H[t2] + db, H[t2] + N[t2] + db)
+                    fl |= solid[I[2], I[1], I[0]].T          # [tangential, z]
+            p.fluid = ~fl
+            p.data = p.raw.copy()
+        for p in self.planes:
+            if p.name == "theta" or p.fluid.all():
+                continue
+            t1 = 1 if p.axis == 0 else 0
+            sol = ~p.fluid                                  # [tangential a, z b]
+            for arr in (p.raw, p.data):
+                if p.axis == 0:
+                    view = arr[H[2]:H[2] + N[2], H[1]:H[1] + N[1], :]      # [k, j, layer]
+                    view[sol.T] = 0.0
+                else:
+                    view = arr[H[2]:H[2] + N[2], :, H[0]:H[0] + N[0]]      # [k, layer, i]
+                    view.transpose(0, 2, 1)[sol.T] = 0.0
+        self.correct()
+
+    @property
+    def radiating(self):
+        """The per-side flags (west, east, south, north) of a :convective outflow."""
+        return np.array([self.outflow.get(sd, "dirichlet") == "convective" for sd in ("west", "east", "south", "north")],
+                        dtype=np.int32)
+
+    @property
+    def correction_code(self):
+        return CORRECTIONS.index(self.correction)
 
     def plane(self, name, side):
         for p in self.planes:
@@ -160,11 +221,47 @@ class OpenBoundarySet:
             area = g.dx * g.dz
         s = 1.0 if p.high else -1.0
         f = p.fluid.T                                                  # [k, tangential]
+        wa = area * self.weight(p).T
         out = s * vals
-        q = float(np.sum(np.where(f, out * area, 0.0)))
-        ao = float(np.sum(np.where(f & (out > 0), area, 0.0)))
-        aa = float(np.sum(np.where(f, area, 0.0)))
+        q = float(np.sum(np.where(f, out * wa, 0.0)))
+        ao = float(np.sum(np.where(f & (out > 0), wa, 0.0)))
+        aa = float(np.sum(np.where(f, wa, 0.0)))
         return q, ao, aa
+
+    def weight(self, p):
+        """The open fraction of each boundary face of normal plane p ([tangential, z]):
+        its aperture when set_apertures gave them, else 1."""
+        w = getattr(p, "weight", None)
+        return np.ones_like(p.fluid, dtype=np.float64) if w is None else w
+
+    def set_apertures(self, apertures):
+        """Weight the mass-flux correction by the open fraction of each boundary
+        face (the cut-cell apertures (ax, ay, az) of the projection, face
+        layout of aeolus_b200_mgpcg.h), so that the corrected planes carry no
+        net flux through the faces the projection sees; a face with aperture
+        0 is solid (zero velocity, out of the correction).  The reference's
+        correction counts whole faces (`fluid` flags only); with 0/1
+        apertures the two agree."""
+        g = self.grid
+        ax, ay, _ = (np.asarray(a, dtype=np.float64) for a in apertures)
+        for p in self.planes:
+            if not p.normal:
+                continue
+            if p.axis == 0:
+                w = (ax[:, :, -1] if p.high else ax[:, :, 0]).T        # [j, k]
+            else:
+                w = (ay[:, -1, :] if p.high else ay[:, 0, :]).T        # [i, k]
+            p.weight = np.ascontiguousarray(w)
+            p.fluid = p.fluid & (w > 0)
+            for arr in (p.raw, p.data):
+                H = g.halo
+                if p.axis == 0:
+                    arr[H[2]:H[2] + g.nz, H[1]:H[1] + g.ny, :][(~p.fluid).T] = 0.0
+                else:
+                    arr[H[2]:H[2] + g.nz, :, H[0]:H[0] + g.nx].transpose(0, 2, 1)[(~p.fluid).T] = 0.0
+        for p in self.planes:
+            p.data[...] = p.raw
+        self.correct()
 
     def flux(self):
         """Net outward volume flux Q = sum u.n A over the open fluid faces
@@ -211,8 +308,20 @@ class OpenBoundarySet:
         return delta
 
     # ---- the device image ---------------------------------------------------------------
-    def packed(self):
-        """The planes as the arrays aeo_set_open takes: x planes
+    def face_weights(self):
+        """The weights of the normal planes' boundary faces in the correction
+        (0 solid, else the open fraction): x faces [side][Nz][Ny], y faces
+        [side][Nz][Nx], FP64."""
+        g = self.grid
+        xf = np.ones((2, g.nz, g.ny))
+        yf = np.ones((2, g.nz, g.nx))
+        for p in self.planes:
+            if p.normal:
+                (xf if p.axis == 0 else yf)[1 if p.high else 0] = (self.weight(p) * p.fluid).T
+        return xf, yf
+
+    def packed(self, raw=False):
+        """The planes (raw: the data before the correction) as the arrays aeo_set_open takes: x planes
         [field][side][k][j][layer] (NZ x NY x (H+1)) and y planes
         [field][side][k][layer][i] (NZ x (H+1) x NX), field order u, v, w,
         theta, layer = storage index along the normal on the low side and
@@ -235,23 +344,29 @@ class OpenBoundarySet:
             N = g.size[p.axis]
             off = p.start - (H + N) if p.high else p.start
             n = p.data.shape[2 - p.axis]
+            d = p.raw if raw else p.data
             if p.axis == 0:
-                xp[f, side, :, :, off:off + n] = p.data
+                xp[f, side, :, :, off:off + n] = d
             else:
-                yp[f, side, :, off:off + n, :] = p.data
+                yp[f, side, :, off:off + n, :] = d
         return np.ascontiguousarray(xp), np.ascontiguousarray(yp), modes
 
 
 def open_boundary_conditions(grid: Grid, data, x: str = "open", y: str = "periodic",
                              fields=FIELDS, correction: str = "uniform", normal_halo: str = "value",
-                             scalar_halo: str = "value", outflow: str = "dirichlet") -> OpenBoundarySet:
+                             scalar_halo: str = "value", outflow: str = "dirichlet", solid=None,
+                             apertures=None) -> OpenBoundarySet:
     """A box with open lateral faces fed by `data` (`open_boundary_conditions`,
     :532-638): `x` and `y` each "open" or "periodic" (both faces of an axis
     alike), bottom and top walls.  `fields` names the fields with boundary
     data (the three velocity components and theta); the planes are filled
     from `data` and the normal velocities corrected (`correction`).
+    `outflow` is "dirichlet" or "convective", or a dict of those per side;
+    `solid` (a storage-shaped bool mask) marks where obstacles touch the
+    faces (OpenBoundarySet.mark_solids); `apertures` (the projection's face
+    apertures) weight the correction (OpenBoundarySet.set_apertures).
     Raises ValueError for what is not built (an open top or bottom, the
-    :odd normal halo, radiating outflow, the :inflow scalar halo)."""
+    :odd normal halo, the :orlanski outflow, the :inflow scalar halo)."""
     if x not in ("open", "periodic") or y not in ("open", "periodic"):
         raise ValueError("x and y are 'open' or 'periodic'")
     if x == "periodic" and y == "periodic":
@@ -266,8 +381,16 @@ def open_boundary_conditions(grid: Grid, data, x: str = "open", y: str = "period
         raise ValueError("normal_halo = :odd is not built (the normal velocity's halo takes the data)")
     if scalar_halo not in ("value", "mirror"):
         raise ValueError("scalar_halo must be 'value' or 'mirror' (the :inflow mode is not built)")
-    if outflow != "dirichlet":
-        raise ValueError("radiating outflow (:convective, :orlanski) is not built; outflow = 'dirichlet'")
+    sides_all = ("west", "east", "south", "north")
+    given_per_side = not isinstance(outflow, str)
+    if isinstance(outflow, str):
+        outflow = {sd: outflow for sd in sides_all}
+    outflow = dict(outflow)
+    for sd, mode in outflow.items():
+        if sd not in sides_all:
+            raise ValueError(f"outflow: unknown side {sd!r} (use {sides_all}; an open top is not built)")
+        if mode not in ("dirichlet", "convective"):
+            raise ValueError(f"outflow mode must be 'dirichlet' or 'convective' (:orlanski is not built), got {mode!r}")
     for need in ("u", "v", "w"):
         if need not in fields:
             raise ValueError("open faces need data for u, v and w")
@@ -304,6 +427,14 @@ def open_boundary_conditions(grid: Grid, data, x: str = "open", y: str = "period
                 vals = np.array(data.value(name, xc, yc, zc, zs), dtype=np.float64)
             fluid = np.ones((ny if ax == 0 else nx, nz), dtype=bool)
             planes.append(OpenPlane(name, side, ax, high, normal, mode, int(r[0]), np.ascontiguousarray(vals), fluid))
-    obs = OpenBoundarySet(grid, planes, correction, x == "open", y == "open")
+    for sd, mode in outflow.items():
+        if mode == "convective" and sd not in sides and given_per_side:
+            raise ValueError(f"outflow: side {sd!r} is not an open face of this box")
+    obs = OpenBoundarySet(grid, planes, correction, x == "open", y == "open",
+                          {sd: outflow.get(sd, "dirichlet") for sd in sides})
     obs.correct()
+    if solid is not None:
+        obs.mark_solids(solid)
+    if apertures is not None:
+        obs.set_apertures(apertures)
     return obs

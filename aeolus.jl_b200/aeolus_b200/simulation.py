@@ -336,7 +336,20 @@ class Simulation:
         xp, yp, modes = obc.packed()
         _lib.check(self._lib.aeo_set_open(self._h, int(obc.open_x), int(obc.open_y), _ptr(xp), _ptr(yp),
                                           modes.ctypes.data_as(C.POINTER(C.c_int32))), self._h)
+        rad = np.ascontiguousarray(obc.radiating, dtype=np.int32)
+        xd, yd, _ = obc.packed(raw=True)
+        xw, yw = obc.face_weights()
+        _lib.check(self._lib.aeo_set_open_outflow(self._h, rad.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                  int(obc.correction_code), _ptr(xd), _ptr(yd), _ptr(xw), _ptr(yw)),
+                   self._h)
         self._open = obc
+
+    def open_ledger(self) -> dict:
+        """Q, residual and delta of the last mass-flux correction on the device
+        (a radiating open set)."""
+        out = np.zeros(3)
+        _lib.check(self._lib.aeo_open_ledger(self._h, _ptr(out)), self._h)
+        return {"Q": out[0], "residual": out[1], "delta": out[2]}
 
     def pcg_harvest(self, cap: int = 10):
         """Residual -> error pairs from the run's own snapshot: the right-hand

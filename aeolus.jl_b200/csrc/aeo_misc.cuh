@@ -90,15 +90,238 @@ __global__ void __launch_bounds__(256) halo_fill_kernel(Geo g, HaloSet<R> hs) {
 // and bs/bn [k][i] (interior), feed the projection.
 template <typename R>
 struct OpenSet {
-    const R* xp;
-    const R* yp;
-    const R* bw;
-    const R* be;
-    const R* bs;
-    const R* bn;
+    R* xp;
+    R* yp;
+    R* bw;
+    R* be;
+    R* bs;
+    R* bn;
     int ox, oy, L;
     int mode[4];
+    // radiating (:convective) outflow (src/boundary_conditions/outflow.jl):
+    // per side (west, east, south, north) the flag; the raw data planes, the
+    // step-start snapshot and the stage-start buffers (the layout of xp / yp);
+    // per plane point ([f][side][NZ][NY] x faces, [f][side][NZ][NX] y faces)
+    // the phase speed (NaN: an inflow point) and the two stage-start
+    // interior layers; the correction mode (0 uniform, 1 outflow only, 2
+    // none) and the ledger (Q, residual, delta) of the last correction
+    int rad[4];
+    int corr;
+    const R* xd;
+    const R* yd;
+    R* xs;
+    R* ys;
+    R* xv;
+    R* yv;
+    R* xc;
+    R* yc;
+    R* x1;
+    R* y1;
+    R* x2;
+    R* y2;
+    double* led;
+    const double* xw;     // weights of the normal planes' boundary faces, [side][Nz][Ny] / [side][Nz][Nx] (0 solid)
+    const double* yw;
 };
+
+// ---- radiating outflow (src/boundary_conditions/outflow.jl) --------------------
+// Plane geometry: element (layer l, tangential a, b) of plane (f, side) of
+// axis 0 (a = storage j, b = storage k) or 1 (a = storage i, b = storage k).
+template <typename R>
+__device__ __forceinline__ size_t ob_pi(const Geo& g, const OpenSet<R>& ob, int axis, int f, int side, int l, int a,
+                                        int b) {
+    const int NX = g.nx + 2 * AEO_H, NY = g.ny + 2 * AEO_H, NZ = g.nz + 2 * AEO_H;
+    if (axis == 0) return (((size_t)(f * 2 + side) * NZ + b) * NY + a) * ob.L + l;
+    return (((size_t)(f * 2 + side) * NZ + b) * ob.L + l) * NX + a;
+}
+// the storage index of a plane's boundary layer, its local layer, the
+// outward step and the layer count (_boundary_storage / _boundary_local /
+// _outward, outflow.jl:104-106)
+__device__ __forceinline__ void ob_geom(const Geo& g, int axis, int f, int side, int* sb, int* lb, int* o, int* nl) {
+    const int H = AEO_H, N = axis == 0 ? g.nx : g.ny;
+    if (side) { *sb = H + N; *lb = 0; *o = 1; *nl = H; }
+    else { *sb = f == axis ? H : H - 1; *lb = *sb; *o = -1; *nl = *sb + 1; }
+}
+// a tangential plane point t of the x faces (t < 8 NZ NY) or the y faces
+__device__ __forceinline__ bool ob_point(const Geo& g, long long t, int* axis, int* f, int* side, int* a, int* b) {
+    const long long NX = g.nx + 2 * AEO_H, NY = g.ny + 2 * AEO_H, NZ = g.nz + 2 * AEO_H;
+    long long n = 8 * NZ * NY;
+    int ax = 0;
+    if (t >= n) { t -= n; ax = 1; n = 8 * NZ * NX; if (t >= n) return false; }
+    const long long NA = ax == 0 ? NY : NX;
+    *a = (int)(t % NA); t /= NA;
+    *b = (int)(t % NZ); t /= NZ;
+    *side = (int)(t % 2);
+    *f = (int)(t / 2);
+    *axis = ax;
+    return true;
+}
+template <typename R>
+__device__ __forceinline__ R field_at(const Geo& g, const R* d, int axis, int li, int a, int b) {
+    return axis == 0 ? d[pidx(g, li - AEO_H, a - AEO_H, b - AEO_H)] : d[pidx(g, a - AEO_H, li - AEO_H, b - AEO_H)];
+}
+
+// prepare_open_boundaries! (open_boundary.jl:1189-1200, outflow.jl:113-182):
+// per radiating plane point the phase speed c = the outward normal velocity
+// of the boundary face (the mean of two faces for a component staggered
+// along the face), NaN where it does not point out (the data is kept)
+template <typename R>
+__global__ void ob_phase_kernel(Geo g, OpenSet<R> ob) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int axis, f, side, a, b;
+    if (!ob_point(g, t, &axis, &f, &side, &a, &b)) return;
+    R* C = axis == 0 ? ob.xc : ob.yc;
+    const long long ti = t - (axis == 0 ? 0 : 8LL * (g.nz + 2 * AEO_H) * (g.ny + 2 * AEO_H));
+    if (!ob.rad[axis * 2 + side] || ob.mode[f] != 0) { C[ti] = R(NAN); return; }
+    const R* P = axis == 0 ? ob.xp : ob.yp;
+    const int fl = side ? 0 : AEO_H;
+    const R sg = side ? R(1) : R(-1);
+    const bool st1 = (axis == 0 && f == 1) || (axis == 1 && f == 0), st2 = f == 2;
+    R un;
+    if (st1) {
+        const int am = a > 0 ? a - 1 : 0;
+        un = sg * (P[ob_pi(g, ob, axis, axis, side, fl, am, b)] + P[ob_pi(g, ob, axis, axis, side, fl, a, b)]) / R(2);
+    } else if (st2) {
+        const int bm = b > 0 ? b - 1 : 0;
+        un = sg * (P[ob_pi(g, ob, axis, axis, side, fl, a, bm)] + P[ob_pi(g, ob, axis, axis, side, fl, a, b)]) / R(2);
+    } else {
+        un = sg * P[ob_pi(g, ob, axis, axis, side, fl, a, b)];
+    }
+    C[ti] = un > R(0) ? un : R(NAN);
+}
+
+// mark_open_boundary_stage! (outflow.jl:198-237): the two interior layers next
+// to every radiating face at the start of a (sub)stage
+template <typename R>
+__global__ void ob_mark_kernel(Geo g, OpenSet<R> ob, const R* u, const R* v, const R* w, const R* th) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int axis, f, side, a, b;
+    if (!ob_point(g, t, &axis, &f, &side, &a, &b)) return;
+    if (!ob.rad[axis * 2 + side]) return;
+    const long long ti = t - (axis == 0 ? 0 : 8LL * (g.nz + 2 * AEO_H) * (g.ny + 2 * AEO_H));
+    int sb, lb, o, nl;
+    ob_geom(g, axis, f, side, &sb, &lb, &o, &nl);
+    const R* d = f == 0 ? u : f == 1 ? v : f == 2 ? w : th;
+    (axis == 0 ? ob.x1 : ob.y1)[ti] = field_at(g, d, axis, sb - o, a, b);
+    (axis == 0 ? ob.x2 : ob.y2)[ti] = field_at(g, d, axis, sb - 2 * o, a, b);
+}
+
+// _radiate_body! (outflow.jl:262-285): at an outflow point every layer from
+// the face outward, phi_b = phi_b0 - r (3 phi_b0 - 4 phi_{b-1}0 + phi_{b-2}0) / 2,
+// r = min(c dt / dn, 1), from the stage-start values (the buffer before the
+// update and the marked interior layers)
+template <typename R>
+__global__ void ob_radiate_kernel(Geo g, OpenSet<R> ob, const double* __restrict__ dtp) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int axis, f, side, a, b;
+    if (!ob_point(g, t, &axis, &f, &side, &a, &b)) return;
+    if (!ob.rad[axis * 2 + side]) return;
+    const long long ti = t - (axis == 0 ? 0 : 8LL * (g.nz + 2 * AEO_H) * (g.ny + 2 * AEO_H));
+    const R c = (axis == 0 ? ob.xc : ob.yc)[ti];
+    if (c != c) return;                                   // NaN: an inflow point keeps the data
+    const R dn = R(axis == 0 ? g.dx : g.dy);
+    const R r0 = c * R(*dtp) / dn, r = r0 < R(1) ? r0 : R(1);
+    R i1 = (axis == 0 ? ob.x1 : ob.y1)[ti], i2 = (axis == 0 ? ob.x2 : ob.y2)[ti];
+    int sb, lb, o, nl;
+    ob_geom(g, axis, f, side, &sb, &lb, &o, &nl);
+    R* Pl = axis == 0 ? ob.xp : ob.yp;
+    const R* P0 = axis == 0 ? ob.xv : ob.yv;
+    for (int q = 0, l = lb; q < nl; ++q, l += o) {
+        const size_t e = ob_pi(g, ob, axis, f, side, l, a, b);
+        const R p0 = P0[e];
+        Pl[e] = p0 - r * (R(3) * p0 - R(4) * i1 + i2) / R(2);
+        i2 = i1;
+        i1 = p0;
+    }
+}
+
+// correct_boundary_mass_flux! (open_boundary.jl:1024-1083) on the buffers, one
+// block (FP64 sums in a fixed order), then the boundary-face arrays of the
+// projection from the corrected buffers; led = (Q, residual, delta)
+template <typename R>
+__global__ void __launch_bounds__(1024) ob_correct_kernel(Geo g, OpenSet<R> ob) {
+    __shared__ double red[3][1024];
+    const int tid = threadIdx.x;
+    const long long nxf = ob.ox ? 2LL * g.ny * g.nz : 0, nyf = ob.oy ? 2LL * g.nx * g.nz : 0;
+    // face e of the normal planes: its buffer value, weighted area (0: solid) and outward sign
+    auto face = [&](long long e, R** pv, double* area, double* sg) {
+        int axis = 0;
+        if (e >= nxf) { e -= nxf; axis = 1; }
+        const double wt = (axis == 0 ? ob.xw : ob.yw)[e];
+        const int nt = axis == 0 ? g.ny : g.nx;
+        const int a = (int)(e % nt) + AEO_H;
+        e /= nt;
+        const int b = (int)(e % g.nz) + AEO_H;
+        const int side = (int)(e / g.nz);
+        *pv = (axis == 0 ? ob.xp : ob.yp) + ob_pi(g, ob, axis, axis, side, side ? 0 : AEO_H, a, b);
+        *area = (axis == 0 ? g.dy : g.dx) * g.dz * wt;
+        *sg = side ? 1.0 : -1.0;
+    };
+    double q = 0, ao = 0, aa = 0;
+    for (long long e = tid; e < nxf + nyf; e += blockDim.x) {
+        R* pv; double area, sg;
+        face(e, &pv, &area, &sg);
+        if (!(area > 0)) continue;
+        const double out = sg * (double)*pv;
+        q += out * area;
+        if (out > 0) ao += area;
+        aa += area;
+    }
+    red[0][tid] = q; red[1][tid] = ao; red[2][tid] = aa;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (tid < w)
+            for (int c = 0; c < 3; ++c) red[c][tid] += red[c][tid + w];
+        __syncthreads();
+    }
+    const double Q = red[0][0], Aout = red[1][0], Aall = red[2][0];
+    __syncthreads();
+    double delta = 0;
+    bool only_out = ob.corr == 1;
+    if (ob.corr != 2 && Q != 0) {
+        double A = only_out ? Aout : Aall;
+        if (A == 0) { only_out = false; A = Aall; }
+        delta = Q / A;
+        for (long long e = tid; e < nxf + nyf; e += blockDim.x) {
+            R* pv; double area, sg;
+            face(e, &pv, &area, &sg);
+            if (area > 0 && (!only_out || sg * (double)*pv > 0)) *pv = R((double)*pv - sg * delta);
+        }
+    }
+    __syncthreads();
+    double rr = 0;
+    for (long long e = tid; e < nxf + nyf; e += blockDim.x) {
+        R* pv; double area, sg;
+        face(e, &pv, &area, &sg);
+        if (area > 0) rr += sg * (double)*pv * area;
+    }
+    red[0][tid] = rr;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (tid < w) red[0][tid] += red[0][tid + w];
+        __syncthreads();
+    }
+    if (tid == 0) { ob.led[0] = Q; ob.led[1] = red[0][0]; ob.led[2] = delta; }
+    // the projection's boundary-face values
+    const int H = AEO_H;
+    for (long long e = tid; e < (long long)g.ny * g.nz && ob.ox; e += blockDim.x) {
+        const int j = (int)(e % g.ny), k = (int)(e / g.ny);
+        ob.bw[e] = ob.xp[ob_pi(g, ob, 0, 0, 0, H, j + H, k + H)];
+        ob.be[e] = ob.xp[ob_pi(g, ob, 0, 0, 1, 0, j + H, k + H)];
+    }
+    for (long long e = tid; e < (long long)g.nx * g.nz && ob.oy; e += blockDim.x) {
+        const int i = (int)(e % g.nx), k = (int)(e / g.nx);
+        ob.bs[e] = ob.yp[ob_pi(g, ob, 1, 1, 0, H, i + H, k + H)];
+        ob.bn[e] = ob.yp[ob_pi(g, ob, 1, 1, 1, 0, i + H, k + H)];
+    }
+}
+
+// combine_open_boundaries! (open_boundary.jl:1262-1280): buffer = a snapshot + b buffer
+template <typename R>
+__global__ void ob_combine_kernel(R* __restrict__ p, const R* __restrict__ snap, long long n, R ca, R cb) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        p[q] = ca * snap[q] + cb * p[q];
+}
 
 // The composite map of the reference's fill order (x, then y, then z) with
 // open faces: z first (the z fill copies whole x-y planes), then y (an open y

@@ -195,6 +195,80 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs& a, uint32_t tacc, 
     }
 }
 
+// The operands the epilogue of a cell reads from global memory (add, gate),
+// loaded ahead so that their latency hides behind the wait for the MMAs.
+template <int COUT>
+struct EpiIn {
+    uint4 add[COUT / 8];
+    uint4 gate[COUT / 8];
+};
+template <int COUT>
+__device__ __forceinline__ void epi_prefetch(const ConvArgs& a, int cell, EpiIn<COUT>& e) {
+    if (a.add) {
+        const uint4* ap = reinterpret_cast<const uint4*>(a.add + (size_t)cell * COUT);
+#pragma unroll
+        for (int u = 0; u < COUT / 8; ++u) e.add[u] = ap[u];
+    }
+    if (a.gate) {
+        const uint4* gp = reinterpret_cast<const uint4*>(a.gate + (size_t)cell * COUT);
+#pragma unroll
+        for (int u = 0; u < COUT / 8; ++u) e.gate[u] = gp[u];
+    }
+}
+// conv_epilogue with the prefetched operands
+template <int COUT>
+__device__ __forceinline__ void conv_epilogue_pre(const ConvArgs& a, uint32_t tacc, int cell, const EpiIn<COUT>& e) {
+    float v[COUT];
+    {
+        float h[16];
+        tc::tmem_ld16(tacc, h);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = h[q];
+        if constexpr (COUT == 32) {
+            tc::tmem_ld16(tacc + 16u, h);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) v[16 + q] = h[q];
+        }
+    }
+    if (a.bias)
+#pragma unroll
+        for (int q = 0; q < COUT; ++q) v[q] += a.bias[q];
+    if (a.add)
+#pragma unroll
+        for (int u = 0; u < COUT / 8; ++u) {
+            const bf16* x = reinterpret_cast<const bf16*>(&e.add[u]);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v[8 * u + q] += __bfloat162float(x[q]);
+        }
+    if (a.relu)
+#pragma unroll
+        for (int q = 0; q < COUT; ++q) v[q] = fmaxf(v[q], 0.0f);
+    if (a.gate)
+#pragma unroll
+        for (int u = 0; u < COUT / 8; ++u) {
+            const bf16* x = reinterpret_cast<const bf16*>(&e.gate[u]);
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (!(__bfloat162float(x[q]) > 0.0f)) v[8 * u + q] = 0.0f;
+        }
+    if (a.out) {
+        uint4* op = reinterpret_cast<uint4*>(a.out + (size_t)cell * COUT);
+#pragma unroll
+        for (int u = 0; u < COUT / 8; ++u) {
+            uint4 w;
+            bf16* x = reinterpret_cast<bf16*>(&w);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) x[q] = __float2bfloat16_rn(v[8 * u + q]);
+            op[u] = w;
+        }
+    }
+    if (a.out0) {
+        float sc = a.out0_scale ? (float)*a.out0_scale : 1.0f;
+        if (a.out0_mask) sc *= a.out0_mask[cell];
+        a.out0[cell] = v[0] * sc;
+    }
+}
+
 template <int CIN, int COUT>
 constexpr size_t conv_smem_weights() { return (size_t)(CIN / 8) * 27 * COUT * 16; }
 
@@ -371,7 +445,7 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_ring_kernel(ConvArgs a) {
     const uint32_t tmem = tslot;
     const uint32_t idesc = tc::idesc_bf16(COUT, false, false);
     constexpr uint32_t lboA = (uint32_t)(R * 3 * PITCH * 16), lboB = 27u * COUT * 16u;
-    const uint32_t aBase = tc::smem_u32(sR), bBase = tc::smem_u32(sB);
+    const uint64_t descA = tc::sdesc(tc::smem_u32(sR), lboA, 128), descB = tc::sdesc(tc::smem_u32(sB), lboB, 128);
     const uint4* inp = reinterpret_cast<const uint4*>(a.in);
     int ql = -1;                        // stream index of the last entry loaded
     auto load_tile = [&](int iu) {
@@ -405,16 +479,20 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_ring_kernel(ConvArgs a) {
         if (threadIdx.x == 0) {
             tc::fence_after();
             const uint32_t dacc = tmem + (uint32_t)((i & 1) * COUT);
-#pragma unroll 1
+            // the descriptors' start-address field (bits 0-13, address >> 4) is
+            // linear in the address, and every operand lies below 256 KB, so a
+            // tap's descriptor is the base one plus its 16-byte offset
+            int srow[3];
+#pragma unroll
+            for (int dy = 0; dy < 3; ++dy) srow[dy] = ((qm - 2 + dy) % R) * 3 * PITCH;
+#pragma unroll
             for (int t = 0; t < 27; ++t) {
                 const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;      // each 0..2 (offset + 1)
-                const int slot = (qm - 2 + dy) % R;
 #pragma unroll
                 for (int ks = 0; ks < CIN / 16; ++ks) {
-                    const uint32_t aa = aBase + (uint32_t)((((2 * ks * R + slot) * 3 + dz) * PITCH + dx) * 16);
-                    const uint32_t bb = bBase + (uint32_t)((2 * ks * 27 + t) * COUT * 16);
-                    tc::mma_bf16(dacc, tc::sdesc(aa, lboA, 128), tc::sdesc(bb, lboB, 128), idesc,
-                                 (t | ks) ? 1u : 0u);
+                    const uint64_t ad = descA + (uint64_t)(2 * ks * R * 3 * PITCH + srow[dy] + dz * PITCH + dx);
+                    const uint64_t bd = descB + (uint64_t)((2 * ks * 27 + t) * COUT);
+                    tc::mma_bf16(dacc, ad, bd, idesc, (t | ks) ? 1u : 0u);
                 }
             }
             tc::commit(&mbar[i & 1]);
@@ -422,6 +500,11 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_ring_kernel(ConvArgs a) {
         ++issued;
         if (i > 0) {
             const int ip = i - 1;
+            const int tp = tau - 1, jp = tp % T.ny, colp = tp / T.ny;
+            const int kp = colp / T.tx, x0p = (colp - kp * T.tx) * TM;
+            const int cell = (kp * T.ny + jp) * T.nx + x0p + warp * 32 + lane;
+            EpiIn<COUT> ein;
+            epi_prefetch<COUT>(a, cell, ein);
             const bool ok = tc::mbar_wait(&mbar[ip & 1], (uint32_t)((ip >> 1) & 1), WAIT_LIMIT);
             if (__syncthreads_or(!ok)) {
                 failed = true;
@@ -429,10 +512,7 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_ring_kernel(ConvArgs a) {
             }
             ++drained;
             tc::fence_after();
-            const int tp = tau - 1, jp = tp % T.ny, colp = tp / T.ny;
-            const int kp = colp / T.tx, x0p = (colp - kp * T.tx) * TM;
-            conv_epilogue<COUT>(a, tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((ip & 1) * COUT),
-                                (kp * T.ny + jp) * T.nx + x0p + warp * 32 + lane);
+            conv_epilogue_pre<COUT>(a, tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((ip & 1) * COUT), cell, ein);
         }
         if (i + PF < cnt) load_tile(i + PF);
         cp_async_commit();

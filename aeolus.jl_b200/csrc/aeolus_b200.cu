@@ -120,6 +120,9 @@ struct CoreBase {
     virtual aeo_status pcg_set_learned(aeo_unet* net, double stagnation) = 0;
     virtual aeo_status pcg_harvest(int cap, double* b, double* x, double* rh, double* xh, int* count) = 0;
     virtual aeo_status set_open(int ox, int oy, const double* xp, const double* yp, const int* modes) = 0;
+    virtual aeo_status set_open_outflow(const int* rad, int corr, const double* xd, const double* yd, const double* xw,
+                                        const double* yw) = 0;
+    virtual aeo_status open_ledger(double* out) = 0;
     virtual aeo_status set_ibm(const uint8_t* mask, double tau) = 0;
     virtual aeo_status set_sgs_buoyancy(const double* bg) = 0;
     virtual aeo_status set_lagrangian(double c0, double theta, double memory_time) = 0;
@@ -167,6 +170,7 @@ struct Core : CoreBase {
     std::vector<double> h_ap[3];   // the apertures the PCG operator was built from
     // open lateral faces (aeo_set_open): plane buffers and boundary-face values
     bool open_x = false, open_y = false;
+    bool ob_rad = false;           // a radiating (:convective) open face
     OpenSet<R> ob{};
     int pcg_maxit = 200;
     double* d_stage = nullptr; // host-layout staging (device)
@@ -1016,11 +1020,111 @@ struct Core : CoreBase {
         open_y = oy != 0;
         g.ox = ob.ox;     // the sweeps' closure fields take the mirror across open faces
         g.oy = ob.oy;
+        ob_rad = false;   // Dirichlet until set_open_outflow
+        for (int q = 0; q < 4; ++q) ob.rad[q] = 0;
         if (aeo_status e = make_pcg(h_ap[0].data(), h_ap[1].data(), h_ap[2].data())) return e;
         R* f[4] = {P[cur][0], P[cur][1], P[cur][2], P[cur][3]};
         int l[4] = {LOC_FX, LOC_FY, LOC_FZ, LOC_C};
         if (aeo_status e = halo(f, l, 4)) return e;
         CK(cudaStreamSynchronize(st));
+        return AEO_OK;
+    }
+
+    // The radiating outflow of the open faces already set (set_open): per side
+    // (west, east, south, north) 1 = :convective, the correction mode and the
+    // raw data planes (before the correction) in the buffers' layout; the
+    // step then refills, radiates and corrects the buffers before every
+    // projection (update_open_boundaries!, open_boundary.jl:1137-1152).
+    aeo_status set_open_outflow(const int* rad, int corr, const double* xd, const double* yd, const double* xw,
+                                const double* yw) override {
+        if (!(open_x || open_y)) { fail("set_open_outflow: no open face (aeo_set_open first)"); return AEO_ERR_STATE; }
+        if (!rad || corr < 0 || corr > 2) { fail("set_open_outflow: NULL flags or a correction mode outside 0..2"); return AEO_ERR_ARGUMENT; }
+        bool any = false;
+        for (int q = 0; q < 4; ++q) {
+            if (rad[q] && !(q < 2 ? open_x : open_y)) { fail("set_open_outflow: a radiating side that is not open"); return AEO_ERR_ARGUMENT; }
+            any = any || rad[q];
+        }
+        if (any && ((open_x && !xd) || (open_y && !yd))) { fail("set_open_outflow: NULL data planes"); return AEO_ERR_ARGUMENT; }
+        CK(cudaStreamSynchronize(st));
+        drop_graphs();
+        ob.corr = corr;
+        for (int q = 0; q < 4; ++q) ob.rad[q] = rad[q] ? 1 : 0;
+        ob_rad = any;
+        if (!any) return AEO_OK;
+        const int H = AEO_H, NX = g.nx + 2 * H, NY = g.ny + 2 * H, NZ = g.nz + 2 * H, L = H + 1;
+        const size_t nxp = (size_t)8 * NZ * NY * L, nyp = (size_t)8 * NZ * L * NX;
+        const size_t ntx = (size_t)8 * NZ * NY, nty = (size_t)8 * NZ * NX;
+        if (!ob.xs) {
+            R* b[12] = {};
+            const size_t n[12] = {nxp, nyp, nxp, nyp, nxp, nyp, ntx, nty, ntx, nty, ntx, nty};
+            for (int q = 0; q < 12; ++q)
+                if (aeo_status e = alloc(&b[q], n[q])) return e;
+            double* led = nullptr;
+            if (aeo_status e = alloc(&led, 4)) return e;
+            double *dxw = nullptr, *dyw = nullptr;
+            if (aeo_status e = alloc(&dxw, (size_t)2 * g.nz * g.ny)) return e;
+            if (aeo_status e = alloc(&dyw, (size_t)2 * g.nz * g.nx)) return e;
+            ob.xw = dxw;
+            ob.yw = dyw;
+            ob.xd = b[0]; ob.yd = b[1]; ob.xs = b[2]; ob.ys = b[3]; ob.xv = b[4]; ob.yv = b[5];
+            ob.xc = b[6]; ob.yc = b[7]; ob.x1 = b[8]; ob.y1 = b[9]; ob.x2 = b[10]; ob.y2 = b[11];
+            ob.led = led;
+        }
+        std::vector<R> hx(nxp, R(0)), hy(nyp, R(0));
+        if (open_x)
+            for (size_t q = 0; q < nxp; ++q) hx[q] = R(xd[q] - (q / (nxp / 4) == 3 ? th_off : 0.0));
+        if (open_y)
+            for (size_t q = 0; q < nyp; ++q) hy[q] = R(yd[q] - (q / (nyp / 4) == 3 ? th_off : 0.0));
+        CK(cudaMemcpy((void*)ob.xd, hx.data(), nxp * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy((void*)ob.yd, hy.data(), nyp * sizeof(R), cudaMemcpyHostToDevice));
+        std::vector<double> wx((size_t)2 * g.nz * g.ny, 1.0), wy((size_t)2 * g.nz * g.nx, 1.0);
+        if (xw) std::copy(xw, xw + wx.size(), wx.begin());
+        if (yw) std::copy(yw, yw + wy.size(), wy.begin());
+        for (double v : wx) if (!(v >= 0.0 && v <= 1.0)) { fail("set_open_outflow: face weights lie in [0, 1]"); return AEO_ERR_ARGUMENT; }
+        for (double v : wy) if (!(v >= 0.0 && v <= 1.0)) { fail("set_open_outflow: face weights lie in [0, 1]"); return AEO_ERR_ARGUMENT; }
+        CK(cudaMemcpy((void*)ob.xw, wx.data(), wx.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy((void*)ob.yw, wy.data(), wy.size() * sizeof(double), cudaMemcpyHostToDevice));
+        return AEO_OK;
+    }
+
+    aeo_status open_ledger(double* out) override {
+        if (!ob_rad) { fail("open_ledger: no radiating open face"); return AEO_ERR_STATE; }
+        CK(cudaStreamSynchronize(st));
+        CK(cudaMemcpy(out, ob.led, 3 * sizeof(double), cudaMemcpyDeviceToHost));
+        return AEO_OK;
+    }
+
+    // the radiating outflow's step-start, stage-start, update and combination
+    unsigned ob_blocks() const {
+        const long long n = 8LL * (g.nz + 2 * AEO_H) * ((g.ny + 2 * AEO_H) + (g.nx + 2 * AEO_H));
+        return (unsigned)((n + 255) / 256);
+    }
+    size_t ob_nxp() const { return (size_t)8 * (g.nz + 2 * AEO_H) * (g.ny + 2 * AEO_H) * (AEO_H + 1); }
+    size_t ob_nyp() const { return (size_t)8 * (g.nz + 2 * AEO_H) * (AEO_H + 1) * (g.nx + 2 * AEO_H); }
+    aeo_status ob_prepare() {
+        CK(cudaMemcpyAsync(ob.xs, ob.xp, ob_nxp() * sizeof(R), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(ob.ys, ob.yp, ob_nyp() * sizeof(R), cudaMemcpyDeviceToDevice, st));
+        ob_phase_kernel<R><<<ob_blocks(), 256, 0, st>>>(g, ob);
+        CKL();
+        return AEO_OK;
+    }
+    aeo_status ob_update(int s_in) {
+        (void)s_in;
+        CK(cudaMemcpyAsync(ob.xv, ob.xp, ob_nxp() * sizeof(R), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(ob.yv, ob.yp, ob_nyp() * sizeof(R), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(ob.xp, ob.xd, ob_nxp() * sizeof(R), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(ob.yp, ob.yd, ob_nyp() * sizeof(R), cudaMemcpyDeviceToDevice, st));
+        ob_radiate_kernel<R><<<ob_blocks(), 256, 0, st>>>(g, ob, &d_sc->dt);
+        CKL();
+        ob_correct_kernel<R><<<1, 1024, 0, st>>>(g, ob);
+        CKL();
+        return AEO_OK;
+    }
+    aeo_status ob_combine(R ca, R cb) {
+        ob_combine_kernel<R><<<296, 256, 0, st>>>(ob.xp, ob.xs, (long long)ob_nxp(), ca, cb);
+        CKL();
+        ob_combine_kernel<R><<<296, 256, 0, st>>>(ob.yp, ob.ys, (long long)ob_nyp(), ca, cb);
+        CKL();
         return AEO_OK;
     }
 
@@ -1325,6 +1429,10 @@ struct Core : CoreBase {
     // with the step-start set s_u0 (stages 2, 3).
     aeo_status substage(int s_in, int s_out, int s_u0, int stage, R ca, R cb) {
         R** out = P[s_out];
+        if (ob_rad) {   // the stage-start interior layers of the radiating faces
+            ob_mark_kernel<R><<<ob_blocks(), 256, 0, st>>>(g, ob, P[s_in][0], P[s_in][1], P[s_in][2], P[s_in][3]);
+            CKL();
+        }
         SweepArgs<R> a{};
         a.g = g;
         a.u = P[s_in][0]; a.v = P[s_in][1]; a.w = P[s_in][2]; a.th = P[s_in][3];
@@ -1357,8 +1465,12 @@ struct Core : CoreBase {
             CKL();
         }
         mark(AEO_K_SWEEP);
+        if (ob_rad)     // 7c. open boundaries: data, radiation, mass-flux correction
+            if (aeo_status e = ob_update(s_in)) return e;
         if (aeo_status e = solve(nullptr)) return e;
         if (aeo_status e = correct(out, stage, ca, cb, &d_sc->dt, s_u0)) return e;
+        if (ob_rad && stage)   // the buffers combined like the fields (combine_open_boundaries!)
+            if (aeo_status e = ob_combine(ca, cb)) return e;
         mark(AEO_K_CORRECT);
         R* f[4] = {out[0], out[1], out[2], out[3]};
         int l[4] = {LOC_FX, LOC_FY, LOC_FZ, LOC_C};
@@ -1389,6 +1501,8 @@ struct Core : CoreBase {
         if (pick)
             if (aeo_status e = enqueue_pick(c)) return e;
         const R inv3 = R(1) / R(3), two3 = R(2) * inv3;
+        if (ob_rad)
+            if (aeo_status e = ob_prepare()) return e;
         if (aeo_status e = substage(c, 2, c, 0, R(0), R(0))) return e;
         if (aeo_status e = substage(2, 3, c, 1, R(0.75), R(0.25))) return e;
         if (aeo_status e = substage(3, c ^ 1, c, 1, inv3, two3)) return e;
@@ -1533,6 +1647,8 @@ struct Core : CoreBase {
         set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt, dt);
         CKL();
         for (int s = 0; s < n; ++s) {
+            if (ob_rad)
+                if (aeo_status e = ob_prepare()) return e;
             if (aeo_status e = substage(cur, cur ^ 1, cur, 0, R(0), R(0))) return e;
             if (aeo_status e = commit_sgs(cur ^ 1)) return e;
             cur ^= 1;
@@ -1612,6 +1728,10 @@ struct Core : CoreBase {
     // untouched) is kept and the step retried with half the dt.
     aeo_status step_adaptive(const aeo_cfl* c, int n, double* dt_prev_io, aeo_adaptive_stats* stats) override {
         if (aeo_status e = sgs_ready()) return e;
+        if (ob_rad) {   // a retry would have to rewind the radiated buffers too
+            fail("step_adaptive: not built with a radiating open face (step_rk3 with a chosen dt)");
+            return AEO_ERR_STATE;
+        }
         set_cfl(c);
         double dt_prev = (dt_prev_io && *dt_prev_io > 0) ? *dt_prev_io : 0.0;
         set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt_prev, dt_prev);
@@ -2264,6 +2384,18 @@ aeo_status aeo_set_open(aeo_sim* h, int32_t open_x, int32_t open_y, const double
                         const int32_t* modes) {
     ENTER(h);
     return h->core->set_open(open_x, open_y, x_planes, y_planes, modes);
+}
+
+aeo_status aeo_set_open_outflow(aeo_sim* h, const int32_t* radiate, int32_t correction, const double* x_data,
+                                const double* y_data, const double* x_weights, const double* y_weights) {
+    ENTER(h);
+    return h->core->set_open_outflow(radiate, correction, x_data, y_data, x_weights, y_weights);
+}
+
+aeo_status aeo_open_ledger(aeo_sim* h, double* out) {
+    ENTER(h);
+    if (!out) return AEO_ERR_ARGUMENT;
+    return h->core->open_ledger(out);
 }
 
 aeo_status aeo_pcg_harvest(aeo_sim* h, int32_t cap, double* b, double* x, double* r_hist, double* x_hist,

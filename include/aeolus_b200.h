@@ -403,6 +403,29 @@ aeo_status aeo_pcg_set_learned(aeo_sim* h, struct aeo_unet* net, double stagnati
  * open_x = open_y = 0 closes the faces again. */
 aeo_status aeo_set_open(aeo_sim* h, int32_t open_x, int32_t open_y, const double* x_planes, const double* y_planes,
                         const int32_t* modes);
+/* Radiating outflow of the open faces set by aeo_set_open (the :convective
+ * outflow of open_boundary_conditions, src/boundary_conditions/outflow.jl):
+ * radiate[4] (west, east, south, north) 1 = :convective, 0 = :dirichlet;
+ * correction 0 :uniform, 1 :outflow_only, 2 :none; x_data / y_data the raw
+ * boundary data (before the correction) in aeo_set_open's layout.  Each step
+ * then fixes, at its start, the outflow points (outward normal velocity of
+ * the boundary face > 0) and their phase speed c = that velocity
+ * (prepare_open_boundaries!, open_boundary.jl:1189-1200); before every
+ * projection it refills the planes from the data, advances the outflow
+ * points by the second-order upstream radiation update from the stage-start
+ * values, r = min(c dt / dn, 1), and applies the mass-flux correction
+ * (update_open_boundaries!, :1137-1152; _radiate_body!, outflow.jl:262-285);
+ * RK3 stages combine the planes like the fields (combine_open_boundaries!,
+ * :1262-1280).  x_weights [side][Nz][Ny] / y_weights [side][Nz][Nx] (NULL: 1)
+ * weight each normal boundary face in the correction: 0 a solid face
+ * (mark_open_boundary_solids!, :809-868), else its open fraction (the
+ * projection's aperture there, so the corrected planes carry no net flux the
+ * cut-cell divergence sees).  Not with aeo_step_adaptive (AEO_ERR_STATE). */
+aeo_status aeo_set_open_outflow(aeo_sim* h, const int32_t* radiate, int32_t correction, const double* x_data,
+                                const double* y_data, const double* x_weights, const double* y_weights);
+/* Q, residual and delta of the last mass-flux correction of a radiating open
+ * set (open_boundary_ledger, open_boundary.jl:1437-1450); synchronises */
+aeo_status aeo_open_ledger(aeo_sim* h, double* out);
 /* Residual -> error pairs from the run's own snapshots (no reference
  * counterpart; it feeds the learned preconditioner): b receives the
  * right-hand side of the last projection's solve (the predictor's cut-cell

@@ -97,7 +97,24 @@ struct oc_sim {
     int omode[4];
     double cg_tol;
     int cg_maxit;
+    /* radiating outflow (:convective) of the open faces: per side (west, east,
+     * south, north) the flag; the raw data planes, the step-start snapshot and
+     * the stage-start buffers (the layout of oxp / oyp); the phase speeds and
+     * the stage-start interior layers per plane point ([f][side][NZ][NY or NX]);
+     * the correction mode (0 uniform, 1 outflow only, 2 none) and its ledger */
+    int orad[4], ocorr, omarked;
+    double *oxf, *oyf;            /* weights of the normal planes' boundary faces (0 solid) */
+    double *oxd, *oyd, *oxs, *oys, *oxv, *oyv;
+    double *oxc, *oyc, *ox1, *oy1, *ox2, *oy2;
+    double oQ, odelta, oresid;
 };
+
+/* the radiating outflow of open faces (defined with oc_set_open) */
+static int ob_radiates(const oc_sim* s);
+static void ob_prepare(oc_sim* s);
+static void ob_mark(oc_sim* s);
+static void ob_update(oc_sim* s, double dt);
+static void ob_combine(oc_sim* s, double a, double b);
 
 #define ID(s, i, j, k) ((int64_t)(i) + (int64_t)(s)->NX * ((int64_t)(j) + (int64_t)(s)->NY * (int64_t)(k)))
 #define A(f, i, j, k) (f)[ID(s, i, j, k)]
@@ -1771,6 +1788,7 @@ static void substage(oc_sim* s, double dt, int stage, double ca, double cb) {
     const oc_params* P = &s->p;
     int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
     int anel = P->core == OC_CORE_ANELASTIC;
+    if (ob_radiates(s)) ob_mark(s);          /* the stage-start layers (src/Simulations.jl:538) */
     oc_fill_state_halos(s);
     compute_tendencies(s);
     /* 7. predictor */
@@ -1784,6 +1802,7 @@ static void substage(oc_sim* s, double dt, int stage, double ca, double cb) {
                 s->w[q] = s->w[q] + dt * s->tw[q];
             }
     if (s->ibm) ibm_correct(s, dt);
+    ob_update(s, dt);                        /* 7c. open boundaries (src/Simulations.jl:630-633) */
     /* 8. divergence into the solver's buffer */
     fill_halos(s, s->u, LOC_FX);
     fill_halos(s, s->v, LOC_FY);
@@ -1875,6 +1894,7 @@ int oc_project(oc_sim* s) {
 
 int oc_step_euler(oc_sim* s, double dt, int nsteps) {
     for (int n = 0; n < nsteps; ++n) {
+        if (ob_radiates(s)) ob_prepare(s);
         substage(s, dt, 0, 0.0, 0.0);
         if (s->p.c_s != 0 && s->p.sgs_model == OC_SGS_LAGRANGIAN) lag_commit(s, dt);   /* once per step */
         if (s->p.c_s != 0 && s->p.sgs_model == OC_SGS_TKE) tke_commit(s, dt);
@@ -1972,10 +1992,13 @@ int oc_step_rk3(oc_sim* s, double dt, int nsteps) {
     size_t b = sizeof(double) * (size_t)s->n;
     double inv3 = 1.0 / 3, two3 = 2 * inv3;
     for (int n = 0; n < nsteps; ++n) {
+        if (ob_radiates(s)) ob_prepare(s);
         memcpy(s->u0, s->u, b); memcpy(s->v0, s->v, b); memcpy(s->w0, s->w, b); memcpy(s->th0, s->th, b);
         substage(s, dt, 0, 0.0, 0.0);
         substage(s, dt, 1, 0.75, 0.25);
+        ob_combine(s, 0.75, 0.25);
         substage(s, dt, 1, inv3, two3);
+        ob_combine(s, inv3, two3);
         if (s->p.c_s != 0 && s->p.sgs_model == OC_SGS_LAGRANGIAN) lag_commit(s, dt);   /* once per step */
         if (s->p.c_s != 0 && s->p.sgs_model == OC_SGS_TKE) tke_commit(s, dt);
     }
@@ -2448,6 +2471,206 @@ int oc_set_apertures(oc_sim* s, const double* ax, const double* ay, const double
     return 0;
 }
 
+/* ---- radiating outflow (src/boundary_conditions/outflow.jl) ------------- */
+
+static int ob_radiates(const oc_sim* s) { return s->orad[0] || s->orad[1] || s->orad[2] || s->orad[3]; }
+
+/* element (layer l, tangential a, b) of plane (f, side) of axis 0 (x faces:
+ * a = storage j, b = storage k) or 1 (y faces: a = storage i, b = storage k) */
+static inline int64_t ob_pi(const oc_sim* s, int axis, int f, int side, int l, int a, int b) {
+    if (axis == 0) return (((int64_t)(f * 2 + side) * s->NZ + b) * s->NY + a) * s->oL + l;
+    return (((int64_t)(f * 2 + side) * s->NZ + b) * s->oL + l) * s->NX + a;
+}
+static inline int64_t ob_ti(const oc_sim* s, int axis, int f, int side, int a, int b) {
+    return ((int64_t)(f * 2 + side) * s->NZ + b) * (axis == 0 ? s->NY : s->NX) + a;
+}
+static inline double* ob_field(oc_sim* s, int f) { return f == 0 ? s->u : f == 1 ? s->v : f == 2 ? s->w : s->th; }
+static inline double ob_at(const oc_sim* s, const double* d, int axis, int li, int a, int b) {
+    return axis == 0 ? A(d, li, a, b) : A(d, a, li, b);
+}
+/* storage index of the boundary layer (the normal velocity's face, the first
+ * halo cell of the rest), the local layer of it, the outward step
+ * (_boundary_storage, _boundary_local, _outward, outflow.jl:104-106) */
+static inline void ob_geom(const oc_sim* s, int axis, int f, int side, int* sb, int* lb, int* o, int* nl) {
+    int H = axis == 0 ? s->p.hx : s->p.hy, N = axis == 0 ? s->p.nx : s->p.ny;
+    if (side) { *sb = H + N; *lb = 0; *o = 1; *nl = H; }
+    else { *sb = f == axis ? H : H - 1; *lb = *sb; *o = -1; *nl = *sb + 1; }
+}
+
+/* prepare_open_boundaries! (open_boundary.jl:1189-1200): the step-start
+ * snapshot of every buffer, and per radiating plane point the phase speed
+ * c = the outward normal velocity of the boundary face when positive, else
+ * NaN (an inflow point keeps its data) (_outward_un, _phase_speed_body!,
+ * outflow.jl:113-182; :convective) */
+static void ob_prepare(oc_sim* s) {
+    int64_t nxp = (int64_t)8 * s->NZ * s->NY * s->oL, nyp = (int64_t)8 * s->NZ * s->oL * s->NX;
+    memcpy(s->oxs, s->oxp, sizeof(double) * nxp);
+    memcpy(s->oys, s->oyp, sizeof(double) * nyp);
+    for (int axis = 0; axis < 2; ++axis)
+        for (int side = 0; side < 2; ++side) {
+            if (!s->orad[axis * 2 + side]) continue;
+            const double* P = axis == 0 ? s->oxp : s->oyp;
+            double* C = axis == 0 ? s->oxc : s->oyc;
+            int NA = axis == 0 ? s->NY : s->NX;
+            int H = axis == 0 ? s->p.hx : s->p.hy;
+            int fl = side ? 0 : H;                       /* the normal plane's boundary face */
+            double sg = side ? 1.0 : -1.0;
+            for (int f = 0; f < 4; ++f)
+                for (int b = 0; b < s->NZ; ++b)
+                    for (int a = 0; a < NA; ++a) {
+                        double un;
+                        /* staggered along a tangential direction: the mean of the two faces */
+                        int st1 = (axis == 0 && f == 1) || (axis == 1 && f == 0), st2 = f == 2;
+                        if (st1) {
+                            int am = a > 0 ? a - 1 : 0;
+                            un = sg * (P[ob_pi(s, axis, axis, side, fl, am, b)] + P[ob_pi(s, axis, axis, side, fl, a, b)]) / 2;
+                        } else if (st2) {
+                            int bm = b > 0 ? b - 1 : 0;
+                            un = sg * (P[ob_pi(s, axis, axis, side, fl, a, bm)] + P[ob_pi(s, axis, axis, side, fl, a, b)]) / 2;
+                        } else {
+                            un = sg * P[ob_pi(s, axis, axis, side, fl, a, b)];
+                        }
+                        C[ob_ti(s, axis, f, side, a, b)] = (s->omode[f] == 0 && un > 0) ? un : NAN;
+                    }
+        }
+}
+
+/* mark_open_boundary_stage! (outflow.jl:198-237): the two interior layers
+ * next to every radiating face at the start of a (sub)stage */
+static void ob_mark(oc_sim* s) {
+    for (int axis = 0; axis < 2; ++axis)
+        for (int side = 0; side < 2; ++side) {
+            if (!s->orad[axis * 2 + side]) continue;
+            int NA = axis == 0 ? s->NY : s->NX;
+            double* S1 = axis == 0 ? s->ox1 : s->oy1;
+            double* S2 = axis == 0 ? s->ox2 : s->oy2;
+            for (int f = 0; f < 4; ++f) {
+                int sb, lb, o, nl;
+                ob_geom(s, axis, f, side, &sb, &lb, &o, &nl);
+                const double* d = ob_field(s, f);
+                for (int b = 0; b < s->NZ; ++b)
+                    for (int a = 0; a < NA; ++a) {
+                        S1[ob_ti(s, axis, f, side, a, b)] = ob_at(s, d, axis, sb - o, a, b);
+                        S2[ob_ti(s, axis, f, side, a, b)] = ob_at(s, d, axis, sb - 2 * o, a, b);
+                    }
+            }
+        }
+    s->omarked = 1;
+}
+
+/* correct_boundary_mass_flux! (open_boundary.jl:1024-1083) on the buffers */
+static void ob_correct(oc_sim* s) {
+    const oc_params* P = &s->p;
+    double Q = 0, Aout = 0, Aall = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        double delta = 0;
+        int only_out = 0;
+        if (pass == 1) {
+            if (s->ocorr == 2 || Q == 0) break;
+            only_out = s->ocorr == 1;
+            double Ar = only_out ? Aout : Aall;
+            if (Ar == 0) { only_out = 0; Ar = Aall; }
+            delta = Q / Ar;
+            s->odelta = delta;
+        }
+        for (int axis = 0; axis < 2; ++axis) {
+            if (!(axis == 0 ? s->open_x : s->open_y)) continue;
+            double* Pl = axis == 0 ? s->oxp : s->oyp;
+            int H = axis == 0 ? P->hx : P->hy, Ht = axis == 0 ? P->hy : P->hx, Nt = axis == 0 ? P->ny : P->nx;
+            double area = (axis == 0 ? s->dy : s->dx) * s->dz;
+            for (int side = 0; side < 2; ++side) {
+                int fl = side ? 0 : H;
+                double sg = side ? 1.0 : -1.0;
+                for (int b = P->hz; b < P->hz + P->nz; ++b)
+                    for (int a = Ht; a < Ht + Nt; ++a) {
+                        const double* F = axis == 0 ? s->oxf : s->oyf;
+                        const double wt = F ? F[((int64_t)side * P->nz + (b - P->hz)) * Nt + (a - Ht)] : 1.0;
+                        if (!(wt > 0)) continue;
+                        double* v = &Pl[ob_pi(s, axis, axis, side, fl, a, b)];
+                        double out = sg * *v;
+                        if (pass == 0) {
+                            Q += out * area * wt;
+                            if (out > 0) Aout += area * wt;
+                            Aall += area * wt;
+                        } else if (!only_out || out > 0) {
+                            *v -= sg * delta;
+                        }
+                    }
+            }
+        }
+    }
+    s->oQ = Q;
+    if (s->ocorr == 2 || Q == 0) s->odelta = 0;
+    double R = 0;
+    for (int axis = 0; axis < 2; ++axis) {
+        if (!(axis == 0 ? s->open_x : s->open_y)) continue;
+        double* Pl = axis == 0 ? s->oxp : s->oyp;
+        int H = axis == 0 ? P->hx : P->hy, Ht = axis == 0 ? P->hy : P->hx, Nt = axis == 0 ? P->ny : P->nx;
+        double area = (axis == 0 ? s->dy : s->dx) * s->dz;
+        const double* F = axis == 0 ? s->oxf : s->oyf;
+        for (int side = 0; side < 2; ++side)
+            for (int b = P->hz; b < P->hz + P->nz; ++b)
+                for (int a = Ht; a < Ht + Nt; ++a) {
+                    const double wt = F ? F[((int64_t)side * P->nz + (b - P->hz)) * Nt + (a - Ht)] : 1.0;
+                    if (wt > 0) R += (side ? 1.0 : -1.0) * Pl[ob_pi(s, axis, axis, side, side ? 0 : H, a, b)] * area * wt;
+                }
+    }
+    s->oresid = R;
+}
+
+/* update_open_boundaries! (open_boundary.jl:1137-1152) with a radiating face:
+ * the buffers from the data, the outflow points advanced by the explicit
+ * second-order upstream radiation update from the stage-start values
+ * (_radiate_body!, outflow.jl:240-285), then the mass-flux correction */
+static void ob_update(oc_sim* s, double dt) {
+    if (!ob_radiates(s)) return;
+    int64_t nxp = (int64_t)8 * s->NZ * s->NY * s->oL, nyp = (int64_t)8 * s->NZ * s->oL * s->NX;
+    memcpy(s->oxv, s->oxp, sizeof(double) * nxp);
+    memcpy(s->oyv, s->oyp, sizeof(double) * nyp);
+    memcpy(s->oxp, s->oxd, sizeof(double) * nxp);
+    memcpy(s->oyp, s->oyd, sizeof(double) * nyp);
+    for (int axis = 0; axis < 2; ++axis)
+        for (int side = 0; side < 2; ++side) {
+            if (!s->orad[axis * 2 + side]) continue;
+            int NA = axis == 0 ? s->NY : s->NX;
+            double dn = axis == 0 ? s->dx : s->dy;
+            double* Pl = axis == 0 ? s->oxp : s->oyp;
+            const double* P0 = axis == 0 ? s->oxv : s->oyv;
+            const double* C = axis == 0 ? s->oxc : s->oyc;
+            const double* S1 = axis == 0 ? s->ox1 : s->oy1;
+            const double* S2 = axis == 0 ? s->ox2 : s->oy2;
+            for (int f = 0; f < 4; ++f) {
+                int sb, lb, o, nl;
+                ob_geom(s, axis, f, side, &sb, &lb, &o, &nl);
+                const double* d = ob_field(s, f);
+                for (int b = 0; b < s->NZ; ++b)
+                    for (int a = 0; a < NA; ++a) {
+                        double c = C[ob_ti(s, axis, f, side, a, b)];
+                        if (isnan(c)) continue;
+                        double r = fmin(c * dt / dn, 1.0);
+                        double i1 = s->omarked ? S1[ob_ti(s, axis, f, side, a, b)] : ob_at(s, d, axis, sb - o, a, b);
+                        double i2 = s->omarked ? S2[ob_ti(s, axis, f, side, a, b)] : ob_at(s, d, axis, sb - 2 * o, a, b);
+                        for (int q = 0, l = lb; q < nl; ++q, l += o) {
+                            double p0 = P0[ob_pi(s, axis, f, side, l, a, b)];
+                            Pl[ob_pi(s, axis, f, side, l, a, b)] = p0 - r * (3 * p0 - 4 * i1 + i2) / 2;
+                            i2 = i1;
+                            i1 = p0;
+                        }
+                    }
+            }
+        }
+    s->omarked = 0;
+    ob_correct(s);
+}
+
+/* combine_open_boundaries! (open_boundary.jl:1262-1280): buffer = a snapshot + b buffer */
+static void ob_combine(oc_sim* s, double a, double b) {
+    if (!ob_radiates(s)) return;
+    int64_t nxp = (int64_t)8 * s->NZ * s->NY * s->oL, nyp = (int64_t)8 * s->NZ * s->oL * s->NX;
+    for (int64_t q = 0; q < nxp; ++q) s->oxp[q] = a * s->oxs[q] + b * s->oxp[q];
+    for (int64_t q = 0; q < nyp; ++q) s->oyp[q] = a * s->oys[q] + b * s->oyp[q];
+}
+
 /* Open lateral faces (open_boundary_conditions and the halo fills of
  * src/boundary_conditions/open_boundary.jl:532-807): copies of the planes
  * (the layout of aeo_set_open), the modes; the CG rebuilt on the domain's
@@ -2471,6 +2694,7 @@ int oc_set_open(oc_sim* s, int open_x, int open_y, const double* xp, const doubl
     s->oL = L;
     s->open_x = open_x != 0;
     s->open_y = open_y != 0;
+    for (int q = 0; q < 4; ++q) s->orad[q] = 0;   /* Dirichlet until oc_set_open_outflow */
     /* the operator on the current apertures (the wall faces already closed) */
     int64_t n[3] = {(int64_t)(P->nx + 1) * P->ny * P->nz, (int64_t)P->nx * (P->ny + 1) * P->nz,
                     (int64_t)P->nx * P->ny * (P->nz + 1)};
@@ -2484,6 +2708,40 @@ int oc_set_open(oc_sim* s, int open_x, int open_y, const double* xp, const doubl
     for (int d = 0; d < 3; ++d) free(a[d]);
     if (r) return r;
     oc_fill_state_halos(s);
+    return 0;
+}
+
+/* The radiating outflow of open faces already set (oc_set_open): rad[4]
+ * (west, east, south, north) 1 = :convective, the correction mode (0 uniform,
+ * 1 outflow only, 2 none) and the raw data planes (before the correction) in
+ * the layout of the buffers.  All zero: Dirichlet outflow everywhere. */
+void oc_open_ledger(const oc_sim* s, double* out) { out[0] = s->oQ; out[1] = s->oresid; out[2] = s->odelta; }
+
+int oc_set_open_outflow(oc_sim* s, const int* rad, int corr, const double* xd, const double* yd,
+                        const double* xf, const double* yf) {
+    if (!(s->open_x || s->open_y) || !rad || corr < 0 || corr > 2) return -1;
+    for (int q = 0; q < 4; ++q) {
+        if (rad[q] && !(q < 2 ? s->open_x : s->open_y)) return -1;
+        s->orad[q] = rad[q] != 0;
+    }
+    s->ocorr = corr;
+    int64_t nxp = (int64_t)8 * s->NZ * s->NY * s->oL, nyp = (int64_t)8 * s->NZ * s->oL * s->NX;
+    int64_t ntx = (int64_t)8 * s->NZ * s->NY, nty = (int64_t)8 * s->NZ * s->NX;
+    double** bufs[6] = {&s->oxd, &s->oyd, &s->oxs, &s->oys, &s->oxv, &s->oyv};
+    for (int q = 0; q < 6; ++q) { free(*bufs[q]); *bufs[q] = dalloc(q % 2 ? nyp : nxp); }
+    double** tb[6] = {&s->oxc, &s->oyc, &s->ox1, &s->oy1, &s->ox2, &s->oy2};
+    for (int q = 0; q < 6; ++q) { free(*tb[q]); *tb[q] = dalloc(q % 2 ? nty : ntx); }
+    free(s->oxf); free(s->oyf);
+    s->oxf = dalloc((int64_t)2 * s->p.nz * s->p.ny);
+    s->oyf = dalloc((int64_t)2 * s->p.nz * s->p.nx);
+    for (int64_t q = 0; q < (int64_t)2 * s->p.nz * s->p.ny; ++q) s->oxf[q] = xf ? xf[q] : 1.0;
+    for (int64_t q = 0; q < (int64_t)2 * s->p.nz * s->p.nx; ++q) s->oyf[q] = yf ? yf[q] : 1.0;
+    if (ob_radiates(s)) {
+        if ((s->open_x && !xd) || (s->open_y && !yd)) return -1;
+        if (s->open_x) memcpy(s->oxd, xd, sizeof(double) * nxp);
+        if (s->open_y) memcpy(s->oyd, yd, sizeof(double) * nyp);
+    }
+    s->omarked = 0;
     return 0;
 }
 
@@ -2505,6 +2763,9 @@ void oc_destroy(oc_sim* s) {
     for (size_t q = 0; q < sizeof(ptrs) / sizeof(ptrs[0]); ++q) free(ptrs[q]);
     free(s->hat); free(s->twx);
     free(s->apx); free(s->apy); free(s->apz); free(s->cgx); free(s->ibm); free(s->oxp); free(s->oyp);
+    free(s->oxd); free(s->oyd); free(s->oxs); free(s->oys); free(s->oxv); free(s->oyv);
+    free(s->oxc); free(s->oyc); free(s->ox1); free(s->oy1); free(s->ox2); free(s->oy2);
+    free(s->oxf); free(s->oyf);
     for (int f = 0; f < 10; ++f) free(s->dyn[f]);
     free(s->dyn_lm); free(s->dyn_mm); free(s->cs2); free(s->amd_bg);
     free(s->lag_ilm); free(s->lag_imm); free(s->lag_up); free(s->lag_vp); free(s->lag_wp);

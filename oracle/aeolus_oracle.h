@@ -108,6 +108,11 @@ int oc_set_ibm(oc_sim* s, const unsigned char* mask, double tau);
 int oc_pcg_stats(const oc_sim* s, int* iterations, int* status, double* residual, double* bnorm);
 /* open lateral faces: planes in the layout of aeo_set_open (FP64), modes[4] */
 int oc_set_open(oc_sim* s, int open_x, int open_y, const double* xp, const double* yp, const int* modes);
+/* radiating (:convective) outflow per side, the correction mode, the raw data planes */
+int oc_set_open_outflow(oc_sim* s, const int* rad, int corr, const double* xd, const double* yd,
+                        const double* xf, const double* yf);
+/* Q, residual, delta of the last correction on the device-side update */
+void oc_open_ledger(const oc_sim* s, double* out);
 void oc_set_threads(int n);
 /* advect_positive! (src/AdvectionSchemes.jl:1100-1160): add (accumulate) or
  * write -div(u phi) with the positivity limiter; storage arrays of the

@@ -86,6 +86,9 @@ def load():
     lib.oc_advect_positive.argtypes = [P, _D, _D, _D, _D, _D, C.c_double, C.c_int, C.c_int]
     lib.oc_set_apertures.argtypes = [P, _D, _D, _D, C.c_double, C.c_int]
     lib.oc_set_open.argtypes = [P, C.c_int, C.c_int, _D, _D, C.POINTER(C.c_int)]
+    lib.oc_set_open_outflow.argtypes = [P, C.POINTER(C.c_int), C.c_int, _D, _D, _D, _D]
+    lib.oc_open_ledger.argtypes = [P, _D]
+    lib.oc_open_ledger.restype = None
     lib.oc_set_sgs_buoyancy.argtypes = [P, _D]
     lib.oc_set_lagrangian.argtypes = [P, C.c_double, C.c_double, C.c_double]
     lib.oc_set_tke.argtypes = [P, C.c_double, C.c_double, C.c_double, C.c_int]
@@ -308,6 +311,18 @@ class OracleSimulation:
                                  m.ctypes.data_as(C.POINTER(C.c_int))) != 0:
             raise ValueError("oracle: set_open rejected (needs the PCG solver on the uniform Boussinesq core, "
                              "walls in z, a static SGS closure if any)")
+        rad = np.ascontiguousarray(obc.radiating, dtype=np.int32)
+        xd, yd, _ = obc.packed(raw=True)
+        xf, yf = obc.face_weights()
+        self._open_raw = (rad, xd, yd, xf, yf)
+        if self._lib.oc_set_open_outflow(self._h, rad.ctypes.data_as(C.POINTER(C.c_int)), int(obc.correction_code),
+                                         _p(xd), _p(yd), _p(xf), _p(yf)) != 0:
+            raise ValueError("oracle: set_open_outflow rejected")
+
+    def open_ledger(self):
+        out = np.zeros(3)
+        self._lib.oc_open_ledger(self._h, _p(out))
+        return {"Q": out[0], "residual": out[1], "delta": out[2]}
 
     def pcg_stats(self):
         it, stt = C.c_int(), C.c_int()
