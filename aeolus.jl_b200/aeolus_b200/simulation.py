@@ -344,6 +344,12 @@ class Simulation:
                    self._h)
         self._open = obc
 
+    def open_planes(self):
+        """The current plane buffers (x, y) in OpenBoundarySet.packed's layout."""
+        xp, yp, _ = self._open.packed()
+        _lib.check(self._lib.aeo_get_open_planes(self._h, _ptr(xp), _ptr(yp)), self._h)
+        return xp, yp
+
     def open_ledger(self) -> dict:
         """Q, residual and delta of the last mass-flux correction on the device
         (a radiating open set)."""

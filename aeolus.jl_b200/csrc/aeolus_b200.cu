@@ -123,6 +123,7 @@ struct CoreBase {
     virtual aeo_status set_open_outflow(const int* rad, int corr, const double* xd, const double* yd, const double* xw,
                                         const double* yw) = 0;
     virtual aeo_status open_ledger(double* out) = 0;
+    virtual aeo_status get_open_planes(double* xp, double* yp) = 0;
     virtual aeo_status set_ibm(const uint8_t* mask, double tau) = 0;
     virtual aeo_status set_sgs_buoyancy(const double* bg) = 0;
     virtual aeo_status set_lagrangian(double c0, double theta, double memory_time) = 0;
@@ -1084,6 +1085,22 @@ struct Core : CoreBase {
         for (double v : wy) if (!(v >= 0.0 && v <= 1.0)) { fail("set_open_outflow: face weights lie in [0, 1]"); return AEO_ERR_ARGUMENT; }
         CK(cudaMemcpy((void*)ob.xw, wx.data(), wx.size() * sizeof(double), cudaMemcpyHostToDevice));
         CK(cudaMemcpy((void*)ob.yw, wy.data(), wy.size() * sizeof(double), cudaMemcpyHostToDevice));
+        return AEO_OK;
+    }
+
+    // The current plane buffers (state of a radiating open set: at its outflow
+    // points they hold radiated values the data cannot reproduce;
+    // open_boundary_checkpoint, open_boundary.jl:1282-1305), FP64 in
+    // aeo_set_open's layout (theta with its offset added back)
+    aeo_status get_open_planes(double* xo, double* yo) override {
+        if (!(open_x || open_y)) { fail("get_open_planes: no open face"); return AEO_ERR_STATE; }
+        CK(cudaStreamSynchronize(st));
+        const size_t nxp = ob_nxp(), nyp = ob_nyp();
+        std::vector<R> hx(nxp), hy(nyp);
+        CK(cudaMemcpy(hx.data(), ob.xp, nxp * sizeof(R), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(hy.data(), ob.yp, nyp * sizeof(R), cudaMemcpyDeviceToHost));
+        if (xo) for (size_t q = 0; q < nxp; ++q) xo[q] = (double)hx[q] + (q / (nxp / 4) == 3 ? th_off : 0.0);
+        if (yo) for (size_t q = 0; q < nyp; ++q) yo[q] = (double)hy[q] + (q / (nyp / 4) == 3 ? th_off : 0.0);
         return AEO_OK;
     }
 
@@ -2390,6 +2407,11 @@ aeo_status aeo_set_open_outflow(aeo_sim* h, const int32_t* radiate, int32_t corr
                                 const double* y_data, const double* x_weights, const double* y_weights) {
     ENTER(h);
     return h->core->set_open_outflow(radiate, correction, x_data, y_data, x_weights, y_weights);
+}
+
+aeo_status aeo_get_open_planes(aeo_sim* h, double* x_planes, double* y_planes) {
+    ENTER(h);
+    return h->core->get_open_planes(x_planes, y_planes);
 }
 
 aeo_status aeo_open_ledger(aeo_sim* h, double* out) {

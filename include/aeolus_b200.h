@@ -426,6 +426,11 @@ aeo_status aeo_set_open_outflow(aeo_sim* h, const int32_t* radiate, int32_t corr
 /* Q, residual and delta of the last mass-flux correction of a radiating open
  * set (open_boundary_ledger, open_boundary.jl:1437-1450); synchronises */
 aeo_status aeo_open_ledger(aeo_sim* h, double* out);
+/* The current open-face plane buffers in aeo_set_open's layout (FP64): on a
+ * radiating face they are state, the radiated outflow points included
+ * (open_boundary_checkpoint, src/boundary_conditions/open_boundary.jl:1282-1305);
+ * synchronises */
+aeo_status aeo_get_open_planes(aeo_sim* h, double* x_planes, double* y_planes);
 /* Residual -> error pairs from the run's own snapshots (no reference
  * counterpart; it feeds the learned preconditioner): b receives the
  * right-hand side of the last projection's solve (the predictor's cut-cell

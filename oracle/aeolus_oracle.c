@@ -1788,8 +1788,8 @@ static void substage(oc_sim* s, double dt, int stage, double ca, double cb) {
     const oc_params* P = &s->p;
     int Hx = P->hx, Hy = P->hy, Hz = P->hz, Nx = P->nx, Ny = P->ny, Nz = P->nz;
     int anel = P->core == OC_CORE_ANELASTIC;
-    if (ob_radiates(s)) ob_mark(s);          /* the stage-start layers (src/Simulations.jl:538) */
     oc_fill_state_halos(s);
+    if (ob_radiates(s)) ob_mark(s);          /* the stage-start layers, after the fill (src/Simulations.jl:537-538) */
     compute_tendencies(s);
     /* 7. predictor */
 #pragma omp parallel for collapse(2) schedule(static)
@@ -2715,6 +2715,12 @@ int oc_set_open(oc_sim* s, int open_x, int open_y, const double* xp, const doubl
  * (west, east, south, north) 1 = :convective, the correction mode (0 uniform,
  * 1 outflow only, 2 none) and the raw data planes (before the correction) in
  * the layout of the buffers.  All zero: Dirichlet outflow everywhere. */
+void oc_get_open_planes(const oc_sim* s, double* xp, double* yp) {
+    int64_t nxp = (int64_t)8 * s->NZ * s->NY * s->oL, nyp = (int64_t)8 * s->NZ * s->oL * s->NX;
+    if (xp && s->oxp) memcpy(xp, s->oxp, sizeof(double) * nxp);
+    if (yp && s->oyp) memcpy(yp, s->oyp, sizeof(double) * nyp);
+}
+
 void oc_open_ledger(const oc_sim* s, double* out) { out[0] = s->oQ; out[1] = s->oresid; out[2] = s->odelta; }
 
 int oc_set_open_outflow(oc_sim* s, const int* rad, int corr, const double* xd, const double* yd,

@@ -113,6 +113,8 @@ int oc_set_open_outflow(oc_sim* s, const int* rad, int corr, const double* xd, c
                         const double* xf, const double* yf);
 /* Q, residual, delta of the last correction on the device-side update */
 void oc_open_ledger(const oc_sim* s, double* out);
+/* the current plane buffers (layout of oc_set_open) */
+void oc_get_open_planes(const oc_sim* s, double* xp, double* yp);
 void oc_set_threads(int n);
 /* advect_positive! (src/AdvectionSchemes.jl:1100-1160): add (accumulate) or
  * write -div(u phi) with the positivity limiter; storage arrays of the

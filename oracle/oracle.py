@@ -89,6 +89,8 @@ def load():
     lib.oc_set_open_outflow.argtypes = [P, C.POINTER(C.c_int), C.c_int, _D, _D, _D, _D]
     lib.oc_open_ledger.argtypes = [P, _D]
     lib.oc_open_ledger.restype = None
+    lib.oc_get_open_planes.argtypes = [P, _D, _D]
+    lib.oc_get_open_planes.restype = None
     lib.oc_set_sgs_buoyancy.argtypes = [P, _D]
     lib.oc_set_lagrangian.argtypes = [P, C.c_double, C.c_double, C.c_double]
     lib.oc_set_tke.argtypes = [P, C.c_double, C.c_double, C.c_double, C.c_int]
@@ -318,6 +320,11 @@ class OracleSimulation:
         if self._lib.oc_set_open_outflow(self._h, rad.ctypes.data_as(C.POINTER(C.c_int)), int(obc.correction_code),
                                          _p(xd), _p(yd), _p(xf), _p(yf)) != 0:
             raise ValueError("oracle: set_open_outflow rejected")
+
+    def open_planes(self):
+        xp, yp = (np.zeros_like(a) for a in self._open_raw[1:3])
+        self._lib.oc_get_open_planes(self._h, _p(xp), _p(yp))
+        return xp, yp
 
     def open_ledger(self):
         out = np.zeros(3)
