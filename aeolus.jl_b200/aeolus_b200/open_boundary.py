@@ -22,10 +22,11 @@ net boundary flux vanishes.
 Built here: open x and/or y faces over a wall bottom and a wall (rigid-lid)
 top, on the uniform Boussinesq core with the PCG projection; steady data
 (`ProfileBoundaryData`, :336-408, and `FunctionBoundaryData` evaluated at one
-time, :330-380); outflow `:dirichlet` (every point takes the data) or
-`:convective` per side (src/boundary_conditions/outflow.jl: an outflow point
-is advanced by the radiation equation with the outward normal velocity as
-phase speed, on the device before every projection); normal halo `:value`;
+time, :330-380); outflow `:dirichlet` (every point takes the data),
+`:convective` or `:orlanski` per side (src/boundary_conditions/outflow.jl: an
+outflow point is advanced by the radiation equation with the outward normal
+velocity, or the Orlanski phase speed, on the device before every
+projection); normal halo `:value`;
 scalar halo `:value` or `:mirror`; corrections `:uniform`, `:outflow_only`
 and `:none`.  Dirichlet buffers are static, so their correction is applied
 once here (the reference applies the same correction to the same data
@@ -191,8 +192,10 @@ class OpenBoundarySet:
 
     @property
     def radiating(self):
-        """The per-side flags (west, east, south, north) of a :convective outflow."""
-        return np.array([self.outflow.get(sd, "dirichlet") == "convective" for sd in ("west", "east", "south", "north")],
+        """The per-side outflow codes (west, east, south, north): 0 :dirichlet,
+        1 :convective, 2 :orlanski."""
+        code = {"dirichlet": 0, "convective": 1, "orlanski": 2}
+        return np.array([code[self.outflow.get(sd, "dirichlet")] for sd in ("west", "east", "south", "north")],
                         dtype=np.int32)
 
     @property
@@ -361,12 +364,12 @@ def open_boundary_conditions(grid: Grid, data, x: str = "open", y: str = "period
     alike), bottom and top walls.  `fields` names the fields with boundary
     data (the three velocity components and theta); the planes are filled
     from `data` and the normal velocities corrected (`correction`).
-    `outflow` is "dirichlet" or "convective", or a dict of those per side;
+    `outflow` is "dirichlet", "convective" or "orlanski", or a dict of those per side;
     `solid` (a storage-shaped bool mask) marks where obstacles touch the
     faces (OpenBoundarySet.mark_solids); `apertures` (the projection's face
     apertures) weight the correction (OpenBoundarySet.set_apertures).
     Raises ValueError for what is not built (an open top or bottom, the
-    :odd normal halo, the :orlanski outflow, the :inflow scalar halo)."""
+    :odd normal halo, the :inflow scalar halo)."""
     if x not in ("open", "periodic") or y not in ("open", "periodic"):
         raise ValueError("x and y are 'open' or 'periodic'")
     if x == "periodic" and y == "periodic":
@@ -389,8 +392,8 @@ def open_boundary_conditions(grid: Grid, data, x: str = "open", y: str = "period
     for sd, mode in outflow.items():
         if sd not in sides_all:
             raise ValueError(f"outflow: unknown side {sd!r} (use {sides_all}; an open top is not built)")
-        if mode not in ("dirichlet", "convective"):
-            raise ValueError(f"outflow mode must be 'dirichlet' or 'convective' (:orlanski is not built), got {mode!r}")
+        if mode not in ("dirichlet", "convective", "orlanski"):
+            raise ValueError(f"outflow mode must be 'dirichlet', 'convective' or 'orlanski', got {mode!r}")
     for need in ("u", "v", "w"):
         if need not in fields:
             raise ValueError("open faces need data for u, v and w")
@@ -428,7 +431,7 @@ def open_boundary_conditions(grid: Grid, data, x: str = "open", y: str = "period
             fluid = np.ones((ny if ax == 0 else nx, nz), dtype=bool)
             planes.append(OpenPlane(name, side, ax, high, normal, mode, int(r[0]), np.ascontiguousarray(vals), fluid))
     for sd, mode in outflow.items():
-        if mode == "convective" and sd not in sides and given_per_side:
+        if mode != "dirichlet" and sd not in sides and given_per_side:
             raise ValueError(f"outflow: side {sd!r} is not an open face of this box")
     obs = OpenBoundarySet(grid, planes, correction, x == "open", y == "open",
                           {sd: outflow.get(sd, "dirichlet") for sd in sides})

@@ -122,6 +122,13 @@ struct OpenSet {
     double* led;
     const double* xw;     // weights of the normal planes' boundary faces, [side][Nz][Ny] / [side][Nz][Nx] (0 solid)
     const double* yw;
+    // the :orlanski outflow (rad[q] == 2): the interior layer next to the face
+    // at the previous step start per plane point, and (device) whether it is
+    // set and the length of the previous step
+    R* xh;
+    R* yh;
+    int* hist_ok;
+    double* last_dt;
 };
 
 // ---- radiating outflow (src/boundary_conditions/outflow.jl) --------------------
@@ -165,14 +172,30 @@ __device__ __forceinline__ R field_at(const Geo& g, const R* d, int axis, int li
 // per radiating plane point the phase speed c = the outward normal velocity
 // of the boundary face (the mean of two faces for a component staggered
 // along the face), NaN where it does not point out (the data is kept)
+//
+// :orlanski (outflow.jl:152-181): for the tangential velocities and the
+// scalars, c = -(dphi/dt)/(dphi/dn) at the interior layer next to the face
+// from its value at this and at the previous step start, clipped to
+// [0, dn/dtau] (Miller & Thorpe 1981), NaN -> 0; the convective speed on the
+// first step and for the normal velocity.  The fields are the step-start state.
 template <typename R>
-__global__ void ob_phase_kernel(Geo g, OpenSet<R> ob) {
+__global__ void ob_phase_kernel(Geo g, OpenSet<R> ob, const R* u, const R* v, const R* w, const R* th,
+                                const double* __restrict__ dtp) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     int axis, f, side, a, b;
     if (!ob_point(g, t, &axis, &f, &side, &a, &b)) return;
     R* C = axis == 0 ? ob.xc : ob.yc;
     const long long ti = t - (axis == 0 ? 0 : 8LL * (g.nz + 2 * AEO_H) * (g.ny + 2 * AEO_H));
-    if (!ob.rad[axis * 2 + side] || ob.mode[f] != 0) { C[ti] = R(NAN); return; }
+    const int mode = ob.rad[axis * 2 + side];
+    if (!mode || ob.mode[f] != 0) { C[ti] = R(NAN); return; }
+    R phi1 = R(0), phi2 = R(0);
+    if (mode == 2) {
+        int sb, lb, o, nl;
+        ob_geom(g, axis, f, side, &sb, &lb, &o, &nl);
+        const R* d = f == 0 ? u : f == 1 ? v : f == 2 ? w : th;
+        phi1 = field_at(g, d, axis, sb - o, a, b);
+        phi2 = field_at(g, d, axis, sb - 2 * o, a, b);
+    }
     const R* P = axis == 0 ? ob.xp : ob.yp;
     const int fl = side ? 0 : AEO_H;
     const R sg = side ? R(1) : R(-1);
@@ -187,7 +210,28 @@ __global__ void ob_phase_kernel(Geo g, OpenSet<R> ob) {
     } else {
         un = sg * P[ob_pi(g, ob, axis, axis, side, fl, a, b)];
     }
-    C[ti] = un > R(0) ? un : R(NAN);
+    R* Hs = axis == 0 ? ob.xh : ob.yh;
+    if (!(un > R(0))) {
+        C[ti] = R(NAN);
+    } else if (mode == 2 && f != axis && *ob.hist_ok) {
+        const double dtau = *ob.last_dt, dn = axis == 0 ? g.dx : g.dy;
+        const double num = -((double)phi1 - (double)Hs[ti]) / dtau;
+        const double den = ((double)phi1 - (double)phi2) / dn;
+        const double c = num / den;
+        const double cmax = dn / dtau;
+        C[ti] = R(c != c ? 0.0 : (c < 0.0 ? 0.0 : (c > cmax ? cmax : c)));
+    } else {
+        C[ti] = un;
+    }
+    if (mode == 2) Hs[ti] = phi1;
+    (void)dtp;
+}
+
+// after the phase speeds of a step: the history is set, and this step's length
+// is the next one's tau
+__global__ void ob_hist_kernel(int* hist_ok, double* last_dt, const double* __restrict__ dtp) {
+    *hist_ok = 1;
+    *last_dt = *dtp;
 }
 
 // mark_open_boundary_stage! (outflow.jl:198-237): the two interior layers next

@@ -1042,6 +1042,7 @@ struct Core : CoreBase {
         if (!rad || corr < 0 || corr > 2) { fail("set_open_outflow: NULL flags or a correction mode outside 0..2"); return AEO_ERR_ARGUMENT; }
         bool any = false;
         for (int q = 0; q < 4; ++q) {
+            if (rad[q] < 0 || rad[q] > 2) { fail("set_open_outflow: a side's mode is 0 dirichlet, 1 convective or 2 orlanski"); return AEO_ERR_ARGUMENT; }
             if (rad[q] && !(q < 2 ? open_x : open_y)) { fail("set_open_outflow: a radiating side that is not open"); return AEO_ERR_ARGUMENT; }
             any = any || rad[q];
         }
@@ -1049,7 +1050,7 @@ struct Core : CoreBase {
         CK(cudaStreamSynchronize(st));
         drop_graphs();
         ob.corr = corr;
-        for (int q = 0; q < 4; ++q) ob.rad[q] = rad[q] ? 1 : 0;
+        for (int q = 0; q < 4; ++q) ob.rad[q] = rad[q];
         ob_rad = any;
         if (!any) return AEO_OK;
         const int H = AEO_H, NX = g.nx + 2 * H, NY = g.ny + 2 * H, NZ = g.nz + 2 * H, L = H + 1;
@@ -1067,6 +1068,14 @@ struct Core : CoreBase {
             if (aeo_status e = alloc(&dyw, (size_t)2 * g.nz * g.nx)) return e;
             ob.xw = dxw;
             ob.yw = dyw;
+            R *hx_ = nullptr, *hy_ = nullptr;
+            if (aeo_status e = alloc(&hx_, ntx)) return e;
+            if (aeo_status e = alloc(&hy_, nty)) return e;
+            int* hok = nullptr;
+            double* ldt = nullptr;
+            if (aeo_status e = alloc(&hok, 1)) return e;
+            if (aeo_status e = alloc(&ldt, 1)) return e;
+            ob.xh = hx_; ob.yh = hy_; ob.hist_ok = hok; ob.last_dt = ldt;
             ob.xd = b[0]; ob.yd = b[1]; ob.xs = b[2]; ob.ys = b[3]; ob.xv = b[4]; ob.yv = b[5];
             ob.xc = b[6]; ob.yc = b[7]; ob.x1 = b[8]; ob.y1 = b[9]; ob.x2 = b[10]; ob.y2 = b[11];
             ob.led = led;
@@ -1078,6 +1087,7 @@ struct Core : CoreBase {
             for (size_t q = 0; q < nyp; ++q) hy[q] = R(yd[q] - (q / (nyp / 4) == 3 ? th_off : 0.0));
         CK(cudaMemcpy((void*)ob.xd, hx.data(), nxp * sizeof(R), cudaMemcpyHostToDevice));
         CK(cudaMemcpy((void*)ob.yd, hy.data(), nyp * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemset(ob.hist_ok, 0, sizeof(int)));   // the Orlanski history starts empty
         std::vector<double> wx((size_t)2 * g.nz * g.ny, 1.0), wy((size_t)2 * g.nz * g.nx, 1.0);
         if (xw) std::copy(xw, xw + wx.size(), wx.begin());
         if (yw) std::copy(yw, yw + wy.size(), wy.begin());
@@ -1118,10 +1128,13 @@ struct Core : CoreBase {
     }
     size_t ob_nxp() const { return (size_t)8 * (g.nz + 2 * AEO_H) * (g.ny + 2 * AEO_H) * (AEO_H + 1); }
     size_t ob_nyp() const { return (size_t)8 * (g.nz + 2 * AEO_H) * (AEO_H + 1) * (g.nx + 2 * AEO_H); }
-    aeo_status ob_prepare() {
+    aeo_status ob_prepare(int s_state) {
         CK(cudaMemcpyAsync(ob.xs, ob.xp, ob_nxp() * sizeof(R), cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(ob.ys, ob.yp, ob_nyp() * sizeof(R), cudaMemcpyDeviceToDevice, st));
-        ob_phase_kernel<R><<<ob_blocks(), 256, 0, st>>>(g, ob);
+        R** f = P[s_state];
+        ob_phase_kernel<R><<<ob_blocks(), 256, 0, st>>>(g, ob, f[0], f[1], f[2], f[3], &d_sc->dt);
+        CKL();
+        ob_hist_kernel<<<1, 1, 0, st>>>(ob.hist_ok, ob.last_dt, &d_sc->dt);
         CKL();
         return AEO_OK;
     }
@@ -1519,7 +1532,7 @@ struct Core : CoreBase {
             if (aeo_status e = enqueue_pick(c)) return e;
         const R inv3 = R(1) / R(3), two3 = R(2) * inv3;
         if (ob_rad)
-            if (aeo_status e = ob_prepare()) return e;
+            if (aeo_status e = ob_prepare(c)) return e;
         if (aeo_status e = substage(c, 2, c, 0, R(0), R(0))) return e;
         if (aeo_status e = substage(2, 3, c, 1, R(0.75), R(0.25))) return e;
         if (aeo_status e = substage(3, c ^ 1, c, 1, inv3, two3)) return e;
@@ -1665,7 +1678,7 @@ struct Core : CoreBase {
         CKL();
         for (int s = 0; s < n; ++s) {
             if (ob_rad)
-                if (aeo_status e = ob_prepare()) return e;
+                if (aeo_status e = ob_prepare(cur)) return e;
             if (aeo_status e = substage(cur, cur ^ 1, cur, 0, R(0), R(0))) return e;
             if (aeo_status e = commit_sgs(cur ^ 1)) return e;
             cur ^= 1;

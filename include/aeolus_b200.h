@@ -405,7 +405,11 @@ aeo_status aeo_set_open(aeo_sim* h, int32_t open_x, int32_t open_y, const double
                         const int32_t* modes);
 /* Radiating outflow of the open faces set by aeo_set_open (the :convective
  * outflow of open_boundary_conditions, src/boundary_conditions/outflow.jl):
- * radiate[4] (west, east, south, north) 1 = :convective, 0 = :dirichlet;
+ * radiate[4] (west, east, south, north) 0 = :dirichlet, 1 = :convective,
+ * 2 = :orlanski (the tangential velocities and theta take the Orlanski 1976
+ * phase speed of the interior layer next to the face between this and the
+ * previous step start, clipped to [0, dn/dtau]; the normal velocity and the
+ * first step the convective one; outflow.jl:136-182);
  * correction 0 :uniform, 1 :outflow_only, 2 :none; x_data / y_data the raw
  * boundary data (before the correction) in aeo_set_open's layout.  Each step
  * then fixes, at its start, the outflow points (outward normal velocity of

@@ -104,6 +104,9 @@ struct oc_sim {
      * the correction mode (0 uniform, 1 outflow only, 2 none) and its ledger */
     int orad[4], ocorr, omarked;
     double *oxf, *oyf;            /* weights of the normal planes' boundary faces (0 solid) */
+    double *oxh, *oyh;            /* :orlanski history: the interior layer at the previous step start */
+    int ohist;
+    double olast_dt;
     double *oxd, *oyd, *oxs, *oys, *oxv, *oyv;
     double *oxc, *oyc, *ox1, *oy1, *ox2, *oy2;
     double oQ, odelta, oresid;
@@ -111,7 +114,7 @@ struct oc_sim {
 
 /* the radiating outflow of open faces (defined with oc_set_open) */
 static int ob_radiates(const oc_sim* s);
-static void ob_prepare(oc_sim* s);
+static void ob_prepare(oc_sim* s, double dt);
 static void ob_mark(oc_sim* s);
 static void ob_update(oc_sim* s, double dt);
 static void ob_combine(oc_sim* s, double a, double b);
@@ -1894,7 +1897,7 @@ int oc_project(oc_sim* s) {
 
 int oc_step_euler(oc_sim* s, double dt, int nsteps) {
     for (int n = 0; n < nsteps; ++n) {
-        if (ob_radiates(s)) ob_prepare(s);
+        if (ob_radiates(s)) ob_prepare(s, dt);
         substage(s, dt, 0, 0.0, 0.0);
         if (s->p.c_s != 0 && s->p.sgs_model == OC_SGS_LAGRANGIAN) lag_commit(s, dt);   /* once per step */
         if (s->p.c_s != 0 && s->p.sgs_model == OC_SGS_TKE) tke_commit(s, dt);
@@ -1992,7 +1995,7 @@ int oc_step_rk3(oc_sim* s, double dt, int nsteps) {
     size_t b = sizeof(double) * (size_t)s->n;
     double inv3 = 1.0 / 3, two3 = 2 * inv3;
     for (int n = 0; n < nsteps; ++n) {
-        if (ob_radiates(s)) ob_prepare(s);
+        if (ob_radiates(s)) ob_prepare(s, dt);
         memcpy(s->u0, s->u, b); memcpy(s->v0, s->v, b); memcpy(s->w0, s->w, b); memcpy(s->th0, s->th, b);
         substage(s, dt, 0, 0.0, 0.0);
         substage(s, dt, 1, 0.75, 0.25);
@@ -2502,7 +2505,7 @@ static inline void ob_geom(const oc_sim* s, int axis, int f, int side, int* sb, 
  * c = the outward normal velocity of the boundary face when positive, else
  * NaN (an inflow point keeps its data) (_outward_un, _phase_speed_body!,
  * outflow.jl:113-182; :convective) */
-static void ob_prepare(oc_sim* s) {
+static void ob_prepare(oc_sim* s, double dt) {
     int64_t nxp = (int64_t)8 * s->NZ * s->NY * s->oL, nyp = (int64_t)8 * s->NZ * s->oL * s->NX;
     memcpy(s->oxs, s->oxp, sizeof(double) * nxp);
     memcpy(s->oys, s->oyp, sizeof(double) * nyp);
@@ -2515,10 +2518,19 @@ static void ob_prepare(oc_sim* s) {
             int H = axis == 0 ? s->p.hx : s->p.hy;
             int fl = side ? 0 : H;                       /* the normal plane's boundary face */
             double sg = side ? 1.0 : -1.0;
+            int mode = s->orad[axis * 2 + side];
+            double* Hs = axis == 0 ? s->oxh : s->oyh;
+            double dn = axis == 0 ? s->dx : s->dy;
             for (int f = 0; f < 4; ++f)
                 for (int b = 0; b < s->NZ; ++b)
                     for (int a = 0; a < NA; ++a) {
-                        double un;
+                        double un, phi1 = 0, phi2 = 0;
+                        if (mode == 2) {
+                            int sb, lb, o, nl;
+                            ob_geom(s, axis, f, side, &sb, &lb, &o, &nl);
+                            phi1 = ob_at(s, ob_field(s, f), axis, sb - o, a, b);
+                            phi2 = ob_at(s, ob_field(s, f), axis, sb - 2 * o, a, b);
+                        }
                         /* staggered along a tangential direction: the mean of the two faces */
                         int st1 = (axis == 0 && f == 1) || (axis == 1 && f == 0), st2 = f == 2;
                         if (st1) {
@@ -2530,9 +2542,22 @@ static void ob_prepare(oc_sim* s) {
                         } else {
                             un = sg * P[ob_pi(s, axis, axis, side, fl, a, b)];
                         }
-                        C[ob_ti(s, axis, f, side, a, b)] = (s->omode[f] == 0 && un > 0) ? un : NAN;
+                        int64_t ti = ob_ti(s, axis, f, side, a, b);
+                        if (!(s->omode[f] == 0 && un > 0)) {
+                            C[ti] = NAN;
+                        } else if (mode == 2 && f != axis && s->ohist) {
+                            /* Orlanski (1976), clipped to [0, dn/dtau] (Miller & Thorpe 1981) */
+                            double num = -(phi1 - Hs[ti]) / s->olast_dt, den = (phi1 - phi2) / dn;
+                            double c = num / den, cmax = dn / s->olast_dt;
+                            C[ti] = isnan(c) ? 0.0 : (c < 0 ? 0.0 : (c > cmax ? cmax : c));
+                        } else {
+                            C[ti] = un;
+                        }
+                        if (mode == 2) Hs[ti] = phi1;
                     }
         }
+    s->ohist = 1;
+    s->olast_dt = dt;
 }
 
 /* mark_open_boundary_stage! (outflow.jl:198-237): the two interior layers
@@ -2727,16 +2752,17 @@ int oc_set_open_outflow(oc_sim* s, const int* rad, int corr, const double* xd, c
                         const double* xf, const double* yf) {
     if (!(s->open_x || s->open_y) || !rad || corr < 0 || corr > 2) return -1;
     for (int q = 0; q < 4; ++q) {
-        if (rad[q] && !(q < 2 ? s->open_x : s->open_y)) return -1;
-        s->orad[q] = rad[q] != 0;
+        if (rad[q] < 0 || rad[q] > 2 || (rad[q] && !(q < 2 ? s->open_x : s->open_y))) return -1;
+        s->orad[q] = rad[q];
     }
+    s->ohist = 0;
     s->ocorr = corr;
     int64_t nxp = (int64_t)8 * s->NZ * s->NY * s->oL, nyp = (int64_t)8 * s->NZ * s->oL * s->NX;
     int64_t ntx = (int64_t)8 * s->NZ * s->NY, nty = (int64_t)8 * s->NZ * s->NX;
     double** bufs[6] = {&s->oxd, &s->oyd, &s->oxs, &s->oys, &s->oxv, &s->oyv};
     for (int q = 0; q < 6; ++q) { free(*bufs[q]); *bufs[q] = dalloc(q % 2 ? nyp : nxp); }
-    double** tb[6] = {&s->oxc, &s->oyc, &s->ox1, &s->oy1, &s->ox2, &s->oy2};
-    for (int q = 0; q < 6; ++q) { free(*tb[q]); *tb[q] = dalloc(q % 2 ? nty : ntx); }
+    double** tb[8] = {&s->oxc, &s->oyc, &s->ox1, &s->oy1, &s->ox2, &s->oy2, &s->oxh, &s->oyh};
+    for (int q = 0; q < 8; ++q) { free(*tb[q]); *tb[q] = dalloc(q % 2 ? nty : ntx); }
     free(s->oxf); free(s->oyf);
     s->oxf = dalloc((int64_t)2 * s->p.nz * s->p.ny);
     s->oyf = dalloc((int64_t)2 * s->p.nz * s->p.nx);
@@ -2771,7 +2797,7 @@ void oc_destroy(oc_sim* s) {
     free(s->apx); free(s->apy); free(s->apz); free(s->cgx); free(s->ibm); free(s->oxp); free(s->oyp);
     free(s->oxd); free(s->oyd); free(s->oxs); free(s->oys); free(s->oxv); free(s->oyv);
     free(s->oxc); free(s->oyc); free(s->ox1); free(s->oy1); free(s->ox2); free(s->oy2);
-    free(s->oxf); free(s->oyf);
+    free(s->oxf); free(s->oyf); free(s->oxh); free(s->oyh);
     for (int f = 0; f < 10; ++f) free(s->dyn[f]);
     free(s->dyn_lm); free(s->dyn_mm); free(s->cs2); free(s->amd_bg);
     free(s->lag_ilm); free(s->lag_imm); free(s->lag_up); free(s->lag_vp); free(s->lag_wp);

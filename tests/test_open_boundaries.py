@@ -76,7 +76,7 @@ def test_planes_hold_the_data_at_the_storage_points():
     with pytest.raises(ValueError):
         open_boundary_conditions(g, ProfileBoundaryData(u=1.0), x="open")           # no theta data
     with pytest.raises(ValueError):
-        open_boundary_conditions(g, imb_data(), x="open", outflow="orlanski")        # not built
+        open_boundary_conditions(g, imb_data(), x="open", outflow="sommerfeld")      # no such mode
 
 
 # ---------------------------------------------------------------- steps
@@ -285,7 +285,8 @@ def test_oracle_convective_outflow_lets_a_pulse_leave():
     from oracle.oracle import OracleSimulation
     kept, _ = pulse_residual(OracleSimulation, "dirichlet")
     left, _ = pulse_residual(OracleSimulation, "convective")
-    assert kept > 0.9 and left < 1e-3, (kept, left)
+    orl, _ = pulse_residual(OracleSimulation, "orlanski")
+    assert kept > 0.9 and left < 1e-3 and orl < 1e-2, (kept, left, orl)
 
 
 def test_oracle_convective_outflow_over_boxes_stays_compatible():
@@ -316,13 +317,17 @@ def test_convective_outflow_options():
     assert list(o.radiating) == [0, 1, 0, 0]
     with pytest.raises(ValueError):
         open_boundary_conditions(g, imb_data(), x="open", outflow={"north": "convective"})   # y is periodic
+    o2 = open_boundary_conditions(g, imb_data(), x="open", outflow={"east": "orlanski"})
+    assert list(o2.radiating) == [0, 2, 0, 0]
     with pytest.raises(ValueError):
-        open_boundary_conditions(g, imb_data(), x="open", outflow={"east": "orlanski"})
+        open_boundary_conditions(g, imb_data(), x="open", outflow={"east": "sommerfeld"})
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("outflow,c_s", [({"east": "convective", "north": "convective"}, 0.0),
-                                         ({"east": "convective"}, 0.17), ({"north": "convective"}, 0.17)])
+                                         ({"east": "convective"}, 0.17), ({"north": "convective"}, 0.17),
+                                         ({"east": "orlanski", "north": "convective"}, 0.0),
+                                         ({"north": "orlanski"}, 0.17)])
 def test_convective_outflow_matches_the_oracle(outflow, c_s):
     # radiating outflow over boxes that touch the faces, x and y open; the
     # imbalance of the data and the radiated points corrected before every
@@ -355,6 +360,7 @@ def test_convective_outflow_matches_the_oracle(outflow, c_s):
 def test_convective_outflow_lets_a_pulse_leave_on_the_device():
     from aeolus_b200.simulation import Simulation
     from oracle.oracle import OracleSimulation
-    left, s = pulse_residual(Simulation, "convective")
-    ref, o = pulse_residual(OracleSimulation, "convective")
-    assert left < 1e-3 and abs(left - ref) <= 1e-9, (left, ref)
+    for mode, bound in (("convective", 1e-3), ("orlanski", 1e-2)):
+        left, s = pulse_residual(Simulation, mode)
+        ref, o = pulse_residual(OracleSimulation, mode)
+        assert left < bound and abs(left - ref) <= 1e-9, (mode, left, ref)
