@@ -264,7 +264,7 @@ struct aeo_unet {
         constexpr size_t sm = un::RingShape<CIN, COUT, PF>::smem;
         const int per_sm = sm <= 113 * 1024 ? 2 : 1;
         const int g = Tl.ntiles < sms * per_sm ? Tl.ntiles : sms * per_sm;
-        un::conv_ring_kernel<CIN, COUT, PF><<<g, un::CONV_THREADS, sm, st>>>(a);
+        un::conv_ring_kernel<CIN, COUT, PF><<<g, un::RING_THREADS, sm, st>>>(a);
     }
 
     // one convolution (forward, or transposed with the backward image)

@@ -416,9 +416,23 @@ __device__ __forceinline__ void ring_load_entry(const Tiles& T, const uint4* __r
     }
 }
 
+// Named barriers between the loader / epilogue warps (0-3, which arrive) and
+// the MMA warp (4, which waits): ids 1, 2 "tile i's entries landed" (by the
+// parity of i), ids 3, 4 "the accumulator of tile j is drained" (by the
+// parity of j).  An arrival and its wait are issued the same number of times
+// on every id, whatever happens, so no wait can outlast the kernel.
+__device__ __forceinline__ void nb_arrive(int id) { asm volatile("bar.arrive %0, 160;" :: "r"(id) : "memory"); }
+__device__ __forceinline__ void nb_sync(int id) { asm volatile("bar.sync %0, 160;" :: "r"(id) : "memory"); }
+
+constexpr int RING_THREADS = 160;
+
 // out = act(conv(in) + bias + add) * gate, per the flags (mode 0 tiles).
+// Warps 0-3 load the ring entries and drain the accumulators (a warp reads
+// its TMEM lane quarter); warp 4 issues the 27 MMAs of each tile as soon as
+// its entries have landed and its accumulator is free, so the MMAs of tile i
+// run while warps 0-3 drain tile i-1 and load tile i+PF.
 template <int CIN, int COUT, int PF>
-__global__ void __launch_bounds__(CONV_THREADS) conv_ring_kernel(ConvArgs a) {
+__global__ void __launch_bounds__(RING_THREADS) conv_ring_kernel(ConvArgs a) {
     static_assert(CIN % 16 == 0 && (COUT == 16 || COUT == 32), "CIN multiple of 16, COUT 16 or 32");
     static_assert(PF >= 1 && PF <= 4, "prefetch depth 1..4");
     using RS = RingShape<CIN, COUT, PF>;
@@ -443,99 +457,106 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_ring_kernel(ConvArgs a) {
     __syncthreads();
     tc::fence_after();
     const uint32_t tmem = tslot;
-    const uint32_t idesc = tc::idesc_bf16(COUT, false, false);
-    constexpr uint32_t lboA = (uint32_t)(R * 3 * PITCH * 16), lboB = 27u * COUT * 16u;
-    const uint64_t descA = tc::sdesc(tc::smem_u32(sR), lboA, 128), descB = tc::sdesc(tc::smem_u32(sB), lboB, 128);
     const uint4* inp = reinterpret_cast<const uint4*>(a.in);
-    int ql = -1;                        // stream index of the last entry loaded
-    auto load_tile = [&](int iu) {
-        const int tau = t0 + iu;
-        const int j = tau % T.ny, col = tau / T.ny;
-        const int k = col / T.tx, x0 = (col - k * T.tx) * TM;
-        const bool fresh = iu == 0 || j == 0;
-        for (int dy = fresh ? -1 : 1; dy <= 1; ++dy) {
-            int jj = j + dy;
-            jj = jj < 0 ? jj + T.ny : (jj >= T.ny ? jj - T.ny : jj);
-            ++ql;
-            ring_load_entry<CIN, COUT, PF>(T, inp, sR, ql % R, k, x0, jj);
-        }
-    };
+
+    if (warp == 4) {
+        // ---- the MMA warp
+        const uint32_t idesc = tc::idesc_bf16(COUT, false, false);
+        constexpr uint32_t lboA = (uint32_t)(R * 3 * PITCH * 16), lboB = 27u * COUT * 16u;
+        const uint64_t descA = tc::sdesc(tc::smem_u32(sR), lboA, 128), descB = tc::sdesc(tc::smem_u32(sB), lboB, 128);
+        int qm = -1;
 #pragma unroll 1
-    for (int iu = 0; iu < PF; ++iu) {
-        if (iu < cnt) load_tile(iu);
-        cp_async_commit();
-    }
-    int qm = -1;                        // stream index of the last entry of the tile in the MMA
-    int issued = 0, drained = 0;
-    bool failed = false;
-#pragma unroll 1
-    for (int i = 0; i < cnt; ++i) {
-        const int tau = t0 + i;
-        qm += (i == 0 || tau % T.ny == 0) ? 3 : 1;
-        cp_async_wait<PF - 1>();        // tile i's entries (the group committed PF groups ago)
-        tc::fence_async_smem();
-        tc::fence_before();
-        __syncthreads();
-        if (threadIdx.x == 0) {
+        for (int i = 0; i < cnt; ++i) {
+            const int tau = t0 + i;
+            qm += (i == 0 || tau % T.ny == 0) ? 3 : 1;
+            nb_sync(1 + (i & 1));                         // tile i's entries landed
+            if (i >= 2) nb_sync(3 + (i & 1));             // tile i-2 drained its accumulator
             tc::fence_after();
-            const uint32_t dacc = tmem + (uint32_t)((i & 1) * COUT);
-            // the descriptors' start-address field (bits 0-13, address >> 4) is
-            // linear in the address, and every operand lies below 256 KB, so a
-            // tap's descriptor is the base one plus its 16-byte offset
-            int srow[3];
+            if (lane == 0) {
+                const uint32_t dacc = tmem + (uint32_t)((i & 1) * COUT);
+                int srow[3];
 #pragma unroll
-            for (int dy = 0; dy < 3; ++dy) srow[dy] = ((qm - 2 + dy) % R) * 3 * PITCH;
+                for (int dy = 0; dy < 3; ++dy) srow[dy] = ((qm - 2 + dy) % R) * 3 * PITCH;
 #pragma unroll
-            for (int t = 0; t < 27; ++t) {
-                const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;      // each 0..2 (offset + 1)
+                for (int t = 0; t < 27; ++t) {
+                    const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
 #pragma unroll
-                for (int ks = 0; ks < CIN / 16; ++ks) {
-                    const uint64_t ad = descA + (uint64_t)(2 * ks * R * 3 * PITCH + srow[dy] + dz * PITCH + dx);
-                    const uint64_t bd = descB + (uint64_t)((2 * ks * 27 + t) * COUT);
-                    tc::mma_bf16(dacc, ad, bd, idesc, (t | ks) ? 1u : 0u);
+                    for (int ks = 0; ks < CIN / 16; ++ks) {
+                        const uint64_t ad = descA + (uint64_t)(2 * ks * R * 3 * PITCH + srow[dy] + dz * PITCH + dx);
+                        const uint64_t bd = descB + (uint64_t)((2 * ks * 27 + t) * COUT);
+                        tc::mma_bf16(dacc, ad, bd, idesc, (t | ks) ? 1u : 0u);
+                    }
+                }
+                tc::commit(&mbar[i & 1]);
+            }
+            __syncwarp();
+        }
+    } else {
+        // ---- warps 0-3: loads and epilogues
+        const int tid = threadIdx.x;                  // 0 .. 127
+        int ql = -1;
+        auto load_tile = [&](int iu) {
+            const int tau = t0 + iu;
+            const int j = tau % T.ny, col = tau / T.ny;
+            const int k = col / T.tx, x0 = (col - k * T.tx) * TM;
+            const bool fresh = iu == 0 || j == 0;
+            for (int dy = fresh ? -1 : 1; dy <= 1; ++dy) {
+                int jj = j + dy;
+                jj = jj < 0 ? jj + T.ny : (jj >= T.ny ? jj - T.ny : jj);
+                ++ql;
+                const int slot = ql % R;
+                constexpr int TOTAL = 3 * NCH * PITCH;
+                for (int idx = tid; idx < TOTAL; idx += 128) {
+                    const int c = idx % NCH, rest = idx / NCH;
+                    const int x = rest % PITCH, d = rest / PITCH;
+                    const int gz = k + d - 1;
+                    const bool zin = gz >= 0 && gz < T.nz;
+                    int gx = x0 - 1 + x;
+                    gx = gx < 0 ? gx + T.nx : (gx >= T.nx ? gx - T.nx : gx);
+                    const uint4* src = inp + ((size_t)((zin ? gz : 0) * T.ny + jj) * T.nx + gx) * NCH + c;
+                    cp_async16(sR + ((size_t)((c * R + slot) * 3 + d)) * PITCH + x, src, zin);
                 }
             }
-            tc::commit(&mbar[i & 1]);
+        };
+#pragma unroll 1
+        for (int iu = 0; iu < PF; ++iu) {
+            if (iu < cnt) load_tile(iu);
+            cp_async_commit();
         }
-        ++issued;
-        if (i > 0) {
-            const int ip = i - 1;
-            const int tp = tau - 1, jp = tp % T.ny, colp = tp / T.ny;
+        bool failed = false;
+        auto drain = [&](int ip) {
+            const int tp = t0 + ip, jp = tp % T.ny, colp = tp / T.ny;
             const int kp = colp / T.tx, x0p = (colp - kp * T.tx) * TM;
             const int cell = (kp * T.ny + jp) * T.nx + x0p + warp * 32 + lane;
             EpiIn<COUT> ein;
             epi_prefetch<COUT>(a, cell, ein);
-            const bool ok = tc::mbar_wait(&mbar[ip & 1], (uint32_t)((ip >> 1) & 1), WAIT_LIMIT);
-            if (__syncthreads_or(!ok)) {
+            const bool ok = !failed && tc::mbar_wait(&mbar[ip & 1], (uint32_t)((ip >> 1) & 1), WAIT_LIMIT);
+            if (!ok) {
                 failed = true;
-                break;
+            } else {
+                tc::fence_after();
+                conv_epilogue_pre<COUT>(a, tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((ip & 1) * COUT), cell,
+                                        ein);
             }
-            ++drained;
-            tc::fence_after();
-            conv_epilogue_pre<COUT>(a, tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((ip & 1) * COUT), cell, ein);
+            tc::fence_before();
+            if (ip + 2 <= cnt - 1) nb_arrive(3 + (ip & 1));   // the MMA warp reuses this accumulator for tile ip+2
+        };
+#pragma unroll 1
+        for (int i = 0; i < cnt; ++i) {
+            cp_async_wait<PF - 1>();                  // tile i's entries (the group committed PF groups ago)
+            tc::fence_async_smem();
+            nb_arrive(1 + (i & 1));
+            if (i > 0) drain(i - 1);                  // its MMAs done: tile i-1's ring slots are free too
+            if (i + PF < cnt && !failed) load_tile(i + PF);
+            cp_async_commit();
         }
-        if (i + PF < cnt) load_tile(i + PF);
-        cp_async_commit();
-    }
-    if (!failed && cnt > 0) {
-        const int ip = cnt - 1;
-        const bool ok = tc::mbar_wait(&mbar[ip & 1], (uint32_t)((ip >> 1) & 1), WAIT_LIMIT);
-        if (__syncthreads_or(!ok)) {
-            failed = true;
-        } else {
-            ++drained;
-            tc::fence_after();
-            const int tp = t0 + ip, jp = tp % T.ny, colp = tp / T.ny;
-            const int kp = colp / T.tx, x0p = (colp - kp * T.tx) * TM;
-            conv_epilogue<COUT>(a, tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((ip & 1) * COUT),
-                                (kp * T.ny + jp) * T.nx + x0p + warp * 32 + lane);
+        if (cnt > 0) drain(cnt - 1);
+        cp_async_wait<0>();
+        if (failed) {
+            if (lane == 0) atomicExch(a.err, 1);
+            // the MMAs still in flight, bounded
+            for (int u = cnt - 2 < 0 ? 0 : cnt - 2; u < cnt; ++u) tc::mbar_wait(&mbar[u & 1], (uint32_t)((u >> 1) & 1), WAIT_LIMIT);
         }
-    }
-    cp_async_wait<0>();
-    if (failed) {
-        if (threadIdx.x == 0) atomicExch(a.err, 1);
-        // the MMAs still in flight (at most two tiles), bounded
-        for (int u = drained; u < issued; ++u) tc::mbar_wait(&mbar[u & 1], (uint32_t)((u >> 1) & 1), WAIT_LIMIT);
     }
     tc::fence_before();
     __syncthreads();
