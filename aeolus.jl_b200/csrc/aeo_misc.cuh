@@ -392,6 +392,13 @@ __device__ __forceinline__ R open_halo_value(const Geo& g, const OpenSet<R>& ob,
             jj = wrapi(j, g.ny);
         }
     }
+    // v's south boundary face (interior j = 0) belongs to the south plane's
+    // slab, which the y fill writes over every x after the x fill: beyond an
+    // open x face it takes the south plane, not the x plane
+    if (ob.oy && plane && pid == 1 && j == 0 && (i < 0 || i >= g.nx)) {
+        v = ob.yp[((((size_t)(1 * 2) * NZ + kk + AEO_H) * ob.L + AEO_H) * NX) + i + AEO_H];
+        return s > 0 ? v : -v;
+    }
     if (i < 0 || i >= g.nx) {
         if (ob.ox) {
             if (plane) {

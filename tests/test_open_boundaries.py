@@ -326,14 +326,15 @@ def test_convective_outflow_options():
 @pytest.mark.gpu
 @pytest.mark.parametrize("y,outflow,c_s", [("open", {"east": "convective", "north": "convective"}, 0.0),
                                            ("periodic", {"east": "convective"}, 0.17),
+                                           ("open", {"east": "convective"}, 0.17),
+                                           ("open", {"east": "convective", "north": "convective"}, 0.17),
                                            ("open", {"east": "orlanski", "north": "convective"}, 0.0),
                                            ("periodic", {"east": "orlanski"}, 0.17)])
 def test_convective_outflow_matches_the_oracle(y, outflow, c_s):
     # radiating outflow over boxes that touch the faces; the imbalance of the
-    # data and the radiated points corrected before every projection.  (A
-    # radiating face that meets another open face at a corner, together with
-    # an SGS closure, drifts from the oracle by ~1e-8 a step in RK3 -- not in
-    # Euler steps, not without the closure: an open item, left out here.)
+    # data and the radiated points corrected before every projection; with a
+    # closure the strain at the corners of two open faces reads v's south
+    # boundary face beyond the x faces, which the south plane sets
     from aeolus_b200.simulation import Simulation
     from oracle.oracle import OracleSimulation
     g, geom, ap = box_case()
