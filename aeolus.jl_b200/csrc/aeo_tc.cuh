@@ -90,6 +90,12 @@ __device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(mbar)), "r"(count) : "memory");
 }
 
+// One arrival of the calling thread (release: its earlier shared-memory
+// writes are visible to a thread that observes the phase complete).
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(mbar)) : "memory");
+}
+
 // Bounded wait for the mbarrier phase `parity`; false when the limit ran out.
 __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint32_t limit) {
     uint32_t done = 0;

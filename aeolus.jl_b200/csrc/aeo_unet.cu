@@ -228,6 +228,10 @@ struct aeo_unet {
                                 (int)un::RingShape<32, 32, 1>::smem));
         CK(cudaFuncSetAttribute(un::conv_ring_kernel<32, 16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)un::RingShape<32, 16, 1>::smem));
+        CK(cudaFuncSetAttribute(un::conv_wgrad_ring_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)un::WgShape<16>::smem));
+        CK(cudaFuncSetAttribute(un::conv_wgrad_ring_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)un::WgShape<32>::smem));
         CK(cudaFuncSetAttribute(un::conv_wgrad_kernel<16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w1616));
         CK(cudaFuncSetAttribute(un::conv_wgrad_kernel<16, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w1632));
         CK(cudaFuncSetAttribute(un::conv_wgrad_kernel<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w3232));
@@ -318,6 +322,13 @@ struct aeo_unet {
         a.dW = dW(l);
         a.db = db(l);
         a.err = derr;
+        if (ci == 16 && Tl.mode == 0 && Tl.ny >= 3) {   // x-segment tiles: the pipelined ring kernel, one CTA an SM
+            const int g1 = Tl.ntiles < sms ? Tl.ntiles : sms;
+            if (co == 16) un::conv_wgrad_ring_kernel<16><<<g1, un::RING_THREADS, un::WgShape<16>::smem, st>>>(a);
+            else un::conv_wgrad_ring_kernel<32><<<g1, un::RING_THREADS, un::WgShape<32>::smem, st>>>(a);
+            CKL();
+            return AEO_OK;
+        }
         const int gsz = conv_grid(Tl);
         if (ci == 16 && co == 16) un::conv_wgrad_kernel<16, 16><<<gsz, un::CONV_THREADS, wg_smem<16, 16>(Tl), st>>>(a);
         else if (ci == 16 && co == 32) un::conv_wgrad_kernel<16, 32><<<gsz, un::CONV_THREADS, wg_smem<16, 32>(Tl), st>>>(a);

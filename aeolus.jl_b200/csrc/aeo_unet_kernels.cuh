@@ -416,13 +416,12 @@ __device__ __forceinline__ void ring_load_entry(const Tiles& T, const uint4* __r
     }
 }
 
-// Named barriers between the loader / epilogue warps (0-3, which arrive) and
-// the MMA warp (4, which waits): ids 1, 2 "tile i's entries landed" (by the
-// parity of i), ids 3, 4 "the accumulator of tile j is drained" (by the
-// parity of j).  An arrival and its wait are issued the same number of times
-// on every id, whatever happens, so no wait can outlast the kernel.
-__device__ __forceinline__ void nb_arrive(int id) { asm volatile("bar.arrive %0, 160;" :: "r"(id) : "memory"); }
-__device__ __forceinline__ void nb_sync(int id) { asm volatile("bar.sync %0, 160;" :: "r"(id) : "memory"); }
+// The loader / epilogue warps (0-3) and the MMA warp (4) meet only through
+// mbarriers, every wait bounded: "tile i's entries landed" (rdy, by the parity
+// of i, 128 arrivals) and "the accumulator of tile j is drained" (drn, by the
+// parity of j, 128 arrivals) for the MMA warp; the MMA commits for warps 0-3.
+// A named barrier joins warps 0-3 among themselves only.
+__device__ __forceinline__ void nb_sync_n(int id, int n) { asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(n) : "memory"); }
 
 constexpr int RING_THREADS = 160;
 
@@ -439,8 +438,9 @@ __global__ void __launch_bounds__(RING_THREADS) conv_ring_kernel(ConvArgs a) {
     constexpr int NCH = RS::NCH, R = RS::R, PITCH = RS::PITCH;
     constexpr int WROWS = NCH * 27 * COUT;
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ uint64_t mbar[2];
+    __shared__ uint64_t mbar[2], rdy[2], drn[2];
     __shared__ uint32_t tslot;
+    __shared__ int mma_failed;
     const Tiles& T = a.T;
     uint4* sB = reinterpret_cast<uint4*>(smem);
     uint4* sR = sB + WROWS;
@@ -451,6 +451,11 @@ __global__ void __launch_bounds__(RING_THREADS) conv_ring_kernel(ConvArgs a) {
     if (threadIdx.x == 0) {
         tc::mbar_init(&mbar[0], 1);
         tc::mbar_init(&mbar[1], 1);
+        tc::mbar_init(&rdy[0], 128);
+        tc::mbar_init(&rdy[1], 128);
+        tc::mbar_init(&drn[0], 128);
+        tc::mbar_init(&drn[1], 128);
+        mma_failed = 0;
     }
     if (warp == 0) tc::tmem_alloc(&tslot, RS::tmem_cols);
     tc::fence_before();
@@ -469,8 +474,13 @@ __global__ void __launch_bounds__(RING_THREADS) conv_ring_kernel(ConvArgs a) {
         for (int i = 0; i < cnt; ++i) {
             const int tau = t0 + i;
             qm += (i == 0 || tau % T.ny == 0) ? 3 : 1;
-            nb_sync(1 + (i & 1));                         // tile i's entries landed
-            if (i >= 2) nb_sync(3 + (i & 1));             // tile i-2 drained its accumulator
+            bool ok = tc::mbar_wait(&rdy[i & 1], (uint32_t)((i >> 1) & 1), WAIT_LIMIT);          // entries landed
+            if (ok && i >= 2) ok = tc::mbar_wait(&drn[i & 1], (uint32_t)(((i - 2) >> 1) & 1), WAIT_LIMIT);  // i-2 drained
+            if (!ok) {          // no MMAs on data that may not be there; warps 0-3 time out on the commit
+                if (lane == 0) mma_failed = 1;
+                __syncwarp();
+                continue;
+            }
             tc::fence_after();
             if (lane == 0) {
                 const uint32_t dacc = tmem + (uint32_t)((i & 1) * COUT);
@@ -539,13 +549,13 @@ __global__ void __launch_bounds__(RING_THREADS) conv_ring_kernel(ConvArgs a) {
                                         ein);
             }
             tc::fence_before();
-            if (ip + 2 <= cnt - 1) nb_arrive(3 + (ip & 1));   // the MMA warp reuses this accumulator for tile ip+2
+            if (ip + 2 <= cnt - 1) tc::mbar_arrive(&drn[ip & 1]);   // the MMA warp reuses this accumulator for tile ip+2
         };
 #pragma unroll 1
         for (int i = 0; i < cnt; ++i) {
             cp_async_wait<PF - 1>();                  // tile i's entries (the group committed PF groups ago)
             tc::fence_async_smem();
-            nb_arrive(1 + (i & 1));
+            tc::mbar_arrive(&rdy[i & 1]);
             if (i > 0) drain(i - 1);                  // its MMAs done: tile i-1's ring slots are free too
             if (i + PF < cnt && !failed) load_tile(i + PF);
             cp_async_commit();
@@ -560,6 +570,7 @@ __global__ void __launch_bounds__(RING_THREADS) conv_ring_kernel(ConvArgs a) {
     }
     tc::fence_before();
     __syncthreads();
+    if (threadIdx.x == 0 && mma_failed) atomicExch(a.err, 1);
     if (warp == 0) tc::tmem_dealloc(tmem, RS::tmem_cols);
 }
 
@@ -686,6 +697,202 @@ __global__ void __launch_bounds__(CONV_THREADS) conv_wgrad_kernel(WgradArgs a) {
     tc::fence_before();
     __syncthreads();
     if (warp == 0) tc::tmem_dealloc(tmem, NCOL);
+}
+
+// The weight gradient on x-segment tiles as a pipeline (CIN = 16): the input
+// rows in the forward kernel's ring (PF = 1, R = 6 entries), the tile's
+// output-gradient rows beside it (two buffers), and the (tap, channel) rows of
+// each M-tile materialised into one of two shared buffers by warps 0-3 while
+// warp 4 multiplies the other: the 8 MMAs (K = 128 cells) of M-tile q run
+// while the rows of M-tile q+1 are gathered.  Named barriers 1, 2 "M buffer
+// ready" (arrived at by warps 0-3, waited on by warp 4, by the parity of q),
+// 5 the loader warps among themselves; the M buffers come back through the
+// MMA commits (mbarriers).  Accumulated in TMEM over the CTA's tiles, added
+// to dW at the end.
+template <int COUT>
+struct WgShape {
+    static constexpr int CIN = 16, NCH = 2, NCO = COUT / 8, PF = 1;
+    static constexpr int NMT = wg_mtiles<16>();
+    static constexpr size_t ring_rows = (size_t)RingShape<16, COUT, 1>::R * RingShape<16, COUT, 1>::slot_rows;
+    static constexpr size_t g_rows = (size_t)NCO * TM;           // one tile's gradient rows
+    static constexpr size_t m_rows = (size_t)16 * TM;            // one M buffer
+    static constexpr size_t smem = (ring_rows + 2 * g_rows + 2 * m_rows) * 16;
+    static constexpr uint32_t tmem_cols = wg_tmem_cols<16, COUT>();
+};
+
+template <int COUT>
+__global__ void __launch_bounds__(RING_THREADS) conv_wgrad_ring_kernel(WgradArgs a) {
+    using W = WgShape<COUT>;
+    using RS = RingShape<16, COUT, 1>;
+    constexpr int NCH = W::NCH, NCO = W::NCO, NMT = W::NMT, R = RS::R, PITCH = RS::PITCH;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t mbM[2], rdy[2];
+    __shared__ uint32_t tslot;
+    __shared__ int mma_failed;
+    const Tiles& T = a.T;
+    uint4* sR = reinterpret_cast<uint4*>(smem);
+    uint4* sG = sR + W::ring_rows;                 // 2 x NCO planes x 128 rows
+    uint4* sM = sG + 2 * W::g_rows;                // 2 x 16 planes x 128 rows
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t0 = (int)((long long)T.ntiles * blockIdx.x / gridDim.x);
+    const int cnt = (int)((long long)T.ntiles * (blockIdx.x + 1) / gridDim.x) - t0;
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&mbM[0], 1);
+        tc::mbar_init(&mbM[1], 1);
+        tc::mbar_init(&rdy[0], 128);
+        tc::mbar_init(&rdy[1], 128);
+        mma_failed = 0;
+    }
+    if (warp == 0) tc::tmem_alloc(&tslot, W::tmem_cols);
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = tslot;
+    const int nq = cnt * NMT;
+    bool failed = false;
+
+    if (warp == 4) {
+        // ---- the MMA warp: M-tile q of tile i = q / NMT into TMEM columns (q % NMT) * COUT
+        const uint32_t idesc = tc::idesc_bf16(COUT, true, true);
+#pragma unroll 1
+        for (int q = 0; q < nq; ++q) {
+            const int i = q / NMT, mt = q - i * NMT;
+            if (!tc::mbar_wait(&rdy[q & 1], (uint32_t)((q >> 1) & 1), WAIT_LIMIT)) {
+                if (lane == 0) mma_failed = 1;
+                __syncwarp();
+                continue;
+            }
+            tc::fence_after();
+            if (lane == 0) {
+                const uint32_t mBase = tc::smem_u32(sM + (size_t)(q & 1) * W::m_rows);
+                const uint32_t gBase = tc::smem_u32(sG + (size_t)(i & 1) * W::g_rows);
+#pragma unroll
+                for (int kk = 0; kk < TM / 16; ++kk) {
+                    const uint64_t ad = tc::sdesc(mBase + kk * 256u, 128u, (uint32_t)TM * 16u);
+                    const uint64_t bd = tc::sdesc(gBase + kk * 256u, 128u, (uint32_t)TM * 16u);
+                    tc::mma_bf16(tmem + (uint32_t)(mt * COUT), ad, bd, idesc, (i > 0 || kk > 0) ? 1u : 0u);
+                }
+                tc::commit(&mbM[q & 1]);
+            }
+            __syncwarp();
+        }
+    } else {
+        // ---- warps 0-3: loads, gradient sums, the M rows
+        const int tid = threadIdx.x;
+        const uint4* inp = reinterpret_cast<const uint4*>(a.x);
+        const uint4* gp = reinterpret_cast<const uint4*>(a.g);
+        int ql = -1;
+        auto load_tile = [&](int iu) {
+            const int tau = t0 + iu;
+            const int j = tau % T.ny, col = tau / T.ny;
+            const int k = col / T.tx, x0 = (col - k * T.tx) * TM;
+            const bool fresh = iu == 0 || j == 0;
+            for (int dy = fresh ? -1 : 1; dy <= 1; ++dy) {
+                int jj = j + dy;
+                jj = jj < 0 ? jj + T.ny : (jj >= T.ny ? jj - T.ny : jj);
+                ++ql;
+                const int slot = ql % R;
+                constexpr int TOTAL = 3 * NCH * PITCH;
+                for (int idx = tid; idx < TOTAL; idx += 128) {
+                    const int c = idx % NCH, rest = idx / NCH;
+                    const int x = rest % PITCH, d = rest / PITCH;
+                    const int gz = k + d - 1;
+                    const bool zin = gz >= 0 && gz < T.nz;
+                    int gx = x0 - 1 + x;
+                    gx = gx < 0 ? gx + T.nx : (gx >= T.nx ? gx - T.nx : gx);
+                    const uint4* src = inp + ((size_t)((zin ? gz : 0) * T.ny + jj) * T.nx + gx) * NCH + c;
+                    cp_async16(sR + ((size_t)((c * R + slot) * 3 + d)) * PITCH + x, src, zin);
+                }
+            }
+            // the tile's gradient rows, N chunk c of cell m at sG[c * 128 + m]
+            uint4* dstG = sG + (size_t)(iu & 1) * W::g_rows;
+            const size_t cell0 = ((size_t)k * T.ny + j) * T.nx + x0;
+            for (int idx = tid; idx < NCO * TM; idx += 128) {
+                const int c = idx % NCO, m = idx / NCO;
+                cp_async16(dstG + (size_t)c * TM + m, gp + (cell0 + m) * NCO + c, true);
+            }
+        };
+        if (cnt > 0) load_tile(0);
+        cp_async_commit();
+        float dbacc = 0.0f;
+        int qm = -1;
+#pragma unroll 1
+        for (int i = 0; i < cnt; ++i) {
+            const int tau = t0 + i;
+            qm += (i == 0 || tau % T.ny == 0) ? 3 : 1;
+            cp_async_wait<0>();                        // tile i's rows and gradient landed
+            nb_sync_n(5, 128);                         // every loader's copies, before anyone reads them
+            if (tid < COUT) {
+                const int c = tid / 8, e = tid % 8;
+                const bf16* g8 = reinterpret_cast<const bf16*>(sG + (size_t)(i & 1) * W::g_rows + (size_t)c * TM);
+                for (int m = 0; m < TM; ++m) dbacc += __bfloat162float(g8[m * 8 + e]);
+            }
+#pragma unroll 1
+            for (int mt = 0; mt < NMT; ++mt) {
+                const int q = i * NMT + mt, b = q & 1;
+                if (q >= 2)                            // the MMAs of M-tile q-2 read this buffer
+                    if (!tc::mbar_wait(&mbM[b], (uint32_t)(((q - 2) >> 1) & 1), WAIT_LIMIT)) failed = true;
+                // warp w gathers M chunks 4w .. 4w+3 (one (tap, channel-chunk) row each),
+                // its lanes along the cells
+                uint4* dM = sM + (size_t)b * W::m_rows;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int gl = warp * 4 + u, G = mt * 16 + gl;
+                    uint4* dst = dM + (size_t)gl * TM;
+                    if (G < 27 * NCH) {
+                        const int t = G / NCH, c = G - t * NCH;
+                        const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+                        const uint4* src = sR + ((size_t)((c * R + (qm - 2 + dy) % R) * 3 + dz)) * PITCH + dx;
+#pragma unroll
+                        for (int m = lane; m < TM; m += 32) dst[m] = src[m];
+                    } else {
+#pragma unroll
+                        for (int m = lane; m < TM; m += 32) dst[m] = make_uint4(0u, 0u, 0u, 0u);
+                    }
+                }
+                tc::fence_async_smem();
+                tc::mbar_arrive(&rdy[b]);              // M-tile q ready
+            }
+            // every loader is done with tile i-1's ring slots and (its MMAs having
+            // completed, M-tile i*NMT-1 was waited for above) its gradient rows
+            nb_sync_n(5, 128);
+            if (i + 1 < cnt) load_tile(i + 1);
+            cp_async_commit();
+        }
+        cp_async_wait<0>();
+        // the last two M-tiles' MMAs (the accumulators complete), bounded
+        for (int q = nq - 2 < 0 ? 0 : nq - 2; q < nq; ++q)
+            if (!tc::mbar_wait(&mbM[q & 1], (uint32_t)((q >> 1) & 1), WAIT_LIMIT)) failed = true;
+        if (tid < COUT && cnt > 0) atomicAdd(&a.db[tid], dbacc);
+        if (failed) {
+            if (tid == 0) atomicExch(a.err, 1);
+        } else if (cnt > 0) {
+            tc::fence_after();
+            const int m = warp * 32 + lane;
+            for (int mt = 0; mt < NMT; ++mt) {
+                float v[COUT];
+                float h[16];
+                tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(mt * COUT), h);
+#pragma unroll
+                for (int r = 0; r < 16; ++r) v[r] = h[r];
+                if constexpr (COUT == 32) {
+                    tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(mt * COUT + 16), h);
+#pragma unroll
+                    for (int r = 0; r < 16; ++r) v[16 + r] = h[r];
+                }
+                const int G = mt * 16 + m / 8;
+                if (G < 27 * NCH) {
+                    const int t = G / NCH, ci = (G % NCH) * 8 + m % 8;
+#pragma unroll
+                    for (int co = 0; co < COUT; ++co) atomicAdd(&a.dW[((size_t)t * COUT + co) * 16 + ci], v[co]);
+                }
+            }
+        }
+    }
+    tc::fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0 && mma_failed) atomicExch(a.err, 1);
+    if (warp == 0) tc::tmem_dealloc(tmem, W::tmem_cols);
 }
 
 // ---------------------------------------------------------------- helpers
