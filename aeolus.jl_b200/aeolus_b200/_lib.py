@@ -18,7 +18,7 @@ SYMBOLS = (
     "aeo_pressure_solve", "aeo_project", "aeo_kinetic_energy", "aeo_max_divergence", "aeo_step_rk3_async",
     "aeo_synchronize", "aeo_profile_step", "aeo_launches_per_step", "aeo_stream", "aeo_fill_uniform",
     "aeo_pressure_solve_column_noalloc", "aeo_step_adaptive", "aeo_cfl_diagnostics", "aeo_init_isotropic", "aeo_last_error",
-    "aeo_set_pcg", "aeo_pcg_stats", "aeo_pcg_set_learned", "aeo_pcg_harvest", "aeo_set_open", "aeo_set_open_outflow", "aeo_open_ledger", "aeo_get_open_planes", "aeo_advect_positive", "aeo_advect_positive_device", "aeo_set_ibm", "aeo_set_sgs_buoyancy", "aeo_set_lagrangian", "aeo_set_tke", "aeo_get_sgs_state", "aeo_set_sgs_state", "aeo_set_field_f32", "aeo_get_field_f32",
+    "aeo_set_pcg", "aeo_pcg_stats", "aeo_pcg_set_learned", "aeo_pcg_harvest", "aeo_set_open", "aeo_set_open_outflow", "aeo_open_ledger", "aeo_get_open_planes", "aeo_set_open_planes", "aeo_get_open_history", "aeo_set_open_history", "aeo_advect_positive", "aeo_advect_positive_device", "aeo_set_ibm", "aeo_set_sgs_buoyancy", "aeo_set_lagrangian", "aeo_set_tke", "aeo_get_sgs_state", "aeo_set_sgs_state", "aeo_set_field_f32", "aeo_get_field_f32",
     "aeo_version",
     "aeo_mg_create", "aeo_mg_destroy", "aeo_mg_levels", "aeo_mg_solve", "aeo_mg_solve_device",
     "aeo_mg_vcycle_solve", "aeo_mg_apply", "aeo_mg_precondition", "aeo_mg_profile",
@@ -144,6 +144,9 @@ def load():
     lib.aeo_set_open_outflow.argtypes = [P, I32, C.c_int32, D, D, D, D]
     lib.aeo_open_ledger.argtypes = [P, D]
     lib.aeo_get_open_planes.argtypes = [P, D, D]
+    lib.aeo_set_open_planes.argtypes = [P, D, D]
+    lib.aeo_get_open_history.argtypes = [P, D, D, D]
+    lib.aeo_set_open_history.argtypes = [P, D, D, D]
     lib.aeo_profile_step.argtypes = [P, C.c_double, D, C.c_int32]
     lib.aeo_launches_per_step.argtypes = [P, C.POINTER(C.c_int32)]
     lib.aeo_stream.argtypes = [P]

@@ -6,8 +6,10 @@ record, the simulation time, copies of the prognostic storage fields (u, v,
 w, theta and the pressure, halos included), the scalar parameters of the
 CoreSpec, the closure name and its state (the Lagrangian closure's
 memories, sgs_state / restore_sgs_state!), the stepper state (the last
-accepted dt of an adaptive run) and free-form extras. `buffers` (the fields of an earlier
-payload of the same domain) are refilled in place, so a run that keeps its
+accepted dt of an adaptive run), the state of open lateral faces
+(open_boundary_checkpoint: the plane buffers and the Orlanski history, as
+`Simulation.open_checkpoint` reads them) and free-form extras. `buffers` (the
+fields of an earlier payload of the same domain) are refilled in place, so a run that keeps its
 last good state (a rollback snapshot) allocates once.
 
 On disk a payload is one .npz file: the arrays plus the rest as a JSON
@@ -94,6 +96,7 @@ def checkpoint_payload(sim, t: float = 0.0, stepper: Optional[Dict[str, Any]] = 
         "closure_type": spec.sgs if spec.c_s != 0 else "",
         "closure": closure_state(sim),
         "stepper": None if stepper is None else dict(stepper),
+        "open": open_state(sim),
         "extra": {} if extra is None else dict(extra),
     }
 
@@ -116,7 +119,7 @@ def write_checkpoint(path: str, payload: Dict[str, Any]) -> str:
     (write_checkpoint, src/io/checkpoint.jl:400-417)."""
     d = os.path.dirname(os.path.abspath(path))
     os.makedirs(d, exist_ok=True)
-    head = {k: v for k, v in payload.items() if k not in ("fields", "closure")}
+    head = {k: v for k, v in payload.items() if k not in ("fields", "closure", "open")}
     head["field_names"] = sorted(payload["fields"])
     arrays = {"field_" + k: v for k, v in payload["fields"].items()}
     cl = payload.get("closure")
@@ -124,6 +127,11 @@ def write_checkpoint(path: str, payload: Dict[str, Any]) -> str:
     if cl is not None:
         head["closure"]["arrays"] = sorted(k for k, v in cl.items() if isinstance(v, np.ndarray))
         arrays.update({"closure_" + k: v for k, v in cl.items() if isinstance(v, np.ndarray)})
+    ob = payload.get("open")
+    head["open"] = None if ob is None else {k: v for k, v in ob.items() if not isinstance(v, np.ndarray)}
+    if ob is not None:
+        head["open"]["arrays"] = sorted(k for k, v in ob.items() if isinstance(v, np.ndarray))
+        arrays.update({"open_" + k: v for k, v in ob.items() if isinstance(v, np.ndarray)})
     tmp = path + ".tmp"
     with open(tmp, "wb") as f:
         np.savez(f, header=np.frombuffer(json.dumps(head).encode(), dtype=np.uint8), **arrays)
@@ -140,6 +148,8 @@ def read_checkpoint(path: str) -> Dict[str, Any]:
         fields = {k: np.array(z["field_" + k]) for k in head.pop("field_names")}
         if head.get("closure") is not None:
             head["closure"].update({k: np.array(z["closure_" + k]) for k in head["closure"].pop("arrays")})
+        if head.get("open") is not None:
+            head["open"].update({k: np.array(z["open_" + k]) for k in head["open"].pop("arrays")})
     head["fields"] = fields
     return head
 
@@ -176,14 +186,26 @@ def restore(sim, payload, check_parameters: bool = True):
     cl = payload.get("closure")
     if (cl is None) != (closure_state_kind(sim) is None):
         raise ValueError("the checkpoint's closure state does not fit the domain's closure")
+    ob = payload.get("open")
+    if (ob is None) != (getattr(sim, "_open", None) is None):
+        raise ValueError("the checkpoint's open faces do not fit the domain's")
     for name in FIELDS:
         sim.set_field(name, np.ascontiguousarray(payload["fields"][name], dtype=np.float64))
+    if ob is not None:
+        sim.restore_open_checkpoint(ob)
     if cl is not None:
         if closure_state_kind(sim) == "tke":
             sim.set_sgs_state(cl["e"])
         else:
             sim.set_sgs_state(tuple(cl[k] for k in CLOSURE_ARRAYS) + (bool(cl["initialised"]),))
     return payload["t"], payload["stepper"]
+
+
+def open_state(sim) -> Optional[Dict[str, Any]]:
+    """The open faces' restart state of `sim` (None: no open face, or a
+    domain without them)."""
+    f = getattr(sim, "open_checkpoint", None)
+    return None if f is None else f()
 
 
 def closure_state_kind(sim) -> Optional[str]:

@@ -350,6 +350,42 @@ class Simulation:
         _lib.check(self._lib.aeo_get_open_planes(self._h, _ptr(xp), _ptr(yp)), self._h)
         return xp, yp
 
+    def open_checkpoint(self):
+        """The state of the open faces a restart needs (open_boundary_checkpoint,
+        src/boundary_conditions/open_boundary.jl:1282-1305): the plane buffers
+        and, on a radiating set, the Orlanski history; None without open faces."""
+        if getattr(self, "_open", None) is None:
+            return None
+        xp, yp = self.open_planes()
+        out = {"planes_x": xp, "planes_y": yp}
+        if self._open.radiating.any():
+            g = self.grid
+            NZ, NY, NX = g.storage_shape
+            hx, hy, sc = np.zeros((4, 2, NZ, NY)), np.zeros((4, 2, NZ, NX)), np.zeros(2)
+            _lib.check(self._lib.aeo_get_open_history(self._h, _ptr(hx), _ptr(hy), _ptr(sc)), self._h)
+            out.update({"hist_x": hx, "hist_y": hy, "hist_set": float(sc[0]), "last_dt": float(sc[1])})
+        return out
+
+    def restore_open_checkpoint(self, state):
+        """Copy an open_checkpoint back (restore_open_boundary_checkpoint!,
+        :1307-1350): the faces must be built as the checkpointed ones."""
+        if state is None:
+            return
+        if getattr(self, "_open", None) is None:
+            raise ValueError("restore: the checkpoint has open faces, the domain none")
+        xp, yp, _ = self._open.packed()
+        if state["planes_x"].shape != xp.shape or state["planes_y"].shape != yp.shape:
+            raise ValueError("restore: the open faces are built differently from the checkpoint's")
+        if ("hist_x" in state) != bool(self._open.radiating.any()):
+            raise ValueError("restore: the radiating faces differ from the checkpoint's")
+        _lib.check(self._lib.aeo_set_open_planes(self._h, _ptr(np.ascontiguousarray(state["planes_x"])),
+                                                 _ptr(np.ascontiguousarray(state["planes_y"]))), self._h)
+        if "hist_x" in state:
+            sc = np.array([state["hist_set"], state["last_dt"]])
+            _lib.check(self._lib.aeo_set_open_history(self._h, _ptr(np.ascontiguousarray(state["hist_x"])),
+                                                      _ptr(np.ascontiguousarray(state["hist_y"])), _ptr(sc)),
+                       self._h)
+
     def open_ledger(self) -> dict:
         """Q, residual and delta of the last mass-flux correction on the device
         (a radiating open set)."""

@@ -124,6 +124,8 @@ struct CoreBase {
                                         const double* yw) = 0;
     virtual aeo_status open_ledger(double* out) = 0;
     virtual aeo_status get_open_planes(double* xp, double* yp) = 0;
+    virtual aeo_status open_state(double* hx, double* hy, double* sc, bool set) = 0;
+    virtual aeo_status set_open_planes(const double* xp, const double* yp) = 0;
     virtual aeo_status set_ibm(const uint8_t* mask, double tau) = 0;
     virtual aeo_status set_sgs_buoyancy(const double* bg) = 0;
     virtual aeo_status set_lagrangian(double c0, double theta, double memory_time) = 0;
@@ -1111,6 +1113,75 @@ struct Core : CoreBase {
         CK(cudaMemcpy(hy.data(), ob.yp, nyp * sizeof(R), cudaMemcpyDeviceToHost));
         if (xo) for (size_t q = 0; q < nxp; ++q) xo[q] = (double)hx[q] + (q / (nxp / 4) == 3 ? th_off : 0.0);
         if (yo) for (size_t q = 0; q < nyp; ++q) yo[q] = (double)hy[q] + (q / (nyp / 4) == 3 ? th_off : 0.0);
+        return AEO_OK;
+    }
+
+    // The planes back from a checkpoint (the buffers only: the data, weights
+    // and modes are the set's own), the projection's boundary faces from them,
+    // the state's halos refilled
+    aeo_status set_open_planes(const double* xi, const double* yi) override {
+        if (!(open_x || open_y)) { fail("set_open_planes: no open face"); return AEO_ERR_STATE; }
+        if (!xi || !yi) { fail("set_open_planes: NULL plane array"); return AEO_ERR_ARGUMENT; }
+        CK(cudaStreamSynchronize(st));
+        const int H = AEO_H, NX = g.nx + 2 * H, NY = g.ny + 2 * H, NZ = g.nz + 2 * H, L = H + 1;
+        const size_t nxp = ob_nxp(), nyp = ob_nyp();
+        std::vector<R> hx(nxp), hy(nyp);
+        for (size_t q = 0; q < nxp; ++q) hx[q] = R(xi[q] - (q / (nxp / 4) == 3 ? th_off : 0.0));
+        for (size_t q = 0; q < nyp; ++q) hy[q] = R(yi[q] - (q / (nyp / 4) == 3 ? th_off : 0.0));
+        std::vector<R> bw((size_t)g.ny * g.nz), be(bw.size()), bs((size_t)g.nx * g.nz), bn(bs.size());
+        for (int k = 0; k < g.nz; ++k) {
+            for (int j = 0; j < g.ny; ++j) {
+                bw[(size_t)k * g.ny + j] = hx[(((size_t)0 * NZ + k + H) * NY + j + H) * L + H];
+                be[(size_t)k * g.ny + j] = hx[(((size_t)1 * NZ + k + H) * NY + j + H) * L + 0];
+            }
+            for (int i = 0; i < g.nx; ++i) {
+                bs[(size_t)k * g.nx + i] = hy[(((size_t)2 * NZ + k + H) * L + H) * NX + i + H];
+                bn[(size_t)k * g.nx + i] = hy[(((size_t)3 * NZ + k + H) * L + 0) * NX + i + H];
+            }
+        }
+        CK(cudaMemcpy((void*)ob.xp, hx.data(), nxp * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy((void*)ob.yp, hy.data(), nyp * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy((void*)ob.bw, bw.data(), bw.size() * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy((void*)ob.be, be.data(), be.size() * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy((void*)ob.bs, bs.data(), bs.size() * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy((void*)ob.bn, bn.data(), bn.size() * sizeof(R), cudaMemcpyHostToDevice));
+        R* f[4] = {P[cur][0], P[cur][1], P[cur][2], P[cur][3]};
+        int l[4] = {LOC_FX, LOC_FY, LOC_FZ, LOC_C};
+        if (aeo_status e = halo(f, l, 4)) return e;
+        CK(cudaStreamSynchronize(st));
+        return AEO_OK;
+    }
+
+    // The Orlanski history of a radiating set (hx [f][side][NZ][NY], hy
+    // [f][side][NZ][NX], the interior layer at the last step start) and sc =
+    // (history set, the last step's length): read (set = false) or written
+    aeo_status open_state(double* hx, double* hy, double* sc, bool set) override {
+        if (!ob_rad) { fail("open_state: no radiating open face"); return AEO_ERR_STATE; }
+        if (!hx || !hy || !sc) { fail("open_state: NULL array"); return AEO_ERR_ARGUMENT; }
+        CK(cudaStreamSynchronize(st));
+        const size_t ntx = (size_t)8 * (g.nz + 2 * AEO_H) * (g.ny + 2 * AEO_H), nty = (size_t)8 * (g.nz + 2 * AEO_H) * (g.nx + 2 * AEO_H);
+        std::vector<R> bx(ntx), by(nty);
+        int ok = 0;
+        double ldt = 0.0;
+        if (set) {
+            for (size_t q = 0; q < ntx; ++q) bx[q] = R(hx[q] - ((q / (ntx / 4)) == 3 ? th_off : 0.0));
+            for (size_t q = 0; q < nty; ++q) by[q] = R(hy[q] - ((q / (nty / 4)) == 3 ? th_off : 0.0));
+            ok = sc[0] != 0.0;
+            ldt = sc[1];
+            CK(cudaMemcpy(ob.xh, bx.data(), ntx * sizeof(R), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(ob.yh, by.data(), nty * sizeof(R), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(ob.hist_ok, &ok, sizeof(int), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(ob.last_dt, &ldt, sizeof(double), cudaMemcpyHostToDevice));
+        } else {
+            CK(cudaMemcpy(bx.data(), ob.xh, ntx * sizeof(R), cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(by.data(), ob.yh, nty * sizeof(R), cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(&ok, ob.hist_ok, sizeof(int), cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(&ldt, ob.last_dt, sizeof(double), cudaMemcpyDeviceToHost));
+            for (size_t q = 0; q < ntx; ++q) hx[q] = (double)bx[q] + ((q / (ntx / 4)) == 3 ? th_off : 0.0);
+            for (size_t q = 0; q < nty; ++q) hy[q] = (double)by[q] + ((q / (nty / 4)) == 3 ? th_off : 0.0);
+            sc[0] = ok;
+            sc[1] = ldt;
+        }
         return AEO_OK;
     }
 
@@ -2425,6 +2496,22 @@ aeo_status aeo_set_open_outflow(aeo_sim* h, const int32_t* radiate, int32_t corr
 aeo_status aeo_get_open_planes(aeo_sim* h, double* x_planes, double* y_planes) {
     ENTER(h);
     return h->core->get_open_planes(x_planes, y_planes);
+}
+
+aeo_status aeo_set_open_planes(aeo_sim* h, const double* x_planes, const double* y_planes) {
+    ENTER(h);
+    return h->core->set_open_planes(x_planes, y_planes);
+}
+
+aeo_status aeo_get_open_history(aeo_sim* h, double* x_hist, double* y_hist, double* scalars) {
+    ENTER(h);
+    return h->core->open_state(x_hist, y_hist, scalars, false);
+}
+
+aeo_status aeo_set_open_history(aeo_sim* h, const double* x_hist, const double* y_hist, const double* scalars) {
+    ENTER(h);
+    return h->core->open_state(const_cast<double*>(x_hist), const_cast<double*>(y_hist), const_cast<double*>(scalars),
+                               true);
 }
 
 aeo_status aeo_open_ledger(aeo_sim* h, double* out) {

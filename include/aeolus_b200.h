@@ -435,6 +435,15 @@ aeo_status aeo_open_ledger(aeo_sim* h, double* out);
  * (open_boundary_checkpoint, src/boundary_conditions/open_boundary.jl:1282-1305);
  * synchronises */
 aeo_status aeo_get_open_planes(aeo_sim* h, double* x_planes, double* y_planes);
+/* A checkpoint's planes back into the buffers (restore_open_boundary_checkpoint!,
+ * open_boundary.jl:1307-1350; the open set itself as built by aeo_set_open /
+ * aeo_set_open_outflow); the state's halos refilled */
+aeo_status aeo_set_open_planes(aeo_sim* h, const double* x_planes, const double* y_planes);
+/* The Orlanski history of a radiating set (hist, t_hist, has_hist of the
+ * checkpoint): x_hist [field][side][NZ][NY], y_hist [field][side][NZ][NX],
+ * scalars = (history set, the last step's length) */
+aeo_status aeo_get_open_history(aeo_sim* h, double* x_hist, double* y_hist, double* scalars);
+aeo_status aeo_set_open_history(aeo_sim* h, const double* x_hist, const double* y_hist, const double* scalars);
 /* Residual -> error pairs from the run's own snapshots (no reference
  * counterpart; it feeds the learned preconditioner): b receives the
  * right-hand side of the last projection's solve (the predictor's cut-cell

@@ -2746,6 +2746,36 @@ void oc_get_open_planes(const oc_sim* s, double* xp, double* yp) {
     if (yp && s->oyp) memcpy(yp, s->oyp, sizeof(double) * nyp);
 }
 
+/* A checkpoint's planes back into the buffers (restore_open_boundary_checkpoint!,
+ * open_boundary.jl:1307-1350), the state's halos refilled from them */
+int oc_set_open_planes(oc_sim* s, const double* xp, const double* yp) {
+    if (!(s->open_x || s->open_y) || !xp || !yp) return -1;
+    int64_t nxp = (int64_t)8 * s->NZ * s->NY * s->oL, nyp = (int64_t)8 * s->NZ * s->oL * s->NX;
+    memcpy(s->oxp, xp, sizeof(double) * nxp);
+    memcpy(s->oyp, yp, sizeof(double) * nyp);
+    oc_fill_state_halos(s);
+    return 0;
+}
+
+/* The :orlanski history of a radiating set ([f][side][NZ][NY or NX]) and
+ * sc = (history set, the last step's length): read (set 0) or written */
+int oc_open_history(oc_sim* s, double* xh, double* yh, double* sc, int set) {
+    if (!ob_radiates(s) || !xh || !yh || !sc) return -1;
+    int64_t ntx = (int64_t)8 * s->NZ * s->NY, nty = (int64_t)8 * s->NZ * s->NX;
+    if (set) {
+        memcpy(s->oxh, xh, sizeof(double) * ntx);
+        memcpy(s->oyh, yh, sizeof(double) * nty);
+        s->ohist = sc[0] != 0.0;
+        s->olast_dt = sc[1];
+    } else {
+        memcpy(xh, s->oxh, sizeof(double) * ntx);
+        memcpy(yh, s->oyh, sizeof(double) * nty);
+        sc[0] = s->ohist;
+        sc[1] = s->olast_dt;
+    }
+    return 0;
+}
+
 void oc_open_ledger(const oc_sim* s, double* out) { out[0] = s->oQ; out[1] = s->oresid; out[2] = s->odelta; }
 
 int oc_set_open_outflow(oc_sim* s, const int* rad, int corr, const double* xd, const double* yd,

@@ -115,6 +115,10 @@ int oc_set_open_outflow(oc_sim* s, const int* rad, int corr, const double* xd, c
 void oc_open_ledger(const oc_sim* s, double* out);
 /* the current plane buffers (layout of oc_set_open) */
 void oc_get_open_planes(const oc_sim* s, double* xp, double* yp);
+/* a checkpoint's planes back (the halos refilled) */
+int oc_set_open_planes(oc_sim* s, const double* xp, const double* yp);
+/* the :orlanski history and (history set, last dt): read (set 0) or written */
+int oc_open_history(oc_sim* s, double* xh, double* yh, double* sc, int set);
 void oc_set_threads(int n);
 /* advect_positive! (src/AdvectionSchemes.jl:1100-1160): add (accumulate) or
  * write -div(u phi) with the positivity limiter; storage arrays of the

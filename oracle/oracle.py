@@ -91,6 +91,10 @@ def load():
     lib.oc_open_ledger.restype = None
     lib.oc_get_open_planes.argtypes = [P, _D, _D]
     lib.oc_get_open_planes.restype = None
+    lib.oc_set_open_planes.argtypes = [P, _D, _D]
+    lib.oc_set_open_planes.restype = C.c_int
+    lib.oc_open_history.argtypes = [P, _D, _D, _D, C.c_int]
+    lib.oc_open_history.restype = C.c_int
     lib.oc_set_sgs_buoyancy.argtypes = [P, _D]
     lib.oc_set_lagrangian.argtypes = [P, C.c_double, C.c_double, C.c_double]
     lib.oc_set_tke.argtypes = [P, C.c_double, C.c_double, C.c_double, C.c_int]
@@ -305,6 +309,7 @@ class OracleSimulation:
         if obc is None:
             if self._lib.oc_set_open(self._h, 0, 0, None, None, None) != 0:
                 raise ValueError("oracle: set_open rejected")
+            self._open = None
             return
         xp, yp, modes = obc.packed()
         m = np.ascontiguousarray(modes, dtype=np.int32)
@@ -325,6 +330,39 @@ class OracleSimulation:
         xp, yp = (np.zeros_like(a) for a in self._open_raw[1:3])
         self._lib.oc_get_open_planes(self._h, _p(xp), _p(yp))
         return xp, yp
+
+    def open_checkpoint(self):
+        """The planes and, on a radiating set, the :orlanski history
+        (open_boundary_checkpoint, open_boundary.jl:1282-1305); None without
+        open faces."""
+        if getattr(self, "_open", None) is None:
+            return None
+        xp, yp = self.open_planes()
+        out = {"planes_x": xp, "planes_y": yp}
+        if self._open_raw[0].any():
+            NZ, NY, NX = self.grid.storage_shape
+            hx, hy, sc = np.zeros((4, 2, NZ, NY)), np.zeros((4, 2, NZ, NX)), np.zeros(2)
+            assert self._lib.oc_open_history(self._h, _p(hx), _p(hy), _p(sc), 0) == 0
+            out.update({"hist_x": hx, "hist_y": hy, "hist_set": float(sc[0]), "last_dt": float(sc[1])})
+        return out
+
+    def restore_open_checkpoint(self, state):
+        """Copy an open_checkpoint back (restore_open_boundary_checkpoint!,
+        open_boundary.jl:1307-1350) into faces built as the checkpointed ones."""
+        if state is None:
+            return
+        if getattr(self, "_open", None) is None:
+            raise ValueError("restore: the checkpoint has open faces, the domain none")
+        if state["planes_x"].shape != self._open[0].shape or state["planes_y"].shape != self._open[1].shape:
+            raise ValueError("restore: the open faces are built differently from the checkpoint's")
+        if ("hist_x" in state) != bool(self._open_raw[0].any()):
+            raise ValueError("restore: the radiating faces differ from the checkpoint's")
+        xp, yp = (np.ascontiguousarray(state[k], dtype=np.float64) for k in ("planes_x", "planes_y"))
+        assert self._lib.oc_set_open_planes(self._h, _p(xp), _p(yp)) == 0
+        if "hist_x" in state:
+            hx, hy = (np.ascontiguousarray(state[k], dtype=np.float64) for k in ("hist_x", "hist_y"))
+            sc = np.array([state["hist_set"], state["last_dt"]])
+            assert self._lib.oc_open_history(self._h, _p(hx), _p(hy), _p(sc), 1) == 0
 
     def open_ledger(self):
         out = np.zeros(3)
