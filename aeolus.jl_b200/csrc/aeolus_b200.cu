@@ -1197,6 +1197,28 @@ struct Core : CoreBase {
         const long long n = 8LL * (g.nz + 2 * AEO_H) * ((g.ny + 2 * AEO_H) + (g.nx + 2 * AEO_H));
         return (unsigned)((n + 255) / 256);
     }
+    // step_adaptive's keep of the radiated state (the planes, the boundary
+    // faces and the Orlanski history) before a step, written back before a retry
+    void* ob_kept[10] = {};
+    aeo_status ob_keep(bool back) {
+        const size_t ntx = (size_t)8 * (g.nz + 2 * AEO_H) * (g.ny + 2 * AEO_H), nty = (size_t)8 * (g.nz + 2 * AEO_H) * (g.nx + 2 * AEO_H);
+        void* live[10] = {ob.xp, ob.yp, ob.bw, ob.be, ob.bs, ob.bn, ob.xh, ob.yh, ob.hist_ok, ob.last_dt};
+        const size_t bytes[10] = {ob_nxp() * sizeof(R), ob_nyp() * sizeof(R), (size_t)g.ny * g.nz * sizeof(R),
+                                  (size_t)g.ny * g.nz * sizeof(R), (size_t)g.nx * g.nz * sizeof(R),
+                                  (size_t)g.nx * g.nz * sizeof(R), ntx * sizeof(R), nty * sizeof(R), sizeof(int),
+                                  sizeof(double)};
+        for (int q = 0; q < 10; ++q) {
+            if (!ob_kept[q]) {
+                unsigned char* b = nullptr;
+                if (aeo_status e = alloc(&b, bytes[q])) return e;
+                ob_kept[q] = b;
+            }
+            CK(cudaMemcpyAsync(back ? live[q] : ob_kept[q], back ? ob_kept[q] : live[q], bytes[q],
+                               cudaMemcpyDeviceToDevice, st));
+        }
+        return AEO_OK;
+    }
+
     size_t ob_nxp() const { return (size_t)8 * (g.nz + 2 * AEO_H) * (g.ny + 2 * AEO_H) * (AEO_H + 1); }
     size_t ob_nyp() const { return (size_t)8 * (g.nz + 2 * AEO_H) * (AEO_H + 1) * (g.nx + 2 * AEO_H); }
     aeo_status ob_prepare(int s_state) {
@@ -1829,10 +1851,6 @@ struct Core : CoreBase {
     // untouched) is kept and the step retried with half the dt.
     aeo_status step_adaptive(const aeo_cfl* c, int n, double* dt_prev_io, aeo_adaptive_stats* stats) override {
         if (aeo_status e = sgs_ready()) return e;
-        if (ob_rad) {   // a retry would have to rewind the radiated buffers too
-            fail("step_adaptive: not built with a radiating open face (step_rk3 with a chosen dt)");
-            return AEO_ERR_STATE;
-        }
         set_cfl(c);
         double dt_prev = (dt_prev_io && *dt_prev_io > 0) ? *dt_prev_io : 0.0;
         set_scalar_kernel<<<1, 1, 0, st>>>(&d_sc->dt_prev, dt_prev);
@@ -1842,6 +1860,9 @@ struct Core : CoreBase {
             // the closure's memory as committed before the step: a retry starts from it
             if (lag()) CK(cudaMemcpyAsync(d_lag_state + 2, d_lag_state, 2 * sizeof(int), cudaMemcpyDeviceToDevice, st));
             if (tke()) CK(cudaMemcpyAsync(d_tke_keep, d_tke, padded_count() * sizeof(R), cudaMemcpyDeviceToDevice, st));
+            // a radiating open set's planes and history: the step rewrites them in place
+            if (ob_rad)
+                if (aeo_status e = ob_keep(false)) return e;
             if (aeo_status e = launch_step(true)) return e;
             StepScalars h;
             if (aeo_status e = read_scalars(&h)) return e;
@@ -1867,6 +1888,8 @@ struct Core : CoreBase {
                     if (aeo_status e = lag_refresh()) return e;
                 }
                 if (tke()) CK(cudaMemcpyAsync(d_tke, d_tke_keep, padded_count() * sizeof(R), cudaMemcpyDeviceToDevice, st));
+                if (ob_rad)
+                    if (aeo_status e = ob_keep(true)) return e;
                 if (retries >= c->max_retries) {
                     fail(std::string("step_adaptive: step failed (") + (!fin ? "nonfinite" : (dv > c->divergence_tol ? "divergence" : "velocity")) +
                          ") after " + std::to_string(retries) + " retries; the state is the one before the step");

@@ -435,3 +435,59 @@ def test_restart_with_open_faces_continues_exactly(tmp_path, outflow):
     same, dropped = open_restart(Simulation, tmp_path, outflow)
     assert same
     assert dropped is None or dropped > 1e-9, dropped
+
+
+def radiating_domain(sim_cls):
+    g = regular_grid((64, 8, 8), (64.0, 8.0, 8.0), halo=(3, 3, 3), bc_z="wall")
+    obc = open_boundary_conditions(g, ProfileBoundaryData(u=1.0, v=0.1, w=0.0, theta=300.0), x="open", y="open",
+                                   outflow={"east": "orlanski", "north": "convective"})
+    s = sim_cls(CoreSpec(grid=g, nu=1e-3, theta0=300.0, advection="weno_js5", solver="pcg"))
+    s.set_pcg(None, tol=1e-12, maxit=500)
+    s.set_open_boundaries(obc)
+    th = np.full(g.storage_shape, 300.0)
+    th[g.interior] += np.exp(-((g.xnodes("c") - 40.0) / 4.0) ** 2)[None, None, :]
+    rng = np.random.default_rng(5)
+    v = g.zeros()
+    v[g.interior] = 0.1 + 0.05 * rng.standard_normal(v[g.interior].shape)
+    s.set_state(g.zeros() + 1.0, v, g.zeros(), th)
+    s.project()
+    return g, s
+
+
+@pytest.mark.gpu
+def test_adaptive_step_with_radiating_faces_matches_the_oracle_and_rewinds_a_retry():
+    # step_adaptive! over a radiating open set: the CFL pick and the steps
+    # match the oracle's; a step whose guard fails is retried from its start,
+    # the plane buffers, the boundary faces and the Orlanski history included,
+    # so a run that failed once continues exactly as one that never did
+    from aeolus_b200._lib import NumericalFailure
+    from aeolus_b200.simulation import CFLConstraints, Simulation
+    from oracle.oracle import OracleSimulation
+    g, s = radiating_domain(Simulation)
+    _, o = radiating_domain(OracleSimulation)
+    c = CFLConstraints(C_advective=0.5, growth_max=1.1)
+    dts_o = o.step_adaptive(c, 4)
+    dts, dp = [], None
+    for _ in range(4):
+        st = s.step_adaptive(c, 1, dp)
+        dts.append(st["dt"])
+        dp = st["dt"]
+        assert st["retries"] == 0
+    assert np.allclose(dts, dts_o, rtol=1e-11, atol=0), (dts, dts_o)
+    o.fill_halos()
+    errs = {n: rel_l2(s.get_field(n), o.get_field(n), g) for n in FIELDS}
+    assert all(e <= 1e-10 for e in errs.values()), errs
+    _, a = radiating_domain(Simulation)
+    _, b = radiating_domain(Simulation)
+    a.step_rk3(0.25, 3)
+    b.step_rk3(0.25, 3)
+    with pytest.raises(NumericalFailure):
+        a.step_adaptive(CFLConstraints(max_velocity=1e-3, max_retries=2), 1)
+    for x in (a, b):
+        x.step_adaptive(c, 3, 0.25)
+    for n in FIELDS + ("p",):
+        assert np.array_equal(a.get_field(n)[g.interior], b.get_field(n)[g.interior]), n
+    (xa, ya), (xb, yb) = a.open_planes(), b.open_planes()
+    (hx, hy, hz), (nx, ny, nz) = g.halo, g.size
+    assert np.array_equal(xa[:, :, hz:hz + nz, hy:hy + ny], xb[:, :, hz:hz + nz, hy:hy + ny])
+    assert np.array_equal(ya[:, :, hz:hz + nz, :, hx:hx + nx], yb[:, :, hz:hz + nz, :, hx:hx + nx])
